@@ -1,0 +1,130 @@
+/*
+ * gm1b.h - C ABI of the B200 (sm_100a) dynamical-core library libgm1b.so.
+ *
+ * Every entry point takes plain device pointers, sizes and scalars, enqueues
+ * its kernels on the given CUDA stream (a cudaStream_t passed as void*, NULL
+ * for the legacy default stream), returns without synchronising, and reports
+ * argument errors through its int32_t return value (GM1B_OK on success).
+ * The message of the last failure on the calling thread is available from
+ * gm1b_last_error().
+ *
+ * Arrays are float32, C order (z, y, x), with the padded shapes and names of
+ * the reference operator API:
+ *
+ *   scalar  (nk+2, nj+2, ni+2)   u (nk+2, nj+2, ni+1)
+ *   v       (nk+2, nj+1, ni+2)   w (nk+2, nj,   ni  )
+ *   dtu0    (nj+2, ni+1)         dtv0 (nj+1, ni+2)
+ *   uf, uh  (ni+2)               vf, vh (nj+2)
+ *
+ * (src/cm1core/cuda_sound3_periodic.py:449-491,
+ *  src/cm1core/cuda_psolver3_trajectory.py:93-126).
+ * The caller owns every array; the library allocates no device memory in
+ * these entry points.
+ */
+#ifndef GM1B_H
+#define GM1B_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GM1B_ABI_VERSION 1
+
+/* Return codes: 0 ok, negative = argument or launch error. */
+#define GM1B_OK 0
+#define GM1B_ERR_ARGUMENT (-1)
+#define GM1B_ERR_SCHEDULE (-2)
+#define GM1B_ERR_CUDA (-3)
+
+/* flags for the acoustic stage and the trajectory */
+/* Write the reference-semantics acoustic scratch outputs of the last small
+ * step (fpk, divh, hadvp, elim_c, elim_d, tri_aa, tri_bb, tri_cc, tri_dd,
+ * tri_pivot, tri_residual).  Without it those arrays are scratch. */
+#define GM1B_FLAG_SCRATCH_OUTPUTS 1u
+
+/* ablation bits of the dry trajectory
+ * (src/cm1core/cuda_psolver3_trajectory.py:429-436 TrajectoryAblations);
+ * a set bit DISABLES the term. */
+#define GM1B_ABLATE_MOMENTUM_ADVECTION 1u
+#define GM1B_ABLATE_SCALAR_ADVECTION 2u
+#define GM1B_ABLATE_BASE_THETA_ADVECTION 4u
+#define GM1B_ABLATE_BUOYANCY 8u
+#define GM1B_ABLATE_POST_STEP_PPX 16u
+#define GM1B_ABLATE_CARRIER_PROMOTION 32u
+
+/*
+ * Arrays of the serial-periodic flat lane.  Field order is the reference's
+ * ALL_ARRAY_NAMES order: the acoustic-stage arrays of
+ * src/cm1core/cuda_sound3_periodic.py:51-99 followed by the trajectory
+ * extras of src/cm1core/cuda_psolver3_trajectory.py:93-104.  The acoustic
+ * entry point ignores the trailing trajectory fields.
+ */
+typedef struct gm1b_periodic_arrays {
+    /* scalar shape */
+    float *mh, *rr0, *rf0, *c1, *c2, *mf, *piadv, *ppterm, *thv, *ppten;
+    float *ppi, *pp3d, *ppx, *ppd, *qk, *pk1, *pk2, *mm, *fpk, *divh;
+    float *hadvp, *elim_c, *elim_d, *tri_aa, *tri_bb, *tri_cc, *tri_dd;
+    float *tri_pivot, *tri_residual;
+    /* w shape */
+    float *wten, *wa, *w3d, *rrw;
+    /* u shape */
+    float *ua, *u3d, *uten, *rru;
+    /* v shape */
+    float *va, *v3d, *vten, *rrv;
+    /* metrics */
+    float *dtu0, *dtv0, *uf, *vf, *uh, *vh;
+    /* trajectory extras, scalar shape */
+    float *pi0, *rho0, *rrf0, *th0, *rth0, *tha, *th3d, *sadv, *thten, *divx;
+} gm1b_periodic_arrays;
+
+/* ABI version of the loaded library (GM1B_ABI_VERSION at build time). */
+int32_t gm1b_abi_version(void);
+
+/* Message of the last failed call on this thread ("" if none). */
+const char *gm1b_last_error(void);
+
+/*
+ * Small-step count and small time step of one RK stage.
+ * Replaces sound3_stage_schedule_f32 (src/cm1core/cuda_sound3_column.py:391-417):
+ * nsound must be even and >= 4, nrk in {1,2,3}.
+ */
+int32_t gm1b_sound3_stage_schedule(float dt, int32_t nsound, int32_t nrk,
+                                   int32_t *nloop, float *dts);
+
+/* RK stage time step dt/(4-nrk) in float32
+ * (src/cm1core/cuda_sound3_column.py:420-424).  Returns NaN for a bad nrk. */
+float gm1b_rk_stage_dt(float dt, int32_t nrk);
+
+/*
+ * Three psolver=3 acoustic RK stages (nrk = 1, 2, 3) of the serial-periodic
+ * flat lane on device arrays, in place.
+ * Replaces launch_cuda_sound3_periodic_three_stage
+ * (src/cm1core/cuda_sound3_periodic.py:1216) and its CPU twin
+ * cpu_sound3_periodic_three_stage_inplace (:1071).
+ */
+int32_t gm1b_sound3_periodic_three_stage(
+    int32_t ni, int32_t nj, int32_t nk, const gm1b_periodic_arrays *arrays,
+    float dt, int32_t nsound, float rdx, float rdy, float rdz, float cp,
+    float alph, float kdiv, uint32_t flags, void *stream);
+
+/*
+ * `steps` dry RK3 large steps of the flat serial-periodic rigid-lid
+ * trajectory (prepare, mass flux, divergence, fifth-order momentum advection
+ * with buoyancy, the psolver=3 acoustic stage, averaged-flux theta advection
+ * and update, ppx completion and carrier promotion), in place.
+ * Replaces launch_cuda_psolver3_trajectory
+ * (src/cm1core/cuda_psolver3_trajectory.py:1460) and its CPU twin
+ * cpu_psolver3_trajectory_inplace (:761).
+ */
+int32_t gm1b_psolver3_trajectory(
+    int32_t ni, int32_t nj, int32_t nk, const gm1b_periodic_arrays *arrays,
+    int32_t steps, float dt, int32_t nsound, float dx, float dy, float dz,
+    uint32_t ablations, uint32_t flags, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GM1B_H */

@@ -1,0 +1,227 @@
+"""Generate the golden vectors of tests/golden by running the REFERENCE itself.
+
+Run in a container where the reference source tree is present (it is read
+only, never copied):
+
+    python tests/golden/make_golden.py --reference /path/to/gm1 small
+    python tests/golden/make_golden.py --reference /path/to/gm1 c1 --steps 10
+
+``small`` writes compressed .npz fixtures of whole input/output array sets on
+small grids (operator-level raw-bit pins), ``c1`` writes SHA-256 digests of
+every array of the 64x64x40 dry bubble after 1 and after N large steps of the
+reference's CPU twin (a full-size pin that stays a few KB).  Inputs come from
+gm1_b200.initial_state, whose digests are stored too so a test can prove it
+rebuilt the same inputs.
+
+Reference entry points used (their CPU twins, single-threaded NumPy):
+  cpu_sound3_periodic_three_stage_inplace  src/cm1core/cuda_sound3_periodic.py:1071
+  cpu_psolver3_trajectory_inplace          src/cm1core/cuda_psolver3_trajectory.py:761
+"""
+
+from __future__ import annotations
+
+import argparse
+import copy
+import hashlib
+import json
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ROOT = HERE.parents[1]
+sys.path.insert(0, str(ROOT))
+
+from gm1_b200.arrays import (  # noqa: E402
+    ALL_ARRAY_NAMES,
+    SOUND_ARRAY_NAMES,
+    array_shapes,
+    default_periodic_face_weights,
+    fill_periodic_scalar_inplace,
+    fill_periodic_uv_inplace,
+)
+from gm1_b200.initial_state import DRY_BUBBLE_64, DryBubbleCase, dry_periodic_state  # noqa: E402
+
+ABLATION_FIELDS = (
+    "momentum_advection",
+    "scalar_advection",
+    "base_theta_advection",
+    "buoyancy",
+    "post_step_ppx",
+    "carrier_promotion",
+)
+
+# Small trajectory fixture: a 7x6x7 periodic box with a background wind and a
+# seeded smooth perturbation so both upwind branches of every flux occur.
+SMALL_CASE = DryBubbleCase(
+    ni=7, nj=6, nk=7, dx=1000.0, dy=1000.0, dz=500.0, dt=0.4, nsound=6,
+    bubble_radius_h=2500.0, bubble_radius_v=1500.0, bubble_center_z=1500.0,
+    noise_amplitude=0.05, seed=7, u0=2.0, v0=-0.7, wind_perturbation=1.5,
+)
+# A second shape with nsound=8 and a larger dt, uneven ni/nj.
+SMALL_CASE_B = DryBubbleCase(
+    ni=9, nj=5, nk=8, dx=800.0, dy=1200.0, dz=400.0, dt=3.0, nsound=8,
+    bubble_radius_h=3000.0, bubble_radius_v=1200.0, bubble_center_z=1000.0,
+    noise_amplitude=0.1, seed=11, u0=-3.0, v0=1.5, wind_perturbation=2.5,
+)
+
+
+def digest(a: np.ndarray) -> str:
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes(order="C")).hexdigest()
+
+
+def sound_fixture(ni: int, nj: int, nk: int, seed: int) -> dict[str, np.ndarray]:
+    """Horizontally varying acoustic-stage inputs satisfying the periodic
+    contract of src/cm1core/cuda_sound3_periodic.py:569-602."""
+    rng = np.random.default_rng(seed)
+    shapes = array_shapes(ni, nj, nk)
+    a = {name: np.zeros(shape, dtype=np.float32) for name, shape in shapes.items()}
+    a["dtu0"], a["dtv0"] = default_periodic_face_weights(ni, nj)
+    for name in ("uf", "vf", "uh", "vh"):
+        a[name].fill(np.float32(1.0))
+    z = (np.arange(nk + 2, dtype=np.float64) / (nk + 1))[:, None, None]
+    hx = np.sin(2 * np.pi * np.arange(ni + 2) / ni)[None, None, :]
+    hy = np.cos(2 * np.pi * np.arange(nj + 2) / nj)[None, :, None]
+    h = 0.6 * hx + 0.3 * hy
+    ones = np.ones((nk + 2, nj + 2, ni + 2))
+    a["mh"][...] = (1.0 + 0.02 * z * ones).astype(np.float32)
+    a["mf"][...] = (1.0 - 0.01 * z * ones).astype(np.float32)
+    a["rr0"][...] = (0.9 + 0.2 * z + 0.001 * h).astype(np.float32)
+    a["rf0"][...] = (1.1 - 0.15 * z + 0.001 * h).astype(np.float32)
+    a["c1"][...] = (0.4 + 0.1 * z * ones).astype(np.float32)
+    a["c2"][...] = (np.float32(1.0) - a["c1"]).astype(np.float32)
+    a["piadv"][...] = (1.0 - 0.05 * z + 2e-5 * h).astype(np.float32)
+    a["ppterm"][...] = (0.35 + 0.01 * z + 1e-4 * h).astype(np.float32)
+    a["thv"][...] = (300.0 + 8.0 * z + 0.2 * h).astype(np.float32)
+    a["ppten"][...] = (1e-6 * h + 5e-7 * z).astype(np.float32)
+    pressure = (2e-4 * h + 4e-5 * z).astype(np.float32)
+    a["ppi"][...] = pressure
+    a["ppx"][...] = (0.2 * pressure + 1e-6 * z).astype(np.float32)
+    for name in ("mh", "rr0", "rf0", "c1", "c2", "mf", "piadv", "ppterm", "thv", "ppten", "ppi", "ppx"):
+        fill_periodic_scalar_inplace(a[name], ni=ni, nj=nj, nk=nk)
+    a["ua"][1 : nk + 1, 1 : nj + 1, :] = rng.uniform(-3, 3, size=(nk, nj, ni + 1)).astype(np.float32)
+    a["ua"][1 : nk + 1, 1 : nj + 1, ni] = a["ua"][1 : nk + 1, 1 : nj + 1, 0]
+    a["va"][1 : nk + 1, :, 1 : ni + 1] = rng.uniform(-3, 3, size=(nk, nj + 1, ni)).astype(np.float32)
+    a["va"][1 : nk + 1, nj, 1 : ni + 1] = a["va"][1 : nk + 1, 0, 1 : ni + 1]
+    fill_periodic_uv_inplace(a["ua"], a["va"], ni=ni, nj=nj, nk=nk)
+    a["wa"][2 : nk + 1] = rng.uniform(-0.3, 0.3, size=(nk - 1, nj, ni)).astype(np.float32)
+    a["uten"][1 : nk + 1, 1 : nj + 1, :] = rng.uniform(-1e-3, 1e-3, size=(nk, nj, ni + 1)).astype(np.float32)
+    a["vten"][1 : nk + 1, :, 1 : ni + 1] = rng.uniform(-1e-3, 1e-3, size=(nk, nj + 1, ni)).astype(np.float32)
+    a["wten"][2 : nk + 1] = rng.uniform(-1e-2, 1e-2, size=(nk - 1, nj, ni)).astype(np.float32)
+    np.copyto(a["u3d"], a["ua"])
+    np.copyto(a["v3d"], a["va"])
+    np.copyto(a["w3d"], a["wa"])
+    np.copyto(a["pp3d"], a["ppi"])
+    return a
+
+
+def make_small(reference: Path) -> None:
+    sys.path.insert(0, str(reference / "src"))
+    from cm1core.cuda_psolver3_trajectory import (
+        TrajectoryAblations,
+        cpu_psolver3_trajectory_inplace,
+    )
+    from cm1core.cuda_sound3_column import sound3_stage_schedule_f32
+    from cm1core.cuda_sound3_periodic import cpu_sound3_periodic_three_stage_inplace
+
+    # 1. acoustic operator, three stages, two shapes
+    for tag, (ni, nj, nk, seed, dt, nsound) in {
+        "sound3_5x4x7": (5, 4, 7, 3, 2.0, 6),
+        "sound3_8x6x12": (8, 6, 12, 5, 4.0, 10),
+    }.items():
+        a = sound_fixture(ni, nj, nk, seed)
+        inputs = {f"in_{k}": v.copy() for k, v in a.items()}
+        params = dict(ni=ni, nj=nj, nk=nk, dt=dt, nsound=nsound, rdx=1.0 / 1000.0, rdy=1.0 / 900.0, rdz=1.0 / 450.0)
+        result = cpu_sound3_periodic_three_stage_inplace(a, **params)
+        outputs = {f"out_{k}": v for k, v in a.items()}
+        meta = dict(params, nloop=[s.nloop for s in result.cadence], dts=[s.dts_f32 for s in result.cadence])
+        np.savez_compressed(HERE / f"{tag}.npz", meta=json.dumps(meta), **inputs, **outputs)
+        print("wrote", tag)
+
+    # 2. dry trajectory, two cases, 3 steps each
+    for tag, case, steps in (("traj_7x6x7", SMALL_CASE, 3), ("traj_9x5x8", SMALL_CASE_B, 2)):
+        a = dry_periodic_state(case)
+        inputs = {f"in_{k}": v.copy() for k, v in a.items()}
+        params = dict(ni=case.ni, nj=case.nj, nk=case.nk, dt=case.dt, nsound=case.nsound,
+                      dx=case.dx, dy=case.dy, dz=case.dz)
+        result = cpu_psolver3_trajectory_inplace(a, steps=steps, **params)
+        outputs = {f"out_{k}": v for k, v in a.items()}
+        cadence = [
+            dict(large_step=c.large_step, nrk=c.nrk, nloop=c.nloop, dts=c.dts_f32, dttmp=c.dttmp_f32,
+                 max_tridiagonal_residual=c.max_tridiagonal_residual,
+                 horizontal_mass_flux_sum=c.horizontal_mass_flux_sum,
+                 total_mass_flux_divergence_sum=c.total_mass_flux_divergence_sum,
+                 rigid=c.rigid_w_boundary_exact)
+            for c in result.cadence
+        ]
+        meta = dict(params, steps=steps, cadence=cadence, ledgers=list(result.ledgers))
+        np.savez_compressed(HERE / f"{tag}.npz", meta=json.dumps(meta), **inputs, **outputs)
+        print("wrote", tag)
+
+    # 3. ablations: digests of every array after one step with each term off
+    case = SMALL_CASE
+    params = dict(ni=case.ni, nj=case.nj, nk=case.nk, dt=case.dt, nsound=case.nsound,
+                  dx=case.dx, dy=case.dy, dz=case.dz)
+    record = {}
+    for bit, field in enumerate(ABLATION_FIELDS):
+        a = dry_periodic_state(case)
+        cpu_psolver3_trajectory_inplace(a, steps=1, ablations=TrajectoryAblations(**{field: False}), **params)
+        record[field] = {"mask": 1 << bit, "digests": {n: digest(a[n]) for n in ALL_ARRAY_NAMES}}
+    (HERE / "traj_ablations_7x6x7.json").write_text(json.dumps(record, indent=1, sort_keys=True))
+    print("wrote ablations")
+
+    # 4. schedule table
+    table = []
+    for dt in (0.4, 2.0, 3.0, 5.0, 6.0, 0.6, 1.0, 7.3):
+        for nsound in (4, 6, 8, 10, 12, 16):
+            for nrk in (1, 2, 3):
+                n, d = sound3_stage_schedule_f32(dt, nsound, nrk)
+                table.append([dt, nsound, nrk, n, float(np.float32(d))])
+    (HERE / "schedule.json").write_text(json.dumps(table))
+    print("wrote schedule")
+
+
+def make_c1(reference: Path, steps: int, checkpoints: list[int]) -> None:
+    sys.path.insert(0, str(reference / "src"))
+    from cm1core.cuda_psolver3_trajectory import cpu_psolver3_trajectory_inplace
+
+    case = DRY_BUBBLE_64
+    a = dry_periodic_state(case)
+    record = {
+        "case": "dry bubble 64x64x40 (dx=dy=1 km, dz=500 m, dt=6 s, nsound=6)",
+        "input_digests": {n: digest(a[n]) for n in ALL_ARRAY_NAMES},
+        "steps": {},
+    }
+    params = dict(ni=case.ni, nj=case.nj, nk=case.nk, dt=case.dt, nsound=case.nsound,
+                  dx=case.dx, dy=case.dy, dz=case.dz)
+    out = HERE / "traj_c1_digests.json"
+    t0 = time.time()
+    for step in range(1, steps + 1):
+        result = cpu_psolver3_trajectory_inplace(a, steps=1, **params)
+        if step in checkpoints:
+            record["steps"][str(step)] = {
+                "digests": {n: digest(a[n]) for n in ALL_ARRAY_NAMES},
+                "max_abs": {n: float(np.max(np.abs(a[n]))) for n in ("u3d", "v3d", "w3d", "pp3d", "th3d")},
+                "max_tridiagonal_residual": max(c.max_tridiagonal_residual for c in result.cadence),
+                "reference_cpu_seconds_total": time.time() - t0,
+            }
+            out.write_text(json.dumps(record, indent=1, sort_keys=True))
+            print("checkpoint", step, time.time() - t0, flush=True)
+
+
+def main() -> None:
+    p = argparse.ArgumentParser()
+    p.add_argument("--reference", type=Path, required=True, help="root of the reference source tree")
+    p.add_argument("what", choices=("small", "c1"))
+    p.add_argument("--steps", type=int, default=1)
+    args = p.parse_args()
+    if args.what == "small":
+        make_small(args.reference)
+    else:
+        make_c1(args.reference, args.steps, sorted({1, args.steps}))
+
+
+if __name__ == "__main__":
+    main()
