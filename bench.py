@@ -1,0 +1,374 @@
+#!/usr/bin/env python
+"""Throughput of the RK3 large step on B200: cell-updates/s.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Workload: the dry warm bubble on the flat serial-periodic lane, 64x64x40
+cells (dx = dy = 1 km, dz = 500 m, dt = 6 s, nsound = 6, so 2 + 3 + 6 = 11
+acoustic small steps per large step), seeded synthetic initial state.  One
+"step" is one full RK3 large step (three stages: prepare, mass flux,
+momentum advection with buoyancy, the psolver=3 acoustic stage, theta
+advection and update; then ppx completion and carrier promotion) through the
+library's C ABI.  Inputs are device resident; the step is captured once as a
+CUDA graph and replayed; L2 is flushed (a 256 MiB write) before every timed
+step, outside its event pair.  Under torchrun every rank runs its own replica
+(weak scaling, no collective on the data path) and the job time is the max
+over ranks.
+
+Also measured: e2e (the same steps through the public Python API with the
+prognostic arrays copied from pinned host memory before and back after every
+step), the per-kernel device time of each kernel (library launch profiler,
+CUDA events on the launching stream) for the roofline of the dominant kernel,
+and the CPU oracle on the host cores as the CPU baseline.
+
+--impl reference times the reference algorithm's CPU implementation on the
+host cores: the C restatement of the reference's NumPy twins in oracle/
+(bit-identical to them; the reference itself is Python/CuPy and cannot run on
+the GPU box), with all host threads, on the same workload and metric.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "cell-updates/s per RK3 step (fwd, adjoint, ensemble) and % of HBM roofline"
+UNIT = "cell-updates/s"
+WORKLOAD = "dry periodic RK3 trajectory, warm bubble 64x64x40 (dx=dy=1 km, dz=500 m, dt=6 s, nsound=6)"
+
+# Algorithmic bytes of one full RK3 large step per cell-update for this
+# workload (dry, nsound = 6: 3*(8+6) + 20*11 + 2 = 264 words = 1,056 B).
+STEP_BYTES_PER_CELL = 1056
+
+# Algorithmic words per cell of one launch of each kernel: every full field
+# the launch must read or write once (stencil re-reads, halo words and
+# horizontally uniform 1-D profiles are not counted; 3-D base-state arrays
+# that the API passes as full fields are counted once).
+KERNEL_WORDS_PER_CELL = {
+    # in: u v w th3d pp3d th0 pi0 rho0 rf0; out: thv piadv ppterm rru rrv rrw divx
+    "traj_prepare_kernel": 16,
+    # in: u v w rru rrv rrw divx th3d c1 c2 rr0 rrf0 rth0; out: uten vten wten
+    "traj_momentum_kernel": 16,
+    # in: ppx ppi ua va wa mh rr0 rf0 mf c1 c2 piadv thv ppterm; out: ppd pp3d u3d v3d w3d rru rrv rrw qk pk1 pk2 mm
+    "sound_prep_kernel": 26,
+    # in+out: u v rru rrv; in: ppd thv uten vten
+    "sound_uv_kernel": 12,
+    # in: u v piadv ppterm ppten qk pk1 pk2 mm wten; in+out: w pp3d rrw; out: ppd
+    "sound_column_kernel": 17,
+    # in+out: rru rrv rrw; in: th3d th0; out: sadv
+    "traj_theta_prep_kernel": 9,
+    # in: rru rrv rrw sadv tha c1 c2 rr0; out: divx thten th3d
+    "traj_theta_kernel": 11,
+}
+
+PROGNOSTIC = ("ua", "u3d", "va", "v3d", "wa", "w3d", "ppi", "pp3d", "ppx", "tha", "th3d")
+
+
+def load_peaks() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except Exception:  # noqa: BLE001
+            pass
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+        self.thread = None
+
+    def start(self) -> None:
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.index)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self) -> None:
+        assert self.proc is not None and self.proc.stdout is not None
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread is not None:
+            self.thread.join(timeout=5)
+        sm, smax, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in self.lines:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_step_rate(steps_min: int, seconds_target: float, threads: int) -> dict:
+    """Time the CPU oracle on the workload on the host cores."""
+    from gm1_b200.initial_state import DRY_BUBBLE_64, dry_periodic_state
+    from oracle import periodic as orc
+
+    c = DRY_BUBBLE_64
+    orc.set_threads(threads)
+    a = dry_periodic_state(c)
+    p = dict(ni=c.ni, nj=c.nj, nk=c.nk, steps=1, dt=c.dt, nsound=c.nsound, dx=c.dx, dy=c.dy, dz=c.dz)
+    orc.traj_steps(a, **p)  # warm-up
+    n = 0
+    t0 = time.perf_counter()
+    while n < steps_min or time.perf_counter() - t0 < seconds_target:
+        orc.traj_steps(a, **p)
+        n += 1
+    dt = time.perf_counter() - t0
+    return {"value": c.cells * n / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{n} RK3 large steps of the full 64x64x40 domain in {dt:.2f} s "
+                      f"(C restatement of the reference NumPy twins, bit-identical to them)"}
+
+
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    from gm1_b200.initial_state import DRY_BUBBLE_64, dry_periodic_state
+    from oracle import periodic as orc
+
+    c = DRY_BUBBLE_64
+    orc.set_threads(threads)
+    a = dry_periodic_state(c)
+    p = dict(ni=c.ni, nj=c.nj, nk=c.nk, steps=1, dt=c.dt, nsound=c.nsound, dx=c.dx, dy=c.dy, dz=c.dz)
+    for _ in range(args.warmup):
+        orc.traj_steps(a, **p)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        orc.traj_steps(a, **p)
+    dt = time.perf_counter() - t0
+    value = c.cells * args.steps / dt
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded dry warm bubble)",
+        "config": {"workload": WORKLOAD, "cells": c.cells, "device": "host CPU"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} timed RK3 large steps of the full domain after {args.warmup} "
+                                   "warm-up steps (C restatement of the reference NumPy twins)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    from gm1_b200 import _native
+    from gm1_b200.initial_state import DRY_BUBBLE_64, dry_periodic_state
+    from gm1_b200.periodic import launch_cuda_psolver3_trajectory, to_device
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=device)
+
+    c = DRY_BUBBLE_64
+    host = dry_periodic_state(c)
+    dev = to_device(host, device)
+    p = dict(ni=c.ni, nj=c.nj, nk=c.nk, steps=1, dt=c.dt, nsound=c.nsound, dx=c.dx, dy=c.dy, dz=c.dz,
+             scratch_outputs=False)
+    stream = torch.cuda.Stream(device)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
+
+    def barrier():
+        torch.cuda.synchronize(device)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(device)
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            launch_cuda_psolver3_trajectory(dev, stream=stream, **p)
+        stream.synchronize()
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, stream=stream):
+            launch_cuda_psolver3_trajectory(dev, stream=stream, **p)
+        for _ in range(args.warmup):
+            graph.replay()
+        stream.synchronize()
+
+    # ---- timed region: K graph replays, L2 flushed before each ----------
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    sampler = ClockSampler(local)
+    barrier()
+    sampler.start()
+    with torch.cuda.stream(stream):
+        for q in range(args.steps):
+            flush.zero_()
+            starts[q].record(stream)
+            graph.replay()
+            ends[q].record(stream)
+    barrier()
+    clocks = sampler.stop()
+    local_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+    total_ms = max_over_ranks(local_ms)
+    ms_per_step = total_ms / args.steps
+    value = world * c.cells * args.steps / (total_ms * 1e-3)
+
+    # ---- per-kernel device time (same steps, no graph, profiler on) ------
+    _native.profiler_enable(True)
+    with torch.cuda.stream(stream):
+        for _ in range(args.steps):
+            flush.zero_()
+            launch_cuda_psolver3_trajectory(dev, stream=stream, **p)
+    stream.synchronize()
+    _native.profiler_enable(False)
+    stats = _native.profiler_collect()
+    launches_per_step = sum(s["launches"] for s in stats) / args.steps
+    top = stats[0]
+    avg_ms = top["total_ms"] / top["launches"]
+    alg_bytes = KERNEL_WORDS_PER_CELL[top["name"]] * 4 * c.cells
+    peak, peak_kind = load_peaks()
+    achieved = alg_bytes / (avg_ms * 1e-3) / 1e9
+    traffic = None
+    tfile = ROOT / "profiles" / "traffic_per_launch.json"
+    if tfile.exists():
+        traffic = json.loads(tfile.read_text()).get(top["name"])
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "kernel": top["name"], "avg_launch_ms": avg_ms,
+                "alg_bytes_per_launch": alg_bytes, "peak_source": f"{peak_kind} hbm_gbs"}
+    kernel_share = {s["name"]: round(s["total_ms"] / sum(x["total_ms"] for x in stats), 4) for s in stats}
+
+    # ---- e2e through the public API with pinned host buffers -------------
+    pinned = {n: torch.from_numpy(host[n]).pin_memory() for n in PROGNOSTIC}
+    h2d = sum(t.numel() * 4 for t in pinned.values())
+    e_start = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    e_end = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    pe = dict(p)
+    barrier()
+    with torch.cuda.stream(stream):
+        for q in range(args.steps):
+            flush.zero_()
+            e_start[q].record(stream)
+            for n, t in pinned.items():
+                dev[n].copy_(t, non_blocking=True)
+            launch_cuda_psolver3_trajectory(dev, stream=stream, **pe)
+            for n, t in pinned.items():
+                t.copy_(dev[n], non_blocking=True)
+            e_end[q].record(stream)
+    barrier()
+    e2e_ms = max_over_ranks(sum(s.elapsed_time(e) for s, e in zip(e_start, e_end)))
+    e2e_value = world * c.cells * args.steps / (e2e_ms * 1e-3)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_step_rate(3, 10.0, os.cpu_count() or 1)
+
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_per_step,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded dry warm bubble, numpy default_rng(1) noise)",
+        "config": {
+            "workload": WORKLOAD,
+            "mode": "fwd",
+            "cells": c.cells,
+            "large_steps_per_timed_step": 1,
+            "acoustic_small_steps_per_step": 11,
+            "l2": "flushed before every timed step (256 MiB write, outside the event pair)",
+            "cuda_graph": True,
+            "parallelism": f"replicas x{world}" if world > 1 else "single domain",
+        },
+        "step_roofline": {"bytes_per_cell_update": STEP_BYTES_PER_CELL,
+                          "achieved_gbs": STEP_BYTES_PER_CELL * value / world / 1e9,
+                          "frac": STEP_BYTES_PER_CELL * value / world / 1e9 / peak},
+        "roofline": roofline,
+        "kernel_share": kernel_share,
+        "gpu_launches": int(round(launches_per_step * args.steps)),
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d},
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -32,6 +32,12 @@ extern "C" {
 
 #define GM1B_ABI_VERSION 1
 
+#if defined(__GNUC__)
+#define GM1B_API __attribute__((visibility("default")))
+#else
+#define GM1B_API
+#endif
+
 /* Return codes: 0 ok, negative = argument or launch error. */
 #define GM1B_OK 0
 #define GM1B_ERR_ARGUMENT (-1)
@@ -80,22 +86,22 @@ typedef struct gm1b_periodic_arrays {
 } gm1b_periodic_arrays;
 
 /* ABI version of the loaded library (GM1B_ABI_VERSION at build time). */
-int32_t gm1b_abi_version(void);
+GM1B_API int32_t gm1b_abi_version(void);
 
 /* Message of the last failed call on this thread ("" if none). */
-const char *gm1b_last_error(void);
+GM1B_API const char *gm1b_last_error(void);
 
 /*
  * Small-step count and small time step of one RK stage.
  * Replaces sound3_stage_schedule_f32 (src/cm1core/cuda_sound3_column.py:391-417):
  * nsound must be even and >= 4, nrk in {1,2,3}.
  */
-int32_t gm1b_sound3_stage_schedule(float dt, int32_t nsound, int32_t nrk,
+GM1B_API int32_t gm1b_sound3_stage_schedule(float dt, int32_t nsound, int32_t nrk,
                                    int32_t *nloop, float *dts);
 
 /* RK stage time step dt/(4-nrk) in float32
  * (src/cm1core/cuda_sound3_column.py:420-424).  Returns NaN for a bad nrk. */
-float gm1b_rk_stage_dt(float dt, int32_t nrk);
+GM1B_API float gm1b_rk_stage_dt(float dt, int32_t nrk);
 
 /*
  * Three psolver=3 acoustic RK stages (nrk = 1, 2, 3) of the serial-periodic
@@ -104,7 +110,7 @@ float gm1b_rk_stage_dt(float dt, int32_t nrk);
  * (src/cm1core/cuda_sound3_periodic.py:1216) and its CPU twin
  * cpu_sound3_periodic_three_stage_inplace (:1071).
  */
-int32_t gm1b_sound3_periodic_three_stage(
+GM1B_API int32_t gm1b_sound3_periodic_three_stage(
     int32_t ni, int32_t nj, int32_t nk, const gm1b_periodic_arrays *arrays,
     float dt, int32_t nsound, float rdx, float rdy, float rdz, float cp,
     float alph, float kdiv, uint32_t flags, void *stream);
@@ -118,10 +124,29 @@ int32_t gm1b_sound3_periodic_three_stage(
  * (src/cm1core/cuda_psolver3_trajectory.py:1460) and its CPU twin
  * cpu_psolver3_trajectory_inplace (:761).
  */
-int32_t gm1b_psolver3_trajectory(
+GM1B_API int32_t gm1b_psolver3_trajectory(
     int32_t ni, int32_t nj, int32_t nk, const gm1b_periodic_arrays *arrays,
     int32_t steps, float dt, int32_t nsound, float dx, float dy, float dz,
     uint32_t ablations, uint32_t flags, void *stream);
+
+
+/*
+ * Launch profiler.  While enabled, every kernel launch of the library is
+ * bracketed by a pair of CUDA events recorded on its own stream (the
+ * per-phase device timing of src/cm1core/runtime_profiler.py:1-48, per
+ * kernel).  gm1b_profiler_collect waits for the recorded events, returns
+ * per-kernel launch counts and total device milliseconds (sorted by total,
+ * descending) and clears the record.  Events are created once and reused;
+ * no device memory is allocated.
+ */
+typedef struct gm1b_kernel_stat {
+    char name[48];
+    int32_t launches;
+    double total_ms;
+} gm1b_kernel_stat;
+
+GM1B_API int32_t gm1b_profiler_enable(int32_t on);
+GM1B_API int32_t gm1b_profiler_collect(gm1b_kernel_stat *out, int32_t capacity, int32_t *count);
 
 #ifdef __cplusplus
 }
