@@ -4,7 +4,7 @@ Run in a container where the reference source tree is present (it is read
 only, never copied):
 
     python tests/golden/make_golden.py --reference /path/to/gm1 small
-    python tests/golden/make_golden.py --reference /path/to/gm1 c1 --steps 10
+    python tests/golden/make_golden.py --reference /path/to/gm1 c1 --checkpoints 1 10
 
 ``small`` writes compressed .npz fixtures of whole input/output array sets on
 small grids (operator-level raw-bit pins), ``c1`` writes SHA-256 digests of
@@ -183,44 +183,49 @@ def make_small(reference: Path) -> None:
     print("wrote schedule")
 
 
-def make_c1(reference: Path, steps: int, checkpoints: list[int]) -> None:
+def make_c1(reference: Path, checkpoints: list[int]) -> None:
+    """Digests after each checkpoint N, each from a fresh state with one call
+    of steps=N (the reference refuses a non-fresh entry state, ppx != pp3d,
+    src/cm1core/cuda_psolver3_trajectory.py:242-246).  Checkpoints already in
+    the output file are kept."""
     sys.path.insert(0, str(reference / "src"))
     from cm1core.cuda_psolver3_trajectory import cpu_psolver3_trajectory_inplace
 
     case = DRY_BUBBLE_64
-    a = dry_periodic_state(case)
-    record = {
-        "case": "dry bubble 64x64x40 (dx=dy=1 km, dz=500 m, dt=6 s, nsound=6)",
-        "input_digests": {n: digest(a[n]) for n in ALL_ARRAY_NAMES},
-        "steps": {},
-    }
+    out = HERE / "traj_c1_digests.json"
+    fresh = dry_periodic_state(case)
+    record = json.loads(out.read_text()) if out.exists() else {}
+    record["case"] = "dry bubble 64x64x40 (dx=dy=1 km, dz=500 m, dt=6 s, nsound=6)"
+    record["input_digests"] = {n: digest(fresh[n]) for n in ALL_ARRAY_NAMES}
+    record.setdefault("steps", {})
     params = dict(ni=case.ni, nj=case.nj, nk=case.nk, dt=case.dt, nsound=case.nsound,
                   dx=case.dx, dy=case.dy, dz=case.dz)
-    out = HERE / "traj_c1_digests.json"
-    t0 = time.time()
-    for step in range(1, steps + 1):
-        result = cpu_psolver3_trajectory_inplace(a, steps=1, **params)
-        if step in checkpoints:
-            record["steps"][str(step)] = {
-                "digests": {n: digest(a[n]) for n in ALL_ARRAY_NAMES},
-                "max_abs": {n: float(np.max(np.abs(a[n]))) for n in ("u3d", "v3d", "w3d", "pp3d", "th3d")},
-                "max_tridiagonal_residual": max(c.max_tridiagonal_residual for c in result.cadence),
-                "reference_cpu_seconds_total": time.time() - t0,
-            }
-            out.write_text(json.dumps(record, indent=1, sort_keys=True))
-            print("checkpoint", step, time.time() - t0, flush=True)
+    for n in checkpoints:
+        if str(n) in record["steps"]:
+            continue
+        a = copy.deepcopy(fresh)
+        t0 = time.time()
+        result = cpu_psolver3_trajectory_inplace(a, steps=n, **params)
+        record["steps"][str(n)] = {
+            "digests": {name: digest(a[name]) for name in ALL_ARRAY_NAMES},
+            "max_abs": {name: float(np.max(np.abs(a[name]))) for name in ("u3d", "v3d", "w3d", "pp3d", "th3d")},
+            "max_tridiagonal_residual": max(c.max_tridiagonal_residual for c in result.cadence),
+            "reference_cpu_seconds": time.time() - t0,
+        }
+        out.write_text(json.dumps(record, indent=1, sort_keys=True))
+        print("checkpoint", n, time.time() - t0, flush=True)
 
 
 def main() -> None:
     p = argparse.ArgumentParser()
     p.add_argument("--reference", type=Path, required=True, help="root of the reference source tree")
     p.add_argument("what", choices=("small", "c1"))
-    p.add_argument("--steps", type=int, default=1)
+    p.add_argument("--checkpoints", type=int, nargs="+", default=[1])
     args = p.parse_args()
     if args.what == "small":
         make_small(args.reference)
     else:
-        make_c1(args.reference, args.steps, sorted({1, args.steps}))
+        make_c1(args.reference, sorted(set(args.checkpoints)))
 
 
 if __name__ == "__main__":
