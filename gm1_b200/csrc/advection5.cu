@@ -1,0 +1,423 @@
+// advection5.cu - sm_100a kernels of the padded (ng = 3) lane: terrain mass
+// flux with its divergence, and fifth-order / WENO5 scalar advection.
+//
+// Behaviour followed (reference file:line):
+//   cpu_terrain_mass_flux5_inplace   src/cm1core/cuda_advection5.py:271-437
+//   cpu_scalar_advection5_inplace    src/cm1core/cuda_advection5.py:440-579
+//   lateral-side tendency of the reference kernel
+//   cm1_adv5_scalar_tendency_v1      src/cm1core/cuda_advection5.py:669
+//
+// Design (B200): the scalar advection is ONE fused pass.  A CTA owns a 32x4
+// column tile and marches up a chunk of levels: at each level the x and y
+// face fluxes of the tile (33 x 4 and 32 x 5 faces) are formed once into
+// shared memory, the vertical flux of the upper face is formed in a register
+// and carried to the next level as the lower face, and the tendency is
+// written.  The face-flux scratch arrays of the reference (three passes
+// through HBM) are optional outputs here.  WENO smoothness weights are
+// binary64 as in the reference.
+#include "gm1b_common.cuh"
+
+namespace gm1b {
+namespace {
+
+constexpr int NG = 3;
+constexpr int kAX = 32;  // tile x
+constexpr int kAY = 4;   // tile y
+
+constexpr float kC13_12 = 0x1.155556p+0f;
+constexpr float kCm7_6 = -0x1.2aaaaap+0f;
+constexpr float kC11_6 = 0x1.d55556p+0f;
+constexpr float kC1_6 = 0x1.555556p-3f;
+// largest binary32 below 1e-20: |x| < 1e-20 (binary64 test of the reference
+// twin) is |x| <= this for every binary32 x
+constexpr float kDivClamp = 0x1.79ca1p-67f;
+
+struct PaddedDims {
+    int ni, nj, nk;
+    __host__ __device__ __forceinline__ size_t s(int k, int y, int x) const {
+        return ((size_t)k * (nj + 2 * NG) + (size_t)y) * (size_t)(ni + 2 * NG) + (size_t)x;
+    }
+    __host__ __device__ __forceinline__ size_t u(int k, int y, int x) const {
+        return ((size_t)k * (nj + 2 * NG) + (size_t)y) * (size_t)(ni + 1 + 2 * NG) + (size_t)x;
+    }
+    __host__ __device__ __forceinline__ size_t v(int k, int y, int x) const {
+        return ((size_t)k * (nj + 1 + 2 * NG) + (size_t)y) * (size_t)(ni + 2 * NG) + (size_t)x;
+    }
+    __host__ __device__ __forceinline__ size_t c(int k, int j, int i) const {  // (nk', nj, ni)
+        return ((size_t)k * nj + (size_t)j) * (size_t)ni + (size_t)i;
+    }
+};
+
+__device__ __forceinline__ double dmin30(double x) { return x < 1.0e30 ? x : 1.0e30; }
+
+__device__ __forceinline__ float weno5(float s1, float s2, float s3, float s4, float s5, double eps) {
+    const float d1 = (s1 - 2.0f * s2) + s3;
+    const float e1 = (s1 - 4.0f * s2) + 3.0f * s3;
+    const float b1r = kC13_12 * (d1 * d1) + 0.25f * (e1 * e1);
+    const float d2 = (s2 - 2.0f * s3) + s4;
+    const float e2 = s2 - s4;
+    const float b2r = kC13_12 * (d2 * d2) + 0.25f * (e2 * e2);
+    const float d3 = (s3 - 2.0f * s4) + s5;
+    const float e3 = (3.0f * s3 - 4.0f * s4) + s5;
+    const float b3r = kC13_12 * (d3 * d3) + 0.25f * (e3 * e3);
+    const double b1 = b1r, b2 = b2r, b3 = b3r;
+    const double tau = fabs(b1 - b3);
+    const double q1 = dmin30(tau / (b1 + eps));
+    const double q2 = dmin30(tau / (b2 + eps));
+    const double q3 = dmin30(tau / (b3 + eps));
+    const double w1 = (double)0.1f * (1.0 + q1 * q1);
+    const double w2 = (double)0.6f * (1.0 + q2 * q2);
+    const double w3 = (double)0.3f * (1.0 + q3 * q3);
+    const float p1 = (kF3_3 * s1 + kCm7_6 * s2) + kC11_6 * s3;
+    const float p2 = (kF3_1 * s2 + kF3_2 * s3) + kF3_3 * s4;
+    const float p3 = (kF3_3 * s3 + kF3_2 * s4) + kF3_1 * s5;
+    return (float)((w1 * (double)p1 + w2 * (double)p2 + w3 * (double)p3) / (w1 + w2 + w3));
+}
+
+__device__ __forceinline__ float upstrpd(float s1, float s2, float s3, float weps) {
+    const float dd = s2 - s1;
+    const float se = copysignf(fabsf(weps), dd);
+    const float rr = (s3 - s2) / (se + dd);
+    const float cand = kC1_6 + kF3_3 * rr;
+    const float phi = fmaxf(0.0f, fminf(rr, fminf(cand, 1.0f)));
+    return s2 + phi * (s2 - s1);
+}
+
+template <bool WENO>
+__device__ __forceinline__ float recon(float s1, float s2, float s3, float s4, float s5, double eps) {
+    if (WENO) return weno5(s1, s2, s3, s4, s5, eps);
+    return flx5(s1, s2, s3, s4, s5);
+}
+
+// ---------------------------------------------------------------------------
+// terrain mass flux, part 1: interior horizontal faces, zero rrw lid/floor
+// grid (x over i in 0..ni-1, y over j in 0..nj-1, z over k = 1..nk)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kAX *kAY)
+    mass_flux_horizontal_kernel(gm1b_mass_flux5_arrays a, PaddedDims d) {
+    const int i = blockIdx.x * kAX + threadIdx.x;
+    const int j = blockIdx.y * kAY + threadIdx.y;
+    const int k = blockIdx.z + 1;
+    const int ni = d.ni, nj = d.nj, nk = d.nk;
+    if (i >= ni || j >= nj) return;
+    const int y = j + NG, x = i + NG;
+    if (i >= 1) {
+        const float density = a.rho0_3d[d.c(k - 1, j, i - 1)] + a.rho0_3d[d.c(k - 1, j, i)];
+        a.rru[d.u(k, y, x)] = (0.5f * density) * (a.u3d[d.u(k, y, x)] * a.rgzu[(size_t)j * (ni + 1) + i]);
+    }
+    if (j >= 1) {
+        const float density = a.rho0_3d[d.c(k - 1, j - 1, i)] + a.rho0_3d[d.c(k - 1, j, i)];
+        a.rrv[d.v(k, y, x)] = (0.5f * density) * (a.v3d[d.v(k, y, x)] * a.rgzv[(size_t)j * ni + i]);
+    }
+    if (k == 1) {
+        a.rrw[d.s(1, y, x)] = 0.0f;
+        a.rrw[d.s(nk + 1, y, x)] = 0.0f;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// terrain mass flux, part 2: one thread per interior column marches up k,
+// forming rrw(k) (terrain term included) and the divergence of level k-1
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kAX *kAY)
+    mass_flux_column_kernel(gm1b_mass_flux5_arrays a, PaddedDims d, float dz, float rdx, float rdy) {
+    const int i = blockIdx.x * kAX + threadIdx.x + 1;
+    const int j = blockIdx.y * kAY + threadIdx.y + 1;
+    const int ni = d.ni, nj = d.nj, nk = d.nk;
+    if (i >= ni - 1 || j >= nj - 1) return;
+    const int y = j + NG, x = i + NG;
+    const float zt = (float)nk * dz;
+    const float rzt = 1.0f / zt;
+    const float rdsf = 1.0f / dz;
+    const float dzdx = a.dzdx[(size_t)j * ni + i], dzdy = a.dzdy[(size_t)j * ni + i], gz = a.gz[(size_t)j * ni + i];
+    float w_lo = 0.0f;  // rrw(k) for the level below (k = 1: zero floor)
+    float ru_lo = a.rru[d.u(1, y, x)] + a.rru[d.u(1, y, x + 1)];
+    float rv_lo = a.rrv[d.v(1, y, x)] + a.rrv[d.v(1, y + 1, x)];
+    for (int k = 1; k <= nk; ++k) {
+        float w_hi = 0.0f;
+        float ru_hi = 0.0f, rv_hi = 0.0f;
+        if (k + 1 <= nk) {
+            const int kk = k + 1;
+            const float sigmaf = (float)(kk - 1) * dz;
+            const float sigma = (float)((double)kk - 1.5) * dz;
+            float r2 = (sigmaf - sigma) * (1.0f / dz);
+            const float r1 = 0.5f * (1.0f - r2);
+            r2 = 0.5f * r2;
+            ru_hi = a.rru[d.u(kk, y, x)] + a.rru[d.u(kk, y, x + 1)];
+            rv_hi = a.rrv[d.v(kk, y, x)] + a.rrv[d.v(kk, y + 1, x)];
+            const float ux = r2 * ru_hi + r1 * ru_lo;
+            const float vy = r2 * rv_hi + r1 * rv_lo;
+            float terrain = ux * dzdx + vy * dzdy;
+            terrain = terrain * (sigmaf - zt);
+            terrain = terrain * gz;
+            terrain = terrain * rzt;
+            w_hi = a.rf0[d.c(kk - 1, j, i)] * a.w3d[d.s(kk, y, x)] + terrain;
+            a.rrw[d.s(kk, y, x)] = w_hi;
+        }
+        float value = (a.rru[d.u(k, y, x + 1)] - a.rru[d.u(k, y, x)]) * rdx +
+                      (a.rrv[d.v(k, y + 1, x)] - a.rrv[d.v(k, y, x)]) * rdy;
+        value = value + (w_hi - w_lo) * rdsf;
+        a.divx[d.c(k - 1, j, i)] = (fabsf(value) <= kDivClamp) ? 0.0f : value;
+        w_lo = w_hi;
+        ru_lo = ru_hi;
+        rv_lo = rv_hi;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// fused scalar advection: grid (ceil(ni/32), ceil(nj/4), chunks of levels)
+// ---------------------------------------------------------------------------
+template <bool WENO>
+__device__ __forceinline__ float vertical_flux(const float *__restrict__ s, const PaddedDims &d,
+                                               const gm1b_scalar_advection5_arrays &a, int k, int j, int i, int y,
+                                               int x, double eps, float wepsf) {
+    const int nk = d.nk;
+    if (k <= 1 || k >= nk + 1) return 0.0f;
+    const float m = a.rrw[d.s(k, y, x)];
+#define SK(kk) __ldg(s + d.s((kk), y, x))
+    float r;
+    if (k == 2) {
+        if (m >= 0.0f)
+            r = a.c1[d.c(k - 1, j, i)] * SK(k - 1) + a.c2[d.c(k - 1, j, i)] * SK(k);
+        else if (WENO)
+            r = upstrpd(SK(k + 1), SK(k), SK(k - 1), wepsf);
+        else
+            r = flx3(SK(k + 1), SK(k), SK(k - 1));
+    } else if (k == nk) {
+        const bool up = WENO ? (m > 0.0f) : (m >= 0.0f);
+        if (up)
+            r = WENO ? upstrpd(SK(k - 2), SK(k - 1), SK(k), wepsf) : flx3(SK(k - 2), SK(k - 1), SK(k));
+        else
+            r = a.c1[d.c(k - 1, j, i)] * SK(k - 1) + a.c2[d.c(k - 1, j, i)] * SK(k);
+    } else if (k == 3) {
+        if (m >= 0.0f)
+            r = WENO ? upstrpd(SK(k - 2), SK(k - 1), SK(k), wepsf) : flx3(SK(k - 2), SK(k - 1), SK(k));
+        else
+            r = recon<WENO>(SK(k + 2), SK(k + 1), SK(k), SK(k - 1), SK(k - 2), eps);
+    } else if (k == nk - 1) {
+        if (m >= 0.0f)
+            r = recon<WENO>(SK(k - 3), SK(k - 2), SK(k - 1), SK(k), SK(k + 1), eps);
+        else if (WENO)
+            r = upstrpd(SK(k + 1), SK(k), SK(k - 1), wepsf);
+        else
+            r = flx3(SK(k + 1), SK(k), SK(k - 1));
+    } else if (m >= 0.0f) {
+        r = recon<WENO>(SK(k - 3), SK(k - 2), SK(k - 1), SK(k), SK(k + 1), eps);
+    } else {
+        r = recon<WENO>(SK(k + 2), SK(k + 1), SK(k), SK(k - 1), SK(k - 2), eps);
+    }
+#undef SK
+    return m * r;
+}
+
+template <bool WENO>
+__device__ __forceinline__ float x_face_flux(const float *__restrict__ s, const PaddedDims &d, const float *rru,
+                                             int k, int y, int x, double eps) {
+    const float m = __ldg(rru + d.u(k, y, x));
+    const float *row = s + d.s(k, y, 0);
+    float r;
+    if (m >= 0.0f)
+        r = recon<WENO>(__ldg(row + x - 3), __ldg(row + x - 2), __ldg(row + x - 1), __ldg(row + x), __ldg(row + x + 1),
+                        eps);
+    else
+        r = recon<WENO>(__ldg(row + x + 2), __ldg(row + x + 1), __ldg(row + x), __ldg(row + x - 1), __ldg(row + x - 2),
+                        eps);
+    return m * r;
+}
+
+template <bool WENO>
+__device__ __forceinline__ float y_face_flux(const float *__restrict__ s, const PaddedDims &d, const float *rrv,
+                                             int k, int y, int x, double eps) {
+    const float m = __ldg(rrv + d.v(k, y, x));
+    const size_t sy = (size_t)(d.ni + 2 * NG);
+    const float *col = s + d.s(k, 0, x);
+    float r;
+    if (m >= 0.0f)
+        r = recon<WENO>(__ldg(col + (y - 3) * sy), __ldg(col + (y - 2) * sy), __ldg(col + (y - 1) * sy),
+                        __ldg(col + y * sy), __ldg(col + (y + 1) * sy), eps);
+    else
+        r = recon<WENO>(__ldg(col + (y + 2) * sy), __ldg(col + (y + 1) * sy), __ldg(col + y * sy),
+                        __ldg(col + (y - 1) * sy), __ldg(col + (y - 2) * sy), eps);
+    return m * r;
+}
+
+template <bool WENO>
+__global__ void __launch_bounds__(kAX *kAY)
+    scalar_advection5_kernel(gm1b_scalar_advection5_arrays a, PaddedDims d, int levels_per_chunk, float rdx,
+                             float rdy, float rdsf, double eps, float wepsf, unsigned obc) {
+    __shared__ float s_fx[kAY][kAX + 1];
+    __shared__ float s_fy[kAY + 1][kAX];
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int i = blockIdx.x * kAX + tx;
+    const int j = blockIdx.y * kAY + ty;
+    const int ni = d.ni, nj = d.nj, nk = d.nk;
+    const bool cell = i < ni && j < nj;
+    const int x = i + NG, y = j + NG;
+    const int k_begin = 1 + blockIdx.z * levels_per_chunk;
+    const int k_end = min(nk, k_begin + levels_per_chunk - 1);
+    const float *s = a.scalar;
+    const bool owned = cell && (obc != 0u || (i >= 3 && i + 3 < ni && j >= 3 && j + 3 < nj));
+    const bool east_face = cell && (tx == kAX - 1 || i == ni - 1);
+    const bool north_face = cell && (ty == kAY - 1 || j == nj - 1);
+    float fz_lo = 0.0f;
+    if (cell) {
+        fz_lo = vertical_flux<WENO>(s, d, a, k_begin, j, i, y, x, eps, wepsf);
+        if (a.flux_z != nullptr && k_begin == 1) a.flux_z[d.s(1, y, x)] = 0.0f;
+    }
+    for (int k = k_begin; k <= k_end; ++k) {
+        if (cell) {
+            const float fw = x_face_flux<WENO>(s, d, a.rru, k, y, x, eps);
+            s_fx[ty][tx] = fw;
+            if (a.flux_x != nullptr) a.flux_x[d.u(k, y, x)] = fw;
+            if (east_face) {
+                const float fe = x_face_flux<WENO>(s, d, a.rru, k, y, x + 1, eps);
+                s_fx[ty][tx + 1] = fe;
+                if (a.flux_x != nullptr && i == ni - 1) a.flux_x[d.u(k, y, x + 1)] = fe;
+            }
+            const float fs = y_face_flux<WENO>(s, d, a.rrv, k, y, x, eps);
+            s_fy[ty][tx] = fs;
+            if (a.flux_y != nullptr) a.flux_y[d.v(k, y, x)] = fs;
+            if (north_face) {
+                const float fn = y_face_flux<WENO>(s, d, a.rrv, k, y + 1, x, eps);
+                s_fy[ty + 1][tx] = fn;
+                if (a.flux_y != nullptr && j == nj - 1) a.flux_y[d.v(k, y + 1, x)] = fn;
+            }
+        }
+        __syncthreads();
+        if (cell) {
+            const float fz_hi = vertical_flux<WENO>(s, d, a, k + 1, j, i, y, x, eps, wepsf);
+            if (a.flux_z != nullptr) a.flux_z[d.s(k + 1, y, x)] = fz_hi;
+            if (owned) {
+                float fw = s_fx[ty][tx], fe = s_fx[ty][tx + 1];
+                float fs = s_fy[ty][tx], fn = s_fy[ty + 1][tx];
+                const float sv = __ldg(s + d.s(k, y, x));
+                const float uw = __ldg(a.rru + d.u(k, y, x)), ue = __ldg(a.rru + d.u(k, y, x + 1));
+                const float vs = __ldg(a.rrv + d.v(k, y, x)), vn = __ldg(a.rrv + d.v(k, y + 1, x));
+                const bool iw = (i == 0) && ((obc & 15u) == 2u) && uw >= 0.0f;
+                const bool ie = (i + 1 == ni) && (((obc >> 4) & 15u) == 2u) && ue <= 0.0f;
+                const bool js = (j == 0) && (((obc >> 8) & 15u) == 2u) && vs >= 0.0f;
+                const bool jn = (j + 1 == nj) && (((obc >> 12) & 15u) == 2u) && vn <= 0.0f;
+                if (iw) fw = fe;
+                if (ie) fe = fw;
+                if (js) fs = fn;
+                if (jn) fn = fs;
+                float ax = (fw - fe) * rdx;
+                float ay = (fs - fn) * rdy;
+                if (iw) ax = ax - (sv * (ue - uw)) * rdx;
+                if (ie) ax = ax - (sv * (ue - uw)) * rdx;
+                if (js) ay = ay - (sv * (vn - vs)) * rdy;
+                if (jn) ay = ay - (sv * (vn - vs)) * rdy;
+                float az;
+                if (k == 1)
+                    az = (-fz_hi) * rdsf;
+                else if (k == nk)
+                    az = fz_lo * rdsf;
+                else
+                    az = (fz_lo - fz_hi) * rdsf;
+                float total = (ax + ay) + az;
+                total = total + sv * __ldg(a.divx + d.c(k - 1, j, i));
+                a.tendency[d.c(k - 1, j, i)] =
+                    (total * __ldg(a.rr0 + d.c(k - 1, j, i))) * __ldg(a.gz + (size_t)j * ni + i);
+            }
+            fz_lo = fz_hi;
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace
+}  // namespace gm1b
+
+using namespace gm1b;
+
+extern "C" int32_t gm1b_terrain_mass_flux5(int32_t ni, int32_t nj, int32_t nk, const gm1b_mass_flux5_arrays *arrays,
+                                          float dx, float dy, float dz, void *stream) {
+    if (arrays == nullptr || ni < 8 || nj < 8 || nk < 8) {
+        gm1b_set_error("gm1b_terrain_mass_flux5: need arrays and ni, nj, nk >= 8");
+        return GM1B_ERR_ARGUMENT;
+    }
+    if (!(dx > 0.0f) || !(dy > 0.0f) || !(dz > 0.0f) || !isfinite(dx) || !isfinite(dy) || !isfinite(dz)) {
+        gm1b_set_error("gm1b_terrain_mass_flux5: dx, dy, dz must be finite and > 0");
+        return GM1B_ERR_ARGUMENT;
+    }
+    const float *const *p = reinterpret_cast<const float *const *>(arrays);
+    for (size_t q = 0; q < sizeof(gm1b_mass_flux5_arrays) / sizeof(float *); ++q)
+        if (p[q] == nullptr) {
+            gm1b_set_error("gm1b_terrain_mass_flux5: array #%zu is NULL", q);
+            return GM1B_ERR_ARGUMENT;
+        }
+    const PaddedDims d{ni, nj, nk};
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    {
+        ProfScope ps("mass_flux_horizontal_kernel", st);
+        mass_flux_horizontal_kernel<<<dim3((ni + kAX - 1) / kAX, (nj + kAY - 1) / kAY, nk), dim3(kAX, kAY), 0, st>>>(
+            *arrays, d);
+        ps.stop();
+    }
+    if (cudaPeekAtLastError() != cudaSuccess) {
+        gm1b_set_error("mass_flux_horizontal_kernel: %s", cudaGetErrorString(cudaGetLastError()));
+        return GM1B_ERR_CUDA;
+    }
+    const float rdx = 1.0f / dx, rdy = 1.0f / dy;
+    {
+        ProfScope ps("mass_flux_column_kernel", st);
+        mass_flux_column_kernel<<<dim3((ni - 2 + kAX - 1) / kAX, (nj - 2 + kAY - 1) / kAY), dim3(kAX, kAY), 0, st>>>(
+            *arrays, d, dz, rdx, rdy);
+        ps.stop();
+    }
+    if (cudaPeekAtLastError() != cudaSuccess) {
+        gm1b_set_error("mass_flux_column_kernel: %s", cudaGetErrorString(cudaGetLastError()));
+        return GM1B_ERR_CUDA;
+    }
+    return GM1B_OK;
+}
+
+extern "C" int32_t gm1b_scalar_advection5(int32_t ni, int32_t nj, int32_t nk,
+                                         const gm1b_scalar_advection5_arrays *arrays, int32_t nrk, int32_t wflag,
+                                         float dx, float dy, float dz, double weps, uint32_t lateral_obc,
+                                         int32_t levels_per_chunk, void *stream) {
+    if (arrays == nullptr || ni < 8 || nj < 8 || nk < 8) {
+        gm1b_set_error("gm1b_scalar_advection5: need arrays and ni, nj, nk >= 8");
+        return GM1B_ERR_ARGUMENT;
+    }
+    if (nrk < 1 || nrk > 3) {
+        gm1b_set_error("gm1b_scalar_advection5: the low-storage RK3 schedule requires nrk = 1..3");
+        return GM1B_ERR_ARGUMENT;
+    }
+    if (!(weps > 0.0) || !isfinite(weps) || !(dx > 0.0f) || !(dy > 0.0f) || !(dz > 0.0f)) {
+        gm1b_set_error("gm1b_scalar_advection5: weps, dx, dy, dz must be finite and > 0");
+        return GM1B_ERR_ARGUMENT;
+    }
+    const gm1b_scalar_advection5_arrays &a = *arrays;
+    if (!a.scalar || !a.rru || !a.rrv || !a.rrw || !a.c1 || !a.c2 || !a.rr0 || !a.gz || !a.divx || !a.tendency) {
+        gm1b_set_error("gm1b_scalar_advection5: a required array is NULL (only the flux outputs may be)");
+        return GM1B_ERR_ARGUMENT;
+    }
+    for (int side = 0; side < 4; ++side) {
+        const unsigned code = (lateral_obc >> (4 * side)) & 15u;
+        if (lateral_obc != 0u && (code < 1u || code > 4u)) {
+            gm1b_set_error("gm1b_scalar_advection5: lateral side codes must be 1..4 (or all 0 for a tile)");
+            return GM1B_ERR_ARGUMENT;
+        }
+    }
+    int chunk = levels_per_chunk > 0 ? levels_per_chunk : 16;
+    if (chunk > nk) chunk = nk;
+    const PaddedDims d{ni, nj, nk};
+    const bool weno = wflag != 0 && nrk == 3;
+    const dim3 grid((ni + kAX - 1) / kAX, (nj + kAY - 1) / kAY, (nk + chunk - 1) / chunk);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const float rdx = 1.0f / dx, rdy = 1.0f / dy, rdsf = 1.0f / dz;
+    ProfScope ps(weno ? "scalar_advection5_weno_kernel" : "scalar_advection5_kernel", st);
+    if (weno)
+        scalar_advection5_kernel<true>
+            <<<grid, dim3(kAX, kAY), 0, st>>>(a, d, chunk, rdx, rdy, rdsf, weps, (float)weps, lateral_obc);
+    else
+        scalar_advection5_kernel<false>
+            <<<grid, dim3(kAX, kAY), 0, st>>>(a, d, chunk, rdx, rdy, rdsf, weps, (float)weps, lateral_obc);
+    ps.stop();
+    if (cudaPeekAtLastError() != cudaSuccess) {
+        gm1b_set_error("scalar_advection5_kernel: %s", cudaGetErrorString(cudaGetLastError()));
+        return GM1B_ERR_CUDA;
+    }
+    return GM1B_OK;
+}

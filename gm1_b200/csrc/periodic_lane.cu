@@ -25,7 +25,7 @@ using Arr = gm1b_periodic_arrays;
 
 constexpr int kTX = 32;  // x extent of a 3-D elementwise block
 constexpr int kTY = 4;   // y extent
-constexpr int kColWarps = 8;  // warps of the column CTA
+constexpr int kColWarps = 16;  // warps of the column CTA
 constexpr int kColArrays = 11;  // shared-memory column arrays of the column CTA
 
 // ---------------------------------------------------------------------------
@@ -212,13 +212,13 @@ __global__ void __launch_bounds__(kTX *kTY) traj_momentum_kernel(Arr a, Dims d, 
     // u at face f = x of row j = y
     if (y < nj && advect) {
         const int j = y, js = y + 1, f = x;
-        const int fu = f % ni;
-        const int fm = pmod(fu - 1, ni), fp = (fu + 1) % ni;
+        const int fu = f == ni ? 0 : f;
+        const int fm = pmod(fu - 1, ni), fp = pmod(fu + 1, ni);
         const float east_v = 0.5f * (rru.at(k, j, fu) + rru.at(k, j, fp));
         const float west_v = 0.5f * (rru.at(k, j, fm) + rru.at(k, j, fu));
         const float fx_e = x_flux5c(u, east_v, fu, j, k, ni);
         const float fx_w = x_flux5c(u, west_v, fu - 1, j, k, ni);
-        const int jn = (j + 1) % nj;
+        const int jn = pmod(j + 1, nj);
         const float south_v = 0.5f * (rrv.at(k, j, fu) + rrv.at(k, j, fm));
         const float north_v = 0.5f * (rrv.at(k, jn, fu) + rrv.at(k, jn, fm));
         const float fy_s = y_flux5(u, south_v, fu, j, k, nj);
@@ -254,8 +254,8 @@ __global__ void __launch_bounds__(kTX *kTY) traj_momentum_kernel(Arr a, Dims d, 
     // v at face g = y of column i = x
     if (x < ni && advect) {
         const int i = x, is = x + 1, g = y;
-        const int gv = g % nj;
-        const int gm = pmod(gv - 1, nj), gp = (gv + 1) % nj, ip = (i + 1) % ni;
+        const int gv = g == nj ? 0 : g;
+        const int gm = pmod(gv - 1, nj), gp = pmod(gv + 1, nj), ip = pmod(i + 1, ni);
         const float west_v = 0.5f * (rru.at(k, gv, i) + rru.at(k, gm, i));
         const float east_v = 0.5f * (rru.at(k, gv, ip) + rru.at(k, gm, ip));
         const float fx_w = x_flux5(v, west_v, i, gv, k, ni);
@@ -295,7 +295,7 @@ __global__ void __launch_bounds__(kTX *kTY) traj_momentum_kernel(Arr a, Dims d, 
         if (advect) {
             const float c2 = a.c2[d.s(qs, js, is)];
             const float c1 = 1.0f - c2;
-            const int i1 = (i + 1) % ni, j1 = (j + 1) % nj;
+            const int i1 = pmod(i + 1, ni), j1 = pmod(j + 1, nj);
             const float ux_w = c2 * rru.at(q, j, i) + c1 * rru.at(q - 1, j, i);
             const float ux_e = c2 * rru.at(q, j, i1) + c1 * rru.at(q - 1, j, i1);
             const float vy_s = c2 * rrv.at(q, j, i) + c1 * rrv.at(q - 1, j, i);
@@ -440,7 +440,7 @@ struct ColumnArgs {
     int post_ppx;    // trajectory post-step ppx completion fused at nrk=3
 };
 
-__global__ void __launch_bounds__(kTX *kColWarps) sound_column_kernel(Arr a, Dims d, ColumnArgs p) {
+__global__ void __launch_bounds__(kTX *kColWarps, 1) sound_column_kernel(Arr a, Dims d, ColumnArgs p) {
     extern __shared__ float smem[];
     const int ni = d.ni, nj = d.nj, nk = d.nk;
     const int lane = threadIdx.x;
@@ -465,6 +465,7 @@ __global__ void __launch_bounds__(kTX *kColWarps) sound_column_kernel(Arr a, Dim
 
     // phase A: k-parallel divergence, pressure advection and fpk
     if (live) {
+#pragma unroll 2
         for (int k = 1 + wy; k <= nk + 1; k += kColWarps) {
             SM(s_w, k) = a.w3d[d.w(k, j - 1, i - 1)];
             if (k > nk) continue;
@@ -506,6 +507,7 @@ __global__ void __launch_bounds__(kTX *kColWarps) sound_column_kernel(Arr a, Dim
     __syncthreads();
     // phase A2: tridiagonal coefficients and right-hand side, k = 2..nk
     if (live) {
+#pragma unroll 2
         for (int k = 2 + wy; k <= nk; k += kColWarps) {
             const float mm = SM(s_mm, k);
             const float aa = (k >= 3) ? (-p.asq) * (mm * SM(s_a1, k - 1)) : 0.0f;
@@ -558,6 +560,7 @@ __global__ void __launch_bounds__(kTX *kColWarps) sound_column_kernel(Arr a, Dim
         const int rows[3] = {j, wrap_j0 ? 0 : -1, wrap_j1 ? nj + 1 : -1};
         const int cols[3] = {i, wrap_i0 ? 0 : -1, wrap_i1 ? ni + 1 : -1};
         const bool halo_cell = wrap_j0 || wrap_j1 || wrap_i0 || wrap_i1;
+#pragma unroll 2
         for (int k = 1 + wy; k <= nk; k += kColWarps) {
             const size_t c = d.s(k, j, i);
             const float wk = SM(s_w, k), wk1 = SM(s_w, k + 1);
@@ -585,9 +588,9 @@ __global__ void __launch_bounds__(kTX *kColWarps) sound_column_kernel(Arr a, Dim
             const size_t wc = d.w(k, j - 1, i - 1);
             a.rrw[wc] = last ? (a.rrw[wc] + wk * p.alph) * p.rnloop : a.rrw[wc] + wk;
             if (halo_cell) {
-                for (int r = 0; r < 3; ++r) {
+                _Pragma("unroll") for (int r = 0; r < 3; ++r) {
                     if (rows[r] < 0) continue;
-                    for (int q = 0; q < 3; ++q) {
+                    _Pragma("unroll") for (int q = 0; q < 3; ++q) {
                         if (cols[q] < 0 || (r == 0 && q == 0)) continue;
                         const size_t h = d.s(k, rows[r], cols[q]);
                         if (!last) a.ppd[h] = ppd;
@@ -692,9 +695,9 @@ __global__ void __launch_bounds__(kTX *kTY) traj_theta_kernel(Arr a, Dims d, flo
     float tendency = 0.0f;
     if (enabled) {
         const float fx_w = x_flux5(th, rru.at(k, j, i), i, j, k, ni);
-        const float fx_e = x_flux5(th, rru.at(k, j, (i + 1) % ni), i + 1, j, k, ni);
+        const float fx_e = x_flux5(th, rru.at(k, j, pmod(i + 1, ni)), i + 1, j, k, ni);
         const float fy_s = y_flux5(th, rrv.at(k, j, i), i, j, k, nj);
-        const float fy_n = y_flux5(th, rrv.at(k, (j + 1) % nj, i), i, j + 1, k, nj);
+        const float fy_n = y_flux5(th, rrv.at(k, pmod(j + 1, nj), i), i, j + 1, k, nj);
         const float advx = (-(fx_e - fx_w)) * rdx;
         const float advy = (-(fy_n - fy_s)) * rdy;
         float advz;
@@ -721,9 +724,9 @@ __global__ void __launch_bounds__(kTX *kTY) traj_theta_kernel(Arr a, Dims d, flo
     // periodic th3d halos mirrored from this live cell
     const int rows[3] = {js, js == nj ? 0 : -1, js == 1 ? nj + 1 : -1};
     const int cols[3] = {is, is == ni ? 0 : -1, is == 1 ? ni + 1 : -1};
-    for (int r = 0; r < 3; ++r) {
+    _Pragma("unroll") for (int r = 0; r < 3; ++r) {
         if (rows[r] < 0) continue;
-        for (int q = 0; q < 3; ++q) {
+        _Pragma("unroll") for (int q = 0; q < 3; ++q) {
             if (cols[q] < 0 || (r == 0 && q == 0)) continue;
             a.th3d[d.s(ks, rows[r], cols[q])] = updated;
         }

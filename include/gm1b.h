@@ -130,6 +130,58 @@ GM1B_API int32_t gm1b_psolver3_trajectory(
     uint32_t ablations, uint32_t flags, void *stream);
 
 
+/* ------------------------------------------------------------------------
+ * Padded lane (ng = 3 lateral ghost cells, CM1_OPEN_NGXY): shapes
+ *   scalar (nk+2, nj+6, ni+6)   u/rru (nk+2, nj+6, ni+7)
+ *   v/rrv  (nk+2, nj+7, ni+6)   w/rrw (nk+3, nj+6, ni+6)
+ *   cell fields (nk, nj, ni), face-level fields (nk+1, nj, ni),
+ *   rgzu (nj, ni+1), rgzv (nj+1, ni), dzdx/dzdy/gz (nj, ni)
+ * (src/cm1core/cuda_advection5.py:293-300,987-995;
+ *  src/cm1core/cuda_terrain_open_boundary.py:429-459).
+ * ---------------------------------------------------------------------- */
+
+typedef struct gm1b_mass_flux5_arrays {
+    const float *u3d, *v3d, *w3d;
+    float *rru, *rrv, *rrw;
+    const float *rho0_3d, *rf0, *rgzu, *rgzv, *dzdx, *dzdy, *gz;
+    float *divx;
+} gm1b_mass_flux5_arrays;
+
+/*
+ * Terrain mass flux rru/rrv on interior faces, rrw (with the terrain term)
+ * and the interior divergence divx of one RK stage.
+ * Replaces launch_cuda_terrain_mass_flux5
+ * (src/cm1core/cuda_advection5.py:849) and its CPU twin
+ * cpu_terrain_mass_flux5_inplace (:271).  ni, nj, nk >= 8.
+ */
+GM1B_API int32_t gm1b_terrain_mass_flux5(int32_t ni, int32_t nj, int32_t nk,
+                                         const gm1b_mass_flux5_arrays *arrays,
+                                         float dx, float dy, float dz, void *stream);
+
+typedef struct gm1b_scalar_advection5_arrays {
+    const float *scalar, *rru, *rrv, *rrw;
+    const float *c1, *c2, *rr0, *gz, *divx;
+    float *tendency;
+    /* face fluxes (shapes of rru, rrv, rrw); NULL = not written */
+    float *flux_x, *flux_y, *flux_z;
+} gm1b_scalar_advection5_arrays;
+
+/*
+ * Fifth-order (nrk = 1, 2) or WENO5-Z (nrk = 3 with wflag) flux-divergence
+ * tendency of one scalar.  lateral_obc packs CM1's lateral side codes
+ * wbc | ebc<<4 | sbc<<8 | nbc<<12 (1 periodic, 2 open, 3 rigid, 4 ...) for a
+ * whole-domain call, or 0 for a tile-local call that leaves the outer three
+ * cells unwritten.  levels_per_chunk sets the z-chunk of the marching CTAs
+ * (<= 0: default).
+ * Replaces launch_cuda_scalar_advection5 (src/cm1core/cuda_advection5.py:948)
+ * and its CPU twin cpu_scalar_advection5_inplace (:440).  ni, nj, nk >= 8.
+ */
+GM1B_API int32_t gm1b_scalar_advection5(int32_t ni, int32_t nj, int32_t nk,
+                                        const gm1b_scalar_advection5_arrays *arrays,
+                                        int32_t nrk, int32_t wflag, float dx, float dy,
+                                        float dz, double weps, uint32_t lateral_obc,
+                                        int32_t levels_per_chunk, void *stream);
+
 /*
  * Launch profiler.  While enabled, every kernel launch of the library is
  * bracketed by a pair of CUDA events recorded on its own stream (the

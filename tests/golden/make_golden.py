@@ -183,6 +183,87 @@ def make_small(reference: Path) -> None:
     print("wrote schedule")
 
 
+def advection_fixture(ni: int, nj: int, nk: int, seed: int) -> dict[str, np.ndarray]:
+    """Padded-lane (ng = 3) inputs of the terrain mass flux and scalar
+    advection, with both signs and exact (signed) zeros in every mass flux."""
+    ng = 3
+    rng = np.random.default_rng(seed)
+
+    def field(shape, lo, hi):
+        return rng.uniform(lo, hi, size=shape).astype(np.float32)
+
+    a = {
+        "u3d": field((nk + 2, nj + 2 * ng, ni + 1 + 2 * ng), -12.0, 12.0),
+        "v3d": field((nk + 2, nj + 1 + 2 * ng, ni + 2 * ng), -12.0, 12.0),
+        "w3d": field((nk + 3, nj + 2 * ng, ni + 2 * ng), -3.0, 3.0),
+        "rho0_3d": field((nk, nj, ni), 0.6, 1.2),
+        "rf0": field((nk + 1, nj, ni), 0.6, 1.2),
+        "rgzu": field((nj, ni + 1), 0.95, 1.05),
+        "rgzv": field((nj + 1, ni), 0.95, 1.05),
+        "dzdx": field((nj, ni), -0.02, 0.02),
+        "dzdy": field((nj, ni), -0.02, 0.02),
+        "gz": field((nj, ni), 0.97, 1.03),
+        "c1": field((nk + 1, nj, ni), 0.3, 0.7),
+        "rr0": field((nk, nj, ni), 0.8, 1.6),
+        "scalar": field((nk + 2, nj + 2 * ng, ni + 2 * ng), 290.0, 310.0),
+        "qscalar": (field((nk + 2, nj + 2 * ng, ni + 2 * ng), 0.0, 1.0) ** 4 * np.float32(0.01)).astype(np.float32),
+        "adv_rru": field((nk + 2, nj + 2 * ng, ni + 1 + 2 * ng), -9.0, 9.0),
+        "adv_rrv": field((nk + 2, nj + 1 + 2 * ng, ni + 2 * ng), -9.0, 9.0),
+        "adv_rrw": field((nk + 3, nj + 2 * ng, ni + 2 * ng), -2.0, 2.0),
+        "adv_divx": field((nk, nj, ni), -1e-3, 1e-3),
+    }
+    a["c2"] = (np.float32(1.0) - a["c1"]).astype(np.float32)
+    # smooth stretch of the scalar so WENO weights vary, and flat patches
+    a["scalar"][:, :, : ni // 3] = np.float32(300.0)
+    for name in ("adv_rru", "adv_rrv", "adv_rrw"):
+        flat = a[name].reshape(-1)
+        idx = rng.choice(flat.size, size=max(4, flat.size // 25), replace=False)
+        flat[idx[: len(idx) // 2]] = np.float32(0.0)
+        flat[idx[len(idx) // 2 :]] = np.float32(-0.0)
+    # signed zeros on the top interior face where WENO tests rrw > 0
+    a["adv_rrw"][nk, ng : ng + 2, ng : ng + 3] = np.float32(-0.0)
+    a["adv_rrw"][nk, ng + 2 : ng + 4, ng : ng + 3] = np.float32(0.0)
+    return a
+
+
+def make_advection(reference: Path) -> None:
+    sys.path.insert(0, str(reference / "src"))
+    from cm1core.cuda_advection5 import cpu_scalar_advection5_inplace, cpu_terrain_mass_flux5_inplace
+    from cm1core.cuda_terrain_open_boundary import terrain_static_shapes
+
+    for tag, (ni, nj, nk, seed) in {"adv5_12x10x9": (12, 10, 9, 21), "adv5_9x11x10": (9, 11, 10, 22)}.items():
+        a = advection_fixture(ni, nj, nk, seed)
+        inputs = {f"in_{k}": v.copy() for k, v in a.items()}
+        outputs = {}
+        dx, dy, dz = 1000.0, 900.0, 250.0
+        shapes = terrain_static_shapes(ni=ni, nj=nj, nk=nk)
+        metrics = {name: np.zeros(shape, dtype=np.float32) for name, shape in shapes.items()}
+        for name in ("rho0_3d", "rf0", "rgzu", "rgzv", "dzdx", "dzdy", "gz", "c1", "c2", "rr0"):
+            metrics[name][...] = a[name]
+        mf = {n: a[n].copy() for n in ("u3d", "v3d", "w3d")}
+        for n, src in (("rru", "u3d"), ("rrv", "v3d"), ("rrw", "w3d")):
+            mf[n] = np.full_like(a[src], np.float32(7.0))  # untouched words keep this sentinel
+        divx = np.full((nk, nj, ni), np.float32(7.0), dtype=np.float32)
+        cpu_terrain_mass_flux5_inplace(mf, metrics, divx, ni=ni, nj=nj, nk=nk, dx=dx, dy=dy, dz=dz)
+        outputs.update({"out_mf_rru": mf["rru"], "out_mf_rrv": mf["rrv"], "out_mf_rrw": mf["rrw"], "out_mf_divx": divx})
+        for nrk in (1, 3):
+            for sname, weps in (("scalar", 1.0e-6), ("qscalar", 1.0e-2 * 1.0e-18)):
+                arrays = {"rru": a["adv_rru"], "rrv": a["adv_rrv"], "rrw": a["adv_rrw"]}
+                fluxes = {"x": np.full_like(a["adv_rru"], np.float32(7.0)),
+                          "y": np.full_like(a["adv_rrv"], np.float32(7.0)),
+                          "z": np.full_like(a["adv_rrw"], np.float32(7.0))}
+                tend = np.full((nk, nj, ni), np.float32(7.0), dtype=np.float32)
+                cpu_scalar_advection5_inplace(a[sname], arrays, metrics, a["adv_divx"], tend, fluxes,
+                                              ni=ni, nj=nj, nk=nk, nrk=nrk, dx=dx, dy=dy, dz=dz, weps=weps)
+                key = f"{sname}_nrk{nrk}"
+                outputs.update({f"out_{key}_fx": fluxes["x"], f"out_{key}_fy": fluxes["y"],
+                                f"out_{key}_fz": fluxes["z"], f"out_{key}_tend": tend})
+        meta = dict(ni=ni, nj=nj, nk=nk, dx=dx, dy=dy, dz=dz, weps={"scalar": 1.0e-6, "qscalar": 1.0e-2 * 1.0e-18},
+                    sentinel=7.0)
+        np.savez_compressed(HERE / f"{tag}.npz", meta=json.dumps(meta), **inputs, **outputs)
+        print("wrote", tag)
+
+
 def make_c1(reference: Path, checkpoints: list[int]) -> None:
     """Digests after each checkpoint N, each from a fresh state with one call
     of steps=N (the reference refuses a non-fresh entry state, ppx != pp3d,
@@ -219,11 +300,13 @@ def make_c1(reference: Path, checkpoints: list[int]) -> None:
 def main() -> None:
     p = argparse.ArgumentParser()
     p.add_argument("--reference", type=Path, required=True, help="root of the reference source tree")
-    p.add_argument("what", choices=("small", "c1"))
+    p.add_argument("what", choices=("small", "c1", "advection"))
     p.add_argument("--checkpoints", type=int, nargs="+", default=[1])
     args = p.parse_args()
     if args.what == "small":
         make_small(args.reference)
+    elif args.what == "advection":
+        make_advection(args.reference)
     else:
         make_c1(args.reference, sorted(set(args.checkpoints)))
 
