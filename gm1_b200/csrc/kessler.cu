@@ -1,0 +1,484 @@
+// kessler.cu - sm_100a kernels of the complete Kessler warm-rain operator
+// (ptype = 1, efall = 0): pdefq(qv, qc, qr), rain fall speed and rain-energy
+// budget, fallout sub-stepping, local conversion and saturation adjustment,
+// with the FP64 budgets.
+//
+// Behaviour followed (reference file:line):
+//   cpu_gm1_kessler_driver_inplace  src/cm1core/cuda_gm1_kessler_driver.py:431-559
+//   _cpu_pdefq                      src/cm1core/cuda_gm1_kessler_driver.py:300-335
+//   _cpu_satadj                     src/cm1core/cuda_gm1_kessler_driver.py:337-428
+//   cpu_gm1_kessler_local_inplace   src/cm1core/cuda_gm1_kessler_local.py:251-432
+//
+// Design (B200): the reference runs its column phases one thread per j ROW
+// (serial over i, k and the fallout sub-steps) and its budget finishes on a
+// single thread.  Here every COLUMN is a thread (pdefq x3, fall speed,
+// nfall, the fallout sub-steps marching up k with the flux of the level
+// above carried in a register), every CELL is a thread for the local
+// conversion fused with the saturation adjustment, and the FP64 budgets are
+// reduced in a fixed order: per-column sums in the twin's k order, row sums
+// in its i order, then a short ordered finish.  The budget scratch lives in a
+// caller-provided workspace; its first 16 bytes are status words.
+#include "gm1b_common.cuh"
+
+namespace gm1b {
+namespace {
+
+constexpr int kKX = 128;  // cell-kernel CTA: a run of 128 cells of one row at one level
+constexpr int kCX = 32, kCY = 4;
+
+struct KConst {
+    float rd, cp, cpv, rv, xlv, cv, cvv, rovcp, eps, reps, cpl, lv2, lv1, rp00, cpdcv, rddcv, cpdrd, p00;
+};
+
+__host__ KConst make_constants() {
+    KConst c;
+    c.rd = 287.04f;
+    c.cp = 1005.7f;
+    c.cpv = 1870.0f;
+    c.rv = 461.5f;
+    c.xlv = 2501000.0f;
+    c.cv = c.cp - c.rd;
+    c.cvv = c.cpv - c.rv;
+    c.rovcp = c.rd / c.cp;
+    c.eps = c.rd / c.rv;
+    c.reps = c.rv / c.rd;
+    c.cpl = 4190.0f;
+    c.lv2 = c.cpl - c.cpv;
+    c.lv1 = c.xlv + c.lv2 * 273.15f;
+    c.p00 = 1.0e5f;
+    c.rp00 = 1.0f / c.p00;
+    c.cpdcv = c.cp / c.cv;
+    c.rddcv = c.rd / c.cv;
+    c.cpdrd = c.cp / c.rd;
+    return c;
+}
+
+__device__ __forceinline__ float pymax(float a, float b) { return (b > a) ? b : a; }
+__device__ __forceinline__ float pymin(float a, float b) { return (b < a) ? b : a; }
+
+__device__ __forceinline__ float esl_capped(float t, float prs) {
+    const float esl = 611.2f * expf((17.67f * (t - 273.15f)) / (t - 29.65f));
+    return pymin(esl, prs * 0.5f);
+}
+
+struct KDims {
+    int ni, nj, nk;
+    __device__ __forceinline__ size_t c(int k, int j, int i) const {
+        return ((size_t)k * nj + (size_t)j) * (size_t)ni + (size_t)i;
+    }
+};
+
+// workspace layout (doubles after a 16-byte status block)
+struct KWork {
+    int32_t *status;   // [0] satadj non-converged cells, [1] max fallout sub-steps
+    double *colterm;   // [5][nj*ni]
+    double *rows;      // [5][nj]
+    double *partial;   // [5][nk][nj][nbx]
+    int nbx;
+};
+
+__host__ size_t workspace_bytes(int ni, int nj, int nk) {
+    const size_t ncol = (size_t)ni * nj;
+    const size_t nbx = (size_t)((ni + kKX - 1) / kKX);
+    return 16 + sizeof(double) * (5 * ncol + 5 * (size_t)nj + 5 * (size_t)nk * nj * nbx);
+}
+
+__host__ KWork carve(void *ws, int ni, int nj, int nk) {
+    KWork w;
+    char *p = static_cast<char *>(ws);
+    w.status = reinterpret_cast<int32_t *>(p);
+    w.colterm = reinterpret_cast<double *>(p + 16);
+    w.rows = w.colterm + 5 * (size_t)ni * nj;
+    w.partial = w.rows + 5 * (size_t)nj;
+    w.nbx = (ni + kKX - 1) / kKX;
+    return w;
+}
+
+// pdefq of one column: returns a2 - a1 and rescales q in place
+__device__ __forceinline__ double pdefq_column(const gm1b_kessler_arrays &a, float *q, float rmax, const KDims &d,
+                                               int j, int i) {
+    double t1 = 0.0, t2 = 0.0, a1 = 0.0, a2 = 0.0;
+    const float ruh = a.ruh[i], rvh = a.rvh[j];
+    for (int k = 0; k < d.nk; ++k) {
+        const size_t p = d.c(k, j, i);
+        const float rho = a.rho[p], qk = q[p], rmh = a.rmh[p];
+        const float rq = rho * qk;
+        t1 += (double)rq;
+        const float cell = (((rho * qk) * ruh) * rvh) * rmh;
+        a1 += (double)cell;
+        const float qc = (qk < rmax) ? 0.0f : qk;
+        t2 += (double)(rho * qc);
+    }
+    double t3 = (t1 + 1.0e-20) / (t2 + 1.0e-20);
+    if (t3 < 0.0) t3 = 1.0;
+    for (int k = 0; k < d.nk; ++k) {
+        const size_t p = d.c(k, j, i);
+        const float rho = a.rho[p];
+        const float qk0 = q[p];
+        const float qc = (qk0 < rmax) ? 0.0f : qk0;
+        const float qn = (float)(t3 * (double)qc);
+        q[p] = qn;
+        const float cell = (((rho * qn) * ruh) * rvh) * a.rmh[p];
+        a2 += (double)cell;
+    }
+    return a2 - a1;
+}
+
+// grid (ceil(ni/32), ceil(nj/4)): one thread per column
+__global__ void __launch_bounds__(kCX *kCY)
+    kessler_column_kernel(gm1b_kessler_arrays a, KDims d, KWork w, KConst c, float dt, float rdz) {
+    const int i = blockIdx.x * kCX + threadIdx.x;
+    const int j = blockIdx.y * kCY + threadIdx.y;
+    if (i >= d.ni || j >= d.nj) return;
+    const int nk = d.nk;
+    const size_t col = (size_t)j * d.ni + i;
+    const size_t ncol = (size_t)d.ni * d.nj;
+    const size_t p0 = d.c(0, j, i);
+    const float temp0 = (a.th0[p0] + a.th3d[p0]) * (a.pi0[p0] + a.pp3d[p0]);
+    w.colterm[0 * ncol + col] = pdefq_column(a, a.qv, 0.0f, d, j, i);
+    w.colterm[1 * ncol + col] = pdefq_column(a, a.qc, 1.0e-14f, d, j, i);
+    w.colterm[2 * ncol + col] = pdefq_column(a, a.qr, 1.0e-14f, d, j, i);
+    // rain fall speed and the largest Courant number of the column
+    float crmax = 0.0f;
+    for (int k = 0; k < nk; ++k) {
+        const size_t p = d.c(k, j, i);
+        const float rho = a.rho[p], qr = a.qr[p];
+        float v = 0.0f;
+        if (qr > 1.0e-12f) v = (14.34f * powf(rho * qr, 0.1346f)) * sqrtf(1.15f / rho);
+        a.fall_velocity[p] = v;
+        crmax = pymax(crmax, ((v * dt) * rdz) * a.mh[p]);
+    }
+    const float ruh = a.ruh[i], rvh = a.rvh[j];
+    {
+        float term = dt * a.fall_velocity[p0];
+        term = term * a.rr[p0];
+        term = term * a.qr[p0];
+        term = term * (c.cpl * temp0 - c.lv1);
+        term = term * ruh;
+        term = term * rvh;
+        w.colterm[3 * ncol + col] = (double)term;
+    }
+    int nfall = (int)(crmax + 1.0f);
+    if (nfall < 1) nfall = 1;
+    if (a.nfall != nullptr) a.nfall[col] = nfall;
+    atomicMax(&w.status[1], nfall);
+    // below-threshold rain takes the fall speed of the level above
+    for (int k = nk - 2; k >= 0; --k) {
+        const size_t p = d.c(k, j, i);
+        if (a.qr[p] < 1.0e-8f) a.fall_velocity[p] = a.fall_velocity[d.c(k + 1, j, i)];
+    }
+    const float dtfall = dt / (float)nfall;
+    double bud = 0.0;
+    for (int n = 0; n < nfall; ++n) {
+        float rq_k = (a.rho[p0] * a.fall_velocity[p0]) * pymax(0.0f, a.qr[p0]);
+        const float rq0 = rq_k;
+        for (int k = 0; k < nk; ++k) {
+            const size_t p = d.c(k, j, i);
+            float rq_up = 0.0f;
+            if (k + 1 < nk) {
+                const size_t pu = d.c(k + 1, j, i);
+                rq_up = (a.rho[pu] * a.fall_velocity[pu]) * pymax(0.0f, a.qr[pu]);
+            }
+            const float delta = (((dtfall * (rq_up - rq_k)) * rdz) * a.mh[p]) / a.rho[p];
+            a.qr[p] = a.qr[p] + delta;
+            rq_k = rq_up;
+        }
+        a.rain[col] = a.rain[col] + (0.1f * dtfall) * rq0;
+        a.prate[col] = rq0;
+        float term = dtfall * a.rr[p0];
+        term = term * a.fall_velocity[p0];
+        term = term * pymax(0.0f, a.qr[p0]);
+        term = term * ruh;
+        term = term * rvh;
+        bud += (double)term;
+    }
+    w.colterm[4 * ncol + col] = bud;
+}
+
+__device__ __forceinline__ double block_sum(double v, double *smem) {
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) smem[warp] = v;
+    __syncthreads();
+    double s = 0.0;
+    if (threadIdx.x == 0)
+        for (int q = 0; q < (int)(blockDim.x >> 5); ++q) s += smem[q];
+    __syncthreads();
+    return s;
+}
+
+// grid (nbx, nj, nk): one thread per cell; local conversion then satadj
+__global__ void __launch_bounds__(kKX)
+    kessler_cell_kernel(gm1b_kessler_arrays a, KDims d, KWork w, KConst c, float dt, int eqtset) {
+    __shared__ double s_red[kKX / 32];
+    const int i = blockIdx.x * kKX + threadIdx.x;
+    const int j = blockIdx.y, k = blockIdx.z;
+    double terms[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    if (i < d.ni) {
+        const size_t p = d.c(k, j, i);
+        const float th0 = a.th0[p], pi0 = a.pi0[p], rr = a.rr[p];
+        float th3d = a.th3d[p], pp3d = a.pp3d[p], prs = a.prs[p], rho = a.rho[p];
+        float qvnew = a.qv[p], qcnew = a.qc[p], qrnew = a.qr[p];
+        const float tem = (a.ruh[i] * a.rvh[j]) * a.rmh[p];
+        // --- local conversion ---
+        {
+            float pisum = pi0 + pp3d;
+            const float tmp = (th0 + th3d) * pisum;
+            float ar = 0.0f, cr = 0.0f, er = 0.0f;
+            if (qcnew > 0.0f) {
+                ar = pymax(0.001f * (qcnew - 0.001f), 0.0f);
+                ar = ar * dt;
+            }
+            if (qcnew > 0.0f && qrnew > 0.0f) cr = ((2.2f * qcnew) * powf(qrnew, 0.875f)) * dt;
+            if (qrnew > 0.0f) {
+                const float esl = esl_capped(tmp, prs);
+                const float qvs = (c.eps * esl) / (prs - esl);
+                if (qvnew < qvs) {
+                    const float rhoqr = rho * qrnew;
+                    const float vent = 1.6f + 30.3922f * powf(rhoqr, 0.2046f);
+                    const float deficit = 1.0f - qvnew / qvs;
+                    const float num = (vent * deficit) * powf(rhoqr, 0.525f);
+                    const float den = (2.03e4f + 9.584e6f / (qvs * prs)) * rho;
+                    er = pymin((num / den) * dt, qrnew);
+                    if (qvnew + er > qvs) er = qvs - qvnew;
+                }
+            }
+            if (ar + cr > qcnew) {
+                const float term1 = ar + cr;
+                ar = (qcnew * ar) / term1;
+                cr = (qcnew * cr) / term1;
+            }
+            qvnew = qvnew + er;
+            qcnew = qcnew - (ar + cr);
+            qrnew = qrnew + ((ar + cr) - er);
+            if (er > 1.0e-7f) {
+                if (eqtset == 2) {
+                    const float cpml = (c.cp + c.cpv * qvnew) + c.cpl * (qcnew + qrnew);
+                    const float cvml = (c.cv + c.cvv * qvnew) + c.cpl * (qcnew + qrnew);
+                    const float rm = c.rd + c.rv * qvnew;
+                    const float latent = c.lv1 - c.lv2 * tmp;
+                    const float first = latent / ((c.cpdcv * cvml) * pisum);
+                    const float second = ((th0 + th3d) * (c.rv / cvml)) * (1.0f - (c.rovcp * cpml) / rm);
+                    th3d = th3d - er * (first - second);
+                    const float base = ((rho * rm) * (th0 + th3d)) * c.rp00;
+                    pp3d = powf(base, c.rddcv) - pi0;
+                    pisum = pi0 + pp3d;
+                    prs = c.p00 * powf(pisum, c.cpdrd);
+                } else {
+                    const float latent = c.lv1 - c.lv2 * tmp;
+                    th3d = th3d - er * (latent / (c.cp * pisum));
+                    const float den = ((c.rd * (th0 + th3d)) * pisum) * (1.0f + qvnew * c.reps);
+                    rho = prs / den;
+                }
+            }
+            terms[0] = (double)((rr * ar) * tem);
+            terms[1] = (double)((rr * cr) * tem);
+            terms[2] = (double)((rr * er) * tem);
+        }
+        // --- saturation adjustment ---
+        {
+            const float old_qv = qvnew, old_qc = qcnew;
+            float tnew = (th0 + th3d) * (pi0 + pp3d);
+            float esl = esl_capped(tnew, prs);
+            float qvs = (c.eps * esl) / (prs - esl);
+            uint32_t iterations = 0;
+            if (eqtset == 2) {
+                if (old_qc > 1.0e-12f || old_qv > qvs) {
+                    const float ql = pymax(old_qc + qrnew, 0.0f);
+                    const float cvml = (c.cv + c.cvv * qvnew) + c.cpl * ql;
+                    const float lhv = c.lv1 - c.lv2 * tnew;
+                    const float t1 = (lhv - c.rv * tnew) / cvml;
+                    const float d1 = (t1 * 17.67f) * 243.5f;
+                    const float converge = 2.0f * 0.0001f;
+                    float tlast = tnew, pnew = prs;
+                    int n = 0;
+                    for (;;) {  // bounded: leaves at the 100th pass at the latest
+                        n += 1;
+                        const float denom = 1.0f + (d1 * qvs) / ((tnew - 29.65f) * (tnew - 29.65f));
+                        float dqv = (qvs - qvnew) / denom;
+                        dqv = pymin(dqv, qcnew);
+                        if (qvnew + dqv < 1.0e-20f) dqv = 1.0e-20f - qvnew;
+                        qvnew = qvnew + dqv;
+                        qcnew = qcnew - dqv;
+                        tnew = tnew - dqv * t1;
+                        pnew = (rho * (c.rd + c.rv * qvnew)) * tnew;
+                        const bool conv = fabsf(tnew - tlast) <= converge;
+                        if (!conv) {
+                            tlast = tnew;
+                            esl = esl_capped(tnew, prs);
+                            qvs = (c.eps * esl) / (pnew - esl);
+                        }
+                        if (n == 100) {
+                            atomicAdd(&w.status[0], 1);
+                            break;
+                        }
+                        if (conv) break;
+                    }
+                    iterations = (uint32_t)n;
+                    prs = pnew;
+                    pp3d = powf(pnew * c.rp00, c.rovcp) - pi0;
+                    th3d = tnew / (pi0 + pp3d) - th0;
+                }
+            } else {
+                const float lhv = c.lv1 - c.lv2 * tnew;
+                const float square = (tnew - 29.65f) * (tnew - 29.65f);
+                const float numerator = ((lhv * qvs) * 17.67f) * 243.5f;
+                float dqv = (qvs - qvnew) / (1.0f + numerator / (c.cp * square));
+                if (qvnew + dqv < 1.0e-20f) dqv = 1.0e-20f - qvnew;
+                dqv = pymin(dqv, pymax(0.0f, qcnew));
+                qvnew = qvnew + dqv;
+                qcnew = qcnew - dqv;
+                iterations = 1;
+                th3d = th3d - dqv * (lhv / (c.cp * (pi0 + pp3d)));
+                const float den = ((c.rd * (th0 + th3d)) * (pi0 + pp3d)) * (1.0f + qvnew * c.reps);
+                rho = prs / den;
+            }
+            if (a.satadj_iterations != nullptr) a.satadj_iterations[p] = iterations;
+            const float cond = pymax(qcnew - old_qc, 0.0f);
+            const float evac = pymax(qvnew - old_qv, 0.0f);
+            terms[3] = (double)((rr * cond) * tem);
+            terms[4] = (double)((rr * evac) * tem);
+        }
+        a.th3d[p] = th3d;
+        a.pp3d[p] = pp3d;
+        a.prs[p] = prs;
+        a.rho[p] = rho;
+        a.qv[p] = qvnew;
+        a.qc[p] = qcnew;
+        a.qr[p] = qrnew;
+    }
+    const size_t slot = ((size_t)k * d.nj + j) * w.nbx + blockIdx.x;
+    const size_t plane = (size_t)d.nk * d.nj * w.nbx;
+#pragma unroll
+    for (int t = 0; t < 5; ++t) {
+        const double s = block_sum(terms[t], s_red);
+        if (threadIdx.x == 0) w.partial[t * plane + slot] = s;
+    }
+}
+
+// one thread per (budget type, row): row sums of the column terms in i order
+__global__ void kessler_rows_kernel(KDims d, KWork w) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= 5 * d.nj) return;
+    const int t = q / d.nj, j = q % d.nj;
+    const size_t ncol = (size_t)d.ni * d.nj;
+    double s = 0.0;
+    for (int i = 0; i < d.ni; ++i) s += w.colterm[t * ncol + (size_t)j * d.ni + i];
+    w.rows[(size_t)t * d.nj + j] = s;
+}
+
+// single thread: ordered finish of every budget
+__global__ void kessler_finish_kernel(gm1b_kessler_arrays a, KDims d, KWork w, double volume, double dxd,
+                                      double dyd, double area) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    for (int s = 0; s < 3; ++s)
+        for (int j = 0; j < d.nj; ++j) a.asq[s] += w.rows[(size_t)s * d.nj + j] * volume;
+    for (int j = 0; j < d.nj; ++j) a.qbudget[6] += w.rows[(size_t)3 * d.nj + j] * dxd * dyd;
+    for (int j = 0; j < d.nj; ++j) a.qbudget[5] += w.rows[(size_t)4 * d.nj + j] * area;
+    const size_t plane = (size_t)d.nk * d.nj * w.nbx;
+    for (int p = 0; p < 3; ++p)
+        for (int k = 0; k < d.nk; ++k) {
+            double s = 0.0;
+            for (size_t q = 0; q < (size_t)d.nj * w.nbx; ++q) s += w.partial[p * plane + (size_t)k * d.nj * w.nbx + q];
+            a.qbudget[2 + p] = a.qbudget[2 + p] + s * volume;
+        }
+    for (int p = 3; p < 5; ++p)
+        for (int k = 0; k < d.nk; ++k) {
+            double s = 0.0;
+            for (size_t q = 0; q < (size_t)d.nj * w.nbx; ++q) s += w.partial[p * plane + (size_t)k * d.nj * w.nbx + q];
+            a.qbudget[p - 3] += s * volume;
+        }
+}
+
+bool launched(const char *what) {
+    cudaError_t e = cudaPeekAtLastError();
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        gm1b_set_error("%s: %s", what, cudaGetErrorString(e));
+        return false;
+    }
+    return true;
+}
+
+}  // namespace
+}  // namespace gm1b
+
+using namespace gm1b;
+
+extern "C" size_t gm1b_kessler_workspace_bytes(int32_t ni, int32_t nj, int32_t nk) {
+    if (ni < 1 || nj < 1 || nk < 1) return 0;
+    return workspace_bytes(ni, nj, nk);
+}
+
+extern "C" int32_t gm1b_kessler_driver(int32_t ni, int32_t nj, int32_t nk, const gm1b_kessler_arrays *arrays,
+                                      float dx, float dy, float dz, float dt, int32_t equation_set, int32_t efall,
+                                      void *workspace, size_t workspace_size, void *stream) {
+    if (arrays == nullptr || ni < 1 || nj < 1 || nk < 1) {
+        gm1b_set_error("gm1b_kessler_driver: need arrays and ni, nj, nk >= 1");
+        return GM1B_ERR_ARGUMENT;
+    }
+    if (equation_set != 1 && equation_set != 2) {
+        gm1b_set_error("gm1b_kessler_driver: equation_set must be 1 or 2");
+        return GM1B_ERR_ARGUMENT;
+    }
+    if (efall != 0) {
+        gm1b_set_error("gm1b_kessler_driver: only efall=0 (no precipitation-energy fallout) is built");
+        return GM1B_ERR_ARGUMENT;
+    }
+    if (!(dx > 0.0f) || !(dy > 0.0f) || !(dz > 0.0f) || !(dt > 0.0f) || !isfinite(dx) || !isfinite(dy) ||
+        !isfinite(dz) || !isfinite(dt)) {
+        gm1b_set_error("gm1b_kessler_driver: dx, dy, dz, dt must be finite and > 0");
+        return GM1B_ERR_ARGUMENT;
+    }
+    const gm1b_kessler_arrays &a = *arrays;
+    const void *required[] = {a.ruh, a.rvh, a.rmh, a.mh, a.pi0, a.th0, a.rr, a.rho, a.pp3d, a.th3d, a.prs,
+                              a.qv,  a.qc,  a.qr,  a.fall_velocity, a.rain, a.prate, a.asq, a.qbudget};
+    for (const void *p : required)
+        if (p == nullptr) {
+            gm1b_set_error("gm1b_kessler_driver: a required array is NULL");
+            return GM1B_ERR_ARGUMENT;
+        }
+    if (workspace == nullptr || workspace_size < workspace_bytes(ni, nj, nk) ||
+        (reinterpret_cast<uintptr_t>(workspace) & 15u) != 0u) {
+        gm1b_set_error("gm1b_kessler_driver: workspace must be 16-byte aligned and hold %zu bytes",
+                       workspace_bytes(ni, nj, nk));
+        return GM1B_ERR_ARGUMENT;
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const KDims d{ni, nj, nk};
+    const KWork w = carve(workspace, ni, nj, nk);
+    const KConst c = make_constants();
+    if (cudaMemsetAsync(w.status, 0, 16, st) != cudaSuccess) {
+        gm1b_set_error("gm1b_kessler_driver: status reset failed");
+        return GM1B_ERR_CUDA;
+    }
+    const float rdz = 1.0f / dz;
+    {
+        ProfScope ps("kessler_column_kernel", st);
+        kessler_column_kernel<<<dim3((ni + kCX - 1) / kCX, (nj + kCY - 1) / kCY), dim3(kCX, kCY), 0, st>>>(a, d, w, c,
+                                                                                                         dt, rdz);
+        ps.stop();
+    }
+    if (!launched("kessler_column_kernel")) return GM1B_ERR_CUDA;
+    {
+        ProfScope ps("kessler_cell_kernel", st);
+        kessler_cell_kernel<<<dim3(w.nbx, nj, nk), kKX, 0, st>>>(a, d, w, c, dt, equation_set);
+        ps.stop();
+    }
+    if (!launched("kessler_cell_kernel")) return GM1B_ERR_CUDA;
+    {
+        ProfScope ps("kessler_rows_kernel", st);
+        kessler_rows_kernel<<<(5 * nj + 127) / 128, 128, 0, st>>>(d, w);
+        ps.stop();
+    }
+    if (!launched("kessler_rows_kernel")) return GM1B_ERR_CUDA;
+    const double volume = (double)((dx * dy) * dz);
+    const double area = (double)(dx * dy);
+    {
+        ProfScope ps("kessler_finish_kernel", st);
+        kessler_finish_kernel<<<1, 1, 0, st>>>(a, d, w, volume, (double)dx, (double)dy, area);
+        ps.stop();
+    }
+    if (!launched("kessler_finish_kernel")) return GM1B_ERR_CUDA;
+    return GM1B_OK;
+}

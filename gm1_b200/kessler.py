@@ -1,0 +1,208 @@
+"""Kessler warm rain with saturation adjustment on B200.
+
+Drop-in mirror of the reference operator API (torch CUDA tensors in place of
+CuPy arrays; the same array names, shapes, dtypes, keywords and refusals):
+
+  Gm1KesslerDriverSelection                 src/cm1core/cuda_gm1_kessler_driver.py:100-160
+  gm1_kessler_driver_shapes                 src/cm1core/cuda_gm1_kessler_driver.py:183-206
+  create_cuda_gm1_kessler_driver_workspace  src/cm1core/cuda_gm1_kessler_driver.py:806
+  launch_cuda_gm1_kessler_driver            src/cm1core/cuda_gm1_kessler_driver.py:907
+
+Only efall = 0 is built (the benchmark configurations use it); efall = 1 is
+refused by name.  Device faults never stand in for errors: the saturation
+adjustment's non-convergence is a status word that ``CudaKesslerLaunch.check``
+turns into the reference's RuntimeError.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import math
+from dataclasses import dataclass
+from typing import Any, Mapping
+
+import torch
+
+from . import _native
+from .errors import refuse
+
+
+@dataclass(frozen=True, slots=True)
+class Gm1KesslerDriverSelection:
+    ptype: int = 1
+    equation_set: int = 1
+    testcase: int = 0
+    pdscheme: int = 1
+    efall: int = 0
+    axisymmetric: int = 0
+    moving_domain: int = 0
+    rain_bins: int = 1
+    nrk: int = 4
+    input_phase: str = "pre-pdefq"
+    output_phase: str = "post-satadj"
+
+
+DEFAULT_GM1_KESSLER_DRIVER_SELECTION = Gm1KesslerDriverSelection()
+
+INPUT_NAMES = ("ruh", "rvh", "rmh", "mh", "pi0", "th0", "rr")
+INOUT_NAMES = ("rho", "pp3d", "th3d", "prs", "qv", "qc", "qr", "fall_velocity", "rain", "prate", "asq", "qbudget")
+ALL_ARRAY_NAMES = INPUT_NAMES + INOUT_NAMES
+DOUBLE_NAMES = ("asq", "qbudget")
+
+
+def _validate_selection(selection: Gm1KesslerDriverSelection) -> None:
+    if not isinstance(selection, Gm1KesslerDriverSelection):
+        raise TypeError("selection must be a Gm1KesslerDriverSelection")
+    fixed = {"ptype": 1, "testcase": 0, "pdscheme": 1, "axisymmetric": 0, "moving_domain": 0, "rain_bins": 1,
+             "nrk": 4, "input_phase": "pre-pdefq", "output_phase": "post-satadj"}
+    for name, wanted in fixed.items():
+        value = getattr(selection, name)
+        if type(value) is not type(wanted) or value != wanted:
+            refuse(code="GM1-KESSLER-DRIVER-SELECTION", gate="physics-seam", option=name, value=value,
+                   reason="the Kessler operator is built for one exact native branch",
+                   remedy=f"use {name}={wanted!r}")
+    if type(selection.efall) is not int or selection.efall != 0:
+        refuse(code="GM1-KESSLER-DRIVER-EFALL", gate="physics-seam", option="efall", value=selection.efall,
+               reason="only the disabled precipitation-energy fallout branch (efall=0) is built here",
+               remedy="use efall=0")
+    if type(selection.equation_set) is not int or selection.equation_set not in (1, 2):
+        refuse(code="GM1-KESSLER-DRIVER-EQTSET", gate="physics-seam", option="equation_set",
+               value=selection.equation_set,
+               reason="the authority has exactly traditional and energy-conserving branches",
+               remedy="use equation_set=1 or equation_set=2")
+
+
+def gm1_kessler_driver_shapes(ni: int, nj: int, nk: int) -> dict[str, tuple[int, ...]]:
+    for name, value in (("ni", ni), ("nj", nj), ("nk", nk)):
+        if type(value) is not int or value < 1:
+            raise ValueError(f"{name} must be an integer >= 1")
+    mass = (nk, nj, ni)
+    shapes = {name: mass for name in ("rmh", "mh", "pi0", "th0", "rho", "rr", "pp3d", "th3d", "prs", "qv", "qc",
+                                      "qr", "fall_velocity")}
+    shapes.update({"ruh": (ni,), "rvh": (nj,), "rain": (1, nj, ni), "prate": (nj, ni), "asq": (3,),
+                   "qbudget": (10,)})
+    return shapes
+
+
+class _KesslerArrays(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_void_p) for n in (*INPUT_NAMES, "rho", "pp3d", "th3d", "prs", "qv", "qc", "qr",
+                                               "fall_velocity", "rain", "prate", "asq", "qbudget",
+                                               "satadj_iterations", "nfall")]
+
+
+def _bind() -> ctypes.CDLL:
+    lib = _native.lib()
+    if not getattr(lib, "_kessler_bound", False):
+        i32, f32 = ctypes.c_int32, ctypes.c_float
+        lib.gm1b_kessler_workspace_bytes.argtypes = [i32, i32, i32]
+        lib.gm1b_kessler_workspace_bytes.restype = ctypes.c_size_t
+        lib.gm1b_kessler_driver.argtypes = [i32, i32, i32, ctypes.POINTER(_KesslerArrays), f32, f32, f32, f32, i32,
+                                            i32, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]
+        lib.gm1b_kessler_driver.restype = i32
+        lib._kessler_bound = True
+    return lib
+
+
+@dataclass
+class Gm1KesslerDriverWorkspace:
+    """Caller-owned device scratch of the operator (budget partial sums and
+    the two status words)."""
+
+    ni: int
+    nj: int
+    nk: int
+    buffer: torch.Tensor
+
+    @property
+    def status(self) -> torch.Tensor:
+        return self.buffer[:16].view(torch.int32)
+
+
+def create_cuda_gm1_kessler_driver_workspace(*, ni: int, nj: int, nk: int,
+                                             device: torch.device | str = "cuda") -> Gm1KesslerDriverWorkspace:
+    gm1_kessler_driver_shapes(ni, nj, nk)
+    nbytes = int(_bind().gm1b_kessler_workspace_bytes(ni, nj, nk))
+    buf = torch.empty(((nbytes + 255) // 256) * 256, dtype=torch.uint8, device=device)
+    return Gm1KesslerDriverWorkspace(ni, nj, nk, buf)
+
+
+@dataclass(frozen=True)
+class CudaKesslerLaunch:
+    ready_event: torch.cuda.Event
+    workspace: Gm1KesslerDriverWorkspace
+    receipt: dict[str, Any]
+
+    def status(self) -> dict[str, int]:
+        """Waits for the launch and reads its status words."""
+        self.ready_event.synchronize()
+        s = self.workspace.status.cpu().tolist()
+        return {"satadj_nonconverged_cells": int(s[0]), "max_fall_substeps": int(s[1])}
+
+    def check(self) -> dict[str, int]:
+        """status(), raising like the reference if any saturation adjustment
+        did not converge within 100 iterations."""
+        s = self.status()
+        if s["satadj_nonconverged_cells"]:
+            raise RuntimeError("GM1 Kessler satadj failed to converge in 100 iterations "
+                               f"({s['satadj_nonconverged_cells']} cells)")
+        return s
+
+
+def _positive(name: str, value: float) -> float:
+    if isinstance(value, bool) or not isinstance(value, (int, float)):
+        raise TypeError(f"{name} must be a finite positive number")
+    result = float(value)
+    if not math.isfinite(result) or result <= 0.0:
+        raise ValueError(f"{name} must be finite and > 0")
+    return result
+
+
+def launch_cuda_gm1_kessler_driver(
+    arrays: Mapping[str, Any], *, ni: int, nj: int, nk: int, dx: float, dy: float, dz: float, dt: float,
+    selection: Gm1KesslerDriverSelection = DEFAULT_GM1_KESSLER_DRIVER_SELECTION, stream: Any | None = None,
+    workspace: Gm1KesslerDriverWorkspace | None = None, satadj_iterations: torch.Tensor | None = None,
+    nfall: torch.Tensor | None = None,
+) -> CudaKesslerLaunch:
+    """Enqueue the complete Kessler operator in place without synchronising."""
+    _validate_selection(selection)
+    shapes = gm1_kessler_driver_shapes(ni, nj, nk)
+    dx, dy, dz, dt = (_positive(n, v) for n, v in (("dx", dx), ("dy", dy), ("dz", dz), ("dt", dt)))
+    missing = [n for n in ALL_ARRAY_NAMES if n not in arrays]
+    if missing:
+        raise ValueError(f"missing GM1 Kessler driver arrays: {', '.join(missing)}")
+    a: dict[str, torch.Tensor] = {}
+    for n in ALL_ARRAY_NAMES:
+        t = arrays[n]
+        dtype = torch.float64 if n in DOUBLE_NAMES else torch.float32
+        if not isinstance(t, torch.Tensor) or not t.is_cuda or t.dtype != dtype or tuple(t.shape) != shapes[n] \
+                or not t.is_contiguous():
+            raise ValueError(f"{n} must be a contiguous CUDA {dtype} tensor with shape {shapes[n]}")
+        a[n] = t
+    if satadj_iterations is not None:
+        if satadj_iterations.dtype != torch.int32 or tuple(satadj_iterations.shape) != (nk, nj, ni):
+            raise ValueError("satadj_iterations must be an int32 (uint32 words) tensor of the mass shape")
+        a["satadj_iterations"] = satadj_iterations
+    if nfall is not None:
+        if nfall.dtype != torch.int32 or tuple(nfall.shape) != (nj, ni):
+            raise ValueError("nfall must be an int32 tensor of shape (nj, ni)")
+        a["nfall"] = nfall
+    ptrs = [t.data_ptr() for t in a.values()]
+    if len(set(ptrs)) != len(ptrs):
+        raise ValueError("GM1 Kessler driver arrays must not alias")
+    device = a["rho"].device
+    if workspace is None:
+        workspace = create_cuda_gm1_kessler_driver_workspace(ni=ni, nj=nj, nk=nk, device=device)
+    elif (workspace.ni, workspace.nj, workspace.nk) != (ni, nj, nk):
+        raise ValueError("workspace was created for another grid")
+    s = _KesslerArrays(**{n: t.data_ptr() for n, t in a.items()})
+    st = torch.cuda.current_stream(device) if stream is None else stream
+    with torch.cuda.device(device):
+        _native.check(_bind().gm1b_kessler_driver(ni, nj, nk, ctypes.byref(s), dx, dy, dz, dt,
+                                                  selection.equation_set, selection.efall,
+                                                  ctypes.c_void_p(workspace.buffer.data_ptr()),
+                                                  workspace.buffer.numel(), ctypes.c_void_p(st.cuda_stream)),
+                      "gm1b_kessler_driver")
+        ev = torch.cuda.Event()
+        ev.record(st)
+    return CudaKesslerLaunch(ev, workspace, {"operator": "gm1-kessler-driver", "equation_set": selection.equation_set,
+                                             "efall": selection.efall, "domain": {"ni": ni, "nj": nj, "nk": nk}})

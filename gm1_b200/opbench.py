@@ -1,0 +1,119 @@
+"""Per-operator device throughput on B200 (library profiling facility).
+
+    python -m gm1_b200.opbench [--ops adv5 adv5-weno massflux] [--grid 256 256 80] [--iters 20]
+
+For each operator: seeded synthetic inputs of the given padded-lane grid
+resident in HBM, a 256 MiB L2 flush before every launch, CUDA events around
+each launch on the launching stream; prints one JSON line per operator with
+cells/s, the average launch time, the algorithmic bytes per cell (every full
+field read or written once; halos, stencil re-reads and 2-D metrics not
+counted) and the fraction of the measured HBM copy bandwidth.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+from pathlib import Path
+
+import torch
+
+from .advection import launch_cuda_scalar_advection5, launch_cuda_terrain_mass_flux5, padded_shapes
+
+ROOT = Path(__file__).resolve().parents[1]
+
+# words per cell
+ALG_WORDS = {
+    # in: scalar rru rrv rrw divx rr0 c1 c2; out: tendency
+    "adv5": 9,
+    "adv5-weno": 9,
+    # in: u v w rho0 rf0; out: rru rrv rrw divx
+    "massflux": 9,
+}
+
+
+def hbm_peak() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def synthetic_padded(ni: int, nj: int, nk: int, device: torch.device, seed: int = 0) -> dict[str, torch.Tensor]:
+    g = torch.Generator(device=device).manual_seed(seed)
+    sh = padded_shapes(ni, nj, nk)
+
+    def u(shape, lo, hi):
+        return (torch.rand(shape, generator=g, device=device) * (hi - lo) + lo).contiguous()
+
+    a = {
+        "scalar": u(sh["scalar"], 290.0, 310.0),
+        "rru": u(sh["u"], -9.0, 9.0), "rrv": u(sh["v"], -9.0, 9.0), "rrw": u(sh["w"], -2.0, 2.0),
+        "u3d": u(sh["u"], -12.0, 12.0), "v3d": u(sh["v"], -12.0, 12.0), "w3d": u(sh["w"], -3.0, 3.0),
+        "c1": u(sh["face"], 0.3, 0.7), "rr0": u(sh["cell"], 0.8, 1.6), "rho0_3d": u(sh["cell"], 0.6, 1.2),
+        "rf0": u(sh["face"], 0.6, 1.2), "divx": u(sh["cell"], -1e-3, 1e-3),
+        "gz": u((nj, ni), 0.97, 1.03), "rgzu": u((nj, ni + 1), 0.95, 1.05), "rgzv": u((nj + 1, ni), 0.95, 1.05),
+        "dzdx": u((nj, ni), -0.02, 0.02), "dzdy": u((nj, ni), -0.02, 0.02),
+        "tendency": torch.zeros(sh["cell"], device=device),
+        "mf_rru": torch.zeros(sh["u"], device=device), "mf_rrv": torch.zeros(sh["v"], device=device),
+        "mf_rrw": torch.zeros(sh["w"], device=device), "mf_divx": torch.zeros(sh["cell"], device=device),
+    }
+    a["c2"] = 1.0 - a["c1"]
+    return a
+
+
+def run(op: str, a: dict[str, torch.Tensor], ni: int, nj: int, nk: int, stream: torch.cuda.Stream, chunk: int | None):
+    if op in ("adv5", "adv5-weno"):
+        launch_cuda_scalar_advection5(
+            a["scalar"], {k: a[k] for k in ("rru", "rrv", "rrw")}, {k: a[k] for k in ("c1", "c2", "rr0", "gz")},
+            a["divx"], a["tendency"], None, ni=ni, nj=nj, nk=nk, nrk=3 if op == "adv5-weno" else 1,
+            dx=1000.0, dy=1000.0, dz=250.0, weps=1e-6, lateral_sides=(1, 1, 1, 1), write_fluxes=False,
+            levels_per_chunk=chunk, stream=stream)
+    elif op == "massflux":
+        launch_cuda_terrain_mass_flux5(
+            {"u3d": a["u3d"], "v3d": a["v3d"], "w3d": a["w3d"], "rru": a["mf_rru"], "rrv": a["mf_rrv"],
+             "rrw": a["mf_rrw"]},
+            {k: a[k] for k in ("rho0_3d", "rf0", "rgzu", "rgzv", "dzdx", "dzdy", "gz")}, a["mf_divx"],
+            ni=ni, nj=nj, nk=nk, dx=1000.0, dy=1000.0, dz=250.0, stream=stream)
+    else:
+        raise ValueError(op)
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ops", nargs="+", default=["adv5", "adv5-weno", "massflux"])
+    ap.add_argument("--grid", nargs=3, type=int, default=[256, 256, 80], metavar=("NI", "NJ", "NK"))
+    ap.add_argument("--iters", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--chunk", type=int, default=None)
+    args = ap.parse_args()
+    ni, nj, nk = args.grid
+    device = torch.device("cuda", 0)
+    a = synthetic_padded(ni, nj, nk, device)
+    flush = torch.empty(256 * 1024 * 1024 // 4, device=device)
+    stream = torch.cuda.Stream(device)
+    peak, kind = hbm_peak()
+    cells = ni * nj * nk
+    for op in args.ops:
+        with torch.cuda.stream(stream):
+            for _ in range(args.warmup):
+                run(op, a, ni, nj, nk, stream, args.chunk)
+            starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.iters)]
+            ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.iters)]
+            for q in range(args.iters):
+                flush.zero_()
+                starts[q].record(stream)
+                run(op, a, ni, nj, nk, stream, args.chunk)
+                ends[q].record(stream)
+        stream.synchronize()
+        ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends)) / args.iters
+        alg = ALG_WORDS[op] * 4 * cells
+        gbs = alg / (ms * 1e-3) / 1e9
+        print(json.dumps({"op": op, "grid": [ni, nj, nk], "cells": cells, "ms_per_launch": ms,
+                          "cells_per_s": cells / (ms * 1e-3), "alg_bytes_per_cell": ALG_WORDS[op] * 4,
+                          "achieved_gbs": gbs, "peak_gbs": peak, "frac": gbs / peak, "peak_source": kind,
+                          "chunk": args.chunk}), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -24,6 +24,7 @@
 #ifndef GM1B_H
 #define GM1B_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -181,6 +182,44 @@ GM1B_API int32_t gm1b_scalar_advection5(int32_t ni, int32_t nj, int32_t nk,
                                         int32_t nrk, int32_t wflag, float dx, float dy,
                                         float dz, double weps, uint32_t lateral_obc,
                                         int32_t levels_per_chunk, void *stream);
+
+/* ------------------------------------------------------------------------
+ * Kessler warm rain (compact mass arrays (nk, nj, ni), no halos)
+ * ---------------------------------------------------------------------- */
+typedef struct gm1b_kessler_arrays {
+    /* inputs: ruh (ni), rvh (nj), rmh/mh/pi0/th0/rr mass-shaped */
+    const float *ruh, *rvh, *rmh, *mh, *pi0, *th0, *rr;
+    /* in/out, mass-shaped except rain (1, nj, ni) and prate (nj, ni) */
+    float *rho, *pp3d, *th3d, *prs, *qv, *qc, *qr, *fall_velocity, *rain, *prate;
+    /* in/out FP64 budgets: asq[3] (pdefq of qv, qc, qr), qbudget[10] */
+    double *asq, *qbudget;
+    /* optional outputs (NULL = not written): saturation-adjustment
+     * iterations per cell (uint32, mass-shaped) and fallout sub-steps per
+     * column (int32, (nj, ni)) */
+    uint32_t *satadj_iterations;
+    int32_t *nfall;
+} gm1b_kessler_arrays;
+
+/* Bytes of device workspace gm1b_kessler_driver needs for this grid. */
+GM1B_API size_t gm1b_kessler_workspace_bytes(int32_t ni, int32_t nj, int32_t nk);
+
+/*
+ * The complete Kessler operator, in place: pdefq(qv, qc, qr), rain fall
+ * speed, rain-energy budget, fallout sub-stepping, local conversion and
+ * saturation adjustment (equation_set 1 or 2; efall must be 0).
+ * `workspace` (16-byte aligned, gm1b_kessler_workspace_bytes) holds the
+ * budget partial sums; its first two int32 words are set by the call to the
+ * number of cells whose saturation adjustment did not converge within 100
+ * iterations (the reference raises on any) and the largest fallout
+ * sub-step count.
+ * Replaces launch_cuda_gm1_kessler_driver
+ * (src/cm1core/cuda_gm1_kessler_driver.py:907) and its CPU twin
+ * cpu_gm1_kessler_driver_inplace (:431).
+ */
+GM1B_API int32_t gm1b_kessler_driver(int32_t ni, int32_t nj, int32_t nk,
+                                     const gm1b_kessler_arrays *arrays, float dx, float dy,
+                                     float dz, float dt, int32_t equation_set, int32_t efall,
+                                     void *workspace, size_t workspace_size, void *stream);
 
 /*
  * Launch profiler.  While enabled, every kernel launch of the library is

@@ -264,6 +264,74 @@ def make_advection(reference: Path) -> None:
         print("wrote", tag)
 
 
+def kessler_fixture(ni: int, nj: int, nk: int, dz: float, seed: int) -> dict[str, np.ndarray]:
+    """Compact Kessler driver inputs: a moist, partly saturated column set
+    with cloud, rain heavy enough for several fallout sub-steps, and small
+    negative mixing ratios for pdefq to repair."""
+    rng = np.random.default_rng(seed)
+    rd, cp, p00 = 287.04, 1005.7, 1.0e5
+    z = (np.arange(nk) + 0.5) * dz
+    th0 = 300.0 + 0.004 * z
+    pi0 = 1.0 - 9.81 * z / (cp * 305.0)
+    shape = (nk, nj, ni)
+
+    def bc(x):
+        return np.broadcast_to(x[:, None, None], shape).astype(np.float32).copy()
+
+    a = {
+        "ruh": (1.0 + 0.01 * rng.standard_normal(ni)).astype(np.float32),
+        "rvh": (1.0 + 0.01 * rng.standard_normal(nj)).astype(np.float32),
+        "rmh": (1.0 + 0.02 * rng.random(shape)).astype(np.float32),
+        "mh": (1.0 + 0.02 * rng.random(shape)).astype(np.float32),
+        "pi0": bc(pi0),
+        "th0": bc(th0),
+        "th3d": rng.uniform(-1.5, 2.5, shape).astype(np.float32),
+        "pp3d": rng.uniform(-2e-4, 2e-4, shape).astype(np.float32),
+    }
+    t = (a["th0"] + a["th3d"]) * (a["pi0"] + a["pp3d"])
+    prs = p00 * (a["pi0"] + a["pp3d"]).astype(np.float64) ** (cp / rd)
+    a["prs"] = prs.astype(np.float32)
+    a["rho"] = (prs / (rd * t)).astype(np.float32)
+    a["rr"] = a["rho"].copy()
+    esl = 611.2 * np.exp(17.67 * (t - 273.15) / (t - 29.65))
+    qvs = 0.622 * esl / (prs - esl)
+    a["qv"] = (qvs * rng.uniform(0.7, 1.08, shape)).astype(np.float32)
+    a["qc"] = np.where(rng.random(shape) < 0.5, rng.uniform(0.0, 2.5e-3, shape), 0.0).astype(np.float32)
+    a["qr"] = np.where(rng.random(shape) < 0.6, rng.uniform(0.0, 6.0e-3, shape), 0.0).astype(np.float32)
+    for name in ("qc", "qr"):
+        flat = a[name].reshape(-1)
+        idx = rng.choice(flat.size, size=flat.size // 20, replace=False)
+        flat[idx] = rng.uniform(-2e-5, 0.0, idx.size).astype(np.float32)
+    a["qc"][0, 0, 0] = np.float32(5e-15)  # below rmax: pdefq clears it
+    a["fall_velocity"] = np.zeros(shape, np.float32)
+    a["rain"] = rng.uniform(0.0, 0.5, (1, nj, ni)).astype(np.float32)
+    a["prate"] = np.zeros((nj, ni), np.float32)
+    a["asq"] = rng.uniform(-1.0, 1.0, 3)
+    a["qbudget"] = rng.uniform(-1.0, 1.0, 10)
+    return a
+
+
+def make_kessler(reference: Path) -> None:
+    sys.path.insert(0, str(reference / "src"))
+    from cm1core.cuda_gm1_kessler_driver import Gm1KesslerDriverSelection, cpu_gm1_kessler_driver_inplace
+
+    for tag, (ni, nj, nk, dz, dt, eqtset, seed) in {
+        "kessler_eqt2_7x5x12": (7, 5, 12, 100.0, 30.0, 2, 31),
+        "kessler_eqt1_6x6x10": (6, 6, 10, 150.0, 12.0, 1, 32),
+    }.items():
+        a = kessler_fixture(ni, nj, nk, dz, seed)
+        inputs = {f"in_{k}": v.copy() for k, v in a.items()}
+        result = cpu_gm1_kessler_driver_inplace(a, ni=ni, nj=nj, nk=nk, dx=1000.0, dy=1000.0, dz=dz, dt=dt,
+                                                selection=Gm1KesslerDriverSelection(equation_set=eqtset))
+        outputs = {f"out_{k}": v for k, v in a.items()}
+        outputs["out_satadj_iterations"] = result["satadj"]["iterations"]
+        meta = dict(ni=ni, nj=nj, nk=nk, dx=1000.0, dy=1000.0, dz=dz, dt=dt, eqtset=eqtset,
+                    max_fall_substeps=result["max_fall_substeps"])
+        np.savez_compressed(HERE / f"{tag}.npz", meta=json.dumps(meta), **inputs, **outputs)
+        print("wrote", tag, "max nfall", result["max_fall_substeps"],
+              "iterations", int(result["satadj"]["iterations"].max()))
+
+
 def make_c1(reference: Path, checkpoints: list[int]) -> None:
     """Digests after each checkpoint N, each from a fresh state with one call
     of steps=N (the reference refuses a non-fresh entry state, ppx != pp3d,
@@ -300,13 +368,15 @@ def make_c1(reference: Path, checkpoints: list[int]) -> None:
 def main() -> None:
     p = argparse.ArgumentParser()
     p.add_argument("--reference", type=Path, required=True, help="root of the reference source tree")
-    p.add_argument("what", choices=("small", "c1", "advection"))
+    p.add_argument("what", choices=("small", "c1", "advection", "kessler"))
     p.add_argument("--checkpoints", type=int, nargs="+", default=[1])
     args = p.parse_args()
     if args.what == "small":
         make_small(args.reference)
     elif args.what == "advection":
         make_advection(args.reference)
+    elif args.what == "kessler":
+        make_kessler(args.reference)
     else:
         make_c1(args.reference, sorted(set(args.checkpoints)))
 

@@ -1,0 +1,72 @@
+"""Parity of the CUDA Kessler operator (through the C ABI) with the
+reference's own CPU twin (golden vectors) and with the oracle, under the
+tolerances stated in tests/kessler_common.py."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+from gm1_b200.kessler import Gm1KesslerDriverSelection, launch_cuda_gm1_kessler_driver
+from oracle import kessler as ko
+from tests._golden import load_npz
+from tests.kessler_common import assert_budgets_close, assert_fields_close
+from tests.test_oracle_kessler import TAGS
+
+pytestmark = pytest.mark.gpu
+
+
+def run_gpu(inputs, meta):
+    d = {k: torch.from_numpy(np.ascontiguousarray(v)).cuda() for k, v in inputs.items()}
+    it = torch.zeros((meta["nk"], meta["nj"], meta["ni"]), dtype=torch.int32, device="cuda")
+    nf = torch.zeros((meta["nj"], meta["ni"]), dtype=torch.int32, device="cuda")
+    launch = launch_cuda_gm1_kessler_driver(
+        d, ni=meta["ni"], nj=meta["nj"], nk=meta["nk"], dx=meta["dx"], dy=meta["dy"], dz=meta["dz"], dt=meta["dt"],
+        selection=Gm1KesslerDriverSelection(equation_set=meta["eqtset"]), satadj_iterations=it, nfall=nf)
+    status = launch.check()
+    got = {k: v.cpu().numpy() for k, v in d.items()}
+    return got, it.cpu().numpy().view(np.uint32), nf.cpu().numpy(), status
+
+
+@pytest.mark.parametrize("tag", TAGS)
+def test_kessler_matches_reference(tag):
+    meta, inputs, out = load_npz(tag)
+    got, it, _, status = run_gpu(inputs, meta)
+    assert status["max_fall_substeps"] == meta["max_fall_substeps"]
+    assert np.array_equal(it, out["satadj_iterations"])
+    assert_fields_close(out, got)
+    assert np.array_equal(got["asq"].view(np.uint64), out["asq"].view(np.uint64))
+    assert_budgets_close(out["qbudget"], got["qbudget"])
+
+
+@pytest.mark.parametrize("tag", TAGS)
+def test_kessler_matches_oracle_and_is_repeatable(tag):
+    meta, inputs, _ = load_npz(tag)
+    want = {k: v.copy() for k, v in inputs.items()}
+    nf_want = np.zeros((meta["nj"], meta["ni"]), np.int32)
+    it_want = np.zeros((meta["nk"], meta["nj"], meta["ni"]), np.uint32)
+    ko.kessler_driver(want, ni=meta["ni"], nj=meta["nj"], nk=meta["nk"], dx=meta["dx"], dy=meta["dy"],
+                      dz=meta["dz"], dt=meta["dt"], eqtset=meta["eqtset"], iterations=it_want, nfall=nf_want)
+    got, it, nf, _ = run_gpu(inputs, meta)
+    again, _, _, _ = run_gpu(inputs, meta)
+    assert np.array_equal(nf, nf_want)
+    assert np.array_equal(it, it_want)
+    assert_fields_close(want, got)
+    for k in got:  # run-to-run bit reproducibility (fixed-order reductions)
+        assert np.array_equal(np.ascontiguousarray(got[k]).view(np.uint8), np.ascontiguousarray(again[k]).view(np.uint8)), k
+
+
+def test_kessler_large_domain_matches_oracle():
+    """A 96x64x40 domain exercises many CTAs and budget partials."""
+    from tests.golden.make_golden import kessler_fixture
+
+    ni, nj, nk, dz, dt = 96, 64, 40, 100.0, 20.0
+    inputs = kessler_fixture(ni, nj, nk, dz, 77)
+    meta = dict(ni=ni, nj=nj, nk=nk, dx=1000.0, dy=1000.0, dz=dz, dt=dt, eqtset=2)
+    want = {k: v.copy() for k, v in inputs.items()}
+    ko.kessler_driver(want, ni=ni, nj=nj, nk=nk, dx=1000.0, dy=1000.0, dz=dz, dt=dt, eqtset=2)
+    got, _, _, _ = run_gpu(inputs, meta)
+    assert_fields_close(want, got)
+    assert np.array_equal(got["asq"].view(np.uint64), want["asq"].view(np.uint64))
+    assert_budgets_close(want["qbudget"], got["qbudget"])
