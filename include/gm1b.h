@@ -221,6 +221,28 @@ GM1B_API int32_t gm1b_kessler_driver(int32_t ni, int32_t nj, int32_t nk,
                                      float dz, float dt, int32_t equation_set, int32_t efall,
                                      void *workspace, size_t workspace_size, void *stream);
 
+/* ------------------------------------------------------------------------
+ * SGS/TKE local algebra: every array (nk+1, nj, ni) (w levels) except
+ * ruh (ni) and rvh (nj)
+ * ---------------------------------------------------------------------- */
+typedef struct gm1b_sgs_tke_arrays {
+    const float *ruh, *rvh, *rmf, *nm, *defv, *defh;
+    float *tkea, *tk, *grdscl, *rgrdscl, *lenscl, *dissten;
+    float *cme, *ce1, *ce2, *csm, *kmh, *kmv, *khh, *khv, *tketen;
+    /* optional (NULL = not written): count of clipped TKE words */
+    uint32_t *clip_count;
+} gm1b_sgs_tke_arrays;
+
+/*
+ * Deardorff tkekm on levels 1..nk-1 (grid and length scales, Km = Kh/Pr,
+ * dissipation added into dissten), the free-slip lower face (tkebc) and the
+ * pre-turbt TKE source tketen = -Kh N^2 - dissten + Km max(0, defv + defh).
+ * Replaces launch_cuda_sgs_tke (src/cm1core/cuda_sgs_tke.py:637) and its CPU
+ * twin cpu_sgs_tke_inplace (:220).
+ */
+GM1B_API int32_t gm1b_sgs_tke(int32_t ni, int32_t nj, int32_t nk, const gm1b_sgs_tke_arrays *arrays,
+                              float dx, float dy, float dz, void *stream);
+
 /*
  * Launch profiler.  While enabled, every kernel launch of the library is
  * bracketed by a pair of CUDA events recorded on its own stream (the

@@ -332,6 +332,43 @@ def make_kessler(reference: Path) -> None:
               "iterations", int(result["satadj"]["iterations"].max()))
 
 
+def sgs_tke_fixture(ni: int, nj: int, nk: int, seed: int) -> dict[str, np.ndarray]:
+    rng = np.random.default_rng(seed)
+    cell = (nk + 1, nj, ni)
+    a = {
+        "ruh": (1.0 + 0.05 * rng.standard_normal(ni)).astype(np.float32),
+        "rvh": (1.0 + 0.05 * rng.standard_normal(nj)).astype(np.float32),
+        "rmf": rng.uniform(0.7, 1.4, cell).astype(np.float32),
+        "nm": rng.uniform(-2e-4, 3e-4, cell).astype(np.float32),
+        "defv": rng.uniform(-1e-5, 4e-4, cell).astype(np.float32),
+        "defh": rng.uniform(-1e-5, 4e-4, cell).astype(np.float32),
+        "tkea": (rng.uniform(0.0, 1.0, cell) ** 3 * 2.5).astype(np.float32),
+        "dissten": rng.uniform(-1e-4, 1e-4, cell).astype(np.float32),
+    }
+    flat = a["tkea"].reshape(-1)
+    flat[rng.choice(flat.size, size=flat.size // 10, replace=False)] = np.float32(1e-11)
+    for name in ("tk", "grdscl", "rgrdscl", "lenscl", "cme", "ce1", "ce2", "csm", "kmh", "kmv", "khh", "khv",
+                 "tketen"):
+        a[name] = np.full(cell, np.float32(7.0), dtype=np.float32)
+    return a
+
+
+def make_tke(reference: Path) -> None:
+    sys.path.insert(0, str(reference / "src"))
+    from cm1core.cuda_sgs_tke import cpu_sgs_tke_inplace, sgs_constants_f32
+
+    for tag, (ni, nj, nk, dx, dy, dz, seed) in {"sgs_tke_9x7x12": (9, 7, 12, 1000.0, 1000.0, 250.0, 41),
+                                                 "sgs_tke_6x8x10": (6, 8, 10, 100.0, 120.0, 40.0, 42)}.items():
+        a = sgs_tke_fixture(ni, nj, nk, seed)
+        inputs = {f"in_{k}": v.copy() for k, v in a.items()}
+        r = cpu_sgs_tke_inplace(a, ni=ni, nj=nj, nk=nk, dx=dx, dy=dy, dz=dz)
+        outputs = {f"out_{k}": v for k, v in a.items()}
+        meta = dict(ni=ni, nj=nj, nk=nk, dx=dx, dy=dy, dz=dz, clipped=r.clipped_tke_words,
+                    constants={k: float(v) for k, v in sgs_constants_f32().items()})
+        np.savez_compressed(HERE / f"{tag}.npz", meta=json.dumps(meta), **inputs, **outputs)
+        print("wrote", tag, "clipped", r.clipped_tke_words)
+
+
 def make_c1(reference: Path, checkpoints: list[int]) -> None:
     """Digests after each checkpoint N, each from a fresh state with one call
     of steps=N (the reference refuses a non-fresh entry state, ppx != pp3d,
@@ -368,7 +405,7 @@ def make_c1(reference: Path, checkpoints: list[int]) -> None:
 def main() -> None:
     p = argparse.ArgumentParser()
     p.add_argument("--reference", type=Path, required=True, help="root of the reference source tree")
-    p.add_argument("what", choices=("small", "c1", "advection", "kessler"))
+    p.add_argument("what", choices=("small", "c1", "advection", "kessler", "tke"))
     p.add_argument("--checkpoints", type=int, nargs="+", default=[1])
     args = p.parse_args()
     if args.what == "small":
@@ -377,6 +414,8 @@ def main() -> None:
         make_advection(args.reference)
     elif args.what == "kessler":
         make_kessler(args.reference)
+    elif args.what == "tke":
+        make_tke(args.reference)
     else:
         make_c1(args.reference, sorted(set(args.checkpoints)))
 
