@@ -241,6 +241,221 @@ __device__ __forceinline__ float y_face_flux(const float *__restrict__ s, const 
     return m * r;
 }
 
+// ---------------------------------------------------------------------------
+// tiled fused scalar advection: grid (ceil(ni/32), ceil(nj/8), level chunks)
+//
+// Per level the CTA stages the scalar plane of its 32x8 tile plus a 3-cell
+// halo (38 x 14 words) in shared memory and forms every x and y face flux of
+// the tile once from it; each thread keeps the six levels k-2..k+3 of its own
+// column in registers for the vertical flux of face k+1, whose value is
+// carried to the next level as the lower face.  Offsets are 32-bit.
+// ---------------------------------------------------------------------------
+constexpr int kTX5 = 32, kTY5 = 8;
+constexpr int kPX = kTX5 + 6, kPY = kTY5 + 6;
+
+template <bool WENO>
+__device__ __forceinline__ float recon_dir(const float *p, int stride, float m, double eps) {
+    // p points at the face's upwind-side cell x-1 for m >= 0 ... reconstruction
+    // over p[-2..2] (m >= 0: s(x-3..x+1) oriented; m < 0: s(x+2..x-2))
+    if (m >= 0.0f)
+        return recon<WENO>(p[-3 * stride], p[-2 * stride], p[-1 * stride], p[0], p[stride], eps);
+    return recon<WENO>(p[2 * stride], p[stride], p[0], p[-1 * stride], p[-2 * stride], eps);
+}
+
+template <bool WENO>
+__device__ __forceinline__ float z_face(const float win[6], float m, float c1, float c2, int face, int nk,
+                                        double eps, float wepsf) {
+    // win[q] holds level face-3+q (q = 0..5), i.e. win[3] = level face
+#define L(lev) win[(lev) - face + 3]
+    float r;
+    if (face == 2) {
+        if (m >= 0.0f)
+            r = c1 * L(1) + c2 * L(2);
+        else if (WENO)
+            r = upstrpd(L(3), L(2), L(1), wepsf);
+        else
+            r = flx3(L(3), L(2), L(1));
+    } else if (face == nk) {
+        const bool up = WENO ? (m > 0.0f) : (m >= 0.0f);
+        if (up)
+            r = WENO ? upstrpd(L(face - 2), L(face - 1), L(face), wepsf) : flx3(L(face - 2), L(face - 1), L(face));
+        else
+            r = c1 * L(face - 1) + c2 * L(face);
+    } else if (face == 3) {
+        if (m >= 0.0f)
+            r = WENO ? upstrpd(L(1), L(2), L(3), wepsf) : flx3(L(1), L(2), L(3));
+        else
+            r = recon<WENO>(L(5), L(4), L(3), L(2), L(1), eps);
+    } else if (face == nk - 1) {
+        if (m >= 0.0f)
+            r = recon<WENO>(L(face - 3), L(face - 2), L(face - 1), L(face), L(face + 1), eps);
+        else if (WENO)
+            r = upstrpd(L(face + 1), L(face), L(face - 1), wepsf);
+        else
+            r = flx3(L(face + 1), L(face), L(face - 1));
+    } else if (m >= 0.0f) {
+        r = recon<WENO>(L(face - 3), L(face - 2), L(face - 1), L(face), L(face + 1), eps);
+    } else {
+        r = recon<WENO>(L(face + 2), L(face + 1), L(face), L(face - 1), L(face - 2), eps);
+    }
+#undef L
+    return m * r;
+}
+
+template <bool WENO>
+__global__ void __launch_bounds__(kTX5 *kTY5)
+    scalar_advection5_tiled_kernel(gm1b_scalar_advection5_arrays a, PaddedDims d, int levels_per_chunk, float rdx,
+                                   float rdy, float rdsf, double eps, float wepsf, unsigned obc) {
+    __shared__ float s_plane[kPY][kPX];
+    __shared__ float s_fx[kTY5][kTX5 + 1];
+    __shared__ float s_fy[kTY5 + 1][kTX5];
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int tid = ty * kTX5 + tx;
+    const int i0 = blockIdx.x * kTX5, j0 = blockIdx.y * kTY5;
+    const int i = i0 + tx, j = j0 + ty;
+    const int ni = d.ni, nj = d.nj, nk = d.nk;
+    const int sx = ni + 2 * NG, sy = nj + 2 * NG;        // scalar / w plane
+    const int ux = ni + 1 + 2 * NG;                      // u row length
+    const int vy = nj + 1 + 2 * NG;                      // v rows
+    const int splane = sx * sy, uplane = ux * sy, vplane = sx * vy, cplane = ni * nj;
+    const bool cell = i < ni && j < nj;
+    const int x = i + NG, y = j + NG;
+    const int k_begin = 1 + blockIdx.z * levels_per_chunk;
+    const int k_end = min(nk, k_begin + levels_per_chunk - 1);
+    const float *s = a.scalar;
+    const bool owned = cell && (obc != 0u || (i >= 3 && i + 3 < ni && j >= 3 && j + 3 < nj));
+    const bool east_face = cell && (tx == kTX5 - 1 || i == ni - 1);
+    const bool north_face = cell && (ty == kTY5 - 1 || j == nj - 1);
+    const float gz = cell ? __ldg(a.gz + j * ni + i) : 0.0f;
+    const int col = y * sx + x;  // offset of this column inside a scalar/w plane
+    // register window of this column: win[q] = level (k+1) - 3 + q, k = k_begin - 1 initially
+    float win[6];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+        const int lev = k_begin - 3 + q;  // face k_begin needs levels k_begin-3 .. k_begin+2
+        win[q] = (cell && lev >= 0 && lev <= nk + 1) ? __ldg(s + lev * splane + col) : 0.0f;
+    }
+    float fz_lo = 0.0f;
+    if (cell) {
+        const int f = k_begin;
+        if (f >= 2 && f <= nk) {
+            const float m = __ldg(a.rrw + f * splane + col);
+            const float c1 = (f == 2 || f == nk) ? __ldg(a.c1 + (f - 1) * cplane + j * ni + i) : 0.0f;
+            const float c2 = (f == 2 || f == nk) ? __ldg(a.c2 + (f - 1) * cplane + j * ni + i) : 0.0f;
+            fz_lo = z_face<WENO>(win, m, c1, c2, f, nk, eps, wepsf);
+        }
+        if (a.flux_z != nullptr && k_begin == 1) a.flux_z[1 * splane + col] = 0.0f;
+    }
+    for (int k = k_begin; k <= k_end; ++k) {
+        // stage the scalar plane of level k: tile columns x0-3 .. x0+34, rows y0-3 .. y0+10
+        const float *plane = s + k * splane;
+        for (int q = tid; q < kPX * kPY; q += kTX5 * kTY5) {
+            const int py = q / kPX, px = q - py * kPX;
+            const int gx = i0 + px, gy = j0 + py;  // padded coords (tile origin x0 - 3 = i0)
+            s_plane[py][px] = (gx < sx && gy < sy) ? __ldg(plane + gy * sx + gx) : 0.0f;
+        }
+        // shift the column window to levels k-2 .. k+3 (face k+1)
+#pragma unroll
+        for (int q = 0; q < 5; ++q) win[q] = win[q + 1];
+        {
+            const int lev = k + 3;
+            win[5] = (cell && lev <= nk + 1) ? __ldg(s + lev * splane + col) : 0.0f;
+        }
+        __syncthreads();
+        if (cell) {
+            const float *urow = a.rru + k * uplane + y * ux;
+            const float mw = __ldg(urow + x);
+            const float fw = mw * (mw >= 0.0f ? recon<WENO>(s_plane[ty + 3][tx], s_plane[ty + 3][tx + 1],
+                                                            s_plane[ty + 3][tx + 2], s_plane[ty + 3][tx + 3],
+                                                            s_plane[ty + 3][tx + 4], eps)
+                                              : recon<WENO>(s_plane[ty + 3][tx + 5], s_plane[ty + 3][tx + 4],
+                                                            s_plane[ty + 3][tx + 3], s_plane[ty + 3][tx + 2],
+                                                            s_plane[ty + 3][tx + 1], eps));
+            s_fx[ty][tx] = fw;
+            if (a.flux_x != nullptr) a.flux_x[k * uplane + y * ux + x] = fw;
+            if (east_face) {
+                const float me = __ldg(urow + x + 1);
+                const float fe = me * (me >= 0.0f ? recon<WENO>(s_plane[ty + 3][tx + 1], s_plane[ty + 3][tx + 2],
+                                                                s_plane[ty + 3][tx + 3], s_plane[ty + 3][tx + 4],
+                                                                s_plane[ty + 3][tx + 5], eps)
+                                                  : recon<WENO>(s_plane[ty + 3][tx + 6], s_plane[ty + 3][tx + 5],
+                                                                s_plane[ty + 3][tx + 4], s_plane[ty + 3][tx + 3],
+                                                                s_plane[ty + 3][tx + 2], eps));
+                s_fx[ty][tx + 1] = fe;
+                if (a.flux_x != nullptr && i == ni - 1) a.flux_x[k * uplane + y * ux + x + 1] = fe;
+            }
+            const float *vplane_k = a.rrv + k * vplane;
+            const float ms = __ldg(vplane_k + y * sx + x);
+            const float fs = ms * (ms >= 0.0f ? recon<WENO>(s_plane[ty][tx + 3], s_plane[ty + 1][tx + 3],
+                                                            s_plane[ty + 2][tx + 3], s_plane[ty + 3][tx + 3],
+                                                            s_plane[ty + 4][tx + 3], eps)
+                                              : recon<WENO>(s_plane[ty + 5][tx + 3], s_plane[ty + 4][tx + 3],
+                                                            s_plane[ty + 3][tx + 3], s_plane[ty + 2][tx + 3],
+                                                            s_plane[ty + 1][tx + 3], eps));
+            s_fy[ty][tx] = fs;
+            if (a.flux_y != nullptr) a.flux_y[k * vplane + y * sx + x] = fs;
+            if (north_face) {
+                const float mn = __ldg(vplane_k + (y + 1) * sx + x);
+                const float fn = mn * (mn >= 0.0f ? recon<WENO>(s_plane[ty + 1][tx + 3], s_plane[ty + 2][tx + 3],
+                                                                s_plane[ty + 3][tx + 3], s_plane[ty + 4][tx + 3],
+                                                                s_plane[ty + 5][tx + 3], eps)
+                                                  : recon<WENO>(s_plane[ty + 6][tx + 3], s_plane[ty + 5][tx + 3],
+                                                                s_plane[ty + 4][tx + 3], s_plane[ty + 3][tx + 3],
+                                                                s_plane[ty + 2][tx + 3], eps));
+                s_fy[ty + 1][tx] = fn;
+                if (a.flux_y != nullptr && j == nj - 1) a.flux_y[k * vplane + (y + 1) * sx + x] = fn;
+            }
+        }
+        __syncthreads();
+        if (cell) {
+            float fz_hi = 0.0f;
+            const int f = k + 1;
+            if (f <= nk) {
+                const float m = __ldg(a.rrw + f * splane + col);
+                const float c1 = (f == 2 || f == nk) ? __ldg(a.c1 + (f - 1) * cplane + j * ni + i) : 0.0f;
+                const float c2 = (f == 2 || f == nk) ? __ldg(a.c2 + (f - 1) * cplane + j * ni + i) : 0.0f;
+                fz_hi = z_face<WENO>(win, m, c1, c2, f, nk, eps, wepsf);
+            }
+            if (a.flux_z != nullptr) a.flux_z[f * splane + col] = fz_hi;
+            if (owned) {
+                float fw = s_fx[ty][tx], fe = s_fx[ty][tx + 1];
+                float fs = s_fy[ty][tx], fn = s_fy[ty + 1][tx];
+                const float sv = s_plane[ty + 3][tx + 3];
+                const float *urow = a.rru + k * uplane + y * ux;
+                const float *vcol = a.rrv + k * vplane + x;
+                const float uw = __ldg(urow + x), ue = __ldg(urow + x + 1);
+                const float vs = __ldg(vcol + y * sx), vn = __ldg(vcol + (y + 1) * sx);
+                const bool iw = (i == 0) && ((obc & 15u) == 2u) && uw >= 0.0f;
+                const bool ie = (i + 1 == ni) && (((obc >> 4) & 15u) == 2u) && ue <= 0.0f;
+                const bool js = (j == 0) && (((obc >> 8) & 15u) == 2u) && vs >= 0.0f;
+                const bool jn = (j + 1 == nj) && (((obc >> 12) & 15u) == 2u) && vn <= 0.0f;
+                if (iw) fw = fe;
+                if (ie) fe = fw;
+                if (js) fs = fn;
+                if (jn) fn = fs;
+                float ax = (fw - fe) * rdx;
+                float ay = (fs - fn) * rdy;
+                if (iw) ax = ax - (sv * (ue - uw)) * rdx;
+                if (ie) ax = ax - (sv * (ue - uw)) * rdx;
+                if (js) ay = ay - (sv * (vn - vs)) * rdy;
+                if (jn) ay = ay - (sv * (vn - vs)) * rdy;
+                float az;
+                if (k == 1)
+                    az = (-fz_hi) * rdsf;
+                else if (k == nk)
+                    az = fz_lo * rdsf;
+                else
+                    az = (fz_lo - fz_hi) * rdsf;
+                const int c = (k - 1) * cplane + j * ni + i;
+                float total = (ax + ay) + az;
+                total = total + sv * __ldg(a.divx + c);
+                a.tendency[c] = (total * __ldg(a.rr0 + c)) * gz;
+            }
+            fz_lo = fz_hi;
+        }
+    }
+}
+
 template <bool WENO>
 __global__ void __launch_bounds__(kAX *kAY)
     scalar_advection5_kernel(gm1b_scalar_advection5_arrays a, PaddedDims d, int levels_per_chunk, float rdx,
@@ -404,16 +619,16 @@ extern "C" int32_t gm1b_scalar_advection5(int32_t ni, int32_t nj, int32_t nk,
     if (chunk > nk) chunk = nk;
     const PaddedDims d{ni, nj, nk};
     const bool weno = wflag != 0 && nrk == 3;
-    const dim3 grid((ni + kAX - 1) / kAX, (nj + kAY - 1) / kAY, (nk + chunk - 1) / chunk);
+    const dim3 grid((ni + kTX5 - 1) / kTX5, (nj + kTY5 - 1) / kTY5, (nk + chunk - 1) / chunk);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const float rdx = 1.0f / dx, rdy = 1.0f / dy, rdsf = 1.0f / dz;
     ProfScope ps(weno ? "scalar_advection5_weno_kernel" : "scalar_advection5_kernel", st);
     if (weno)
-        scalar_advection5_kernel<true>
-            <<<grid, dim3(kAX, kAY), 0, st>>>(a, d, chunk, rdx, rdy, rdsf, weps, (float)weps, lateral_obc);
+        scalar_advection5_tiled_kernel<true>
+            <<<grid, dim3(kTX5, kTY5), 0, st>>>(a, d, chunk, rdx, rdy, rdsf, weps, (float)weps, lateral_obc);
     else
-        scalar_advection5_kernel<false>
-            <<<grid, dim3(kAX, kAY), 0, st>>>(a, d, chunk, rdx, rdy, rdsf, weps, (float)weps, lateral_obc);
+        scalar_advection5_tiled_kernel<false>
+            <<<grid, dim3(kTX5, kTY5), 0, st>>>(a, d, chunk, rdx, rdy, rdsf, weps, (float)weps, lateral_obc);
     ps.stop();
     if (cudaPeekAtLastError() != cudaSuccess) {
         gm1b_set_error("scalar_advection5_kernel: %s", cudaGetErrorString(cudaGetLastError()));
