@@ -254,15 +254,6 @@ constexpr int kTX5 = 32, kTY5 = 8;
 constexpr int kPX = kTX5 + 6, kPY = kTY5 + 6;
 
 template <bool WENO>
-__device__ __forceinline__ float recon_dir(const float *p, int stride, float m, double eps) {
-    // p points at the face's upwind-side cell x-1 for m >= 0 ... reconstruction
-    // over p[-2..2] (m >= 0: s(x-3..x+1) oriented; m < 0: s(x+2..x-2))
-    if (m >= 0.0f)
-        return recon<WENO>(p[-3 * stride], p[-2 * stride], p[-1 * stride], p[0], p[stride], eps);
-    return recon<WENO>(p[2 * stride], p[stride], p[0], p[-1 * stride], p[-2 * stride], eps);
-}
-
-template <bool WENO>
 __device__ __forceinline__ float z_face(const float win[6], float m, float c1, float c2, int face, int nk,
                                         double eps, float wepsf) {
     // win[q] holds level face-3+q (q = 0..5), i.e. win[3] = level face
@@ -420,7 +411,10 @@ __global__ void __launch_bounds__(kTX5 *kTY5)
             if (owned) {
                 float fw = s_fx[ty][tx], fe = s_fx[ty][tx + 1];
                 float fs = s_fy[ty][tx], fn = s_fy[ty + 1][tx];
-                const float sv = s_plane[ty + 3][tx + 3];
+                // this cell's value from the register window (levels k-2..k+3):
+                // the shared plane may already hold level k+1 for threads
+                // that moved on
+                const float sv = win[2];
                 const float *urow = a.rru + k * uplane + y * ux;
                 const float *vcol = a.rrv + k * vplane + x;
                 const float uw = __ldg(urow + x), ue = __ldg(urow + x + 1);
