@@ -18,6 +18,8 @@
 // reduced in a fixed order: per-column sums in the twin's k order, row sums
 // in its i order, then a short ordered finish.  The budget scratch lives in a
 // caller-provided workspace; its first 16 bytes are status words.
+#include <mutex>
+
 #include "gm1b_common.cuh"
 
 namespace gm1b {
@@ -480,5 +482,76 @@ extern "C" int32_t gm1b_kessler_driver(int32_t ni, int32_t nj, int32_t nk, const
         ps.stop();
     }
     if (!launched("kessler_finish_kernel")) return GM1B_ERR_CUDA;
+    return GM1B_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant.  Some callers cannot allocate device memory of
+// their own: a host model that hands this library only its state arrays
+// (for instance a Fortran or C model bound through this C ABI whose device
+// memory belongs to another runtime's pool), or a process whose device
+// memory is reserved up front by another framework's allocator.  They
+// cannot supply the workspace gm1b_kessler_driver needs, so this entry point
+// keeps that scratch in a file-scope device array instead.  Every GPU that
+// loads the library holds the array until the process exits; every call on
+// a device shares it and finds the previous call's contents there.
+// ---------------------------------------------------------------------------
+namespace {
+
+static __device__ __align__(256) unsigned char g_kessler_static_scratch[GM1B_KESSLER_STATIC_SCRATCH_BYTES];
+
+std::mutex g_static_mu;
+void *g_static_ptr[64] = {};  // device address of the array, per device ordinal
+
+// Device address of the scratch array on the current device, resolved once
+// per device (host code may not use the symbol itself: on the host it names
+// a stand-in, not device memory).
+void *static_scratch_address() {
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    std::lock_guard<std::mutex> g(g_static_mu);
+    if (g_static_ptr[dev] == nullptr) {
+        void *p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_kessler_static_scratch) != cudaSuccess) return nullptr;
+        g_static_ptr[dev] = p;
+    }
+    return g_static_ptr[dev];
+}
+
+}  // namespace
+
+extern "C" int32_t gm1b_kessler_driver_static(int32_t ni, int32_t nj, int32_t nk, const gm1b_kessler_arrays *arrays,
+                                             float dx, float dy, float dz, float dt, int32_t equation_set,
+                                             int32_t efall, int32_t *status_out, void *stream) {
+    if (ni < 1 || nj < 1 || nk < 1) {
+        gm1b_set_error("gm1b_kessler_driver_static: need ni, nj, nk >= 1");
+        return GM1B_ERR_ARGUMENT;
+    }
+    const size_t need = workspace_bytes(ni, nj, nk);
+    if (need > (size_t)GM1B_KESSLER_STATIC_SCRATCH_BYTES) {
+        gm1b_set_error("gm1b_kessler_driver_static: a %dx%dx%d grid needs %zu bytes of scratch, more than the %u-byte "
+                       "static array; use gm1b_kessler_driver with a caller workspace",
+                       ni, nj, nk, need, (unsigned)GM1B_KESSLER_STATIC_SCRATCH_BYTES);
+        return GM1B_ERR_ARGUMENT;
+    }
+    void *scratch = static_scratch_address();
+    if (scratch == nullptr) {
+        cudaGetLastError();
+        gm1b_set_error("gm1b_kessler_driver_static: cudaGetSymbolAddress of the static scratch failed");
+        return GM1B_ERR_CUDA;
+    }
+    // gm1b_kessler_driver clears the status words and overwrites every
+    // partial sum it reads, so leftover contents of a previous call are inert.
+    const int32_t rc = gm1b_kessler_driver(ni, nj, nk, arrays, dx, dy, dz, dt, equation_set, efall, scratch,
+                                           (size_t)GM1B_KESSLER_STATIC_SCRATCH_BYTES, stream);
+    if (rc != GM1B_OK) return rc;
+    if (status_out != nullptr) {
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        if (cudaMemcpyAsync(status_out, scratch, 2 * sizeof(int32_t), cudaMemcpyDeviceToDevice, st) != cudaSuccess) {
+            cudaGetLastError();
+            gm1b_set_error("gm1b_kessler_driver_static: status copy failed");
+            return GM1B_ERR_CUDA;
+        }
+    }
     return GM1B_OK;
 }

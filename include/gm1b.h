@@ -221,6 +221,35 @@ GM1B_API int32_t gm1b_kessler_driver(int32_t ni, int32_t nj, int32_t nk,
                                      float dz, float dt, int32_t equation_set, int32_t efall,
                                      void *workspace, size_t workspace_size, void *stream);
 
+/*
+ * gm1b_kessler_driver without a workspace argument, for callers that cannot
+ * allocate device memory of their own (for instance a Fortran or C host
+ * model bound through this ABI whose device memory belongs to another
+ * runtime's pool, or a process whose device memory another framework
+ * reserves up front): the budget scratch lives in a static device array of
+ * GM1B_KESSLER_STATIC_SCRATCH_BYTES (8 MiB), which every GPU that loads the
+ * library holds until the process exits.  No counterpart in the reference
+ * (its launcher always allocates a workspace).
+ *
+ * - Grids whose scratch (gm1b_kessler_workspace_bytes) exceeds 8 MiB are
+ *   rejected with GM1B_ERR_ARGUMENT; 8 MiB covers, e.g., 256x256x80.
+ * - The first call on a device resolves the array's device address for that
+ *   device (cudaGetSymbolAddress, with the device current); make that first
+ *   call before any stream capture.
+ * - All calls on a device share the one array: calls that overlap on the GPU
+ *   (different streams, or other threads) race and must be serialised by the
+ *   caller.  Each call clears the status words it uses.
+ * - status_out (device pointer to 2 int32 words, or NULL) receives the
+ *   non-converged saturation-adjustment cell count and the largest fallout
+ *   sub-step count, stream-ordered after the operator.
+ * - The call allocates no device memory and calls no allocator.
+ */
+#define GM1B_KESSLER_STATIC_SCRATCH_BYTES (8u * 1024u * 1024u)
+GM1B_API int32_t gm1b_kessler_driver_static(int32_t ni, int32_t nj, int32_t nk,
+                                            const gm1b_kessler_arrays *arrays, float dx, float dy,
+                                            float dz, float dt, int32_t equation_set, int32_t efall,
+                                            int32_t *status_out, void *stream);
+
 /* ------------------------------------------------------------------------
  * SGS/TKE local algebra: every array (nk+1, nj, ni) (w levels) except
  * ruh (ni) and rvh (nj)
