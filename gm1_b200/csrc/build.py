@@ -22,7 +22,8 @@ PKG = CSRC.parent
 ROOT = PKG.parent
 LIB_DIR = PKG / "lib"
 LIB = LIB_DIR / "libgm1b.so"
-SOURCES = ("capi.cu", "periodic_lane.cu", "advection5.cu", "kessler.cu", "tke.cu")
+SOURCES = ("capi.cu", "periodic_lane.cu", "advection5.cu", "kessler.cu", "tke.cu", "scalar_rk.cu",
+           "moist_bridge.cu")
 ARCH = ("-gencode", "arch=compute_100a,code=sm_100a")
 FLAGS = (
     "-O3", "-std=c++17", "-lineinfo",

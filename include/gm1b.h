@@ -184,6 +184,89 @@ GM1B_API int32_t gm1b_scalar_advection5(int32_t ni, int32_t nj, int32_t nk,
                                         int32_t levels_per_chunk, void *stream);
 
 /* ------------------------------------------------------------------------
+ * eqtset=2 moist stage terms
+ * ---------------------------------------------------------------------- */
+typedef struct gm1b_eqtset2_arrays {
+    /* base state: (nk) profiles, or (nk, nj, ni) with base3d; qc0/qi0 may be
+     * NULL (base condensate exactly zero) */
+    const float *th0, *qv0, *pi0, *qc0, *qi0;
+    const float *th3d;  /* (nk, nj, ni) */
+    const float *q3d;   /* (6, nk, nj, ni): qv, qc, qr, qi, qs, qg */
+    const float *pp3d;  /* (nk+2, nj+2, ni+2) */
+    float *thv, *ppterm; /* (nk+2, nj+2, ni+2), live cells written */
+    float *buoyancy;     /* padded-lane scalar (nk+2, nj+6, ni+6), live cells written */
+    float *thterm;       /* (nk, nj, ni) */
+    float *piadv;        /* (nk+2, nj+2, ni+2), levels 1..nk incl. halos */
+} gm1b_eqtset2_arrays;
+
+/*
+ * Moist buoyancy g*(th3d/th0 + (Rv/Rd-1)(qv-qv0) - (ql+qi-qc0-qi0)),
+ * theta-rho, the theta and pressure energy terms of eqtset=2, and piadv.
+ * Replaces the cell algebra of cpu_eqtset2_cell_f32
+ * (src/cm1core/cuda_moist_stage_bridge.py:62) as applied by
+ * launch_cuda_eqtset2_stage_terms (:378); the open-boundary halo fills that
+ * launch adds are the boundary family's, not this operator's.
+ */
+GM1B_API int32_t gm1b_eqtset2_stage_terms(int32_t ni, int32_t nj, int32_t nk,
+                                          const gm1b_eqtset2_arrays *arrays, int32_t base3d,
+                                          void *stream);
+
+/* ------------------------------------------------------------------------
+ * Scalar/moisture RK stage pieces (padded lane)
+ * ---------------------------------------------------------------------- */
+
+/*
+ * Theta transport carrier: padded[k+1, j+3, i+3] = (th0[k] - 300) + th3d[k, j, i]
+ * (th0 (nk), th3d (nk, nj, ni), padded scalar shape; halos untouched).
+ * Replaces cpu_theta_transport_scalar_inplace
+ * (src/cm1core/cuda_scalar_moist_rk.py:255) and the packing kernel
+ * cm1_rk_pack_theta_v1 (:587).
+ */
+GM1B_API int32_t gm1b_theta_transport_pack(int32_t ni, int32_t nj, int32_t nk, const float *th0,
+                                           const float *th3d, float *padded, void *stream);
+
+typedef struct gm1b_scalar_rk_compose_arrays {
+    /* theta: `cells` words each */
+    const float *theta_a, *theta_held, *theta_divterm, *theta_adv;
+    float *theta_cur;
+    /* moisture: nq * cells words each (species-major) */
+    const float *q_a, *q_held, *q_adv;
+    float *q_cur;
+} gm1b_scalar_rk_compose_arrays;
+
+/*
+ * A-anchored RK update of theta and nq moisture species, dttmp = dt/(4-nrk):
+ * theta = A + dttmp*((held - t11*thterm) + adv), q = A + dttmp*(held + adv),
+ * |x| < 1e-30 flushed to 0.
+ * Replaces cpu_compose_scalar_moist_rk_stage_inplace
+ * (src/cm1core/cuda_scalar_moist_rk.py:283) and cm1_rk_compose_{theta,moisture}_v1.
+ */
+GM1B_API int32_t gm1b_scalar_moist_rk_compose(size_t cells, int32_t nq,
+                                              const gm1b_scalar_rk_compose_arrays *arrays,
+                                              int32_t nrk, float dt, void *stream);
+
+typedef struct gm1b_pdef_arrays {
+    const float *scalar_a;      /* (nk, nj, ni) */
+    const float *scalar_padded; /* padded scalar shape */
+    const float *rho0;          /* (nk, nj, ni) */
+    const float *gz, *rgz;      /* (nj, ni) */
+    const float *mass_flux;     /* rru (axis x), rrv (y) or rrw (z) shape */
+    float *directional;         /* (nk, nj, ni), in/out */
+    float *candidate;           /* (nk, nj, ni), out */
+} gm1b_pdef_arrays;
+
+/*
+ * One terrain positive-definite direction pass (pdef x, y or z; axis 0/1/2):
+ * candidate = rho0*A + dt*(directional + s*div(mass flux))*gz, then the
+ * donor-cell repair of negative candidates along each line and the matching
+ * update of `directional`.
+ * Replaces cpu_pdef_direction_inplace (src/cm1core/cuda_scalar_moist_rk.py:352)
+ * and cm1_rk_pdef_{directional,candidate_*,correct_*}_v1.
+ */
+GM1B_API int32_t gm1b_pdef_direction(int32_t ni, int32_t nj, int32_t nk, const gm1b_pdef_arrays *arrays,
+                                     int32_t axis, float dt, float spacing, void *stream);
+
+/* ------------------------------------------------------------------------
  * Kessler warm rain (compact mass arrays (nk, nj, ni), no halos)
  * ---------------------------------------------------------------------- */
 typedef struct gm1b_kessler_arrays {

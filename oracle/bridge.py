@@ -1,0 +1,31 @@
+"""ctypes driver of the eqtset=2 cell oracle (rk_oracle.c) - TEST
+INFRASTRUCTURE ONLY.  Mirrors cpu_eqtset2_cell_f32
+(src/cm1core/cuda_moist_stage_bridge.py:62)."""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from oracle.periodic import load
+
+_F = ctypes.POINTER(ctypes.c_float)
+
+
+def _lib():
+    lib = load()
+    if not getattr(lib, "_bridge_ready", False):
+        f = ctypes.c_float
+        lib.oracle_eqtset2_cell.argtypes = [f, f, f, f, f, f, f, _F, _F]
+        lib.oracle_eqtset2_cell.restype = None
+        lib._bridge_ready = True
+    return lib
+
+
+def eqtset2_cell(th0, qv0, pi0, qc0, qi0, th3d, pp3d, q) -> np.ndarray:
+    """(buoyancy, theta_rho, theta_term, pressure_term) of one cell."""
+    qq = np.ascontiguousarray(q, dtype=np.float32)
+    out = np.zeros(4, np.float32)
+    _lib().oracle_eqtset2_cell(th0, qv0, pi0, qc0, qi0, th3d, pp3d, qq.ctypes.data_as(_F), out.ctypes.data_as(_F))
+    return out

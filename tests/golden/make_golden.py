@@ -369,6 +369,102 @@ def make_tke(reference: Path) -> None:
         print("wrote", tag, "clipped", r.clipped_tke_words)
 
 
+def rk_fixture(ni: int, nj: int, nk: int, seed: int) -> dict[str, np.ndarray]:
+    ng = 3
+    rng = np.random.default_rng(seed)
+
+    def u(shape, lo, hi):
+        return rng.uniform(lo, hi, shape).astype(np.float32)
+
+    cell = (nk, nj, ni)
+    a = {
+        "th0": u((nk,), 295.0, 340.0),
+        "th3d": u(cell, -3.0, 3.0),
+        "theta_pad": np.zeros((nk + 2, nj + 2 * ng, ni + 2 * ng), np.float32),
+        "theta_a": u(cell, -3.0, 3.0), "theta_held": u(cell, -1e-3, 1e-3), "theta_divterm": u(cell, -1e-3, 1e-3),
+        "theta_adv": u(cell, -1e-2, 1e-2),
+        "q_a": (u((6,) + cell, 0.0, 1.0) ** 3 * np.float32(0.012)).astype(np.float32),
+        "q_held": u((6,) + cell, -1e-6, 1e-6), "q_adv": u((6,) + cell, -2e-5, 2e-5),
+        "pd_scalar_a": (u(cell, -0.3, 1.0) * np.float32(2e-3)).astype(np.float32),
+        "pd_scalar_padded": (u((nk + 2, nj + 2 * ng, ni + 2 * ng), -0.3, 1.0) * np.float32(2e-3)).astype(np.float32),
+        "pd_rho0": u(cell, 0.6, 1.2), "pd_gz": u((nj, ni), 0.97, 1.03),
+        "pd_flux_x": u((nk + 2, nj + 2 * ng, ni + 1 + 2 * ng), -8.0, 8.0),
+        "pd_flux_y": u((nk + 2, nj + 1 + 2 * ng, ni + 2 * ng), -8.0, 8.0),
+        "pd_flux_z": u((nk + 3, nj + 2 * ng, ni + 2 * ng), -2.0, 2.0),
+        "pd_directional": u(cell, -4e-6, 4e-6),
+    }
+    a["q_a"][:, :, 0, :] = np.float32(0.0)
+    a["theta_a"][0, 0, :4] = np.float32(1e-31)  # below smeps after the update
+    a["pd_rgz"] = (np.float32(1.0) / a["pd_gz"]).astype(np.float32)
+    return a
+
+
+def make_rk(reference: Path) -> None:
+    sys.path.insert(0, str(reference / "src"))
+    from cm1core.cuda_scalar_moist_rk import (
+        cpu_compose_scalar_moist_rk_stage_inplace,
+        cpu_pdef_direction_inplace,
+        cpu_theta_transport_scalar_inplace,
+    )
+
+    for tag, (ni, nj, nk, seed) in {"rk_11x9x8": (11, 9, 8, 51), "rk_7x12x10": (7, 12, 10, 52)}.items():
+        a = rk_fixture(ni, nj, nk, seed)
+        inputs = {f"in_{k}": v.copy() for k, v in a.items()}
+        out = {}
+        pad = a["theta_pad"].copy()
+        cpu_theta_transport_scalar_inplace(a["th0"].copy(), a["th3d"].copy(), pad, ni=ni, nj=nj, nk=nk)
+        out["out_theta_pad"] = pad
+        for nrk in (1, 2, 3):
+            tc = np.zeros_like(a["theta_a"])
+            qc = np.zeros_like(a["q_a"])
+            cpu_compose_scalar_moist_rk_stage_inplace(
+                a["theta_a"].copy(), a["q_a"].copy(), a["theta_held"].copy(), a["q_held"].copy(),
+                a["theta_divterm"].copy(), a["theta_adv"].copy(), a["q_adv"].copy(), tc, qc, nrk=nrk, dt=5.0)
+            out[f"out_theta_cur_{nrk}"] = tc
+            out[f"out_q_cur_{nrk}"] = qc
+        for axis, spacing in (("x", 1000.0), ("y", 900.0), ("z", 250.0)):
+            d = a["pd_directional"].copy()
+            cand = np.zeros_like(d)
+            cpu_pdef_direction_inplace(a["pd_scalar_a"].copy(), a["pd_scalar_padded"].copy(), a["pd_rho0"].copy(),
+                                       a["pd_gz"].copy(), a["pd_rgz"].copy(), a[f"pd_flux_{axis}"].copy(), d, cand,
+                                       axis=axis, dt=5.0 / 3.0, spacing=spacing)
+            out[f"out_pd_directional_{axis}"] = d
+            out[f"out_pd_candidate_{axis}"] = cand
+        meta = dict(ni=ni, nj=nj, nk=nk, dt=5.0, pdef_dt=5.0 / 3.0, spacing={"x": 1000.0, "y": 900.0, "z": 250.0})
+        np.savez_compressed(HERE / f"{tag}.npz", meta=json.dumps(meta), **inputs, **out)
+        print("wrote", tag)
+
+
+def make_bridge(reference: Path) -> None:
+    """eqtset=2 stage terms, cell by cell, through the reference's twin."""
+    sys.path.insert(0, str(reference / "src"))
+    from cm1core.cuda_moist_stage_bridge import cpu_eqtset2_cell_f32
+
+    rng = np.random.default_rng(61)
+    n = 400
+    inp = {
+        "th0": rng.uniform(295.0, 345.0, n).astype(np.float32),
+        "qv0": rng.uniform(0.0, 0.014, n).astype(np.float32),
+        "pi0": rng.uniform(0.6, 1.0, n).astype(np.float32),
+        "qc0": np.where(rng.random(n) < 0.2, rng.uniform(0.0, 1e-4, n), 0.0).astype(np.float32),
+        "qi0": np.where(rng.random(n) < 0.2, rng.uniform(0.0, 1e-4, n), 0.0).astype(np.float32),
+        "th3d": rng.uniform(-4.0, 4.0, n).astype(np.float32),
+        "pp3d": rng.uniform(-3e-3, 3e-3, n).astype(np.float32),
+        "q": rng.uniform(-2e-5, 6e-3, (6, n)).astype(np.float32),
+    }
+    inp["q"][0] = rng.uniform(-1e-5, 0.016, n).astype(np.float32)
+    out = np.zeros((4, n), np.float32)
+    for c in range(n):
+        r = cpu_eqtset2_cell_f32(th0=inp["th0"][c], qv0=inp["qv0"][c], pi0=inp["pi0"][c], qc0=inp["qc0"][c],
+                                 qi0=inp["qi0"][c], th3d=inp["th3d"][c], pp3d=inp["pp3d"][c], qv=inp["q"][0, c],
+                                 qc=inp["q"][1, c], qr=inp["q"][2, c], qi=inp["q"][3, c], qs=inp["q"][4, c],
+                                 qg=inp["q"][5, c])
+        out[:, c] = [r["buoyancy"], r["theta_rho"], r["theta_term"], r["pressure_term"]]
+    np.savez_compressed(HERE / "eqtset2_cells.npz", meta=json.dumps({"cells": n}),
+                        **{f"in_{k}": v for k, v in inp.items()}, out_terms=out)
+    print("wrote eqtset2_cells")
+
+
 def make_c1(reference: Path, checkpoints: list[int]) -> None:
     """Digests after each checkpoint N, each from a fresh state with one call
     of steps=N (the reference refuses a non-fresh entry state, ppx != pp3d,
@@ -405,7 +501,7 @@ def make_c1(reference: Path, checkpoints: list[int]) -> None:
 def main() -> None:
     p = argparse.ArgumentParser()
     p.add_argument("--reference", type=Path, required=True, help="root of the reference source tree")
-    p.add_argument("what", choices=("small", "c1", "advection", "kessler", "tke"))
+    p.add_argument("what", choices=("small", "c1", "advection", "kessler", "tke", "rk", "bridge"))
     p.add_argument("--checkpoints", type=int, nargs="+", default=[1])
     args = p.parse_args()
     if args.what == "small":
@@ -414,6 +510,10 @@ def main() -> None:
         make_advection(args.reference)
     elif args.what == "kessler":
         make_kessler(args.reference)
+    elif args.what == "rk":
+        make_rk(args.reference)
+    elif args.what == "bridge":
+        make_bridge(args.reference)
     elif args.what == "tke":
         make_tke(args.reference)
     else:
