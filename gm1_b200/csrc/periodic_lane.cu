@@ -86,8 +86,10 @@ __global__ void __launch_bounds__(kTX *kTY) traj_prepare_kernel(Arr a, Dims d, f
 struct View {
     const float *p;
     int sz, sy, oz, oy, ox;
+    // 32-bit offsets: every periodic-lane array holds fewer than 2^31 words
+    // (the entry points reject larger grids)
     __device__ __forceinline__ float at(int k, int j, int i) const {
-        return __ldg(p + (size_t)(k + oz) * sz + (size_t)(j + oy) * sy + (i + ox));
+        return __ldg(p + ((k + oz) * sz + (j + oy) * sy + (i + ox)));
     }
 };
 
@@ -438,6 +440,10 @@ struct ColumnArgs {
     int scratch_outputs;
     int fill_pp3d;   // write pp3d halos at the last small step
     int post_ppx;    // trajectory post-step ppx completion fused at nrk=3
+    // fast mode (no scratch outputs): the first small step stores 1/pivot in
+    // tri_pivot and the elimination coefficients in tri_cc, later small
+    // steps of the stage read them back
+    int store_consts, use_consts;
 };
 
 __global__ void __launch_bounds__(kTX *kColWarps, 1) sound_column_kernel(Arr a, Dims d, ColumnArgs p) {
@@ -511,17 +517,25 @@ __global__ void __launch_bounds__(kTX *kColWarps, 1) sound_column_kernel(Arr a, 
         for (int k = 2 + wy; k <= nk; k += kColWarps) {
             const float mm = SM(s_mm, k);
             const float aa = (k >= 3) ? (-p.asq) * (mm * SM(s_a1, k - 1)) : 0.0f;
-            const float cc = (k < nk) ? (-p.asq) * ((-mm) * SM(s_a2, k)) : 0.0f;
-            const float diag = (-SM(s_a1, k)) + SM(s_a2, k - 1);
-            const float bb = 1.0f - p.asq * (mm * diag);
             const float pd = SM(s_pp, k) - SM(s_pp, k - 1);
             const float fwk = p.dts * a.wten[d.w(k, j - 1, i - 1)] + p.beta * ((-mm) * pd);
             const float upd = (SM(s_pp, k) + SM(s_fpk, k)) - (SM(s_pp, k - 1) + SM(s_fpk, k - 1));
             const float dd = (SM(s_w, k) + fwk) + p.alph * ((-mm) * upd);
             SM(s_aa, k) = aa;
+            SM(s_dd, k) = dd;
+            if (p.use_consts) {
+                // stage-constant 1/pivot and elimination coefficient stored by
+                // the first small step of this stage (identical words)
+                const size_t c = d.s(k, j, i);
+                SM(s_bb, k) = a.tri_pivot[c];
+                SM(s_cc, k) = (k < nk) ? a.tri_cc[c] : 0.0f;
+                continue;
+            }
+            const float cc = (k < nk) ? (-p.asq) * ((-mm) * SM(s_a2, k)) : 0.0f;
+            const float diag = (-SM(s_a1, k)) + SM(s_a2, k - 1);
+            const float bb = 1.0f - p.asq * (mm * diag);
             SM(s_bb, k) = bb;
             SM(s_cc, k) = cc;
-            SM(s_dd, k) = dd;
             if (p.scratch_outputs && last) {
                 const size_t c = d.s(k, j, i);
                 a.tri_aa[c] = aa;
@@ -533,13 +547,28 @@ __global__ void __launch_bounds__(kTX *kColWarps, 1) sound_column_kernel(Arr a, 
     }
     __syncthreads();
     // phase B: Thomas sweep, one lane per column, out of shared memory
-    if (wy == 0 && live) {
+    if (wy == 0 && live && p.use_consts) {
+        // forward elimination of the right-hand side only: no division
+        float ed = 0.0f;
+        for (int k = 2; k <= nk; ++k) {
+            const float aa = SM(s_aa, k), dd = SM(s_dd, k), inv = SM(s_bb, k);
+            if (k < nk) {
+                const float num = (k < 3) ? dd : (dd - aa * ed);
+                ed = num * inv;
+                SM(s_ed, k) = ed;
+            } else {
+                SM(s_w, k) = (dd - aa * ed) * inv;
+            }
+        }
+        for (int k = nk - 1; k >= 2; --k) SM(s_w, k) = SM(s_cc, k) * SM(s_w, k + 1) + SM(s_ed, k);
+    } else if (wy == 0 && live) {
         float ec = 0.0f, ed = 0.0f;
         for (int k = 2; k <= nk; ++k) {
             const float aa = SM(s_aa, k), bb = SM(s_bb, k), cc = SM(s_cc, k), dd = SM(s_dd, k);
             const float pivot = (k < 3) ? bb : (aa * ec + bb);
             const float inv = 1.0f / pivot;
             if (p.scratch_outputs && last) a.tri_pivot[d.s(k, j, i)] = pivot;
+            if (p.store_consts) a.tri_pivot[d.s(k, j, i)] = inv;
             if (k < nk) {
                 const float num = (k < 3) ? dd : (dd - aa * ed);
                 ec = (-cc) * inv;
@@ -547,6 +576,7 @@ __global__ void __launch_bounds__(kTX *kColWarps, 1) sound_column_kernel(Arr a, 
                 SM(s_cc, k) = ec;  // elimination coefficient replaces cc
                 SM(s_ed, k) = ed;
                 if (p.scratch_outputs && last) a.elim_d[d.s(k, j, i)] = ed;
+                if (p.store_consts) a.tri_cc[d.s(k, j, i)] = ec;
             } else {
                 SM(s_w, k) = (dd - aa * ed) * inv;
             }
@@ -846,6 +876,8 @@ int enqueue_sound_stage(const Arr &a, const Dims &d, float dt, int nsound, int n
                 }
         if (!check_launch("sound_uv_kernel")) return GM1B_ERR_CUDA;
         p.n = n;
+        p.store_consts = (!scratch_outputs && n == 1) ? 1 : 0;
+        p.use_consts = (!scratch_outputs && n > 1) ? 1 : 0;
         {
                     ProfScope ps_("sound_column_kernel", st);
                     sound_column_kernel<<<col_grid, dim3(kTX, kColWarps), smem, st>>>(a, d, p);
@@ -918,6 +950,10 @@ extern "C" int32_t gm1b_psolver3_trajectory(int32_t ni, int32_t nj, int32_t nk, 
                                            uint32_t ablations, uint32_t flags, void *stream) {
     if (arrays == nullptr || ni < 5 || nj < 5 || nk < 6 || steps < 1) {
         gm1b_set_error("gm1b_psolver3_trajectory: need arrays, ni >= 5, nj >= 5, nk >= 6, steps >= 1");
+        return GM1B_ERR_ARGUMENT;
+    }
+    if ((double)(nk + 2) * (nj + 2) * (ni + 2) >= 2147483647.0) {
+        gm1b_set_error("gm1b_psolver3_trajectory: arrays of 2^31 or more words are not supported");
         return GM1B_ERR_ARGUMENT;
     }
     if (!(dt > 0.0f) || !(dx > 0.0f) || !(dy > 0.0f) || !(dz > 0.0f)) {
