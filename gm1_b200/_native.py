@@ -15,6 +15,7 @@ LIB_PATH = Path(__file__).resolve().parent / "lib" / "libgm1b.so"
 ABI_VERSION = 1
 
 GM1B_OK = 0
+GM1B_ERR_ARGUMENT = -1
 GM1B_FLAG_SCRATCH_OUTPUTS = 1
 
 # ablation bits of include/gm1b.h, keyed by the reference field names

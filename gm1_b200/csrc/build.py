@@ -23,12 +23,12 @@ ROOT = PKG.parent
 LIB_DIR = PKG / "lib"
 LIB = LIB_DIR / "libgm1b.so"
 SOURCES = ("capi.cu", "periodic_lane.cu", "advection5.cu", "kessler.cu", "tke.cu", "scalar_rk.cu",
-           "moist_bridge.cu")
+           "moist_bridge.cu", "initial_state.cu")
 ARCH = ("-gencode", "arch=compute_100a,code=sm_100a")
 FLAGS = (
     "-O3", "-std=c++17", "-lineinfo",
     "--fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false",
-    "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
+    "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden", "-Xcompiler", "-ffp-contract=off",
     "--expt-relaxed-constexpr",
 )
 

@@ -355,6 +355,43 @@ typedef struct gm1b_sgs_tke_arrays {
 GM1B_API int32_t gm1b_sgs_tke(int32_t ni, int32_t nj, int32_t nk, const gm1b_sgs_tke_arrays *arrays,
                               float dx, float dy, float dz, void *stream);
 
+/* ------------------------------------------------------------------------
+ * Analytic initial state (host, once per run, except the bubble field)
+ * ---------------------------------------------------------------------- */
+
+/*
+ * Weisman-Klemp base column (CM1 isnd=5) on nk HOST mass heights zh (m,
+ * strictly increasing above 0): th0, qv0, pi0, prs0 required; thv0, t0,
+ * rh0 optional (NULL = not written).  imoist 0 or 1; iterations = 20 is
+ * CM1's count.  Binary32, one operation at a time, on the host.  Replaces
+ * weisman_klemp_column_with_iterations
+ * (rust/cm1-state/src/storm_initialization.rs:194) and the error cases it
+ * refuses (nk < 1, imoist outside {0,1}, zero iterations, non-increasing
+ * heights, non-physical column).
+ */
+GM1B_API int32_t gm1b_wk_base_column(int32_t nk, const float *zh, int32_t imoist, int32_t iterations, float *th0,
+                                     float *qv0, float *thv0, float *pi0, float *prs0, float *t0, float *rh0);
+
+/*
+ * iwnd=2 quarter-circle base wind on n HOST face heights: u on zu, v on zv
+ * (either output may be NULL).  Replaces analytic_shear_u / analytic_shear_v
+ * (rust/cm1-state/src/storm_initialization.rs:354,379).
+ */
+GM1B_API int32_t gm1b_analytic_shear(int32_t n, const float *zu, const float *zv, float *u, float *v);
+
+/*
+ * iinit=1 cos^2 warm bubble written into the interior of the DEVICE scalar
+ * lane tha: ng = 0 dense (nk, nj, ni); ng = 1 periodic lane (nk+2, nj+2,
+ * ni+2); ng = 3 padded lane (nk+2, nj+6, ni+6).  xh (ni), yh (nj), zh (nk)
+ * are device mass-point coordinates (m).  Halo words are not written.
+ * Replaces build_theta_perturbation for iinit=1
+ * (rust/cm1-state/src/initial_perturbation.rs:425,449-466).
+ */
+GM1B_API int32_t gm1b_theta_bubble(int32_t ni, int32_t nj, int32_t nk, int32_t ng, const float *xh, const float *yh,
+                                   const float *zh, float center_x, float center_y, float center_z,
+                                   float horizontal_radius, float vertical_radius, float amplitude, float *tha,
+                                   void *stream);
+
 /*
  * Launch profiler.  While enabled, every kernel launch of the library is
  * bracketed by a pair of CUDA events recorded on its own stream (the

@@ -465,6 +465,35 @@ def make_bridge(reference: Path) -> None:
     print("wrote eqtset2_cells")
 
 
+def make_wk(reference: Path) -> None:
+    """CM1 r21.1's own Weisman-Klemp base state (isnd=5, nz=40, dz=500 m) as
+    float32 words, from the CM1 output the reference keeps
+    (tests/data/cm1-ref-24x24/stats-run-t1500.npz: th0, qv0, pi0, prs0;
+    variants.json: the derived variant's pi0 column), plus the sealed SHA-256
+    digests of the qv0 and pi0 words in the reference's binary32 restatement
+    tests (rust/cm1-state/src/storm_initialization.rs, test
+    hydrostatic_fixed_point_is_settled_at_the_source_iteration_count)."""
+    import re  # noqa: PLC0415
+
+    data = reference / "tests" / "data" / "cm1-ref-24x24"
+    state = np.load(data / "stats-run-t1500.npz")
+    variants = json.loads((data / "variants.json").read_text())
+    words = {n: [f"{int(w):08x}" for w in state[n].astype(np.float32).view(np.uint32)]
+             for n in ("th0", "qv0", "pi0", "prs0")}
+    column = variants["variants"]["derived"]["block"]["pi0_column"]
+    rust = (reference / "rust" / "cm1-state" / "src" / "storm_initialization.rs").read_text()
+    sealed = dict(re.findall(r'raw_sha256\(twenty\.(qv_kg_per_kg|pi)\(\)\),\s*"([0-9a-f]{64})"', rust))
+    record = {
+        "case": "CM1 r21.1 supercell namelist, isnd=5 imoist=1, nz=40, dz=500 m (mass heights 250..19750 m)",
+        "nz": 40, "dz": 500.0,
+        "cm1_words": words,
+        "cm1_pi0_column_derived_variant": column,
+        "sealed_sha256": {"qv0": sealed["qv_kg_per_kg"], "pi0": sealed["pi"]},
+    }
+    (HERE / "wk_cm1_nz40.json").write_text(json.dumps(record, indent=1, sort_keys=True))
+    print("wrote wk_cm1_nz40")
+
+
 def make_c1(reference: Path, checkpoints: list[int]) -> None:
     """Digests after each checkpoint N, each from a fresh state with one call
     of steps=N (the reference refuses a non-fresh entry state, ppx != pp3d,
@@ -501,7 +530,7 @@ def make_c1(reference: Path, checkpoints: list[int]) -> None:
 def main() -> None:
     p = argparse.ArgumentParser()
     p.add_argument("--reference", type=Path, required=True, help="root of the reference source tree")
-    p.add_argument("what", choices=("small", "c1", "advection", "kessler", "tke", "rk", "bridge"))
+    p.add_argument("what", choices=("small", "c1", "advection", "kessler", "tke", "rk", "bridge", "wk"))
     p.add_argument("--checkpoints", type=int, nargs="+", default=[1])
     args = p.parse_args()
     if args.what == "small":
@@ -516,6 +545,8 @@ def main() -> None:
         make_bridge(args.reference)
     elif args.what == "tke":
         make_tke(args.reference)
+    elif args.what == "wk":
+        make_wk(args.reference)
     else:
         make_c1(args.reference, sorted(set(args.checkpoints)))
 
