@@ -356,6 +356,39 @@ GM1B_API int32_t gm1b_sgs_tke(int32_t ni, int32_t nj, int32_t nk, const gm1b_sgs
                               float dx, float dy, float dz, void *stream);
 
 /* ------------------------------------------------------------------------
+ * CM1 limits: small-step bound, substep count, advective Courant number
+ * ---------------------------------------------------------------------- */
+
+/* 0.60*min(dx,dy)/360 in binary64 (misclibs.F:867).  Replaces
+ * cm1_acoustic_small_step_limit_s (src/cm1core/gm1_runtime.py:249); returns
+ * NaN (message in gm1b_last_error) unless dx, dy are finite and positive. */
+GM1B_API double gm1b_acoustic_small_step_limit(double dx, double dy);
+
+/* The nsound CM1 would choose for dt on this grid (misclibs.F:883-885).
+ * Replaces cm1_diagnostic_acoustic_substeps (src/cm1core/gm1_runtime.py:284). */
+GM1B_API int32_t gm1b_diagnostic_acoustic_substeps(double dt, double dx, double dy, int32_t *nsound);
+
+/* Scalar advective Courant number of one wind vector, binary64
+ * (misclibs.F:2747-2765).  Replaces cm1_advective_courant
+ * (src/cm1core/gm1_runtime.py:458). */
+GM1B_API int32_t gm1b_advective_courant(double dt, double dx, double dy, double dz, double u, double v, double w,
+                                        double *out);
+
+/*
+ * Domain advective Courant number (CM1 calccflquick) of DEVICE winds u
+ * (nk, nj, ni+1), v (nk, nj+1, ni), w (nk+1, nj, ni) with stretching
+ * factors uh (ni), vh (nj), mh (nk) and dtdx = 0.5*dt*rdx etc. as binary32.
+ * level_keys (nk words, device) receives each level's maximum as an order
+ * key (float bits; 0xffffffff = a NaN in that level); *out (device) the
+ * maximum over levels, a NaN level never replacing the running maximum.
+ * Replaces advective_courant_number / _reduce_courant
+ * (src/cm1core/storm_diagnostics.py:249,195).
+ */
+GM1B_API int32_t gm1b_courant_max(int32_t ni, int32_t nj, int32_t nk, const float *u, const float *v, const float *w,
+                                  const float *uh, const float *vh, const float *mh, float dtdx, float dtdy,
+                                  float dtdz, uint32_t *level_keys, float *out, void *stream);
+
+/* ------------------------------------------------------------------------
  * Analytic initial state (host, once per run, except the bubble field)
  * ---------------------------------------------------------------------- */
 

@@ -465,6 +465,79 @@ def make_bridge(reference: Path) -> None:
     print("wrote eqtset2_cells")
 
 
+def make_limits(reference: Path) -> None:
+    """CM1 limits through the reference's own functions: the small-step
+    bound, the diagnostic substep count and the scalar Courant number on a
+    table of grids and winds (src/cm1core/gm1_runtime.py:249,284,458), and the
+    domain Courant number of advective_courant_number
+    (src/cm1core/storm_diagnostics.py:249) run on seeded winds with NumPy in
+    place of CuPy (the function only uses cp.add/multiply/sqrt with out=,
+    cp.amax, cp.empty and cp.asnumpy)."""
+    import contextlib  # noqa: PLC0415
+    import types  # noqa: PLC0415
+
+    sys.path.insert(0, str(reference / "src"))
+    from cm1core.gm1_runtime import (
+        cm1_acoustic_small_step_limit_s,
+        cm1_advective_courant,
+        cm1_diagnostic_acoustic_substeps,
+    )
+    from cm1core.storm_diagnostics import advective_courant_number
+
+    rng = np.random.default_rng(71)
+    table = []
+    for dx, dy in ((1000.0, 1000.0), (250.0, 250.0), (333.33, 500.0), (2000.0, 1500.0), (100.0, 3000.0),
+                   (20.0, 20.0)):
+        for dt in (1.0, 2.5, 6.0, 7.5, 10.0, 12.0, 30.0):
+            u, v, w = (float(x) for x in rng.normal(0.0, 25.0, 3))
+            dz = float(rng.uniform(20.0, 500.0))
+            table.append({
+                "dx": dx, "dy": dy, "dt": dt, "dz": dz, "u": u, "v": v, "w": w,
+                "limit": cm1_acoustic_small_step_limit_s(dx_m=dx, dy_m=dy),
+                "nsound": cm1_diagnostic_acoustic_substeps(dt_s=dt, dx_m=dx, dy_m=dy),
+                "courant": cm1_advective_courant(dt_s=dt, dx_m=dx, dy_m=dy, dz_m=dz, u_m_s=u, v_m_s=v, w_m_s=w),
+            })
+
+    shim = types.SimpleNamespace(float32=np.float32, empty=np.empty, add=np.add, multiply=np.multiply,
+                                 sqrt=np.sqrt, amax=np.amax, asnumpy=np.asarray)
+    cases = {}
+    for tag, (nx, ny, nz, dx, dy, dz, dt, stretch, poison) in {
+        "a": (12, 10, 9, 1000.0, 1000.0, 500.0, 6.0, False, None),
+        "b": (9, 11, 6, 250.0, 333.0, 100.0, 2.0, True, None),
+        "c": (16, 8, 7, 500.0, 500.0, 250.0, 3.0, False, (0, "nan")),
+        "d": (10, 10, 8, 1000.0, 1000.0, 500.0, 6.0, True, (3, "nan")),
+        "e": (8, 9, 5, 1000.0, 1000.0, 500.0, 6.0, False, (2, "inf")),
+    }.items():
+        u = rng.normal(5.0, 20.0, (nz, ny, nx + 1)).astype(np.float32)
+        v = rng.normal(-3.0, 15.0, (nz, ny + 1, nx)).astype(np.float32)
+        w = rng.normal(0.0, 8.0, (nz + 1, ny, nx)).astype(np.float32)
+        uh = np.ones(nx + 6, np.float32)
+        vh = np.ones(ny + 6, np.float32)
+        mh = np.ones(nz, np.float32)
+        if stretch:
+            uh[3:3 + nx] = rng.uniform(0.8, 1.25, nx).astype(np.float32)
+            vh[3:3 + ny] = rng.uniform(0.8, 1.25, ny).astype(np.float32)
+            mh[:] = rng.uniform(0.5, 2.0, nz).astype(np.float32)
+        if poison is not None:
+            level, kind = poison
+            u[level, ny // 2, nx // 2] = np.float32("nan") if kind == "nan" else np.float32("inf")
+        grid = types.SimpleNamespace(nx=nx, ny=ny, nz=nz, dx_m=dx, dy_m=dy, dz_m=dz)
+        runtime = types.SimpleNamespace(
+            cp=shim, stream=contextlib.nullcontext(),
+            config=types.SimpleNamespace(grid=grid, dt_s=dt),
+            dynamics=types.SimpleNamespace(fields={"u3d": u, "v3d": v, "w3d": w}, arrays={"uh": uh, "vh": vh},
+                                           metrics={"mh": mh}))
+        with np.errstate(invalid="ignore", over="ignore"):
+            number = advective_courant_number(runtime)
+        cases[tag] = dict(meta=json.dumps({"nx": nx, "ny": ny, "nz": nz, "dx": dx, "dy": dy, "dz": dz, "dt": dt,
+                                           "courant": number}),
+                          u=u, v=v, w=w, uh=uh[3:3 + nx].copy(), vh=vh[3:3 + ny].copy(), mh=mh)
+    np.savez_compressed(HERE / "limits_courant.npz",
+                        table=json.dumps(table),
+                        **{f"{tag}_{k}": val for tag, c in cases.items() for k, val in c.items()})
+    print("wrote limits_courant", {t: json.loads(c["meta"])["courant"] for t, c in cases.items()})
+
+
 def make_wk(reference: Path) -> None:
     """CM1 r21.1's own Weisman-Klemp base state (isnd=5, nz=40, dz=500 m) as
     float32 words, from the CM1 output the reference keeps
@@ -530,7 +603,7 @@ def make_c1(reference: Path, checkpoints: list[int]) -> None:
 def main() -> None:
     p = argparse.ArgumentParser()
     p.add_argument("--reference", type=Path, required=True, help="root of the reference source tree")
-    p.add_argument("what", choices=("small", "c1", "advection", "kessler", "tke", "rk", "bridge", "wk"))
+    p.add_argument("what", choices=("small", "c1", "advection", "kessler", "tke", "rk", "bridge", "wk", "limits"))
     p.add_argument("--checkpoints", type=int, nargs="+", default=[1])
     args = p.parse_args()
     if args.what == "small":
@@ -547,6 +620,8 @@ def main() -> None:
         make_tke(args.reference)
     elif args.what == "wk":
         make_wk(args.reference)
+    elif args.what == "limits":
+        make_limits(args.reference)
     else:
         make_c1(args.reference, sorted(set(args.checkpoints)))
 
