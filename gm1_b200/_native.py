@@ -17,6 +17,7 @@ ABI_VERSION = 1
 GM1B_OK = 0
 GM1B_ERR_ARGUMENT = -1
 GM1B_FLAG_SCRATCH_OUTPUTS = 1
+GM1B_FLAG_MULTI_LAUNCH_STAGE = 2
 
 # ablation bits of include/gm1b.h, keyed by the reference field names
 ABLATION_BITS = {

@@ -14,6 +14,7 @@
 // one CTA per 32-column row tile: the k-parallel parts (divergence, pi'
 // advection, fpk, tridiagonal coefficients, pressure update) use all warps,
 // and the sequential Thomas sweep runs on one warp out of shared memory.
+#include <cstdint>
 #include <cstdio>
 
 #include "gm1b_common.cuh"
@@ -330,12 +331,17 @@ __global__ void __launch_bounds__(kTX *kTY) traj_momentum_kernel(Arr a, Dims d, 
 // acoustic stage: preparation (cpu_sound3_periodic_stage_inplace :690-822)
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kTX *kTY) sound_prep_kernel(Arr a, Dims d, int nrk, float dts, float rdz, float cp,
-                                                              float beta, int scratch_outputs) {
+                                                              float beta, int scratch_outputs, int fused_reset) {
     const int i = blockIdx.x * kTX + threadIdx.x;
     const int j = blockIdx.y * kTY + threadIdx.y;
     const int k = blockIdx.z;
     const int ni = d.ni, nj = d.nj, nk = d.nk;
     if (i >= ni + 2 || j >= nj + 2) return;
+    if (fused_reset && i == 0 && j == 0 && k == 0) {
+        // grid-barrier counter and status of the fused stage kernel
+        *reinterpret_cast<unsigned long long *>(a.tri_residual) = 0ull;
+        reinterpret_cast<int *>(a.tri_residual)[2] = 0;
+    }
     const size_t c = d.s(k, j, i);
     const bool klive = k >= 1 && k <= nk;
     if (klive) {
@@ -652,6 +658,8 @@ __global__ void __launch_bounds__(kTX *kColWarps, 1) sound_column_kernel(Arr a, 
 #undef SM
 }
 
+#include "periodic_stage_fused.cuh"
+
 // ---------------------------------------------------------------------------
 // trajectory: averaged-flux rescale and the advected theta carrier
 // (_scale_averages_cpu :496-512, sadv part of _theta_tendency_update_cpu)
@@ -825,10 +833,71 @@ bool prepare_column_kernel(int nk) {
     return true;
 }
 
+// Whether the fused stage kernel can run this stage: benchmark path (no
+// scratch outputs, multi-launch not forced), at least two small steps, the
+// stage state within one CTA's shared memory, every row-tile CTA co-resident
+// (cooperative launch), and an 8-byte aligned barrier word.  Attributes are
+// set once per device.
+bool fused_stage_eligible(const Arr &a, const Dims &d, int nloop, uint32_t flags) {
+    if ((flags & (GM1B_FLAG_SCRATCH_OUTPUTS | GM1B_FLAG_MULTI_LAUNCH_STAGE)) != 0 || nloop < 2) return false;
+    if ((reinterpret_cast<uintptr_t>(a.tri_residual) & 7u) != 0) return false;
+    // the kernel's fixed-trip loops cover (kFusedMaxNk + 1) levels
+    static_assert(34 * (kFusedMaxNk + 1) <= kLoadTrips * kFusedThreads, "stage-load trips");
+    static_assert(kFusedMaxNk + 1 <= kLoadTrips * kColWarps, "level trips");
+    if (d.nk > kFusedMaxNk) return false;
+    const size_t bytes = fused_smem_floats(d.nk) * sizeof(float);
+    if (bytes > 227 * 1024) return false;
+    static int capacity[64] = {};  // co-resident CTAs per device, -1 = unusable
+    static size_t configured[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return false;
+    if (configured[dev] < bytes) {
+        int coop = 0, sms = 0, per_sm = 0;
+        cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaError_t e =
+            cudaFuncSetAttribute(sound_stage_fused_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        if (e == cudaSuccess)
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sound_stage_fused_kernel, kFusedThreads, bytes);
+        if (e != cudaSuccess || !coop) {
+            cudaGetLastError();
+            capacity[dev] = -1;
+        } else {
+            capacity[dev] = per_sm * sms;
+        }
+        configured[dev] = bytes;
+    }
+    const long long ctas = (long long)((d.ni + kTX - 1) / kTX) * d.nj;
+    return capacity[dev] > 0 && ctas <= capacity[dev];
+}
+
+int launch_fused_stage(const Arr &a, const Dims &d, const FusedArgs &p, cudaStream_t st) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((d.ni + kTX - 1) / kTX, d.nj);
+    cfg.blockDim = dim3(kTX, kColWarps);
+    cfg.dynamicSmemBytes = fused_smem_floats(d.nk) * sizeof(float);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    ProfScope ps_("sound_stage_fused_kernel", st);
+    cudaError_t e = cudaLaunchKernelEx(&cfg, sound_stage_fused_kernel, a, d, p);
+    ps_.stop();
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        gm1b_set_error("sound_stage_fused_kernel (cooperative launch): %s", cudaGetErrorString(e));
+        return GM1B_ERR_CUDA;
+    }
+    return check_launch("sound_stage_fused_kernel") ? GM1B_OK : GM1B_ERR_CUDA;
+}
+
 // One acoustic RK stage; returns nloop, or a negative status.
 int enqueue_sound_stage(const Arr &a, const Dims &d, float dt, int nsound, int nrk, float rdx, float rdy, float rdz,
-                        float cp, float alph, float kdiv, int scratch_outputs, int trajectory, int post_ppx,
+                        float cp, float alph, float kdiv, uint32_t flags, int trajectory, int post_ppx,
                         cudaStream_t st) {
+    const int scratch_outputs = (flags & GM1B_FLAG_SCRATCH_OUTPUTS) ? 1 : 0;
     int nloop;
     float dts;
     if (schedule(dt, nsound, nrk, &nloop, &dts) != 0) {
@@ -837,15 +906,39 @@ int enqueue_sound_stage(const Arr &a, const Dims &d, float dt, int nsound, int n
     }
     const float beta = 1.0f - alph;
     const float asq = alph * alph;
+    const bool fused = fused_stage_eligible(a, d, nloop, flags);
     {
             ProfScope ps_("sound_prep_kernel", st);
             sound_prep_kernel<<<box_grid(d.ni + 2, d.nj + 2, d.nk + 2), dim3(kTX, kTY), 0, st>>>(a, d, nrk, dts, rdz, cp, beta,
-                                                                                        scratch_outputs);
+                                                                                        scratch_outputs, fused ? 1 : 0);
             ps_.stop();
         }
     if (!check_launch("sound_prep_kernel")) return GM1B_ERR_CUDA;
     const float tem1x = (rdx * cp) * 0.5f;
     const float tem2y = (rdy * cp) * 0.5f;
+    if (fused) {
+        FusedArgs f;
+        f.nrk = nrk;
+        f.nloop = nloop;
+        f.dts = dts;
+        f.rdx = rdx;
+        f.rdy = rdy;
+        f.alph = alph;
+        f.beta = beta;
+        f.asq = asq;
+        f.kdiv = kdiv;
+        f.smeps = kSmeps;
+        f.temx = (dts * 0.5f) * rdx;
+        f.temy = (dts * 0.5f) * rdy;
+        f.rnloop = 1.0f / (float)nloop;
+        f.tem1x = tem1x;
+        f.tem2y = tem2y;
+        f.tavg = 1.0f / (float)nloop;
+        f.fill_pp3d = (nrk < 3) || trajectory;
+        f.post_ppx = post_ppx;
+        const int r = launch_fused_stage(a, d, f, st);
+        return r < 0 ? r : nloop;
+    }
     ColumnArgs p;
     p.nrk = nrk;
     p.nloop = nloop;
@@ -937,9 +1030,8 @@ extern "C" int32_t gm1b_sound3_periodic_three_stage(int32_t ni, int32_t nj, int3
     if (!prepare_column_kernel(nk)) return GM1B_ERR_CUDA;
     const Dims d{ni, nj, nk};
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    const int scratch = (flags & GM1B_FLAG_SCRATCH_OUTPUTS) ? 1 : 0;
     for (int nrk = 1; nrk <= 3; ++nrk) {
-        int r = enqueue_sound_stage(*arrays, d, dt, nsound, nrk, rdx, rdy, rdz, cp, alph, kdiv, scratch, 0, 0, st);
+        int r = enqueue_sound_stage(*arrays, d, dt, nsound, nrk, rdx, rdy, rdz, cp, alph, kdiv, flags, 0, 0, st);
         if (r < 0) return r;
     }
     return GM1B_OK;
@@ -974,7 +1066,6 @@ extern "C" int32_t gm1b_psolver3_trajectory(int32_t ni, int32_t nj, int32_t nk, 
     const Dims d{ni, nj, nk};
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const float rdx = 1.0f / dx, rdy = 1.0f / dy, rdz = 1.0f / dz;
-    const int scratch = (flags & GM1B_FLAG_SCRATCH_OUTPUTS) ? 1 : 0;
     const int advect = !(ablations & GM1B_ABLATE_MOMENTUM_ADVECTION);
     const int buoy = !(ablations & GM1B_ABLATE_BUOYANCY);
     const int theta_adv = !(ablations & GM1B_ABLATE_SCALAR_ADVECTION);
@@ -1010,7 +1101,7 @@ extern "C" int32_t gm1b_psolver3_trajectory(int32_t ni, int32_t nj, int32_t nk, 
                             ps_.stop();
                         }
             if (!check_launch("traj_momentum_kernel")) return GM1B_ERR_CUDA;
-            int r = enqueue_sound_stage(a, d, dt, nsound, nrk, rdx, rdy, rdz, kCp, kAlph, kKdiv, scratch, 1,
+            int r = enqueue_sound_stage(a, d, dt, nsound, nrk, rdx, rdy, rdz, kCp, kAlph, kKdiv, flags, 1,
                                         post_ppx, st);
             if (r < 0) return r;
             {

@@ -139,18 +139,23 @@ def launch_cuda_sound3_periodic_three_stage(
     kdiv: float = CM1_SOUND3_PERIODIC_KDIV_F32,
     stream: Any | None = None,
     scratch_outputs: bool = False,
+    fused_stage: bool = True,
 ) -> CudaLaunch:
     """Enqueue the three periodic acoustic RK stages without synchronising.
 
     ``scratch_outputs`` also writes the reference-semantics scratch arrays of
     the last small step (fpk, divh, hadvp, elim_c, elim_d, tri_*); without it
-    those arrays are left unspecified."""
+    those arrays are left unspecified.  ``fused_stage`` lets a stage without
+    scratch outputs run as one persistent kernel (same words); False forces
+    two launches per small step."""
     for nrk in (1, 2, 3):
         sound3_stage_schedule_f32(dt, nsound, nrk)
     a, device = _require_device_arrays(arrays, SOUND_ARRAY_NAMES, array_shapes(ni, nj, nk), "periodic sound3")
     st = _stream(stream, device)
     s = _struct(a)
     flags = _native.GM1B_FLAG_SCRATCH_OUTPUTS if scratch_outputs else 0
+    if not fused_stage:
+        flags |= _native.GM1B_FLAG_MULTI_LAUNCH_STAGE
     with torch.cuda.device(device):
         status = _native.lib().gm1b_sound3_periodic_three_stage(
             ni, nj, nk, ctypes.byref(s), dt, nsound, rdx, rdy, rdz, cp, alph, kdiv, flags,
@@ -192,12 +197,14 @@ def launch_cuda_psolver3_trajectory(
     ablations: TrajectoryAblations | int | None = None,
     stream: Any | None = None,
     scratch_outputs: bool = True,
+    fused_stage: bool = True,
 ) -> CudaLaunch:
     """Enqueue ``steps`` dry RK3 large steps of the periodic trajectory.
 
     ``scratch_outputs`` (default, as the reference's outputs include them)
     writes tri_pivot/tri_residual and the other acoustic scratch arrays of the
-    final small step; pass False for the fastest path."""
+    final small step; pass False for the fastest path, where each acoustic
+    stage runs as one persistent kernel unless ``fused_stage`` is False."""
     if isinstance(steps, bool) or not isinstance(steps, int) or steps < 1:
         raise ValueError("steps must be an integer >= 1")
     _validate_run_parameters(ni=ni, nj=nj, nk=nk, dt=dt, nsound=nsound, dx=dx, dy=dy, dz=dz)
@@ -212,6 +219,8 @@ def launch_cuda_psolver3_trajectory(
     st = _stream(stream, device)
     s = _struct(a)
     flags = _native.GM1B_FLAG_SCRATCH_OUTPUTS if scratch_outputs else 0
+    if not fused_stage:
+        flags |= _native.GM1B_FLAG_MULTI_LAUNCH_STAGE
     with torch.cuda.device(device):
         status = _native.lib().gm1b_psolver3_trajectory(
             ni, nj, nk, ctypes.byref(s), steps, dt, nsound, dx, dy, dz, mask, flags,

@@ -50,6 +50,15 @@ extern "C" {
  * step (fpk, divh, hadvp, elim_c, elim_d, tri_aa, tri_bb, tri_cc, tri_dd,
  * tri_pivot, tri_residual).  Without it those arrays are scratch. */
 #define GM1B_FLAG_SCRATCH_OUTPUTS 1u
+/* Without scratch outputs, each acoustic stage normally runs as one
+ * persistent cooperative kernel (all small steps, one bounded grid barrier
+ * per small step) when its row tiles are co-resident and nk <= 44; that
+ * kernel uses tri_aa/tri_bb as a double buffer of ppd and tri_residual
+ * words 0-2 as its barrier counter and status (word 2 nonzero = a grid
+ * barrier gave up and the stage was abandoned).  This flag forces the
+ * multi-launch stage (two kernels per small step) instead; both produce the
+ * same words in every non-scratch array. */
+#define GM1B_FLAG_MULTI_LAUNCH_STAGE 2u
 
 /* ablation bits of the dry trajectory
  * (src/cm1core/cuda_psolver3_trajectory.py:429-436 TrajectoryAblations);

@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 import torch
 
-from gm1_b200.arrays import ALL_ARRAY_NAMES, SOUND_ARRAY_NAMES, TRAJECTORY_STATE_NAMES
+from gm1_b200.arrays import ALL_ARRAY_NAMES, SCRATCH_OUTPUT_NAMES, SOUND_ARRAY_NAMES, TRAJECTORY_STATE_NAMES
 from gm1_b200.initial_state import DRY_BUBBLE_64, dry_periodic_state
 from gm1_b200.periodic import (
     TrajectoryAblations,
@@ -41,11 +41,38 @@ def test_sound3_three_stage_bit_exact_vs_reference(tag):
     assert bit_mismatches(expected, got, SOUND_ARRAY_NAMES) == {}
 
 
-def test_sound3_without_scratch_outputs_keeps_state_bits():
-    meta, inputs, expected = load_npz("sound3_5x4x7")
-    got, _ = _run_sound(inputs, meta, scratch=False)
+@pytest.mark.parametrize("fused", [True, False])
+@pytest.mark.parametrize("tag", ["sound3_5x4x7", "sound3_8x6x12"])
+def test_sound3_without_scratch_outputs_keeps_state_bits(tag, fused):
+    """Both stage paths without scratch outputs: the persistent one-kernel
+    stage (fused) and two launches per small step."""
+    meta, inputs, expected = load_npz(tag)
+    dev = to_device(inputs)
+    keys = ("ni", "nj", "nk", "dt", "nsound", "rdx", "rdy", "rdz")
+    launch = launch_cuda_sound3_periodic_three_stage(dev, scratch_outputs=False, fused_stage=fused,
+                                                     **{k: meta[k] for k in keys})
+    launch.ready_event.synchronize()
+    got = to_host(dev)
     state = ("u3d", "v3d", "w3d", "pp3d", "ppx", "ppd", "rru", "rrv", "rrw", "qk", "pk1", "pk2", "mm")
     assert bit_mismatches(expected, got, state) == {}
+    if fused:  # barrier status word of the fused stage: no barrier gave up
+        assert int(got["tri_residual"].reshape(-1)[:3].view(np.int32)[2]) == 0
+
+
+@pytest.mark.parametrize("fused", [True, False])
+@pytest.mark.parametrize("tag", ["traj_7x6x7", "traj_9x5x8"])
+def test_trajectory_fast_paths_match_reference_on_state_words(tag, fused):
+    """The benchmark path on the reference's golden trajectories: every array
+    except the acoustic scratch outputs bit-identical."""
+    meta, inputs, expected = load_npz(tag)
+    dev = to_device(inputs)
+    keys = ("ni", "nj", "nk", "steps", "dt", "nsound", "dx", "dy", "dz")
+    launch = launch_cuda_psolver3_trajectory(dev, scratch_outputs=False, fused_stage=fused,
+                                             **{k: meta[k] for k in keys})
+    launch.ready_event.synchronize()
+    got = to_host(dev)
+    names = [n for n in ALL_ARRAY_NAMES if n not in SCRATCH_OUTPUT_NAMES]
+    assert bit_mismatches(expected, got, names) == {}
 
 
 @pytest.mark.parametrize("tag", ["traj_7x6x7", "traj_9x5x8"])
@@ -122,18 +149,28 @@ def test_c1_matches_reference_digests():
         assert bad == [], (step, bad)
 
 
-def test_fast_path_without_scratch_outputs_keeps_every_state_word():
+@pytest.mark.parametrize("fused", [True, False])
+def test_fast_path_without_scratch_outputs_keeps_every_state_word(fused):
     """The benchmark path (no scratch outputs: stage-constant tridiagonal
-    coefficients reused across small steps) is bit-identical to the oracle
-    on every array the reference's trajectory compares, except the acoustic
-    scratch it repurposes."""
+    coefficients reused across small steps; with ``fused`` each acoustic
+    stage is one persistent kernel) is bit-identical to the oracle on every
+    array except the acoustic scratch it repurposes."""
     host = dry_periodic_state(DRY_BUBBLE_64)
     dev = to_device(host)
-    launch_cuda_psolver3_trajectory(dev, scratch_outputs=False, **_c1_params(3))
+    launch_cuda_psolver3_trajectory(dev, scratch_outputs=False, fused_stage=fused, **_c1_params(3))
     orc.traj_steps(host, **_c1_params(3))
     torch.cuda.synchronize()
+    got = to_host(dev)
     names = [n for n in TRAJECTORY_STATE_NAMES if n not in ("tri_pivot", "tri_residual")]
-    assert bit_mismatches(host, to_host(dev), names) == {}
+    assert bit_mismatches(host, got, names) == {}
+    names = [n for n in ALL_ARRAY_NAMES if n not in SCRATCH_OUTPUT_NAMES]
+    assert bit_mismatches(host, got, names) == {}
+    if fused:
+        words = got["tri_residual"].reshape(-1)[:3].view(np.int32)
+        assert int(words[2]) == 0
+        # 64-bit arrive count after the last stage: (nloop - 1) barriers x 128 CTAs
+        count = int(got["tri_residual"].reshape(-1)[:2].view(np.uint64)[0])
+        assert count == 5 * 2 * 64
 
 
 def test_repeat_runs_are_bit_identical_and_streams_are_honoured():
