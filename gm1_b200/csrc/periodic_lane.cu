@@ -94,48 +94,36 @@ struct View {
     }
 };
 
-__device__ __forceinline__ float x_flux5(const View &s, float vel, int face, int j, int k, int n) {
-    float r;
-    if (vel >= 0.0f)
-        r = flx5(s.at(k, j, pmod(face - 3, n)), s.at(k, j, pmod(face - 2, n)), s.at(k, j, pmod(face - 1, n)),
-                 s.at(k, j, pmod(face, n)), s.at(k, j, pmod(face + 1, n)));
-    else
-        r = flx5(s.at(k, j, pmod(face + 2, n)), s.at(k, j, pmod(face + 1, n)), s.at(k, j, pmod(face, n)),
-                 s.at(k, j, pmod(face - 1, n)), s.at(k, j, pmod(face - 2, n)));
+// Upwind fifth-order face value from the six points lo..lo+5 that hold both
+// upwind stencils: vel >= 0 uses lo..lo+4, vel < 0 uses lo+5..lo+1 (the same
+// flx5 operand order as the reference's two branches).  All six points are
+// read before the sign of vel is known, so no load waits on the velocity.
+__device__ __forceinline__ float upwind5(float vel, float s0, float s1, float s2, float s3, float s4, float s5) {
+    const bool pos = vel >= 0.0f;
+    const float r = flx5(pos ? s0 : s5, pos ? s1 : s4, pos ? s2 : s3, pos ? s3 : s2, pos ? s4 : s1);
     return vel * r;
+}
+
+// x flux at the face between points face-1 and face (stencil face-3..face+2)
+__device__ __forceinline__ float x_flux5(const View &s, float vel, int face, int j, int k, int n) {
+    return upwind5(vel, s.at(k, j, pmod(face - 3, n)), s.at(k, j, pmod(face - 2, n)), s.at(k, j, pmod(face - 1, n)),
+                   s.at(k, j, pmod(face, n)), s.at(k, j, pmod(face + 1, n)), s.at(k, j, pmod(face + 2, n)));
 }
 
 __device__ __forceinline__ float y_flux5(const View &s, float vel, int i, int face, int k, int n) {
-    float r;
-    if (vel >= 0.0f)
-        r = flx5(s.at(k, pmod(face - 3, n), i), s.at(k, pmod(face - 2, n), i), s.at(k, pmod(face - 1, n), i),
-                 s.at(k, pmod(face, n), i), s.at(k, pmod(face + 1, n), i));
-    else
-        r = flx5(s.at(k, pmod(face + 2, n), i), s.at(k, pmod(face + 1, n), i), s.at(k, pmod(face, n), i),
-                 s.at(k, pmod(face - 1, n), i), s.at(k, pmod(face - 2, n), i));
-    return vel * r;
+    return upwind5(vel, s.at(k, pmod(face - 3, n), i), s.at(k, pmod(face - 2, n), i), s.at(k, pmod(face - 1, n), i),
+                   s.at(k, pmod(face, n), i), s.at(k, pmod(face + 1, n), i), s.at(k, pmod(face + 2, n), i));
 }
 
+// flux at the face between points b and b+1 (stencil b-2..b+3)
 __device__ __forceinline__ float x_flux5c(const View &s, float vel, int b, int j, int k, int n) {
-    float r;
-    if (vel >= 0.0f)
-        r = flx5(s.at(k, j, pmod(b - 2, n)), s.at(k, j, pmod(b - 1, n)), s.at(k, j, pmod(b, n)),
-                 s.at(k, j, pmod(b + 1, n)), s.at(k, j, pmod(b + 2, n)));
-    else
-        r = flx5(s.at(k, j, pmod(b + 3, n)), s.at(k, j, pmod(b + 2, n)), s.at(k, j, pmod(b + 1, n)),
-                 s.at(k, j, pmod(b, n)), s.at(k, j, pmod(b - 1, n)));
-    return vel * r;
+    return upwind5(vel, s.at(k, j, pmod(b - 2, n)), s.at(k, j, pmod(b - 1, n)), s.at(k, j, pmod(b, n)),
+                   s.at(k, j, pmod(b + 1, n)), s.at(k, j, pmod(b + 2, n)), s.at(k, j, pmod(b + 3, n)));
 }
 
 __device__ __forceinline__ float y_flux5c(const View &s, float vel, int i, int b, int k, int n) {
-    float r;
-    if (vel >= 0.0f)
-        r = flx5(s.at(k, pmod(b - 2, n), i), s.at(k, pmod(b - 1, n), i), s.at(k, pmod(b, n), i),
-                 s.at(k, pmod(b + 1, n), i), s.at(k, pmod(b + 2, n), i));
-    else
-        r = flx5(s.at(k, pmod(b + 3, n), i), s.at(k, pmod(b + 2, n), i), s.at(k, pmod(b + 1, n), i),
-                 s.at(k, pmod(b, n), i), s.at(k, pmod(b - 1, n), i));
-    return vel * r;
+    return upwind5(vel, s.at(k, pmod(b - 2, n), i), s.at(k, pmod(b - 1, n), i), s.at(k, pmod(b, n), i),
+                   s.at(k, pmod(b + 1, n), i), s.at(k, pmod(b + 2, n), i), s.at(k, pmod(b + 3, n), i));
 }
 
 // CM1 stag=1/2/3 vertical flux at Fortran face `face`; nk levels in the view
@@ -155,12 +143,9 @@ __device__ __forceinline__ float z_flux_mass(const View &s, float v, int face, i
     } else if (face == nk) {
         recon = (v >= 0.0f) ? flx3(s.at(nk - 3, j, i), s.at(nk - 2, j, i), s.at(nk - 1, j, i))
                             : (c1 * s.at(nk - 2, j, i) + c2 * s.at(nk - 1, j, i));
-    } else if (v >= 0.0f) {
-        recon = flx5(s.at(face - 4, j, i), s.at(face - 3, j, i), s.at(face - 2, j, i), s.at(face - 1, j, i),
-                     s.at(face, j, i));
     } else {
-        recon = flx5(s.at(face + 1, j, i), s.at(face, j, i), s.at(face - 1, j, i), s.at(face - 2, j, i),
-                     s.at(face - 3, j, i));
+        return upwind5(v, s.at(face - 4, j, i), s.at(face - 3, j, i), s.at(face - 2, j, i), s.at(face - 1, j, i),
+                       s.at(face, j, i), s.at(face + 1, j, i));
     }
     return v * recon;
 }
@@ -181,12 +166,9 @@ __device__ __forceinline__ float z_flux_w(const View &s, float v, int level, int
     } else if (level == nk) {
         recon = (v >= 0.0f) ? flx3(s.at(nk - 2, j, i), s.at(nk - 1, j, i), s.at(nk, j, i))
                             : (0.5f * (s.at(nk - 1, j, i) + s.at(nk, j, i)));
-    } else if (v >= 0.0f) {
-        recon = flx5(s.at(level - 3, j, i), s.at(level - 2, j, i), s.at(level - 1, j, i), s.at(level, j, i),
-                     s.at(level + 1, j, i));
     } else {
-        recon = flx5(s.at(level + 2, j, i), s.at(level + 1, j, i), s.at(level, j, i), s.at(level - 1, j, i),
-                     s.at(level - 2, j, i));
+        return upwind5(v, s.at(level - 3, j, i), s.at(level - 2, j, i), s.at(level - 1, j, i), s.at(level, j, i),
+                       s.at(level + 1, j, i), s.at(level + 2, j, i));
     }
     return v * recon;
 }
