@@ -365,6 +365,51 @@ GM1B_API int32_t gm1b_sgs_tke(int32_t ni, int32_t nj, int32_t nk, const gm1b_sgs
                               float dx, float dy, float dz, void *stream);
 
 /* ------------------------------------------------------------------------
+ * TKE source inputs: deformation and moist N^2 (compact physical arrays)
+ * ---------------------------------------------------------------------- */
+
+/* u3d (nk, nj, ni+1), v3d (nk, nj+1, ni), w3d/rf/c1/c2/gx/gy/defv/defh
+ * (nk+1, nj, ni), rho (nk, nj, ni), gz/rgz (nj, ni), rgzu (nj, ni+1),
+ * rgzv (nj+1, ni).  The reference's gzu and gzv enter no formula of this
+ * branch and are not passed. */
+typedef struct gm1b_deformation_arrays {
+    const float *u3d, *v3d, *w3d, *rho, *rf, *c1, *c2, *gz, *rgz, *rgzu, *rgzv, *gx, *gy;
+    float *defv, *defh;
+} gm1b_deformation_arrays;
+
+/*
+ * CM1 calcdef, Cartesian terrain branch with four open sides: defv and
+ * defh on face levels 1..nk-1 (levels 0 and nk are zero).  One kernel, no
+ * device scratch.  Replaces launch_cuda_terrain_deformation
+ * (src/cm1core/cuda_terrain_deformation.py:914) and its CPU twin
+ * cpu_terrain_deformation_inplace (:234).  ni, nj, nk >= 3.
+ */
+GM1B_API int32_t gm1b_terrain_deformation(int32_t ni, int32_t nj, int32_t nk, const gm1b_deformation_arrays *arrays,
+                                          float dx, float dy, float dz, void *stream);
+
+/* c1/c2/mf/nm (nk+1, nj, ni), pi0/th0 (nk), prs/pp3d/th3d and the cell
+ * outputs (nk, nj, ni), q3d (6, nk, nj, ni) in the order qv qc qr qi qs qg,
+ * saturation_mask uint8 (nk, nj, ni).  counts (optional, NULL = not
+ * written): four uint64 words ADDED to, saturated, liquid, mixed and ice
+ * face words. */
+typedef struct gm1b_moist_nm_arrays {
+    const float *c1, *c2, *mf, *pi0, *th0, *prs, *pp3d, *th3d, *q3d;
+    float *nm, *temperature, *qt, *thv, *qvci;
+    uint8_t *saturation_mask;
+    uint64_t *counts;
+} gm1b_moist_nm_arrays;
+
+/*
+ * CM1 calcnm, six-species ice-aware branch (liquid at T >= 273.15 K, ice at
+ * T <= 233.15 K, a linear blend between): nm on face levels 1..nk-1 (0 at
+ * levels 0 and nk) and the cell diagnostics.  Replaces launch_cuda_moist_nm
+ * (src/cm1core/cuda_moist_nm.py:542) and its CPU twin cpu_moist_nm_inplace
+ * (:292).  ni, nj >= 1, nk >= 2.
+ */
+GM1B_API int32_t gm1b_moist_nm(int32_t ni, int32_t nj, int32_t nk, const gm1b_moist_nm_arrays *arrays, float dz,
+                               void *stream);
+
+/* ------------------------------------------------------------------------
  * CM1 limits: small-step bound, substep count, advective Courant number
  * ---------------------------------------------------------------------- */
 

@@ -538,6 +538,114 @@ def make_limits(reference: Path) -> None:
     print("wrote limits_courant", {t: json.loads(c["meta"])["courant"] for t, c in cases.items()})
 
 
+def deformation_fixture(ni: int, nj: int, nk: int, seed: int) -> dict[str, np.ndarray]:
+    """Terrain-following calcdef inputs: a smooth seeded terrain, its CM1
+    metric terms, sheared winds with noise, a decreasing density."""
+    rng = np.random.default_rng(seed)
+    f = np.float32
+    dx, dy, dz = f(100.0), f(120.0), f(200.0)
+    zt = f(nk) * dz
+    jj, ii = np.meshgrid(np.arange(nj), np.arange(ni), indexing="ij")
+    zs = (150.0 + 60.0 * np.sin(0.7 * ii + 0.3) * np.cos(0.5 * jj) + rng.uniform(0, 10, (nj, ni))).astype(f)
+    a = {"gz": (zt / (zt - zs)).astype(f), "rgz": ((zt - zs) / zt).astype(f)}
+    zu = np.empty((nj, ni + 1), f)
+    for i in range(ni + 1):
+        zu[:, i] = f(0.5) * (zs[:, max(i - 1, 0)] + zs[:, min(i, ni - 1)])
+    zv = np.empty((nj + 1, ni), f)
+    for j in range(nj + 1):
+        zv[j] = f(0.5) * (zs[max(j - 1, 0)] + zs[min(j, nj - 1)])
+    a["rgzu"] = ((zt - zu) / zt).astype(f)
+    a["rgzv"] = ((zt - zv) / zt).astype(f)
+    a["gzu"] = (zt / (zt - zu)).astype(f)
+    a["gzv"] = (zt / (zt - zv)).astype(f)
+    sigf = (np.arange(nk + 1, dtype=f) * dz)[:, None, None]
+    a["gx"] = ((zt - sigf) * a["gz"] * (a["rgzu"][:, 1:] - a["rgzu"][:, :-1]) / dx).astype(f)
+    a["gy"] = ((zt - sigf) * a["gz"] * (a["rgzv"][1:] - a["rgzv"][:-1]) / dy).astype(f)
+    k = np.arange(nk)[:, None, None]
+    a["u3d"] = (5.0 + 0.4 * k + rng.normal(0, 1.5, (nk, nj, ni + 1))).astype(f)
+    a["v3d"] = (-2.0 + 0.3 * k + rng.normal(0, 1.5, (nk, nj + 1, ni))).astype(f)
+    w = rng.normal(0, 0.8, (nk + 1, nj, ni)).astype(f)
+    w[0] = 0.0
+    w[nk] = 0.0
+    a["w3d"] = w
+    rho = (1.15 * np.exp(-0.00011 * (k + 0.5) * 200.0) + rng.uniform(-0.01, 0.01, (nk, nj, ni))).astype(f)
+    a["rho"] = rho
+    rf = np.empty((nk + 1, nj, ni), f)
+    rf[1:nk] = f(0.5) * (rho[:-1] + rho[1:])
+    rf[0] = f(1.5) * rho[0] - f(0.5) * rho[1]
+    rf[nk] = f(1.5) * rho[nk - 1] - f(0.5) * rho[nk - 2]
+    a["rf"] = rf
+    c1 = rng.uniform(0.4, 0.6, (nk + 1, nj, ni)).astype(f)
+    a["c1"] = c1
+    a["c2"] = (f(1.0) - c1).astype(f)
+    a["defv"] = np.full((nk + 1, nj, ni), np.nan, f)
+    a["defh"] = np.full((nk + 1, nj, ni), np.nan, f)
+    return {n: np.ascontiguousarray(v) for n, v in a.items()} | {"_spacing": np.array([dx, dy, dz], f)}
+
+
+def moist_nm_fixture(ni: int, nj: int, nk: int, seed: int) -> dict[str, np.ndarray]:
+    """calcnm inputs whose temperatures span ~300 K to ~210 K, with vapour
+    near saturation and seeded condensate, so the liquid, mixed-phase and ice
+    branches all occur."""
+    rng = np.random.default_rng(seed)
+    f = np.float32
+    z = (np.arange(nk) + 0.5) / nk
+    t_col = 300.0 - 95.0 * z
+    pi0 = (1.0 - 0.45 * z).astype(f)
+    th0 = (t_col / pi0).astype(f)
+    cells = (nk, nj, ni)
+    a = {"pi0": pi0, "th0": th0}
+    a["pp3d"] = rng.normal(0, 2e-4, cells).astype(f)
+    a["th3d"] = rng.normal(0, 1.5, cells).astype(f)
+    exner = pi0[:, None, None] + a["pp3d"]
+    a["prs"] = (1.0e5 * exner.astype(np.float64) ** (1005.7 / 287.04)).astype(f)
+    temp = (th0[:, None, None] + a["th3d"]) * exner
+    es = 611.2 * np.exp(17.67 * (temp - 273.15) / (temp - 29.65))
+    qsat = 0.622 * es / (a["prs"] - es)
+    q = np.zeros((6,) + cells, f)
+    q[0] = (qsat * rng.uniform(0.85, 1.1, cells)).astype(f)
+    for s, scale in ((1, 4e-4), (2, 2e-4), (3, 2e-4), (4, 1e-4), (5, 1e-4)):
+        q[s] = np.where(rng.random(cells) < 0.5, rng.uniform(0, scale, cells), 0.0).astype(f)
+    a["q3d"] = q
+    face = (nk + 1, nj, ni)
+    c1 = rng.uniform(0.4, 0.6, face).astype(f)
+    a["c1"] = c1
+    a["c2"] = (f(1.0) - c1).astype(f)
+    a["mf"] = rng.uniform(0.9, 1.1, face).astype(f)
+    for n in ("nm",):
+        a[n] = np.full(face, np.nan, f)
+    for n in ("temperature", "qt", "thv", "qvci"):
+        a[n] = np.full(cells, np.nan, f)
+    a["saturation_mask"] = np.full(cells, 7, np.uint8)
+    return {n: np.ascontiguousarray(v) for n, v in a.items()}
+
+
+def make_closure(reference: Path) -> None:
+    """calcdef and calcnm through the reference's CPU twins on seeded inputs."""
+    sys.path.insert(0, str(reference / "src"))
+    from cm1core.cuda_moist_nm import cpu_moist_nm_inplace
+    from cm1core.cuda_terrain_deformation import cpu_terrain_deformation_inplace
+
+    for tag, (ni, nj, nk, seed) in {"calcdef_9x7x8": (9, 7, 8, 41), "calcdef_12x6x10": (12, 6, 10, 43)}.items():
+        a = deformation_fixture(ni, nj, nk, seed)
+        dx, dy, dz = (float(x) for x in a.pop("_spacing"))
+        inputs = {f"in_{k}": v.copy() for k, v in a.items()}
+        cpu_terrain_deformation_inplace(a, ni=ni, nj=nj, nk=nk, dx=dx, dy=dy, dz=dz)
+        meta = {"ni": ni, "nj": nj, "nk": nk, "dx": dx, "dy": dy, "dz": dz}
+        np.savez_compressed(HERE / f"{tag}.npz", meta=json.dumps(meta), **inputs,
+                            out_defv=a["defv"], out_defh=a["defh"])
+        print("wrote", tag)
+    for tag, (ni, nj, nk, seed) in {"moist_nm_8x6x14": (8, 6, 14, 47), "moist_nm_5x9x20": (5, 9, 20, 53)}.items():
+        a = moist_nm_fixture(ni, nj, nk, seed)
+        inputs = {f"in_{k}": v.copy() for k, v in a.items()}
+        r = cpu_moist_nm_inplace(a, ni=ni, nj=nj, nk=nk, dz=250.0)
+        meta = {"ni": ni, "nj": nj, "nk": nk, "dz": 250.0, "saturated": r.saturated_words, "liquid": r.liquid_words,
+                "mixed": r.mixed_words, "ice": r.ice_words}
+        outs = {f"out_{k}": a[k] for k in ("nm", "temperature", "qt", "thv", "qvci", "saturation_mask")}
+        np.savez_compressed(HERE / f"{tag}.npz", meta=json.dumps(meta), **inputs, **outs)
+        print("wrote", tag, meta)
+
+
 def make_wk(reference: Path) -> None:
     """CM1 r21.1's own Weisman-Klemp base state (isnd=5, nz=40, dz=500 m) as
     float32 words, from the CM1 output the reference keeps
@@ -603,7 +711,7 @@ def make_c1(reference: Path, checkpoints: list[int]) -> None:
 def main() -> None:
     p = argparse.ArgumentParser()
     p.add_argument("--reference", type=Path, required=True, help="root of the reference source tree")
-    p.add_argument("what", choices=("small", "c1", "advection", "kessler", "tke", "rk", "bridge", "wk", "limits"))
+    p.add_argument("what", choices=("small", "c1", "advection", "kessler", "tke", "rk", "bridge", "wk", "limits", "closure"))
     p.add_argument("--checkpoints", type=int, nargs="+", default=[1])
     args = p.parse_args()
     if args.what == "small":
@@ -622,6 +730,8 @@ def main() -> None:
         make_wk(args.reference)
     elif args.what == "limits":
         make_limits(args.reference)
+    elif args.what == "closure":
+        make_closure(args.reference)
     else:
         make_c1(args.reference, sorted(set(args.checkpoints)))
 
