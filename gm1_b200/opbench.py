@@ -1,6 +1,6 @@
 """Per-operator device throughput on B200 (library profiling facility).
 
-    python -m gm1_b200.opbench [--ops adv5 adv5-weno massflux] [--grid 256 256 80] [--iters 20]
+    python -m gm1_b200.opbench [--ops adv5 adv5-weno massflux calcdef moistnm courant] [--grid 256 256 80] [--iters 20]
 
 For each operator: seeded synthetic inputs of the given padded-lane grid
 resident in HBM, a 256 MiB L2 flush before every launch, CUDA events around
@@ -29,7 +29,52 @@ ALG_WORDS = {
     "adv5-weno": 9,
     # in: u v w rho0 rf0; out: rru rrv rrw divx
     "massflux": 9,
+    # in: u v w rho rf c1 c2 gx gy; out: defv defh
+    "calcdef": 11,
+    # in: c1 c2 mf prs pp3d th3d q3d(6); out: nm temperature qt thv qvci, mask (1 byte)
+    "moistnm": 17.25,
+    # in: u v w (one reduction)
+    "courant": 3,
 }
+
+_COMPACT: dict = {}
+
+
+def compact_inputs(op: str, ni: int, nj: int, nk: int, device: torch.device) -> dict:
+    """Seeded compact-layout inputs of the closure operators (built once)."""
+    key = (op, ni, nj, nk)
+    if key in _COMPACT:
+        return _COMPACT[key]
+    g = torch.Generator(device="cpu").manual_seed(3)
+
+    def r(shape, lo, hi):
+        return (torch.rand(shape, generator=g) * (hi - lo) + lo).to(device)
+
+    cell, face = (nk, nj, ni), (nk + 1, nj, ni)
+    if op == "calcdef":
+        a = {"u3d": r((nk, nj, ni + 1), -10, 10), "v3d": r((nk, nj + 1, ni), -10, 10), "w3d": r(face, -2, 2),
+             "rho": r(cell, 0.6, 1.2), "rf": r(face, 0.6, 1.2), "c1": r(face, 0.4, 0.6), "gz": r((nj, ni), 1, 1.02),
+             "rgz": r((nj, ni), 0.98, 1), "gzu": r((nj, ni + 1), 1, 1.02), "rgzu": r((nj, ni + 1), 0.98, 1),
+             "gzv": r((nj + 1, ni), 1, 1.02), "rgzv": r((nj + 1, ni), 0.98, 1), "gx": r(face, -1e-3, 1e-3),
+             "gy": r(face, -1e-3, 1e-3), "defv": torch.empty(face, device=device),
+             "defh": torch.empty(face, device=device)}
+        a["c2"] = 1.0 - a["c1"]
+    elif op == "moistnm":
+        a = {"c1": r(face, 0.4, 0.6), "mf": r(face, 0.9, 1.1), "pi0": torch.linspace(1.0, 0.55, nk, device=device),
+             "th0": torch.linspace(300.0, 380.0, nk, device=device), "prs": r(cell, 2e4, 1e5),
+             "pp3d": r(cell, -1e-3, 1e-3), "th3d": r(cell, -2, 2), "q3d": r((6, nk, nj, ni), 0, 2e-3)}
+        a["c2"] = 1.0 - a["c1"]
+        for n in ("temperature", "qt", "thv", "qvci"):
+            a[n] = torch.empty(cell, device=device)
+        a["nm"] = torch.empty(face, device=device)
+        a["saturation_mask"] = torch.empty(cell, dtype=torch.uint8, device=device)
+    else:  # courant
+        a = {"u": r((nk, nj, ni + 1), -30, 30), "v": r((nk, nj + 1, ni), -30, 30), "w": r((nk + 1, nj, ni), -5, 5),
+             "uh": torch.ones(ni, device=device), "vh": torch.ones(nj, device=device),
+             "mh": torch.ones(nk, device=device), "keys": torch.empty(nk, dtype=torch.int32, device=device),
+             "out": torch.empty(1, device=device)}
+    _COMPACT[key] = a
+    return a
 
 
 def hbm_peak() -> tuple[float, str]:
@@ -75,6 +120,23 @@ def run(op: str, a: dict[str, torch.Tensor], ni: int, nj: int, nk: int, stream: 
              "rrw": a["mf_rrw"]},
             {k: a[k] for k in ("rho0_3d", "rf0", "rgzu", "rgzv", "dzdx", "dzdy", "gz")}, a["mf_divx"],
             ni=ni, nj=nj, nk=nk, dx=1000.0, dy=1000.0, dz=250.0, stream=stream)
+    elif op == "calcdef":
+        from .closure import launch_cuda_terrain_deformation  # noqa: PLC0415
+
+        c = compact_inputs(op, ni, nj, nk, a["u3d"].device)
+        launch_cuda_terrain_deformation(c, ni=ni, nj=nj, nk=nk, dx=1000.0, dy=1000.0, dz=250.0, stream=stream)
+    elif op == "moistnm":
+        from .closure import launch_cuda_moist_nm  # noqa: PLC0415
+
+        c = compact_inputs(op, ni, nj, nk, a["u3d"].device)
+        launch_cuda_moist_nm(c, ni=ni, nj=nj, nk=nk, dz=250.0, stream=stream)
+    elif op == "courant":
+        from .limits import advective_courant_number  # noqa: PLC0415
+
+        c = compact_inputs(op, ni, nj, nk, a["u3d"].device)
+        advective_courant_number(u=c["u"], v=c["v"], w=c["w"], uh=c["uh"], vh=c["vh"], mh=c["mh"], dt_s=6.0,
+                                 dx_m=1000.0, dy_m=1000.0, dz_m=250.0, level_keys=c["keys"], stream=stream,
+                                 out=c["out"])
     else:
         raise ValueError(op)
 
