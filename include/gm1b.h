@@ -365,6 +365,41 @@ GM1B_API int32_t gm1b_sgs_tke(int32_t ni, int32_t nj, int32_t nk, const gm1b_sgs
                               float dx, float dy, float dz, void *stream);
 
 /* ------------------------------------------------------------------------
+ * TKE evolution on the terrain lane: turbt and the flux-form RK stages.
+ * Face fields (nk+1, nj, ni): tkea, tke3d, tketen, kmh, kmv, rf, mf, c1, c2,
+ * rrf0; mass fields (nk, nj, ni): rho, mh, divx; gz, rgz (nj, ni), rgzu
+ * (nj, ni+1), rgzv (nj+1, ni); padded mass fluxes rru (nk+2, nj+6, ni+7),
+ * rrv (nk+2, nj+7, ni+6), rrw (nk+3, nj+6, ni+6).
+ * ---------------------------------------------------------------------- */
+typedef struct gm1b_tke_evolution_arrays {
+    float *tkea, *tke3d, *tketen;
+    const float *kmh, *kmv, *rho, *rf, *mh, *mf, *gz, *rgz, *rgzu, *rgzv, *c1, *c2, *rrf0, *rru, *rrv, *rrw, *divx;
+} gm1b_tke_evolution_arrays;
+
+/* turbt: the horizontal TKE flux divergence with the terrain correction
+ * (zero on the outermost columns) and the vertically implicit diffusion,
+ * added into tketen.  Replaces launch_cuda_tke_diffusion
+ * (src/cm1core/cuda_tke_evolution.py:421).  nk <= 201. */
+GM1B_API int32_t gm1b_tke_diffusion(int32_t ni, int32_t nj, int32_t nk, const gm1b_tke_evolution_arrays *arrays,
+                                    float dx, float dy, float dz, float dt, void *stream);
+
+/* One RK stage nrk (1..3) from the stage-start field cur into nxt (distinct
+ * face volumes): fifth-order (WENO5 at nrk = 3) flux-form advection with the
+ * open-side edits and the divergence correction, tkea + dt/(4-nrk) *
+ * tendency, words below 1e-10 set to zero.  Replaces
+ * launch_cuda_tke_rk_stage (src/cm1core/cuda_tke_evolution.py:430). */
+GM1B_API int32_t gm1b_tke_rk_stage(int32_t ni, int32_t nj, int32_t nk, const gm1b_tke_evolution_arrays *arrays,
+                                   const float *cur, float *nxt, int32_t nrk, float dx, float dy, float dz, float dt,
+                                   void *stream);
+
+/* The whole operator: turbt, the three RK stages from tke3d, and the commit
+ * tke3d = tkea = result.  workspace: one face volume.  Replaces
+ * launch_cuda_tke_evolution (src/cm1core/cuda_tke_evolution.py:481) and the
+ * CPU twin cpu_tke_evolution_inplace (:206). */
+GM1B_API int32_t gm1b_tke_evolution(int32_t ni, int32_t nj, int32_t nk, const gm1b_tke_evolution_arrays *arrays,
+                                    float *workspace, float dx, float dy, float dz, float dt, void *stream);
+
+/* ------------------------------------------------------------------------
  * TKE source inputs: deformation and moist N^2 (compact physical arrays)
  * ---------------------------------------------------------------------- */
 

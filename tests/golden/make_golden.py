@@ -646,6 +646,50 @@ def make_closure(reference: Path) -> None:
         print("wrote", tag, meta)
 
 
+def tke_evolution_fixture(ni: int, nj: int, nk: int, seed: int) -> dict[str, np.ndarray]:
+    """Seeded inputs of the terrain-lane TKE evolution: positive TKE and
+    eddy viscosities, a terrain metric, mass fluxes of both signs."""
+    rng = np.random.default_rng(seed)
+    f = np.float32
+    face, mass = (nk + 1, nj, ni), (nk, nj, ni)
+    ng = 3
+    a = {
+        "tke3d": rng.uniform(0.0, 2.0, face).astype(f), "tkea": rng.uniform(0.0, 2.0, face).astype(f),
+        "tketen": rng.normal(0.0, 1e-3, face).astype(f), "kmh": rng.uniform(1.0, 60.0, face).astype(f),
+        "kmv": rng.uniform(1.0, 40.0, face).astype(f), "rho": rng.uniform(0.7, 1.2, mass).astype(f),
+        "rf": rng.uniform(0.7, 1.2, face).astype(f), "mh": rng.uniform(0.9, 1.1, mass).astype(f),
+        "mf": rng.uniform(0.9, 1.1, face).astype(f), "gz": rng.uniform(1.0, 1.05, (nj, ni)).astype(f),
+        "rgzu": rng.uniform(0.95, 1.0, (nj, ni + 1)).astype(f), "rgzv": rng.uniform(0.95, 1.0, (nj + 1, ni)).astype(f),
+        "c1": rng.uniform(0.4, 0.6, face).astype(f), "rrf0": rng.uniform(0.8, 1.4, face).astype(f),
+        "rru": rng.normal(4.0, 8.0, (nk + 2, nj + 2 * ng, ni + 1 + 2 * ng)).astype(f),
+        "rrv": rng.normal(-2.0, 8.0, (nk + 2, nj + 1 + 2 * ng, ni + 2 * ng)).astype(f),
+        "rrw": rng.normal(0.0, 1.5, (nk + 3, nj + 2 * ng, ni + 2 * ng)).astype(f),
+        "divx": rng.normal(0.0, 1e-3, mass).astype(f),
+    }
+    a["rgz"] = (f(1.0) / a["gz"]).astype(f)
+    a["c2"] = (f(1.0) - a["c1"]).astype(f)
+    for k in (0, nk):
+        a["tke3d"][k] = 0.0
+        a["tkea"][k] = 0.0
+    return {n: np.ascontiguousarray(v) for n, v in a.items()}
+
+
+def make_tke_evolution(reference: Path) -> None:
+    """turbt + three TKE RK stages through the reference's CPU twin."""
+    sys.path.insert(0, str(reference / "src"))
+    from cm1core.cuda_tke_evolution import cpu_tke_evolution_inplace
+
+    for tag, (ni, nj, nk, seed) in {"tke_evolution_9x8x10": (9, 8, 10, 71), "tke_evolution_7x10x9": (7, 10, 9, 73)}.items():
+        a = tke_evolution_fixture(ni, nj, nk, seed)
+        inputs = {f"in_{k}": v.copy() for k, v in a.items()}
+        p = {"ni": ni, "nj": nj, "nk": nk, "dx": 250.0, "dy": 300.0, "dz": 200.0, "dt": 3.0}
+        r = cpu_tke_evolution_inplace(a, **p)
+        meta = dict(p, stage_sha256=r["stage_sha256"])
+        np.savez_compressed(HERE / f"{tag}.npz", meta=json.dumps(meta), **inputs,
+                            **{f"out_{k}": a[k] for k in ("tke3d", "tkea", "tketen")})
+        print("wrote", tag)
+
+
 def make_wk(reference: Path) -> None:
     """CM1 r21.1's own Weisman-Klemp base state (isnd=5, nz=40, dz=500 m) as
     float32 words, from the CM1 output the reference keeps
@@ -711,7 +755,7 @@ def make_c1(reference: Path, checkpoints: list[int]) -> None:
 def main() -> None:
     p = argparse.ArgumentParser()
     p.add_argument("--reference", type=Path, required=True, help="root of the reference source tree")
-    p.add_argument("what", choices=("small", "c1", "advection", "kessler", "tke", "rk", "bridge", "wk", "limits", "closure"))
+    p.add_argument("what", choices=("small", "c1", "advection", "kessler", "tke", "rk", "bridge", "wk", "limits", "closure", "tkeevo"))
     p.add_argument("--checkpoints", type=int, nargs="+", default=[1])
     args = p.parse_args()
     if args.what == "small":
@@ -732,6 +776,8 @@ def main() -> None:
         make_limits(args.reference)
     elif args.what == "closure":
         make_closure(args.reference)
+    elif args.what == "tkeevo":
+        make_tke_evolution(args.reference)
     else:
         make_c1(args.reference, sorted(set(args.checkpoints)))
 
