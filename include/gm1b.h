@@ -365,6 +365,43 @@ GM1B_API int32_t gm1b_sgs_tke(int32_t ni, int32_t nj, int32_t nk, const gm1b_sgs
                               float dx, float dy, float dz, void *stream);
 
 /* ------------------------------------------------------------------------
+ * Terrain/open fifth-order momentum advection of the padded lane (shapes as
+ * above; uh (ni+6), vh (nj+6); rho0_3d (nk, nj, ni); rf0, rrf0, c2
+ * (nk+1, nj, ni); gz, dzdx, dzdy (nj, ni); gzu, rgzu (nj, ni+1); gzv, rgzv
+ * (nj+1, ni); divx (nk, nj, ni)).
+ * ---------------------------------------------------------------------- */
+typedef struct gm1b_momentum5_arrays {
+    const float *u3d;
+    float *uten, *rru;
+    const float *v3d;
+    float *vten, *rrv;
+    const float *w3d;
+    float *wten, *rrw;
+    const float *uh, *vh, *rho0_3d, *rf0, *rrf0, *c2, *gz, *gzu, *gzv, *rgzu, *rgzv, *dzdx, *dzdy;
+    float *divx;
+} gm1b_momentum5_arrays;
+
+/* Mass fluxes rru, rrv (every face) and rrw (with the terrain term), the
+ * divergence divx, and the advu / advv / advw increments added into uten,
+ * vten, wten.  lateral_obc packs CM1's (wbc, ebc, sbc, nbc) as
+ * wbc|ebc<<4|sbc<<8|nbc<<12 (1 periodic on both sides of a direction, 2
+ * open, 3/4 walls).  Replaces launch_cuda_terrain_open_momentum_advection5
+ * (src/cm1core/cuda_momentum_advection5.py:1173) and its CPU twin
+ * cpu_terrain_open_momentum_advection5_inplace (:753).  ni, nj >= 7, nk >= 8. */
+GM1B_API int32_t gm1b_momentum_advection5(int32_t ni, int32_t nj, int32_t nk, const gm1b_momentum5_arrays *arrays,
+                                          uint32_t lateral_obc, float dx, float dy, float dz, void *stream);
+
+/* The two halves of gm1b_momentum_advection5, for a caller that edits the
+ * fluxes or divx between them (the reference's post_divergence_hook seam):
+ * the mass fluxes and divx, then the advu / advv / advw increments from the
+ * fluxes and divx already formed (_cpu_momentum_transport5,
+ * src/cm1core/cuda_momentum_advection5.py:871). */
+GM1B_API int32_t gm1b_momentum_mass_flux5(int32_t ni, int32_t nj, int32_t nk, const gm1b_momentum5_arrays *arrays,
+                                          uint32_t lateral_obc, float dx, float dy, float dz, void *stream);
+GM1B_API int32_t gm1b_momentum_transport5(int32_t ni, int32_t nj, int32_t nk, const gm1b_momentum5_arrays *arrays,
+                                          uint32_t lateral_obc, float dx, float dy, float dz, void *stream);
+
+/* ------------------------------------------------------------------------
  * TKE evolution on the terrain lane: turbt and the flux-form RK stages.
  * Face fields (nk+1, nj, ni): tkea, tke3d, tketen, kmh, kmv, rf, mf, c1, c2,
  * rrf0; mass fields (nk, nj, ni): rho, mh, divx; gz, rgz (nj, ni), rgzu

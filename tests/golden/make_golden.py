@@ -690,6 +690,64 @@ def make_tke_evolution(reference: Path) -> None:
         print("wrote", tag)
 
 
+def momentum_fixture(ni: int, nj: int, nk: int, seed: int) -> tuple[dict[str, np.ndarray], dict[str, np.ndarray],
+                                                                    np.ndarray]:
+    """Padded-lane momentum-advection inputs: seeded winds with filled halos,
+    accumulated tendencies, terrain metrics."""
+    rng = np.random.default_rng(seed)
+    f = np.float32
+    ng = 3
+    su, sv, sw = (nk + 2, nj + 2 * ng, ni + 1 + 2 * ng), (nk + 2, nj + 1 + 2 * ng, ni + 2 * ng), \
+        (nk + 3, nj + 2 * ng, ni + 2 * ng)
+    a = {
+        "u3d": rng.normal(6.0, 6.0, su).astype(f), "uten": rng.normal(0.0, 1e-3, su).astype(f),
+        "rru": np.zeros(su, f), "v3d": rng.normal(-2.0, 6.0, sv).astype(f),
+        "vten": rng.normal(0.0, 1e-3, sv).astype(f), "rrv": np.zeros(sv, f),
+        "w3d": rng.normal(0.0, 1.5, sw).astype(f), "wten": rng.normal(0.0, 1e-3, sw).astype(f),
+        "rrw": np.zeros(sw, f), "uh": rng.uniform(0.95, 1.05, ni + 2 * ng).astype(f),
+        "vh": rng.uniform(0.95, 1.05, nj + 2 * ng).astype(f),
+    }
+    face = (nk + 1, nj, ni)
+    m = {
+        "rho0_3d": rng.uniform(0.7, 1.2, (nk, nj, ni)).astype(f), "rf0": rng.uniform(0.7, 1.2, face).astype(f),
+        "c2": rng.uniform(0.4, 0.6, face).astype(f), "gz": rng.uniform(1.0, 1.05, (nj, ni)).astype(f),
+        "gzu": rng.uniform(1.0, 1.05, (nj, ni + 1)).astype(f), "gzv": rng.uniform(1.0, 1.05, (nj + 1, ni)).astype(f),
+        "dzdx": rng.normal(0.0, 0.02, (nj, ni)).astype(f), "dzdy": rng.normal(0.0, 0.02, (nj, ni)).astype(f),
+    }
+    m["rrf0"] = (f(1.0) / m["rf0"]).astype(f)
+    m["rgzu"] = (f(1.0) / m["gzu"]).astype(f)
+    m["rgzv"] = (f(1.0) / m["gzv"]).astype(f)
+    m["c1"] = (f(1.0) - m["c2"]).astype(f)
+    m["rr0"] = (f(1.0) / m["rho0_3d"]).astype(f)
+    return a, m, np.zeros((nk, nj, ni), f)
+
+
+MOMENTUM_CASES = {
+    "momentum5_open_9x8x10": (9, 8, 10, 81, (2, 2, 2, 2)),
+    "momentum5_perx_8x9x9": (8, 9, 9, 83, (1, 1, 2, 2)),
+    "momentum5_walls_10x7x8": (10, 7, 8, 89, (3, 4, 1, 1)),
+}
+
+
+def make_momentum(reference: Path) -> None:
+    """Terrain/open momentum advection through the reference's CPU twin."""
+    sys.path.insert(0, str(reference / "src"))
+    from cm1core.cuda_momentum_advection5 import cpu_terrain_open_momentum_advection5_inplace
+    from cm1core.cuda_terrain_open_boundary import terrain_static_shapes
+
+    for tag, (ni, nj, nk, seed, sides) in MOMENTUM_CASES.items():
+        a, m, divx = momentum_fixture(ni, nj, nk, seed)
+        full = {n: np.zeros(shape, np.float32) for n, shape in terrain_static_shapes(ni=ni, nj=nj, nk=nk).items()}
+        full.update(m)
+        inputs = {f"in_{k}": v.copy() for k, v in {**a, **m}.items()}
+        p = {"ni": ni, "nj": nj, "nk": nk, "dx": 400.0, "dy": 350.0, "dz": 180.0}
+        cpu_terrain_open_momentum_advection5_inplace(a, full, divx, nrk=1, lateral_sides=sides, **p)
+        meta = dict(p, lateral_sides=list(sides))
+        outs = {f"out_{k}": a[k] for k in ("uten", "vten", "wten", "rru", "rrv", "rrw")}
+        np.savez_compressed(HERE / f"{tag}.npz", meta=json.dumps(meta), **inputs, **outs, out_divx=divx)
+        print("wrote", tag)
+
+
 def make_wk(reference: Path) -> None:
     """CM1 r21.1's own Weisman-Klemp base state (isnd=5, nz=40, dz=500 m) as
     float32 words, from the CM1 output the reference keeps
@@ -755,7 +813,7 @@ def make_c1(reference: Path, checkpoints: list[int]) -> None:
 def main() -> None:
     p = argparse.ArgumentParser()
     p.add_argument("--reference", type=Path, required=True, help="root of the reference source tree")
-    p.add_argument("what", choices=("small", "c1", "advection", "kessler", "tke", "rk", "bridge", "wk", "limits", "closure", "tkeevo"))
+    p.add_argument("what", choices=("small", "c1", "advection", "kessler", "tke", "rk", "bridge", "wk", "limits", "closure", "tkeevo", "momentum"))
     p.add_argument("--checkpoints", type=int, nargs="+", default=[1])
     args = p.parse_args()
     if args.what == "small":
@@ -778,6 +836,8 @@ def main() -> None:
         make_closure(args.reference)
     elif args.what == "tkeevo":
         make_tke_evolution(args.reference)
+    elif args.what == "momentum":
+        make_momentum(args.reference)
     else:
         make_c1(args.reference, sorted(set(args.checkpoints)))
 
