@@ -1,0 +1,94 @@
+"""ctypes driver of the terrain/open acoustic-stage oracle
+(terrain_open_oracle.c) - TEST INFRASTRUCTURE ONLY.  Mirrors
+cpu_psolver3_terrain_open_stage_inplace and the three-stage composition
+(src/cm1core/cuda_psolver3_terrain_open.py:774-913)."""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from oracle.periodic import load
+
+_F = ctypes.POINTER(ctypes.c_float)
+ARRAY_NAMES = ("ppi", "pp3d", "ppx", "ppd", "piadv", "ppterm", "ppten", "thv", "qk", "pk1", "pk2", "mm", "fpk",
+               "divh", "hadvp", "dum3", "elim_c", "elim_d", "tri_aa", "tri_bb", "tri_cc", "tri_dd", "tri_pivot",
+               "tri_residual", "ua", "u3d", "uten", "rru", "va", "v3d", "vten", "rrv", "wa", "w3d", "wten", "rrw",
+               "radbcw", "radbce", "radbcs", "radbcn", "uh", "vh", "ruf", "rvf", "scalar")
+METRIC_NAMES = ("rho0_3d", "rr0", "rf0", "rrf0", "c1", "c2", "gz", "rgzu", "rgzv", "dzdx", "dzdy", "gx", "gxu", "gy",
+                "gyv")
+ABLATION_BITS = {"open_consumption": 1, "terrain_pressure_gradient": 2, "transformed_divergence": 4,
+                 "pressure_advection": 8, "implicit_vertical_solve": 16, "between_step_pressure_fill": 32,
+                 "radiation_history_production": 64, "stage_family_fills": 128}
+ALL_ABLATIONS = 255
+
+
+class TosArrays(ctypes.Structure):
+    _fields_ = [(n, _F) for n in ARRAY_NAMES]
+
+
+class TosMetrics(ctypes.Structure):
+    _fields_ = [(n, _F) for n in METRIC_NAMES]
+
+
+@dataclass(frozen=True)
+class StageDiagnostics:
+    nrk: int
+    nloop: int
+    dts_f32: float
+    max_tridiagonal_residual: float
+
+
+def _lib():
+    lib = load()
+    if not getattr(lib, "_tos_ready", False):
+        c = ctypes
+        lib.oracle_terrain_open_stage.argtypes = [c.POINTER(TosArrays), c.POINTER(TosMetrics)] + [c.c_int] * 4 + \
+            [c.c_float, c.c_int, c.c_float, c.c_float, c.c_double, c.c_float, c.c_float, c.c_uint, c.POINTER(c.c_float)]
+        lib.oracle_terrain_open_stage.restype = c.c_int
+        lib.oracle_terrain_edge_weights.argtypes = [c.c_int, c.c_float, c.POINTER(c.c_float), c.POINTER(c.c_float)]
+        lib.oracle_terrain_edge_weights.restype = None
+        lib._tos_ready = True
+    return lib
+
+
+def _bind(struct_type, names, d):
+    s = struct_type()
+    for n in names:
+        v = d[n]
+        assert v.dtype == np.float32 and v.flags.c_contiguous, n
+        setattr(s, n, v.ctypes.data_as(_F))
+    return s
+
+
+def terrain_open_stage(a, m, *, ni, nj, nk, nrk, dt, nsound, dx, dy, dz, alph=0.6, kdiv=0.1,
+                       ablations=ALL_ABLATIONS) -> StageDiagnostics:
+    sa, sm = _bind(TosArrays, ARRAY_NAMES, a), _bind(TosMetrics, METRIC_NAMES, m)
+    diag = (ctypes.c_float * 3)()
+    rc = _lib().oracle_terrain_open_stage(ctypes.byref(sa), ctypes.byref(sm), ni, nj, nk, nrk, dt, nsound, dx, dy,
+                                         float(dz), alph, kdiv, ablations, diag)
+    if rc != 0:
+        raise ValueError(f"oracle_terrain_open_stage failed ({rc})")
+    return StageDiagnostics(nrk, int(diag[0]), float(diag[1]), float(diag[2]))
+
+
+def terrain_open_three_stage(a, m, **kw) -> tuple[StageDiagnostics, ...]:
+    return tuple(terrain_open_stage(a, m, nrk=nrk, **kw) for nrk in (1, 2, 3))
+
+
+def edge_weights(nk: int, dz: float) -> tuple[tuple[float, ...], tuple[float, ...]]:
+    cgs, cgt = (ctypes.c_float * 3)(), (ctypes.c_float * 3)()
+    _lib().oracle_terrain_edge_weights(nk, dz, cgs, cgt)
+    return tuple(cgs), tuple(cgt)
+
+
+def ablation_mask(**disabled: bool) -> int:
+    """Mask of enabled terrain/open phases; keywords name a disabled phase
+    (``open_consumption=False`` etc.), as TerrainOpenSoundAblations does."""
+    mask = ALL_ABLATIONS
+    for name, enabled in disabled.items():
+        if not enabled:
+            mask &= ~ABLATION_BITS[name]
+    return mask

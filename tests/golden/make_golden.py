@@ -748,6 +748,141 @@ def make_momentum(reference: Path) -> None:
         print("wrote", tag)
 
 
+TERRAIN_OPEN_ARRAYS = ("ppi", "pp3d", "ppx", "ppd", "piadv", "ppterm", "ppten", "thv", "qk", "pk1", "pk2", "mm",
+                       "fpk", "divh", "hadvp", "dum3", "elim_c", "elim_d", "tri_aa", "tri_bb", "tri_cc", "tri_dd",
+                       "tri_pivot", "tri_residual", "ua", "u3d", "uten", "rru", "va", "v3d", "vten", "rrv", "wa",
+                       "w3d", "wten", "rrw", "radbcw", "radbce", "radbcs", "radbcn", "uh", "vh", "ruf", "rvf",
+                       "scalar")
+
+
+def terrain_open_fixture(ni: int, nj: int, nk: int, seed: int) -> tuple[dict[str, np.ndarray],
+                                                                       dict[str, np.ndarray]]:
+    """Seeded terrain/open acoustic-stage inputs: winds, pressure family and
+    radiation histories with random halos, garbage in every scratch array
+    (the stage must overwrite or zero it), and the 25 terrain metrics with a
+    non-broadcast base density."""
+    rng = np.random.default_rng(seed)
+    f = np.float32
+    ng = 3
+    pr, su, sv = (nk + 2, nj + 2, ni + 2), (nk + 2, nj + 2 * ng, ni + 1 + 2 * ng), (nk + 2, nj + 1 + 2 * ng, ni + 2 * ng)
+    sw, ss = (nk + 3, nj + 2 * ng, ni + 2 * ng), (nk + 2, nj + 2 * ng, ni + 2 * ng)
+    a: dict[str, np.ndarray] = {}
+    for n in TERRAIN_OPEN_ARRAYS[:24]:
+        a[n] = rng.normal(0.0, 0.5, pr).astype(f)
+    pert = rng.normal(0.0, 2e-4, pr).astype(f)
+    a["ppi"] = pert.copy()
+    a["pp3d"] = (pert + rng.normal(0.0, 2e-5, pr)).astype(f)
+    a["ppx"] = (pert + rng.normal(0.0, 2e-5, pr)).astype(f)
+    a["piadv"] = (f(0.9) + rng.normal(0.0, 2e-3, pr)).astype(f)
+    a["ppterm"] = (a["piadv"] * f(287.04 / (1005.7 - 287.04))).astype(f)
+    a["thv"] = (f(300.0) + np.arange(nk + 2, dtype=f)[:, None, None] * f(0.4) + rng.normal(0.0, 0.3, pr)).astype(f)
+    a["ppten"] = rng.normal(0.0, 1e-6, pr).astype(f)
+    a["u3d"] = rng.normal(8.0, 3.0, su).astype(f)
+    a["ua"] = (a["u3d"] + rng.normal(0.0, 0.05, su)).astype(f)
+    a["uten"] = rng.normal(0.0, 2e-3, su).astype(f)
+    a["rru"] = rng.normal(0.0, 1.0, su).astype(f)
+    a["v3d"] = rng.normal(-3.0, 3.0, sv).astype(f)
+    a["va"] = (a["v3d"] + rng.normal(0.0, 0.05, sv)).astype(f)
+    a["vten"] = rng.normal(0.0, 2e-3, sv).astype(f)
+    a["rrv"] = rng.normal(0.0, 1.0, sv).astype(f)
+    a["w3d"] = rng.normal(0.0, 0.5, sw).astype(f)
+    a["wa"] = (a["w3d"] + rng.normal(0.0, 0.02, sw)).astype(f)
+    a["wten"] = rng.normal(0.0, 2e-3, sw).astype(f)
+    a["rrw"] = rng.normal(0.0, 1.0, sw).astype(f)
+    a["radbcw"] = rng.uniform(-25.0, 0.0, (nk + 2, nj + 2 * ng)).astype(f)
+    a["radbce"] = rng.uniform(0.0, 25.0, (nk + 2, nj + 2 * ng)).astype(f)
+    a["radbcs"] = rng.uniform(-25.0, 0.0, (nk + 2, ni + 2 * ng)).astype(f)
+    a["radbcn"] = rng.uniform(0.0, 25.0, (nk + 2, ni + 2 * ng)).astype(f)
+    a["uh"] = np.ones(ni + 2 * ng, f)
+    a["vh"] = np.ones(nj + 2 * ng, f)
+    a["ruf"] = np.ones(ni + 1 + 2 * ng, f)
+    a["rvf"] = np.ones(nj + 1 + 2 * ng, f)
+    a["scalar"] = rng.normal(1.0, 0.2, ss).astype(f)
+    mass, face, plane = (nk, nj, ni), (nk + 1, nj, ni), (nj, ni)
+    m: dict[str, np.ndarray] = {}
+    terrain = rng.uniform(0.0, 400.0, plane).astype(f)
+    m["terrain_msl"] = terrain
+    m["zh"] = rng.uniform(100.0, 9000.0, mass).astype(f)
+    m["zf"] = rng.uniform(0.0, 9000.0, face).astype(f)
+    for n, shape in (("mh", mass), ("mf", face)):
+        m[n] = rng.uniform(0.95, 1.05, shape).astype(f)
+        m["r" + n] = (f(1.0) / m[n]).astype(f)
+    m["c1"] = rng.uniform(0.4, 0.6, face).astype(f)
+    m["c2"] = (f(1.0) - m["c1"]).astype(f)
+    base = np.linspace(1.15, 0.6, nk, dtype=f)
+    m["rho0_3d"] = (base[:, None, None] * rng.uniform(0.98, 1.02, mass)).astype(f)
+    m["rr0"] = (f(1.0) / m["rho0_3d"]).astype(f)
+    m["rf0"] = (np.linspace(1.18, 0.58, nk + 1, dtype=f)[:, None, None] * rng.uniform(0.98, 1.02, face)).astype(f)
+    m["rrf0"] = (f(1.0) / m["rf0"]).astype(f)
+    for n, shape in (("gz", plane), ("gzu", (nj, ni + 1)), ("gzv", (nj + 1, ni))):
+        m[n] = rng.uniform(1.0, 1.06, shape).astype(f)
+    m["rgz"] = (f(1.0) / m["gz"]).astype(f)
+    m["rgzu"] = (f(1.0) / m["gzu"]).astype(f)
+    m["rgzv"] = (f(1.0) / m["gzv"]).astype(f)
+    m["dzdx"] = rng.normal(0.0, 0.02, plane).astype(f)
+    m["dzdy"] = rng.normal(0.0, 0.02, plane).astype(f)
+    m["gx"] = rng.normal(0.0, 0.005, face).astype(f)
+    m["gxu"] = rng.normal(0.0, 0.005, (nk + 1, nj, ni + 1)).astype(f)
+    m["gy"] = rng.normal(0.0, 0.005, face).astype(f)
+    m["gyv"] = rng.normal(0.0, 0.005, (nk + 1, nj + 1, ni)).astype(f)
+    return a, m
+
+
+TERRAIN_OPEN_CASES = {
+    # name: (ni, nj, nk, seed, dt, nsound, dx, dy, dz)
+    "tos_seeded_9x7x8": (9, 7, 8, 97, 3.0, 6, 500.0, 400.0, 333.3),
+    "tos_seeded_6x10x6": (6, 10, 6, 101, 2.4, 8, 300.0, 350.0, 180.0),
+}
+TERRAIN_OPEN_ABLATIONS = ("open_consumption", "terrain_pressure_gradient", "transformed_divergence",
+                          "pressure_advection", "implicit_vertical_solve", "between_step_pressure_fill",
+                          "radiation_history_production", "stage_family_fills")
+
+
+def make_terrain_open(reference: Path) -> None:
+    """The terrain/open acoustic stage through the reference's CPU twin:
+    the reference test's own 5x4x5 inputs and two seeded cases over three RK
+    stages (full arrays and per-stage digests of every array), each of the
+    eight ablations, and non-default alph/kdiv."""
+    sys.path.insert(0, str(reference / "src"))
+    sys.path.insert(0, str(reference / "tests"))
+    from cm1core.cuda_psolver3_terrain_open import TerrainOpenSoundAblations, cpu_psolver3_terrain_open_stage_inplace
+    import test_cuda_psolver3_terrain_open as reftest
+
+    def run(a, m, p, *, ablations=None, alph=None, kdiv=None):
+        stages = []
+        for nrk in (1, 2, 3):
+            d = cpu_psolver3_terrain_open_stage_inplace(a, m, nrk=nrk, ablations=ablations, alph=alph, kdiv=kdiv, **p)
+            stages.append({"nrk": nrk, "nloop": d.nloop, "dts_f32": d.dts_f32,
+                           "max_tridiagonal_residual": d.max_tridiagonal_residual,
+                           "digests": {n: digest(a[n]) for n in TERRAIN_OPEN_ARRAYS}})
+        return stages
+
+    cases = {"tos_reftest_5x4x5": (reftest._arrays(5, 4, 5), reftest._metrics(5, 4, 5),
+                                   dict(ni=5, nj=4, nk=5, dt=0.6, nsound=6, dx=100.0, dy=100.0, dz=200.0))}
+    for tag, (ni, nj, nk, seed, dt, nsound, dx, dy, dz) in TERRAIN_OPEN_CASES.items():
+        a, m = terrain_open_fixture(ni, nj, nk, seed)
+        cases[tag] = (a, m, dict(ni=ni, nj=nj, nk=nk, dt=dt, nsound=nsound, dx=dx, dy=dy, dz=dz))
+    for tag, (a, m, p) in cases.items():
+        inputs = {f"in_{k}": v.copy() for k, v in a.items()}
+        minputs = {f"metric_{k}": v for k, v in m.items()}
+        t0 = time.time()
+        stages = run(a, m, p)
+        meta = dict(p, stages=stages)
+        if tag == "tos_reftest_5x4x5":
+            abl = {}
+            for name in TERRAIN_OPEN_ABLATIONS:
+                b = {k[3:]: v.copy() for k, v in inputs.items()}
+                run(b, m, p, ablations=TerrainOpenSoundAblations(**{name: False}))
+                abl[name] = {n: digest(b[n]) for n in TERRAIN_OPEN_ARRAYS}
+            meta["ablations"] = abl
+        if tag == "tos_seeded_9x7x8":
+            b = {k[3:]: v.copy() for k, v in inputs.items()}
+            meta["alph_kdiv"] = {"alph": 0.5, "kdiv": 0.05, "stages": run(b, m, p, alph=0.5, kdiv=0.05)}
+        outs = {f"out_{k}": a[k] for k in TERRAIN_OPEN_ARRAYS}
+        np.savez_compressed(HERE / f"{tag}.npz", meta=json.dumps(meta), **inputs, **minputs, **outs)
+        print("wrote", tag, round(time.time() - t0, 1), "s", flush=True)
+
+
 def make_wk(reference: Path) -> None:
     """CM1 r21.1's own Weisman-Klemp base state (isnd=5, nz=40, dz=500 m) as
     float32 words, from the CM1 output the reference keeps
@@ -813,7 +948,7 @@ def make_c1(reference: Path, checkpoints: list[int]) -> None:
 def main() -> None:
     p = argparse.ArgumentParser()
     p.add_argument("--reference", type=Path, required=True, help="root of the reference source tree")
-    p.add_argument("what", choices=("small", "c1", "advection", "kessler", "tke", "rk", "bridge", "wk", "limits", "closure", "tkeevo", "momentum"))
+    p.add_argument("what", choices=("small", "c1", "advection", "kessler", "tke", "rk", "bridge", "wk", "limits", "closure", "tkeevo", "momentum", "terrainopen"))
     p.add_argument("--checkpoints", type=int, nargs="+", default=[1])
     args = p.parse_args()
     if args.what == "small":
@@ -838,6 +973,8 @@ def main() -> None:
         make_tke_evolution(args.reference)
     elif args.what == "momentum":
         make_momentum(args.reference)
+    elif args.what == "terrainopen":
+        make_terrain_open(args.reference)
     else:
         make_c1(args.reference, sorted(set(args.checkpoints)))
 
