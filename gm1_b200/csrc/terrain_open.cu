@@ -1,0 +1,923 @@
+// terrain_open.cu - sm_100a kernels of the terrain + all-open psolver=3
+// acoustic RK stage on the padded (ng = 3) lane.
+//
+// Behaviour followed (reference file:line):
+//   cpu_psolver3_terrain_open_stage_inplace   src/cm1core/cuda_psolver3_terrain_open.py:774-894
+//     (_prepare_coefficients :300, _terrain_pressure_gradient :393,
+//      _transformed_velocity_terms :482, _initial_fpk :544,
+//      _pressure_advection :595, _implicit_and_pressure_update :678,
+//      _average_velocities :748)
+//   cpu_ssopen_terrain_all_inplace, _interp_u_at_w, cpu_bcwsfc_terrain_physical_inplace
+//                                             src/cm1core/cuda_terrain_open_boundary.py:666-850
+//   terrain_coordinate_profiles (uniform)     :486-560
+//   cpu_bc{p,s,u,v,w}_open_inplace            src/cm1core/cuda_sound3_open_boundary.py:249-335
+//   cpu_radiation4_inplace                    src/cm1core/cuda_lateral_closure.py:390-472
+//
+// Design (B200).  Per stage: one prepare pass.  Per small step: three
+// launches - (1) the four open edges (a CTA per boundary line snapshots both
+// w-level interpolations of its two face columns in shared memory, then
+// advances every level at once), (2) the terrain pressure gradient on the
+// interior faces (a 32x4 tile marching up the column, each vertical ppd
+// difference formed once), (3) one column pass per 32 columns of a row that
+// keeps the whole column in shared memory: transformed divergence, surface
+// w, pi' advection and fpk, the tridiagonal coefficients, the Thomas sweep,
+// the pi' update with the kdiv filter, the ppd halo copy between small steps
+// and the rru/rrv/rrw averages (the reference takes eight launches and
+// global elimination scratch for the same small step).  After the last small
+// step: the radiation histories (one warp per boundary line, the column sum
+// in level order) and the stage fills in two ordered passes (the first
+// direction of every fill, then the second).  Scratch arrays are written only
+// at the last small step, and only under GM1B_TOS_DIAGNOSTICS: their final
+// words are the CPU twin's.  The vertical coordinate is formed in-kernel with
+// the twin's own float32 operations.  Binary32 one operation at a time in the
+// reference's order: word-identical.
+#include "gm1b_common.cuh"
+
+namespace gm1b {
+namespace {
+
+constexpr int kTosWarps = 8;     // k-parallel warps of the column pass
+constexpr int kTosMaxNk = 140;   // column pass keeps 12 words per level per column in shared memory
+constexpr int kTosArrays = 12;
+
+struct TosArgs {
+    gm1b_terrain_open_arrays a;
+    gm1b_terrain_metrics m;
+    int ni, nj, nk, nrk, n, nloop;
+    unsigned abl, diag;
+    float dts, rdx, rdy, dz, alph, beta, asq, kdiv, temx, temy, tavg, zt, rzt, halfcp;
+    float cgs[3], cgt[3];
+};
+
+struct Ix {
+    int ni, nj;
+    __device__ __forceinline__ size_t p(int k, int j, int i) const {
+        return ((size_t)k * (nj + 2) + j) * (size_t)(ni + 2) + i;
+    }
+    __device__ __forceinline__ size_t u(int k, int y, int x) const {
+        return ((size_t)k * (nj + 6) + y) * (size_t)(ni + 7) + x;
+    }
+    __device__ __forceinline__ size_t v(int k, int y, int x) const {
+        return ((size_t)k * (nj + 7) + y) * (size_t)(ni + 6) + x;
+    }
+    __device__ __forceinline__ size_t w(int k, int y, int x) const {
+        return ((size_t)k * (nj + 6) + y) * (size_t)(ni + 6) + x;
+    }
+    __device__ __forceinline__ size_t m(int k0, int j0, int i0) const {
+        return ((size_t)k0 * nj + j0) * (size_t)ni + i0;
+    }
+    __device__ __forceinline__ size_t h(int j0, int i0) const { return (size_t)j0 * ni + i0; }
+};
+
+// uniform terrain coordinate, the twin's float32 words (terrain_coordinate_profiles)
+__device__ __forceinline__ float sig(int k, float dz) { return ((float)k - 0.5f) * dz; }
+__device__ __forceinline__ float sigf(int k, float dz) { return (float)(k - 1) * dz; }
+__device__ __forceinline__ float rds(int k, float dz) { return 1.0f / (sig(k, dz) - sig(k - 1, dz)); }
+__device__ __forceinline__ float rdsf(int k, float dz) { return 1.0f / (sigf(k + 1, dz) - sigf(k, dz)); }
+
+// numpy.minimum / numpy.maximum: NaN propagates, a tie returns the second
+__device__ __forceinline__ float np_min(float a, float b) { return a != a ? a : (b != b ? b : (a < b ? a : b)); }
+__device__ __forceinline__ float np_max(float a, float b) { return a != a ? a : (b != b ? b : (a > b ? a : b)); }
+
+// ---------------------------------------------------------------------------
+// stage start: coefficients, carriers, accumulators (and scratch zeroing)
+// one thread per (k = 1..nk, j = 0..nj+1, i = 0..ni+1)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) tos_prepare_kernel(TosArgs p) {
+    const Ix X{p.ni, p.nj};
+    const int ni = p.ni, nj = p.nj, nk = p.nk;
+    const size_t plane = (size_t)(nj + 2) * (ni + 2), total = plane * nk;
+    const gm1b_terrain_open_arrays &a = p.a;
+    const gm1b_terrain_metrics &m = p.m;
+    for (size_t z = (size_t)blockIdx.x * blockDim.x + threadIdx.x; z < total; z += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(z % (ni + 2));
+        const int j = (int)((z / (ni + 2)) % (nj + 2));
+        const int k = (int)(z / plane) + 1;
+        const size_t c = X.p(k, j, i);
+        a.ppd[c] = a.ppx[c];
+        if (p.nrk != 1) a.pp3d[c] = a.ppi[c];
+        const int y = j + 2, x = i + 2;
+        const size_t qu = X.u(k, y, x), qv = X.v(k, y, x), qw = X.w(k, y, x);
+        a.rru[qu] = 0.0f;
+        a.rrv[qv] = 0.0f;
+        a.rrw[qw] = a.wa[qw] * p.beta;
+        if (p.nrk != 1) {
+            a.u3d[qu] = a.ua[qu];
+            a.v3d[qv] = a.va[qv];
+            a.w3d[qw] = a.wa[qw];
+        }
+        const bool phys = j >= 1 && j <= nj && i >= 1 && i <= ni;
+        if (phys) {
+            const int j0 = j - 1, i0 = i - 1;
+            const float gz = m.gz[X.h(j0, i0)];
+            const float tem = p.dts * rdsf(k, p.dz);
+            a.qk[c] = (tem * a.ppterm[c]) * gz;
+            const float tem2 = ((p.dts * gz) * rdsf(k, p.dz)) * m.rr0[X.m(k - 1, j0, i0)];
+            const float pc = a.piadv[c];
+            const float b2 = (-m.c2[X.m(k, j0, i0)]) * a.piadv[X.p(k + 1, j, i)] + (1.0f - m.c1[X.m(k, j0, i0)]) * pc;
+            const float b1 = m.c1[X.m(k - 1, j0, i0)] * a.piadv[X.p(k - 1, j, i)] + (m.c2[X.m(k - 1, j0, i0)] - 1.0f) * pc;
+            a.pk2[c] = k == nk ? 0.0f : (tem2 * m.rf0[X.m(k, j0, i0)]) * b2;
+            a.pk1[c] = k == 1 ? 0.0f : (tem2 * m.rf0[X.m(k - 1, j0, i0)]) * b1;
+            float mmv = 0.0f;
+            if (k >= 2) {
+                const float tem1 = (p.dts * rds(k, p.dz)) * 1005.7f;
+                const float th = m.c2[X.m(k - 1, j0, i0)] * a.thv[c] + m.c1[X.m(k - 1, j0, i0)] * a.thv[X.p(k - 1, j, i)];
+                mmv = (tem1 * th) * gz;
+            }
+            if (k >= 2 || p.diag) a.mm[c] = mmv;
+        }
+        if (p.diag) {
+            float *zero[] = {a.fpk, a.divh, a.hadvp, a.dum3, a.elim_c, a.elim_d, a.tri_aa, a.tri_bb, a.tri_cc,
+                             a.tri_dd, a.tri_pivot, a.tri_residual, a.qk, a.pk1, a.pk2, a.mm};
+            const int nz = phys ? 12 : 16;  // the coefficients of a live cell were just written
+#pragma unroll 1
+            for (int q = 0; q < nz; ++q) zero[q][c] = 0.0f;
+            if (k == 1 || k == nk) {
+                const size_t e = X.p(k == 1 ? 0 : nk + 1, j, i);
+#pragma unroll 1
+                for (int q = 0; q < 16; ++q) zero[q][e] = 0.0f;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// open-side normal velocity (ssopenbc*): one CTA per boundary line
+// lines: [0, nj) west, [nj, 2nj) east, [2nj, 2nj+ni) south, [.., 2nj+2ni) north
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) tos_edge_kernel(TosArgs p) {
+    extern __shared__ float sh[];
+    const Ix X{p.ni, p.nj};
+    const int ni = p.ni, nj = p.nj, nk = p.nk, L = nk + 2;
+    float *q0 = sh, *q1 = sh + L, *s0 = sh + 2 * L, *s1 = sh + 3 * L;
+    const gm1b_terrain_open_arrays &a = p.a;
+    const gm1b_terrain_metrics &m = p.m;
+    int line = blockIdx.x, side;
+    if (line < nj) side = 0;
+    else if (line < 2 * nj) side = 1, line -= nj;
+    else if (line < 2 * nj + ni) side = 2, line -= 2 * nj;
+    else side = 3, line -= 2 * nj + ni;
+    const bool ew = side < 2;
+    // face columns: q0 at (y0, x0), q1 at (y1, x1); the updated one is q0
+    // on the west/south side and q1 on the east/north side
+    int y0, x0, y1, x1;
+    if (side == 0) y0 = y1 = line + 3, x0 = 3, x1 = 4;
+    else if (side == 1) y0 = y1 = line + 3, x0 = ni + 2, x1 = ni + 3;
+    else if (side == 2) x0 = x1 = line + 3, y0 = 3, y1 = 4;
+    else x0 = x1 = line + 3, y0 = nj + 2, y1 = nj + 3;
+    const float *q = ew ? a.u3d : a.v3d;
+    for (int k = 1 + threadIdx.x; k <= nk; k += blockDim.x) {
+        q0[k] = q[ew ? X.u(k, y0, x0) : X.v(k, y0, x0)];
+        q1[k] = q[ew ? X.u(k, y1, x1) : X.v(k, y1, x1)];
+    }
+    __syncthreads();
+    for (int kf = 1 + threadIdx.x; kf <= nk + 1; kf += blockDim.x) {
+        float r0, r1v;
+        if (kf == 1) {
+            r0 = (p.cgs[0] * q0[1] + p.cgs[1] * q0[2]) + p.cgs[2] * q0[3];
+            r1v = (p.cgs[0] * q1[1] + p.cgs[1] * q1[2]) + p.cgs[2] * q1[3];
+        } else if (kf == nk + 1) {
+            r0 = (p.cgt[0] * q0[nk] + p.cgt[1] * q0[nk - 1]) + p.cgt[2] * q0[nk - 2];
+            r1v = (p.cgt[0] * q1[nk] + p.cgt[1] * q1[nk - 1]) + p.cgt[2] * q1[nk - 2];
+        } else {
+            const float r2 = (sigf(kf, p.dz) - sig(kf - 1, p.dz)) * rds(kf, p.dz);
+            const float r1 = 1.0f - r2;
+            r0 = r1 * q0[kf - 1] + r2 * q0[kf];
+            r1v = r1 * q1[kf - 1] + r2 * q1[kf];
+        }
+        s0[kf] = r0;
+        s1[kf] = r1v;
+    }
+    __syncthreads();
+    const int j0 = ew ? line : (side == 2 ? 0 : nj - 1);   // metric row of the edge cell
+    const int i0 = ew ? (side == 0 ? 0 : ni - 1) : line;   // metric column of the edge cell
+    const float gz = m.gz[X.h(j0, i0)];
+    float rg0, rg1, hmet, rd;
+    const float *gmet;
+    const float *rad;
+    const float *ten;
+    if (side == 0) rg0 = m.rgzu[(size_t)j0 * (ni + 1)], rg1 = m.rgzu[(size_t)j0 * (ni + 1) + 1], hmet = a.uh[3];
+    else if (side == 1) rg0 = m.rgzu[(size_t)j0 * (ni + 1) + ni - 1], rg1 = m.rgzu[(size_t)j0 * (ni + 1) + ni], hmet = a.uh[ni + 2];
+    else if (side == 2) rg0 = m.rgzv[i0], rg1 = m.rgzv[(size_t)ni + i0], hmet = a.vh[3];
+    else rg0 = m.rgzv[(size_t)(nj - 1) * ni + i0], rg1 = m.rgzv[(size_t)nj * ni + i0], hmet = a.vh[nj + 2];
+    rd = ew ? p.rdx : p.rdy;
+    gmet = ew ? m.gx : m.gy;
+    rad = side == 0 ? a.radbcw : side == 1 ? a.radbce : side == 2 ? a.radbcs : a.radbcn;
+    ten = ew ? a.uten : a.vten;
+    const bool upd0 = side == 0 || side == 2;
+    const int yu = upd0 ? y0 : y1, xu = upd0 ? x0 : x1;
+    const size_t radstride = ew ? (size_t)(nj + 6) : (size_t)(ni + 6);
+    const int radpos = ew ? yu : xu;
+    float *qout = ew ? a.u3d : a.v3d;
+    for (int k = 1 + threadIdx.x; k <= nk; k += blockDim.x) {
+        float hz = gz * (q1[k] * rg1 - q0[k] * rg0);
+        hz = (hz * rd) * hmet;
+        float vt = gmet[X.m(k, j0, i0)] * (s1[k + 1] + s0[k + 1]) - gmet[X.m(k - 1, j0, i0)] * (s1[k] + s0[k]);
+        vt = (0.5f * vt) * rdsf(k, p.dz);
+        const float r = (-rad[(size_t)k * radstride + radpos]) * (hz + vt);
+        const size_t o = ew ? X.u(k, yu, xu) : X.v(k, yu, xu);
+        const float tnd = r + ten[o];
+        qout[o] = (upd0 ? q0[k] : q1[k]) + p.dts * tnd;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// terrain pressure gradient on the interior faces (u faces 2..ni of the
+// physical rows, v faces 2..nj of the physical columns).  One thread per
+// pressure point (j, i), j = 0..nj+1, i = 0..ni+1, marching k = 1..nk with
+// the vertical ppd differences of its own, west and south points carried in
+// registers.  Under diagnostics with the pi' advection ablated, the last
+// small step leaves those differences in hadvp, as the twin does.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) tos_pgrad_kernel(TosArgs p) {
+    const Ix X{p.ni, p.nj};
+    const int ni = p.ni, nj = p.nj, nk = p.nk;
+    const int i = blockIdx.x * 32 + threadIdx.x;
+    const int j = blockIdx.y * 4 + threadIdx.y;
+    if (i > ni + 1 || j > nj + 1) return;
+    const gm1b_terrain_open_arrays &a = p.a;
+    const gm1b_terrain_metrics &m = p.m;
+    const bool du = j >= 1 && j <= nj && i >= 2 && i <= ni;
+    const bool dv = j >= 2 && j <= nj && i >= 1 && i <= ni;
+    const bool dh = p.diag && p.n == p.nloop && !(p.abl & GM1B_TOS_PRESSURE_ADVECTION);
+    if (!du && !dv && !dh) return;
+    const int iw = du ? i - 1 : i, js = dv ? j - 1 : j;   // neighbour points (own point when unused)
+    float pc = a.ppd[X.p(1, j, i)], pw = a.ppd[X.p(1, j, iw)], ps = a.ppd[X.p(1, js, i)];
+    float vc = 0.0f, vw = 0.0f, vs = 0.0f;  // vertical difference at level k (zero at k = 1)
+    float gxu_lo = du ? m.gxu[((size_t)0 * nj + (j - 1)) * (ni + 1) + (i - 1)] : 0.0f;
+    float gyv_lo = dv ? m.gyv[((size_t)0 * (nj + 1) + (j - 1)) * ni + (i - 1)] : 0.0f;
+    for (int k = 1; k <= nk; ++k) {
+        float vc1 = 0.0f, vw1 = 0.0f, vs1 = 0.0f, pc1 = 0.0f, pw1 = 0.0f, ps1 = 0.0f;
+        if (k < nk) {
+            const float r = rds(k + 1, p.dz);
+            pc1 = a.ppd[X.p(k + 1, j, i)];
+            pw1 = a.ppd[X.p(k + 1, j, iw)];
+            ps1 = a.ppd[X.p(k + 1, js, i)];
+            vc1 = (pc1 - pc) * r;
+            vw1 = (pw1 - pw) * r;
+            vs1 = (ps1 - ps) * r;
+        }
+        if (dh && k >= 2) a.hadvp[X.p(k, j, i)] = vc;
+        if (du) {
+            const float gxu_hi = m.gxu[((size_t)k * nj + (j - 1)) * (ni + 1) + (i - 1)];
+            const float th = a.thv[X.p(k, j, i)] + a.thv[X.p(k, j, iw)];
+            const float hz = (pc - pw) * p.rdx;
+            const float vsum = (vc1 + vw1) + (vc + vw);
+            const float tr = (0.125f * vsum) * (gxu_lo + gxu_hi);
+            const float pg = (p.halfcp * th) * (hz + tr);
+            const size_t o = X.u(k, j + 2, i + 2);
+            a.u3d[o] = a.u3d[o] + p.dts * (a.uten[o] - pg);
+            gxu_lo = gxu_hi;
+        }
+        if (dv) {
+            const float gyv_hi = m.gyv[((size_t)k * (nj + 1) + (j - 1)) * ni + (i - 1)];
+            const float th = a.thv[X.p(k, j, i)] + a.thv[X.p(k, js, i)];
+            const float hz = (pc - ps) * p.rdy;
+            const float vsum = (vc1 + vs1) + (vc + vs);
+            const float tr = (0.125f * vsum) * (gyv_lo + gyv_hi);
+            const float pg = (p.halfcp * th) * (hz + tr);
+            const size_t o = X.v(k, j + 2, i + 2);
+            a.v3d[o] = a.v3d[o] + p.dts * (a.vten[o] - pg);
+            gyv_lo = gyv_hi;
+        }
+        pc = pc1, pw = pw1, ps = ps1;
+        vc = vc1, vw = vw1, vs = vs1;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// column pass of one small step.  CTA = 32 consecutive columns of row j,
+// kTosWarps warps sharing the levels.  Shared memory holds, per level and
+// column: the four transformed face velocities (later aa, bb, cc/ec, dd),
+// w, dum3 (later ed), the pi' advection term hadvp, fpk, pk1+qk, pk2-qk, mm
+// and pp3d.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(32 * kTosWarps, 1) tos_column_kernel(TosArgs p) {
+    extern __shared__ float sh[];
+    const Ix X{p.ni, p.nj};
+    const int ni = p.ni, nj = p.nj, nk = p.nk, L = nk + 2;
+    const int lane = threadIdx.x, wy = threadIdx.y;
+    const int i = blockIdx.x * 32 + lane + 1;
+    const int j = blockIdx.y + 1;
+    const bool live = i <= ni;
+    const int i0 = i - 1, j0 = j - 1, y = j + 2, x = i + 2;
+    const gm1b_terrain_open_arrays &a = p.a;
+    const gm1b_terrain_metrics &m = p.m;
+    const bool last = p.n == p.nloop;
+    const bool dlast = p.diag && last;
+    const bool do_div = p.abl & GM1B_TOS_TRANSFORMED_DIVERGENCE;
+    const bool do_adv = p.abl & GM1B_TOS_PRESSURE_ADVECTION;
+    const bool do_imp = p.abl & GM1B_TOS_IMPLICIT_SOLVE;
+    float *s_xw = sh, *s_xe = s_xw + L * 32, *s_ys = s_xe + L * 32, *s_yn = s_ys + L * 32;
+    float *s_w = s_yn + L * 32, *s_d3 = s_w + L * 32, *s_ha = s_d3 + L * 32, *s_fpk = s_ha + L * 32;
+    float *s_a1 = s_fpk + L * 32, *s_a2 = s_a1 + L * 32, *s_mm = s_a2 + L * 32, *s_pp = s_mm + L * 32;
+    float *s_aa = s_xw, *s_bb = s_xe, *s_cc = s_ys, *s_dd = s_yn, *s_ed = s_d3;
+#define SM(arr, k) arr[(k) * 32 + lane]
+    float gz = 0.0f, dzdx = 0.0f, dzdy = 0.0f;
+    if (live) {
+        gz = m.gz[X.h(j0, i0)];
+        dzdx = m.dzdx[X.h(j0, i0)];
+        dzdy = m.dzdy[X.h(j0, i0)];
+    }
+    // A1: face velocities over the terrain factor, w, and the surface w
+    if (live) {
+        const float rgw = m.rgzu[(size_t)j0 * (ni + 1) + i0], rge = m.rgzu[(size_t)j0 * (ni + 1) + i0 + 1];
+        const float rgs = m.rgzv[(size_t)j0 * ni + i0], rgn = m.rgzv[(size_t)(j0 + 1) * ni + i0];
+        for (int k = 1 + wy; k <= nk + 1; k += kTosWarps) {
+            if (k > nk) {
+                SM(s_w, k) = a.w3d[X.w(k, y, x)];
+                continue;
+            }
+            const float uw = a.u3d[X.u(k, y, x)], ue = a.u3d[X.u(k, y, x + 1)];
+            const float vs = a.v3d[X.v(k, y, x)], vn = a.v3d[X.v(k, y + 1, x)];
+            SM(s_xw, k) = uw * rgw;
+            SM(s_xe, k) = ue * rge;
+            SM(s_ys, k) = vs * rgs;
+            SM(s_yn, k) = vn * rgn;
+            if (k == 1) {  // bc.F:1151-1178, the surface w of this small step
+                const float ut = (uw + ue) * dzdx, vt = (vs + vn) * dzdy;
+                const float ws = (0.5f * (ut + vt)) * gz;
+                a.w3d[X.w(1, y, x)] = ws;
+                SM(s_w, 1) = ws;
+            } else {
+                SM(s_w, k) = a.w3d[X.w(k, y, x)];
+            }
+        }
+        if (wy == 0) {
+            SM(s_d3, 1) = 0.0f;
+            SM(s_d3, nk + 1) = 0.0f;
+            SM(s_ha, 1) = 0.0f;
+            SM(s_ha, nk + 1) = 0.0f;
+        }
+    }
+    __syncthreads();
+    // A2: dum3 and hadvp on the interior w levels
+    if (live) {
+        for (int kf = 2 + wy; kf <= nk; kf += kTosWarps) {
+            const float r2 = (sigf(kf, p.dz) - sig(kf - 1, p.dz)) * rds(kf, p.dz);
+            const float r1 = 1.0f - r2;
+            const float height = (sigf(kf, p.dz) - p.zt) * p.rzt;
+            const float xw = SM(s_xw, kf), xe = SM(s_xe, kf), xwl = SM(s_xw, kf - 1), xel = SM(s_xe, kf - 1);
+            const float ys = SM(s_ys, kf), yn = SM(s_yn, kf), ysl = SM(s_ys, kf - 1), ynl = SM(s_yn, kf - 1);
+            {
+                const float uh = xw + xe, ul = xwl + xel, vh = ys + yn, vl = ysl + ynl;
+                const float xt = (r2 * uh + r1 * ul) * dzdx;
+                const float yt = (r2 * vh + r1 * vl) * dzdy;
+                const float d3 = ((0.5f * (xt + yt)) * height) * gz;
+                SM(s_d3, kf) = d3;
+                if (dlast) a.dum3[X.p(kf, j, i)] = d3;
+            }
+            if (do_adv) {
+                const float rk = m.rho0_3d[X.m(kf - 1, 0, 0)], rl = m.rho0_3d[X.m(kf - 2, 0, 0)];
+                const float uh = rk * xw + rk * xe, ul = rl * xwl + rl * xel;
+                const float vh = rk * ys + rk * yn, vl = rl * ysl + rl * ynl;
+                const float xt = (r2 * uh + r1 * ul) * dzdx;
+                const float yt = (r2 * vh + r1 * vl) * dzdy;
+                const float ha = (((0.5f * (xt + yt)) * height) * gz) * m.rrf0[X.m(kf - 1, j0, i0)];
+                SM(s_ha, kf) = ha;
+                if (dlast) a.hadvp[X.p(kf, j, i)] = ha;
+            }
+        }
+    }
+    __syncthreads();
+    // A3: divergence, fpk (initial + pi' advection), column coefficients
+    if (live) {
+        for (int k = 1 + wy; k <= nk; k += kTosWarps) {
+            const size_t c = X.p(k, j, i);
+            const float xw = SM(s_xw, k), xe = SM(s_xe, k), ys = SM(s_ys, k), yn = SM(s_yn, k);
+            float div = 0.0f;
+            if (do_div) {
+                const float hz = (xe - xw) * p.rdx + (yn - ys) * p.rdy;
+                const float vt = (SM(s_d3, k + 1) - SM(s_d3, k)) * rdsf(k, p.dz);
+                div = gz * (hz + vt);
+                if (fabsf(div) < 1.0e-20f) div = 0.0f;
+            }
+            const float w1 = k == 1 ? 0.0f : SM(s_w, k), w2 = k == nk ? 0.0f : SM(s_w, k + 1);
+            const float qk = a.qk[c], pk1 = a.pk1[c], pk2 = a.pk2[c];
+            const float src = p.dts * (a.ppten[c] - a.ppterm[c] * div);
+            float fpk = src + p.beta * ((-qk) * (w2 - w1));
+            if (dlast) a.divh[c] = div;
+            if (do_adv) {
+                const float rho = m.rho0_3d[X.m(k - 1, 0, 0)];
+                const float u2 = p.temx * (rho * xe), u1 = p.temx * (rho * xw);
+                const float v2 = p.temy * (rho * yn), v1 = p.temy * (rho * ys);
+                const float ww2 = SM(s_ha, k + 1) + p.beta * SM(s_w, k + 1);
+                const float ww1 = SM(s_ha, k) + p.beta * SM(s_w, k);
+                const float pc = a.piadv[c];
+                const float xa = u2 * (a.piadv[c + 1] - pc) + u1 * (pc - a.piadv[c - 1]);
+                const float ya = v2 * (a.piadv[X.p(k, j + 1, i)] - pc) + v1 * (pc - a.piadv[X.p(k, j - 1, i)]);
+                float hz = (-(xa + ya)) * m.rr0[X.m(k - 1, j0, i0)];
+                hz = hz * gz;
+                const float vt = ww1 * pk1 + ww2 * pk2;
+                fpk = fpk + (hz + vt);
+            }
+            if (dlast) a.fpk[c] = fpk;
+            SM(s_fpk, k) = fpk;
+            SM(s_a1, k) = pk1 + qk;
+            SM(s_a2, k) = pk2 - qk;
+            SM(s_mm, k) = a.mm[c];
+            SM(s_pp, k) = a.pp3d[c];
+        }
+    }
+    __syncthreads();
+    // A4: tridiagonal coefficients and right-hand side, k = 2..nk
+    if (live && do_imp) {
+        for (int k = 2 + wy; k <= nk; k += kTosWarps) {
+            const float mmk = SM(s_mm, k);
+            const float aa = k >= 3 ? (-p.asq) * (mmk * SM(s_a1, k - 1)) : 0.0f;
+            const float cc = k < nk ? (-p.asq) * ((-mmk) * SM(s_a2, k)) : 0.0f;
+            const float dg = (-SM(s_a1, k)) + SM(s_a2, k - 1);
+            const float bb = 1.0f - p.asq * (mmk * dg);
+            const float pd = SM(s_pp, k) - SM(s_pp, k - 1);
+            const float fwk = p.dts * a.wten[X.w(k, y, x)] + p.beta * ((-mmk) * pd);
+            const float ud = (SM(s_pp, k) + SM(s_fpk, k)) - (SM(s_pp, k - 1) + SM(s_fpk, k - 1));
+            const float dd = (SM(s_w, k) + fwk) + p.alph * ((-mmk) * ud);
+            SM(s_aa, k) = aa;
+            SM(s_bb, k) = bb;
+            SM(s_cc, k) = cc;
+            SM(s_dd, k) = dd;
+            if (dlast) {
+                const size_t c = X.p(k, j, i);
+                a.tri_aa[c] = aa;
+                a.tri_bb[c] = bb;
+                a.tri_cc[c] = cc;
+                a.tri_dd[c] = dd;
+            }
+        }
+    }
+    __syncthreads();
+    // B: Thomas sweep, one lane per column
+    if (live && do_imp && wy == 0) {
+        float ec = 0.0f, ed = 0.0f;
+        for (int k = 2; k <= nk; ++k) {
+            const float aa = SM(s_aa, k), bb = SM(s_bb, k), cc = SM(s_cc, k), dd = SM(s_dd, k);
+            const float piv = k == 2 ? bb : aa * ec + bb;
+            const float inv = 1.0f / piv;
+            if (dlast) a.tri_pivot[X.p(k, j, i)] = piv;
+            if (k < nk) {
+                ec = (-cc) * inv;
+                ed = (k == 2 ? dd : dd - aa * ed) * inv;
+                SM(s_cc, k) = ec;
+                SM(s_ed, k) = ed;
+                if (dlast) a.elim_d[X.p(k, j, i)] = ed;
+            } else {
+                SM(s_w, k) = (dd - aa * ed) * inv;
+            }
+        }
+        for (int k = nk - 1; k >= 2; --k) SM(s_w, k) = SM(s_cc, k) * SM(s_w, k + 1) + SM(s_ed, k);
+    }
+    __syncthreads();
+    // C: pressure update, filter, halo copy, averages
+    if (live) {
+        const bool fill = p.n < p.nloop && (p.abl & GM1B_TOS_BETWEEN_STEP_FILL);
+        const bool east = i == ni, north = j == nj;
+        for (int k = 1 + wy; k <= nk; k += kTosWarps) {
+            const size_t c = X.p(k, j, i);
+            const float wk = SM(s_w, k), wk1 = SM(s_w, k + 1);
+            if (do_imp && k >= 2) {
+                a.w3d[X.w(k, y, x)] = wk;
+                if (dlast) {
+                    float lhs = SM(s_aa, k) * SM(s_w, k - 1) + SM(s_bb, k) * wk;
+                    const float cc = k < nk ? (-p.asq) * ((-SM(s_mm, k)) * SM(s_a2, k)) : 0.0f;
+                    lhs = lhs + cc * wk1;
+                    a.tri_residual[c] = lhs - SM(s_dd, k);
+                }
+            }
+            const float w1 = k == 1 ? 0.0f : wk, w2 = k == nk ? 0.0f : wk1;
+            const float old = SM(s_pp, k);
+            const float vt = w1 * SM(s_a1, k) + w2 * SM(s_a2, k);
+            float up = (old + SM(s_fpk, k)) + p.alph * vt;
+            if (fabsf(up) < 1.0e-20f) up = 0.0f;
+            const float tend = p.kdiv * (up - old);
+            const float pd = up + tend;
+            a.pp3d[c] = up;
+            a.ppd[c] = pd;
+            if (dlast) a.elim_c[c] = tend;
+            if (p.nrk == 3 && last) a.ppx[c] = tend;
+            if (fill) {  // bcp: the halo takes its clamped interior neighbour
+                const int rows[3] = {j, j == 1 ? 0 : -1, north ? nj + 1 : -1};
+                const int cols[3] = {i, i == 1 ? 0 : -1, east ? ni + 1 : -1};
+#pragma unroll
+                for (int r = 0; r < 3; ++r) {
+                    if (rows[r] < 0) continue;
+#pragma unroll
+                    for (int q = 0; q < 3; ++q) {
+                        if (cols[q] < 0 || (r == 0 && q == 0)) continue;
+                        a.ppd[X.p(k, rows[r], cols[q])] = pd;
+                    }
+                }
+            }
+            // rru/rrv/rrw over faces 1..ni+1 and rows 1..nj+1
+#pragma unroll
+            for (int dy = 0; dy < 2; ++dy) {
+                if (dy == 1 && !north) break;
+#pragma unroll
+                for (int dx = 0; dx < 2; ++dx) {
+                    if (dx == 1 && !east) break;
+                    const size_t qu = X.u(k, y + dy, x + dx), qv = X.v(k, y + dy, x + dx), qw = X.w(k, y + dy, x + dx);
+                    const float uu = a.u3d[qu], vv = a.v3d[qv];
+                    const float ww = (dy == 0 && dx == 0) ? wk : a.w3d[qw];
+                    const float su = a.rru[qu] + uu, sv = a.rrv[qv] + vv;
+                    const float sw = a.rrw[qw] + (last ? ww * p.alph : ww);
+                    a.rru[qu] = last ? su * p.tavg : su;
+                    a.rrv[qv] = last ? sv * p.tavg : sv;
+                    a.rrw[qw] = last ? sw * p.tavg : sw;
+                }
+            }
+        }
+    }
+#undef SM
+}
+
+// ---------------------------------------------------------------------------
+// radiation histories (radbcew4/radbcns4): one warp per boundary line, the
+// clamped phase speeds of all levels in parallel, their column mean summed
+// in level order by lane 0
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) tos_radiation_kernel(TosArgs p, float dx, float dy, float dttmp) {
+    extern __shared__ float sh[];
+    const Ix X{p.ni, p.nj};
+    const int ni = p.ni, nj = p.nj, nk = p.nk;
+    const int lane = threadIdx.x, wy = threadIdx.y;
+    int line = blockIdx.x * 4 + wy;
+    const int lines = 2 * nj + 2 * ni;
+    if (line >= lines) return;
+    float *s = sh + wy * (nk + 1);
+    const gm1b_terrain_open_arrays &a = p.a;
+    int side;
+    if (line < nj) side = 0;
+    else if (line < 2 * nj) side = 1, line -= nj;
+    else if (line < 2 * nj + ni) side = 2, line -= 2 * nj;
+    else side = 3, line -= 2 * nj + ni;
+    const float eps = 1.0e-10f, limit = 350.0f;
+    for (int k = 1 + lane; k <= nk; k += 32) {
+        float foo, num, c;
+        if (side == 0) {
+            const int yy = line + 3;
+            foo = a.ua[X.u(k, yy, 5)] - a.ua[X.u(k, yy, 4)];
+            num = (dx * a.ruf[4]) * (a.ua[X.u(k, yy, 4)] - a.u3d[X.u(k, yy, 4)]);
+        } else if (side == 1) {
+            const int yy = line + 3;
+            foo = a.ua[X.u(k, yy, ni + 2)] - a.ua[X.u(k, yy, ni + 1)];
+            num = (dx * a.ruf[ni + 2]) * (a.ua[X.u(k, yy, ni + 2)] - a.u3d[X.u(k, yy, ni + 2)]);
+        } else if (side == 2) {
+            const int xx = line + 3;
+            foo = a.va[X.v(k, 5, xx)] - a.va[X.v(k, 4, xx)];
+            num = (dy * a.rvf[4]) * (a.va[X.v(k, 4, xx)] - a.v3d[X.v(k, 4, xx)]);
+        } else {
+            const int xx = line + 3;
+            foo = a.va[X.v(k, nj + 2, xx)] - a.va[X.v(k, nj + 1, xx)];
+            num = (dy * a.rvf[nj + 2]) * (a.va[X.v(k, nj + 2, xx)] - a.v3d[X.v(k, nj + 2, xx)]);
+        }
+        const float den = dttmp * (copysignf(eps, foo) + foo);
+        c = num / den;
+        s[k - 1] = (side == 0 || side == 2) ? np_max(np_min(c, 0.0f), -limit) : np_min(np_max(c, 0.0f), limit);
+    }
+    __syncwarp();
+    if (lane == 0) {
+        float avg = 0.0f;
+        for (int k = 0; k < nk; ++k) avg = avg + s[k];
+        s[nk] = avg / (float)nk;
+    }
+    __syncwarp();
+    const float avg = s[nk];
+    float *rad = side == 0 ? a.radbcw : side == 1 ? a.radbce : side == 2 ? a.radbcs : a.radbcn;
+    const size_t stride = side < 2 ? (size_t)(nj + 6) : (size_t)(ni + 6);
+    for (int k = 1 + lane; k <= nk; k += 32) rad[(size_t)k * stride + line + 3] = avg;
+}
+
+// ---------------------------------------------------------------------------
+// stage fills, pass 1: bcu west/east, bcv south/north, bcw west/east on
+// k = 2..nk with the flag-1 zero of w levels 1 and nk+1, and (nrk < 3) bcp
+// west/east of pp3d and bcs west/east of the scalar
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) tos_fill1_kernel(TosArgs p) {
+    const Ix X{p.ni, p.nj};
+    const int ni = p.ni, nj = p.nj, nk = p.nk;
+    const gm1b_terrain_open_arrays &a = p.a;
+    const bool more = p.nrk < 3;
+    const size_t nA = (size_t)nk * (nj + 2) * 6;           // u W/E, rows 0..nj+1
+    const size_t nB = (size_t)nk * 6 * (ni + 2);           // v S/N, columns 0..ni+1
+    const size_t nC = (size_t)(nk - 1) * (nj + 2) * 6;     // w W/E, k = 2..nk
+    const size_t nD = (size_t)2 * (nj + 2) * (ni + 2);     // w levels 1 and nk+1
+    const size_t nE = more ? (size_t)nk * (nj + 2) * 2 : 0;  // pp3d W/E
+    const size_t nF = more ? (size_t)nk * (nj + 2) * 6 : 0;  // scalar W/E
+    const size_t total = nA + nB + nC + nD + nE + nF;
+    for (size_t z = (size_t)blockIdx.x * blockDim.x + threadIdx.x; z < total; z += (size_t)gridDim.x * blockDim.x) {
+        size_t q = z;
+        if (q < nA) {
+            const int h = (int)(q % 6), j = (int)((q / 6) % (nj + 2)), k = (int)(q / (6 * (size_t)(nj + 2))) + 1;
+            const int y = j + 2;
+            if (h < 3) a.u3d[X.u(k, y, h)] = a.u3d[X.u(k, y, 3)];
+            else a.u3d[X.u(k, y, ni + 1 + h)] = a.u3d[X.u(k, y, ni + 3)];
+            continue;
+        }
+        q -= nA;
+        if (q < nB) {
+            const int i = (int)(q % (ni + 2)), h = (int)((q / (ni + 2)) % 6), k = (int)(q / (6 * (size_t)(ni + 2))) + 1;
+            const int x = i + 2;
+            if (h < 3) a.v3d[X.v(k, h, x)] = a.v3d[X.v(k, 3, x)];
+            else a.v3d[X.v(k, nj + 1 + h, x)] = a.v3d[X.v(k, nj + 3, x)];
+            continue;
+        }
+        q -= nB;
+        if (q < nC) {
+            const int h = (int)(q % 6), j = (int)((q / 6) % (nj + 2)), k = (int)(q / (6 * (size_t)(nj + 2))) + 2;
+            const int y = j + 2;
+            if (h < 3) a.w3d[X.w(k, y, h)] = a.w3d[X.w(k, y, 3)];
+            else a.w3d[X.w(k, y, ni + h)] = a.w3d[X.w(k, y, ni + 2)];
+            continue;
+        }
+        q -= nC;
+        if (q < nD) {
+            const int i = (int)(q % (ni + 2)), j = (int)((q / (ni + 2)) % (nj + 2));
+            const int k = q / ((size_t)(ni + 2) * (nj + 2)) == 0 ? 1 : nk + 1;
+            a.w3d[X.w(k, j + 2, i + 2)] = 0.0f;
+            continue;
+        }
+        q -= nD;
+        if (q < nE) {
+            const int e = (int)(q % 2), j = (int)((q / 2) % (nj + 2)), k = (int)(q / (2 * (size_t)(nj + 2))) + 1;
+            if (e == 0) a.pp3d[X.p(k, j, 0)] = a.pp3d[X.p(k, j, 1)];
+            else a.pp3d[X.p(k, j, ni + 1)] = a.pp3d[X.p(k, j, ni)];
+            continue;
+        }
+        q -= nE;
+        {
+            const int h = (int)(q % 6), j = (int)((q / 6) % (nj + 2)), k = (int)(q / (6 * (size_t)(nj + 2))) + 1;
+            const int y = j + 2;
+            if (h < 3) a.scalar[X.w(k, y, h)] = a.scalar[X.w(k, y, 3)];
+            else a.scalar[X.w(k, y, ni + h)] = a.scalar[X.w(k, y, ni + 2)];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// stage fills, pass 2: bcu south/north, bcv west/east, bcw south/north on
+// k = 2..nk, the surface w (bcwsfc), and (nrk < 3) bcp south/north of pp3d
+// and bcs south/north of the scalar
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) tos_fill2_kernel(TosArgs p) {
+    const Ix X{p.ni, p.nj};
+    const int ni = p.ni, nj = p.nj, nk = p.nk;
+    const gm1b_terrain_open_arrays &a = p.a;
+    const gm1b_terrain_metrics &m = p.m;
+    const bool more = p.nrk < 3;
+    const size_t nA = (size_t)nk * 6 * (ni + 3);           // u S/N, faces 0..ni+2
+    const size_t nB = (size_t)nk * (nj + 3) * 6;           // v W/E, rows 0..nj+2
+    const size_t nC = (size_t)(nk - 1) * 6 * (ni + 2);     // w S/N, k = 2..nk
+    const size_t nD = (size_t)nj * ni;                     // bcwsfc
+    const size_t nE = more ? (size_t)nk * 2 * (ni + 2) : 0;  // pp3d S/N
+    const size_t nF = more ? (size_t)nk * 6 * (ni + 2) : 0;  // scalar S/N
+    const size_t total = nA + nB + nC + nD + nE + nF;
+    for (size_t z = (size_t)blockIdx.x * blockDim.x + threadIdx.x; z < total; z += (size_t)gridDim.x * blockDim.x) {
+        size_t q = z;
+        if (q < nA) {
+            const int i = (int)(q % (ni + 3)), h = (int)((q / (ni + 3)) % 6), k = (int)(q / (6 * (size_t)(ni + 3))) + 1;
+            const int x = i + 2;
+            if (h < 3) a.u3d[X.u(k, h, x)] = a.u3d[X.u(k, 3, x)];
+            else a.u3d[X.u(k, nj + h, x)] = a.u3d[X.u(k, nj + 2, x)];
+            continue;
+        }
+        q -= nA;
+        if (q < nB) {
+            const int h = (int)(q % 6), j = (int)((q / 6) % (nj + 3)), k = (int)(q / (6 * (size_t)(nj + 3))) + 1;
+            const int y = j + 2;
+            if (h < 3) a.v3d[X.v(k, y, h)] = a.v3d[X.v(k, y, 3)];
+            else a.v3d[X.v(k, y, ni + h)] = a.v3d[X.v(k, y, ni + 2)];
+            continue;
+        }
+        q -= nB;
+        if (q < nC) {
+            const int i = (int)(q % (ni + 2)), h = (int)((q / (ni + 2)) % 6), k = (int)(q / (6 * (size_t)(ni + 2))) + 2;
+            const int x = i + 2;
+            if (h < 3) a.w3d[X.w(k, h, x)] = a.w3d[X.w(k, 3, x)];
+            else a.w3d[X.w(k, nj + h, x)] = a.w3d[X.w(k, nj + 2, x)];
+            continue;
+        }
+        q -= nC;
+        if (q < nD) {
+            const int i0 = (int)(q % ni), j0 = (int)(q / ni);
+            const int y = j0 + 3, x = i0 + 3;
+            const float ut = (a.u3d[X.u(1, y, x)] + a.u3d[X.u(1, y, x + 1)]) * m.dzdx[X.h(j0, i0)];
+            const float vt = (a.v3d[X.v(1, y, x)] + a.v3d[X.v(1, y + 1, x)]) * m.dzdy[X.h(j0, i0)];
+            a.w3d[X.w(1, y, x)] = (0.5f * (ut + vt)) * m.gz[X.h(j0, i0)];
+            continue;
+        }
+        q -= nD;
+        if (q < nE) {
+            const int i = (int)(q % (ni + 2)), e = (int)((q / (ni + 2)) % 2), k = (int)(q / (2 * (size_t)(ni + 2))) + 1;
+            if (e == 0) a.pp3d[X.p(k, 0, i)] = a.pp3d[X.p(k, 1, i)];
+            else a.pp3d[X.p(k, nj + 1, i)] = a.pp3d[X.p(k, nj, i)];
+            continue;
+        }
+        q -= nE;
+        {
+            const int i = (int)(q % (ni + 2)), h = (int)((q / (ni + 2)) % 6), k = (int)(q / (6 * (size_t)(ni + 2))) + 1;
+            const int x = i + 2;
+            if (h < 3) a.scalar[X.w(k, h, x)] = a.scalar[X.w(k, 3, x)];
+            else a.scalar[X.w(k, nj + h, x)] = a.scalar[X.w(k, nj + 2, x)];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+bool launch_ok(const char *what) {
+    const cudaError_t e = cudaPeekAtLastError();
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        gm1b_set_error("%s: %s", what, cudaGetErrorString(e));
+        return false;
+    }
+    return true;
+}
+
+// Fornberg (1988): weights of the three-point value stencil at x0 from the
+// first three of four nodes, in double precision (param.F:9016-9035).
+void fornberg_value_weights(const double alpha[4], double x0, double out[3]) {
+    double d[4][6][4] = {};
+    d[0][1][0] = 1.0;
+    double c1 = 1.0;
+    for (int n = 1; n < 4; ++n) {
+        double c2 = 1.0;
+        for (int nu = 0; nu < n; ++nu) {
+            const double c3 = alpha[n] - alpha[nu];
+            c2 = c2 * c3;
+            d[n - 1][n + 1][nu] = 0.0;
+            for (int mo = 0; mo <= n; ++mo)
+                d[n][mo + 1][nu] = ((alpha[n] - x0) * d[n - 1][mo + 1][nu] - mo * d[n - 1][mo][nu]) / c3;
+        }
+        for (int mo = 0; mo <= n; ++mo)
+            d[n][mo + 1][n] = (c1 / c2) * (mo * d[n - 1][mo][n - 1] - (alpha[n - 1] - x0) * d[n - 1][mo + 1][n - 1]);
+        c1 = c2;
+    }
+    for (int nu = 0; nu < 3; ++nu) out[nu] = d[2][1][nu];
+}
+
+// cgs (ground) / cgt (lid) of the uniform column, float32 levels as the twin
+// forms them (fornberg_extrapolation_weights, cm1_vertical_grid.py:422-454)
+bool edge_weights(int nk, float dz, bool top, float out[3]) {
+    auto sg = [dz](int k) { return ((float)k - 0.5f) * dz; };
+    auto sf = [dz](int k) { return (float)(k - 1) * dz; };
+    float den, num, nodes[4];
+    if (top) {
+        den = sf(nk + 1) - sf(nk);
+        num = sf(nk + 1);
+        for (int q = 0; q < 4; ++q) nodes[q] = sg(nk - q);
+    } else {
+        den = sf(2) - sf(1);
+        num = sf(1);
+        for (int q = 0; q < 4; ++q) nodes[q] = sg(1 + q);
+    }
+    if (!(den > 0.0f) || !std::isfinite(den)) return false;
+    double alpha[4], w[3];
+    for (int q = 0; q < 4; ++q) alpha[q] = (double)(nodes[q] / den);
+    for (int q = 0; q < 4; ++q)
+        for (int r = 0; r < q; ++r)
+            if (alpha[q] == alpha[r]) return false;
+    fornberg_value_weights(alpha, (double)(num / den), w);
+    for (int q = 0; q < 3; ++q) out[q] = (float)w[q];
+    return true;
+}
+
+unsigned grid_for(size_t work, int block) {
+    const size_t want = (work + (size_t)block - 1) / (size_t)block;
+    const size_t cap = (size_t)148 * 16;
+    return (unsigned)std::max<size_t>(1, std::min(want, cap));
+}
+
+}  // namespace
+}  // namespace gm1b
+
+using namespace gm1b;
+
+extern "C" int32_t gm1b_terrain_open_stage(int32_t ni, int32_t nj, int32_t nk, int32_t nrk, float dt, int32_t nsound,
+                                           float dx, float dy, double dz, float alph, float kdiv, uint32_t ablations,
+                                           uint32_t flags, const gm1b_terrain_open_arrays *arrays,
+                                           const gm1b_terrain_metrics *metrics, void *stream) {
+    if (arrays == nullptr || metrics == nullptr || ni < 3 || nj < 3 || nk < 4 || nk > kTosMaxNk || nrk < 1 ||
+        nrk > 3) {
+        gm1b_set_error("gm1b_terrain_open_stage: need arrays and metrics, ni >= 3, nj >= 3, 4 <= nk <= %d, "
+                       "nrk in 1..3", kTosMaxNk);
+        return GM1B_ERR_ARGUMENT;
+    }
+    if (!(dx > 0.0f) || !(dy > 0.0f) || !(dz > 0.0) || !std::isfinite(dx) || !std::isfinite(dy) ||
+        !std::isfinite(dz) || !(dt > 0.0f) || !std::isfinite(dt)) {
+        gm1b_set_error("gm1b_terrain_open_stage: dt, dx, dy, dz must be finite and > 0");
+        return GM1B_ERR_ARGUMENT;
+    }
+    if (!(alph >= 0.0f && alph <= 1.0f) || !(kdiv >= 0.0f && kdiv <= 1.0f)) {
+        gm1b_set_error("gm1b_terrain_open_stage: alph and kdiv must lie in [0, 1]");
+        return GM1B_ERR_ARGUMENT;
+    }
+    if (ablations & ~GM1B_TOS_ALL) {
+        gm1b_set_error("gm1b_terrain_open_stage: unknown ablation bits 0x%x", ablations & ~GM1B_TOS_ALL);
+        return GM1B_ERR_ARGUMENT;
+    }
+    const float *const *mp = reinterpret_cast<const float *const *>(metrics);
+    for (size_t q = 0; q < sizeof(gm1b_terrain_metrics) / sizeof(float *); ++q)
+        if (mp[q] == nullptr) {
+            gm1b_set_error("gm1b_terrain_open_stage: a metric pointer is NULL");
+            return GM1B_ERR_ARGUMENT;
+        }
+    float *const *ap = reinterpret_cast<float *const *>(arrays);
+    for (size_t q = 0; q < sizeof(gm1b_terrain_open_arrays) / sizeof(float *); ++q)
+        if (ap[q] == nullptr) {
+            gm1b_set_error("gm1b_terrain_open_stage: an array pointer is NULL");
+            return GM1B_ERR_ARGUMENT;
+        }
+    int32_t nloop = 0;
+    float dts = 0.0f;
+    if (gm1b_sound3_stage_schedule(dt, nsound, nrk, &nloop, &dts) != GM1B_OK) return GM1B_ERR_ARGUMENT;
+    TosArgs p{};
+    p.a = *arrays;
+    p.m = *metrics;
+    p.ni = ni, p.nj = nj, p.nk = nk, p.nrk = nrk, p.nloop = nloop;
+    p.abl = ablations;
+    p.diag = (flags & GM1B_TOS_DIAGNOSTICS) ? 1u : 0u;
+    p.dts = dts;
+    p.rdx = 1.0f / dx;
+    p.rdy = 1.0f / dy;
+    p.dz = (float)dz;
+    p.alph = alph;
+    p.beta = 1.0f - alph;
+    p.asq = alph * alph;
+    p.kdiv = kdiv;
+    p.temx = (dts * 0.5f) * p.rdx;
+    p.temy = (dts * 0.5f) * p.rdy;
+    p.tavg = 1.0f / (float)nloop;
+    p.zt = (float)((double)nk * dz);
+    p.rzt = 1.0f / p.zt;
+    p.halfcp = 1005.7f * 0.5f;
+    if (!edge_weights(nk, p.dz, false, p.cgs) || !edge_weights(nk, p.dz, true, p.cgt)) {
+        gm1b_set_error("gm1b_terrain_open_stage: degenerate vertical levels for dz=%g", dz);
+        return GM1B_ERR_ARGUMENT;
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const size_t col_smem = (size_t)kTosArrays * (size_t)(nk + 2) * 32 * sizeof(float);
+    static bool attr_set = false;
+    if (!attr_set) {
+        const cudaError_t e = cudaFuncSetAttribute(tos_column_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   (int)((size_t)kTosArrays * (kTosMaxNk + 2) * 32 * sizeof(float)));
+        if (e != cudaSuccess) {
+            gm1b_set_error("cudaFuncSetAttribute(tos_column_kernel): %s", cudaGetErrorString(e));
+            return GM1B_ERR_CUDA;
+        }
+        attr_set = true;
+    }
+    {
+        ProfScope ps("tos_prepare_kernel", st);
+        tos_prepare_kernel<<<grid_for((size_t)nk * (nj + 2) * (ni + 2), 256), 256, 0, st>>>(p);
+        ps.stop();
+    }
+    if (!launch_ok("tos_prepare_kernel")) return GM1B_ERR_CUDA;
+    const dim3 pg_grid((ni + 2 + 31) / 32, (nj + 2 + 3) / 4), col_grid((ni + 31) / 32, nj);
+    for (int n = 1; n <= nloop; ++n) {
+        p.n = n;
+        if (ablations & GM1B_TOS_OPEN_CONSUMPTION) {
+            ProfScope ps("tos_edge_kernel", st);
+            tos_edge_kernel<<<2 * nj + 2 * ni, 128, 4 * (size_t)(nk + 2) * sizeof(float), st>>>(p);
+            ps.stop();
+            if (!launch_ok("tos_edge_kernel")) return GM1B_ERR_CUDA;
+        }
+        if (ablations & GM1B_TOS_PRESSURE_GRADIENT) {
+            ProfScope ps("tos_pgrad_kernel", st);
+            tos_pgrad_kernel<<<pg_grid, dim3(32, 4), 0, st>>>(p);
+            ps.stop();
+            if (!launch_ok("tos_pgrad_kernel")) return GM1B_ERR_CUDA;
+        }
+        {
+            ProfScope ps("tos_column_kernel", st);
+            tos_column_kernel<<<col_grid, dim3(32, kTosWarps), col_smem, st>>>(p);
+            ps.stop();
+            if (!launch_ok("tos_column_kernel")) return GM1B_ERR_CUDA;
+        }
+    }
+    if (ablations & GM1B_TOS_RADIATION) {
+        const int lines = 2 * nj + 2 * ni;
+        ProfScope ps("tos_radiation_kernel", st);
+        tos_radiation_kernel<<<(lines + 3) / 4, dim3(32, 4), 4 * (size_t)(nk + 1) * sizeof(float), st>>>(
+            p, dx, dy, gm1b_rk_stage_dt(dt, nrk));
+        ps.stop();
+        if (!launch_ok("tos_radiation_kernel")) return GM1B_ERR_CUDA;
+    }
+    if (ablations & GM1B_TOS_STAGE_FILLS) {
+        const size_t w1 = (size_t)nk * (nj + 2) * 6 * 3 + (size_t)nk * 6 * (ni + 2) + (size_t)2 * (nj + 2) * (ni + 2);
+        const size_t w2 = (size_t)nk * 6 * (ni + 3) * 2 + (size_t)nk * (nj + 3) * 6 + (size_t)nj * ni;
+        {
+            ProfScope ps("tos_fill1_kernel", st);
+            tos_fill1_kernel<<<grid_for(w1, 256), 256, 0, st>>>(p);
+            ps.stop();
+        }
+        if (!launch_ok("tos_fill1_kernel")) return GM1B_ERR_CUDA;
+        {
+            ProfScope ps("tos_fill2_kernel", st);
+            tos_fill2_kernel<<<grid_for(w2, 256), 256, 0, st>>>(p);
+            ps.stop();
+        }
+        if (!launch_ok("tos_fill2_kernel")) return GM1B_ERR_CUDA;
+    }
+    return GM1B_OK;
+}

@@ -391,6 +391,50 @@ typedef struct gm1b_momentum5_arrays {
 GM1B_API int32_t gm1b_momentum_advection5(int32_t ni, int32_t nj, int32_t nk, const gm1b_momentum5_arrays *arrays,
                                           uint32_t lateral_obc, float dx, float dy, float dz, void *stream);
 
+/* ------------------------------------------------------------------------
+ * Terrain + all-open psolver=3 acoustic RK stage (padded ng = 3 lane).
+ * Replaces launch_cuda_psolver3_terrain_open_stage / _three_stage
+ * (src/cm1core/cuda_psolver3_terrain_open.py:1436, :1217) and their CPU twin
+ * cpu_psolver3_terrain_open_stage_inplace (:774).  Shapes as
+ * terrain_open_sound_shapes (:162): pressure family (nk+2, nj+2, ni+2),
+ * u (nk+2, nj+6, ni+7), v (nk+2, nj+7, ni+6), w (nk+3, nj+6, ni+6), scalar
+ * (nk+2, nj+6, ni+6), radbcw/e (nk+2, nj+6), radbcs/n (nk+2, ni+6), uh
+ * (ni+6), vh (nj+6), ruf (ni+7), rvf (nj+7); metrics as terrain_static_shapes
+ * (src/cm1core/cuda_terrain_open_boundary.py:429).  ni, nj >= 3, nk >= 4.
+ * ------------------------------------------------------------------------ */
+typedef struct gm1b_terrain_open_arrays {
+    float *ppi, *pp3d, *ppx, *ppd, *piadv, *ppterm, *ppten, *thv, *qk, *pk1, *pk2, *mm, *fpk, *divh, *hadvp, *dum3,
+        *elim_c, *elim_d, *tri_aa, *tri_bb, *tri_cc, *tri_dd, *tri_pivot, *tri_residual;
+    float *ua, *u3d, *uten, *rru, *va, *v3d, *vten, *rrv, *wa, *w3d, *wten, *rrw;
+    float *radbcw, *radbce, *radbcs, *radbcn, *uh, *vh, *ruf, *rvf, *scalar;
+} gm1b_terrain_open_arrays;
+
+typedef struct gm1b_terrain_metrics {
+    const float *rho0_3d, *rr0, *rf0, *rrf0, *c1, *c2, *gz, *rgzu, *rgzv, *dzdx, *dzdy, *gx, *gxu, *gy, *gyv;
+} gm1b_terrain_metrics;
+
+/* TerrainOpenSoundAblations (:276): a set bit runs that phase */
+#define GM1B_TOS_OPEN_CONSUMPTION 1u
+#define GM1B_TOS_PRESSURE_GRADIENT 2u
+#define GM1B_TOS_TRANSFORMED_DIVERGENCE 4u
+#define GM1B_TOS_PRESSURE_ADVECTION 8u
+#define GM1B_TOS_IMPLICIT_SOLVE 16u
+#define GM1B_TOS_BETWEEN_STEP_FILL 32u
+#define GM1B_TOS_RADIATION 64u
+#define GM1B_TOS_STAGE_FILLS 128u
+#define GM1B_TOS_ALL 255u
+/* flags: leave every scratch array (qk .. tri_residual) as the CPU twin
+ * does; without it only the prognostic and radiation arrays are written
+ * (qk, pk1, pk2, mm hold this stage's coefficients) */
+#define GM1B_TOS_DIAGNOSTICS 1u
+
+/* One RK stage nrk (1..3).  dz is double because the lid height is
+ * float32(nk * dz) of a double dz (:528).  Allocation-free; graph-capturable. */
+GM1B_API int32_t gm1b_terrain_open_stage(int32_t ni, int32_t nj, int32_t nk, int32_t nrk, float dt, int32_t nsound,
+                                         float dx, float dy, double dz, float alph, float kdiv, uint32_t ablations,
+                                         uint32_t flags, const gm1b_terrain_open_arrays *arrays,
+                                         const gm1b_terrain_metrics *metrics, void *stream);
+
 /* The two halves of gm1b_momentum_advection5, for a caller that edits the
  * fluxes or divx between them (the reference's post_divergence_hook seam):
  * the mass fluxes and divx, then the advu / advv / advw increments from the

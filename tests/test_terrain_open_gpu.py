@@ -1,0 +1,115 @@
+"""Parity of the CUDA terrain/open acoustic stage through the C ABI with the
+reference's CPU twin (golden fixtures: every array after every RK stage, the
+eight ablations, alph/kdiv) and with the oracle on multi-tile and minimum
+grids, with and without the diagnostic scratch words.  Bar: every float32
+word identical."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+from gm1_b200 import terrain_open as tos
+from gm1_b200._native import Gm1bError
+from oracle import terrain_open as orc
+from tests.golden.make_golden import terrain_open_fixture
+from tests.test_oracle_terrain_open import PARAMS, TAGS, digest, load
+
+pytestmark = pytest.mark.gpu
+
+PROGNOSTIC = tuple(n for n in tos.COMPARE_OUTPUT_NAMES if n not in tos.COLUMN_DIAGNOSTIC_NAMES) + ("scalar",)
+
+
+def _dev(d):
+    return {k: torch.from_numpy(np.ascontiguousarray(v)).cuda() for k, v in d.items()}
+
+
+def _digests(dev):
+    torch.cuda.synchronize()
+    return {n: digest(dev[n].cpu().numpy()) for n in tos.ALL_ARRAY_NAMES}
+
+
+def _bad(got: dict, want: dict, names) -> list[str]:
+    out = []
+    for n in names:
+        g = got[n].cpu().numpy() if isinstance(got[n], torch.Tensor) else got[n]
+        w = want[n]
+        if not np.array_equal(g.view(np.uint32), w.view(np.uint32)):
+            k = int(np.count_nonzero(g.view(np.uint32) != w.view(np.uint32)))
+            out.append(f"{n}({k})")
+    return out
+
+
+@pytest.mark.parametrize("tag", TAGS)
+def test_stages_bit_exact_vs_reference(tag):
+    meta, a, m, want = load(tag)
+    p = {k: meta[k] for k in PARAMS}
+    dev, mdev = _dev(a), _dev(m)
+    for stage in meta["stages"]:
+        r = tos.launch_cuda_psolver3_terrain_open_stage(dev, mdev, nrk=stage["nrk"], **p)
+        assert r.cadence[0]["nloop"] == stage["nloop"]
+        got = _digests(dev)
+        assert sorted(n for n in got if got[n] != stage["digests"][n]) == [], f"nrk={stage['nrk']}"
+    assert _bad(dev, want, tos.ALL_ARRAY_NAMES) == []
+
+
+@pytest.mark.parametrize("name", list(orc.ABLATION_BITS))
+def test_each_ablation_bit_exact_vs_reference(name):
+    meta, a, m, _ = load("tos_reftest_5x4x5")
+    p = {k: meta[k] for k in PARAMS}
+    dev, mdev = _dev(a), _dev(m)
+    tos.launch_cuda_psolver3_terrain_open_three_stage(
+        dev, mdev, ablations=tos.TerrainOpenSoundAblations(**{name: False}), **p)
+    got = _digests(dev)
+    assert sorted(n for n in got if got[n] != meta["ablations"][name][n]) == []
+
+
+def test_alph_kdiv_bit_exact_vs_reference():
+    meta, a, m, _ = load("tos_seeded_9x7x8")
+    p = {k: meta[k] for k in PARAMS}
+    ak = meta["alph_kdiv"]
+    dev, mdev = _dev(a), _dev(m)
+    for stage in ak["stages"]:
+        tos.launch_cuda_psolver3_terrain_open_stage(dev, mdev, nrk=stage["nrk"], alph=ak["alph"], kdiv=ak["kdiv"], **p)
+        got = _digests(dev)
+        assert sorted(n for n in got if got[n] != stage["digests"][n]) == []
+
+
+@pytest.mark.parametrize("ni,nj,nk,nsound,dz", [(70, 37, 20, 6, 250.0), (45, 66, 12, 8, 333.3), (3, 3, 4, 6, 200.0),
+                                               (33, 5, 41, 4, 480.0)])
+def test_three_stages_bit_exact_vs_oracle(ni, nj, nk, nsound, dz):
+    a, m = terrain_open_fixture(ni, nj, nk, 7 + ni + nj)
+    p = dict(ni=ni, nj=nj, nk=nk, dt=2.0, nsound=nsound, dx=450.0, dy=520.0, dz=dz)
+    ref = {k: v.copy() for k, v in a.items()}
+    orc.terrain_open_three_stage(ref, m, **p)
+    dev, mdev = _dev(a), _dev(m)
+    tos.launch_cuda_psolver3_terrain_open_three_stage(dev, mdev, **p)
+    torch.cuda.synchronize()
+    assert _bad(dev, ref, tos.ALL_ARRAY_NAMES) == []
+
+
+def test_compact_mode_prognostics_match_and_skip_scratch():
+    ni, nj, nk = 70, 37, 20
+    a, m = terrain_open_fixture(ni, nj, nk, 11)
+    p = dict(ni=ni, nj=nj, nk=nk, dt=2.0, nsound=6, dx=450.0, dy=520.0, dz=250.0)
+    ref = {k: v.copy() for k, v in a.items()}
+    orc.terrain_open_three_stage(ref, m, **p)
+    compact = {k: v for k, v in a.items()}
+    for n in tos.COLUMN_DIAGNOSTIC_NAMES:
+        compact[n] = np.full((1,), 7.0, np.float32)
+    dev, mdev = _dev(compact), _dev(m)
+    tos.launch_cuda_psolver3_terrain_open_three_stage(
+        dev, mdev, compiled=tos.compile_cuda_psolver3_terrain_open(retain_column_diagnostics=False), **p)
+    torch.cuda.synchronize()
+    assert _bad(dev, ref, PROGNOSTIC) == []
+    assert all(float(dev[n][0]) == 7.0 for n in tos.COLUMN_DIAGNOSTIC_NAMES)
+
+
+def test_oversized_column_refused_by_the_library():
+    ni, nj, nk = 4, 4, 141
+    a, m = terrain_open_fixture(ni, nj, nk, 3)
+    dev, mdev = _dev(a), _dev(m)
+    with pytest.raises(Gm1bError, match="nk"):
+        tos.launch_cuda_psolver3_terrain_open_three_stage(dev, mdev, ni=ni, nj=nj, nk=nk, dt=2.0, nsound=6, dx=1.0,
+                                                          dy=1.0, dz=100.0)
