@@ -37,8 +37,8 @@ namespace gm1b {
 namespace {
 
 constexpr int kTosWarps = 8;     // k-parallel warps of the column pass
-constexpr int kTosMaxNk = 140;   // column pass keeps 12 words per level per column in shared memory
-constexpr int kTosArrays = 12;
+constexpr int kTosMaxNk = 160;   // column pass keeps 10 words per level per column in shared memory
+constexpr int kTosArrays = 10;
 
 struct TosArgs {
     gm1b_terrain_open_arrays a;
@@ -242,42 +242,44 @@ __global__ void __launch_bounds__(128) tos_pgrad_kernel(TosArgs p) {
     const bool dh = p.diag && p.n == p.nloop && !(p.abl & GM1B_TOS_PRESSURE_ADVECTION);
     if (!du && !dv && !dh) return;
     const int iw = du ? i - 1 : i, js = dv ? j - 1 : j;   // neighbour points (own point when unused)
-    float pc = a.ppd[X.p(1, j, i)], pw = a.ppd[X.p(1, j, iw)], ps = a.ppd[X.p(1, js, i)];
+    float pc = __ldg(a.ppd + X.p(1, j, i)), pw = __ldg(a.ppd + X.p(1, j, iw)), ps = __ldg(a.ppd + X.p(1, js, i));
     float vc = 0.0f, vw = 0.0f, vs = 0.0f;  // vertical difference at level k (zero at k = 1)
-    float gxu_lo = du ? m.gxu[((size_t)0 * nj + (j - 1)) * (ni + 1) + (i - 1)] : 0.0f;
-    float gyv_lo = dv ? m.gyv[((size_t)0 * (nj + 1) + (j - 1)) * ni + (i - 1)] : 0.0f;
+    float gxu_lo = du ? __ldg(m.gxu + (size_t)(j - 1) * (ni + 1) + (i - 1)) : 0.0f;
+    float gyv_lo = dv ? __ldg(m.gyv + (size_t)(j - 1) * ni + (i - 1)) : 0.0f;
+#pragma unroll 2
     for (int k = 1; k <= nk; ++k) {
         float vc1 = 0.0f, vw1 = 0.0f, vs1 = 0.0f, pc1 = 0.0f, pw1 = 0.0f, ps1 = 0.0f;
         if (k < nk) {
             const float r = rds(k + 1, p.dz);
-            pc1 = a.ppd[X.p(k + 1, j, i)];
-            pw1 = a.ppd[X.p(k + 1, j, iw)];
-            ps1 = a.ppd[X.p(k + 1, js, i)];
+            pc1 = __ldg(a.ppd + X.p(k + 1, j, i));
+            pw1 = __ldg(a.ppd + X.p(k + 1, j, iw));
+            ps1 = __ldg(a.ppd + X.p(k + 1, js, i));
             vc1 = (pc1 - pc) * r;
             vw1 = (pw1 - pw) * r;
             vs1 = (ps1 - ps) * r;
         }
         if (dh && k >= 2) a.hadvp[X.p(k, j, i)] = vc;
+        const float thc = __ldg(a.thv + X.p(k, j, i));
         if (du) {
-            const float gxu_hi = m.gxu[((size_t)k * nj + (j - 1)) * (ni + 1) + (i - 1)];
-            const float th = a.thv[X.p(k, j, i)] + a.thv[X.p(k, j, iw)];
+            const float gxu_hi = __ldg(m.gxu + ((size_t)k * nj + (j - 1)) * (ni + 1) + (i - 1));
+            const float th = thc + __ldg(a.thv + X.p(k, j, iw));
             const float hz = (pc - pw) * p.rdx;
             const float vsum = (vc1 + vw1) + (vc + vw);
             const float tr = (0.125f * vsum) * (gxu_lo + gxu_hi);
             const float pg = (p.halfcp * th) * (hz + tr);
             const size_t o = X.u(k, j + 2, i + 2);
-            a.u3d[o] = a.u3d[o] + p.dts * (a.uten[o] - pg);
+            a.u3d[o] = a.u3d[o] + p.dts * (__ldg(a.uten + o) - pg);
             gxu_lo = gxu_hi;
         }
         if (dv) {
-            const float gyv_hi = m.gyv[((size_t)k * (nj + 1) + (j - 1)) * ni + (i - 1)];
-            const float th = a.thv[X.p(k, j, i)] + a.thv[X.p(k, js, i)];
+            const float gyv_hi = __ldg(m.gyv + ((size_t)k * (nj + 1) + (j - 1)) * ni + (i - 1));
+            const float th = thc + __ldg(a.thv + X.p(k, js, i));
             const float hz = (pc - ps) * p.rdy;
             const float vsum = (vc1 + vs1) + (vc + vs);
             const float tr = (0.125f * vsum) * (gyv_lo + gyv_hi);
             const float pg = (p.halfcp * th) * (hz + tr);
             const size_t o = X.v(k, j + 2, i + 2);
-            a.v3d[o] = a.v3d[o] + p.dts * (a.vten[o] - pg);
+            a.v3d[o] = a.v3d[o] + p.dts * (__ldg(a.vten + o) - pg);
             gyv_lo = gyv_hi;
         }
         pc = pc1, pw = pw1, ps = ps1;
@@ -287,12 +289,42 @@ __global__ void __launch_bounds__(128) tos_pgrad_kernel(TosArgs p) {
 
 // ---------------------------------------------------------------------------
 // column pass of one small step.  CTA = 32 consecutive columns of row j,
-// kTosWarps warps sharing the levels.  Shared memory holds, per level and
-// column: the four transformed face velocities (later aa, bb, cc/ec, dd),
-// w, dum3 (later ed), the pi' advection term hadvp, fpk, pk1+qk, pk2-qk, mm
-// and pp3d.
+// kTosWarps warps sharing the levels; two CTAs per SM so that one's serial
+// Thomas sweep overlaps the other's loads.  Shared memory holds, per level
+// and column: the four transformed face velocities (later aa, bb, cc/ec,
+// dd), w, fpk, pk1+qk, pk2-qk, pp3d and the eliminated right-hand side ed.
+// dum3 and hadvp are formed where they are used (levels k and k+1), with
+// the same operations as the twin; read-only fields take the non-coherent
+// path so the unrolled level loops keep several levels' loads in flight.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(32 * kTosWarps, 1) tos_column_kernel(TosArgs p) {
+__device__ __forceinline__ void tos_level_terms(const float *s_xw, const float *s_xe, const float *s_ys,
+                                                const float *s_yn, int lane, int kf, const TosArgs &p, float dzdx,
+                                                float dzdy, float gz, float rk, float rl, float rrf0, bool adv,
+                                                float &d3, float &ha) {
+    const float r2 = (sigf(kf, p.dz) - sig(kf - 1, p.dz)) * rds(kf, p.dz);
+    const float r1 = 1.0f - r2;
+    const float height = (sigf(kf, p.dz) - p.zt) * p.rzt;
+    const float xw = s_xw[kf * 32 + lane], xe = s_xe[kf * 32 + lane];
+    const float xwl = s_xw[(kf - 1) * 32 + lane], xel = s_xe[(kf - 1) * 32 + lane];
+    const float ys = s_ys[kf * 32 + lane], yn = s_yn[kf * 32 + lane];
+    const float ysl = s_ys[(kf - 1) * 32 + lane], ynl = s_yn[(kf - 1) * 32 + lane];
+    {
+        const float uh = xw + xe, ul = xwl + xel, vh = ys + yn, vl = ysl + ynl;
+        const float xt = (r2 * uh + r1 * ul) * dzdx;
+        const float yt = (r2 * vh + r1 * vl) * dzdy;
+        d3 = ((0.5f * (xt + yt)) * height) * gz;
+    }
+    ha = 0.0f;
+    if (adv) {
+        const float uh = rk * xw + rk * xe, ul = rl * xwl + rl * xel;
+        const float vh = rk * ys + rk * yn, vl = rl * ysl + rl * ynl;
+        const float xt = (r2 * uh + r1 * ul) * dzdx;
+        const float yt = (r2 * vh + r1 * vl) * dzdy;
+        ha = (((0.5f * (xt + yt)) * height) * gz) * rrf0;
+    }
+}
+
+__global__ void __launch_bounds__(32 * kTosWarps, 2) tos_column_kernel(TosArgs p) {
     extern __shared__ float sh[];
     const Ix X{p.ni, p.nj};
     const int ni = p.ni, nj = p.nj, nk = p.nk, L = nk + 2;
@@ -309,104 +341,90 @@ __global__ void __launch_bounds__(32 * kTosWarps, 1) tos_column_kernel(TosArgs p
     const bool do_adv = p.abl & GM1B_TOS_PRESSURE_ADVECTION;
     const bool do_imp = p.abl & GM1B_TOS_IMPLICIT_SOLVE;
     float *s_xw = sh, *s_xe = s_xw + L * 32, *s_ys = s_xe + L * 32, *s_yn = s_ys + L * 32;
-    float *s_w = s_yn + L * 32, *s_d3 = s_w + L * 32, *s_ha = s_d3 + L * 32, *s_fpk = s_ha + L * 32;
-    float *s_a1 = s_fpk + L * 32, *s_a2 = s_a1 + L * 32, *s_mm = s_a2 + L * 32, *s_pp = s_mm + L * 32;
-    float *s_aa = s_xw, *s_bb = s_xe, *s_cc = s_ys, *s_dd = s_yn, *s_ed = s_d3;
+    float *s_w = s_yn + L * 32, *s_fpk = s_w + L * 32, *s_a1 = s_fpk + L * 32, *s_a2 = s_a1 + L * 32;
+    float *s_pp = s_a2 + L * 32, *s_ed = s_pp + L * 32;
+    float *s_aa = s_xw, *s_bb = s_xe, *s_cc = s_ys, *s_dd = s_yn;
 #define SM(arr, k) arr[(k) * 32 + lane]
     float gz = 0.0f, dzdx = 0.0f, dzdy = 0.0f;
     if (live) {
-        gz = m.gz[X.h(j0, i0)];
-        dzdx = m.dzdx[X.h(j0, i0)];
-        dzdy = m.dzdy[X.h(j0, i0)];
+        gz = __ldg(m.gz + X.h(j0, i0));
+        dzdx = __ldg(m.dzdx + X.h(j0, i0));
+        dzdy = __ldg(m.dzdy + X.h(j0, i0));
     }
     // A1: face velocities over the terrain factor, w, and the surface w
     if (live) {
-        const float rgw = m.rgzu[(size_t)j0 * (ni + 1) + i0], rge = m.rgzu[(size_t)j0 * (ni + 1) + i0 + 1];
-        const float rgs = m.rgzv[(size_t)j0 * ni + i0], rgn = m.rgzv[(size_t)(j0 + 1) * ni + i0];
+        const float rgw = __ldg(m.rgzu + (size_t)j0 * (ni + 1) + i0), rge = __ldg(m.rgzu + (size_t)j0 * (ni + 1) + i0 + 1);
+        const float rgs = __ldg(m.rgzv + (size_t)j0 * ni + i0), rgn = __ldg(m.rgzv + (size_t)(j0 + 1) * ni + i0);
+#pragma unroll 4
         for (int k = 1 + wy; k <= nk + 1; k += kTosWarps) {
+            const float wv = a.w3d[X.w(k, y, x)];
             if (k > nk) {
-                SM(s_w, k) = a.w3d[X.w(k, y, x)];
+                SM(s_w, k) = wv;
                 continue;
             }
-            const float uw = a.u3d[X.u(k, y, x)], ue = a.u3d[X.u(k, y, x + 1)];
-            const float vs = a.v3d[X.v(k, y, x)], vn = a.v3d[X.v(k, y + 1, x)];
+            const float uw = __ldg(a.u3d + X.u(k, y, x)), ue = __ldg(a.u3d + X.u(k, y, x + 1));
+            const float vs = __ldg(a.v3d + X.v(k, y, x)), vn = __ldg(a.v3d + X.v(k, y + 1, x));
             SM(s_xw, k) = uw * rgw;
             SM(s_xe, k) = ue * rge;
             SM(s_ys, k) = vs * rgs;
             SM(s_yn, k) = vn * rgn;
-            if (k == 1) {  // bc.F:1151-1178, the surface w of this small step
-                const float ut = (uw + ue) * dzdx, vt = (vs + vn) * dzdy;
-                const float ws = (0.5f * (ut + vt)) * gz;
-                a.w3d[X.w(1, y, x)] = ws;
-                SM(s_w, 1) = ws;
-            } else {
-                SM(s_w, k) = a.w3d[X.w(k, y, x)];
-            }
-        }
-        if (wy == 0) {
-            SM(s_d3, 1) = 0.0f;
-            SM(s_d3, nk + 1) = 0.0f;
-            SM(s_ha, 1) = 0.0f;
-            SM(s_ha, nk + 1) = 0.0f;
+            // bc.F:1151-1178: the surface w of this small step (stored in phase C)
+            SM(s_w, k) = k == 1 ? (0.5f * ((uw + ue) * dzdx + (vs + vn) * dzdy)) * gz : wv;
         }
     }
     __syncthreads();
-    // A2: dum3 and hadvp on the interior w levels
+    // A2: divergence, fpk (initial + pi' advection), column coefficients
     if (live) {
-        for (int kf = 2 + wy; kf <= nk; kf += kTosWarps) {
-            const float r2 = (sigf(kf, p.dz) - sig(kf - 1, p.dz)) * rds(kf, p.dz);
-            const float r1 = 1.0f - r2;
-            const float height = (sigf(kf, p.dz) - p.zt) * p.rzt;
-            const float xw = SM(s_xw, kf), xe = SM(s_xe, kf), xwl = SM(s_xw, kf - 1), xel = SM(s_xe, kf - 1);
-            const float ys = SM(s_ys, kf), yn = SM(s_yn, kf), ysl = SM(s_ys, kf - 1), ynl = SM(s_yn, kf - 1);
-            {
-                const float uh = xw + xe, ul = xwl + xel, vh = ys + yn, vl = ysl + ynl;
-                const float xt = (r2 * uh + r1 * ul) * dzdx;
-                const float yt = (r2 * vh + r1 * vl) * dzdy;
-                const float d3 = ((0.5f * (xt + yt)) * height) * gz;
-                SM(s_d3, kf) = d3;
-                if (dlast) a.dum3[X.p(kf, j, i)] = d3;
-            }
-            if (do_adv) {
-                const float rk = m.rho0_3d[X.m(kf - 1, 0, 0)], rl = m.rho0_3d[X.m(kf - 2, 0, 0)];
-                const float uh = rk * xw + rk * xe, ul = rl * xwl + rl * xel;
-                const float vh = rk * ys + rk * yn, vl = rl * ysl + rl * ynl;
-                const float xt = (r2 * uh + r1 * ul) * dzdx;
-                const float yt = (r2 * vh + r1 * vl) * dzdy;
-                const float ha = (((0.5f * (xt + yt)) * height) * gz) * m.rrf0[X.m(kf - 1, j0, i0)];
-                SM(s_ha, kf) = ha;
-                if (dlast) a.hadvp[X.p(kf, j, i)] = ha;
-            }
-        }
-    }
-    __syncthreads();
-    // A3: divergence, fpk (initial + pi' advection), column coefficients
-    if (live) {
+#pragma unroll 2
         for (int k = 1 + wy; k <= nk; k += kTosWarps) {
             const size_t c = X.p(k, j, i);
+            const float rk = do_adv ? __ldg(m.rho0_3d + X.m(k - 1, 0, 0)) : 0.0f;
+            const float rl = (do_adv && k >= 2) ? __ldg(m.rho0_3d + X.m(k - 2, 0, 0)) : 0.0f;
+            const float rk1 = (do_adv && k < nk) ? __ldg(m.rho0_3d + X.m(k, 0, 0)) : 0.0f;
+            const float rrf_k = (do_adv && k >= 2) ? __ldg(m.rrf0 + X.m(k - 1, j0, i0)) : 0.0f;
+            const float rrf_k1 = (do_adv && k < nk) ? __ldg(m.rrf0 + X.m(k, j0, i0)) : 0.0f;
+            const float qk = __ldg(a.qk + c), pk1 = __ldg(a.pk1 + c), pk2 = __ldg(a.pk2 + c);
+            const float ppten = __ldg(a.ppten + c), ppterm = __ldg(a.ppterm + c);
+            const float pp = a.pp3d[c];
+            float pc = 0.0f, pe = 0.0f, pw = 0.0f, pn = 0.0f, ps = 0.0f, rr0 = 0.0f;
+            if (do_adv) {
+                pc = __ldg(a.piadv + c);
+                pe = __ldg(a.piadv + c + 1);
+                pw = __ldg(a.piadv + c - 1);
+                pn = __ldg(a.piadv + X.p(k, j + 1, i));
+                ps = __ldg(a.piadv + X.p(k, j - 1, i));
+                rr0 = __ldg(m.rr0 + X.m(k - 1, j0, i0));
+            }
+            float d3k = 0.0f, d3k1 = 0.0f, hak = 0.0f, hak1 = 0.0f;
+            if (k >= 2) tos_level_terms(s_xw, s_xe, s_ys, s_yn, lane, k, p, dzdx, dzdy, gz, rk, rl, rrf_k, do_adv, d3k, hak);
+            if (k < nk)
+                tos_level_terms(s_xw, s_xe, s_ys, s_yn, lane, k + 1, p, dzdx, dzdy, gz, rk1, rk, rrf_k1, do_adv, d3k1,
+                                hak1);
+            if (dlast && k >= 2) {
+                a.dum3[c] = d3k;
+                if (do_adv) a.hadvp[c] = hak;
+            }
             const float xw = SM(s_xw, k), xe = SM(s_xe, k), ys = SM(s_ys, k), yn = SM(s_yn, k);
             float div = 0.0f;
             if (do_div) {
                 const float hz = (xe - xw) * p.rdx + (yn - ys) * p.rdy;
-                const float vt = (SM(s_d3, k + 1) - SM(s_d3, k)) * rdsf(k, p.dz);
+                const float vt = (d3k1 - d3k) * rdsf(k, p.dz);
                 div = gz * (hz + vt);
                 if (fabsf(div) < 1.0e-20f) div = 0.0f;
             }
-            const float w1 = k == 1 ? 0.0f : SM(s_w, k), w2 = k == nk ? 0.0f : SM(s_w, k + 1);
-            const float qk = a.qk[c], pk1 = a.pk1[c], pk2 = a.pk2[c];
-            const float src = p.dts * (a.ppten[c] - a.ppterm[c] * div);
+            const float wk = SM(s_w, k), wk1 = SM(s_w, k + 1);
+            const float w1 = k == 1 ? 0.0f : wk, w2 = k == nk ? 0.0f : wk1;
+            const float src = p.dts * (ppten - ppterm * div);
             float fpk = src + p.beta * ((-qk) * (w2 - w1));
             if (dlast) a.divh[c] = div;
             if (do_adv) {
-                const float rho = m.rho0_3d[X.m(k - 1, 0, 0)];
-                const float u2 = p.temx * (rho * xe), u1 = p.temx * (rho * xw);
-                const float v2 = p.temy * (rho * yn), v1 = p.temy * (rho * ys);
-                const float ww2 = SM(s_ha, k + 1) + p.beta * SM(s_w, k + 1);
-                const float ww1 = SM(s_ha, k) + p.beta * SM(s_w, k);
-                const float pc = a.piadv[c];
-                const float xa = u2 * (a.piadv[c + 1] - pc) + u1 * (pc - a.piadv[c - 1]);
-                const float ya = v2 * (a.piadv[X.p(k, j + 1, i)] - pc) + v1 * (pc - a.piadv[X.p(k, j - 1, i)]);
-                float hz = (-(xa + ya)) * m.rr0[X.m(k - 1, j0, i0)];
+                const float u2 = p.temx * (rk * xe), u1 = p.temx * (rk * xw);
+                const float v2 = p.temy * (rk * yn), v1 = p.temy * (rk * ys);
+                const float ww2 = hak1 + p.beta * wk1;
+                const float ww1 = hak + p.beta * wk;
+                const float xa = u2 * (pe - pc) + u1 * (pc - pw);
+                const float ya = v2 * (pn - pc) + v1 * (pc - ps);
+                float hz = (-(xa + ya)) * rr0;
                 hz = hz * gz;
                 const float vt = ww1 * pk1 + ww2 * pk2;
                 fpk = fpk + (hz + vt);
@@ -415,21 +433,23 @@ __global__ void __launch_bounds__(32 * kTosWarps, 1) tos_column_kernel(TosArgs p
             SM(s_fpk, k) = fpk;
             SM(s_a1, k) = pk1 + qk;
             SM(s_a2, k) = pk2 - qk;
-            SM(s_mm, k) = a.mm[c];
-            SM(s_pp, k) = a.pp3d[c];
+            SM(s_pp, k) = pp;
         }
     }
     __syncthreads();
-    // A4: tridiagonal coefficients and right-hand side, k = 2..nk
+    // A3: tridiagonal coefficients and right-hand side, k = 2..nk
     if (live && do_imp) {
+#pragma unroll 2
         for (int k = 2 + wy; k <= nk; k += kTosWarps) {
-            const float mmk = SM(s_mm, k);
+            const size_t c = X.p(k, j, i);
+            const float mmk = __ldg(a.mm + c);
+            const float wt = __ldg(a.wten + X.w(k, y, x));
             const float aa = k >= 3 ? (-p.asq) * (mmk * SM(s_a1, k - 1)) : 0.0f;
             const float cc = k < nk ? (-p.asq) * ((-mmk) * SM(s_a2, k)) : 0.0f;
             const float dg = (-SM(s_a1, k)) + SM(s_a2, k - 1);
             const float bb = 1.0f - p.asq * (mmk * dg);
             const float pd = SM(s_pp, k) - SM(s_pp, k - 1);
-            const float fwk = p.dts * a.wten[X.w(k, y, x)] + p.beta * ((-mmk) * pd);
+            const float fwk = p.dts * wt + p.beta * ((-mmk) * pd);
             const float ud = (SM(s_pp, k) + SM(s_fpk, k)) - (SM(s_pp, k - 1) + SM(s_fpk, k - 1));
             const float dd = (SM(s_w, k) + fwk) + p.alph * ((-mmk) * ud);
             SM(s_aa, k) = aa;
@@ -437,7 +457,6 @@ __global__ void __launch_bounds__(32 * kTosWarps, 1) tos_column_kernel(TosArgs p
             SM(s_cc, k) = cc;
             SM(s_dd, k) = dd;
             if (dlast) {
-                const size_t c = X.p(k, j, i);
                 a.tri_aa[c] = aa;
                 a.tri_bb[c] = bb;
                 a.tri_cc[c] = cc;
@@ -446,13 +465,14 @@ __global__ void __launch_bounds__(32 * kTosWarps, 1) tos_column_kernel(TosArgs p
         }
     }
     __syncthreads();
-    // B: Thomas sweep, one lane per column
+    // B: Thomas sweep, one lane per column (1/pivot by the correctly rounded
+    // reciprocal, the same word as 1.0f / pivot)
     if (live && do_imp && wy == 0) {
         float ec = 0.0f, ed = 0.0f;
         for (int k = 2; k <= nk; ++k) {
             const float aa = SM(s_aa, k), bb = SM(s_bb, k), cc = SM(s_cc, k), dd = SM(s_dd, k);
             const float piv = k == 2 ? bb : aa * ec + bb;
-            const float inv = 1.0f / piv;
+            const float inv = __frcp_rn(piv);
             if (dlast) a.tri_pivot[X.p(k, j, i)] = piv;
             if (k < nk) {
                 ec = (-cc) * inv;
@@ -471,14 +491,19 @@ __global__ void __launch_bounds__(32 * kTosWarps, 1) tos_column_kernel(TosArgs p
     if (live) {
         const bool fill = p.n < p.nloop && (p.abl & GM1B_TOS_BETWEEN_STEP_FILL);
         const bool east = i == ni, north = j == nj;
+#pragma unroll 2
         for (int k = 1 + wy; k <= nk; k += kTosWarps) {
             const size_t c = X.p(k, j, i);
+            const size_t qu = X.u(k, y, x), qv = X.v(k, y, x), qw = X.w(k, y, x);
+            const float uu = __ldg(a.u3d + qu), vv = __ldg(a.v3d + qv);
+            const float ru = a.rru[qu], rv = a.rrv[qv], rw = a.rrw[qw];
             const float wk = SM(s_w, k), wk1 = SM(s_w, k + 1);
+            if (k == 1) a.w3d[qw] = wk;
             if (do_imp && k >= 2) {
-                a.w3d[X.w(k, y, x)] = wk;
+                a.w3d[qw] = wk;
                 if (dlast) {
                     float lhs = SM(s_aa, k) * SM(s_w, k - 1) + SM(s_bb, k) * wk;
-                    const float cc = k < nk ? (-p.asq) * ((-SM(s_mm, k)) * SM(s_a2, k)) : 0.0f;
+                    const float cc = k < nk ? (-p.asq) * ((-__ldg(a.mm + c)) * SM(s_a2, k)) : 0.0f;
                     lhs = lhs + cc * wk1;
                     a.tri_residual[c] = lhs - SM(s_dd, k);
                 }
@@ -508,20 +533,24 @@ __global__ void __launch_bounds__(32 * kTosWarps, 1) tos_column_kernel(TosArgs p
                 }
             }
             // rru/rrv/rrw over faces 1..ni+1 and rows 1..nj+1
+            {
+                const float su = ru + uu, sv = rv + vv, sw = rw + (last ? wk * p.alph : wk);
+                a.rru[qu] = last ? su * p.tavg : su;
+                a.rrv[qv] = last ? sv * p.tavg : sv;
+                a.rrw[qw] = last ? sw * p.tavg : sw;
+            }
+            if (east || north) {
 #pragma unroll
-            for (int dy = 0; dy < 2; ++dy) {
-                if (dy == 1 && !north) break;
-#pragma unroll
-                for (int dx = 0; dx < 2; ++dx) {
-                    if (dx == 1 && !east) break;
-                    const size_t qu = X.u(k, y + dy, x + dx), qv = X.v(k, y + dy, x + dx), qw = X.w(k, y + dy, x + dx);
-                    const float uu = a.u3d[qu], vv = a.v3d[qv];
-                    const float ww = (dy == 0 && dx == 0) ? wk : a.w3d[qw];
-                    const float su = a.rru[qu] + uu, sv = a.rrv[qv] + vv;
-                    const float sw = a.rrw[qw] + (last ? ww * p.alph : ww);
-                    a.rru[qu] = last ? su * p.tavg : su;
-                    a.rrv[qv] = last ? sv * p.tavg : sv;
-                    a.rrw[qw] = last ? sw * p.tavg : sw;
+                for (int e = 1; e < 4; ++e) {
+                    const int dx = e & 1, dy = e >> 1;
+                    if ((dx && !east) || (dy && !north)) continue;
+                    const size_t eu = X.u(k, y + dy, x + dx), ev = X.v(k, y + dy, x + dx), ew = X.w(k, y + dy, x + dx);
+                    const float su = a.rru[eu] + __ldg(a.u3d + eu), sv = a.rrv[ev] + __ldg(a.v3d + ev);
+                    const float wv = a.w3d[ew];
+                    const float sw = a.rrw[ew] + (last ? wv * p.alph : wv);
+                    a.rru[eu] = last ? su * p.tavg : su;
+                    a.rrv[ev] = last ? sv * p.tavg : sv;
+                    a.rrw[ew] = last ? sw * p.tavg : sw;
                 }
             }
         }

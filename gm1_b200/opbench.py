@@ -1,6 +1,7 @@
 """Per-operator device throughput on B200 (library profiling facility).
 
-    python -m gm1_b200.opbench [--ops adv5 adv5-weno massflux calcdef moistnm courant] [--grid 256 256 80] [--iters 20]
+    python -m gm1_b200.opbench [--ops adv5 adv5-weno massflux calcdef moistnm courant tos tos-diag]
+                               [--grid 256 256 80] [--iters 20] [--nsound 10]
 
 For each operator: seeded synthetic inputs of the given padded-lane grid
 resident in HBM, a 256 MiB L2 flush before every launch, CUDA events around
@@ -37,7 +38,18 @@ ALG_WORDS = {
     "courant": 3,
 }
 
+
+def tos_words(nloop: int) -> int:
+    """Words per cell of one terrain/open acoustic stage: the prepare pass
+    (in: ppx ppi ua va wa ppterm piadv c1 c2 rf0 rr0 thv; out: ppd pp3d rru
+    rrv rrw u v w qk pk1 pk2 mm) and per small step the pressure gradient
+    (in: ppd thv uten vten gxu gyv u v; out: u v) and the column pass (in: u
+    v w pp3d qk pk1 pk2 mm ppten ppterm piadv rr0 rrf0 wten rru rrv rrw;
+    out: w pp3d ppd rru rrv rrw)."""
+    return 24 + 33 * nloop
+
 _COMPACT: dict = {}
+NSOUND = [10]
 
 
 def compact_inputs(op: str, ni: int, nj: int, nk: int, device: torch.device) -> dict:
@@ -75,6 +87,50 @@ def compact_inputs(op: str, ni: int, nj: int, nk: int, device: torch.device) -> 
              "out": torch.empty(1, device=device)}
     _COMPACT[key] = a
     return a
+
+
+def tos_inputs(ni: int, nj: int, nk: int, device: torch.device, diag: bool) -> tuple[dict, dict]:
+    """Seeded terrain/open acoustic-stage state and metrics (built once)."""
+    key = ("tos", ni, nj, nk, diag)
+    if key in _COMPACT:
+        return _COMPACT[key]
+    from .terrain_open import COLUMN_DIAGNOSTIC_NAMES, terrain_open_sound_shapes, terrain_static_shapes  # noqa: PLC0415
+
+    g = torch.Generator(device=device).manual_seed(5)
+
+    def r(shape, lo, hi):
+        return torch.rand(shape, generator=g, device=device) * (hi - lo) + lo
+
+    sh = terrain_open_sound_shapes(ni, nj, nk)
+    a = {n: r(s, -0.5, 0.5) for n, s in sh.items()}
+    for n in ("ppi", "pp3d", "ppx"):
+        a[n] = r(sh[n], -2e-4, 2e-4)
+    a["piadv"] = r(sh["piadv"], 0.89, 0.91)
+    a["ppterm"] = a["piadv"] * 0.4
+    a["thv"] = r(sh["thv"], 299.0, 331.0)
+    a["ppten"] = r(sh["ppten"], -1e-6, 1e-6)
+    for n, lo, hi in (("u3d", 4.0, 12.0), ("v3d", -6.0, 2.0), ("w3d", -0.5, 0.5)):
+        a[n] = r(sh[n], lo, hi)
+        a[n[0] + "a"] = a[n] + r(sh[n], -0.05, 0.05)
+    for n in ("uten", "vten", "wten"):
+        a[n] = r(sh[n], -2e-3, 2e-3)
+    a["radbcw"], a["radbcs"] = r(sh["radbcw"], -25.0, 0.0), r(sh["radbcs"], -25.0, 0.0)
+    a["radbce"], a["radbcn"] = r(sh["radbce"], 0.0, 25.0), r(sh["radbcn"], 0.0, 25.0)
+    for n in ("uh", "vh", "ruf", "rvf"):
+        a[n] = torch.ones(sh[n], device=device)
+    if not diag:
+        for n in COLUMN_DIAGNOSTIC_NAMES:
+            a[n] = torch.zeros((1,), device=device)
+    ms = terrain_static_shapes(ni=ni, nj=nj, nk=nk)
+    m = {n: r(s, 0.95, 1.05) for n, s in ms.items()}
+    m["c1"] = r(ms["c1"], 0.4, 0.6)
+    m["c2"] = 1.0 - m["c1"]
+    for n in ("dzdx", "dzdy"):
+        m[n] = r(ms[n], -0.02, 0.02)
+    for n in ("gx", "gxu", "gy", "gyv"):
+        m[n] = r(ms[n], -0.005, 0.005)
+    _COMPACT[key] = (a, m)
+    return a, m
 
 
 def hbm_peak() -> tuple[float, str]:
@@ -137,6 +193,14 @@ def run(op: str, a: dict[str, torch.Tensor], ni: int, nj: int, nk: int, stream: 
         advective_courant_number(u=c["u"], v=c["v"], w=c["w"], uh=c["uh"], vh=c["vh"], mh=c["mh"], dt_s=6.0,
                                  dx_m=1000.0, dy_m=1000.0, dz_m=250.0, level_keys=c["keys"], stream=stream,
                                  out=c["out"])
+    elif op in ("tos", "tos-diag"):
+        from .terrain_open import compile_cuda_psolver3_terrain_open, launch_cuda_psolver3_terrain_open_stage  # noqa: PLC0415
+
+        diag = op == "tos-diag"
+        st, m = tos_inputs(ni, nj, nk, a["u3d"].device, diag)
+        launch_cuda_psolver3_terrain_open_stage(
+            st, m, ni=ni, nj=nj, nk=nk, nrk=3, dt=6.0, nsound=NSOUND[0], dx=1000.0, dy=1000.0, dz=250.0,
+            compiled=compile_cuda_psolver3_terrain_open(retain_column_diagnostics=diag), stream=stream)
     else:
         raise ValueError(op)
 
@@ -148,7 +212,9 @@ def main() -> None:
     ap.add_argument("--iters", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--chunk", type=int, default=None)
+    ap.add_argument("--nsound", type=int, default=10, help="acoustic substeps of the terrain/open stage (nrk=3)")
     args = ap.parse_args()
+    NSOUND[0] = args.nsound
     ni, nj, nk = args.grid
     device = torch.device("cuda", 0)
     a = synthetic_padded(ni, nj, nk, device)
@@ -169,10 +235,11 @@ def main() -> None:
                 ends[q].record(stream)
         stream.synchronize()
         ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends)) / args.iters
-        alg = ALG_WORDS[op] * 4 * cells
+        words = tos_words(args.nsound) if op.startswith("tos") else ALG_WORDS[op]
+        alg = words * 4 * cells
         gbs = alg / (ms * 1e-3) / 1e9
         print(json.dumps({"op": op, "grid": [ni, nj, nk], "cells": cells, "ms_per_launch": ms,
-                          "cells_per_s": cells / (ms * 1e-3), "alg_bytes_per_cell": ALG_WORDS[op] * 4,
+                          "cells_per_s": cells / (ms * 1e-3), "alg_bytes_per_cell": words * 4,
                           "achieved_gbs": gbs, "peak_gbs": peak, "frac": gbs / peak, "peak_source": kind,
                           "chunk": args.chunk}), flush=True)
 

@@ -107,7 +107,7 @@ def test_compact_mode_prognostics_match_and_skip_scratch():
 
 
 def test_oversized_column_refused_by_the_library():
-    ni, nj, nk = 4, 4, 141
+    ni, nj, nk = 4, 4, 161
     a, m = terrain_open_fixture(ni, nj, nk, 3)
     dev, mdev = _dev(a), _dev(m)
     with pytest.raises(Gm1bError, match="nk"):
