@@ -555,3 +555,111 @@ extern "C" int32_t gm1b_kessler_driver_static(int32_t ni, int32_t nj, int32_t nk
     }
     return GM1B_OK;
 }
+
+// ---------------------------------------------------------------------------
+// once-per-large-step Kessler transition (cpu_gm1_kessler_large_step_inplace,
+// src/cm1core/cuda_gm1_kessler_large_step.py:183-292): with equation set 2
+// the previous held rates are removed from pp3d/th3d/qv/qc and each carrier
+// takes the pre-physics state (solve2.F:1561-1579); the pre-physics pressure
+// and moist density follow (solve2.F:1582-1595), rr takes the density, the
+// driver runs, and the carriers become the next step's held rates
+// (solve3.F:319-337).  Two elementwise launches around the driver.
+// ---------------------------------------------------------------------------
+namespace gm1b {
+namespace {
+
+struct KesslerEos {
+    float cpdrd, p00, rd, rv;
+};
+
+__global__ void __launch_bounds__(256) kessler_pre_physics_kernel(gm1b_kessler_arrays a, gm1b_kessler_held h,
+                                                                  size_t n, float dt, int eqt2, KesslerEos c) {
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+        float pp = a.pp3d[q], th = a.th3d[q], qv = a.qv[q];
+        if (eqt2) {
+            float *state[4] = {&pp, &th, &qv, nullptr};
+            float *rate[4] = {h.qpten, h.qtten, h.qvten, h.qcten};
+            float qc = a.qc[q];
+            state[3] = &qc;
+#pragma unroll
+            for (int s = 0; s < 4; ++s) {
+                const float w = rate[s][q] * dt;
+                *state[s] = *state[s] - w;
+                rate[s][q] = *state[s];
+            }
+            a.pp3d[q] = pp;
+            a.th3d[q] = th;
+            a.qv[q] = qv;
+            a.qc[q] = qc;
+        }
+        const float pi = a.pi0[q] + pp;
+        float prs = powf(pi, c.cpdrd);
+        prs = prs * c.p00;
+        float rho = a.th0[q] + th;
+        rho = rho * pi;
+        float w = fmaxf(qv, 0.0f);
+        w = w * c.rv;
+        w = w + c.rd;
+        rho = rho * w;
+        rho = prs / rho;
+        a.prs[q] = prs;
+        a.rho[q] = rho;
+        const_cast<float *>(a.rr)[q] = rho;
+    }
+}
+
+__global__ void __launch_bounds__(256) kessler_recapture_kernel(gm1b_kessler_arrays a, gm1b_kessler_held h, size_t n,
+                                                                float dt) {
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+        h.qpten[q] = (a.pp3d[q] - h.qpten[q]) / dt;
+        h.qtten[q] = (a.th3d[q] - h.qtten[q]) / dt;
+        h.qvten[q] = (a.qv[q] - h.qvten[q]) / dt;
+        h.qcten[q] = (a.qc[q] - h.qcten[q]) / dt;
+    }
+}
+
+}  // namespace
+}  // namespace gm1b
+
+extern "C" int32_t gm1b_kessler_large_step(int32_t ni, int32_t nj, int32_t nk, const gm1b_kessler_arrays *arrays,
+                                           const gm1b_kessler_held *held, float dx, float dy, float dz, float dt,
+                                           int32_t equation_set, int32_t efall, void *workspace,
+                                           size_t workspace_size, void *stream) {
+    if (arrays == nullptr || ni < 1 || nj < 1 || nk < 2) {
+        gm1b_set_error("gm1b_kessler_large_step: need arrays, ni >= 1, nj >= 1, nk >= 2");
+        return GM1B_ERR_ARGUMENT;
+    }
+    const bool eqt2 = equation_set == 2;
+    if (eqt2 && (held == nullptr || held->qpten == nullptr || held->qtten == nullptr || held->qvten == nullptr ||
+                 held->qcten == nullptr)) {
+        gm1b_set_error("gm1b_kessler_large_step: equation set 2 needs the four held-rate carriers");
+        return GM1B_ERR_ARGUMENT;
+    }
+    if (!(dt > 0.0f) || !isfinite(dt)) {
+        gm1b_set_error("gm1b_kessler_large_step: dt must be finite and > 0");
+        return GM1B_ERR_ARGUMENT;
+    }
+    const gm1b_kessler_held none{nullptr, nullptr, nullptr, nullptr};
+    const gm1b_kessler_held h = eqt2 ? *held : none;
+    const size_t n = (size_t)ni * nj * nk;
+    // CM1 constants.F: cpdrd = cp / rd of the default-real operands
+    const float cp = 1005.7f, rd = 287.04f;
+    const KesslerEos c{(float)((double)cp / (double)rd), 100000.0f, rd, 461.5f};
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const unsigned grid = (unsigned)std::min<size_t>((n + 255) / 256, (size_t)148 * 8);
+    {
+        ProfScope ps("kessler_pre_physics_kernel", st);
+        kessler_pre_physics_kernel<<<grid, 256, 0, st>>>(*arrays, h, n, dt, eqt2 ? 1 : 0, c);
+        ps.stop();
+    }
+    if (!launched("kessler_pre_physics_kernel")) return GM1B_ERR_CUDA;
+    const int32_t rc = gm1b_kessler_driver(ni, nj, nk, arrays, dx, dy, dz, dt, equation_set, efall, workspace,
+                                           workspace_size, stream);
+    if (rc != GM1B_OK || !eqt2) return rc;
+    {
+        ProfScope ps("kessler_recapture_kernel", st);
+        kessler_recapture_kernel<<<grid, 256, 0, st>>>(*arrays, h, n, dt);
+        ps.stop();
+    }
+    return launched("kessler_recapture_kernel") ? GM1B_OK : GM1B_ERR_CUDA;
+}

@@ -1,0 +1,842 @@
+// moist_step.cu - sm_100a kernels that join the operators of the moist
+// large step on the padded (ng = 3) open lane.
+//
+// Behaviour followed (reference file:line):
+//   open-lateral halo fills bcp/bcs/bcu/bcv/bcw     src/cm1core/cuda_sound3_open_boundary.py:249-335
+//   moist buoyancy, getdiv, getdivx                 src/cm1core/cuda_moist_stage_bridge.py:160-194 (kernel
+//                                                   source), launchers :433-501
+//   final-stage moisture pdef chain (WENO face fluxes, directional advection,
+//   candidate/correction per direction, total)     src/cm1core/cuda_scalar_moist_rk.py:560-700 (kernel
+//                                                   source), launcher :1336-1500
+//   held-tendency composition                       src/cm1core/cuda_gm1_child_step_composer.py:547-556
+//   solve3 density                                  src/cm1core/cuda_gm1_forecast.py:548 (gm1_solve3_density_v1)
+//
+// Design (B200): each piece is an elementwise or per-line pass with the
+// reference's operation order; the open fills run as the reference's two
+// ordered passes (first direction of the family, then the second), so a
+// halo corner takes the words CM1's sequential loops leave there.
+#include "gm1b_common.cuh"
+#include "weno.cuh"
+
+namespace gm1b {
+namespace {
+
+bool launch_ok(const char *what) {
+    const cudaError_t e = cudaPeekAtLastError();
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        gm1b_set_error("%s: %s", what, cudaGetErrorString(e));
+        return false;
+    }
+    return true;
+}
+
+unsigned grid_for(size_t work) {
+    return (unsigned)std::max<size_t>(1, std::min<size_t>((work + 255) / 256, (size_t)148 * 16));
+}
+
+// ---------------------------------------------------------------------------
+// open-lateral halo fills
+// ---------------------------------------------------------------------------
+struct FillGeom {
+    float *q;
+    int nx, ny;          // row length and rows per level
+    int g;               // halo width (3 on the padded lane, 1 for the pressure family)
+    int x0, xl, y0, yl;  // first and last live column / row
+    int k0, k1;          // levels filled
+    int ew_first;        // west/east pass first (all but bcv)
+    int zero_w;          // bcw flag 1: zero levels 1 and nk+1 over rows y0-1..yl+1, columns x0-1..xl+1
+    int nk;
+};
+
+// one pass: ew = 1 fills the west/east halo columns of rows y0-1..yl+1,
+// ew = 0 the south/north halo rows of columns x0-1..xl+1
+__global__ void __launch_bounds__(256) open_fill_pass_kernel(FillGeom f, int ew, int zero) {
+    const int nlev = f.k1 - f.k0 + 1;
+    const size_t lines = ew ? (size_t)(f.yl - f.y0 + 3) : (size_t)(f.xl - f.x0 + 3);
+    const size_t per = lines * (size_t)(2 * f.g);
+    const size_t total = per * nlev;
+    const size_t plane = (size_t)f.ny * f.nx;
+    for (size_t z = (size_t)blockIdx.x * blockDim.x + threadIdx.x; z < total; z += (size_t)gridDim.x * blockDim.x) {
+        const int h = (int)(z % (2 * f.g));
+        const int l = (int)((z / (2 * f.g)) % lines);
+        const int k = (int)(z / per) + f.k0;
+        float *lev = f.q + (size_t)k * plane;
+        if (ew) {
+            const int y = f.y0 - 1 + l;
+            const int x = h < f.g ? f.x0 - f.g + h : f.xl + 1 + (h - f.g);
+            const int src = h < f.g ? f.x0 : f.xl;
+            lev[(size_t)y * f.nx + x] = lev[(size_t)y * f.nx + src];
+        } else {
+            const int x = f.x0 - 1 + l;
+            const int y = h < f.g ? f.y0 - f.g + h : f.yl + 1 + (h - f.g);
+            const int src = h < f.g ? f.y0 : f.yl;
+            lev[(size_t)y * f.nx + x] = lev[(size_t)src * f.nx + x];
+        }
+    }
+    if (zero) {
+        const size_t rows = (size_t)(f.yl - f.y0 + 3), cols = (size_t)(f.xl - f.x0 + 3);
+        for (size_t z = (size_t)blockIdx.x * blockDim.x + threadIdx.x; z < 2 * rows * cols;
+             z += (size_t)gridDim.x * blockDim.x) {
+            const int x = f.x0 - 1 + (int)(z % cols);
+            const int y = f.y0 - 1 + (int)((z / cols) % rows);
+            const int k = z / (rows * cols) == 0 ? 1 : f.nk + 1;
+            f.q[(size_t)k * plane + (size_t)y * f.nx + x] = 0.0f;
+        }
+    }
+}
+
+bool fill_geometry(int kind, int ni, int nj, int nk, float *q, FillGeom &f) {
+    f = FillGeom{};
+    f.q = q;
+    f.nk = nk;
+    f.k0 = 1;
+    f.k1 = nk;
+    f.ew_first = 1;
+    switch (kind) {
+        case GM1B_FILL_PRESSURE:
+            f.nx = ni + 2, f.ny = nj + 2, f.g = 1, f.x0 = 1, f.xl = ni, f.y0 = 1, f.yl = nj;
+            return true;
+        case GM1B_FILL_SCALAR:
+            f.nx = ni + 6, f.ny = nj + 6, f.g = 3, f.x0 = 3, f.xl = ni + 2, f.y0 = 3, f.yl = nj + 2;
+            return true;
+        case GM1B_FILL_U:
+            f.nx = ni + 7, f.ny = nj + 6, f.g = 3, f.x0 = 3, f.xl = ni + 3, f.y0 = 3, f.yl = nj + 2;
+            return true;
+        case GM1B_FILL_V:
+            f.nx = ni + 6, f.ny = nj + 7, f.g = 3, f.x0 = 3, f.xl = ni + 2, f.y0 = 3, f.yl = nj + 3;
+            f.ew_first = 0;
+            return true;
+        case GM1B_FILL_W:
+        case GM1B_FILL_W_KEEP_ENDS:
+            f.nx = ni + 6, f.ny = nj + 6, f.g = 3, f.x0 = 3, f.xl = ni + 2, f.y0 = 3, f.yl = nj + 2;
+            f.k0 = 2;
+            f.zero_w = kind == GM1B_FILL_W;
+            return true;
+        default:
+            return false;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// moist stage bridge
+// ---------------------------------------------------------------------------
+struct Lane {
+    int ni, nj, nk;
+    __device__ __forceinline__ size_t s(int k, int y, int x) const {  // scalar / w layout, padded coordinates
+        return ((size_t)k * (nj + 6) + y) * (size_t)(ni + 6) + x;
+    }
+    __device__ __forceinline__ size_t u(int k, int y, int x) const {
+        return ((size_t)k * (nj + 6) + y) * (size_t)(ni + 7) + x;
+    }
+    __device__ __forceinline__ size_t v(int k, int y, int x) const {
+        return ((size_t)k * (nj + 7) + y) * (size_t)(ni + 6) + x;
+    }
+    __device__ __forceinline__ size_t m(int k0, int j0, int i0) const {
+        return ((size_t)k0 * nj + j0) * (size_t)ni + i0;
+    }
+};
+
+// dum8 on w levels: c1(kf) dum8(kf-1) + c2(kf) dum8(kf), zero at the ends
+__device__ __forceinline__ float buoy_face(const float *dum8, const float *c1, const float *c2, const Lane &L, int kf,
+                                           int j, int i) {
+    if (kf == 1 || kf == L.nk + 1) return 0.0f;
+    const size_t p = L.m(kf - 1, j, i);
+    return c1[p] * dum8[L.s(kf - 1, j + 3, i + 3)] + c2[p] * dum8[L.s(kf, j + 3, i + 3)];
+}
+
+__global__ void __launch_bounds__(256) msb_buoyancy_kernel(const float *dum8, const float *c1, const float *c2,
+                                                          const float *gxu, const float *gyv, float *uten,
+                                                          float *vten, float *wten, Lane L) {
+    const int ni = L.ni, nj = L.nj, nk = L.nk;
+    const size_t nw = (size_t)(nk - 1) * nj * ni, nu = (size_t)nk * nj * (ni - 1), nv = (size_t)nk * (nj - 1) * ni;
+    for (size_t z = (size_t)blockIdx.x * blockDim.x + threadIdx.x; z < nw + nu + nv; z += (size_t)gridDim.x * blockDim.x) {
+        if (z < nw) {
+            const int i = (int)(z % ni), j = (int)((z / ni) % nj), kf = (int)(z / ((size_t)ni * nj)) + 2;
+            const size_t p = L.m(kf - 1, j, i);
+            const float add = c1[p] * dum8[L.s(kf - 1, j + 3, i + 3)] + c2[p] * dum8[L.s(kf, j + 3, i + 3)];
+            const size_t d = L.s(kf, j + 3, i + 3);
+            wten[d] = wten[d] + add;
+        } else if (z < nw + nu) {
+            const size_t q = z - nw;
+            const int f = (int)(q % (ni - 1)) + 1, j = (int)((q / (ni - 1)) % nj), k = (int)(q / ((size_t)(ni - 1) * nj)) + 1;
+            float t = (buoy_face(dum8, c1, c2, L, k + 1, j, f) + buoy_face(dum8, c1, c2, L, k + 1, j, f - 1)) +
+                      (buoy_face(dum8, c1, c2, L, k, j, f) + buoy_face(dum8, c1, c2, L, k, j, f - 1));
+            t = 0.125f * t;
+            t = t - 0.25f * (dum8[L.s(k, j + 3, f + 3)] + dum8[L.s(k, j + 3, f + 2)]);
+            t = t * (gxu[((size_t)(k - 1) * nj + j) * (ni + 1) + f] + gxu[((size_t)k * nj + j) * (ni + 1) + f]);
+            const size_t d = L.u(k, j + 3, f + 3);
+            uten[d] = uten[d] + t;
+        } else {
+            const size_t q = z - nw - nu;
+            const int i = (int)(q % ni), f = (int)((q / ni) % (nj - 1)) + 1, k = (int)(q / ((size_t)ni * (nj - 1))) + 1;
+            float t = (buoy_face(dum8, c1, c2, L, k + 1, f, i) + buoy_face(dum8, c1, c2, L, k + 1, f - 1, i)) +
+                      (buoy_face(dum8, c1, c2, L, k, f, i) + buoy_face(dum8, c1, c2, L, k, f - 1, i));
+            t = 0.125f * t;
+            t = t - 0.25f * (dum8[L.s(k, f + 3, i + 3)] + dum8[L.s(k, f + 2, i + 3)]);
+            t = t * (gyv[((size_t)(k - 1) * (nj + 1) + f) * ni + i] + gyv[((size_t)k * (nj + 1) + f) * ni + i]);
+            const size_t d = L.v(k, f + 3, i + 3);
+            vten[d] = vten[d] + t;
+        }
+    }
+}
+
+struct Getdiv {
+    const float *rru, *rrv, *rrw, *rgzu, *rgzv, *dzdx, *dzdy, *gz, *thterm;
+    float *div, *theta_div;
+    float rdx, rdy, rdsf, dz, zt, rzt;
+};
+
+__device__ __forceinline__ float gd_xu(const Getdiv &a, const Lane &L, int k, int j, int f) {
+    return a.rru[L.u(k, j + 3, f + 3)] * a.rgzu[(size_t)j * (L.ni + 1) + f];
+}
+__device__ __forceinline__ float gd_yv(const Getdiv &a, const Lane &L, int k, int f, int i) {
+    return a.rrv[L.v(k, f + 3, i + 3)] * a.rgzv[(size_t)f * L.ni + i];
+}
+// transformed w on w levels (getdiv's own grouping: r1 = 0.5 (1 - r2), r2 = 0.5 r2)
+__device__ __forceinline__ float gd_wt(const Getdiv &a, const Lane &L, int kf, int j, int i) {
+    if (kf == 1 || kf == L.nk + 1) return 0.0f;
+    const float rds = 1.0f / a.dz;
+    const float sf = (float)(kf - 1) * a.dz, sm = ((float)(kf - 1) - 0.5f) * a.dz;
+    float r2 = (sf - sm) * rds;
+    const float r1 = 0.5f * (1.0f - r2);
+    r2 = 0.5f * r2;
+    const float ux = r2 * (gd_xu(a, L, kf, j, i) + gd_xu(a, L, kf, j, i + 1)) +
+                     r1 * (gd_xu(a, L, kf - 1, j, i) + gd_xu(a, L, kf - 1, j, i + 1));
+    const float vy = r2 * (gd_yv(a, L, kf, j, i) + gd_yv(a, L, kf, j + 1, i)) +
+                     r1 * (gd_yv(a, L, kf - 1, j, i) + gd_yv(a, L, kf - 1, j + 1, i));
+    float terrain = ux * a.dzdx[(size_t)j * L.ni + i] + vy * a.dzdy[(size_t)j * L.ni + i];
+    terrain = ((terrain * (sf - a.zt)) * a.gz[(size_t)j * L.ni + i]) * (1.0f / a.zt);
+    return a.rrw[L.s(kf, j + 3, i + 3)] + terrain;
+}
+
+__global__ void __launch_bounds__(256) msb_getdiv_kernel(Getdiv a, Lane L) {
+    const size_t n = (size_t)L.nk * L.nj * L.ni;
+    for (size_t z = (size_t)blockIdx.x * blockDim.x + threadIdx.x; z < n; z += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(z % L.ni), j = (int)((z / L.ni) % L.nj), k = (int)(z / ((size_t)L.ni * L.nj)) + 1;
+        float d = (gd_xu(a, L, k, j, i + 1) - gd_xu(a, L, k, j, i)) * a.rdx +
+                  (gd_yv(a, L, k, j + 1, i) - gd_yv(a, L, k, j, i)) * a.rdy;
+        d = d + (gd_wt(a, L, k + 1, j, i) - gd_wt(a, L, k, j, i)) * a.rdsf;
+        if (fabsf(d) < 1.0e-20f) d = 0.0f;
+        a.div[z] = d;
+        a.theta_div[z] = d * a.thterm[z];
+    }
+}
+
+__global__ void __launch_bounds__(256) msb_getdivx_horizontal_kernel(const float *rho0, const float *rgzu,
+                                                                    const float *rgzv, float *rru, float *rrv, Lane L) {
+    const int ni = L.ni, nj = L.nj, nk = L.nk;
+    const size_t nu = (size_t)nk * nj * (ni + 1), nv = (size_t)nk * (nj + 1) * ni;
+    for (size_t z = (size_t)blockIdx.x * blockDim.x + threadIdx.x; z < nu + nv; z += (size_t)gridDim.x * blockDim.x) {
+        if (z < nu) {
+            const int f = (int)(z % (ni + 1)), j = (int)((z / (ni + 1)) % nj), k = (int)(z / ((size_t)(ni + 1) * nj)) + 1;
+            const int l = f == 0 ? 0 : f - 1, r = f == ni ? ni - 1 : f;
+            const float den = 0.5f * (rho0[L.m(k - 1, j, l)] + rho0[L.m(k - 1, j, r)]);
+            const size_t p = L.u(k, j + 3, f + 3);
+            rru[p] = (den * rru[p]) * rgzu[(size_t)j * (ni + 1) + f];
+        } else {
+            const size_t q = z - nu;
+            const int i = (int)(q % ni), f = (int)((q / ni) % (nj + 1)), k = (int)(q / ((size_t)ni * (nj + 1))) + 1;
+            const int s = f == 0 ? 0 : f - 1, nn = f == nj ? nj - 1 : f;
+            const float den = 0.5f * (rho0[L.m(k - 1, s, i)] + rho0[L.m(k - 1, nn, i)]);
+            const size_t p = L.v(k, f + 3, i + 3);
+            rrv[p] = (den * rrv[p]) * rgzv[(size_t)f * ni + i];
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) msb_getdivx_vertical_kernel(const float *rf0, const float *dzdx,
+                                                                  const float *dzdy, const float *gz, const float *rru,
+                                                                  const float *rrv, float *rrw, float dz, Lane L) {
+    const int ni = L.ni, nj = L.nj, nk = L.nk;
+    const size_t n = (size_t)(nk + 1) * nj * ni;
+    const float rds = 1.0f / dz, zt = (float)nk * dz, rzt = 1.0f / zt;
+    for (size_t z = (size_t)blockIdx.x * blockDim.x + threadIdx.x; z < n; z += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(z % ni), j = (int)((z / ni) % nj), kf = (int)(z / ((size_t)ni * nj)) + 1;
+        const size_t p = L.s(kf, j + 3, i + 3);
+        if (kf == 1 || kf == nk + 1) {
+            rrw[p] = 0.0f;
+            continue;
+        }
+        const float sf = (float)(kf - 1) * dz, sm = ((float)(kf - 1) - 0.5f) * dz;
+        float r2 = (sf - sm) * rds;
+        const float r1 = 0.5f * (1.0f - r2);
+        r2 = 0.5f * r2;
+        const float ux = r2 * (rru[L.u(kf, j + 3, i + 3)] + rru[L.u(kf, j + 3, i + 4)]) +
+                         r1 * (rru[L.u(kf - 1, j + 3, i + 3)] + rru[L.u(kf - 1, j + 3, i + 4)]);
+        const float vy = r2 * (rrv[L.v(kf, j + 3, i + 3)] + rrv[L.v(kf, j + 4, i + 3)]) +
+                         r1 * (rrv[L.v(kf - 1, j + 3, i + 3)] + rrv[L.v(kf - 1, j + 4, i + 3)]);
+        float terrain = ux * dzdx[(size_t)j * ni + i] + vy * dzdy[(size_t)j * ni + i];
+        terrain = ((terrain * (sf - zt)) * gz[(size_t)j * ni + i]) * rzt;
+        rrw[p] = rf0[L.m(kf - 1, j, i)] * rrw[p] + terrain;
+    }
+}
+
+__global__ void __launch_bounds__(256) msb_getdivx_divergence_kernel(const float *rru, const float *rrv,
+                                                                    const float *rrw, float *divx, float rdx,
+                                                                    float rdy, float rdsf, Lane L) {
+    const size_t n = (size_t)L.nk * L.nj * L.ni;
+    for (size_t z = (size_t)blockIdx.x * blockDim.x + threadIdx.x; z < n; z += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(z % L.ni), j = (int)((z / L.ni) % L.nj), k = (int)(z / ((size_t)L.ni * L.nj)) + 1;
+        float d = (rru[L.u(k, j + 3, i + 4)] - rru[L.u(k, j + 3, i + 3)]) * rdx +
+                  (rrv[L.v(k, j + 4, i + 3)] - rrv[L.v(k, j + 3, i + 3)]) * rdy;
+        d = d + (rrw[L.s(k + 1, j + 3, i + 3)] - rrw[L.s(k, j + 3, i + 3)]) * rdsf;
+        divx[z] = fabsf(d) < 1.0e-20f ? 0.0f : d;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// final-stage moisture pdef chain
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float max5abs(float a, float b, float c, float d, float e) {
+    return fmaxf(fmaxf(fabsf(a), fabsf(b)), fmaxf(fabsf(c), fmaxf(fabsf(d), fabsf(e))));
+}
+__device__ __forceinline__ unsigned obc_side(unsigned obc, unsigned side) { return (obc >> (4u * side)) & 15u; }
+__device__ __forceinline__ bool obc_owned(int i, int j, int ni, int nj, unsigned obc) {
+    return obc != 0u || (i >= 3 && i + 3 < ni && j >= 3 && j + 3 < nj);
+}
+__device__ __forceinline__ bool inflow_lo(int i, unsigned obc, unsigned side, float m) {
+    return i == 0 && obc_side(obc, side) == 2u && m >= 0.0f;
+}
+__device__ __forceinline__ bool inflow_hi(int i, int n, unsigned obc, unsigned side, float m) {
+    return i + 1 == n && obc_side(obc, side) == 2u && m <= 0.0f;
+}
+// pdef.F:125-166 on a whole row: cell c in [-2, n+1] as bcs fills it (1 periodic, 2 zero gradient, 3/4 mirror)
+__device__ __forceinline__ long long pdef_cell(long long c, long long n, unsigned lo, unsigned hi) {
+    if (c < 0) {
+        if (lo == 1u) return c + n;
+        if (lo == 2u) return 0;
+        return -c - 1;
+    }
+    if (c >= n) {
+        if (hi == 1u) return c - n;
+        if (hi == 2u) return n - 1;
+        return 2 * n - 1 - c;
+    }
+    return c;
+}
+__device__ __forceinline__ float pdef_at(const float *d, long long base, long long stride, long long c, long long n,
+                                         unsigned lo, unsigned hi) {
+    return d[base + pdef_cell(c, n, lo, hi) * stride];
+}
+__device__ __forceinline__ float pdef_ratio(const float *d, long long base, long long stride, long long c, long long n,
+                                            unsigned lo, unsigned hi) {
+    const float v = pdef_at(d, base, stride, c, n, lo, hi);
+    if (v >= 0.0f) return 0.0f;
+    const float f1 = fmaxf(0.0f, pdef_at(d, base, stride, c - 1, n, lo, hi));
+    const float f2 = fmaxf(0.0f, pdef_at(d, base, stride, c + 1, n, lo, hi));
+    const float sum = f1 + f2;
+    return sum > 1.0e-30f ? fmaxf(v, -sum) / sum : 0.0f;
+}
+__device__ __forceinline__ void pdef_row_mass(const float *d, long long base, long long stride, long long c,
+                                              long long n, unsigned lo, unsigned hi, float *mass, bool *flag) {
+    const float v = pdef_at(d, base, stride, c, n, lo, hi);
+    if (v < 0.0f) {
+        const float r = pdef_ratio(d, base, stride, c, n, lo, hi);
+        if (r != 0.0f) {
+            const float sum = fmaxf(0.0f, pdef_at(d, base, stride, c - 1, n, lo, hi)) +
+                              fmaxf(0.0f, pdef_at(d, base, stride, c + 1, n, lo, hi));
+            *mass = 0.0f - sum * r;
+            *flag = true;
+        }
+    } else if (v > 1.0e-30f) {
+        const float rl = pdef_ratio(d, base, stride, c - 1, n, lo, hi);
+        const float rr = pdef_ratio(d, base, stride, c + 1, n, lo, hi);
+        if (rl != 0.0f) {
+            *mass = *mass + v * rl;
+            *flag = true;
+        }
+        if (rr != 0.0f) {
+            *mass = *mass + v * rr;
+            *flag = true;
+        }
+    }
+}
+// interior-only repair row (tile-local launch, obc = 0)
+__device__ __forceinline__ float ratio1(const float *d, long long c, long long lo, long long hi, long long stride) {
+    if (c <= lo || c >= hi || d[c] >= 0.0f) return 0.0f;
+    const float f1 = fmaxf(0.0f, d[c - stride]), f2 = fmaxf(0.0f, d[c + stride]);
+    const float sum = f1 + f2;
+    return sum > 1.0e-30f ? fmaxf(d[c], -sum) / sum : 0.0f;
+}
+
+struct Pdef {
+    const float *a;      // moisture at the stage's A level, compact
+    const float *s;      // the advected moisture, padded scalar layout
+    const float *rho0, *gz, *rgz, *rr0, *c1, *c2, *divx;
+    const float *rru, *rrv, *rrw;
+    float *fx, *fy, *fz;  // face fluxes (u, v, w layouts)
+    float *ax, *ay, *az, *dum, *adv;  // compact
+    float dt, dx, dy, dz, rdx, rdy, rdz, rdt;
+    double weps;
+    unsigned obc;
+    int pdefweno;
+};
+
+__global__ void __launch_bounds__(256) pdef_horizontal_flux_kernel(Pdef p, Lane L) {
+    const int ni = L.ni, nj = L.nj;
+    const size_t n = (size_t)L.nk * (nj + 1) * (ni + 1);
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(q % (ni + 1)), j = (int)((q / (ni + 1)) % (nj + 1)), k = (int)(q / ((size_t)(ni + 1) * (nj + 1))) + 1;
+        const int x = i + 3, y = j + 3;
+        if (j < nj) {
+            const float m = p.rru[L.u(k, y, x)];
+            float s1, s2, s3, s4, s5;
+            if (m >= 0.0f) {
+                s1 = p.s[L.s(k, y, x - 3)], s2 = p.s[L.s(k, y, x - 2)], s3 = p.s[L.s(k, y, x - 1)];
+                s4 = p.s[L.s(k, y, x)], s5 = p.s[L.s(k, y, x + 1)];
+            } else {
+                s1 = p.s[L.s(k, y, x + 2)], s2 = p.s[L.s(k, y, x + 1)], s3 = p.s[L.s(k, y, x)];
+                s4 = p.s[L.s(k, y, x - 1)], s5 = p.s[L.s(k, y, x - 2)];
+            }
+            p.fx[L.u(k, y, x)] = (double)max5abs(s1, s2, s3, s4, s5) > p.weps ? m * weno5(s1, s2, s3, s4, s5, p.weps) : 0.0f;
+        }
+        if (i < ni) {
+            const float m = p.rrv[L.v(k, y, x)];
+            float s1, s2, s3, s4, s5;
+            if (m >= 0.0f) {
+                s1 = p.s[L.s(k, y - 3, x)], s2 = p.s[L.s(k, y - 2, x)], s3 = p.s[L.s(k, y - 1, x)];
+                s4 = p.s[L.s(k, y, x)], s5 = p.s[L.s(k, y + 1, x)];
+            } else {
+                s1 = p.s[L.s(k, y + 2, x)], s2 = p.s[L.s(k, y + 1, x)], s3 = p.s[L.s(k, y, x)];
+                s4 = p.s[L.s(k, y - 1, x)], s5 = p.s[L.s(k, y - 2, x)];
+            }
+            p.fy[L.v(k, y, x)] = (double)max5abs(s1, s2, s3, s4, s5) > p.weps ? m * weno5(s1, s2, s3, s4, s5, p.weps) : 0.0f;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) pdef_vertical_flux_kernel(Pdef p, Lane L) {
+    const int ni = L.ni, nj = L.nj, nk = L.nk;
+    const size_t n = (size_t)(nk - 1) * nj * ni;
+    const float ew = (float)p.weps;
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(q % ni), j = (int)((q / ni) % nj), k = (int)(q / ((size_t)ni * nj)) + 2;
+        const int x = i + 3, y = j + 3;
+        const float m = p.rrw[L.s(k, y, x)];
+        const size_t cm = ((size_t)(k - 1) * nj + j) * ni + i;
+        float r;
+        if (k == 2) {
+            r = m >= 0.0f ? p.c1[cm] * p.s[L.s(k - 1, y, x)] + p.c2[cm] * p.s[L.s(k, y, x)]
+                          : upstrpd(p.s[L.s(k + 1, y, x)], p.s[L.s(k, y, x)], p.s[L.s(k - 1, y, x)], ew);
+        } else if (k == nk) {
+            r = m > 0.0f ? upstrpd(p.s[L.s(k - 2, y, x)], p.s[L.s(k - 1, y, x)], p.s[L.s(k, y, x)], ew)
+                         : p.c1[cm] * p.s[L.s(k - 1, y, x)] + p.c2[cm] * p.s[L.s(k, y, x)];
+        } else {
+            const bool low = (k == 3 && (p.pdefweno ? m > 0.0f : m >= 0.0f)) || (k == nk - 1 && m < 0.0f);
+            if (low) {
+                r = k == 3 ? upstrpd(p.s[L.s(k - 2, y, x)], p.s[L.s(k - 1, y, x)], p.s[L.s(k, y, x)], ew)
+                           : upstrpd(p.s[L.s(k + 1, y, x)], p.s[L.s(k, y, x)], p.s[L.s(k - 1, y, x)], ew);
+            } else {
+                float s1, s2, s3, s4, s5;
+                if (m >= 0.0f) {
+                    s1 = p.s[L.s(k - 3, y, x)], s2 = p.s[L.s(k - 2, y, x)], s3 = p.s[L.s(k - 1, y, x)];
+                    s4 = p.s[L.s(k, y, x)], s5 = p.s[L.s(k + 1, y, x)];
+                } else {
+                    s1 = p.s[L.s(k + 2, y, x)], s2 = p.s[L.s(k + 1, y, x)], s3 = p.s[L.s(k, y, x)];
+                    s4 = p.s[L.s(k - 1, y, x)], s5 = p.s[L.s(k - 2, y, x)];
+                }
+                if (p.pdefweno && (double)max5abs(s1, s2, s3, s4, s5) <= p.weps) {
+                    p.fz[L.s(k, y, x)] = 0.0f;
+                    continue;
+                }
+                r = weno5(s1, s2, s3, s4, s5, p.weps);
+            }
+        }
+        p.fz[L.s(k, y, x)] = m * r;
+    }
+}
+
+__global__ void __launch_bounds__(256) pdef_directional_kernel(Pdef p, Lane L) {
+    const int ni = L.ni, nj = L.nj, nk = L.nk;
+    const size_t n = (size_t)nk * nj * ni;
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(q % ni), j = (int)((q / ni) % nj), k = (int)(q / ((size_t)ni * nj)) + 1;
+        const int x = i + 3, y = j + 3;
+        float fw = p.fx[L.u(k, y, x)], fe = p.fx[L.u(k, y, x + 1)], fs = p.fy[L.v(k, y, x)], fn = p.fy[L.v(k, y + 1, x)];
+        const float uw = p.rru[L.u(k, y, x)], ue = p.rru[L.u(k, y, x + 1)];
+        const float vs = p.rrv[L.v(k, y, x)], vn = p.rrv[L.v(k, y + 1, x)];
+        const bool iw = inflow_lo(i, p.obc, 0u, uw), ie = inflow_hi(i, ni, p.obc, 1u, ue);
+        const bool js = inflow_lo(j, p.obc, 2u, vs), jn = inflow_hi(j, nj, p.obc, 3u, vn);
+        if (iw) fw = fe;
+        if (ie) fe = fw;
+        if (js) fs = fn;
+        if (jn) fn = fs;
+        float axv = (fw - fe) * p.rdx, ayv = (fs - fn) * p.rdy;
+        if (iw || ie || js || jn) {
+            const float sv = p.s[L.s(k, y, x)];
+            if (iw) axv = axv - (sv * (ue - uw)) * p.rdx;
+            if (ie) axv = axv - (sv * (ue - uw)) * p.rdx;
+            if (js) ayv = ayv - (sv * (vn - vs)) * p.rdy;
+            if (jn) ayv = ayv - (sv * (vn - vs)) * p.rdy;
+        }
+        p.ax[q] = axv;
+        p.ay[q] = ayv;
+        p.az[q] = k == 1 ? (-p.fz[L.s(2, y, x)]) * p.rdz
+                         : (k == nk ? p.fz[L.s(nk, y, x)] * p.rdz : (p.fz[L.s(k, y, x)] - p.fz[L.s(k + 1, y, x)]) * p.rdz);
+    }
+}
+
+// axis 0/1/2 = x/y/z candidate: dum = rho0 a + (dt (adv + (s dflux) rspacing)) gz
+__global__ void __launch_bounds__(256) pdef_candidate_kernel(Pdef p, Lane L, int axis) {
+    const int ni = L.ni, nj = L.nj, nk = L.nk;
+    const size_t n = (size_t)nk * nj * ni;
+    const float *dir = axis == 0 ? p.ax : axis == 1 ? p.ay : p.az;
+    const float rsp = axis == 0 ? p.rdx : axis == 1 ? p.rdy : p.rdz;
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(q % ni), j = (int)((q / ni) % nj), k = (int)(q / ((size_t)ni * nj)) + 1;
+        const int x = i + 3, y = j + 3;
+        float m0, m1;
+        bool inflow = false;
+        if (axis == 0) {
+            m0 = p.rru[L.u(k, y, x)], m1 = p.rru[L.u(k, y, x + 1)];
+            inflow = inflow_lo(i, p.obc, 0u, m0) || inflow_hi(i, ni, p.obc, 1u, m1);
+        } else if (axis == 1) {
+            m0 = p.rrv[L.v(k, y, x)], m1 = p.rrv[L.v(k, y + 1, x)];
+            inflow = inflow_lo(j, p.obc, 2u, m0) || inflow_hi(j, nj, p.obc, 3u, m1);
+        } else {
+            m0 = p.rrw[L.s(k, y, x)], m1 = p.rrw[L.s(k + 1, y, x)];
+        }
+        const float dm = m1 - m0;
+        const float r0a = p.rho0[q] * p.a[q];
+        p.dum[q] = inflow ? r0a : r0a + (p.dt * (dir[q] + (p.s[L.s(k, y, x)] * dm) * rsp)) * p.gz[(size_t)j * ni + i];
+    }
+}
+
+__device__ __forceinline__ float zval(const float *d, long long q, int k, size_t slab, int nk) {
+    return (k < 0 || k >= nk) ? 0.0f : d[q + (long long)k * (long long)slab];
+}
+__device__ __forceinline__ float zratio(const float *d, long long base, int k, size_t slab, int nk) {
+    const float c = zval(d, base, k, slab, nk);
+    if (c >= 0.0f) return 0.0f;
+    const float f1 = fmaxf(0.0f, zval(d, base, k - 1, slab, nk)), f2 = fmaxf(0.0f, zval(d, base, k + 1, slab, nk));
+    const float sum = f1 + f2;
+    return sum > 1.0e-30f ? fmaxf(c, -sum) / sum : 0.0f;
+}
+
+__global__ void __launch_bounds__(256) pdef_correct_kernel(Pdef p, Lane L, int axis) {
+    const int ni = L.ni, nj = L.nj, nk = L.nk;
+    const size_t n = (size_t)nk * nj * ni, slab = (size_t)ni * nj;
+    float *dir = axis == 0 ? p.ax : axis == 1 ? p.ay : p.az;
+    const float rsp = axis == 0 ? p.rdx : axis == 1 ? p.rdy : p.rdz;
+    const float *d = p.dum;
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(q % ni), j = (int)((q / ni) % nj), k0 = (int)(q / slab);
+        float mass = 0.0f;
+        bool flag = false;
+        if (axis == 2) {
+            const long long base = (long long)(q - (size_t)k0 * slab);
+            const float cur = d[q];
+            if (cur < 0.0f) {
+                const float r = zratio(d, base, k0, slab, nk);
+                if (r != 0.0f) {
+                    const float sum = fmaxf(0.0f, zval(d, base, k0 - 1, slab, nk)) + fmaxf(0.0f, zval(d, base, k0 + 1, slab, nk));
+                    mass = 0.0f - sum * r;
+                    flag = true;
+                }
+            } else if (cur > 1.0e-30f) {
+                const float rl = zratio(d, base, k0 - 1, slab, nk), rr = zratio(d, base, k0 + 1, slab, nk);
+                if (rl != 0.0f) mass = mass + cur * rl, flag = true;
+                if (rr != 0.0f) mass = mass + cur * rr, flag = true;
+            }
+        } else {
+            const int c = axis == 0 ? i : j, nn = axis == 0 ? ni : nj;
+            const long long stride = axis == 0 ? 1 : (long long)ni;
+            const long long base = (long long)q - (long long)c * stride;
+            if (p.obc != 0u) {
+                pdef_row_mass(d, base, stride, c, nn, obc_side(p.obc, axis == 0 ? 0u : 2u),
+                              obc_side(p.obc, axis == 0 ? 1u : 3u), &mass, &flag);
+            } else if (c > 0 && c + 1 < nn) {
+                const long long lo = base, hi = base + (long long)(nn - 1) * stride;
+                if (d[q] < 0.0f) {
+                    const float r = ratio1(d, (long long)q, lo, hi, stride);
+                    if (r != 0.0f) {
+                        const float sum = fmaxf(0.0f, d[q - stride]) + fmaxf(0.0f, d[q + stride]);
+                        mass = 0.0f - sum * r;
+                        flag = true;
+                    }
+                } else if (d[q] > 1.0e-30f) {
+                    const float rl = ratio1(d, (long long)q - stride, lo, hi, stride);
+                    const float rr = ratio1(d, (long long)q + stride, lo, hi, stride);
+                    if (rl != 0.0f) mass = mass + d[q] * rl, flag = true;
+                    if (rr != 0.0f) mass = mass + d[q] * rr, flag = true;
+                }
+            }
+        }
+        if (flag) {
+            const int k = k0 + 1, x = i + 3, y = j + 3;
+            const float first = (((d[q] + mass) - p.rho0[q] * p.a[q]) * p.rdt) * p.rgz[(size_t)j * ni + i];
+            float dm;
+            if (axis == 0) dm = p.rru[L.u(k, y, x + 1)] - p.rru[L.u(k, y, x)];
+            else if (axis == 1) dm = p.rrv[L.v(k, y + 1, x)] - p.rrv[L.v(k, y, x)];
+            else dm = p.rrw[L.s(k + 1, y, x)] - p.rrw[L.s(k, y, x)];
+            dir[q] = first - (p.s[L.s(k, y, x)] * dm) * rsp;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) pdef_total_kernel(Pdef p, Lane L) {
+    const int ni = L.ni, nj = L.nj;
+    const size_t n = (size_t)L.nk * nj * ni;
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(q % ni), j = (int)((q / ni) % nj), k = (int)(q / ((size_t)ni * nj)) + 1;
+        if (!obc_owned(i, j, ni, nj, p.obc)) continue;
+        float t = (p.ax[q] + p.ay[q]) + p.az[q];
+        t = t + p.s[L.s(k, j + 3, i + 3)] * p.divx[q];
+        p.adv[q] = (t * p.rr0[q]) * p.gz[(size_t)j * ni + i];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// held tendencies, solve3 density, scalar pack
+// ---------------------------------------------------------------------------
+struct Held {
+    const float *th0, *pi0, *rho, *ppi, *tha, *qa, *qpten, *qtten, *qvten, *qcten;
+    float *thheld, *qheld, *ppten;
+};
+
+__global__ void __launch_bounds__(256) held_compose_kernel(Held h, int ni, int nj, int nk, float dt) {
+    const size_t n = (size_t)ni * nj * nk;
+    const float rd = 287.04f, rv = 461.5f, rp00 = 1.0f / 100000.0f, rddcv = 287.04f / (1005.7f - 287.04f);
+    const float tem = 0.0001f * 0.0001f, qsmall = 1.0e-14f;
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(q % ni), j = (int)((q / ni) % nj), k = (int)(q / ((size_t)ni * nj));
+        const size_t pp = ((size_t)(k + 1) * (nj + 2) + (j + 1)) * (size_t)(ni + 2) + (i + 1);
+        const float ht = h.thheld[q], qvt = h.qheld[q];
+        if (fabsf(dt * ht) > tem || fabsf(dt * qvt) > qsmall) {
+            const float thnew = h.tha[q] + dt * ht, qvnew = h.qa[q] + dt * qvt;
+            float base = (h.rho[q] * (h.th0[q] + thnew)) * (rd + rv * qvnew);
+            base = base * rp00;
+            const float pinew = powf(base, rddcv) - h.pi0[q];
+            h.ppten[pp] = (pinew - h.ppi[q]) / dt + h.qpten[q];
+        } else {
+            h.ppten[pp] = h.qpten[q];
+        }
+        h.thheld[q] = ht + h.qtten[q];
+        h.qheld[q] = qvt + h.qvten[q];
+        h.qheld[n + q] = h.qheld[n + q] + h.qcten[q];
+    }
+}
+
+__global__ void __launch_bounds__(256) solve3_density_kernel(const float *rho, const float *c1, const float *c2,
+                                                            float *rr, float *rf, int ni, int nj, int nk) {
+    const size_t n = (size_t)ni * nj * nk, nf = (size_t)ni * nj * (nk + 1), plane = (size_t)ni * nj;
+    for (size_t z = (size_t)blockIdx.x * blockDim.x + threadIdx.x; z < nf; z += (size_t)gridDim.x * blockDim.x) {
+        if (z < n) rr[z] = 1.0f / rho[z];
+        const size_t h = z % plane;
+        const int f = (int)(z / plane);
+        if (f == 0) rf[z] = (1.875f * rho[h] + (-1.25f) * rho[plane + h]) + 0.375f * rho[2 * plane + h];
+        else if (f == nk)
+            rf[z] = (1.875f * rho[(size_t)(nk - 1) * plane + h] + (-1.25f) * rho[(size_t)(nk - 2) * plane + h]) +
+                    0.375f * rho[(size_t)(nk - 3) * plane + h];
+        else rf[z] = c1[z] * rho[(size_t)(f - 1) * plane + h] + c2[z] * rho[(size_t)f * plane + h];
+    }
+}
+
+__global__ void __launch_bounds__(256) pack_scalar_kernel(const float *s, float *padded, Lane L) {
+    const size_t n = (size_t)L.nk * L.nj * L.ni;
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(q % L.ni), j = (int)((q / L.ni) % L.nj), k = (int)(q / ((size_t)L.ni * L.nj)) + 1;
+        padded[L.s(k, j + 3, i + 3)] = s[q];
+    }
+}
+
+}  // namespace
+}  // namespace gm1b
+
+using namespace gm1b;
+
+namespace {
+bool grid_ok(int ni, int nj, int nk, int mi, int mj, int mk, const char *what) {
+    if (ni < mi || nj < mj || nk < mk) {
+        gm1b_set_error("%s: need ni >= %d, nj >= %d, nk >= %d", what, mi, mj, mk);
+        return false;
+    }
+    return true;
+}
+}  // namespace
+
+extern "C" int32_t gm1b_open_fill(int32_t ni, int32_t nj, int32_t nk, int32_t kind, float *q, void *stream) {
+    FillGeom f;
+    if (q == nullptr || !grid_ok(ni, nj, nk, 2, 2, 2, "gm1b_open_fill") || !fill_geometry(kind, ni, nj, nk, q, f)) {
+        if (q == nullptr || kind < 0 || kind > GM1B_FILL_W_KEEP_ENDS)
+            gm1b_set_error("gm1b_open_fill: need an array and a GM1B_FILL_* kind");
+        return GM1B_ERR_ARGUMENT;
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const size_t work = (size_t)(nk + 2) * (size_t)(std::max(ni, nj) + 8) * 6;
+    for (int pass = 0; pass < 2; ++pass) {
+        const int ew = pass == 0 ? f.ew_first : !f.ew_first;
+        ProfScope ps("open_fill_pass_kernel", st);
+        open_fill_pass_kernel<<<grid_for(work), 256, 0, st>>>(f, ew, pass == 1 && f.zero_w);
+        ps.stop();
+        if (!launch_ok("open_fill_pass_kernel")) return GM1B_ERR_CUDA;
+    }
+    return GM1B_OK;
+}
+
+extern "C" int32_t gm1b_moist_buoyancy(int32_t ni, int32_t nj, int32_t nk, const float *dum8, const float *c1,
+                                       const float *c2, const float *gxu, const float *gyv, float *uten, float *vten,
+                                       float *wten, void *stream) {
+    if (!dum8 || !c1 || !c2 || !gxu || !gyv || !uten || !vten || !wten ||
+        !grid_ok(ni, nj, nk, 2, 2, 2, "gm1b_moist_buoyancy")) {
+        if (!dum8 || !c1 || !c2 || !gxu || !gyv || !uten || !vten || !wten)
+            gm1b_set_error("gm1b_moist_buoyancy: NULL array");
+        return GM1B_ERR_ARGUMENT;
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const Lane L{ni, nj, nk};
+    const size_t work = (size_t)(nk - 1) * nj * ni + (size_t)nk * nj * (ni - 1) + (size_t)nk * (nj - 1) * ni;
+    ProfScope ps("msb_buoyancy_kernel", st);
+    msb_buoyancy_kernel<<<grid_for(work), 256, 0, st>>>(dum8, c1, c2, gxu, gyv, uten, vten, wten, L);
+    ps.stop();
+    return launch_ok("msb_buoyancy_kernel") ? GM1B_OK : GM1B_ERR_CUDA;
+}
+
+extern "C" int32_t gm1b_post_acoustic_flux(int32_t ni, int32_t nj, int32_t nk, const gm1b_post_acoustic_arrays *a,
+                                           float dx, float dy, float dz, void *stream) {
+    if (a == nullptr || !grid_ok(ni, nj, nk, 2, 2, 2, "gm1b_post_acoustic_flux")) {
+        if (a == nullptr) gm1b_set_error("gm1b_post_acoustic_flux: NULL arrays");
+        return GM1B_ERR_ARGUMENT;
+    }
+    const void *need[] = {a->rru, a->rrv, a->rrw, a->rgzu, a->rgzv, a->dzdx, a->dzdy, a->gz, a->rho0_3d, a->rf0,
+                          a->thterm, a->divergence, a->theta_divergence_term, a->divx};
+    for (const void *q : need)
+        if (q == nullptr) {
+            gm1b_set_error("gm1b_post_acoustic_flux: NULL array");
+            return GM1B_ERR_ARGUMENT;
+        }
+    if (!(dx > 0.0f) || !(dy > 0.0f) || !(dz > 0.0f)) {
+        gm1b_set_error("gm1b_post_acoustic_flux: dx, dy, dz must be > 0");
+        return GM1B_ERR_ARGUMENT;
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const Lane L{ni, nj, nk};
+    const size_t n = (size_t)ni * nj * nk;
+    const float rdx = 1.0f / dx, rdy = 1.0f / dy, rdsf = 1.0f / dz;
+    Getdiv g{a->rru, a->rrv, a->rrw, a->rgzu, a->rgzv, a->dzdx, a->dzdy, a->gz, a->thterm, a->divergence,
+             a->theta_divergence_term, rdx, rdy, rdsf, dz, (float)nk * dz, 0.0f};
+    {
+        ProfScope ps("msb_getdiv_kernel", st);
+        msb_getdiv_kernel<<<grid_for(n), 256, 0, st>>>(g, L);
+        ps.stop();
+    }
+    if (!launch_ok("msb_getdiv_kernel")) return GM1B_ERR_CUDA;
+    {
+        ProfScope ps("msb_getdivx_horizontal_kernel", st);
+        msb_getdivx_horizontal_kernel<<<grid_for(2 * n + (size_t)nk * (ni + nj + 1)), 256, 0, st>>>(
+            a->rho0_3d, a->rgzu, a->rgzv, a->rru, a->rrv, L);
+        ps.stop();
+    }
+    if (!launch_ok("msb_getdivx_horizontal_kernel")) return GM1B_ERR_CUDA;
+    {
+        ProfScope ps("msb_getdivx_vertical_kernel", st);
+        msb_getdivx_vertical_kernel<<<grid_for(n + (size_t)ni * nj), 256, 0, st>>>(a->rf0, a->dzdx, a->dzdy, a->gz,
+                                                                                  a->rru, a->rrv, a->rrw, dz, L);
+        ps.stop();
+    }
+    if (!launch_ok("msb_getdivx_vertical_kernel")) return GM1B_ERR_CUDA;
+    {
+        ProfScope ps("msb_getdivx_divergence_kernel", st);
+        msb_getdivx_divergence_kernel<<<grid_for(n), 256, 0, st>>>(a->rru, a->rrv, a->rrw, a->divx, rdx, rdy, rdsf, L);
+        ps.stop();
+    }
+    return launch_ok("msb_getdivx_divergence_kernel") ? GM1B_OK : GM1B_ERR_CUDA;
+}
+
+extern "C" int32_t gm1b_pdef_moisture_chain(int32_t ni, int32_t nj, int32_t nk, const gm1b_pdef_chain_arrays *a,
+                                            float dttmp, float dx, float dy, float dz, double weps,
+                                            uint32_t lateral_obc, int32_t pdefweno, void *stream) {
+    if (a == nullptr || !grid_ok(ni, nj, nk, 2, 2, 4, "gm1b_pdef_moisture_chain")) {
+        if (a == nullptr) gm1b_set_error("gm1b_pdef_moisture_chain: NULL arrays");
+        return GM1B_ERR_ARGUMENT;
+    }
+    const void *need[] = {a->scalar_a, a->scalar_padded, a->rho0_3d, a->gz, a->rgz, a->rr0, a->c1, a->c2, a->divx,
+                          a->rru, a->rrv, a->rrw, a->fx, a->fy, a->fz, a->advx, a->advy, a->advz, a->candidate,
+                          a->advection};
+    for (const void *q : need)
+        if (q == nullptr) {
+            gm1b_set_error("gm1b_pdef_moisture_chain: NULL array");
+            return GM1B_ERR_ARGUMENT;
+        }
+    for (int s = 0; s < 4; ++s) {
+        const unsigned v = (lateral_obc >> (4 * s)) & 15u;
+        if (v > 4) {
+            gm1b_set_error("gm1b_pdef_moisture_chain: lateral side codes must be 0..4");
+            return GM1B_ERR_ARGUMENT;
+        }
+    }
+    if (!(dttmp > 0.0f) || !(dx > 0.0f) || !(dy > 0.0f) || !(dz > 0.0f)) {
+        gm1b_set_error("gm1b_pdef_moisture_chain: dttmp, dx, dy, dz must be > 0");
+        return GM1B_ERR_ARGUMENT;
+    }
+    Pdef p{};
+    p.a = a->scalar_a, p.s = a->scalar_padded, p.rho0 = a->rho0_3d, p.gz = a->gz, p.rgz = a->rgz, p.rr0 = a->rr0;
+    p.c1 = a->c1, p.c2 = a->c2, p.divx = a->divx, p.rru = a->rru, p.rrv = a->rrv, p.rrw = a->rrw;
+    p.fx = a->fx, p.fy = a->fy, p.fz = a->fz, p.ax = a->advx, p.ay = a->advy, p.az = a->advz;
+    p.dum = a->candidate, p.adv = a->advection;
+    p.dt = dttmp, p.dx = dx, p.dy = dy, p.dz = dz;
+    p.rdx = 1.0f / dx, p.rdy = 1.0f / dy, p.rdz = 1.0f / dz, p.rdt = 1.0f / dttmp;
+    p.weps = weps, p.obc = lateral_obc, p.pdefweno = pdefweno ? 1 : 0;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const Lane L{ni, nj, nk};
+    const size_t n = (size_t)ni * nj * nk;
+#define TOS_LAUNCH(name, work, ...)                                    \
+    do {                                                               \
+        ProfScope ps(#name, st);                                       \
+        name<<<grid_for(work), 256, 0, st>>>(__VA_ARGS__);             \
+        ps.stop();                                                     \
+        if (!launch_ok(#name)) return GM1B_ERR_CUDA;                   \
+    } while (0)
+    TOS_LAUNCH(pdef_horizontal_flux_kernel, (size_t)nk * (nj + 1) * (ni + 1), p, L);
+    TOS_LAUNCH(pdef_vertical_flux_kernel, (size_t)(nk - 1) * nj * ni, p, L);
+    TOS_LAUNCH(pdef_directional_kernel, n, p, L);
+    for (int axis = 0; axis < 3; ++axis) {
+        TOS_LAUNCH(pdef_candidate_kernel, n, p, L, axis);
+        TOS_LAUNCH(pdef_correct_kernel, n, p, L, axis);
+    }
+    TOS_LAUNCH(pdef_total_kernel, n, p, L);
+#undef TOS_LAUNCH
+    return GM1B_OK;
+}
+
+extern "C" int32_t gm1b_held_compose(int32_t ni, int32_t nj, int32_t nk, const gm1b_held_arrays *a, float dt,
+                                     void *stream) {
+    if (a == nullptr || !grid_ok(ni, nj, nk, 1, 1, 1, "gm1b_held_compose") || !(dt > 0.0f)) {
+        if (a == nullptr || !(dt > 0.0f)) gm1b_set_error("gm1b_held_compose: need arrays and dt > 0");
+        return GM1B_ERR_ARGUMENT;
+    }
+    Held h{a->th0, a->pi0, a->rho, a->ppi, a->tha, a->qa, a->qpten, a->qtten, a->qvten, a->qcten,
+           a->thheld, a->qheld, a->ppten};
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    ProfScope ps("held_compose_kernel", st);
+    held_compose_kernel<<<grid_for((size_t)ni * nj * nk), 256, 0, st>>>(h, ni, nj, nk, dt);
+    ps.stop();
+    return launch_ok("held_compose_kernel") ? GM1B_OK : GM1B_ERR_CUDA;
+}
+
+extern "C" int32_t gm1b_solve3_density(int32_t ni, int32_t nj, int32_t nk, const float *rho, const float *c1,
+                                       const float *c2, float *rr, float *rf, void *stream) {
+    if (!rho || !c1 || !c2 || !rr || !rf || !grid_ok(ni, nj, nk, 1, 1, 3, "gm1b_solve3_density")) {
+        if (!rho || !c1 || !c2 || !rr || !rf) gm1b_set_error("gm1b_solve3_density: NULL array");
+        return GM1B_ERR_ARGUMENT;
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    ProfScope ps("solve3_density_kernel", st);
+    solve3_density_kernel<<<grid_for((size_t)ni * nj * (nk + 1)), 256, 0, st>>>(rho, c1, c2, rr, rf, ni, nj, nk);
+    ps.stop();
+    return launch_ok("solve3_density_kernel") ? GM1B_OK : GM1B_ERR_CUDA;
+}
+
+extern "C" int32_t gm1b_pack_scalar(int32_t ni, int32_t nj, int32_t nk, const float *scalar, float *padded,
+                                    void *stream) {
+    if (!scalar || !padded || !grid_ok(ni, nj, nk, 1, 1, 1, "gm1b_pack_scalar")) {
+        if (!scalar || !padded) gm1b_set_error("gm1b_pack_scalar: NULL array");
+        return GM1B_ERR_ARGUMENT;
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    ProfScope ps("pack_scalar_kernel", st);
+    pack_scalar_kernel<<<grid_for((size_t)ni * nj * nk), 256, 0, st>>>(scalar, padded, Lane{ni, nj, nk});
+    ps.stop();
+    return launch_ok("pack_scalar_kernel") ? GM1B_OK : GM1B_ERR_CUDA;
+}

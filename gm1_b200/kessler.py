@@ -206,3 +206,133 @@ def launch_cuda_gm1_kessler_driver(
         ev.record(st)
     return CudaKesslerLaunch(ev, workspace, {"operator": "gm1-kessler-driver", "equation_set": selection.equation_set,
                                              "efall": selection.efall, "domain": {"ni": ni, "nj": nj, "nk": nk}})
+
+
+# ---------------------------------------------------------------------------
+# once-per-large-step transition (src/cm1core/cuda_gm1_kessler_large_step.py)
+# ---------------------------------------------------------------------------
+HELD_NAMES = ("qpten", "qtten", "qvten", "qcten")
+
+
+@dataclass(slots=True)
+class Gm1KesslerHeldCarriers:
+    qpten: torch.Tensor
+    qtten: torch.Tensor
+    qvten: torch.Tensor
+    qcten: torch.Tensor
+
+
+class _HeldArrays(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_void_p) for n in HELD_NAMES]
+
+
+@dataclass(frozen=True, slots=True)
+class Gm1KesslerLargeStepResult:
+    ready_event: Any
+    completed_transitions: int
+    receipt: Mapping[str, Any]
+
+
+class CudaGm1KesslerLargeStepTransition:
+    """Persistent source-ordered Kessler transition of one CUDA state: held
+    rate remove/snapshot, pre-physics EOS, the driver, held recapture, all in
+    one library call (gm1b_kessler_large_step)."""
+
+    def __init__(self, arrays: dict[str, torch.Tensor], carriers: Gm1KesslerHeldCarriers, *, ni: int, nj: int,
+                 nk: int, dx: float, dy: float, dz: float, dt: float, selection: Gm1KesslerDriverSelection,
+                 stream: Any, workspace: Gm1KesslerDriverWorkspace, completed_transitions: int = 0) -> None:
+        self.arrays, self.carriers = arrays, carriers
+        self.ni, self.nj, self.nk = ni, nj, nk
+        self.dx, self.dy, self.dz, self.dt = dx, dy, dz, dt
+        self.selection, self.stream, self.workspace = selection, stream, workspace
+        self.completed_transitions = completed_transitions
+
+    def apply(self, *, final_rk: bool = True, refl_10cm_due: bool = False,
+              pre_component_hook: Any | None = None) -> Gm1KesslerLargeStepResult:
+        if type(final_rk) is not bool or not final_rk:
+            refuse(code="GM1-KESSLER-LARGE-STEP-CADENCE", gate="physics-seam", option="final_rk", value=final_rk,
+                   reason="CM1 r21.1 calls mp_driver once after the completed RK solve",
+                   remedy="invoke the transition only after final RK stage 3")
+        if type(refl_10cm_due) is not bool:
+            raise TypeError("refl_10cm_due must be boolean")
+        if refl_10cm_due:
+            refuse(code="GM1-KESSLER-REFLECTIVITY-UNPORTED", gate="physics-seam", option="refl_10cm_due",
+                   value=True, reason="CM1 does not admit the selected reflectivity consumer for ptype=1",
+                   remedy="disable reflectivity or select an admitted microphysics consumer")
+        if pre_component_hook is not None:
+            refuse(code="GM1-KESSLER-LARGE-STEP-HOOK", gate="physics-seam", option="pre_component_hook",
+                   value=type(pre_component_hook).__name__,
+                   reason="the dry-mass hook between the pre-physics EOS and the driver is not part of this "
+                          "operator (one fused library call)", remedy="run the transition without a hook")
+        a, h = self.arrays, self.carriers
+        s = _KesslerArrays(**{n: t.data_ptr() for n, t in a.items() if n in ALL_ARRAY_NAMES})
+        held = _HeldArrays(**{n: getattr(h, n).data_ptr() for n in HELD_NAMES})
+        device = a["rho"].device
+        st = torch.cuda.current_stream(device) if self.stream is None else self.stream
+        lib = _bind()
+        if not getattr(lib, "_kls_bound", False):
+            c = ctypes
+            lib.gm1b_kessler_large_step.argtypes = [c.c_int32] * 3 + [c.POINTER(_KesslerArrays), c.POINTER(_HeldArrays)] + \
+                [c.c_float] * 4 + [c.c_int32, c.c_int32, c.c_void_p, c.c_size_t, c.c_void_p]
+            lib.gm1b_kessler_large_step.restype = c.c_int32
+            lib._kls_bound = True
+        with torch.cuda.device(device):
+            _native.check(lib.gm1b_kessler_large_step(self.ni, self.nj, self.nk, ctypes.byref(s), ctypes.byref(held),
+                                                      self.dx, self.dy, self.dz, self.dt, self.selection.equation_set,
+                                                      self.selection.efall,
+                                                      ctypes.c_void_p(self.workspace.buffer.data_ptr()),
+                                                      self.workspace.buffer.numel(), ctypes.c_void_p(st.cuda_stream)),
+                          "gm1b_kessler_large_step")
+            ev = torch.cuda.Event()
+            ev.record(st)
+        self.completed_transitions += 1
+        return Gm1KesslerLargeStepResult(ev, self.completed_transitions, {
+            "operator": "gm1-kessler-large-step", "equation_set": self.selection.equation_set,
+            "source_order": ("solve2-held-remove-snapshot", "solve2-pre-physics-eos", "cm1-mp_driver-ptype1",
+                             "solve3-held-recapture"),
+            "domain": {"ni": self.ni, "nj": self.nj, "nk": self.nk}})
+
+
+def create_cuda_gm1_kessler_large_step_transition(
+        arrays: Mapping[str, Any], *, ni: int, nj: int, nk: int, dx: float, dy: float, dz: float, dt: float,
+        selection: Gm1KesslerDriverSelection, stream: Any | None = None,
+        workspace: Gm1KesslerDriverWorkspace | None = None,
+        carriers: Gm1KesslerHeldCarriers | None = None) -> CudaGm1KesslerLargeStepTransition:
+    """Bind an already Kessler-initialised device state.  rr, fall_velocity,
+    rain, prate, asq and qbudget are allocated (zero) when absent, as are the
+    held carriers (the reference's fresh-start restart state)."""
+    for name, value, minimum in (("ni", ni, 1), ("nj", nj, 1), ("nk", nk, 2)):
+        if type(value) is not int or value < minimum:
+            raise ValueError(f"{name} must be an integer >= {minimum}")
+    dx, dy, dz, dt = (_positive(n, v) for n, v in (("dx", dx), ("dy", dy), ("dz", dz), ("dt", dt)))
+    _validate_selection(selection)
+    shapes = gm1_kessler_driver_shapes(ni, nj, nk)
+    base = ("ruh", "rvh", "rmh", "mh", "pi0", "th0", "rho", "pp3d", "th3d", "prs", "qv", "qc", "qr")
+    missing = [n for n in base if n not in arrays]
+    if missing:
+        raise ValueError("missing GM1 Kessler large-step arrays: " + ", ".join(missing))
+    device = arrays["rho"].device
+    bound: dict[str, torch.Tensor] = {}
+    for n in ALL_ARRAY_NAMES:
+        dtype = torch.float64 if n in DOUBLE_NAMES else torch.float32
+        t = arrays.get(n)
+        if t is None and n not in base:
+            t = torch.zeros(shapes[n], dtype=dtype, device=device)
+        if not isinstance(t, torch.Tensor) or not t.is_cuda or t.dtype != dtype or tuple(t.shape) != shapes[n] \
+                or not t.is_contiguous():
+            raise ValueError(f"{n} must be C-order CUDA {dtype} with shape {shapes[n]}")
+        bound[n] = t
+    if len({t.data_ptr() for t in bound.values()}) != len(bound):
+        raise ValueError("GM1 Kessler large-step arrays must not alias")
+    mass = (nk, nj, ni)
+    if carriers is None:
+        carriers = Gm1KesslerHeldCarriers(*(torch.zeros(mass, device=device) for _ in HELD_NAMES))
+    for n in HELD_NAMES:
+        t = getattr(carriers, n)
+        if not isinstance(t, torch.Tensor) or t.dtype != torch.float32 or tuple(t.shape) != mass \
+                or not t.is_contiguous() or t.device != device:
+            raise ValueError(f"held {n} must be C-order CUDA float32 with shape {mass}")
+    if workspace is None:
+        workspace = create_cuda_gm1_kessler_driver_workspace(ni=ni, nj=nj, nk=nk, device=device)
+    return CudaGm1KesslerLargeStepTransition(bound, carriers, ni=ni, nj=nj, nk=nk, dx=dx, dy=dy, dz=dz, dt=dt,
+                                             selection=selection, stream=stream, workspace=workspace)

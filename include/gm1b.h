@@ -336,6 +336,26 @@ GM1B_API int32_t gm1b_kessler_driver(int32_t ni, int32_t nj, int32_t nk,
  *   sub-step count, stream-ordered after the operator.
  * - The call allocates no device memory and calls no allocator.
  */
+/* Held-rate carriers of the equation-set-2 Kessler lifecycle, mass-shaped
+ * (Gm1KesslerHeldCarriers, src/cm1core/cuda_gm1_kessler_large_step.py:112). */
+typedef struct gm1b_kessler_held {
+    float *qpten, *qtten, *qvten, *qcten;
+} gm1b_kessler_held;
+
+/*
+ * The once-per-large-step Kessler transition, in place: with equation set 2
+ * remove the held rates from pp3d, th3d, qv, qc and snapshot the result into
+ * the carriers, form the pre-physics prs and rho (and rr = rho), run
+ * gm1b_kessler_driver, then turn the carriers into the next step's rates
+ * (state - snapshot) / dt.  held may be NULL for equation set 1.  Replaces
+ * CudaGm1KesslerLargeStepTransition.apply (cuda_gm1_kessler_large_step.py:392)
+ * and its CPU twin cpu_gm1_kessler_large_step_inplace (:183).
+ */
+GM1B_API int32_t gm1b_kessler_large_step(int32_t ni, int32_t nj, int32_t nk, const gm1b_kessler_arrays *arrays,
+                                         const gm1b_kessler_held *held, float dx, float dy, float dz, float dt,
+                                         int32_t equation_set, int32_t efall, void *workspace, size_t workspace_size,
+                                         void *stream);
+
 #define GM1B_KESSLER_STATIC_SCRATCH_BYTES (8u * 1024u * 1024u)
 GM1B_API int32_t gm1b_kessler_driver_static(int32_t ni, int32_t nj, int32_t nk,
                                             const gm1b_kessler_arrays *arrays, float dx, float dy,
@@ -434,6 +454,79 @@ GM1B_API int32_t gm1b_terrain_open_stage(int32_t ni, int32_t nj, int32_t nk, int
                                          float dx, float dy, double dz, float alph, float kdiv, uint32_t ablations,
                                          uint32_t flags, const gm1b_terrain_open_arrays *arrays,
                                          const gm1b_terrain_metrics *metrics, void *stream);
+
+/* ------------------------------------------------------------------------
+ * Pieces that join the operators of the moist large step on the open lane.
+ * ------------------------------------------------------------------------ */
+/* Open-lateral halo fills in the reference's two ordered passes
+ * (cpu_bcp/bcs/bcu/bcv/bcw_open_inplace, src/cm1core/cuda_sound3_open_boundary.py:249-335). */
+#define GM1B_FILL_PRESSURE 0     /* bcp: (nk+2, nj+2, ni+2), levels 1..nk */
+#define GM1B_FILL_SCALAR 1       /* bcs: (nk+2, nj+6, ni+6), levels 1..nk */
+#define GM1B_FILL_U 2            /* bcu: (nk+2, nj+6, ni+7) */
+#define GM1B_FILL_V 3            /* bcv: (nk+2, nj+7, ni+6) */
+#define GM1B_FILL_W 4            /* bcw flag 1: (nk+3, nj+6, ni+6), levels 2..nk, then w(1) = w(nk+1) = 0 */
+#define GM1B_FILL_W_KEEP_ENDS 5  /* bcw flag 0 */
+GM1B_API int32_t gm1b_open_fill(int32_t ni, int32_t nj, int32_t nk, int32_t kind, float *q, void *stream);
+
+/* Moist buoyancy into the live tendencies: wten += c1 dum8 + c2 dum8 on the
+ * interior w levels, uten/vten += the terrain-horizontal part
+ * (launch_cuda_moist_buoyancy, src/cm1core/cuda_moist_stage_bridge.py:433;
+ * kernel cm1_msb_buoyancy_v1 in that file's source).  dum8 is the scalar
+ * layout (nk+2, nj+6, ni+6) with open halos; c1, c2 (nk+1, nj, ni); gxu
+ * (nk+1, nj, ni+1); gyv (nk+1, nj+1, ni). */
+GM1B_API int32_t gm1b_moist_buoyancy(int32_t ni, int32_t nj, int32_t nk, const float *dum8, const float *c1,
+                                     const float *c2, const float *gxu, const float *gyv, float *uten, float *vten,
+                                     float *wten, void *stream);
+
+/* Post-acoustic getdiv on the acoustic-averaged velocities (divergence and
+ * theta_divergence_term = divergence * thterm, compact), then getdivx in
+ * place: rru/rrv/rrw become mass fluxes and divx their divergence
+ * (launch_cuda_post_acoustic_flux_bridge, cuda_moist_stage_bridge.py:461). */
+typedef struct gm1b_post_acoustic_arrays {
+    float *rru, *rrv, *rrw;
+    const float *rgzu, *rgzv, *dzdx, *dzdy, *gz, *rho0_3d, *rf0, *thterm;
+    float *divergence, *theta_divergence_term, *divx;
+} gm1b_post_acoustic_arrays;
+GM1B_API int32_t gm1b_post_acoustic_flux(int32_t ni, int32_t nj, int32_t nk, const gm1b_post_acoustic_arrays *arrays,
+                                         float dx, float dy, float dz, void *stream);
+
+/* The final-stage positive-definite moisture chain of one species: WENO
+ * face fluxes (horizontal, vertical with the lower/upper closures), the
+ * directional advection with the open-side inflow edits, the pdef
+ * candidate/correction in x, y and z (boundary-family repair rows when
+ * lateral_obc != 0), and the total advection (launch_cuda_scalar_moist_rk_stage
+ * final stage, src/cm1core/cuda_scalar_moist_rk.py:1336-1500).  pdefweno is 0
+ * for qv and 1 for the other species. */
+typedef struct gm1b_pdef_chain_arrays {
+    const float *scalar_a, *scalar_padded, *rho0_3d, *gz, *rgz, *rr0, *c1, *c2, *divx, *rru, *rrv, *rrw;
+    float *fx, *fy, *fz, *advx, *advy, *advz, *candidate, *advection;
+} gm1b_pdef_chain_arrays;
+GM1B_API int32_t gm1b_pdef_moisture_chain(int32_t ni, int32_t nj, int32_t nk, const gm1b_pdef_chain_arrays *arrays,
+                                          float dttmp, float dx, float dy, float dz, double weps, uint32_t lateral_obc,
+                                          int32_t pdefweno, void *stream);
+
+/* Held-tendency composition once per large step: ppten from the held theta
+ * and qv tendencies (or the microphysics pressure rate alone), then the
+ * microphysics rates join the held theta/qv/qc tendencies
+ * (gm1_child_predict_and_compose_held_base3d_v1,
+ * src/cm1core/cuda_gm1_child_step_composer.py:547-556).  Mass-shaped except
+ * ppten (nk+2, nj+2, ni+2) and qheld (2+, nk, nj, ni). */
+typedef struct gm1b_held_arrays {
+    const float *th0, *pi0, *rho, *ppi, *tha, *qa, *qpten, *qtten, *qvten, *qcten;
+    float *thheld, *qheld, *ppten;
+} gm1b_held_arrays;
+GM1B_API int32_t gm1b_held_compose(int32_t ni, int32_t nj, int32_t nk, const gm1b_held_arrays *arrays, float dt,
+                                   void *stream);
+
+/* solve3 density: rr = 1/rho, rf = face average (c1, c2) with the uniform
+ * Fornberg ends (gm1_solve3_density_v1, src/cm1core/cuda_gm1_forecast.py:548). */
+GM1B_API int32_t gm1b_solve3_density(int32_t ni, int32_t nj, int32_t nk, const float *rho, const float *c1,
+                                     const float *c2, float *rr, float *rf, void *stream);
+
+/* Copy a compact (nk, nj, ni) scalar into the interior of its padded
+ * (nk+2, nj+6, ni+6) carrier (cm1_rk_pack_scalar_v1). */
+GM1B_API int32_t gm1b_pack_scalar(int32_t ni, int32_t nj, int32_t nk, const float *scalar, float *padded,
+                                  void *stream);
 
 /* The two halves of gm1b_momentum_advection5, for a caller that edits the
  * fluxes or divx between them (the reference's post_divergence_hook seam):

@@ -53,3 +53,32 @@ def kessler_driver(arrays, *, ni, nj, nk, dx, dy, dz, dt, eqtset, iterations=Non
     if r < -100:
         raise RuntimeError(f"Kessler satadj failed to converge in 100 iterations ({-r - 100} cells)")
     return r
+
+
+HELD_NAMES = ("qpten", "qtten", "qvten", "qcten")
+
+
+def kessler_large_step(arrays, held, *, ni, nj, nk, dx, dy, dz, dt, eqtset, nfall=None) -> int:
+    """cpu_gm1_kessler_large_step_inplace restated: held remove/snapshot,
+    pre-physics EOS, the driver, held recapture (in place)."""
+    s = KesslerArrays()
+    for n in FLOAT_NAMES:
+        a = arrays[n]
+        assert a.dtype == np.float32 and a.flags.c_contiguous
+        setattr(s, n, a.ctypes.data_as(_F))
+    for n in ("asq", "qbudget"):
+        setattr(s, n, arrays[n].ctypes.data_as(_D))
+    hp = (_F * 4)(*[held[n].ctypes.data_as(_F) for n in HELD_NAMES])
+    lib = _lib()
+    if not getattr(lib, "_kls_ready", False):
+        lib.oracle_kessler_large_step.argtypes = [ctypes.POINTER(KesslerArrays), ctypes.POINTER(_F)] + \
+            [ctypes.c_int] * 3 + [ctypes.c_float] * 4 + [ctypes.c_int, ctypes.POINTER(ctypes.c_int32)]
+        lib.oracle_kessler_large_step.restype = ctypes.c_int
+        lib._kls_ready = True
+    nf = nfall.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)) if nfall is not None else None
+    r = lib.oracle_kessler_large_step(ctypes.byref(s), hp, ni, nj, nk, dx, dy, dz, dt, eqtset, nf)
+    if r == -1:
+        raise ValueError("invalid Kessler arguments")
+    if r < -100:
+        raise RuntimeError(f"Kessler satadj failed to converge in 100 iterations ({-r - 100} cells)")
+    return r

@@ -342,3 +342,43 @@ int oracle_kessler_driver(const kessler_arrays *a, int ni, int nj, int nk, float
     if (failures) return -(100 + failures);
     return max_nfall;
 }
+
+/* cpu_gm1_kessler_large_step_inplace (src/cm1core/cuda_gm1_kessler_large_step.py:183-292):
+ * equation-set-2 held remove/snapshot, pre-physics EOS (numpy float32 power:
+ * libm powf), rr = rho, the driver, held recapture.  held[0..3] = qpten,
+ * qtten, qvten, qcten (ignored for equation set 1).  Returns the driver's
+ * result. */
+int oracle_kessler_large_step(const kessler_arrays *a, float *const held[4], int ni, int nj, int nk, float dx,
+                              float dy, float dz, float dt, int eqtset, int *nfall) {
+    const size_t n = (size_t)ni * nj * nk;
+    float *state[4] = {a->pp3d, a->th3d, a->qv, a->qc};
+    if (eqtset == 2)
+        for (int s = 0; s < 4; ++s)
+            for (size_t q = 0; q < n; ++q) {
+                const float w = held[s][q] * dt;
+                state[s][q] = state[s][q] - w;
+                held[s][q] = state[s][q];
+            }
+    const float cpdrd = (float)((double)1005.7f / (double)287.04f);
+    for (size_t q = 0; q < n; ++q) {
+        const float pi = a->pi0[q] + a->pp3d[q];
+        float prs = powf(pi, cpdrd);
+        prs = prs * 100000.0f;
+        float rho = a->th0[q] + a->th3d[q];
+        rho = rho * pi;
+        float w = a->qv[q] > 0.0f ? a->qv[q] : 0.0f;
+        if (a->qv[q] != a->qv[q]) w = a->qv[q];
+        w = w * 461.5f;
+        w = w + 287.04f;
+        rho = rho * w;
+        rho = prs / rho;
+        a->prs[q] = prs;
+        a->rho[q] = rho;
+        ((float *)a->rr)[q] = rho;
+    }
+    const int r = oracle_kessler_driver(a, ni, nj, nk, dx, dy, dz, dt, eqtset, nfall);
+    if (r < 0 || eqtset != 2) return r;
+    for (int s = 0; s < 4; ++s)
+        for (size_t q = 0; q < n; ++q) held[s][q] = (state[s][q] - held[s][q]) / dt;
+    return r;
+}

@@ -1,0 +1,91 @@
+"""ctypes driver of the moist-step pieces of the oracle
+(moist_step_oracle.c, terrain_open_oracle.c's fills) - TEST INFRASTRUCTURE
+ONLY."""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from oracle.periodic import load
+
+_F = ctypes.POINTER(ctypes.c_float)
+POST_NAMES = ("rru", "rrv", "rrw", "rgzu", "rgzv", "dzdx", "dzdy", "gz", "rho0_3d", "rf0", "thterm", "divergence",
+              "theta_divergence_term", "divx")
+CHAIN_NAMES = ("scalar_a", "scalar_padded", "rho0_3d", "gz", "rgz", "rr0", "c1", "c2", "divx", "rru", "rrv", "rrw",
+               "fx", "fy", "fz", "advx", "advy", "advz", "candidate", "advection")
+HELD_NAMES = ("th0", "pi0", "rho", "ppi", "tha", "qa", "qpten", "qtten", "qvten", "qcten", "thheld", "qheld", "ppten")
+FILL = {"pressure": 0, "scalar": 1, "u": 2, "v": 3, "w": 4, "w_keep_ends": 5}
+
+
+def _struct(names):
+    class S(ctypes.Structure):
+        _fields_ = [(n, _F) for n in names]
+    return S
+
+
+_Post, _Chain, _Held = _struct(POST_NAMES), _struct(CHAIN_NAMES), _struct(HELD_NAMES)
+
+
+def _p(a):
+    assert a.dtype == np.float32 and a.flags.c_contiguous
+    return a.ctypes.data_as(_F)
+
+
+def _lib():
+    lib = load()
+    if not getattr(lib, "_ms_ready", False):
+        c = ctypes
+        lib.oracle_open_fill.argtypes = [c.c_int] * 4 + [_F]
+        lib.oracle_moist_buoyancy.argtypes = [c.c_int] * 3 + [_F] * 8
+        lib.oracle_post_acoustic_flux.argtypes = [c.c_int] * 3 + [c.POINTER(_Post)] + [c.c_float] * 3
+        lib.oracle_pdef_moisture_chain.argtypes = [c.c_int] * 3 + [c.POINTER(_Chain)] + [c.c_float] * 4 + \
+            [c.c_double, c.c_uint, c.c_int]
+        lib.oracle_pdef_moisture_directional.argtypes = lib.oracle_pdef_moisture_chain.argtypes
+        lib.oracle_pdef_moisture_directional.restype = None
+        lib.oracle_held_compose.argtypes = [c.c_int] * 3 + [c.POINTER(_Held), c.c_float]
+        lib.oracle_solve3_density.argtypes = [c.c_int] * 3 + [_F] * 5
+        lib.oracle_pack_scalar.argtypes = [c.c_int] * 3 + [_F] * 2
+        for f in ("oracle_open_fill", "oracle_moist_buoyancy", "oracle_post_acoustic_flux",
+                  "oracle_pdef_moisture_chain", "oracle_held_compose", "oracle_solve3_density", "oracle_pack_scalar"):
+            getattr(lib, f).restype = None
+        lib._ms_ready = True
+    return lib
+
+
+def open_fill(q, kind, *, ni, nj, nk):
+    _lib().oracle_open_fill(ni, nj, nk, FILL[kind], _p(q))
+
+
+def moist_buoyancy(dum8, c1, c2, gxu, gyv, uten, vten, wten, *, ni, nj, nk):
+    _lib().oracle_moist_buoyancy(ni, nj, nk, *(_p(x) for x in (dum8, c1, c2, gxu, gyv, uten, vten, wten)))
+
+
+def post_acoustic_flux(a, *, ni, nj, nk, dx, dy, dz):
+    s = _Post(**{n: _p(a[n]) for n in POST_NAMES})
+    _lib().oracle_post_acoustic_flux(ni, nj, nk, ctypes.byref(s), dx, dy, dz)
+
+
+def pdef_moisture_chain(a, *, ni, nj, nk, dttmp, dx, dy, dz, weps, lateral_obc, pdefweno):
+    s = _Chain(**{n: _p(a[n]) for n in CHAIN_NAMES})
+    _lib().oracle_pdef_moisture_chain(ni, nj, nk, ctypes.byref(s), dttmp, dx, dy, dz, weps, lateral_obc, pdefweno)
+
+
+def pdef_moisture_directional(a, *, ni, nj, nk, dttmp, dx, dy, dz, weps, lateral_obc, pdefweno):
+    """The chain up to the directional advection (advx/advy/advz before any repair)."""
+    s = _Chain(**{n: _p(a[n]) for n in CHAIN_NAMES})
+    _lib().oracle_pdef_moisture_directional(ni, nj, nk, ctypes.byref(s), dttmp, dx, dy, dz, weps, lateral_obc, pdefweno)
+
+
+def held_compose(a, *, ni, nj, nk, dt):
+    s = _Held(**{n: _p(a[n]) for n in HELD_NAMES})
+    _lib().oracle_held_compose(ni, nj, nk, ctypes.byref(s), dt)
+
+
+def solve3_density(rho, c1, c2, rr, rf, *, ni, nj, nk):
+    _lib().oracle_solve3_density(ni, nj, nk, *(_p(x) for x in (rho, c1, c2, rr, rf)))
+
+
+def pack_scalar(s, padded, *, ni, nj, nk):
+    _lib().oracle_pack_scalar(ni, nj, nk, _p(s), _p(padded))

@@ -717,3 +717,17 @@ int oracle_terrain_open_stage(TosArrays *a, const TosMetrics *m, int ni, int nj,
     free_profiles(&p);
     return 0;
 }
+
+/* the open-lateral fills on their own (GM1B_FILL_* kinds) */
+void oracle_open_fill(int ni, int nj, int nk, int kind, float *q) {
+    const G g = {ni, nj, nk};
+    switch (kind) {
+        case 0: bcp_open(q, &g); break;
+        case 1: bcs_open(q, &g, 1, nk); break;
+        case 2: bcu_open(q, &g); break;
+        case 3: bcv_open(q, &g); break;
+        case 4: bcw_open_flag1(q, &g); break;
+        case 5: bcs_open(q, &g, 2, nk); break;
+        default: break;
+    }
+}

@@ -332,6 +332,46 @@ def make_kessler(reference: Path) -> None:
               "iterations", int(result["satadj"]["iterations"].max()))
 
 
+KESSLER_LARGE_STEP_CASES = {
+    "kessler_large_step_eqt2_7x5x12": (7, 5, 12, 100.0, 30.0, 2, 41),
+    "kessler_large_step_eqt1_6x6x10": (6, 6, 10, 150.0, 12.0, 1, 42),
+}
+
+
+def kessler_large_step_fixture(ni: int, nj: int, nk: int, dz: float, seed: int) -> tuple[dict, dict]:
+    """Driver inputs plus held-rate carriers of a previous step (small
+    seeded rates of the four equation-set-2 fields)."""
+    a = kessler_fixture(ni, nj, nk, dz, seed)
+    rng = np.random.default_rng(seed + 1000)
+    shape = (nk, nj, ni)
+    held = {"qpten": rng.normal(0.0, 1e-7, shape).astype(np.float32),
+            "qtten": rng.normal(0.0, 2e-3, shape).astype(np.float32),
+            "qvten": rng.normal(0.0, 2e-7, shape).astype(np.float32),
+            "qcten": rng.normal(0.0, 1e-7, shape).astype(np.float32)}
+    return a, held
+
+
+def make_kessler_large_step(reference: Path) -> None:
+    """The once-per-large-step Kessler transition through the reference's CPU
+    twin cpu_gm1_kessler_large_step_inplace."""
+    sys.path.insert(0, str(reference / "src"))
+    from cm1core.cuda_gm1_kessler_driver import Gm1KesslerDriverSelection
+    from cm1core.cuda_gm1_kessler_large_step import cpu_gm1_kessler_large_step_inplace
+
+    for tag, (ni, nj, nk, dz, dt, eqtset, seed) in KESSLER_LARGE_STEP_CASES.items():
+        a, held = kessler_large_step_fixture(ni, nj, nk, dz, seed)
+        inputs = {f"in_{k}": v.copy() for k, v in a.items()}
+        hin = {f"held_in_{k}": v.copy() for k, v in held.items()}
+        result = cpu_gm1_kessler_large_step_inplace(a, held, ni=ni, nj=nj, nk=nk, dx=1000.0, dy=1000.0, dz=dz, dt=dt,
+                                                    selection=Gm1KesslerDriverSelection(equation_set=eqtset))
+        outputs = {f"out_{k}": v for k, v in a.items()}
+        hout = {f"held_out_{k}": v for k, v in held.items()}
+        meta = dict(ni=ni, nj=nj, nk=nk, dx=1000.0, dy=1000.0, dz=dz, dt=dt, eqtset=eqtset,
+                    max_fall_substeps=result["driver"]["max_fall_substeps"])
+        np.savez_compressed(HERE / f"{tag}.npz", meta=json.dumps(meta), **inputs, **hin, **outputs, **hout)
+        print("wrote", tag)
+
+
 def sgs_tke_fixture(ni: int, nj: int, nk: int, seed: int) -> dict[str, np.ndarray]:
     rng = np.random.default_rng(seed)
     cell = (nk + 1, nj, ni)
@@ -883,6 +923,66 @@ def make_terrain_open(reference: Path) -> None:
         print("wrote", tag, round(time.time() - t0, 1), "s", flush=True)
 
 
+def moist_piece_fixture(ni: int, nj: int, nk: int, seed: int) -> dict[str, np.ndarray]:
+    """Seeded inputs of the moist-step pieces: padded winds / mass fluxes,
+    a moisture field near zero with some negative words (so the pdef repair
+    rows fire), buoyancy on the scalar layout, terrain metrics."""
+    rng = np.random.default_rng(seed)
+    f = np.float32
+    su, sv, sw = (nk + 2, nj + 6, ni + 7), (nk + 2, nj + 7, ni + 6), (nk + 3, nj + 6, ni + 6)
+    ss, mass, face = (nk + 2, nj + 6, ni + 6), (nk, nj, ni), (nk + 1, nj, ni)
+    a = {
+        "rru": rng.normal(0.0, 8.0, su).astype(f), "rrv": rng.normal(0.0, 8.0, sv).astype(f),
+        "rrw": rng.normal(0.0, 1.0, sw).astype(f), "uten": rng.normal(0.0, 1e-3, su).astype(f),
+        "vten": rng.normal(0.0, 1e-3, sv).astype(f), "wten": rng.normal(0.0, 1e-3, sw).astype(f),
+        "dum8": rng.normal(0.0, 0.05, ss).astype(f), "thterm": rng.uniform(80.0, 120.0, mass).astype(f),
+        "scalar_padded": np.where(rng.random(ss) < 0.15, rng.normal(-2e-6, 1e-6, ss),
+                                  rng.uniform(0.0, 1.2e-2, ss)).astype(f),
+        "scalar_a": rng.uniform(0.0, 1.2e-2, mass).astype(f),
+        "c1": rng.uniform(0.4, 0.6, face).astype(f), "rho0_3d": rng.uniform(0.6, 1.2, mass).astype(f),
+        "rf0": rng.uniform(0.6, 1.2, face).astype(f), "gz": rng.uniform(0.97, 1.03, (nj, ni)).astype(f),
+        "rgzu": rng.uniform(0.95, 1.05, (nj, ni + 1)).astype(f), "rgzv": rng.uniform(0.95, 1.05, (nj + 1, ni)).astype(f),
+        "dzdx": rng.normal(0.0, 0.02, (nj, ni)).astype(f), "dzdy": rng.normal(0.0, 0.02, (nj, ni)).astype(f),
+        "gxu": rng.normal(0.0, 0.004, (nk + 1, nj, ni + 1)).astype(f),
+        "gyv": rng.normal(0.0, 0.004, (nk + 1, nj + 1, ni)).astype(f),
+        "divx": rng.normal(0.0, 1e-3, mass).astype(f),
+    }
+    a["c2"] = (f(1.0) - a["c1"]).astype(f)
+    a["rgz"] = (f(1.0) / a["gz"]).astype(f)
+    a["rr0"] = (f(1.0) / a["rho0_3d"]).astype(f)
+    return a
+
+
+def make_fills(reference: Path) -> None:
+    """The open-lateral fills through the reference's own functions on seeded
+    arrays with garbage halos."""
+    sys.path.insert(0, str(reference / "src"))
+    from cm1core.cuda_sound3_open_boundary import (cpu_bcp_open_inplace, cpu_bcs_open_inplace, cpu_bcu_open_inplace,
+                                                   cpu_bcv_open_inplace, cpu_bcw_open_inplace)
+
+    ni, nj, nk = 9, 7, 6
+    rng = np.random.default_rng(321)
+    shapes = {"pressure": (nk + 2, nj + 2, ni + 2), "scalar": (nk + 2, nj + 6, ni + 6), "u": (nk + 2, nj + 6, ni + 7),
+              "v": (nk + 2, nj + 7, ni + 6), "w": (nk + 3, nj + 6, ni + 6), "w_keep_ends": (nk + 3, nj + 6, ni + 6)}
+    out = {}
+    for kind, shape in shapes.items():
+        q = rng.normal(0.0, 1.0, shape).astype(np.float32)
+        out[f"in_{kind}"] = q.copy()
+        if kind == "pressure":
+            cpu_bcp_open_inplace(q, ni=ni, nj=nj, nk=nk)
+        elif kind == "scalar":
+            cpu_bcs_open_inplace(q, ni=ni, nj=nj, nk=nk)
+        elif kind == "u":
+            cpu_bcu_open_inplace(q, ni=ni, nj=nj, nk=nk)
+        elif kind == "v":
+            cpu_bcv_open_inplace(q, ni=ni, nj=nj, nk=nk)
+        else:
+            cpu_bcw_open_inplace(q, ni=ni, nj=nj, nk=nk, flag=1 if kind == "w" else 0)
+        out[f"out_{kind}"] = q
+    np.savez_compressed(HERE / "open_fills_9x7x6.npz", meta=json.dumps(dict(ni=ni, nj=nj, nk=nk)), **out)
+    print("wrote open_fills_9x7x6")
+
+
 def make_wk(reference: Path) -> None:
     """CM1 r21.1's own Weisman-Klemp base state (isnd=5, nz=40, dz=500 m) as
     float32 words, from the CM1 output the reference keeps
@@ -948,7 +1048,7 @@ def make_c1(reference: Path, checkpoints: list[int]) -> None:
 def main() -> None:
     p = argparse.ArgumentParser()
     p.add_argument("--reference", type=Path, required=True, help="root of the reference source tree")
-    p.add_argument("what", choices=("small", "c1", "advection", "kessler", "tke", "rk", "bridge", "wk", "limits", "closure", "tkeevo", "momentum", "terrainopen"))
+    p.add_argument("what", choices=("small", "c1", "advection", "kessler", "tke", "rk", "bridge", "wk", "limits", "closure", "tkeevo", "momentum", "terrainopen", "kesslerstep", "fills"))
     p.add_argument("--checkpoints", type=int, nargs="+", default=[1])
     args = p.parse_args()
     if args.what == "small":
@@ -975,6 +1075,10 @@ def main() -> None:
         make_momentum(args.reference)
     elif args.what == "terrainopen":
         make_terrain_open(args.reference)
+    elif args.what == "kesslerstep":
+        make_kessler_large_step(args.reference)
+    elif args.what == "fills":
+        make_fills(args.reference)
     else:
         make_c1(args.reference, sorted(set(args.checkpoints)))
 

@@ -1,0 +1,70 @@
+"""Pins of the moist-step pieces of the oracle: the open-lateral fills
+against the reference's own cpu_bc*_open_inplace (golden), and the interior
+of the final-stage pdef chain against the twin-pinned pdef direction
+(cpu_pdef_direction_inplace restated in rk_oracle.c): fed the chain's own
+directional advection, it must leave the same words the chain leaves on
+every interior cell of every axis.  The chain's fluxes, the moist buoyancy
+and getdiv/getdivx restate the reference's kernel source (no CPU twin
+exists for them)."""
+
+from __future__ import annotations
+
+import json
+
+import numpy as np
+import pytest
+
+from oracle import moist_step as om
+from oracle import rk as rk
+from tests._golden import GOLDEN
+from tests.golden.make_golden import moist_piece_fixture
+
+
+@pytest.mark.parametrize("kind", list(om.FILL))
+def test_fill_matches_reference(kind):
+    z = np.load(GOLDEN / "open_fills_9x7x6.npz")
+    meta = json.loads(str(z["meta"]))
+    q = z[f"in_{kind}"].copy()
+    om.open_fill(q, kind, **meta)
+    assert np.array_equal(q.view(np.uint32), z[f"out_{kind}"].view(np.uint32))
+
+
+def chain_arrays(ni, nj, nk, seed):
+    a = moist_piece_fixture(ni, nj, nk, seed)
+    mass, su, sv, sw = (nk, nj, ni), a["rru"].shape, a["rrv"].shape, a["rrw"].shape
+    c = {n: a[n] for n in ("scalar_a", "scalar_padded", "rho0_3d", "gz", "rgz", "rr0", "c1", "c2", "divx", "rru",
+                           "rrv", "rrw")}
+    c.update(fx=np.zeros(su, np.float32), fy=np.zeros(sv, np.float32), fz=np.zeros(sw, np.float32),
+             advx=np.zeros(mass, np.float32), advy=np.zeros(mass, np.float32), advz=np.zeros(mass, np.float32),
+             candidate=np.zeros(mass, np.float32), advection=np.zeros(mass, np.float32))
+    return c
+
+
+def test_chain_interior_matches_twin_pinned_pdef_direction():
+    ni, nj, nk = 13, 11, 10
+    kw = dict(ni=ni, nj=nj, nk=nk, dttmp=2.0, dx=400.0, dy=300.0, dz=200.0, weps=1e-20, lateral_obc=0, pdefweno=1)
+    pre = chain_arrays(ni, nj, nk, 5)
+    om.pdef_moisture_directional(pre, **kw)
+    full = chain_arrays(ni, nj, nk, 5)
+    om.pdef_moisture_chain(full, **kw)
+    flux = {"x": pre["rru"], "y": pre["rrv"], "z": pre["rrw"]}
+    spacing = {"x": 400.0, "y": 300.0, "z": 200.0}
+    repaired = 0
+    for axis, name in (("x", "advx"), ("y", "advy"), ("z", "advz")):
+        d = pre[name].copy()
+        cand = np.zeros_like(d)
+        rk.pdef_direction(pre["scalar_a"], pre["scalar_padded"], pre["rho0_3d"], pre["gz"], pre["rgz"], flux[axis], d,
+                          cand, axis=axis, dt=2.0, spacing=spacing[axis])
+        inner = (slice(None), slice(1, nj - 1), slice(1, ni - 1)) if axis != "z" else (slice(None),) * 3
+        assert np.array_equal(d[inner].view(np.uint32), full[name][inner].view(np.uint32)), axis
+        repaired += int(np.count_nonzero(d != pre[name]))
+    assert repaired > 0
+
+
+def test_chain_with_open_sides_fills_every_cell():
+    ni, nj, nk = 12, 9, 8
+    a = chain_arrays(ni, nj, nk, 6)
+    a["advection"][:] = np.nan
+    om.pdef_moisture_chain(a, ni=ni, nj=nj, nk=nk, dttmp=1.5, dx=250.0, dy=250.0, dz=150.0, weps=1e-20,
+                           lateral_obc=0x2222, pdefweno=0)
+    assert np.isfinite(a["advection"]).all()
