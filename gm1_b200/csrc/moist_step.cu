@@ -641,6 +641,37 @@ __global__ void __launch_bounds__(256) pack_scalar_kernel(const float *s, float 
     }
 }
 
+// bc.F:1151-1178 on the physical bottom faces (cpu_bcwsfc_terrain_physical_inplace)
+__global__ void __launch_bounds__(256) bcwsfc_kernel(const float *u, const float *v, float *w, const float *gz,
+                                                    const float *dzdx, const float *dzdy, Lane L) {
+    const size_t n = (size_t)L.nj * L.ni;
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+        const int i0 = (int)(q % L.ni), j0 = (int)(q / L.ni), y = j0 + 3, x = i0 + 3;
+        const float ut = (u[L.u(1, y, x)] + u[L.u(1, y, x + 1)]) * dzdx[q];
+        const float vt = (v[L.v(1, y, x)] + v[L.v(1, y + 1, x)]) * dzdy[q];
+        w[L.s(1, y, x)] = (0.5f * (ut + vt)) * gz[q];
+    }
+}
+
+// cm1_momentum_rk_bc2d_open_v1: the w(1) slab's open halo, west and east
+// over every row (pass 0), then south and north over every column (pass 1)
+__global__ void __launch_bounds__(256) w_level1_fill_kernel(float *w, Lane L, int pass) {
+    const int nx = L.ni + 6, ny = L.nj + 6;
+    const size_t n = pass == 0 ? (size_t)ny * 6 : (size_t)nx * 6;
+    float *s = w + (size_t)1 * nx * ny;
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+        if (pass == 0) {
+            const int y = (int)(q / 6), h = (int)(q % 6);
+            const int x = h < 3 ? h : 3 + L.ni + (h - 3), sx = h < 3 ? 3 : 3 + L.ni - 1;
+            s[(size_t)y * nx + x] = s[(size_t)y * nx + sx];
+        } else {
+            const int x = (int)(q % nx), h = (int)(q / nx);
+            const int y = h < 3 ? h : 3 + L.nj + (h - 3), sy = h < 3 ? 3 : 3 + L.nj - 1;
+            s[(size_t)y * nx + x] = s[(size_t)sy * nx + x];
+        }
+    }
+}
+
 }  // namespace
 }  // namespace gm1b
 
@@ -839,4 +870,32 @@ extern "C" int32_t gm1b_pack_scalar(int32_t ni, int32_t nj, int32_t nk, const fl
     pack_scalar_kernel<<<grid_for((size_t)ni * nj * nk), 256, 0, st>>>(scalar, padded, Lane{ni, nj, nk});
     ps.stop();
     return launch_ok("pack_scalar_kernel") ? GM1B_OK : GM1B_ERR_CUDA;
+}
+
+extern "C" int32_t gm1b_bcwsfc(int32_t ni, int32_t nj, int32_t nk, const float *u3d, const float *v3d, float *w3d,
+                               const float *gz, const float *dzdx, const float *dzdy, void *stream) {
+    if (!u3d || !v3d || !w3d || !gz || !dzdx || !dzdy || !grid_ok(ni, nj, nk, 1, 1, 1, "gm1b_bcwsfc")) {
+        if (!u3d || !v3d || !w3d || !gz || !dzdx || !dzdy) gm1b_set_error("gm1b_bcwsfc: NULL array");
+        return GM1B_ERR_ARGUMENT;
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    ProfScope ps("bcwsfc_kernel", st);
+    bcwsfc_kernel<<<grid_for((size_t)ni * nj), 256, 0, st>>>(u3d, v3d, w3d, gz, dzdx, dzdy, Lane{ni, nj, nk});
+    ps.stop();
+    return launch_ok("bcwsfc_kernel") ? GM1B_OK : GM1B_ERR_CUDA;
+}
+
+extern "C" int32_t gm1b_w_level1_fill(int32_t ni, int32_t nj, int32_t nk, float *w3d, void *stream) {
+    if (!w3d || !grid_ok(ni, nj, nk, 1, 1, 1, "gm1b_w_level1_fill")) {
+        if (!w3d) gm1b_set_error("gm1b_w_level1_fill: NULL array");
+        return GM1B_ERR_ARGUMENT;
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    for (int pass = 0; pass < 2; ++pass) {
+        ProfScope ps("w_level1_fill_kernel", st);
+        w_level1_fill_kernel<<<grid_for((size_t)(std::max(ni, nj) + 6) * 6), 256, 0, st>>>(w3d, Lane{ni, nj, nk}, pass);
+        ps.stop();
+        if (!launch_ok("w_level1_fill_kernel")) return GM1B_ERR_CUDA;
+    }
+    return GM1B_OK;
 }

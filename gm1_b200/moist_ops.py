@@ -52,7 +52,9 @@ def _lib():
         lib.gm1b_held_compose.argtypes = [i, i, i, c.POINTER(_Held), f, vp]
         lib.gm1b_solve3_density.argtypes = [i, i, i] + [vp] * 5 + [vp]
         lib.gm1b_pack_scalar.argtypes = [i, i, i, vp, vp, vp]
-        for n in ("gm1b_open_fill", "gm1b_moist_buoyancy", "gm1b_post_acoustic_flux", "gm1b_pdef_moisture_chain",
+        lib.gm1b_bcwsfc.argtypes = [i, i, i] + [vp] * 7
+        lib.gm1b_w_level1_fill.argtypes = [i, i, i, vp, vp]
+        for n in ("gm1b_bcwsfc", "gm1b_w_level1_fill", "gm1b_open_fill", "gm1b_moist_buoyancy", "gm1b_post_acoustic_flux", "gm1b_pdef_moisture_chain",
                   "gm1b_held_compose", "gm1b_solve3_density", "gm1b_pack_scalar"):
             getattr(lib, n).restype = i
         lib._mops_bound = True
@@ -114,3 +116,14 @@ def solve3_density(rho, c1, c2, rr, rf, *, ni: int, nj: int, nk: int, stream: An
 def pack_scalar(scalar, padded, *, ni: int, nj: int, nk: int, stream: Any | None = None) -> None:
     _native.check(_lib().gm1b_pack_scalar(ni, nj, nk, _f32(scalar, "scalar"), _f32(padded, "padded"),
                                           _st(stream, scalar.device)), "gm1b_pack_scalar")
+
+
+
+def bcwsfc(u3d, v3d, w3d, gz, dzdx, dzdy, *, ni: int, nj: int, nk: int, stream: Any | None = None) -> None:
+    ptrs = [_f32(t, n) for t, n in zip((u3d, v3d, w3d, gz, dzdx, dzdy), ("u3d", "v3d", "w3d", "gz", "dzdx", "dzdy"))]
+    _native.check(_lib().gm1b_bcwsfc(ni, nj, nk, *ptrs, _st(stream, u3d.device)), "gm1b_bcwsfc")
+
+
+def w_level1_fill(w3d, *, ni: int, nj: int, nk: int, stream: Any | None = None) -> None:
+    _native.check(_lib().gm1b_w_level1_fill(ni, nj, nk, _f32(w3d, "w3d"), _st(stream, w3d.device)),
+                  "gm1b_w_level1_fill")

@@ -1,0 +1,483 @@
+"""The moist large step on B200: the operators of this package composed in
+the reference's large-step schedule (StepPhase / large_step_schedule,
+src/cm1core/gm1_runtime.py:611-627, :1969-2007) on the padded (ng = 3)
+open-lateral lane with Kessler warm rain, WENO5 moisture and the 1.5-order
+TKE closure.
+
+Phase bindings (reference phase methods they follow):
+
+  CLOSURE             calcnm, calcdef, tkekm + TKE source, turbt once per step
+                      (CartesianClosure, src/cm1core/cuda_cartesian_closure.py:1118-1200)
+  HELD_TENDENCIES     held theta/qv/qc rates and ppten (finalize_held_tendencies,
+                      src/cm1core/cuda_cartesian_dynamics.py:1014)
+  PRE_ACOUSTIC        eqtset2 stage terms, w(1) surface fill, momentum advection with the
+                      bcw(rrw) lateral fill between mass flux and transport, moist buoyancy (:1047-1125)
+  ACOUSTIC            terrain/open psolver3 stage without its stage fills (:1127-1202)
+  POST_ACOUSTIC       getdiv on the averaged velocities, getdivx mass fluxes and divx (:1204-1233)
+  SCALAR_MOIST        theta and qv/qc/qr advection (WENO5 at nrk = 3) and the RK update; the
+                      final stage's moisture advection is the pdef chain alone (:1235-1274)
+  MOMENTUM_BOUNDARIES bcu, bcv, bcw(flag 1), bcwsfc (:1276-1297)
+  SCALAR_BOUNDARIES   bcp of pp3d between stages (:1299-1318)
+  TKE                 TKE advection + RK stage (CartesianClosure.tke_rk, :1635)
+  MICROPHYSICS        the Kessler once-per-large-step transition: held-rate remove and snapshot,
+                      pre-physics EOS, the Kessler operator, held-rate recapture
+                      (cpu_gm1_kessler_large_step_inplace, src/cm1core/cuda_gm1_kessler_large_step.py:183);
+                      REMOVE_HELD_EOS and POST_PHYSICS are its first and last parts
+  SOLVE3              ppx accumulation, A-level promotion, rr/rf (cuda_cartesian_finish.py:739)
+
+Left out identically in this composition and in the oracle's: SGS stress and
+scalar diffusion tendencies, Rayleigh damping, the dry-mass correction
+(MASS_BEGIN / MASS_FINISH), surface fluxes.  Terrain metrics may be flat
+(gz = 1, zero slopes); every operator keeps its terrain arithmetic.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import functools
+from dataclasses import dataclass
+from enum import Enum
+from typing import Any
+
+import numpy as np
+import torch
+
+from . import _native
+from . import moist_ops as mo
+from .advection import launch_cuda_scalar_advection5
+from .closure import launch_cuda_moist_nm, launch_cuda_terrain_deformation
+from .kessler import (Gm1KesslerDriverSelection, Gm1KesslerHeldCarriers, create_cuda_gm1_kessler_large_step_transition)
+from .moist_bridge import launch_cuda_eqtset2_stage_terms
+from .scalar_rk import (compose_scalar_moist_rk_stage, moisture_weps_f64, scalar_moist_rk_stage_timestep_f32,
+                        theta_transport_scalar, theta_weps_f64)
+from .terrain_open import (ALL_ARRAY_NAMES as TOS_ARRAY_NAMES, COLUMN_DIAGNOSTIC_NAMES, GM1B_TOS_DIAGNOSTICS,
+                           _STRUCT_METRICS as TOS_METRICS, _Arrays as _TosArrays, _Metrics as _TosMetrics,
+                           _lib as _tos_lib)
+from .tke import launch_cuda_sgs_tke
+from .tke_evolution import launch_cuda_tke_diffusion, launch_cuda_tke_rk_stage
+
+
+class StepPhase(str, Enum):
+    CLOSURE = "closure"
+    HELD_TENDENCIES = "solve1-held-tendencies"
+    PRE_ACOUSTIC = "pre-acoustic"
+    ACOUSTIC = "acoustic"
+    POST_ACOUSTIC = "post-acoustic"
+    SCALAR_MOIST = "scalar-moist-rk"
+    REMOVE_HELD_EOS = "remove-held-and-moist-eos"
+    MASS_BEGIN = "dry-mass-reduction"
+    MOMENTUM_BOUNDARIES = "momentum-boundaries"
+    SCALAR_BOUNDARIES = "scalar-boundaries"
+    TKE = "tke-rk"
+    MASS_FINISH = "dry-mass-correction"
+    PDEFQ = "positive-definite-moisture"
+    MICROPHYSICS = "microphysics"
+    POST_PHYSICS = "post-physics-eos"
+    SOLVE3 = "solve3"
+
+
+@dataclass(frozen=True, slots=True)
+class ScheduledOperation:
+    phase: StepPhase
+    nrk: int | None
+
+
+@functools.lru_cache(maxsize=1)
+def large_step_schedule() -> tuple[ScheduledOperation, ...]:
+    """CM1 r21.1 solve1 -> solve2 -> mp_driver -> solve3 chronology."""
+    order = [ScheduledOperation(StepPhase.CLOSURE, None), ScheduledOperation(StepPhase.HELD_TENDENCIES, None)]
+    for nrk in (1, 2, 3):
+        order.extend(ScheduledOperation(p, nrk) for p in (StepPhase.PRE_ACOUSTIC, StepPhase.ACOUSTIC,
+                                                          StepPhase.POST_ACOUSTIC, StepPhase.SCALAR_MOIST))
+        if nrk == 3:
+            order.extend((ScheduledOperation(StepPhase.REMOVE_HELD_EOS, nrk),
+                          ScheduledOperation(StepPhase.MASS_BEGIN, nrk)))
+        order.append(ScheduledOperation(StepPhase.MOMENTUM_BOUNDARIES, nrk))
+        if nrk < 3:
+            order.append(ScheduledOperation(StepPhase.SCALAR_BOUNDARIES, nrk))
+        order.append(ScheduledOperation(StepPhase.TKE, nrk))
+        if nrk == 3:
+            order.append(ScheduledOperation(StepPhase.MASS_FINISH, nrk))
+    order.extend(ScheduledOperation(p, None) for p in (StepPhase.PDEFQ, StepPhase.MICROPHYSICS,
+                                                       StepPhase.POST_PHYSICS, StepPhase.SOLVE3))
+    return tuple(order)
+
+
+@dataclass(frozen=True, slots=True)
+class MoistStepConfig:
+    ni: int
+    nj: int
+    nk: int
+    dx: float
+    dy: float
+    dz: float
+    dt: float
+    nsound: int
+    alph: float = 0.60
+    kdiv: float = 0.10
+    lateral_sides: tuple[int, int, int, int] = (2, 2, 2, 2)
+
+    @property
+    def obc(self) -> int:
+        w, e, s, n = self.lateral_sides
+        return w | (e << 4) | (s << 8) | (n << 12)
+
+
+NUMQ = 3  # Kessler: qv, qc, qr
+QROWS = 6  # the eqtset2 terms and calcnm read six mass rows (the last three zero)
+
+
+def moist_state_shapes(ni: int, nj: int, nk: int) -> dict[str, tuple[int, ...]]:
+    """Every array of the composed state (float32 unless named in
+    MOIST_STATE_DTYPES)."""
+    ng = 3
+    su, sv = (nk + 2, nj + 2 * ng, ni + 1 + 2 * ng), (nk + 2, nj + 1 + 2 * ng, ni + 2 * ng)
+    sw, ss, pr = (nk + 3, nj + 2 * ng, ni + 2 * ng), (nk + 2, nj + 2 * ng, ni + 2 * ng), (nk + 2, nj + 2, ni + 2)
+    mass, face, plane = (nk, nj, ni), (nk + 1, nj, ni), (nj, ni)
+    s: dict[str, tuple[int, ...]] = {}
+    for n in ("ua", "u3d", "uten", "rru"):
+        s[n] = su
+    for n in ("va", "v3d", "vten", "rrv"):
+        s[n] = sv
+    for n in ("wa", "w3d", "wten", "rrw", "fz"):
+        s[n] = sw
+    s["fx"], s["fy"] = su, sv
+    for n in ("ppi", "pp3d", "ppx", "ppd", "piadv", "ppterm", "ppten", "thv", "qk", "pk1", "pk2", "mm", "fpk", "divh",
+              "hadvp", "dum3", "elim_c", "elim_d"):
+        s[n] = pr
+    for n in COLUMN_DIAGNOSTIC_NAMES:
+        s[n] = (1,)
+    s.update(radbcw=(nk + 2, nj + 2 * ng), radbce=(nk + 2, nj + 2 * ng), radbcs=(nk + 2, ni + 2 * ng),
+             radbcn=(nk + 2, ni + 2 * ng), uh=(ni + 2 * ng,), vh=(nj + 2 * ng,), ruf=(ni + 1 + 2 * ng,),
+             rvf=(nj + 1 + 2 * ng,), scalar=ss, dum8=ss, theta_padded=ss, moisture_padded=ss)
+    for n in ("th3d", "tha", "thterm", "divergence", "theta_div", "divx", "pp3d_c", "prs", "rho", "rr", "kessler_rr",
+              "thheld", "qpten", "qtten", "qvten", "qcten", "theta_adv", "advx", "advy", "advz", "candidate",
+              "temperature", "qt", "thv_c", "qvci", "pi0_3d", "th0_3d", "fall_velocity", "ones_mass"):
+        s[n] = mass
+    s["q3d"], s["qa"] = (QROWS, *mass), (QROWS, *mass)
+    s["qheld"], s["moist_adv"] = (NUMQ, *mass), (NUMQ, *mass)
+    s["saturation_mask"] = mass
+    for n in ("rf", "nm", "defv", "defh", "tke3d", "tkea", "tketen", "tk", "grdscl", "rgrdscl", "lenscl", "dissten",
+              "cme", "ce1", "ce2", "csm", "kmh", "kmv", "khh", "khv", "tke_workspace"):
+        s[n] = face
+    s.update(uc=(nk, nj, ni + 1), vc=(nk, nj + 1, ni), wc=face, th0=(nk,), pi0=(nk,), qv0=(nk,), rain=(1, nj, ni),
+             prate=plane, asq=(3,), qbudget=(10,), ruh=(ni,), rvh=(nj,))
+    return s
+
+
+MOIST_STATE_DTYPES = {"saturation_mask": np.uint8, "asq": np.float64, "qbudget": np.float64}
+
+METRIC_NAMES = ("terrain_msl", "zh", "zf", "mh", "rmh", "mf", "rmf", "c1", "c2", "rho0_3d", "rr0", "rf0", "rrf0", "gz",
+                "rgz", "gzu", "rgzu", "gzv", "rgzv", "dzdx", "dzdy", "gx", "gxu", "gy", "gyv")
+
+
+def weisman_klemp_initial_state(cfg: MoistStepConfig, *, seed: int = 0, bubble_k: float = 3.0,
+                                noise_k: float = 0.1, bubble_radius_m: tuple[float, float] = (10000.0, 1400.0),
+                                bubble_center_z_m: float = 1400.0, bubble_cloud: float = 0.0,
+                                bubble_rain: float = 0.0) -> tuple[dict[str, np.ndarray],
+                                                                            dict[str, np.ndarray]]:
+    """Host (numpy float32) state and flat terrain metrics of a
+    Weisman-Klemp supercell start on cfg's grid: the isnd = 5 column
+    (theta, qv, pi on the mass heights), the quarter-circle hodograph, a
+    cos^2 warm bubble at the domain centre plus seeded uniform noise of
+    +-noise_k, cloud and rain water bubble_cloud / bubble_rain (kg/kg) in
+    the bubble's core (r < 1/2), TKE at its floor, zero radiation
+    histories."""
+    from .analytic_state import analytic_shear_u, analytic_shear_v, weisman_klemp_column
+
+    ni, nj, nk = cfg.ni, cfg.nj, cfg.nk
+    f = np.float32
+    shapes = moist_state_shapes(ni, nj, nk)
+    s = {n: np.zeros(sh, dtype=MOIST_STATE_DTYPES.get(n, np.float32)) for n, sh in shapes.items()}
+    zh = ((np.arange(nk, dtype=np.float64) + 0.5) * cfg.dz).astype(f)
+    col = weisman_klemp_column(zh, 1)
+    s["th0"][:], s["pi0"][:], s["qv0"][:] = col.theta_k, col.pi, col.qv_kg_per_kg
+    s["th0_3d"][:] = s["th0"][:, None, None]
+    s["pi0_3d"][:] = s["pi0"][:, None, None]
+    s["prs"][:] = col.pressure_pa[:, None, None]
+    u0 = analytic_shear_u(zh).astype(f)
+    v0 = analytic_shear_v(zh).astype(f)
+    s["u3d"][1:nk + 1] = u0[:, None, None]
+    s["v3d"][1:nk + 1] = v0[:, None, None]
+    rng = np.random.default_rng(seed)
+    x = (np.arange(ni) + 0.5) * cfg.dx - 0.5 * ni * cfg.dx
+    y = (np.arange(nj) + 0.5) * cfg.dy - 0.5 * nj * cfg.dy
+    r = np.sqrt((x[None, None, :] / bubble_radius_m[0]) ** 2 + (y[None, :, None] / bubble_radius_m[0]) ** 2 +
+                ((zh.astype(np.float64)[:, None, None] - bubble_center_z_m) / bubble_radius_m[1]) ** 2)
+    bubble = np.where(r < 1.0, bubble_k * np.cos(0.5 * np.pi * r) ** 2, 0.0)
+    s["th3d"][:] = (bubble + rng.uniform(-noise_k, noise_k, (nk, nj, ni))).astype(f)
+    s["q3d"][0] = s["qv0"][:, None, None]
+    s["q3d"][1] = np.where(r < 0.5, bubble_cloud, 0.0).astype(f)
+    s["q3d"][2] = np.where(r < 0.5, bubble_rain, 0.0).astype(f)
+    tv = (s["th0_3d"].astype(np.float64) + s["th3d"]) * s["pi0_3d"] * (1.0 + 0.61 * s["q3d"][0])
+    s["rho"][:] = (col.pressure_pa[:, None, None] / (287.04 * tv)).astype(f)
+    s["tke3d"][1:nk] = f(1.0e-4)
+    for n in ("uh", "vh", "ruf", "rvf", "ruh", "rvh", "ones_mass"):
+        s[n][:] = f(1.0)
+    m = flat_metrics(cfg, s["rho"])
+    rho = s["rho"]
+    s["rr"][:] = (f(1.0) / rho).astype(f)
+    s["rf"][1:nk] = (m["c1"][1:nk] * rho[:-1] + m["c2"][1:nk] * rho[1:]).astype(f)
+    s["rf"][0], s["rf"][nk] = rho[0], rho[nk - 1]
+    for cur, base in (("ua", "u3d"), ("va", "v3d"), ("wa", "w3d"), ("tha", "th3d"), ("qa", "q3d"), ("tkea", "tke3d"),
+                      ("ppi", "pp3d")):
+        s[cur][:] = s[base]
+    return s, m
+
+
+def flat_metrics(cfg: MoistStepConfig, rho: np.ndarray) -> dict[str, np.ndarray]:
+    """Terrain metrics of a flat uniform column: gz = 1, zero slopes, c1 =
+    c2 = 1/2, base density from the initial moist density's column means."""
+    from .terrain_open import terrain_static_shapes
+
+    ni, nj, nk = cfg.ni, cfg.nj, cfg.nk
+    f = np.float32
+    sh = terrain_static_shapes(ni=ni, nj=nj, nk=nk)
+    m = {n: np.zeros(s, f) for n, s in sh.items()}
+    for n in ("mh", "rmh", "mf", "rmf", "gz", "rgz", "gzu", "rgzu", "gzv", "rgzv"):
+        m[n][:] = f(1.0)
+    m["c1"][:], m["c2"][:] = f(0.5), f(0.5)
+    m["zh"][:] = ((np.arange(nk) + 0.5) * cfg.dz).astype(f)[:, None, None]
+    m["zf"][:] = (np.arange(nk + 1) * cfg.dz).astype(f)[:, None, None]
+    prof = rho.astype(np.float64).mean(axis=(1, 2)).astype(f)
+    m["rho0_3d"][:] = prof[:, None, None]
+    m["rr0"][:] = (f(1.0) / m["rho0_3d"]).astype(f)
+    rf = np.empty(nk + 1, f)
+    rf[1:nk] = (f(0.5) * prof[:-1] + f(0.5) * prof[1:]).astype(f)
+    rf[0], rf[nk] = prof[0], prof[nk - 1]
+    m["rf0"][:] = rf[:, None, None]
+    m["rrf0"][:] = (f(1.0) / m["rf0"]).astype(f)
+    return m
+
+
+class MoistLargeStep:
+    """The composed moist large step on one CUDA device.  ``state`` and
+    ``metrics`` are dicts of device tensors with moist_state_shapes /
+    terrain_static_shapes; everything is enqueued on ``stream`` (the current
+    stream when None) and nothing synchronises, so a whole step can be
+    captured in a CUDA graph."""
+
+    def __init__(self, cfg: MoistStepConfig, state: dict[str, torch.Tensor], metrics: dict[str, torch.Tensor], *,
+                 stream: Any | None = None) -> None:
+        self.cfg, self.s, self.m = cfg, state, metrics
+        self.stream = stream
+        ni, nj, nk = cfg.ni, cfg.nj, cfg.nk
+        s, m = state, metrics
+        self.k3 = dict(ni=ni, nj=nj, nk=nk)
+        self.grid = dict(ni=ni, nj=nj, nk=nk, dx=cfg.dx, dy=cfg.dy, dz=cfg.dz)
+        # views the operators take as whole arrays
+        self.q_rows = [s["q3d"][r] for r in range(NUMQ)]
+        self.qa_rows = [s["qa"][r] for r in range(NUMQ)]
+        self.tke_arrays = {"tkea": s["tkea"], "tke3d": s["tke3d"], "tketen": s["tketen"], "kmh": s["kmh"],
+                           "kmv": s["kmv"], "rho": s["rho"], "rf": s["rf"], "mh": m["mh"], "mf": m["mf"],
+                           "gz": m["gz"], "rgz": m["rgz"], "rgzu": m["rgzu"], "rgzv": m["rgzv"], "c1": m["c1"],
+                           "c2": m["c2"], "rrf0": m["rrf0"], "rru": s["rru"], "rrv": s["rrv"], "rrw": s["rrw"],
+                           "divx": s["divx"]}
+        self.sgs_arrays = {"ruh": s["ruh"], "rvh": s["rvh"], "rmf": m["rmf"], **{n: s[n] for n in (
+            "nm", "defv", "defh", "tkea", "tk", "grdscl", "rgrdscl", "lenscl", "dissten", "cme", "ce1", "ce2", "csm",
+            "kmh", "kmv", "khh", "khv", "tketen")}}
+        self.def_arrays = {"u3d": s["uc"], "v3d": s["vc"], "w3d": s["wc"], "rho": s["rho"], "rf": s["rf"],
+                           **{n: m[n] for n in ("c1", "c2", "gz", "rgz", "gzu", "rgzu", "gzv", "rgzv", "gx", "gy")},
+                           "defv": s["defv"], "defh": s["defh"]}
+        self.nm_arrays = {"c1": m["c1"], "c2": m["c2"], "mf": m["mf"], "pi0": s["pi0"], "th0": s["th0"],
+                          "prs": s["prs"], "pp3d": s["pp3d_c"], "th3d": s["th3d"], "q3d": s["q3d"], "nm": s["nm"],
+                          "temperature": s["temperature"], "qt": s["qt"], "thv": s["thv_c"], "qvci": s["qvci"],
+                          "saturation_mask": s["saturation_mask"]}
+        self.held_arrays = {"th0": s["th0_3d"], "pi0": s["pi0_3d"], "rho": s["rho"], "ppi": s["pp3d_c"],
+                            "tha": s["tha"], "qa": s["qa"], "qpten": s["qpten"], "qtten": s["qtten"],
+                            "qvten": s["qvten"], "qcten": s["qcten"], "thheld": s["thheld"], "qheld": s["qheld"],
+                            "ppten": s["ppten"]}
+        self.post_arrays = {"rru": s["rru"], "rrv": s["rrv"], "rrw": s["rrw"], "rgzu": m["rgzu"], "rgzv": m["rgzv"],
+                            "dzdx": m["dzdx"], "dzdy": m["dzdy"], "gz": m["gz"], "rho0_3d": m["rho0_3d"],
+                            "rf0": m["rf0"], "thterm": s["thterm"], "divergence": s["divergence"],
+                            "theta_divergence_term": s["theta_div"], "divx": s["divx"]}
+        self.chain_arrays = [{"scalar_a": self.qa_rows[r], "scalar_padded": s["moisture_padded"],
+                              "rho0_3d": m["rho0_3d"], "gz": m["gz"], "rgz": m["rgz"], "rr0": m["rr0"], "c1": m["c1"],
+                              "c2": m["c2"], "divx": s["divx"], "rru": s["rru"], "rrv": s["rrv"], "rrw": s["rrw"],
+                              "fx": s["fx"], "fy": s["fy"], "fz": s["fz"], "advx": s["advx"], "advy": s["advy"],
+                              "advz": s["advz"], "candidate": s["candidate"], "advection": s["moist_adv"][r]}
+                             for r in range(NUMQ)]
+        self.kessler = create_cuda_gm1_kessler_large_step_transition(
+            {"ruh": s["ruh"], "rvh": s["rvh"], "rmh": m["rmh"], "mh": m["mh"], "pi0": s["pi0_3d"], "th0": s["th0_3d"],
+             "rr": s["kessler_rr"], "rho": s["rho"], "pp3d": s["pp3d_c"], "th3d": s["th3d"], "prs": s["prs"],
+             "qv": self.q_rows[0], "qc": self.q_rows[1], "qr": self.q_rows[2], "fall_velocity": s["fall_velocity"],
+             "rain": s["rain"], "prate": s["prate"], "asq": s["asq"], "qbudget": s["qbudget"]},
+            **self.grid, dt=cfg.dt, selection=Gm1KesslerDriverSelection(equation_set=2), stream=stream,
+            carriers=Gm1KesslerHeldCarriers(s["qpten"], s["qtten"], s["qvten"], s["qcten"]))
+        from .momentum import _Arrays as _MomArrays, _lib as _mom_lib, _STRUCT as _MOM
+
+        self._mom_lib = _mom_lib()
+        self._mom = _MomArrays(**{n: (s[n] if n in s else m[n]).data_ptr() for n in _MOM})
+        self._tos_lib = _tos_lib()
+        self._tos = _TosArrays(**{n: s[n].data_ptr() for n in TOS_ARRAY_NAMES})
+        self._tos_m = _TosMetrics(**{n: m[n].data_ptr() for n in TOS_METRICS})
+        self.completed_steps = 0
+
+    # -- helpers -----------------------------------------------------------
+    def _st(self):
+        dev = self.s["u3d"].device
+        return torch.cuda.current_stream(dev) if self.stream is None else self.stream
+
+    def _interior_pp3d_to_compact(self) -> None:
+        nk, nj, ni = self.cfg.nk, self.cfg.nj, self.cfg.ni
+        self.s["pp3d_c"].copy_(self.s["pp3d"][1:nk + 1, 1:nj + 1, 1:ni + 1])
+
+    def _compact_pp3d_to_interior(self) -> None:
+        nk, nj, ni = self.cfg.nk, self.cfg.nj, self.cfg.ni
+        self.s["pp3d"][1:nk + 1, 1:nj + 1, 1:ni + 1].copy_(self.s["pp3d_c"])
+
+    # -- phases ------------------------------------------------------------
+    def closure(self) -> None:
+        s, cfg, st = self.s, self.cfg, self._st()
+        nk, nj, ni = cfg.nk, cfg.nj, cfg.ni
+        with torch.cuda.stream(st):
+            s["uc"].copy_(s["u3d"][1:nk + 1, 3:3 + nj, 3:4 + ni])
+            s["vc"].copy_(s["v3d"][1:nk + 1, 3:4 + nj, 3:3 + ni])
+            s["wc"].copy_(s["w3d"][1:nk + 2, 3:3 + nj, 3:3 + ni])
+            self._interior_pp3d_to_compact()
+        launch_cuda_moist_nm(self.nm_arrays, **self.k3, dz=cfg.dz, stream=st)
+        launch_cuda_terrain_deformation(self.def_arrays, **self.grid, stream=st)
+        launch_cuda_sgs_tke(self.sgs_arrays, **self.grid, stream=st)
+        with torch.cuda.stream(st):
+            s["tke3d"].copy_(s["tkea"])
+        launch_cuda_tke_diffusion(self.tke_arrays, **self.grid, dt=cfg.dt, stream=st)
+
+    def held_tendencies(self) -> None:
+        s, st = self.s, self._st()
+        with torch.cuda.stream(st):
+            s["thheld"].zero_()
+            s["qheld"].zero_()
+        mo.held_compose(self.held_arrays, **self.k3, dt=self.cfg.dt, stream=st)
+
+    def pre_acoustic(self, nrk: int) -> None:
+        s, m, cfg, st = self.s, self.m, self.cfg, self._st()
+        launch_cuda_eqtset2_stage_terms(**self.k3, th0=s["th0"], qv0=s["qv0"], pi0=s["pi0"], th3d=s["th3d"],
+                                        q3d=s["q3d"], pp3d=s["pp3d"], thv=s["thv"], ppterm=s["ppterm"],
+                                        buoyancy=s["dum8"], thterm=s["thterm"], piadv=s["piadv"], stream=st)
+        mo.open_fill(s["thv"], "pressure", **self.k3, stream=st)
+        mo.open_fill(s["dum8"], "scalar", **self.k3, stream=st)
+        with torch.cuda.stream(st):
+            s["uten"].zero_()
+            s["vten"].zero_()
+            s["wten"].zero_()
+        if nrk >= 2:
+            mo.bcwsfc(s["u3d"], s["v3d"], s["w3d"], m["gz"], m["dzdx"], m["dzdy"], **self.k3, stream=st)
+            mo.w_level1_fill(s["w3d"], **self.k3, stream=st)
+        args = (cfg.ni, cfg.nj, cfg.nk, ctypes.byref(self._mom), cfg.obc, cfg.dx, cfg.dy, cfg.dz,
+                ctypes.c_void_p(st.cuda_stream))
+        _native.check(self._mom_lib.gm1b_momentum_mass_flux5(*args), "gm1b_momentum_mass_flux5")
+        mo.open_fill(s["rrw"], "w_keep_ends", **self.k3, stream=st)
+        _native.check(self._mom_lib.gm1b_momentum_transport5(*args), "gm1b_momentum_transport5")
+        mo.moist_buoyancy(s["dum8"], m["c1"], m["c2"], m["gxu"], m["gyv"], s["uten"], s["vten"], s["wten"],
+                          **self.k3, stream=st)
+
+    def acoustic(self, nrk: int) -> None:
+        cfg, st = self.cfg, self._st()
+        stage_without_fills = 255 & ~128
+        _native.check(self._tos_lib.gm1b_terrain_open_stage(
+            cfg.ni, cfg.nj, cfg.nk, nrk, cfg.dt, cfg.nsound, cfg.dx, cfg.dy, cfg.dz, float(np.float32(cfg.alph)),
+            float(np.float32(cfg.kdiv)), stage_without_fills, 0, ctypes.byref(self._tos), ctypes.byref(self._tos_m),
+            ctypes.c_void_p(st.cuda_stream)), "gm1b_terrain_open_stage")
+
+    def post_acoustic(self, nrk: int) -> None:
+        mo.post_acoustic_flux(self.post_arrays, **self.grid, stream=self._st())
+
+    def scalar_moist(self, nrk: int) -> None:
+        s, m, cfg, st = self.s, self.m, self.cfg, self._st()
+        flux = {"rru": s["rru"], "rrv": s["rrv"], "rrw": s["rrw"]}
+        met = {"c1": m["c1"], "c2": m["c2"], "rr0": m["rr0"], "gz": m["gz"]}
+        adv = dict(**self.grid, nrk=nrk, stream=st, lateral_sides=cfg.lateral_sides, write_fluxes=False)
+        theta_transport_scalar(s["th0"], s["th3d"], s["theta_padded"], **self.k3, stream=st)
+        mo.open_fill(s["theta_padded"], "scalar", **self.k3, stream=st)
+        with torch.cuda.stream(st):
+            s["theta_adv"].zero_()
+        launch_cuda_scalar_advection5(s["theta_padded"], flux, met, s["divx"], s["theta_adv"], None,
+                                      weps=theta_weps_f64(), **adv)
+        dttmp = scalar_moist_rk_stage_timestep_f32(cfg.dt, nrk)
+        for r in range(NUMQ):
+            mo.pack_scalar(self.q_rows[r], s["moisture_padded"], **self.k3, stream=st)
+            mo.open_fill(s["moisture_padded"], "scalar", **self.k3, stream=st)
+            with torch.cuda.stream(st):
+                s["moist_adv"][r].zero_()
+            weps = moisture_weps_f64(r)
+            if nrk < 3:
+                launch_cuda_scalar_advection5(s["moisture_padded"], flux, met, s["divx"], s["moist_adv"][r], None,
+                                              weps=weps, **adv)
+            else:
+                mo.pdef_moisture_chain(self.chain_arrays[r], **self.grid, dttmp=dttmp, weps=weps,
+                                       lateral_obc=cfg.obc, pdefweno=0 if r == 0 else 1, stream=st)
+        compose_scalar_moist_rk_stage(s["tha"], s["qa"][:NUMQ], s["thheld"], s["qheld"], s["theta_div"],
+                                      s["theta_adv"], s["moist_adv"], s["th3d"], s["q3d"][:NUMQ], nrk=nrk, dt=cfg.dt,
+                                      stream=st)
+
+    def momentum_boundaries(self, nrk: int) -> None:
+        s, m, st = self.s, self.m, self._st()
+        mo.open_fill(s["u3d"], "u", **self.k3, stream=st)
+        mo.open_fill(s["v3d"], "v", **self.k3, stream=st)
+        mo.open_fill(s["w3d"], "w", **self.k3, stream=st)
+        mo.bcwsfc(s["u3d"], s["v3d"], s["w3d"], m["gz"], m["dzdx"], m["dzdy"], **self.k3, stream=st)
+
+    def scalar_boundaries(self, nrk: int) -> None:
+        mo.open_fill(self.s["pp3d"], "pressure", **self.k3, stream=self._st())
+
+    def tke_rk(self, nrk: int) -> None:
+        launch_cuda_tke_rk_stage(self.tke_arrays, workspace=self.s["tke_workspace"], **self.grid, nrk=nrk,
+                                 dt=self.cfg.dt, stream=self._st())
+
+    def microphysics(self) -> None:
+        st = self._st()
+        with torch.cuda.stream(st):
+            self._interior_pp3d_to_compact()
+        self.kessler.stream = st
+        self.kessler.apply()
+        with torch.cuda.stream(st):
+            self._compact_pp3d_to_interior()
+
+    def solve3(self) -> None:
+        s, m, st = self.s, self.m, self._st()
+        with torch.cuda.stream(st):
+            s["ppx"].add_(s["pp3d"])
+            for cur, base in (("ua", "u3d"), ("va", "v3d"), ("wa", "w3d"), ("ppi", "pp3d"), ("tha", "th3d"),
+                              ("qa", "q3d"), ("tkea", "tke3d")):
+                s[cur].copy_(s[base])
+        mo.solve3_density(s["rho"], m["c1"], m["c2"], s["rr"], s["rf"], **self.k3, stream=st)
+
+    # -- driver ------------------------------------------------------------
+    def execute(self, op: ScheduledOperation) -> None:
+        p, nrk = op.phase, op.nrk
+        if p is StepPhase.CLOSURE:
+            self.closure()
+        elif p is StepPhase.HELD_TENDENCIES:
+            self.held_tendencies()
+        elif p is StepPhase.PRE_ACOUSTIC:
+            self.pre_acoustic(nrk)
+        elif p is StepPhase.ACOUSTIC:
+            self.acoustic(nrk)
+        elif p is StepPhase.POST_ACOUSTIC:
+            self.post_acoustic(nrk)
+        elif p is StepPhase.SCALAR_MOIST:
+            self.scalar_moist(nrk)
+        elif p is StepPhase.MOMENTUM_BOUNDARIES:
+            self.momentum_boundaries(nrk)
+        elif p is StepPhase.SCALAR_BOUNDARIES:
+            self.scalar_boundaries(nrk)
+        elif p is StepPhase.TKE:
+            self.tke_rk(nrk)
+        elif p is StepPhase.MICROPHYSICS:
+            self.microphysics()
+        elif p is StepPhase.SOLVE3:
+            self.solve3()
+        # REMOVE_HELD_EOS and POST_PHYSICS are the first and last parts of
+        # the Kessler transition (MICROPHYSICS); nothing between them reads
+        # or writes its fields.  MASS_BEGIN / MASS_FINISH (dry-mass
+        # correction) and PDEFQ (the Kessler operator's own pdefq runs inside
+        # it) take no separate work here.
+
+    def step(self) -> None:
+        for op in large_step_schedule():
+            self.execute(op)
+        self.completed_steps += 1
+
+
+def upload(host: dict[str, np.ndarray], device: torch.device | str = "cuda") -> dict[str, torch.Tensor]:
+    return {k: torch.from_numpy(np.ascontiguousarray(v)).to(device) for k, v in host.items()}

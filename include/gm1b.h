@@ -523,6 +523,17 @@ GM1B_API int32_t gm1b_held_compose(int32_t ni, int32_t nj, int32_t nk, const gm1
 GM1B_API int32_t gm1b_solve3_density(int32_t ni, int32_t nj, int32_t nk, const float *rho, const float *c1,
                                      const float *c2, float *rr, float *rf, void *stream);
 
+/* Surface w on the physical bottom faces from u, v and the terrain slopes
+ * (cpu_bcwsfc_terrain_physical_inplace, src/cm1core/cuda_terrain_open_boundary.py:687);
+ * gz, dzdx, dzdy are (nj, ni). */
+GM1B_API int32_t gm1b_bcwsfc(int32_t ni, int32_t nj, int32_t nk, const float *u3d, const float *v3d, float *w3d,
+                             const float *gz, const float *dzdx, const float *dzdy, void *stream);
+
+/* The open halo of the w(1) slab: west/east over every row, then
+ * south/north over every column (cm1_momentum_rk_bc2d_open_v1,
+ * src/cm1core/cuda_momentum_rk.py, directions 0..3). */
+GM1B_API int32_t gm1b_w_level1_fill(int32_t ni, int32_t nj, int32_t nk, float *w3d, void *stream);
+
 /* Copy a compact (nk, nj, ni) scalar into the interior of its padded
  * (nk+2, nj+6, ni+6) carrier (cm1_rk_pack_scalar_v1). */
 GM1B_API int32_t gm1b_pack_scalar(int32_t ni, int32_t nj, int32_t nk, const float *scalar, float *padded,

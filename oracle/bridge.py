@@ -29,3 +29,17 @@ def eqtset2_cell(th0, qv0, pi0, qc0, qi0, th3d, pp3d, q) -> np.ndarray:
     out = np.zeros(4, np.float32)
     _lib().oracle_eqtset2_cell(th0, qv0, pi0, qc0, qi0, th3d, pp3d, qq.ctypes.data_as(_F), out.ctypes.data_as(_F))
     return out
+
+
+def eqtset2_stage_terms(*, ni, nj, nk, th0, qv0, pi0, th3d, q3d, pp3d, thv, ppterm, buoyancy, thterm, piadv) -> None:
+    """The stage-terms pass over the padded lane (base profiles, zero base condensate)."""
+    lib = _lib()
+    if not getattr(lib, "_terms_ready", False):
+        lib.oracle_eqtset2_stage_terms.argtypes = [ctypes.c_int] * 3 + [_F] * 11
+        lib.oracle_eqtset2_stage_terms.restype = None
+        lib._terms_ready = True
+    ptrs = []
+    for a in (th0, qv0, pi0, th3d, q3d, pp3d, thv, ppterm, buoyancy, thterm, piadv):
+        assert a.dtype == np.float32 and a.flags.c_contiguous
+        ptrs.append(a.ctypes.data_as(_F))
+    lib.oracle_eqtset2_stage_terms(ni, nj, nk, *ptrs)

@@ -1,0 +1,208 @@
+"""The moist large step composed from the oracle's operators - TEST
+INFRASTRUCTURE ONLY.  The same phases, in the reference's large-step
+schedule (src/cm1core/gm1_runtime.py:1969-2007), as the product's
+composition, each phase calling the oracle restatement of the operator the
+product calls there; left out identically: SGS stress and scalar diffusion,
+Rayleigh damping, the dry-mass correction, surface fluxes."""
+
+from __future__ import annotations
+
+import numpy as np
+
+from oracle import advection as oadv
+from oracle import bridge as obr
+from oracle import closure as ocl
+from oracle import kessler as oks
+from oracle import moist_step as oms
+from oracle import momentum as omom
+from oracle import rk as ork
+from oracle import terrain_open as otos
+from oracle import tke as otke
+from oracle import tke_evolution as otev
+
+NUMQ = 3
+QMAG = 1.0e-2
+EPS = 1.0e-18
+
+
+def _f32(x):
+    return float(np.float32(x))
+
+
+def moisture_weps(r: int) -> float:
+    return float(np.float32(np.float32(QMAG) * np.float32(EPS)))
+
+
+def theta_weps() -> float:
+    return float(np.float32(np.float32(10.0) * np.float32(EPS)))
+
+
+class OracleMoistStep:
+    def __init__(self, cfg, state: dict[str, np.ndarray], metrics: dict[str, np.ndarray]) -> None:
+        self.cfg, self.s, self.m = cfg, state, metrics
+        # the oracle's acoustic stage always writes its column diagnostics
+        for n in ("tri_aa", "tri_bb", "tri_cc", "tri_dd", "tri_pivot", "tri_residual"):
+            if state[n].shape != state["pp3d"].shape:
+                state[n] = np.zeros(state["pp3d"].shape, np.float32)
+        self.k3 = dict(ni=cfg.ni, nj=cfg.nj, nk=cfg.nk)
+        self.grid = dict(ni=cfg.ni, nj=cfg.nj, nk=cfg.nk, dx=cfg.dx, dy=cfg.dy, dz=cfg.dz)
+
+    def _pp3d_to_compact(self):
+        c = self.cfg
+        self.s["pp3d_c"][:] = self.s["pp3d"][1:c.nk + 1, 1:c.nj + 1, 1:c.ni + 1]
+
+    def closure(self):
+        s, m, c = self.s, self.m, self.cfg
+        nk, nj, ni = c.nk, c.nj, c.ni
+        s["uc"][:] = s["u3d"][1:nk + 1, 3:3 + nj, 3:4 + ni]
+        s["vc"][:] = s["v3d"][1:nk + 1, 3:4 + nj, 3:3 + ni]
+        s["wc"][:] = s["w3d"][1:nk + 2, 3:3 + nj, 3:3 + ni]
+        self._pp3d_to_compact()
+        ocl.moist_nm({"c1": m["c1"], "c2": m["c2"], "mf": m["mf"], "pi0": s["pi0"], "th0": s["th0"], "prs": s["prs"],
+                      "pp3d": s["pp3d_c"], "th3d": s["th3d"], "q3d": s["q3d"], "nm": s["nm"],
+                      "temperature": s["temperature"], "qt": s["qt"], "thv": s["thv_c"], "qvci": s["qvci"],
+                      "saturation_mask": s["saturation_mask"]}, **self.k3, dz=c.dz)
+        ocl.calcdef({"u3d": s["uc"], "v3d": s["vc"], "w3d": s["wc"], "rho": s["rho"], "rf": s["rf"],
+                     **{n: m[n] for n in ("c1", "c2", "gz", "rgz", "rgzu", "rgzv", "gx", "gy")},
+                     "defv": s["defv"], "defh": s["defh"]}, **self.grid)
+        otke.sgs_tke({"ruh": s["ruh"], "rvh": s["rvh"], "rmf": m["rmf"], **{n: s[n] for n in otke.NAMES
+                                                                          if n not in ("ruh", "rvh", "rmf")}},
+                     **self.grid)
+        s["tke3d"][:] = s["tkea"]
+        otev.tke_diffusion(self._tke(), **self.grid, dt=c.dt)
+
+    def _tke(self):
+        s, m = self.s, self.m
+        return {"tkea": s["tkea"], "tke3d": s["tke3d"], "tketen": s["tketen"], "kmh": s["kmh"], "kmv": s["kmv"],
+                "rho": s["rho"], "rf": s["rf"], "mh": m["mh"], "mf": m["mf"], "gz": m["gz"], "rgz": m["rgz"],
+                "rgzu": m["rgzu"], "rgzv": m["rgzv"], "c1": m["c1"], "c2": m["c2"], "rrf0": m["rrf0"],
+                "rru": s["rru"], "rrv": s["rrv"], "rrw": s["rrw"], "divx": s["divx"]}
+
+    def held_tendencies(self):
+        s = self.s
+        s["thheld"][:] = 0
+        s["qheld"][:] = 0
+        oms.held_compose({"th0": s["th0_3d"], "pi0": s["pi0_3d"], "rho": s["rho"], "ppi": s["pp3d_c"],
+                          "tha": s["tha"], "qa": s["qa"], "qpten": s["qpten"], "qtten": s["qtten"],
+                          "qvten": s["qvten"], "qcten": s["qcten"], "thheld": s["thheld"], "qheld": s["qheld"],
+                          "ppten": s["ppten"]}, **self.k3, dt=self.cfg.dt)
+
+    def _mom(self):
+        s, m = self.s, self.m
+        return {n: (s[n] if n in s else m[n]) for n in omom.NAMES}
+
+    def pre_acoustic(self, nrk):
+        s, m, c = self.s, self.m, self.cfg
+        obr.eqtset2_stage_terms(**self.k3, th0=s["th0"], qv0=s["qv0"], pi0=s["pi0"], th3d=s["th3d"], q3d=s["q3d"],
+                                pp3d=s["pp3d"], thv=s["thv"], ppterm=s["ppterm"], buoyancy=s["dum8"],
+                                thterm=s["thterm"], piadv=s["piadv"])
+        oms.open_fill(s["thv"], "pressure", **self.k3)
+        oms.open_fill(s["dum8"], "scalar", **self.k3)
+        s["uten"][:] = 0
+        s["vten"][:] = 0
+        s["wten"][:] = 0
+        if nrk >= 2:
+            oms.bcwsfc(s["u3d"], s["v3d"], s["w3d"], m["gz"], m["dzdx"], m["dzdy"], **self.k3)
+            oms.w_level1_fill(s["w3d"], **self.k3)
+        a = self._mom()
+        omom.momentum_advection5_phase(a, **self.grid, lateral_sides=c.lateral_sides, phase=1)
+        oms.open_fill(s["rrw"], "w_keep_ends", **self.k3)
+        omom.momentum_advection5_phase(a, **self.grid, lateral_sides=c.lateral_sides, phase=2)
+        oms.moist_buoyancy(s["dum8"], m["c1"], m["c2"], m["gxu"], m["gyv"], s["uten"], s["vten"], s["wten"],
+                           **self.k3)
+
+    def acoustic(self, nrk):
+        c = self.cfg
+        otos.terrain_open_stage(self.s, self.m, nrk=nrk, ni=c.ni, nj=c.nj, nk=c.nk, dt=c.dt, nsound=c.nsound,
+                                dx=c.dx, dy=c.dy, dz=c.dz, alph=_f32(c.alph), kdiv=_f32(c.kdiv), ablations=255 & ~128)
+
+    def post_acoustic(self, nrk):
+        s, m = self.s, self.m
+        oms.post_acoustic_flux({"rru": s["rru"], "rrv": s["rrv"], "rrw": s["rrw"], "rgzu": m["rgzu"],
+                                "rgzv": m["rgzv"], "dzdx": m["dzdx"], "dzdy": m["dzdy"], "gz": m["gz"],
+                                "rho0_3d": m["rho0_3d"], "rf0": m["rf0"], "thterm": s["thterm"],
+                                "divergence": s["divergence"], "theta_divergence_term": s["theta_div"],
+                                "divx": s["divx"]}, **self.grid)
+
+    def _advect(self, padded, tendency, nrk, weps):
+        s, m, c = self.s, self.m, self.cfg
+        oadv.scalar_advection5({"scalar": padded, "rru": s["rru"], "rrv": s["rrv"], "rrw": s["rrw"], "c1": m["c1"],
+                                "c2": m["c2"], "rr0": m["rr0"], "gz": m["gz"], "divx": s["divx"],
+                                "tendency": tendency, "flux_x": s["fx"], "flux_y": s["fy"], "flux_z": s["fz"]},
+                               **self.grid, nrk=nrk, weps=weps, lateral_obc=c.obc)
+
+    def scalar_moist(self, nrk):
+        s, m, c = self.s, self.m, self.cfg
+        ork.theta_pack(s["th0"], s["th3d"], s["theta_padded"], **self.k3)
+        oms.open_fill(s["theta_padded"], "scalar", **self.k3)
+        s["theta_adv"][:] = 0
+        self._advect(s["theta_padded"], s["theta_adv"], nrk, theta_weps())
+        dttmp = ork.rk_stage_dt(c.dt, nrk)
+        for r in range(NUMQ):
+            oms.pack_scalar(s["q3d"][r], s["moisture_padded"], **self.k3)
+            oms.open_fill(s["moisture_padded"], "scalar", **self.k3)
+            s["moist_adv"][r] = 0
+            if nrk < 3:
+                self._advect(s["moisture_padded"], s["moist_adv"][r], nrk, moisture_weps(r))
+            else:
+                oms.pdef_moisture_chain({"scalar_a": s["qa"][r], "scalar_padded": s["moisture_padded"],
+                                         "rho0_3d": m["rho0_3d"], "gz": m["gz"], "rgz": m["rgz"], "rr0": m["rr0"],
+                                         "c1": m["c1"], "c2": m["c2"], "divx": s["divx"], "rru": s["rru"],
+                                         "rrv": s["rrv"], "rrw": s["rrw"], "fx": s["fx"], "fy": s["fy"],
+                                         "fz": s["fz"], "advx": s["advx"], "advy": s["advy"], "advz": s["advz"],
+                                         "candidate": s["candidate"], "advection": s["moist_adv"][r]},
+                                        **self.grid, dttmp=dttmp, weps=moisture_weps(r), lateral_obc=c.obc,
+                                        pdefweno=0 if r == 0 else 1)
+        qa, q = s["qa"][:NUMQ], s["q3d"][:NUMQ]
+        ork.compose(s["tha"], qa, s["thheld"], s["qheld"], s["theta_div"], s["theta_adv"], s["moist_adv"], s["th3d"],
+                    q, nrk=nrk, dt=c.dt)
+
+    def momentum_boundaries(self, nrk):
+        s, m = self.s, self.m
+        oms.open_fill(s["u3d"], "u", **self.k3)
+        oms.open_fill(s["v3d"], "v", **self.k3)
+        oms.open_fill(s["w3d"], "w", **self.k3)
+        oms.bcwsfc(s["u3d"], s["v3d"], s["w3d"], m["gz"], m["dzdx"], m["dzdy"], **self.k3)
+
+    def scalar_boundaries(self, nrk):
+        oms.open_fill(self.s["pp3d"], "pressure", **self.k3)
+
+    def tke_rk(self, nrk):
+        s = self.s
+        otev.tke_rk_stage(self._tke(), s["tke3d"], s["tke_workspace"], **self.grid, nrk=nrk, dt=self.cfg.dt)
+        s["tke3d"][:] = s["tke_workspace"]
+
+    def microphysics(self):
+        s, m, c = self.s, self.m, self.cfg
+        self._pp3d_to_compact()
+        a = {"ruh": s["ruh"], "rvh": s["rvh"], "rmh": m["rmh"], "mh": m["mh"], "pi0": s["pi0_3d"],
+             "th0": s["th0_3d"], "rr": s["kessler_rr"], "rho": s["rho"], "pp3d": s["pp3d_c"], "th3d": s["th3d"],
+             "prs": s["prs"], "qv": s["q3d"][0], "qc": s["q3d"][1], "qr": s["q3d"][2],
+             "fall_velocity": s["fall_velocity"], "rain": s["rain"], "prate": s["prate"], "asq": s["asq"],
+             "qbudget": s["qbudget"]}
+        held = {"qpten": s["qpten"], "qtten": s["qtten"], "qvten": s["qvten"], "qcten": s["qcten"]}
+        oks.kessler_large_step(a, held, **self.grid, dt=c.dt, eqtset=2)
+        s["pp3d"][1:c.nk + 1, 1:c.nj + 1, 1:c.ni + 1] = s["pp3d_c"]
+
+    def solve3(self):
+        s, m = self.s, self.m
+        s["ppx"] += s["pp3d"]
+        for cur, base in (("ua", "u3d"), ("va", "v3d"), ("wa", "w3d"), ("ppi", "pp3d"), ("tha", "th3d"),
+                          ("qa", "q3d"), ("tkea", "tke3d")):
+            s[cur][:] = s[base]
+        oms.solve3_density(s["rho"], m["c1"], m["c2"], s["rr"], s["rf"], **self.k3)
+
+    def step(self):
+        self.closure()
+        self.held_tendencies()
+        for nrk in (1, 2, 3):
+            self.pre_acoustic(nrk)
+            self.acoustic(nrk)
+            self.post_acoustic(nrk)
+            self.scalar_moist(nrk)
+            self.momentum_boundaries(nrk)
+            if nrk < 3:
+                self.scalar_boundaries(nrk)
+            self.tke_rk(nrk)
+        self.microphysics()
+        self.solve3()

@@ -47,7 +47,9 @@ def _lib():
         lib.oracle_held_compose.argtypes = [c.c_int] * 3 + [c.POINTER(_Held), c.c_float]
         lib.oracle_solve3_density.argtypes = [c.c_int] * 3 + [_F] * 5
         lib.oracle_pack_scalar.argtypes = [c.c_int] * 3 + [_F] * 2
-        for f in ("oracle_open_fill", "oracle_moist_buoyancy", "oracle_post_acoustic_flux",
+        lib.oracle_bcwsfc.argtypes = [c.c_int] * 3 + [_F] * 6
+        lib.oracle_w_level1_fill.argtypes = [c.c_int] * 3 + [_F]
+        for f in ("oracle_bcwsfc", "oracle_w_level1_fill", "oracle_open_fill", "oracle_moist_buoyancy", "oracle_post_acoustic_flux",
                   "oracle_pdef_moisture_chain", "oracle_held_compose", "oracle_solve3_density", "oracle_pack_scalar"):
             getattr(lib, f).restype = None
         lib._ms_ready = True
@@ -89,3 +91,11 @@ def solve3_density(rho, c1, c2, rr, rf, *, ni, nj, nk):
 
 def pack_scalar(s, padded, *, ni, nj, nk):
     _lib().oracle_pack_scalar(ni, nj, nk, _p(s), _p(padded))
+
+
+def bcwsfc(u3d, v3d, w3d, gz, dzdx, dzdy, *, ni, nj, nk):
+    _lib().oracle_bcwsfc(ni, nj, nk, *(_p(x) for x in (u3d, v3d, w3d, gz, dzdx, dzdy)))
+
+
+def w_level1_fill(w3d, *, ni, nj, nk):
+    _lib().oracle_w_level1_fill(ni, nj, nk, _p(w3d))

@@ -490,3 +490,30 @@ void oracle_pack_scalar(int ni, int nj, int nk, const float *s, float *padded) {
         for (int j = 0; j < nj; ++j)
             for (int i = 0; i < ni; ++i, ++q) padded[S(&L, k, j + 3, i + 3)] = s[q];
 }
+
+void oracle_bcwsfc(int ni, int nj, int nk, const float *u, const float *v, float *w, const float *gz, const float *dzdx,
+                   const float *dzdy) {
+    const Ln L = {ni, nj, nk};
+    for (int j0 = 0; j0 < nj; ++j0)
+        for (int i0 = 0; i0 < ni; ++i0) {
+            const size_t q = (size_t)j0 * ni + i0;
+            const int y = j0 + 3, x = i0 + 3;
+            const float ut = (u[Uu(&L, 1, y, x)] + u[Uu(&L, 1, y, x + 1)]) * dzdx[q];
+            const float vt = (v[Vv(&L, 1, y, x)] + v[Vv(&L, 1, y + 1, x)]) * dzdy[q];
+            w[S(&L, 1, y, x)] = (0.5f * (ut + vt)) * gz[q];
+        }
+}
+
+void oracle_w_level1_fill(int ni, int nj, int nk, float *w) {
+    const int nx = ni + 6, ny = nj + 6;
+    float *s = w + (size_t)nx * ny;
+    (void)nk;
+    for (int y = 0; y < ny; ++y)
+        for (int h = 0; h < 3; ++h) s[(size_t)y * nx + h] = s[(size_t)y * nx + 3];
+    for (int y = 0; y < ny; ++y)
+        for (int h = 0; h < 3; ++h) s[(size_t)y * nx + 3 + ni + h] = s[(size_t)y * nx + 3 + ni - 1];
+    for (int h = 0; h < 3; ++h)
+        for (int x = 0; x < nx; ++x) s[(size_t)h * nx + x] = s[(size_t)3 * nx + x];
+    for (int h = 0; h < 3; ++h)
+        for (int x = 0; x < nx; ++x) s[(size_t)(3 + nj + h) * nx + x] = s[(size_t)(3 + nj - 1) * nx + x];
+}

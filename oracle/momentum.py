@@ -40,3 +40,18 @@ def momentum_advection5(a, *, ni, nj, nk, dx, dy, dz, lateral_sides=(2, 2, 2, 2)
     rc = _lib().oracle_momentum_advection5(ni, nj, nk, ctypes.byref(s), sides, dx, dy, dz)
     if rc != 0:
         raise ValueError(f"oracle_momentum_advection5 failed ({rc})")
+
+
+def momentum_advection5_phase(a, *, ni, nj, nk, dx, dy, dz, lateral_sides=(2, 2, 2, 2), phase) -> None:
+    """phase 1: mass fluxes and divx; 2: advu/advv/advw from them."""
+    s = MomArrays()
+    for n in NAMES:
+        setattr(s, n, a[n].ctypes.data_as(_F))
+    lib = _lib()
+    if not getattr(lib, "_mom_phase_ready", False):
+        lib.oracle_momentum_advection5_phase.argtypes = list(lib.oracle_momentum_advection5.argtypes) + [ctypes.c_int]
+        lib.oracle_momentum_advection5_phase.restype = ctypes.c_int
+        lib._mom_phase_ready = True
+    sides = (ctypes.c_int * 4)(*lateral_sides)
+    if lib.oracle_momentum_advection5_phase(ni, nj, nk, ctypes.byref(s), sides, dx, dy, dz, phase) != 0:
+        raise ValueError("oracle_momentum_advection5_phase failed")

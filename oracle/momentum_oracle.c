@@ -244,12 +244,14 @@ static float w_z(const mom_ctx* c, int k, int j, int i) {
   return mass * r;
 }
 
-int oracle_momentum_advection5(int ni, int nj, int nk, const mom_arrays* a, const int* sides, float dx, float dy,
-                               float dz) {
+/* phase bit 1: mass fluxes and divx; bit 2: advu/advv/advw from them */
+int oracle_momentum_advection5_phase(int ni, int nj, int nk, const mom_arrays* a, const int* sides, float dx,
+                                     float dy, float dz, int phase) {
   if (ni < 7 || nj < 7 || nk < 8) return -1;
   mom_ctx cc = {ni, nj, nk, {sides[0], sides[1], sides[2], sides[3]}, a};
   const mom_ctx* c = &cc;
   const float half = 0.5f;
+  if (phase & 1) {
   /* horizontal mass fluxes on every face */
   for (int k0 = 0; k0 < nk; ++k0) {
     const int k = k0 + 1;
@@ -311,6 +313,9 @@ int oracle_momentum_advection5(int ni, int nj, int nk, const mom_arrays* a, cons
         C3(c, a->divx, k0, j, i) = fabsf(value) < 1.0e-20f ? 0.0f : value;
       }
   }
+  }
+  if (!(phase & 2)) return 0;
+  const float rdx = 1.0f / dx, rdy = 1.0f / dy, rdz = 1.0f / dz;
   /* advu */
   const int first_face = per(c, 0) ? 0 : 1, last_face = per(c, 1) ? ni : ni - 1;
   const int first_row = per(c, 2) ? 0 : 1, last_row = per(c, 3) ? nj : nj - 1;
@@ -435,4 +440,9 @@ int oracle_momentum_advection5(int ni, int nj, int nk, const mom_arrays* a, cons
       }
     }
   return 0;
+}
+
+int oracle_momentum_advection5(int ni, int nj, int nk, const mom_arrays* a, const int* sides, float dx, float dy,
+                               float dz) {
+  return oracle_momentum_advection5_phase(ni, nj, nk, a, sides, dx, dy, dz, 3);
 }

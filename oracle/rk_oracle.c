@@ -165,3 +165,30 @@ void oracle_eqtset2_cell(float th0, float qv0, float pi0, float qc0, float qi0, 
     out[2] = theta_term;
     out[3] = pressure_term;
 }
+
+/* the eqtset=2 stage-terms pass over the padded lane
+ * (launch_cuda_eqtset2_stage_terms, src/cm1core/cuda_moist_stage_bridge.py:378-430):
+ * live cells give buoyancy (scalar layout), thv and ppterm (pressure box)
+ * and thterm (compact); every cell of the pressure box gets piadv from the
+ * nearest live base-state column.  Base profiles (nk), qc0 = qi0 = 0. */
+void oracle_eqtset2_stage_terms(int ni, int nj, int nk, const float *th0, const float *qv0, const float *pi0,
+                                const float *th3d, const float *q3d, const float *pp3d, float *thv, float *ppterm,
+                                float *buoyancy, float *thterm, float *piadv) {
+    const size_t n = (size_t)ni * nj * nk;
+    for (int k = 0; k < nk; ++k)
+        for (int y = 0; y < nj + 2; ++y)
+            for (int x = 0; x < ni + 2; ++x) {
+                const size_t pp = ((size_t)(k + 1) * (nj + 2) + y) * (size_t)(ni + 2) + x;
+                piadv[pp] = pi0[k] + pp3d[pp];
+                if (x < 1 || x > ni || y < 1 || y > nj) continue;
+                const size_t cell = ((size_t)k * nj + (y - 1)) * (size_t)ni + (x - 1);
+                float q[6];
+                for (int r = 0; r < 6; ++r) q[r] = q3d[(size_t)r * n + cell];
+                float out[4];
+                oracle_eqtset2_cell(th0[k], qv0[k], pi0[k], 0.0f, 0.0f, th3d[cell], pp3d[pp], q, out);
+                buoyancy[((size_t)(k + 1) * (nj + 6) + (y + 2)) * (size_t)(ni + 6) + (x + 2)] = out[0];
+                thv[pp] = out[1];
+                thterm[cell] = out[2];
+                ppterm[pp] = out[3];
+            }
+}
