@@ -1,30 +1,37 @@
 #!/usr/bin/env python
 """Throughput of the RK3 large step on B200: cell-updates/s.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload moist|dry]
 
-Workload: the dry warm bubble on the flat serial-periodic lane, 64x64x40
-cells (dx = dy = 1 km, dz = 500 m, dt = 6 s, nsound = 6, so 2 + 3 + 6 = 11
-acoustic small steps per large step), seeded synthetic initial state.  One
-"step" is one full RK3 large step (three stages: prepare, mass flux,
-momentum advection with buoyancy, the psolver=3 acoustic stage, theta
-advection and update; then ppx completion and carrier promotion) through the
-library's C ABI.  Inputs are device resident; the step is captured once as a
-CUDA graph and replayed; L2 is flushed (a 256 MiB write) before every timed
-step, outside its event pair.  Under torchrun every rank runs its own replica
-(weak scaling, no collective on the data path) and the job time is the max
-over ranks.
+Default workload (moist): the Weisman-Klemp supercell start on 256x256x80
+cells (dx = dy = 1 km, dz = 250 m, dt = 5 s, nsound = 10, so 4 + 5 + 10 =
+19 acoustic small steps per large step; open-radiative laterals), Kessler
+warm rain (equation set 2), WENO5 moisture on the final stage with the
+positive-definite chain, the 1.5-order TKE closure.  One "step" is one full
+moist RK3 large step: closure and held tendencies, three RK stages (moist
+stage terms, momentum advection, buoyancy, the terrain/open psolver=3
+acoustic stage, getdiv/getdivx, theta and qv/qc/qr advection and update,
+boundaries, TKE advection), the Kessler transition and solve3, through the
+library's C ABI.  --workload dry is the 64x64x40 dry warm bubble on the
+serial-periodic lane (nsound 6).
 
-Also measured: e2e (the same steps through the public Python API with the
-prognostic arrays copied from pinned host memory before and back after every
-step), the per-kernel device time of each kernel (library launch profiler,
-CUDA events on the launching stream) for the roofline of the dominant kernel,
-and the CPU oracle on the host cores as the CPU baseline.
+Inputs are device resident; the step is captured once as a CUDA graph and
+replayed; L2 is flushed (a 256 MiB write) before every timed step, outside
+its event pair.  Under torchrun every rank runs its own replica (weak
+scaling, no collective on the data path) and the job time is the max over
+ranks.
+
+Also measured: e2e (the same steps with the prognostic fields copied from
+pinned host memory before and back after every step), the per-kernel device
+time of each kernel (library launch profiler, CUDA events on the launching
+stream) for the roofline of the dominant kernel, and the CPU oracle on the
+host cores as the CPU baseline.
 
 --impl reference times the reference algorithm's CPU implementation on the
-host cores: the C restatement of the reference's NumPy twins in oracle/
-(bit-identical to them; the reference itself is Python/CuPy and cannot run on
-the GPU box), with all host threads, on the same workload and metric.
+host cores: the C restatement of the reference's CPU twins in oracle/ (the
+reference itself is Python/CuPy and cannot run on the GPU box), composed in
+the same large-step schedule, with all host threads, on a bounded sub-block
+of the same workload and the same metric.
 """
 
 from __future__ import annotations
@@ -44,10 +51,18 @@ sys.path.insert(0, str(ROOT))
 METRIC = "cell-updates/s per RK3 step (fwd, adjoint, ensemble) and % of HBM roofline"
 UNIT = "cell-updates/s"
 WORKLOAD = "dry periodic RK3 trajectory, warm bubble 64x64x40 (dx=dy=1 km, dz=500 m, dt=6 s, nsound=6)"
+MOIST_WORKLOAD = ("moist Weisman-Klemp supercell 256x256x80 (dx=dy=1 km, dz=250 m, dt=5 s, nsound=10, Kessler eqtset 2, "
+                  "WENO5 moisture, TKE sgsmodel 1, open-radiative laterals)")
 
-# Algorithmic bytes of one full RK3 large step per cell-update for this
-# workload (dry, nsound = 6: 3*(8+6) + 20*11 + 2 = 264 words = 1,056 B).
+# Algorithmic bytes of one full RK3 large step per cell-update (4-byte
+# words, each compulsory field once read and once written per grid pass):
+# dry, nsound = 6: 3*(8+6) + 20*11 + 2 = 264 words = 1,056 B;
+# moist, nsound = 10: 149 + 20*19 = 529 words = 2,116 B (16 closure/held,
+# 3*(16+23) pre-acoustic and scalar passes, 20 per acoustic small step,
+# 14 Kessler, 2 ppx).
 STEP_BYTES_PER_CELL = 1056
+MOIST_SMALL_STEPS = 4 + 5 + 10
+MOIST_STEP_BYTES_PER_CELL = 4 * (149 + 20 * MOIST_SMALL_STEPS)
 
 # Algorithmic words per cell of one launch of each kernel: every full field
 # the launch must read or write once (stencil re-reads, halo words and
@@ -73,6 +88,17 @@ KERNEL_WORDS_PER_CELL = {
     "traj_theta_prep_kernel": 9,
     # in: rru rrv rrw sadv tha c1 c2 rr0; out: divx thten th3d
     "traj_theta_kernel": 11,
+    # moist step: terrain/open acoustic stage
+    # in: u v w pp3d qk pk1 pk2 mm ppten ppterm piadv rr0 rrf0 wten rru rrv rrw; out: w pp3d ppd rru rrv rrw
+    "tos_column_kernel": 23,
+    # in: ppd thv uten vten gxu gyv u v; out: u v
+    "tos_pgrad_kernel": 10,
+    # in: ppx ppi ua va wa ppterm piadv c1 c2 rf0 rr0 thv; out: ppd pp3d rru rrv rrw u v w qk pk1 pk2 mm
+    "tos_prepare_kernel": 24,
+    # in: scalar rru rrv rrw divx rr0 c1 c2; out: tendency
+    "scalar_advection5_kernel": 9,
+    # in: u v w rru rrv rrw divx rho0 rf0 rrf0 c2 gz; in+out: uten vten wten
+    "mom5_adv_kernel": 18,
 }
 
 PROGNOSTIC = ("ua", "u3d", "va", "v3d", "wa", "w3d", "ppi", "pp3d", "ppx", "tha", "th3d")
@@ -203,18 +229,262 @@ def run_reference(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+MOIST_GRID = dict(ni=256, nj=256, nk=80, dx=1000.0, dy=1000.0, dz=250.0, dt=5.0, nsound=10)
+MOIST_INIT = dict(seed=2, bubble_k=3.0, noise_k=0.1, bubble_radius_m=(10000.0, 1500.0), bubble_center_z_m=1500.0)
+# step-start state a user passes in and reads back: the A-level prognostic
+# fields (each copied into its RK-stage twin on the device) and ppx
+MOIST_PROGNOSTIC = ("ua", "va", "wa", "ppi", "tha", "qa", "tkea", "ppx")
+MOIST_STAGE_TWIN = {"ua": "u3d", "va": "v3d", "wa": "w3d", "ppi": "pp3d", "tha": "th3d", "qa": "q3d", "tkea": "tke3d"}
+CPU_SUBBLOCK = (64, 64, 80)
+
+
+def moist_state(ni, nj, nk):
+    from gm1_b200.moist_step import MoistStepConfig, weisman_klemp_initial_state
+
+    g = dict(MOIST_GRID, ni=ni, nj=nj, nk=nk)
+    cfg = MoistStepConfig(**g)
+    host, metrics = weisman_klemp_initial_state(cfg, **MOIST_INIT)
+    return cfg, host, metrics
+
+
+def moist_cpu_rate(steps_min: int, seconds_target: float, threads: int, warmup: int = 1) -> tuple[float, int, float]:
+    """The oracle composition on a sub-block of the moist workload on the
+    host cores: (cell-updates/s, steps, seconds)."""
+    from oracle import periodic as orc
+    from oracle.moist_composition import OracleMoistStep
+
+    orc.set_threads(threads)
+    cfg, host, metrics = moist_state(*CPU_SUBBLOCK)
+    o = OracleMoistStep(cfg, host, metrics)
+    for _ in range(warmup):
+        o.step()
+    n = 0
+    t0 = time.perf_counter()
+    while n < steps_min or time.perf_counter() - t0 < seconds_target:
+        o.step()
+        n += 1
+    dt = time.perf_counter() - t0
+    return cfg.ni * cfg.nj * cfg.nk * n / dt, n, dt
+
+
+def run_reference_moist(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    value, n, dt = moist_cpu_rate(args.steps, 0.0, threads, warmup=args.warmup)
+    ni, nj, nk = CPU_SUBBLOCK
+    sample = (f"{n} moist RK3 large steps of a {ni}x{nj}x{nk} sub-block of the workload (same spacing, dt, "
+              f"nsound and initial state) in {dt:.2f} s after {args.warmup} warm-up steps: the oracle's C "
+              "restatements of the reference CPU twins composed in the large-step schedule")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / n,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded Weisman-Klemp supercell start)",
+        "config": {"workload": MOIST_WORKLOAD, "cells": 256 * 256 * 80, "device": "host CPU",
+                   "sample": f"{ni}x{nj}x{nk} sub-block per step"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def _dist_setup():
+    import torch
+    import torch.distributed as dist
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=device)
+
+    def barrier():
+        torch.cuda.synchronize(device)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(device)
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    return rank, world, local, device, barrier, max_over_ranks
+
+
+def run_moist(args) -> None:
+    import torch
+    import torch.distributed as dist
+
+    from gm1_b200 import _native
+    from gm1_b200.moist_step import MoistLargeStep, upload
+
+    rank, world, local, device, barrier, max_over_ranks = _dist_setup()
+    cfg, host, metrics = moist_state(MOIST_GRID["ni"], MOIST_GRID["nj"], MOIST_GRID["nk"])
+    cells = cfg.ni * cfg.nj * cfg.nk
+    stream = torch.cuda.Stream(device)
+    dev_state, dev_metrics = upload(host, device), upload(metrics, device)
+    with torch.cuda.stream(stream):
+        model = MoistLargeStep(cfg, dev_state, dev_metrics, stream=stream)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            model.step()
+        stream.synchronize()
+        graph = torch.cuda.CUDAGraph()
+        try:
+            with torch.cuda.graph(graph, stream=stream):
+                model.step()
+            use_graph = True
+        except Exception as exc:  # noqa: BLE001 - capture refused: time direct launches
+            print(f"CUDA graph capture failed ({exc}); timing direct launches", file=sys.stderr)
+            torch.cuda.synchronize(device)
+            use_graph = False
+
+        def step() -> None:
+            if use_graph:
+                graph.replay()
+            else:
+                model.step()
+
+        for _ in range(args.warmup):
+            step()
+        stream.synchronize()
+
+    # ---- timed region: K graph replays, L2 flushed before each ----------
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    sampler = ClockSampler(local)
+    barrier()
+    sampler.start()
+    with torch.cuda.stream(stream):
+        for q in range(args.steps):
+            flush.zero_()
+            starts[q].record(stream)
+            step()
+            ends[q].record(stream)
+    barrier()
+    clocks = sampler.stop()
+    total_ms = max_over_ranks(sum(s.elapsed_time(e) for s, e in zip(starts, ends)))
+    ms_per_step = total_ms / args.steps
+    value = world * cells * args.steps / (total_ms * 1e-3)
+
+    # ---- per-kernel device time (eager steps, launch profiler on) -------
+    nprof = min(args.steps, 5)
+    _native.profiler_enable(True)
+    with torch.cuda.stream(stream):
+        for _ in range(nprof):
+            flush.zero_()
+            model.step()
+    stream.synchronize()
+    _native.profiler_enable(False)
+    stats = _native.profiler_collect()
+    launches_per_step = sum(s["launches"] for s in stats) / nprof
+    top = stats[0]
+    avg_ms = top["total_ms"] / top["launches"]
+    peak, peak_kind = load_peaks()
+    words = KERNEL_WORDS_PER_CELL.get(top["name"])
+    achieved = None if words is None else words * 4 * cells / (avg_ms * 1e-3) / 1e9
+    traffic = None
+    tfile = ROOT / "profiles" / "traffic_per_launch.json"
+    if tfile.exists():
+        traffic = json.loads(tfile.read_text()).get(top["name"])
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": None if achieved is None else achieved / peak, "traffic": traffic, "kernel": top["name"],
+                "avg_launch_ms": avg_ms, "alg_bytes_per_launch": None if words is None else words * 4 * cells,
+                "peak_source": f"{peak_kind} hbm_gbs"}
+    tot = sum(x["total_ms"] for x in stats)
+    kernel_share = {s["name"]: round(s["total_ms"] / tot, 4) for s in stats[:16]}
+
+    # ---- e2e: prognostic fields in from pinned host memory, out after ----
+    pinned = {n: torch.from_numpy(host[n]).pin_memory() for n in MOIST_PROGNOSTIC}
+    with torch.cuda.stream(stream):
+        for n, t in pinned.items():
+            t.copy_(dev_state[n], non_blocking=True)
+    stream.synchronize()
+    h2d = sum(t.numel() * 4 for t in pinned.values())
+    e_start = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    e_end = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    barrier()
+    with torch.cuda.stream(stream):
+        for q in range(args.steps):
+            flush.zero_()
+            e_start[q].record(stream)
+            for n, t in pinned.items():
+                dev_state[n].copy_(t, non_blocking=True)
+            for n, twin in MOIST_STAGE_TWIN.items():
+                dev_state[twin].copy_(dev_state[n])
+            step()
+            for n, t in pinned.items():
+                t.copy_(dev_state[n], non_blocking=True)
+            e_end[q].record(stream)
+    barrier()
+    e2e_ms = max_over_ranks(sum(s.elapsed_time(e) for s, e in zip(e_start, e_end)))
+    e2e_value = world * cells * args.steps / (e2e_ms * 1e-3)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        rate, n, dt = moist_cpu_rate(3, 10.0, threads)
+        ni, nj, nk = CPU_SUBBLOCK
+        cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"{n} moist RK3 large steps of a {ni}x{nj}x{nk} sub-block of the workload in {dt:.2f} s "
+                         "(the oracle's C restatements of the reference CPU twins composed in the same schedule)"}
+    del graph
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded Weisman-Klemp supercell start: isnd 5 column, iwnd 2 hodograph, +3 K bubble, "
+                "U(+-0.1 K) noise from numpy default_rng(2))",
+        "config": {"workload": MOIST_WORKLOAD, "mode": "fwd", "cells": cells, "large_steps_per_timed_step": 1,
+                   "acoustic_small_steps_per_step": MOIST_SMALL_STEPS,
+                   "l2": "flushed before every timed step (256 MiB write, outside the event pair)",
+                   "cuda_graph": use_graph, "lateral_boundaries": "open-radiative (wbc=ebc=sbc=nbc=2)",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single domain"},
+        "step_roofline": {"bytes_per_cell_update": MOIST_STEP_BYTES_PER_CELL,
+                          "achieved_gbs": MOIST_STEP_BYTES_PER_CELL * value / world / 1e9,
+                          "frac": MOIST_STEP_BYTES_PER_CELL * value / world / 1e9 / peak},
+        "roofline": roofline, "kernel_share": kernel_share,
+        "gpu_launches": int(round(launches_per_step * args.steps)),
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d},
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", choices=("moist", "dry"), default="moist")
     args = ap.parse_args()
+    if args.steps is None:
+        args.steps = 20 if args.workload == "moist" else 2000
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":
-        run_reference(args)
+        (run_reference_moist if args.workload == "moist" else run_reference)(args)
+        return
+    if args.workload == "moist":
+        run_moist(args)
         return
 
     import torch

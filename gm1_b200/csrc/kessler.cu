@@ -369,7 +369,24 @@ __global__ void kessler_rows_kernel(KDims d, KWork w) {
     w.rows[(size_t)t * d.nj + j] = s;
 }
 
-// single thread: ordered finish of every budget
+// grid (nk, 5): block (k, t) sums the nj*nbx cell-kernel partials of budget
+// term t at level k (strided per thread, then a fixed warp/block tree, so the
+// result is the same on every run) and leaves the level total in the level's
+// first slot, where the finish kernel reads it.
+constexpr int kLevelThreads = 256;
+__global__ void __launch_bounds__(kLevelThreads) kessler_levels_kernel(KDims d, KWork w) {
+    __shared__ double s_red[kLevelThreads / 32];
+    const int k = blockIdx.x, t = blockIdx.y;
+    const size_t n = (size_t)d.nj * w.nbx;
+    double *level = w.partial + (size_t)t * d.nk * n + (size_t)k * n;
+    double s = 0.0;
+    for (size_t q = threadIdx.x; q < n; q += kLevelThreads) s += level[q];
+    s = block_sum(s, s_red);
+    if (threadIdx.x == 0) level[0] = s;
+}
+
+// single thread: ordered finish of every budget (row sums of asq in j order,
+// level totals of qbudget in k order)
 __global__ void kessler_finish_kernel(gm1b_kessler_arrays a, KDims d, KWork w, double volume, double dxd,
                                       double dyd, double area) {
     if (blockIdx.x != 0 || threadIdx.x != 0) return;
@@ -377,19 +394,11 @@ __global__ void kessler_finish_kernel(gm1b_kessler_arrays a, KDims d, KWork w, d
         for (int j = 0; j < d.nj; ++j) a.asq[s] += w.rows[(size_t)s * d.nj + j] * volume;
     for (int j = 0; j < d.nj; ++j) a.qbudget[6] += w.rows[(size_t)3 * d.nj + j] * dxd * dyd;
     for (int j = 0; j < d.nj; ++j) a.qbudget[5] += w.rows[(size_t)4 * d.nj + j] * area;
-    const size_t plane = (size_t)d.nk * d.nj * w.nbx;
+    const size_t n = (size_t)d.nj * w.nbx, plane = (size_t)d.nk * n;
     for (int p = 0; p < 3; ++p)
-        for (int k = 0; k < d.nk; ++k) {
-            double s = 0.0;
-            for (size_t q = 0; q < (size_t)d.nj * w.nbx; ++q) s += w.partial[p * plane + (size_t)k * d.nj * w.nbx + q];
-            a.qbudget[2 + p] = a.qbudget[2 + p] + s * volume;
-        }
+        for (int k = 0; k < d.nk; ++k) a.qbudget[2 + p] = a.qbudget[2 + p] + w.partial[p * plane + (size_t)k * n] * volume;
     for (int p = 3; p < 5; ++p)
-        for (int k = 0; k < d.nk; ++k) {
-            double s = 0.0;
-            for (size_t q = 0; q < (size_t)d.nj * w.nbx; ++q) s += w.partial[p * plane + (size_t)k * d.nj * w.nbx + q];
-            a.qbudget[p - 3] += s * volume;
-        }
+        for (int k = 0; k < d.nk; ++k) a.qbudget[p - 3] += w.partial[p * plane + (size_t)k * n] * volume;
 }
 
 bool launched(const char *what) {
@@ -474,6 +483,12 @@ extern "C" int32_t gm1b_kessler_driver(int32_t ni, int32_t nj, int32_t nk, const
         ps.stop();
     }
     if (!launched("kessler_rows_kernel")) return GM1B_ERR_CUDA;
+    {
+        ProfScope ps("kessler_levels_kernel", st);
+        kessler_levels_kernel<<<dim3(nk, 5), kLevelThreads, 0, st>>>(d, w);
+        ps.stop();
+    }
+    if (!launched("kessler_levels_kernel")) return GM1B_ERR_CUDA;
     const double volume = (double)((dx * dy) * dz);
     const double area = (double)(dx * dy);
     {

@@ -1,6 +1,6 @@
 """Per-operator device throughput on B200 (library profiling facility).
 
-    python -m gm1_b200.opbench [--ops adv5 adv5-weno massflux calcdef moistnm courant tos tos-diag]
+    python -m gm1_b200.opbench [--ops adv5 adv5-weno massflux calcdef moistnm courant tos tos-diag moist]
                                [--grid 256 256 80] [--iters 20] [--nsound 10]
 
 For each operator: seeded synthetic inputs of the given padded-lane grid
@@ -39,6 +39,14 @@ ALG_WORDS = {
 }
 
 
+def moist_words(nsound: int) -> int:
+    """Words per cell of one composed moist large step: 149 outside the
+    acoustic loops plus 20 per small step over the three stages."""
+    from .periodic import sound3_stage_schedule_f32  # noqa: PLC0415
+
+    return 149 + 20 * sum(sound3_stage_schedule_f32(5.0, nsound, nrk)[0] for nrk in (1, 2, 3))
+
+
 def tos_words(nloop: int) -> int:
     """Words per cell of one terrain/open acoustic stage: the prepare pass
     (in: ppx ppi ua va wa ppterm piadv c1 c2 rf0 rr0 thv; out: ppd pp3d rru
@@ -50,6 +58,7 @@ def tos_words(nloop: int) -> int:
 
 _COMPACT: dict = {}
 NSOUND = [10]
+_CACHE: dict = {}
 
 
 def compact_inputs(op: str, ni: int, nj: int, nk: int, device: torch.device) -> dict:
@@ -193,6 +202,17 @@ def run(op: str, a: dict[str, torch.Tensor], ni: int, nj: int, nk: int, stream: 
         advective_courant_number(u=c["u"], v=c["v"], w=c["w"], uh=c["uh"], vh=c["vh"], mh=c["mh"], dt_s=6.0,
                                  dx_m=1000.0, dy_m=1000.0, dz_m=250.0, level_keys=c["keys"], stream=stream,
                                  out=c["out"])
+    elif op == "moist":
+        key = ("moist", ni, nj, nk)
+        if key not in _CACHE:
+            from .moist_step import MoistLargeStep, MoistStepConfig, upload, weisman_klemp_initial_state  # noqa: PLC0415
+
+            cfg = MoistStepConfig(ni, nj, nk, 1000.0, 1000.0, 250.0, 5.0, NSOUND[0])
+            host, metrics = weisman_klemp_initial_state(cfg, seed=2, bubble_radius_m=(10000.0, 1500.0),
+                                                        bubble_center_z_m=1500.0)
+            dev = a["u3d"].device
+            _CACHE[key] = MoistLargeStep(cfg, upload(host, dev), upload(metrics, dev), stream=stream)
+        _CACHE[key].step()
     elif op in ("tos", "tos-diag"):
         from .terrain_open import compile_cuda_psolver3_terrain_open, launch_cuda_psolver3_terrain_open_stage  # noqa: PLC0415
 
@@ -235,7 +255,8 @@ def main() -> None:
                 ends[q].record(stream)
         stream.synchronize()
         ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends)) / args.iters
-        words = tos_words(args.nsound) if op.startswith("tos") else ALG_WORDS[op]
+        words = (tos_words(args.nsound) if op.startswith("tos")
+                 else moist_words(args.nsound) if op == "moist" else ALG_WORDS[op])
         alg = words * 4 * cells
         gbs = alg / (ms * 1e-3) / 1e9
         print(json.dumps({"op": op, "grid": [ni, nj, nk], "cells": cells, "ms_per_launch": ms,
