@@ -467,6 +467,155 @@ def run_moist(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def _kernel_roofline(stats, cells_per_launch_unit: float, peak: float, peak_kind: str) -> dict:
+    """roofline of the kernel with the most device time: its algorithmic
+    words per cell x cells per launch over its average launch time."""
+    top = stats[0]
+    avg_ms = top["total_ms"] / top["launches"]
+    words = KERNEL_WORDS_PER_CELL.get(top["name"])
+    alg = None if words is None else words * 4 * cells_per_launch_unit
+    achieved = None if alg is None else alg / (avg_ms * 1e-3) / 1e9
+    traffic = None
+    tfile = ROOT / "profiles" / "traffic_per_launch.json"
+    if tfile.exists():
+        traffic = json.loads(tfile.read_text()).get(top["name"])
+    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": None if achieved is None else achieved / peak, "traffic": traffic, "kernel": top["name"],
+            "avg_launch_ms": avg_ms, "alg_bytes_per_launch": alg, "peak_source": f"{peak_kind} hbm_gbs"}
+
+
+def run_ensemble(args) -> None:
+    """Configuration 5: uneven Weisman-Klemp members, batched (one CUDA graph
+    per ensemble step over 8 streams) against the same members launched one
+    by one; members sharded over ranks by cell count."""
+    import torch
+    import torch.distributed as dist
+
+    from gm1_b200 import _native
+    from gm1_b200.ensemble import ENSEMBLE_GRID, MoistEnsemble, ensemble_members, member_initial_state
+    from gm1_b200.replicas import member_shard
+
+    rank, world, local, device, barrier, max_over_ranks = _dist_setup()
+    members = ensemble_members(args.members)
+    cells_all = [m.cells for m in members]
+    mine = [members[q] for q in member_shard(cells_all, rank, world)]
+    my_cells = sum(m.cells for m in mine)
+    total_cells = sum(cells_all)
+    hosts = [member_initial_state(m) for m in mine]
+    batched = MoistEnsemble(mine, device, streams=8, hosts=hosts)
+    plain = MoistEnsemble(mine, device, streams=1, hosts=hosts)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
+    for _ in range(args.warmup):
+        batched.step_eager()
+        plain.step_eager()
+    torch.cuda.synchronize(device)
+    batched.capture()
+    for _ in range(args.warmup):
+        batched.replay()
+    torch.cuda.synchronize(device)
+
+    def timed(ens, fn, sampler=None):
+        st, en = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ms = 0.0
+        barrier()
+        if sampler is not None:
+            sampler.start()
+        for _ in range(args.steps):
+            with torch.cuda.stream(ens.main):
+                flush.zero_()
+                st.record(ens.main)
+            fn()
+            with torch.cuda.stream(ens.main):
+                en.record(ens.main)
+            en.synchronize()
+            ms += st.elapsed_time(en)
+        barrier()
+        clocks = sampler.stop() if sampler is not None else None
+        return max_over_ranks(ms), clocks
+
+    sampler = ClockSampler(local)
+    b_ms, clocks = timed(batched, batched.replay, sampler)
+    p_ms, _ = timed(plain, plain.step_eager)
+    value = total_cells * args.steps / (b_ms * 1e-3)
+    plain_value = total_cells * args.steps / (p_ms * 1e-3)
+
+    # per-kernel device time of one eager batched step (launch profiler)
+    _native.profiler_enable(True)
+    batched.step_eager()
+    torch.cuda.synchronize(device)
+    _native.profiler_enable(False)
+    stats = _native.profiler_collect()
+    launches_per_step = sum(x["launches"] for x in stats)
+    peak, peak_kind = load_peaks()
+    # every member launches the top kernel equally often, so its average
+    # launch covers the members' mean cell count
+    roofline = _kernel_roofline(stats, my_cells / len(mine), peak, peak_kind)
+    tot = sum(x["total_ms"] for x in stats)
+    kernel_share = {x["name"]: round(x["total_ms"] / tot, 4) for x in stats[:12]}
+
+    # e2e: each member's step-start state in from pinned host memory, out after
+    pinned = [{n: torch.from_numpy(h[0][n]).pin_memory() for n in MOIST_PROGNOSTIC} for h in hosts]
+    for ens_state, pin in zip(batched.steps, pinned):
+        for n, t in pin.items():
+            t.copy_(ens_state.s[n])
+    h2d = sum(t.numel() * 4 for pin in pinned for t in pin.values())
+
+    def e2e_step():
+        with torch.cuda.stream(batched.main):
+            for ens_state, pin in zip(batched.steps, pinned):
+                for n, t in pin.items():
+                    ens_state.s[n].copy_(t, non_blocking=True)
+                for n, twin in MOIST_STAGE_TWIN.items():
+                    ens_state.s[twin].copy_(ens_state.s[n])
+        batched.replay()
+        with torch.cuda.stream(batched.main):
+            for ens_state, pin in zip(batched.steps, pinned):
+                for n, t in pin.items():
+                    t.copy_(ens_state.s[n], non_blocking=True)
+
+    e_ms, _ = timed(batched, e2e_step)
+    e2e_value = total_cells * args.steps / (e_ms * 1e-3)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        rate, n, dt = moist_cpu_rate(3, 10.0, threads)
+        ni, nj, nk = CPU_SUBBLOCK
+        cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"{n} moist RK3 large steps of one {ni}x{nj}x{nk} domain in {dt:.2f} s (per-cell rate of "
+                         "the oracle composition; every member runs the same per-cell work)"}
+    batched.release()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    g = ENSEMBLE_GRID
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": b_ms / args.steps, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+        "data": f"synthetic ({args.members} seeded Weisman-Klemp members, numpy default_rng(5))",
+        "config": {"workload": f"ensemble of {args.members} uneven moist members (nx, ny in 48..160, nz in 40..64, "
+                               f"dx=dy={g['dx'] / 1000:g} km, dz={g['dz']:g} m, dt={g['dt']:g} s, nsound={g['nsound']}, "
+                               "bubble U[1,3] K jittered +-5 km, Kessler, WENO5, TKE, open-radiative laterals)",
+                   "mode": "ensemble", "cells": total_cells, "members": args.members,
+                   "batched": "one CUDA graph per ensemble step, members over 8 streams",
+                   "plain_cell_updates_per_s": plain_value, "plain_ms_per_step": p_ms / args.steps,
+                   "batched_over_plain": value / plain_value,
+                   "l2": "flushed before every timed step (256 MiB write, outside the event pair)",
+                   "parallelism": f"members sharded over {world} ranks by cell count" if world > 1 else "one GPU"},
+        "step_roofline": {"bytes_per_cell_update": MOIST_STEP_BYTES_PER_CELL,
+                          "achieved_gbs": MOIST_STEP_BYTES_PER_CELL * value / world / 1e9,
+                          "frac": MOIST_STEP_BYTES_PER_CELL * value / world / 1e9 / peak},
+        "roofline": roofline, "kernel_share": kernel_share,
+        "gpu_launches": int(launches_per_step * args.steps),
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d},
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -474,17 +623,21 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=("moist", "dry"), default="moist")
+    ap.add_argument("--workload", choices=("moist", "dry", "ensemble"), default="moist")
+    ap.add_argument("--members", type=int, default=64, help="ensemble members (--workload ensemble)")
     args = ap.parse_args()
     if args.steps is None:
-        args.steps = 20 if args.workload == "moist" else 2000
+        args.steps = {"moist": 20, "ensemble": 10}.get(args.workload, 2000)
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":
-        (run_reference_moist if args.workload == "moist" else run_reference)(args)
+        (run_reference if args.workload == "dry" else run_reference_moist)(args)
         return
     if args.workload == "moist":
         run_moist(args)
+        return
+    if args.workload == "ensemble":
+        run_ensemble(args)
         return
 
     import torch

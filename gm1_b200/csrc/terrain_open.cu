@@ -39,6 +39,9 @@ namespace {
 constexpr int kTosWarps = 8;     // k-parallel warps of the column pass
 constexpr int kTosMaxNk = 160;   // column pass keeps 10 words per level per column in shared memory
 constexpr int kTosArrays = 10;
+constexpr int kPgLevels = 4;     // levels whose loads the pressure-gradient march issues together
+constexpr int kA2Levels = 2;     // levels per warp whose column-pass loads are issued together (phase A2)
+constexpr int kColLevels = 4;    // the same for phases A3 and C
 
 struct TosArgs {
     gm1b_terrain_open_arrays a;
@@ -246,44 +249,77 @@ __global__ void __launch_bounds__(128) tos_pgrad_kernel(TosArgs p) {
     float vc = 0.0f, vw = 0.0f, vs = 0.0f;  // vertical difference at level k (zero at k = 1)
     float gxu_lo = du ? __ldg(m.gxu + (size_t)(j - 1) * (ni + 1) + (i - 1)) : 0.0f;
     float gyv_lo = dv ? __ldg(m.gyv + (size_t)(j - 1) * ni + (i - 1)) : 0.0f;
-#pragma unroll 2
-    for (int k = 1; k <= nk; ++k) {
-        float vc1 = 0.0f, vw1 = 0.0f, vs1 = 0.0f, pc1 = 0.0f, pw1 = 0.0f, ps1 = 0.0f;
-        if (k < nk) {
-            const float r = rds(k + 1, p.dz);
-            pc1 = __ldg(a.ppd + X.p(k + 1, j, i));
-            pw1 = __ldg(a.ppd + X.p(k + 1, j, iw));
-            ps1 = __ldg(a.ppd + X.p(k + 1, js, i));
-            vc1 = (pc1 - pc) * r;
-            vw1 = (pw1 - pw) * r;
-            vs1 = (ps1 - ps) * r;
+    // Levels go in chunks of kPgLevels: every load of a chunk is issued before
+    // its first store, so the chunk's loads are in flight together (the
+    // stores to u3d/v3d would otherwise order each level's loads behind the
+    // previous level's stores).
+    for (int k0 = 1; k0 <= nk; k0 += kPgLevels) {
+        float lp[kPgLevels], lw[kPgLevels], ls[kPgLevels], lth[kPgLevels], lthw[kPgLevels], lths[kPgLevels];
+        float lgx[kPgLevels], lgy[kPgLevels], lut[kPgLevels], luu[kPgLevels], lvt[kPgLevels], lvv[kPgLevels];
+#pragma unroll
+        for (int q = 0; q < kPgLevels; ++q) {
+            const int k = k0 + q;
+            lp[q] = lw[q] = ls[q] = lth[q] = lthw[q] = lths[q] = 0.0f;
+            lgx[q] = lgy[q] = lut[q] = luu[q] = lvt[q] = lvv[q] = 0.0f;
+            if (k > nk) continue;
+            if (k < nk) {
+                lp[q] = __ldg(a.ppd + X.p(k + 1, j, i));
+                lw[q] = __ldg(a.ppd + X.p(k + 1, j, iw));
+                ls[q] = __ldg(a.ppd + X.p(k + 1, js, i));
+            }
+            lth[q] = __ldg(a.thv + X.p(k, j, i));
+            if (du) {
+                const size_t o = X.u(k, j + 2, i + 2);
+                lthw[q] = __ldg(a.thv + X.p(k, j, iw));
+                lgx[q] = __ldg(m.gxu + ((size_t)k * nj + (j - 1)) * (ni + 1) + (i - 1));
+                lut[q] = __ldg(a.uten + o);
+                luu[q] = a.u3d[o];
+            }
+            if (dv) {
+                const size_t o = X.v(k, j + 2, i + 2);
+                lths[q] = __ldg(a.thv + X.p(k, js, i));
+                lgy[q] = __ldg(m.gyv + ((size_t)k * (nj + 1) + (j - 1)) * ni + (i - 1));
+                lvt[q] = __ldg(a.vten + o);
+                lvv[q] = a.v3d[o];
+            }
         }
-        if (dh && k >= 2) a.hadvp[X.p(k, j, i)] = vc;
-        const float thc = __ldg(a.thv + X.p(k, j, i));
-        if (du) {
-            const float gxu_hi = __ldg(m.gxu + ((size_t)k * nj + (j - 1)) * (ni + 1) + (i - 1));
-            const float th = thc + __ldg(a.thv + X.p(k, j, iw));
-            const float hz = (pc - pw) * p.rdx;
-            const float vsum = (vc1 + vw1) + (vc + vw);
-            const float tr = (0.125f * vsum) * (gxu_lo + gxu_hi);
-            const float pg = (p.halfcp * th) * (hz + tr);
-            const size_t o = X.u(k, j + 2, i + 2);
-            a.u3d[o] = a.u3d[o] + p.dts * (__ldg(a.uten + o) - pg);
-            gxu_lo = gxu_hi;
+#pragma unroll
+        for (int q = 0; q < kPgLevels; ++q) {
+            const int k = k0 + q;
+            if (k > nk) break;
+            float vc1 = 0.0f, vw1 = 0.0f, vs1 = 0.0f;
+            const float pc1 = lp[q], pw1 = lw[q], ps1 = ls[q];
+            if (k < nk) {
+                const float r = rds(k + 1, p.dz);
+                vc1 = (pc1 - pc) * r;
+                vw1 = (pw1 - pw) * r;
+                vs1 = (ps1 - ps) * r;
+            }
+            if (dh && k >= 2) a.hadvp[X.p(k, j, i)] = vc;
+            const float thc = lth[q];
+            if (du) {
+                const float gxu_hi = lgx[q];
+                const float th = thc + lthw[q];
+                const float hz = (pc - pw) * p.rdx;
+                const float vsum = (vc1 + vw1) + (vc + vw);
+                const float tr = (0.125f * vsum) * (gxu_lo + gxu_hi);
+                const float pg = (p.halfcp * th) * (hz + tr);
+                a.u3d[X.u(k, j + 2, i + 2)] = luu[q] + p.dts * (lut[q] - pg);
+                gxu_lo = gxu_hi;
+            }
+            if (dv) {
+                const float gyv_hi = lgy[q];
+                const float th = thc + lths[q];
+                const float hz = (pc - ps) * p.rdy;
+                const float vsum = (vc1 + vs1) + (vc + vs);
+                const float tr = (0.125f * vsum) * (gyv_lo + gyv_hi);
+                const float pg = (p.halfcp * th) * (hz + tr);
+                a.v3d[X.v(k, j + 2, i + 2)] = lvv[q] + p.dts * (lvt[q] - pg);
+                gyv_lo = gyv_hi;
+            }
+            pc = pc1, pw = pw1, ps = ps1;
+            vc = vc1, vw = vw1, vs = vs1;
         }
-        if (dv) {
-            const float gyv_hi = __ldg(m.gyv + ((size_t)k * (nj + 1) + (j - 1)) * ni + (i - 1));
-            const float th = thc + __ldg(a.thv + X.p(k, js, i));
-            const float hz = (pc - ps) * p.rdy;
-            const float vsum = (vc1 + vs1) + (vc + vs);
-            const float tr = (0.125f * vsum) * (gyv_lo + gyv_hi);
-            const float pg = (p.halfcp * th) * (hz + tr);
-            const size_t o = X.v(k, j + 2, i + 2);
-            a.v3d[o] = a.v3d[o] + p.dts * (__ldg(a.vten + o) - pg);
-            gyv_lo = gyv_hi;
-        }
-        pc = pc1, pw = pw1, ps = ps1;
-        vc = vc1, vw = vw1, vs = vs1;
     }
 }
 
@@ -297,6 +333,39 @@ __global__ void __launch_bounds__(128) tos_pgrad_kernel(TosArgs p) {
 // the same operations as the twin; read-only fields take the non-coherent
 // path so the unrolled level loops keep several levels' loads in flight.
 // ---------------------------------------------------------------------------
+// global words one level of phase A2 reads (zero where the level or the
+// pi' advection does not use them)
+struct A2Load {
+    float rk, rl, rk1, rrf_k, rrf_k1, qk, pk1, pk2, ppten, ppterm, pp, pc, pe, pw, pn, ps, rr0;
+    __device__ __forceinline__ void load(const gm1b_terrain_open_arrays &a, const gm1b_terrain_metrics &m,
+                                         const Ix &X, int k, int nk, int j, int i, bool adv) {
+        rk = rl = rk1 = rrf_k = rrf_k1 = qk = pk1 = pk2 = ppten = ppterm = pp = 0.0f;
+        pc = pe = pw = pn = ps = rr0 = 0.0f;
+        if (k > nk) return;
+        const int j0 = j - 1, i0 = i - 1;
+        const size_t c = X.p(k, j, i);
+        if (adv) {
+            rk = __ldg(m.rho0_3d + X.m(k - 1, 0, 0));
+            if (k >= 2) rl = __ldg(m.rho0_3d + X.m(k - 2, 0, 0));
+            if (k < nk) rk1 = __ldg(m.rho0_3d + X.m(k, 0, 0));
+            if (k >= 2) rrf_k = __ldg(m.rrf0 + X.m(k - 1, j0, i0));
+            if (k < nk) rrf_k1 = __ldg(m.rrf0 + X.m(k, j0, i0));
+            pc = __ldg(a.piadv + c);
+            pe = __ldg(a.piadv + c + 1);
+            pw = __ldg(a.piadv + c - 1);
+            pn = __ldg(a.piadv + X.p(k, j + 1, i));
+            ps = __ldg(a.piadv + X.p(k, j - 1, i));
+            rr0 = __ldg(m.rr0 + X.m(k - 1, j0, i0));
+        }
+        qk = __ldg(a.qk + c);
+        pk1 = __ldg(a.pk1 + c);
+        pk2 = __ldg(a.pk2 + c);
+        ppten = __ldg(a.ppten + c);
+        ppterm = __ldg(a.ppterm + c);
+        pp = a.pp3d[c];
+    }
+};
+
 __device__ __forceinline__ void tos_level_terms(const float *s_xw, const float *s_xe, const float *s_ys,
                                                 const float *s_yn, int lane, int kf, const TosArgs &p, float dzdx,
                                                 float dzdy, float gz, float rk, float rl, float rrf0, bool adv,
@@ -375,26 +444,20 @@ __global__ void __launch_bounds__(32 * kTosWarps, 2) tos_column_kernel(TosArgs p
     __syncthreads();
     // A2: divergence, fpk (initial + pi' advection), column coefficients
     if (live) {
-#pragma unroll 2
-        for (int k = 1 + wy; k <= nk; k += kTosWarps) {
+        for (int kb = 1 + wy; kb <= nk; kb += kTosWarps * kA2Levels) {
+            A2Load ld[kA2Levels];
+#pragma unroll
+            for (int q = 0; q < kA2Levels; ++q) ld[q].load(a, m, X, kb + q * kTosWarps, nk, j, i, do_adv);
+#pragma unroll
+            for (int q = 0; q < kA2Levels; ++q) {
+            const int k = kb + q * kTosWarps;
+            if (k > nk) break;
             const size_t c = X.p(k, j, i);
-            const float rk = do_adv ? __ldg(m.rho0_3d + X.m(k - 1, 0, 0)) : 0.0f;
-            const float rl = (do_adv && k >= 2) ? __ldg(m.rho0_3d + X.m(k - 2, 0, 0)) : 0.0f;
-            const float rk1 = (do_adv && k < nk) ? __ldg(m.rho0_3d + X.m(k, 0, 0)) : 0.0f;
-            const float rrf_k = (do_adv && k >= 2) ? __ldg(m.rrf0 + X.m(k - 1, j0, i0)) : 0.0f;
-            const float rrf_k1 = (do_adv && k < nk) ? __ldg(m.rrf0 + X.m(k, j0, i0)) : 0.0f;
-            const float qk = __ldg(a.qk + c), pk1 = __ldg(a.pk1 + c), pk2 = __ldg(a.pk2 + c);
-            const float ppten = __ldg(a.ppten + c), ppterm = __ldg(a.ppterm + c);
-            const float pp = a.pp3d[c];
-            float pc = 0.0f, pe = 0.0f, pw = 0.0f, pn = 0.0f, ps = 0.0f, rr0 = 0.0f;
-            if (do_adv) {
-                pc = __ldg(a.piadv + c);
-                pe = __ldg(a.piadv + c + 1);
-                pw = __ldg(a.piadv + c - 1);
-                pn = __ldg(a.piadv + X.p(k, j + 1, i));
-                ps = __ldg(a.piadv + X.p(k, j - 1, i));
-                rr0 = __ldg(m.rr0 + X.m(k - 1, j0, i0));
-            }
+            const float rk = ld[q].rk, rl = ld[q].rl, rk1 = ld[q].rk1, rrf_k = ld[q].rrf_k, rrf_k1 = ld[q].rrf_k1;
+            const float qk = ld[q].qk, pk1 = ld[q].pk1, pk2 = ld[q].pk2;
+            const float ppten = ld[q].ppten, ppterm = ld[q].ppterm;
+            const float pp = ld[q].pp;
+            const float pc = ld[q].pc, pe = ld[q].pe, pw = ld[q].pw, pn = ld[q].pn, ps = ld[q].ps, rr0 = ld[q].rr0;
             float d3k = 0.0f, d3k1 = 0.0f, hak = 0.0f, hak1 = 0.0f;
             if (k >= 2) tos_level_terms(s_xw, s_xe, s_ys, s_yn, lane, k, p, dzdx, dzdy, gz, rk, rl, rrf_k, do_adv, d3k, hak);
             if (k < nk)
@@ -434,16 +497,27 @@ __global__ void __launch_bounds__(32 * kTosWarps, 2) tos_column_kernel(TosArgs p
             SM(s_a1, k) = pk1 + qk;
             SM(s_a2, k) = pk2 - qk;
             SM(s_pp, k) = pp;
+            }
         }
     }
     __syncthreads();
     // A3: tridiagonal coefficients and right-hand side, k = 2..nk
     if (live && do_imp) {
-#pragma unroll 2
-        for (int k = 2 + wy; k <= nk; k += kTosWarps) {
+        for (int kb = 2 + wy; kb <= nk; kb += kTosWarps * kColLevels) {
+            float lmm[kColLevels], lwt[kColLevels];
+#pragma unroll
+            for (int q = 0; q < kColLevels; ++q) {
+                const int k = kb + q * kTosWarps;
+                lmm[q] = k <= nk ? __ldg(a.mm + X.p(k, j, i)) : 0.0f;
+                lwt[q] = k <= nk ? __ldg(a.wten + X.w(k, y, x)) : 0.0f;
+            }
+#pragma unroll
+            for (int q = 0; q < kColLevels; ++q) {
+            const int k = kb + q * kTosWarps;
+            if (k > nk) break;
             const size_t c = X.p(k, j, i);
-            const float mmk = __ldg(a.mm + c);
-            const float wt = __ldg(a.wten + X.w(k, y, x));
+            const float mmk = lmm[q];
+            const float wt = lwt[q];
             const float aa = k >= 3 ? (-p.asq) * (mmk * SM(s_a1, k - 1)) : 0.0f;
             const float cc = k < nk ? (-p.asq) * ((-mmk) * SM(s_a2, k)) : 0.0f;
             const float dg = (-SM(s_a1, k)) + SM(s_a2, k - 1);
@@ -461,6 +535,7 @@ __global__ void __launch_bounds__(32 * kTosWarps, 2) tos_column_kernel(TosArgs p
                 a.tri_bb[c] = bb;
                 a.tri_cc[c] = cc;
                 a.tri_dd[c] = dd;
+            }
             }
         }
     }
@@ -491,12 +566,28 @@ __global__ void __launch_bounds__(32 * kTosWarps, 2) tos_column_kernel(TosArgs p
     if (live) {
         const bool fill = p.n < p.nloop && (p.abl & GM1B_TOS_BETWEEN_STEP_FILL);
         const bool east = i == ni, north = j == nj;
-#pragma unroll 2
-        for (int k = 1 + wy; k <= nk; k += kTosWarps) {
+        for (int kb = 1 + wy; kb <= nk; kb += kTosWarps * kColLevels) {
+            float luu[kColLevels], lvv[kColLevels], lru[kColLevels], lrv[kColLevels], lrw[kColLevels];
+#pragma unroll
+            for (int q = 0; q < kColLevels; ++q) {
+                const int k = kb + q * kTosWarps;
+                luu[q] = lvv[q] = lru[q] = lrv[q] = lrw[q] = 0.0f;
+                if (k > nk) continue;
+                const size_t qu = X.u(k, y, x), qv = X.v(k, y, x), qw = X.w(k, y, x);
+                luu[q] = __ldg(a.u3d + qu);
+                lvv[q] = __ldg(a.v3d + qv);
+                lru[q] = a.rru[qu];
+                lrv[q] = a.rrv[qv];
+                lrw[q] = a.rrw[qw];
+            }
+#pragma unroll
+            for (int q = 0; q < kColLevels; ++q) {
+            const int k = kb + q * kTosWarps;
+            if (k > nk) break;
             const size_t c = X.p(k, j, i);
             const size_t qu = X.u(k, y, x), qv = X.v(k, y, x), qw = X.w(k, y, x);
-            const float uu = __ldg(a.u3d + qu), vv = __ldg(a.v3d + qv);
-            const float ru = a.rru[qu], rv = a.rrv[qv], rw = a.rrw[qw];
+            const float uu = luu[q], vv = lvv[q];
+            const float ru = lru[q], rv = lrv[q], rw = lrw[q];
             const float wk = SM(s_w, k), wk1 = SM(s_w, k + 1);
             if (k == 1) a.w3d[qw] = wk;
             if (do_imp && k >= 2) {
@@ -552,6 +643,7 @@ __global__ void __launch_bounds__(32 * kTosWarps, 2) tos_column_kernel(TosArgs p
                     a.rrv[ev] = last ? sv * p.tavg : sv;
                     a.rrw[ew] = last ? sw * p.tavg : sw;
                 }
+            }
             }
         }
     }
@@ -886,15 +978,21 @@ extern "C" int32_t gm1b_terrain_open_stage(int32_t ni, int32_t nj, int32_t nk, i
     }
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const size_t col_smem = (size_t)kTosArrays * (size_t)(nk + 2) * 32 * sizeof(float);
-    static bool attr_set = false;
-    if (!attr_set) {
+    static bool attr_set[64] = {};  // per device: the attribute belongs to each device's context
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+        cudaGetLastError();
+        gm1b_set_error("gm1b_terrain_open_stage: no usable current device");
+        return GM1B_ERR_CUDA;
+    }
+    if (!attr_set[dev]) {
         const cudaError_t e = cudaFuncSetAttribute(tos_column_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                    (int)((size_t)kTosArrays * (kTosMaxNk + 2) * 32 * sizeof(float)));
         if (e != cudaSuccess) {
             gm1b_set_error("cudaFuncSetAttribute(tos_column_kernel): %s", cudaGetErrorString(e));
             return GM1B_ERR_CUDA;
         }
-        attr_set = true;
+        attr_set[dev] = true;
     }
     {
         ProfScope ps("tos_prepare_kernel", st);

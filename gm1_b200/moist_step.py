@@ -174,12 +174,14 @@ METRIC_NAMES = ("terrain_msl", "zh", "zf", "mh", "rmh", "mf", "rmf", "c1", "c2",
 def weisman_klemp_initial_state(cfg: MoistStepConfig, *, seed: int = 0, bubble_k: float = 3.0,
                                 noise_k: float = 0.1, bubble_radius_m: tuple[float, float] = (10000.0, 1400.0),
                                 bubble_center_z_m: float = 1400.0, bubble_cloud: float = 0.0,
-                                bubble_rain: float = 0.0) -> tuple[dict[str, np.ndarray],
+                                bubble_rain: float = 0.0,
+                                bubble_offset_m: tuple[float, float] = (0.0, 0.0)) -> tuple[dict[str, np.ndarray],
                                                                             dict[str, np.ndarray]]:
     """Host (numpy float32) state and flat terrain metrics of a
     Weisman-Klemp supercell start on cfg's grid: the isnd = 5 column
     (theta, qv, pi on the mass heights), the quarter-circle hodograph, a
-    cos^2 warm bubble at the domain centre plus seeded uniform noise of
+    cos^2 warm bubble at the domain centre (shifted by bubble_offset_m in x
+    and y) plus seeded uniform noise of
     +-noise_k, cloud and rain water bubble_cloud / bubble_rain (kg/kg) in
     the bubble's core (r < 1/2), TKE at its floor, zero radiation
     histories."""
@@ -200,8 +202,8 @@ def weisman_klemp_initial_state(cfg: MoistStepConfig, *, seed: int = 0, bubble_k
     s["u3d"][1:nk + 1] = u0[:, None, None]
     s["v3d"][1:nk + 1] = v0[:, None, None]
     rng = np.random.default_rng(seed)
-    x = (np.arange(ni) + 0.5) * cfg.dx - 0.5 * ni * cfg.dx
-    y = (np.arange(nj) + 0.5) * cfg.dy - 0.5 * nj * cfg.dy
+    x = (np.arange(ni) + 0.5) * cfg.dx - 0.5 * ni * cfg.dx - bubble_offset_m[0]
+    y = (np.arange(nj) + 0.5) * cfg.dy - 0.5 * nj * cfg.dy - bubble_offset_m[1]
     r = np.sqrt((x[None, None, :] / bubble_radius_m[0]) ** 2 + (y[None, :, None] / bubble_radius_m[0]) ** 2 +
                 ((zh.astype(np.float64)[:, None, None] - bubble_center_z_m) / bubble_radius_m[1]) ** 2)
     bubble = np.where(r < 1.0, bubble_k * np.cos(0.5 * np.pi * r) ** 2, 0.0)
