@@ -700,6 +700,43 @@ GM1B_API int32_t gm1b_theta_bubble(int32_t ni, int32_t nj, int32_t nk, int32_t n
                                    void *stream);
 
 /*
+ * CM1 vertical coordinates (stretch_z = 0 uniform, stretch_z = 1
+ * Wilhelmson-Chen stretching), CM1-indexed float32 profiles: zf, sigmaf, mf,
+ * rmf and rdsf hold nk + 3 words, zh, sigma, mh, rmh and rds nk + 2.  rds and
+ * rdsf are init_terrain.F:292-298's 1/(sigma(k)-sigma(k-1)) (k = 2..nk) and
+ * 1/(sigmaf(k+1)-sigmaf(k)) (k = 1..nk), zero elsewhere.
+ */
+typedef struct gm1b_stretch_z1_derived {
+    int32_t nk1, nk2, nk3; /* layers below str_bot, stretched, above str_top */
+    float nominal, c1, c2; /* (dz_bot + dz_top) / 2 and the quadratic's coefficients */
+} gm1b_stretch_z1_derived;
+
+typedef struct gm1b_vertical_profiles {
+    float *zf, *zh, *sigmaf, *sigma, *mh, *mf, *rmh, *rmf, *rds, *rdsf;
+} gm1b_vertical_profiles;
+
+/* derive_stretch_z1 (src/cm1core/cuda_stretch_z1.py:130-201): the segment
+ * counts and c1/c2 of a stretch_z = 1 column, with the reference's
+ * feasibility refusals (param.F:7814-7914).  Host only. */
+GM1B_API int32_t gm1b_stretch_z1_derive(int32_t nk, float dz, float ztop, float str_bot, float str_top, float dz_bot,
+                                        float dz_top, gm1b_stretch_z1_derived *out);
+
+/* build_vertical_levels for stretch_z 0 and 1 (src/cm1core/cm1_vertical_grid.py:780-927):
+ * every profile into HOST memory plus the Fornberg boundary weights cgs/cgt
+ * (fornberg_extrapolation_weights, :422-454).  stretch_z = 0 requires
+ * ztop == dz * nk in float32 (param.F:2608) and ignores the stretch words.
+ * rds/rdsf may be NULL.  Host only. */
+GM1B_API int32_t gm1b_vertical_levels(int32_t stretch_z, int32_t nk, float dz, float ztop, float str_bot,
+                                      float str_top, float dz_bot, float dz_top, const gm1b_vertical_profiles *host,
+                                      float cgs[3], float cgt[3]);
+
+/* launch_cuda_stretch_z1 (src/cm1core/cuda_stretch_z1.py:418): the same
+ * profiles written into DEVICE memory by one device thread on `stream`
+ * (rds/rdsf may be NULL).  The parameters are checked on the host first. */
+GM1B_API int32_t gm1b_stretch_z1(int32_t nk, float dz, float ztop, float str_bot, float str_top, float dz_bot,
+                                 float dz_top, const gm1b_vertical_profiles *device, void *stream);
+
+/*
  * Launch profiler.  While enabled, every kernel launch of the library is
  * bracketed by a pair of CUDA events recorded on its own stream (the
  * per-phase device timing of src/cm1core/runtime_profiler.py:1-48, per

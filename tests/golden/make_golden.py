@@ -1045,10 +1045,69 @@ def make_c1(reference: Path, checkpoints: list[int]) -> None:
         print("checkpoint", n, time.time() - t0, flush=True)
 
 
+VERTICAL_CASES = {
+    # name: (stretch_z, nk, dz, ztop, str_bot, str_top, dz_bot, dz_top)
+    "child_15km_nk75": (1, 75, 100.0, 15000.0, 200.0, 7000.0, 20.0, 320.0),
+    "stretch_20_500_nk80": (1, 80, 100.0, 20800.0, 200.0, 15800.0, 20.0, 500.0),
+    "stretch_from_ground_nk50": (1, 50, 200.0, 11500.0, 0.0, 8000.0, 50.0, 350.0),
+    "uniform_nk80_dz250": (0, 80, 250.0, 20000.0, 0.0, 0.0, 0.0, 0.0),
+    "uniform_nk40_dz500": (0, 40, 500.0, 20000.0, 0.0, 0.0, 0.0, 0.0),
+}
+VERTICAL_REFUSALS = {
+    "infeasible_dz_bot": (1, 75, 100.0, 15000.0, 200.0, 7000.0, 30.0, 320.0),
+    "uniform_wrong_top": (0, 40, 500.0, 19000.0, 0.0, 0.0, 0.0, 0.0),
+    "stretch_z2": (2, 75, 200.0, 15000.0, 0.0, 0.0, 0.0, 0.0),
+    "too_few_levels": (0, 3, 500.0, 1500.0, 0.0, 0.0, 0.0, 0.0),
+}
+
+
+def make_vertical(reference: Path) -> None:
+    """CM1 vertical coordinates (stretch_z 0 and 1) through the reference's
+    own build_vertical_levels and derive_stretch_z1: every profile's float32
+    words, rds/rdsf, the Fornberg weights, the derived segment counts and the
+    sealed digests; refused parameter sets with the reference's error."""
+    sys.path.insert(0, str(reference / "src"))
+    from cm1core.cm1_vertical_grid import build_vertical_levels
+    from cm1core.cuda_stretch_z1 import StretchZ1Parameters, derive_stretch_z1
+
+    def words(a) -> list[int]:
+        return [int(w) for w in np.ascontiguousarray(a, dtype=np.float32).view(np.uint32)]
+
+    out = {"cases": {}, "refusals": {}}
+    for name, (sz, nk, dz, ztop, sb, st, db, dt) in VERTICAL_CASES.items():
+        lv = build_vertical_levels(stretch_z=sz, nk=nk, dz_m=dz, ztop_m=ztop, str_bot_m=sb, str_top_m=st,
+                                   dz_bot_m=db, dz_top_m=dt)
+        rec = {"args": [sz, nk, dz, ztop, sb, st, db, dt], "ztop_m": lv.ztop_m, "sha256": lv.sha256,
+               "cgs": words(np.array(lv.cgs, np.float32)), "cgt": words(np.array(lv.cgt, np.float32))}
+        for f in ("zf", "zh", "sigmaf", "sigma", "mh", "mf", "rmh", "rmf", "rds", "rdsf"):
+            rec[f] = words(getattr(lv, f))
+        p = lv.stretch_parameters()
+        d = derive_stretch_z1(p)
+        rec["derived"] = {"nk1": d.nk1, "nk2": d.nk2, "nk3": d.nk3,
+                          "nominal": words(np.array([d.nominal_dz_f32], np.float32))[0],
+                          "c1": words(np.array([d.c1_f32], np.float32))[0],
+                          "c2": words(np.array([d.c2_f32], np.float32))[0]}
+        rec["stretch_parameters"] = [p.nk, p.dz, p.ztop, p.str_bot, p.str_top, p.dz_bot, p.dz_top]
+        out["cases"][name] = rec
+    for name, (sz, nk, dz, ztop, sb, st, db, dt) in VERTICAL_REFUSALS.items():
+        try:
+            build_vertical_levels(stretch_z=sz, nk=nk, dz_m=dz, ztop_m=ztop, str_bot_m=sb, str_top_m=st,
+                                  dz_bot_m=db, dz_top_m=dt)
+        except Exception as e:  # noqa: BLE001 - the reference's refusal is the record
+            out["refusals"][name] = {"args": [sz, nk, dz, ztop, sb, st, db, dt], "error": type(e).__name__,
+                                     "message": str(e)[:200]}
+        else:
+            raise AssertionError(f"{name} was not refused by the reference")
+    from cm1core.stretch_z1_child_15km import STRETCH_Z1_CHILD_15KM_PROFILE_SHA256
+
+    out["sealed_child_15km_profile_sha256"] = dict(STRETCH_Z1_CHILD_15KM_PROFILE_SHA256)
+    (HERE / "vertical_levels.json").write_text(json.dumps(out, indent=1, sort_keys=True))
+
+
 def main() -> None:
     p = argparse.ArgumentParser()
     p.add_argument("--reference", type=Path, required=True, help="root of the reference source tree")
-    p.add_argument("what", choices=("small", "c1", "advection", "kessler", "tke", "rk", "bridge", "wk", "limits", "closure", "tkeevo", "momentum", "terrainopen", "kesslerstep", "fills"))
+    p.add_argument("what", choices=("small", "c1", "advection", "kessler", "tke", "rk", "bridge", "wk", "limits", "closure", "tkeevo", "momentum", "terrainopen", "kesslerstep", "fills", "vertical"))
     p.add_argument("--checkpoints", type=int, nargs="+", default=[1])
     args = p.parse_args()
     if args.what == "small":
@@ -1079,6 +1138,8 @@ def main() -> None:
         make_kessler_large_step(args.reference)
     elif args.what == "fills":
         make_fills(args.reference)
+    elif args.what == "vertical":
+        make_vertical(args.reference)
     else:
         make_c1(args.reference, sorted(set(args.checkpoints)))
 
