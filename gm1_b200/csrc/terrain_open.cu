@@ -42,6 +42,7 @@ constexpr int kTosArrays = 10;
 constexpr int kPgLevels = 4;     // levels whose loads the pressure-gradient march issues together
 constexpr int kA2Levels = 2;     // levels per warp whose column-pass loads are issued together (phase A2)
 constexpr int kColLevels = 4;    // the same for phases A3 and C
+constexpr int kThomasChunk = 8;  // back-substitution levels whose coefficients are read together
 
 struct TosArgs {
     gm1b_terrain_open_arrays a;
@@ -52,24 +53,27 @@ struct TosArgs {
     float cgs[3], cgt[3];
 };
 
+// 32-bit element offsets: the host refuses grids whose largest padded
+// array reaches 2^31 words, so every offset below fits (a 640x768x80 padded
+// scalar is 41 M words)
 struct Ix {
     int ni, nj;
-    __device__ __forceinline__ size_t p(int k, int j, int i) const {
-        return ((size_t)k * (nj + 2) + j) * (size_t)(ni + 2) + i;
+    __device__ __forceinline__ unsigned p(int k, int j, int i) const {
+        return ((unsigned)k * (unsigned)(nj + 2) + (unsigned)j) * (unsigned)(ni + 2) + (unsigned)i;
     }
-    __device__ __forceinline__ size_t u(int k, int y, int x) const {
-        return ((size_t)k * (nj + 6) + y) * (size_t)(ni + 7) + x;
+    __device__ __forceinline__ unsigned u(int k, int y, int x) const {
+        return ((unsigned)k * (unsigned)(nj + 6) + (unsigned)y) * (unsigned)(ni + 7) + (unsigned)x;
     }
-    __device__ __forceinline__ size_t v(int k, int y, int x) const {
-        return ((size_t)k * (nj + 7) + y) * (size_t)(ni + 6) + x;
+    __device__ __forceinline__ unsigned v(int k, int y, int x) const {
+        return ((unsigned)k * (unsigned)(nj + 7) + (unsigned)y) * (unsigned)(ni + 6) + (unsigned)x;
     }
-    __device__ __forceinline__ size_t w(int k, int y, int x) const {
-        return ((size_t)k * (nj + 6) + y) * (size_t)(ni + 6) + x;
+    __device__ __forceinline__ unsigned w(int k, int y, int x) const {
+        return ((unsigned)k * (unsigned)(nj + 6) + (unsigned)y) * (unsigned)(ni + 6) + (unsigned)x;
     }
-    __device__ __forceinline__ size_t m(int k0, int j0, int i0) const {
-        return ((size_t)k0 * nj + j0) * (size_t)ni + i0;
+    __device__ __forceinline__ unsigned m(int k0, int j0, int i0) const {
+        return ((unsigned)k0 * (unsigned)nj + (unsigned)j0) * (unsigned)ni + (unsigned)i0;
     }
-    __device__ __forceinline__ size_t h(int j0, int i0) const { return (size_t)j0 * ni + i0; }
+    __device__ __forceinline__ unsigned h(int j0, int i0) const { return (unsigned)j0 * (unsigned)ni + (unsigned)i0; }
 };
 
 // uniform terrain coordinate, the twin's float32 words (terrain_coordinate_profiles)
@@ -96,11 +100,11 @@ __global__ void __launch_bounds__(256) tos_prepare_kernel(TosArgs p) {
         const int i = (int)(z % (ni + 2));
         const int j = (int)((z / (ni + 2)) % (nj + 2));
         const int k = (int)(z / plane) + 1;
-        const size_t c = X.p(k, j, i);
+        const unsigned c = X.p(k, j, i);
         a.ppd[c] = a.ppx[c];
         if (p.nrk != 1) a.pp3d[c] = a.ppi[c];
         const int y = j + 2, x = i + 2;
-        const size_t qu = X.u(k, y, x), qv = X.v(k, y, x), qw = X.w(k, y, x);
+        const unsigned qu = X.u(k, y, x), qv = X.v(k, y, x), qw = X.w(k, y, x);
         a.rru[qu] = 0.0f;
         a.rrv[qv] = 0.0f;
         a.rrw[qw] = a.wa[qw] * p.beta;
@@ -136,7 +140,7 @@ __global__ void __launch_bounds__(256) tos_prepare_kernel(TosArgs p) {
 #pragma unroll 1
             for (int q = 0; q < nz; ++q) zero[q][c] = 0.0f;
             if (k == 1 || k == nk) {
-                const size_t e = X.p(k == 1 ? 0 : nk + 1, j, i);
+                const unsigned e = X.p(k == 1 ? 0 : nk + 1, j, i);
 #pragma unroll 1
                 for (int q = 0; q < 16; ++q) zero[q][e] = 0.0f;
             }
@@ -269,16 +273,16 @@ __global__ void __launch_bounds__(128) tos_pgrad_kernel(TosArgs p) {
             }
             lth[q] = __ldg(a.thv + X.p(k, j, i));
             if (du) {
-                const size_t o = X.u(k, j + 2, i + 2);
+                const unsigned o = X.u(k, j + 2, i + 2);
                 lthw[q] = __ldg(a.thv + X.p(k, j, iw));
-                lgx[q] = __ldg(m.gxu + ((size_t)k * nj + (j - 1)) * (ni + 1) + (i - 1));
+                lgx[q] = __ldg(m.gxu + ((unsigned)k * (unsigned)nj + (unsigned)(j - 1)) * (unsigned)(ni + 1) + (unsigned)(i - 1));
                 lut[q] = __ldg(a.uten + o);
                 luu[q] = a.u3d[o];
             }
             if (dv) {
-                const size_t o = X.v(k, j + 2, i + 2);
+                const unsigned o = X.v(k, j + 2, i + 2);
                 lths[q] = __ldg(a.thv + X.p(k, js, i));
-                lgy[q] = __ldg(m.gyv + ((size_t)k * (nj + 1) + (j - 1)) * ni + (i - 1));
+                lgy[q] = __ldg(m.gyv + ((unsigned)k * (unsigned)(nj + 1) + (unsigned)(j - 1)) * (unsigned)ni + (unsigned)(i - 1));
                 lvt[q] = __ldg(a.vten + o);
                 lvv[q] = a.v3d[o];
             }
@@ -343,7 +347,7 @@ struct A2Load {
         pc = pe = pw = pn = ps = rr0 = 0.0f;
         if (k > nk) return;
         const int j0 = j - 1, i0 = i - 1;
-        const size_t c = X.p(k, j, i);
+        const unsigned c = X.p(k, j, i);
         if (adv) {
             rk = __ldg(m.rho0_3d + X.m(k - 1, 0, 0));
             if (k >= 2) rl = __ldg(m.rho0_3d + X.m(k - 2, 0, 0));
@@ -441,18 +445,27 @@ __global__ void __launch_bounds__(32 * kTosWarps, 2) tos_column_kernel(TosArgs p
             SM(s_w, k) = k == 1 ? (0.5f * ((uw + ue) * dzdx + (vs + vn) * dzdy)) * gz : wv;
         }
     }
+    // Each phase's first chunk of global loads is issued before the barrier
+    // that opens the phase (they read nothing the earlier phases write), so
+    // their latency overlaps the other warps' remaining work.
+    A2Load ld[kA2Levels];
+    if (live) {
+#pragma unroll
+        for (int q = 0; q < kA2Levels; ++q) ld[q].load(a, m, X, 1 + wy + q * kTosWarps, nk, j, i, do_adv);
+    }
     __syncthreads();
     // A2: divergence, fpk (initial + pi' advection), column coefficients
     if (live) {
         for (int kb = 1 + wy; kb <= nk; kb += kTosWarps * kA2Levels) {
-            A2Load ld[kA2Levels];
+            if (kb != 1 + wy) {
 #pragma unroll
-            for (int q = 0; q < kA2Levels; ++q) ld[q].load(a, m, X, kb + q * kTosWarps, nk, j, i, do_adv);
+                for (int q = 0; q < kA2Levels; ++q) ld[q].load(a, m, X, kb + q * kTosWarps, nk, j, i, do_adv);
+            }
 #pragma unroll
             for (int q = 0; q < kA2Levels; ++q) {
             const int k = kb + q * kTosWarps;
             if (k > nk) break;
-            const size_t c = X.p(k, j, i);
+            const unsigned c = X.p(k, j, i);
             const float rk = ld[q].rk, rl = ld[q].rl, rk1 = ld[q].rk1, rrf_k = ld[q].rrf_k, rrf_k1 = ld[q].rrf_k1;
             const float qk = ld[q].qk, pk1 = ld[q].pk1, pk2 = ld[q].pk2;
             const float ppten = ld[q].ppten, ppterm = ld[q].ppterm;
@@ -500,22 +513,26 @@ __global__ void __launch_bounds__(32 * kTosWarps, 2) tos_column_kernel(TosArgs p
             }
         }
     }
+    float lmm[kColLevels], lwt[kColLevels];
+    auto a3_loads = [&](int kb) {
+#pragma unroll
+        for (int q = 0; q < kColLevels; ++q) {
+            const int k = kb + q * kTosWarps;
+            lmm[q] = k <= nk ? __ldg(a.mm + X.p(k, j, i)) : 0.0f;
+            lwt[q] = k <= nk ? __ldg(a.wten + X.w(k, y, x)) : 0.0f;
+        }
+    };
+    if (live && do_imp) a3_loads(2 + wy);
     __syncthreads();
     // A3: tridiagonal coefficients and right-hand side, k = 2..nk
     if (live && do_imp) {
         for (int kb = 2 + wy; kb <= nk; kb += kTosWarps * kColLevels) {
-            float lmm[kColLevels], lwt[kColLevels];
-#pragma unroll
-            for (int q = 0; q < kColLevels; ++q) {
-                const int k = kb + q * kTosWarps;
-                lmm[q] = k <= nk ? __ldg(a.mm + X.p(k, j, i)) : 0.0f;
-                lwt[q] = k <= nk ? __ldg(a.wten + X.w(k, y, x)) : 0.0f;
-            }
+            if (kb != 2 + wy) a3_loads(kb);
 #pragma unroll
             for (int q = 0; q < kColLevels; ++q) {
             const int k = kb + q * kTosWarps;
             if (k > nk) break;
-            const size_t c = X.p(k, j, i);
+            const unsigned c = X.p(k, j, i);
             const float mmk = lmm[q];
             const float wt = lwt[q];
             const float aa = k >= 3 ? (-p.asq) * (mmk * SM(s_a1, k - 1)) : 0.0f;
@@ -539,13 +556,42 @@ __global__ void __launch_bounds__(32 * kTosWarps, 2) tos_column_kernel(TosArgs p
             }
         }
     }
+    // phase C's first chunk, in flight while warp 0 runs the Thomas sweep
+    float luu[kColLevels], lvv[kColLevels], lru[kColLevels], lrv[kColLevels], lrw[kColLevels];
+    auto c_loads = [&](int kb) {
+#pragma unroll
+        for (int q = 0; q < kColLevels; ++q) {
+            const int k = kb + q * kTosWarps;
+            luu[q] = lvv[q] = lru[q] = lrv[q] = lrw[q] = 0.0f;
+            if (k > nk) continue;
+            const unsigned qu = X.u(k, y, x), qv = X.v(k, y, x), qw = X.w(k, y, x);
+            luu[q] = __ldg(a.u3d + qu);
+            lvv[q] = __ldg(a.v3d + qv);
+            lru[q] = a.rru[qu];
+            lrv[q] = a.rrv[qv];
+            lrw[q] = a.rrw[qw];
+        }
+    };
+    if (live) c_loads(1 + wy);
     __syncthreads();
     // B: Thomas sweep, one lane per column (1/pivot by the correctly rounded
     // reciprocal, the same word as 1.0f / pivot)
+    // The next level's coefficients are read while this level eliminates, and
+    // the back substitution carries w(k+1) in a register and reads its
+    // coefficients kThomasChunk levels at a time, so shared-memory latency
+    // stays off the sweep's dependency chain (same operations, same order).
     if (live && do_imp && wy == 0) {
         float ec = 0.0f, ed = 0.0f;
+        float aa = SM(s_aa, 2), bb = SM(s_bb, 2), cc = SM(s_cc, 2), dd = SM(s_dd, 2);
+        float wtop = 0.0f;
         for (int k = 2; k <= nk; ++k) {
-            const float aa = SM(s_aa, k), bb = SM(s_bb, k), cc = SM(s_cc, k), dd = SM(s_dd, k);
+            float naa = 0.0f, nbb = 0.0f, ncc = 0.0f, ndd = 0.0f;
+            if (k < nk) {
+                naa = SM(s_aa, k + 1);
+                nbb = SM(s_bb, k + 1);
+                ncc = SM(s_cc, k + 1);
+                ndd = SM(s_dd, k + 1);
+            }
             const float piv = k == 2 ? bb : aa * ec + bb;
             const float inv = __frcp_rn(piv);
             if (dlast) a.tri_pivot[X.p(k, j, i)] = piv;
@@ -556,10 +602,28 @@ __global__ void __launch_bounds__(32 * kTosWarps, 2) tos_column_kernel(TosArgs p
                 SM(s_ed, k) = ed;
                 if (dlast) a.elim_d[X.p(k, j, i)] = ed;
             } else {
-                SM(s_w, k) = (dd - aa * ed) * inv;
+                wtop = (dd - aa * ed) * inv;
+                SM(s_w, k) = wtop;
+            }
+            aa = naa, bb = nbb, cc = ncc, dd = ndd;
+        }
+        float wn = wtop;
+        for (int kb = nk - 1; kb >= 2; kb -= kThomasChunk) {
+            float ce[kThomasChunk], ee[kThomasChunk];
+#pragma unroll
+            for (int q = 0; q < kThomasChunk; ++q) {
+                const int k = kb - q;
+                ce[q] = k >= 2 ? SM(s_cc, k) : 0.0f;
+                ee[q] = k >= 2 ? SM(s_ed, k) : 0.0f;
+            }
+#pragma unroll
+            for (int q = 0; q < kThomasChunk; ++q) {
+                const int k = kb - q;
+                if (k < 2) break;
+                wn = ce[q] * wn + ee[q];
+                SM(s_w, k) = wn;
             }
         }
-        for (int k = nk - 1; k >= 2; --k) SM(s_w, k) = SM(s_cc, k) * SM(s_w, k + 1) + SM(s_ed, k);
     }
     __syncthreads();
     // C: pressure update, filter, halo copy, averages
@@ -567,25 +631,13 @@ __global__ void __launch_bounds__(32 * kTosWarps, 2) tos_column_kernel(TosArgs p
         const bool fill = p.n < p.nloop && (p.abl & GM1B_TOS_BETWEEN_STEP_FILL);
         const bool east = i == ni, north = j == nj;
         for (int kb = 1 + wy; kb <= nk; kb += kTosWarps * kColLevels) {
-            float luu[kColLevels], lvv[kColLevels], lru[kColLevels], lrv[kColLevels], lrw[kColLevels];
-#pragma unroll
-            for (int q = 0; q < kColLevels; ++q) {
-                const int k = kb + q * kTosWarps;
-                luu[q] = lvv[q] = lru[q] = lrv[q] = lrw[q] = 0.0f;
-                if (k > nk) continue;
-                const size_t qu = X.u(k, y, x), qv = X.v(k, y, x), qw = X.w(k, y, x);
-                luu[q] = __ldg(a.u3d + qu);
-                lvv[q] = __ldg(a.v3d + qv);
-                lru[q] = a.rru[qu];
-                lrv[q] = a.rrv[qv];
-                lrw[q] = a.rrw[qw];
-            }
+            if (kb != 1 + wy) c_loads(kb);
 #pragma unroll
             for (int q = 0; q < kColLevels; ++q) {
             const int k = kb + q * kTosWarps;
             if (k > nk) break;
-            const size_t c = X.p(k, j, i);
-            const size_t qu = X.u(k, y, x), qv = X.v(k, y, x), qw = X.w(k, y, x);
+            const unsigned c = X.p(k, j, i);
+            const unsigned qu = X.u(k, y, x), qv = X.v(k, y, x), qw = X.w(k, y, x);
             const float uu = luu[q], vv = lvv[q];
             const float ru = lru[q], rv = lrv[q], rw = lrw[q];
             const float wk = SM(s_w, k), wk1 = SM(s_w, k + 1);
@@ -635,7 +687,7 @@ __global__ void __launch_bounds__(32 * kTosWarps, 2) tos_column_kernel(TosArgs p
                 for (int e = 1; e < 4; ++e) {
                     const int dx = e & 1, dy = e >> 1;
                     if ((dx && !east) || (dy && !north)) continue;
-                    const size_t eu = X.u(k, y + dy, x + dx), ev = X.v(k, y + dy, x + dx), ew = X.w(k, y + dy, x + dx);
+                    const unsigned eu = X.u(k, y + dy, x + dx), ev = X.v(k, y + dy, x + dx), ew = X.w(k, y + dy, x + dx);
                     const float su = a.rru[eu] + __ldg(a.u3d + eu), sv = a.rrv[ev] + __ldg(a.v3d + ev);
                     const float wv = a.w3d[ew];
                     const float sw = a.rrw[ew] + (last ? wv * p.alph : wv);
@@ -922,6 +974,11 @@ extern "C" int32_t gm1b_terrain_open_stage(int32_t ni, int32_t nj, int32_t nk, i
         nrk > 3) {
         gm1b_set_error("gm1b_terrain_open_stage: need arrays and metrics, ni >= 3, nj >= 3, 4 <= nk <= %d, "
                        "nrk in 1..3", kTosMaxNk);
+        return GM1B_ERR_ARGUMENT;
+    }
+    if ((size_t)(nk + 3) * (size_t)(nj + 7) * (size_t)(ni + 7) >= ((size_t)1 << 31)) {
+        gm1b_set_error("gm1b_terrain_open_stage: a %dx%dx%d grid's padded arrays reach 2^31 words; the kernels "
+                       "index with 32-bit offsets", ni, nj, nk);
         return GM1B_ERR_ARGUMENT;
     }
     if (!(dx > 0.0f) || !(dy > 0.0f) || !(dz > 0.0) || !std::isfinite(dx) || !std::isfinite(dy) ||
