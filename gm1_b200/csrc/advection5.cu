@@ -31,17 +31,19 @@ constexpr float kDivClamp = 0x1.79ca1p-67f;
 
 struct PaddedDims {
     int ni, nj, nk;
-    __host__ __device__ __forceinline__ size_t s(int k, int y, int x) const {
-        return ((size_t)k * (nj + 2 * NG) + (size_t)y) * (size_t)(ni + 2 * NG) + (size_t)x;
+    // 32-bit element offsets: the entry points refuse grids whose padded
+    // arrays reach 2^31 words
+    __host__ __device__ __forceinline__ unsigned s(int k, int y, int x) const {
+        return ((unsigned)k * (unsigned)(nj + 2 * NG) + (unsigned)y) * (unsigned)(ni + 2 * NG) + (unsigned)x;
     }
-    __host__ __device__ __forceinline__ size_t u(int k, int y, int x) const {
-        return ((size_t)k * (nj + 2 * NG) + (size_t)y) * (size_t)(ni + 1 + 2 * NG) + (size_t)x;
+    __host__ __device__ __forceinline__ unsigned u(int k, int y, int x) const {
+        return ((unsigned)k * (unsigned)(nj + 2 * NG) + (unsigned)y) * (unsigned)(ni + 1 + 2 * NG) + (unsigned)x;
     }
-    __host__ __device__ __forceinline__ size_t v(int k, int y, int x) const {
-        return ((size_t)k * (nj + 1 + 2 * NG) + (size_t)y) * (size_t)(ni + 2 * NG) + (size_t)x;
+    __host__ __device__ __forceinline__ unsigned v(int k, int y, int x) const {
+        return ((unsigned)k * (unsigned)(nj + 1 + 2 * NG) + (unsigned)y) * (unsigned)(ni + 2 * NG) + (unsigned)x;
     }
-    __host__ __device__ __forceinline__ size_t c(int k, int j, int i) const {  // (nk', nj, ni)
-        return ((size_t)k * nj + (size_t)j) * (size_t)ni + (size_t)i;
+    __host__ __device__ __forceinline__ unsigned c(int k, int j, int i) const {  // (nk', nj, ni)
+        return ((unsigned)k * (unsigned)nj + (unsigned)j) * (unsigned)ni + (unsigned)i;
     }
 };
 
@@ -507,6 +509,11 @@ extern "C" int32_t gm1b_terrain_mass_flux5(int32_t ni, int32_t nj, int32_t nk, c
         gm1b_set_error("gm1b_terrain_mass_flux5: need arrays and ni, nj, nk >= 8");
         return GM1B_ERR_ARGUMENT;
     }
+    if ((size_t)(nk + 3) * (size_t)(nj + 7) * (size_t)(ni + 7) >= ((size_t)1 << 31)) {
+        gm1b_set_error("gm1b_terrain_mass_flux5: a %dx%dx%d grid's padded arrays reach 2^31 words; the kernels index with 32-bit "
+                       "offsets", ni, nj, nk);
+        return GM1B_ERR_ARGUMENT;
+    }
     if (!(dx > 0.0f) || !(dy > 0.0f) || !(dz > 0.0f) || !isfinite(dx) || !isfinite(dy) || !isfinite(dz)) {
         gm1b_set_error("gm1b_terrain_mass_flux5: dx, dy, dz must be finite and > 0");
         return GM1B_ERR_ARGUMENT;
@@ -549,6 +556,11 @@ extern "C" int32_t gm1b_scalar_advection5(int32_t ni, int32_t nj, int32_t nk,
                                          int32_t levels_per_chunk, void *stream) {
     if (arrays == nullptr || ni < 8 || nj < 8 || nk < 8) {
         gm1b_set_error("gm1b_scalar_advection5: need arrays and ni, nj, nk >= 8");
+        return GM1B_ERR_ARGUMENT;
+    }
+    if ((size_t)(nk + 3) * (size_t)(nj + 7) * (size_t)(ni + 7) >= ((size_t)1 << 31)) {
+        gm1b_set_error("gm1b_scalar_advection5: a %dx%dx%d grid's padded arrays reach 2^31 words; the kernels index with 32-bit "
+                       "offsets", ni, nj, nk);
         return GM1B_ERR_ARGUMENT;
     }
     if (nrk < 1 || nrk > 3) {

@@ -32,17 +32,19 @@ struct MomArgs {
     float rdx, rdy, rdz, dz;
 };
 
-__device__ __forceinline__ size_t iu(const MomArgs &a, int k, int y, int x) {
-    return ((size_t)k * (a.nj + 2 * G) + (size_t)y) * (size_t)(a.ni + 1 + 2 * G) + (size_t)x;
+// 32-bit element offsets (the host refuses grids whose padded arrays reach
+// 2^31 words)
+__device__ __forceinline__ unsigned iu(const MomArgs &a, int k, int y, int x) {
+    return ((unsigned)k * (unsigned)(a.nj + 2 * G) + (unsigned)y) * (unsigned)(a.ni + 1 + 2 * G) + (unsigned)x;
 }
-__device__ __forceinline__ size_t iv(const MomArgs &a, int k, int y, int x) {
-    return ((size_t)k * (a.nj + 1 + 2 * G) + (size_t)y) * (size_t)(a.ni + 2 * G) + (size_t)x;
+__device__ __forceinline__ unsigned iv(const MomArgs &a, int k, int y, int x) {
+    return ((unsigned)k * (unsigned)(a.nj + 1 + 2 * G) + (unsigned)y) * (unsigned)(a.ni + 2 * G) + (unsigned)x;
 }
-__device__ __forceinline__ size_t iw(const MomArgs &a, int k, int y, int x) {
-    return ((size_t)k * (a.nj + 2 * G) + (size_t)y) * (size_t)(a.ni + 2 * G) + (size_t)x;
+__device__ __forceinline__ unsigned iw(const MomArgs &a, int k, int y, int x) {
+    return ((unsigned)k * (unsigned)(a.nj + 2 * G) + (unsigned)y) * (unsigned)(a.ni + 2 * G) + (unsigned)x;
 }
-__device__ __forceinline__ size_t ic(const MomArgs &a, int k, int j, int i) {
-    return ((size_t)k * a.nj + (size_t)j) * (size_t)a.ni + (size_t)i;
+__device__ __forceinline__ unsigned ic(const MomArgs &a, int k, int j, int i) {
+    return ((unsigned)k * (unsigned)a.nj + (unsigned)j) * (unsigned)a.ni + (unsigned)i;
 }
 __device__ __forceinline__ int clampn(int x, int n) { return x < 0 ? 0 : (x >= n ? n - 1 : x); }
 // periodic wraps of a cell (c*) and a face (f*) index
@@ -283,7 +285,7 @@ __global__ void __launch_bounds__(128) mom5_adv_kernel(MomArgs a) {
         total = total + uc * (0.5f * (a.divx[ic(a, k0, j, east)] + a.divx[ic(a, k0, j, west)]));
         const float scale = __ldg(a.gzu + (size_t)j * (ni + 1) + f) /
                             (0.5f * (__ldg(a.rho0 + ic(a, k0, j, west)) + __ldg(a.rho0 + ic(a, k0, j, east))));
-        const size_t p = iu(a, k, y, x);
+        const unsigned p = iu(a, k, y, x);
         a.uten[p] = a.uten[p] + total * scale;
     }
     // advv at face g = yy of column i = xx
@@ -314,7 +316,7 @@ __global__ void __launch_bounds__(128) mom5_adv_kernel(MomArgs a) {
         total = total + vc * (0.5f * (a.divx[ic(a, k0, north, i)] + a.divx[ic(a, k0, south, i)]));
         const float scale = __ldg(a.gzv + (size_t)g * ni + i) /
                             (0.5f * (__ldg(a.rho0 + ic(a, k0, south, i)) + __ldg(a.rho0 + ic(a, k0, north, i))));
-        const size_t p = iv(a, k, y, x);
+        const unsigned p = iv(a, k, y, x);
         a.vten[p] = a.vten[p] + total * scale;
     }
     // advw at Fortran face kf = k + 1 (2..nk) of column (yy, xx)
@@ -354,7 +356,7 @@ __global__ void __launch_bounds__(128) mom5_adv_kernel(MomArgs a) {
         float total = (advx + advy) + advz;
         total = total + wc * (c2 * a.divx[ic(a, kf - 1, j, i)] + c1 * a.divx[ic(a, kf - 2, j, i)]);
         const float scale = __ldg(a.rrf0 + ic(a, kf - 1, j, i)) * __ldg(a.gz + (size_t)j * ni + i);
-        const size_t p = iw(a, kf, y, x);
+        const unsigned p = iw(a, kf, y, x);
         a.wten[p] = a.wten[p] + total * scale;
     }
 }
@@ -380,6 +382,11 @@ int mom_args(int ni, int nj, int nk, const gm1b_momentum5_arrays *s, uint32_t la
              float dz, MomArgs &a, const char *what) {
     if (s == nullptr || ni < 7 || nj < 7 || nk < 8) {
         gm1b_set_error("%s: need arrays, ni >= 7, nj >= 7, nk >= 8", what);
+        return GM1B_ERR_ARGUMENT;
+    }
+    if ((size_t)(nk + 3) * (size_t)(nj + 7) * (size_t)(ni + 7) >= ((size_t)1 << 31)) {
+        gm1b_set_error("%s: a %dx%dx%d grid's padded arrays reach 2^31 words; the kernels index with 32-bit offsets",
+                       what, ni, nj, nk);
         return GM1B_ERR_ARGUMENT;
     }
     if (!(dx > 0.0f) || !(dy > 0.0f) || !(dz > 0.0f) || !isfinite(dx) || !isfinite(dy) || !isfinite(dz)) {
