@@ -38,8 +38,10 @@ struct DefArgs {
     float rdx, rdy, rds, zt, dz;
 };
 
-__device__ __forceinline__ size_t i3(int k, int j, int i, int ny, int nx) {
-    return ((size_t)k * ny + (size_t)j) * (size_t)nx + (size_t)i;
+// 32-bit element offsets (the entry points refuse grids whose arrays reach
+// 2^31 words)
+__device__ __forceinline__ unsigned i3(int k, int j, int i, int ny, int nx) {
+    return ((unsigned)k * (unsigned)ny + (unsigned)j) * (unsigned)nx + (unsigned)i;
 }
 
 // face-level value of a u- or v-shaped field (levels nk, rows ny, row nx)
@@ -60,17 +62,17 @@ __device__ __forceinline__ float atw(const float *q, int kf, int j, int i, int n
 // s11, s22, s33 at mass level k, cell (j, i)
 __device__ __forceinline__ void strain_diag(const DefArgs &p, int k, int j, int i, float &s11, float &s22, float &s33) {
     const int ni = p.ni, nj = p.nj, nk = p.nk, ux = ni + 1, vy = nj + 1;
-    const size_t c = i3(k, j, i, nj, ni);
-    const float g = p.gz[(size_t)j * ni + i], r = p.rho[c];
-    float hor = g * (p.u[i3(k, j, i + 1, nj, ux)] * p.rgzu[(size_t)j * ux + i + 1] -
-                     p.u[i3(k, j, i, nj, ux)] * p.rgzu[(size_t)j * ux + i]);
+    const unsigned c = i3(k, j, i, nj, ni);
+    const float g = p.gz[(unsigned)j * ni + i], r = p.rho[c];
+    float hor = g * (p.u[i3(k, j, i + 1, nj, ux)] * p.rgzu[(unsigned)j * ux + i + 1] -
+                     p.u[i3(k, j, i, nj, ux)] * p.rgzu[(unsigned)j * ux + i]);
     hor = hor * p.rdx;
     float up = p.gx[i3(k + 1, j, i, nj, ni)] * (atw(p.u, k + 1, j, i, nk, nj, ux) + atw(p.u, k + 1, j, i + 1, nk, nj, ux));
     float lo = p.gx[c] * (atw(p.u, k, j, i, nk, nj, ux) + atw(p.u, k, j, i + 1, nk, nj, ux));
     float vert = ((up - lo) * 0.5f) * p.rds;
     s11 = (hor + vert) * r;
-    hor = g * (p.v[i3(k, j + 1, i, vy, ni)] * p.rgzv[(size_t)(j + 1) * ni + i] -
-               p.v[i3(k, j, i, vy, ni)] * p.rgzv[(size_t)j * ni + i]);
+    hor = g * (p.v[i3(k, j + 1, i, vy, ni)] * p.rgzv[(unsigned)(j + 1) * ni + i] -
+               p.v[i3(k, j, i, vy, ni)] * p.rgzv[(unsigned)j * ni + i]);
     hor = hor * p.rdy;
     up = p.gy[i3(k + 1, j, i, nj, ni)] * (atw(p.v, k + 1, j, i, nk, vy, ni) + atw(p.v, k + 1, j + 1, i, nk, vy, ni));
     lo = p.gy[c] * (atw(p.v, k, j, i, nk, vy, ni) + atw(p.v, k, j + 1, i, nk, vy, ni));
@@ -86,17 +88,17 @@ __device__ __forceinline__ float strain_s12(const DefArgs &p, int k, int jc, int
     const int jj = jc < 1 ? 1 : (jc > nj - 1 ? nj - 1 : jc);
     const int ii = ic < 1 ? 1 : (ic > ni - 1 ? ni - 1 : ic);
     const float sig_lo = (float)k * p.dz, sig_hi = (float)(k + 1) * p.dz;
-    float r1 = p.rho[i3(k, jj - 1, ii - 1, nj, ni)] * p.gz[(size_t)(jj - 1) * ni + ii - 1] +
-               p.rho[i3(k, jj, ii, nj, ni)] * p.gz[(size_t)jj * ni + ii];
-    r1 = r1 + (p.rho[i3(k, jj, ii - 1, nj, ni)] * p.gz[(size_t)jj * ni + ii - 1] +
-               p.rho[i3(k, jj - 1, ii, nj, ni)] * p.gz[(size_t)(jj - 1) * ni + ii]);
+    float r1 = p.rho[i3(k, jj - 1, ii - 1, nj, ni)] * p.gz[(unsigned)(jj - 1) * ni + ii - 1] +
+               p.rho[i3(k, jj, ii, nj, ni)] * p.gz[(unsigned)jj * ni + ii];
+    r1 = r1 + (p.rho[i3(k, jj, ii - 1, nj, ni)] * p.gz[(unsigned)jj * ni + ii - 1] +
+               p.rho[i3(k, jj - 1, ii, nj, ni)] * p.gz[(unsigned)(jj - 1) * ni + ii]);
     r1 = 0.25f * r1;
-    const float rgzu_t = p.rgzu[(size_t)jj * ux + ii], rgzu_b = p.rgzu[(size_t)(jj - 1) * ux + ii];
+    const float rgzu_t = p.rgzu[(unsigned)jj * ux + ii], rgzu_b = p.rgzu[(unsigned)(jj - 1) * ux + ii];
     const float x1 = (r1 * (p.u[i3(k, jj, ii, nj, ux)] * rgzu_t - p.u[i3(k, jj - 1, ii, nj, ux)] * rgzu_b)) * p.rdy;
     const float xu = (p.zt - sig_hi) * (atw(p.u, k + 1, jj - 1, ii, nk, nj, ux) + atw(p.u, k + 1, jj, ii, nk, nj, ux));
     const float xl = (p.zt - sig_lo) * (atw(p.u, k, jj - 1, ii, nk, nj, ux) + atw(p.u, k, jj, ii, nk, nj, ux));
     const float x2 = ((((0.5f * (xu - xl)) * p.rds) * r1) * (rgzu_t - rgzu_b)) * p.rdy;
-    const float rgzv_r = p.rgzv[(size_t)jj * ni + ii], rgzv_l = p.rgzv[(size_t)jj * ni + ii - 1];
+    const float rgzv_r = p.rgzv[(unsigned)jj * ni + ii], rgzv_l = p.rgzv[(unsigned)jj * ni + ii - 1];
     const float y1 = (r1 * (p.v[i3(k, jj, ii, vy, ni)] * rgzv_r - p.v[i3(k, jj, ii - 1, vy, ni)] * rgzv_l)) * p.rdx;
     const float yu = (p.zt - sig_hi) * (atw(p.v, k + 1, jj, ii - 1, nk, vy, ni) + atw(p.v, k + 1, jj, ii, nk, vy, ni));
     const float yl = (p.zt - sig_lo) * (atw(p.v, k, jj, ii - 1, nk, vy, ni) + atw(p.v, k, jj, ii, nk, vy, ni));
@@ -110,7 +112,7 @@ __device__ __forceinline__ float strain_s13(const DefArgs &p, int kf, int j, int
     const int il = ic - 1 < 0 ? 0 : ic - 1, ir = ic < ni - 1 ? ic : ni - 1;
     const float sig_l = ((float)kf - 0.5f) * p.dz, sig_u = ((float)kf + 0.5f) * p.dz;
     const float wr = p.w[i3(kf, j, ir, nj, ni)], wl = p.w[i3(kf, j, il, nj, ni)];
-    const float rgr = p.rgz[(size_t)j * ni + ir], rgl = p.rgz[(size_t)j * ni + il];
+    const float rgr = p.rgz[(unsigned)j * ni + ir], rgl = p.rgz[(unsigned)j * ni + il];
     const float du = (p.u[i3(kf, j, ic, nj, ux)] - p.u[i3(kf - 1, j, ic, nj, ux)]) * p.rds;
     const float hw = (wr * rgr - wl * rgl) * p.rdx;
     const float upper = (p.zt - sig_u) * (0.5f * (wr + p.w[i3(kf + 1, j, ir, nj, ni)]) +
@@ -119,8 +121,8 @@ __device__ __forceinline__ float strain_s13(const DefArgs &p, int kf, int j, int
                                           0.5f * (p.w[i3(kf - 1, j, il, nj, ni)] + wl));
     const float terrain = (((0.5f * p.rds) * (upper - lower)) * (rgr - rgl)) * p.rdx;
     const float strain = 0.5f * ((du + hw) + terrain);
-    const float density = 0.5f * (p.gz[(size_t)j * ni + il] * p.rf[i3(kf, j, il, nj, ni)] +
-                                  p.gz[(size_t)j * ni + ir] * p.rf[i3(kf, j, ir, nj, ni)]);
+    const float density = 0.5f * (p.gz[(unsigned)j * ni + il] * p.rf[i3(kf, j, il, nj, ni)] +
+                                  p.gz[(unsigned)j * ni + ir] * p.rf[i3(kf, j, ir, nj, ni)]);
     return strain * density;
 }
 
@@ -130,7 +132,7 @@ __device__ __forceinline__ float strain_s23(const DefArgs &p, int kf, int jc, in
     const int jb = jc - 1 < 0 ? 0 : jc - 1, jt = jc < nj - 1 ? jc : nj - 1;
     const float sig_l = ((float)kf - 0.5f) * p.dz, sig_u = ((float)kf + 0.5f) * p.dz;
     const float wt = p.w[i3(kf, jt, i, nj, ni)], wb = p.w[i3(kf, jb, i, nj, ni)];
-    const float rgt = p.rgz[(size_t)jt * ni + i], rgb = p.rgz[(size_t)jb * ni + i];
+    const float rgt = p.rgz[(unsigned)jt * ni + i], rgb = p.rgz[(unsigned)jb * ni + i];
     const float dv = (p.v[i3(kf, jc, i, vy, ni)] - p.v[i3(kf - 1, jc, i, vy, ni)]) * p.rds;
     const float hw = (wt * rgt - wb * rgb) * p.rdy;
     const float upper = (p.zt - sig_u) * (0.5f * (wt + p.w[i3(kf + 1, jt, i, nj, ni)]) +
@@ -139,8 +141,8 @@ __device__ __forceinline__ float strain_s23(const DefArgs &p, int kf, int jc, in
                                           0.5f * (p.w[i3(kf - 1, jb, i, nj, ni)] + wb));
     const float terrain = (((0.5f * p.rds) * (upper - lower)) * (rgt - rgb)) * p.rdy;
     const float strain = 0.5f * ((dv + hw) + terrain);
-    const float density = 0.5f * (p.gz[(size_t)jb * ni + i] * p.rf[i3(kf, jb, i, nj, ni)] +
-                                  p.gz[(size_t)jt * ni + i] * p.rf[i3(kf, jt, i, nj, ni)]);
+    const float density = 0.5f * (p.gz[(unsigned)jb * ni + i] * p.rf[i3(kf, jb, i, nj, ni)] +
+                                  p.gz[(unsigned)jt * ni + i] * p.rf[i3(kf, jt, i, nj, ni)]);
     return strain * density;
 }
 
@@ -182,7 +184,7 @@ __global__ void __launch_bounds__(kDX *kDY) calcdef_tile_kernel(DefArgs p) {
         }
         __syncthreads();
         if (own) {
-            const size_t f = i3(kf, j, i, nj, ni);
+            const unsigned f = i3(kf, j, i, nj, ni);
             const float a = p.c1[f], b = p.c2[f];
             const float t11 = a * sq(p11) + b * sq(c11);
             const float t22 = a * sq(p22) + b * sq(c22);
@@ -231,8 +233,8 @@ struct NmCell {
     float t, qt, thv, qvci;
 };
 
-__device__ __forceinline__ NmCell nm_cell(const NmArgs &a, int k, size_t p) {
-    const size_t cells = (size_t)a.nk * a.nj * a.ni;
+__device__ __forceinline__ NmCell nm_cell(const NmArgs &a, int k, unsigned p) {
+    const unsigned cells = (unsigned)a.nk * a.nj * a.ni;
     NmCell r;
     const float qv = a.q3d[p];
     r.qvci = (qv + a.q3d[cells + p]) + a.q3d[3 * cells + p];
@@ -303,8 +305,8 @@ __global__ void __launch_bounds__(128) moist_nm_kernel(NmArgs a) {
     const bool in = i < ni && j < nj;
     int sat = 0, liq = 0, mix = 0, ice = 0;
     if (in) {
-        const size_t col = (size_t)j * ni + i, plane = (size_t)nj * ni;
-        const size_t m = (size_t)kf * plane + col, f = m;
+        const unsigned col = (unsigned)j * ni + i, plane = (unsigned)nj * ni;
+        const unsigned m = (unsigned)kf * plane + col, f = m;
         NmCell up{}, lo{};
         if (kf < nk) {
             up = nm_cell(a, kf, m);
@@ -315,7 +317,7 @@ __global__ void __launch_bounds__(128) moist_nm_kernel(NmArgs a) {
         }
         float value = 0.0f;
         if (kf >= 1 && kf < nk) {
-            const size_t l = m - plane;
+            const unsigned l = m - plane;
             lo = nm_cell(a, kf - 1, l);
             const NmConsts &c = a.c;
             const float mrdz = a.rdz * a.mf[f];
@@ -414,8 +416,8 @@ extern "C" int32_t gm1b_terrain_deformation(int32_t ni, int32_t nj, int32_t nk,
             gm1b_set_error("gm1b_terrain_deformation: a required array is NULL");
             return GM1B_ERR_ARGUMENT;
         }
-    if ((double)(nk + 1) * (nj + 1) * (ni + 1) >= 2147483647.0 * 4.0) {
-        gm1b_set_error("gm1b_terrain_deformation: grid too large");
+    if ((size_t)(nk + 3) * (size_t)(nj + 7) * (size_t)(ni + 7) >= ((size_t)1 << 31)) {
+        gm1b_set_error("gm1b_terrain_deformation: grid too large (the kernels index with 32-bit offsets)");
         return GM1B_ERR_ARGUMENT;
     }
     DefArgs p;
@@ -453,6 +455,10 @@ extern "C" int32_t gm1b_moist_nm(int32_t ni, int32_t nj, int32_t nk, const gm1b_
                                  void *stream) {
     if (arrays == nullptr || ni < 1 || nj < 1 || nk < 2 || nk > 65534) {
         gm1b_set_error("gm1b_moist_nm: need arrays, ni >= 1, nj >= 1 and 2 <= nk <= 65534");
+        return GM1B_ERR_ARGUMENT;
+    }
+    if ((size_t)(nk + 3) * (size_t)(nj + 7) * (size_t)(ni + 7) >= ((size_t)1 << 31)) {
+        gm1b_set_error("gm1b_moist_nm: grid too large (the kernels index with 32-bit offsets)");
         return GM1B_ERR_ARGUMENT;
     }
     if (!(dz > 0.0f) || !isfinite(dz)) {

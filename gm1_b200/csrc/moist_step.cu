@@ -53,35 +53,35 @@ struct FillGeom {
 // ew = 0 the south/north halo rows of columns x0-1..xl+1
 __global__ void __launch_bounds__(256) open_fill_pass_kernel(FillGeom f, int ew, int zero) {
     const int nlev = f.k1 - f.k0 + 1;
-    const size_t lines = ew ? (size_t)(f.yl - f.y0 + 3) : (size_t)(f.xl - f.x0 + 3);
-    const size_t per = lines * (size_t)(2 * f.g);
-    const size_t total = per * nlev;
-    const size_t plane = (size_t)f.ny * f.nx;
-    for (size_t z = (size_t)blockIdx.x * blockDim.x + threadIdx.x; z < total; z += (size_t)gridDim.x * blockDim.x) {
+    const unsigned lines = ew ? (unsigned)(f.yl - f.y0 + 3) : (unsigned)(f.xl - f.x0 + 3);
+    const unsigned per = lines * (unsigned)(2 * f.g);
+    const unsigned total = per * nlev;
+    const unsigned plane = (unsigned)f.ny * f.nx;
+    for (unsigned z = (unsigned)blockIdx.x * blockDim.x + threadIdx.x; z < total; z += (unsigned)gridDim.x * blockDim.x) {
         const int h = (int)(z % (2 * f.g));
         const int l = (int)((z / (2 * f.g)) % lines);
         const int k = (int)(z / per) + f.k0;
-        float *lev = f.q + (size_t)k * plane;
+        float *lev = f.q + (unsigned)k * plane;
         if (ew) {
             const int y = f.y0 - 1 + l;
             const int x = h < f.g ? f.x0 - f.g + h : f.xl + 1 + (h - f.g);
             const int src = h < f.g ? f.x0 : f.xl;
-            lev[(size_t)y * f.nx + x] = lev[(size_t)y * f.nx + src];
+            lev[(unsigned)y * f.nx + x] = lev[(unsigned)y * f.nx + src];
         } else {
             const int x = f.x0 - 1 + l;
             const int y = h < f.g ? f.y0 - f.g + h : f.yl + 1 + (h - f.g);
             const int src = h < f.g ? f.y0 : f.yl;
-            lev[(size_t)y * f.nx + x] = lev[(size_t)src * f.nx + x];
+            lev[(unsigned)y * f.nx + x] = lev[(unsigned)src * f.nx + x];
         }
     }
     if (zero) {
-        const size_t rows = (size_t)(f.yl - f.y0 + 3), cols = (size_t)(f.xl - f.x0 + 3);
-        for (size_t z = (size_t)blockIdx.x * blockDim.x + threadIdx.x; z < 2 * rows * cols;
-             z += (size_t)gridDim.x * blockDim.x) {
+        const unsigned rows = (unsigned)(f.yl - f.y0 + 3), cols = (unsigned)(f.xl - f.x0 + 3);
+        for (unsigned z = (unsigned)blockIdx.x * blockDim.x + threadIdx.x; z < 2 * rows * cols;
+             z += (unsigned)gridDim.x * blockDim.x) {
             const int x = f.x0 - 1 + (int)(z % cols);
             const int y = f.y0 - 1 + (int)((z / cols) % rows);
             const int k = z / (rows * cols) == 0 ? 1 : f.nk + 1;
-            f.q[(size_t)k * plane + (size_t)y * f.nx + x] = 0.0f;
+            f.q[(unsigned)k * plane + (unsigned)y * f.nx + x] = 0.0f;
         }
     }
 }
@@ -123,17 +123,17 @@ bool fill_geometry(int kind, int ni, int nj, int nk, float *q, FillGeom &f) {
 // ---------------------------------------------------------------------------
 struct Lane {
     int ni, nj, nk;
-    __device__ __forceinline__ size_t s(int k, int y, int x) const {  // scalar / w layout, padded coordinates
-        return ((size_t)k * (nj + 6) + y) * (size_t)(ni + 6) + x;
+    __device__ __forceinline__ unsigned s(int k, int y, int x) const {  // scalar / w layout, padded coordinates
+        return ((unsigned)k * (nj + 6) + y) * (unsigned)(ni + 6) + x;
     }
-    __device__ __forceinline__ size_t u(int k, int y, int x) const {
-        return ((size_t)k * (nj + 6) + y) * (size_t)(ni + 7) + x;
+    __device__ __forceinline__ unsigned u(int k, int y, int x) const {
+        return ((unsigned)k * (nj + 6) + y) * (unsigned)(ni + 7) + x;
     }
-    __device__ __forceinline__ size_t v(int k, int y, int x) const {
-        return ((size_t)k * (nj + 7) + y) * (size_t)(ni + 6) + x;
+    __device__ __forceinline__ unsigned v(int k, int y, int x) const {
+        return ((unsigned)k * (nj + 7) + y) * (unsigned)(ni + 6) + x;
     }
-    __device__ __forceinline__ size_t m(int k0, int j0, int i0) const {
-        return ((size_t)k0 * nj + j0) * (size_t)ni + i0;
+    __device__ __forceinline__ unsigned m(int k0, int j0, int i0) const {
+        return ((unsigned)k0 * nj + j0) * (unsigned)ni + i0;
     }
 };
 
@@ -141,7 +141,7 @@ struct Lane {
 __device__ __forceinline__ float buoy_face(const float *dum8, const float *c1, const float *c2, const Lane &L, int kf,
                                            int j, int i) {
     if (kf == 1 || kf == L.nk + 1) return 0.0f;
-    const size_t p = L.m(kf - 1, j, i);
+    const unsigned p = L.m(kf - 1, j, i);
     return c1[p] * dum8[L.s(kf - 1, j + 3, i + 3)] + c2[p] * dum8[L.s(kf, j + 3, i + 3)];
 }
 
@@ -149,33 +149,33 @@ __global__ void __launch_bounds__(256) msb_buoyancy_kernel(const float *dum8, co
                                                           const float *gxu, const float *gyv, float *uten,
                                                           float *vten, float *wten, Lane L) {
     const int ni = L.ni, nj = L.nj, nk = L.nk;
-    const size_t nw = (size_t)(nk - 1) * nj * ni, nu = (size_t)nk * nj * (ni - 1), nv = (size_t)nk * (nj - 1) * ni;
-    for (size_t z = (size_t)blockIdx.x * blockDim.x + threadIdx.x; z < nw + nu + nv; z += (size_t)gridDim.x * blockDim.x) {
+    const unsigned nw = (unsigned)(nk - 1) * nj * ni, nu = (unsigned)nk * nj * (ni - 1), nv = (unsigned)nk * (nj - 1) * ni;
+    for (unsigned z = (unsigned)blockIdx.x * blockDim.x + threadIdx.x; z < nw + nu + nv; z += (unsigned)gridDim.x * blockDim.x) {
         if (z < nw) {
-            const int i = (int)(z % ni), j = (int)((z / ni) % nj), kf = (int)(z / ((size_t)ni * nj)) + 2;
-            const size_t p = L.m(kf - 1, j, i);
+            const int i = (int)(z % ni), j = (int)((z / ni) % nj), kf = (int)(z / ((unsigned)ni * nj)) + 2;
+            const unsigned p = L.m(kf - 1, j, i);
             const float add = c1[p] * dum8[L.s(kf - 1, j + 3, i + 3)] + c2[p] * dum8[L.s(kf, j + 3, i + 3)];
-            const size_t d = L.s(kf, j + 3, i + 3);
+            const unsigned d = L.s(kf, j + 3, i + 3);
             wten[d] = wten[d] + add;
         } else if (z < nw + nu) {
-            const size_t q = z - nw;
-            const int f = (int)(q % (ni - 1)) + 1, j = (int)((q / (ni - 1)) % nj), k = (int)(q / ((size_t)(ni - 1) * nj)) + 1;
+            const unsigned q = z - nw;
+            const int f = (int)(q % (ni - 1)) + 1, j = (int)((q / (ni - 1)) % nj), k = (int)(q / ((unsigned)(ni - 1) * nj)) + 1;
             float t = (buoy_face(dum8, c1, c2, L, k + 1, j, f) + buoy_face(dum8, c1, c2, L, k + 1, j, f - 1)) +
                       (buoy_face(dum8, c1, c2, L, k, j, f) + buoy_face(dum8, c1, c2, L, k, j, f - 1));
             t = 0.125f * t;
             t = t - 0.25f * (dum8[L.s(k, j + 3, f + 3)] + dum8[L.s(k, j + 3, f + 2)]);
-            t = t * (gxu[((size_t)(k - 1) * nj + j) * (ni + 1) + f] + gxu[((size_t)k * nj + j) * (ni + 1) + f]);
-            const size_t d = L.u(k, j + 3, f + 3);
+            t = t * (gxu[((unsigned)(k - 1) * nj + j) * (ni + 1) + f] + gxu[((unsigned)k * nj + j) * (ni + 1) + f]);
+            const unsigned d = L.u(k, j + 3, f + 3);
             uten[d] = uten[d] + t;
         } else {
-            const size_t q = z - nw - nu;
-            const int i = (int)(q % ni), f = (int)((q / ni) % (nj - 1)) + 1, k = (int)(q / ((size_t)ni * (nj - 1))) + 1;
+            const unsigned q = z - nw - nu;
+            const int i = (int)(q % ni), f = (int)((q / ni) % (nj - 1)) + 1, k = (int)(q / ((unsigned)ni * (nj - 1))) + 1;
             float t = (buoy_face(dum8, c1, c2, L, k + 1, f, i) + buoy_face(dum8, c1, c2, L, k + 1, f - 1, i)) +
                       (buoy_face(dum8, c1, c2, L, k, f, i) + buoy_face(dum8, c1, c2, L, k, f - 1, i));
             t = 0.125f * t;
             t = t - 0.25f * (dum8[L.s(k, f + 3, i + 3)] + dum8[L.s(k, f + 2, i + 3)]);
-            t = t * (gyv[((size_t)(k - 1) * (nj + 1) + f) * ni + i] + gyv[((size_t)k * (nj + 1) + f) * ni + i]);
-            const size_t d = L.v(k, f + 3, i + 3);
+            t = t * (gyv[((unsigned)(k - 1) * (nj + 1) + f) * ni + i] + gyv[((unsigned)k * (nj + 1) + f) * ni + i]);
+            const unsigned d = L.v(k, f + 3, i + 3);
             vten[d] = vten[d] + t;
         }
     }
@@ -188,10 +188,10 @@ struct Getdiv {
 };
 
 __device__ __forceinline__ float gd_xu(const Getdiv &a, const Lane &L, int k, int j, int f) {
-    return a.rru[L.u(k, j + 3, f + 3)] * a.rgzu[(size_t)j * (L.ni + 1) + f];
+    return a.rru[L.u(k, j + 3, f + 3)] * a.rgzu[(unsigned)j * (L.ni + 1) + f];
 }
 __device__ __forceinline__ float gd_yv(const Getdiv &a, const Lane &L, int k, int f, int i) {
-    return a.rrv[L.v(k, f + 3, i + 3)] * a.rgzv[(size_t)f * L.ni + i];
+    return a.rrv[L.v(k, f + 3, i + 3)] * a.rgzv[(unsigned)f * L.ni + i];
 }
 // transformed w on w levels (getdiv's own grouping: r1 = 0.5 (1 - r2), r2 = 0.5 r2)
 __device__ __forceinline__ float gd_wt(const Getdiv &a, const Lane &L, int kf, int j, int i) {
@@ -205,15 +205,15 @@ __device__ __forceinline__ float gd_wt(const Getdiv &a, const Lane &L, int kf, i
                      r1 * (gd_xu(a, L, kf - 1, j, i) + gd_xu(a, L, kf - 1, j, i + 1));
     const float vy = r2 * (gd_yv(a, L, kf, j, i) + gd_yv(a, L, kf, j + 1, i)) +
                      r1 * (gd_yv(a, L, kf - 1, j, i) + gd_yv(a, L, kf - 1, j + 1, i));
-    float terrain = ux * a.dzdx[(size_t)j * L.ni + i] + vy * a.dzdy[(size_t)j * L.ni + i];
-    terrain = ((terrain * (sf - a.zt)) * a.gz[(size_t)j * L.ni + i]) * (1.0f / a.zt);
+    float terrain = ux * a.dzdx[(unsigned)j * L.ni + i] + vy * a.dzdy[(unsigned)j * L.ni + i];
+    terrain = ((terrain * (sf - a.zt)) * a.gz[(unsigned)j * L.ni + i]) * (1.0f / a.zt);
     return a.rrw[L.s(kf, j + 3, i + 3)] + terrain;
 }
 
 __global__ void __launch_bounds__(256) msb_getdiv_kernel(Getdiv a, Lane L) {
-    const size_t n = (size_t)L.nk * L.nj * L.ni;
-    for (size_t z = (size_t)blockIdx.x * blockDim.x + threadIdx.x; z < n; z += (size_t)gridDim.x * blockDim.x) {
-        const int i = (int)(z % L.ni), j = (int)((z / L.ni) % L.nj), k = (int)(z / ((size_t)L.ni * L.nj)) + 1;
+    const unsigned n = (unsigned)L.nk * L.nj * L.ni;
+    for (unsigned z = (unsigned)blockIdx.x * blockDim.x + threadIdx.x; z < n; z += (unsigned)gridDim.x * blockDim.x) {
+        const int i = (int)(z % L.ni), j = (int)((z / L.ni) % L.nj), k = (int)(z / ((unsigned)L.ni * L.nj)) + 1;
         float d = (gd_xu(a, L, k, j, i + 1) - gd_xu(a, L, k, j, i)) * a.rdx +
                   (gd_yv(a, L, k, j + 1, i) - gd_yv(a, L, k, j, i)) * a.rdy;
         d = d + (gd_wt(a, L, k + 1, j, i) - gd_wt(a, L, k, j, i)) * a.rdsf;
@@ -226,21 +226,21 @@ __global__ void __launch_bounds__(256) msb_getdiv_kernel(Getdiv a, Lane L) {
 __global__ void __launch_bounds__(256) msb_getdivx_horizontal_kernel(const float *rho0, const float *rgzu,
                                                                     const float *rgzv, float *rru, float *rrv, Lane L) {
     const int ni = L.ni, nj = L.nj, nk = L.nk;
-    const size_t nu = (size_t)nk * nj * (ni + 1), nv = (size_t)nk * (nj + 1) * ni;
-    for (size_t z = (size_t)blockIdx.x * blockDim.x + threadIdx.x; z < nu + nv; z += (size_t)gridDim.x * blockDim.x) {
+    const unsigned nu = (unsigned)nk * nj * (ni + 1), nv = (unsigned)nk * (nj + 1) * ni;
+    for (unsigned z = (unsigned)blockIdx.x * blockDim.x + threadIdx.x; z < nu + nv; z += (unsigned)gridDim.x * blockDim.x) {
         if (z < nu) {
-            const int f = (int)(z % (ni + 1)), j = (int)((z / (ni + 1)) % nj), k = (int)(z / ((size_t)(ni + 1) * nj)) + 1;
+            const int f = (int)(z % (ni + 1)), j = (int)((z / (ni + 1)) % nj), k = (int)(z / ((unsigned)(ni + 1) * nj)) + 1;
             const int l = f == 0 ? 0 : f - 1, r = f == ni ? ni - 1 : f;
             const float den = 0.5f * (rho0[L.m(k - 1, j, l)] + rho0[L.m(k - 1, j, r)]);
-            const size_t p = L.u(k, j + 3, f + 3);
-            rru[p] = (den * rru[p]) * rgzu[(size_t)j * (ni + 1) + f];
+            const unsigned p = L.u(k, j + 3, f + 3);
+            rru[p] = (den * rru[p]) * rgzu[(unsigned)j * (ni + 1) + f];
         } else {
-            const size_t q = z - nu;
-            const int i = (int)(q % ni), f = (int)((q / ni) % (nj + 1)), k = (int)(q / ((size_t)ni * (nj + 1))) + 1;
+            const unsigned q = z - nu;
+            const int i = (int)(q % ni), f = (int)((q / ni) % (nj + 1)), k = (int)(q / ((unsigned)ni * (nj + 1))) + 1;
             const int s = f == 0 ? 0 : f - 1, nn = f == nj ? nj - 1 : f;
             const float den = 0.5f * (rho0[L.m(k - 1, s, i)] + rho0[L.m(k - 1, nn, i)]);
-            const size_t p = L.v(k, f + 3, i + 3);
-            rrv[p] = (den * rrv[p]) * rgzv[(size_t)f * ni + i];
+            const unsigned p = L.v(k, f + 3, i + 3);
+            rrv[p] = (den * rrv[p]) * rgzv[(unsigned)f * ni + i];
         }
     }
 }
@@ -249,11 +249,11 @@ __global__ void __launch_bounds__(256) msb_getdivx_vertical_kernel(const float *
                                                                   const float *dzdy, const float *gz, const float *rru,
                                                                   const float *rrv, float *rrw, float dz, Lane L) {
     const int ni = L.ni, nj = L.nj, nk = L.nk;
-    const size_t n = (size_t)(nk + 1) * nj * ni;
+    const unsigned n = (unsigned)(nk + 1) * nj * ni;
     const float rds = 1.0f / dz, zt = (float)nk * dz, rzt = 1.0f / zt;
-    for (size_t z = (size_t)blockIdx.x * blockDim.x + threadIdx.x; z < n; z += (size_t)gridDim.x * blockDim.x) {
-        const int i = (int)(z % ni), j = (int)((z / ni) % nj), kf = (int)(z / ((size_t)ni * nj)) + 1;
-        const size_t p = L.s(kf, j + 3, i + 3);
+    for (unsigned z = (unsigned)blockIdx.x * blockDim.x + threadIdx.x; z < n; z += (unsigned)gridDim.x * blockDim.x) {
+        const int i = (int)(z % ni), j = (int)((z / ni) % nj), kf = (int)(z / ((unsigned)ni * nj)) + 1;
+        const unsigned p = L.s(kf, j + 3, i + 3);
         if (kf == 1 || kf == nk + 1) {
             rrw[p] = 0.0f;
             continue;
@@ -266,8 +266,8 @@ __global__ void __launch_bounds__(256) msb_getdivx_vertical_kernel(const float *
                          r1 * (rru[L.u(kf - 1, j + 3, i + 3)] + rru[L.u(kf - 1, j + 3, i + 4)]);
         const float vy = r2 * (rrv[L.v(kf, j + 3, i + 3)] + rrv[L.v(kf, j + 4, i + 3)]) +
                          r1 * (rrv[L.v(kf - 1, j + 3, i + 3)] + rrv[L.v(kf - 1, j + 4, i + 3)]);
-        float terrain = ux * dzdx[(size_t)j * ni + i] + vy * dzdy[(size_t)j * ni + i];
-        terrain = ((terrain * (sf - zt)) * gz[(size_t)j * ni + i]) * rzt;
+        float terrain = ux * dzdx[(unsigned)j * ni + i] + vy * dzdy[(unsigned)j * ni + i];
+        terrain = ((terrain * (sf - zt)) * gz[(unsigned)j * ni + i]) * rzt;
         rrw[p] = rf0[L.m(kf - 1, j, i)] * rrw[p] + terrain;
     }
 }
@@ -275,9 +275,9 @@ __global__ void __launch_bounds__(256) msb_getdivx_vertical_kernel(const float *
 __global__ void __launch_bounds__(256) msb_getdivx_divergence_kernel(const float *rru, const float *rrv,
                                                                     const float *rrw, float *divx, float rdx,
                                                                     float rdy, float rdsf, Lane L) {
-    const size_t n = (size_t)L.nk * L.nj * L.ni;
-    for (size_t z = (size_t)blockIdx.x * blockDim.x + threadIdx.x; z < n; z += (size_t)gridDim.x * blockDim.x) {
-        const int i = (int)(z % L.ni), j = (int)((z / L.ni) % L.nj), k = (int)(z / ((size_t)L.ni * L.nj)) + 1;
+    const unsigned n = (unsigned)L.nk * L.nj * L.ni;
+    for (unsigned z = (unsigned)blockIdx.x * blockDim.x + threadIdx.x; z < n; z += (unsigned)gridDim.x * blockDim.x) {
+        const int i = (int)(z % L.ni), j = (int)((z / L.ni) % L.nj), k = (int)(z / ((unsigned)L.ni * L.nj)) + 1;
         float d = (rru[L.u(k, j + 3, i + 4)] - rru[L.u(k, j + 3, i + 3)]) * rdx +
                   (rrv[L.v(k, j + 4, i + 3)] - rrv[L.v(k, j + 3, i + 3)]) * rdy;
         d = d + (rrw[L.s(k + 1, j + 3, i + 3)] - rrw[L.s(k, j + 3, i + 3)]) * rdsf;
@@ -375,9 +375,9 @@ struct Pdef {
 
 __global__ void __launch_bounds__(256) pdef_horizontal_flux_kernel(Pdef p, Lane L) {
     const int ni = L.ni, nj = L.nj;
-    const size_t n = (size_t)L.nk * (nj + 1) * (ni + 1);
-    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
-        const int i = (int)(q % (ni + 1)), j = (int)((q / (ni + 1)) % (nj + 1)), k = (int)(q / ((size_t)(ni + 1) * (nj + 1))) + 1;
+    const unsigned n = (unsigned)L.nk * (nj + 1) * (ni + 1);
+    for (unsigned q = (unsigned)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (unsigned)gridDim.x * blockDim.x) {
+        const int i = (int)(q % (ni + 1)), j = (int)((q / (ni + 1)) % (nj + 1)), k = (int)(q / ((unsigned)(ni + 1) * (nj + 1))) + 1;
         const int x = i + 3, y = j + 3;
         if (j < nj) {
             const float m = p.rru[L.u(k, y, x)];
@@ -408,13 +408,13 @@ __global__ void __launch_bounds__(256) pdef_horizontal_flux_kernel(Pdef p, Lane 
 
 __global__ void __launch_bounds__(256) pdef_vertical_flux_kernel(Pdef p, Lane L) {
     const int ni = L.ni, nj = L.nj, nk = L.nk;
-    const size_t n = (size_t)(nk - 1) * nj * ni;
+    const unsigned n = (unsigned)(nk - 1) * nj * ni;
     const float ew = (float)p.weps;
-    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
-        const int i = (int)(q % ni), j = (int)((q / ni) % nj), k = (int)(q / ((size_t)ni * nj)) + 2;
+    for (unsigned q = (unsigned)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (unsigned)gridDim.x * blockDim.x) {
+        const int i = (int)(q % ni), j = (int)((q / ni) % nj), k = (int)(q / ((unsigned)ni * nj)) + 2;
         const int x = i + 3, y = j + 3;
         const float m = p.rrw[L.s(k, y, x)];
-        const size_t cm = ((size_t)(k - 1) * nj + j) * ni + i;
+        const unsigned cm = ((unsigned)(k - 1) * nj + j) * ni + i;
         float r;
         if (k == 2) {
             r = m >= 0.0f ? p.c1[cm] * p.s[L.s(k - 1, y, x)] + p.c2[cm] * p.s[L.s(k, y, x)]
@@ -449,9 +449,9 @@ __global__ void __launch_bounds__(256) pdef_vertical_flux_kernel(Pdef p, Lane L)
 
 __global__ void __launch_bounds__(256) pdef_directional_kernel(Pdef p, Lane L) {
     const int ni = L.ni, nj = L.nj, nk = L.nk;
-    const size_t n = (size_t)nk * nj * ni;
-    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
-        const int i = (int)(q % ni), j = (int)((q / ni) % nj), k = (int)(q / ((size_t)ni * nj)) + 1;
+    const unsigned n = (unsigned)nk * nj * ni;
+    for (unsigned q = (unsigned)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (unsigned)gridDim.x * blockDim.x) {
+        const int i = (int)(q % ni), j = (int)((q / ni) % nj), k = (int)(q / ((unsigned)ni * nj)) + 1;
         const int x = i + 3, y = j + 3;
         float fw = p.fx[L.u(k, y, x)], fe = p.fx[L.u(k, y, x + 1)], fs = p.fy[L.v(k, y, x)], fn = p.fy[L.v(k, y + 1, x)];
         const float uw = p.rru[L.u(k, y, x)], ue = p.rru[L.u(k, y, x + 1)];
@@ -480,11 +480,11 @@ __global__ void __launch_bounds__(256) pdef_directional_kernel(Pdef p, Lane L) {
 // axis 0/1/2 = x/y/z candidate: dum = rho0 a + (dt (adv + (s dflux) rspacing)) gz
 __global__ void __launch_bounds__(256) pdef_candidate_kernel(Pdef p, Lane L, int axis) {
     const int ni = L.ni, nj = L.nj, nk = L.nk;
-    const size_t n = (size_t)nk * nj * ni;
+    const unsigned n = (unsigned)nk * nj * ni;
     const float *dir = axis == 0 ? p.ax : axis == 1 ? p.ay : p.az;
     const float rsp = axis == 0 ? p.rdx : axis == 1 ? p.rdy : p.rdz;
-    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
-        const int i = (int)(q % ni), j = (int)((q / ni) % nj), k = (int)(q / ((size_t)ni * nj)) + 1;
+    for (unsigned q = (unsigned)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (unsigned)gridDim.x * blockDim.x) {
+        const int i = (int)(q % ni), j = (int)((q / ni) % nj), k = (int)(q / ((unsigned)ni * nj)) + 1;
         const int x = i + 3, y = j + 3;
         float m0, m1;
         bool inflow = false;
@@ -499,14 +499,14 @@ __global__ void __launch_bounds__(256) pdef_candidate_kernel(Pdef p, Lane L, int
         }
         const float dm = m1 - m0;
         const float r0a = p.rho0[q] * p.a[q];
-        p.dum[q] = inflow ? r0a : r0a + (p.dt * (dir[q] + (p.s[L.s(k, y, x)] * dm) * rsp)) * p.gz[(size_t)j * ni + i];
+        p.dum[q] = inflow ? r0a : r0a + (p.dt * (dir[q] + (p.s[L.s(k, y, x)] * dm) * rsp)) * p.gz[(unsigned)j * ni + i];
     }
 }
 
-__device__ __forceinline__ float zval(const float *d, long long q, int k, size_t slab, int nk) {
+__device__ __forceinline__ float zval(const float *d, long long q, int k, unsigned slab, int nk) {
     return (k < 0 || k >= nk) ? 0.0f : d[q + (long long)k * (long long)slab];
 }
-__device__ __forceinline__ float zratio(const float *d, long long base, int k, size_t slab, int nk) {
+__device__ __forceinline__ float zratio(const float *d, long long base, int k, unsigned slab, int nk) {
     const float c = zval(d, base, k, slab, nk);
     if (c >= 0.0f) return 0.0f;
     const float f1 = fmaxf(0.0f, zval(d, base, k - 1, slab, nk)), f2 = fmaxf(0.0f, zval(d, base, k + 1, slab, nk));
@@ -516,16 +516,16 @@ __device__ __forceinline__ float zratio(const float *d, long long base, int k, s
 
 __global__ void __launch_bounds__(256) pdef_correct_kernel(Pdef p, Lane L, int axis) {
     const int ni = L.ni, nj = L.nj, nk = L.nk;
-    const size_t n = (size_t)nk * nj * ni, slab = (size_t)ni * nj;
+    const unsigned n = (unsigned)nk * nj * ni, slab = (unsigned)ni * nj;
     float *dir = axis == 0 ? p.ax : axis == 1 ? p.ay : p.az;
     const float rsp = axis == 0 ? p.rdx : axis == 1 ? p.rdy : p.rdz;
     const float *d = p.dum;
-    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+    for (unsigned q = (unsigned)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (unsigned)gridDim.x * blockDim.x) {
         const int i = (int)(q % ni), j = (int)((q / ni) % nj), k0 = (int)(q / slab);
         float mass = 0.0f;
         bool flag = false;
         if (axis == 2) {
-            const long long base = (long long)(q - (size_t)k0 * slab);
+            const long long base = (long long)(q - (unsigned)k0 * slab);
             const float cur = d[q];
             if (cur < 0.0f) {
                 const float r = zratio(d, base, k0, slab, nk);
@@ -565,7 +565,7 @@ __global__ void __launch_bounds__(256) pdef_correct_kernel(Pdef p, Lane L, int a
         }
         if (flag) {
             const int k = k0 + 1, x = i + 3, y = j + 3;
-            const float first = (((d[q] + mass) - p.rho0[q] * p.a[q]) * p.rdt) * p.rgz[(size_t)j * ni + i];
+            const float first = (((d[q] + mass) - p.rho0[q] * p.a[q]) * p.rdt) * p.rgz[(unsigned)j * ni + i];
             float dm;
             if (axis == 0) dm = p.rru[L.u(k, y, x + 1)] - p.rru[L.u(k, y, x)];
             else if (axis == 1) dm = p.rrv[L.v(k, y + 1, x)] - p.rrv[L.v(k, y, x)];
@@ -577,13 +577,13 @@ __global__ void __launch_bounds__(256) pdef_correct_kernel(Pdef p, Lane L, int a
 
 __global__ void __launch_bounds__(256) pdef_total_kernel(Pdef p, Lane L) {
     const int ni = L.ni, nj = L.nj;
-    const size_t n = (size_t)L.nk * nj * ni;
-    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
-        const int i = (int)(q % ni), j = (int)((q / ni) % nj), k = (int)(q / ((size_t)ni * nj)) + 1;
+    const unsigned n = (unsigned)L.nk * nj * ni;
+    for (unsigned q = (unsigned)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (unsigned)gridDim.x * blockDim.x) {
+        const int i = (int)(q % ni), j = (int)((q / ni) % nj), k = (int)(q / ((unsigned)ni * nj)) + 1;
         if (!obc_owned(i, j, ni, nj, p.obc)) continue;
         float t = (p.ax[q] + p.ay[q]) + p.az[q];
         t = t + p.s[L.s(k, j + 3, i + 3)] * p.divx[q];
-        p.adv[q] = (t * p.rr0[q]) * p.gz[(size_t)j * ni + i];
+        p.adv[q] = (t * p.rr0[q]) * p.gz[(unsigned)j * ni + i];
     }
 }
 
@@ -596,12 +596,12 @@ struct Held {
 };
 
 __global__ void __launch_bounds__(256) held_compose_kernel(Held h, int ni, int nj, int nk, float dt) {
-    const size_t n = (size_t)ni * nj * nk;
+    const unsigned n = (unsigned)ni * nj * nk;
     const float rd = 287.04f, rv = 461.5f, rp00 = 1.0f / 100000.0f, rddcv = 287.04f / (1005.7f - 287.04f);
     const float tem = 0.0001f * 0.0001f, qsmall = 1.0e-14f;
-    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
-        const int i = (int)(q % ni), j = (int)((q / ni) % nj), k = (int)(q / ((size_t)ni * nj));
-        const size_t pp = ((size_t)(k + 1) * (nj + 2) + (j + 1)) * (size_t)(ni + 2) + (i + 1);
+    for (unsigned q = (unsigned)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (unsigned)gridDim.x * blockDim.x) {
+        const int i = (int)(q % ni), j = (int)((q / ni) % nj), k = (int)(q / ((unsigned)ni * nj));
+        const unsigned pp = ((unsigned)(k + 1) * (nj + 2) + (j + 1)) * (unsigned)(ni + 2) + (i + 1);
         const float ht = h.thheld[q], qvt = h.qheld[q];
         if (fabsf(dt * ht) > tem || fabsf(dt * qvt) > qsmall) {
             const float thnew = h.tha[q] + dt * ht, qvnew = h.qa[q] + dt * qvt;
@@ -620,23 +620,23 @@ __global__ void __launch_bounds__(256) held_compose_kernel(Held h, int ni, int n
 
 __global__ void __launch_bounds__(256) solve3_density_kernel(const float *rho, const float *c1, const float *c2,
                                                             float *rr, float *rf, int ni, int nj, int nk) {
-    const size_t n = (size_t)ni * nj * nk, nf = (size_t)ni * nj * (nk + 1), plane = (size_t)ni * nj;
-    for (size_t z = (size_t)blockIdx.x * blockDim.x + threadIdx.x; z < nf; z += (size_t)gridDim.x * blockDim.x) {
+    const unsigned n = (unsigned)ni * nj * nk, nf = (unsigned)ni * nj * (nk + 1), plane = (unsigned)ni * nj;
+    for (unsigned z = (unsigned)blockIdx.x * blockDim.x + threadIdx.x; z < nf; z += (unsigned)gridDim.x * blockDim.x) {
         if (z < n) rr[z] = 1.0f / rho[z];
-        const size_t h = z % plane;
+        const unsigned h = z % plane;
         const int f = (int)(z / plane);
         if (f == 0) rf[z] = (1.875f * rho[h] + (-1.25f) * rho[plane + h]) + 0.375f * rho[2 * plane + h];
         else if (f == nk)
-            rf[z] = (1.875f * rho[(size_t)(nk - 1) * plane + h] + (-1.25f) * rho[(size_t)(nk - 2) * plane + h]) +
-                    0.375f * rho[(size_t)(nk - 3) * plane + h];
-        else rf[z] = c1[z] * rho[(size_t)(f - 1) * plane + h] + c2[z] * rho[(size_t)f * plane + h];
+            rf[z] = (1.875f * rho[(unsigned)(nk - 1) * plane + h] + (-1.25f) * rho[(unsigned)(nk - 2) * plane + h]) +
+                    0.375f * rho[(unsigned)(nk - 3) * plane + h];
+        else rf[z] = c1[z] * rho[(unsigned)(f - 1) * plane + h] + c2[z] * rho[(unsigned)f * plane + h];
     }
 }
 
 __global__ void __launch_bounds__(256) pack_scalar_kernel(const float *s, float *padded, Lane L) {
-    const size_t n = (size_t)L.nk * L.nj * L.ni;
-    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
-        const int i = (int)(q % L.ni), j = (int)((q / L.ni) % L.nj), k = (int)(q / ((size_t)L.ni * L.nj)) + 1;
+    const unsigned n = (unsigned)L.nk * L.nj * L.ni;
+    for (unsigned q = (unsigned)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (unsigned)gridDim.x * blockDim.x) {
+        const int i = (int)(q % L.ni), j = (int)((q / L.ni) % L.nj), k = (int)(q / ((unsigned)L.ni * L.nj)) + 1;
         padded[L.s(k, j + 3, i + 3)] = s[q];
     }
 }
@@ -644,8 +644,8 @@ __global__ void __launch_bounds__(256) pack_scalar_kernel(const float *s, float 
 // bc.F:1151-1178 on the physical bottom faces (cpu_bcwsfc_terrain_physical_inplace)
 __global__ void __launch_bounds__(256) bcwsfc_kernel(const float *u, const float *v, float *w, const float *gz,
                                                     const float *dzdx, const float *dzdy, Lane L) {
-    const size_t n = (size_t)L.nj * L.ni;
-    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+    const unsigned n = (unsigned)L.nj * L.ni;
+    for (unsigned q = (unsigned)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (unsigned)gridDim.x * blockDim.x) {
         const int i0 = (int)(q % L.ni), j0 = (int)(q / L.ni), y = j0 + 3, x = i0 + 3;
         const float ut = (u[L.u(1, y, x)] + u[L.u(1, y, x + 1)]) * dzdx[q];
         const float vt = (v[L.v(1, y, x)] + v[L.v(1, y + 1, x)]) * dzdy[q];
@@ -657,17 +657,17 @@ __global__ void __launch_bounds__(256) bcwsfc_kernel(const float *u, const float
 // over every row (pass 0), then south and north over every column (pass 1)
 __global__ void __launch_bounds__(256) w_level1_fill_kernel(float *w, Lane L, int pass) {
     const int nx = L.ni + 6, ny = L.nj + 6;
-    const size_t n = pass == 0 ? (size_t)ny * 6 : (size_t)nx * 6;
-    float *s = w + (size_t)1 * nx * ny;
-    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+    const unsigned n = pass == 0 ? (unsigned)ny * 6 : (unsigned)nx * 6;
+    float *s = w + (unsigned)1 * nx * ny;
+    for (unsigned q = (unsigned)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (unsigned)gridDim.x * blockDim.x) {
         if (pass == 0) {
             const int y = (int)(q / 6), h = (int)(q % 6);
             const int x = h < 3 ? h : 3 + L.ni + (h - 3), sx = h < 3 ? 3 : 3 + L.ni - 1;
-            s[(size_t)y * nx + x] = s[(size_t)y * nx + sx];
+            s[(unsigned)y * nx + x] = s[(unsigned)y * nx + sx];
         } else {
             const int x = (int)(q % nx), h = (int)(q / nx);
             const int y = h < 3 ? h : 3 + L.nj + (h - 3), sy = h < 3 ? 3 : 3 + L.nj - 1;
-            s[(size_t)y * nx + x] = s[(size_t)sy * nx + x];
+            s[(unsigned)y * nx + x] = s[(unsigned)sy * nx + x];
         }
     }
 }
@@ -681,6 +681,12 @@ namespace {
 bool grid_ok(int ni, int nj, int nk, int mi, int mj, int mk, const char *what) {
     if (ni < mi || nj < mj || nk < mk) {
         gm1b_set_error("%s: need ni >= %d, nj >= %d, nk >= %d", what, mi, mj, mk);
+        return false;
+    }
+    // the kernels index and count with 32-bit words
+    if ((size_t)(nk + 3) * (size_t)(nj + 7) * (size_t)(ni + 7) * 2 >= ((size_t)1 << 31)) {
+        gm1b_set_error("%s: a %dx%dx%d grid's padded arrays reach 2^30 words; the kernels index with 32-bit offsets",
+                       what, ni, nj, nk);
         return false;
     }
     return true;

@@ -37,15 +37,17 @@ struct TkeArgs {
 };
 
 __device__ __forceinline__ int clampi(int x, int n) { return x < 0 ? 0 : (x >= n ? n - 1 : x); }
-__device__ __forceinline__ size_t f3(const TkeArgs &a, int k, int j, int i) {
-    return ((size_t)k * a.nj + (size_t)j) * (size_t)a.ni + (size_t)i;
+// 32-bit element offsets (the entry points refuse grids whose padded arrays
+// reach 2^31 words)
+__device__ __forceinline__ unsigned f3(const TkeArgs &a, int k, int j, int i) {
+    return ((unsigned)k * (unsigned)a.nj + (unsigned)j) * (unsigned)a.ni + (unsigned)i;
 }
 // value at a clamped column (constant extension beyond the open sides)
 __device__ __forceinline__ float cellc(const TkeArgs &a, const float *p, int k, int j, int i) {
     return p[f3(a, k, clampi(j, a.nj), clampi(i, a.ni))];
 }
 __device__ __forceinline__ float g2c(const TkeArgs &a, const float *p, int j, int i) {
-    return p[(size_t)clampi(j, a.nj) * a.ni + clampi(i, a.ni)];
+    return p[(unsigned)clampi(j, a.nj) * (unsigned)a.ni + (unsigned)clampi(i, a.ni)];
 }
 __device__ __forceinline__ float tsm(const TkeArgs &a, int m, int j, int i) {
     return 0.5f * (cellc(a, a.t, m, j, i) + cellc(a, a.t, m + 1, j, i));
@@ -91,14 +93,14 @@ __global__ void __launch_bounds__(kTT) tke_turbt_kernel(TkeArgs a, float dt) {
     const int ni = a.ni, nj = a.nj, nk = a.nk, n = nk - 1;
     const bool own = i < ni && j < nj;
     float *cp = s_col, *dp = s_col + (size_t)n * kTT;
-#define CP(p) cp[(size_t)(p) * kTT + tid]
-#define DP(p) dp[(size_t)(p) * kTT + tid]
+#define CP(p) cp[(unsigned)(p) * kTT + tid]
+#define DP(p) dp[(unsigned)(p) * kTT + tid]
     const float rdt = 1.0f / dt;
     // ---- vertically implicit diffusion of the own column -------------------
     if (own) {
         const float tema = -1.0f * (dt * (a.rdz * a.rdz));
         int f = 1;
-        size_t z = f3(a, f, j, i);
+        unsigned z = f3(a, f, j, i);
         float rrf = a.mf[z] / a.rf[z];
         float r2 = (a.kmv[z] + a.kmv[f3(a, f + 1, j, i)]) * (a.mh[f3(a, f, j, i)] * (a.rho[f3(a, f, j, i)] * rrf));
         float cfc = tema * r2, cfb = 1.0f - cfc, inv = 1.0f / cfb;
@@ -179,7 +181,7 @@ __global__ void __launch_bounds__(kTT) tke_turbt_kernel(TkeArgs a, float dt) {
             y = y - 0.5f * ((up - lo) * (a.rdz * ((rv1 - rv0) * (gzji * a.rdy))));
             const float hx = (i == 0 || i == ni - 1) ? 0.0f : x;
             const float hy = (j == 0 || j == nj - 1) ? 0.0f : y;
-            const size_t z = f3(a, f, j, i);
+            const unsigned z = f3(a, f, j, i);
             const float rfz = a.rf[z];
             const float vz = rfz * ((DP(f - 1) - a.t[z]) * rdt);
             a.tketen[z] = a.tketen[z] + ((hx + hy) + vz) / rfz;
@@ -192,13 +194,16 @@ __global__ void __launch_bounds__(kTT) tke_turbt_kernel(TkeArgs a, float dt) {
 
 // ------------------------------------------------------------- RK stage
 __device__ __forceinline__ float rru_at(const TkeArgs &a, int k, int j, int f) {
-    return a.rru[((size_t)k * (a.nj + 2 * kG) + (size_t)(j + kG)) * (size_t)(a.ni + 1 + 2 * kG) + (size_t)(f + kG)];
+    return a.rru[((unsigned)k * (unsigned)(a.nj + 2 * kG) + (unsigned)(j + kG)) * (unsigned)(a.ni + 1 + 2 * kG) +
+                 (unsigned)(f + kG)];
 }
 __device__ __forceinline__ float rrv_at(const TkeArgs &a, int k, int f, int i) {
-    return a.rrv[((size_t)k * (a.nj + 1 + 2 * kG) + (size_t)(f + kG)) * (size_t)(a.ni + 2 * kG) + (size_t)(i + kG)];
+    return a.rrv[((unsigned)k * (unsigned)(a.nj + 1 + 2 * kG) + (unsigned)(f + kG)) * (unsigned)(a.ni + 2 * kG) +
+                 (unsigned)(i + kG)];
 }
 __device__ __forceinline__ float rrw_at(const TkeArgs &a, int k, int j, int i) {
-    return a.rrw[((size_t)k * (a.nj + 2 * kG) + (size_t)(j + kG)) * (size_t)(a.ni + 2 * kG) + (size_t)(i + kG)];
+    return a.rrw[((unsigned)k * (unsigned)(a.nj + 2 * kG) + (unsigned)(j + kG)) * (unsigned)(a.ni + 2 * kG) +
+                 (unsigned)(i + kG)];
 }
 
 // mass flux through x face `face` of row j (axis 0) or y face `face` of
@@ -289,7 +294,7 @@ __global__ void __launch_bounds__(128) tke_rk_stage_kernel(TkeArgs a, const floa
     const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 4 + threadIdx.y, f = blockIdx.z;
     const int ni = a.ni, nj = a.nj, nk = a.nk;
     if (i >= ni || j >= nj) return;
-    const size_t z = f3(a, f, j, i);
+    const unsigned z = f3(a, f, j, i);
     if (f == 0 || f == nk) {
         nxt[z] = 0.0f;
         if (nxt2) nxt2[z] = 0.0f;
@@ -345,6 +350,11 @@ int tke_args(int ni, int nj, int nk, const gm1b_tke_evolution_arrays *s, float d
              TkeArgs &a, const char *what) {
     if (s == nullptr || ni < 3 || nj < 3 || nk < 6) {
         gm1b_set_error("%s: need arrays, ni >= 3, nj >= 3, nk >= 6", what);
+        return GM1B_ERR_ARGUMENT;
+    }
+    if ((size_t)(nk + 3) * (size_t)(nj + 7) * (size_t)(ni + 7) >= ((size_t)1 << 31)) {
+        gm1b_set_error("%s: a %dx%dx%d grid's padded arrays reach 2^31 words; the kernels index with 32-bit offsets",
+                       what, ni, nj, nk);
         return GM1B_ERR_ARGUMENT;
     }
     const float v[4] = {dx, dy, dz, dt};
