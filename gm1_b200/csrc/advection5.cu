@@ -583,10 +583,14 @@ extern "C" int32_t gm1b_scalar_advection5(int32_t ni, int32_t nj, int32_t nk,
             return GM1B_ERR_ARGUMENT;
         }
     }
-    int chunk = levels_per_chunk > 0 ? levels_per_chunk : 16;
+    const bool weno = wflag != 0 && nrk == 3;
+    // default level chunk per CTA (measured at 256x256x80 on B200): short
+    // chunks give the fifth-order pass more CTAs to overlap its per-level
+    // staging (4 levels: 0.154 ms, 16: 0.191 ms); the WENO pass is bound by its
+    // binary64 weights and is flat between 4 and 16
+    int chunk = levels_per_chunk > 0 ? levels_per_chunk : (weno ? 16 : 4);
     if (chunk > nk) chunk = nk;
     const PaddedDims d{ni, nj, nk};
-    const bool weno = wflag != 0 && nrk == 3;
     const dim3 grid((ni + kTX5 - 1) / kTX5, (nj + kTY5 - 1) / kTY5, (nk + chunk - 1) / chunk);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const float rdx = 1.0f / dx, rdy = 1.0f / dy, rdsf = 1.0f / dz;

@@ -390,15 +390,31 @@ __global__ void __launch_bounds__(kLevelThreads) kessler_levels_kernel(KDims d, 
 __global__ void kessler_finish_kernel(gm1b_kessler_arrays a, KDims d, KWork w, double volume, double dxd,
                                       double dyd, double area) {
     if (blockIdx.x != 0 || threadIdx.x != 0) return;
-    for (int s = 0; s < 3; ++s)
-        for (int j = 0; j < d.nj; ++j) a.asq[s] += w.rows[(size_t)s * d.nj + j] * volume;
-    for (int j = 0; j < d.nj; ++j) a.qbudget[6] += w.rows[(size_t)3 * d.nj + j] * dxd * dyd;
-    for (int j = 0; j < d.nj; ++j) a.qbudget[5] += w.rows[(size_t)4 * d.nj + j] * area;
+    // Each budget accumulates in a register in the same order as a running
+    // sum in memory would, and is stored once: the row and level totals are
+    // then independent loads that can all be in flight together.
+    const double *rows = w.rows;
+    for (int s = 0; s < 3; ++s) {
+        double acc = a.asq[s];
+        for (int j = 0; j < d.nj; ++j) acc += rows[(size_t)s * d.nj + j] * volume;
+        a.asq[s] = acc;
+    }
+    double q6 = a.qbudget[6], q5 = a.qbudget[5];
+    for (int j = 0; j < d.nj; ++j) q6 += rows[(size_t)3 * d.nj + j] * dxd * dyd;
+    for (int j = 0; j < d.nj; ++j) q5 += rows[(size_t)4 * d.nj + j] * area;
+    a.qbudget[6] = q6;
+    a.qbudget[5] = q5;
     const size_t n = (size_t)d.nj * w.nbx, plane = (size_t)d.nk * n;
-    for (int p = 0; p < 3; ++p)
-        for (int k = 0; k < d.nk; ++k) a.qbudget[2 + p] = a.qbudget[2 + p] + w.partial[p * plane + (size_t)k * n] * volume;
-    for (int p = 3; p < 5; ++p)
-        for (int k = 0; k < d.nk; ++k) a.qbudget[p - 3] += w.partial[p * plane + (size_t)k * n] * volume;
+    for (int p = 0; p < 3; ++p) {
+        double acc = a.qbudget[2 + p];
+        for (int k = 0; k < d.nk; ++k) acc = acc + w.partial[p * plane + (size_t)k * n] * volume;
+        a.qbudget[2 + p] = acc;
+    }
+    for (int p = 3; p < 5; ++p) {
+        double acc = a.qbudget[p - 3];
+        for (int k = 0; k < d.nk; ++k) acc += w.partial[p * plane + (size_t)k * n] * volume;
+        a.qbudget[p - 3] = acc;
+    }
 }
 
 bool launched(const char *what) {

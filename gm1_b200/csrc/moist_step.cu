@@ -138,16 +138,21 @@ struct Lane {
 };
 
 // dum8 on w levels: c1(kf) dum8(kf-1) + c2(kf) dum8(kf), zero at the ends
-__device__ __forceinline__ float buoy_face(const float *dum8, const float *c1, const float *c2, const Lane &L, int kf,
-                                           int j, int i) {
+__device__ __forceinline__ float buoy_face(const float *__restrict__ dum8, const float *__restrict__ c1,
+                                           const float *__restrict__ c2, const Lane &L, int kf, int j, int i) {
     if (kf == 1 || kf == L.nk + 1) return 0.0f;
     const unsigned p = L.m(kf - 1, j, i);
     return c1[p] * dum8[L.s(kf - 1, j + 3, i + 3)] + c2[p] * dum8[L.s(kf, j + 3, i + 3)];
 }
 
-__global__ void __launch_bounds__(256) msb_buoyancy_kernel(const float *dum8, const float *c1, const float *c2,
-                                                          const float *gxu, const float *gyv, float *uten,
-                                                          float *vten, float *wten, Lane L) {
+// inputs and the three tendencies are distinct arrays (the entry point
+// refuses a call that passes one array twice), so every load may be issued
+// ahead of the stores
+__global__ void __launch_bounds__(256) msb_buoyancy_kernel(const float *__restrict__ dum8,
+                                                          const float *__restrict__ c1, const float *__restrict__ c2,
+                                                          const float *__restrict__ gxu,
+                                                          const float *__restrict__ gyv, float *__restrict__ uten,
+                                                          float *__restrict__ vten, float *__restrict__ wten, Lane L) {
     const int ni = L.ni, nj = L.nj, nk = L.nk;
     const unsigned nw = (unsigned)(nk - 1) * nj * ni, nu = (unsigned)nk * nj * (ni - 1), nv = (unsigned)nk * (nj - 1) * ni;
     for (unsigned z = (unsigned)blockIdx.x * blockDim.x + threadIdx.x; z < nw + nu + nv; z += (unsigned)gridDim.x * blockDim.x) {
@@ -721,6 +726,13 @@ extern "C" int32_t gm1b_moist_buoyancy(int32_t ni, int32_t nj, int32_t nk, const
             gm1b_set_error("gm1b_moist_buoyancy: NULL array");
         return GM1B_ERR_ARGUMENT;
     }
+    const void *all[8] = {dum8, c1, c2, gxu, gyv, uten, vten, wten};
+    for (int x = 0; x < 8; ++x)
+        for (int y = x + 1; y < 8; ++y)
+            if (all[x] == all[y]) {
+                gm1b_set_error("gm1b_moist_buoyancy: the eight arrays must be distinct");
+                return GM1B_ERR_ARGUMENT;
+            }
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const Lane L{ni, nj, nk};
     const size_t work = (size_t)(nk - 1) * nj * ni + (size_t)nk * nj * (ni - 1) + (size_t)nk * (nj - 1) * ni;
