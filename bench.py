@@ -378,7 +378,10 @@ def run_moist(args) -> None:
     value = world * cells * args.steps / (total_ms * 1e-3)
 
     # ---- per-kernel device time (eager steps, launch profiler on) -------
+    # run operation by operation on one stream: the profiler's event pairs
+    # time each launch alone only when launches do not overlap
     nprof = min(args.steps, 5)
+    model.concurrent = False
     _native.profiler_enable(True)
     with torch.cuda.stream(stream):
         for _ in range(nprof):
@@ -386,6 +389,7 @@ def run_moist(args) -> None:
             model.step()
     stream.synchronize()
     _native.profiler_enable(False)
+    model.concurrent = True
     stats = _native.profiler_collect()
     launches_per_step = sum(s["launches"] for s in stats) / nprof
     top = stats[0]
@@ -539,9 +543,10 @@ def run_ensemble(args) -> None:
     value = total_cells * args.steps / (b_ms * 1e-3)
     plain_value = total_cells * args.steps / (p_ms * 1e-3)
 
-    # per-kernel device time of one eager batched step (launch profiler)
+    # per-kernel device time of one plain step (launch profiler; the plain
+    # ensemble launches one kernel at a time, so each event pair times one)
     _native.profiler_enable(True)
-    batched.step_eager()
+    plain.step_eager()
     torch.cuda.synchronize(device)
     _native.profiler_enable(False)
     stats = _native.profiler_collect()

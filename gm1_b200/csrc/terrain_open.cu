@@ -38,10 +38,10 @@ namespace {
 
 constexpr int kTosWarps = 8;     // k-parallel warps of the column pass
 constexpr int kTosMaxNk = 160;   // column pass keeps 10 words per level per column in shared memory
-constexpr int kTosArrays = 10;
+constexpr int kTosArrays = 7;
 constexpr int kPgLevels = 4;     // levels whose loads the pressure-gradient march issues together
 constexpr int kA2Levels = 2;     // levels per warp whose column-pass loads are issued together (phase A2)
-constexpr int kColLevels = 4;    // the same for phases A3 and C
+constexpr int kColLevels = 2;    // the same for phases A3 and C
 constexpr int kThomasChunk = 8;  // back-substitution levels whose coefficients are read together
 
 struct TosArgs {
@@ -329,10 +329,11 @@ __global__ void __launch_bounds__(128) tos_pgrad_kernel(TosArgs p) {
 
 // ---------------------------------------------------------------------------
 // column pass of one small step.  CTA = 32 consecutive columns of row j,
-// kTosWarps warps sharing the levels; two CTAs per SM so that one's serial
-// Thomas sweep overlaps the other's loads.  Shared memory holds, per level
+// kTosWarps warps sharing the levels; three CTAs per SM so that one's serial
+// Thomas sweep overlaps the others' loads.  Shared memory holds, per level
 // and column: the four transformed face velocities (later aa, bb, cc/ec,
-// dd), w, fpk, pk1+qk, pk2-qk, pp3d and the eliminated right-hand side ed.
+// dd), w, fpk and the eliminated right-hand side ed; pk1+qk, pk2-qk and
+// pp3d are re-read from global memory (L2-resident) where they are used.
 // dum3 and hadvp are formed where they are used (levels k and k+1), with
 // the same operations as the twin; read-only fields take the non-coherent
 // path so the unrolled level loops keep several levels' loads in flight.
@@ -340,10 +341,10 @@ __global__ void __launch_bounds__(128) tos_pgrad_kernel(TosArgs p) {
 // global words one level of phase A2 reads (zero where the level or the
 // pi' advection does not use them)
 struct A2Load {
-    float rk, rl, rk1, rrf_k, rrf_k1, qk, pk1, pk2, ppten, ppterm, pp, pc, pe, pw, pn, ps, rr0;
+    float rk, rl, rk1, rrf_k, rrf_k1, qk, pk1, pk2, ppten, ppterm, pc, pe, pw, pn, ps, rr0;
     __device__ __forceinline__ void load(const gm1b_terrain_open_arrays &a, const gm1b_terrain_metrics &m,
                                          const Ix &X, int k, int nk, int j, int i, bool adv) {
-        rk = rl = rk1 = rrf_k = rrf_k1 = qk = pk1 = pk2 = ppten = ppterm = pp = 0.0f;
+        rk = rl = rk1 = rrf_k = rrf_k1 = qk = pk1 = pk2 = ppten = ppterm = 0.0f;
         pc = pe = pw = pn = ps = rr0 = 0.0f;
         if (k > nk) return;
         const int j0 = j - 1, i0 = i - 1;
@@ -366,7 +367,6 @@ struct A2Load {
         pk2 = __ldg(a.pk2 + c);
         ppten = __ldg(a.ppten + c);
         ppterm = __ldg(a.ppterm + c);
-        pp = a.pp3d[c];
     }
 };
 
@@ -397,7 +397,7 @@ __device__ __forceinline__ void tos_level_terms(const float *s_xw, const float *
     }
 }
 
-__global__ void __launch_bounds__(32 * kTosWarps, 2) tos_column_kernel(TosArgs p) {
+__global__ void __launch_bounds__(32 * kTosWarps, 3) tos_column_kernel(TosArgs p) {
     extern __shared__ float sh[];
     const Ix X{p.ni, p.nj};
     const int ni = p.ni, nj = p.nj, nk = p.nk, L = nk + 2;
@@ -414,8 +414,7 @@ __global__ void __launch_bounds__(32 * kTosWarps, 2) tos_column_kernel(TosArgs p
     const bool do_adv = p.abl & GM1B_TOS_PRESSURE_ADVECTION;
     const bool do_imp = p.abl & GM1B_TOS_IMPLICIT_SOLVE;
     float *s_xw = sh, *s_xe = s_xw + L * 32, *s_ys = s_xe + L * 32, *s_yn = s_ys + L * 32;
-    float *s_w = s_yn + L * 32, *s_fpk = s_w + L * 32, *s_a1 = s_fpk + L * 32, *s_a2 = s_a1 + L * 32;
-    float *s_pp = s_a2 + L * 32, *s_ed = s_pp + L * 32;
+    float *s_w = s_yn + L * 32, *s_fpk = s_w + L * 32, *s_ed = s_fpk + L * 32;
     float *s_aa = s_xw, *s_bb = s_xe, *s_cc = s_ys, *s_dd = s_yn;
 #define SM(arr, k) arr[(k) * 32 + lane]
     float gz = 0.0f, dzdx = 0.0f, dzdy = 0.0f;
@@ -469,7 +468,6 @@ __global__ void __launch_bounds__(32 * kTosWarps, 2) tos_column_kernel(TosArgs p
             const float rk = ld[q].rk, rl = ld[q].rl, rk1 = ld[q].rk1, rrf_k = ld[q].rrf_k, rrf_k1 = ld[q].rrf_k1;
             const float qk = ld[q].qk, pk1 = ld[q].pk1, pk2 = ld[q].pk2;
             const float ppten = ld[q].ppten, ppterm = ld[q].ppterm;
-            const float pp = ld[q].pp;
             const float pc = ld[q].pc, pe = ld[q].pe, pw = ld[q].pw, pn = ld[q].pn, ps = ld[q].ps, rr0 = ld[q].rr0;
             float d3k = 0.0f, d3k1 = 0.0f, hak = 0.0f, hak1 = 0.0f;
             if (k >= 2) tos_level_terms(s_xw, s_xe, s_ys, s_yn, lane, k, p, dzdx, dzdy, gz, rk, rl, rrf_k, do_adv, d3k, hak);
@@ -507,19 +505,31 @@ __global__ void __launch_bounds__(32 * kTosWarps, 2) tos_column_kernel(TosArgs p
             }
             if (dlast) a.fpk[c] = fpk;
             SM(s_fpk, k) = fpk;
-            SM(s_a1, k) = pk1 + qk;
-            SM(s_a2, k) = pk2 - qk;
-            SM(s_pp, k) = pp;
             }
         }
     }
-    float lmm[kColLevels], lwt[kColLevels];
+    // A3 reads pk1 + qk, pk2 - qk and pp3d of levels k and k-1 again from
+    // global memory (L2-resident after A2) instead of keeping them in shared
+    // memory: seven shared words per level let three CTAs share an SM
+    float lmm[kColLevels], lwt[kColLevels], lq[kColLevels], lp1[kColLevels], lp2[kColLevels], lpp[kColLevels];
+    float lqm[kColLevels], lp1m[kColLevels], lp2m[kColLevels], lppm[kColLevels];
     auto a3_loads = [&](int kb) {
 #pragma unroll
         for (int q = 0; q < kColLevels; ++q) {
             const int k = kb + q * kTosWarps;
-            lmm[q] = k <= nk ? __ldg(a.mm + X.p(k, j, i)) : 0.0f;
-            lwt[q] = k <= nk ? __ldg(a.wten + X.w(k, y, x)) : 0.0f;
+            lmm[q] = lwt[q] = lq[q] = lp1[q] = lp2[q] = lpp[q] = lqm[q] = lp1m[q] = lp2m[q] = lppm[q] = 0.0f;
+            if (k > nk) continue;
+            const unsigned c = X.p(k, j, i), cm = X.p(k - 1, j, i);
+            lmm[q] = __ldg(a.mm + c);
+            lwt[q] = __ldg(a.wten + X.w(k, y, x));
+            lq[q] = __ldg(a.qk + c);
+            lp1[q] = __ldg(a.pk1 + c);
+            lp2[q] = __ldg(a.pk2 + c);
+            lpp[q] = a.pp3d[c];
+            lqm[q] = __ldg(a.qk + cm);
+            lp1m[q] = __ldg(a.pk1 + cm);
+            lp2m[q] = __ldg(a.pk2 + cm);
+            lppm[q] = a.pp3d[cm];
         }
     };
     if (live && do_imp) a3_loads(2 + wy);
@@ -535,13 +545,15 @@ __global__ void __launch_bounds__(32 * kTosWarps, 2) tos_column_kernel(TosArgs p
             const unsigned c = X.p(k, j, i);
             const float mmk = lmm[q];
             const float wt = lwt[q];
-            const float aa = k >= 3 ? (-p.asq) * (mmk * SM(s_a1, k - 1)) : 0.0f;
-            const float cc = k < nk ? (-p.asq) * ((-mmk) * SM(s_a2, k)) : 0.0f;
-            const float dg = (-SM(s_a1, k)) + SM(s_a2, k - 1);
+            const float a1k = lp1[q] + lq[q], a2k = lp2[q] - lq[q];
+            const float a1m = lp1m[q] + lqm[q], a2m = lp2m[q] - lqm[q];
+            const float aa = k >= 3 ? (-p.asq) * (mmk * a1m) : 0.0f;
+            const float cc = k < nk ? (-p.asq) * ((-mmk) * a2k) : 0.0f;
+            const float dg = (-a1k) + a2m;
             const float bb = 1.0f - p.asq * (mmk * dg);
-            const float pd = SM(s_pp, k) - SM(s_pp, k - 1);
+            const float pd = lpp[q] - lppm[q];
             const float fwk = p.dts * wt + p.beta * ((-mmk) * pd);
-            const float ud = (SM(s_pp, k) + SM(s_fpk, k)) - (SM(s_pp, k - 1) + SM(s_fpk, k - 1));
+            const float ud = (lpp[q] + SM(s_fpk, k)) - (lppm[q] + SM(s_fpk, k - 1));
             const float dd = (SM(s_w, k) + fwk) + p.alph * ((-mmk) * ud);
             SM(s_aa, k) = aa;
             SM(s_bb, k) = bb;
@@ -557,19 +569,25 @@ __global__ void __launch_bounds__(32 * kTosWarps, 2) tos_column_kernel(TosArgs p
         }
     }
     // phase C's first chunk, in flight while warp 0 runs the Thomas sweep
+    // (pp3d of level k is read here before this thread writes it in C)
     float luu[kColLevels], lvv[kColLevels], lru[kColLevels], lrv[kColLevels], lrw[kColLevels];
+    float cpp[kColLevels], ca1[kColLevels], ca2[kColLevels];
     auto c_loads = [&](int kb) {
 #pragma unroll
         for (int q = 0; q < kColLevels; ++q) {
             const int k = kb + q * kTosWarps;
-            luu[q] = lvv[q] = lru[q] = lrv[q] = lrw[q] = 0.0f;
+            luu[q] = lvv[q] = lru[q] = lrv[q] = lrw[q] = cpp[q] = ca1[q] = ca2[q] = 0.0f;
             if (k > nk) continue;
-            const unsigned qu = X.u(k, y, x), qv = X.v(k, y, x), qw = X.w(k, y, x);
+            const unsigned qu = X.u(k, y, x), qv = X.v(k, y, x), qw = X.w(k, y, x), c = X.p(k, j, i);
             luu[q] = __ldg(a.u3d + qu);
             lvv[q] = __ldg(a.v3d + qv);
             lru[q] = a.rru[qu];
             lrv[q] = a.rrv[qv];
             lrw[q] = a.rrw[qw];
+            cpp[q] = a.pp3d[c];
+            const float qk = __ldg(a.qk + c);
+            ca1[q] = __ldg(a.pk1 + c) + qk;
+            ca2[q] = __ldg(a.pk2 + c) - qk;
         }
     };
     if (live) c_loads(1 + wy);
@@ -646,14 +664,14 @@ __global__ void __launch_bounds__(32 * kTosWarps, 2) tos_column_kernel(TosArgs p
                 a.w3d[qw] = wk;
                 if (dlast) {
                     float lhs = SM(s_aa, k) * SM(s_w, k - 1) + SM(s_bb, k) * wk;
-                    const float cc = k < nk ? (-p.asq) * ((-__ldg(a.mm + c)) * SM(s_a2, k)) : 0.0f;
+                    const float cc = k < nk ? (-p.asq) * ((-__ldg(a.mm + c)) * ca2[q]) : 0.0f;
                     lhs = lhs + cc * wk1;
                     a.tri_residual[c] = lhs - SM(s_dd, k);
                 }
             }
             const float w1 = k == 1 ? 0.0f : wk, w2 = k == nk ? 0.0f : wk1;
-            const float old = SM(s_pp, k);
-            const float vt = w1 * SM(s_a1, k) + w2 * SM(s_a2, k);
+            const float old = cpp[q];
+            const float vt = w1 * ca1[q] + w2 * ca2[q];
             float up = (old + SM(s_fpk, k)) + p.alph * vt;
             if (fabsf(up) < 1.0e-20f) up = 0.0f;
             const float tend = p.kdiv * (up - old);

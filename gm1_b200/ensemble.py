@@ -109,8 +109,10 @@ class MoistEnsemble:
             host, metrics = member_initial_state(mb, grid) if hosts is None else hosts[n]
             st = self.streams[n % len(self.streams)]
             with torch.cuda.stream(st):
+                # members already overlap one another, so each steps its own
+                # operations in order on its stream
                 self.steps.append(MoistLargeStep(member_config(mb, grid), upload(host, self.device),
-                                                 upload(metrics, self.device), stream=st))
+                                                 upload(metrics, self.device), stream=st, concurrent=False))
         self.graph: torch.cuda.CUDAGraph | None = None
 
     @property

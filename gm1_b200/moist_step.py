@@ -103,6 +103,12 @@ def large_step_schedule() -> tuple[ScheduledOperation, ...]:
     return tuple(order)
 
 
+# operations that may follow SCALAR_MOIST in the same stage's concurrent tail
+# (REMOVE_HELD_EOS / MASS_BEGIN / MASS_FINISH take no separate work here)
+TAIL_PHASES = frozenset({StepPhase.MOMENTUM_BOUNDARIES, StepPhase.SCALAR_BOUNDARIES, StepPhase.TKE,
+                         StepPhase.REMOVE_HELD_EOS, StepPhase.MASS_BEGIN, StepPhase.MASS_FINISH})
+
+
 @dataclass(frozen=True, slots=True)
 class MoistStepConfig:
     ni: int
@@ -124,6 +130,10 @@ class MoistStepConfig:
 
 
 NUMQ = 3  # Kessler: qv, qc, qr
+# per-species scratch of the moisture advection and pdef chain
+SPECIES_SCRATCH = ("moisture_padded", "fx", "fy", "fz", "advx", "advy", "advz", "candidate")
+# theta + the moisture species, momentum/pressure boundaries, TKE
+SIDE_STREAMS = 1 + NUMQ + 2
 QROWS = 6  # the eqtset2 terms and calcnm read six mass rows (the last three zero)
 
 
@@ -260,7 +270,7 @@ class MoistLargeStep:
     captured in a CUDA graph."""
 
     def __init__(self, cfg: MoistStepConfig, state: dict[str, torch.Tensor], metrics: dict[str, torch.Tensor], *,
-                 stream: Any | None = None) -> None:
+                 stream: Any | None = None, concurrent: bool = True) -> None:
         self.cfg, self.s, self.m = cfg, state, metrics
         self.stream = stream
         ni, nj, nk = cfg.ni, cfg.nj, cfg.nk
@@ -293,12 +303,22 @@ class MoistLargeStep:
                             "dzdx": m["dzdx"], "dzdy": m["dzdy"], "gz": m["gz"], "rho0_3d": m["rho0_3d"],
                             "rf0": m["rf0"], "thterm": s["thterm"], "divergence": s["divergence"],
                             "theta_divergence_term": s["theta_div"], "divx": s["divx"]}
-        self.chain_arrays = [{"scalar_a": self.qa_rows[r], "scalar_padded": s["moisture_padded"],
+        # Each moisture species has its own packing and pdef scratch (species 0
+        # uses the state's), so the species can advect concurrently; fresh
+        # scratch starts at zero as the state's does.
+        self.species_scratch = [{n: s[n] for n in SPECIES_SCRATCH}] + [
+            {n: torch.zeros_like(s[n]) for n in SPECIES_SCRATCH} for _ in range(1, NUMQ)]
+        self.chain_arrays = [{"scalar_a": self.qa_rows[r], "scalar_padded": self.species_scratch[r]["moisture_padded"],
                               "rho0_3d": m["rho0_3d"], "gz": m["gz"], "rgz": m["rgz"], "rr0": m["rr0"], "c1": m["c1"],
                               "c2": m["c2"], "divx": s["divx"], "rru": s["rru"], "rrv": s["rrv"], "rrw": s["rrw"],
-                              "fx": s["fx"], "fy": s["fy"], "fz": s["fz"], "advx": s["advx"], "advy": s["advy"],
-                              "advz": s["advz"], "candidate": s["candidate"], "advection": s["moist_adv"][r]}
+                              **{n: self.species_scratch[r][n] for n in SPECIES_SCRATCH if n != "moisture_padded"},
+                              "advection": s["moist_adv"][r]}
                              for r in range(NUMQ)]
+        # side streams of the concurrent step (created here so that a CUDA
+        # graph capture of step() can fork onto them)
+        dev = s["u3d"].device
+        self.concurrent = concurrent
+        self._side = [torch.cuda.Stream(dev) for _ in range(SIDE_STREAMS)] if concurrent else []
         self.kessler = create_cuda_gm1_kessler_large_step_transition(
             {"ruh": s["ruh"], "rvh": s["rvh"], "rmh": m["rmh"], "mh": m["mh"], "pi0": s["pi0_3d"], "th0": s["th0_3d"],
              "rr": s["kessler_rr"], "rho": s["rho"], "pp3d": s["pp3d_c"], "th3d": s["th3d"], "prs": s["prs"],
@@ -384,30 +404,51 @@ class MoistLargeStep:
     def post_acoustic(self, nrk: int) -> None:
         mo.post_acoustic_flux(self.post_arrays, **self.grid, stream=self._st())
 
-    def scalar_moist(self, nrk: int) -> None:
-        s, m, cfg, st = self.s, self.m, self.cfg, self._st()
+    def _theta_advection(self, nrk: int, st) -> None:
+        s, m, cfg = self.s, self.m, self.cfg
         flux = {"rru": s["rru"], "rrv": s["rrv"], "rrw": s["rrw"]}
         met = {"c1": m["c1"], "c2": m["c2"], "rr0": m["rr0"], "gz": m["gz"]}
-        adv = dict(**self.grid, nrk=nrk, stream=st, lateral_sides=cfg.lateral_sides, write_fluxes=False)
         theta_transport_scalar(s["th0"], s["th3d"], s["theta_padded"], **self.k3, stream=st)
         mo.open_fill(s["theta_padded"], "scalar", **self.k3, stream=st)
         with torch.cuda.stream(st):
             s["theta_adv"].zero_()
         launch_cuda_scalar_advection5(s["theta_padded"], flux, met, s["divx"], s["theta_adv"], None,
-                                      weps=theta_weps_f64(), **adv)
-        dttmp = scalar_moist_rk_stage_timestep_f32(cfg.dt, nrk)
-        for r in range(NUMQ):
-            mo.pack_scalar(self.q_rows[r], s["moisture_padded"], **self.k3, stream=st)
-            mo.open_fill(s["moisture_padded"], "scalar", **self.k3, stream=st)
-            with torch.cuda.stream(st):
-                s["moist_adv"][r].zero_()
-            weps = moisture_weps_f64(r)
-            if nrk < 3:
-                launch_cuda_scalar_advection5(s["moisture_padded"], flux, met, s["divx"], s["moist_adv"][r], None,
-                                              weps=weps, **adv)
-            else:
-                mo.pdef_moisture_chain(self.chain_arrays[r], **self.grid, dttmp=dttmp, weps=weps,
-                                       lateral_obc=cfg.obc, pdefweno=0 if r == 0 else 1, stream=st)
+                                      weps=theta_weps_f64(), **self.grid, nrk=nrk, stream=st,
+                                      lateral_sides=cfg.lateral_sides, write_fluxes=False)
+
+    def _species_advection(self, r: int, nrk: int, st) -> None:
+        s, m, cfg = self.s, self.m, self.cfg
+        padded = self.species_scratch[r]["moisture_padded"]
+        mo.pack_scalar(self.q_rows[r], padded, **self.k3, stream=st)
+        mo.open_fill(padded, "scalar", **self.k3, stream=st)
+        with torch.cuda.stream(st):
+            s["moist_adv"][r].zero_()
+        weps = moisture_weps_f64(r)
+        if nrk < 3:
+            launch_cuda_scalar_advection5(padded, {"rru": s["rru"], "rrv": s["rrv"], "rrw": s["rrw"]},
+                                          {"c1": m["c1"], "c2": m["c2"], "rr0": m["rr0"], "gz": m["gz"]},
+                                          s["divx"], s["moist_adv"][r], None, weps=weps, **self.grid, nrk=nrk,
+                                          stream=st, lateral_sides=cfg.lateral_sides, write_fluxes=False)
+        else:
+            mo.pdef_moisture_chain(self.chain_arrays[r], **self.grid,
+                                   dttmp=scalar_moist_rk_stage_timestep_f32(cfg.dt, nrk), weps=weps,
+                                   lateral_obc=cfg.obc, pdefweno=0 if r == 0 else 1, stream=st)
+
+    def scalar_moist(self, nrk: int) -> None:
+        """theta and the moisture species advect (concurrently, each on its own
+        side stream, when the step is concurrent), then one RK compose."""
+        s, cfg, st = self.s, self.cfg, self._st()
+        if self.concurrent:
+            lanes = self._side[:1 + NUMQ]
+            self._fork(st, lanes)
+            self._theta_advection(nrk, lanes[0])
+            for r in range(NUMQ):
+                self._species_advection(r, nrk, lanes[1 + r])
+            self._join(st, lanes)
+        else:
+            self._theta_advection(nrk, st)
+            for r in range(NUMQ):
+                self._species_advection(r, nrk, st)
         compose_scalar_moist_rk_stage(s["tha"], s["qa"][:NUMQ], s["thheld"], s["qheld"], s["theta_div"],
                                       s["theta_adv"], s["moist_adv"], s["th3d"], s["q3d"][:NUMQ], nrk=nrk, dt=cfg.dt,
                                       stream=st)
@@ -475,9 +516,62 @@ class MoistLargeStep:
         # correction) and PDEFQ (the Kessler operator's own pdefq runs inside
         # it) take no separate work here.
 
+    # -- concurrency -------------------------------------------------------
+    @staticmethod
+    def _fork(main, lanes) -> None:
+        ev = torch.cuda.Event()
+        ev.record(main)
+        for ln in lanes:
+            ln.wait_event(ev)
+
+    @staticmethod
+    def _join(main, lanes) -> None:
+        for ln in lanes:
+            ev = torch.cuda.Event()
+            ev.record(ln)
+            main.wait_event(ev)
+
+    def _stage_tail(self, ops) -> None:
+        """SCALAR_MOIST, MOMENTUM_BOUNDARIES, SCALAR_BOUNDARIES and TKE of one
+        RK stage touch disjoint fields (scalars and moisture / u, v, w and
+        pi' / TKE; all read the same mass fluxes), so they run concurrently:
+        the scalars on the main stream (forking its own side streams), the
+        boundaries and TKE on two more, joined before the next stage."""
+        main = self._st()
+        bnd, tke = self._side[1 + NUMQ], self._side[2 + NUMQ]
+        self._fork(main, (bnd, tke))
+        saved = self.stream
+        for op in ops:
+            if op.phase in (StepPhase.MOMENTUM_BOUNDARIES, StepPhase.SCALAR_BOUNDARIES):
+                self.stream = bnd
+            elif op.phase is StepPhase.TKE:
+                self.stream = tke
+            else:
+                self.stream = main
+            try:
+                self.execute(op)
+            finally:
+                self.stream = saved
+        self._join(main, (bnd, tke))
+
     def step(self) -> None:
-        for op in large_step_schedule():
+        """One large step: the operations of large_step_schedule() in order
+        (each stage's scalar / boundary / TKE tail concurrently when the step
+        is concurrent)."""
+        ops = large_step_schedule()
+        q = 0
+        while q < len(ops):
+            op = ops[q]
+            if self.concurrent and op.phase is StepPhase.SCALAR_MOIST:
+                tail = [op]
+                q += 1
+                while q < len(ops) and ops[q].nrk == op.nrk and ops[q].phase in TAIL_PHASES:
+                    tail.append(ops[q])
+                    q += 1
+                self._stage_tail(tail)
+                continue
             self.execute(op)
+            q += 1
         self.completed_steps += 1
 
 

@@ -84,3 +84,27 @@ def test_graph_replay_gives_the_eager_words():
     torch.cuda.synchronize()
     for n in FIELDS:
         assert torch.equal(eager.s[n].view(torch.int32), graphed.s[n].view(torch.int32)), n
+
+
+def test_concurrent_stage_tail_gives_the_sequential_words():
+    """The concurrent step (scalars, boundaries and TKE of each stage on side
+    streams) writes the same words as the same step run operation by
+    operation on one stream, including when captured as a CUDA graph."""
+    ni, nj, nk = 40, 33, 16
+    cfg = MoistStepConfig(ni, nj, nk, 1000.0, 1000.0, 250.0, 5.0, 10)
+    host, metrics = weisman_klemp_initial_state(cfg, seed=5, bubble_cloud=1.0e-3, bubble_rain=5.0e-4)
+    seq = MoistLargeStep(cfg, upload(host), upload(metrics), concurrent=False)
+    stream = torch.cuda.Stream()
+    con = MoistLargeStep(cfg, upload(host), upload(metrics), stream=stream, concurrent=True)
+    for _ in range(2):
+        seq.step()
+    with torch.cuda.stream(stream):
+        con.step()
+    stream.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=stream):
+        con.step()
+    graph.replay()
+    torch.cuda.synchronize()
+    for n in FIELDS + ("rain", "ppx", "tha", "qa"):
+        assert np.array_equal(seq.s[n].cpu().numpy().view(np.uint32), con.s[n].cpu().numpy().view(np.uint32)), n
