@@ -291,20 +291,38 @@ template <bool W>
 __global__ void __launch_bounds__(128) tke_rk_stage_kernel(TkeArgs a, const float *__restrict__ cur,
                                                            float *__restrict__ nxt, float *__restrict__ nxt2,
                                                            float dttmp, double eps) {
-    const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 4 + threadIdx.y, f = blockIdx.z;
+    // The x face fluxes pass to the next lane by warp shuffle and the y face
+    // fluxes to the next warp row through shared memory (the last lane or row
+    // forms its outer one itself): each face flux is formed once, by the same
+    // function of the same arguments.
+    __shared__ float s_fy[4][32], s_my[4][32];
+    const int lane = threadIdx.x, row = threadIdx.y;
+    const int i = blockIdx.x * 32 + lane, j = blockIdx.y * 4 + row, f = blockIdx.z;
     const int ni = a.ni, nj = a.nj, nk = a.nk;
+    const bool inner = f > 0 && f < nk;  // uniform over the block
+    float mw = 0.0f, me = 0.0f, ms = 0.0f, mn = 0.0f, fx0 = 0.0f, fx1 = 0.0f, fy0 = 0.0f, fy1 = 0.0f;
+    if (inner) {
+        if (j < nj && i <= ni) fx0 = face_flux<W>(a, cur, 0, f, j, i, eps, &mw);
+        fx1 = __shfl_down_sync(0xffffffffu, fx0, 1);
+        me = __shfl_down_sync(0xffffffffu, mw, 1);
+        if (lane == 31 && j < nj && i < ni) fx1 = face_flux<W>(a, cur, 0, f, j, i + 1, eps, &me);
+        if (i < ni && j <= nj) fy0 = face_flux<W>(a, cur, 1, f, i, j, eps, &ms);
+        s_fy[row][lane] = fy0;
+        s_my[row][lane] = ms;
+    }
+    __syncthreads();
+    if (inner && row < 3) {
+        fy1 = s_fy[row + 1][lane];
+        mn = s_my[row + 1][lane];
+    }
     if (i >= ni || j >= nj) return;
     const unsigned z = f3(a, f, j, i);
-    if (f == 0 || f == nk) {
+    if (!inner) {
         nxt[z] = 0.0f;
         if (nxt2) nxt2[z] = 0.0f;
         return;
     }
-    float mw, me, ms, mn;
-    const float fx0 = face_flux<W>(a, cur, 0, f, j, i, eps, &mw);
-    const float fx1 = face_flux<W>(a, cur, 0, f, j, i + 1, eps, &me);
-    const float fy0 = face_flux<W>(a, cur, 1, f, i, j, eps, &ms);
-    const float fy1 = face_flux<W>(a, cur, 1, f, i, j + 1, eps, &mn);
+    if (row == 3) fy1 = face_flux<W>(a, cur, 1, f, i, j + 1, eps, &mn);
     float ax = -1.0f * ((fx1 - fx0) * a.rdx);
     float ay = -1.0f * ((fy1 - fy0) * a.rdy);
     const float c2 = a.c2[z], c1 = 1.0f - c2;
