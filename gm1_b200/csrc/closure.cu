@@ -197,7 +197,7 @@ __global__ void __launch_bounds__(kDX *kDY) calcdef_tile_kernel(DefArgs p) {
             const float t13 = 0.5f * (sq(s13[ty][tx]) + sq(s13[ty][tx + 1]));
             const float t23 = 0.5f * (sq(s23[ty][tx]) + sq(s23[ty + 1][tx]));
             const float rfv = p.rf[f];
-            const float rrf = 1.0f / (rfv * rfv);
+            const float rrf = rcp_rn(rfv * rfv);
             p.defv[f] = (4.0f * (t13 + t23)) * rrf;
             p.defh[f] = ((2.0f * ((t11 + t22) + t33)) + 4.0f * t12) * rrf;
         }

@@ -40,6 +40,24 @@ __device__ __forceinline__ float flx3(float s1, float s2, float s3) {
     return r + kF3_3 * s3;
 }
 
+// Correctly rounded binary32 reciprocal on the short path: the hardware's
+// approximate reciprocal (PTX rcp.approx.ftz.f32, at most 1 ulp from 1/b)
+// refined by one FMA Newton-Raphson step in Markstein's form (P. Markstein,
+// "Computation of elementary functions on the IBM RISC System/6000
+// processor", IBM J. Res. Dev. 34(1), 1990): e = 1 - b*y exactly, then
+// y + y*e rounded once.  Used where |b| lies in [2^-125, 2^125]; elsewhere
+// (subnormal-adjacent, huge, zero, inf, NaN) it defers to __frcp_rn.
+// gm1b_selftest_reciprocal compares it with __frcp_rn on every one of the
+// 2^32 binary32 words.
+__device__ __forceinline__ float rcp_rn(float b) {
+    const float ab = fabsf(b);
+    if (!(ab >= 0x1p-125f && ab <= 0x1p125f)) return __frcp_rn(b);
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(b));
+    const float e = fmaf(-b, y, 1.0f);
+    return fmaf(y, e, y);
+}
+
 __device__ __forceinline__ float flx5(float s1, float s2, float s3, float s4, float s5) {
     float r = kF5_1 * s1;
     r = r + kF5_2 * s2;

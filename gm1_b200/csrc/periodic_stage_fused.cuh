@@ -91,7 +91,7 @@ __device__ __forceinline__ bool fused_grid_sync(unsigned long long *ctr, int *er
 // (nk >= 3), in the operation order of the multi-launch column kernel.
 // first: inv holds bb and ec holds cc on entry; the sweep replaces them with
 // 1/pivot and the elimination coefficient, the stage constants that later
-// small steps (first = false) reuse.  The reciprocal is __frcp_rn, the
+// small steps (first = false) reuse.  The reciprocal is rcp_rn (the word of __frcp_rn), the
 // correctly rounded 1/x, i.e. the same word as 1.0f / x under IEEE division.
 // Each level's operands are read one level ahead of its dependent chain.
 __device__ __forceinline__ void column_sweep(int nk, bool first, const float *aa, float *inv, float *ec,
@@ -101,7 +101,7 @@ __device__ __forceinline__ void column_sweep(int nk, bool first, const float *aa
     if (first) {
         float c;  // elimination coefficient of the previous level
         {
-            const float iv = __frcp_rn(inv[2 * S]);
+            const float iv = rcp_rn(inv[2 * S]);
             inv[2 * S] = iv;
             c = (-ec[2 * S]) * iv;
             e = dd[2 * S] * iv;
@@ -116,7 +116,7 @@ __device__ __forceinline__ void column_sweep(int nk, bool first, const float *aa
             c_n = ec[(k + 1) * S];
             d_n = dd[(k + 1) * S];
             const float pivot = a_k * c + b_k;
-            const float iv = __frcp_rn(pivot);
+            const float iv = rcp_rn(pivot);
             inv[k * S] = iv;
             const float num = d_k - a_k * e;
             c = (-c_k) * iv;
@@ -125,7 +125,7 @@ __device__ __forceinline__ void column_sweep(int nk, bool first, const float *aa
             ed[k * S] = e;
         }
         const float pivot = a_n * c + b_n;
-        const float iv = __frcp_rn(pivot);
+        const float iv = rcp_rn(pivot);
         inv[nk * S] = iv;
         w[nk * S] = (d_n - a_n * e) * iv;
     } else {

@@ -79,8 +79,8 @@ struct Ix {
 // uniform terrain coordinate, the twin's float32 words (terrain_coordinate_profiles)
 __device__ __forceinline__ float sig(int k, float dz) { return ((float)k - 0.5f) * dz; }
 __device__ __forceinline__ float sigf(int k, float dz) { return (float)(k - 1) * dz; }
-__device__ __forceinline__ float rds(int k, float dz) { return 1.0f / (sig(k, dz) - sig(k - 1, dz)); }
-__device__ __forceinline__ float rdsf(int k, float dz) { return 1.0f / (sigf(k + 1, dz) - sigf(k, dz)); }
+__device__ __forceinline__ float rds(int k, float dz) { return rcp_rn(sig(k, dz) - sig(k - 1, dz)); }
+__device__ __forceinline__ float rdsf(int k, float dz) { return rcp_rn(sigf(k + 1, dz) - sigf(k, dz)); }
 
 // numpy.minimum / numpy.maximum: NaN propagates, a tie returns the second
 __device__ __forceinline__ float np_min(float a, float b) { return a != a ? a : (b != b ? b : (a < b ? a : b)); }
@@ -593,7 +593,7 @@ __global__ void __launch_bounds__(32 * kTosWarps, 3) tos_column_kernel(TosArgs p
     if (live) c_loads(1 + wy);
     __syncthreads();
     // B: Thomas sweep, one lane per column (1/pivot by the correctly rounded
-    // reciprocal, the same word as 1.0f / pivot)
+    // reciprocal rcp_rn, the same word as 1.0f / pivot)
     // The next level's coefficients are read while this level eliminates, and
     // the back substitution carries w(k+1) in a register and reads its
     // coefficients kThomasChunk levels at a time, so shared-memory latency
@@ -611,7 +611,7 @@ __global__ void __launch_bounds__(32 * kTosWarps, 3) tos_column_kernel(TosArgs p
                 ndd = SM(s_dd, k + 1);
             }
             const float piv = k == 2 ? bb : aa * ec + bb;
-            const float inv = __frcp_rn(piv);
+            const float inv = rcp_rn(piv);
             if (dlast) a.tri_pivot[X.p(k, j, i)] = piv;
             if (k < nk) {
                 ec = (-cc) * inv;

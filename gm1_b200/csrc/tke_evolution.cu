@@ -103,7 +103,7 @@ __global__ void __launch_bounds__(kTT) tke_turbt_kernel(TkeArgs a, float dt) {
         unsigned z = f3(a, f, j, i);
         float rrf = a.mf[z] / a.rf[z];
         float r2 = (a.kmv[z] + a.kmv[f3(a, f + 1, j, i)]) * (a.mh[f3(a, f, j, i)] * (a.rho[f3(a, f, j, i)] * rrf));
-        float cfc = tema * r2, cfb = 1.0f - cfc, inv = 1.0f / cfb;
+        float cfc = tema * r2, cfb = 1.0f - cfc, inv = rcp_rn(cfb);
         float cprev = -1.0f * (cfc * inv), dprev = a.t[z] * inv;
         CP(0) = cprev;
         DP(0) = dprev;
@@ -117,7 +117,7 @@ __global__ void __launch_bounds__(kTT) tke_turbt_kernel(TkeArgs a, float dt) {
             const float cfa = tema * r1;
             cfc = tema * r2;
             cfb = (1.0f - cfa) - cfc;
-            inv = 1.0f / (cfa * cprev + cfb);
+            inv = rcp_rn(cfa * cprev + cfb);
             cprev = -1.0f * (cfc * inv);
             dprev = (a.t[z] - cfa * dprev) * inv;
             CP(p) = cprev;
@@ -130,7 +130,7 @@ __global__ void __launch_bounds__(kTT) tke_turbt_kernel(TkeArgs a, float dt) {
             (a.kmv[f3(a, f - 1, j, i)] + a.kmv[z]) * (a.mh[f3(a, f - 1, j, i)] * (a.rho[f3(a, f - 1, j, i)] * rrf));
         const float cfa = tema * r1;
         cfb = 1.0f - cfa;
-        float sol = (a.t[z] - cfa * DP(n - 2)) * (1.0f / (cfa * CP(n - 2) + cfb));
+        float sol = (a.t[z] - cfa * DP(n - 2)) * rcp_rn(cfa * CP(n - 2) + cfb);
         DP(n - 1) = sol;
         for (int p = n - 2; p >= 0; --p) {
             sol = CP(p) * sol + DP(p);

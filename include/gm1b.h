@@ -737,6 +737,18 @@ GM1B_API int32_t gm1b_stretch_z1(int32_t nk, float dz, float ztop, float str_bot
                                  float dz_top, const gm1b_vertical_profiles *device, void *stream);
 
 /*
+ * Self-check of the short-path correctly rounded reciprocal the column
+ * solves use (the hardware approximate reciprocal refined by one FMA
+ * Newton-Raphson step, used for |b| in [2^-125, 2^125]): compares it with
+ * CUDA's __frcp_rn on all 2^32 binary32 words on `stream`.  device_counts[0]
+ * receives the number of differing words, device_counts[1] the number of
+ * words on the short path; device_first_mismatch the smallest differing word
+ * (0xffffffff when none).  No host synchronisation.
+ */
+GM1B_API int32_t gm1b_selftest_reciprocal(unsigned long long *device_counts, uint32_t *device_first_mismatch,
+                                          void *stream);
+
+/*
  * Launch profiler.  While enabled, every kernel launch of the library is
  * bracketed by a pair of CUDA events recorded on its own stream (the
  * per-phase device timing of src/cm1core/runtime_profiler.py:1-48, per
