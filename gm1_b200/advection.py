@@ -163,12 +163,34 @@ class _ScalarAdvArrays(ctypes.Structure):
                                                "tendency", "flux_x", "flux_y", "flux_z")]
 
 
+class _VerticalColumn(ctypes.Structure):
+    _fields_ = [("flat", ctypes.c_int32), ("rdsf", ctypes.c_void_p), ("mh", ctypes.c_void_p), ("rdz", ctypes.c_float)]
+
+
+@dataclass(frozen=True)
+class StretchedColumn:
+    """The vertical column a stretched-grid operator reads (the profiles the
+    reference binds from its Gm1ChildStretchedMetrics): ``flat=False`` is
+    CM1's terrain branch with ``rdsf`` (nk+3 words, CM1-indexed: 1/(sigmaf(k+1)
+    - sigmaf(k)) at k = 1..nk); ``flat=True`` the flat column with ``mh``
+    (nk+2 words) and ``rdz`` = 1/dz of the metric reference."""
+
+    flat: bool
+    rdsf: Any = None
+    mh: Any = None
+    rdz: float = 0.0
+
+
 def _bind() -> ctypes.CDLL:
     lib = _native.lib()
     if not getattr(lib, "_adv_bound", False):
         i32, f32, vp = ctypes.c_int32, ctypes.c_float, ctypes.c_void_p
         lib.gm1b_terrain_mass_flux5.argtypes = [i32, i32, i32, ctypes.POINTER(_MassFluxArrays), f32, f32, f32, vp]
         lib.gm1b_terrain_mass_flux5.restype = i32
+        lib.gm1b_scalar_advection5_column.argtypes = [i32, i32, i32, ctypes.POINTER(_ScalarAdvArrays), i32, i32, f32,
+                                                      f32, ctypes.c_double, ctypes.c_uint32, i32,
+                                                      ctypes.POINTER(_VerticalColumn), ctypes.c_void_p]
+        lib.gm1b_scalar_advection5_column.restype = i32
         lib.gm1b_scalar_advection5.argtypes = [i32, i32, i32, ctypes.POINTER(_ScalarAdvArrays), i32, i32, f32, f32,
                                                f32, ctypes.c_double, ctypes.c_uint32, i32, vp]
         lib.gm1b_scalar_advection5.restype = i32
@@ -256,3 +278,65 @@ def launch_cuda_scalar_advection5(
         ev = torch.cuda.Event()
         ev.record(st)
     return CudaLaunch(ev, {"operation": "scalar-advection5", "nrk": nrk, "weno": use_weno, "lateral_obc": obc})
+
+
+def launch_cuda_gm1_child_stretched_scalar_advection5(
+    scalar: Any, arrays: Mapping[str, Any], metrics: Mapping[str, Any], divx: Any, tendency: Any,
+    fluxes: Mapping[str, Any] | None, vertical: StretchedColumn, *, ni: int, nj: int, nk: int, nrk: int, dx: float,
+    dy: float, weps: float, wflag: bool = True, stream: Any | None = None,
+    lateral_sides: tuple[int, int, int, int] | None = None, write_fluxes: bool = True,
+    levels_per_chunk: int | None = None,
+) -> CudaLaunch:
+    """The scalar tendency on a stretched column
+    (launch_cuda_gm1_child_stretched_scalar_advection5,
+    src/cm1core/cuda_gm1_child_stretched_scalar.py:666): the fluxes of
+    launch_cuda_scalar_advection5, the vertical derivative with the column's
+    own rdsf(k) (terrain branch) or rdz*mh(k) and rr0(k) (flat column)."""
+    if not isinstance(vertical, StretchedColumn):
+        raise TypeError("vertical must be a StretchedColumn")
+    use_weno = scalar_advection_uses_weno(nrk, wflag=wflag)
+    _validated_grid(ni, nj, nk)
+    dx, dy = (_validated_spacing(n, v) for n, v in (("dx", dx), ("dy", dy)))
+    if isinstance(weps, bool) or not isinstance(weps, (int, float)):
+        raise TypeError("weps must be numeric")
+    weps = float(weps)
+    if not math.isfinite(weps) or weps <= 0.0:
+        raise ValueError("weps must be finite and > 0")
+    obc = scalar_open_boundary_code(lateral_sides)
+    sh = padded_shapes(ni, nj, nk)
+    a = {
+        "scalar": _require(scalar, "scalar", sh["scalar"]),
+        "rru": _require(arrays["rru"], "rru", sh["u"]), "rrv": _require(arrays["rrv"], "rrv", sh["v"]),
+        "rrw": _require(arrays["rrw"], "rrw", sh["w"]),
+        "c1": _require(metrics["c1"], "c1", sh["face"]), "c2": _require(metrics["c2"], "c2", sh["face"]),
+        "rr0": _require(metrics["rr0"], "rr0", sh["cell"]), "gz": _require(metrics["gz"], "gz", (nj, ni)),
+        "divx": _require(divx, "divx", sh["cell"]), "tendency": _require(tendency, "tendency", sh["cell"]),
+    }
+    if write_fluxes:
+        if fluxes is None:
+            raise ValueError("write_fluxes requires the fluxes x/y/z arrays")
+        a["flux_x"] = _require(fluxes["x"], "flux_x", sh["u"])
+        a["flux_y"] = _require(fluxes["y"], "flux_y", sh["v"])
+        a["flux_z"] = _require(fluxes["z"], "flux_z", sh["w"])
+    if vertical.flat:
+        prof = _require(vertical.mh, "mh", (nk + 2,))
+        rdz = float(vertical.rdz)
+        if not (math.isfinite(rdz) and rdz > 0.0):
+            raise ValueError("a flat column needs rdz > 0")
+        col = _VerticalColumn(1, None, prof.data_ptr(), rdz)
+    else:
+        prof = _require(vertical.rdsf, "rdsf", (nk + 3,))
+        col = _VerticalColumn(0, prof.data_ptr(), None, 0.0)
+    _no_alias(list(a.values()) + [prof], "stretched scalar inputs, profile, flux scratch, and tendency")
+    s = _ScalarAdvArrays(**{n: t.data_ptr() for n, t in a.items()})
+    device = a["scalar"].device
+    st = torch.cuda.current_stream(device) if stream is None else stream
+    with torch.cuda.device(device):
+        _native.check(_bind().gm1b_scalar_advection5_column(ni, nj, nk, ctypes.byref(s), nrk, 1 if wflag else 0, dx,
+                                                            dy, weps, obc, int(levels_per_chunk or 0),
+                                                            ctypes.byref(col), ctypes.c_void_p(st.cuda_stream)),
+                      "gm1b_scalar_advection5_column")
+        ev = torch.cuda.Event()
+        ev.record(st)
+    return CudaLaunch(ev, {"operation": "stretched-scalar-advection5", "flat": bool(vertical.flat), "nrk": nrk,
+                           "weno": use_weno, "lateral_obc": obc})

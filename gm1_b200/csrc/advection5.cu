@@ -257,10 +257,21 @@ __device__ __forceinline__ float z_face(const float win[6], float m, float c1, f
     return m * r;
 }
 
+// vertical column of the tendency: mode 0 uniform (rdsf = 1/dz); mode 1
+// terrain-following stretched, rdsf(k) per level; mode 2 flat stretched,
+// ((d*rdz)*mh(k)) with the column's rr0(k) and no gz
+// (cuda_gm1_child_stretched_scalar.py:89-153 and :262-352)
+struct VertCol {
+    int mode;
+    const float *rdsf;  // (nk+3,) CM1-indexed
+    const float *mh;    // (nk+2,) CM1-indexed
+    float rdz;
+};
+
 template <bool WENO>
 __global__ void __launch_bounds__(kTX5 *kTY5)
     scalar_advection5_tiled_kernel(gm1b_scalar_advection5_arrays a, PaddedDims d, int levels_per_chunk, float rdx,
-                                   float rdy, float rdsf, double eps, float wepsf, unsigned obc) {
+                                   float rdy, float rdsf, double eps, float wepsf, unsigned obc, VertCol vc) {
     __shared__ float s_plane[kPY][kPX];
     __shared__ float s_fx[kTY5][kTX5 + 1];
     __shared__ float s_fy[kTY5 + 1][kTX5];
@@ -398,16 +409,30 @@ __global__ void __launch_bounds__(kTX5 *kTY5)
                 if (js) ay = ay - (sv * (vn - vs)) * rdy;
                 if (jn) ay = ay - (sv * (vn - vs)) * rdy;
                 float az;
-                if (k == 1)
-                    az = (-fz_hi) * rdsf;
-                else if (k == nk)
-                    az = fz_lo * rdsf;
-                else
-                    az = (fz_lo - fz_hi) * rdsf;
+                if (vc.mode == 2) {
+                    const float mhk = __ldg(vc.mh + k);
+                    if (k == 1)
+                        az = ((-fz_hi) * vc.rdz) * mhk;
+                    else if (k == nk)
+                        az = (fz_lo * vc.rdz) * mhk;
+                    else
+                        az = ((-(fz_hi - fz_lo)) * vc.rdz) * mhk;
+                } else {
+                    const float r = vc.mode == 1 ? __ldg(vc.rdsf + k) : rdsf;
+                    if (k == 1)
+                        az = (-fz_hi) * r;
+                    else if (k == nk)
+                        az = fz_lo * r;
+                    else
+                        az = (fz_lo - fz_hi) * r;
+                }
                 const int c = (k - 1) * cplane + j * ni + i;
                 float total = (ax + ay) + az;
                 total = total + sv * __ldg(a.divx + c);
-                a.tendency[c] = (total * __ldg(a.rr0 + c)) * gz;
+                if (vc.mode == 2)
+                    a.tendency[c] = total * __ldg(a.rr0 + (k - 1) * cplane);
+                else
+                    a.tendency[c] = (total * __ldg(a.rr0 + c)) * gz;
             }
             fz_lo = fz_hi;
         }
@@ -550,10 +575,10 @@ extern "C" int32_t gm1b_terrain_mass_flux5(int32_t ni, int32_t nj, int32_t nk, c
     return GM1B_OK;
 }
 
-extern "C" int32_t gm1b_scalar_advection5(int32_t ni, int32_t nj, int32_t nk,
-                                         const gm1b_scalar_advection5_arrays *arrays, int32_t nrk, int32_t wflag,
-                                         float dx, float dy, float dz, double weps, uint32_t lateral_obc,
-                                         int32_t levels_per_chunk, void *stream) {
+namespace {
+int32_t scalar_advection5_launch(int32_t ni, int32_t nj, int32_t nk, const gm1b_scalar_advection5_arrays *arrays,
+                                 int32_t nrk, int32_t wflag, float dx, float dy, float dz, double weps,
+                                 uint32_t lateral_obc, int32_t levels_per_chunk, VertCol vc, void *stream) {
     if (arrays == nullptr || ni < 8 || nj < 8 || nk < 8) {
         gm1b_set_error("gm1b_scalar_advection5: need arrays and ni, nj, nk >= 8");
         return GM1B_ERR_ARGUMENT;
@@ -597,14 +622,43 @@ extern "C" int32_t gm1b_scalar_advection5(int32_t ni, int32_t nj, int32_t nk,
     ProfScope ps(weno ? "scalar_advection5_weno_kernel" : "scalar_advection5_kernel", st);
     if (weno)
         scalar_advection5_tiled_kernel<true>
-            <<<grid, dim3(kTX5, kTY5), 0, st>>>(a, d, chunk, rdx, rdy, rdsf, weps, (float)weps, lateral_obc);
+            <<<grid, dim3(kTX5, kTY5), 0, st>>>(a, d, chunk, rdx, rdy, rdsf, weps, (float)weps, lateral_obc, vc);
     else
         scalar_advection5_tiled_kernel<false>
-            <<<grid, dim3(kTX5, kTY5), 0, st>>>(a, d, chunk, rdx, rdy, rdsf, weps, (float)weps, lateral_obc);
+            <<<grid, dim3(kTX5, kTY5), 0, st>>>(a, d, chunk, rdx, rdy, rdsf, weps, (float)weps, lateral_obc, vc);
     ps.stop();
     if (cudaPeekAtLastError() != cudaSuccess) {
         gm1b_set_error("scalar_advection5_kernel: %s", cudaGetErrorString(cudaGetLastError()));
         return GM1B_ERR_CUDA;
     }
     return GM1B_OK;
+}
+}  // namespace
+
+extern "C" int32_t gm1b_scalar_advection5(int32_t ni, int32_t nj, int32_t nk,
+                                         const gm1b_scalar_advection5_arrays *arrays, int32_t nrk, int32_t wflag,
+                                         float dx, float dy, float dz, double weps, uint32_t lateral_obc,
+                                         int32_t levels_per_chunk, void *stream) {
+    return scalar_advection5_launch(ni, nj, nk, arrays, nrk, wflag, dx, dy, dz, weps, lateral_obc, levels_per_chunk,
+                                    VertCol{0, nullptr, nullptr, 0.0f}, stream);
+}
+
+extern "C" int32_t gm1b_scalar_advection5_column(int32_t ni, int32_t nj, int32_t nk,
+                                                const gm1b_scalar_advection5_arrays *arrays, int32_t nrk,
+                                                int32_t wflag, float dx, float dy, double weps, uint32_t lateral_obc,
+                                                int32_t levels_per_chunk, const gm1b_vertical_column *column,
+                                                void *stream) {
+    if (column == nullptr || (column->flat != 0 && column->flat != 1)) {
+        gm1b_set_error("gm1b_scalar_advection5_column: need a vertical column with flat = 0 or 1");
+        return GM1B_ERR_ARGUMENT;
+    }
+    if (column->flat ? (column->mh == nullptr || !(column->rdz > 0.0f) || !isfinite(column->rdz))
+                     : column->rdsf == nullptr) {
+        gm1b_set_error("gm1b_scalar_advection5_column: a flat column needs mh and rdz > 0, a terrain column rdsf");
+        return GM1B_ERR_ARGUMENT;
+    }
+    const VertCol vc{column->flat ? 2 : 1, column->rdsf, column->mh, column->rdz};
+    // dz only forms the uniform reciprocal, which a stretched column never reads
+    return scalar_advection5_launch(ni, nj, nk, arrays, nrk, wflag, dx, dy, 1.0f, weps, lateral_obc,
+                                    levels_per_chunk, vc, stream);
 }

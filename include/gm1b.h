@@ -192,6 +192,29 @@ GM1B_API int32_t gm1b_scalar_advection5(int32_t ni, int32_t nj, int32_t nk,
                                         float dz, double weps, uint32_t lateral_obc,
                                         int32_t levels_per_chunk, void *stream);
 
+/*
+ * The stretched-column scalar advection of
+ * launch_cuda_gm1_child_stretched_scalar_advection5
+ * (src/cm1core/cuda_gm1_child_stretched_scalar.py:666-842): the same face
+ * fluxes, with the tendency's vertical derivative taken on a stretched
+ * column.  flat = 0: CM1's terrain branch, -(d*rdsf(k)) with rdsf the
+ * (nk+3,) CM1-indexed profile (:89-153); flat = 1: the flat column,
+ * -((d*rdz)*mh(k)) with mh the (nk+2,) profile and the tendency scaled by
+ * the column's rr0(k) without gz (:262-352; adv.F:555-572, 646-656).
+ */
+typedef struct gm1b_vertical_column {
+    int32_t flat;
+    const float *rdsf; /* flat = 0 */
+    const float *mh;   /* flat = 1 */
+    float rdz;         /* flat = 1: 1/dz of the metric reference */
+} gm1b_vertical_column;
+
+GM1B_API int32_t gm1b_scalar_advection5_column(int32_t ni, int32_t nj, int32_t nk,
+                                               const gm1b_scalar_advection5_arrays *arrays, int32_t nrk,
+                                               int32_t wflag, float dx, float dy, double weps,
+                                               uint32_t lateral_obc, int32_t levels_per_chunk,
+                                               const gm1b_vertical_column *column, void *stream);
+
 /* ------------------------------------------------------------------------
  * eqtset=2 moist stage terms
  * ---------------------------------------------------------------------- */

@@ -47,6 +47,11 @@ def _lib():
                                                  ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_float,
                                                  ctypes.c_float, ctypes.c_double, ctypes.c_uint]
         lib.oracle_scalar_advection5.restype = None
+        lib.oracle_scalar_advection5_column.argtypes = [ctypes.POINTER(ScalarAdvArrays), ctypes.c_int, ctypes.c_int,
+                                                        ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_float,
+                                                        ctypes.c_double, ctypes.c_uint, ctypes.c_int, _F, _F,
+                                                        ctypes.c_float]
+        lib.oracle_scalar_advection5_column.restype = None
         lib.oracle_weno5.argtypes = [ctypes.c_float] * 5 + [ctypes.c_double]
         lib.oracle_weno5.restype = ctypes.c_float
         lib._adv_ready = True
@@ -62,6 +67,18 @@ def scalar_advection5(arrays, *, ni, nj, nk, nrk, dx, dy, dz, weps, wflag=True, 
     use_weno = 1 if (wflag and nrk == 3) else 0
     s = _fill(ScalarAdvArrays(), arrays)
     _lib().oracle_scalar_advection5(ctypes.byref(s), ni, nj, nk, use_weno, dx, dy, dz, weps, lateral_obc)
+
+
+def scalar_advection5_column(arrays, *, ni, nj, nk, nrk, dx, dy, weps, flat, profile, rdz=0.0, wflag=True,
+                             lateral_obc=0) -> None:
+    """Stretched column: flat=False takes profile = rdsf (nk+3 words, CM1
+    indexing), flat=True profile = mh (nk+2 words) with rdz."""
+    use_weno = 1 if (wflag and nrk == 3) else 0
+    s = _fill(ScalarAdvArrays(), arrays)
+    prof = np.ascontiguousarray(profile, dtype=np.float32)
+    ptr = prof.ctypes.data_as(_F)
+    _lib().oracle_scalar_advection5_column(ctypes.byref(s), ni, nj, nk, use_weno, dx, dy, weps, lateral_obc,
+                                           2 if flat else 1, None if flat else ptr, ptr if flat else None, rdz)
 
 
 def weno5(values, weps) -> float:

@@ -178,9 +178,24 @@ void oracle_terrain_mass_flux5(const mass_flux_arrays *a, int ni, int nj, int nk
     }
 }
 
+/* Vertical column of the tendency: mode 0 uniform (rdsf = 1/dz); mode 1
+ * terrain-following stretched, rdsf(k) per level
+ * (cuda_gm1_child_stretched_scalar.py:138-153); mode 2 flat stretched,
+ * ((d*rdz)*mh(k)) and the column's rr0(k) without gz
+ * (cuda_gm1_child_stretched_scalar.py:324-348; adv.F:555-572, 646-656). */
+typedef struct {
+    int mode;
+    const float *rdsf; /* (nk+3,) CM1-indexed, mode 1 */
+    const float *mh;   /* (nk+2,) CM1-indexed, mode 2 */
+    float rdz;         /* mode 2 */
+} vertical_column;
+
+static const vertical_column kUniformColumn = {0, 0, 0, 0.0f};
+
 /* One cell of the tendency with CM1 lateral side codes (0 = tile-local). */
 static float tendency_cell(const scalar_adv_arrays *a, const float *fx, const float *fy, const float *fz, int ni,
-                           int nj, int nk, int k, int j, int i, unsigned obc, float rdx, float rdy, float rdsf) {
+                           int nj, int nk, int k, int j, int i, unsigned obc, float rdx, float rdy, float rdsf,
+                           const vertical_column *vc) {
     const int x = i + NG, y = j + NG;
     float fw = PU(fx, k, y, x), fe = PU(fx, k, y, x + 1);
     float fs = PV(fy, k, y, x), fn = PV(fy, k, y + 1, x);
@@ -202,19 +217,30 @@ static float tendency_cell(const scalar_adv_arrays *a, const float *fx, const fl
     if (js) ay = ay - (sv * (vn - vs)) * rdy;
     if (jn) ay = ay - (sv * (vn - vs)) * rdy;
     float az;
-    if (k == 1)
-        az = (-PW(fz, 2, y, x)) * rdsf;
-    else if (k == nk)
-        az = PW(fz, nk, y, x) * rdsf;
-    else
-        az = (PW(fz, k, y, x) - PW(fz, k + 1, y, x)) * rdsf;
+    if (vc->mode == 2) {
+        if (k == 1)
+            az = ((-PW(fz, 2, y, x)) * vc->rdz) * vc->mh[k];
+        else if (k == nk)
+            az = (PW(fz, nk, y, x) * vc->rdz) * vc->mh[k];
+        else
+            az = ((-(PW(fz, k + 1, y, x) - PW(fz, k, y, x))) * vc->rdz) * vc->mh[k];
+    } else {
+        const float r = vc->mode == 1 ? vc->rdsf[k] : rdsf;
+        if (k == 1)
+            az = (-PW(fz, 2, y, x)) * r;
+        else if (k == nk)
+            az = PW(fz, nk, y, x) * r;
+        else
+            az = (PW(fz, k, y, x) - PW(fz, k + 1, y, x)) * r;
+    }
     float total = (ax + ay) + az;
     total = total + sv * C3(a->divx, k - 1, j, i);
+    if (vc->mode == 2) return total * C3(a->rr0, k - 1, 0, 0);
     return (total * C3(a->rr0, k - 1, j, i)) * M2(a->gz, j, i, ni);
 }
 
-void oracle_scalar_advection5(const scalar_adv_arrays *a, int ni, int nj, int nk, int use_weno, float dx, float dy,
-                              float dz, double weps, unsigned obc) {
+static void scalar_advection5_column(const scalar_adv_arrays *a, int ni, int nj, int nk, int use_weno, float dx,
+                                     float dy, float dz, double weps, unsigned obc, const vertical_column *vc) {
     float *fx = a->flux_x, *fy = a->flux_y, *fz = a->flux_z;
     const float *s = a->scalar;
     for (int k = 1; k <= nk; ++k) {
@@ -307,6 +333,22 @@ void oracle_scalar_advection5(const scalar_adv_arrays *a, int ni, int nj, int nk
                 const int owned = obc != 0u || (i >= 3 && i + 3 < ni && j >= 3 && j + 3 < nj);
                 if (!owned) continue;
                 C3(a->tendency, k - 1, j, i) =
-                    tendency_cell(a, fx, fy, fz, ni, nj, nk, k, j, i, obc, rdx, rdy, rdsf);
+                    tendency_cell(a, fx, fy, fz, ni, nj, nk, k, j, i, obc, rdx, rdy, rdsf, vc);
             }
+}
+
+void oracle_scalar_advection5(const scalar_adv_arrays *a, int ni, int nj, int nk, int use_weno, float dx, float dy,
+                              float dz, double weps, unsigned obc) {
+    scalar_advection5_column(a, ni, nj, nk, use_weno, dx, dy, dz, weps, obc, &kUniformColumn);
+}
+
+/* launch_cuda_gm1_child_stretched_scalar_advection5
+ * (src/cm1core/cuda_gm1_child_stretched_scalar.py:666-842): the same face
+ * fluxes with the tendency's vertical derivative on a stretched column,
+ * mode 1 (terrain branch, rdsf(k)) or mode 2 (flat, rdz*mh(k), rr0(k)). */
+void oracle_scalar_advection5_column(const scalar_adv_arrays *a, int ni, int nj, int nk, int use_weno, float dx,
+                                     float dy, double weps, unsigned obc, int mode, const float *rdsf,
+                                     const float *mh, float rdz) {
+    const vertical_column vc = {mode, rdsf, mh, rdz};
+    scalar_advection5_column(a, ni, nj, nk, use_weno, dx, dy, 1.0f, weps, obc, &vc);
 }

@@ -80,3 +80,37 @@ def test_fused_path_without_flux_writes_and_any_chunk_is_identical(chunk):
                      write_fluxes=False, chunk=chunk)
     assert bit_mismatches({"tendency": out["qscalar_nrk3_tend"]}, got, ("tendency",)) == {}
     assert np.all(got["flux_x"] == np.float32(meta["sentinel"]))
+
+
+@pytest.mark.parametrize("flat", [False, True])
+@pytest.mark.parametrize("nrk", [1, 3])
+@pytest.mark.parametrize("sides", [(2, 2, 2, 2), (1, 2, 3, 4)])
+def test_stretched_column_matches_oracle(flat, nrk, sides):
+    """launch_cuda_gm1_child_stretched_scalar_advection5 on seeded stretched
+    profiles (rdsf per level, or mh per level with rdz) against the oracle
+    restatement, word for word."""
+    from gm1_b200.advection import (StretchedColumn, launch_cuda_gm1_child_stretched_scalar_advection5,
+                                    scalar_open_boundary_code)
+
+    meta, inputs, _ = load_npz(TAGS[0])
+    nk = meta["nk"]
+    h = advection_inputs(inputs, meta, "scalar")
+    rng = np.random.default_rng(5)
+    rdsf = np.zeros(nk + 3, np.float32)
+    rdsf[1:nk + 1] = (np.float32(1.0) / np.float32(meta["dz"])) * rng.uniform(0.4, 2.5, nk).astype(np.float32)
+    mh = rng.uniform(0.3, 3.0, nk + 2).astype(np.float32)
+    rdz = float(np.float32(1.0) / np.float32(100.0))
+    want = {k: v.copy() for k, v in h.items()}
+    adv.scalar_advection5_column(want, ni=meta["ni"], nj=meta["nj"], nk=nk, nrk=nrk, dx=meta["dx"], dy=meta["dy"],
+                                 weps=meta["weps"]["scalar"], flat=flat, profile=mh if flat else rdsf, rdz=rdz,
+                                 lateral_obc=scalar_open_boundary_code(sides))
+    d = {k: dev(v) for k, v in h.items()}
+    column = StretchedColumn(flat=True, mh=dev(mh), rdz=rdz) if flat else StretchedColumn(flat=False, rdsf=dev(rdsf))
+    launch_cuda_gm1_child_stretched_scalar_advection5(
+        d["scalar"], {k: d[k] for k in ("rru", "rrv", "rrw")}, {k: d[k] for k in ("c1", "c2", "rr0", "gz")},
+        d["divx"], d["tendency"], {"x": d["flux_x"], "y": d["flux_y"], "z": d["flux_z"]}, column,
+        ni=meta["ni"], nj=meta["nj"], nk=nk, nrk=nrk, dx=meta["dx"], dy=meta["dy"], weps=meta["weps"]["scalar"],
+        lateral_sides=sides)
+    torch.cuda.synchronize()
+    got = {k: d[k].cpu().numpy() for k in ("tendency", "flux_x", "flux_y", "flux_z")}
+    assert bit_mismatches(want, got, ("tendency", "flux_x", "flux_y", "flux_z")) == {}
