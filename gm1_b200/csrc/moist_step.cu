@@ -376,7 +376,17 @@ struct Pdef {
     double weps;
     unsigned obc;
     int pdefweno;
+    // vertical column: 0 uniform (rdz = 1/dz); 1 terrain branch, rdsf(k);
+    // 2 flat column, (x*rdz)*mh(k) with the column's rho0(k) / rr0(k) and no
+    // gz or rgz (cuda_gm1_child_stretched_scalar.py:160-255, :355-470)
+    int vmode;
+    const float *rdsf, *mh;
 };
+
+__device__ __forceinline__ float pdef_zterm(const Pdef &p, float x, int k) {
+    if (p.vmode == 2) return (x * p.rdz) * __ldg(p.mh + k);
+    return x * (p.vmode == 1 ? __ldg(p.rdsf + k) : p.rdz);
+}
 
 __global__ void __launch_bounds__(256) pdef_horizontal_flux_kernel(Pdef p, Lane L) {
     const int ni = L.ni, nj = L.nj;
@@ -477,8 +487,9 @@ __global__ void __launch_bounds__(256) pdef_directional_kernel(Pdef p, Lane L) {
         }
         p.ax[q] = axv;
         p.ay[q] = ayv;
-        p.az[q] = k == 1 ? (-p.fz[L.s(2, y, x)]) * p.rdz
-                         : (k == nk ? p.fz[L.s(nk, y, x)] * p.rdz : (p.fz[L.s(k, y, x)] - p.fz[L.s(k + 1, y, x)]) * p.rdz);
+        p.az[q] = k == 1 ? pdef_zterm(p, -p.fz[L.s(2, y, x)], k)
+                         : (k == nk ? pdef_zterm(p, p.fz[L.s(nk, y, x)], k)
+                                    : pdef_zterm(p, p.fz[L.s(k, y, x)] - p.fz[L.s(k + 1, y, x)], k));
     }
 }
 
@@ -487,7 +498,8 @@ __global__ void __launch_bounds__(256) pdef_candidate_kernel(Pdef p, Lane L, int
     const int ni = L.ni, nj = L.nj, nk = L.nk;
     const unsigned n = (unsigned)nk * nj * ni;
     const float *dir = axis == 0 ? p.ax : axis == 1 ? p.ay : p.az;
-    const float rsp = axis == 0 ? p.rdx : axis == 1 ? p.rdy : p.rdz;
+    const float rsp = axis == 0 ? p.rdx : p.rdy;  // x and y spacing; z goes through pdef_zterm
+    const bool flat = p.vmode == 2;
     for (unsigned q = (unsigned)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (unsigned)gridDim.x * blockDim.x) {
         const int i = (int)(q % ni), j = (int)((q / ni) % nj), k = (int)(q / ((unsigned)ni * nj)) + 1;
         const int x = i + 3, y = j + 3;
@@ -503,8 +515,10 @@ __global__ void __launch_bounds__(256) pdef_candidate_kernel(Pdef p, Lane L, int
             m0 = p.rrw[L.s(k, y, x)], m1 = p.rrw[L.s(k + 1, y, x)];
         }
         const float dm = m1 - m0;
-        const float r0a = p.rho0[q] * p.a[q];
-        p.dum[q] = inflow ? r0a : r0a + (p.dt * (dir[q] + (p.s[L.s(k, y, x)] * dm) * rsp)) * p.gz[(unsigned)j * ni + i];
+        const float r0a = (flat ? p.rho0[(unsigned)(k - 1) * ni * nj] : p.rho0[q]) * p.a[q];
+        const float sdm = p.s[L.s(k, y, x)] * dm;
+        const float inc = p.dt * (dir[q] + (axis == 2 ? pdef_zterm(p, sdm, k) : sdm * rsp));
+        p.dum[q] = inflow ? r0a : (flat ? r0a + inc : r0a + inc * p.gz[(unsigned)j * ni + i]);
     }
 }
 
@@ -523,7 +537,8 @@ __global__ void __launch_bounds__(256) pdef_correct_kernel(Pdef p, Lane L, int a
     const int ni = L.ni, nj = L.nj, nk = L.nk;
     const unsigned n = (unsigned)nk * nj * ni, slab = (unsigned)ni * nj;
     float *dir = axis == 0 ? p.ax : axis == 1 ? p.ay : p.az;
-    const float rsp = axis == 0 ? p.rdx : axis == 1 ? p.rdy : p.rdz;
+    const float rsp = axis == 0 ? p.rdx : p.rdy;  // x and y spacing; z goes through pdef_zterm
+    const bool flat = p.vmode == 2;
     const float *d = p.dum;
     for (unsigned q = (unsigned)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (unsigned)gridDim.x * blockDim.x) {
         const int i = (int)(q % ni), j = (int)((q / ni) % nj), k0 = (int)(q / slab);
@@ -570,12 +585,15 @@ __global__ void __launch_bounds__(256) pdef_correct_kernel(Pdef p, Lane L, int a
         }
         if (flag) {
             const int k = k0 + 1, x = i + 3, y = j + 3;
-            const float first = (((d[q] + mass) - p.rho0[q] * p.a[q]) * p.rdt) * p.rgz[(unsigned)j * ni + i];
+            const float r0 = flat ? p.rho0[(unsigned)k0 * slab] : p.rho0[q];
+            float first = ((d[q] + mass) - r0 * p.a[q]) * p.rdt;
+            if (!flat) first = first * p.rgz[(unsigned)j * ni + i];
             float dm;
             if (axis == 0) dm = p.rru[L.u(k, y, x + 1)] - p.rru[L.u(k, y, x)];
             else if (axis == 1) dm = p.rrv[L.v(k, y + 1, x)] - p.rrv[L.v(k, y, x)];
             else dm = p.rrw[L.s(k + 1, y, x)] - p.rrw[L.s(k, y, x)];
-            dir[q] = first - (p.s[L.s(k, y, x)] * dm) * rsp;
+            const float sdm = p.s[L.s(k, y, x)] * dm;
+            dir[q] = first - (axis == 2 ? pdef_zterm(p, sdm, k) : sdm * rsp);
         }
     }
 }
@@ -588,7 +606,7 @@ __global__ void __launch_bounds__(256) pdef_total_kernel(Pdef p, Lane L) {
         if (!obc_owned(i, j, ni, nj, p.obc)) continue;
         float t = (p.ax[q] + p.ay[q]) + p.az[q];
         t = t + p.s[L.s(k, j + 3, i + 3)] * p.divx[q];
-        p.adv[q] = (t * p.rr0[q]) * p.gz[(unsigned)j * ni + i];
+        p.adv[q] = p.vmode == 2 ? t * p.rr0[(unsigned)(k - 1) * ni * nj] : (t * p.rr0[q]) * p.gz[(unsigned)j * ni + i];
     }
 }
 
@@ -793,9 +811,10 @@ extern "C" int32_t gm1b_post_acoustic_flux(int32_t ni, int32_t nj, int32_t nk, c
     return launch_ok("msb_getdivx_divergence_kernel") ? GM1B_OK : GM1B_ERR_CUDA;
 }
 
-extern "C" int32_t gm1b_pdef_moisture_chain(int32_t ni, int32_t nj, int32_t nk, const gm1b_pdef_chain_arrays *a,
-                                            float dttmp, float dx, float dy, float dz, double weps,
-                                            uint32_t lateral_obc, int32_t pdefweno, void *stream) {
+namespace {
+int32_t pdef_chain_launch(int32_t ni, int32_t nj, int32_t nk, const gm1b_pdef_chain_arrays *a, float dttmp, float dx,
+                          float dy, float dz, double weps, uint32_t lateral_obc, int32_t pdefweno, int vmode,
+                          const float *rdsf, const float *mh, float rdz, void *stream) {
     if (a == nullptr || !grid_ok(ni, nj, nk, 2, 2, 4, "gm1b_pdef_moisture_chain")) {
         if (a == nullptr) gm1b_set_error("gm1b_pdef_moisture_chain: NULL arrays");
         return GM1B_ERR_ARGUMENT;
@@ -825,8 +844,9 @@ extern "C" int32_t gm1b_pdef_moisture_chain(int32_t ni, int32_t nj, int32_t nk, 
     p.fx = a->fx, p.fy = a->fy, p.fz = a->fz, p.ax = a->advx, p.ay = a->advy, p.az = a->advz;
     p.dum = a->candidate, p.adv = a->advection;
     p.dt = dttmp, p.dx = dx, p.dy = dy, p.dz = dz;
-    p.rdx = 1.0f / dx, p.rdy = 1.0f / dy, p.rdz = 1.0f / dz, p.rdt = 1.0f / dttmp;
+    p.rdx = 1.0f / dx, p.rdy = 1.0f / dy, p.rdz = vmode == 0 ? 1.0f / dz : rdz, p.rdt = 1.0f / dttmp;
     p.weps = weps, p.obc = lateral_obc, p.pdefweno = pdefweno ? 1 : 0;
+    p.vmode = vmode, p.rdsf = rdsf, p.mh = mh;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const Lane L{ni, nj, nk};
     const size_t n = (size_t)ni * nj * nk;
@@ -847,6 +867,28 @@ extern "C" int32_t gm1b_pdef_moisture_chain(int32_t ni, int32_t nj, int32_t nk, 
     TOS_LAUNCH(pdef_total_kernel, n, p, L);
 #undef TOS_LAUNCH
     return GM1B_OK;
+}
+}  // namespace
+
+extern "C" int32_t gm1b_pdef_moisture_chain(int32_t ni, int32_t nj, int32_t nk, const gm1b_pdef_chain_arrays *a,
+                                            float dttmp, float dx, float dy, float dz, double weps,
+                                            uint32_t lateral_obc, int32_t pdefweno, void *stream) {
+    return pdef_chain_launch(ni, nj, nk, a, dttmp, dx, dy, dz, weps, lateral_obc, pdefweno, 0, nullptr, nullptr, 0.0f,
+                             stream);
+}
+
+extern "C" int32_t gm1b_pdef_moisture_chain_column(int32_t ni, int32_t nj, int32_t nk,
+                                                   const gm1b_pdef_chain_arrays *a, float dttmp, float dx, float dy,
+                                                   double weps, uint32_t lateral_obc, int32_t pdefweno,
+                                                   const gm1b_vertical_column *column, void *stream) {
+    if (column == nullptr || (column->flat != 0 && column->flat != 1) ||
+        (column->flat ? (column->mh == nullptr || !(column->rdz > 0.0f) || !isfinite(column->rdz))
+                      : column->rdsf == nullptr)) {
+        gm1b_set_error("gm1b_pdef_moisture_chain_column: need a flat column (mh, rdz > 0) or a terrain column (rdsf)");
+        return GM1B_ERR_ARGUMENT;
+    }
+    return pdef_chain_launch(ni, nj, nk, a, dttmp, dx, dy, 1.0f, weps, lateral_obc, pdefweno, column->flat ? 2 : 1,
+                             column->rdsf, column->mh, column->rdz, stream);
 }
 
 extern "C" int32_t gm1b_held_compose(int32_t ni, int32_t nj, int32_t nk, const gm1b_held_arrays *a, float dt,

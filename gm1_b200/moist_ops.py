@@ -22,6 +22,7 @@ from typing import Any, Mapping
 import torch
 
 from . import _native
+from .advection import StretchedColumn, _VerticalColumn
 
 FILL_KINDS = {"pressure": 0, "scalar": 1, "u": 2, "v": 3, "w": 4, "w_keep_ends": 5}
 POST_NAMES = ("rru", "rrv", "rrw", "rgzu", "rgzv", "dzdx", "dzdy", "gz", "rho0_3d", "rf0", "thterm", "divergence",
@@ -49,6 +50,9 @@ def _lib():
         lib.gm1b_moist_buoyancy.argtypes = [i, i, i] + [vp] * 8 + [vp]
         lib.gm1b_post_acoustic_flux.argtypes = [i, i, i, c.POINTER(_Post), f, f, f, vp]
         lib.gm1b_pdef_moisture_chain.argtypes = [i, i, i, c.POINTER(_Chain), f, f, f, f, c.c_double, c.c_uint32, i, vp]
+        lib.gm1b_pdef_moisture_chain_column.argtypes = [i, i, i, c.POINTER(_Chain), f, f, f, c.c_double, c.c_uint32,
+                                                        i, c.POINTER(_VerticalColumn), vp]
+        lib.gm1b_pdef_moisture_chain_column.restype = i
         lib.gm1b_held_compose.argtypes = [i, i, i, c.POINTER(_Held), f, vp]
         lib.gm1b_solve3_density.argtypes = [i, i, i] + [vp] * 5 + [vp]
         lib.gm1b_pack_scalar.argtypes = [i, i, i, vp, vp, vp]
@@ -99,6 +103,31 @@ def pdef_moisture_chain(a: Mapping[str, torch.Tensor], *, ni: int, nj: int, nk: 
     s = _Chain(**{n: _f32(a[n], n) for n in CHAIN_NAMES})
     _native.check(_lib().gm1b_pdef_moisture_chain(ni, nj, nk, ctypes.byref(s), dttmp, dx, dy, dz, weps, lateral_obc,
                                                   pdefweno, _st(stream, a["rru"].device)), "gm1b_pdef_moisture_chain")
+
+
+def pdef_moisture_chain_column(a: Mapping[str, torch.Tensor], column: StretchedColumn, *, ni: int, nj: int, nk: int,
+                               dttmp: float, dx: float, dy: float, weps: float, lateral_obc: int, pdefweno: int,
+                               stream: Any | None = None) -> None:
+    """The final-stage moisture chain on a stretched column
+    (launch_cuda_gm1_child_stretched_pdef_moisture,
+    src/cm1core/cuda_gm1_child_stretched_scalar.py:851): the terrain branch's
+    rdsf(k), or the flat column's rdz*mh(k) with its own base state."""
+    if not isinstance(column, StretchedColumn):
+        raise TypeError("column must be a StretchedColumn")
+    if column.flat:
+        prof = column.mh
+        if not isinstance(prof, torch.Tensor) or tuple(prof.shape) != (nk + 2,):
+            raise ValueError(f"mh must be a ({nk + 2},) tensor")
+        col = _VerticalColumn(1, None, _f32(prof, "mh"), float(column.rdz))
+    else:
+        prof = column.rdsf
+        if not isinstance(prof, torch.Tensor) or tuple(prof.shape) != (nk + 3,):
+            raise ValueError(f"rdsf must be a ({nk + 3},) tensor")
+        col = _VerticalColumn(0, _f32(prof, "rdsf"), None, 0.0)
+    s = _Chain(**{n: _f32(a[n], n) for n in CHAIN_NAMES})
+    _native.check(_lib().gm1b_pdef_moisture_chain_column(ni, nj, nk, ctypes.byref(s), dttmp, dx, dy, weps, lateral_obc,
+                                                         pdefweno, ctypes.byref(col), _st(stream, a["rru"].device)),
+                  "gm1b_pdef_moisture_chain_column")
 
 
 def held_compose(a: Mapping[str, torch.Tensor], *, ni: int, nj: int, nk: int, dt: float,

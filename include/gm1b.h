@@ -528,6 +528,14 @@ GM1B_API int32_t gm1b_pdef_moisture_chain(int32_t ni, int32_t nj, int32_t nk, co
                                           float dttmp, float dx, float dy, float dz, double weps, uint32_t lateral_obc,
                                           int32_t pdefweno, void *stream);
 
+/* The chain on a stretched column (launch_cuda_gm1_child_stretched_pdef_moisture,
+ * src/cm1core/cuda_gm1_child_stretched_scalar.py:851): flat = 0, the
+ * terrain branch's rdsf(k) in every vertical derivative; flat = 1, the flat
+ * column's rdz*mh(k) with the column's rho0(k) and rr0(k) and no gz or rgz. */
+GM1B_API int32_t gm1b_pdef_moisture_chain_column(int32_t ni, int32_t nj, int32_t nk, const gm1b_pdef_chain_arrays *a,
+                                                 float dttmp, float dx, float dy, double weps, uint32_t lateral_obc,
+                                                 int32_t pdefweno, const gm1b_vertical_column *column, void *stream);
+
 /* Held-tendency composition once per large step: ppten from the held theta
  * and qv tendencies (or the microphysics pressure rate alone), then the
  * microphysics rates join the held theta/qv/qc tendencies

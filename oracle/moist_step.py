@@ -44,6 +44,9 @@ def _lib():
             [c.c_double, c.c_uint, c.c_int]
         lib.oracle_pdef_moisture_directional.argtypes = lib.oracle_pdef_moisture_chain.argtypes
         lib.oracle_pdef_moisture_directional.restype = None
+        lib.oracle_pdef_moisture_chain_column.argtypes = [c.c_int] * 3 + [c.POINTER(_Chain)] + [c.c_float] * 3 + \
+            [c.c_double, c.c_uint, c.c_int, c.c_int, _F, _F, c.c_float]
+        lib.oracle_pdef_moisture_chain_column.restype = None
         lib.oracle_held_compose.argtypes = [c.c_int] * 3 + [c.POINTER(_Held), c.c_float]
         lib.oracle_solve3_density.argtypes = [c.c_int] * 3 + [_F] * 5
         lib.oracle_pack_scalar.argtypes = [c.c_int] * 3 + [_F] * 2
@@ -72,6 +75,16 @@ def post_acoustic_flux(a, *, ni, nj, nk, dx, dy, dz):
 def pdef_moisture_chain(a, *, ni, nj, nk, dttmp, dx, dy, dz, weps, lateral_obc, pdefweno):
     s = _Chain(**{n: _p(a[n]) for n in CHAIN_NAMES})
     _lib().oracle_pdef_moisture_chain(ni, nj, nk, ctypes.byref(s), dttmp, dx, dy, dz, weps, lateral_obc, pdefweno)
+
+
+def pdef_moisture_chain_column(a, *, ni, nj, nk, dttmp, dx, dy, weps, lateral_obc, pdefweno, flat, profile, rdz=0.0):
+    """The chain on a stretched column: flat=False takes profile = rdsf
+    (nk+3 words, CM1 indexing), flat=True profile = mh (nk+2 words) and rdz."""
+    s = _Chain(**{n: _p(a[n]) for n in CHAIN_NAMES})
+    prof = np.ascontiguousarray(profile, dtype=np.float32)
+    _lib().oracle_pdef_moisture_chain_column(ni, nj, nk, ctypes.byref(s), dttmp, dx, dy, weps, lateral_obc, pdefweno,
+                                             2 if flat else 1, None if flat else _p(prof), _p(prof) if flat else None,
+                                             rdz)
 
 
 def pdef_moisture_directional(a, *, ni, nj, nk, dttmp, dx, dy, dz, weps, lateral_obc, pdefweno):

@@ -255,12 +255,28 @@ typedef struct {
     float *fx, *fy, *fz, *advx, *advy, *advz, *candidate, *advection;
 } chain_arrays;
 
-static void chain_impl(int ni, int nj, int nk, const chain_arrays *a, float dttmp, float dx, float dy, float dz,
-                       double weps, unsigned obc, int pdefweno, int stop_after_directional) {
+/* the chain's vertical column: mode 0 uniform (rdz = 1/dz), mode 1 terrain
+ * branch with rdsf(k), mode 2 flat column with (x*rdz)*mh(k), the column's
+ * rho0(k) / rr0(k) and no gz or rgz (cuda_gm1_child_stretched_scalar.py:160-255,
+ * :355-470; pdef.F:37-47, 146-178, 263-275, 381-411, 477-486, 548-557) */
+typedef struct {
+    int mode;
+    const float *rdsf, *mh;
+    float rdz;
+} chain_column;
+
+static inline float zterm(const chain_column *vc, float x, int k) {
+    if (vc->mode == 2) return (x * vc->rdz) * vc->mh[k];
+    return x * (vc->mode == 1 ? vc->rdsf[k] : vc->rdz);
+}
+
+static void chain_impl(int ni, int nj, int nk, const chain_arrays *a, float dttmp, float dx, float dy,
+                       const chain_column *vc, double weps, unsigned obc, int pdefweno, int stop_after_directional) {
     const Ln L = {ni, nj, nk};
     const float *s = a->scalar_padded;
     const float ew = (float)weps;
-    const float rdx = 1.0f / dx, rdy = 1.0f / dy, rdz = 1.0f / dz, rdt = 1.0f / dttmp;
+    const float rdx = 1.0f / dx, rdy = 1.0f / dy, rdt = 1.0f / dttmp;
+    const int flat = vc->mode == 2;
     for (int k = 1; k <= nk; ++k)
         for (int j = 0; j <= nj; ++j)
             for (int i = 0; i <= ni; ++i) {
@@ -340,13 +356,14 @@ static void chain_impl(int ni, int nj, int nk, const chain_arrays *a, float dttm
         }
         a->advx[q] = axv;
         a->advy[q] = ayv;
-        a->advz[q] = k == 1 ? (-a->fz[S(&L, 2, y, x)]) * rdz
-                            : (k == nk ? a->fz[S(&L, nk, y, x)] * rdz : (a->fz[S(&L, k, y, x)] - a->fz[S(&L, k + 1, y, x)]) * rdz);
+        a->advz[q] = k == 1 ? zterm(vc, -a->fz[S(&L, 2, y, x)], k)
+                            : (k == nk ? zterm(vc, a->fz[S(&L, nk, y, x)], k)
+                                       : zterm(vc, a->fz[S(&L, k, y, x)] - a->fz[S(&L, k + 1, y, x)], k));
     }
     if (stop_after_directional) return;
     for (int axis = 0; axis < 3; ++axis) {
         float *dir = axis == 0 ? a->advx : axis == 1 ? a->advy : a->advz;
-        const float rsp = axis == 0 ? rdx : axis == 1 ? rdy : rdz;
+        const float rsp = axis == 0 ? rdx : rdy;  /* x and y spacing; z goes through zterm */
         float *d = a->candidate;
         for (size_t q = 0; q < n; ++q) {
             const int i = (int)(q % ni), j = (int)((q / ni) % nj), k = (int)(q / slab) + 1, x = i + 3, y = j + 3;
@@ -362,8 +379,10 @@ static void chain_impl(int ni, int nj, int nk, const chain_arrays *a, float dttm
                 m0 = a->rrw[S(&L, k, y, x)], m1 = a->rrw[S(&L, k + 1, y, x)];
             }
             const float dm = m1 - m0;
-            const float r0a = a->rho0_3d[q] * a->scalar_a[q];
-            d[q] = inflow ? r0a : r0a + (dttmp * (dir[q] + (s[S(&L, k, y, x)] * dm) * rsp)) * a->gz[(size_t)j * ni + i];
+            const float r0a = (flat ? a->rho0_3d[(size_t)(k - 1) * slab] : a->rho0_3d[q]) * a->scalar_a[q];
+            const float sdm = s[S(&L, k, y, x)] * dm;
+            const float inc = dttmp * (dir[q] + (axis == 2 ? zterm(vc, sdm, k) : sdm * rsp));
+            d[q] = inflow ? r0a : (flat ? r0a + inc : r0a + inc * a->gz[(size_t)j * ni + i]);
         }
         for (size_t q = 0; q < n; ++q) {
             const int i = (int)(q % ni), j = (int)((q / ni) % nj), k0 = (int)(q / slab);
@@ -410,12 +429,15 @@ static void chain_impl(int ni, int nj, int nk, const chain_arrays *a, float dttm
             }
             if (flag) {
                 const int k = k0 + 1, x = i + 3, y = j + 3;
-                const float first = (((d[q] + mass) - a->rho0_3d[q] * a->scalar_a[q]) * rdt) * a->rgz[(size_t)j * ni + i];
+                const float r0 = flat ? a->rho0_3d[(size_t)k0 * slab] : a->rho0_3d[q];
+                float first = ((d[q] + mass) - r0 * a->scalar_a[q]) * rdt;
+                if (!flat) first = first * a->rgz[(size_t)j * ni + i];
                 float dm;
                 if (axis == 0) dm = a->rru[Uu(&L, k, y, x + 1)] - a->rru[Uu(&L, k, y, x)];
                 else if (axis == 1) dm = a->rrv[Vv(&L, k, y + 1, x)] - a->rrv[Vv(&L, k, y, x)];
                 else dm = a->rrw[S(&L, k + 1, y, x)] - a->rrw[S(&L, k, y, x)];
-                dir[q] = first - (s[S(&L, k, y, x)] * dm) * rsp;
+                const float sdm = s[S(&L, k, y, x)] * dm;
+                dir[q] = first - (axis == 2 ? zterm(vc, sdm, k) : sdm * rsp);
             }
         }
     }
@@ -424,19 +446,32 @@ static void chain_impl(int ni, int nj, int nk, const chain_arrays *a, float dttm
         if (!(obc != 0u || (i >= 3 && i + 3 < ni && j >= 3 && j + 3 < nj))) continue;
         float t = (a->advx[q] + a->advy[q]) + a->advz[q];
         t = t + s[S(&L, k, j + 3, i + 3)] * a->divx[q];
-        a->advection[q] = (t * a->rr0[q]) * a->gz[(size_t)j * ni + i];
+        a->advection[q] = flat ? t * a->rr0[(size_t)(k - 1) * slab] : (t * a->rr0[q]) * a->gz[(size_t)j * ni + i];
     }
 }
 
 void oracle_pdef_moisture_chain(int ni, int nj, int nk, const chain_arrays *a, float dttmp, float dx, float dy,
                                 float dz, double weps, unsigned obc, int pdefweno) {
-    chain_impl(ni, nj, nk, a, dttmp, dx, dy, dz, weps, obc, pdefweno, 0);
+    const chain_column vc = {0, 0, 0, 1.0f / dz};
+    chain_impl(ni, nj, nk, a, dttmp, dx, dy, &vc, weps, obc, pdefweno, 0);
 }
 
 /* the chain up to the directional advection (before any repair) */
 void oracle_pdef_moisture_directional(int ni, int nj, int nk, const chain_arrays *a, float dttmp, float dx, float dy,
                                       float dz, double weps, unsigned obc, int pdefweno) {
-    chain_impl(ni, nj, nk, a, dttmp, dx, dy, dz, weps, obc, pdefweno, 1);
+    const chain_column vc = {0, 0, 0, 1.0f / dz};
+    chain_impl(ni, nj, nk, a, dttmp, dx, dy, &vc, weps, obc, pdefweno, 1);
+}
+
+/* launch_cuda_gm1_child_stretched_pdef_moisture
+ * (src/cm1core/cuda_gm1_child_stretched_scalar.py:851): the chain on a
+ * stretched column, mode 1 (terrain branch, rdsf(k)) or mode 2 (flat
+ * column, rdz*mh(k) with the column's base state). */
+void oracle_pdef_moisture_chain_column(int ni, int nj, int nk, const chain_arrays *a, float dttmp, float dx, float dy,
+                                       double weps, unsigned obc, int pdefweno, int mode, const float *rdsf,
+                                       const float *mh, float rdz) {
+    const chain_column vc = {mode, rdsf, mh, rdz};
+    chain_impl(ni, nj, nk, a, dttmp, dx, dy, &vc, weps, obc, pdefweno, 0);
 }
 
 /* ------------------------------------------------------------------ */

@@ -119,3 +119,26 @@ def test_solve3_density_and_pack():
     om.pack_scalar(s, pad, ni=NI, nj=NJ, nk=NK)
     mo.pack_scalar(torch.from_numpy(s).cuda(), dp, ni=NI, nj=NJ, nk=NK)
     _same(dp, pad, "padded")
+
+
+@pytest.mark.parametrize("flat", [False, True])
+@pytest.mark.parametrize("obc", [0x2222, 0])
+def test_pdef_moisture_chain_on_a_stretched_column(flat, obc):
+    """The chain with the terrain branch's rdsf(k) or the flat column's
+    rdz*mh(k) (seeded profiles) against the oracle restatement, word for word."""
+    from gm1_b200.advection import StretchedColumn
+
+    a = chain_arrays(NI, NJ, NK, 17)
+    d = _dev(a)
+    rng = np.random.default_rng(19)
+    rdsf = np.zeros(NK + 3, np.float32)
+    rdsf[1:NK + 1] = rng.uniform(1.0 / 600.0, 1.0 / 40.0, NK).astype(np.float32)
+    mh = rng.uniform(0.3, 3.0, NK + 2).astype(np.float32)
+    rdz = float(np.float32(1.0) / np.float32(100.0))
+    kw = dict(ni=NI, nj=NJ, nk=NK, dttmp=2.0, dx=400.0, dy=300.0, weps=1e-20, lateral_obc=obc, pdefweno=1)
+    om.pdef_moisture_chain_column(a, flat=flat, profile=mh if flat else rdsf, rdz=rdz, **kw)
+    column = (StretchedColumn(flat=True, mh=torch.from_numpy(mh).cuda(), rdz=rdz) if flat
+              else StretchedColumn(flat=False, rdsf=torch.from_numpy(rdsf).cuda()))
+    mo.pdef_moisture_chain_column(d, column, **kw)
+    for n in ("fx", "fy", "fz", "advx", "advy", "advz", "candidate", "advection"):
+        _same(d[n], a[n], n)

@@ -68,3 +68,28 @@ def test_chain_with_open_sides_fills_every_cell():
     om.pdef_moisture_chain(a, ni=ni, nj=nj, nk=nk, dttmp=1.5, dx=250.0, dy=250.0, dz=150.0, weps=1e-20,
                            lateral_obc=0x2222, pdefweno=0)
     assert np.isfinite(a["advection"]).all()
+
+
+@pytest.mark.parametrize("obc", [0x2222, 0])
+def test_chain_on_uniform_columns_is_the_uniform_chain(obc):
+    """The stretched-column chain (restatement of the reference's
+    profile-bound pdef texts) reduces word for word to the uniform chain: a
+    terrain column whose rdsf(k) is 1/dz, and a flat column (mh = 1,
+    rdz = 1/dz) over a horizontally uniform base state with flat metrics."""
+    ni, nj, nk = 12, 10, 9
+    dz = 200.0
+    kw = dict(ni=ni, nj=nj, nk=nk, dttmp=2.0, dx=400.0, dy=300.0, weps=1e-20, lateral_obc=obc, pdefweno=1)
+    rdz = float(np.float32(1.0) / np.float32(dz))
+    for flat in (False, True):
+        a = chain_arrays(ni, nj, nk, 23)
+        if flat:
+            a["rho0_3d"][:] = a["rho0_3d"][:, :1, :1]
+            a["rr0"][:] = a["rr0"][:, :1, :1]
+            a["gz"][:] = np.float32(1.0)
+            a["rgz"][:] = np.float32(1.0)
+        want = {k: v.copy() for k, v in a.items()}
+        om.pdef_moisture_chain(want, dz=dz, **kw)
+        prof = np.ones(nk + 2, np.float32) if flat else np.full(nk + 3, np.float32(rdz), np.float32)
+        om.pdef_moisture_chain_column(a, flat=flat, profile=prof, rdz=rdz, **kw)
+        for n in ("advx", "advy", "advz", "candidate", "advection"):
+            assert np.array_equal(a[n].view(np.uint32), want[n].view(np.uint32)), (flat, n)
