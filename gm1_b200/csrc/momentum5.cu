@@ -30,6 +30,13 @@ struct MomArgs {
     int ni, nj, nk;
     int per[4], opn[4];  // west, east, south, north
     float rdx, rdy, rdz, dz;
+    // vertical column: 0 uniform (dz); 1 terrain branch on a stretched column
+    // (sigma, sigmaf, rds, rdsf profiles, physical top ztop, base density from
+    // the padded rho0p); 2 flat column (rdz*mh / rdz*mf, the column's rho0p,
+    // rf0, rr0, rrf0; no terrain terms), cuda_gm1_child_stretched_momentum.py:56-330
+    int vmode;
+    const float *rho0p, *sigma, *sigmaf, *rds, *rdsf, *mh, *mf, *rr0;
+    float ztop, rdzm;
 };
 
 // 32-bit element offsets (the host refuses grids whose padded arrays reach
@@ -63,6 +70,23 @@ __device__ __forceinline__ int fyw(const MomArgs &a, int j) {
 // face-level c2 at Fortran face kface, clamped column
 __device__ __forceinline__ float c2m(const MomArgs &a, int kface, int j, int i) {
     return __ldg(a.c2 + ic(a, kface - 1, clampn(j, a.nj), clampn(i, a.ni)));
+}
+
+// x * the column's vertical reciprocal at mass level k (uniform rdz, the
+// terrain branch's rdsf(k), or the flat column's (x*rdz)*mh(k))
+__device__ __forceinline__ float zmass(const MomArgs &a, float x, int k) {
+    if (a.vmode == 2) return (x * a.rdzm) * __ldg(a.mh + k);
+    return x * (a.vmode == 1 ? __ldg(a.rdsf + k) : a.rdz);
+}
+// the same at w level kf (rds(kf) / (x*rdz)*mf(kf))
+__device__ __forceinline__ float zface(const MomArgs &a, float x, int kf) {
+    if (a.vmode == 2) return (x * a.rdzm) * __ldg(a.mf + kf);
+    return x * (a.vmode == 1 ? __ldg(a.rds + kf) : a.rdz);
+}
+// a boundary correction: uniform and terrain ((q*c)*(r*h)) as adv.F is
+// grouped in the uniform text; the flat text groups it ((q*c)*r)*h
+__device__ __forceinline__ float bcorr(const MomArgs &a, float q, float c, float r, float h) {
+    return a.vmode == 2 ? ((q * c) * r) * h : q * (c * (r * h));
 }
 
 __device__ __forceinline__ float up5(float m, float s0, float s1, float s2, float s3, float s4, float s5) {
@@ -207,14 +231,22 @@ __global__ void __launch_bounds__(128) mom5_mass_kernel(MomArgs a) {
     const int x = blockIdx.x * 32 + threadIdx.x, yy = blockIdx.y * 4 + threadIdx.y, k = blockIdx.z + 1;
     const int ni = a.ni, nj = a.nj, k0 = k - 1;
     if (x > ni || yy > nj) return;
+    if (a.vmode == 2) {  // flat column: rho0(1,1,k) u and rho0(1,1,k) v
+        const float r0 = __ldg(a.rho0p + iw(a, k, G, G));
+        if (yy < nj) RU(k, yy + G, x + G) = r0 * LU(k, yy + G, x + G);
+        if (x < ni) RV(k, yy + G, x + G) = r0 * LV(k, yy + G, x + G);
+        return;
+    }
     if (yy < nj) {  // u face (row yy, face x)
         const int j = yy, l = x - 1 < 0 ? 0 : x - 1, r = x < ni - 1 ? x : ni - 1;
-        const float density = __ldg(a.rho0 + ic(a, k0, j, l)) + __ldg(a.rho0 + ic(a, k0, j, r));
+        const float density = a.vmode == 1 ? __ldg(a.rho0p + iw(a, k, j + G, x + G - 1)) + __ldg(a.rho0p + iw(a, k, j + G, x + G))
+                                           : __ldg(a.rho0 + ic(a, k0, j, l)) + __ldg(a.rho0 + ic(a, k0, j, r));
         RU(k, j + G, x + G) = (0.5f * density) * (LU(k, j + G, x + G) * __ldg(a.rgzu + (size_t)j * (ni + 1) + x));
     }
     if (x < ni) {  // v face (face yy, column x)
         const int s = yy - 1 < 0 ? 0 : yy - 1, n = yy < nj - 1 ? yy : nj - 1;
-        const float density = __ldg(a.rho0 + ic(a, k0, s, x)) + __ldg(a.rho0 + ic(a, k0, n, x));
+        const float density = a.vmode == 1 ? __ldg(a.rho0p + iw(a, k, yy + G - 1, x + G)) + __ldg(a.rho0p + iw(a, k, yy + G, x + G))
+                                           : __ldg(a.rho0 + ic(a, k0, s, x)) + __ldg(a.rho0 + ic(a, k0, n, x));
         RV(k, yy + G, x + G) = (0.5f * density) * (LV(k, yy + G, x + G) * __ldg(a.rgzv + (size_t)yy * ni + x));
     }
 }
@@ -222,10 +254,12 @@ __global__ void __launch_bounds__(128) mom5_mass_kernel(MomArgs a) {
 // rrw at level k (2..nk) of cell (j, i); 0 at levels 1 and nk+1
 __device__ __forceinline__ float rrw_value(const MomArgs &a, int k, int j, int i) {
     if (k <= 1 || k >= a.nk + 1) return 0.0f;
-    const float zt = (float)a.nk * a.dz, rzt = 1.0f / zt, rdz0 = 1.0f / a.dz;
-    const float sigmaf = (float)(k - 1) * a.dz;
-    const float sigma = ((float)k - 1.5f) * a.dz;
-    float r2 = (sigmaf - sigma) * rdz0;
+    if (a.vmode == 2) return __ldg(a.rf0 + ic(a, k - 1, 0, 0)) * LW(k, j + G, i + G);
+    const bool pr = a.vmode == 1;
+    const float zt = pr ? a.ztop : (float)a.nk * a.dz, rzt = 1.0f / zt, rdz0 = 1.0f / a.dz;
+    const float sigmaf = pr ? __ldg(a.sigmaf + k) : (float)(k - 1) * a.dz;
+    const float sigma = pr ? __ldg(a.sigma + k - 1) : ((float)k - 1.5f) * a.dz;
+    float r2 = (sigmaf - sigma) * (pr ? __ldg(a.rds + k) : rdz0);
     const float r1 = 0.5f * (1.0f - r2);
     r2 = 0.5f * r2;
     const int y = j + G, x = i + G;
@@ -248,7 +282,12 @@ __global__ void __launch_bounds__(128) mom5_rrw_divx_kernel(MomArgs a) {
     RW(k, y, x) = lo;
     if (k == a.nk) RW(k + 1, y, x) = hi;
     float value = (RU(k, y, x + 1) - RU(k, y, x)) * a.rdx + (RV(k, y + 1, x) - RV(k, y, x)) * a.rdy;
-    value = value + (hi - lo) * a.rdz;
+    if (a.vmode == 2) {  // the flat column's ((d*rdz)*mh(k)) with cm1.F's smeps 1e-30
+        value = value + ((hi - lo) * a.rdzm) * __ldg(a.mh + k);
+        a.divx[ic(a, k0, j, i)] = fabsf(value) < 1.0e-30f ? 0.0f : value;
+        return;
+    }
+    value = value + (hi - lo) * (a.vmode == 1 ? __ldg(a.rdsf + k) : a.rdz);
     a.divx[ic(a, k0, j, i)] = fabsf(value) < 1.0e-20f ? 0.0f : value;
 }
 
@@ -268,23 +307,24 @@ __global__ void __launch_bounds__(128) mom5_adv_kernel(MomArgs a) {
             const float m = RV(k, G, east + G) + RV(k, G, west + G);
             if (m >= 0.0f) {
                 const float corr = (RV(k, G + 1, west + G) - RV(k, G, west + G)) + (RV(k, G + 1, east + G) - RV(k, G, east + G));
-                advy = advy - (uc * 0.5f) * (corr * (a.rdy * __ldg(a.vh + y)));
+                advy = advy - bcorr(a, uc * 0.5f, corr, a.rdy, __ldg(a.vh + y));
             }
         } else if (j == nj - 1 && a.opn[3]) {
             const float m = RV(k, G + nj, east + G) + RV(k, G + nj, west + G);
             if (m <= 0.0f) {
                 const float corr = (RV(k, y + 1, west + G) - RV(k, y, west + G)) + (RV(k, y + 1, east + G) - RV(k, y, east + G));
-                advy = advy - (uc * 0.5f) * (corr * (a.rdy * __ldg(a.vh + y)));
+                advy = advy - bcorr(a, uc * 0.5f, corr, a.rdy, __ldg(a.vh + y));
             }
         }
         float advz;
-        if (k == 1) advz = -uv_z(a, true, 2, j, f) * a.rdz;
-        else if (k == nk) advz = uv_z(a, true, nk, j, f) * a.rdz;
-        else advz = -(uv_z(a, true, k + 1, j, f) - uv_z(a, true, k, j, f)) * a.rdz;
+        if (k == 1) advz = zmass(a, -uv_z(a, true, 2, j, f), k);
+        else if (k == nk) advz = zmass(a, uv_z(a, true, nk, j, f), k);
+        else advz = zmass(a, -(uv_z(a, true, k + 1, j, f) - uv_z(a, true, k, j, f)), k);
         float total = (advx + advy) + advz;
         total = total + uc * (0.5f * (a.divx[ic(a, k0, j, east)] + a.divx[ic(a, k0, j, west)]));
-        const float scale = __ldg(a.gzu + (size_t)j * (ni + 1) + f) /
-                            (0.5f * (__ldg(a.rho0 + ic(a, k0, j, west)) + __ldg(a.rho0 + ic(a, k0, j, east))));
+        const float scale = a.vmode == 2 ? __ldg(a.rr0 + ic(a, k0, 0, 0))
+                                         : __ldg(a.gzu + (size_t)j * (ni + 1) + f) /
+                                               (0.5f * (__ldg(a.rho0 + ic(a, k0, j, west)) + __ldg(a.rho0 + ic(a, k0, j, east))));
         const unsigned p = iu(a, k, y, x);
         a.uten[p] = a.uten[p] + total * scale;
     }
@@ -299,63 +339,66 @@ __global__ void __launch_bounds__(128) mom5_adv_kernel(MomArgs a) {
             const float m = RU(k, north + G, G) + RU(k, south + G, G);
             if (m >= 0.0f) {
                 const float corr = (RU(k, south + G, G + 1) - RU(k, south + G, G)) + (RU(k, north + G, G + 1) - RU(k, north + G, G));
-                advx = advx - (vc * 0.5f) * (corr * (a.rdx * __ldg(a.uh + G)));
+                advx = advx - bcorr(a, vc * 0.5f, corr, a.rdx, __ldg(a.uh + G));
             }
         } else if (i == ni - 1 && a.opn[1]) {
             const float m = RU(k, north + G, G + ni) + RU(k, south + G, G + ni);
             if (m <= 0.0f) {
                 const float corr = (RU(k, south + G, x + 1) - RU(k, south + G, x)) + (RU(k, north + G, x + 1) - RU(k, north + G, x));
-                advx = advx - (vc * 0.5f) * (corr * (a.rdx * __ldg(a.uh + x)));
+                advx = advx - bcorr(a, vc * 0.5f, corr, a.rdx, __ldg(a.uh + x));
             }
         }
         float advz;
-        if (k == 1) advz = -uv_z(a, false, 2, g, i) * a.rdz;
-        else if (k == nk) advz = uv_z(a, false, nk, g, i) * a.rdz;
-        else advz = -(uv_z(a, false, k + 1, g, i) - uv_z(a, false, k, g, i)) * a.rdz;
+        if (k == 1) advz = zmass(a, -uv_z(a, false, 2, g, i), k);
+        else if (k == nk) advz = zmass(a, uv_z(a, false, nk, g, i), k);
+        else advz = zmass(a, -(uv_z(a, false, k + 1, g, i) - uv_z(a, false, k, g, i)), k);
         float total = (advx + advy) + advz;
         total = total + vc * (0.5f * (a.divx[ic(a, k0, north, i)] + a.divx[ic(a, k0, south, i)]));
-        const float scale = __ldg(a.gzv + (size_t)g * ni + i) /
-                            (0.5f * (__ldg(a.rho0 + ic(a, k0, south, i)) + __ldg(a.rho0 + ic(a, k0, north, i))));
+        const float scale = a.vmode == 2 ? __ldg(a.rr0 + ic(a, k0, 0, 0))
+                                         : __ldg(a.gzv + (size_t)g * ni + i) /
+                                               (0.5f * (__ldg(a.rho0 + ic(a, k0, south, i)) + __ldg(a.rho0 + ic(a, k0, north, i))));
         const unsigned p = iv(a, k, y, x);
         a.vten[p] = a.vten[p] + total * scale;
     }
     // advw at Fortran face kf = k + 1 (2..nk) of column (yy, xx)
     if (xx < ni && yy < nj && k < nk) {
         const int kf = k + 1, j = yy, i = xx, y = j + G, x = i + G;
-        float advx = -(w_fx(a, kf, j, i + 1) - w_fx(a, kf, j, i)) * (a.rdx * __ldg(a.uh + x));
-        float advy = -(w_fy(a, kf, j + 1, i) - w_fy(a, kf, j, i)) * (a.rdy * __ldg(a.vh + y));
+        const float dfx = -(w_fx(a, kf, j, i + 1) - w_fx(a, kf, j, i)), dfy = -(w_fy(a, kf, j + 1, i) - w_fy(a, kf, j, i));
+        float advx = a.vmode == 2 ? (dfx * a.rdx) * __ldg(a.uh + x) : dfx * (a.rdx * __ldg(a.uh + x));
+        float advy = a.vmode == 2 ? (dfy * a.rdy) * __ldg(a.vh + y) : dfy * (a.rdy * __ldg(a.vh + y));
         const float c2 = __ldg(a.c2 + ic(a, kf - 1, j, i)), c1 = 1.0f - c2;
         const float wc = LW(kf, y, x);
         if (i == 0 && a.opn[0]) {
             const float m = c2 * RU(kf, y, G) + c1 * RU(kf - 1, y, G);
             if (m >= 0.0f) {
                 const float corr = c1 * (RU(kf - 1, y, G + 1) - RU(kf - 1, y, G)) + c2 * (RU(kf, y, G + 1) - RU(kf, y, G));
-                advx = advx - wc * (corr * (a.rdx * __ldg(a.uh + x)));
+                advx = advx - bcorr(a, wc, corr, a.rdx, __ldg(a.uh + x));
             }
         } else if (i == ni - 1 && a.opn[1]) {
             const float m = c2 * RU(kf, y, G + ni) + c1 * RU(kf - 1, y, G + ni);
             if (m <= 0.0f) {
                 const float corr = c1 * (RU(kf - 1, y, x + 1) - RU(kf - 1, y, x)) + c2 * (RU(kf, y, x + 1) - RU(kf, y, x));
-                advx = advx - wc * (corr * (a.rdx * __ldg(a.uh + x)));
+                advx = advx - bcorr(a, wc, corr, a.rdx, __ldg(a.uh + x));
             }
         }
         if (j == 0 && a.opn[2]) {
             const float m = c2 * RV(kf, G, x) + c1 * RV(kf - 1, G, x);
             if (m >= 0.0f) {
                 const float corr = c1 * (RV(kf - 1, G + 1, x) - RV(kf - 1, G, x)) + c2 * (RV(kf, G + 1, x) - RV(kf, G, x));
-                advy = advy - wc * (corr * (a.rdy * __ldg(a.vh + y)));
+                advy = advy - bcorr(a, wc, corr, a.rdy, __ldg(a.vh + y));
             }
         } else if (j == nj - 1 && a.opn[3]) {
             const float m = c2 * RV(kf, G + nj, x) + c1 * RV(kf - 1, G + nj, x);
             if (m <= 0.0f) {
                 const float corr = c1 * (RV(kf - 1, y + 1, x) - RV(kf - 1, y, x)) + c2 * (RV(kf, y + 1, x) - RV(kf, y, x));
-                advy = advy - wc * (corr * (a.rdy * __ldg(a.vh + y)));
+                advy = advy - bcorr(a, wc, corr, a.rdy, __ldg(a.vh + y));
             }
         }
-        const float advz = -(w_z(a, kf, j, i) - w_z(a, kf - 1, j, i)) * a.rdz;
+        const float advz = zface(a, -(w_z(a, kf, j, i) - w_z(a, kf - 1, j, i)), kf);
         float total = (advx + advy) + advz;
         total = total + wc * (c2 * a.divx[ic(a, kf - 1, j, i)] + c1 * a.divx[ic(a, kf - 2, j, i)]);
-        const float scale = __ldg(a.rrf0 + ic(a, kf - 1, j, i)) * __ldg(a.gz + (size_t)j * ni + i);
+        const float scale = a.vmode == 2 ? __ldg(a.rrf0 + ic(a, kf - 1, 0, 0))
+                                         : __ldg(a.rrf0 + ic(a, kf - 1, j, i)) * __ldg(a.gz + (size_t)j * ni + i);
         const unsigned p = iw(a, kf, y, x);
         a.wten[p] = a.wten[p] + total * scale;
     }
@@ -380,6 +423,9 @@ namespace {
 
 int mom_args(int ni, int nj, int nk, const gm1b_momentum5_arrays *s, uint32_t lateral_obc, float dx, float dy,
              float dz, MomArgs &a, const char *what) {
+    a.vmode = 0;
+    a.rho0p = a.sigma = a.sigmaf = a.rds = a.rdsf = a.mh = a.mf = a.rr0 = nullptr;
+    a.ztop = a.rdzm = 0.0f;
     if (s == nullptr || ni < 7 || nj < 7 || nk < 8) {
         gm1b_set_error("%s: need arrays, ni >= 7, nj >= 7, nk >= 8", what);
         return GM1B_ERR_ARGUMENT;
@@ -495,6 +541,64 @@ extern "C" int32_t gm1b_momentum_advection5(int32_t ni, int32_t nj, int32_t nk, 
                                             uint32_t lateral_obc, float dx, float dy, float dz, void *stream) {
     MomArgs a;
     const int r = mom_args(ni, nj, nk, s, lateral_obc, dx, dy, dz, a, "gm1b_momentum_advection5");
+    if (r != GM1B_OK) return r;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int m = enqueue_mass(a, st);
+    return m != GM1B_OK ? m : enqueue_transport(a, st);
+}
+
+// ---------------------------------------------------------------------------
+// the same operator on a stretched column (launch_cuda_gm1_child_stretched_momentum5,
+// src/cm1core/cuda_gm1_child_stretched_momentum.py:540-780): terrain branch
+// (rdsf / rds / sigma / sigmaf and the physical top) or flat column
+// (rdz*mh / rdz*mf and the column's base state)
+// ---------------------------------------------------------------------------
+namespace {
+int column_args(int ni, int nj, int nk, const gm1b_momentum5_arrays *s, uint32_t lateral_obc, float dx, float dy,
+                const gm1b_momentum_column *c, MomArgs &a, const char *what) {
+    if (c == nullptr || (c->flat != 0 && c->flat != 1) || c->rho0_padded == nullptr) {
+        gm1b_set_error("%s: need a column with flat = 0 or 1 and the padded base density", what);
+        return GM1B_ERR_ARGUMENT;
+    }
+    if (c->flat ? (c->mh == nullptr || c->mf == nullptr || c->rr0 == nullptr || !(c->rdz > 0.0f) ||
+                   !isfinite(c->rdz))
+                : (c->sigma == nullptr || c->sigmaf == nullptr || c->rds == nullptr || c->rdsf == nullptr ||
+                   !(c->ztop > 0.0f) || !isfinite(c->ztop))) {
+        gm1b_set_error("%s: a flat column needs mh, mf, rr0 and rdz > 0; a terrain column sigma, sigmaf, rds, rdsf "
+                       "and ztop > 0", what);
+        return GM1B_ERR_ARGUMENT;
+    }
+    // dz forms only the uniform reciprocals, which a stretched column never reads
+    const int r = mom_args(ni, nj, nk, s, lateral_obc, dx, dy, 1.0f, a, what);
+    if (r != GM1B_OK) return r;
+    a.vmode = c->flat ? 2 : 1;
+    a.rho0p = c->rho0_padded, a.sigma = c->sigma, a.sigmaf = c->sigmaf, a.rds = c->rds, a.rdsf = c->rdsf;
+    a.mh = c->mh, a.mf = c->mf, a.rr0 = c->rr0, a.ztop = c->ztop, a.rdzm = c->rdz;
+    return GM1B_OK;
+}
+}  // namespace
+
+extern "C" int32_t gm1b_momentum_mass_flux5_column(int32_t ni, int32_t nj, int32_t nk, const gm1b_momentum5_arrays *s,
+                                                   uint32_t lateral_obc, float dx, float dy,
+                                                   const gm1b_momentum_column *column, void *stream) {
+    MomArgs a;
+    const int r = column_args(ni, nj, nk, s, lateral_obc, dx, dy, column, a, "gm1b_momentum_mass_flux5_column");
+    return r != GM1B_OK ? r : enqueue_mass(a, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int32_t gm1b_momentum_transport5_column(int32_t ni, int32_t nj, int32_t nk, const gm1b_momentum5_arrays *s,
+                                                   uint32_t lateral_obc, float dx, float dy,
+                                                   const gm1b_momentum_column *column, void *stream) {
+    MomArgs a;
+    const int r = column_args(ni, nj, nk, s, lateral_obc, dx, dy, column, a, "gm1b_momentum_transport5_column");
+    return r != GM1B_OK ? r : enqueue_transport(a, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int32_t gm1b_momentum_advection5_column(int32_t ni, int32_t nj, int32_t nk, const gm1b_momentum5_arrays *s,
+                                                   uint32_t lateral_obc, float dx, float dy,
+                                                   const gm1b_momentum_column *column, void *stream) {
+    MomArgs a;
+    const int r = column_args(ni, nj, nk, s, lateral_obc, dx, dy, column, a, "gm1b_momentum_advection5_column");
     if (r != GM1B_OK) return r;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const int m = enqueue_mass(a, st);

@@ -125,12 +125,45 @@ class CudaMomentumAdvection5Launch:
     receipt: dict[str, Any]
 
 
+class _Column(ctypes.Structure):
+    _fields_ = [("flat", ctypes.c_int32), ("rho0_padded", ctypes.c_void_p), ("sigma", ctypes.c_void_p),
+                ("sigmaf", ctypes.c_void_p), ("rds", ctypes.c_void_p), ("rdsf", ctypes.c_void_p),
+                ("ztop", ctypes.c_float), ("mh", ctypes.c_void_p), ("mf", ctypes.c_void_p), ("rr0", ctypes.c_void_p),
+                ("rdz", ctypes.c_float)]
+
+
+@dataclass(frozen=True)
+class StretchedMomentumColumn:
+    """The vertical column of the stretched momentum operator (the profiles
+    the reference binds from its Gm1ChildStretchedMetrics): ``rho0_padded`` the
+    (nk+2, nj+6, ni+6) base density; terrain branch (``flat=False``) with
+    ``sigma`` (nk+2), ``sigmaf`` (nk+3), ``rds`` (nk+2), ``rdsf`` (nk+3) and the
+    physical top ``ztop``; flat column (``flat=True``) with ``mh`` (nk+2),
+    ``mf`` (nk+3), ``rr0`` (nk, nj, ni) and ``rdz``."""
+
+    flat: bool
+    rho0_padded: Any
+    sigma: Any = None
+    sigmaf: Any = None
+    rds: Any = None
+    rdsf: Any = None
+    ztop: float = 0.0
+    mh: Any = None
+    mf: Any = None
+    rr0: Any = None
+    rdz: float = 0.0
+
+
 def _lib():
     lib = _native.lib()
     if not getattr(lib, "_mom5_bound", False):
         i32, u32, f32, vp = ctypes.c_int32, ctypes.c_uint32, ctypes.c_float, ctypes.c_void_p
         for fn in (lib.gm1b_momentum_advection5, lib.gm1b_momentum_mass_flux5, lib.gm1b_momentum_transport5):
             fn.argtypes = [i32, i32, i32, ctypes.POINTER(_Arrays), u32, f32, f32, f32, vp]
+            fn.restype = i32
+        for fn in (lib.gm1b_momentum_advection5_column, lib.gm1b_momentum_mass_flux5_column,
+                   lib.gm1b_momentum_transport5_column):
+            fn.argtypes = [i32, i32, i32, ctypes.POINTER(_Arrays), u32, f32, f32, ctypes.POINTER(_Column), vp]
             fn.restype = i32
         lib._mom5_bound = True
     return lib
@@ -239,4 +272,82 @@ def launch_cuda_terrain_open_momentum_advection5(
         receipt["rrw_open_boundary"] = dict(rrw_receipt)
     if post_receipt is not None:
         receipt["post_divergence"] = dict(post_receipt)
+    return CudaMomentumAdvection5Launch(divx, ev, receipt)
+
+
+def launch_cuda_gm1_child_stretched_momentum5(
+        arrays: Mapping[str, Any], metrics: Mapping[str, Any], vertical: StretchedMomentumColumn, *, ni: int, nj: int,
+        nk: int, nrk: int, dx: float, dy: float, divx: Any | None = None, stream: Any | None = None,
+        rrw_boundary_hook: Any | None = None,
+        lateral_sides: tuple[int, int, int, int] = MOMENTUM_ALL_OPEN_SIDES) -> CudaMomentumAdvection5Launch:
+    """The momentum advection on a stretched column
+    (launch_cuda_gm1_child_stretched_momentum5,
+    src/cm1core/cuda_gm1_child_stretched_momentum.py:540): terrain branch
+    (rdsf / rds / sigma / sigmaf, the physical top) or flat column
+    (rdz*mh / rdz*mf and the column's base state).  ``rrw_boundary_hook``
+    runs between the mass fluxes and the transport (a terrain-branch
+    bcw(rrw,0); a flat column takes none)."""
+    if not isinstance(vertical, StretchedMomentumColumn):
+        raise TypeError("vertical must be a StretchedMomentumColumn")
+    if vertical.flat and rrw_boundary_hook is not None:
+        raise ValueError("solve2.F:575's bcw(rrw,0) is a terrain statement: a flat column takes no rrw hook")
+    lateral_sides = momentum_lateral_sides(lateral_sides)
+    obc = momentum_open_boundary_code(lateral_sides)
+    ni = _positive_int("ni", ni, 7)
+    nj = _positive_int("nj", nj, 7)
+    nk = _positive_int("nk", nk, 8)
+    if isinstance(nrk, bool) or not isinstance(nrk, int) or nrk not in (1, 2, 3):
+        raise ValueError("nrk must be an integer in 1..3")
+    dx, dy = (_spacing(n, v) for n, v in (("dx", dx), ("dy", dy)))
+    shapes = momentum_advection5_shapes(ni, nj, nk)
+    a = {n: _require_cuda(arrays[n], n, shapes[n]) for n in _STATE}
+    m = {n: _require_cuda(metrics[n], n, shapes[n]) for n in _METRICS}
+    device = a["u3d"].device
+    divx = torch.empty((nk, nj, ni), dtype=torch.float32, device=device) if divx is None else \
+        _require_cuda(divx, "divx", (nk, nj, ni))
+    rho0p = _require_cuda(vertical.rho0_padded, "rho0_padded", (nk + 2, nj + 6, ni + 6))
+    prof = {}
+    if vertical.flat:
+        for n, shape in (("mh", (nk + 2,)), ("mf", (nk + 3,)), ("rr0", (nk, nj, ni))):
+            prof[n] = _require_cuda(getattr(vertical, n), n, shape)
+        rdz = float(vertical.rdz)
+        if not (math.isfinite(rdz) and rdz > 0.0):
+            raise ValueError("a flat column needs rdz > 0")
+        col = _Column(1, rho0p.data_ptr(), None, None, None, None, 0.0, prof["mh"].data_ptr(), prof["mf"].data_ptr(),
+                      prof["rr0"].data_ptr(), rdz)
+    else:
+        for n, shape in (("sigma", (nk + 2,)), ("sigmaf", (nk + 3,)), ("rds", (nk + 2,)), ("rdsf", (nk + 3,))):
+            prof[n] = _require_cuda(getattr(vertical, n), n, shape)
+        ztop = float(vertical.ztop)
+        if not (math.isfinite(ztop) and ztop > 0.0):
+            raise ValueError("a terrain column needs its physical top ztop > 0")
+        col = _Column(0, rho0p.data_ptr(), prof["sigma"].data_ptr(), prof["sigmaf"].data_ptr(),
+                      prof["rds"].data_ptr(), prof["rdsf"].data_ptr(), ztop, None, None, None, 0.0)
+    mutable = [a[n] for n in _WRITABLE] + [divx]
+    others = [a[n] for n in _STATE if n not in _WRITABLE] + list(m.values()) + [rho0p] + list(prof.values())
+    for i, t in enumerate(mutable):
+        lo, hi = _spans(t)
+        for o in mutable[i + 1:] + others:
+            olo, ohi = _spans(o)
+            if lo < ohi and olo < hi:
+                raise ValueError("stretched momentum mutable arrays, metrics and profiles must not alias")
+    lib = _lib()
+    st = torch.cuda.current_stream(device) if stream is None else stream
+    s = _Arrays(**{n: (divx if n == "divx" else a[n] if n in a else m[n]).data_ptr() for n in _STRUCT})
+    args = (ni, nj, nk, ctypes.byref(s), obc, dx, dy, ctypes.byref(col), ctypes.c_void_p(st.cuda_stream))
+    rrw_receipt = None
+    with torch.cuda.device(device), torch.cuda.stream(st):
+        if rrw_boundary_hook is None:
+            _native.check(lib.gm1b_momentum_advection5_column(*args), "gm1b_momentum_advection5_column")
+        else:
+            _native.check(lib.gm1b_momentum_mass_flux5_column(*args), "gm1b_momentum_mass_flux5_column")
+            rrw_receipt = rrw_boundary_hook(a["rrw"], stream=st, ni=ni, nj=nj, nk=nk)
+            _native.check(lib.gm1b_momentum_transport5_column(*args), "gm1b_momentum_transport5_column")
+        ev = torch.cuda.Event()
+        ev.record(st)
+    receipt: dict[str, Any] = {"terrain": not vertical.flat, "stretch_z": 1, "nrk": nrk,
+                               "lateral_boundaries": list(lateral_sides), "domain": {"ni": ni, "nj": nj, "nk": nk},
+                               "launches": 3}
+    if rrw_receipt is not None:
+        receipt["rrw_open_boundary"] = dict(rrw_receipt)
     return CudaMomentumAdvection5Launch(divx, ev, receipt)

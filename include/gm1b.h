@@ -434,6 +434,37 @@ typedef struct gm1b_momentum5_arrays {
 GM1B_API int32_t gm1b_momentum_advection5(int32_t ni, int32_t nj, int32_t nk, const gm1b_momentum5_arrays *arrays,
                                           uint32_t lateral_obc, float dx, float dy, float dz, void *stream);
 
+/*
+ * The momentum advection on a stretched column
+ * (launch_cuda_gm1_child_stretched_momentum5,
+ * src/cm1core/cuda_gm1_child_stretched_momentum.py:540-780).  flat = 0: CM1's
+ * terrain branch with the column's sigma (nk+2), sigmaf (nk+3), rds (nk+2)
+ * and rdsf (nk+3) profiles, the physical top ztop and the base density from
+ * rho0_padded ((nk+2, nj+6, ni+6)); flat = 1: the flat column
+ * (solve2.F:493-520, 605-617; adv.F's rdz*mh / rdz*mf statements) with mh
+ * (nk+2), mf (nk+3), rdz, and the column's rho0_padded(k, 3, 3), rf0, rr0 and
+ * rrf0 words.  The split entries place a hook (an rrw fill) between the mass
+ * fluxes and the transport as the uniform ones do.
+ */
+typedef struct gm1b_momentum_column {
+    int32_t flat;
+    const float *rho0_padded;
+    const float *sigma, *sigmaf, *rds, *rdsf; /* flat = 0 */
+    float ztop;                               /* flat = 0 */
+    const float *mh, *mf, *rr0;               /* flat = 1 (rr0 compact (nk, nj, ni)) */
+    float rdz;                                /* flat = 1 */
+} gm1b_momentum_column;
+
+GM1B_API int32_t gm1b_momentum_advection5_column(int32_t ni, int32_t nj, int32_t nk, const gm1b_momentum5_arrays *s,
+                                                 uint32_t lateral_obc, float dx, float dy,
+                                                 const gm1b_momentum_column *column, void *stream);
+GM1B_API int32_t gm1b_momentum_mass_flux5_column(int32_t ni, int32_t nj, int32_t nk, const gm1b_momentum5_arrays *s,
+                                                 uint32_t lateral_obc, float dx, float dy,
+                                                 const gm1b_momentum_column *column, void *stream);
+GM1B_API int32_t gm1b_momentum_transport5_column(int32_t ni, int32_t nj, int32_t nk, const gm1b_momentum5_arrays *s,
+                                                 uint32_t lateral_obc, float dx, float dy,
+                                                 const gm1b_momentum_column *column, void *stream);
+
 /* ------------------------------------------------------------------------
  * Terrain + all-open psolver=3 acoustic RK stage (padded ng = 3 lane).
  * Replaces launch_cuda_psolver3_terrain_open_stage / _three_stage

@@ -55,3 +55,32 @@ def momentum_advection5_phase(a, *, ni, nj, nk, dx, dy, dz, lateral_sides=(2, 2,
     sides = (ctypes.c_int * 4)(*lateral_sides)
     if lib.oracle_momentum_advection5_phase(ni, nj, nk, ctypes.byref(s), sides, dx, dy, dz, phase) != 0:
         raise ValueError("oracle_momentum_advection5_phase failed")
+
+
+COLUMN_PROFILES = ("rho0p", "sigma", "sigmaf", "rds", "rdsf", "mh", "mf", "rr0")
+
+
+def momentum_advection5_column(a, column, *, ni, nj, nk, dx, dy, lateral_sides=(2, 2, 2, 2), phase=3) -> None:
+    """The operator on a stretched column.  ``column`` holds ``flat`` and the
+    profiles: rho0p (padded base density), and sigma/sigmaf/rds/rdsf/ztop
+    (terrain branch) or mh/mf/rr0/rdz (flat column)."""
+    s = MomArrays()
+    for n in NAMES:
+        setattr(s, n, a[n].ctypes.data_as(_F))
+    lib = _lib()
+    if not getattr(lib, "_mom_column_ready", False):
+        lib.oracle_momentum_advection5_column_phase.argtypes = (
+            [ctypes.c_int] * 3 + [ctypes.POINTER(MomArrays), ctypes.POINTER(ctypes.c_int), ctypes.c_float,
+                                  ctypes.c_float, ctypes.c_int, ctypes.c_int] + [_F] * 5 + [ctypes.c_float] +
+            [_F] * 3 + [ctypes.c_float])
+        lib.oracle_momentum_advection5_column_phase.restype = ctypes.c_int
+        lib._mom_column_ready = True
+    keep = {n: np.ascontiguousarray(column[n], dtype=np.float32) for n in COLUMN_PROFILES if column.get(n) is not None}
+    ptr = {n: (keep[n].ctypes.data_as(_F) if n in keep else None) for n in COLUMN_PROFILES}
+    sides = (ctypes.c_int * 4)(*lateral_sides)
+    rc = lib.oracle_momentum_advection5_column_phase(
+        ni, nj, nk, ctypes.byref(s), sides, dx, dy, phase, 1 if column["flat"] else 0, ptr["rho0p"], ptr["sigma"],
+        ptr["sigmaf"], ptr["rds"], ptr["rdsf"], float(column.get("ztop", 0.0)), ptr["mh"], ptr["mf"], ptr["rr0"],
+        float(column.get("rdz", 0.0)))
+    if rc != 0:
+        raise ValueError("oracle_momentum_advection5_column_phase failed")

@@ -30,6 +30,13 @@ typedef struct {
   int ni, nj, nk;
   int side[4];
   const mom_arrays* a;
+  /* vertical column: 0 uniform; 1 terrain branch on a stretched column
+   * (sigma/sigmaf/rds/rdsf, ztop, padded base density); 2 flat column
+   * (rdz*mh / rdz*mf, the column's base state) -
+   * cuda_gm1_child_stretched_momentum.py:56-330 */
+  int vmode;
+  const float *rho0p, *sigma, *sigmaf, *rds, *rdsf, *mh, *mf, *rr0;
+  float ztop, rdzm;
 } mom_ctx;
 
 #define UX(c) ((c)->ni + 1 + 2 * NG)
@@ -244,12 +251,24 @@ static float w_z(const mom_ctx* c, int k, int j, int i) {
   return mass * r;
 }
 
+#define P_(c, p, k, y, x) (p)[(((int64_t)(k)) * UY(c) + (y)) * VX(c) + (x)]
+
+static float zmass(const mom_ctx* c, float x, int k, float rdz) {
+  if (c->vmode == 2) return (x * c->rdzm) * c->mh[k];
+  return x * (c->vmode == 1 ? c->rdsf[k] : rdz);
+}
+static float zface(const mom_ctx* c, float x, int kf, float rdz) {
+  if (c->vmode == 2) return (x * c->rdzm) * c->mf[kf];
+  return x * (c->vmode == 1 ? c->rds[kf] : rdz);
+}
+static float bcorr(const mom_ctx* c, float q, float cr, float r, float h) {
+  return c->vmode == 2 ? ((q * cr) * r) * h : q * (cr * (r * h));
+}
+
 /* phase bit 1: mass fluxes and divx; bit 2: advu/advv/advw from them */
-int oracle_momentum_advection5_phase(int ni, int nj, int nk, const mom_arrays* a, const int* sides, float dx,
-                                     float dy, float dz, int phase) {
-  if (ni < 7 || nj < 7 || nk < 8) return -1;
-  mom_ctx cc = {ni, nj, nk, {sides[0], sides[1], sides[2], sides[3]}, a};
-  const mom_ctx* c = &cc;
+static int mom_phase(const mom_ctx* c, float dx, float dy, float dz, int phase) {
+  const int ni = c->ni, nj = c->nj, nk = c->nk;
+  const mom_arrays* a = c->a;
   const float half = 0.5f;
   if (phase & 1) {
   /* horizontal mass fluxes on every face */
@@ -258,8 +277,13 @@ int oracle_momentum_advection5_phase(int ni, int nj, int nk, const mom_arrays* a
     for (int j = 0; j < nj; ++j) {
       const int y = j + NG;
       for (int face = 0; face <= ni; ++face) {
+        if (c->vmode == 2) {
+          U_(c, a->rru, k, y, face + NG) = P_(c, c->rho0p, k, NG, NG) * U_(c, a->u3d, k, y, face + NG);
+          continue;
+        }
         const int l = face - 1 < 0 ? 0 : face - 1, r = face < ni - 1 ? face : ni - 1;
-        const float density = C3(c, a->rho0_3d, k0, j, l) + C3(c, a->rho0_3d, k0, j, r);
+        const float density = c->vmode == 1 ? P_(c, c->rho0p, k, y, face + NG - 1) + P_(c, c->rho0p, k, y, face + NG)
+                                            : C3(c, a->rho0_3d, k0, j, l) + C3(c, a->rho0_3d, k0, j, r);
         U_(c, a->rru, k, y, face + NG) = (half * density) * (U_(c, a->u3d, k, y, face + NG) * a->rgzu[(int64_t)j * (ni + 1) + face]);
       }
     }
@@ -267,7 +291,12 @@ int oracle_momentum_advection5_phase(int ni, int nj, int nk, const mom_arrays* a
       const int s = face - 1 < 0 ? 0 : face - 1, n = face < nj - 1 ? face : nj - 1;
       const int y = face + NG;
       for (int i = 0; i < ni; ++i) {
-        const float density = C3(c, a->rho0_3d, k0, s, i) + C3(c, a->rho0_3d, k0, n, i);
+        if (c->vmode == 2) {
+          V_(c, a->rrv, k, y, i + NG) = P_(c, c->rho0p, k, NG, NG) * V_(c, a->v3d, k, y, i + NG);
+          continue;
+        }
+        const float density = c->vmode == 1 ? P_(c, c->rho0p, k, y - 1, i + NG) + P_(c, c->rho0p, k, y, i + NG)
+                                            : C3(c, a->rho0_3d, k0, s, i) + C3(c, a->rho0_3d, k0, n, i);
         V_(c, a->rrv, k, y, i + NG) = (half * density) * (V_(c, a->v3d, k, y, i + NG) * a->rgzv[(int64_t)face * ni + i]);
       }
     }
@@ -278,11 +307,17 @@ int oracle_momentum_advection5_phase(int ni, int nj, int nk, const mom_arrays* a
       W_(c, a->rrw, 1, j + NG, i + NG) = 0.0f;
       W_(c, a->rrw, nk + 1, j + NG, i + NG) = 0.0f;
     }
-  const float zt = (float)nk * dz, rzt = 1.0f / zt, rdz0 = 1.0f / dz;
+  const float zt = c->vmode == 1 ? c->ztop : (float)nk * dz, rzt = 1.0f / zt, rdz0 = 1.0f / dz;
   for (int k = 2; k <= nk; ++k) {
-    const float sigmaf = (float)(k - 1) * dz;
-    const float sigma = (float)((double)k - 1.5) * dz;
-    float r2 = (sigmaf - sigma) * rdz0;
+    if (c->vmode == 2) {
+      for (int j = 0; j < nj; ++j)
+        for (int i = 0; i < ni; ++i)
+          W_(c, a->rrw, k, j + NG, i + NG) = a->rf0[(int64_t)(k - 1) * nj * ni] * W_(c, a->w3d, k, j + NG, i + NG);
+      continue;
+    }
+    const float sigmaf = c->vmode == 1 ? c->sigmaf[k] : (float)(k - 1) * dz;
+    const float sigma = c->vmode == 1 ? c->sigma[k - 1] : (float)((double)k - 1.5) * dz;
+    float r2 = (sigmaf - sigma) * (c->vmode == 1 ? c->rds[k] : rdz0);
     const float r1 = half * (1.0f - r2);
     r2 = half * r2;
     for (int j = 0; j < nj; ++j) {
@@ -309,8 +344,8 @@ int oracle_momentum_advection5_phase(int ni, int nj, int nk, const mom_arrays* a
         const int y = j + NG, x = i + NG;
         float value = (U_(c, a->rru, k, y, x + 1) - U_(c, a->rru, k, y, x)) * rdx +
                       (V_(c, a->rrv, k, y + 1, x) - V_(c, a->rrv, k, y, x)) * rdy;
-        value = value + (W_(c, a->rrw, k + 1, y, x) - W_(c, a->rrw, k, y, x)) * rdz;
-        C3(c, a->divx, k0, j, i) = fabsf(value) < 1.0e-20f ? 0.0f : value;
+        value = value + zmass(c, W_(c, a->rrw, k + 1, y, x) - W_(c, a->rrw, k, y, x), k, rdz);
+        C3(c, a->divx, k0, j, i) = fabsf(value) < (c->vmode == 2 ? 1.0e-30f : 1.0e-20f) ? 0.0f : value;
       }
   }
   }
@@ -333,24 +368,25 @@ int oracle_momentum_advection5_phase(int ni, int nj, int nk, const mom_arrays* a
           if (mass >= 0.0f) {
             const float corr = (V_(c, a->rrv, k, NG + 1, west + NG) - V_(c, a->rrv, k, NG, west + NG)) +
                                (V_(c, a->rrv, k, NG + 1, east + NG) - V_(c, a->rrv, k, NG, east + NG));
-            advy = advy - (uc * half) * (corr * (rdy * a->vh[y]));
+            advy = advy - bcorr(c, uc * half, corr, rdy, a->vh[y]);
           }
         } else if (j == nj - 1 && opn(c, 3)) {
           const float mass = V_(c, a->rrv, k, NG + nj, east + NG) + V_(c, a->rrv, k, NG + nj, west + NG);
           if (mass <= 0.0f) {
             const float corr = (V_(c, a->rrv, k, y + 1, west + NG) - V_(c, a->rrv, k, y, west + NG)) +
                                (V_(c, a->rrv, k, y + 1, east + NG) - V_(c, a->rrv, k, y, east + NG));
-            advy = advy - (uc * half) * (corr * (rdy * a->vh[y]));
+            advy = advy - bcorr(c, uc * half, corr, rdy, a->vh[y]);
           }
         }
         float advz;
-        if (k == 1) advz = -uv_z(c, 1, 2, j, f) * rdz;
-        else if (k == nk) advz = uv_z(c, 1, nk, j, f) * rdz;
-        else advz = -(uv_z(c, 1, k + 1, j, f) - uv_z(c, 1, k, j, f)) * rdz;
+        if (k == 1) advz = zmass(c, -uv_z(c, 1, 2, j, f), k, rdz);
+        else if (k == nk) advz = zmass(c, uv_z(c, 1, nk, j, f), k, rdz);
+        else advz = zmass(c, -(uv_z(c, 1, k + 1, j, f) - uv_z(c, 1, k, j, f)), k, rdz);
         float total = (advx + advy) + advz;
         total = total + uc * (half * (C3(c, a->divx, k0, j, east) + C3(c, a->divx, k0, j, west)));
-        const float scale = a->gzu[(int64_t)j * (ni + 1) + f] /
-                            (half * (C3(c, a->rho0_3d, k0, j, west) + C3(c, a->rho0_3d, k0, j, east)));
+        const float scale = c->vmode == 2 ? C3(c, c->rr0, k0, 0, 0)
+                                          : a->gzu[(int64_t)j * (ni + 1) + f] /
+                                                (half * (C3(c, a->rho0_3d, k0, j, west) + C3(c, a->rho0_3d, k0, j, east)));
         U_(c, a->uten, k, y, x) = U_(c, a->uten, k, y, x) + total * scale;
       }
     }
@@ -370,24 +406,25 @@ int oracle_momentum_advection5_phase(int ni, int nj, int nk, const mom_arrays* a
           if (mass >= 0.0f) {
             const float corr = (U_(c, a->rru, k, south + NG, NG + 1) - U_(c, a->rru, k, south + NG, NG)) +
                                (U_(c, a->rru, k, north + NG, NG + 1) - U_(c, a->rru, k, north + NG, NG));
-            advx = advx - (vc * half) * (corr * (rdx * a->uh[NG]));
+            advx = advx - bcorr(c, vc * half, corr, rdx, a->uh[NG]);
           }
         } else if (i == ni - 1 && opn(c, 1)) {
           const float mass = U_(c, a->rru, k, north + NG, NG + ni) + U_(c, a->rru, k, south + NG, NG + ni);
           if (mass <= 0.0f) {
             const float corr = (U_(c, a->rru, k, south + NG, x + 1) - U_(c, a->rru, k, south + NG, x)) +
                                (U_(c, a->rru, k, north + NG, x + 1) - U_(c, a->rru, k, north + NG, x));
-            advx = advx - (vc * half) * (corr * (rdx * a->uh[x]));
+            advx = advx - bcorr(c, vc * half, corr, rdx, a->uh[x]);
           }
         }
         float advz;
-        if (k == 1) advz = -uv_z(c, 0, 2, g, i) * rdz;
-        else if (k == nk) advz = uv_z(c, 0, nk, g, i) * rdz;
-        else advz = -(uv_z(c, 0, k + 1, g, i) - uv_z(c, 0, k, g, i)) * rdz;
+        if (k == 1) advz = zmass(c, -uv_z(c, 0, 2, g, i), k, rdz);
+        else if (k == nk) advz = zmass(c, uv_z(c, 0, nk, g, i), k, rdz);
+        else advz = zmass(c, -(uv_z(c, 0, k + 1, g, i) - uv_z(c, 0, k, g, i)), k, rdz);
         float total = (advx + advy) + advz;
         total = total + vc * (half * (C3(c, a->divx, k0, north, i) + C3(c, a->divx, k0, south, i)));
-        const float scale = a->gzv[(int64_t)g * ni + i] /
-                            (half * (C3(c, a->rho0_3d, k0, south, i) + C3(c, a->rho0_3d, k0, north, i)));
+        const float scale = c->vmode == 2 ? C3(c, c->rr0, k0, 0, 0)
+                                          : a->gzv[(int64_t)g * ni + i] /
+                                                (half * (C3(c, a->rho0_3d, k0, south, i) + C3(c, a->rho0_3d, k0, north, i)));
         V_(c, a->vten, k, y, x) = V_(c, a->vten, k, y, x) + total * scale;
       }
     }
@@ -398,8 +435,9 @@ int oracle_momentum_advection5_phase(int ni, int nj, int nk, const mom_arrays* a
       const int y = j + NG;
       for (int i = 0; i < ni; ++i) {
         const int x = i + NG;
-        float advx = -(w_fx(c, kf, j, i + 1) - w_fx(c, kf, j, i)) * (rdx * a->uh[x]);
-        float advy = -(w_fy(c, kf, j + 1, i) - w_fy(c, kf, j, i)) * (rdy * a->vh[y]);
+        const float dfx = -(w_fx(c, kf, j, i + 1) - w_fx(c, kf, j, i)), dfy = -(w_fy(c, kf, j + 1, i) - w_fy(c, kf, j, i));
+        float advx = c->vmode == 2 ? (dfx * rdx) * a->uh[x] : dfx * (rdx * a->uh[x]);
+        float advy = c->vmode == 2 ? (dfy * rdy) * a->vh[y] : dfy * (rdy * a->vh[y]);
         const float c2 = a->c2[((int64_t)(kf - 1) * nj + j) * ni + i], c1 = 1.0f - c2;
         const float wc = W_(c, a->w3d, kf, y, x);
         if (i == 0 && opn(c, 0)) {
@@ -407,14 +445,14 @@ int oracle_momentum_advection5_phase(int ni, int nj, int nk, const mom_arrays* a
           if (mass >= 0.0f) {
             const float corr = c1 * (U_(c, a->rru, kf - 1, y, NG + 1) - U_(c, a->rru, kf - 1, y, NG)) +
                                c2 * (U_(c, a->rru, kf, y, NG + 1) - U_(c, a->rru, kf, y, NG));
-            advx = advx - wc * (corr * (rdx * a->uh[x]));
+            advx = advx - bcorr(c, wc, corr, rdx, a->uh[x]);
           }
         } else if (i == ni - 1 && opn(c, 1)) {
           const float mass = c2 * U_(c, a->rru, kf, y, NG + ni) + c1 * U_(c, a->rru, kf - 1, y, NG + ni);
           if (mass <= 0.0f) {
             const float corr = c1 * (U_(c, a->rru, kf - 1, y, x + 1) - U_(c, a->rru, kf - 1, y, x)) +
                                c2 * (U_(c, a->rru, kf, y, x + 1) - U_(c, a->rru, kf, y, x));
-            advx = advx - wc * (corr * (rdx * a->uh[x]));
+            advx = advx - bcorr(c, wc, corr, rdx, a->uh[x]);
           }
         }
         if (j == 0 && opn(c, 2)) {
@@ -422,24 +460,46 @@ int oracle_momentum_advection5_phase(int ni, int nj, int nk, const mom_arrays* a
           if (mass >= 0.0f) {
             const float corr = c1 * (V_(c, a->rrv, kf - 1, NG + 1, x) - V_(c, a->rrv, kf - 1, NG, x)) +
                                c2 * (V_(c, a->rrv, kf, NG + 1, x) - V_(c, a->rrv, kf, NG, x));
-            advy = advy - wc * (corr * (rdy * a->vh[y]));
+            advy = advy - bcorr(c, wc, corr, rdy, a->vh[y]);
           }
         } else if (j == nj - 1 && opn(c, 3)) {
           const float mass = c2 * V_(c, a->rrv, kf, NG + nj, x) + c1 * V_(c, a->rrv, kf - 1, NG + nj, x);
           if (mass <= 0.0f) {
             const float corr = c1 * (V_(c, a->rrv, kf - 1, y + 1, x) - V_(c, a->rrv, kf - 1, y, x)) +
                                c2 * (V_(c, a->rrv, kf, y + 1, x) - V_(c, a->rrv, kf, y, x));
-            advy = advy - wc * (corr * (rdy * a->vh[y]));
+            advy = advy - bcorr(c, wc, corr, rdy, a->vh[y]);
           }
         }
-        const float advz = -(w_z(c, kf, j, i) - w_z(c, kf - 1, j, i)) * rdz;
+        const float advz = zface(c, -(w_z(c, kf, j, i) - w_z(c, kf - 1, j, i)), kf, rdz);
         float total = (advx + advy) + advz;
         total = total + wc * (c2 * C3(c, a->divx, kf - 1, j, i) + c1 * C3(c, a->divx, kf - 2, j, i));
-        const float scale = a->rrf0[((int64_t)(kf - 1) * nj + j) * ni + i] * a->gz[(int64_t)j * ni + i];
+        const float scale = c->vmode == 2 ? a->rrf0[(int64_t)(kf - 1) * nj * ni]
+                                          : a->rrf0[((int64_t)(kf - 1) * nj + j) * ni + i] * a->gz[(int64_t)j * ni + i];
         W_(c, a->wten, kf, y, x) = W_(c, a->wten, kf, y, x) + total * scale;
       }
     }
   return 0;
+}
+
+int oracle_momentum_advection5_phase(int ni, int nj, int nk, const mom_arrays* a, const int* sides, float dx,
+                                     float dy, float dz, int phase) {
+  if (ni < 7 || nj < 7 || nk < 8) return -1;
+  mom_ctx cc = {ni, nj, nk, {sides[0], sides[1], sides[2], sides[3]}, a, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0.0f, 0.0f};
+  return mom_phase(&cc, dx, dy, dz, phase);
+}
+
+/* launch_cuda_gm1_child_stretched_momentum5
+ * (src/cm1core/cuda_gm1_child_stretched_momentum.py:540-780): flat = 0 the
+ * terrain branch (sigma, sigmaf, rds, rdsf, ztop, padded rho0); flat = 1 the
+ * flat column (mh, mf, rdz, the column's padded rho0, rf0, rr0, rrf0). */
+int oracle_momentum_advection5_column_phase(int ni, int nj, int nk, const mom_arrays* a, const int* sides, float dx,
+                                            float dy, int phase, int flat, const float* rho0p, const float* sigma,
+                                            const float* sigmaf, const float* rds, const float* rdsf, float ztop,
+                                            const float* mh, const float* mf, const float* rr0, float rdz) {
+  if (ni < 7 || nj < 7 || nk < 8) return -1;
+  mom_ctx cc = {ni, nj, nk, {sides[0], sides[1], sides[2], sides[3]}, a, flat ? 2 : 1, rho0p, sigma, sigmaf, rds,
+                rdsf, mh, mf, rr0, ztop, rdz};
+  return mom_phase(&cc, dx, dy, 1.0f, phase);
 }
 
 int oracle_momentum_advection5(int ni, int nj, int nk, const mom_arrays* a, const int* sides, float dx, float dy,

@@ -100,3 +100,43 @@ def test_aliasing_refused():
     with pytest.raises(ValueError, match="alias"):
         mom.launch_cuda_terrain_open_momentum_advection5(dev, dev, ni=ni, nj=nj, nk=nk, nrk=1, dx=1.0, dy=1.0,
                                                          dz=1.0)
+
+
+@pytest.mark.parametrize("flat", [False, True])
+@pytest.mark.parametrize("tag", ["momentum5_open_9x8x10", "momentum5_perx_8x9x9"])
+def test_stretched_column_matches_oracle(flat, tag):
+    """launch_cuda_gm1_child_stretched_momentum5 on a generated stretched
+    column (20 m at the ground to 200 m at the top) against the oracle
+    restatement, word for word, in the terrain branch and the flat column."""
+    from gm1_b200.momentum import StretchedMomentumColumn, launch_cuda_gm1_child_stretched_momentum5
+    from gm1_b200.vertical import build_vertical_levels
+    from tests.test_oracle_momentum import _padded_rho0, load
+
+    meta, a, _ = load(tag)
+    ni, nj, nk = meta["ni"], meta["nj"], meta["nk"]
+    spec = {10: (1100.0, 40.0, 700.0), 9: (990.0, 40.0, 590.0)}[nk]
+    lv = build_vertical_levels(stretch_z=1, nk=nk, dz_m=100.0, ztop_m=spec[0], str_bot_m=spec[1], str_top_m=spec[2],
+                               dz_bot_m=20.0, dz_top_m=200.0)
+    rho0p = _padded_rho0(a["rho0_3d"], ni, nj, nk)
+    rr0 = (np.float32(1.0) / a["rho0_3d"]).astype(np.float32)
+    rdz = float(np.float32(1.0) / np.float32(100.0))
+    a["divx"] = np.zeros((nk, nj, ni), np.float32)
+    want = {k: v.copy() for k, v in a.items()}
+    col = {"flat": flat, "rho0p": rho0p, "sigma": lv.sigma, "sigmaf": lv.sigmaf, "rds": lv.rds, "rdsf": lv.rdsf,
+           "ztop": lv.ztop_m, "mh": lv.mh, "mf": lv.mf, "rr0": rr0, "rdz": rdz}
+    if flat:
+        for n in ("sigma", "sigmaf", "rds", "rdsf"):
+            col[n] = None
+    sides = tuple(meta["lateral_sides"])
+    orc.momentum_advection5_column(want, col, ni=ni, nj=nj, nk=nk, dx=meta["dx"], dy=meta["dy"], lateral_sides=sides)
+    d = {k: torch.from_numpy(np.ascontiguousarray(v)).cuda() for k, v in a.items()}
+    t = lambda x: torch.from_numpy(np.array(x, dtype=np.float32)).cuda()  # noqa: E731
+    vertical = (StretchedMomentumColumn(True, t(rho0p), mh=t(lv.mh), mf=t(lv.mf), rr0=t(rr0), rdz=rdz) if flat else
+                StretchedMomentumColumn(False, t(rho0p), sigma=t(lv.sigma), sigmaf=t(lv.sigmaf), rds=t(lv.rds),
+                                        rdsf=t(lv.rdsf), ztop=lv.ztop_m))
+    launch_cuda_gm1_child_stretched_momentum5(d, d, vertical, ni=ni, nj=nj, nk=nk, nrk=1, dx=meta["dx"],
+                                              dy=meta["dy"], divx=d["divx"], lateral_sides=sides)
+    torch.cuda.synchronize()
+    for n in ("uten", "vten", "wten", "rru", "rrv", "rrw", "divx"):
+        got = d[n].cpu().numpy()
+        assert np.array_equal(got.view(np.uint32), want[n].view(np.uint32)), n

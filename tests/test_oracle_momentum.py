@@ -78,3 +78,37 @@ def test_launcher_refuses_before_touching_a_device():
     cpu = {k: torch.from_numpy(v) for k, v in a.items()}
     with pytest.raises(TypeError, match="CUDA"):
         mom.launch_cuda_terrain_open_momentum_advection5(cpu, cpu, **kw)
+
+
+def _padded_rho0(rho0, ni, nj, nk):
+    """(nk+2, nj+6, ni+6) base density whose halo repeats the edge column /
+    row (the clamp the uniform operator applies)."""
+    p = np.zeros((nk + 2, nj + 6, ni + 6), np.float32)
+    p[1:nk + 1, 3:nj + 3, 3:ni + 3] = rho0
+    p[1:nk + 1, 3:nj + 3, :3] = rho0[:, :, :1]
+    p[1:nk + 1, 3:nj + 3, ni + 3:] = rho0[:, :, -1:]
+    p[:, :3, :] = p[:, 3:4, :]
+    p[:, nj + 3:, :] = p[:, nj + 2:nj + 3, :]
+    return p
+
+
+def test_uniform_terrain_column_is_the_uniform_operator():
+    """The stretched momentum (restatement of the reference's profile-bound
+    text, cuda_gm1_child_stretched_momentum.py:56-200) on the uniform column's
+    own sigma/sigmaf/rds/rdsf words and a clamped-halo padded density is the
+    twin-pinned uniform operator word for word."""
+    from gm1_b200.vertical import uniform_vertical_levels
+
+    meta, a, _ = load(TAGS[0])
+    ni, nj, nk = meta["ni"], meta["nj"], meta["nk"]
+    a["divx"] = np.zeros((nk, nj, ni), np.float32)
+    b = {k: v.copy() for k, v in a.items()}
+    orc.momentum_advection5(a, ni=ni, nj=nj, nk=nk, dx=meta["dx"], dy=meta["dy"], dz=meta["dz"],
+                            lateral_sides=tuple(meta["lateral_sides"]))
+    lv = uniform_vertical_levels(nk, meta["dz"])
+    col = {"flat": False, "rho0p": _padded_rho0(b["rho0_3d"], ni, nj, nk), "sigma": lv.sigma, "sigmaf": lv.sigmaf,
+           "rds": lv.rds, "rdsf": lv.rdsf, "ztop": lv.ztop_m}
+    orc.momentum_advection5_column(b, col, ni=ni, nj=nj, nk=nk, dx=meta["dx"], dy=meta["dy"],
+                                   lateral_sides=tuple(meta["lateral_sides"]))
+    for n in OUTS:
+        assert np.array_equal(a[n].view(np.uint32), b[n].view(np.uint32)), n
