@@ -152,10 +152,12 @@ __global__ void __launch_bounds__(256) msb_buoyancy_kernel(const float *__restri
                                                           const float *__restrict__ c1, const float *__restrict__ c2,
                                                           const float *__restrict__ gxu,
                                                           const float *__restrict__ gyv, float *__restrict__ uten,
-                                                          float *__restrict__ vten, float *__restrict__ wten, Lane L) {
+                                                          float *__restrict__ vten, float *__restrict__ wten, Lane L,
+                                                          int w_only) {
     const int ni = L.ni, nj = L.nj, nk = L.nk;
     const unsigned nw = (unsigned)(nk - 1) * nj * ni, nu = (unsigned)nk * nj * (ni - 1), nv = (unsigned)nk * (nj - 1) * ni;
-    for (unsigned z = (unsigned)blockIdx.x * blockDim.x + threadIdx.x; z < nw + nu + nv; z += (unsigned)gridDim.x * blockDim.x) {
+    const unsigned total = w_only ? nw : nw + nu + nv;
+    for (unsigned z = (unsigned)blockIdx.x * blockDim.x + threadIdx.x; z < total; z += (unsigned)gridDim.x * blockDim.x) {
         if (z < nw) {
             const int i = (int)(z % ni), j = (int)((z / ni) % nj), kf = (int)(z / ((unsigned)ni * nj)) + 2;
             const unsigned p = L.m(kf - 1, j, i);
@@ -190,61 +192,88 @@ struct Getdiv {
     const float *rru, *rrv, *rrw, *rgzu, *rgzv, *dzdx, *dzdy, *gz, *thterm;
     float *div, *theta_div;
     float rdx, rdy, rdsf, dz, zt, rzt;
+    // vertical column: 0 uniform; 1 terrain branch on a stretched column
+    // (sigma/sigmaf/rds/rdsf, physical top zt); 2 flat column (rdz*mh, no
+    // terrain w, no rgzu/rgzv) - cuda_gm1_child_stretched_moist.py:35-110
+    int vmode;
+    const float *sigma, *sigmaf, *rds, *rdsfp, *mh;
+    float rdzm;
 };
 
+template <int VM>
 __device__ __forceinline__ float gd_xu(const Getdiv &a, const Lane &L, int k, int j, int f) {
+    if (VM == 2) return a.rru[L.u(k, j + 3, f + 3)];
     return a.rru[L.u(k, j + 3, f + 3)] * a.rgzu[(unsigned)j * (L.ni + 1) + f];
 }
+template <int VM>
 __device__ __forceinline__ float gd_yv(const Getdiv &a, const Lane &L, int k, int f, int i) {
+    if (VM == 2) return a.rrv[L.v(k, f + 3, i + 3)];
     return a.rrv[L.v(k, f + 3, i + 3)] * a.rgzv[(unsigned)f * L.ni + i];
 }
 // transformed w on w levels (getdiv's own grouping: r1 = 0.5 (1 - r2), r2 = 0.5 r2)
+template <int VM>
 __device__ __forceinline__ float gd_wt(const Getdiv &a, const Lane &L, int kf, int j, int i) {
     if (kf == 1 || kf == L.nk + 1) return 0.0f;
-    const float rds = 1.0f / a.dz;
-    const float sf = (float)(kf - 1) * a.dz, sm = ((float)(kf - 1) - 0.5f) * a.dz;
+    if (VM == 2) return a.rrw[L.s(kf, j + 3, i + 3)];
+    const bool pr = VM == 1;
+    const float rds = pr ? a.rds[kf] : 1.0f / a.dz;
+    const float sf = pr ? a.sigmaf[kf] : (float)(kf - 1) * a.dz, sm = pr ? a.sigma[kf - 1] : ((float)(kf - 1) - 0.5f) * a.dz;
     float r2 = (sf - sm) * rds;
     const float r1 = 0.5f * (1.0f - r2);
     r2 = 0.5f * r2;
-    const float ux = r2 * (gd_xu(a, L, kf, j, i) + gd_xu(a, L, kf, j, i + 1)) +
-                     r1 * (gd_xu(a, L, kf - 1, j, i) + gd_xu(a, L, kf - 1, j, i + 1));
-    const float vy = r2 * (gd_yv(a, L, kf, j, i) + gd_yv(a, L, kf, j + 1, i)) +
-                     r1 * (gd_yv(a, L, kf - 1, j, i) + gd_yv(a, L, kf - 1, j + 1, i));
+    const float ux = r2 * (gd_xu<VM>(a, L, kf, j, i) + gd_xu<VM>(a, L, kf, j, i + 1)) +
+                     r1 * (gd_xu<VM>(a, L, kf - 1, j, i) + gd_xu<VM>(a, L, kf - 1, j, i + 1));
+    const float vy = r2 * (gd_yv<VM>(a, L, kf, j, i) + gd_yv<VM>(a, L, kf, j + 1, i)) +
+                     r1 * (gd_yv<VM>(a, L, kf - 1, j, i) + gd_yv<VM>(a, L, kf - 1, j + 1, i));
     float terrain = ux * a.dzdx[(unsigned)j * L.ni + i] + vy * a.dzdy[(unsigned)j * L.ni + i];
     terrain = ((terrain * (sf - a.zt)) * a.gz[(unsigned)j * L.ni + i]) * (1.0f / a.zt);
     return a.rrw[L.s(kf, j + 3, i + 3)] + terrain;
 }
 
+template <int VM>
 __global__ void __launch_bounds__(256) msb_getdiv_kernel(Getdiv a, Lane L) {
     const unsigned n = (unsigned)L.nk * L.nj * L.ni;
     for (unsigned z = (unsigned)blockIdx.x * blockDim.x + threadIdx.x; z < n; z += (unsigned)gridDim.x * blockDim.x) {
         const int i = (int)(z % L.ni), j = (int)((z / L.ni) % L.nj), k = (int)(z / ((unsigned)L.ni * L.nj)) + 1;
-        float d = (gd_xu(a, L, k, j, i + 1) - gd_xu(a, L, k, j, i)) * a.rdx +
-                  (gd_yv(a, L, k, j + 1, i) - gd_yv(a, L, k, j, i)) * a.rdy;
-        d = d + (gd_wt(a, L, k + 1, j, i) - gd_wt(a, L, k, j, i)) * a.rdsf;
-        if (fabsf(d) < 1.0e-20f) d = 0.0f;
+        float d = (gd_xu<VM>(a, L, k, j, i + 1) - gd_xu<VM>(a, L, k, j, i)) * a.rdx +
+                  (gd_yv<VM>(a, L, k, j + 1, i) - gd_yv<VM>(a, L, k, j, i)) * a.rdy;
+        const float dw = gd_wt<VM>(a, L, k + 1, j, i) - gd_wt<VM>(a, L, k, j, i);
+        d = d + (VM == 2 ? (dw * a.rdzm) * a.mh[k] : dw * (VM == 1 ? a.rdsfp[k] : a.rdsf));
+        if (fabsf(d) < (VM == 2 ? 1.0e-30f : 1.0e-20f)) d = 0.0f;
         a.div[z] = d;
         a.theta_div[z] = d * a.thterm[z];
     }
 }
 
+// vmode 1: base density from the padded rho0p; vmode 2: rho0p(k, 3, 3) alone
 __global__ void __launch_bounds__(256) msb_getdivx_horizontal_kernel(const float *rho0, const float *rgzu,
-                                                                    const float *rgzv, float *rru, float *rrv, Lane L) {
+                                                                    const float *rgzv, float *rru, float *rrv, Lane L,
+                                                                    int vmode, const float *rho0p) {
     const int ni = L.ni, nj = L.nj, nk = L.nk;
     const unsigned nu = (unsigned)nk * nj * (ni + 1), nv = (unsigned)nk * (nj + 1) * ni;
     for (unsigned z = (unsigned)blockIdx.x * blockDim.x + threadIdx.x; z < nu + nv; z += (unsigned)gridDim.x * blockDim.x) {
         if (z < nu) {
             const int f = (int)(z % (ni + 1)), j = (int)((z / (ni + 1)) % nj), k = (int)(z / ((unsigned)(ni + 1) * nj)) + 1;
-            const int l = f == 0 ? 0 : f - 1, r = f == ni ? ni - 1 : f;
-            const float den = 0.5f * (rho0[L.m(k - 1, j, l)] + rho0[L.m(k - 1, j, r)]);
             const unsigned p = L.u(k, j + 3, f + 3);
+            if (vmode == 2) {
+                rru[p] = rru[p] * rho0p[L.s(k, 3, 3)];
+                continue;
+            }
+            const int l = f == 0 ? 0 : f - 1, r = f == ni ? ni - 1 : f;
+            const float den = vmode == 1 ? 0.5f * (rho0p[L.s(k, j + 3, f + 2)] + rho0p[L.s(k, j + 3, f + 3)])
+                                         : 0.5f * (rho0[L.m(k - 1, j, l)] + rho0[L.m(k - 1, j, r)]);
             rru[p] = (den * rru[p]) * rgzu[(unsigned)j * (ni + 1) + f];
         } else {
             const unsigned q = z - nu;
             const int i = (int)(q % ni), f = (int)((q / ni) % (nj + 1)), k = (int)(q / ((unsigned)ni * (nj + 1))) + 1;
-            const int s = f == 0 ? 0 : f - 1, nn = f == nj ? nj - 1 : f;
-            const float den = 0.5f * (rho0[L.m(k - 1, s, i)] + rho0[L.m(k - 1, nn, i)]);
             const unsigned p = L.v(k, f + 3, i + 3);
+            if (vmode == 2) {
+                rrv[p] = rrv[p] * rho0p[L.s(k, 3, 3)];
+                continue;
+            }
+            const int s = f == 0 ? 0 : f - 1, nn = f == nj ? nj - 1 : f;
+            const float den = vmode == 1 ? 0.5f * (rho0p[L.s(k, f + 2, i + 3)] + rho0p[L.s(k, f + 3, i + 3)])
+                                         : 0.5f * (rho0[L.m(k - 1, s, i)] + rho0[L.m(k - 1, nn, i)]);
             rrv[p] = (den * rrv[p]) * rgzv[(unsigned)f * ni + i];
         }
     }
@@ -252,10 +281,13 @@ __global__ void __launch_bounds__(256) msb_getdivx_horizontal_kernel(const float
 
 __global__ void __launch_bounds__(256) msb_getdivx_vertical_kernel(const float *rf0, const float *dzdx,
                                                                   const float *dzdy, const float *gz, const float *rru,
-                                                                  const float *rrv, float *rrw, float dz, Lane L) {
+                                                                  const float *rrv, float *rrw, float dz, Lane L,
+                                                                  int vmode, const float *sigma, const float *sigmaf,
+                                                                  const float *rdsp, float ztop) {
     const int ni = L.ni, nj = L.nj, nk = L.nk;
     const unsigned n = (unsigned)(nk + 1) * nj * ni;
-    const float rds = 1.0f / dz, zt = (float)nk * dz, rzt = 1.0f / zt;
+    const bool pr = vmode == 1;
+    const float rds = 1.0f / dz, zt = pr ? ztop : (float)nk * dz, rzt = 1.0f / zt;
     for (unsigned z = (unsigned)blockIdx.x * blockDim.x + threadIdx.x; z < n; z += (unsigned)gridDim.x * blockDim.x) {
         const int i = (int)(z % ni), j = (int)((z / ni) % nj), kf = (int)(z / ((unsigned)ni * nj)) + 1;
         const unsigned p = L.s(kf, j + 3, i + 3);
@@ -263,8 +295,12 @@ __global__ void __launch_bounds__(256) msb_getdivx_vertical_kernel(const float *
             rrw[p] = 0.0f;
             continue;
         }
-        const float sf = (float)(kf - 1) * dz, sm = ((float)(kf - 1) - 0.5f) * dz;
-        float r2 = (sf - sm) * rds;
+        if (vmode == 2) {  // the flat column: rf0(1,1,k) rrw
+            rrw[p] = rrw[p] * rf0[L.m(kf - 1, 0, 0)];
+            continue;
+        }
+        const float sf = pr ? sigmaf[kf] : (float)(kf - 1) * dz, sm = pr ? sigma[kf - 1] : ((float)(kf - 1) - 0.5f) * dz;
+        float r2 = (sf - sm) * (pr ? rdsp[kf] : rds);
         const float r1 = 0.5f * (1.0f - r2);
         r2 = 0.5f * r2;
         const float ux = r2 * (rru[L.u(kf, j + 3, i + 3)] + rru[L.u(kf, j + 3, i + 4)]) +
@@ -279,14 +315,16 @@ __global__ void __launch_bounds__(256) msb_getdivx_vertical_kernel(const float *
 
 __global__ void __launch_bounds__(256) msb_getdivx_divergence_kernel(const float *rru, const float *rrv,
                                                                     const float *rrw, float *divx, float rdx,
-                                                                    float rdy, float rdsf, Lane L) {
+                                                                    float rdy, float rdsf, Lane L, int vmode,
+                                                                    const float *rdsfp, const float *mh, float rdzm) {
     const unsigned n = (unsigned)L.nk * L.nj * L.ni;
     for (unsigned z = (unsigned)blockIdx.x * blockDim.x + threadIdx.x; z < n; z += (unsigned)gridDim.x * blockDim.x) {
         const int i = (int)(z % L.ni), j = (int)((z / L.ni) % L.nj), k = (int)(z / ((unsigned)L.ni * L.nj)) + 1;
         float d = (rru[L.u(k, j + 3, i + 4)] - rru[L.u(k, j + 3, i + 3)]) * rdx +
                   (rrv[L.v(k, j + 4, i + 3)] - rrv[L.v(k, j + 3, i + 3)]) * rdy;
-        d = d + (rrw[L.s(k + 1, j + 3, i + 3)] - rrw[L.s(k, j + 3, i + 3)]) * rdsf;
-        divx[z] = fabsf(d) < 1.0e-20f ? 0.0f : d;
+        const float dw = rrw[L.s(k + 1, j + 3, i + 3)] - rrw[L.s(k, j + 3, i + 3)];
+        d = d + (vmode == 2 ? (dw * rdzm) * mh[k] : dw * (vmode == 1 ? rdsfp[k] : rdsf));
+        divx[z] = fabsf(d) < (vmode == 2 ? 1.0e-30f : 1.0e-20f) ? 0.0f : d;
     }
 }
 
@@ -735,9 +773,10 @@ extern "C" int32_t gm1b_open_fill(int32_t ni, int32_t nj, int32_t nk, int32_t ki
     return GM1B_OK;
 }
 
-extern "C" int32_t gm1b_moist_buoyancy(int32_t ni, int32_t nj, int32_t nk, const float *dum8, const float *c1,
-                                       const float *c2, const float *gxu, const float *gyv, float *uten, float *vten,
-                                       float *wten, void *stream) {
+namespace {
+int32_t buoyancy_launch(int32_t ni, int32_t nj, int32_t nk, const float *dum8, const float *c1, const float *c2,
+                        const float *gxu, const float *gyv, float *uten, float *vten, float *wten, int w_only,
+                        void *stream) {
     if (!dum8 || !c1 || !c2 || !gxu || !gyv || !uten || !vten || !wten ||
         !grid_ok(ni, nj, nk, 2, 2, 2, "gm1b_moist_buoyancy")) {
         if (!dum8 || !c1 || !c2 || !gxu || !gyv || !uten || !vten || !wten)
@@ -755,13 +794,36 @@ extern "C" int32_t gm1b_moist_buoyancy(int32_t ni, int32_t nj, int32_t nk, const
     const Lane L{ni, nj, nk};
     const size_t work = (size_t)(nk - 1) * nj * ni + (size_t)nk * nj * (ni - 1) + (size_t)nk * (nj - 1) * ni;
     ProfScope ps("msb_buoyancy_kernel", st);
-    msb_buoyancy_kernel<<<grid_for(work), 256, 0, st>>>(dum8, c1, c2, gxu, gyv, uten, vten, wten, L);
+    msb_buoyancy_kernel<<<grid_for(work), 256, 0, st>>>(dum8, c1, c2, gxu, gyv, uten, vten, wten, L, w_only);
     ps.stop();
     return launch_ok("msb_buoyancy_kernel") ? GM1B_OK : GM1B_ERR_CUDA;
 }
+}  // namespace
 
-extern "C" int32_t gm1b_post_acoustic_flux(int32_t ni, int32_t nj, int32_t nk, const gm1b_post_acoustic_arrays *a,
-                                           float dx, float dy, float dz, void *stream) {
+extern "C" int32_t gm1b_moist_buoyancy(int32_t ni, int32_t nj, int32_t nk, const float *dum8, const float *c1,
+                                       const float *c2, const float *gxu, const float *gyv, float *uten, float *vten,
+                                       float *wten, void *stream) {
+    return buoyancy_launch(ni, nj, nk, dum8, c1, c2, gxu, gyv, uten, vten, wten, 0, stream);
+}
+
+// launch_cuda_gm1_flat_stretched_buoyancy (src/cm1core/cuda_gm1_child_stretched_moist.py:240):
+// a flat column adds the buoyancy to wten only (solve2.F:897-906; the
+// uten/vten term of :971-1008 is a terrain statement); gxu, gyv, uten and
+// vten may be NULL
+extern "C" int32_t gm1b_moist_buoyancy_flat(int32_t ni, int32_t nj, int32_t nk, const float *dum8, const float *c1,
+                                            const float *c2, float *wten, void *stream) {
+    // the w-only launch never reads or writes the u/v arrays; distinct stand-ins keep the aliasing check meaningful
+    if (!dum8 || !c1 || !c2 || !wten) {
+        gm1b_set_error("gm1b_moist_buoyancy_flat: NULL array");
+        return GM1B_ERR_ARGUMENT;
+    }
+    static float standin[4];
+    return buoyancy_launch(ni, nj, nk, dum8, c1, c2, standin, standin + 1, standin + 2, standin + 3, wten, 1, stream);
+}
+
+namespace {
+int32_t post_acoustic_launch(int32_t ni, int32_t nj, int32_t nk, const gm1b_post_acoustic_arrays *a, float dx,
+                             float dy, float dz, const gm1b_momentum_column *c, void *stream) {
     if (a == nullptr || !grid_ok(ni, nj, nk, 2, 2, 2, "gm1b_post_acoustic_flux")) {
         if (a == nullptr) gm1b_set_error("gm1b_post_acoustic_flux: NULL arrays");
         return GM1B_ERR_ARGUMENT;
@@ -781,34 +843,66 @@ extern "C" int32_t gm1b_post_acoustic_flux(int32_t ni, int32_t nj, int32_t nk, c
     const Lane L{ni, nj, nk};
     const size_t n = (size_t)ni * nj * nk;
     const float rdx = 1.0f / dx, rdy = 1.0f / dy, rdsf = 1.0f / dz;
+    const int vmode = c == nullptr ? 0 : (c->flat ? 2 : 1);
+    const float zt = vmode == 1 ? c->ztop : (float)nk * dz;
     Getdiv g{a->rru, a->rrv, a->rrw, a->rgzu, a->rgzv, a->dzdx, a->dzdy, a->gz, a->thterm, a->divergence,
-             a->theta_divergence_term, rdx, rdy, rdsf, dz, (float)nk * dz, 0.0f};
+             a->theta_divergence_term, rdx, rdy, rdsf, dz, zt, 0.0f, vmode,
+             c ? c->sigma : nullptr, c ? c->sigmaf : nullptr, c ? c->rds : nullptr, c ? c->rdsf : nullptr,
+             c ? c->mh : nullptr, c ? c->rdz : 0.0f};
     {
         ProfScope ps("msb_getdiv_kernel", st);
-        msb_getdiv_kernel<<<grid_for(n), 256, 0, st>>>(g, L);
+        if (vmode == 2)
+            msb_getdiv_kernel<2><<<grid_for(n), 256, 0, st>>>(g, L);
+        else if (vmode == 1)
+            msb_getdiv_kernel<1><<<grid_for(n), 256, 0, st>>>(g, L);
+        else
+            msb_getdiv_kernel<0><<<grid_for(n), 256, 0, st>>>(g, L);
         ps.stop();
     }
     if (!launch_ok("msb_getdiv_kernel")) return GM1B_ERR_CUDA;
     {
         ProfScope ps("msb_getdivx_horizontal_kernel", st);
         msb_getdivx_horizontal_kernel<<<grid_for(2 * n + (size_t)nk * (ni + nj + 1)), 256, 0, st>>>(
-            a->rho0_3d, a->rgzu, a->rgzv, a->rru, a->rrv, L);
+            a->rho0_3d, a->rgzu, a->rgzv, a->rru, a->rrv, L, vmode, c ? c->rho0_padded : nullptr);
         ps.stop();
     }
     if (!launch_ok("msb_getdivx_horizontal_kernel")) return GM1B_ERR_CUDA;
     {
         ProfScope ps("msb_getdivx_vertical_kernel", st);
         msb_getdivx_vertical_kernel<<<grid_for(n + (size_t)ni * nj), 256, 0, st>>>(a->rf0, a->dzdx, a->dzdy, a->gz,
-                                                                                  a->rru, a->rrv, a->rrw, dz, L);
+                                                                                  a->rru, a->rrv, a->rrw, dz, L, vmode,
+                                                                                  g.sigma, g.sigmaf, g.rds, zt);
         ps.stop();
     }
     if (!launch_ok("msb_getdivx_vertical_kernel")) return GM1B_ERR_CUDA;
     {
         ProfScope ps("msb_getdivx_divergence_kernel", st);
-        msb_getdivx_divergence_kernel<<<grid_for(n), 256, 0, st>>>(a->rru, a->rrv, a->rrw, a->divx, rdx, rdy, rdsf, L);
+        msb_getdivx_divergence_kernel<<<grid_for(n), 256, 0, st>>>(a->rru, a->rrv, a->rrw, a->divx, rdx, rdy, rdsf, L,
+                                                                   vmode, g.rdsfp, g.mh, g.rdzm);
         ps.stop();
     }
     return launch_ok("msb_getdivx_divergence_kernel") ? GM1B_OK : GM1B_ERR_CUDA;
+}
+}  // namespace
+
+extern "C" int32_t gm1b_post_acoustic_flux(int32_t ni, int32_t nj, int32_t nk, const gm1b_post_acoustic_arrays *a,
+                                           float dx, float dy, float dz, void *stream) {
+    return post_acoustic_launch(ni, nj, nk, a, dx, dy, dz, nullptr, stream);
+}
+
+extern "C" int32_t gm1b_post_acoustic_flux_column(int32_t ni, int32_t nj, int32_t nk,
+                                                  const gm1b_post_acoustic_arrays *a, float dx, float dy,
+                                                  const gm1b_momentum_column *column, void *stream) {
+    if (column == nullptr || (column->flat != 0 && column->flat != 1) || column->rho0_padded == nullptr ||
+        (column->flat ? (column->mh == nullptr || !(column->rdz > 0.0f))
+                      : (column->sigma == nullptr || column->sigmaf == nullptr || column->rds == nullptr ||
+                         column->rdsf == nullptr || !(column->ztop > 0.0f)))) {
+        gm1b_set_error("gm1b_post_acoustic_flux_column: need the padded base density and a flat column (mh, rdz > 0) "
+                       "or a terrain column (sigma, sigmaf, rds, rdsf, ztop > 0)");
+        return GM1B_ERR_ARGUMENT;
+    }
+    // dz forms only the uniform reciprocals, which a stretched column never reads
+    return post_acoustic_launch(ni, nj, nk, a, dx, dy, 1.0f, column, stream);
 }
 
 namespace {

@@ -53,6 +53,12 @@ def _lib():
         lib.gm1b_pdef_moisture_chain_column.argtypes = [i, i, i, c.POINTER(_Chain), f, f, f, c.c_double, c.c_uint32,
                                                         i, c.POINTER(_VerticalColumn), vp]
         lib.gm1b_pdef_moisture_chain_column.restype = i
+        from .momentum import _Column  # noqa: PLC0415
+
+        lib.gm1b_post_acoustic_flux_column.argtypes = [i, i, i, c.POINTER(_Post), f, f, c.POINTER(_Column), vp]
+        lib.gm1b_post_acoustic_flux_column.restype = i
+        lib.gm1b_moist_buoyancy_flat.argtypes = [i, i, i] + [vp] * 4 + [vp]
+        lib.gm1b_moist_buoyancy_flat.restype = i
         lib.gm1b_held_compose.argtypes = [i, i, i, c.POINTER(_Held), f, vp]
         lib.gm1b_solve3_density.argtypes = [i, i, i] + [vp] * 5 + [vp]
         lib.gm1b_pack_scalar.argtypes = [i, i, i, vp, vp, vp]
@@ -128,6 +134,32 @@ def pdef_moisture_chain_column(a: Mapping[str, torch.Tensor], column: StretchedC
     _native.check(_lib().gm1b_pdef_moisture_chain_column(ni, nj, nk, ctypes.byref(s), dttmp, dx, dy, weps, lateral_obc,
                                                          pdefweno, ctypes.byref(col), _st(stream, a["rru"].device)),
                   "gm1b_pdef_moisture_chain_column")
+
+
+def post_acoustic_flux_column(a: Mapping[str, torch.Tensor], column: Any, *, ni: int, nj: int, nk: int, dx: float,
+                              dy: float, stream: Any | None = None) -> None:
+    """getdiv/getdivx on a stretched column (launch_cuda_gm1_child_stretched_post_acoustic,
+    src/cm1core/cuda_gm1_child_stretched_moist.py:286): ``column`` is a
+    gm1_b200.momentum.StretchedMomentumColumn (terrain branch or flat)."""
+    from .momentum import StretchedMomentumColumn, _Column  # noqa: PLC0415
+
+    if not isinstance(column, StretchedMomentumColumn):
+        raise TypeError("column must be a StretchedMomentumColumn")
+    ptr = {n: (_f32(getattr(column, n), n) if getattr(column, n) is not None else None)
+           for n in ("rho0_padded", "sigma", "sigmaf", "rds", "rdsf", "mh")}
+    col = _Column(1 if column.flat else 0, ptr["rho0_padded"], ptr["sigma"], ptr["sigmaf"], ptr["rds"], ptr["rdsf"],
+                  float(column.ztop), ptr["mh"], None, None, float(column.rdz))
+    s = _Post(**{n: _f32(a[n], n) for n in POST_NAMES})
+    _native.check(_lib().gm1b_post_acoustic_flux_column(ni, nj, nk, ctypes.byref(s), dx, dy, ctypes.byref(col),
+                                                        _st(stream, a["rru"].device)), "gm1b_post_acoustic_flux_column")
+
+
+def moist_buoyancy_flat(dum8, c1, c2, wten, *, ni: int, nj: int, nk: int, stream: Any | None = None) -> None:
+    """The flat column's buoyancy, into wten only (launch_cuda_gm1_flat_stretched_buoyancy,
+    src/cm1core/cuda_gm1_child_stretched_moist.py:240)."""
+    ptrs = [_f32(t, n) for t, n in zip((dum8, c1, c2, wten), ("dum8", "c1", "c2", "wten"))]
+    _native.check(_lib().gm1b_moist_buoyancy_flat(ni, nj, nk, *ptrs, _st(stream, dum8.device)),
+                  "gm1b_moist_buoyancy_flat")
 
 
 def held_compose(a: Mapping[str, torch.Tensor], *, ni: int, nj: int, nk: int, dt: float,

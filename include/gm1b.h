@@ -532,6 +532,11 @@ GM1B_API int32_t gm1b_moist_buoyancy(int32_t ni, int32_t nj, int32_t nk, const f
                                      const float *c2, const float *gxu, const float *gyv, float *uten, float *vten,
                                      float *wten, void *stream);
 
+/* launch_cuda_gm1_flat_stretched_buoyancy (src/cm1core/cuda_gm1_child_stretched_moist.py:240):
+ * the flat column's buoyancy, added to wten only. */
+GM1B_API int32_t gm1b_moist_buoyancy_flat(int32_t ni, int32_t nj, int32_t nk, const float *dum8, const float *c1,
+                                          const float *c2, float *wten, void *stream);
+
 /* Post-acoustic getdiv on the acoustic-averaged velocities (divergence and
  * theta_divergence_term = divergence * thterm, compact), then getdivx in
  * place: rru/rrv/rrw become mass fluxes and divx their divergence
@@ -543,6 +548,17 @@ typedef struct gm1b_post_acoustic_arrays {
 } gm1b_post_acoustic_arrays;
 GM1B_API int32_t gm1b_post_acoustic_flux(int32_t ni, int32_t nj, int32_t nk, const gm1b_post_acoustic_arrays *arrays,
                                          float dx, float dy, float dz, void *stream);
+
+/* The post-acoustic getdiv/getdivx on a stretched column
+ * (launch_cuda_gm1_child_stretched_post_acoustic,
+ * src/cm1core/cuda_gm1_child_stretched_moist.py:286; the flat texts :83-110):
+ * flat = 0, the terrain branch with the column's sigma/sigmaf/rds/rdsf, its
+ * physical top and the padded base density; flat = 1, the flat column's
+ * rdz*mh(k), rho0_padded(k, 3, 3) and rf0(1,1,k), no terrain w.  Reads only
+ * the column fields named there. */
+GM1B_API int32_t gm1b_post_acoustic_flux_column(int32_t ni, int32_t nj, int32_t nk,
+                                                const gm1b_post_acoustic_arrays *arrays, float dx, float dy,
+                                                const gm1b_momentum_column *column, void *stream);
 
 /* The final-stage positive-definite moisture chain of one species: WENO
  * face fluxes (horizontal, vertical with the lower/upper closures), the

@@ -47,6 +47,11 @@ def _lib():
         lib.oracle_pdef_moisture_chain_column.argtypes = [c.c_int] * 3 + [c.POINTER(_Chain)] + [c.c_float] * 3 + \
             [c.c_double, c.c_uint, c.c_int, c.c_int, _F, _F, c.c_float]
         lib.oracle_pdef_moisture_chain_column.restype = None
+        lib.oracle_post_acoustic_flux_column.argtypes = [c.c_int] * 3 + [c.POINTER(_Post)] + [c.c_float] * 2 + \
+            [c.c_int] + [_F] * 5 + [c.c_float, _F, c.c_float]
+        lib.oracle_post_acoustic_flux_column.restype = None
+        lib.oracle_moist_buoyancy_flat.argtypes = [c.c_int] * 3 + [_F] * 4
+        lib.oracle_moist_buoyancy_flat.restype = None
         lib.oracle_held_compose.argtypes = [c.c_int] * 3 + [c.POINTER(_Held), c.c_float]
         lib.oracle_solve3_density.argtypes = [c.c_int] * 3 + [_F] * 5
         lib.oracle_pack_scalar.argtypes = [c.c_int] * 3 + [_F] * 2
@@ -70,6 +75,22 @@ def moist_buoyancy(dum8, c1, c2, gxu, gyv, uten, vten, wten, *, ni, nj, nk):
 def post_acoustic_flux(a, *, ni, nj, nk, dx, dy, dz):
     s = _Post(**{n: _p(a[n]) for n in POST_NAMES})
     _lib().oracle_post_acoustic_flux(ni, nj, nk, ctypes.byref(s), dx, dy, dz)
+
+
+def post_acoustic_flux_column(a, column, *, ni, nj, nk, dx, dy):
+    """getdiv/getdivx on a stretched column: ``column`` holds flat, rho0p and
+    sigma/sigmaf/rds/rdsf/ztop (terrain branch) or mh/rdz (flat column)."""
+    s = _Post(**{n: _p(a[n]) for n in POST_NAMES})
+    keep = {n: np.ascontiguousarray(column[n], dtype=np.float32) for n in ("rho0p", "sigma", "sigmaf", "rds", "rdsf",
+                                                                           "mh") if column.get(n) is not None}
+    ptr = {n: (_p(keep[n]) if n in keep else None) for n in ("rho0p", "sigma", "sigmaf", "rds", "rdsf", "mh")}
+    _lib().oracle_post_acoustic_flux_column(ni, nj, nk, ctypes.byref(s), dx, dy, 1 if column["flat"] else 0,
+                                            ptr["rho0p"], ptr["sigma"], ptr["sigmaf"], ptr["rds"], ptr["rdsf"],
+                                            float(column.get("ztop", 0.0)), ptr["mh"], float(column.get("rdz", 0.0)))
+
+
+def moist_buoyancy_flat(dum8, c1, c2, wten, *, ni, nj, nk):
+    _lib().oracle_moist_buoyancy_flat(ni, nj, nk, _p(dum8), _p(c1), _p(c2), _p(wten))
 
 
 def pdef_moisture_chain(a, *, ni, nj, nk, dttmp, dx, dy, dz, weps, lateral_obc, pdefweno):

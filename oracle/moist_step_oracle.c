@@ -33,8 +33,10 @@ static float buoy_face(const float *dum8, const float *c1, const float *c2, cons
     return c1[p] * dum8[S(L, kf - 1, j + 3, i + 3)] + c2[p] * dum8[S(L, kf, j + 3, i + 3)];
 }
 
-void oracle_moist_buoyancy(int ni, int nj, int nk, const float *dum8, const float *c1, const float *c2,
-                           const float *gxu, const float *gyv, float *uten, float *vten, float *wten) {
+/* the flat column's buoyancy (launch_cuda_gm1_flat_stretched_buoyancy,
+ * src/cm1core/cuda_gm1_child_stretched_moist.py:240): wten only */
+void oracle_moist_buoyancy_flat(int ni, int nj, int nk, const float *dum8, const float *c1, const float *c2,
+                                float *wten) {
     const Ln L = {ni, nj, nk};
     for (int kf = 2; kf <= nk; ++kf)
         for (int j = 0; j < nj; ++j)
@@ -44,6 +46,12 @@ void oracle_moist_buoyancy(int ni, int nj, int nk, const float *dum8, const floa
                 const size_t d = S(&L, kf, j + 3, i + 3);
                 wten[d] = wten[d] + add;
             }
+}
+
+void oracle_moist_buoyancy(int ni, int nj, int nk, const float *dum8, const float *c1, const float *c2,
+                           const float *gxu, const float *gyv, float *uten, float *vten, float *wten) {
+    const Ln L = {ni, nj, nk};
+    oracle_moist_buoyancy_flat(ni, nj, nk, dum8, c1, c2, wten);
     for (int k = 1; k <= nk; ++k)
         for (int j = 0; j < nj; ++j)
             for (int f = 1; f < ni; ++f) {
@@ -75,60 +83,89 @@ typedef struct {
     float *divergence, *theta_divergence_term, *divx;
 } post_arrays;
 
-static float gd_xu(const post_arrays *a, const Ln *L, int k, int j, int f) {
+/* the post-acoustic column: mode 0 uniform; 1 terrain branch on a stretched
+ * column (sigma/sigmaf/rds/rdsf, physical top, padded base density); 2 flat
+ * column (rdz*mh, rho0p(k,3,3), rf0(1,1,k), no terrain w, no rgzu/rgzv) -
+ * cuda_gm1_child_stretched_moist.py:35-110 */
+typedef struct {
+    int mode;
+    const float *rho0p, *sigma, *sigmaf, *rds, *rdsf, *mh;
+    float ztop, rdz;
+} post_column;
+static const post_column kUniformPost = {0, 0, 0, 0, 0, 0, 0, 0.0f, 0.0f};
+
+static float gd_xu(const post_arrays *a, const Ln *L, int k, int j, int f, const post_column *c) {
+    if (c->mode == 2) return a->rru[Uu(L, k, j + 3, f + 3)];
     return a->rru[Uu(L, k, j + 3, f + 3)] * a->rgzu[(size_t)j * (L->ni + 1) + f];
 }
-static float gd_yv(const post_arrays *a, const Ln *L, int k, int f, int i) {
+static float gd_yv(const post_arrays *a, const Ln *L, int k, int f, int i, const post_column *c) {
+    if (c->mode == 2) return a->rrv[Vv(L, k, f + 3, i + 3)];
     return a->rrv[Vv(L, k, f + 3, i + 3)] * a->rgzv[(size_t)f * L->ni + i];
 }
-static float gd_wt(const post_arrays *a, const Ln *L, int kf, int j, int i, float dz) {
+static float gd_wt(const post_arrays *a, const Ln *L, int kf, int j, int i, float dz, const post_column *c) {
     if (kf == 1 || kf == L->nk + 1) return 0.0f;
-    const float rds = 1.0f / dz;
-    const float sf = (float)(kf - 1) * dz, sm = ((float)(kf - 1) - 0.5f) * dz;
+    if (c->mode == 2) return a->rrw[S(L, kf, j + 3, i + 3)];
+    const int pr = c->mode == 1;
+    const float rds = pr ? c->rds[kf] : 1.0f / dz;
+    const float sf = pr ? c->sigmaf[kf] : (float)(kf - 1) * dz, sm = pr ? c->sigma[kf - 1] : ((float)(kf - 1) - 0.5f) * dz;
     float r2 = (sf - sm) * rds;
     const float r1 = 0.5f * (1.0f - r2);
     r2 = 0.5f * r2;
-    const float ux = r2 * (gd_xu(a, L, kf, j, i) + gd_xu(a, L, kf, j, i + 1)) +
-                     r1 * (gd_xu(a, L, kf - 1, j, i) + gd_xu(a, L, kf - 1, j, i + 1));
-    const float vy = r2 * (gd_yv(a, L, kf, j, i) + gd_yv(a, L, kf, j + 1, i)) +
-                     r1 * (gd_yv(a, L, kf - 1, j, i) + gd_yv(a, L, kf - 1, j + 1, i));
+    const float ux = r2 * (gd_xu(a, L, kf, j, i, c) + gd_xu(a, L, kf, j, i + 1, c)) +
+                     r1 * (gd_xu(a, L, kf - 1, j, i, c) + gd_xu(a, L, kf - 1, j, i + 1, c));
+    const float vy = r2 * (gd_yv(a, L, kf, j, i, c) + gd_yv(a, L, kf, j + 1, i, c)) +
+                     r1 * (gd_yv(a, L, kf - 1, j, i, c) + gd_yv(a, L, kf - 1, j + 1, i, c));
     float terrain = ux * a->dzdx[(size_t)j * L->ni + i] + vy * a->dzdy[(size_t)j * L->ni + i];
-    const float zt = (float)L->nk * dz;
+    const float zt = pr ? c->ztop : (float)L->nk * dz;
     terrain = ((terrain * (sf - zt)) * a->gz[(size_t)j * L->ni + i]) * (1.0f / zt);
     return a->rrw[S(L, kf, j + 3, i + 3)] + terrain;
 }
 
-void oracle_post_acoustic_flux(int ni, int nj, int nk, const post_arrays *a, float dx, float dy, float dz) {
+static void post_acoustic_impl(int ni, int nj, int nk, const post_arrays *a, float dx, float dy, float dz,
+                               const post_column *c) {
     const Ln L = {ni, nj, nk};
+    const int flat = c->mode == 2, pr = c->mode == 1;
+    const float smeps = flat ? 1.0e-30f : 1.0e-20f;
     const float rdx = 1.0f / dx, rdy = 1.0f / dy, rdsf = 1.0f / dz;
     size_t z = 0;
     for (int k = 1; k <= nk; ++k)
         for (int j = 0; j < nj; ++j)
             for (int i = 0; i < ni; ++i, ++z) {
-                float d = (gd_xu(a, &L, k, j, i + 1) - gd_xu(a, &L, k, j, i)) * rdx +
-                          (gd_yv(a, &L, k, j + 1, i) - gd_yv(a, &L, k, j, i)) * rdy;
-                d = d + (gd_wt(a, &L, k + 1, j, i, dz) - gd_wt(a, &L, k, j, i, dz)) * rdsf;
-                if (fabsf(d) < 1.0e-20f) d = 0.0f;
+                float d = (gd_xu(a, &L, k, j, i + 1, c) - gd_xu(a, &L, k, j, i, c)) * rdx +
+                          (gd_yv(a, &L, k, j + 1, i, c) - gd_yv(a, &L, k, j, i, c)) * rdy;
+                const float dw = gd_wt(a, &L, k + 1, j, i, dz, c) - gd_wt(a, &L, k, j, i, dz, c);
+                d = d + (flat ? (dw * c->rdz) * c->mh[k] : dw * (pr ? c->rdsf[k] : rdsf));
+                if (fabsf(d) < smeps) d = 0.0f;
                 a->divergence[z] = d;
                 a->theta_divergence_term[z] = d * a->thterm[z];
             }
     for (int k = 1; k <= nk; ++k)
         for (int j = 0; j < nj; ++j)
             for (int f = 0; f <= ni; ++f) {
-                const int l = f == 0 ? 0 : f - 1, r = f == ni ? ni - 1 : f;
-                const float den = 0.5f * (a->rho0_3d[Mm(&L, k - 1, j, l)] + a->rho0_3d[Mm(&L, k - 1, j, r)]);
                 const size_t p = Uu(&L, k, j + 3, f + 3);
+                if (flat) {
+                    a->rru[p] = a->rru[p] * c->rho0p[S(&L, k, 3, 3)];
+                    continue;
+                }
+                const int l = f == 0 ? 0 : f - 1, r = f == ni ? ni - 1 : f;
+                const float den = pr ? 0.5f * (c->rho0p[S(&L, k, j + 3, f + 2)] + c->rho0p[S(&L, k, j + 3, f + 3)])
+                                     : 0.5f * (a->rho0_3d[Mm(&L, k - 1, j, l)] + a->rho0_3d[Mm(&L, k - 1, j, r)]);
                 a->rru[p] = (den * a->rru[p]) * a->rgzu[(size_t)j * (ni + 1) + f];
             }
     for (int k = 1; k <= nk; ++k)
         for (int f = 0; f <= nj; ++f)
             for (int i = 0; i < ni; ++i) {
-                const int s = f == 0 ? 0 : f - 1, n = f == nj ? nj - 1 : f;
-                const float den = 0.5f * (a->rho0_3d[Mm(&L, k - 1, s, i)] + a->rho0_3d[Mm(&L, k - 1, n, i)]);
                 const size_t p = Vv(&L, k, f + 3, i + 3);
+                if (flat) {
+                    a->rrv[p] = a->rrv[p] * c->rho0p[S(&L, k, 3, 3)];
+                    continue;
+                }
+                const int s = f == 0 ? 0 : f - 1, n = f == nj ? nj - 1 : f;
+                const float den = pr ? 0.5f * (c->rho0p[S(&L, k, f + 2, i + 3)] + c->rho0p[S(&L, k, f + 3, i + 3)])
+                                     : 0.5f * (a->rho0_3d[Mm(&L, k - 1, s, i)] + a->rho0_3d[Mm(&L, k - 1, n, i)]);
                 a->rrv[p] = (den * a->rrv[p]) * a->rgzv[(size_t)f * ni + i];
             }
-    const float rds = 1.0f / dz, zt = (float)nk * dz, rzt = 1.0f / zt;
+    const float rds = 1.0f / dz, zt = pr ? c->ztop : (float)nk * dz, rzt = 1.0f / zt;
     for (int kf = 1; kf <= nk + 1; ++kf)
         for (int j = 0; j < nj; ++j)
             for (int i = 0; i < ni; ++i) {
@@ -137,8 +174,12 @@ void oracle_post_acoustic_flux(int ni, int nj, int nk, const post_arrays *a, flo
                     a->rrw[p] = 0.0f;
                     continue;
                 }
-                const float sf = (float)(kf - 1) * dz, sm = ((float)(kf - 1) - 0.5f) * dz;
-                float r2 = (sf - sm) * rds;
+                if (flat) {
+                    a->rrw[p] = a->rrw[p] * a->rf0[Mm(&L, kf - 1, 0, 0)];
+                    continue;
+                }
+                const float sf = pr ? c->sigmaf[kf] : (float)(kf - 1) * dz, sm = pr ? c->sigma[kf - 1] : ((float)(kf - 1) - 0.5f) * dz;
+                float r2 = (sf - sm) * (pr ? c->rds[kf] : rds);
                 const float r1 = 0.5f * (1.0f - r2);
                 r2 = 0.5f * r2;
                 const float ux = r2 * (a->rru[Uu(&L, kf, j + 3, i + 3)] + a->rru[Uu(&L, kf, j + 3, i + 4)]) +
@@ -155,9 +196,22 @@ void oracle_post_acoustic_flux(int ni, int nj, int nk, const post_arrays *a, flo
             for (int i = 0; i < ni; ++i, ++z) {
                 float d = (a->rru[Uu(&L, k, j + 3, i + 4)] - a->rru[Uu(&L, k, j + 3, i + 3)]) * rdx +
                           (a->rrv[Vv(&L, k, j + 4, i + 3)] - a->rrv[Vv(&L, k, j + 3, i + 3)]) * rdy;
-                d = d + (a->rrw[S(&L, k + 1, j + 3, i + 3)] - a->rrw[S(&L, k, j + 3, i + 3)]) * rdsf;
-                a->divx[z] = fabsf(d) < 1.0e-20f ? 0.0f : d;
+                const float dw = a->rrw[S(&L, k + 1, j + 3, i + 3)] - a->rrw[S(&L, k, j + 3, i + 3)];
+                d = d + (flat ? (dw * c->rdz) * c->mh[k] : dw * (pr ? c->rdsf[k] : rdsf));
+                a->divx[z] = fabsf(d) < smeps ? 0.0f : d;
             }
+}
+
+void oracle_post_acoustic_flux(int ni, int nj, int nk, const post_arrays *a, float dx, float dy, float dz) {
+    post_acoustic_impl(ni, nj, nk, a, dx, dy, dz, &kUniformPost);
+}
+
+/* launch_cuda_gm1_child_stretched_post_acoustic (src/cm1core/cuda_gm1_child_stretched_moist.py:286) */
+void oracle_post_acoustic_flux_column(int ni, int nj, int nk, const post_arrays *a, float dx, float dy, int flat,
+                                      const float *rho0p, const float *sigma, const float *sigmaf, const float *rds,
+                                      const float *rdsf, float ztop, const float *mh, float rdz) {
+    const post_column c = {flat ? 2 : 1, rho0p, sigma, sigmaf, rds, rdsf, mh, ztop, rdz};
+    post_acoustic_impl(ni, nj, nk, a, dx, dy, 1.0f, &c);
 }
 
 /* ------------------------------------------------------------------ */

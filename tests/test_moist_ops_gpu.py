@@ -142,3 +142,39 @@ def test_pdef_moisture_chain_on_a_stretched_column(flat, obc):
     mo.pdef_moisture_chain_column(d, column, **kw)
     for n in ("fx", "fy", "fz", "advx", "advy", "advz", "candidate", "advection"):
         _same(d[n], a[n], n)
+
+
+@pytest.mark.parametrize("flat", [False, True])
+def test_post_acoustic_flux_on_a_stretched_column(flat):
+    """getdiv/getdivx on a generated stretched column (terrain branch or flat)
+    against the oracle restatement of the reference's stretched texts, word
+    for word; and the flat column's w-only buoyancy."""
+    from gm1_b200.momentum import StretchedMomentumColumn
+    from gm1_b200.vertical import build_vertical_levels
+    from tests.test_oracle_momentum import _padded_rho0
+
+    a = moist_piece_fixture(NI, NJ, NK, 31)
+    mass = (NK, NJ, NI)
+    for n in ("divergence", "theta_divergence_term"):
+        a[n] = np.zeros(mass, np.float32)
+    lv = build_vertical_levels(stretch_z=1, nk=NK, dz_m=100.0, ztop_m=1630.0, str_bot_m=40.0, str_top_m=1030.0,
+                               dz_bot_m=20.0, dz_top_m=200.0)
+    rho0p = _padded_rho0(a["rho0_3d"], NI, NJ, NK)
+    rdz = float(np.float32(1.0) / np.float32(100.0))
+    col = {"flat": flat, "rho0p": rho0p, "sigma": lv.sigma, "sigmaf": lv.sigmaf, "rds": lv.rds, "rdsf": lv.rdsf,
+           "ztop": lv.ztop_m, "mh": lv.mh, "rdz": rdz}
+    d = _dev(a)
+    om.post_acoustic_flux_column(a, col, ni=NI, nj=NJ, nk=NK, dx=400.0, dy=350.0)
+    t = lambda x: torch.from_numpy(np.array(x, dtype=np.float32)).cuda()  # noqa: E731
+    vertical = (StretchedMomentumColumn(True, t(rho0p), mh=t(lv.mh), rdz=rdz) if flat else
+                StretchedMomentumColumn(False, t(rho0p), sigma=t(lv.sigma), sigmaf=t(lv.sigmaf), rds=t(lv.rds),
+                                        rdsf=t(lv.rdsf), ztop=lv.ztop_m))
+    mo.post_acoustic_flux_column(d, vertical, ni=NI, nj=NJ, nk=NK, dx=400.0, dy=350.0)
+    for n in ("rru", "rrv", "rrw", "divergence", "theta_divergence_term", "divx"):
+        _same(d[n], a[n], n)
+    if flat:
+        b = moist_piece_fixture(NI, NJ, NK, 11)
+        db = _dev(b)
+        om.moist_buoyancy_flat(b["dum8"], b["c1"], b["c2"], b["wten"], ni=NI, nj=NJ, nk=NK)
+        mo.moist_buoyancy_flat(db["dum8"], db["c1"], db["c2"], db["wten"], ni=NI, nj=NJ, nk=NK)
+        _same(db["wten"], b["wten"], "wten")

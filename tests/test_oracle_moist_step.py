@@ -93,3 +93,24 @@ def test_chain_on_uniform_columns_is_the_uniform_chain(obc):
         om.pdef_moisture_chain_column(a, flat=flat, profile=prof, rdz=rdz, **kw)
         for n in ("advx", "advy", "advz", "candidate", "advection"):
             assert np.array_equal(a[n].view(np.uint32), want[n].view(np.uint32)), (flat, n)
+
+
+def test_post_acoustic_on_the_uniform_terrain_column_is_the_uniform_operator():
+    """The stretched getdiv/getdivx restatement on the uniform column's own
+    profile words and a clamped-halo padded density reduces word for word to
+    the uniform post-acoustic flux."""
+    from gm1_b200.vertical import uniform_vertical_levels
+    from tests.test_oracle_momentum import _padded_rho0
+
+    ni, nj, nk, dz = 14, 11, 9, 180.0
+    a = moist_piece_fixture(ni, nj, nk, 12)
+    for n in ("divergence", "theta_divergence_term"):
+        a[n] = np.zeros((nk, nj, ni), np.float32)
+    b = {k: v.copy() for k, v in a.items()}
+    om.post_acoustic_flux(a, ni=ni, nj=nj, nk=nk, dx=400.0, dy=350.0, dz=dz)
+    lv = uniform_vertical_levels(nk, dz)
+    col = {"flat": False, "rho0p": _padded_rho0(b["rho0_3d"], ni, nj, nk), "sigma": lv.sigma, "sigmaf": lv.sigmaf,
+           "rds": lv.rds, "rdsf": lv.rdsf, "ztop": lv.ztop_m}
+    om.post_acoustic_flux_column(b, col, ni=ni, nj=nj, nk=nk, dx=400.0, dy=350.0)
+    for n in ("rru", "rrv", "rrw", "divergence", "theta_divergence_term", "divx"):
+        assert np.array_equal(a[n].view(np.uint32), b[n].view(np.uint32)), n
