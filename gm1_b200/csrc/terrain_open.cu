@@ -51,6 +51,11 @@ struct TosArgs {
     unsigned abl, diag;
     float dts, rdx, rdy, dz, alph, beta, asq, kdiv, temx, temy, tavg, zt, rzt, halfcp;
     float cgs[3], cgt[3];
+    // the stretched terrain column (vmode 1): CM1-indexed sigma (nk+2),
+    // sigmaf (nk+3), rds (nk+2), rdsf (nk+3) and the source-valid padded base
+    // density (nk+2, nj+6, ni+6); unused on the uniform column (vmode 0)
+    int vmode;
+    const float *sgm, *sgmf, *rdsp, *rdsfp, *rho0p;
 };
 
 // 32-bit element offsets: the host refuses grids whose largest padded
@@ -81,6 +86,30 @@ __device__ __forceinline__ float sig(int k, float dz) { return ((float)k - 0.5f)
 __device__ __forceinline__ float sigf(int k, float dz) { return (float)(k - 1) * dz; }
 __device__ __forceinline__ float rds(int k, float dz) { return rcp_rn(sig(k, dz) - sig(k - 1, dz)); }
 __device__ __forceinline__ float rdsf(int k, float dz) { return rcp_rn(sigf(k + 1, dz) - sigf(k, dz)); }
+
+// The column's vertical coordinate: formed in-kernel on the uniform column
+// (VM 0), read from the bound profiles at CM1's indices on the stretched
+// terrain column (VM 1): rds(dz) -> rds[k] / rdsf[k], sig/sigf -> sigma /
+// sigmaf, the lid nk*dz -> ztop (cuda_gm1_child_psolver3_open.py:152-280)
+template <int VM> __device__ __forceinline__ float col_rds(const TosArgs &p, int k) {
+    return VM ? __ldg(p.rdsp + k) : rds(k, p.dz);
+}
+template <int VM> __device__ __forceinline__ float col_rdsf(const TosArgs &p, int k) {
+    return VM ? __ldg(p.rdsfp + k) : rdsf(k, p.dz);
+}
+template <int VM> __device__ __forceinline__ float col_sigf(const TosArgs &p, int kf) {
+    return VM ? __ldg(p.sgmf + kf) : sigf(kf, p.dz);
+}
+// r2 of the face-to-level interpolation r2*q(kf) + (1-r2)*q(kf-1)
+template <int VM> __device__ __forceinline__ float col_r2(const TosArgs &p, int kf) {
+    return VM ? (__ldg(p.sgmf + kf) - __ldg(p.sgm + kf - 1)) * __ldg(p.rdsp + kf)
+              : (sigf(kf, p.dz) - sig(kf - 1, p.dz)) * rds(kf, p.dz);
+}
+__device__ __forceinline__ float vrds(const TosArgs &p, int k) { return p.vmode ? col_rds<1>(p, k) : col_rds<0>(p, k); }
+__device__ __forceinline__ float vrdsf(const TosArgs &p, int k) {
+    return p.vmode ? col_rdsf<1>(p, k) : col_rdsf<0>(p, k);
+}
+__device__ __forceinline__ float vr2(const TosArgs &p, int kf) { return p.vmode ? col_r2<1>(p, kf) : col_r2<0>(p, kf); }
 
 // numpy.minimum / numpy.maximum: NaN propagates, a tie returns the second
 __device__ __forceinline__ float np_min(float a, float b) { return a != a ? a : (b != b ? b : (a < b ? a : b)); }
@@ -117,9 +146,9 @@ __global__ void __launch_bounds__(256) tos_prepare_kernel(TosArgs p) {
         if (phys) {
             const int j0 = j - 1, i0 = i - 1;
             const float gz = m.gz[X.h(j0, i0)];
-            const float tem = p.dts * rdsf(k, p.dz);
+            const float tem = p.dts * vrdsf(p, k);
             a.qk[c] = (tem * a.ppterm[c]) * gz;
-            const float tem2 = ((p.dts * gz) * rdsf(k, p.dz)) * m.rr0[X.m(k - 1, j0, i0)];
+            const float tem2 = ((p.dts * gz) * vrdsf(p, k)) * m.rr0[X.m(k - 1, j0, i0)];
             const float pc = a.piadv[c];
             const float b2 = (-m.c2[X.m(k, j0, i0)]) * a.piadv[X.p(k + 1, j, i)] + (1.0f - m.c1[X.m(k, j0, i0)]) * pc;
             const float b1 = m.c1[X.m(k - 1, j0, i0)] * a.piadv[X.p(k - 1, j, i)] + (m.c2[X.m(k - 1, j0, i0)] - 1.0f) * pc;
@@ -127,7 +156,7 @@ __global__ void __launch_bounds__(256) tos_prepare_kernel(TosArgs p) {
             a.pk1[c] = k == 1 ? 0.0f : (tem2 * m.rf0[X.m(k - 1, j0, i0)]) * b1;
             float mmv = 0.0f;
             if (k >= 2) {
-                const float tem1 = (p.dts * rds(k, p.dz)) * 1005.7f;
+                const float tem1 = (p.dts * vrds(p, k)) * 1005.7f;
                 const float th = m.c2[X.m(k - 1, j0, i0)] * a.thv[c] + m.c1[X.m(k - 1, j0, i0)] * a.thv[X.p(k - 1, j, i)];
                 mmv = (tem1 * th) * gz;
             }
@@ -187,7 +216,7 @@ __global__ void __launch_bounds__(128) tos_edge_kernel(TosArgs p) {
             r0 = (p.cgt[0] * q0[nk] + p.cgt[1] * q0[nk - 1]) + p.cgt[2] * q0[nk - 2];
             r1v = (p.cgt[0] * q1[nk] + p.cgt[1] * q1[nk - 1]) + p.cgt[2] * q1[nk - 2];
         } else {
-            const float r2 = (sigf(kf, p.dz) - sig(kf - 1, p.dz)) * rds(kf, p.dz);
+            const float r2 = vr2(p, kf);
             const float r1 = 1.0f - r2;
             r0 = r1 * q0[kf - 1] + r2 * q0[kf];
             r1v = r1 * q1[kf - 1] + r2 * q1[kf];
@@ -220,7 +249,7 @@ __global__ void __launch_bounds__(128) tos_edge_kernel(TosArgs p) {
         float hz = gz * (q1[k] * rg1 - q0[k] * rg0);
         hz = (hz * rd) * hmet;
         float vt = gmet[X.m(k, j0, i0)] * (s1[k + 1] + s0[k + 1]) - gmet[X.m(k - 1, j0, i0)] * (s1[k] + s0[k]);
-        vt = (0.5f * vt) * rdsf(k, p.dz);
+        vt = (0.5f * vt) * vrdsf(p, k);
         const float r = (-rad[(size_t)k * radstride + radpos]) * (hz + vt);
         const size_t o = ew ? X.u(k, yu, xu) : X.v(k, yu, xu);
         const float tnd = r + ten[o];
@@ -294,7 +323,7 @@ __global__ void __launch_bounds__(128) tos_pgrad_kernel(TosArgs p) {
             float vc1 = 0.0f, vw1 = 0.0f, vs1 = 0.0f;
             const float pc1 = lp[q], pw1 = lw[q], ps1 = ls[q];
             if (k < nk) {
-                const float r = rds(k + 1, p.dz);
+                const float r = vrds(p, k + 1);
                 vc1 = (pc1 - pc) * r;
                 vw1 = (pw1 - pw) * r;
                 vs1 = (ps1 - ps) * r;
@@ -370,13 +399,14 @@ struct A2Load {
     }
 };
 
+template <int VM>
 __device__ __forceinline__ void tos_level_terms(const float *s_xw, const float *s_xe, const float *s_ys,
-                                                const float *s_yn, int lane, int kf, const TosArgs &p, float dzdx,
-                                                float dzdy, float gz, float rk, float rl, float rrf0, bool adv,
-                                                float &d3, float &ha) {
-    const float r2 = (sigf(kf, p.dz) - sig(kf - 1, p.dz)) * rds(kf, p.dz);
+                                                const float *s_yn, const float *s_r, int lane, int kf,
+                                                const TosArgs &p, float dzdx, float dzdy, float gz, float rk,
+                                                float rl, float rrf0, bool adv, float &d3, float &ha) {
+    const float r2 = col_r2<VM>(p, kf);
     const float r1 = 1.0f - r2;
-    const float height = (sigf(kf, p.dz) - p.zt) * p.rzt;
+    const float height = (col_sigf<VM>(p, kf) - p.zt) * p.rzt;
     const float xw = s_xw[kf * 32 + lane], xe = s_xe[kf * 32 + lane];
     const float xwl = s_xw[(kf - 1) * 32 + lane], xel = s_xe[(kf - 1) * 32 + lane];
     const float ys = s_ys[kf * 32 + lane], yn = s_yn[kf * 32 + lane];
@@ -389,14 +419,24 @@ __device__ __forceinline__ void tos_level_terms(const float *s_xw, const float *
     }
     ha = 0.0f;
     if (adv) {
-        const float uh = rk * xw + rk * xe, ul = rl * xwl + rl * xel;
-        const float vh = rk * ys + rk * yn, vl = rl * ysl + rl * ynl;
+        float uh, ul, vh, vl;
+        if (VM) {
+            // face-averaged base density times the face velocity, formed in
+            // phase A1 (s_r: west, east, south, north arrays of L*32 words)
+            const int L32 = (p.nk + 2) * 32, o = kf * 32 + lane, ol = (kf - 1) * 32 + lane;
+            uh = s_r[o] + s_r[L32 + o], ul = s_r[ol] + s_r[L32 + ol];
+            vh = s_r[2 * L32 + o] + s_r[3 * L32 + o], vl = s_r[2 * L32 + ol] + s_r[3 * L32 + ol];
+        } else {
+            uh = rk * xw + rk * xe, ul = rl * xwl + rl * xel;
+            vh = rk * ys + rk * yn, vl = rl * ysl + rl * ynl;
+        }
         const float xt = (r2 * uh + r1 * ul) * dzdx;
         const float yt = (r2 * vh + r1 * vl) * dzdy;
         ha = (((0.5f * (xt + yt)) * height) * gz) * rrf0;
     }
 }
 
+template <int VM>
 __global__ void __launch_bounds__(32 * kTosWarps, 3) tos_column_kernel(TosArgs p) {
     extern __shared__ float sh[];
     const Ix X{p.ni, p.nj};
@@ -416,6 +456,8 @@ __global__ void __launch_bounds__(32 * kTosWarps, 3) tos_column_kernel(TosArgs p
     float *s_xw = sh, *s_xe = s_xw + L * 32, *s_ys = s_xe + L * 32, *s_yn = s_ys + L * 32;
     float *s_w = s_yn + L * 32, *s_fpk = s_w + L * 32, *s_ed = s_fpk + L * 32;
     float *s_aa = s_xw, *s_bb = s_xe, *s_cc = s_ys, *s_dd = s_yn;
+    // VM 1: the four rho-weighted face velocities (west, east, south, north)
+    float *s_r = s_ed + L * 32, *s_re = s_r + L * 32, *s_rs = s_re + L * 32, *s_rn = s_rs + L * 32;
 #define SM(arr, k) arr[(k) * 32 + lane]
     float gz = 0.0f, dzdx = 0.0f, dzdy = 0.0f;
     if (live) {
@@ -442,6 +484,17 @@ __global__ void __launch_bounds__(32 * kTosWarps, 3) tos_column_kernel(TosArgs p
             SM(s_yn, k) = vn * rgn;
             // bc.F:1151-1178: the surface w of this small step (stored in phase C)
             SM(s_w, k) = k == 1 ? (0.5f * ((uw + ue) * dzdx + (vs + vn) * dzdy)) * gz : wv;
+            if (VM && do_adv) {
+                // xurho / yvrho: the face's own average of the padded base
+                // density (sound.F:604-613; cuda_gm1_child_psolver3_open.py:199-205)
+                const float rc = __ldg(p.rho0p + X.w(k, y, x));
+                const float rw = __ldg(p.rho0p + X.w(k, y, x - 1)), re = __ldg(p.rho0p + X.w(k, y, x + 1));
+                const float rs = __ldg(p.rho0p + X.w(k, y - 1, x)), rn = __ldg(p.rho0p + X.w(k, y + 1, x));
+                SM(s_r, k) = (0.5f * (rw + rc)) * SM(s_xw, k);
+                SM(s_re, k) = (0.5f * (rc + re)) * SM(s_xe, k);
+                SM(s_rs, k) = (0.5f * (rs + rc)) * SM(s_ys, k);
+                SM(s_rn, k) = (0.5f * (rc + rn)) * SM(s_yn, k);
+            }
         }
     }
     // Each phase's first chunk of global loads is issued before the barrier
@@ -470,10 +523,12 @@ __global__ void __launch_bounds__(32 * kTosWarps, 3) tos_column_kernel(TosArgs p
             const float ppten = ld[q].ppten, ppterm = ld[q].ppterm;
             const float pc = ld[q].pc, pe = ld[q].pe, pw = ld[q].pw, pn = ld[q].pn, ps = ld[q].ps, rr0 = ld[q].rr0;
             float d3k = 0.0f, d3k1 = 0.0f, hak = 0.0f, hak1 = 0.0f;
-            if (k >= 2) tos_level_terms(s_xw, s_xe, s_ys, s_yn, lane, k, p, dzdx, dzdy, gz, rk, rl, rrf_k, do_adv, d3k, hak);
+            if (k >= 2)
+                tos_level_terms<VM>(s_xw, s_xe, s_ys, s_yn, s_r, lane, k, p, dzdx, dzdy, gz, rk, rl, rrf_k, do_adv,
+                                    d3k, hak);
             if (k < nk)
-                tos_level_terms(s_xw, s_xe, s_ys, s_yn, lane, k + 1, p, dzdx, dzdy, gz, rk1, rk, rrf_k1, do_adv, d3k1,
-                                hak1);
+                tos_level_terms<VM>(s_xw, s_xe, s_ys, s_yn, s_r, lane, k + 1, p, dzdx, dzdy, gz, rk1, rk, rrf_k1,
+                                    do_adv, d3k1, hak1);
             if (dlast && k >= 2) {
                 a.dum3[c] = d3k;
                 if (do_adv) a.hadvp[c] = hak;
@@ -482,7 +537,7 @@ __global__ void __launch_bounds__(32 * kTosWarps, 3) tos_column_kernel(TosArgs p
             float div = 0.0f;
             if (do_div) {
                 const float hz = (xe - xw) * p.rdx + (yn - ys) * p.rdy;
-                const float vt = (d3k1 - d3k) * rdsf(k, p.dz);
+                const float vt = (d3k1 - d3k) * col_rdsf<VM>(p, k);
                 div = gz * (hz + vt);
                 if (fabsf(div) < 1.0e-20f) div = 0.0f;
             }
@@ -492,8 +547,15 @@ __global__ void __launch_bounds__(32 * kTosWarps, 3) tos_column_kernel(TosArgs p
             float fpk = src + p.beta * ((-qk) * (w2 - w1));
             if (dlast) a.divh[c] = div;
             if (do_adv) {
-                const float u2 = p.temx * (rk * xe), u1 = p.temx * (rk * xw);
-                const float v2 = p.temy * (rk * yn), v1 = p.temy * (rk * ys);
+                float rxe, rxw, ryn, rys;
+                if (VM) {
+                    rxw = SM(s_r, k), rxe = SM(s_re, k);
+                    rys = SM(s_rs, k), ryn = SM(s_rn, k);
+                } else {
+                    rxe = rk * xe, rxw = rk * xw, ryn = rk * yn, rys = rk * ys;
+                }
+                const float u2 = p.temx * rxe, u1 = p.temx * rxw;
+                const float v2 = p.temy * ryn, v1 = p.temy * rys;
                 const float ww2 = hak1 + p.beta * wk1;
                 const float ww1 = hak + p.beta * wk;
                 const float xa = u2 * (pe - pc) + u1 * (pc - pw);
@@ -984,10 +1046,15 @@ unsigned grid_for(size_t work, int block) {
 
 using namespace gm1b;
 
-extern "C" int32_t gm1b_terrain_open_stage(int32_t ni, int32_t nj, int32_t nk, int32_t nrk, float dt, int32_t nsound,
-                                           float dx, float dy, double dz, float alph, float kdiv, uint32_t ablations,
-                                           uint32_t flags, const gm1b_terrain_open_arrays *arrays,
-                                           const gm1b_terrain_metrics *metrics, void *stream) {
+namespace gm1b {
+namespace {
+
+// one stage on the uniform column (col == nullptr, dz) or on the stretched
+// terrain column bound in col
+int32_t terrain_open_stage(int32_t ni, int32_t nj, int32_t nk, int32_t nrk, float dt, int32_t nsound, float dx,
+                           float dy, double dz, float alph, float kdiv, uint32_t ablations, uint32_t flags,
+                           const gm1b_terrain_open_arrays *arrays, const gm1b_terrain_metrics *metrics,
+                           const gm1b_momentum_column *col, void *stream) {
     if (arrays == nullptr || metrics == nullptr || ni < 3 || nj < 3 || nk < 4 || nk > kTosMaxNk || nrk < 1 ||
         nrk > 3) {
         gm1b_set_error("gm1b_terrain_open_stage: need arrays and metrics, ni >= 3, nj >= 3, 4 <= nk <= %d, "
@@ -998,6 +1065,20 @@ extern "C" int32_t gm1b_terrain_open_stage(int32_t ni, int32_t nj, int32_t nk, i
         gm1b_set_error("gm1b_terrain_open_stage: a %dx%dx%d grid's padded arrays reach 2^31 words; the kernels "
                        "index with 32-bit offsets", ni, nj, nk);
         return GM1B_ERR_ARGUMENT;
+    }
+    if (col != nullptr) {
+        if (col->flat) {
+            gm1b_set_error("gm1b_terrain_open_stage_column: the flat column's acoustic statements (sound.F:119-143, "
+                           "318-342, 491-509, 742-765) are not built; bind a terrain column (flat = 0)");
+            return GM1B_ERR_ARGUMENT;
+        }
+        if (col->sigma == nullptr || col->sigmaf == nullptr || col->rds == nullptr || col->rdsf == nullptr ||
+            col->rho0_padded == nullptr || !(col->ztop > 0.0f) || !std::isfinite(col->ztop)) {
+            gm1b_set_error("gm1b_terrain_open_stage_column: the terrain column needs sigma, sigmaf, rds, rdsf, "
+                           "rho0_padded and a finite ztop > 0");
+            return GM1B_ERR_ARGUMENT;
+        }
+        dz = 1.0;  // the scalar spacing is not used on a bound column
     }
     if (!(dx > 0.0f) || !(dy > 0.0f) || !(dz > 0.0) || !std::isfinite(dx) || !std::isfinite(dy) ||
         !std::isfinite(dz) || !(dt > 0.0f) || !std::isfinite(dt)) {
@@ -1047,12 +1128,25 @@ extern "C" int32_t gm1b_terrain_open_stage(int32_t ni, int32_t nj, int32_t nk, i
     p.zt = (float)((double)nk * dz);
     p.rzt = 1.0f / p.zt;
     p.halfcp = 1005.7f * 0.5f;
-    if (!edge_weights(nk, p.dz, false, p.cgs) || !edge_weights(nk, p.dz, true, p.cgt)) {
+    if (col != nullptr) {
+        // the lid is the bound top; the edge-face extrapolation keeps the
+        // open-boundary text's own 1.875 / -1.25 / 0.375 weights, which the
+        // profile patch leaves in place (cuda_terrain_open_boundary.py:845-850,
+        // cuda_gm1_child_psolver3_open.py:289-330)
+        p.vmode = 1;
+        p.sgm = col->sigma, p.sgmf = col->sigmaf, p.rdsp = col->rds, p.rdsfp = col->rdsf;
+        p.rho0p = col->rho0_padded;
+        p.zt = col->ztop;
+        p.rzt = 1.0f / p.zt;
+        const float w[3] = {1.875f, -1.25f, 0.375f};
+        for (int q = 0; q < 3; ++q) p.cgs[q] = p.cgt[q] = w[q];
+    } else if (!edge_weights(nk, p.dz, false, p.cgs) || !edge_weights(nk, p.dz, true, p.cgt)) {
         gm1b_set_error("gm1b_terrain_open_stage: degenerate vertical levels for dz=%g", dz);
         return GM1B_ERR_ARGUMENT;
     }
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    const size_t col_smem = (size_t)kTosArrays * (size_t)(nk + 2) * 32 * sizeof(float);
+    const int col_arrays = kTosArrays + (p.vmode ? 4 : 0);
+    const size_t col_smem = (size_t)col_arrays * (size_t)(nk + 2) * 32 * sizeof(float);
     static bool attr_set[64] = {};  // per device: the attribute belongs to each device's context
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
@@ -1061,8 +1155,11 @@ extern "C" int32_t gm1b_terrain_open_stage(int32_t ni, int32_t nj, int32_t nk, i
         return GM1B_ERR_CUDA;
     }
     if (!attr_set[dev]) {
-        const cudaError_t e = cudaFuncSetAttribute(tos_column_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                   (int)((size_t)kTosArrays * (kTosMaxNk + 2) * 32 * sizeof(float)));
+        cudaError_t e = cudaFuncSetAttribute(tos_column_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)((size_t)kTosArrays * (kTosMaxNk + 2) * 32 * sizeof(float)));
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(tos_column_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)((size_t)(kTosArrays + 4) * (kTosMaxNk + 2) * 32 * sizeof(float)));
         if (e != cudaSuccess) {
             gm1b_set_error("cudaFuncSetAttribute(tos_column_kernel): %s", cudaGetErrorString(e));
             return GM1B_ERR_CUDA;
@@ -1092,7 +1189,10 @@ extern "C" int32_t gm1b_terrain_open_stage(int32_t ni, int32_t nj, int32_t nk, i
         }
         {
             ProfScope ps("tos_column_kernel", st);
-            tos_column_kernel<<<col_grid, dim3(32, kTosWarps), col_smem, st>>>(p);
+            if (p.vmode)
+                tos_column_kernel<1><<<col_grid, dim3(32, kTosWarps), col_smem, st>>>(p);
+            else
+                tos_column_kernel<0><<<col_grid, dim3(32, kTosWarps), col_smem, st>>>(p);
             ps.stop();
             if (!launch_ok("tos_column_kernel")) return GM1B_ERR_CUDA;
         }
@@ -1122,4 +1222,29 @@ extern "C" int32_t gm1b_terrain_open_stage(int32_t ni, int32_t nj, int32_t nk, i
         if (!launch_ok("tos_fill2_kernel")) return GM1B_ERR_CUDA;
     }
     return GM1B_OK;
+}
+
+}  // namespace
+}  // namespace gm1b
+
+extern "C" int32_t gm1b_terrain_open_stage(int32_t ni, int32_t nj, int32_t nk, int32_t nrk, float dt, int32_t nsound,
+                                           float dx, float dy, double dz, float alph, float kdiv, uint32_t ablations,
+                                           uint32_t flags, const gm1b_terrain_open_arrays *arrays,
+                                           const gm1b_terrain_metrics *metrics, void *stream) {
+    return terrain_open_stage(ni, nj, nk, nrk, dt, nsound, dx, dy, dz, alph, kdiv, ablations, flags, arrays, metrics,
+                              nullptr, stream);
+}
+
+extern "C" int32_t gm1b_terrain_open_stage_column(int32_t ni, int32_t nj, int32_t nk, int32_t nrk, float dt,
+                                                  int32_t nsound, float dx, float dy, float alph, float kdiv,
+                                                  uint32_t ablations, uint32_t flags,
+                                                  const gm1b_terrain_open_arrays *arrays,
+                                                  const gm1b_terrain_metrics *metrics,
+                                                  const gm1b_momentum_column *column, void *stream) {
+    if (column == nullptr) {
+        gm1b_set_error("gm1b_terrain_open_stage_column: column is NULL");
+        return GM1B_ERR_ARGUMENT;
+    }
+    return terrain_open_stage(ni, nj, nk, nrk, dt, nsound, dx, dy, 1.0, alph, kdiv, ablations, flags, arrays, metrics,
+                              column, stream);
 }

@@ -192,6 +192,13 @@ def _lib():
                                                                   c.c_uint32, c.POINTER(_Arrays),
                                                                   c.POINTER(_Metrics), c.c_void_p]
         lib.gm1b_terrain_open_stage.restype = c.c_int32
+        from .momentum import _Column
+        lib.gm1b_terrain_open_stage_column.argtypes = [c.c_int32] * 4 + [c.c_float, c.c_int32, c.c_float, c.c_float,
+                                                                         c.c_float, c.c_float, c.c_uint32,
+                                                                         c.c_uint32, c.POINTER(_Arrays),
+                                                                         c.POINTER(_Metrics), c.POINTER(_Column),
+                                                                         c.c_void_p]
+        lib.gm1b_terrain_open_stage_column.restype = c.c_int32
         lib._tos_bound = True
     return lib
 
@@ -357,3 +364,132 @@ def launch_cuda_psolver3_terrain_open_stage(arrays: Mapping[str, Any], metrics: 
                                                            dx=dx, dy=dy, dz=dz, _nrk_sequence=(nrk,), **kwargs)
     receipt = {**launch.receipt, "nrk": nrk, "three_stage_composition": False}
     return CudaPsolver3TerrainOpenLaunch(launch.ready_event, launch.compiled, launch.cadence, receipt)
+
+
+def launch_cuda_gm1_child_psolver3_open_stage(
+        arrays: Mapping[str, Any], metrics: Mapping[str, Any], *, ni: int, nj: int, nk: int, nrk: int, dt: float,
+        nsound: int, dx: float, dy: float, vertical: Any, selection: TerrainOpenSelection = DEFAULT_TERRAIN_OPEN_SELECTION,
+        ablations: TerrainOpenSoundAblations | None = None, stream: Any | None = None,
+        compiled: CompiledPsolver3TerrainOpenKernels | None = None, alph: float | None = None,
+        kdiv: float | None = None, lateral_sides: tuple[int, int, int, int] = (2, 2, 2, 2),
+        **unused: Any) -> CudaPsolver3TerrainOpenLaunch:
+    """Enqueue one acoustic RK stage on a stretched terrain column
+    (src/cm1core/cuda_gm1_child_psolver3_open.py:848, terrain branch).
+    ``vertical`` is a :class:`gm1_b200.momentum.StretchedMomentumColumn` with
+    ``flat=False``: its ``sigma`` (nk+2), ``sigmaf`` (nk+3), ``rds`` (nk+2),
+    ``rdsf`` (nk+3) and the lid ``ztop``, which must be the column's own
+    sigmaf(nk+1) (param.F:8193).  ``metrics`` carries the 25 terrain metrics
+    and ``rho0_padded`` (nk+2, nj+6, ni+6), the source-valid padded base
+    density whose face averages weight the pressure advection.  There is no
+    dz: every vertical derivative reads the profiles.  The terrain stage is
+    sealed to four open sides; the flat column's stage is not built."""
+    from .momentum import StretchedMomentumColumn, _Column
+    from .periodic import sound3_stage_schedule_f32
+
+    for name in unused:
+        if name not in ("open_compiled", "lateral_compiled", "workspace", "allow_compact_validation",
+                        "allow_uniform_idealized_validation", "nest_substep"):
+            raise TypeError(f"unexpected keyword {name!r}")
+    if unused.get("nest_substep") is not None:
+        refuse(code="CM1-TERRAIN-NEST-SUBSTEP", gate="dry-dynamics", option="nest_substep",
+               value=type(unused["nest_substep"]).__name__, reason="a nest's specified zone edits the state between "
+               "the phases of every small step", remedy="run the stage without a live nest")
+    validate_terrain_open_selection(selection)
+    if not isinstance(vertical, StretchedMomentumColumn):
+        raise TypeError("vertical must be a StretchedMomentumColumn")
+    if vertical.flat:
+        raise ValueError("the flat column's acoustic statements (sound.F:119-143, 318-342, 491-509, 742-765) are not "
+                         "built; bind a terrain column (flat=False)")
+    if tuple(lateral_sides) != (2, 2, 2, 2):
+        raise ValueError(f"lateral_sides {tuple(lateral_sides)}: the terrain child acoustic stage runs bc.F's ssopenbc "
+                         "on all four sides and its pressure gradient skips every boundary face")
+    for name, value in (("alph", alph), ("kdiv", kdiv)):
+        if value is None:
+            continue
+        if isinstance(value, bool) or not isinstance(value, (int, float)):
+            raise TypeError(f"{name} must be numeric or None")
+        if not (0.0 <= float(value) <= 1.0):
+            raise ValueError(f"{name}={value} is outside CM1's admitted [0, 1]")
+    for name, value in (("ni", ni), ("nj", nj), ("nk", nk)):
+        if isinstance(value, bool) or not isinstance(value, int):
+            raise ValueError(f"{name} must be an integer")
+    if nk < 4:
+        raise ValueError("child psolver requires nk >= 4; param.F:8985-9060 extrapolates from four scalar levels at "
+                         "each end of the column")
+    if ni < 3 or nj < 3:
+        raise ValueError("child psolver requires ni,nj >= 3")
+    if isinstance(nrk, bool) or not isinstance(nrk, int) or nrk not in (1, 2, 3):
+        raise ValueError("nrk must be 1, 2, or 3")
+    dt, dx, dy = (_positive(n, v) for n, v in (("dt", dt), ("dx", dx), ("dy", dy)))
+    if isinstance(nsound, bool) or not isinstance(nsound, int) or nsound < 1:
+        raise ValueError("nsound must be a positive integer")
+    if ablations is None:
+        ablations = TerrainOpenSoundAblations()
+    if not isinstance(ablations, TerrainOpenSoundAblations):
+        raise TypeError("ablations must be TerrainOpenSoundAblations")
+    compiled = compiled or compile_cuda_psolver3_terrain_open()
+    if not isinstance(compiled, CompiledPsolver3TerrainOpenKernels):
+        raise TypeError("compiled must come from compile_cuda_psolver3_terrain_open")
+    retain = compiled.retain_column_diagnostics
+    a = _require_device_arrays(arrays, ni=ni, nj=nj, nk=nk, retain_column_diagnostics=retain)
+    m = _require_device_metrics(metrics, ni=ni, nj=nj, nk=nk)
+    if "rho0_padded" not in metrics:
+        raise ValueError("metrics must expose source-valid padded rho0 as rho0_padded; physical rho0_3d cannot "
+                         "source outer-face averages")
+    rho0p = metrics["rho0_padded"]
+    shape = (nk + 2, nj + 6, ni + 6)
+    if not (isinstance(rho0p, torch.Tensor) and rho0p.is_cuda and rho0p.dtype == torch.float32
+            and tuple(rho0p.shape) == shape and rho0p.is_contiguous()):
+        raise ValueError(f"rho0_padded must be device C-f32 {shape}")
+    if any(rho0p.data_ptr() == t.data_ptr() for t in a.values()):
+        raise ValueError("rho0_padded must not alias a mutable acoustic array")
+    prof = {}
+    for n, pshape in (("sigma", (nk + 2,)), ("sigmaf", (nk + 3,)), ("rds", (nk + 2,)), ("rdsf", (nk + 3,))):
+        t = getattr(vertical, n)
+        if not (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == torch.float32
+                and tuple(t.shape) == pshape and t.is_contiguous()):
+            raise ValueError(f"vertical {n} must be device C-f32 {pshape}")
+        prof[n] = t
+    if len({t.data_ptr() for t in prof.values()}) != 4:
+        raise ValueError("vertical profiles must not alias")
+    ztop = float(np.float32(vertical.ztop))
+    if not (math.isfinite(ztop) and ztop > 0.0):
+        raise ValueError("vertical top must be finite and greater than zero")
+    top_face = float(prof["sigmaf"][nk + 1].item())
+    if top_face != ztop:
+        raise ValueError(f"vertical top {ztop} m is not this coordinate's own sigmaf(nk+1) of {top_face} m "
+                         "(param.F:8193)")
+    device = a["u3d"].device
+    if any(t.device != device for t in (*a.values(), *m.values(), rho0p, *prof.values())):
+        raise ValueError("terrain/open arrays, metrics and profiles must live on one CUDA device")
+    alph32 = float(np.float32(CM1_ALPH_F32 if alph is None else alph))
+    kdiv32 = float(np.float32(CM1_KDIV_F32 if kdiv is None else kdiv))
+    mask = _ablation_mask(ablations)
+    lib = _lib()
+    st = torch.cuda.current_stream(device) if stream is None else stream
+    sa = _Arrays(**{n: a[n].data_ptr() for n in ALL_ARRAY_NAMES})
+    sm = _Metrics(**{n: m[n].data_ptr() for n in _STRUCT_METRICS})
+    col = _Column(0, rho0p.data_ptr(), prof["sigma"].data_ptr(), prof["sigmaf"].data_ptr(), prof["rds"].data_ptr(),
+                  prof["rdsf"].data_ptr(), ztop, None, None, None, 0.0)
+    nloop, dts = sound3_stage_schedule_f32(dt, nsound, nrk)
+    with torch.cuda.device(device), torch.cuda.stream(st):
+        _native.check(lib.gm1b_terrain_open_stage_column(ni, nj, nk, nrk, dt, nsound, dx, dy, alph32, kdiv32, mask,
+                                                         GM1B_TOS_DIAGNOSTICS if retain else 0, ctypes.byref(sa),
+                                                         ctypes.byref(sm), ctypes.byref(col),
+                                                         ctypes.c_void_p(st.cuda_stream)),
+                      "gm1b_terrain_open_stage_column")
+        event = torch.cuda.Event()
+        event.record(st)
+    cadence = ({"nrk": nrk, "nloop": nloop, "dts_f32": float(dts),
+                "open_consumptions": nloop if ablations.open_consumption else 0,
+                "pressure_fills": nloop - 1 if ablations.between_step_pressure_fill else 0,
+                "radiation_productions": 1 if ablations.radiation_history_production else 0},)
+    receipt: dict[str, Any] = {
+        "domain": {"ni": ni, "nj": nj, "nk": nk, "ngxy": CM1_OPEN_NGXY},
+        "vertical": {"branch": "terrain", "ztop_f32": ztop, "dz": None},
+        "cadence": list(cadence), "nrk": nrk,
+        "acoustic_reals": {"alph": alph32, "kdiv": kdiv32},
+        "comparison_contract": {"mode": "raw-bit", "max_ulp": 0, "null_or_missing_is_pass": False},
+        "lateral_boundaries": {"selection": {"wbc": 2, "ebc": 2, "sbc": 2, "nbc": 2}},
+    }
+    return CudaPsolver3TerrainOpenLaunch(event, compiled, cadence, receipt)

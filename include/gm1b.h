@@ -509,6 +509,19 @@ GM1B_API int32_t gm1b_terrain_open_stage(int32_t ni, int32_t nj, int32_t nk, int
                                          uint32_t flags, const gm1b_terrain_open_arrays *arrays,
                                          const gm1b_terrain_metrics *metrics, void *stream);
 
+/* The same stage on a stretched terrain column (replaces
+ * launch_cuda_gm1_child_psolver3_open_stage, cuda_gm1_child_psolver3_open.py:848,
+ * terrain branch): sigma/sigmaf/rds/rdsf at CM1's indices, the lid ztop and
+ * the padded base density rho0_padded (nk+2, nj+6, ni+6) come from column
+ * (flat = 0; a flat column is refused).  No dz: every vertical derivative
+ * reads the profiles.  Allocation-free; graph-capturable. */
+GM1B_API int32_t gm1b_terrain_open_stage_column(int32_t ni, int32_t nj, int32_t nk, int32_t nrk, float dt,
+                                                int32_t nsound, float dx, float dy, float alph, float kdiv,
+                                                uint32_t ablations, uint32_t flags,
+                                                const gm1b_terrain_open_arrays *arrays,
+                                                const gm1b_terrain_metrics *metrics,
+                                                const gm1b_momentum_column *column, void *stream);
+
 /* ------------------------------------------------------------------------
  * Pieces that join the operators of the moist large step on the open lane.
  * ------------------------------------------------------------------------ */

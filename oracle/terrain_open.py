@@ -50,6 +50,10 @@ def _lib():
         lib.oracle_terrain_open_stage.restype = c.c_int
         lib.oracle_terrain_edge_weights.argtypes = [c.c_int, c.c_float, c.POINTER(c.c_float), c.POINTER(c.c_float)]
         lib.oracle_terrain_edge_weights.restype = None
+        lib.oracle_terrain_open_stage_column.argtypes = [c.POINTER(TosArrays), c.POINTER(TosMetrics)] + \
+            [c.c_int] * 4 + [c.c_float, c.c_int, c.c_float, c.c_float] + [_F] * 4 + [c.c_float, _F] + \
+            [c.c_float, c.c_float, c.c_uint, c.POINTER(c.c_float)]
+        lib.oracle_terrain_open_stage_column.restype = c.c_int
         lib._tos_ready = True
     return lib
 
@@ -71,6 +75,25 @@ def terrain_open_stage(a, m, *, ni, nj, nk, nrk, dt, nsound, dx, dy, dz, alph=0.
                                          float(dz), alph, kdiv, ablations, diag)
     if rc != 0:
         raise ValueError(f"oracle_terrain_open_stage failed ({rc})")
+    return StageDiagnostics(nrk, int(diag[0]), float(diag[1]), float(diag[2]))
+
+
+def terrain_open_stage_column(a, m, column, *, ni, nj, nk, nrk, dt, nsound, dx, dy, alph=0.6, kdiv=0.1,
+                              ablations=ALL_ABLATIONS) -> StageDiagnostics:
+    """One stage on a stretched terrain column: ``column`` maps sigma,
+    sigmaf, rds, rdsf (CM1-indexed float32 profiles), ztop and rho0p (the
+    padded base density, (nk+2, nj+6, ni+6))."""
+    sa, sm = _bind(TosArrays, ARRAY_NAMES, a), _bind(TosMetrics, METRIC_NAMES, m)
+    prof = {n: np.ascontiguousarray(column[n], dtype=np.float32) for n in ("sigma", "sigmaf", "rds", "rdsf", "rho0p")}
+    assert prof["rho0p"].shape == (nk + 2, nj + 6, ni + 6)
+    diag = (ctypes.c_float * 3)()
+    ptr = {n: v.ctypes.data_as(_F) for n, v in prof.items()}
+    rc = _lib().oracle_terrain_open_stage_column(ctypes.byref(sa), ctypes.byref(sm), ni, nj, nk, nrk, dt, nsound, dx,
+                                                dy, ptr["sigma"], ptr["sigmaf"], ptr["rds"], ptr["rdsf"],
+                                                float(np.float32(column["ztop"])), ptr["rho0p"], alph, kdiv,
+                                                ablations, diag)
+    if rc != 0:
+        raise ValueError(f"oracle_terrain_open_stage_column failed ({rc})")
     return StageDiagnostics(nrk, int(diag[0]), float(diag[1]), float(diag[2]))
 
 

@@ -513,15 +513,29 @@ static void initial_fpk(TosArrays *a, const TosMetrics *m, const G *g, const Pro
             }
 }
 
+/* rho0p == NULL: the uniform operator's base density rho0_3d(k, 1, 1) on
+ * every face.  Otherwise each face's own average of the padded base density
+ * (nk+2, nj+6, ni+6), the stretched terrain column's xurho / yvrho
+ * (cuda_gm1_child_psolver3_open.py:199-205, sound.F:604-613). */
 static void pressure_advection(TosArrays *a, const TosMetrics *m, const G *g, const Prof *p, float *xu, float *yv,
-                               float dts, float rdx, float rdy, float beta, float zt, float rzt) {
+                               float dts, float rdx, float rdy, float beta, float zt, float rzt, const float *rho0p) {
     const int ni = g->ni, nj = g->nj, nk = g->nk;
+    const size_t pw = (size_t)ni + 6, pp = (size_t)(nj + 6) * pw;
     for (int k = 1; k <= nk; ++k) {
         const float rho = m->rho0_3d[M(g, k - 1, 0, 0)];
+        const float *r = rho0p ? rho0p + (size_t)k * pp : NULL;
         for (int j0 = 0; j0 < nj; ++j0)
-            for (int f = 0; f <= ni; ++f) XU(k, j0, f) = rho * XU(k, j0, f);
+            for (int f = 0; f <= ni; ++f) {
+                const size_t o = (size_t)(j0 + 3) * pw + (size_t)(f + 2);
+                const float dens = r ? 0.5f * (r[o] + r[o + 1]) : rho;
+                XU(k, j0, f) = dens * XU(k, j0, f);
+            }
         for (int f = 0; f <= nj; ++f)
-            for (int i0 = 0; i0 < ni; ++i0) YV(k, f, i0) = rho * YV(k, f, i0);
+            for (int i0 = 0; i0 < ni; ++i0) {
+                const size_t o = (size_t)(f + 2) * pw + (size_t)(i0 + 3);
+                const float dens = r ? 0.5f * (r[o] + r[o + pw]) : rho;
+                YV(k, f, i0) = dens * YV(k, f, i0);
+            }
     }
     memset(a->hadvp, 0, sizeof(float) * (size_t)(nk + 2) * (nj + 2) * (ni + 2));
     for (int kf = 2; kf <= nk; ++kf) {
@@ -641,17 +655,49 @@ static void average_velocities(TosArrays *a, const G *g, int n, int nloop, float
  * taken in double (the reference forms zt as float32(nk * dz) with a Python
  * float dz); everything else is binary32.  diag[0] = nloop, diag[1] = dts,
  * diag[2] = max |tri_residual| over the physical levels 2..nk. */
+static int stage_impl(TosArrays *a, const TosMetrics *m, int ni, int nj, int nk, int nrk, float dt, int nsound,
+                      float dx, float dy, const Prof *pp, float zt, const float *rho0p, float alph, float kdiv,
+                      unsigned ablations, float *diag);
+
 int oracle_terrain_open_stage(TosArrays *a, const TosMetrics *m, int ni, int nj, int nk, int nrk, float dt,
                               int nsound, float dx, float dy, double dz, float alph, float kdiv, unsigned ablations,
                               float *diag) {
     if (ni < 3 || nj < 3 || nk < 4 || nrk < 1 || nrk > 3) return -1;
+    Prof p;
+    make_profiles(&p, nk, (float)dz);
+    const int rc = stage_impl(a, m, ni, nj, nk, nrk, dt, nsound, dx, dy, &p, (float)((double)nk * dz), NULL, alph,
+                              kdiv, ablations, diag);
+    free_profiles(&p);
+    return rc;
+}
+
+/* The stage on a stretched terrain column (cuda_gm1_child_psolver3_open.py:
+ * 152-330 patching the uniform texts): the caller's CM1-indexed sigma (nk+2),
+ * sigmaf (nk+3), rds (nk+2), rdsf (nk+3) in place of the in-kernel uniform
+ * coordinate, the lid ztop in place of nk*dz, face-averaged padded base
+ * density in the pressure advection, and the open-boundary text's literal
+ * 1.875 / -1.25 / 0.375 edge-face weights (cuda_terrain_open_boundary.py:
+ * 845-850, untouched by the patch) in place of the column's own. */
+int oracle_terrain_open_stage_column(TosArrays *a, const TosMetrics *m, int ni, int nj, int nk, int nrk, float dt,
+                                     int nsound, float dx, float dy, const float *sigma, const float *sigmaf,
+                                     const float *rds, const float *rdsf, float ztop, const float *rho0p, float alph,
+                                     float kdiv, unsigned ablations, float *diag) {
+    if (ni < 3 || nj < 3 || nk < 4 || nrk < 1 || nrk > 3 || !rho0p) return -1;
+    Prof p;
+    p.sigma = (float *)sigma, p.sigmaf = (float *)sigmaf, p.rds = (float *)rds, p.rdsf = (float *)rdsf;
+    const float w[3] = {1.875f, -1.25f, 0.375f};
+    for (int q = 0; q < 3; ++q) p.cgs[q] = p.cgt[q] = w[q];
+    return stage_impl(a, m, ni, nj, nk, nrk, dt, nsound, dx, dy, &p, ztop, rho0p, alph, kdiv, ablations, diag);
+}
+
+static int stage_impl(TosArrays *a, const TosMetrics *m, int ni, int nj, int nk, int nrk, float dt, int nsound,
+                      float dx, float dy, const Prof *pp, float zt, const float *rho0p, float alph, float kdiv,
+                      unsigned ablations, float *diag) {
     const G g = {ni, nj, nk};
     int nloop;
     float dts;
     if (oracle_stage_schedule(dt, nsound, nrk, &nloop, &dts) != 0) return -1;
-    Prof p;
-    make_profiles(&p, nk, (float)dz);
-    const float zt = (float)((double)nk * dz);
+    const Prof p = *pp;
     const float rzt = 1.0f / zt;
     const float beta = 1.0f - alph;
     const float rdx = 1.0f / dx, rdy = 1.0f / dy;
@@ -684,7 +730,7 @@ int oracle_terrain_open_stage(TosArrays *a, const TosMetrics *m, int ni, int nj,
         transformed_terms(a, m, &g, &p, zt, rzt, xu, yv);
         initial_fpk(a, m, &g, &p, xu, yv, dts, rdx, rdy, beta, (ablations & ABL_DIV) != 0);
         bcwsfc(a, m, &g);
-        if (ablations & ABL_PADV) pressure_advection(a, m, &g, &p, xu, yv, dts, rdx, rdy, beta, zt, rzt);
+        if (ablations & ABL_PADV) pressure_advection(a, m, &g, &p, xu, yv, dts, rdx, rdy, beta, zt, rzt, rho0p);
         implicit_and_update(a, &g, dts, nrk, n, nloop, alph, beta, kdiv, (ablations & ABL_IMPLICIT) != 0);
         if (n < nloop && (ablations & ABL_PFILL)) bcp_open(a->ppd, &g);
         average_velocities(a, &g, n, nloop, alph);
@@ -714,7 +760,6 @@ int oracle_terrain_open_stage(TosArrays *a, const TosMetrics *m, int ni, int nj,
     }
     free(xu);
     free(yv);
-    free_profiles(&p);
     return 0;
 }
 

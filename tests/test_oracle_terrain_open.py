@@ -86,3 +86,55 @@ def test_uniform_edge_weights_are_fornberg_quadratic():
     cgs, cgt = orc.edge_weights(8, 333.3)
     assert cgs == pytest.approx((1.875, -1.25, 0.375), abs=2e-6)
     assert cgt == pytest.approx((1.875, -1.25, 0.375), abs=2e-6)
+
+
+def _differs(x, y) -> bool:
+    return not np.array_equal(np.asarray(x).view(np.uint32), np.asarray(y).view(np.uint32))
+
+
+def _stretched_column(m, ni, nj, nk, lv):
+    from tests.test_oracle_momentum import _padded_rho0
+
+    return {"sigma": lv.sigma, "sigmaf": lv.sigmaf, "rds": lv.rds, "rdsf": lv.rdsf, "ztop": lv.ztop_m,
+            "rho0p": _padded_rho0(m["rho0_3d"], ni, nj, nk)}
+
+
+@pytest.mark.parametrize("ni,nj,nk,dz", [(9, 7, 6, 200.0), (12, 5, 10, 250.0)])
+def test_stretched_terrain_stage_on_a_uniform_column_is_the_uniform_stage(ni, nj, nk, dz):
+    """The stretched terrain-column restatement (the reference's profile-bound
+    acoustic texts, src/cm1core/cuda_gm1_child_psolver3_open.py:152-330) on a
+    uniform column with a horizontally uniform base density reproduces the
+    twin-pinned uniform stage word for word over three RK stages."""
+    from gm1_b200.vertical import uniform_vertical_levels
+    from tests.golden.make_golden import terrain_open_fixture
+
+    a, m = terrain_open_fixture(ni, nj, nk, 40 + ni)
+    m["rho0_3d"][:] = m["rho0_3d"][:, :1, :1]
+    lv = uniform_vertical_levels(nk, dz)
+    col = _stretched_column(m, ni, nj, nk, lv)
+    p = dict(ni=ni, nj=nj, nk=nk, dt=2.0, nsound=6, dx=450.0, dy=520.0)
+    want, got = {k: v.copy() for k, v in a.items()}, {k: v.copy() for k, v in a.items()}
+    for nrk in (1, 2, 3):
+        orc.terrain_open_stage(want, m, nrk=nrk, dz=dz, **p)
+        orc.terrain_open_stage_column(got, m, col, nrk=nrk, **p)
+    assert [n for n in orc.ARRAY_NAMES if _differs(got[n], want[n])] == []
+
+
+def test_stretched_terrain_stage_moves_with_the_profiles():
+    """On a stretched column (20 m at the ground to 200 m aloft) and a
+    horizontally varying base density the stage differs from the uniform one
+    in the prognostic winds and pressure, and stays finite."""
+    from gm1_b200.vertical import build_vertical_levels
+    from tests.golden.make_golden import terrain_open_fixture
+
+    ni, nj, nk = 9, 8, 10
+    a, m = terrain_open_fixture(ni, nj, nk, 77)
+    lv = build_vertical_levels(stretch_z=1, nk=nk, dz_m=100.0, ztop_m=1100.0, str_bot_m=40.0, str_top_m=700.0,
+                               dz_bot_m=20.0, dz_top_m=200.0)
+    col = _stretched_column(m, ni, nj, nk, lv)
+    p = dict(ni=ni, nj=nj, nk=nk, nrk=2, dt=2.0, nsound=6, dx=450.0, dy=520.0)
+    want, got = {k: v.copy() for k, v in a.items()}, {k: v.copy() for k, v in a.items()}
+    orc.terrain_open_stage(want, m, dz=110.0, **p)
+    orc.terrain_open_stage_column(got, m, col, **p)
+    for n in ("u3d", "v3d", "w3d", "pp3d"):
+        assert np.isfinite(got[n]).all() and _differs(got[n], want[n]), n

@@ -113,3 +113,79 @@ def test_oversized_column_refused_by_the_library():
     with pytest.raises(Gm1bError, match="nk"):
         tos.launch_cuda_psolver3_terrain_open_three_stage(dev, mdev, ni=ni, nj=nj, nk=nk, dt=2.0, nsound=6, dx=1.0,
                                                           dy=1.0, dz=100.0)
+
+
+def _column(lv, m, ni, nj, nk):
+    from gm1_b200.momentum import StretchedMomentumColumn
+    from tests.test_oracle_momentum import _padded_rho0
+
+    rho0p = _padded_rho0(m["rho0_3d"], ni, nj, nk)
+    t = lambda x: torch.from_numpy(np.array(x, dtype=np.float32)).cuda()  # noqa: E731
+    vertical = StretchedMomentumColumn(False, None, sigma=t(lv.sigma), sigmaf=t(lv.sigmaf), rds=t(lv.rds),
+                                       rdsf=t(lv.rdsf), ztop=lv.ztop_m)
+    host = {"sigma": lv.sigma, "sigmaf": lv.sigmaf, "rds": lv.rds, "rdsf": lv.rdsf, "ztop": lv.ztop_m,
+            "rho0p": rho0p}
+    return vertical, host, t(rho0p)
+
+
+@pytest.mark.parametrize("ni,nj,nk,spec", [(37, 21, 10, (1100.0, 40.0, 700.0)), (70, 9, 14, (1630.0, 40.0, 1030.0)),
+                                           (3, 3, 10, (1100.0, 40.0, 700.0))])
+def test_stretched_terrain_stage_matches_oracle(ni, nj, nk, spec):
+    """launch_cuda_gm1_child_psolver3_open_stage on a generated stretched
+    column (20 m at the ground to 200 m aloft) and a horizontally varying
+    padded base density: every array, scratch included, word-identical to the
+    oracle restatement after each of the three RK stages."""
+    from gm1_b200.vertical import build_vertical_levels
+
+    lv = build_vertical_levels(stretch_z=1, nk=nk, dz_m=100.0, ztop_m=spec[0], str_bot_m=spec[1],
+                               str_top_m=spec[2], dz_bot_m=20.0, dz_top_m=200.0)
+    a, m = terrain_open_fixture(ni, nj, nk, 300 + ni)
+    vertical, host, rho0p = _column(lv, m, ni, nj, nk)
+    p = dict(ni=ni, nj=nj, nk=nk, dt=2.0, nsound=6, dx=450.0, dy=520.0)
+    ref = {k: v.copy() for k, v in a.items()}
+    dev, mdev = _dev(a), _dev(m)
+    mdev["rho0_padded"] = rho0p
+    for nrk in (1, 2, 3):
+        orc.terrain_open_stage_column(ref, m, host, nrk=nrk, **p)
+        r = tos.launch_cuda_gm1_child_psolver3_open_stage(dev, mdev, nrk=nrk, vertical=vertical, **p)
+        r.ready_event.synchronize()
+        assert _bad(dev, ref, tos.ALL_ARRAY_NAMES) == [], f"nrk={nrk}"
+
+
+def test_stretched_terrain_stage_on_a_uniform_column_is_the_uniform_stage():
+    from gm1_b200.vertical import uniform_vertical_levels
+
+    ni, nj, nk, dz = 40, 11, 12, 250.0
+    a, m = terrain_open_fixture(ni, nj, nk, 5)
+    m["rho0_3d"][:] = m["rho0_3d"][:, :1, :1]
+    vertical, _, rho0p = _column(uniform_vertical_levels(nk, dz), m, ni, nj, nk)
+    p = dict(ni=ni, nj=nj, nk=nk, dt=2.0, nsound=6, dx=450.0, dy=520.0)
+    one, two, mdev = _dev(a), _dev(a), _dev(m)
+    mdev["rho0_padded"] = rho0p
+    tos.launch_cuda_psolver3_terrain_open_three_stage(one, mdev, dz=dz, **p)
+    for nrk in (1, 2, 3):
+        tos.launch_cuda_gm1_child_psolver3_open_stage(two, mdev, nrk=nrk, vertical=vertical, **p)
+    torch.cuda.synchronize()
+    assert _bad(two, {k: v.cpu().numpy() for k, v in one.items()}, tos.ALL_ARRAY_NAMES) == []
+
+
+def test_stretched_terrain_stage_refusals():
+    from gm1_b200.momentum import StretchedMomentumColumn
+    from gm1_b200.vertical import uniform_vertical_levels
+
+    ni, nj, nk = 9, 8, 6
+    a, m = terrain_open_fixture(ni, nj, nk, 5)
+    vertical, _, rho0p = _column(uniform_vertical_levels(nk, 200.0), m, ni, nj, nk)
+    dev, mdev = _dev(a), _dev(m)
+    p = dict(ni=ni, nj=nj, nk=nk, nrk=1, dt=2.0, nsound=6, dx=450.0, dy=520.0)
+    with pytest.raises(ValueError, match="rho0_padded"):
+        tos.launch_cuda_gm1_child_psolver3_open_stage(dev, mdev, vertical=vertical, **p)
+    mdev["rho0_padded"] = rho0p
+    with pytest.raises(ValueError, match="flat column"):
+        tos.launch_cuda_gm1_child_psolver3_open_stage(dev, mdev, vertical=StretchedMomentumColumn(True, None), **p)
+    with pytest.raises(ValueError, match="sigmaf"):
+        bad = StretchedMomentumColumn(False, None, sigma=vertical.sigma, sigmaf=vertical.sigmaf, rds=vertical.rds,
+                                      rdsf=vertical.rdsf, ztop=vertical.ztop + 10.0)
+        tos.launch_cuda_gm1_child_psolver3_open_stage(dev, mdev, vertical=bad, **p)
+    with pytest.raises(ValueError, match="four sides"):
+        tos.launch_cuda_gm1_child_psolver3_open_stage(dev, mdev, vertical=vertical, lateral_sides=(1, 1, 2, 2), **p)
