@@ -56,6 +56,11 @@ struct TosArgs {
     // density (nk+2, nj+6, ni+6); unused on the uniform column (vmode 0)
     int vmode;
     const float *sgm, *sgmf, *rdsp, *rdsfp, *rho0p;
+    // the flat stretched column (vmode 2): mh (nk+2), mf (nk+3), rdz and the
+    // packed lateral code wbc | ebc << 4 | sbc << 8 | nbc << 12
+    const float *mhp, *mfp;
+    float rdz;
+    unsigned obc;
 };
 
 // 32-bit element offsets: the host refuses grids whose largest padded
@@ -143,7 +148,23 @@ __global__ void __launch_bounds__(256) tos_prepare_kernel(TosArgs p) {
             a.w3d[qw] = a.wa[qw];
         }
         const bool phys = j >= 1 && j <= nj && i >= 1 && i <= ni;
-        if (phys) {
+        if (phys && p.vmode == 2) {
+            // sound.F:119-143 on the flat column: rdz*mh(k), rdz*mf(k) and the
+            // base state at CM1's (1,1,k); mm at every level
+            // (cuda_gm1_child_psolver3_open.py:374-385)
+            const float t0 = (p.dts * p.rdz) * __ldg(p.mhp + k);
+            const float rr = m.rr0[X.m(k - 1, 0, 0)];
+            const float r2 = (t0 * rr) * m.rf0[X.m(k, 0, 0)];
+            const float r1 = (t0 * rr) * m.rf0[X.m(k - 1, 0, 0)];
+            const float tem1 = ((p.dts * p.rdz) * 1005.7f) * __ldg(p.mfp + k);
+            const float c1a = m.c1[X.m(k - 1, 0, 0)], c1b = m.c1[X.m(k, 0, 0)];
+            const float c2a = m.c2[X.m(k - 1, 0, 0)], c2b = m.c2[X.m(k, 0, 0)];
+            const float pc = a.piadv[c];
+            a.qk[c] = t0 * a.ppterm[c];
+            a.pk2[c] = k == nk ? 0.0f : r2 * ((-c2b) * a.piadv[X.p(k + 1, j, i)] + (1.0f - c1b) * pc);
+            a.pk1[c] = k == 1 ? 0.0f : r1 * (c1a * a.piadv[X.p(k - 1, j, i)] + (c2a - 1.0f) * pc);
+            a.mm[c] = tem1 * (c2a * a.thv[c] + c1a * a.thv[X.p(k - 1, j, i)]);
+        } else if (phys) {
             const int j0 = j - 1, i0 = i - 1;
             const float gz = m.gz[X.h(j0, i0)];
             const float tem = p.dts * vrdsf(p, k);
@@ -254,6 +275,83 @@ __global__ void __launch_bounds__(128) tos_edge_kernel(TosArgs p) {
         const size_t o = ew ? X.u(k, yu, xu) : X.v(k, yu, xu);
         const float tnd = r + ten[o];
         qout[o] = (upd0 ? q0[k] : q1[k]) + p.dts * tnd;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// flat column, open-side normal velocity (bc.F:2410-2419 and its three
+// twins): one thread per (k, row) of the west/east faces, then per (k,
+// column) of the south/north faces; only sides whose code is 2 (open)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) tos_flat_edge_kernel(TosArgs p) {
+    const Ix X{p.ni, p.nj};
+    const int ni = p.ni, nj = p.nj, nk = p.nk;
+    const gm1b_terrain_open_arrays &a = p.a;
+    const unsigned we = (unsigned)nk * (unsigned)nj, total = we + (unsigned)nk * (unsigned)ni;
+    for (unsigned z = blockIdx.x * blockDim.x + threadIdx.x; z < total; z += gridDim.x * blockDim.x) {
+        if (z < we) {
+            const int k = (int)(z / (unsigned)nj) + 1, y = (int)(z % (unsigned)nj) + 3;
+            const size_t r = (size_t)k * (nj + 6) + y;
+            if ((p.obc & 15u) == 2u) {
+                const unsigned b = X.u(k, y, 3);
+                const float t = (((-a.radbcw[r]) * (a.u3d[X.u(k, y, 4)] - a.u3d[b])) * p.rdx) * a.uh[3] + a.uten[b];
+                a.u3d[b] = a.u3d[b] + p.dts * t;
+            }
+            if (((p.obc >> 4) & 15u) == 2u) {
+                const unsigned b = X.u(k, y, ni + 3);
+                const float t =
+                    (((-a.radbce[r]) * (a.u3d[b] - a.u3d[X.u(k, y, ni + 2)])) * p.rdx) * a.uh[ni + 2] + a.uten[b];
+                a.u3d[b] = a.u3d[b] + p.dts * t;
+            }
+        } else {
+            const unsigned q = z - we;
+            const int k = (int)(q / (unsigned)ni) + 1, x = (int)(q % (unsigned)ni) + 3;
+            const size_t r = (size_t)k * (ni + 6) + x;
+            if (((p.obc >> 8) & 15u) == 2u) {
+                const unsigned b = X.v(k, 3, x);
+                const float t = (((-a.radbcs[r]) * (a.v3d[X.v(k, 4, x)] - a.v3d[b])) * p.rdy) * a.vh[3] + a.vten[b];
+                a.v3d[b] = a.v3d[b] + p.dts * t;
+            }
+            if (((p.obc >> 12) & 15u) == 2u) {
+                const unsigned b = X.v(k, nj + 3, x);
+                const float t =
+                    (((-a.radbcn[r]) * (a.v3d[b] - a.v3d[X.v(k, nj + 2, x)])) * p.rdy) * a.vh[nj + 2] + a.vten[b];
+                a.v3d[b] = a.v3d[b] + p.dts * t;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// flat column pressure gradient (sound.F:318-342): every face i = 1..ni+1,
+// j = 1..nj+1 takes u + (dts*dtu0)*(uten - pgrad), dtu0 = 1 on the faces
+// param.F:9182-9219 admits (a periodic side's boundary face included), 0
+// elsewhere; one thread per (j, i), marching k
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) tos_flat_pgrad_kernel(TosArgs p) {
+    const Ix X{p.ni, p.nj};
+    const int ni = p.ni, nj = p.nj, nk = p.nk;
+    const int i = blockIdx.x * 32 + threadIdx.x + 1;
+    const int j = blockIdx.y * 4 + threadIdx.y + 1;
+    if (i > ni + 1 || j > nj + 1) return;
+    const gm1b_terrain_open_arrays &a = p.a;
+    const bool pw = (p.obc & 15u) == 1u, pe = ((p.obc >> 4) & 15u) == 1u;
+    const bool ps = ((p.obc >> 8) & 15u) == 1u, pn = ((p.obc >> 12) & 15u) == 1u;
+    const float wu = (j <= nj && (i > 1 || pw) && (i < ni + 1 || pe)) ? 1.0f : 0.0f;
+    const float wv = (i <= ni && (j > 1 || ps) && (j < nj + 1 || pn)) ? 1.0f : 0.0f;
+    const float tem1 = (p.rdx * 1005.7f) * 0.5f, tem2 = (p.rdy * 1005.7f) * 0.5f;
+    const float du = p.dts * wu, dv = p.dts * wv;
+    for (int k = 1; k <= nk; ++k) {
+        const unsigned c = X.p(k, j, i);
+        const float pc = __ldg(a.ppd + c), tc = __ldg(a.thv + c);
+        float pu = tem1 * (pc - __ldg(a.ppd + X.p(k, j, i - 1)));
+        pu = pu * (tc + __ldg(a.thv + X.p(k, j, i - 1)));
+        const unsigned xu = X.u(k, j + 2, i + 2);
+        a.u3d[xu] = a.u3d[xu] + du * (__ldg(a.uten + xu) - pu);
+        float pv = tem2 * (pc - __ldg(a.ppd + X.p(k, j - 1, i)));
+        pv = pv * (tc + __ldg(a.thv + X.p(k, j - 1, i)));
+        const unsigned xv = X.v(k, j + 2, i + 2);
+        a.v3d[xv] = a.v3d[xv] + dv * (__ldg(a.vten + xv) - pv);
     }
 }
 
@@ -372,13 +470,19 @@ __global__ void __launch_bounds__(128) tos_pgrad_kernel(TosArgs p) {
 struct A2Load {
     float rk, rl, rk1, rrf_k, rrf_k1, qk, pk1, pk2, ppten, ppterm, pc, pe, pw, pn, ps, rr0;
     __device__ __forceinline__ void load(const gm1b_terrain_open_arrays &a, const gm1b_terrain_metrics &m,
-                                         const Ix &X, int k, int nk, int j, int i, bool adv) {
+                                         const Ix &X, int k, int nk, int j, int i, bool adv, bool flat) {
         rk = rl = rk1 = rrf_k = rrf_k1 = qk = pk1 = pk2 = ppten = ppterm = 0.0f;
         pc = pe = pw = pn = ps = rr0 = 0.0f;
         if (k > nk) return;
         const int j0 = j - 1, i0 = i - 1;
         const unsigned c = X.p(k, j, i);
-        if (adv) {
+        if (flat) {  // the flat column's pi' advection reads piadv only
+            pc = __ldg(a.piadv + c);
+            pe = __ldg(a.piadv + c + 1);
+            pw = __ldg(a.piadv + c - 1);
+            pn = __ldg(a.piadv + X.p(k, j + 1, i));
+            ps = __ldg(a.piadv + X.p(k, j - 1, i));
+        } else if (adv) {
             rk = __ldg(m.rho0_3d + X.m(k - 1, 0, 0));
             if (k >= 2) rl = __ldg(m.rho0_3d + X.m(k - 2, 0, 0));
             if (k < nk) rk1 = __ldg(m.rho0_3d + X.m(k, 0, 0));
@@ -478,6 +582,14 @@ __global__ void __launch_bounds__(32 * kTosWarps, 3) tos_column_kernel(TosArgs p
             }
             const float uw = __ldg(a.u3d + X.u(k, y, x)), ue = __ldg(a.u3d + X.u(k, y, x + 1));
             const float vs = __ldg(a.v3d + X.v(k, y, x)), vn = __ldg(a.v3d + X.v(k, y + 1, x));
+            if (VM == 2) {  // flat column: the face velocities and w as they are
+                SM(s_xw, k) = uw;
+                SM(s_xe, k) = ue;
+                SM(s_ys, k) = vs;
+                SM(s_yn, k) = vn;
+                SM(s_w, k) = wv;
+                continue;
+            }
             SM(s_xw, k) = uw * rgw;
             SM(s_xe, k) = ue * rge;
             SM(s_ys, k) = vs * rgs;
@@ -503,7 +615,7 @@ __global__ void __launch_bounds__(32 * kTosWarps, 3) tos_column_kernel(TosArgs p
     A2Load ld[kA2Levels];
     if (live) {
 #pragma unroll
-        for (int q = 0; q < kA2Levels; ++q) ld[q].load(a, m, X, 1 + wy + q * kTosWarps, nk, j, i, do_adv);
+        for (int q = 0; q < kA2Levels; ++q) ld[q].load(a, m, X, 1 + wy + q * kTosWarps, nk, j, i, do_adv, VM == 2);
     }
     __syncthreads();
     // A2: divergence, fpk (initial + pi' advection), column coefficients
@@ -511,7 +623,7 @@ __global__ void __launch_bounds__(32 * kTosWarps, 3) tos_column_kernel(TosArgs p
         for (int kb = 1 + wy; kb <= nk; kb += kTosWarps * kA2Levels) {
             if (kb != 1 + wy) {
 #pragma unroll
-                for (int q = 0; q < kA2Levels; ++q) ld[q].load(a, m, X, kb + q * kTosWarps, nk, j, i, do_adv);
+                for (int q = 0; q < kA2Levels; ++q) ld[q].load(a, m, X, kb + q * kTosWarps, nk, j, i, do_adv, VM == 2);
             }
 #pragma unroll
             for (int q = 0; q < kA2Levels; ++q) {
@@ -522,6 +634,32 @@ __global__ void __launch_bounds__(32 * kTosWarps, 3) tos_column_kernel(TosArgs p
             const float qk = ld[q].qk, pk1 = ld[q].pk1, pk2 = ld[q].pk2;
             const float ppten = ld[q].ppten, ppterm = ld[q].ppterm;
             const float pc = ld[q].pc, pe = ld[q].pe, pw = ld[q].pw, pn = ld[q].pn, ps = ld[q].ps, rr0 = ld[q].rr0;
+            if (VM == 2) {
+                // sound.F:491-509 (cuda_gm1_child_psolver3_open.py:407-419):
+                // fpk = ((dts*(ppten - ppterm*div)) + H) + beta*W, the flat
+                // divergence (smeps 1e-30) and pressure advection, W with
+                // w(k) and w(k+1) as they are
+                const float xw = SM(s_xw, k), xe = SM(s_xe, k), ys = SM(s_ys, k), yn = SM(s_yn, k);
+                float div = 0.0f;
+                if (do_div) {
+                    div = (xe - xw) * p.rdx + (yn - ys) * p.rdy;
+                    if (fabsf(div) < 1.0e-30f) div = 0.0f;
+                }
+                float hx = xw * (pc - pw) + xe * (pe - pc);
+                hx = (-hx) * p.temx;
+                float hy = ys * (pc - ps) + yn * (pn - pc);
+                hy = (-hy) * p.temy;
+                const float hp = hx + hy;
+                const float vert = SM(s_w, k) * (pk1 + qk) + SM(s_w, k + 1) * (pk2 - qk);
+                const float fpk = ((p.dts * (ppten - ppterm * div)) + hp) + p.beta * vert;
+                if (dlast) {
+                    a.divh[c] = div;
+                    a.hadvp[c] = hp;
+                    a.fpk[c] = fpk;
+                }
+                SM(s_fpk, k) = fpk;
+                continue;
+            }
             float d3k = 0.0f, d3k1 = 0.0f, hak = 0.0f, hak1 = 0.0f;
             if (k >= 2)
                 tos_level_terms<VM>(s_xw, s_xe, s_ys, s_yn, s_r, lane, k, p, dzdx, dzdy, gz, rk, rl, rrf_k, do_adv,
@@ -731,11 +869,12 @@ __global__ void __launch_bounds__(32 * kTosWarps, 3) tos_column_kernel(TosArgs p
                     a.tri_residual[c] = lhs - SM(s_dd, k);
                 }
             }
-            const float w1 = k == 1 ? 0.0f : wk, w2 = k == nk ? 0.0f : wk1;
+            // the flat column keeps w(1) and w(nk+1) and filters at 1e-30
+            const float w1 = (k == 1 && VM != 2) ? 0.0f : wk, w2 = (k == nk && VM != 2) ? 0.0f : wk1;
             const float old = cpp[q];
             const float vt = w1 * ca1[q] + w2 * ca2[q];
             float up = (old + SM(s_fpk, k)) + p.alph * vt;
-            if (fabsf(up) < 1.0e-20f) up = 0.0f;
+            if (fabsf(up) < (VM == 2 ? 1.0e-30f : 1.0e-20f)) up = 0.0f;
             const float tend = p.kdiv * (up - old);
             const float pd = up + tend;
             a.pp3d[c] = up;
@@ -919,7 +1058,7 @@ __global__ void __launch_bounds__(256) tos_fill2_kernel(TosArgs p) {
     const size_t nA = (size_t)nk * 6 * (ni + 3);           // u S/N, faces 0..ni+2
     const size_t nB = (size_t)nk * (nj + 3) * 6;           // v W/E, rows 0..nj+2
     const size_t nC = (size_t)(nk - 1) * 6 * (ni + 2);     // w S/N, k = 2..nk
-    const size_t nD = (size_t)nj * ni;                     // bcwsfc
+    const size_t nD = p.vmode == 2 ? 0 : (size_t)nj * ni;  // bcwsfc (none on the flat column)
     const size_t nE = more ? (size_t)nk * 2 * (ni + 2) : 0;  // pp3d S/N
     const size_t nF = more ? (size_t)nk * 6 * (ni + 2) : 0;  // scalar S/N
     const size_t total = nA + nB + nC + nD + nE + nF;
@@ -1053,7 +1192,7 @@ namespace {
 // terrain column bound in col
 int32_t terrain_open_stage(int32_t ni, int32_t nj, int32_t nk, int32_t nrk, float dt, int32_t nsound, float dx,
                            float dy, double dz, float alph, float kdiv, uint32_t ablations, uint32_t flags,
-                           const gm1b_terrain_open_arrays *arrays, const gm1b_terrain_metrics *metrics,
+                           uint32_t obc, const gm1b_terrain_open_arrays *arrays, const gm1b_terrain_metrics *metrics,
                            const gm1b_momentum_column *col, void *stream) {
     if (arrays == nullptr || metrics == nullptr || ni < 3 || nj < 3 || nk < 4 || nk > kTosMaxNk || nrk < 1 ||
         nrk > 3) {
@@ -1066,10 +1205,29 @@ int32_t terrain_open_stage(int32_t ni, int32_t nj, int32_t nk, int32_t nrk, floa
                        "index with 32-bit offsets", ni, nj, nk);
         return GM1B_ERR_ARGUMENT;
     }
-    if (col != nullptr) {
-        if (col->flat) {
-            gm1b_set_error("gm1b_terrain_open_stage_column: the flat column's acoustic statements (sound.F:119-143, "
-                           "318-342, 491-509, 742-765) are not built; bind a terrain column (flat = 0)");
+    if (col != nullptr && col->flat) {
+        if (col->mh == nullptr || col->mf == nullptr || !(col->rdz > 0.0f) || !std::isfinite(col->rdz)) {
+            gm1b_set_error("gm1b_terrain_open_stage_column: the flat column needs mh, mf and a finite rdz > 0");
+            return GM1B_ERR_ARGUMENT;
+        }
+        for (int side = 0; side < 4; ++side) {
+            const unsigned code = (obc >> (4 * side)) & 15u;
+            if (code < 1u || code > 4u) {
+                gm1b_set_error("gm1b_terrain_open_stage_column: lateral code 0x%x: each side is 1..4", obc);
+                return GM1B_ERR_ARGUMENT;
+            }
+        }
+        if ((obc >> 16) != 0u || (((obc & 15u) == 1u) != (((obc >> 4) & 15u) == 1u)) ||
+            ((((obc >> 8) & 15u) == 1u) != (((obc >> 12) & 15u) == 1u))) {
+            gm1b_set_error("gm1b_terrain_open_stage_column: lateral code 0x%x: a periodic direction is periodic on "
+                           "both sides (param.F:2562-2588)", obc);
+            return GM1B_ERR_ARGUMENT;
+        }
+        dz = 1.0;  // the scalar spacing is not used on a bound column
+    } else if (col != nullptr) {
+        if (obc != 0x2222u) {
+            gm1b_set_error("gm1b_terrain_open_stage_column: lateral code 0x%x: the terrain column's stage runs "
+                           "ssopenbc on all four sides (0x2222)", obc);
             return GM1B_ERR_ARGUMENT;
         }
         if (col->sigma == nullptr || col->sigmaf == nullptr || col->rds == nullptr || col->rdsf == nullptr ||
@@ -1128,7 +1286,11 @@ int32_t terrain_open_stage(int32_t ni, int32_t nj, int32_t nk, int32_t nrk, floa
     p.zt = (float)((double)nk * dz);
     p.rzt = 1.0f / p.zt;
     p.halfcp = 1005.7f * 0.5f;
-    if (col != nullptr) {
+    p.obc = obc;
+    if (col != nullptr && col->flat) {
+        p.vmode = 2;
+        p.mhp = col->mh, p.mfp = col->mf, p.rdz = col->rdz;
+    } else if (col != nullptr) {
         // the lid is the bound top; the edge-face extrapolation keeps the
         // open-boundary text's own 1.875 / -1.25 / 0.375 weights, which the
         // profile patch leaves in place (cuda_terrain_open_boundary.py:845-850,
@@ -1145,7 +1307,7 @@ int32_t terrain_open_stage(int32_t ni, int32_t nj, int32_t nk, int32_t nrk, floa
         return GM1B_ERR_ARGUMENT;
     }
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    const int col_arrays = kTosArrays + (p.vmode ? 4 : 0);
+    const int col_arrays = kTosArrays + (p.vmode == 1 ? 4 : 0);
     const size_t col_smem = (size_t)col_arrays * (size_t)(nk + 2) * 32 * sizeof(float);
     static bool attr_set[64] = {};  // per device: the attribute belongs to each device's context
     int dev = 0;
@@ -1160,6 +1322,9 @@ int32_t terrain_open_stage(int32_t ni, int32_t nj, int32_t nk, int32_t nrk, floa
         if (e == cudaSuccess)
             e = cudaFuncSetAttribute(tos_column_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)((size_t)(kTosArrays + 4) * (kTosMaxNk + 2) * 32 * sizeof(float)));
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(tos_column_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)((size_t)kTosArrays * (kTosMaxNk + 2) * 32 * sizeof(float)));
         if (e != cudaSuccess) {
             gm1b_set_error("cudaFuncSetAttribute(tos_column_kernel): %s", cudaGetErrorString(e));
             return GM1B_ERR_CUDA;
@@ -1175,13 +1340,23 @@ int32_t terrain_open_stage(int32_t ni, int32_t nj, int32_t nk, int32_t nrk, floa
     const dim3 pg_grid((ni + 2 + 31) / 32, (nj + 2 + 3) / 4), col_grid((ni + 31) / 32, nj);
     for (int n = 1; n <= nloop; ++n) {
         p.n = n;
-        if (ablations & GM1B_TOS_OPEN_CONSUMPTION) {
+        if ((ablations & GM1B_TOS_OPEN_CONSUMPTION) && p.vmode == 2) {
+            ProfScope ps("tos_flat_edge_kernel", st);
+            tos_flat_edge_kernel<<<grid_for((size_t)nk * (nj + ni), 256), 256, 0, st>>>(p);
+            ps.stop();
+            if (!launch_ok("tos_flat_edge_kernel")) return GM1B_ERR_CUDA;
+        } else if (ablations & GM1B_TOS_OPEN_CONSUMPTION) {
             ProfScope ps("tos_edge_kernel", st);
             tos_edge_kernel<<<2 * nj + 2 * ni, 128, 4 * (size_t)(nk + 2) * sizeof(float), st>>>(p);
             ps.stop();
             if (!launch_ok("tos_edge_kernel")) return GM1B_ERR_CUDA;
         }
-        if (ablations & GM1B_TOS_PRESSURE_GRADIENT) {
+        if ((ablations & GM1B_TOS_PRESSURE_GRADIENT) && p.vmode == 2) {
+            ProfScope ps("tos_flat_pgrad_kernel", st);
+            tos_flat_pgrad_kernel<<<dim3((ni + 1 + 31) / 32, (nj + 1 + 3) / 4), dim3(32, 4), 0, st>>>(p);
+            ps.stop();
+            if (!launch_ok("tos_flat_pgrad_kernel")) return GM1B_ERR_CUDA;
+        } else if (ablations & GM1B_TOS_PRESSURE_GRADIENT) {
             ProfScope ps("tos_pgrad_kernel", st);
             tos_pgrad_kernel<<<pg_grid, dim3(32, 4), 0, st>>>(p);
             ps.stop();
@@ -1189,7 +1364,9 @@ int32_t terrain_open_stage(int32_t ni, int32_t nj, int32_t nk, int32_t nrk, floa
         }
         {
             ProfScope ps("tos_column_kernel", st);
-            if (p.vmode)
+            if (p.vmode == 2)
+                tos_column_kernel<2><<<col_grid, dim3(32, kTosWarps), col_smem, st>>>(p);
+            else if (p.vmode == 1)
                 tos_column_kernel<1><<<col_grid, dim3(32, kTosWarps), col_smem, st>>>(p);
             else
                 tos_column_kernel<0><<<col_grid, dim3(32, kTosWarps), col_smem, st>>>(p);
@@ -1231,13 +1408,13 @@ extern "C" int32_t gm1b_terrain_open_stage(int32_t ni, int32_t nj, int32_t nk, i
                                            float dx, float dy, double dz, float alph, float kdiv, uint32_t ablations,
                                            uint32_t flags, const gm1b_terrain_open_arrays *arrays,
                                            const gm1b_terrain_metrics *metrics, void *stream) {
-    return terrain_open_stage(ni, nj, nk, nrk, dt, nsound, dx, dy, dz, alph, kdiv, ablations, flags, arrays, metrics,
-                              nullptr, stream);
+    return terrain_open_stage(ni, nj, nk, nrk, dt, nsound, dx, dy, dz, alph, kdiv, ablations, flags, 0x2222u, arrays,
+                              metrics, nullptr, stream);
 }
 
 extern "C" int32_t gm1b_terrain_open_stage_column(int32_t ni, int32_t nj, int32_t nk, int32_t nrk, float dt,
                                                   int32_t nsound, float dx, float dy, float alph, float kdiv,
-                                                  uint32_t ablations, uint32_t flags,
+                                                  uint32_t ablations, uint32_t flags, uint32_t lateral_obc,
                                                   const gm1b_terrain_open_arrays *arrays,
                                                   const gm1b_terrain_metrics *metrics,
                                                   const gm1b_momentum_column *column, void *stream) {
@@ -1245,6 +1422,6 @@ extern "C" int32_t gm1b_terrain_open_stage_column(int32_t ni, int32_t nj, int32_
         gm1b_set_error("gm1b_terrain_open_stage_column: column is NULL");
         return GM1B_ERR_ARGUMENT;
     }
-    return terrain_open_stage(ni, nj, nk, nrk, dt, nsound, dx, dy, 1.0, alph, kdiv, ablations, flags, arrays, metrics,
-                              column, stream);
+    return terrain_open_stage(ni, nj, nk, nrk, dt, nsound, dx, dy, 1.0, alph, kdiv, ablations, flags, lateral_obc,
+                              arrays, metrics, column, stream);
 }

@@ -195,7 +195,7 @@ def _lib():
         from .momentum import _Column
         lib.gm1b_terrain_open_stage_column.argtypes = [c.c_int32] * 4 + [c.c_float, c.c_int32, c.c_float, c.c_float,
                                                                          c.c_float, c.c_float, c.c_uint32,
-                                                                         c.c_uint32, c.POINTER(_Arrays),
+                                                                         c.c_uint32, c.c_uint32, c.POINTER(_Arrays),
                                                                          c.POINTER(_Metrics), c.POINTER(_Column),
                                                                          c.c_void_p]
         lib.gm1b_terrain_open_stage_column.restype = c.c_int32
@@ -373,17 +373,20 @@ def launch_cuda_gm1_child_psolver3_open_stage(
         compiled: CompiledPsolver3TerrainOpenKernels | None = None, alph: float | None = None,
         kdiv: float | None = None, lateral_sides: tuple[int, int, int, int] = (2, 2, 2, 2),
         **unused: Any) -> CudaPsolver3TerrainOpenLaunch:
-    """Enqueue one acoustic RK stage on a stretched terrain column
-    (src/cm1core/cuda_gm1_child_psolver3_open.py:848, terrain branch).
-    ``vertical`` is a :class:`gm1_b200.momentum.StretchedMomentumColumn` with
-    ``flat=False``: its ``sigma`` (nk+2), ``sigmaf`` (nk+3), ``rds`` (nk+2),
+    """Enqueue one acoustic RK stage on a stretched column
+    (src/cm1core/cuda_gm1_child_psolver3_open.py:848).  ``vertical`` is a
+    :class:`gm1_b200.momentum.StretchedMomentumColumn`.  Terrain column
+    (``flat=False``): its ``sigma`` (nk+2), ``sigmaf`` (nk+3), ``rds`` (nk+2),
     ``rdsf`` (nk+3) and the lid ``ztop``, which must be the column's own
-    sigmaf(nk+1) (param.F:8193).  ``metrics`` carries the 25 terrain metrics
-    and ``rho0_padded`` (nk+2, nj+6, ni+6), the source-valid padded base
-    density whose face averages weight the pressure advection.  There is no
-    dz: every vertical derivative reads the profiles.  The terrain stage is
-    sealed to four open sides; the flat column's stage is not built."""
-    from .momentum import StretchedMomentumColumn, _Column
+    sigmaf(nk+1) (param.F:8193); the stage is sealed to four open sides.
+    Flat column (``flat=True``): sound.F's terrain_flag=.false. statements on
+    ``mh`` (nk+2), ``mf`` (nk+3) and ``rdz``, with ``lateral_sides`` as
+    sound.F takes it (the pressure gradient's dtu0/dtv0 mask, ssopenbc on
+    the open sides only).  ``metrics`` carries the 25 terrain metrics and
+    ``rho0_padded`` (nk+2, nj+6, ni+6), the source-valid padded base density
+    whose face averages weight the terrain column's pressure advection.
+    There is no dz: every vertical derivative reads the profiles."""
+    from .momentum import StretchedMomentumColumn, _Column, momentum_lateral_sides, momentum_open_boundary_code
     from .periodic import sound3_stage_schedule_f32
 
     for name in unused:
@@ -397,10 +400,9 @@ def launch_cuda_gm1_child_psolver3_open_stage(
     validate_terrain_open_selection(selection)
     if not isinstance(vertical, StretchedMomentumColumn):
         raise TypeError("vertical must be a StretchedMomentumColumn")
-    if vertical.flat:
-        raise ValueError("the flat column's acoustic statements (sound.F:119-143, 318-342, 491-509, 742-765) are not "
-                         "built; bind a terrain column (flat=False)")
-    if tuple(lateral_sides) != (2, 2, 2, 2):
+    flat = bool(vertical.flat)
+    obc = momentum_open_boundary_code(lateral_sides)
+    if not flat and tuple(lateral_sides) != (2, 2, 2, 2):
         raise ValueError(f"lateral_sides {tuple(lateral_sides)}: the terrain child acoustic stage runs bc.F's ssopenbc "
                          "on all four sides and its pressure gradient skips every boundary face")
     for name, value in (("alph", alph), ("kdiv", kdiv)):
@@ -444,21 +446,29 @@ def launch_cuda_gm1_child_psolver3_open_stage(
     if any(rho0p.data_ptr() == t.data_ptr() for t in a.values()):
         raise ValueError("rho0_padded must not alias a mutable acoustic array")
     prof = {}
-    for n, pshape in (("sigma", (nk + 2,)), ("sigmaf", (nk + 3,)), ("rds", (nk + 2,)), ("rdsf", (nk + 3,))):
+    names = (("mh", (nk + 2,)), ("mf", (nk + 3,))) if flat else \
+        (("sigma", (nk + 2,)), ("sigmaf", (nk + 3,)), ("rds", (nk + 2,)), ("rdsf", (nk + 3,)))
+    for n, pshape in names:
         t = getattr(vertical, n)
         if not (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == torch.float32
                 and tuple(t.shape) == pshape and t.is_contiguous()):
             raise ValueError(f"vertical {n} must be device C-f32 {pshape}")
         prof[n] = t
-    if len({t.data_ptr() for t in prof.values()}) != 4:
+    if len({t.data_ptr() for t in prof.values()}) != len(prof):
         raise ValueError("vertical profiles must not alias")
-    ztop = float(np.float32(vertical.ztop))
-    if not (math.isfinite(ztop) and ztop > 0.0):
-        raise ValueError("vertical top must be finite and greater than zero")
-    top_face = float(prof["sigmaf"][nk + 1].item())
-    if top_face != ztop:
-        raise ValueError(f"vertical top {ztop} m is not this coordinate's own sigmaf(nk+1) of {top_face} m "
-                         "(param.F:8193)")
+    ztop = rdz = 0.0
+    if flat:
+        rdz = float(np.float32(vertical.rdz))
+        if not (math.isfinite(rdz) and rdz > 0.0):
+            raise ValueError("a flat column needs rdz > 0")
+    else:
+        ztop = float(np.float32(vertical.ztop))
+        if not (math.isfinite(ztop) and ztop > 0.0):
+            raise ValueError("vertical top must be finite and greater than zero")
+        top_face = float(prof["sigmaf"][nk + 1].item())
+        if top_face != ztop:
+            raise ValueError(f"vertical top {ztop} m is not this coordinate's own sigmaf(nk+1) of {top_face} m "
+                             "(param.F:8193)")
     device = a["u3d"].device
     if any(t.device != device for t in (*a.values(), *m.values(), rho0p, *prof.values())):
         raise ValueError("terrain/open arrays, metrics and profiles must live on one CUDA device")
@@ -469,12 +479,16 @@ def launch_cuda_gm1_child_psolver3_open_stage(
     st = torch.cuda.current_stream(device) if stream is None else stream
     sa = _Arrays(**{n: a[n].data_ptr() for n in ALL_ARRAY_NAMES})
     sm = _Metrics(**{n: m[n].data_ptr() for n in _STRUCT_METRICS})
-    col = _Column(0, rho0p.data_ptr(), prof["sigma"].data_ptr(), prof["sigmaf"].data_ptr(), prof["rds"].data_ptr(),
-                  prof["rdsf"].data_ptr(), ztop, None, None, None, 0.0)
+    if flat:
+        col = _Column(1, rho0p.data_ptr(), None, None, None, None, 0.0, prof["mh"].data_ptr(), prof["mf"].data_ptr(),
+                      None, rdz)
+    else:
+        col = _Column(0, rho0p.data_ptr(), prof["sigma"].data_ptr(), prof["sigmaf"].data_ptr(),
+                      prof["rds"].data_ptr(), prof["rdsf"].data_ptr(), ztop, None, None, None, 0.0)
     nloop, dts = sound3_stage_schedule_f32(dt, nsound, nrk)
     with torch.cuda.device(device), torch.cuda.stream(st):
         _native.check(lib.gm1b_terrain_open_stage_column(ni, nj, nk, nrk, dt, nsound, dx, dy, alph32, kdiv32, mask,
-                                                         GM1B_TOS_DIAGNOSTICS if retain else 0, ctypes.byref(sa),
+                                                         GM1B_TOS_DIAGNOSTICS if retain else 0, obc, ctypes.byref(sa),
                                                          ctypes.byref(sm), ctypes.byref(col),
                                                          ctypes.c_void_p(st.cuda_stream)),
                       "gm1b_terrain_open_stage_column")
@@ -486,10 +500,12 @@ def launch_cuda_gm1_child_psolver3_open_stage(
                 "radiation_productions": 1 if ablations.radiation_history_production else 0},)
     receipt: dict[str, Any] = {
         "domain": {"ni": ni, "nj": nj, "nk": nk, "ngxy": CM1_OPEN_NGXY},
-        "vertical": {"branch": "terrain", "ztop_f32": ztop, "dz": None},
+        "vertical": {"branch": "flat" if flat else "terrain", "ztop_f32": None if flat else ztop,
+                     "rdz_f32": rdz if flat else None, "dz": None},
         "cadence": list(cadence), "nrk": nrk,
         "acoustic_reals": {"alph": alph32, "kdiv": kdiv32},
         "comparison_contract": {"mode": "raw-bit", "max_ulp": 0, "null_or_missing_is_pass": False},
-        "lateral_boundaries": {"selection": {"wbc": 2, "ebc": 2, "sbc": 2, "nbc": 2}},
+        "lateral_boundaries": {"selection": dict(zip(("wbc", "ebc", "sbc", "nbc"),
+                                                     momentum_lateral_sides(lateral_sides)))},
     }
     return CudaPsolver3TerrainOpenLaunch(event, compiled, cadence, receipt)

@@ -509,15 +509,19 @@ GM1B_API int32_t gm1b_terrain_open_stage(int32_t ni, int32_t nj, int32_t nk, int
                                          uint32_t flags, const gm1b_terrain_open_arrays *arrays,
                                          const gm1b_terrain_metrics *metrics, void *stream);
 
-/* The same stage on a stretched terrain column (replaces
- * launch_cuda_gm1_child_psolver3_open_stage, cuda_gm1_child_psolver3_open.py:848,
- * terrain branch): sigma/sigmaf/rds/rdsf at CM1's indices, the lid ztop and
- * the padded base density rho0_padded (nk+2, nj+6, ni+6) come from column
- * (flat = 0; a flat column is refused).  No dz: every vertical derivative
- * reads the profiles.  Allocation-free; graph-capturable. */
+/* The same stage on a stretched column (replaces
+ * launch_cuda_gm1_child_psolver3_open_stage, cuda_gm1_child_psolver3_open.py:848).
+ * Terrain column (column->flat = 0): sigma/sigmaf/rds/rdsf at CM1's indices,
+ * the lid ztop and the padded base density rho0_padded (nk+2, nj+6, ni+6);
+ * lateral_obc must be all-open 0x2222.  Flat column (flat = 1): sound.F's
+ * terrain_flag=.false. statements on mh (nk+2), mf (nk+3) and rdz, the base
+ * state at CM1's (1,1,k), no bcwsfc; lateral_obc = wbc | ebc << 4 |
+ * sbc << 8 | nbc << 12 (the pressure gradient's dtu0/dtv0 mask, ssopenbc on
+ * the open sides).  No dz: every vertical derivative reads the profiles.
+ * Allocation-free; graph-capturable. */
 GM1B_API int32_t gm1b_terrain_open_stage_column(int32_t ni, int32_t nj, int32_t nk, int32_t nrk, float dt,
                                                 int32_t nsound, float dx, float dy, float alph, float kdiv,
-                                                uint32_t ablations, uint32_t flags,
+                                                uint32_t ablations, uint32_t flags, uint32_t lateral_obc,
                                                 const gm1b_terrain_open_arrays *arrays,
                                                 const gm1b_terrain_metrics *metrics,
                                                 const gm1b_momentum_column *column, void *stream);

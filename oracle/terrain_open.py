@@ -54,6 +54,10 @@ def _lib():
             [c.c_int] * 4 + [c.c_float, c.c_int, c.c_float, c.c_float] + [_F] * 4 + [c.c_float, _F] + \
             [c.c_float, c.c_float, c.c_uint, c.POINTER(c.c_float)]
         lib.oracle_terrain_open_stage_column.restype = c.c_int
+        lib.oracle_terrain_open_stage_flat.argtypes = [c.POINTER(TosArrays), c.POINTER(TosMetrics)] + \
+            [c.c_int] * 4 + [c.c_float, c.c_int, c.c_float, c.c_float, _F, _F, c.c_float, c.c_uint] + \
+            [c.c_float, c.c_float, c.c_uint, c.POINTER(c.c_float)]
+        lib.oracle_terrain_open_stage_flat.restype = c.c_int
         lib._tos_ready = True
     return lib
 
@@ -94,6 +98,22 @@ def terrain_open_stage_column(a, m, column, *, ni, nj, nk, nrk, dt, nsound, dx, 
                                                 ablations, diag)
     if rc != 0:
         raise ValueError(f"oracle_terrain_open_stage_column failed ({rc})")
+    return StageDiagnostics(nrk, int(diag[0]), float(diag[1]), float(diag[2]))
+
+
+def terrain_open_stage_flat(a, m, column, *, ni, nj, nk, nrk, dt, nsound, dx, dy, obc=0x2222, alph=0.6, kdiv=0.1,
+                            ablations=ALL_ABLATIONS) -> StageDiagnostics:
+    """One stage on a flat stretched column: ``column`` maps mh (nk+2), mf
+    (nk+3) and rdz; ``obc`` packs wbc | ebc << 4 | sbc << 8 | nbc << 12."""
+    sa, sm = _bind(TosArrays, ARRAY_NAMES, a), _bind(TosMetrics, METRIC_NAMES, m)
+    mh = np.ascontiguousarray(column["mh"], dtype=np.float32)
+    mf = np.ascontiguousarray(column["mf"], dtype=np.float32)
+    diag = (ctypes.c_float * 3)()
+    rc = _lib().oracle_terrain_open_stage_flat(ctypes.byref(sa), ctypes.byref(sm), ni, nj, nk, nrk, dt, nsound, dx, dy,
+                                              mh.ctypes.data_as(_F), mf.ctypes.data_as(_F),
+                                              float(np.float32(column["rdz"])), obc, alph, kdiv, ablations, diag)
+    if rc != 0:
+        raise ValueError(f"oracle_terrain_open_stage_flat failed ({rc})")
     return StageDiagnostics(nrk, int(diag[0]), float(diag[1]), float(diag[2]))
 
 

@@ -575,10 +575,12 @@ static void pressure_advection(TosArrays *a, const TosMetrics *m, const G *g, co
 #undef XU
 #undef YV
 
+/* flat != 0: the flat column's update (sound.F:742-765) keeps w(1) and
+ * w(nk+1) as they are and filters with cm1.F:311's smeps 1.0e-30 */
 static void implicit_and_update(TosArrays *a, const G *g, float dts, int nrk, int n, int nloop, float alph, float beta,
-                                float kdiv, int implicit) {
+                                float kdiv, int implicit, int flat) {
     const int ni = g->ni, nj = g->nj, nk = g->nk;
-    const float asq = alph * alph, smeps = 1.0e-20f;
+    const float asq = alph * alph, smeps = flat ? 1.0e-30f : 1.0e-20f;
     for (int j0 = 0; j0 < nj; ++j0)
         for (int i0 = 0; i0 < ni; ++i0) {
             const int j = j0 + 1, i = i0 + 1, y = Y(j), x = X(i);
@@ -618,7 +620,7 @@ static void implicit_and_update(TosArrays *a, const G *g, float dts, int nrk, in
                 }
             }
             for (int k = 1; k <= nk; ++k) {
-                const float w1 = k == 1 ? 0.0f : WW(k), w2 = k == nk ? 0.0f : WW(k + 1);
+                const float w1 = (k == 1 && !flat) ? 0.0f : WW(k), w2 = (k == nk && !flat) ? 0.0f : WW(k + 1);
                 const float old = a->pp3d[C(k)];
                 const float vt = w1 * (a->pk1[C(k)] + a->qk[C(k)]) + w2 * (a->pk2[C(k)] - a->qk[C(k)]);
                 float up = (old + a->fpk[C(k)]) + alph * vt;
@@ -731,7 +733,7 @@ static int stage_impl(TosArrays *a, const TosMetrics *m, int ni, int nj, int nk,
         initial_fpk(a, m, &g, &p, xu, yv, dts, rdx, rdy, beta, (ablations & ABL_DIV) != 0);
         bcwsfc(a, m, &g);
         if (ablations & ABL_PADV) pressure_advection(a, m, &g, &p, xu, yv, dts, rdx, rdy, beta, zt, rzt, rho0p);
-        implicit_and_update(a, &g, dts, nrk, n, nloop, alph, beta, kdiv, (ablations & ABL_IMPLICIT) != 0);
+        implicit_and_update(a, &g, dts, nrk, n, nloop, alph, beta, kdiv, (ablations & ABL_IMPLICIT) != 0, 0);
         if (n < nloop && (ablations & ABL_PFILL)) bcp_open(a->ppd, &g);
         average_velocities(a, &g, n, nloop, alph);
     }
@@ -775,4 +777,194 @@ void oracle_open_fill(int ni, int nj, int nk, int kind, float *q) {
         case 5: bcs_open(q, &g, 2, nk); break;
         default: break;
     }
+}
+
+/* ---------------------------------------------------------------------- */
+/* the flat stretched column (terrain_flag=.false.)                        */
+/* cuda_gm1_child_psolver3_open.py:343-507 (the flat texts) and :1618-1795 */
+/* (their order): the terrain stage's substeps less the u/v reconstruction */
+/* before the open-edge update and every bcwsfc.                           */
+/* ---------------------------------------------------------------------- */
+
+/* sound.F:119-143: qk, pk1, pk2 and mm from rdz*mh(k) / rdz*mf(k) and the
+ * column's base state at CM1's (1,1,k); mm at every level */
+static void prepare_flat(TosArrays *a, const TosMetrics *m, const G *g, const float *mh, const float *mf, float rdz,
+                         float dts) {
+    const int ni = g->ni, nj = g->nj, nk = g->nk;
+    const size_t np = (size_t)(nk + 2) * (nj + 2) * (ni + 2);
+    float *scratch[NSCRATCH] = {a->qk, a->pk1, a->pk2, a->mm, a->fpk, a->divh, a->hadvp, a->dum3,
+                                a->elim_c, a->elim_d, a->tri_aa, a->tri_bb, a->tri_cc, a->tri_dd, a->tri_pivot,
+                                a->tri_residual};
+    for (int s = 0; s < NSCRATCH; ++s) memset(scratch[s], 0, np * sizeof(float));
+    const float cp = 1005.7f;
+    for (int k = 1; k <= nk; ++k) {
+        const float t0 = (dts * rdz) * mh[k];
+        const float rr = m->rr0[M(g, k - 1, 0, 0)];
+        const float r2 = (t0 * rr) * m->rf0[M(g, k, 0, 0)];
+        const float r1 = (t0 * rr) * m->rf0[M(g, k - 1, 0, 0)];
+        const float tem1 = ((dts * rdz) * cp) * mf[k];
+        const float c1a = m->c1[M(g, k - 1, 0, 0)], c1b = m->c1[M(g, k, 0, 0)];
+        const float c2a = m->c2[M(g, k - 1, 0, 0)], c2b = m->c2[M(g, k, 0, 0)];
+        for (int j = 1; j <= nj; ++j)
+            for (int i = 1; i <= ni; ++i) {
+                const size_t c = P(g, k, j, i);
+                a->qk[c] = t0 * a->ppterm[c];
+                a->pk2[c] = r2 * ((-c2b) * a->piadv[P(g, k + 1, j, i)] + (1.0f - c1b) * a->piadv[c]);
+                a->pk1[c] = r1 * (c1a * a->piadv[P(g, k - 1, j, i)] + (c2a - 1.0f) * a->piadv[c]);
+                a->mm[c] = tem1 * (c2a * a->thv[c] + c1a * a->thv[P(g, k - 1, j, i)]);
+                if (k == 1) a->pk1[c] = 0.0f;
+                if (k == nk) a->pk2[c] = 0.0f;
+            }
+    }
+}
+
+/* bc.F:2410-2419 and its three twins: u(1) = u(1) + dts*(((-radbcw*(u(2)-u(1)))
+ * *rdx)*uh(1) + uten(1)) on each open side (code 2 in the side's nibble) */
+static void ssopen_flat(TosArrays *a, const G *g, float dts, float rdx, float rdy, unsigned obc) {
+    const int ni = g->ni, nj = g->nj, nk = g->nk;
+    const size_t ry = (size_t)nj + 6, rx = (size_t)ni + 6;
+    for (int k = 1; k <= nk; ++k)
+        for (int j0 = 0; j0 < nj; ++j0) {
+            const int y = j0 + 3;
+            if ((obc & 15u) == 2u) {
+                const size_t b = U(g, k, y, 3);
+                const float t = (((-a->radbcw[k * ry + y]) * (a->u3d[U(g, k, y, 4)] - a->u3d[b])) * rdx) * a->uh[3] +
+                                a->uten[b];
+                a->u3d[b] = a->u3d[b] + dts * t;
+            }
+            if (((obc >> 4) & 15u) == 2u) {
+                const size_t b = U(g, k, y, ni + 3);
+                const float t = (((-a->radbce[k * ry + y]) * (a->u3d[b] - a->u3d[U(g, k, y, ni + 2)])) * rdx) *
+                                    a->uh[ni + 2] + a->uten[b];
+                a->u3d[b] = a->u3d[b] + dts * t;
+            }
+        }
+    for (int k = 1; k <= nk; ++k)
+        for (int i0 = 0; i0 < ni; ++i0) {
+            const int x = i0 + 3;
+            if (((obc >> 8) & 15u) == 2u) {
+                const size_t b = V(g, k, 3, x);
+                const float t = (((-a->radbcs[k * rx + x]) * (a->v3d[V(g, k, 4, x)] - a->v3d[b])) * rdy) * a->vh[3] +
+                                a->vten[b];
+                a->v3d[b] = a->v3d[b] + dts * t;
+            }
+            if (((obc >> 12) & 15u) == 2u) {
+                const size_t b = V(g, k, nj + 3, x);
+                const float t = (((-a->radbcn[k * rx + x]) * (a->v3d[b] - a->v3d[V(g, k, nj + 2, x)])) * rdy) *
+                                    a->vh[nj + 2] + a->vten[b];
+                a->v3d[b] = a->v3d[b] + dts * t;
+            }
+        }
+}
+
+/* sound.F:318-342: every face i = 1..ni+1, j = 1..nj+1 takes u + (dts*dtu0)*
+ * (uten - pgrad), dtu0 = 1 on the faces param.F:9182-9219 admits (a
+ * periodic side's boundary face included), 0 elsewhere */
+static void pgrad_flat(TosArrays *a, const G *g, float dts, float rdx, float rdy, unsigned obc) {
+    const int ni = g->ni, nj = g->nj, nk = g->nk;
+    const float cp = 1005.7f, tem1 = (rdx * cp) * 0.5f, tem2 = (rdy * cp) * 0.5f;
+    const int pw = (obc & 15u) == 1u, pe = ((obc >> 4) & 15u) == 1u;
+    const int ps = ((obc >> 8) & 15u) == 1u, pn = ((obc >> 12) & 15u) == 1u;
+    for (int k = 1; k <= nk; ++k)
+        for (int j = 1; j <= nj + 1; ++j)
+            for (int i = 1; i <= ni + 1; ++i) {
+                const float wu = (j <= nj && (i > 1 || pw) && (i < ni + 1 || pe)) ? 1.0f : 0.0f;
+                const float wv = (i <= ni && (j > 1 || ps) && (j < nj + 1 || pn)) ? 1.0f : 0.0f;
+                const size_t c = P(g, k, j, i);
+                float pu = tem1 * (a->ppd[c] - a->ppd[P(g, k, j, i - 1)]);
+                pu = pu * (a->thv[c] + a->thv[P(g, k, j, i - 1)]);
+                const size_t xu = U(g, k, j + 2, i + 2);
+                a->u3d[xu] = a->u3d[xu] + (dts * wu) * (a->uten[xu] - pu);
+                float pv = tem2 * (a->ppd[c] - a->ppd[P(g, k, j - 1, i)]);
+                pv = pv * (a->thv[c] + a->thv[P(g, k, j - 1, i)]);
+                const size_t xv = V(g, k, j + 2, i + 2);
+                a->v3d[xv] = a->v3d[xv] + (dts * wv) * (a->vten[xv] - pv);
+            }
+}
+
+/* sound.F:491-509: fpk = ((dts*(ppten - ppterm*div)) + H) + beta*W with the
+ * flat divergence and pressure advection */
+static void initial_flat(TosArrays *a, const G *g, float dts, float rdx, float rdy, float beta, int do_div) {
+    const int ni = g->ni, nj = g->nj, nk = g->nk;
+    const float temx = (dts * 0.5f) * rdx, temy = (dts * 0.5f) * rdy;
+    for (int k = 1; k <= nk; ++k)
+        for (int j = 1; j <= nj; ++j)
+            for (int i = 1; i <= ni; ++i) {
+                const int y = Y(j), x = X(i);
+                const size_t c = P(g, k, j, i);
+                const float uw = a->u3d[U(g, k, y, x)], ue = a->u3d[U(g, k, y, x + 1)];
+                const float vs = a->v3d[V(g, k, y, x)], vn = a->v3d[V(g, k, y + 1, x)];
+                float div = 0.0f;
+                if (do_div) {
+                    div = (ue - uw) * rdx + (vn - vs) * rdy;
+                    if (fabsf(div) < 1.0e-30f) div = 0.0f;
+                }
+                const float pc = a->piadv[c];
+                float hx = uw * (pc - a->piadv[P(g, k, j, i - 1)]) + ue * (a->piadv[P(g, k, j, i + 1)] - pc);
+                hx = (-hx) * temx;
+                float hy = vs * (pc - a->piadv[P(g, k, j - 1, i)]) + vn * (a->piadv[P(g, k, j + 1, i)] - pc);
+                hy = (-hy) * temy;
+                const float hp = hx + hy;
+                const float vert = a->w3d[W(g, k, y, x)] * (a->pk1[c] + a->qk[c]) +
+                                   a->w3d[W(g, k + 1, y, x)] * (a->pk2[c] - a->qk[c]);
+                a->divh[c] = div;
+                a->hadvp[c] = hp;
+                a->fpk[c] = ((dts * (a->ppten[c] - a->ppterm[c] * div)) + hp) + beta * vert;
+            }
+}
+
+int oracle_terrain_open_stage_flat(TosArrays *a, const TosMetrics *m, int ni, int nj, int nk, int nrk, float dt,
+                                   int nsound, float dx, float dy, const float *mh, const float *mf, float rdz,
+                                   unsigned obc, float alph, float kdiv, unsigned ablations, float *diag) {
+    if (ni < 3 || nj < 3 || nk < 4 || nrk < 1 || nrk > 3 || !mh || !mf) return -1;
+    const G g = {ni, nj, nk};
+    int nloop;
+    float dts;
+    if (oracle_stage_schedule(dt, nsound, nrk, &nloop, &dts) != 0) return -1;
+    const float beta = 1.0f - alph;
+    const float rdx = 1.0f / dx, rdy = 1.0f / dy;
+    prepare_flat(a, m, &g, mh, mf, rdz, dts);
+    for (int k = 1; k <= nk; ++k)
+        for (int j = 0; j <= nj + 1; ++j)
+            for (int i = 0; i <= ni + 1; ++i) {
+                a->ppd[P(&g, k, j, i)] = a->ppx[P(&g, k, j, i)];
+                if (nrk != 1) a->pp3d[P(&g, k, j, i)] = a->ppi[P(&g, k, j, i)];
+            }
+    for (int k = 1; k <= nk; ++k)
+        for (int j = 0; j <= nj + 1; ++j)
+            for (int i = 0; i <= ni + 1; ++i) {
+                const int y = Y(j), x = X(i);
+                a->rru[U(&g, k, y, x)] = 0.0f;
+                a->rrv[V(&g, k, y, x)] = 0.0f;
+                a->rrw[W(&g, k, y, x)] = a->wa[W(&g, k, y, x)] * beta;
+                if (nrk != 1) {
+                    a->u3d[U(&g, k, y, x)] = a->ua[U(&g, k, y, x)];
+                    a->v3d[V(&g, k, y, x)] = a->va[V(&g, k, y, x)];
+                    a->w3d[W(&g, k, y, x)] = a->wa[W(&g, k, y, x)];
+                }
+            }
+    for (int n = 1; n <= nloop; ++n) {
+        if (ablations & ABL_OPEN) ssopen_flat(a, &g, dts, rdx, rdy, obc);
+        if (ablations & ABL_PGRAD) pgrad_flat(a, &g, dts, rdx, rdy, obc);
+        initial_flat(a, &g, dts, rdx, rdy, beta, (ablations & ABL_DIV) != 0);
+        implicit_and_update(a, &g, dts, nrk, n, nloop, alph, beta, kdiv, (ablations & ABL_IMPLICIT) != 0, 1);
+        if (n < nloop && (ablations & ABL_PFILL)) bcp_open(a->ppd, &g);
+        average_velocities(a, &g, n, nloop, alph);
+    }
+    if (ablations & ABL_RADIATION) radiation4(a, &g, dx, dy, oracle_rk_stage_dt(dt, nrk));
+    if (ablations & ABL_FILLS) {
+        bcu_open(a->u3d, &g);
+        bcv_open(a->v3d, &g);
+        bcw_open_flag1(a->w3d, &g);
+        if (nrk < 3) {
+            bcp_open(a->pp3d, &g);
+            bcs_open(a->scalar, &g, 1, nk);
+        }
+    }
+    if (diag) {
+        diag[0] = (float)nloop;
+        diag[1] = dts;
+        diag[2] = 0.0f;
+    }
+    return 0;
 }

@@ -138,3 +138,51 @@ def test_stretched_terrain_stage_moves_with_the_profiles():
     orc.terrain_open_stage_column(got, m, col, **p)
     for n in ("u3d", "v3d", "w3d", "pp3d"):
         assert np.isfinite(got[n]).all() and _differs(got[n], want[n]), n
+
+
+def _flat_column(nk):
+    from gm1_b200.vertical import build_vertical_levels
+
+    spec = {10: (1100.0, 40.0, 700.0), 14: (1630.0, 40.0, 1030.0)}[nk]
+    lv = build_vertical_levels(stretch_z=1, nk=nk, dz_m=100.0, ztop_m=spec[0], str_bot_m=spec[1], str_top_m=spec[2],
+                               dz_bot_m=20.0, dz_top_m=200.0)
+    return {"mh": lv.mh, "mf": lv.mf, "rdz": float(np.float32(1.0) / np.float32(100.0))}
+
+
+def test_flat_stage_keeps_a_resting_atmosphere_at_rest():
+    """The flat-column restatement (sound.F's terrain_flag=.false. texts,
+    src/cm1core/cuda_gm1_child_psolver3_open.py:343-507, in the order of
+    :1618-1795) leaves a state with no wind, no perturbation pressure and no
+    tendencies unchanged, on every lateral family it takes."""
+    from tests.golden.make_golden import terrain_open_fixture
+
+    ni, nj, nk = 9, 8, 10
+    a, m = terrain_open_fixture(ni, nj, nk, 11)
+    for n in ("u3d", "ua", "uten", "v3d", "va", "vten", "w3d", "wa", "wten", "ppi", "pp3d", "ppx", "ppten"):
+        a[n][:] = 0.0
+    for obc in (0x2222, 0x2211, 0x1111):
+        got = {k: v.copy() for k, v in a.items()}
+        for nrk in (1, 2, 3):
+            orc.terrain_open_stage_flat(got, m, _flat_column(nk), ni=ni, nj=nj, nk=nk, nrk=nrk, dt=2.0, nsound=6,
+                                        dx=450.0, dy=520.0, obc=obc)
+        for n in ("u3d", "v3d", "w3d", "pp3d", "ppd"):
+            assert not np.any(got[n][1:nk + 1]), (hex(obc), n)
+
+
+def test_flat_stage_lateral_family_moves_the_boundary_faces():
+    """Periodic and open west/east sides take different boundary-face
+    updates (the pressure gradient's dtu0 mask against the open-side
+    radiation update); the stage stays finite on both."""
+    from tests.golden.make_golden import terrain_open_fixture
+
+    ni, nj, nk = 12, 9, 10
+    a, m = terrain_open_fixture(ni, nj, nk, 12)
+    p = dict(ni=ni, nj=nj, nk=nk, nrk=1, dt=2.0, nsound=6, dx=450.0, dy=520.0)
+    only = orc.ablation_mask(between_step_pressure_fill=False, radiation_history_production=False,
+                             stage_family_fills=False)
+    one, two = {k: v.copy() for k, v in a.items()}, {k: v.copy() for k, v in a.items()}
+    orc.terrain_open_stage_flat(one, m, _flat_column(nk), obc=0x2222, ablations=only, **p)
+    orc.terrain_open_stage_flat(two, m, _flat_column(nk), obc=0x2211, ablations=only, **p)
+    # u faces x = 3 and x = ni+3 are the west and east boundary faces
+    assert _differs(one["u3d"][1:nk + 1, 3:nj + 3, 3], two["u3d"][1:nk + 1, 3:nj + 3, 3])
+    assert np.isfinite(one["pp3d"]).all() and np.isfinite(two["pp3d"]).all()

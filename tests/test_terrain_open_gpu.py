@@ -181,7 +181,7 @@ def test_stretched_terrain_stage_refusals():
     with pytest.raises(ValueError, match="rho0_padded"):
         tos.launch_cuda_gm1_child_psolver3_open_stage(dev, mdev, vertical=vertical, **p)
     mdev["rho0_padded"] = rho0p
-    with pytest.raises(ValueError, match="flat column"):
+    with pytest.raises(ValueError, match="vertical mh"):
         tos.launch_cuda_gm1_child_psolver3_open_stage(dev, mdev, vertical=StretchedMomentumColumn(True, None), **p)
     with pytest.raises(ValueError, match="sigmaf"):
         bad = StretchedMomentumColumn(False, None, sigma=vertical.sigma, sigmaf=vertical.sigmaf, rds=vertical.rds,
@@ -189,3 +189,31 @@ def test_stretched_terrain_stage_refusals():
         tos.launch_cuda_gm1_child_psolver3_open_stage(dev, mdev, vertical=bad, **p)
     with pytest.raises(ValueError, match="four sides"):
         tos.launch_cuda_gm1_child_psolver3_open_stage(dev, mdev, vertical=vertical, lateral_sides=(1, 1, 2, 2), **p)
+
+
+@pytest.mark.parametrize("ni,nj,nk,sides", [(37, 21, 10, (2, 2, 2, 2)), (70, 9, 14, (1, 1, 2, 2)),
+                                            (33, 40, 10, (2, 2, 1, 1)), (3, 3, 10, (1, 1, 1, 1))])
+def test_flat_stretched_stage_matches_oracle(ni, nj, nk, sides):
+    """The flat column's stage (sound.F's terrain_flag=.false. texts) on
+    rdz*mh / rdz*mf of a generated stretched column, on four lateral
+    families: every array, scratch included, word-identical to the oracle
+    restatement after each of the three RK stages."""
+    from gm1_b200.momentum import StretchedMomentumColumn, momentum_open_boundary_code
+    from tests.test_oracle_terrain_open import _flat_column
+
+    col = _flat_column(nk)
+    a, m = terrain_open_fixture(ni, nj, nk, 500 + ni)
+    t = lambda x: torch.from_numpy(np.array(x, dtype=np.float32)).cuda()  # noqa: E731
+    vertical = StretchedMomentumColumn(True, None, mh=t(col["mh"]), mf=t(col["mf"]), rdz=col["rdz"])
+    from tests.test_oracle_momentum import _padded_rho0
+
+    p = dict(ni=ni, nj=nj, nk=nk, dt=2.0, nsound=6, dx=450.0, dy=520.0)
+    ref = {k: v.copy() for k, v in a.items()}
+    dev, mdev = _dev(a), _dev(m)
+    mdev["rho0_padded"] = t(_padded_rho0(m["rho0_3d"], ni, nj, nk))
+    for nrk in (1, 2, 3):
+        orc.terrain_open_stage_flat(ref, m, col, nrk=nrk, obc=momentum_open_boundary_code(sides), **p)
+        r = tos.launch_cuda_gm1_child_psolver3_open_stage(dev, mdev, nrk=nrk, vertical=vertical, lateral_sides=sides,
+                                                          **p)
+        r.ready_event.synchronize()
+        assert _bad(dev, ref, tos.ALL_ARRAY_NAMES) == [], f"nrk={nrk}"
