@@ -1,6 +1,7 @@
 """Per-operator device throughput on B200 (library profiling facility).
 
-    python -m gm1_b200.opbench [--ops adv5 adv5-weno massflux calcdef moistnm courant tos tos-diag moist]
+    python -m gm1_b200.opbench [--ops adv5 adv5-weno massflux calcdef moistnm courant tos tos-diag
+                                      tos-stretched tos-flat moist]
                                [--grid 256 256 80] [--iters 20] [--nsound 10]
 
 For each operator: seeded synthetic inputs of the given padded-lane grid
@@ -17,6 +18,7 @@ import argparse
 import json
 from pathlib import Path
 
+import numpy as np
 import torch
 
 from .advection import launch_cuda_scalar_advection5, launch_cuda_terrain_mass_flux5, padded_shapes
@@ -221,6 +223,32 @@ def run(op: str, a: dict[str, torch.Tensor], ni: int, nj: int, nk: int, stream: 
         launch_cuda_psolver3_terrain_open_stage(
             st, m, ni=ni, nj=nj, nk=nk, nrk=3, dt=6.0, nsound=NSOUND[0], dx=1000.0, dy=1000.0, dz=250.0,
             compiled=compile_cuda_psolver3_terrain_open(retain_column_diagnostics=diag), stream=stream)
+    elif op in ("tos-stretched", "tos-flat"):
+        # the acoustic stage on the stretched column of the 640x768x80
+        # supercell (stretch_z 1, 20 m at the ground to 500 m aloft, lid
+        # 20.8 km): terrain branch or flat column, compact scratch
+        from .momentum import StretchedMomentumColumn  # noqa: PLC0415
+        from .terrain_open import (compile_cuda_psolver3_terrain_open,  # noqa: PLC0415
+                                   launch_cuda_gm1_child_psolver3_open_stage)
+        from .vertical import build_vertical_levels  # noqa: PLC0415
+
+        dev = a["u3d"].device
+        st, m = tos_inputs(ni, nj, nk, dev, False)
+        key = (op, ni, nj, nk)
+        if key not in _CACHE:
+            if nk != 80:
+                raise ValueError(f"{op} runs the nk = 80 stretched column")
+            lv = build_vertical_levels(stretch_z=1, nk=80, dz_m=100.0, ztop_m=20800.0, str_bot_m=200.0,
+                                       str_top_m=15800.0, dz_bot_m=20.0, dz_top_m=500.0)
+            t = lambda x: torch.from_numpy(np.array(x, dtype=np.float32)).to(dev)  # noqa: E731
+            m["rho0_padded"] = torch.ones((nk + 2, nj + 6, ni + 6), device=dev)
+            _CACHE[key] = (StretchedMomentumColumn(True, None, mh=t(lv.mh), mf=t(lv.mf), rdz=0.01)
+                           if op == "tos-flat" else
+                           StretchedMomentumColumn(False, None, sigma=t(lv.sigma), sigmaf=t(lv.sigmaf), rds=t(lv.rds),
+                                                   rdsf=t(lv.rdsf), ztop=lv.ztop_m))
+        launch_cuda_gm1_child_psolver3_open_stage(
+            st, m, ni=ni, nj=nj, nk=nk, nrk=3, dt=6.0, nsound=NSOUND[0], dx=1000.0, dy=1000.0, vertical=_CACHE[key],
+            compiled=compile_cuda_psolver3_terrain_open(retain_column_diagnostics=False), stream=stream)
     else:
         raise ValueError(op)
 
