@@ -26,6 +26,7 @@ namespace gm1b {
 namespace {
 
 constexpr int kTTX = 32, kTTY = 4, kTT = kTTX * kTTY;  // turbt tile
+constexpr int kTTChunk = 8;  // levels whose column-solve loads turbt issues together
 constexpr int kG = 3;                                    // padded-lane halo of rru/rrv/rrw
 
 struct TkeArgs {
@@ -107,27 +108,49 @@ __global__ void __launch_bounds__(kTT) tke_turbt_kernel(TkeArgs a, float dt) {
         float cprev = -1.0f * (cfc * inv), dprev = a.t[z] * inv;
         CP(0) = cprev;
         DP(0) = dprev;
-        for (int p = 1; p < n - 1; ++p) {
-            f = p + 1;
-            z = f3(a, f, j, i);
-            rrf = a.mf[z] / a.rf[z];
-            const float r1 =
-                (a.kmv[f3(a, f - 1, j, i)] + a.kmv[z]) * (a.mh[f3(a, f - 1, j, i)] * (a.rho[f3(a, f - 1, j, i)] * rrf));
-            r2 = (a.kmv[z] + a.kmv[f3(a, f + 1, j, i)]) * (a.mh[z] * (a.rho[z] * rrf));
-            const float cfa = tema * r1;
-            cfc = tema * r2;
-            cfb = (1.0f - cfa) - cfc;
-            inv = rcp_rn(cfa * cprev + cfb);
-            cprev = -1.0f * (cfc * inv);
-            dprev = (a.t[z] - cfa * dprev) * inv;
-            CP(p) = cprev;
-            DP(p) = dprev;
+        // kmv(f-1), kmv(f), mh(f-1) and rho(f-1) of the level being
+        // eliminated ride in registers; each chunk of kTTChunk levels issues
+        // all of its loads before its first elimination, so their latency is
+        // paid once per chunk rather than once per level (same operations,
+        // same order)
+        float km1 = a.kmv[z], k0 = a.kmv[f3(a, 2, j, i)], mhm = a.mh[z], rhom = a.rho[z];
+        for (int p0 = 1; p0 < n - 1; p0 += kTTChunk) {
+            float lkn[kTTChunk], lmh[kTTChunk], lrho[kTTChunk], lmf[kTTChunk], lrf[kTTChunk], lt[kTTChunk];
+#pragma unroll
+            for (int q = 0; q < kTTChunk; ++q) {
+                lkn[q] = lmh[q] = lrho[q] = lt[q] = 0.0f;
+                lmf[q] = lrf[q] = 1.0f;
+                if (p0 + q >= n - 1) continue;
+                const unsigned zq = f3(a, p0 + q + 1, j, i);
+                lkn[q] = a.kmv[f3(a, p0 + q + 2, j, i)];
+                lmh[q] = a.mh[zq];
+                lrho[q] = a.rho[zq];
+                lmf[q] = a.mf[zq];
+                lrf[q] = a.rf[zq];
+                lt[q] = a.t[zq];
+            }
+#pragma unroll
+            for (int q = 0; q < kTTChunk; ++q) {
+                const int p = p0 + q;
+                if (p >= n - 1) break;
+                rrf = lmf[q] / lrf[q];
+                const float r1 = (km1 + k0) * (mhm * (rhom * rrf));
+                r2 = (k0 + lkn[q]) * (lmh[q] * (lrho[q] * rrf));
+                const float cfa = tema * r1;
+                cfc = tema * r2;
+                cfb = (1.0f - cfa) - cfc;
+                inv = rcp_rn(cfa * cprev + cfb);
+                cprev = -1.0f * (cfc * inv);
+                dprev = (lt[q] - cfa * dprev) * inv;
+                CP(p) = cprev;
+                DP(p) = dprev;
+                km1 = k0, k0 = lkn[q], mhm = lmh[q], rhom = lrho[q];
+            }
         }
         f = nk - 1;
         z = f3(a, f, j, i);
         rrf = a.mf[z] / a.rf[z];
-        const float r1 =
-            (a.kmv[f3(a, f - 1, j, i)] + a.kmv[z]) * (a.mh[f3(a, f - 1, j, i)] * (a.rho[f3(a, f - 1, j, i)] * rrf));
+        const float r1 = (km1 + k0) * (mhm * (rhom * rrf));
         const float cfa = tema * r1;
         cfb = 1.0f - cfa;
         float sol = (a.t[z] - cfa * DP(n - 2)) * rcp_rn(cfa * CP(n - 2) + cfb);
