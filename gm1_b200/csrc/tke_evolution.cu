@@ -86,8 +86,8 @@ __device__ float tke_ty(const TkeArgs &a, int f, int face, int i) {
 // (nk-1) levels x kTT columns
 __global__ void __launch_bounds__(kTT) tke_turbt_kernel(TkeArgs a, float dt) {
     extern __shared__ float s_col[];
-    __shared__ float s_tx[3][kTTY][kTTX + 1];
-    __shared__ float s_ty[3][kTTY + 1][kTTX];
+    __shared__ float s_tx[4][kTTY][kTTX + 1];
+    __shared__ float s_ty[4][kTTY + 1][kTTX];
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kTTX + tx;
     const int i0 = blockIdx.x * kTTX, j0 = blockIdx.y * kTTY;
     const int i = i0 + tx, j = j0 + ty;
@@ -161,20 +161,43 @@ __global__ void __launch_bounds__(kTT) tke_turbt_kernel(TkeArgs a, float dt) {
         }
     }
     // ---- horizontal divergence, walking the face levels --------------------
+    // Four level slots: while level f is formed from slots f-1, f, f+1, this
+    // thread's share of level f+2's face terms is evaluated into registers
+    // (its loads in flight during the level's arithmetic) and stored into the
+    // fourth slot, which no thread reads until after the closing barrier.
     constexpr int kXF = kTTY * (kTTX + 1), kYF = (kTTY + 1) * kTTX;
-    auto fill = [&](int lev) {
-        const int slot = lev % 3;
-        for (int e = tid; e < kXF; e += kTT) {
-            const int r = e / (kTTX + 1), q = e - r * (kTTX + 1);
-            if (j0 + r < nj && i0 + q <= ni) s_tx[slot][r][q] = tke_tx(a, lev, j0 + r, i0 + q);
+    constexpr int kXE = (kXF + kTT - 1) / kTT, kYE = (kYF + kTT - 1) / kTT;
+    float rx[kXE], ry[kYE];
+    auto eval = [&](int lev) {
+#pragma unroll
+        for (int q2 = 0; q2 < kXE; ++q2) {
+            const int e = tid + q2 * kTT, r = e / (kTTX + 1), q = e - r * (kTTX + 1);
+            rx[q2] = (e < kXF && j0 + r < nj && i0 + q <= ni) ? tke_tx(a, lev, j0 + r, i0 + q) : 0.0f;
         }
-        for (int e = tid; e < kYF; e += kTT) {
-            const int r = e / kTTX, q = e - r * kTTX;
-            if (j0 + r <= nj && i0 + q < ni) s_ty[slot][r][q] = tke_ty(a, lev, j0 + r, i0 + q);
+#pragma unroll
+        for (int q2 = 0; q2 < kYE; ++q2) {
+            const int e = tid + q2 * kTT, r = e / kTTX, q = e - r * kTTX;
+            ry[q2] = (e < kYF && j0 + r <= nj && i0 + q < ni) ? tke_ty(a, lev, j0 + r, i0 + q) : 0.0f;
         }
     };
-    fill(0);
-    fill(1);
+    auto store = [&](int lev) {
+        const int slot = lev % 4;
+#pragma unroll
+        for (int q2 = 0; q2 < kXE; ++q2) {
+            const int e = tid + q2 * kTT, r = e / (kTTX + 1), q = e - r * (kTTX + 1);
+            if (e < kXF) s_tx[slot][r][q] = rx[q2];
+        }
+#pragma unroll
+        for (int q2 = 0; q2 < kYE; ++q2) {
+            const int e = tid + q2 * kTT, r = e / kTTX, q = e - r * kTTX;
+            if (e < kYF) s_ty[slot][r][q] = ry[q2];
+        }
+    };
+    for (int lev = 0; lev <= 2 && lev <= nk; ++lev) {
+        eval(lev);
+        store(lev);
+    }
+    __syncthreads();
     float gzji = 0.0f, ru0 = 0.0f, ru1 = 0.0f, rv0 = 0.0f, rv1 = 0.0f;
     if (own) {
         gzji = a.gz[(size_t)j * ni + i];
@@ -184,10 +207,10 @@ __global__ void __launch_bounds__(kTT) tke_turbt_kernel(TkeArgs a, float dt) {
         rv1 = a.rgzv[(size_t)(j + 1) * ni + i];
     }
     for (int f = 1; f < nk; ++f) {
-        fill(f + 1);
-        __syncthreads();
+        const bool ahead = f + 2 <= nk;
+        if (ahead) eval(f + 2);
         if (own) {
-            const int cm = (f - 1) % 3, c0 = f % 3, cpl = (f + 1) % 3;
+            const int cm = (f - 1) % 4, c0 = f % 4, cpl = (f + 1) % 4;
             const float x0 = s_tx[c0][ty][tx], x1 = s_tx[c0][ty][tx + 1];
             float x = -1.0f * ((x1 * ru1 - x0 * ru0) * (gzji * a.rdx));
             const float sxf0 = 0.5f * (x0 + s_tx[cpl][ty][tx]), sxf1 = 0.5f * (x1 + s_tx[cpl][ty][tx + 1]);
@@ -209,6 +232,7 @@ __global__ void __launch_bounds__(kTT) tke_turbt_kernel(TkeArgs a, float dt) {
             const float vz = rfz * ((DP(f - 1) - a.t[z]) * rdt);
             a.tketen[z] = a.tketen[z] + ((hx + hy) + vz) / rfz;
         }
+        if (ahead) store(f + 2);
         __syncthreads();
     }
 #undef CP
