@@ -560,8 +560,11 @@ __global__ void __launch_bounds__(32 * kTosWarps, 3) tos_column_kernel(TosArgs p
     float *s_xw = sh, *s_xe = s_xw + L * 32, *s_ys = s_xe + L * 32, *s_yn = s_ys + L * 32;
     float *s_w = s_yn + L * 32, *s_fpk = s_w + L * 32, *s_ed = s_fpk + L * 32;
     float *s_aa = s_xw, *s_bb = s_xe, *s_cc = s_ys, *s_dd = s_yn;
-    // VM 1: the four rho-weighted face velocities (west, east, south, north)
-    float *s_r = s_ed + L * 32, *s_re = s_r + L * 32, *s_rs = s_re + L * 32, *s_rn = s_rs + L * 32;
+    // VM 1: the four rho-weighted face velocities (west, east, south, north),
+    // read only in phases A1-A2; the west array shares its words with ed,
+    // which phase B first writes (three more arrays per level, so two CTAs
+    // share an SM at nk = 80)
+    float *s_r = s_ed, *s_re = s_r + L * 32, *s_rs = s_re + L * 32, *s_rn = s_rs + L * 32;
 #define SM(arr, k) arr[(k) * 32 + lane]
     float gz = 0.0f, dzdx = 0.0f, dzdy = 0.0f;
     if (live) {
@@ -1307,7 +1310,7 @@ int32_t terrain_open_stage(int32_t ni, int32_t nj, int32_t nk, int32_t nrk, floa
         return GM1B_ERR_ARGUMENT;
     }
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    const int col_arrays = kTosArrays + (p.vmode == 1 ? 4 : 0);
+    const int col_arrays = kTosArrays + (p.vmode == 1 ? 3 : 0);
     const size_t col_smem = (size_t)col_arrays * (size_t)(nk + 2) * 32 * sizeof(float);
     static bool attr_set[64] = {};  // per device: the attribute belongs to each device's context
     int dev = 0;
@@ -1321,7 +1324,7 @@ int32_t terrain_open_stage(int32_t ni, int32_t nj, int32_t nk, int32_t nrk, floa
                                              (int)((size_t)kTosArrays * (kTosMaxNk + 2) * 32 * sizeof(float)));
         if (e == cudaSuccess)
             e = cudaFuncSetAttribute(tos_column_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)((size_t)(kTosArrays + 4) * (kTosMaxNk + 2) * 32 * sizeof(float)));
+                                     (int)((size_t)(kTosArrays + 3) * (kTosMaxNk + 2) * 32 * sizeof(float)));
         if (e == cudaSuccess)
             e = cudaFuncSetAttribute(tos_column_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)((size_t)kTosArrays * (kTosMaxNk + 2) * 32 * sizeof(float)));
