@@ -217,3 +217,36 @@ def test_flat_stretched_stage_matches_oracle(ni, nj, nk, sides):
                                                           **p)
         r.ready_event.synchronize()
         assert _bad(dev, ref, tos.ALL_ARRAY_NAMES) == [], f"nrk={nrk}"
+
+
+def test_flat_stretched_stage_replays_from_a_cuda_graph():
+    """The stretched-column stage allocates nothing and synchronises nothing
+    on a flat column: captured once in a CUDA graph and replayed, it leaves
+    the same words as the eager launch."""
+    from gm1_b200.momentum import StretchedMomentumColumn
+    from tests.test_oracle_momentum import _padded_rho0
+    from tests.test_oracle_terrain_open import _flat_column
+
+    ni, nj, nk, sides = 40, 12, 10, (1, 1, 2, 2)
+    col = _flat_column(nk)
+    a, m = terrain_open_fixture(ni, nj, nk, 77)
+    t = lambda x: torch.from_numpy(np.array(x, dtype=np.float32)).cuda()  # noqa: E731
+    vertical = StretchedMomentumColumn(True, None, mh=t(col["mh"]), mf=t(col["mf"]), rdz=col["rdz"])
+    p = dict(ni=ni, nj=nj, nk=nk, nrk=2, dt=2.0, nsound=6, dx=450.0, dy=520.0, vertical=vertical,
+             lateral_sides=sides)
+    eager, graphed, mdev = _dev(a), _dev(a), _dev(m)
+    mdev["rho0_padded"] = t(_padded_rho0(m["rho0_3d"], ni, nj, nk))
+    tos.launch_cuda_gm1_child_psolver3_open_stage(eager, mdev, **p)
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):  # first call outside the capture configures the kernels
+        warm = _dev(a)
+        tos.launch_cuda_gm1_child_psolver3_open_stage(warm, mdev, **p)
+    torch.cuda.current_stream().wait_stream(side)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        tos.launch_cuda_gm1_child_psolver3_open_stage(graphed, mdev, stream=torch.cuda.current_stream(), **p)
+    g.replay()
+    torch.cuda.synchronize()
+    assert _bad(graphed, {k: v.cpu().numpy() for k, v in eager.items()}, tos.ALL_ARRAY_NAMES) == []
