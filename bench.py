@@ -239,10 +239,26 @@ CPU_SUBBLOCK = (64, 64, 80)
 
 
 def moist_state(ni, nj, nk):
+    """The GPU arm's starting state (the package's builder)."""
     from gm1_b200.moist_step import MoistStepConfig, weisman_klemp_initial_state
 
     g = dict(MOIST_GRID, ni=ni, nj=nj, nk=nk)
     cfg = MoistStepConfig(**g)
+    host, metrics = weisman_klemp_initial_state(cfg, **MOIST_INIT)
+    return cfg, host, metrics
+
+
+def moist_state_cpu(ni, nj, nk):
+    """The CPU arms' starting state, built by the oracle's own initial-state
+    restatement (the same words as moist_state; no CUDA library is loaded on
+    the CPU baseline or the reference arm)."""
+    from types import SimpleNamespace
+
+    from oracle.moist_initial import weisman_klemp_initial_state
+
+    cfg = SimpleNamespace(**dict(MOIST_GRID, ni=ni, nj=nj, nk=nk, alph=0.60, kdiv=0.10,
+                                 lateral_sides=(2, 2, 2, 2)))
+    cfg.obc = 2 | (2 << 4) | (2 << 8) | (2 << 12)
     host, metrics = weisman_klemp_initial_state(cfg, **MOIST_INIT)
     return cfg, host, metrics
 
@@ -254,7 +270,7 @@ def moist_cpu_rate(steps_min: int, seconds_target: float, threads: int, warmup: 
     from oracle.moist_composition import OracleMoistStep
 
     orc.set_threads(threads)
-    cfg, host, metrics = moist_state(*CPU_SUBBLOCK)
+    cfg, host, metrics = moist_state_cpu(*CPU_SUBBLOCK)
     o = OracleMoistStep(cfg, host, metrics)
     for _ in range(warmup):
         o.step()
@@ -665,8 +681,9 @@ def main() -> None:
     c = DRY_BUBBLE_64
     host = dry_periodic_state(c)
     dev = to_device(host, device)
+    # barrier status words are read once after the timed region, not per step
     p = dict(ni=c.ni, nj=c.nj, nk=c.nk, steps=1, dt=c.dt, nsound=c.nsound, dx=c.dx, dy=c.dy, dz=c.dz,
-             scratch_outputs=False)
+             scratch_outputs=False, check_status=False)
     stream = torch.cuda.Stream(device)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
 
@@ -690,7 +707,7 @@ def main() -> None:
         graph = torch.cuda.CUDAGraph()
         try:
             with torch.cuda.graph(graph, stream=stream):
-                launch_cuda_psolver3_trajectory(dev, stream=stream, **p)
+                captured = launch_cuda_psolver3_trajectory(dev, stream=stream, **p)
             use_graph = True
         except Exception as exc:  # noqa: BLE001 - capture refused: time direct launches
             print(f"CUDA graph capture failed ({exc}); timing direct launches", file=sys.stderr)
@@ -721,6 +738,8 @@ def main() -> None:
             ends[q].record(stream)
     barrier()
     clocks = sampler.stop()
+    if use_graph:
+        captured.check()  # raises if a persistent stage's grid barrier gave up
     local_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
     total_ms = max_over_ranks(local_ms)
     ms_per_step = total_ms / args.steps

@@ -77,6 +77,16 @@ def lib() -> ctypes.CDLL:
         i32, i32, i32, pa, i32, f32, i32, f32, f32, f32, u32, u32, vp,
     ]
     handle.gm1b_psolver3_trajectory.restype = i32
+    handle.gm1b_sound3_periodic_three_stage_checked.argtypes = [
+        i32, i32, i32, pa, f32, i32, f32, f32, f32, f32, f32, f32, u32, i32, vp, vp,
+    ]
+    handle.gm1b_sound3_periodic_three_stage_checked.restype = i32
+    handle.gm1b_psolver3_trajectory_checked.argtypes = [
+        i32, i32, i32, pa, i32, f32, i32, f32, f32, f32, u32, u32, i32, vp, vp,
+    ]
+    handle.gm1b_psolver3_trajectory_checked.restype = i32
+    handle.gm1b_step_status_fold.argtypes = [vp, vp, vp, vp]
+    handle.gm1b_step_status_fold.restype = i32
     handle.gm1b_profiler_enable.argtypes = [i32]
     handle.gm1b_profiler_enable.restype = i32
     handle.gm1b_profiler_collect.argtypes = [ctypes.POINTER(KernelStat), i32, ctypes.POINTER(i32)]

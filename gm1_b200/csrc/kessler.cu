@@ -25,6 +25,7 @@
 namespace gm1b {
 namespace {
 
+constexpr int kMaxFallSubsteps = 1 << 14;  // bound of the fallout sub-steps of one column
 constexpr int kKX = 128;  // cell-kernel CTA: a run of 128 cells of one row at one level
 constexpr int kCX = 32, kCY = 4;
 
@@ -72,7 +73,8 @@ struct KDims {
 
 // workspace layout (doubles after a 16-byte status block)
 struct KWork {
-    int32_t *status;   // [0] satadj non-converged cells, [1] max fallout sub-steps
+    int32_t *status;   // [0] satadj non-converged cells, [1] max fallout sub-steps,
+                       // [2] columns whose fall Courant number was not finite or >= kMaxFallSubsteps
     double *colterm;   // [5][nj*ni]
     double *rows;      // [5][nj]
     double *partial;   // [5][nk][nj][nbx]
@@ -162,6 +164,15 @@ __global__ void __launch_bounds__(kCX *kCY)
     }
     int nfall = (int)(crmax + 1.0f);
     if (nfall < 1) nfall = 1;
+    // A column whose fall Courant number is not finite or above
+    // kMaxFallSubsteps holds no physical state (rain or density already blew
+    // up); int(crmax + 1) would reach 2^31 sub-steps.  It is counted in
+    // status[2] and takes one sub-step, so the launch stays bounded and the
+    // caller refuses the step.
+    if (!(crmax < (float)kMaxFallSubsteps)) {
+        atomicAdd(&w.status[2], 1);
+        nfall = 1;
+    }
     if (a.nfall != nullptr) a.nfall[col] = nfall;
     atomicMax(&w.status[1], nfall);
     // below-threshold rain takes the fall speed of the level above
@@ -537,9 +548,10 @@ void *g_static_ptr[64] = {};  // device address of the array, per device ordinal
 // Device address of the scratch array on the current device, resolved once
 // per device (host code may not use the symbol itself: on the host it names
 // a stand-in, not device memory).
-void *static_scratch_address() {
-    int dev = -1;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+// The cached address stays valid for the life of the device's primary
+// context; a caller that resets the device (cudaDeviceReset) must not call
+// this entry point again in the same process.
+void *static_scratch_address(int dev) {
     std::lock_guard<std::mutex> g(g_static_mu);
     if (g_static_ptr[dev] == nullptr) {
         void *p = nullptr;
@@ -565,7 +577,18 @@ extern "C" int32_t gm1b_kessler_driver_static(int32_t ni, int32_t nj, int32_t nk
                        ni, nj, nk, need, (unsigned)GM1B_KESSLER_STATIC_SCRATCH_BYTES);
         return GM1B_ERR_ARGUMENT;
     }
-    void *scratch = static_scratch_address();
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        gm1b_set_error("gm1b_kessler_driver_static: no current CUDA device");
+        return GM1B_ERR_CUDA;
+    }
+    if (dev < 0 || dev >= 64) {
+        gm1b_set_error("gm1b_kessler_driver_static: device ordinal %d is beyond the 64 devices this entry point "
+                       "serves; use gm1b_kessler_driver with a caller workspace", dev);
+        return GM1B_ERR_ARGUMENT;
+    }
+    void *scratch = static_scratch_address(dev);
     if (scratch == nullptr) {
         cudaGetLastError();
         gm1b_set_error("gm1b_kessler_driver_static: cudaGetSymbolAddress of the static scratch failed");

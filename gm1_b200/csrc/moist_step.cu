@@ -1053,3 +1053,45 @@ extern "C" int32_t gm1b_w_level1_fill(int32_t ni, int32_t nj, int32_t nk, float 
     }
     return GM1B_OK;
 }
+
+// ---------------------------------------------------------------------------
+// step status: the failure words the reference reads back after a step and
+// refuses on (satadj non-convergence, cuda_cartesian_finish.py:638-639; the
+// advective Courant stop, gm1_runtime.py:518-549), folded on the device into
+// one accumulator so a captured step needs no host read.
+// acc: [0] non-converged satadj cells (sum), [1] largest fallout sub-step
+// count, [2] blown-up fall columns (sum), [3] largest Courant number (float
+// bits; a NaN stays), [4] folds of a Courant number, [5] folds of Kessler words.
+// ---------------------------------------------------------------------------
+namespace gm1b {
+namespace {
+__global__ void step_status_fold_kernel(const int32_t *kessler_status, const float *courant, int32_t *acc) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (kessler_status != nullptr) {
+        acc[0] += kessler_status[0];
+        acc[1] = max(acc[1], kessler_status[1]);
+        acc[2] += kessler_status[2];
+        acc[5] += 1;
+    }
+    if (courant != nullptr) {
+        const float c = *courant;
+        const float prev = __int_as_float(acc[3]);
+        if (acc[4] == 0 || c != c || (prev == prev && c > prev)) acc[3] = __float_as_int(c);
+        acc[4] += 1;
+    }
+}
+}  // namespace
+}  // namespace gm1b
+
+extern "C" int32_t gm1b_step_status_fold(const int32_t *kessler_status, const float *courant, int32_t *acc,
+                                         void *stream) {
+    if (acc == nullptr) {
+        gm1b_set_error("gm1b_step_status_fold: NULL accumulator");
+        return GM1B_ERR_ARGUMENT;
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    ProfScope ps("step_status_fold_kernel", st);
+    step_status_fold_kernel<<<1, 32, 0, st>>>(kessler_status, courant, acc);
+    ps.stop();
+    return launch_ok("step_status_fold_kernel") ? GM1B_OK : GM1B_ERR_CUDA;
+}

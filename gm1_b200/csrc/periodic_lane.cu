@@ -320,9 +320,10 @@ __global__ void __launch_bounds__(kTX *kTY) sound_prep_kernel(Arr a, Dims d, int
     const int ni = d.ni, nj = d.nj, nk = d.nk;
     if (i >= ni + 2 || j >= nj + 2) return;
     if (fused_reset && i == 0 && j == 0 && k == 0) {
-        // grid-barrier counter and status of the fused stage kernel
+        // grid-barrier counter of the fused stage kernel; its error word only
+        // on the call's first fused stage (fused_reset == 2)
         *reinterpret_cast<unsigned long long *>(a.tri_residual) = 0ull;
-        reinterpret_cast<int *>(a.tri_residual)[2] = 0;
+        if (fused_reset == 2) reinterpret_cast<int *>(a.tri_residual)[2] = 0;
     }
     const size_t c = d.s(k, j, i);
     const bool klive = k >= 1 && k <= nk;
@@ -875,10 +876,18 @@ int launch_fused_stage(const Arr &a, const Dims &d, const FusedArgs &p, cudaStre
     return check_launch("sound_stage_fused_kernel") ? GM1B_OK : GM1B_ERR_CUDA;
 }
 
+// Per-call control of the fused stage's grid barrier: the spin limit, the
+// caller's status word, and whether a fused stage of this call has run yet.
+struct BarrierControl {
+    int spin_limit = kSpinLimit;
+    int32_t *status = nullptr;
+    bool fused_seen = false;
+};
+
 // One acoustic RK stage; returns nloop, or a negative status.
 int enqueue_sound_stage(const Arr &a, const Dims &d, float dt, int nsound, int nrk, float rdx, float rdy, float rdz,
                         float cp, float alph, float kdiv, uint32_t flags, int trajectory, int post_ppx,
-                        cudaStream_t st) {
+                        BarrierControl &bc, cudaStream_t st) {
     const int scratch_outputs = (flags & GM1B_FLAG_SCRATCH_OUTPUTS) ? 1 : 0;
     int nloop;
     float dts;
@@ -889,10 +898,12 @@ int enqueue_sound_stage(const Arr &a, const Dims &d, float dt, int nsound, int n
     const float beta = 1.0f - alph;
     const float asq = alph * alph;
     const bool fused = fused_stage_eligible(a, d, nloop, flags);
+    const int fused_reset = fused ? (bc.fused_seen ? 1 : 2) : 0;
+    if (fused) bc.fused_seen = true;
     {
             ProfScope ps_("sound_prep_kernel", st);
             sound_prep_kernel<<<box_grid(d.ni + 2, d.nj + 2, d.nk + 2), dim3(kTX, kTY), 0, st>>>(a, d, nrk, dts, rdz, cp, beta,
-                                                                                        scratch_outputs, fused ? 1 : 0);
+                                                                                        scratch_outputs, fused_reset);
             ps_.stop();
         }
     if (!check_launch("sound_prep_kernel")) return GM1B_ERR_CUDA;
@@ -918,6 +929,8 @@ int enqueue_sound_stage(const Arr &a, const Dims &d, float dt, int nsound, int n
         f.tavg = 1.0f / (float)nloop;
         f.fill_pp3d = (nrk < 3) || trajectory;
         f.post_ppx = post_ppx;
+        f.spin_limit = bc.spin_limit;
+        f.status = bc.status;
         const int r = launch_fused_stage(a, d, f, st);
         return r < 0 ? r : nloop;
     }
@@ -1000,10 +1013,29 @@ extern "C" float gm1b_rk_stage_dt(float dt, int32_t nrk) {
     return dt / (float)(4 - nrk);
 }
 
-extern "C" int32_t gm1b_sound3_periodic_three_stage(int32_t ni, int32_t nj, int32_t nk,
-                                                   const gm1b_periodic_arrays *arrays, float dt, int32_t nsound,
-                                                   float rdx, float rdy, float rdz, float cp, float alph, float kdiv,
-                                                   uint32_t flags, void *stream) {
+namespace {
+// Barrier control of one call: spin_limit <= 0 takes the default; the status
+// word (when given) is cleared on the stream before the call's first launch.
+bool barrier_control(BarrierControl *bc, int32_t spin_limit, int32_t *status_dev, cudaStream_t st) {
+    bc->spin_limit = spin_limit > 0 ? spin_limit : kSpinLimit;
+    bc->status = status_dev;
+    if (status_dev != nullptr) {
+        const cudaError_t e = cudaMemsetAsync(status_dev, 0, sizeof(int32_t), st);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            gm1b_set_error("cudaMemsetAsync (barrier status word): %s", cudaGetErrorString(e));
+            return false;
+        }
+    }
+    return true;
+}
+}  // namespace
+
+extern "C" int32_t gm1b_sound3_periodic_three_stage_checked(int32_t ni, int32_t nj, int32_t nk,
+                                                           const gm1b_periodic_arrays *arrays, float dt,
+                                                           int32_t nsound, float rdx, float rdy, float rdz, float cp,
+                                                           float alph, float kdiv, uint32_t flags, int32_t spin_limit,
+                                                           int32_t *status_dev, void *stream) {
     if (arrays == nullptr || ni < 3 || nj < 3 || nk < 3) {
         gm1b_set_error("gm1b_sound3_periodic_three_stage: need arrays and ni, nj, nk >= 3");
         return GM1B_ERR_ARGUMENT;
@@ -1012,16 +1044,35 @@ extern "C" int32_t gm1b_sound3_periodic_three_stage(int32_t ni, int32_t nj, int3
     if (!prepare_column_kernel(nk)) return GM1B_ERR_CUDA;
     const Dims d{ni, nj, nk};
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    BarrierControl bc;
+    if (!barrier_control(&bc, spin_limit, status_dev, st)) return GM1B_ERR_CUDA;
     for (int nrk = 1; nrk <= 3; ++nrk) {
-        int r = enqueue_sound_stage(*arrays, d, dt, nsound, nrk, rdx, rdy, rdz, cp, alph, kdiv, flags, 0, 0, st);
+        int r = enqueue_sound_stage(*arrays, d, dt, nsound, nrk, rdx, rdy, rdz, cp, alph, kdiv, flags, 0, 0, bc, st);
         if (r < 0) return r;
     }
     return GM1B_OK;
 }
 
+extern "C" int32_t gm1b_sound3_periodic_three_stage(int32_t ni, int32_t nj, int32_t nk,
+                                                   const gm1b_periodic_arrays *arrays, float dt, int32_t nsound,
+                                                   float rdx, float rdy, float rdz, float cp, float alph, float kdiv,
+                                                   uint32_t flags, void *stream) {
+    return gm1b_sound3_periodic_three_stage_checked(ni, nj, nk, arrays, dt, nsound, rdx, rdy, rdz, cp, alph, kdiv,
+                                                    flags, 0, nullptr, stream);
+}
+
 extern "C" int32_t gm1b_psolver3_trajectory(int32_t ni, int32_t nj, int32_t nk, const gm1b_periodic_arrays *arrays,
                                            int32_t steps, float dt, int32_t nsound, float dx, float dy, float dz,
                                            uint32_t ablations, uint32_t flags, void *stream) {
+    return gm1b_psolver3_trajectory_checked(ni, nj, nk, arrays, steps, dt, nsound, dx, dy, dz, ablations, flags, 0,
+                                            nullptr, stream);
+}
+
+extern "C" int32_t gm1b_psolver3_trajectory_checked(int32_t ni, int32_t nj, int32_t nk,
+                                                   const gm1b_periodic_arrays *arrays, int32_t steps, float dt,
+                                                   int32_t nsound, float dx, float dy, float dz, uint32_t ablations,
+                                                   uint32_t flags, int32_t spin_limit, int32_t *status_dev,
+                                                   void *stream) {
     if (arrays == nullptr || ni < 5 || nj < 5 || nk < 6 || steps < 1) {
         gm1b_set_error("gm1b_psolver3_trajectory: need arrays, ni >= 5, nj >= 5, nk >= 6, steps >= 1");
         return GM1B_ERR_ARGUMENT;
@@ -1047,6 +1098,8 @@ extern "C" int32_t gm1b_psolver3_trajectory(int32_t ni, int32_t nj, int32_t nk, 
     const Arr &a = *arrays;
     const Dims d{ni, nj, nk};
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    BarrierControl bc;
+    if (!barrier_control(&bc, spin_limit, status_dev, st)) return GM1B_ERR_CUDA;
     const float rdx = 1.0f / dx, rdy = 1.0f / dy, rdz = 1.0f / dz;
     const int advect = !(ablations & GM1B_ABLATE_MOMENTUM_ADVECTION);
     const int buoy = !(ablations & GM1B_ABLATE_BUOYANCY);
@@ -1084,7 +1137,7 @@ extern "C" int32_t gm1b_psolver3_trajectory(int32_t ni, int32_t nj, int32_t nk, 
                         }
             if (!check_launch("traj_momentum_kernel")) return GM1B_ERR_CUDA;
             int r = enqueue_sound_stage(a, d, dt, nsound, nrk, rdx, rdy, rdz, kCp, kAlph, kKdiv, flags, 1,
-                                        post_ppx, st);
+                                        post_ppx, bc, st);
             if (r < 0) return r;
             {
                             ProfScope ps_("traj_theta_prep_kernel", st);

@@ -29,8 +29,12 @@
 //    memory and only their rru / rrv words are written, since the stage-end
 //    periodic fill overwrites their u / v words;
 //  * the grid barrier is an arrive counter (64-bit, reset by sound_prep_kernel
-//    in tri_residual words 0-1) with a bounded spin: after kSpinLimit polls a
-//    CTA records 1 in tri_residual word 2 and every CTA leaves the kernel.
+//    in tri_residual words 0-1) with a bounded spin: after spin_limit polls
+//    (a launch argument, kSpinLimit by default) a CTA records 1 in
+//    tri_residual word 2 and in the caller's status word (when one is given),
+//    and every CTA leaves the kernel at its next barrier.  The error word is
+//    cleared only by the first fused stage of a library call, so after a
+//    failure every later stage of the same call leaves at its first barrier.
 //    The launch is cooperative, so all CTAs are co-resident.
 //
 // Shared-memory layout: arrays of L = nk+2 levels, 32 lanes (columns
@@ -45,6 +49,8 @@ struct FusedArgs {
     int nrk, nloop;
     float dts, rdx, rdy, alph, beta, asq, kdiv, smeps, temx, temy, rnloop, tem1x, tem2y, tavg;
     int fill_pp3d, post_ppx;
+    int spin_limit;  // barrier polls before a CTA gives up
+    int *status;     // caller's status word (device, may be null): 1 once a barrier gave up
 };
 
 __host__ __device__ constexpr size_t fused_smem_floats(int nk) {
@@ -60,7 +66,8 @@ __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long
 __device__ __forceinline__ int ld_volatile_i32(const int *p) { return *reinterpret_cast<const volatile int *>(p); }
 
 // Bounded grid barrier; returns false (all threads) once any CTA gave up.
-__device__ __forceinline__ bool fused_grid_sync(unsigned long long *ctr, int *err, unsigned long long target) {
+__device__ __forceinline__ bool fused_grid_sync(unsigned long long *ctr, int *err, unsigned long long target,
+                                                int spin_limit, int *status) {
     __shared__ int s_fail;
     __syncthreads();
     if (threadIdx.x == 0 && threadIdx.y == 0) {
@@ -73,8 +80,9 @@ __device__ __forceinline__ bool fused_grid_sync(unsigned long long *ctr, int *er
                 fail = 1;
                 break;
             }
-            if (it >= kSpinLimit) {
+            if (it >= spin_limit) {
                 atomicExch(err, 1);
+                if (status != nullptr) atomicExch(status, 1);
                 fail = 1;
                 break;
             }
@@ -498,7 +506,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) sound_stage_fused_kernel(Arr
         }
         if (!last) {
             const unsigned long long target = (unsigned long long)n * (gridDim.x * gridDim.y);
-            if (!fused_grid_sync(ctr, err, target)) return;
+            if (!fused_grid_sync(ctr, err, target, p.spin_limit, p.status)) return;
         }
     }
     // ---- stage end: u, v, rru, rrv and the stage-end periodic u/v fill -----

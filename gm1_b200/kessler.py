@@ -136,15 +136,21 @@ class CudaKesslerLaunch:
         """Waits for the launch and reads its status words."""
         self.ready_event.synchronize()
         s = self.workspace.status.cpu().tolist()
-        return {"satadj_nonconverged_cells": int(s[0]), "max_fall_substeps": int(s[1])}
+        return {"satadj_nonconverged_cells": int(s[0]), "max_fall_substeps": int(s[1]),
+                "blown_up_fall_columns": int(s[2])}
 
     def check(self) -> dict[str, int]:
         """status(), raising like the reference if any saturation adjustment
-        did not converge within 100 iterations."""
+        did not converge within 100 iterations, and if a rain column's fall
+        Courant number was not finite or reached 16384 (a blown-up state that
+        the operator stepped once instead of int(crmax + 1) times)."""
         s = self.status()
         if s["satadj_nonconverged_cells"]:
             raise RuntimeError("GM1 Kessler satadj failed to converge in 100 iterations "
                                f"({s['satadj_nonconverged_cells']} cells)")
+        if s["blown_up_fall_columns"]:
+            raise RuntimeError(f"GM1 Kessler fallout: {s['blown_up_fall_columns']} columns with a fall Courant "
+                               "number that is not finite or at least 16384")
         return s
 
 

@@ -47,6 +47,7 @@ from . import moist_ops as mo
 from .advection import launch_cuda_scalar_advection5
 from .closure import launch_cuda_moist_nm, launch_cuda_terrain_deformation
 from .kessler import (Gm1KesslerDriverSelection, Gm1KesslerHeldCarriers, create_cuda_gm1_kessler_large_step_transition)
+from .limits import CM1_COURANT_STOP, advective_courant_number
 from .moist_bridge import launch_cuda_eqtset2_stage_terms
 from .scalar_rk import (compose_scalar_moist_rk_stage, moisture_weps_f64, scalar_moist_rk_stage_timestep_f32,
                         theta_transport_scalar, theta_weps_f64)
@@ -55,6 +56,18 @@ from .terrain_open import (ALL_ARRAY_NAMES as TOS_ARRAY_NAMES, COLUMN_DIAGNOSTIC
                            _lib as _tos_lib)
 from .tke import launch_cuda_sgs_tke
 from .tke_evolution import launch_cuda_tke_diffusion, launch_cuda_tke_rk_stage
+
+
+class MoistStepFailure(RuntimeError):
+    """A composed step reached a state the reference refuses to continue."""
+
+
+class SatadjNonConvergence(MoistStepFailure):
+    """Saturation adjustment ran out of iterations (CM1 stops the run)."""
+
+
+class CourantStop(MoistStepFailure):
+    """The advective Courant number reached 1.5 or is not finite."""
 
 
 class StepPhase(str, Enum):
@@ -333,6 +346,13 @@ class MoistLargeStep:
         self._tos_lib = _tos_lib()
         self._tos = _TosArrays(**{n: s[n].data_ptr() for n in TOS_ARRAY_NAMES})
         self._tos_m = _TosMetrics(**{n: m[n].data_ptr() for n in TOS_METRICS})
+        # failure words folded on the device every step (gm1b_step_status_fold)
+        self.status_acc = torch.zeros(8, dtype=torch.int32, device=dev)
+        self._courant = torch.zeros(1, dtype=torch.float32, device=dev)
+        self._courant_keys = torch.zeros(nk, dtype=torch.int32, device=dev)
+        self._ones_i = torch.ones(ni, dtype=torch.float32, device=dev)
+        self._ones_j = torch.ones(nj, dtype=torch.float32, device=dev)
+        self._mh_col = m["mh"][:, 0, 0].contiguous()
         self.completed_steps = 0
 
     # -- helpers -----------------------------------------------------------
@@ -357,6 +377,7 @@ class MoistLargeStep:
             s["vc"].copy_(s["v3d"][1:nk + 1, 3:4 + nj, 3:3 + ni])
             s["wc"].copy_(s["w3d"][1:nk + 2, 3:3 + nj, 3:3 + ni])
             self._interior_pp3d_to_compact()
+        self._fold_courant(st)
         launch_cuda_moist_nm(self.nm_arrays, **self.k3, dz=cfg.dz, stream=st)
         launch_cuda_terrain_deformation(self.def_arrays, **self.grid, stream=st)
         launch_cuda_sgs_tke(self.sgs_arrays, **self.grid, stream=st)
@@ -473,6 +494,9 @@ class MoistLargeStep:
             self._interior_pp3d_to_compact()
         self.kessler.stream = st
         self.kessler.apply()
+        _native.check(_native.lib().gm1b_step_status_fold(
+            ctypes.c_void_p(self.kessler.workspace.status.data_ptr()), None,
+            ctypes.c_void_p(self.status_acc.data_ptr()), ctypes.c_void_p(st.cuda_stream)), "gm1b_step_status_fold")
         with torch.cuda.stream(st):
             self._compact_pp3d_to_interior()
 
@@ -484,6 +508,61 @@ class MoistLargeStep:
                               ("qa", "q3d"), ("tkea", "tke3d")):
                 s[cur].copy_(s[base])
         mo.solve3_density(s["rho"], m["c1"], m["c2"], s["rr"], s["rf"], **self.k3, stream=st)
+
+    # -- failure words -----------------------------------------------------
+    def _fold_courant(self, st) -> None:
+        """The advective Courant number of the compact winds uc/vc/wc (the
+        state entering this step), folded into status_acc."""
+        cfg, s = self.cfg, self.s
+        advective_courant_number(u=s["uc"], v=s["vc"], w=s["wc"], uh=self._ones_i, vh=self._ones_j,
+                                 mh=self._mh_col, dt_s=cfg.dt, dx_m=cfg.dx, dy_m=cfg.dy, dz_m=cfg.dz,
+                                 level_keys=self._courant_keys, stream=st, out=self._courant)
+        _native.check(_native.lib().gm1b_step_status_fold(
+            None, ctypes.c_void_p(self._courant.data_ptr()), ctypes.c_void_p(self.status_acc.data_ptr()),
+            ctypes.c_void_p(st.cuda_stream)), "gm1b_step_status_fold")
+
+    def status(self) -> dict[str, Any]:
+        """Waits for the enqueued work and reads the folded failure words of
+        every step since construction (or the last reset_status())."""
+        st = self._st()
+        st.synchronize()
+        acc = self.status_acc.cpu().numpy()
+        return {"satadj_nonconverged_cells": int(acc[0]), "max_fall_substeps": int(acc[1]),
+                "blown_up_fall_columns": int(acc[2]),
+                "max_courant": float(acc[3:4].view(np.float32)[0]) if acc[4] else None,
+                "courant_samples": int(acc[4]), "kessler_samples": int(acc[5])}
+
+    def reset_status(self) -> None:
+        with torch.cuda.stream(self._st()):
+            self.status_acc.zero_()
+
+    def check(self, *, current_state: bool = True) -> dict[str, Any]:
+        """Refuse the integration as the reference does: raise
+        SatadjNonConvergence if any saturation adjustment ran out of
+        iterations (or a fall column blew up) and CourantStop if the
+        advective Courant number reached 1.5 or is not finite
+        (src/cm1core/cuda_cartesian_finish.py:638-639;
+        src/cm1core/gm1_runtime.py:518-549).  The Courant number covers the
+        state entering every step taken and, with current_state, the
+        current state too."""
+        if current_state:
+            cfg, s, st = self.cfg, self.s, self._st()
+            nk, nj, ni = cfg.nk, cfg.nj, cfg.ni
+            with torch.cuda.stream(st):
+                s["uc"].copy_(s["u3d"][1:nk + 1, 3:3 + nj, 3:4 + ni])
+                s["vc"].copy_(s["v3d"][1:nk + 1, 3:4 + nj, 3:3 + ni])
+                s["wc"].copy_(s["w3d"][1:nk + 2, 3:3 + nj, 3:3 + ni])
+            self._fold_courant(st)
+        out = self.status()
+        if out["satadj_nonconverged_cells"] or out["blown_up_fall_columns"]:
+            raise SatadjNonConvergence(
+                f"GM1 Kessler satadj failed to converge in 100 iterations in {out['satadj_nonconverged_cells']} "
+                f"cells ({out['blown_up_fall_columns']} rain columns with a non-finite fall Courant number)")
+        c = out["max_courant"]
+        if c is not None and (not np.isfinite(c) or c >= CM1_COURANT_STOP):
+            raise CourantStop(f"the advective Courant number {c!r} has reached CM1's stop value "
+                              f"{CM1_COURANT_STOP} or is not finite (misclibs.F:2714)")
+        return out
 
     # -- driver ------------------------------------------------------------
     def execute(self, op: ScheduledOperation) -> None:

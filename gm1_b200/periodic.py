@@ -10,7 +10,12 @@ behaviour are the reference's):
 Each call validates its arguments on the host, enqueues the CUDA kernels of
 libgm1b.so on ``stream`` (the current torch stream by default) and returns a
 launch record whose ``ready_event`` completes with the last kernel.  Nothing
-is synchronised and nothing is allocated on the device.
+is allocated on the device but a one-word status.  A stage that runs as the
+one persistent kernel waits at a bounded grid barrier each small step; the
+launch record's ``check()`` raises BarrierTimeout if one gave up, and the
+launchers call it before they return (check_status=True, the default)
+unless the stream is being captured into a CUDA graph, where the caller
+calls ``check()`` after the replay.
 """
 
 from __future__ import annotations
@@ -59,6 +64,22 @@ class TrajectoryAblations:
 class CudaLaunch:
     ready_event: torch.cuda.Event
     receipt: dict[str, Any]
+    # one device int32: 1 once a persistent acoustic stage's grid barrier gave
+    # up (its fields are then invalid), else 0
+    barrier_status: torch.Tensor | None = None
+
+    def check(self) -> None:
+        """Wait for the launch and raise if a persistent acoustic stage's
+        grid barrier gave up (the reference reads its device status words
+        back and refuses in the same way, src/cm1core/cuda_graphs.py:197)."""
+        self.ready_event.synchronize()
+        if self.barrier_status is not None and int(self.barrier_status.item()) != 0:
+            raise BarrierTimeout("a persistent acoustic stage's grid barrier gave up waiting for its CTAs; "
+                                 "the fields of this launch are invalid")
+
+
+class BarrierTimeout(_native.Gm1bError):
+    """A persistent acoustic stage's bounded grid barrier ran out."""
 
 
 def sound3_stage_schedule_f32(dt: float, nsound: int, nrk: int) -> tuple[int, float]:
@@ -140,8 +161,13 @@ def launch_cuda_sound3_periodic_three_stage(
     stream: Any | None = None,
     scratch_outputs: bool = False,
     fused_stage: bool = True,
+    barrier_spin_limit: int = 0,
+    check_status: bool = True,
 ) -> CudaLaunch:
-    """Enqueue the three periodic acoustic RK stages without synchronising.
+    """Enqueue the three periodic acoustic RK stages.
+
+    ``barrier_spin_limit`` bounds the persistent stage's barrier waits in
+    polls (0: the library's default of about a second).
 
     ``scratch_outputs`` also writes the reference-semantics scratch arrays of
     the last small step (fpk, divh, hadvp, elim_c, elim_d, tri_*); without it
@@ -156,10 +182,12 @@ def launch_cuda_sound3_periodic_three_stage(
     flags = _native.GM1B_FLAG_SCRATCH_OUTPUTS if scratch_outputs else 0
     if not fused_stage:
         flags |= _native.GM1B_FLAG_MULTI_LAUNCH_STAGE
+    spin = _spin_limit(barrier_spin_limit)
     with torch.cuda.device(device):
-        status = _native.lib().gm1b_sound3_periodic_three_stage(
-            ni, nj, nk, ctypes.byref(s), dt, nsound, rdx, rdy, rdz, cp, alph, kdiv, flags,
-            ctypes.c_void_p(st.cuda_stream),
+        word = torch.zeros(1, dtype=torch.int32, device=device)
+        status = _native.lib().gm1b_sound3_periodic_three_stage_checked(
+            ni, nj, nk, ctypes.byref(s), dt, nsound, rdx, rdy, rdz, cp, alph, kdiv, flags, spin,
+            ctypes.c_void_p(word.data_ptr()), ctypes.c_void_p(st.cuda_stream),
         )
         _native.check(status, "gm1b_sound3_periodic_three_stage")
         event = torch.cuda.Event()
@@ -168,7 +196,20 @@ def launch_cuda_sound3_periodic_three_stage(
     for nrk in (1, 2, 3):
         nloop, dts = sound3_stage_schedule_f32(dt, nsound, nrk)
         cadence.append({"nrk": nrk, "nloop": nloop, "dts_f32": dts, "dttmp_f32": rk_stage_dt_f32(dt, nrk)})
-    return CudaLaunch(event, {"operator": "sound3_periodic_three_stage", "cadence": cadence})
+    launch = CudaLaunch(event, {"operator": "sound3_periodic_three_stage", "cadence": cadence}, word)
+    _maybe_check(launch, st, check_status)
+    return launch
+
+
+def _spin_limit(value: Any) -> int:
+    if isinstance(value, bool) or not isinstance(value, int) or value < 0 or value > 2**31 - 1:
+        raise ValueError("barrier_spin_limit must be an integer in [0, 2**31)")
+    return value
+
+
+def _maybe_check(launch: CudaLaunch, st: torch.cuda.Stream, check_status: bool) -> None:
+    if check_status and not torch.cuda.is_current_stream_capturing():
+        launch.check()
 
 
 def _validate_run_parameters(*, ni, nj, nk, dt, nsound, dx, dy, dz) -> None:
@@ -198,6 +239,8 @@ def launch_cuda_psolver3_trajectory(
     stream: Any | None = None,
     scratch_outputs: bool = True,
     fused_stage: bool = True,
+    barrier_spin_limit: int = 0,
+    check_status: bool = True,
 ) -> CudaLaunch:
     """Enqueue ``steps`` dry RK3 large steps of the periodic trajectory.
 
@@ -221,10 +264,12 @@ def launch_cuda_psolver3_trajectory(
     flags = _native.GM1B_FLAG_SCRATCH_OUTPUTS if scratch_outputs else 0
     if not fused_stage:
         flags |= _native.GM1B_FLAG_MULTI_LAUNCH_STAGE
+    spin = _spin_limit(barrier_spin_limit)
     with torch.cuda.device(device):
-        status = _native.lib().gm1b_psolver3_trajectory(
-            ni, nj, nk, ctypes.byref(s), steps, dt, nsound, dx, dy, dz, mask, flags,
-            ctypes.c_void_p(st.cuda_stream),
+        word = torch.zeros(1, dtype=torch.int32, device=device)
+        status = _native.lib().gm1b_psolver3_trajectory_checked(
+            ni, nj, nk, ctypes.byref(s), steps, dt, nsound, dx, dy, dz, mask, flags, spin,
+            ctypes.c_void_p(word.data_ptr()), ctypes.c_void_p(st.cuda_stream),
         )
         _native.check(status, "gm1b_psolver3_trajectory")
         event = torch.cuda.Event()
@@ -240,7 +285,9 @@ def launch_cuda_psolver3_trajectory(
         "ablation_mask": mask,
         "cells": ni * nj * nk,
     }
-    return CudaLaunch(event, receipt)
+    launch = CudaLaunch(event, receipt, word)
+    _maybe_check(launch, st, check_status)
+    return launch
 
 
 def to_device(arrays: Mapping[str, np.ndarray], device: str | torch.device = "cuda") -> dict[str, torch.Tensor]:

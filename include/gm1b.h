@@ -139,6 +139,29 @@ GM1B_API int32_t gm1b_psolver3_trajectory(
     int32_t steps, float dt, int32_t nsound, float dx, float dy, float dz,
     uint32_t ablations, uint32_t flags, void *stream);
 
+/*
+ * gm1b_psolver3_trajectory and gm1b_sound3_periodic_three_stage with the
+ * persistent acoustic stage's grid-barrier status surfaced.  When a stage
+ * runs as the one persistent cooperative kernel (no scratch outputs, nk <= 44,
+ * the row tiles co-resident), each small step ends at a grid barrier whose
+ * wait is bounded: after spin_limit polls (<= 0: the default, about a second
+ * of L2 round trips) a CTA gives up, writes 1 into status_dev[0] and every
+ * CTA leaves the kernel, so the fields of that call are invalid but the
+ * context stays usable.  status_dev (one device int32, or NULL) is cleared
+ * on the stream before the call's first launch.  The reference reads its
+ * device status words back and refuses (cuda_graphs.read_device,
+ * src/cm1core/cuda_graphs.py:197); the caller does that here by reading
+ * status_dev after the stream's work.
+ */
+GM1B_API int32_t gm1b_psolver3_trajectory_checked(
+    int32_t ni, int32_t nj, int32_t nk, const gm1b_periodic_arrays *arrays,
+    int32_t steps, float dt, int32_t nsound, float dx, float dy, float dz,
+    uint32_t ablations, uint32_t flags, int32_t spin_limit, int32_t *status_dev, void *stream);
+GM1B_API int32_t gm1b_sound3_periodic_three_stage_checked(
+    int32_t ni, int32_t nj, int32_t nk, const gm1b_periodic_arrays *arrays,
+    float dt, int32_t nsound, float rdx, float rdy, float rdz, float cp,
+    float alph, float kdiv, uint32_t flags, int32_t spin_limit, int32_t *status_dev, void *stream);
+
 
 /* ------------------------------------------------------------------------
  * Padded lane (ng = 3 lateral ghost cells, CM1_OPEN_NGXY): shapes
@@ -323,10 +346,12 @@ GM1B_API size_t gm1b_kessler_workspace_bytes(int32_t ni, int32_t nj, int32_t nk)
  * speed, rain-energy budget, fallout sub-stepping, local conversion and
  * saturation adjustment (equation_set 1 or 2; efall must be 0).
  * `workspace` (16-byte aligned, gm1b_kessler_workspace_bytes) holds the
- * budget partial sums; its first two int32 words are set by the call to the
- * number of cells whose saturation adjustment did not converge within 100
- * iterations (the reference raises on any) and the largest fallout
- * sub-step count.
+ * budget partial sums; its first three int32 words are set by the call to
+ * the number of cells whose saturation adjustment did not converge within
+ * 100 iterations (the reference raises on any), the largest fallout
+ * sub-step count, and the number of columns whose fall Courant number was
+ * not finite or reached 16384 (a blown-up state: such a column takes one
+ * sub-step instead of int(crmax + 1), which would reach 2^31).
  * Replaces launch_cuda_gm1_kessler_driver
  * (src/cm1core/cuda_gm1_kessler_driver.py:907) and its CPU twin
  * cpu_gm1_kessler_driver_inplace (:431).
@@ -336,29 +361,6 @@ GM1B_API int32_t gm1b_kessler_driver(int32_t ni, int32_t nj, int32_t nk,
                                      float dz, float dt, int32_t equation_set, int32_t efall,
                                      void *workspace, size_t workspace_size, void *stream);
 
-/*
- * gm1b_kessler_driver without a workspace argument, for callers that cannot
- * allocate device memory of their own (for instance a Fortran or C host
- * model bound through this ABI whose device memory belongs to another
- * runtime's pool, or a process whose device memory another framework
- * reserves up front): the budget scratch lives in a static device array of
- * GM1B_KESSLER_STATIC_SCRATCH_BYTES (8 MiB), which every GPU that loads the
- * library holds until the process exits.  No counterpart in the reference
- * (its launcher always allocates a workspace).
- *
- * - Grids whose scratch (gm1b_kessler_workspace_bytes) exceeds 8 MiB are
- *   rejected with GM1B_ERR_ARGUMENT; 8 MiB covers, e.g., 256x256x80.
- * - The first call on a device resolves the array's device address for that
- *   device (cudaGetSymbolAddress, with the device current); make that first
- *   call before any stream capture.
- * - All calls on a device share the one array: calls that overlap on the GPU
- *   (different streams, or other threads) race and must be serialised by the
- *   caller.  Each call clears the status words it uses.
- * - status_out (device pointer to 2 int32 words, or NULL) receives the
- *   non-converged saturation-adjustment cell count and the largest fallout
- *   sub-step count, stream-ordered after the operator.
- * - The call allocates no device memory and calls no allocator.
- */
 /* Held-rate carriers of the equation-set-2 Kessler lifecycle, mass-shaped
  * (Gm1KesslerHeldCarriers, src/cm1core/cuda_gm1_kessler_large_step.py:112). */
 typedef struct gm1b_kessler_held {
@@ -379,6 +381,33 @@ GM1B_API int32_t gm1b_kessler_large_step(int32_t ni, int32_t nj, int32_t nk, con
                                          int32_t equation_set, int32_t efall, void *workspace, size_t workspace_size,
                                          void *stream);
 
+/*
+ * gm1b_kessler_driver without a workspace argument, for callers that cannot
+ * allocate device memory of their own (for instance a Fortran or C host
+ * model bound through this ABI whose device memory belongs to another
+ * runtime's pool, or a process whose device memory another framework
+ * reserves up front): the budget scratch lives in a static device array of
+ * GM1B_KESSLER_STATIC_SCRATCH_BYTES (8 MiB), which every GPU that loads the
+ * library holds until the process exits.  No counterpart in the reference
+ * (its launcher always allocates a workspace).
+ *
+ * - Grids whose scratch exceeds 8 MiB are rejected with GM1B_ERR_ARGUMENT.
+ *   The scratch is gm1b_kessler_workspace_bytes(ni, nj, nk) =
+ *   16 + 8 * (5*ni*nj + 5*nj + 5*nk*nj*ceil(ni/128)) bytes: 4.27 MB at
+ *   256x256x80 and 8.20 MB at 480x256x80 fit; 8.53 MB at 512x256x80 and
+ *   32 MB at 640x768x80 are refused.
+ * - Device ordinals 0..63 are served; a higher ordinal is refused.
+ * - The first call on a device resolves the array's device address for that
+ *   device (cudaGetSymbolAddress, with the device current); make that first
+ *   call before any stream capture.
+ * - All calls on a device share the one array: calls that overlap on the GPU
+ *   (different streams, or other threads) race and must be serialised by the
+ *   caller.  Each call clears the status words it uses.
+ * - status_out (device pointer to 2 int32 words, or NULL) receives the
+ *   non-converged saturation-adjustment cell count and the largest fallout
+ *   sub-step count, stream-ordered after the operator.
+ * - The call allocates no device memory and calls no allocator.
+ */
 #define GM1B_KESSLER_STATIC_SCRATCH_BYTES (8u * 1024u * 1024u)
 GM1B_API int32_t gm1b_kessler_driver_static(int32_t ni, int32_t nj, int32_t nk,
                                             const gm1b_kessler_arrays *arrays, float dx, float dy,
@@ -756,6 +785,22 @@ GM1B_API int32_t gm1b_advective_courant(double dt, double dx, double dy, double 
 GM1B_API int32_t gm1b_courant_max(int32_t ni, int32_t nj, int32_t nk, const float *u, const float *v, const float *w,
                                   const float *uh, const float *vh, const float *mh, float dtdx, float dtdy,
                                   float dtdz, uint32_t *level_keys, float *out, void *stream);
+
+/*
+ * Fold one step's failure words into a device accumulator of 8 int32
+ * (zeroed by the caller once): [0] += Kessler status[0] (cells whose
+ * saturation adjustment did not converge), [1] = max(Kessler status[1])
+ * (fallout sub-steps), [2] += Kessler status[2] (blown-up fall columns),
+ * [3] = the largest *courant (float bits; a NaN is kept), [4] counts the
+ * Courant folds, [5] the Kessler folds.  Either input may be NULL.  One
+ * single-thread launch, stream-ordered, so a captured step folds its words
+ * without a host read; the caller reads acc and refuses as the reference
+ * does after a step (satadj non-convergence,
+ * src/cm1core/cuda_cartesian_finish.py:638-639; Courant >= 1.5 or not
+ * finite, src/cm1core/gm1_runtime.py:518-549).
+ */
+GM1B_API int32_t gm1b_step_status_fold(const int32_t *kessler_status, const float *courant, int32_t *acc,
+                                       void *stream);
 
 /* ------------------------------------------------------------------------
  * Analytic initial state (host, once per run, except the bubble field)

@@ -1,0 +1,140 @@
+"""Weisman-Klemp moist starting states for the oracle composition - TEST
+INFRASTRUCTURE ONLY.
+
+The CPU baseline and the reference arm of the benchmark build their inputs
+here, from the oracle's own restatement of the initial column
+(init_oracle.c: weisman_klemp_column_with_iterations and analytic_shear_u/v,
+rust/cm1-state/src/storm_initialization.rs:194,354,373) and NumPy, so that
+nothing on those paths loads the CUDA library.  The state is the one the
+package's weisman_klemp_initial_state builds for the same arguments, word for
+word (tests/test_oracle_moist_step.py checks it): the isnd = 5 column on the
+mass heights, the quarter-circle hodograph, a cos^2 warm bubble plus seeded
+uniform noise from numpy.random.default_rng(seed), optional cloud and rain
+in the bubble's core, TKE at its floor, flat terrain metrics whose base
+density is the initial moist density's level means.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+from oracle.initial import analytic_shear, wk_column
+
+NUMQ = 3
+QROWS = 6
+NG = 3
+DIAGNOSTIC_NAMES = ("tri_aa", "tri_bb", "tri_cc", "tri_dd", "tri_pivot", "tri_residual")
+DTYPES = {"saturation_mask": np.uint8, "asq": np.float64, "qbudget": np.float64}
+
+
+def terrain_static_shapes(ni: int, nj: int, nk: int) -> dict[str, tuple[int, ...]]:
+    """Terrain/metric arrays of the padded lane (terrain_static_shapes of the
+    reference's src/cm1core/cuda_terrain_open_boundary.py)."""
+    mass, face, plane = (nk, nj, ni), (nk + 1, nj, ni), (nj, ni)
+    return {"terrain_msl": plane, "zh": mass, "zf": face, "mh": mass, "rmh": mass, "mf": face, "rmf": face,
+            "c1": face, "c2": face, "rho0_3d": mass, "rr0": mass, "rf0": face, "rrf0": face, "gz": plane,
+            "rgz": plane, "gzu": (nj, ni + 1), "rgzu": (nj, ni + 1), "gzv": (nj + 1, ni), "rgzv": (nj + 1, ni),
+            "dzdx": plane, "dzdy": plane, "gx": face, "gxu": (nk + 1, nj, ni + 1), "gy": face,
+            "gyv": (nk + 1, nj + 1, ni)}
+
+
+def moist_state_shapes(ni: int, nj: int, nk: int) -> dict[str, tuple[int, ...]]:
+    """Every array of the composed moist state (the package's
+    moist_state_shapes)."""
+    su, sv = (nk + 2, nj + 2 * NG, ni + 1 + 2 * NG), (nk + 2, nj + 1 + 2 * NG, ni + 2 * NG)
+    sw, ss, pr = (nk + 3, nj + 2 * NG, ni + 2 * NG), (nk + 2, nj + 2 * NG, ni + 2 * NG), (nk + 2, nj + 2, ni + 2)
+    mass, face, plane = (nk, nj, ni), (nk + 1, nj, ni), (nj, ni)
+    s: dict[str, tuple[int, ...]] = {}
+    for n in ("ua", "u3d", "uten", "rru"):
+        s[n] = su
+    for n in ("va", "v3d", "vten", "rrv"):
+        s[n] = sv
+    for n in ("wa", "w3d", "wten", "rrw", "fz"):
+        s[n] = sw
+    s["fx"], s["fy"] = su, sv
+    for n in ("ppi", "pp3d", "ppx", "ppd", "piadv", "ppterm", "ppten", "thv", "qk", "pk1", "pk2", "mm", "fpk", "divh",
+              "hadvp", "dum3", "elim_c", "elim_d"):
+        s[n] = pr
+    for n in DIAGNOSTIC_NAMES:
+        s[n] = (1,)
+    s.update(radbcw=(nk + 2, nj + 2 * NG), radbce=(nk + 2, nj + 2 * NG), radbcs=(nk + 2, ni + 2 * NG),
+             radbcn=(nk + 2, ni + 2 * NG), uh=(ni + 2 * NG,), vh=(nj + 2 * NG,), ruf=(ni + 1 + 2 * NG,),
+             rvf=(nj + 1 + 2 * NG,), scalar=ss, dum8=ss, theta_padded=ss, moisture_padded=ss)
+    for n in ("th3d", "tha", "thterm", "divergence", "theta_div", "divx", "pp3d_c", "prs", "rho", "rr", "kessler_rr",
+              "thheld", "qpten", "qtten", "qvten", "qcten", "theta_adv", "advx", "advy", "advz", "candidate",
+              "temperature", "qt", "thv_c", "qvci", "pi0_3d", "th0_3d", "fall_velocity", "ones_mass"):
+        s[n] = mass
+    s["q3d"], s["qa"] = (QROWS, *mass), (QROWS, *mass)
+    s["qheld"], s["moist_adv"] = (NUMQ, *mass), (NUMQ, *mass)
+    s["saturation_mask"] = mass
+    for n in ("rf", "nm", "defv", "defh", "tke3d", "tkea", "tketen", "tk", "grdscl", "rgrdscl", "lenscl", "dissten",
+              "cme", "ce1", "ce2", "csm", "kmh", "kmv", "khh", "khv", "tke_workspace"):
+        s[n] = face
+    s.update(uc=(nk, nj, ni + 1), vc=(nk, nj + 1, ni), wc=face, th0=(nk,), pi0=(nk,), qv0=(nk,), rain=(1, nj, ni),
+             prate=plane, asq=(3,), qbudget=(10,), ruh=(ni,), rvh=(nj,))
+    return s
+
+
+def flat_metrics(ni: int, nj: int, nk: int, dz: float, rho: np.ndarray) -> dict[str, np.ndarray]:
+    """Flat uniform-column metrics: gz = 1, zero slopes, c1 = c2 = 1/2, base
+    density from the initial moist density's level means."""
+    f = np.float32
+    m = {n: np.zeros(s, f) for n, s in terrain_static_shapes(ni, nj, nk).items()}
+    for n in ("mh", "rmh", "mf", "rmf", "gz", "rgz", "gzu", "rgzu", "gzv", "rgzv"):
+        m[n][:] = f(1.0)
+    m["c1"][:], m["c2"][:] = f(0.5), f(0.5)
+    m["zh"][:] = ((np.arange(nk) + 0.5) * dz).astype(f)[:, None, None]
+    m["zf"][:] = (np.arange(nk + 1) * dz).astype(f)[:, None, None]
+    prof = rho.astype(np.float64).mean(axis=(1, 2)).astype(f)
+    m["rho0_3d"][:] = prof[:, None, None]
+    m["rr0"][:] = (f(1.0) / m["rho0_3d"]).astype(f)
+    rf = np.empty(nk + 1, f)
+    rf[1:nk] = (f(0.5) * prof[:-1] + f(0.5) * prof[1:]).astype(f)
+    rf[0], rf[nk] = prof[0], prof[nk - 1]
+    m["rf0"][:] = rf[:, None, None]
+    m["rrf0"][:] = (f(1.0) / m["rf0"]).astype(f)
+    return m
+
+
+def weisman_klemp_initial_state(cfg, *, seed: int = 0, bubble_k: float = 3.0, noise_k: float = 0.1,
+                                bubble_radius_m: tuple[float, float] = (10000.0, 1400.0),
+                                bubble_center_z_m: float = 1400.0, bubble_cloud: float = 0.0,
+                                bubble_rain: float = 0.0, bubble_offset_m: tuple[float, float] = (0.0, 0.0)):
+    """(state, metrics) of a Weisman-Klemp start on cfg's uniform grid (cfg
+    has ni, nj, nk, dx, dy, dz)."""
+    ni, nj, nk = cfg.ni, cfg.nj, cfg.nk
+    f = np.float32
+    s = {n: np.zeros(sh, dtype=DTYPES.get(n, np.float32)) for n, sh in moist_state_shapes(ni, nj, nk).items()}
+    zh = ((np.arange(nk, dtype=np.float64) + 0.5) * cfg.dz).astype(f)
+    col = wk_column(zh, 1)
+    s["th0"][:], s["pi0"][:], s["qv0"][:] = col["th0"], col["pi0"], col["qv0"]
+    s["th0_3d"][:] = s["th0"][:, None, None]
+    s["pi0_3d"][:] = s["pi0"][:, None, None]
+    s["prs"][:] = col["prs0"][:, None, None]
+    u0, v0 = analytic_shear(zh, zh)
+    s["u3d"][1:nk + 1] = u0[:, None, None]
+    s["v3d"][1:nk + 1] = v0[:, None, None]
+    rng = np.random.default_rng(seed)
+    x = (np.arange(ni) + 0.5) * cfg.dx - 0.5 * ni * cfg.dx - bubble_offset_m[0]
+    y = (np.arange(nj) + 0.5) * cfg.dy - 0.5 * nj * cfg.dy - bubble_offset_m[1]
+    r = np.sqrt((x[None, None, :] / bubble_radius_m[0]) ** 2 + (y[None, :, None] / bubble_radius_m[0]) ** 2 +
+                ((zh.astype(np.float64)[:, None, None] - bubble_center_z_m) / bubble_radius_m[1]) ** 2)
+    bubble = np.where(r < 1.0, bubble_k * np.cos(0.5 * np.pi * r) ** 2, 0.0)
+    s["th3d"][:] = (bubble + rng.uniform(-noise_k, noise_k, (nk, nj, ni))).astype(f)
+    s["q3d"][0] = s["qv0"][:, None, None]
+    s["q3d"][1] = np.where(r < 0.5, bubble_cloud, 0.0).astype(f)
+    s["q3d"][2] = np.where(r < 0.5, bubble_rain, 0.0).astype(f)
+    tv = (s["th0_3d"].astype(np.float64) + s["th3d"]) * s["pi0_3d"] * (1.0 + 0.61 * s["q3d"][0])
+    s["rho"][:] = (col["prs0"][:, None, None] / (287.04 * tv)).astype(f)
+    s["tke3d"][1:nk] = f(1.0e-4)
+    for n in ("uh", "vh", "ruf", "rvf", "ruh", "rvh", "ones_mass"):
+        s[n][:] = f(1.0)
+    m = flat_metrics(ni, nj, nk, cfg.dz, s["rho"])
+    rho = s["rho"]
+    s["rr"][:] = (f(1.0) / rho).astype(f)
+    s["rf"][1:nk] = (m["c1"][1:nk] * rho[:-1] + m["c2"][1:nk] * rho[1:]).astype(f)
+    s["rf"][0], s["rf"][nk] = rho[0], rho[nk - 1]
+    for cur, base in (("ua", "u3d"), ("va", "v3d"), ("wa", "w3d"), ("tha", "th3d"), ("qa", "q3d"), ("tkea", "tke3d"),
+                      ("ppi", "pp3d")):
+        s[cur][:] = s[base]
+    return s, m

@@ -70,3 +70,24 @@ def test_kessler_large_domain_matches_oracle():
     assert_fields_close(want, got)
     assert np.array_equal(got["asq"].view(np.uint64), want["asq"].view(np.uint64))
     assert_budgets_close(want["qbudget"], got["qbudget"])
+
+
+def test_fallout_substeps_are_bounded_on_a_blown_up_column():
+    """A fall Courant number of about 1.5e7 (rain at 1 kg/kg falling through
+    1 m layers over a 1e6 s step) would take int(crmax + 1) sub-steps; the
+    operator counts such columns in its third status word, steps them once
+    and check() refuses.  Every other column keeps its normal sub-steps."""
+    from tests.golden.make_golden import kessler_fixture
+
+    ni, nj, nk = 16, 8, 10
+    inputs = kessler_fixture(ni, nj, nk, 100.0, 5)
+    inputs["qr"][:, 3, 4] = np.float32(1.0)
+    d = {k: torch.from_numpy(np.ascontiguousarray(v)).cuda() for k, v in inputs.items()}
+    nf = torch.zeros((nj, ni), dtype=torch.int32, device="cuda")
+    launch = launch_cuda_gm1_kessler_driver(d, ni=ni, nj=nj, nk=nk, dx=1000.0, dy=1000.0, dz=1.0, dt=1.0e6,
+                                            selection=Gm1KesslerDriverSelection(equation_set=2), nfall=nf)
+    status = launch.status()
+    assert status["blown_up_fall_columns"] >= 1
+    assert int(nf[3, 4]) == 1
+    with pytest.raises(RuntimeError, match="fall Courant"):
+        launch.check()

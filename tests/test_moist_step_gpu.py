@@ -17,7 +17,8 @@ import numpy as np
 import pytest
 import torch
 
-from gm1_b200.moist_step import MoistLargeStep, MoistStepConfig, upload, weisman_klemp_initial_state
+from gm1_b200.moist_step import (CourantStop, MoistLargeStep, MoistStepConfig, SatadjNonConvergence, upload,
+                                 weisman_klemp_initial_state)
 from oracle.moist_composition import OracleMoistStep
 
 pytestmark = pytest.mark.gpu
@@ -108,3 +109,50 @@ def test_concurrent_stage_tail_gives_the_sequential_words():
     torch.cuda.synchronize()
     for n in FIELDS + ("rain", "ppx", "tha", "qa"):
         assert np.array_equal(seq.s[n].cpu().numpy().view(np.uint32), con.s[n].cpu().numpy().view(np.uint32)), n
+
+
+def _cloudy(ni=24, nj=20, nk=16, seed=7):
+    cfg = MoistStepConfig(ni, nj, nk, 1000.0, 1000.0, 250.0, 5.0, 10)
+    host, metrics = weisman_klemp_initial_state(cfg, seed=seed, bubble_radius_m=(6000.0, 1400.0),
+                                                bubble_cloud=1.0e-3, bubble_rain=5.0e-4)
+    return cfg, host, metrics
+
+
+def test_status_words_of_clean_steps():
+    """Two ordinary steps: no failure word set, the Courant number of the
+    state entering each step and of the current state folded (three
+    samples) and finite below CM1's stop, the Kessler words of both steps."""
+    cfg, host, metrics = _cloudy()
+    dev = MoistLargeStep(cfg, upload(host), upload(metrics))
+    dev.step()
+    dev.step()
+    out = dev.check()
+    assert out["satadj_nonconverged_cells"] == 0 and out["blown_up_fall_columns"] == 0
+    assert out["courant_samples"] == 3 and out["kessler_samples"] == 2
+    assert 0.0 < out["max_courant"] < 1.5 and out["max_fall_substeps"] >= 1
+
+
+def test_satadj_nonconvergence_is_refused():
+    """A cloudy cell whose potential temperature is not a number never meets
+    the saturation adjustment's convergence test: after the Kessler
+    transition the step's status counts it and check() refuses, as CM1 stops
+    the run (the microphysics phase alone is run)."""
+    cfg, host, metrics = _cloudy()
+    k, j, i = np.argwhere(host["q3d"][1] > 0)[0]
+    host["th3d"][k, j, i] = np.float32("nan")
+    dev = MoistLargeStep(cfg, upload(host), upload(metrics))
+    dev.microphysics()
+    assert dev.status()["satadj_nonconverged_cells"] >= 1
+    with pytest.raises(SatadjNonConvergence):
+        dev.check(current_state=False)
+
+
+def test_courant_stop_is_refused():
+    """A 400 m/s jet in a few columns gives an advective Courant number of
+    2 at dt = 5 s, dx = 1 km: check() refuses before any step runs."""
+    cfg, host, metrics = _cloudy()
+    host["u3d"][3:8, 8:10, 10:12] = np.float32(400.0)
+    dev = MoistLargeStep(cfg, upload(host), upload(metrics))
+    with pytest.raises(CourantStop):
+        dev.check()
+    assert dev.status()["max_courant"] >= 1.5

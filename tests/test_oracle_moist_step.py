@@ -114,3 +114,24 @@ def test_post_acoustic_on_the_uniform_terrain_column_is_the_uniform_operator():
     om.post_acoustic_flux_column(b, col, ni=ni, nj=nj, nk=nk, dx=400.0, dy=350.0)
     for n in ("rru", "rrv", "rrw", "divergence", "theta_divergence_term", "divx"):
         assert np.array_equal(a[n].view(np.uint32), b[n].view(np.uint32)), n
+
+
+def test_oracle_initial_state_is_the_package_state_word_for_word():
+    """The benchmark's CPU baseline and reference arm build their inputs with
+    oracle.moist_initial (no CUDA library on that path); it must give the
+    package's starting state and metrics word for word (the package's
+    column is host code in the library, so this runs without a GPU)."""
+    from gm1_b200.moist_step import MoistStepConfig, weisman_klemp_initial_state
+    from oracle.moist_initial import weisman_klemp_initial_state as oracle_state
+
+    cfg = MoistStepConfig(20, 14, 12, 1000.0, 1000.0, 250.0, 5.0, 10)
+    kw = dict(seed=2, bubble_k=3.0, noise_k=0.1, bubble_radius_m=(6000.0, 1500.0), bubble_center_z_m=1500.0,
+              bubble_cloud=1.0e-3, bubble_rain=5.0e-4)
+    hs, hm = weisman_klemp_initial_state(cfg, **kw)
+    os_, om_ = oracle_state(cfg, **kw)
+    assert sorted(hs) == sorted(os_) and sorted(hm) == sorted(om_)
+    for n in hs:
+        assert hs[n].dtype == os_[n].dtype and hs[n].shape == os_[n].shape, n
+        assert np.array_equal(hs[n].view(np.uint8), os_[n].view(np.uint8)), n
+    for n in hm:
+        assert np.array_equal(hm[n].view(np.uint8), om_[n].view(np.uint8)), n

@@ -13,6 +13,7 @@ import torch
 from gm1_b200.arrays import ALL_ARRAY_NAMES, SCRATCH_OUTPUT_NAMES, SOUND_ARRAY_NAMES, TRAJECTORY_STATE_NAMES
 from gm1_b200.initial_state import DRY_BUBBLE_64, dry_periodic_state
 from gm1_b200.periodic import (
+    BarrierTimeout,
     TrajectoryAblations,
     launch_cuda_psolver3_trajectory,
     launch_cuda_sound3_periodic_three_stage,
@@ -202,3 +203,24 @@ def test_launch_rejects_bad_device_arrays():
     bad["tha"] = dev["th3d"]
     with pytest.raises(ValueError, match="alias"):
         launch_cuda_psolver3_trajectory(bad, **_c1_params(1))
+
+
+def test_persistent_stage_barrier_timeout_is_reported_and_context_survives():
+    """The persistent acoustic stage's grid barrier waits at most
+    barrier_spin_limit polls.  With a limit of one poll the CTAs that reach a
+    barrier first give up before the rest arrive: the kernel returns, the
+    status word reports it and the launcher raises.  The context stays
+    usable: the same trajectory with the default limit afterwards matches the
+    oracle word for word."""
+    p = _c1_params(1)
+    dev = to_device(dry_periodic_state(DRY_BUBBLE_64))
+    with pytest.raises(BarrierTimeout):
+        launch_cuda_psolver3_trajectory(dev, scratch_outputs=False, barrier_spin_limit=1, **p)
+    host = dry_periodic_state(DRY_BUBBLE_64)
+    dev = to_device(host)
+    launch = launch_cuda_psolver3_trajectory(dev, scratch_outputs=False, **p)
+    assert int(launch.barrier_status.item()) == 0
+    orc.traj_steps(host, **p)
+    got = to_host(dev)
+    names = [n for n in ALL_ARRAY_NAMES if n not in SCRATCH_OUTPUT_NAMES]
+    assert bit_mismatches(host, got, names) == {}

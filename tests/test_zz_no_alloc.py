@@ -7,9 +7,10 @@ up front) and so cannot hand gm1b_kessler_driver a workspace.  Its scratch is
 a static device array shared by every call on a device.
 
 The test drives both entry points through the C ABI on the same inputs for
-two calls in a row (the second call starting from the first call's output)
-and requires the static one to match the workspace one within the Kessler
-tolerances used everywhere else, including the status words; it also checks
+two calls in a row (the second call starting from the first call's output).
+Both run the same kernels in the same order on the same inputs, only with the
+scratch at another address, so the static one must give the workspace one's
+words exactly: every field, the budgets and the status words.  It also checks
 that a grid too large for the static array is refused with a clear error.
 This file is collected last so a failure here never hides another test.
 """
@@ -24,7 +25,6 @@ import torch
 
 from gm1_b200.kessler import _bind, _KesslerArrays, create_cuda_gm1_kessler_driver_workspace
 from tests.golden.make_golden import kessler_fixture
-from tests.kessler_common import assert_budgets_close, assert_fields_close
 
 pytestmark = pytest.mark.gpu
 
@@ -70,9 +70,9 @@ def test_static_scratch_entry_matches_workspace_entry_on_two_calls():
         torch.cuda.synchronize()
         want = {k: v.cpu().numpy() for k, v in with_ws.items()}
         got = {k: v.cpu().numpy() for k, v in static.items()}
-        assert_fields_close(want, got)
-        assert np.array_equal(want["asq"].view(np.uint64), got["asq"].view(np.uint64)), call
-        assert_budgets_close(want["qbudget"], got["qbudget"])
+        for name in want:
+            w, g = want[name], got[name]
+            assert np.array_equal(w.view(np.uint8), g.view(np.uint8)), (call, name)
         assert status.cpu().tolist() == ws.status.cpu().tolist()[:2], call
 
 
