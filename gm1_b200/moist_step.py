@@ -494,9 +494,7 @@ class MoistLargeStep:
             self._interior_pp3d_to_compact()
         self.kessler.stream = st
         self.kessler.apply()
-        _native.check(_native.lib().gm1b_step_status_fold(
-            ctypes.c_void_p(self.kessler.workspace.status.data_ptr()), None,
-            ctypes.c_void_p(self.status_acc.data_ptr()), ctypes.c_void_p(st.cuda_stream)), "gm1b_step_status_fold")
+        self.fold_kessler_status(st)
         with torch.cuda.stream(st):
             self._compact_pp3d_to_interior()
 
@@ -520,6 +518,15 @@ class MoistLargeStep:
         _native.check(_native.lib().gm1b_step_status_fold(
             None, ctypes.c_void_p(self._courant.data_ptr()), ctypes.c_void_p(self.status_acc.data_ptr()),
             ctypes.c_void_p(st.cuda_stream)), "gm1b_step_status_fold")
+
+    def fold_kessler_status(self, stream: Any | None = None) -> None:
+        """Fold the Kessler operator's status words (those of its last run
+        in the step's workspace) into status_acc; microphysics() calls it
+        after the transition."""
+        st = self._st() if stream is None else stream
+        _native.check(_native.lib().gm1b_step_status_fold(
+            ctypes.c_void_p(self.kessler.workspace.status.data_ptr()), None,
+            ctypes.c_void_p(self.status_acc.data_ptr()), ctypes.c_void_p(st.cuda_stream)), "gm1b_step_status_fold")
 
     def status(self) -> dict[str, Any]:
         """Waits for the enqueued work and reads the folded failure words of

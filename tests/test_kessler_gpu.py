@@ -91,3 +91,51 @@ def test_fallout_substeps_are_bounded_on_a_blown_up_column():
     assert int(nf[3, 4]) == 1
     with pytest.raises(RuntimeError, match="fall Courant"):
         launch.check()
+
+
+def nonconvergent_fixture(ni, nj, nk, seed=0):
+    """Kessler driver inputs with one cell the saturation adjustment cannot
+    settle within its 100 passes: 27.5 % vapour and some cloud at 270 K and
+    Exner 0.964 (about 880 hPa), whose given density is the dry density of
+    that pressure and temperature.  The driver takes rho and prs as inputs,
+    so the state is admissible; the iteration's pressure then disagrees with
+    its saturation pressure.  Mixing ratios from 0.265 to 0.285 all run to
+    the bound in the oracle, so the cell does not sit on a knife edge."""
+    from tests.golden.make_golden import kessler_fixture
+
+    a = kessler_fixture(ni, nj, nk, 100.0, seed)
+    k, j, i = 1, nj // 2, ni // 2
+    t, pi = 270.0, 0.96388626
+    a["qr"][:, j, i] = np.float32(0.0)
+    a["pp3d"][k, j, i] = np.float32(pi - a["pi0"][k, j, i])
+    a["th3d"][k, j, i] = np.float32(t / pi - a["th0"][k, j, i])
+    prs = 1.0e5 * np.float64(pi) ** (1005.7 / 287.04)
+    a["prs"][k, j, i] = np.float32(prs)
+    a["rho"][k, j, i] = np.float32(prs / (287.04 * t))
+    a["qv"][k, j, i] = np.float32(0.275)
+    a["qc"][k, j, i] = np.float32(6.0e-3)
+    return a, (k, j, i)
+
+
+def test_satadj_nonconvergence_is_counted_like_the_oracle():
+    """The non-converging cell takes the full 100 passes on the GPU as in the
+    oracle, the status word counts it and check() refuses it as the
+    reference does."""
+    ni, nj, nk = 8, 8, 4
+    a, cell = nonconvergent_fixture(ni, nj, nk)
+    it_want = np.zeros((nk, nj, ni), np.uint32)
+    want = {k: v.copy() for k, v in a.items()}
+    with pytest.raises(RuntimeError, match="converge"):
+        ko.kessler_driver(want, ni=ni, nj=nj, nk=nk, dx=1000.0, dy=1000.0, dz=100.0, dt=5.0, eqtset=2,
+                          iterations=it_want)
+    d = {k: torch.from_numpy(np.ascontiguousarray(v)).cuda() for k, v in a.items()}
+    it = torch.zeros((nk, nj, ni), dtype=torch.int32, device="cuda")
+    launch = launch_cuda_gm1_kessler_driver(d, ni=ni, nj=nj, nk=nk, dx=1000.0, dy=1000.0, dz=100.0, dt=5.0,
+                                            selection=Gm1KesslerDriverSelection(equation_set=2),
+                                            satadj_iterations=it)
+    status = launch.status()
+    got = it.cpu().numpy().view(np.uint32)
+    assert got[cell] == 100 and it_want[cell] == 100
+    assert status["satadj_nonconverged_cells"] == int(np.count_nonzero(it_want >= 100))
+    with pytest.raises(RuntimeError, match="converge"):
+        launch.check()

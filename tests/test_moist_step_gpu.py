@@ -133,15 +133,24 @@ def test_status_words_of_clean_steps():
 
 
 def test_satadj_nonconvergence_is_refused():
-    """A cloudy cell whose potential temperature is not a number never meets
-    the saturation adjustment's convergence test: after the Kessler
-    transition the step's status counts it and check() refuses, as CM1 stops
-    the run (the microphysics phase alone is run)."""
+    """The step's refusal of a saturation adjustment that ran out of
+    iterations: the Kessler operator is run into the step's own workspace
+    on a state with a non-converging cell (tests/test_kessler_gpu.py), its
+    status words are folded as the step folds them after its Kessler
+    transition, and check() refuses as CM1 stops the run.  (Within a step
+    the transition recomputes the density from the state's own pressure,
+    and no finite state found so far defeats the iteration there.)"""
+    from gm1_b200.kessler import Gm1KesslerDriverSelection, launch_cuda_gm1_kessler_driver
+    from tests.test_kessler_gpu import nonconvergent_fixture
+
     cfg, host, metrics = _cloudy()
-    k, j, i = np.argwhere(host["q3d"][1] > 0)[0]
-    host["th3d"][k, j, i] = np.float32("nan")
     dev = MoistLargeStep(cfg, upload(host), upload(metrics))
-    dev.microphysics()
+    a, _ = nonconvergent_fixture(cfg.ni, cfg.nj, cfg.nk)
+    d = {k: torch.from_numpy(np.ascontiguousarray(v)).cuda() for k, v in a.items()}
+    launch_cuda_gm1_kessler_driver(d, ni=cfg.ni, nj=cfg.nj, nk=cfg.nk, dx=1000.0, dy=1000.0, dz=100.0, dt=5.0,
+                                   selection=Gm1KesslerDriverSelection(equation_set=2),
+                                   workspace=dev.kessler.workspace)
+    dev.fold_kessler_status()
     assert dev.status()["satadj_nonconverged_cells"] >= 1
     with pytest.raises(SatadjNonConvergence):
         dev.check(current_state=False)
