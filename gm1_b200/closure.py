@@ -123,6 +123,54 @@ def launch_cuda_terrain_deformation(
                            "boundary_face_zero_words": 2 * ni * nj})
 
 
+# -------------------------------------------------- calcdef, flat column
+
+FLAT_DEFORMATION_ARRAY_NAMES = ("u3d", "v3d", "w3d", "rho", "rf", "mf", "c1", "c2", "defv", "defh")
+
+
+class _FlatDefArrays(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_void_p) for n in ("u3d", "v3d", "w3d", "rho", "rf", "mf", "c1", "c2", "mh_profile",
+                                               "defv", "defh")]
+
+
+def flat_deformation_shapes(ni: int, nj: int, nk: int) -> dict[str, tuple[int, ...]]:
+    _grid(ni, nj, nk)
+    cell, face = (nk, nj, ni), (nk + 1, nj, ni)
+    return {"u3d": (nk, nj, ni + 1), "v3d": (nk, nj + 1, ni), "w3d": face, "rho": cell, "rf": face, "mf": face,
+            "c1": face, "c2": face, "defv": face, "defh": face, "mh_profile": (nk + 2,)}
+
+
+def launch_cuda_flat_deformation(arrays: Mapping[str, Any], *, mh_profile: Any, ni: int, nj: int, nk: int, dx: float,
+                                 dy: float, rdz: float, stream: Any | None = None) -> CudaLaunch:
+    """calcdef on a flat (terrain_flag=.false.) stretched column
+    (enqueue_flat_calcdef, src/cm1core/cuda_gm1_flat_stretched_closure.py:524,
+    with the zero fill of defv/defh of cuda_cartesian_closure.py:1130-1131):
+    the strains with rdz*mh(k) (``mh_profile``, nk+2 words, CM1-indexed) and
+    rdz*mf(k) (the 3-D face ``mf``), the deformation reduction into defv and
+    defh.  ``rdz`` is the vertical coordinate's reference 1/dz."""
+    shapes = flat_deformation_shapes(ni, nj, nk)
+    dx, dy, rdz = _positive("dx", dx), _positive("dy", dy), _positive("rdz", rdz)
+    a = _require({**arrays, "mh_profile": mh_profile}, FLAT_DEFORMATION_ARRAY_NAMES + ("mh_profile",), shapes,
+                 "flat-deformation")
+    s = _FlatDefArrays(**{f: a[f].data_ptr() for f, _ in _FlatDefArrays._fields_})
+    lib = _native.lib()
+    if not getattr(lib, "_flatdef_bound", False):
+        i32, f32 = ctypes.c_int32, ctypes.c_float
+        lib.gm1b_flat_deformation.argtypes = [i32, i32, i32, ctypes.POINTER(_FlatDefArrays), f32, f32, f32,
+                                              ctypes.c_void_p]
+        lib.gm1b_flat_deformation.restype = i32
+        lib._flatdef_bound = True
+    device = a["defv"].device
+    st = torch.cuda.current_stream(device) if stream is None else stream
+    with torch.cuda.device(device):
+        _native.check(lib.gm1b_flat_deformation(ni, nj, nk, ctypes.byref(s), dx, dy, rdz,
+                                                ctypes.c_void_p(st.cuda_stream)), "gm1b_flat_deformation")
+        ev = torch.cuda.Event()
+        ev.record(st)
+    return CudaLaunch(ev, {"operator": "flat-calcdef", "live_words": ni * nj * (nk - 1),
+                           "boundary_face_zero_words": 2 * ni * nj})
+
+
 # ------------------------------------------------------------------- calcnm
 
 NM_INPUT_NAMES = ("c1", "c2", "mf", "pi0", "th0", "prs", "pp3d", "th3d", "q3d")

@@ -5,6 +5,7 @@
 //
 // Behaviour followed (reference file:line):
 //   cpu_terrain_deformation_inplace   src/cm1core/cuda_terrain_deformation.py:234-736
+//   enqueue_flat_calcdef (flat column) src/cm1core/cuda_gm1_flat_stretched_closure.py:524-553, texts :76-136
 //   cpu_moist_nm_inplace              src/cm1core/cuda_moist_nm.py:292-396
 //
 // Design (B200):
@@ -33,9 +34,11 @@ constexpr int kDX = 32, kDY = 8;  // calcdef tile
 
 struct DefArgs {
     const float *u, *v, *w, *rho, *rf, *c1, *c2, *gz, *rgz, *rgzu, *rgzv, *gx, *gy;
+    const float *mf3, *mhp;  // flat column: face mf (nk+1, nj, ni) and the mh profile (nk+2, CM1-indexed)
     float *defv, *defh;
     int ni, nj, nk;
     float rdx, rdy, rds, zt, dz;
+    float rdz;  // flat column: the vertical coordinate's reference 1/dz
 };
 
 // 32-bit element offsets (the entry points refuse grids whose arrays reach
@@ -146,9 +149,77 @@ __device__ __forceinline__ float strain_s23(const DefArgs &p, int kf, int jc, in
     return strain * density;
 }
 
+// ---- flat column (terrain_flag=.false.) strains: rdz*mh(k) / rdz*mf(k)
+// (gm1_flat_calcdef_mass_v1 / _face_v1, src/cm1core/cuda_gm1_flat_stretched_closure.py:76-112;
+// turb.F:4772-4786, :4880-4895)
+
+// s11, s22, s33 at mass level k, cell (j, i)
+__device__ __forceinline__ void strain_diag_flat(const DefArgs &p, int k, int j, int i, float &s11, float &s22,
+                                                 float &s33) {
+    const int ni = p.ni, nj = p.nj, ux = ni + 1, vy = nj + 1;
+    const unsigned c = i3(k, j, i, nj, ni);
+    const float r = p.rho[c];
+    s11 = (r * (p.u[i3(k, j, i + 1, nj, ux)] - p.u[i3(k, j, i, nj, ux)])) * p.rdx;
+    s22 = (r * (p.v[i3(k, j + 1, i, vy, ni)] - p.v[i3(k, j, i, vy, ni)])) * p.rdy;
+    s33 = (r * (p.w[i3(k + 1, j, i, nj, ni)] - p.w[c])) * (p.rdz * p.mhp[k + 1]);
+}
+
+// s12 at mass level k, corner (jc, ic); open sides take the nearest interior corner
+__device__ __forceinline__ float strain_s12_flat(const DefArgs &p, int k, int jc, int ic) {
+    const int ni = p.ni, nj = p.nj, ux = ni + 1, vy = nj + 1;
+    const int jj = jc < 1 ? 1 : (jc > nj - 1 ? nj - 1 : jc);
+    const int ii = ic < 1 ? 1 : (ic > ni - 1 ? ni - 1 : ic);
+    const float x = (p.u[i3(k, jj, ii, nj, ux)] - p.u[i3(k, jj - 1, ii, nj, ux)]) * p.rdy;
+    const float y = (p.v[i3(k, jj, ii, vy, ni)] - p.v[i3(k, jj, ii - 1, vy, ni)]) * p.rdx;
+    const float rs = (p.rho[i3(k, jj - 1, ii - 1, nj, ni)] + p.rho[i3(k, jj, ii, nj, ni)]) +
+                     (p.rho[i3(k, jj, ii - 1, nj, ni)] + p.rho[i3(k, jj - 1, ii, nj, ni)]);
+    return ((0.5f * (x + y)) * 0.25f) * rs;
+}
+
+// s13 at face level kf (1..nk-1), row j, u-face column ic in [0, ni]
+__device__ __forceinline__ float strain_s13_flat(const DefArgs &p, int kf, int j, int ic) {
+    const int ni = p.ni, nj = p.nj, ux = ni + 1;
+    const int il = ic - 1 < 0 ? 0 : ic - 1, ir = ic < ni - 1 ? ic : ni - 1;
+    const float dw = (p.w[i3(kf, j, ir, nj, ni)] - p.w[i3(kf, j, il, nj, ni)]) * p.rdx;
+    const float du = (((p.u[i3(kf, j, ic, nj, ux)] - p.u[i3(kf - 1, j, ic, nj, ux)]) * p.rdz) * 0.5f) *
+                     (p.mf3[i3(kf, j, il, nj, ni)] + p.mf3[i3(kf, j, ir, nj, ni)]);
+    return ((0.5f * (dw + du)) * 0.5f) * (p.rf[i3(kf, j, il, nj, ni)] + p.rf[i3(kf, j, ir, nj, ni)]);
+}
+
+// s23 at face level kf (1..nk-1), v-face row jc in [0, nj], column i
+__device__ __forceinline__ float strain_s23_flat(const DefArgs &p, int kf, int jc, int i) {
+    const int ni = p.ni, nj = p.nj, vy = nj + 1;
+    const int js = jc - 1 < 0 ? 0 : jc - 1, jn = jc < nj - 1 ? jc : nj - 1;
+    const float dw = (p.w[i3(kf, jn, i, nj, ni)] - p.w[i3(kf, js, i, nj, ni)]) * p.rdy;
+    const float dv = (((p.v[i3(kf, jc, i, vy, ni)] - p.v[i3(kf - 1, jc, i, vy, ni)]) * p.rdz) * 0.5f) *
+                     (p.mf3[i3(kf, js, i, nj, ni)] + p.mf3[i3(kf, jn, i, nj, ni)]);
+    return ((0.5f * (dw + dv)) * 0.5f) * (p.rf[i3(kf, js, i, nj, ni)] + p.rf[i3(kf, jn, i, nj, ni)]);
+}
+
+template <bool FLAT>
+__device__ __forceinline__ void strain_diag_t(const DefArgs &p, int k, int j, int i, float &a, float &b, float &c) {
+    if (FLAT) strain_diag_flat(p, k, j, i, a, b, c);
+    else strain_diag(p, k, j, i, a, b, c);
+}
+template <bool FLAT>
+__device__ __forceinline__ float strain_s12_t(const DefArgs &p, int k, int jc, int ic) {
+    return FLAT ? strain_s12_flat(p, k, jc, ic) : strain_s12(p, k, jc, ic);
+}
+template <bool FLAT>
+__device__ __forceinline__ float strain_s13_t(const DefArgs &p, int kf, int j, int ic) {
+    return FLAT ? strain_s13_flat(p, kf, j, ic) : strain_s13(p, kf, j, ic);
+}
+template <bool FLAT>
+__device__ __forceinline__ float strain_s23_t(const DefArgs &p, int kf, int jc, int i) {
+    return FLAT ? strain_s23_flat(p, kf, jc, i) : strain_s23(p, kf, jc, i);
+}
+
 __device__ __forceinline__ float sq(float x) { return x * x; }
 
-// One CTA = a 32 x 8 tile of columns, walking face levels 1..nk-1.
+// One CTA = a 32 x 8 tile of columns, walking face levels 1..nk-1; FLAT
+// selects the flat column's strain texts (the deformation reduction of
+// turb.F:5361-5385 is the same in both branches).
+template <bool FLAT>
 __global__ void __launch_bounds__(kDX *kDY) calcdef_tile_kernel(DefArgs p) {
     __shared__ float s12[2][kDY + 1][kDX + 1];
     __shared__ float s13[kDY][kDX + 1];
@@ -161,26 +232,26 @@ __global__ void __launch_bounds__(kDX *kDY) calcdef_tile_kernel(DefArgs p) {
     constexpr int kCorners = (kDY + 1) * (kDX + 1), kXFaces = kDY * (kDX + 1), kYFaces = (kDY + 1) * kDX;
 
     float p11 = 0.0f, p22 = 0.0f, p33 = 0.0f;  // mass level kf-1 at the own cell
-    if (own) strain_diag(p, 0, j, i, p11, p22, p33);
+    if (own) strain_diag_t<FLAT>(p, 0, j, i, p11, p22, p33);
     for (int e = tid; e < kCorners; e += kDX * kDY) {
         const int r = e / (kDX + 1), q = e - r * (kDX + 1);
-        if (j0 + r <= nj && i0 + q <= ni) s12[0][r][q] = strain_s12(p, 0, j0 + r, i0 + q);
+        if (j0 + r <= nj && i0 + q <= ni) s12[0][r][q] = strain_s12_t<FLAT>(p, 0, j0 + r, i0 + q);
     }
     for (int kf = 1; kf < nk; ++kf) {
         const int cur = kf & 1;
         float c11 = 0.0f, c22 = 0.0f, c33 = 0.0f;
-        if (own) strain_diag(p, kf, j, i, c11, c22, c33);
+        if (own) strain_diag_t<FLAT>(p, kf, j, i, c11, c22, c33);
         for (int e = tid; e < kCorners; e += kDX * kDY) {
             const int r = e / (kDX + 1), q = e - r * (kDX + 1);
-            if (j0 + r <= nj && i0 + q <= ni) s12[cur][r][q] = strain_s12(p, kf, j0 + r, i0 + q);
+            if (j0 + r <= nj && i0 + q <= ni) s12[cur][r][q] = strain_s12_t<FLAT>(p, kf, j0 + r, i0 + q);
         }
         for (int e = tid; e < kXFaces; e += kDX * kDY) {
             const int r = e / (kDX + 1), q = e - r * (kDX + 1);
-            if (j0 + r < nj && i0 + q <= ni) s13[r][q] = strain_s13(p, kf, j0 + r, i0 + q);
+            if (j0 + r < nj && i0 + q <= ni) s13[r][q] = strain_s13_t<FLAT>(p, kf, j0 + r, i0 + q);
         }
         for (int e = tid; e < kYFaces; e += kDX * kDY) {
             const int r = e / kDX, q = e - r * kDX;
-            if (j0 + r <= nj && i0 + q < ni) s23[r][q] = strain_s23(p, kf, j0 + r, i0 + q);
+            if (j0 + r <= nj && i0 + q < ni) s23[r][q] = strain_s23_t<FLAT>(p, kf, j0 + r, i0 + q);
         }
         __syncthreads();
         if (own) {
@@ -446,9 +517,55 @@ extern "C" int32_t gm1b_terrain_deformation(int32_t ni, int32_t nj, int32_t nk,
     p.dz = dz;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     ProfScope ps("calcdef_tile_kernel", st);
-    calcdef_tile_kernel<<<dim3((ni + kDX - 1) / kDX, (nj + kDY - 1) / kDY), dim3(kDX, kDY), 0, st>>>(p);
+    calcdef_tile_kernel<false><<<dim3((ni + kDX - 1) / kDX, (nj + kDY - 1) / kDY), dim3(kDX, kDY), 0, st>>>(p);
     ps.stop();
     return launch_ok("calcdef_tile_kernel") ? GM1B_OK : GM1B_ERR_CUDA;
+}
+
+extern "C" int32_t gm1b_flat_deformation(int32_t ni, int32_t nj, int32_t nk, const gm1b_flat_deformation_arrays *arrays,
+                                         float dx, float dy, float rdz, void *stream) {
+    if (arrays == nullptr || ni < 3 || nj < 3 || nk < 3) {
+        gm1b_set_error("gm1b_flat_deformation: need arrays and ni, nj, nk >= 3");
+        return GM1B_ERR_ARGUMENT;
+    }
+    if (!(dx > 0.0f) || !(dy > 0.0f) || !(rdz > 0.0f) || !isfinite(dx) || !isfinite(dy) || !isfinite(rdz)) {
+        gm1b_set_error("gm1b_flat_deformation: dx, dy, rdz must be finite and > 0");
+        return GM1B_ERR_ARGUMENT;
+    }
+    const gm1b_flat_deformation_arrays &s = *arrays;
+    const void *need[] = {s.u3d, s.v3d, s.w3d, s.rho, s.rf, s.mf, s.c1, s.c2, s.mh_profile, s.defv, s.defh};
+    for (const void *q : need)
+        if (q == nullptr) {
+            gm1b_set_error("gm1b_flat_deformation: a required array is NULL");
+            return GM1B_ERR_ARGUMENT;
+        }
+    if ((size_t)(nk + 3) * (size_t)(nj + 7) * (size_t)(ni + 7) >= ((size_t)1 << 31)) {
+        gm1b_set_error("gm1b_flat_deformation: grid too large (the kernels index with 32-bit offsets)");
+        return GM1B_ERR_ARGUMENT;
+    }
+    DefArgs p{};
+    p.u = s.u3d;
+    p.v = s.v3d;
+    p.w = s.w3d;
+    p.rho = s.rho;
+    p.rf = s.rf;
+    p.c1 = s.c1;
+    p.c2 = s.c2;
+    p.mf3 = s.mf;
+    p.mhp = s.mh_profile;
+    p.defv = s.defv;
+    p.defh = s.defh;
+    p.ni = ni;
+    p.nj = nj;
+    p.nk = nk;
+    p.rdx = 1.0f / dx;
+    p.rdy = 1.0f / dy;
+    p.rdz = rdz;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    ProfScope ps("calcdef_flat_tile_kernel", st);
+    calcdef_tile_kernel<true><<<dim3((ni + kDX - 1) / kDX, (nj + kDY - 1) / kDY), dim3(kDX, kDY), 0, st>>>(p);
+    ps.stop();
+    return launch_ok("calcdef_flat_tile_kernel") ? GM1B_OK : GM1B_ERR_CUDA;
 }
 
 extern "C" int32_t gm1b_moist_nm(int32_t ni, int32_t nj, int32_t nk, const gm1b_moist_nm_arrays *arrays, float dz,

@@ -5,6 +5,9 @@
 // Behaviour followed (reference file:line):
 //   cpu_tke_evolution_inplace   src/cm1core/cuda_tke_evolution.py:206-327
 //   launch_cuda_tke_diffusion / _rk_stage / _commit / _evolution   :421-492
+//   flat column: gm1_flat_turbt_v1 and gm1_flat_tke_advw_rk_v1
+//               src/cm1core/cuda_gm1_flat_stretched_closure.py:314-359, :401-449
+//               (enqueue_flat_turbt :631; CartesianClosure.tke_rk, cuda_cartesian_closure.py:1658-1663)
 //
 // Design (B200):
 //  * turbt is one kernel per 32 x 4 column tile.  Each thread first solves
@@ -32,9 +35,10 @@ constexpr int kG = 3;                                    // padded-lane halo of 
 struct TkeArgs {
     const float *t, *kmh, *kmv, *rho, *rf, *mh, *mf, *gz, *rgz, *rgzu, *rgzv;
     const float *tkea, *c2, *rrf0, *rru, *rrv, *rrw, *divx;
+    const float *mfp;  // flat column: the mf profile (nk+3, CM1-indexed)
     float *tketen;
     int ni, nj, nk;
-    float rdx, rdy, rdz, dz, zt;
+    float rdx, rdy, rdz, dz, zt;  // flat column: rdz is the coordinate's reference 1/dz
 };
 
 __device__ __forceinline__ int clampi(int x, int n) { return x < 0 ? 0 : (x >= n ? n - 1 : x); }
@@ -239,6 +243,124 @@ __global__ void __launch_bounds__(kTT) tke_turbt_kernel(TkeArgs a, float dt) {
 #undef DP
 }
 
+// ------------------------------------------------- turbt, flat column
+// gm1_flat_turbt_v1 (src/cm1core/cuda_gm1_flat_stretched_closure.py:314-359;
+// turbtend.F:729-1044 with terrain_flag=.false.): the x/y face fluxes
+// -0.25*(rf(a)+rf(a-1))*2*(kmh(a)+kmh(a-1))*(t(a)-t(a-1))*rdx, no terrain
+// correction, and the implicit diffusion with rdz and the 3-D mh/mf.  One
+// CTA per 32 x 4 column tile: the own column's Thomas in shared memory, then
+// per face level the tile's face fluxes (each formed once) in shared memory.
+
+// x face flux at face level f, row j, between cells face-1 and face
+__device__ __forceinline__ float tke_tx_flat(const TkeArgs &a, int f, int j, int face) {
+    const float rs = cellc(a, a.rf, f, j, face) + cellc(a, a.rf, f, j, face - 1);
+    const float ks = cellc(a, a.kmh, f, j, face) + cellc(a, a.kmh, f, j, face - 1);
+    const float dt = cellc(a, a.t, f, j, face) - cellc(a, a.t, f, j, face - 1);
+    return -(((((0.25f * rs) * 2.0f) * ks) * dt) * a.rdx);
+}
+__device__ __forceinline__ float tke_ty_flat(const TkeArgs &a, int f, int face, int i) {
+    const float rs = cellc(a, a.rf, f, face, i) + cellc(a, a.rf, f, face - 1, i);
+    const float ks = cellc(a, a.kmh, f, face, i) + cellc(a, a.kmh, f, face - 1, i);
+    const float dt = cellc(a, a.t, f, face, i) - cellc(a, a.t, f, face - 1, i);
+    return -(((((0.25f * rs) * 2.0f) * ks) * dt) * a.rdy);
+}
+
+__global__ void __launch_bounds__(kTT) tke_turbt_flat_kernel(TkeArgs a, float dt) {
+    extern __shared__ float s_col[];
+    __shared__ float s_tx[kTTY][kTTX + 1];
+    __shared__ float s_ty[kTTY + 1][kTTX];
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kTTX + tx;
+    const int i0 = blockIdx.x * kTTX, j0 = blockIdx.y * kTTY;
+    const int i = i0 + tx, j = j0 + ty;
+    const int ni = a.ni, nj = a.nj, nk = a.nk, n = nk - 1;
+    const bool own = i < ni && j < nj;
+    float *cp = s_col, *dp = s_col + (size_t)n * kTT;
+#define CP(p) cp[(unsigned)(p) * kTT + tid]
+#define DP(p) dp[(unsigned)(p) * kTT + tid]
+    const float rdt = 1.0f / dt;
+    if (own) {
+        const float tema = (((-1.0f * dt) * 1.0f) * a.rdz) * a.rdz;
+        const float temb = ((dt * 0.0f) * a.rdz) * a.rdz;
+        // level f = 1
+        unsigned z = f3(a, 1, j, i);
+        float tprev = a.t[z], tcur = a.t[f3(a, 2, j, i)];
+        float rrf = a.mf[z] / a.rf[z];
+        float kprev = a.kmv[z], kcur = a.kmv[f3(a, 2, j, i)];
+        float r2 = (((kprev + kcur) * a.mh[z]) * a.rho[z]) * rrf;
+        float cfc = tema * r2, cfb = 1.0f - cfc;
+        float cfd = tprev + temb * ((r2 * tcur) - (r2 * tprev));
+        float inv = rcp_rn(cfb);
+        float cprev = -(cfc * inv), dprev = cfd * inv;
+        CP(0) = cprev;
+        DP(0) = dprev;
+        float tm = tprev;  // t(f-1)
+        // levels f = 2 .. nk-2
+        for (int f = 2; f < nk - 1; ++f) {
+            const unsigned zf = f3(a, f, j, i), zm = f3(a, f - 1, j, i);
+            const float tp = a.t[f3(a, f + 1, j, i)];
+            const float knext = a.kmv[f3(a, f + 1, j, i)];
+            rrf = a.mf[zf] / a.rf[zf];
+            const float r1 = (((kprev + kcur) * a.mh[zm]) * a.rho[zm]) * rrf;
+            r2 = (((kcur + knext) * a.mh[zf]) * a.rho[zf]) * rrf;
+            const float cfa = tema * r1;
+            cfc = tema * r2;
+            cfb = (1.0f - cfa) - cfc;
+            const float tf = tcur;
+            cfd = tf + temb * (((r2 * tp) - ((r1 + r2) * tf)) + (r1 * tm));
+            inv = rcp_rn(cfa * cprev + cfb);
+            cprev = -(cfc * inv);
+            dprev = (cfd - cfa * dprev) * inv;
+            CP(f - 1) = cprev;
+            DP(f - 1) = dprev;
+            tm = tf;
+            tcur = tp;
+            kprev = kcur;
+            kcur = knext;
+        }
+        // level f = nk-1
+        {
+            const int f = nk - 1;
+            const unsigned zf = f3(a, f, j, i), zm = f3(a, f - 1, j, i);
+            rrf = a.mf[zf] / a.rf[zf];
+            const float r1 = (((kprev + kcur) * a.mh[zm]) * a.rho[zm]) * rrf;
+            const float cfa = tema * r1;
+            cfb = 1.0f - cfa;
+            const float tf = tcur;
+            cfd = tf + temb * ((-(r1 * tf)) + (r1 * tm));
+            inv = rcp_rn(cfa * cprev + cfb);
+            float sol = (cfd - cfa * dprev) * inv;
+            DP(n - 1) = sol;
+            for (int p = n - 2; p >= 0; --p) {
+                sol = CP(p) * sol + DP(p);
+                DP(p) = sol;
+            }
+        }
+    }
+    constexpr int kXF = kTTY * (kTTX + 1), kYF = (kTTY + 1) * kTTX;
+    for (int f = 1; f < nk; ++f) {
+        for (int e = tid; e < kXF; e += kTT) {
+            const int r = e / (kTTX + 1), q = e - r * (kTTX + 1);
+            if (j0 + r < nj && i0 + q <= ni) s_tx[r][q] = tke_tx_flat(a, f, j0 + r, i0 + q);
+        }
+        for (int e = tid; e < kYF; e += kTT) {
+            const int r = e / kTTX, q = e - r * kTTX;
+            if (j0 + r <= nj && i0 + q < ni) s_ty[r][q] = tke_ty_flat(a, f, j0 + r, i0 + q);
+        }
+        __syncthreads();
+        if (own) {
+            const float hx = (i == 0 || i == ni - 1) ? 0.0f : -((s_tx[ty][tx + 1] - s_tx[ty][tx]) * a.rdx);
+            const float hy = (j == 0 || j == nj - 1) ? 0.0f : -((s_ty[ty + 1][tx] - s_ty[ty][tx]) * a.rdy);
+            const unsigned z = f3(a, f, j, i);
+            const float rfz = a.rf[z];
+            const float tz = (rfz * (DP(f - 1) - a.t[z])) * rdt;
+            a.tketen[z] = a.tketen[z] + ((hx + hy) + tz) / rfz;
+        }
+        __syncthreads();
+    }
+#undef CP
+#undef DP
+}
+
 // ------------------------------------------------------------- RK stage
 __device__ __forceinline__ float rru_at(const TkeArgs &a, int k, int j, int f) {
     return a.rru[((unsigned)k * (unsigned)(a.nj + 2 * kG) + (unsigned)(j + kG)) * (unsigned)(a.ni + 1 + 2 * kG) +
@@ -333,8 +455,13 @@ __device__ float vert_flux(const TkeArgs &a, const float *q, int ks, int j, int 
     return m * r;
 }
 
-// grid: x over i, y over j, z over face level f = 0..nk; nxt2 optional
-template <bool W>
+// grid: x over i, y over j, z over face level f = 0..nk; nxt2 optional.
+// FLAT: the flat column's advw (gm1_flat_tke_advw_rk_v1,
+// src/cm1core/cuda_gm1_flat_stretched_closure.py:401-449; adv.F:3252-3355
+// with terrain_flag=.false.): vertical divergence -(dumz(k)-dumz(k-1))*rdz
+// *mf(k), the column's c1/c2 in the divergence correction and its rrf0, the
+// open-side divergence piece (q*d)*rdx evaluated left to right, no gz.
+template <bool W, bool FLAT>
 __global__ void __launch_bounds__(128) tke_rk_stage_kernel(TkeArgs a, const float *__restrict__ cur,
                                                            float *__restrict__ nxt, float *__restrict__ nxt2,
                                                            float dttmp, double eps) {
@@ -377,17 +504,22 @@ __global__ void __launch_bounds__(128) tke_rk_stage_kernel(TkeArgs a, const floa
     if ((i == 0 && mw >= 0.0f) || (i == ni - 1 && me <= 0.0f)) {
         const float du = c1 * (rru_at(a, f, j, i + 1) - rru_at(a, f, j, i)) +
                          c2 * (rru_at(a, f + 1, j, i + 1) - rru_at(a, f + 1, j, i));
-        ax = ax - q * (du * a.rdx);
+        ax = FLAT ? ax - ((q * du) * a.rdx) : ax - q * (du * a.rdx);
     }
     if ((j == 0 && ms >= 0.0f) || (j == nj - 1 && mn <= 0.0f)) {
         const float dv = c1 * (rrv_at(a, f, j + 1, i) - rrv_at(a, f, j, i)) +
                          c2 * (rrv_at(a, f + 1, j + 1, i) - rrv_at(a, f + 1, j, i));
-        ay = ay - q * (dv * a.rdy);
+        ay = FLAT ? ay - ((q * dv) * a.rdy) : ay - q * (dv * a.rdy);
     }
-    const float az = -1.0f * ((vert_flux<W>(a, cur, f + 1, j, i, eps) - vert_flux<W>(a, cur, f, j, i, eps)) * a.rdz);
+    const float dvf = vert_flux<W>(a, cur, f + 1, j, i, eps) - vert_flux<W>(a, cur, f, j, i, eps);
+    const float az = FLAT ? ((-dvf) * a.rdz) * a.mfp[f + 1] : -1.0f * (dvf * a.rdz);
     float total = (ax + ay) + az;
-    total = total + q * (c2 * a.divx[f3(a, f, j, i)] + c1 * a.divx[f3(a, f - 1, j, i)]);
-    const float wten = a.tketen[z] + total * (a.rrf0[z] * a.gz[(size_t)j * ni + i]);
+    // the divergence correction: the flat text reads the column's c2 here
+    // (the open-side pieces above read the cell's)
+    const float c2d = FLAT ? a.c2[f3(a, f, 0, 0)] : c2, c1d = FLAT ? 1.0f - c2d : c1;
+    total = total + q * (c2d * a.divx[f3(a, f, j, i)] + c1d * a.divx[f3(a, f - 1, j, i)]);
+    const float wten = FLAT ? a.tketen[z] + total * a.rrf0[f3(a, f, 0, 0)]
+                            : a.tketen[z] + total * (a.rrf0[z] * a.gz[(size_t)j * ni + i]);
     const float value = a.tkea[z] + dttmp * wten;
     const float out = value < 1e-10f ? 0.0f : value;
     nxt[z] = out;
@@ -497,11 +629,83 @@ int enqueue_stage(const TkeArgs &a, const float *cur, float *nxt, float *nxt2, i
     const dim3 grid((a.ni + 31) / 32, (a.nj + 3) / 4, a.nk + 1), block(32, 4);
     ProfScope ps("tke_rk_stage_kernel", st);
     if (nrk == 3)
-        tke_rk_stage_kernel<true><<<grid, block, 0, st>>>(a, cur, nxt, nxt2, dttmp, eps);
+        tke_rk_stage_kernel<true, false><<<grid, block, 0, st>>>(a, cur, nxt, nxt2, dttmp, eps);
     else
-        tke_rk_stage_kernel<false><<<grid, block, 0, st>>>(a, cur, nxt, nxt2, dttmp, eps);
+        tke_rk_stage_kernel<false, false><<<grid, block, 0, st>>>(a, cur, nxt, nxt2, dttmp, eps);
     ps.stop();
     return launch_ok("tke_rk_stage_kernel") ? GM1B_OK : GM1B_ERR_CUDA;
+}
+
+int enqueue_stage_flat(const TkeArgs &a, const float *cur, float *nxt, int nrk, float dt, cudaStream_t st) {
+    const float dttmp = dt / (float)(4 - nrk);
+    const double eps = (double)(100.0f * 1e-18f);
+    const dim3 grid((a.ni + 31) / 32, (a.nj + 3) / 4, a.nk + 1), block(32, 4);
+    ProfScope ps("tke_rk_stage_flat_kernel", st);
+    if (nrk == 3)
+        tke_rk_stage_kernel<true, true><<<grid, block, 0, st>>>(a, cur, nxt, nullptr, dttmp, eps);
+    else
+        tke_rk_stage_kernel<false, true><<<grid, block, 0, st>>>(a, cur, nxt, nullptr, dttmp, eps);
+    ps.stop();
+    return launch_ok("tke_rk_stage_flat_kernel") ? GM1B_OK : GM1B_ERR_CUDA;
+}
+
+// Flat column arguments: the arrays the flat turbt and RK stage read.
+int tke_args_flat(int ni, int nj, int nk, const gm1b_tke_evolution_arrays *s, float dx, float dy, float rdz,
+                  float dt, TkeArgs &a, bool stage, const float *mf_profile, const char *what) {
+    if (s == nullptr || ni < 3 || nj < 3 || nk < 6) {
+        gm1b_set_error("%s: need arrays, ni >= 3, nj >= 3, nk >= 6", what);
+        return GM1B_ERR_ARGUMENT;
+    }
+    if ((size_t)(nk + 3) * (size_t)(nj + 7) * (size_t)(ni + 7) >= ((size_t)1 << 31)) {
+        gm1b_set_error("%s: a %dx%dx%d grid's padded arrays reach 2^31 words; the kernels index with 32-bit offsets",
+                       what, ni, nj, nk);
+        return GM1B_ERR_ARGUMENT;
+    }
+    const float v[4] = {dx, dy, rdz, dt};
+    for (float x : v)
+        if (!(x > 0.0f) || !isfinite(x)) {
+            gm1b_set_error("%s: dx, dy, rdz, dt must be finite and > 0", what);
+            return GM1B_ERR_ARGUMENT;
+        }
+    const void *turbt_need[] = {s->tke3d, s->tketen, s->kmh, s->kmv, s->rho, s->rf, s->mh, s->mf};
+    const void *stage_need[] = {s->tkea, s->tketen, s->c2, s->rrf0, s->rru, s->rrv, s->rrw, s->divx, mf_profile};
+    if (stage) {
+        for (const void *q : stage_need)
+            if (q == nullptr) {
+                gm1b_set_error("%s: a required array is NULL", what);
+                return GM1B_ERR_ARGUMENT;
+            }
+    } else {
+        for (const void *q : turbt_need)
+            if (q == nullptr) {
+                gm1b_set_error("%s: a required array is NULL", what);
+                return GM1B_ERR_ARGUMENT;
+            }
+    }
+    a = TkeArgs{};
+    a.t = s->tke3d;
+    a.kmh = s->kmh;
+    a.kmv = s->kmv;
+    a.rho = s->rho;
+    a.rf = s->rf;
+    a.mh = s->mh;
+    a.mf = s->mf;
+    a.tkea = s->tkea;
+    a.c2 = s->c2;
+    a.rrf0 = s->rrf0;
+    a.rru = s->rru;
+    a.rrv = s->rrv;
+    a.rrw = s->rrw;
+    a.divx = s->divx;
+    a.tketen = s->tketen;
+    a.mfp = mf_profile;
+    a.ni = ni;
+    a.nj = nj;
+    a.nk = nk;
+    a.rdx = 1.0f / dx;
+    a.rdy = 1.0f / dy;
+    a.rdz = rdz;
+    return GM1B_OK;
 }
 
 }  // namespace
@@ -512,6 +716,50 @@ extern "C" int32_t gm1b_tke_diffusion(int32_t ni, int32_t nj, int32_t nk, const 
     const int r = tke_args(ni, nj, nk, arrays, dx, dy, dz, dt, a, "gm1b_tke_diffusion");
     if (r != GM1B_OK) return r;
     return enqueue_diffusion(a, dt, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int32_t gm1b_tke_diffusion_flat(int32_t ni, int32_t nj, int32_t nk,
+                                           const gm1b_tke_evolution_arrays *arrays, float dx, float dy, float rdz,
+                                           float dt, void *stream) {
+    TkeArgs a;
+    const int r = tke_args_flat(ni, nj, nk, arrays, dx, dy, rdz, dt, a, false, nullptr, "gm1b_tke_diffusion_flat");
+    if (r != GM1B_OK) return r;
+    const size_t smem = turbt_smem(nk);
+    if (smem > 200 * 1024) {
+        gm1b_set_error("gm1b_tke_diffusion_flat: nk=%d exceeds the column solve's shared memory (nk <= 201)", nk);
+        return GM1B_ERR_ARGUMENT;
+    }
+    static size_t configured[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < 64 && configured[dev] < smem) {
+        const cudaError_t e =
+            cudaFuncSetAttribute(tke_turbt_flat_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            gm1b_set_error("cudaFuncSetAttribute(tke_turbt_flat_kernel): %s", cudaGetErrorString(e));
+            return GM1B_ERR_CUDA;
+        }
+        configured[dev] = 200 * 1024;
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    ProfScope ps("tke_turbt_flat_kernel", st);
+    tke_turbt_flat_kernel<<<dim3((ni + kTTX - 1) / kTTX, (nj + kTTY - 1) / kTTY), dim3(kTTX, kTTY), smem, st>>>(a, dt);
+    ps.stop();
+    return launch_ok("tke_turbt_flat_kernel") ? GM1B_OK : GM1B_ERR_CUDA;
+}
+
+extern "C" int32_t gm1b_tke_rk_stage_flat(int32_t ni, int32_t nj, int32_t nk,
+                                          const gm1b_tke_evolution_arrays *arrays, const float *mf_profile,
+                                          const float *cur, float *nxt, int32_t nrk, float dx, float dy, float rdz,
+                                          float dt, void *stream) {
+    TkeArgs a;
+    const int r = tke_args_flat(ni, nj, nk, arrays, dx, dy, rdz, dt, a, true, mf_profile, "gm1b_tke_rk_stage_flat");
+    if (r != GM1B_OK) return r;
+    if (cur == nullptr || nxt == nullptr || cur == nxt || nrk < 1 || nrk > 3) {
+        gm1b_set_error("gm1b_tke_rk_stage_flat: need distinct cur and nxt and nrk in 1..3");
+        return GM1B_ERR_ARGUMENT;
+    }
+    return enqueue_stage_flat(a, cur, nxt, nrk, dt, static_cast<cudaStream_t>(stream));
 }
 
 extern "C" int32_t gm1b_tke_rk_stage(int32_t ni, int32_t nj, int32_t nk, const gm1b_tke_evolution_arrays *arrays,

@@ -44,8 +44,8 @@ import torch
 
 from . import _native
 from . import moist_ops as mo
-from .advection import launch_cuda_scalar_advection5
-from .closure import launch_cuda_moist_nm, launch_cuda_terrain_deformation
+from .advection import launch_cuda_gm1_child_stretched_scalar_advection5, launch_cuda_scalar_advection5
+from .closure import launch_cuda_flat_deformation, launch_cuda_moist_nm, launch_cuda_terrain_deformation
 from .kessler import (Gm1KesslerDriverSelection, Gm1KesslerHeldCarriers, create_cuda_gm1_kessler_large_step_transition)
 from .limits import CM1_COURANT_STOP, advective_courant_number
 from .moist_bridge import launch_cuda_eqtset2_stage_terms
@@ -55,7 +55,8 @@ from .terrain_open import (ALL_ARRAY_NAMES as TOS_ARRAY_NAMES, COLUMN_DIAGNOSTIC
                            _STRUCT_METRICS as TOS_METRICS, _Arrays as _TosArrays, _Metrics as _TosMetrics,
                            _lib as _tos_lib)
 from .tke import launch_cuda_sgs_tke
-from .tke_evolution import launch_cuda_tke_diffusion, launch_cuda_tke_rk_stage
+from .tke_evolution import (launch_cuda_flat_tke_diffusion, launch_cuda_flat_tke_rk_stage, launch_cuda_tke_diffusion,
+                            launch_cuda_tke_rk_stage)
 
 
 class MoistStepFailure(RuntimeError):
@@ -123,6 +124,26 @@ TAIL_PHASES = frozenset({StepPhase.MOMENTUM_BOUNDARIES, StepPhase.SCALAR_BOUNDAR
 
 
 @dataclass(frozen=True, slots=True)
+class StretchedColumnSpec:
+    """CM1 stretch_z = 1 parameters of a vertically stretched column
+    (param.F:7814-8139 as build_vertical_levels restates it): the physical
+    top, the heights where the stretching starts and ends, and the layer
+    depths below and above; MoistStepConfig.dz is the coordinate's
+    reference dz (rdz = 1/dz)."""
+
+    ztop_m: float
+    str_bot_m: float
+    str_top_m: float
+    dz_bot_m: float
+    dz_top_m: float
+
+
+# The 640x768x80 supercell column: 20 m at the ground to 500 m aloft, lid
+# at 20.8 km, reference dz 100 m.
+SUPERCELL_STRETCHED_COLUMN = StretchedColumnSpec(20800.0, 200.0, 15800.0, 20.0, 500.0)
+
+
+@dataclass(frozen=True, slots=True)
 class MoistStepConfig:
     ni: int
     nj: int
@@ -135,11 +156,29 @@ class MoistStepConfig:
     alph: float = 0.60
     kdiv: float = 0.10
     lateral_sides: tuple[int, int, int, int] = (2, 2, 2, 2)
+    # None: the uniform column (the terrain operator family on flat metrics);
+    # a spec: the flat (terrain_flag=.false.) family on that stretched column
+    column: StretchedColumnSpec | None = None
 
     @property
     def obc(self) -> int:
         w, e, s, n = self.lateral_sides
         return w | (e << 4) | (s << 8) | (n << 12)
+
+    @property
+    def stretched(self) -> bool:
+        return self.column is not None
+
+    def vertical_levels(self):
+        """The CM1 vertical coordinate of the column (stretch_z 1 when a
+        column spec is set, else the uniform coordinate)."""
+        from .vertical import build_vertical_levels, uniform_vertical_levels
+
+        if self.column is None:
+            return uniform_vertical_levels(self.nk, self.dz)
+        c = self.column
+        return build_vertical_levels(stretch_z=1, nk=self.nk, dz_m=self.dz, ztop_m=c.ztop_m, str_bot_m=c.str_bot_m,
+                                     str_top_m=c.str_top_m, dz_bot_m=c.dz_bot_m, dz_top_m=c.dz_top_m)
 
 
 NUMQ = 3  # Kessler: qv, qc, qr
@@ -214,7 +253,9 @@ def weisman_klemp_initial_state(cfg: MoistStepConfig, *, seed: int = 0, bubble_k
     f = np.float32
     shapes = moist_state_shapes(ni, nj, nk)
     s = {n: np.zeros(sh, dtype=MOIST_STATE_DTYPES.get(n, np.float32)) for n, sh in shapes.items()}
-    zh = ((np.arange(nk, dtype=np.float64) + 0.5) * cfg.dz).astype(f)
+    levels = cfg.vertical_levels() if cfg.stretched else None
+    zh = np.asarray(levels.zh[1:nk + 1], f) if levels is not None else \
+        ((np.arange(nk, dtype=np.float64) + 0.5) * cfg.dz).astype(f)
     col = weisman_klemp_column(zh, 1)
     s["th0"][:], s["pi0"][:], s["qv0"][:] = col.theta_k, col.pi, col.qv_kg_per_kg
     s["th0_3d"][:] = s["th0"][:, None, None]
@@ -239,7 +280,7 @@ def weisman_klemp_initial_state(cfg: MoistStepConfig, *, seed: int = 0, bubble_k
     s["tke3d"][1:nk] = f(1.0e-4)
     for n in ("uh", "vh", "ruf", "rvf", "ruh", "rvh", "ones_mass"):
         s[n][:] = f(1.0)
-    m = flat_metrics(cfg, s["rho"])
+    m = flat_metrics(cfg, s["rho"]) if levels is None else stretched_metrics(cfg, levels, s["rho"])
     rho = s["rho"]
     s["rr"][:] = (f(1.0) / rho).astype(f)
     s["rf"][1:nk] = (m["c1"][1:nk] * rho[:-1] + m["c2"][1:nk] * rho[1:]).astype(f)
@@ -272,6 +313,68 @@ def flat_metrics(cfg: MoistStepConfig, rho: np.ndarray) -> dict[str, np.ndarray]
     rf[0], rf[nk] = prof[0], prof[nk - 1]
     m["rf0"][:] = rf[:, None, None]
     m["rrf0"][:] = (f(1.0) / m["rf0"]).astype(f)
+    return m
+
+
+def column_c1_c2(zh: np.ndarray, zf: np.ndarray, nk: int) -> tuple[np.ndarray, np.ndarray]:
+    """Face interpolation weights of a column from its CM1-indexed mass
+    heights zh (nk+2, ghosts at 0 and nk+1) and face heights zf (nk+3):
+    c2(k) = (zf(k) - zh(k-1)) / (zh(k) - zh(k-1)), c1 = 1 - c2, at faces
+    k = 1..nk+1 (the reconstruction of rust/cm1-state/src/child_auxiliary.rs:1043-1050)."""
+    f = np.float32
+    c2 = np.empty(nk + 1, f)
+    for k in range(1, nk + 2):
+        c2[k - 1] = (f(zf[k]) - f(zh[k - 1])) / (f(zh[k]) - f(zh[k - 1]))
+    return (f(1.0) - c2).astype(f), c2
+
+
+def padded_base_density(rho0: np.ndarray) -> np.ndarray:
+    """(nk+2, nj+6, ni+6) base density of the padded lane: the interior
+    rho0_3d, each halo column and row repeating the nearest edge, each ghost
+    level the nearest interior level."""
+    nk, nj, ni = rho0.shape
+    p = np.zeros((nk + 2, nj + 6, ni + 6), np.float32)
+    p[1:nk + 1, 3:nj + 3, 3:ni + 3] = rho0
+    p[1:nk + 1, 3:nj + 3, :3] = rho0[:, :, :1]
+    p[1:nk + 1, 3:nj + 3, ni + 3:] = rho0[:, :, -1:]
+    p[:, :3, :] = p[:, 3:4, :]
+    p[:, nj + 3:, :] = p[:, nj + 2:nj + 3, :]
+    p[0], p[nk + 1] = p[1], p[nk]
+    return p
+
+
+def stretched_metrics(cfg: MoistStepConfig, levels, rho: np.ndarray) -> dict[str, np.ndarray]:
+    """Metrics of a flat stretched column: gz = 1, zero slopes, the
+    generated coordinate's mh/mf/rmh/rmf broadcast over the plane, c1/c2 from
+    its heights, base density from the initial moist density's level means;
+    plus the column profiles the flat operators read (mh_profile nk+2 words,
+    mf_profile nk+3, CM1-indexed) and the padded base density rho0_padded."""
+    from .terrain_open import terrain_static_shapes
+
+    ni, nj, nk = cfg.ni, cfg.nj, cfg.nk
+    f = np.float32
+    m = {n: np.zeros(sh, f) for n, sh in terrain_static_shapes(ni=ni, nj=nj, nk=nk).items()}
+    for n in ("gz", "rgz", "gzu", "rgzu", "gzv", "rgzv"):
+        m[n][:] = f(1.0)
+    mh, mf = np.asarray(levels.mh, f), np.asarray(levels.mf, f)
+    rmh, rmf = np.asarray(levels.rmh, f), np.asarray(levels.rmf, f)
+    m["mh"][:], m["rmh"][:] = mh[1:nk + 1, None, None], rmh[1:nk + 1, None, None]
+    m["mf"][:], m["rmf"][:] = mf[1:nk + 2, None, None], rmf[1:nk + 2, None, None]
+    zh, zf = np.asarray(levels.zh, f), np.asarray(levels.zf, f)
+    c1, c2 = column_c1_c2(zh, zf, nk)
+    m["c1"][:], m["c2"][:] = c1[:, None, None], c2[:, None, None]
+    m["zh"][:] = zh[1:nk + 1, None, None]
+    m["zf"][:] = zf[1:nk + 2, None, None]
+    prof = rho.astype(np.float64).mean(axis=(1, 2)).astype(f)
+    m["rho0_3d"][:] = prof[:, None, None]
+    m["rr0"][:] = (f(1.0) / m["rho0_3d"]).astype(f)
+    rf = np.empty(nk + 1, f)
+    rf[1:nk] = (c1[1:nk] * prof[:-1] + c2[1:nk] * prof[1:]).astype(f)
+    rf[0], rf[nk] = prof[0], prof[nk - 1]
+    m["rf0"][:] = rf[:, None, None]
+    m["rrf0"][:] = (f(1.0) / m["rf0"]).astype(f)
+    m["mh_profile"], m["mf_profile"] = mh.copy(), mf.copy()
+    m["rho0_padded"] = padded_base_density(m["rho0_3d"])
     return m
 
 
@@ -339,13 +442,38 @@ class MoistLargeStep:
              "rain": s["rain"], "prate": s["prate"], "asq": s["asq"], "qbudget": s["qbudget"]},
             **self.grid, dt=cfg.dt, selection=Gm1KesslerDriverSelection(equation_set=2), stream=stream,
             carriers=Gm1KesslerHeldCarriers(s["qpten"], s["qtten"], s["qvten"], s["qcten"]))
-        from .momentum import _Arrays as _MomArrays, _lib as _mom_lib, _STRUCT as _MOM
+        from .momentum import _Arrays as _MomArrays, _Column, _lib as _mom_lib, _STRUCT as _MOM
 
         self._mom_lib = _mom_lib()
         self._mom = _MomArrays(**{n: (s[n] if n in s else m[n]).data_ptr() for n in _MOM})
         self._tos_lib = _tos_lib()
         self._tos = _TosArrays(**{n: s[n].data_ptr() for n in TOS_ARRAY_NAMES})
         self._tos_m = _TosMetrics(**{n: m[n].data_ptr() for n in TOS_METRICS})
+        self.flat = cfg.stretched
+        if self.flat:
+            # the flat (terrain_flag=.false.) family on the stretched column:
+            # the column profiles, the reference rdz, the padded base density
+            from .advection import StretchedColumn
+            from .momentum import StretchedMomentumColumn
+
+            self.rdz = float(np.float32(np.float32(1.0) / np.float32(cfg.dz)))
+            for n, shape in (("mh_profile", (nk + 2,)), ("mf_profile", (nk + 3,)),
+                             ("rho0_padded", (nk + 2, nj + 6, ni + 6))):
+                if n not in m or tuple(m[n].shape) != shape:
+                    raise ValueError(f"a stretched-column step needs metrics[{n!r}] of shape {shape}")
+            self._column = _Column(1, m["rho0_padded"].data_ptr(), None, None, None, None, 0.0,
+                                   m["mh_profile"].data_ptr(), m["mf_profile"].data_ptr(), m["rr0"].data_ptr(),
+                                   self.rdz)
+            self.scalar_column = StretchedColumn(True, mh=m["mh_profile"], rdz=self.rdz)
+            self.post_column = StretchedMomentumColumn(True, m["rho0_padded"], mh=m["mh_profile"], rdz=self.rdz)
+            self.flat_def_arrays = {"u3d": s["uc"], "v3d": s["vc"], "w3d": s["wc"], "rho": s["rho"], "rf": s["rf"],
+                                    "mf": m["mf"], "c1": m["c1"], "c2": m["c2"], "defv": s["defv"],
+                                    "defh": s["defh"]}
+            self.flat_turbt_arrays = {"tke3d": s["tke3d"], "kmh": s["kmh"], "kmv": s["kmv"], "rho": s["rho"],
+                                      "rf": s["rf"], "mh": m["mh"], "mf": m["mf"], "tketen": s["tketen"]}
+            self.flat_stage_arrays = {"tkea": s["tkea"], "tke3d": s["tke3d"], "tketen": s["tketen"], "c2": m["c2"],
+                                      "rrf0": m["rrf0"], "rru": s["rru"], "rrv": s["rrv"], "rrw": s["rrw"],
+                                      "divx": s["divx"]}
         # failure words folded on the device every step (gm1b_step_status_fold)
         self.status_acc = torch.zeros(8, dtype=torch.int32, device=dev)
         self._courant = torch.zeros(1, dtype=torch.float32, device=dev)
@@ -379,11 +507,19 @@ class MoistLargeStep:
             self._interior_pp3d_to_compact()
         self._fold_courant(st)
         launch_cuda_moist_nm(self.nm_arrays, **self.k3, dz=cfg.dz, stream=st)
-        launch_cuda_terrain_deformation(self.def_arrays, **self.grid, stream=st)
+        if self.flat:
+            launch_cuda_flat_deformation(self.flat_def_arrays, mh_profile=self.m["mh_profile"], **self.k3, dx=cfg.dx,
+                                         dy=cfg.dy, rdz=self.rdz, stream=st)
+        else:
+            launch_cuda_terrain_deformation(self.def_arrays, **self.grid, stream=st)
         launch_cuda_sgs_tke(self.sgs_arrays, **self.grid, stream=st)
         with torch.cuda.stream(st):
             s["tke3d"].copy_(s["tkea"])
-        launch_cuda_tke_diffusion(self.tke_arrays, **self.grid, dt=cfg.dt, stream=st)
+        if self.flat:
+            launch_cuda_flat_tke_diffusion(self.flat_turbt_arrays, **self.k3, dx=cfg.dx, dy=cfg.dy, rdz=self.rdz,
+                                           dt=cfg.dt, stream=st)
+        else:
+            launch_cuda_tke_diffusion(self.tke_arrays, **self.grid, dt=cfg.dt, stream=st)
 
     def held_tendencies(self) -> None:
         s, st = self.s, self._st()
@@ -403,6 +539,14 @@ class MoistLargeStep:
             s["uten"].zero_()
             s["vten"].zero_()
             s["wten"].zero_()
+        if self.flat:
+            # solve2.F:484-487 (bcwsfc, bc2d of w(1)) and :575 (bcw(rrw,0)) are
+            # terrain_flag statements: a flat column runs neither
+            _native.check(self._mom_lib.gm1b_momentum_advection5_column(
+                cfg.ni, cfg.nj, cfg.nk, ctypes.byref(self._mom), cfg.obc, cfg.dx, cfg.dy, ctypes.byref(self._column),
+                ctypes.c_void_p(st.cuda_stream)), "gm1b_momentum_advection5_column")
+            mo.moist_buoyancy_flat(s["dum8"], m["c1"], m["c2"], s["wten"], **self.k3, stream=st)
+            return
         if nrk >= 2:
             mo.bcwsfc(s["u3d"], s["v3d"], s["w3d"], m["gz"], m["dzdx"], m["dzdy"], **self.k3, stream=st)
             mo.w_level1_fill(s["w3d"], **self.k3, stream=st)
@@ -417,12 +561,24 @@ class MoistLargeStep:
     def acoustic(self, nrk: int) -> None:
         cfg, st = self.cfg, self._st()
         stage_without_fills = 255 & ~128
+        if self.flat:
+            _native.check(self._tos_lib.gm1b_terrain_open_stage_column(
+                cfg.ni, cfg.nj, cfg.nk, nrk, cfg.dt, cfg.nsound, cfg.dx, cfg.dy, float(np.float32(cfg.alph)),
+                float(np.float32(cfg.kdiv)), stage_without_fills, 0, cfg.obc, ctypes.byref(self._tos),
+                ctypes.byref(self._tos_m), ctypes.byref(self._column), ctypes.c_void_p(st.cuda_stream)),
+                "gm1b_terrain_open_stage_column")
+            return
         _native.check(self._tos_lib.gm1b_terrain_open_stage(
             cfg.ni, cfg.nj, cfg.nk, nrk, cfg.dt, cfg.nsound, cfg.dx, cfg.dy, cfg.dz, float(np.float32(cfg.alph)),
             float(np.float32(cfg.kdiv)), stage_without_fills, 0, ctypes.byref(self._tos), ctypes.byref(self._tos_m),
             ctypes.c_void_p(st.cuda_stream)), "gm1b_terrain_open_stage")
 
     def post_acoustic(self, nrk: int) -> None:
+        if self.flat:
+            cfg = self.cfg
+            mo.post_acoustic_flux_column(self.post_arrays, self.post_column, **self.k3, dx=cfg.dx, dy=cfg.dy,
+                                         stream=self._st())
+            return
         mo.post_acoustic_flux(self.post_arrays, **self.grid, stream=self._st())
 
     def _theta_advection(self, nrk: int, st) -> None:
@@ -433,9 +589,18 @@ class MoistLargeStep:
         mo.open_fill(s["theta_padded"], "scalar", **self.k3, stream=st)
         with torch.cuda.stream(st):
             s["theta_adv"].zero_()
-        launch_cuda_scalar_advection5(s["theta_padded"], flux, met, s["divx"], s["theta_adv"], None,
-                                      weps=theta_weps_f64(), **self.grid, nrk=nrk, stream=st,
-                                      lateral_sides=cfg.lateral_sides, write_fluxes=False)
+        self._advect(s["theta_padded"], flux, met, s["theta_adv"], theta_weps_f64(), nrk, st)
+
+    def _advect(self, padded, flux, met, tendency, weps, nrk: int, st) -> None:
+        s, cfg = self.s, self.cfg
+        if self.flat:
+            launch_cuda_gm1_child_stretched_scalar_advection5(padded, flux, met, s["divx"], tendency, None,
+                                                              self.scalar_column, **self.k3, dx=cfg.dx, dy=cfg.dy,
+                                                              nrk=nrk, weps=weps, stream=st,
+                                                              lateral_sides=cfg.lateral_sides, write_fluxes=False)
+        else:
+            launch_cuda_scalar_advection5(padded, flux, met, s["divx"], tendency, None, weps=weps, **self.grid,
+                                          nrk=nrk, stream=st, lateral_sides=cfg.lateral_sides, write_fluxes=False)
 
     def _species_advection(self, r: int, nrk: int, st) -> None:
         s, m, cfg = self.s, self.m, self.cfg
@@ -446,10 +611,13 @@ class MoistLargeStep:
             s["moist_adv"][r].zero_()
         weps = moisture_weps_f64(r)
         if nrk < 3:
-            launch_cuda_scalar_advection5(padded, {"rru": s["rru"], "rrv": s["rrv"], "rrw": s["rrw"]},
-                                          {"c1": m["c1"], "c2": m["c2"], "rr0": m["rr0"], "gz": m["gz"]},
-                                          s["divx"], s["moist_adv"][r], None, weps=weps, **self.grid, nrk=nrk,
-                                          stream=st, lateral_sides=cfg.lateral_sides, write_fluxes=False)
+            self._advect(padded, {"rru": s["rru"], "rrv": s["rrv"], "rrw": s["rrw"]},
+                         {"c1": m["c1"], "c2": m["c2"], "rr0": m["rr0"], "gz": m["gz"]}, s["moist_adv"][r], weps, nrk,
+                         st)
+        elif self.flat:
+            mo.pdef_moisture_chain_column(self.chain_arrays[r], self.scalar_column, **self.k3, dx=cfg.dx, dy=cfg.dy,
+                                          dttmp=scalar_moist_rk_stage_timestep_f32(cfg.dt, nrk), weps=weps,
+                                          lateral_obc=cfg.obc, pdefweno=0 if r == 0 else 1, stream=st)
         else:
             mo.pdef_moisture_chain(self.chain_arrays[r], **self.grid,
                                    dttmp=scalar_moist_rk_stage_timestep_f32(cfg.dt, nrk), weps=weps,
@@ -479,12 +647,19 @@ class MoistLargeStep:
         mo.open_fill(s["u3d"], "u", **self.k3, stream=st)
         mo.open_fill(s["v3d"], "v", **self.k3, stream=st)
         mo.open_fill(s["w3d"], "w", **self.k3, stream=st)
-        mo.bcwsfc(s["u3d"], s["v3d"], s["w3d"], m["gz"], m["dzdx"], m["dzdy"], **self.k3, stream=st)
+        if not self.flat:  # solve2.F:1676: bcwsfc is a terrain_flag statement
+            mo.bcwsfc(s["u3d"], s["v3d"], s["w3d"], m["gz"], m["dzdx"], m["dzdy"], **self.k3, stream=st)
 
     def scalar_boundaries(self, nrk: int) -> None:
         mo.open_fill(self.s["pp3d"], "pressure", **self.k3, stream=self._st())
 
     def tke_rk(self, nrk: int) -> None:
+        if self.flat:
+            cfg = self.cfg
+            launch_cuda_flat_tke_rk_stage(self.flat_stage_arrays, mf_profile=self.m["mf_profile"],
+                                          workspace=self.s["tke_workspace"], **self.k3, nrk=nrk, dx=cfg.dx,
+                                          dy=cfg.dy, rdz=self.rdz, dt=cfg.dt, stream=self._st())
+            return
         launch_cuda_tke_rk_stage(self.tke_arrays, workspace=self.s["tke_workspace"], **self.grid, nrk=nrk,
                                  dt=self.cfg.dt, stream=self._st())
 

@@ -96,6 +96,10 @@ def _lib():
         lib.gm1b_tke_rk_stage.restype = i32
         lib.gm1b_tke_evolution.argtypes = [i32, i32, i32, pa, vp, f32, f32, f32, f32, vp]
         lib.gm1b_tke_evolution.restype = i32
+        lib.gm1b_tke_diffusion_flat.argtypes = [i32, i32, i32, pa, f32, f32, f32, f32, vp]
+        lib.gm1b_tke_diffusion_flat.restype = i32
+        lib.gm1b_tke_rk_stage_flat.argtypes = [i32, i32, i32, pa, vp, vp, vp, i32, f32, f32, f32, f32, vp]
+        lib.gm1b_tke_rk_stage_flat.restype = i32
         lib._tkeevo_bound = True
     return lib
 
@@ -217,3 +221,83 @@ def launch_cuda_tke_evolution(*args: Any, **kwargs: Any) -> CudaLaunch:
                   "evolved RK trajectory",
            remedy="call launch_cuda_tke_diffusion once, launch_cuda_tke_rk_stage after each nrk getdivx, then "
                   "launch_cuda_tke_commit")
+
+
+# ------------------------------------------------------- flat column family
+
+FLAT_TURBT_NAMES = ("tke3d", "kmh", "kmv", "rho", "rf", "mh", "mf", "tketen")
+FLAT_STAGE_NAMES = ("tkea", "tke3d", "tketen", "c2", "rrf0", "rru", "rrv", "rrw", "divx")
+
+
+def _flat_arrays(arrays: Mapping[str, Any], names, ni: int, nj: int, nk: int) -> dict[str, torch.Tensor]:
+    shapes = tke_evolution_shapes(ni, nj, nk)
+    missing = [n for n in names if n not in arrays]
+    if missing:
+        raise ValueError(f"missing flat TKE arrays: {', '.join(missing)}")
+    out = {}
+    for n in names:
+        t = arrays[n]
+        if not isinstance(t, torch.Tensor) or not t.is_cuda or t.dtype != torch.float32 \
+                or tuple(t.shape) != shapes[n] or not t.is_contiguous():
+            raise ValueError(f"{n} must be a C-order float32 CUDA tensor with shape {shapes[n]}")
+        out[n] = t
+    if len({t.data_ptr() for t in out.values()}) != len(out):
+        raise ValueError("flat TKE arrays must not alias")
+    return out
+
+
+def _flat_struct(a: dict[str, torch.Tensor]) -> _Arrays:
+    return _Arrays(**{n: (a[n].data_ptr() if n in a else None) for n in _STRUCT})
+
+
+def launch_cuda_flat_tke_diffusion(arrays: Mapping[str, Any], *, ni: int, nj: int, nk: int, dx: float, dy: float,
+                                   rdz: float, dt: float, stream: Any | None = None) -> CudaLaunch:
+    """turbt on a flat (terrain_flag=.false.) stretched column
+    (enqueue_flat_turbt, src/cm1core/cuda_gm1_flat_stretched_closure.py:631):
+    the face fluxes without a terrain correction and the implicit diffusion
+    with the coordinate's reference ``rdz`` and the 3-D mh/mf; adds into
+    tketen.  ``arrays``: tke3d, kmh, kmv, rho, rf, mh, mf, tketen."""
+    _validate_grid(ni, nj, nk)
+    dx, dy, rdz, dt = (_spacing(n, v) for n, v in (("dx", dx), ("dy", dy), ("rdz", rdz), ("dt", dt)))
+    a = _flat_arrays(arrays, FLAT_TURBT_NAMES, ni, nj, nk)
+    lib = _lib()
+    device = a["tke3d"].device
+    st = torch.cuda.current_stream(device) if stream is None else stream
+    s = _flat_struct(a)
+    with torch.cuda.device(device):
+        _call(lib.gm1b_tke_diffusion_flat, ni, nj, nk, ctypes.byref(s), dx, dy, rdz, dt,
+              ctypes.c_void_p(st.cuda_stream))
+        ev = torch.cuda.Event()
+        ev.record(st)
+    return CudaLaunch(ev, {"phase": "solve1-turbt-once", "column": "flat"})
+
+
+def launch_cuda_flat_tke_rk_stage(arrays: Mapping[str, Any], *, mf_profile: Any, workspace: Any, ni: int, nj: int,
+                                  nk: int, nrk: int, dx: float, dy: float, rdz: float, dt: float,
+                                  stream: Any | None = None) -> CudaLaunch:
+    """One advw/RK stage on a flat stretched column from tke3d into
+    workspace, then tke3d = workspace (the flat branch of
+    CartesianClosure.tke_rk, src/cm1core/cuda_cartesian_closure.py:1658-1663):
+    vertical divergence with rdz*mf(k) (``mf_profile``, nk+3 words), the
+    column's c2 and rrf0, no gz.  ``arrays``: tkea, tke3d, tketen, c2, rrf0,
+    rru, rrv, rrw, divx."""
+    _validate_grid(ni, nj, nk)
+    if isinstance(nrk, bool) or not isinstance(nrk, int) or nrk not in (1, 2, 3):
+        raise ValueError("nrk must be an integer in 1..3")
+    dx, dy, rdz, dt = (_spacing(n, v) for n, v in (("dx", dx), ("dy", dy), ("rdz", rdz), ("dt", dt)))
+    a = _flat_arrays(arrays, FLAT_STAGE_NAMES, ni, nj, nk)
+    if not isinstance(mf_profile, torch.Tensor) or not mf_profile.is_cuda or mf_profile.dtype != torch.float32 \
+            or tuple(mf_profile.shape) != (nk + 3,) or not mf_profile.is_contiguous():
+        raise ValueError(f"mf_profile must be a C-order float32 CUDA tensor of shape ({nk + 3},)")
+    ws = _workspace(workspace, a, (nk + 1, nj, ni))
+    lib = _lib()
+    device = a["tke3d"].device
+    st = torch.cuda.current_stream(device) if stream is None else stream
+    s = _flat_struct(a)
+    with torch.cuda.device(device), torch.cuda.stream(st):
+        _call(lib.gm1b_tke_rk_stage_flat, ni, nj, nk, ctypes.byref(s), mf_profile.data_ptr(), a["tke3d"].data_ptr(),
+              ws.data_ptr(), nrk, dx, dy, rdz, dt, ctypes.c_void_p(st.cuda_stream))
+        a["tke3d"].copy_(ws)
+        ev = torch.cuda.Event()
+        ev.record(st)
+    return CudaLaunch(ev, {"phase": "solve2-tke-advw-rk-stage", "column": "flat", "nrk": nrk, "uses_weno": nrk == 3})

@@ -701,6 +701,27 @@ GM1B_API int32_t gm1b_tke_rk_stage(int32_t ni, int32_t nj, int32_t nk, const gm1
                                    const float *cur, float *nxt, int32_t nrk, float dx, float dy, float dz, float dt,
                                    void *stream);
 
+/* turbt on a flat (terrain_flag=.false.) stretched column: the face fluxes
+ * -0.25*(rf(a)+rf(a-1))*2*(kmh(a)+kmh(a-1))*(t(a)-t(a-1))*rdx (no terrain
+ * correction; zero divergence on the outermost columns) and the implicit
+ * diffusion with the coordinate's reference rdz and the 3-D mh (mass) and
+ * mf (face), added into tketen.  Reads tke3d, kmh, kmv, rho, rf, mh, mf,
+ * tketen.  Replaces enqueue_flat_turbt
+ * (src/cm1core/cuda_gm1_flat_stretched_closure.py:631).  nk <= 201. */
+GM1B_API int32_t gm1b_tke_diffusion_flat(int32_t ni, int32_t nj, int32_t nk, const gm1b_tke_evolution_arrays *arrays,
+                                         float dx, float dy, float rdz, float dt, void *stream);
+
+/* One RK stage on a flat stretched column: gm1b_tke_rk_stage with the
+ * vertical divergence -(dumz(k)-dumz(k-1))*rdz*mf(k) (mf_profile: nk+3
+ * words, CM1-indexed), the column's c2 and rrf0 (their (k, 0, 0) words),
+ * and the open-side divergence piece (q*d)*rdx.  Reads tkea, tketen, c2,
+ * rrf0, rru, rrv, rrw, divx.  Replaces the flat branch of
+ * CartesianClosure.tke_rk (src/cm1core/cuda_cartesian_closure.py:1658-1663,
+ * kernel gm1_flat_tke_advw_rk_v1 of cuda_gm1_flat_stretched_closure.py). */
+GM1B_API int32_t gm1b_tke_rk_stage_flat(int32_t ni, int32_t nj, int32_t nk, const gm1b_tke_evolution_arrays *arrays,
+                                        const float *mf_profile, const float *cur, float *nxt, int32_t nrk, float dx,
+                                        float dy, float rdz, float dt, void *stream);
+
 /* The whole operator: turbt, the three RK stages from tke3d, and the commit
  * tke3d = tkea = result.  workspace: one face volume.  Replaces
  * launch_cuda_tke_evolution (src/cm1core/cuda_tke_evolution.py:481) and the
@@ -730,6 +751,26 @@ typedef struct gm1b_deformation_arrays {
  */
 GM1B_API int32_t gm1b_terrain_deformation(int32_t ni, int32_t nj, int32_t nk, const gm1b_deformation_arrays *arrays,
                                           float dx, float dy, float dz, void *stream);
+
+/* u3d (nk, nj, ni+1), v3d (nk, nj+1, ni), w3d/rf/mf/c1/c2/defv/defh
+ * (nk+1, nj, ni), rho (nk, nj, ni), mh_profile (nk+2, CM1-indexed: word k+1
+ * is the mh of mass level k). */
+typedef struct gm1b_flat_deformation_arrays {
+    const float *u3d, *v3d, *w3d, *rho, *rf, *mf, *c1, *c2, *mh_profile;
+    float *defv, *defh;
+} gm1b_flat_deformation_arrays;
+
+/*
+ * CM1 calcdef on a flat (terrain_flag=.false.) stretched column: the strains
+ * with rdz*mh(k) and rdz*mf(k), the open sides as an index clamp, and the
+ * deformation reduction; defv and defh on face levels 1..nk-1, levels 0 and
+ * nk zero.  One kernel, no device scratch.  rdz is the vertical coordinate's
+ * reference 1/dz.  Replaces enqueue_flat_calcdef
+ * (src/cm1core/cuda_gm1_flat_stretched_closure.py:524) with the zero fill
+ * of defv/defh before it (cuda_cartesian_closure.py:1130-1131).
+ */
+GM1B_API int32_t gm1b_flat_deformation(int32_t ni, int32_t nj, int32_t nk, const gm1b_flat_deformation_arrays *arrays,
+                                       float dx, float dy, float rdz, void *stream);
 
 /* c1/c2/mf/nm (nk+1, nj, ni), pi0/th0 (nk), prs/pp3d/th3d and the cell
  * outputs (nk, nj, ni), q3d (6, nk, nj, ni) in the order qv qc qr qi qs qg,

@@ -27,6 +27,8 @@ def _lib():
         lib.oracle_moist_nm.argtypes = [i, i, i] + [_F] * 9 + [f] + [_F] * 5 + [ctypes.c_void_p,
                                                                            ctypes.POINTER(ctypes.c_int64)]
         lib.oracle_moist_nm.restype = i
+        lib.oracle_flat_calcdef.argtypes = [i, i, i] + [_F] * 9 + [f, f, f, _F, _F]
+        lib.oracle_flat_calcdef.restype = i
         lib._closure_ready = True
     return lib
 
@@ -42,6 +44,18 @@ def calcdef(arrays, *, ni, nj, nk, dx, dy, dz) -> None:
                                _p(arrays["defv"]), _p(arrays["defh"]))
     if rc != 0:
         raise ValueError(f"oracle_calcdef failed ({rc})")
+
+
+FLAT_DEFORMATION_INPUTS = ("u3d", "v3d", "w3d", "rho", "rf", "mf", "c1", "c2", "mh_profile")
+
+
+def flat_calcdef(arrays, *, ni, nj, nk, dx, dy, rdz) -> None:
+    """calcdef on a flat stretched column (enqueue_flat_calcdef,
+    src/cm1core/cuda_gm1_flat_stretched_closure.py:524); writes defv, defh."""
+    rc = _lib().oracle_flat_calcdef(ni, nj, nk, *(_p(arrays[n]) for n in FLAT_DEFORMATION_INPUTS), dx, dy, rdz,
+                                    _p(arrays["defv"]), _p(arrays["defh"]))
+    if rc != 0:
+        raise ValueError(f"oracle_flat_calcdef failed ({rc})")
 
 
 def moist_nm(arrays, *, ni, nj, nk, dz) -> dict[str, int]:

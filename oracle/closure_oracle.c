@@ -337,3 +337,103 @@ int oracle_moist_nm(int ni, int nj, int nk, const float* c1, const float* c2, co
     }
   return 0;
 }
+
+/* calcdef on a flat (terrain_flag=.false.) stretched column, three passes as
+ * the reference's texts gm1_flat_calcdef_mass_v1 / _face_v1 / _reduce_v1
+ * (src/cm1core/cuda_gm1_flat_stretched_closure.py:76-136; turb.F:4772-4786,
+ * :4880-4895, :5361-5385), with the zero fill of defv/defh before them
+ * (cuda_cartesian_closure.py:1130-1131).  mhp is the mh profile (nk+2,
+ * CM1-indexed: mhp[k+1] belongs to mass level k); mf is the 3-D face array;
+ * rdz the coordinate's reference 1/dz.  Open sides are index clamps. */
+int oracle_flat_calcdef(int ni, int nj, int nk, const float* u, const float* v, const float* w, const float* rho,
+                        const float* rf, const float* mf, const float* c1, const float* c2, const float* mhp,
+                        float dx, float dy, float rdz, float* defv, float* defh) {
+  if (ni < 3 || nj < 3 || nk < 3) return -1;
+  const float rdx = 1.0f / dx, rdy = 1.0f / dy;
+  const int64_t ncell = (int64_t)nk * nj * ni;
+  float* s11 = calloc(ncell, sizeof(float));
+  float* s22 = calloc(ncell, sizeof(float));
+  float* s33 = calloc(ncell, sizeof(float));
+  float* s12 = calloc((int64_t)nk * (nj + 1) * (ni + 1), sizeof(float));
+  float* s13 = calloc((int64_t)(nk + 1) * nj * (ni + 1), sizeof(float));
+  float* s23 = calloc((int64_t)(nk + 1) * (nj + 1) * ni, sizeof(float));
+  if (!s11 || !s22 || !s33 || !s12 || !s13 || !s23) return -2;
+  for (int64_t q = 0; q < (int64_t)(nk + 1) * nj * ni; ++q) {
+    defv[q] = 0.0f;
+    defh[q] = 0.0f;
+  }
+  const int ux = ni + 1, vy = nj + 1;
+  /* mass pass: s11, s22, s33 at cells, s12 at corners */
+  for (int k = 0; k < nk; ++k)
+    for (int jc = 0; jc <= nj; ++jc)
+      for (int ic = 0; ic <= ni; ++ic) {
+        if (ic < ni && jc < nj) {
+          const int64_t p = I3(k, jc, ic, nj, ni);
+          const float r = rho[p];
+          float d = u[I3(k, jc, ic + 1, nj, ux)] - u[I3(k, jc, ic, nj, ux)];
+          s11[p] = (r * d) * rdx;
+          d = v[I3(k, jc + 1, ic, vy, ni)] - v[I3(k, jc, ic, vy, ni)];
+          s22[p] = (r * d) * rdy;
+          d = w[I3(k + 1, jc, ic, nj, ni)] - w[I3(k, jc, ic, nj, ni)];
+          const float m = rdz * mhp[k + 1];
+          s33[p] = (r * d) * m;
+        }
+        const int ii = clampi(ic, 1, ni - 1), jj = clampi(jc, 1, nj - 1);
+        const float x = (u[I3(k, jj, ii, nj, ux)] - u[I3(k, jj - 1, ii, nj, ux)]) * rdy;
+        const float y = (v[I3(k, jj, ii, vy, ni)] - v[I3(k, jj, ii - 1, vy, ni)]) * rdx;
+        float rs = rho[I3(k, jj - 1, ii - 1, nj, ni)] + rho[I3(k, jj, ii, nj, ni)];
+        rs = rs + (rho[I3(k, jj, ii - 1, nj, ni)] + rho[I3(k, jj - 1, ii, nj, ni)]);
+        s12[I3(k, jc, ic, vy, ux)] = ((0.5f * (x + y)) * 0.25f) * rs;
+      }
+  /* face pass: s13 on u-face columns, s23 on v-face rows, face levels 1..nk-1 */
+  for (int kf = 1; kf < nk; ++kf)
+    for (int jc = 0; jc <= nj; ++jc)
+      for (int ic = 0; ic <= ni; ++ic) {
+        if (jc < nj) {
+          const int il = clampi(ic - 1, 0, ni - 1), ir = clampi(ic, 0, ni - 1);
+          const float dw = (w[I3(kf, jc, ir, nj, ni)] - w[I3(kf, jc, il, nj, ni)]) * rdx;
+          float du = (u[I3(kf, jc, ic, nj, ux)] - u[I3(kf - 1, jc, ic, nj, ux)]) * rdz;
+          du = (du * 0.5f) * (mf[I3(kf, jc, il, nj, ni)] + mf[I3(kf, jc, ir, nj, ni)]);
+          const float dens = rf[I3(kf, jc, il, nj, ni)] + rf[I3(kf, jc, ir, nj, ni)];
+          s13[I3(kf, jc, ic, nj, ux)] = ((0.5f * (dw + du)) * 0.5f) * dens;
+        }
+        if (ic < ni) {
+          const int js = clampi(jc - 1, 0, nj - 1), jn = clampi(jc, 0, nj - 1);
+          const float dw = (w[I3(kf, jn, ic, nj, ni)] - w[I3(kf, js, ic, nj, ni)]) * rdy;
+          float dv = (v[I3(kf, jc, ic, vy, ni)] - v[I3(kf - 1, jc, ic, vy, ni)]) * rdz;
+          dv = (dv * 0.5f) * (mf[I3(kf, js, ic, nj, ni)] + mf[I3(kf, jn, ic, nj, ni)]);
+          const float dens = rf[I3(kf, js, ic, nj, ni)] + rf[I3(kf, jn, ic, nj, ni)];
+          s23[I3(kf, jc, ic, vy, ni)] = ((0.5f * (dw + dv)) * 0.5f) * dens;
+        }
+      }
+  /* reduction (the pass both branches share) */
+  for (int kf = 1; kf < nk; ++kf)
+    for (int j = 0; j < nj; ++j)
+      for (int i = 0; i < ni; ++i) {
+        const int64_t p = I3(kf, j, i, nj, ni), lo = I3(kf - 1, j, i, nj, ni);
+        const float a = c1[p], b = c2[p];
+        const float t11 = a * (s11[lo] * s11[lo]) + b * (s11[p] * s11[p]);
+        const float t22 = a * (s22[lo] * s22[lo]) + b * (s22[p] * s22[p]);
+        const float t33 = a * (s33[lo] * s33[lo]) + b * (s33[p] * s33[p]);
+        const float l00 = s12[I3(kf - 1, j, i, vy, ux)], l11 = s12[I3(kf - 1, j + 1, i + 1, vy, ux)];
+        const float l10 = s12[I3(kf - 1, j + 1, i, vy, ux)], l01 = s12[I3(kf - 1, j, i + 1, vy, ux)];
+        const float h00 = s12[I3(kf, j, i, vy, ux)], h11 = s12[I3(kf, j + 1, i + 1, vy, ux)];
+        const float h10 = s12[I3(kf, j + 1, i, vy, ux)], h01 = s12[I3(kf, j, i + 1, vy, ux)];
+        const float lsum = (l00 * l00 + l11 * l11) + (l10 * l10 + l01 * l01);
+        const float hsum = (h00 * h00 + h11 * h11) + (h10 * h10 + h01 * h01);
+        const float t12 = 0.25f * (a * lsum + b * hsum);
+        const float x0 = s13[I3(kf, j, i, nj, ux)], x1 = s13[I3(kf, j, i + 1, nj, ux)];
+        const float y0 = s23[I3(kf, j, i, vy, ni)], y1 = s23[I3(kf, j + 1, i, vy, ni)];
+        const float t13 = 0.5f * (x0 * x0 + x1 * x1), t23 = 0.5f * (y0 * y0 + y1 * y1);
+        const float rrf = 1.0f / (rf[p] * rf[p]);
+        defv[p] = (4.0f * (t13 + t23)) * rrf;
+        defh[p] = ((2.0f * ((t11 + t22) + t33)) + 4.0f * t12) * rrf;
+      }
+  free(s11);
+  free(s22);
+  free(s33);
+  free(s12);
+  free(s13);
+  free(s23);
+  return 0;
+}

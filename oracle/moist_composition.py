@@ -3,7 +3,9 @@ INFRASTRUCTURE ONLY.  The same phases, in the reference's large-step
 schedule (src/cm1core/gm1_runtime.py:1969-2007), as the product's
 composition, each phase calling the oracle restatement of the operator the
 product calls there; left out identically: SGS stress and scalar diffusion,
-Rayleigh damping, the dry-mass correction, surface fluxes."""
+Rayleigh damping, the dry-mass correction, surface fluxes.  A configuration
+with a stretched column (cfg.column set) runs the flat (terrain_flag=.false.)
+family on the column profiles its metrics carry."""
 
 from __future__ import annotations
 
@@ -46,6 +48,17 @@ class OracleMoistStep:
                 state[n] = np.zeros(state["pp3d"].shape, np.float32)
         self.k3 = dict(ni=cfg.ni, nj=cfg.nj, nk=cfg.nk)
         self.grid = dict(ni=cfg.ni, nj=cfg.nj, nk=cfg.nk, dx=cfg.dx, dy=cfg.dy, dz=cfg.dz)
+        # a stretched column runs the flat (terrain_flag=.false.) family on
+        # the column profiles of its metrics (the Cartesian stretched lane,
+        # src/cm1core/cuda_cartesian_dynamics.py:1075-1104, :1148-1187,
+        # :1220-1231, :1254-1269, :1293; cuda_cartesian_closure.py:1133-1141,
+        # :1191-1197, :1658-1663)
+        self.flat = getattr(cfg, "column", None) is not None
+        if self.flat:
+            self.rdz = float(np.float32(np.float32(1.0) / np.float32(cfg.dz)))
+            self.hx = dict(ni=cfg.ni, nj=cfg.nj, nk=cfg.nk, dx=cfg.dx, dy=cfg.dy)
+            self.column = {"flat": True, "rho0p": metrics["rho0_padded"], "mh": metrics["mh_profile"],
+                           "mf": metrics["mf_profile"], "rr0": metrics["rr0"], "rdz": self.rdz}
 
     def _pp3d_to_compact(self):
         c = self.cfg
@@ -62,14 +75,22 @@ class OracleMoistStep:
                       "pp3d": s["pp3d_c"], "th3d": s["th3d"], "q3d": s["q3d"], "nm": s["nm"],
                       "temperature": s["temperature"], "qt": s["qt"], "thv": s["thv_c"], "qvci": s["qvci"],
                       "saturation_mask": s["saturation_mask"]}, **self.k3, dz=c.dz)
-        ocl.calcdef({"u3d": s["uc"], "v3d": s["vc"], "w3d": s["wc"], "rho": s["rho"], "rf": s["rf"],
-                     **{n: m[n] for n in ("c1", "c2", "gz", "rgz", "rgzu", "rgzv", "gx", "gy")},
-                     "defv": s["defv"], "defh": s["defh"]}, **self.grid)
+        if self.flat:
+            ocl.flat_calcdef({"u3d": s["uc"], "v3d": s["vc"], "w3d": s["wc"], "rho": s["rho"], "rf": s["rf"],
+                              "mf": m["mf"], "c1": m["c1"], "c2": m["c2"], "mh_profile": m["mh_profile"],
+                              "defv": s["defv"], "defh": s["defh"]}, **self.hx, rdz=self.rdz)
+        else:
+            ocl.calcdef({"u3d": s["uc"], "v3d": s["vc"], "w3d": s["wc"], "rho": s["rho"], "rf": s["rf"],
+                         **{n: m[n] for n in ("c1", "c2", "gz", "rgz", "rgzu", "rgzv", "gx", "gy")},
+                         "defv": s["defv"], "defh": s["defh"]}, **self.grid)
         otke.sgs_tke({"ruh": s["ruh"], "rvh": s["rvh"], "rmf": m["rmf"], **{n: s[n] for n in otke.NAMES
                                                                           if n not in ("ruh", "rvh", "rmf")}},
                      **self.grid)
         s["tke3d"][:] = s["tkea"]
-        otev.tke_diffusion(self._tke(), **self.grid, dt=c.dt)
+        if self.flat:
+            otev.tke_diffusion_flat(self._tke(), **self.hx, rdz=self.rdz, dt=c.dt)
+        else:
+            otev.tke_diffusion(self._tke(), **self.grid, dt=c.dt)
 
     def _tke(self):
         s, m = self.s, self.m
@@ -101,6 +122,10 @@ class OracleMoistStep:
         s["uten"][:] = 0
         s["vten"][:] = 0
         s["wten"][:] = 0
+        if self.flat:
+            omom.momentum_advection5_column(self._mom(), self.column, **self.hx, lateral_sides=c.lateral_sides)
+            oms.moist_buoyancy_flat(s["dum8"], m["c1"], m["c2"], s["wten"], **self.k3)
+            return
         if nrk >= 2:
             oms.bcwsfc(s["u3d"], s["v3d"], s["w3d"], m["gz"], m["dzdx"], m["dzdy"], **self.k3)
             oms.w_level1_fill(s["w3d"], **self.k3)
@@ -113,23 +138,35 @@ class OracleMoistStep:
 
     def acoustic(self, nrk):
         c = self.cfg
+        if self.flat:
+            otos.terrain_open_stage_flat(self.s, self.m, self.column, nrk=nrk, ni=c.ni, nj=c.nj, nk=c.nk, dt=c.dt,
+                                         nsound=c.nsound, dx=c.dx, dy=c.dy, obc=c.obc, alph=_f32(c.alph),
+                                         kdiv=_f32(c.kdiv), ablations=255 & ~128)
+            return
         otos.terrain_open_stage(self.s, self.m, nrk=nrk, ni=c.ni, nj=c.nj, nk=c.nk, dt=c.dt, nsound=c.nsound,
                                 dx=c.dx, dy=c.dy, dz=c.dz, alph=_f32(c.alph), kdiv=_f32(c.kdiv), ablations=255 & ~128)
 
     def post_acoustic(self, nrk):
         s, m = self.s, self.m
-        oms.post_acoustic_flux({"rru": s["rru"], "rrv": s["rrv"], "rrw": s["rrw"], "rgzu": m["rgzu"],
-                                "rgzv": m["rgzv"], "dzdx": m["dzdx"], "dzdy": m["dzdy"], "gz": m["gz"],
-                                "rho0_3d": m["rho0_3d"], "rf0": m["rf0"], "thterm": s["thterm"],
-                                "divergence": s["divergence"], "theta_divergence_term": s["theta_div"],
-                                "divx": s["divx"]}, **self.grid)
+        a = {"rru": s["rru"], "rrv": s["rrv"], "rrw": s["rrw"], "rgzu": m["rgzu"], "rgzv": m["rgzv"],
+             "dzdx": m["dzdx"], "dzdy": m["dzdy"], "gz": m["gz"], "rho0_3d": m["rho0_3d"], "rf0": m["rf0"],
+             "thterm": s["thterm"], "divergence": s["divergence"], "theta_divergence_term": s["theta_div"],
+             "divx": s["divx"]}
+        if self.flat:
+            oms.post_acoustic_flux_column(a, self.column, **self.hx)
+        else:
+            oms.post_acoustic_flux(a, **self.grid)
 
     def _advect(self, padded, tendency, nrk, weps):
         s, m, c = self.s, self.m, self.cfg
-        oadv.scalar_advection5({"scalar": padded, "rru": s["rru"], "rrv": s["rrv"], "rrw": s["rrw"], "c1": m["c1"],
-                                "c2": m["c2"], "rr0": m["rr0"], "gz": m["gz"], "divx": s["divx"],
-                                "tendency": tendency, "flux_x": s["fx"], "flux_y": s["fy"], "flux_z": s["fz"]},
-                               **self.grid, nrk=nrk, weps=weps, lateral_obc=c.obc)
+        a = {"scalar": padded, "rru": s["rru"], "rrv": s["rrv"], "rrw": s["rrw"], "c1": m["c1"], "c2": m["c2"],
+             "rr0": m["rr0"], "gz": m["gz"], "divx": s["divx"], "tendency": tendency, "flux_x": s["fx"],
+             "flux_y": s["fy"], "flux_z": s["fz"]}
+        if self.flat:
+            oadv.scalar_advection5_column(a, **self.hx, nrk=nrk, weps=weps, flat=True, profile=m["mh_profile"],
+                                          rdz=self.rdz, lateral_obc=c.obc)
+        else:
+            oadv.scalar_advection5(a, **self.grid, nrk=nrk, weps=weps, lateral_obc=c.obc)
 
     def scalar_moist(self, nrk):
         s, m, c = self.s, self.m, self.cfg
@@ -145,14 +182,18 @@ class OracleMoistStep:
             if nrk < 3:
                 self._advect(s["moisture_padded"], s["moist_adv"][r], nrk, moisture_weps(r))
             else:
-                oms.pdef_moisture_chain({"scalar_a": s["qa"][r], "scalar_padded": s["moisture_padded"],
-                                         "rho0_3d": m["rho0_3d"], "gz": m["gz"], "rgz": m["rgz"], "rr0": m["rr0"],
-                                         "c1": m["c1"], "c2": m["c2"], "divx": s["divx"], "rru": s["rru"],
-                                         "rrv": s["rrv"], "rrw": s["rrw"], "fx": s["fx"], "fy": s["fy"],
-                                         "fz": s["fz"], "advx": s["advx"], "advy": s["advy"], "advz": s["advz"],
-                                         "candidate": s["candidate"], "advection": s["moist_adv"][r]},
-                                        **self.grid, dttmp=dttmp, weps=moisture_weps(r), lateral_obc=c.obc,
-                                        pdefweno=0 if r == 0 else 1)
+                chain = {"scalar_a": s["qa"][r], "scalar_padded": s["moisture_padded"], "rho0_3d": m["rho0_3d"],
+                         "gz": m["gz"], "rgz": m["rgz"], "rr0": m["rr0"], "c1": m["c1"], "c2": m["c2"],
+                         "divx": s["divx"], "rru": s["rru"], "rrv": s["rrv"], "rrw": s["rrw"], "fx": s["fx"],
+                         "fy": s["fy"], "fz": s["fz"], "advx": s["advx"], "advy": s["advy"], "advz": s["advz"],
+                         "candidate": s["candidate"], "advection": s["moist_adv"][r]}
+                if self.flat:
+                    oms.pdef_moisture_chain_column(chain, **self.hx, dttmp=dttmp, weps=moisture_weps(r),
+                                                   lateral_obc=c.obc, pdefweno=0 if r == 0 else 1, flat=True,
+                                                   profile=m["mh_profile"], rdz=self.rdz)
+                else:
+                    oms.pdef_moisture_chain(chain, **self.grid, dttmp=dttmp, weps=moisture_weps(r),
+                                            lateral_obc=c.obc, pdefweno=0 if r == 0 else 1)
         qa, q = s["qa"][:NUMQ], s["q3d"][:NUMQ]
         ork.compose(s["tha"], qa, s["thheld"], s["qheld"], s["theta_div"], s["theta_adv"], s["moist_adv"], s["th3d"],
                     q, nrk=nrk, dt=c.dt)
@@ -162,14 +203,19 @@ class OracleMoistStep:
         oms.open_fill(s["u3d"], "u", **self.k3)
         oms.open_fill(s["v3d"], "v", **self.k3)
         oms.open_fill(s["w3d"], "w", **self.k3)
-        oms.bcwsfc(s["u3d"], s["v3d"], s["w3d"], m["gz"], m["dzdx"], m["dzdy"], **self.k3)
+        if not self.flat:
+            oms.bcwsfc(s["u3d"], s["v3d"], s["w3d"], m["gz"], m["dzdx"], m["dzdy"], **self.k3)
 
     def scalar_boundaries(self, nrk):
         oms.open_fill(self.s["pp3d"], "pressure", **self.k3)
 
     def tke_rk(self, nrk):
         s = self.s
-        otev.tke_rk_stage(self._tke(), s["tke3d"], s["tke_workspace"], **self.grid, nrk=nrk, dt=self.cfg.dt)
+        if self.flat:
+            otev.tke_rk_stage_flat(self._tke(), self.m["mf_profile"], s["tke3d"], s["tke_workspace"], **self.hx,
+                                   nrk=nrk, rdz=self.rdz, dt=self.cfg.dt)
+        else:
+            otev.tke_rk_stage(self._tke(), s["tke3d"], s["tke_workspace"], **self.grid, nrk=nrk, dt=self.cfg.dt)
         s["tke3d"][:] = s["tke_workspace"]
 
     def microphysics(self):

@@ -96,16 +96,75 @@ def flat_metrics(ni: int, nj: int, nk: int, dz: float, rho: np.ndarray) -> dict[
     return m
 
 
+def column_levels(cfg) -> dict[str, np.ndarray]:
+    """The oracle's stretch_z = 1 coordinate of cfg.column (reference dz =
+    cfg.dz), CM1-indexed profiles."""
+    from oracle.vertical import vertical_levels
+
+    c = cfg.column
+    rc, lv = vertical_levels(1, cfg.nk, cfg.dz, c.ztop_m, c.str_bot_m, c.str_top_m, c.dz_bot_m, c.dz_top_m)
+    if rc != 0:
+        raise ValueError(f"oracle_vertical_levels refused the column ({rc})")
+    return lv
+
+
+def padded_base_density(rho0: np.ndarray) -> np.ndarray:
+    """(nk+2, nj+6, ni+6) base density: halo columns/rows repeat the edge,
+    ghost levels the nearest interior level."""
+    nk, nj, ni = rho0.shape
+    p = np.zeros((nk + 2, nj + 6, ni + 6), np.float32)
+    p[1:nk + 1, 3:nj + 3, 3:ni + 3] = rho0
+    p[1:nk + 1, 3:nj + 3, :3] = rho0[:, :, :1]
+    p[1:nk + 1, 3:nj + 3, ni + 3:] = rho0[:, :, -1:]
+    p[:, :3, :] = p[:, 3:4, :]
+    p[:, nj + 3:, :] = p[:, nj + 2:nj + 3, :]
+    p[0], p[nk + 1] = p[1], p[nk]
+    return p
+
+
+def stretched_metrics(ni: int, nj: int, nk: int, lv: dict[str, np.ndarray], rho: np.ndarray) -> dict[str, np.ndarray]:
+    """Metrics of a flat stretched column: the generated mh/mf/rmh/rmf over
+    the plane, c2(k) = (zf(k) - zh(k-1)) / (zh(k) - zh(k-1)) and c1 = 1 - c2,
+    base density from the initial density's level means, the column profiles
+    and the padded base density."""
+    f = np.float32
+    m = {n: np.zeros(sh, f) for n, sh in terrain_static_shapes(ni, nj, nk).items()}
+    for n in ("gz", "rgz", "gzu", "rgzu", "gzv", "rgzv"):
+        m[n][:] = f(1.0)
+    m["mh"][:], m["rmh"][:] = lv["mh"][1:nk + 1, None, None], lv["rmh"][1:nk + 1, None, None]
+    m["mf"][:], m["rmf"][:] = lv["mf"][1:nk + 2, None, None], lv["rmf"][1:nk + 2, None, None]
+    zh, zf = lv["zh"], lv["zf"]
+    c2 = np.empty(nk + 1, f)
+    for k in range(1, nk + 2):
+        c2[k - 1] = (zf[k] - zh[k - 1]) / (zh[k] - zh[k - 1])
+    c1 = (f(1.0) - c2).astype(f)
+    m["c1"][:], m["c2"][:] = c1[:, None, None], c2[:, None, None]
+    m["zh"][:] = zh[1:nk + 1, None, None]
+    m["zf"][:] = zf[1:nk + 2, None, None]
+    prof = rho.astype(np.float64).mean(axis=(1, 2)).astype(f)
+    m["rho0_3d"][:] = prof[:, None, None]
+    m["rr0"][:] = (f(1.0) / m["rho0_3d"]).astype(f)
+    rf = np.empty(nk + 1, f)
+    rf[1:nk] = (c1[1:nk] * prof[:-1] + c2[1:nk] * prof[1:]).astype(f)
+    rf[0], rf[nk] = prof[0], prof[nk - 1]
+    m["rf0"][:] = rf[:, None, None]
+    m["rrf0"][:] = (f(1.0) / m["rf0"]).astype(f)
+    m["mh_profile"], m["mf_profile"] = lv["mh"].copy(), lv["mf"].copy()
+    m["rho0_padded"] = padded_base_density(m["rho0_3d"])
+    return m
+
+
 def weisman_klemp_initial_state(cfg, *, seed: int = 0, bubble_k: float = 3.0, noise_k: float = 0.1,
                                 bubble_radius_m: tuple[float, float] = (10000.0, 1400.0),
                                 bubble_center_z_m: float = 1400.0, bubble_cloud: float = 0.0,
                                 bubble_rain: float = 0.0, bubble_offset_m: tuple[float, float] = (0.0, 0.0)):
-    """(state, metrics) of a Weisman-Klemp start on cfg's uniform grid (cfg
-    has ni, nj, nk, dx, dy, dz)."""
+    """(state, metrics) of a Weisman-Klemp start on cfg's grid (cfg has ni,
+    nj, nk, dx, dy, dz and, for a stretched column, column)."""
     ni, nj, nk = cfg.ni, cfg.nj, cfg.nk
     f = np.float32
     s = {n: np.zeros(sh, dtype=DTYPES.get(n, np.float32)) for n, sh in moist_state_shapes(ni, nj, nk).items()}
-    zh = ((np.arange(nk, dtype=np.float64) + 0.5) * cfg.dz).astype(f)
+    lv = column_levels(cfg) if getattr(cfg, "column", None) is not None else None
+    zh = lv["zh"][1:nk + 1].copy() if lv is not None else ((np.arange(nk, dtype=np.float64) + 0.5) * cfg.dz).astype(f)
     col = wk_column(zh, 1)
     s["th0"][:], s["pi0"][:], s["qv0"][:] = col["th0"], col["pi0"], col["qv0"]
     s["th0_3d"][:] = s["th0"][:, None, None]
@@ -129,7 +188,7 @@ def weisman_klemp_initial_state(cfg, *, seed: int = 0, bubble_k: float = 3.0, no
     s["tke3d"][1:nk] = f(1.0e-4)
     for n in ("uh", "vh", "ruf", "rvf", "ruh", "rvh", "ones_mass"):
         s[n][:] = f(1.0)
-    m = flat_metrics(ni, nj, nk, cfg.dz, s["rho"])
+    m = flat_metrics(ni, nj, nk, cfg.dz, s["rho"]) if lv is None else stretched_metrics(ni, nj, nk, lv, s["rho"])
     rho = s["rho"]
     s["rr"][:] = (f(1.0) / rho).astype(f)
     s["rf"][1:nk] = (m["c1"][1:nk] * rho[:-1] + m["c2"][1:nk] * rho[1:]).astype(f)

@@ -25,6 +25,10 @@ def _lib():
         lib.oracle_tke_diffusion.restype = i
         lib.oracle_tke_rk_stage.argtypes = [i, i, i] + [_F] * 12 + [i, f, f, f, f]
         lib.oracle_tke_rk_stage.restype = i
+        lib.oracle_tke_diffusion_flat.argtypes = [i, i, i] + [_F] * 8 + [f, f, f, f]
+        lib.oracle_tke_diffusion_flat.restype = i
+        lib.oracle_tke_rk_stage_flat.argtypes = [i, i, i] + [_F] * 11 + [i, f, f, f, f]
+        lib.oracle_tke_rk_stage_flat.restype = i
         lib._tkeevo_ready = True
     return lib
 
@@ -60,3 +64,23 @@ def tke_evolution(a, *, ni, nj, nk, dx, dy, dz, dt) -> list[str]:
     a["tke3d"][...] = cur
     a["tkea"][...] = cur
     return hashes
+
+
+FLAT_DIFFUSION_NAMES = ("tke3d", "kmh", "kmv", "rho", "rf", "mh", "mf", "tketen")
+FLAT_STAGE_NAMES = ("tkea", "tketen", "c2", "rrf0", "rru", "rrv", "rrw", "divx")
+
+
+def tke_diffusion_flat(a, *, ni, nj, nk, dx, dy, rdz, dt) -> None:
+    """turbt on a flat stretched column (gm1_flat_turbt_v1,
+    src/cm1core/cuda_gm1_flat_stretched_closure.py:314); adds into tketen."""
+    rc = _lib().oracle_tke_diffusion_flat(ni, nj, nk, *(_p(a[n]) for n in FLAT_DIFFUSION_NAMES), dx, dy, rdz, dt)
+    if rc != 0:
+        raise ValueError(f"oracle_tke_diffusion_flat failed ({rc})")
+
+
+def tke_rk_stage_flat(a, mf_profile, cur, nxt, *, ni, nj, nk, nrk, dx, dy, rdz, dt) -> None:
+    """One RK stage on a flat stretched column (gm1_flat_tke_advw_rk_v1)."""
+    rc = _lib().oracle_tke_rk_stage_flat(ni, nj, nk, _p(cur), *(_p(a[n]) for n in FLAT_STAGE_NAMES),
+                                         _p(mf_profile), _p(nxt), nrk, dx, dy, rdz, dt)
+    if rc != 0:
+        raise ValueError(f"oracle_tke_rk_stage_flat failed ({rc})")

@@ -313,3 +313,152 @@ int oracle_tke_rk_stage(int ni, int nj, int nk, const float* cur, const float* t
       }
   return 0;
 }
+
+/* ---- flat (terrain_flag=.false.) stretched column --------------------- */
+
+/* turbt, gm1_flat_turbt_v1 (src/cm1core/cuda_gm1_flat_stretched_closure.py:314-359;
+ * turbtend.F:729-1044): per column, the x/y face fluxes at each face level,
+ * the implicit diffusion with the coordinate's reference rdz and the 3-D mh
+ * (mass) and mf (face), added into tketen. */
+static float tfx_flat(const tke_grid* g, const float* t, int f, int j, int a, float rdx) {
+  float r = 0.25f * (CELL(g, g->rf, f, j, a) + CELL(g, g->rf, f, j, a - 1));
+  r = r * 2.0f;
+  r = r * (CELL(g, g->kmh, f, j, a) + CELL(g, g->kmh, f, j, a - 1));
+  r = r * (CELL(g, t, f, j, a) - CELL(g, t, f, j, a - 1));
+  return -(r * rdx);
+}
+static float tfy_flat(const tke_grid* g, const float* t, int f, int b, int i, float rdy) {
+  float r = 0.25f * (CELL(g, g->rf, f, b, i) + CELL(g, g->rf, f, b - 1, i));
+  r = r * 2.0f;
+  r = r * (CELL(g, g->kmh, f, b, i) + CELL(g, g->kmh, f, b - 1, i));
+  r = r * (CELL(g, t, f, b, i) - CELL(g, t, f, b - 1, i));
+  return -(r * rdy);
+}
+
+int oracle_tke_diffusion_flat(int ni, int nj, int nk, const float* t, const float* kmh, const float* kmv,
+                              const float* rho, const float* rf, const float* mh, const float* mf, float* ten,
+                              float dx, float dy, float rdz, float dt) {
+  if (ni < 3 || nj < 3 || nk < 6) return -1;
+  tke_grid gg = {ni, nj, nk, kmh, kmv, rho, rf, mh, mf, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  const tke_grid* g = &gg;
+  const float rdx = 1.0f / dx, rdy = 1.0f / dy, rdt = 1.0f / dt;
+  const float tema = (((-1.0f * dt) * 1.0f) * rdz) * rdz, temb = ((dt * 0.0f) * rdz) * rdz;
+  float *hx = malloc(sizeof(float) * (nk + 1)), *hy = malloc(sizeof(float) * (nk + 1));
+  float *d1 = malloc(sizeof(float) * (nk + 1)), *d2 = malloc(sizeof(float) * (nk + 1));
+  float *d3 = malloc(sizeof(float) * (nk + 1)), *tz = malloc(sizeof(float) * (nk + 1));
+  if (!hx || !hy || !d1 || !d2 || !d3 || !tz) return -2;
+#define TF(f) t[I3((f), j, i, nj, ni)]
+#define PF(a, f) a[I3((f), j, i, nj, ni)]
+  for (int j = 0; j < nj; ++j)
+    for (int i = 0; i < ni; ++i) {
+      for (int f = 1; f < nk; ++f) {
+        hx[f] = -((tfx_flat(g, t, f, j, i + 1, rdx) - tfx_flat(g, t, f, j, i, rdx)) * rdx);
+        hy[f] = -((tfy_flat(g, t, f, j + 1, i, rdy) - tfy_flat(g, t, f, j, i, rdy)) * rdy);
+        if (i == 0 || i == ni - 1) hx[f] = 0.0f;
+        if (j == 0 || j == nj - 1) hy[f] = 0.0f;
+      }
+      {
+        const int f = 1;
+        const float rrf = PF(mf, f) / PF(rf, f);
+        const float r2 = (((PF(kmv, f) + PF(kmv, f + 1)) * PF(mh, f)) * PF(rho, f)) * rrf;
+        const float cfc = tema * r2, cfb = 1.0f - cfc;
+        const float cfd = TF(f) + temb * ((r2 * TF(f + 1)) - (r2 * TF(f)));
+        const float inv = 1.0f / cfb;
+        d1[f] = -(cfc * inv);
+        d2[f] = cfd * inv;
+      }
+      for (int f = 2; f < nk - 1; ++f) {
+        const float rrf = PF(mf, f) / PF(rf, f);
+        const float r1 = (((PF(kmv, f - 1) + PF(kmv, f)) * PF(mh, f - 1)) * PF(rho, f - 1)) * rrf;
+        const float r2 = (((PF(kmv, f) + PF(kmv, f + 1)) * PF(mh, f)) * PF(rho, f)) * rrf;
+        const float cfa = tema * r1, cfc = tema * r2, cfb = (1.0f - cfa) - cfc;
+        const float cfd = TF(f) + temb * (((r2 * TF(f + 1)) - ((r1 + r2) * TF(f))) + (r1 * TF(f - 1)));
+        const float inv = 1.0f / (cfa * d1[f - 1] + cfb);
+        d1[f] = -(cfc * inv);
+        d2[f] = (cfd - cfa * d2[f - 1]) * inv;
+      }
+      {
+        const int f = nk - 1;
+        const float rrf = PF(mf, f) / PF(rf, f);
+        const float r1 = (((PF(kmv, f - 1) + PF(kmv, f)) * PF(mh, f - 1)) * PF(rho, f - 1)) * rrf;
+        const float cfa = tema * r1, cfb = 1.0f - cfa;
+        const float cfd = TF(f) + temb * ((-(r1 * TF(f))) + (r1 * TF(f - 1)));
+        const float inv = 1.0f / (cfa * d1[f - 1] + cfb);
+        d3[f] = (cfd - cfa * d2[f - 1]) * inv;
+        tz[f] = (PF(rf, f) * (d3[f] - TF(f))) * rdt;
+      }
+      for (int f = nk - 2; f >= 1; --f) {
+        d3[f] = d1[f] * d3[f + 1] + d2[f];
+        tz[f] = (PF(rf, f) * (d3[f] - TF(f))) * rdt;
+      }
+      for (int f = 1; f < nk; ++f) {
+        const int64_t p = I3(f, j, i, nj, ni);
+        ten[p] = ten[p] + ((hx[f] + hy[f]) + tz[f]) / rf[p];
+      }
+    }
+#undef TF
+#undef PF
+  free(hx);
+  free(hy);
+  free(d1);
+  free(d2);
+  free(d3);
+  free(tz);
+  return 0;
+}
+
+/* One RK stage on a flat column, gm1_flat_tke_advw_rk_v1 (the stretched TKE
+ * advw text with the flat patches of
+ * src/cm1core/cuda_gm1_flat_stretched_closure.py:401-449): vertical
+ * divergence -(dumz(k)-dumz(k-1))*rdz*mfp(k) (mfp the nk+3 mf profile,
+ * CM1-indexed), the column's c2 (its (k, 0, 0) word) in the divergence
+ * correction and its rrf0, the cell's c2 in the open-side pieces (q*d)*rdx,
+ * no gz. */
+int oracle_tke_rk_stage_flat(int ni, int nj, int nk, const float* cur, const float* tkea, const float* tketen,
+                             const float* c2, const float* rrf0, const float* rru, const float* rrv, const float* rrw,
+                             const float* divx, const float* mfp, float* nxt, int nrk, float dx, float dy, float rdz,
+                             float dt) {
+  if (ni < 3 || nj < 3 || nk < 6 || nrk < 1 || nrk > 3) return -1;
+  tke_grid gg = {ni, nj, nk, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, c2, rrf0, rru, rrv, rrw, divx};
+  const tke_grid* g = &gg;
+  const float rdx = 1.0f / dx, rdy = 1.0f / dy;
+  const float dttmp = dt / (float)(4 - nrk);
+  const int w = nrk == 3;
+  const double eps = (double)(100.0f * 1e-18f);
+  for (int j = 0; j < nj; ++j)
+    for (int i = 0; i < ni; ++i) {
+      nxt[I3(0, j, i, nj, ni)] = 0.0f;
+      nxt[I3(nk, j, i, nj, ni)] = 0.0f;
+    }
+  for (int f = 1; f < nk; ++f)
+    for (int j = 0; j < nj; ++j)
+      for (int i = 0; i < ni; ++i) {
+        float mw, me, ms, mn;
+        const float fx0 = hflux(g, cur, f, j, i, 0, w, eps, 1, &mw);
+        const float fx1 = hflux(g, cur, f, j, i + 1, 0, w, eps, 1, &me);
+        const float fy0 = hflux(g, cur, f, i, j, 1, w, eps, 1, &ms);
+        const float fy1 = hflux(g, cur, f, i, j + 1, 1, w, eps, 1, &mn);
+        float ax = -1.0f * ((fx1 - fx0) * rdx);
+        float ay = -1.0f * ((fy1 - fy0) * rdy);
+        const int64_t z = I3(f, j, i, nj, ni);
+        const float cc2 = c2[z], cc1 = 1.0f - cc2;
+        const float c2c = c2[I3(f, 0, 0, nj, ni)], c1c = 1.0f - c2c;
+        const float q = cur[z];
+        if ((i == 0 && mw >= 0.0f) || (i == ni - 1 && me <= 0.0f)) {
+          const float d = cc1 * (RRU(f, j, i + 1) - RRU(f, j, i)) + cc2 * (RRU(f + 1, j, i + 1) - RRU(f + 1, j, i));
+          ax = ax - (q * d) * rdx;
+        }
+        if ((j == 0 && ms >= 0.0f) || (j == nj - 1 && mn <= 0.0f)) {
+          const float d = cc1 * (RRV(f, j + 1, i) - RRV(f, j, i)) + cc2 * (RRV(f + 1, j + 1, i) - RRV(f + 1, j, i));
+          ay = ay - (q * d) * rdy;
+        }
+        const float dv = vflux(g, cur, f + 1, j, i, w, eps) - vflux(g, cur, f, j, i, w, eps);
+        const float az = ((-dv) * rdz) * mfp[f + 1];
+        float total = (ax + ay) + az;
+        total = total + q * (c2c * divx[I3(f, j, i, nj, ni)] + c1c * divx[I3(f - 1, j, i, nj, ni)]);
+        const float wten = tketen[z] + total * rrf0[I3(f, 0, 0, nj, ni)];
+        const float value = tkea[z] + dttmp * wten;
+        nxt[z] = value < 1e-10f ? 0.0f : value;
+      }
+  return 0;
+}

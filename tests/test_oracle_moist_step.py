@@ -135,3 +135,22 @@ def test_oracle_initial_state_is_the_package_state_word_for_word():
         assert np.array_equal(hs[n].view(np.uint8), os_[n].view(np.uint8)), n
     for n in hm:
         assert np.array_equal(hm[n].view(np.uint8), om_[n].view(np.uint8)), n
+
+
+def test_oracle_stretched_initial_state_is_the_package_state_word_for_word():
+    """The same on a stretched column (stretch_z 1, 20 m at the ground):
+    the state, the metrics, the column profiles and the padded base density."""
+    from gm1_b200.moist_step import MoistStepConfig, StretchedColumnSpec, weisman_klemp_initial_state
+    from oracle.moist_initial import weisman_klemp_initial_state as oracle_state
+
+    cfg = MoistStepConfig(18, 12, 14, 100.0, 100.0, 100.0, 0.6, 8,
+                          column=StretchedColumnSpec(1630.0, 40.0, 1030.0, 20.0, 200.0))
+    kw = dict(seed=3, bubble_radius_m=(600.0, 500.0), bubble_center_z_m=500.0, bubble_cloud=1.0e-3)
+    hs, hm = weisman_klemp_initial_state(cfg, **kw)
+    os_, om_ = oracle_state(cfg, **kw)
+    assert sorted(hs) == sorted(os_) and sorted(hm) == sorted(om_)
+    for d1, d2 in ((hs, os_), (hm, om_)):
+        for n in d1:
+            assert d1[n].shape == d2[n].shape, n
+            assert np.array_equal(d1[n].view(np.uint8), d2[n].view(np.uint8)), n
+    assert float(hm["mh"].max()) > float(hm["mh"].min())  # stretched
