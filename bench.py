@@ -1,19 +1,25 @@
 #!/usr/bin/env python
 """Throughput of the RK3 large step on B200: cell-updates/s.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload moist|dry]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--workload c3|moist-c2|dry|ensemble]
 
-Default workload (moist): the Weisman-Klemp supercell start on 256x256x80
-cells (dx = dy = 1 km, dz = 250 m, dt = 5 s, nsound = 10, so 4 + 5 + 10 =
-19 acoustic small steps per large step; open-radiative laterals), Kessler
-warm rain (equation set 2), WENO5 moisture on the final stage with the
-positive-definite chain, the 1.5-order TKE closure.  One "step" is one full
+Default workload (c3): the Weisman-Klemp supercell start on 640x768x80 cells
+(39.3 M) of a vertically stretched column (dx = dy = 100 m, stretch_z 1 from
+20 m at the ground to 500 m aloft under a 20.8 km lid, dt = 0.6 s,
+nsound = 8, so 3 + 4 + 8 = 15 acoustic small steps per large step;
+open-radiative laterals), Kessler warm rain (equation set 2), WENO5
+moisture on the final stage with the positive-definite chain, the
+1.5-order TKE closure, in the reference's flat (terrain_flag=.false.)
+operator family for a stretched Cartesian column.  One "step" is one full
 moist RK3 large step: closure and held tendencies, three RK stages (moist
-stage terms, momentum advection, buoyancy, the terrain/open psolver=3
-acoustic stage, getdiv/getdivx, theta and qv/qc/qr advection and update,
-boundaries, TKE advection), the Kessler transition and solve3, through the
-library's C ABI.  --workload dry is the 64x64x40 dry warm bubble on the
-serial-periodic lane (nsound 6).
+stage terms, momentum advection, buoyancy, the psolver=3 acoustic stage,
+getdiv/getdivx, theta and qv/qc/qr advection and update, boundaries, TKE
+advection), the Kessler transition and solve3, through the library's C ABI.
+--workload moist-c2 is the same physics on the uniform 256x256x80 grid
+(dx = 1 km, dz = 250 m, dt = 5 s, nsound = 10); --workload dry the
+64x64x40 dry warm bubble on the serial-periodic lane (nsound 6);
+--workload ensemble the 64 uneven members.
 
 Inputs are device resident; the step is captured once as a CUDA graph and
 replayed; L2 is flushed (a 256 MiB write) before every timed step, outside
@@ -51,15 +57,15 @@ sys.path.insert(0, str(ROOT))
 METRIC = "cell-updates/s per RK3 step (fwd, adjoint, ensemble) and % of HBM roofline"
 UNIT = "cell-updates/s"
 WORKLOAD = "dry periodic RK3 trajectory, warm bubble 64x64x40 (dx=dy=1 km, dz=500 m, dt=6 s, nsound=6)"
-MOIST_WORKLOAD = ("moist Weisman-Klemp supercell 256x256x80 (dx=dy=1 km, dz=250 m, dt=5 s, nsound=10, Kessler eqtset 2, "
-                  "WENO5 moisture, TKE sgsmodel 1, open-radiative laterals)")
 
 # Algorithmic bytes of one full RK3 large step per cell-update (4-byte
 # words, each compulsory field once read and once written per grid pass):
 # dry, nsound = 6: 3*(8+6) + 20*11 + 2 = 264 words = 1,056 B;
-# moist, nsound = 10: 149 + 20*19 = 529 words = 2,116 B (16 closure/held,
-# 3*(16+23) pre-acoustic and scalar passes, 20 per acoustic small step,
-# 14 Kessler, 2 ppx).
+# moist: 149 + 20 * (small steps) words (16 closure/held, 3*(16+23)
+# pre-acoustic and scalar passes, 20 per acoustic small step, 14 Kessler,
+# 2 ppx): 449 words = 1,796 B at nsound 8 (dt 0.6 s, 15 small steps, the
+# 640x768x80 column), 529 words = 2,116 B at nsound 10 (19 small steps,
+# 256x256x80 and the ensemble).
 STEP_BYTES_PER_CELL = 1056
 MOIST_SMALL_STEPS = 4 + 5 + 10
 MOIST_STEP_BYTES_PER_CELL = 4 * (149 + 20 * MOIST_SMALL_STEPS)
@@ -93,6 +99,8 @@ KERNEL_WORDS_PER_CELL = {
     "tos_column_kernel": 23,
     # in: ppd thv uten vten gxu gyv u v; out: u v
     "tos_pgrad_kernel": 10,
+    # flat column: in ppd thv uten vten u v; out u v
+    "tos_flat_pgrad_kernel": 8,
     # in: ppx ppi ua va wa ppterm piadv c1 c2 rf0 rr0 thv; out: ppd pp3d rru rrv rrw u v w qk pk1 pk2 mm
     "tos_prepare_kernel": 24,
     # in: scalar rru rrv rrw divx rr0 c1 c2; out: tendency
@@ -229,26 +237,60 @@ def run_reference(args) -> None:
     print(json.dumps(line), flush=True)
 
 
-MOIST_GRID = dict(ni=256, nj=256, nk=80, dx=1000.0, dy=1000.0, dz=250.0, dt=5.0, nsound=10)
+# The moist workloads.  "c3": the Weisman-Klemp supercell on the 640x768x80
+# stretched column (dx = dy = 100 m, stretch_z 1 from 20 m at the ground to
+# 500 m aloft under a 20.8 km lid, reference dz 100 m, dt 0.6 s, nsound 8:
+# 3 + 4 + 8 = 15 acoustic small steps, 149 + 20*15 = 449 words = 1,796 B per
+# cell-update), the largest single-GPU configuration and the default.
+# "moist-c2": the same physics on the uniform 256x256x80 grid (dx = 1 km,
+# dz = 250 m, dt 5 s, nsound 10: 19 small steps, 529 words = 2,116 B).
+STRETCH_C3 = dict(ztop_m=20800.0, str_bot_m=200.0, str_top_m=15800.0, dz_bot_m=20.0, dz_top_m=500.0)
+MOIST_WORKLOADS = {
+    "c3": {
+        "grid": dict(ni=640, nj=768, nk=80, dx=100.0, dy=100.0, dz=100.0, dt=0.6, nsound=8),
+        "column": STRETCH_C3,
+        "small_steps": 3 + 4 + 8,
+        "name": ("moist Weisman-Klemp supercell 640x768x80 on a stretched column (dx=dy=100 m, stretch_z=1 dz "
+                 "20-500 m, lid 20.8 km, dt=0.6 s, nsound=8, Kessler eqtset 2, WENO5 moisture, TKE sgsmodel 1, "
+                 "open-radiative laterals, flat terrain_flag=.false. operator family)"),
+        "cpu_subblock": (64, 64, 80),
+    },
+    "moist-c2": {
+        "grid": dict(ni=256, nj=256, nk=80, dx=1000.0, dy=1000.0, dz=250.0, dt=5.0, nsound=10),
+        "column": None,
+        "small_steps": 4 + 5 + 10,
+        "name": ("moist Weisman-Klemp supercell 256x256x80 (dx=dy=1 km, dz=250 m, dt=5 s, nsound=10, Kessler "
+                 "eqtset 2, WENO5 moisture, TKE sgsmodel 1, open-radiative laterals)"),
+        "cpu_subblock": (64, 64, 80),
+    },
+}
 MOIST_INIT = dict(seed=2, bubble_k=3.0, noise_k=0.1, bubble_radius_m=(10000.0, 1500.0), bubble_center_z_m=1500.0)
 # step-start state a user passes in and reads back: the A-level prognostic
 # fields (each copied into its RK-stage twin on the device) and ppx
 MOIST_PROGNOSTIC = ("ua", "va", "wa", "ppi", "tha", "qa", "tkea", "ppx")
 MOIST_STAGE_TWIN = {"ua": "u3d", "va": "v3d", "wa": "w3d", "ppi": "pp3d", "tha": "th3d", "qa": "q3d", "tkea": "tke3d"}
-CPU_SUBBLOCK = (64, 64, 80)
 
 
-def moist_state(ni, nj, nk):
+def moist_step_bytes(workload: str) -> int:
+    """Algorithmic bytes of one moist RK3 large step per cell-update:
+    (149 + 20 * small steps) words."""
+    return 4 * (149 + 20 * MOIST_WORKLOADS[workload]["small_steps"])
+
+
+def moist_state(workload: str, ni=None, nj=None, nk=None):
     """The GPU arm's starting state (the package's builder)."""
-    from gm1_b200.moist_step import MoistStepConfig, weisman_klemp_initial_state
+    from gm1_b200.moist_step import MoistStepConfig, StretchedColumnSpec, weisman_klemp_initial_state
 
-    g = dict(MOIST_GRID, ni=ni, nj=nj, nk=nk)
-    cfg = MoistStepConfig(**g)
+    w = MOIST_WORKLOADS[workload]
+    g = dict(w["grid"])
+    g.update({k: v for k, v in (("ni", ni), ("nj", nj), ("nk", nk)) if v is not None})
+    column = None if w["column"] is None else StretchedColumnSpec(**w["column"])
+    cfg = MoistStepConfig(**g, column=column)
     host, metrics = weisman_klemp_initial_state(cfg, **MOIST_INIT)
     return cfg, host, metrics
 
 
-def moist_state_cpu(ni, nj, nk):
+def moist_state_cpu(workload: str, ni, nj, nk):
     """The CPU arms' starting state, built by the oracle's own initial-state
     restatement (the same words as moist_state; no CUDA library is loaded on
     the CPU baseline or the reference arm)."""
@@ -256,21 +298,24 @@ def moist_state_cpu(ni, nj, nk):
 
     from oracle.moist_initial import weisman_klemp_initial_state
 
-    cfg = SimpleNamespace(**dict(MOIST_GRID, ni=ni, nj=nj, nk=nk, alph=0.60, kdiv=0.10,
-                                 lateral_sides=(2, 2, 2, 2)))
+    w = MOIST_WORKLOADS[workload]
+    column = None if w["column"] is None else SimpleNamespace(**w["column"])
+    cfg = SimpleNamespace(**dict(w["grid"], ni=ni, nj=nj, nk=nk, alph=0.60, kdiv=0.10,
+                                 lateral_sides=(2, 2, 2, 2), column=column))
     cfg.obc = 2 | (2 << 4) | (2 << 8) | (2 << 12)
     host, metrics = weisman_klemp_initial_state(cfg, **MOIST_INIT)
     return cfg, host, metrics
 
 
-def moist_cpu_rate(steps_min: int, seconds_target: float, threads: int, warmup: int = 1) -> tuple[float, int, float]:
+def moist_cpu_rate(workload: str, steps_min: int, seconds_target: float, threads: int,
+                   warmup: int = 1) -> tuple[float, int, float]:
     """The oracle composition on a sub-block of the moist workload on the
     host cores: (cell-updates/s, steps, seconds)."""
     from oracle import periodic as orc
     from oracle.moist_composition import OracleMoistStep
 
     orc.set_threads(threads)
-    cfg, host, metrics = moist_state_cpu(*CPU_SUBBLOCK)
+    cfg, host, metrics = moist_state_cpu(workload, *MOIST_WORKLOADS[workload]["cpu_subblock"])
     o = OracleMoistStep(cfg, host, metrics)
     for _ in range(warmup):
         o.step()
@@ -288,17 +333,23 @@ def run_reference_moist(args) -> None:
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    value, n, dt = moist_cpu_rate(args.steps, 0.0, threads, warmup=args.warmup)
-    ni, nj, nk = CPU_SUBBLOCK
-    sample = (f"{n} moist RK3 large steps of a {ni}x{nj}x{nk} sub-block of the workload (same spacing, dt, "
-              f"nsound and initial state) in {dt:.2f} s after {args.warmup} warm-up steps: the oracle's C "
-              "restatements of the reference CPU twins composed in the large-step schedule")
+    # the ensemble's members run the 1 km physics of configuration 2: its
+    # reference arm is that per-cell rate
+    workload = args.workload if args.workload in MOIST_WORKLOADS else "moist-c2"
+    w = MOIST_WORKLOADS[workload]
+    value, n, dt = moist_cpu_rate(workload, args.steps, 0.0, threads, warmup=args.warmup)
+    ni, nj, nk = w["cpu_subblock"]
+    g = w["grid"]
+    sample = (f"{n} moist RK3 large steps of a {ni}x{nj}x{nk} sub-block of the workload (same column, spacing, "
+              f"dt, nsound and initial state) in {dt:.2f} s after {args.warmup} warm-up steps, on all {threads} "
+              "host threads: the oracle's C restatements of the reference's CPU twins (and, where the reference "
+              "has only CUDA text, of that text) composed in the large-step schedule")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / n,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded Weisman-Klemp supercell start)",
-        "config": {"workload": MOIST_WORKLOAD, "cells": 256 * 256 * 80, "device": "host CPU",
+        "config": {"workload": w["name"], "cells": g["ni"] * g["nj"] * g["nk"], "device": "host CPU",
                    "sample": f"{ni}x{nj}x{nk} sub-block per step"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -344,7 +395,9 @@ def run_moist(args) -> None:
     from gm1_b200.moist_step import MoistLargeStep, upload
 
     rank, world, local, device, barrier, max_over_ranks = _dist_setup()
-    cfg, host, metrics = moist_state(MOIST_GRID["ni"], MOIST_GRID["nj"], MOIST_GRID["nk"])
+    wl = MOIST_WORKLOADS[args.workload]
+    step_bytes = moist_step_bytes(args.workload)
+    cfg, host, metrics = moist_state(args.workload)
     cells = cfg.ni * cfg.nj * cfg.nk
     stream = torch.cuda.Stream(device)
     dev_state, dev_metrics = upload(host, device), upload(metrics, device)
@@ -450,11 +503,12 @@ def run_moist(args) -> None:
     e2e_ms = max_over_ranks(sum(s.elapsed_time(e) for s, e in zip(e_start, e_end)))
     e2e_value = world * cells * args.steps / (e2e_ms * 1e-3)
 
+    status = model.check(current_state=False)  # raises on a failure word of any step taken
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        rate, n, dt = moist_cpu_rate(3, 10.0, threads)
-        ni, nj, nk = CPU_SUBBLOCK
+        rate, n, dt = moist_cpu_rate(args.workload, 3, 10.0, threads)
+        ni, nj, nk = wl["cpu_subblock"]
         cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"{n} moist RK3 large steps of a {ni}x{nj}x{nk} sub-block of the workload in {dt:.2f} s "
                          "(the oracle's C restatements of the reference CPU twins composed in the same schedule)"}
@@ -470,14 +524,16 @@ def run_moist(args) -> None:
         "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded Weisman-Klemp supercell start: isnd 5 column, iwnd 2 hodograph, +3 K bubble, "
                 "U(+-0.1 K) noise from numpy default_rng(2))",
-        "config": {"workload": MOIST_WORKLOAD, "mode": "fwd", "cells": cells, "large_steps_per_timed_step": 1,
-                   "acoustic_small_steps_per_step": MOIST_SMALL_STEPS,
+        "config": {"workload": wl["name"], "mode": "fwd", "cells": cells, "large_steps_per_timed_step": 1,
+                   "acoustic_small_steps_per_step": wl["small_steps"],
                    "l2": "flushed before every timed step (256 MiB write, outside the event pair)",
                    "cuda_graph": use_graph, "lateral_boundaries": "open-radiative (wbc=ebc=sbc=nbc=2)",
                    "parallelism": f"replicas x{world}" if world > 1 else "single domain"},
-        "step_roofline": {"bytes_per_cell_update": MOIST_STEP_BYTES_PER_CELL,
-                          "achieved_gbs": MOIST_STEP_BYTES_PER_CELL * value / world / 1e9,
-                          "frac": MOIST_STEP_BYTES_PER_CELL * value / world / 1e9 / peak},
+        "step_roofline": {"bytes_per_cell_update": step_bytes,
+                          "achieved_gbs": step_bytes * value / world / 1e9,
+                          "frac": step_bytes * value / world / 1e9 / peak},
+        "status": {"max_courant": status["max_courant"], "satadj_nonconverged_cells": status["satadj_nonconverged_cells"],
+                   "max_fall_substeps": status["max_fall_substeps"]},
         "roofline": roofline, "kernel_share": kernel_share,
         "gpu_launches": int(round(launches_per_step * args.steps)),
         "cpu_baseline": cpu,
@@ -599,8 +655,8 @@ def run_ensemble(args) -> None:
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        rate, n, dt = moist_cpu_rate(3, 10.0, threads)
-        ni, nj, nk = CPU_SUBBLOCK
+        rate, n, dt = moist_cpu_rate("moist-c2", 3, 10.0, threads)
+        ni, nj, nk = MOIST_WORKLOADS["moist-c2"]["cpu_subblock"]
         cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"{n} moist RK3 large steps of one {ni}x{nj}x{nk} domain in {dt:.2f} s (per-cell rate of "
                          "the oracle composition; every member runs the same per-cell work)"}
@@ -644,17 +700,17 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=("moist", "dry", "ensemble"), default="moist")
+    ap.add_argument("--workload", choices=("c3", "moist-c2", "dry", "ensemble"), default="c3")
     ap.add_argument("--members", type=int, default=64, help="ensemble members (--workload ensemble)")
     args = ap.parse_args()
     if args.steps is None:
-        args.steps = {"moist": 20, "ensemble": 10}.get(args.workload, 2000)
+        args.steps = {"c3": 20, "moist-c2": 20, "ensemble": 10}.get(args.workload, 2000)
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":
         (run_reference if args.workload == "dry" else run_reference_moist)(args)
         return
-    if args.workload == "moist":
+    if args.workload in MOIST_WORKLOADS:
         run_moist(args)
         return
     if args.workload == "ensemble":
