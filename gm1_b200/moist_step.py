@@ -838,3 +838,139 @@ class MoistLargeStep:
 
 def upload(host: dict[str, np.ndarray], device: torch.device | str = "cuda") -> dict[str, torch.Tensor]:
     return {k: torch.from_numpy(np.ascontiguousarray(v)).to(device) for k, v in host.items()}
+
+
+# ---------------------------------------------------------------------------
+# the same step through the C ABI's whole-step entry point
+# ---------------------------------------------------------------------------
+# gm1b_moist_state, in the header's order (the species scratch of species 1
+# and 2 last)
+NATIVE_STATE_NAMES = (
+    "ua", "u3d", "uten", "rru", "va", "v3d", "vten", "rrv", "wa", "w3d", "wten", "rrw", "fz", "fx", "fy",
+    "ppi", "pp3d", "ppx", "ppd", "piadv", "ppterm", "ppten", "thv", "qk", "pk1", "pk2", "mm", "fpk", "divh", "hadvp",
+    "dum3", "elim_c", "elim_d",
+    "tri_aa", "tri_bb", "tri_cc", "tri_dd", "tri_pivot", "tri_residual",
+    "radbcw", "radbce", "radbcs", "radbcn", "uh", "vh", "ruf", "rvf", "scalar", "dum8", "theta_padded",
+    "moisture_padded",
+    "th3d", "tha", "thterm", "divergence", "theta_div", "divx", "pp3d_c", "prs", "rho", "rr", "kessler_rr", "thheld",
+    "qpten", "qtten", "qvten", "qcten", "theta_adv", "advx", "advy", "advz", "candidate", "temperature", "qt",
+    "thv_c", "qvci", "pi0_3d", "th0_3d", "fall_velocity", "ones_mass",
+    "q3d", "qa", "qheld", "moist_adv",
+    "rf", "nm", "defv", "defh", "tke3d", "tkea", "tketen", "tk", "grdscl", "rgrdscl", "lenscl", "dissten", "cme",
+    "ce1", "ce2", "csm", "kmh", "kmv", "khh", "khv", "tke_workspace",
+    "uc", "vc", "wc", "th0", "pi0", "qv0", "rain", "prate", "ruh", "rvh",
+    "saturation_mask", "asq", "qbudget",
+) + tuple(f"{n}_{r}" for r in (1, 2) for n in ("moisture_padded", "fx", "fy", "fz", "advx", "advy", "advz",
+                                                 "candidate"))
+NATIVE_METRIC_NAMES = METRIC_NAMES + ("mh_profile", "mf_profile", "rho0_padded")
+
+
+class _NativeState(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_void_p) for n in NATIVE_STATE_NAMES]
+
+
+class _NativeMetrics(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_void_p) for n in NATIVE_METRIC_NAMES]
+
+
+class _NativeConfig(ctypes.Structure):
+    _fields_ = [("ni", ctypes.c_int32), ("nj", ctypes.c_int32), ("nk", ctypes.c_int32), ("dx", ctypes.c_float),
+                ("dy", ctypes.c_float), ("dz", ctypes.c_float), ("dt", ctypes.c_float), ("nsound", ctypes.c_int32),
+                ("alph", ctypes.c_float), ("kdiv", ctypes.c_float), ("lateral_sides", ctypes.c_int32 * 4),
+                ("stretched", ctypes.c_int32), ("concurrent", ctypes.c_int32)]
+
+
+def _native_lib():
+    lib = _native.lib()
+    if not getattr(lib, "_mls_bound", False):
+        c = ctypes
+        lib.gm1b_moist_step_create.argtypes = [c.POINTER(_NativeConfig), c.POINTER(_NativeState),
+                                               c.POINTER(_NativeMetrics), c.POINTER(c.c_void_p)]
+        lib.gm1b_moist_step_create.restype = c.c_int32
+        lib.gm1b_moist_large_step.argtypes = [c.c_void_p, c.c_void_p]
+        lib.gm1b_moist_large_step.restype = c.c_int32
+        lib.gm1b_moist_step_status.argtypes = [c.c_void_p, c.POINTER(c.c_int32), c.c_int32, c.c_void_p]
+        lib.gm1b_moist_step_status.restype = c.c_int32
+        lib.gm1b_moist_step_destroy.argtypes = [c.c_void_p]
+        lib.gm1b_moist_step_destroy.restype = c.c_int32
+        lib._mls_bound = True
+    return lib
+
+
+class NativeMoistLargeStep:
+    """The composed moist large step through the C ABI's whole-step entry
+    point (gm1b_moist_step_create / gm1b_moist_large_step): one library call
+    per step, the same launches in the same order as MoistLargeStep, so the
+    two leave the same words.  ``state`` and ``metrics`` are the device dicts
+    MoistLargeStep takes; the scratch of moisture species 1 and 2 is
+    allocated here (zero), everything else is the caller's."""
+
+    def __init__(self, cfg: MoistStepConfig, state: dict[str, torch.Tensor], metrics: dict[str, torch.Tensor], *,
+                 stream: Any | None = None, concurrent: bool = True) -> None:
+        self.cfg, self.s, self.m, self.stream = cfg, state, metrics, stream
+        self.scratch = {f"{n}_{r}": torch.zeros_like(state[n]) for r in (1, 2) for n in SPECIES_SCRATCH}
+        arrays = {**state, **self.scratch}
+        missing = [n for n in NATIVE_STATE_NAMES if n not in arrays]
+        if missing:
+            raise ValueError(f"missing moist-step arrays: {', '.join(missing)}")
+        for n in NATIVE_STATE_NAMES:
+            t = arrays[n]
+            if not (isinstance(t, torch.Tensor) and t.is_cuda and t.is_contiguous()):
+                raise ValueError(f"{n} must be a contiguous CUDA tensor")
+        self._state = _NativeState(**{n: arrays[n].data_ptr() for n in NATIVE_STATE_NAMES})
+        self._metrics = _NativeMetrics(**{n: (metrics[n].data_ptr() if n in metrics else None)
+                                          for n in NATIVE_METRIC_NAMES})
+        self._config = _NativeConfig(cfg.ni, cfg.nj, cfg.nk, cfg.dx, cfg.dy, cfg.dz, cfg.dt, cfg.nsound,
+                                     float(np.float32(cfg.alph)), float(np.float32(cfg.kdiv)),
+                                     (ctypes.c_int32 * 4)(*cfg.lateral_sides), 1 if cfg.stretched else 0,
+                                     1 if concurrent else 0)
+        lib = _native_lib()
+        handle = ctypes.c_void_p()
+        with torch.cuda.device(state["u3d"].device):
+            _native.check(lib.gm1b_moist_step_create(ctypes.byref(self._config), ctypes.byref(self._state),
+                                                     ctypes.byref(self._metrics), ctypes.byref(handle)),
+                          "gm1b_moist_step_create")
+        self._handle = handle
+        self.completed_steps = 0
+
+    def _st(self):
+        dev = self.s["u3d"].device
+        return torch.cuda.current_stream(dev) if self.stream is None else self.stream
+
+    def step(self) -> None:
+        _native.check(_native_lib().gm1b_moist_large_step(self._handle, ctypes.c_void_p(self._st().cuda_stream)),
+                      "gm1b_moist_large_step")
+        self.completed_steps += 1
+
+    def status(self, *, reset: bool = False) -> tuple[int, dict[str, Any]]:
+        out = (ctypes.c_int32 * 8)()
+        rc = _native_lib().gm1b_moist_step_status(self._handle, out, 1 if reset else 0,
+                                                  ctypes.c_void_p(self._st().cuda_stream))
+        if rc < 0:
+            _native.check(rc, "gm1b_moist_step_status")
+        words = np.array(out[:], np.int32)
+        return rc, {"satadj_nonconverged_cells": int(words[0]), "max_fall_substeps": int(words[1]),
+                    "blown_up_fall_columns": int(words[2]),
+                    "max_courant": float(words[3:4].view(np.float32)[0]) if words[4] else None,
+                    "courant_samples": int(words[4]), "kessler_samples": int(words[5])}
+
+    def check(self) -> dict[str, Any]:
+        """Refuse as the reference does (SatadjNonConvergence, CourantStop)
+        on the failure words folded over every step taken."""
+        rc, out = self.status()
+        if rc == 1:
+            raise SatadjNonConvergence(f"GM1 Kessler satadj failed to converge ({out})")
+        if rc == 2:
+            raise CourantStop(f"the advective Courant number {out['max_courant']!r} reached CM1's stop value")
+        return out
+
+    def close(self) -> None:
+        if getattr(self, "_handle", None):
+            _native_lib().gm1b_moist_step_destroy(self._handle)
+            self._handle = None
+
+    def __del__(self) -> None:
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001 - interpreter shutdown
+            pass

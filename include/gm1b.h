@@ -947,6 +947,109 @@ typedef struct gm1b_kernel_stat {
 GM1B_API int32_t gm1b_profiler_enable(int32_t on);
 GM1B_API int32_t gm1b_profiler_collect(gm1b_kernel_stat *out, int32_t capacity, int32_t *count);
 
+/* ------------------------------------------------------------------------
+ * The whole moist RK3 large step behind one entry point.
+ *
+ * Every array of the composed state, device pointers in this order (the
+ * arrays of the step's Python mirror, gm1_b200.moist_step.moist_state_shapes):
+ * padded winds u/v (nk+2, nj+6, ni+7 / nj+7, ni+6) and w (nk+3, nj+6, ni+6)
+ * with their tendencies, mass fluxes and scratch fluxes; the pressure-lane
+ * arrays (nk+2, nj+2, ni+2) and the six column diagnostics (one word each);
+ * the radiation histories and boundary profiles; the padded scalars
+ * (nk+2, nj+6, ni+6); the mass fields (nk, nj, ni); q3d/qa (6, nk, nj, ni),
+ * qheld/moist_adv (3, nk, nj, ni); the face fields (nk+1, nj, ni); the
+ * compact winds uc (nk, nj, ni+1), vc (nk, nj+1, ni), wc (nk+1, nj, ni); the
+ * base profiles th0/pi0/qv0 (nk); rain (1, nj, ni), prate (nj, ni); ruh
+ * (ni), rvh (nj); saturation_mask (uint8, mass); asq (3) and qbudget (10)
+ * FP64; and the scratch of moisture species 1 and 2 (each padded scalar,
+ * fx, fy, fz, advx, advy, advz, candidate), which lets the three species
+ * advect concurrently (species 0 uses the state's own).  The caller owns
+ * every array.
+ * ---------------------------------------------------------------------- */
+typedef struct gm1b_moist_state {
+    float *ua, *u3d, *uten, *rru, *va, *v3d, *vten, *rrv, *wa, *w3d, *wten, *rrw, *fz, *fx, *fy;
+    float *ppi, *pp3d, *ppx, *ppd, *piadv, *ppterm, *ppten, *thv, *qk, *pk1, *pk2, *mm, *fpk, *divh, *hadvp, *dum3,
+        *elim_c, *elim_d;
+    float *tri_aa, *tri_bb, *tri_cc, *tri_dd, *tri_pivot, *tri_residual;
+    float *radbcw, *radbce, *radbcs, *radbcn, *uh, *vh, *ruf, *rvf, *scalar, *dum8, *theta_padded, *moisture_padded;
+    float *th3d, *tha, *thterm, *divergence, *theta_div, *divx, *pp3d_c, *prs, *rho, *rr, *kessler_rr, *thheld, *qpten,
+        *qtten, *qvten, *qcten, *theta_adv, *advx, *advy, *advz, *candidate, *temperature, *qt, *thv_c, *qvci,
+        *pi0_3d, *th0_3d, *fall_velocity, *ones_mass;
+    float *q3d, *qa, *qheld, *moist_adv;
+    float *rf, *nm, *defv, *defh, *tke3d, *tkea, *tketen, *tk, *grdscl, *rgrdscl, *lenscl, *dissten, *cme, *ce1,
+        *ce2, *csm, *kmh, *kmv, *khh, *khv, *tke_workspace;
+    float *uc, *vc, *wc, *th0, *pi0, *qv0, *rain, *prate, *ruh, *rvh;
+    uint8_t *saturation_mask;
+    double *asq, *qbudget;
+    float *moisture_padded_1, *fx_1, *fy_1, *fz_1, *advx_1, *advy_1, *advz_1, *candidate_1;
+    float *moisture_padded_2, *fx_2, *fy_2, *fz_2, *advx_2, *advy_2, *advz_2, *candidate_2;
+} gm1b_moist_state;
+
+/* The metrics: the 25 terrain metrics of the padded lane (flat: gz = 1,
+ * zero slopes) and, for a stretched column, its mh (nk+2) and mf (nk+3)
+ * profiles (CM1-indexed) and the padded base density (nk+2, nj+6, ni+6);
+ * the last three may be NULL on a uniform column. */
+typedef struct gm1b_moist_metrics {
+    const float *terrain_msl, *zh, *zf, *mh, *rmh, *mf, *rmf, *c1, *c2, *rho0_3d, *rr0, *rf0, *rrf0, *gz, *rgz, *gzu,
+        *rgzu, *gzv, *rgzv, *dzdx, *dzdy, *gx, *gxu, *gy, *gyv;
+    const float *mh_profile, *mf_profile, *rho0_padded;
+} gm1b_moist_metrics;
+
+/* dz: the uniform layer depth, or a stretched column's reference dz
+ * (rdz = 1/dz).  lateral_sides: CM1's wbc, ebc, sbc, nbc.  stretched = 1
+ * selects the flat (terrain_flag=.false.) operator family on the column the
+ * metrics describe.  concurrent = 1 runs each RK stage's scalar, boundary and
+ * TKE work on side streams (the same words as concurrent = 0). */
+typedef struct gm1b_moist_step_config {
+    int32_t ni, nj, nk;
+    float dx, dy, dz, dt;
+    int32_t nsound;
+    float alph, kdiv;
+    int32_t lateral_sides[4];
+    int32_t stretched;
+    int32_t concurrent;
+} gm1b_moist_step_config;
+
+typedef struct gm1b_moist_step gm1b_moist_step;
+
+/*
+ * Bind a composed moist step to a device state.  The handle keeps the
+ * pointers (the arrays stay the caller's), creates the side streams and
+ * events of the concurrent stage tail, and allocates its own small device
+ * words: the Kessler workspace (gm1b_kessler_workspace_bytes), the folded
+ * status words and the Courant reduction's scratch.  Call with the state's
+ * device current.  Replaces the construction of CudaCartesianRuntime
+ * (src/cm1core/cuda_cartesian_runtime.py) for this step's phases.
+ */
+GM1B_API int32_t gm1b_moist_step_create(const gm1b_moist_step_config *config, const gm1b_moist_state *state,
+                                        const gm1b_moist_metrics *metrics, gm1b_moist_step **out);
+
+/*
+ * One moist RK3 large step on `stream` in the reference's large-step
+ * schedule (StepPhase / large_step_schedule, src/cm1core/gm1_runtime.py:
+ * 611-627, :1969-2007; CartesianBackend.execute, :2010-2014): closure and
+ * held tendencies, three RK stages of pre-acoustic, acoustic, post-acoustic,
+ * scalar/moisture, boundaries and TKE, the Kessler transition and solve3;
+ * the step's failure words (satadj non-convergence, blown-up fall columns,
+ * the advective Courant number of the state entering the step) are folded
+ * on the device.  No host synchronisation and no allocation: the step can
+ * be captured in a CUDA graph on `stream`.
+ */
+GM1B_API int32_t gm1b_moist_large_step(gm1b_moist_step *step, void *stream);
+
+/* The folded failure words of every step since creation (or the last
+ * reset), after waiting for `stream`: out[0] non-converged satadj cells,
+ * out[1] largest fallout sub-step count, out[2] blown-up fall columns,
+ * out[3] the largest Courant number (float bits), out[4] Courant samples,
+ * out[5] Kessler samples.  Returns GM1B_STATUS_SATADJ (1) or
+ * GM1B_STATUS_COURANT (2) when the reference would refuse the run
+ * (cuda_cartesian_finish.py:638-639; gm1_runtime.py:518-549), else 0. */
+#define GM1B_STATUS_SATADJ 1
+#define GM1B_STATUS_COURANT 2
+GM1B_API int32_t gm1b_moist_step_status(gm1b_moist_step *step, int32_t *out, int32_t reset, void *stream);
+
+GM1B_API int32_t gm1b_moist_step_destroy(gm1b_moist_step *step);
+
 #ifdef __cplusplus
 }
 #endif

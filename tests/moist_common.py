@@ -22,12 +22,13 @@ FIELDS = ("u3d", "v3d", "w3d", "th3d", "pp3d", "qv", "qc", "qr", "tke3d")
 SHORT_BARS = {"u3d": (5.0e-5, 2.0e-6), "v3d": (1.0e-4, 3.0e-6), "w3d": (3.0e-4, 7.0e-6), "th3d": (8.0e-4, 2.0e-5),
               "pp3d": (1.0e-3, 3.0e-5), "qv": (3.0e-5, 4.0e-7), "qc": (2.0e-2, 3.0e-4), "qr": (7.0e-6, 2.0e-7),
               "tke3d": (3.0e-4, 7.0e-6)}
-# Worst over 60 steps of a convective start: the ulp differences grow as the
-# flow does and branch switches (saturation, TKE clipping, upwind choices)
-# flip single cells, so the max norm is far looser than the RMS.
-LONG_BARS = {"u3d": (3.0e-3, 1.0e-4), "v3d": (5.0e-3, 2.0e-4), "w3d": (3.0e-2, 8.0e-4), "th3d": (3.0e-3, 2.0e-4),
-             "pp3d": (3.0e-2, 4.0e-3), "qv": (7.0e-5, 4.0e-6), "qc": (1.5e-1, 2.0e-3), "qr": (1.5e-4, 6.0e-6),
-             "tke3d": (9.5e-1, 8.0e-3)}
+# Over 60 steps of a convective start the ulp differences grow as the flow
+# does and branch switches (saturation, TKE clipping, upwind choices) flip
+# single cells.  The oracle itself spreads as far when its own input is
+# moved by one ulp, so long runs are judged against that spread: the GPU's
+# worst error over the run may be at most SPREAD_FACTOR times the oracle's
+# worst spread under a one-ulp change of theta' (plus SHORT_BARS as a floor).
+SPREAD_FACTOR = 3.0
 
 
 def _host(x):
@@ -57,3 +58,24 @@ def format_errors(err) -> str:
 def check_errors(err, bars: dict[str, tuple[float, float]], what: str) -> None:
     bad = {n: e for n, e in err.items() if not (e[0] <= bars[n][0] and e[1] <= bars[n][1])}
     assert not bad, f"{what}: {format_errors(bad)} above {({n: bars[n] for n in bad})}"
+
+
+def ulp_perturbed(host: dict[str, np.ndarray]) -> dict[str, np.ndarray]:
+    """A copy of a starting state with theta' (and its A-level twin) moved up
+    by one ulp in every cell."""
+    h = {k: v.copy() for k, v in host.items()}
+    h["th3d"] = np.nextafter(h["th3d"], np.float32(np.inf)).astype(np.float32)
+    h["tha"][:] = h["th3d"]
+    return h
+
+
+def check_against_spread(err, spread, what: str) -> None:
+    """Every field's worst error within SPREAD_FACTOR times the oracle's own
+    one-ulp spread, with SHORT_BARS as the floor."""
+    bars = {n: (SPREAD_FACTOR * spread[n][0] + SHORT_BARS[n][0], SPREAD_FACTOR * spread[n][1] + SHORT_BARS[n][1])
+            for n in FIELDS}
+    check_errors(err, bars, what)
+
+
+def worst(a, b):
+    return {n: (max(a[n][0], b[n][0]), max(a[n][1], b[n][1])) for n in FIELDS}

@@ -46,6 +46,33 @@ def test_struct_field_order_matches_header_and_oracle():
     assert orc.NAMES == ALL_ARRAY_NAMES
 
 
+def _header_fields(name: str) -> list[str]:
+    text = (ROOT / "include" / "gm1b.h").read_text()
+    body = text[text.index(f"typedef struct {name} {{"):text.index(f"}} {name};")]
+    body = re.sub(r"/\*.*?\*/", "", body[body.index("{") + 1:], flags=re.S)
+    return re.findall(r"\*\s*(\w+)", body)
+
+
+def test_whole_step_struct_order_matches_header():
+    """gm1b_moist_state / gm1b_moist_metrics field order of the header and
+    the Python binding of the whole-step entry point, and the config layout."""
+    from gm1_b200.moist_step import NATIVE_METRIC_NAMES, NATIVE_STATE_NAMES, _NativeConfig
+
+    assert _header_fields("gm1b_moist_state") == list(NATIVE_STATE_NAMES)
+    assert _header_fields("gm1b_moist_metrics") == list(NATIVE_METRIC_NAMES)
+    assert ctypes.sizeof(_NativeConfig) == 4 * (3 + 4 + 1 + 2 + 4 + 2)
+
+
+def test_whole_step_entry_rejects_bad_arguments_without_a_device():
+    from gm1_b200.moist_step import _native_lib
+
+    lib = _native_lib()
+    handle = ctypes.c_void_p()
+    assert lib.gm1b_moist_step_create(None, None, None, ctypes.byref(handle)) == _native.GM1B_ERR_ARGUMENT
+    assert lib.gm1b_moist_large_step(None, None) == _native.GM1B_ERR_ARGUMENT
+    assert b"NULL" in lib.gm1b_last_error()
+
+
 def test_schedule_matches_reference_table():
     lib = _native.lib()
     for dt, nsound, nrk, nloop, dts in load_json("schedule.json"):
