@@ -392,7 +392,7 @@ def run_moist(args) -> None:
     import torch.distributed as dist
 
     from gm1_b200 import _native
-    from gm1_b200.moist_step import MoistLargeStep, upload
+    from gm1_b200.moist_step import NativeMoistLargeStep, upload
 
     rank, world, local, device, barrier, max_over_ranks = _dist_setup()
     wl = MOIST_WORKLOADS[args.workload]
@@ -401,8 +401,10 @@ def run_moist(args) -> None:
     cells = cfg.ni * cfg.nj * cfg.nk
     stream = torch.cuda.Stream(device)
     dev_state, dev_metrics = upload(host, device), upload(metrics, device)
+    # the step through the library's whole-step C entry point
+    # (gm1b_moist_large_step): one call per step, captured once as a graph
     with torch.cuda.stream(stream):
-        model = MoistLargeStep(cfg, dev_state, dev_metrics, stream=stream)
+        model = NativeMoistLargeStep(cfg, dev_state, dev_metrics, stream=stream)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
@@ -450,15 +452,15 @@ def run_moist(args) -> None:
     # run operation by operation on one stream: the profiler's event pairs
     # time each launch alone only when launches do not overlap
     nprof = min(args.steps, 5)
-    model.concurrent = False
+    sequential = NativeMoistLargeStep(cfg, dev_state, dev_metrics, stream=stream, concurrent=False)
     _native.profiler_enable(True)
     with torch.cuda.stream(stream):
         for _ in range(nprof):
             flush.zero_()
-            model.step()
+            sequential.step()
     stream.synchronize()
     _native.profiler_enable(False)
-    model.concurrent = True
+    sequential.close()
     stats = _native.profiler_collect()
     launches_per_step = sum(s["launches"] for s in stats) / nprof
     top = stats[0]
@@ -469,7 +471,7 @@ def run_moist(args) -> None:
     traffic = None
     tfile = ROOT / "profiles" / "traffic_per_launch.json"
     if tfile.exists():
-        traffic = json.loads(tfile.read_text()).get(top["name"])
+        traffic = json.loads(tfile.read_text()).get(args.workload, {}).get(top["name"])
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": None if achieved is None else achieved / peak, "traffic": traffic, "kernel": top["name"],
                 "avg_launch_ms": avg_ms, "alg_bytes_per_launch": None if words is None else words * 4 * cells,
@@ -477,7 +479,8 @@ def run_moist(args) -> None:
     tot = sum(x["total_ms"] for x in stats)
     kernel_share = {s["name"]: round(s["total_ms"] / tot, 4) for s in stats[:16]}
 
-    # ---- e2e: prognostic fields in from pinned host memory, out after ----
+    # ---- e2e: prognostic fields in from pinned host memory, the step
+    # through the C ABI, the fields out again, all inside the event pair ----
     pinned = {n: torch.from_numpy(host[n]).pin_memory() for n in MOIST_PROGNOSTIC}
     with torch.cuda.stream(stream):
         for n, t in pinned.items():
@@ -495,7 +498,7 @@ def run_moist(args) -> None:
                 dev_state[n].copy_(t, non_blocking=True)
             for n, twin in MOIST_STAGE_TWIN.items():
                 dev_state[twin].copy_(dev_state[n])
-            step()
+            model.step()  # the C-ABI call itself (gm1b_moist_large_step), not a graph replay
             for n, t in pinned.items():
                 t.copy_(dev_state[n], non_blocking=True)
             e_end[q].record(stream)
@@ -503,7 +506,7 @@ def run_moist(args) -> None:
     e2e_ms = max_over_ranks(sum(s.elapsed_time(e) for s, e in zip(e_start, e_end)))
     e2e_value = world * cells * args.steps / (e2e_ms * 1e-3)
 
-    status = model.check(current_state=False)  # raises on a failure word of any step taken
+    status = model.check()  # raises on a failure word of any step taken
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -513,6 +516,7 @@ def run_moist(args) -> None:
                "sample": f"{n} moist RK3 large steps of a {ni}x{nj}x{nk} sub-block of the workload in {dt:.2f} s "
                          "(the oracle's C restatements of the reference CPU twins composed in the same schedule)"}
     del graph
+    model.close()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -528,6 +532,7 @@ def run_moist(args) -> None:
                    "acoustic_small_steps_per_step": wl["small_steps"],
                    "l2": "flushed before every timed step (256 MiB write, outside the event pair)",
                    "cuda_graph": use_graph, "lateral_boundaries": "open-radiative (wbc=ebc=sbc=nbc=2)",
+                   "entry_point": "gm1b_moist_large_step (one C-ABI call per step, captured as a CUDA graph)",
                    "parallelism": f"replicas x{world}" if world > 1 else "single domain"},
         "step_roofline": {"bytes_per_cell_update": step_bytes,
                           "achieved_gbs": step_bytes * value / world / 1e9,
@@ -554,7 +559,7 @@ def _kernel_roofline(stats, cells_per_launch_unit: float, peak: float, peak_kind
     traffic = None
     tfile = ROOT / "profiles" / "traffic_per_launch.json"
     if tfile.exists():
-        traffic = json.loads(tfile.read_text()).get(top["name"])
+        traffic = json.loads(tfile.read_text()).get("ensemble", {}).get(top["name"])
     return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": None if achieved is None else achieved / peak, "traffic": traffic, "kernel": top["name"],
             "avg_launch_ms": avg_ms, "alg_bytes_per_launch": alg, "peak_source": f"{peak_kind} hbm_gbs"}
@@ -819,7 +824,7 @@ def main() -> None:
     traffic = None
     tfile = ROOT / "profiles" / "traffic_per_launch.json"
     if tfile.exists():
-        traffic = json.loads(tfile.read_text()).get(top["name"])
+        traffic = json.loads(tfile.read_text()).get("dry", {}).get(top["name"])
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic, "kernel": top["name"], "avg_launch_ms": avg_ms,
                 "alg_bytes_per_launch": alg_bytes, "peak_source": f"{peak_kind} hbm_gbs"}
