@@ -2,7 +2,7 @@
 """Throughput of the RK3 large step on B200: cell-updates/s.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                    [--workload c3|moist-c2|dry|ensemble]
+                    [--workload c3|moist-c2|dry|ensemble|adjoint]
 
 Default workload (c3): the Weisman-Klemp supercell start on 640x768x80 cells
 (39.3 M) of a vertically stretched column (dx = dy = 100 m, stretch_z 1 from
@@ -19,7 +19,8 @@ advection), the Kessler transition and solve3, through the library's C ABI.
 --workload moist-c2 is the same physics on the uniform 256x256x80 grid
 (dx = 1 km, dz = 250 m, dt = 5 s, nsound = 10); --workload dry the
 64x64x40 dry warm bubble on the serial-periodic lane (nsound 6);
---workload ensemble the 64 uneven members.
+--workload ensemble the 64 uneven members; --workload adjoint the gradient
+of the warm-rain transport model on the 96x96x48 supercell (t_adj/t_fwd).
 
 Inputs are device resident; the step is captured once as a CUDA graph and
 replayed; L2 is flushed (a 256 MiB write) before every timed step, outside
@@ -698,6 +699,240 @@ def run_ensemble(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+# Configuration 4: the adjoint.  The warm-rain transport model of
+# gm1_b200.adjoint (theta', qv, qc, qr under RK3 WENO5 transport by frozen
+# mass fluxes, then collection and the single-pass saturation adjustment),
+# linearised about a Weisman-Klemp supercell spun up for ADJOINT_SPINUP
+# large steps of the full moist model on the 96x96x48 grid; J = the
+# domain's condensate sum(rho0 (qc + qr)) at the end of the window.
+ADJOINT_GRID = dict(ni=96, nj=96, nk=48, dx=1000.0, dy=1000.0, dz=300.0, dt=5.0, nsound=6)
+ADJOINT_SPINUP = 10
+ADJOINT_INIT = dict(seed=4, bubble_k=3.0, noise_k=0.1, bubble_radius_m=(10000.0, 1500.0), bubble_center_z_m=1500.0)
+# forward words per cell-update: per scalar and RK stage the transport reads
+# s_prev, s_0, rru, rrv, rrw, divx, rr0, c1, c2 and writes s_new (10 words,
+# 4 scalars x 3 stages), the Kessler pieces read theta', qv, qc, qr, th0,
+# pi0, pp3d, prs and write theta', qv, qc, qr (12): 132 words.  The adjoint
+# step is 3 x that (one forward recompute from the checkpoint, the reverse
+# reading the primal and the adjoint and writing the adjoint).
+ADJOINT_FWD_WORDS = 4 * 3 * 10 + 12
+ADJOINT_WORDS = 3 * ADJOINT_FWD_WORDS
+KERNEL_WORDS_PER_CELL.update({
+    # in: scalar rru rrv rrw c1 c2 rr0 divx tendency-adjoint; out: scalar-adjoint
+    "scalar_advection5_adjoint_kernel": 10,
+    # in: th0 pi0 pp3d prs th3d qv qc g_th g_qv g_qc; out: g_th g_qv g_qc
+    "satadj1_adjoint_kernel": 13,
+})
+
+
+def adjoint_case(device):
+    """Frozen flow and state of the adjoint workload on ``device``."""
+    import torch
+
+    from gm1_b200.adjoint import FrozenFlow
+    from gm1_b200.moist_step import MoistStepConfig, NativeMoistLargeStep, upload, weisman_klemp_initial_state
+    from gm1_b200.scalar_rk import moisture_weps_f64, theta_weps_f64
+
+    g = ADJOINT_GRID
+    cfg = MoistStepConfig(**g)
+    host, metrics = weisman_klemp_initial_state(cfg, **ADJOINT_INIT)
+    model = NativeMoistLargeStep(cfg, upload(host, device), upload(metrics, device))
+    for _ in range(ADJOINT_SPINUP):
+        model.step()
+    model.check()
+    s, m = model.s, model.m
+    ni, nj, nk = g["ni"], g["nj"], g["nk"]
+    fields = {n: s[n].clone() for n in ("rru", "rrv", "rrw", "divx", "prs")}
+    fields.update({n: m[n].clone() for n in ("c1", "c2", "rr0", "gz")})
+    fields["th0"], fields["pi0"] = s["th0_3d"].clone(), s["pi0_3d"].clone()
+    fields["pp3d"] = s["pp3d"][1:nk + 1, 1:nj + 1, 1:ni + 1].contiguous()
+    flow = FrozenFlow(ni, nj, nk, g["dx"], g["dy"], g["dz"], theta_weps_f64(), fields)
+    state = (s["th3d"].clone(), s["q3d"][0].clone(), s["q3d"][1].clone(), s["q3d"][2].clone())
+    weps = {"th3d": theta_weps_f64(), "qv": moisture_weps_f64(0), "qc": moisture_weps_f64(1),
+            "qr": moisture_weps_f64(2)}
+    rho0 = m["rho0_3d"].clone()
+    weights = (torch.zeros_like(rho0), torch.zeros_like(rho0), rho0, rho0)
+    model.close()
+    return flow, state, weps, weights
+
+
+def adjoint_cpu_rate(seconds_target: float, threads: int) -> tuple[float, str]:
+    """The binary64 restatement's gradient (torch autograd on the host
+    cores) on a 32x32x48 sub-block of the workload's grid with a synthetic
+    frozen flow, one large step per gradient."""
+    import numpy as np
+    import torch
+
+    from oracle import adjoint_f64 as f64
+
+    torch.set_num_threads(threads)
+    ni, nj, nk = 32, 32, ADJOINT_GRID["nk"]
+    rng = np.random.default_rng(4)
+    t = lambda a: torch.from_numpy(np.asarray(a, np.float64))  # noqa: E731
+    fr = {"rru": t(rng.uniform(-5, 15, (nk + 2, nj + 6, ni + 7))), "rrv": t(rng.uniform(-5, 15, (nk + 2, nj + 7, ni + 6))),
+          "rrw": t(rng.uniform(-1, 1, (nk + 3, nj + 6, ni + 6))), "c1": t(np.full((nk + 1, nj, ni), 0.5)),
+          "c2": t(np.full((nk + 1, nj, ni), 0.5)), "rr0": t(np.ones((nk, nj, ni))), "gz": t(np.ones((nj, ni))),
+          "divx": t(np.zeros((nk, nj, ni))), "th0": t(np.full((nk, nj, ni), 300.0)),
+          "pi0": t(np.full((nk, nj, ni), 0.95)), "pp3d": t(np.zeros((nk, nj, ni))),
+          "prs": t(np.full((nk, nj, ni), 8.5e4))}
+    state = {"th3d": t(rng.uniform(-1, 1, (nk, nj, ni))), "qv": t(rng.uniform(0.005, 0.015, (nk, nj, ni))),
+             "qc": t(rng.uniform(0, 2e-3, (nk, nj, ni))), "qr": t(rng.uniform(0, 2e-3, (nk, nj, ni)))}
+    kw = dict(ni=ni, nj=nj, nk=nk, dt=ADJOINT_GRID["dt"], dx=ADJOINT_GRID["dx"], dy=ADJOINT_GRID["dy"],
+              dz=ADJOINT_GRID["dz"], weps=1e-6, steps=1)
+    n, t0 = 0, time.perf_counter()
+    while True:
+        x = {k: v.clone().requires_grad_(True) for k, v in state.items()}
+        out = f64.warm_rain_transport(x, fr, **kw)
+        torch.autograd.grad((out["qc"] + out["qr"]).sum(), list(x.values()))
+        n += 1
+        dt = time.perf_counter() - t0
+        if dt >= seconds_target or n >= 20:
+            break
+    return ni * nj * nk * n / dt, f"{n} one-step gradients of a {ni}x{nj}x{nk} sub-block in {dt:.2f} s"
+
+
+def run_reference_adjoint(args) -> None:
+    """The reference has no adjoint: its arm times the binary64 restatement
+    of the same composition (oracle/adjoint_f64.py) on the host cores."""
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    threads = os.cpu_count() or 1
+    value, sample = adjoint_cpu_rate(max(5.0, 2.0 * args.steps), threads)
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0, "steps": args.steps,
+        "warmup": args.warmup, "higher_is_better": True, "dtype": "f64",
+        "config": {"workload": ADJOINT_NAME, "device": "host CPU", "note": "the reference has no adjoint"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+ADJOINT_NAME = ("adjoint of the warm-rain transport (theta', qv, qc, qr: RK3 WENO5 transport by frozen mass fluxes, "
+                "collection, single-pass satadj) about a Weisman-Klemp supercell spun up 10 large steps on 96x96x48 "
+                "(dx=dy=1 km, dz=300 m, dt=5 s); J = sum(rho0 (qc + qr)) at the window's end")
+
+
+def run_adjoint(args) -> None:
+    """Forward sweep storing each large-step boundary, then the reverse sweep
+    (recompute one step from its checkpoint, pull the adjoint back through
+    the adjoint kernels), every step timed alone with L2 flushed before it."""
+    import torch
+    import torch.distributed as dist
+
+    from gm1_b200 import _native
+    from gm1_b200.adjoint import WarmRainTransport
+
+    rank, world, local, device, barrier, max_over_ranks = _dist_setup()
+    flow, state0, weps, weights = adjoint_case(device)
+    model = WarmRainTransport(flow, ADJOINT_GRID["dt"], weps=weps, checkpoint=True)
+    cells = flow.ni * flow.nj * flow.nk
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
+    model.gradient(state0, weights, args.warmup)
+    torch.cuda.synchronize(device)
+
+    def sweep(k: int, fwd_ev, rev_ev):
+        ckpt = [state0]
+        with torch.no_grad():
+            for q in range(k):
+                flush.zero_()
+                fwd_ev[q][0].record()
+                ckpt.append(model.step(*ckpt[-1]))
+                fwd_ev[q][1].record()
+        adj = weights
+        for q in reversed(range(k)):
+            flush.zero_()
+            rev_ev[q][0].record()
+            adj = model.vjp_step(ckpt[q], adj)
+            rev_ev[q][1].record()
+        return adj
+
+    ev = lambda: [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))  # noqa: E731
+                  for _ in range(args.steps)]
+    fwd_ev, rev_ev = ev(), ev()
+    sampler = ClockSampler(local)
+    barrier()
+    sampler.start()
+    grads = sweep(args.steps, fwd_ev, rev_ev)
+    barrier()
+    clocks = sampler.stop()
+    t_fwd = max_over_ranks(sum(a.elapsed_time(b) for a, b in fwd_ev))
+    t_rev = max_over_ranks(sum(a.elapsed_time(b) for a, b in rev_ev))
+    t_adj = t_fwd + t_rev
+    value = world * cells * args.steps / (t_adj * 1e-3)
+    # the same window through torch.utils.checkpoint gives the same words
+    _, ref = model.gradient(state0, weights, args.steps)
+    same = all(torch.equal(a, b) for a, b in zip(grads, ref))
+
+    # per-kernel device time of one reverse step (launch profiler)
+    _native.profiler_enable(True)
+    with torch.no_grad():
+        nxt = model.step(*state0)
+    model.vjp_step(state0, weights)
+    torch.cuda.synchronize(device)
+    _native.profiler_enable(False)
+    stats = _native.profiler_collect()
+    del nxt
+    launches = sum(x["launches"] for x in stats)
+    peak, peak_kind = load_peaks()
+    roofline = _kernel_roofline(stats, cells, peak, peak_kind)
+    tot = sum(x["total_ms"] for x in stats)
+    kernel_share = {x["name"]: round(x["total_ms"] / tot, 4) for x in stats[:12]}
+
+    # e2e: the initial state in from pinned host memory and the gradient out,
+    # around the whole gradient call
+    pinned_in = [t.cpu().pin_memory() for t in state0]
+    pinned_out = [torch.empty_like(t) for t in pinned_in]
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    flush.zero_()
+    e0.record()
+    dev_in = tuple(t.to(device, non_blocking=True) for t in pinned_in)
+    _, g = model.gradient(dev_in, weights, args.steps)
+    for o, x in zip(pinned_out, g):
+        o.copy_(x, non_blocking=True)
+    e1.record()
+    barrier()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1))
+    e2e_value = world * cells * args.steps / (e2e_ms * 1e-3)
+    h2d = sum(t.numel() * 4 for t in pinned_in)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        rate, sample = adjoint_cpu_rate(10.0, threads)
+        cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": sample + " (the binary64 torch restatement of the same composition, autograd)"}
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_adj / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32",
+        "data": f"synthetic (seeded Weisman-Klemp start, numpy default_rng({ADJOINT_INIT['seed']}), spun up "
+                f"{ADJOINT_SPINUP} steps by the moist model)",
+        "config": {"workload": ADJOINT_NAME, "mode": "adjoint", "cells": cells,
+                   "checkpoints": "every large step (forward sweep stores each boundary; the reverse recomputes "
+                                  "one step from it)",
+                   "t_fwd_ms_per_step": t_fwd / args.steps, "t_rev_ms_per_step": t_rev / args.steps,
+                   "t_adj_over_t_fwd": t_adj / t_fwd, "target_t_adj_over_t_fwd": 3.0,
+                   "stepwise_equals_torch_checkpoint": same,
+                   "l2": "flushed before every timed large step, forward and reverse (256 MiB write, outside the "
+                         "event pair)",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single domain"},
+        "step_roofline": {"bytes_per_cell_update": 4 * ADJOINT_WORDS,
+                          "achieved_gbs": 4 * ADJOINT_WORDS * value / world / 1e9,
+                          "frac": 4 * ADJOINT_WORDS * value / world / 1e9 / peak},
+        "roofline": roofline, "kernel_share": kernel_share,
+        "gpu_launches": int(launches * args.steps),
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d // args.steps,
+                "d2h_bytes_per_step": h2d // args.steps},
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -705,15 +940,21 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=("c3", "moist-c2", "dry", "ensemble"), default="c3")
+    ap.add_argument("--workload", choices=("c3", "moist-c2", "dry", "ensemble", "adjoint"), default="c3")
     ap.add_argument("--members", type=int, default=64, help="ensemble members (--workload ensemble)")
     args = ap.parse_args()
     if args.steps is None:
-        args.steps = {"c3": 20, "moist-c2": 20, "ensemble": 10}.get(args.workload, 2000)
+        args.steps = {"c3": 20, "moist-c2": 20, "ensemble": 10, "adjoint": 10}.get(args.workload, 2000)
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":
+        if args.workload == "adjoint":
+            run_reference_adjoint(args)
+            return
         (run_reference if args.workload == "dry" else run_reference_moist)(args)
+        return
+    if args.workload == "adjoint":
+        run_adjoint(args)
         return
     if args.workload in MOIST_WORKLOADS:
         run_moist(args)

@@ -948,6 +948,84 @@ GM1B_API int32_t gm1b_profiler_enable(int32_t on);
 GM1B_API int32_t gm1b_profiler_collect(gm1b_kernel_stat *out, int32_t capacity, int32_t *count);
 
 /* ------------------------------------------------------------------------
+ * Adjoint (reverse-mode) kernels.  The reference has no adjoint; these are
+ * the transposes of this library's forward operators, for gradients of a
+ * scalar objective J with respect to the state.
+ * ---------------------------------------------------------------------- */
+typedef struct gm1b_scalar_advection5_adjoint_arrays {
+    /* the forward's inputs (padded scalar, mass fluxes, metrics, divx) */
+    const float *scalar, *rru, *rrv, *rrw, *c1, *c2, *rr0, *gz, *divx;
+    /* dJ/d tendency (nk, nj, ni) in; dJ/d scalar (padded) out */
+    const float *tendency_adjoint;
+    float *scalar_adjoint;
+} gm1b_scalar_advection5_adjoint_arrays;
+
+/*
+ * dJ/d scalar of gm1b_scalar_advection5's tendency (the whole-domain
+ * operator, lateral_obc != 0) with the mass fluxes held fixed: every padded
+ * scalar word receives the sum over the faces whose stencils read it of
+ * (face adjoint) * (mass flux) * d(reconstruction)/d(word), plus its
+ * divergence and open-side terms.  The WENO-Z weights are differentiated at
+ * their epsilon-regularised form (subgradient 0 for |b1 - b3| at b1 = b3
+ * and beyond the 1e30 cap), upstrpd by its active limiter branch.  One
+ * gather per word, no atomics.  Differentiates cpu_scalar_advection5_inplace
+ * (src/cm1core/cuda_advection5.py:440) / cm1_adv5_scalar_tendency_v1 (:669).
+ */
+GM1B_API int32_t gm1b_scalar_advection5_adjoint(int32_t ni, int32_t nj, int32_t nk,
+                                                const gm1b_scalar_advection5_adjoint_arrays *arrays, int32_t nrk,
+                                                int32_t wflag, float dx, float dy, float dz, double weps,
+                                                uint32_t lateral_obc, void *stream);
+
+/* The transpose of gm1b_open_fill's scalar kind (bcs on open sides,
+ * src/cm1core/cuda_sound3_open_boundary.py:249-335), in place on a padded
+ * adjoint: each halo word's adjoint folds onto the edge word it copied, the
+ * halo words become zero. */
+GM1B_API int32_t gm1b_open_fill_scalar_adjoint(int32_t ni, int32_t nj, int32_t nk, float *q, void *stream);
+
+/*
+ * One tridiagonal solve per column (columns independent; level k of every
+ * column at word k*columns + col): a(k) x(k-1) + b(k) x(k) + c(k) x(k+1) =
+ * d(k), a(0) and c(n-1) unused; transposed = 1 solves A^T x = d (the adjoint
+ * of the acoustic column's vertically implicit w-pi' solve,
+ * cpu_sound3_periodic_stage_inplace, src/cm1core/cuda_sound3_periodic.py:
+ * 824-1027: dJ/dd = A^-T dJ/dx).  work: n*columns words.
+ */
+GM1B_API int32_t gm1b_tridiagonal_solve(int32_t n, size_t columns, const float *a, const float *b, const float *c,
+                                        const float *d, float *x, float *work, int32_t transposed, void *stream);
+
+/*
+ * Kessler collection in place: autoconversion max(0.001(qc - 0.001), 0) dt
+ * and accretion 2.2 qc qr^0.875 dt, limited to the available qc, moved from
+ * qc to qr (the first part of the local conversion of
+ * cpu_gm1_kessler_local_inplace, src/cm1core/cuda_gm1_kessler_local.py:251).
+ * qc, qr >= 0, the reference's own precondition (with qc < 0 the limiter
+ * divides 0 by 0).  The adjoint takes the forward's inputs qc, qr and dJ/d(outputs) in gc, gr,
+ * and overwrites gc, gr with dJ/d(inputs); it takes the subgradient 0 at
+ * the autoconversion switch qc = 0.001 and at qr = 0.
+ */
+GM1B_API int32_t gm1b_kessler_collection(size_t cells, float *qc, float *qr, float dt, void *stream);
+GM1B_API int32_t gm1b_kessler_collection_adjoint(size_t cells, const float *qc, const float *qr, float *gc, float *gr,
+                                                 float dt, void *stream);
+
+/*
+ * Single-pass saturation adjustment, in place (the equation-set-1 branch of
+ * the Kessler operator's _cpu_satadj, src/cm1core/cuda_gm1_kessler_driver.py:
+ * 337-428): at the frozen pressure prs and Exner pi0 + pp3d, one step
+ * dqv = (qvs - qv) / (1 + L qvs 17.67 243.5 / (cp (T - 29.65)^2)), floored
+ * so that qv stays >= 1e-20 and limited to the cloud water; qv += dqv,
+ * qc -= dqv, th3d -= dqv L / (cp pi).  All arrays `cells` words.  The adjoint
+ * takes the forward's inputs and dJ/d(outputs) in g_th, g_qv, g_qc, and
+ * overwrites them with dJ/d(inputs), each limiter differentiated as the
+ * branch the binary32 forward took (the saturation switch: the cloud-water
+ * limit's subgradient is the unlimited branch's at equality).
+ */
+GM1B_API int32_t gm1b_satadj1(size_t cells, const float *th0, const float *pi0, const float *pp3d, const float *prs,
+                              float *th3d, float *qv, float *qc, void *stream);
+GM1B_API int32_t gm1b_satadj1_adjoint(size_t cells, const float *th0, const float *pi0, const float *pp3d,
+                                      const float *prs, const float *th3d, const float *qv, const float *qc,
+                                      float *g_th, float *g_qv, float *g_qc, void *stream);
+
+/* ------------------------------------------------------------------------
  * The whole moist RK3 large step behind one entry point.
  *
  * Every array of the composed state, device pointers in this order (the

@@ -1104,10 +1104,79 @@ def make_vertical(reference: Path) -> None:
     (HERE / "vertical_levels.json").write_text(json.dumps(out, indent=1, sort_keys=True))
 
 
+WARM_RAIN_CASES = {"warm_rain_8x6x5": (8, 6, 5, 20.0, 51), "warm_rain_7x9x6": (7, 9, 6, 6.0, 52)}
+
+
+def warm_rain_fixture(ni: int, nj: int, nk: int, seed: int, saturation: tuple[float, float]) -> dict[str, np.ndarray]:
+    """Compact Kessler inputs for the collection and single-pass adjustment
+    pins: qv at saturation * U(saturation), cloud water on both sides of the
+    autoconversion threshold 0.001 and some cells without, rain from none to
+    heavy enough for the qc limiter."""
+    rng = np.random.default_rng(seed)
+    rd, cp, p00, dz = 287.04, 1005.7, 1.0e5, 400.0
+    z = (np.arange(nk) + 0.5) * dz
+    shape = (nk, nj, ni)
+
+    def bc(x):
+        return np.broadcast_to(x[:, None, None], shape).astype(np.float32).copy()
+
+    a = {
+        "ruh": (1.0 + 0.01 * rng.standard_normal(ni)).astype(np.float32),
+        "rvh": (1.0 + 0.01 * rng.standard_normal(nj)).astype(np.float32),
+        "rmh": (1.0 + 0.02 * rng.random(shape)).astype(np.float32),
+        "pi0": bc(1.0 - 9.81 * z / (cp * 302.0)),
+        "th0": bc(300.0 + 0.004 * z),
+        "th3d": rng.uniform(-1.5, 2.5, shape).astype(np.float32),
+        "pp3d": rng.uniform(-2e-4, 2e-4, shape).astype(np.float32),
+    }
+    t = (a["th0"] + a["th3d"]) * (a["pi0"] + a["pp3d"])
+    prs = p00 * (a["pi0"] + a["pp3d"]).astype(np.float64) ** (cp / rd)
+    a["prs"] = prs.astype(np.float32)
+    a["rho"] = (prs / (rd * t)).astype(np.float32)
+    a["rr"] = a["rho"].copy()
+    esl = 611.2 * np.exp(17.67 * (t - 273.15) / (t - 29.65))
+    qvs = 0.622 * esl / (prs - esl)
+    a["qv"] = (qvs * rng.uniform(*saturation, shape)).astype(np.float32)
+    u = rng.random(shape)
+    a["qc"] = np.where(u < 0.2, 0.0, np.where(u < 0.6, rng.uniform(1e-5, 9.5e-4, shape),
+                                              rng.uniform(1.05e-3, 3e-3, shape))).astype(np.float32)
+    u = rng.random(shape)
+    a["qr"] = np.where(u < 0.3, 0.0, np.where(u < 0.8, rng.uniform(1e-6, 2e-3, shape),
+                                              rng.uniform(8e-3, 2e-2, shape))).astype(np.float32)
+    return a
+
+
+def make_warm_rain(reference: Path) -> None:
+    """The two Kessler pieces the adjoint differentiates, through the
+    reference's own CPU code: cpu_gm1_kessler_local_inplace on supersaturated
+    cells (no rain evaporation, so its qc and qr are the collection's), and
+    the driver's _cpu_satadj with equation set 1 on cells from 85% to 115% of
+    saturation."""
+    sys.path.insert(0, str(reference / "src"))
+    import cm1core.cuda_gm1_kessler_driver as drv
+    from cm1core.cuda_gm1_kessler_local import cpu_gm1_kessler_local_inplace
+
+    for tag, (ni, nj, nk, dt, seed) in WARM_RAIN_CASES.items():
+        a = warm_rain_fixture(ni, nj, nk, seed, (1.01, 1.2))
+        a["budget"] = np.zeros(3, np.float64)
+        inputs = {f"in_coll_{k}": v.copy() for k, v in a.items()}
+        cpu_gm1_kessler_local_inplace(a, ni=ni, nj=nj, nk=nk, dx=1000.0, dy=1000.0, dz=400.0, dt=dt)
+        outputs = {f"out_coll_{k}": a[k].copy() for k in ("qv", "qc", "qr", "th3d")}
+        b = warm_rain_fixture(ni, nj, nk, seed + 100, (0.85, 1.15))
+        b["qbudget"] = np.zeros(10, np.float64)
+        inputs.update({f"in_sat_{k}": v.copy() for k, v in b.items()})
+        drv._cpu_satadj(np, b, ni=ni, nj=nj, nk=nk, dx=np.float32(1000.0), dy=np.float32(1000.0),
+                        dz=np.float32(400.0), dt=np.float32(dt), equation_set=1)
+        outputs.update({f"out_sat_{k}": b[k].copy() for k in ("th3d", "qv", "qc", "rho")})
+        meta = dict(ni=ni, nj=nj, nk=nk, dt=dt)
+        np.savez_compressed(HERE / f"{tag}.npz", meta=json.dumps(meta), **inputs, **outputs)
+        print("wrote", tag)
+
+
 def main() -> None:
     p = argparse.ArgumentParser()
     p.add_argument("--reference", type=Path, required=True, help="root of the reference source tree")
-    p.add_argument("what", choices=("small", "c1", "advection", "kessler", "tke", "rk", "bridge", "wk", "limits", "closure", "tkeevo", "momentum", "terrainopen", "kesslerstep", "fills", "vertical"))
+    p.add_argument("what", choices=("small", "c1", "advection", "kessler", "tke", "rk", "bridge", "wk", "limits", "closure", "tkeevo", "momentum", "terrainopen", "kesslerstep", "fills", "vertical", "warmrain"))
     p.add_argument("--checkpoints", type=int, nargs="+", default=[1])
     args = p.parse_args()
     if args.what == "small":
@@ -1138,6 +1207,8 @@ def main() -> None:
         make_kessler_large_step(args.reference)
     elif args.what == "fills":
         make_fills(args.reference)
+    elif args.what == "warmrain":
+        make_warm_rain(args.reference)
     elif args.what == "vertical":
         make_vertical(args.reference)
     else:
