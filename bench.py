@@ -702,12 +702,14 @@ def run_ensemble(args) -> None:
 # Configuration 4: the adjoint.  The warm-rain transport model of
 # gm1_b200.adjoint (theta', qv, qc, qr under RK3 WENO5 transport by frozen
 # mass fluxes, then collection and the single-pass saturation adjustment),
-# linearised about a Weisman-Klemp supercell spun up for ADJOINT_SPINUP
-# large steps of the full moist model on the 96x96x48 grid; J = the
-# domain's condensate sum(rho0 (qc + qr)) at the end of the window.
+# linearised about a Weisman-Klemp supercell (warm bubble with cloud and
+# rain water in its core) spun up for ADJOINT_SPINUP large steps of the full
+# moist model on the 96x96x48 grid; J = the domain's condensate
+# sum(rho0 (qc + qr)) at the end of the window.
 ADJOINT_GRID = dict(ni=96, nj=96, nk=48, dx=1000.0, dy=1000.0, dz=300.0, dt=5.0, nsound=6)
-ADJOINT_SPINUP = 10
-ADJOINT_INIT = dict(seed=4, bubble_k=3.0, noise_k=0.1, bubble_radius_m=(10000.0, 1500.0), bubble_center_z_m=1500.0)
+ADJOINT_SPINUP = 60
+ADJOINT_INIT = dict(seed=4, bubble_k=3.0, noise_k=0.1, bubble_radius_m=(10000.0, 1500.0), bubble_center_z_m=1500.0,
+                    bubble_cloud=1.0e-3, bubble_rain=5.0e-4)
 # forward words per cell-update: per scalar and RK stage the transport reads
 # s_prev, s_0, rru, rrv, rrw, divx, rr0, c1, c2 and writes s_new (10 words,
 # 4 scalars x 3 stages), the Kessler pieces read theta', qv, qc, qr, th0,
@@ -717,8 +719,14 @@ ADJOINT_INIT = dict(seed=4, bubble_k=3.0, noise_k=0.1, bubble_radius_m=(10000.0,
 ADJOINT_FWD_WORDS = 4 * 3 * 10 + 12
 ADJOINT_WORDS = 3 * ADJOINT_FWD_WORDS
 KERNEL_WORDS_PER_CELL.update({
-    # in: scalar rru rrv rrw c1 c2 rr0 divx tendency-adjoint; out: scalar-adjoint
-    "scalar_advection5_adjoint_kernel": 10,
+    # the advection adjoint's two passes; the 18 face-coefficient words per
+    # cell that pass 1 writes and pass 2 reads are scratch, not counted
+    # in: carrier rru rrv rrw c1 c2 rr0 tendency-adjoint
+    "advection_adjoint_faces_kernel": 8,
+    # in: tendency-adjoint rr0 divx accumulate; out: scalar-adjoint
+    "advection_adjoint_gather_compact_kernel": 5,
+    # in: scalar; out: carrier
+    "scalar_carrier_open_kernel": 2,
     # in: th0 pi0 pp3d prs th3d qv qc g_th g_qv g_qc; out: g_th g_qv g_qc
     "satadj1_adjoint_kernel": 13,
 })
@@ -807,7 +815,8 @@ def run_reference_adjoint(args) -> None:
 
 
 ADJOINT_NAME = ("adjoint of the warm-rain transport (theta', qv, qc, qr: RK3 WENO5 transport by frozen mass fluxes, "
-                "collection, single-pass satadj) about a Weisman-Klemp supercell spun up 10 large steps on 96x96x48 "
+                "collection, single-pass satadj) about a Weisman-Klemp supercell (cloudy bubble core) spun up 60 large "
+                "steps (300 s) on 96x96x48 "
                 "(dx=dy=1 km, dz=300 m, dt=5 s); J = sum(rho0 (qc + qr)) at the window's end")
 
 
@@ -819,58 +828,84 @@ def run_adjoint(args) -> None:
     import torch.distributed as dist
 
     from gm1_b200 import _native
-    from gm1_b200.adjoint import WarmRainTransport
+    from gm1_b200.adjoint import StepGraphs, WarmRainTransport
+    from gm1_b200.autotune import Autotuner
 
     rank, world, local, device, barrier, max_over_ranks = _dist_setup()
     flow, state0, weps, weights = adjoint_case(device)
-    model = WarmRainTransport(flow, ADJOINT_GRID["dt"], weps=weps, checkpoint=True)
+    tuner = Autotuner()
+    model = WarmRainTransport(flow, ADJOINT_GRID["dt"], weps=weps, checkpoint=True, tuner=tuner)
     cells = flow.ni * flow.nj * flow.nk
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
     model.gradient(state0, weights, args.warmup)
+    graphs = StepGraphs(model, state0)
+    graphs.gradient(state0, weights, args.warmup)
     torch.cuda.synchronize(device)
 
+    x0, w0 = StepGraphs.stack(state0), StepGraphs.stack(weights)
+    # the window's checkpoint store, laid out once (64 words per cell-step)
+    store = graphs.store(args.steps)
+
     def sweep(k: int, fwd_ev, rev_ev):
-        ckpt = [state0]
-        with torch.no_grad():
-            for q in range(k):
-                flush.zero_()
-                fwd_ev[q][0].record()
-                ckpt.append(model.step(*ckpt[-1]))
-                fwd_ev[q][1].record()
-        adj = weights
+        inputs, saved = [x0], []
+        for q in range(k):
+            flush.zero_()
+            fwd_ev[q][0].record()
+            saved.append(graphs.forward(inputs[-1], store[q]))
+            fwd_ev[q][1].record()
+            inputs.append(saved[-1][:4])
+        adj = w0
         for q in reversed(range(k)):
             flush.zero_()
             rev_ev[q][0].record()
-            adj = model.vjp_step(ckpt[q], adj)
+            adj = graphs.reverse(inputs[q], saved[q], adj)
             rev_ev[q][1].record()
-        return adj
+        return tuple(adj[q] for q in range(4))
+
+    def plain_forward(k: int, ev_):
+        cur = x0
+        for q in range(k):
+            flush.zero_()
+            ev_[q][0].record()
+            cur = graphs.step(cur)
+            ev_[q][1].record()
 
     ev = lambda: [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))  # noqa: E731
                   for _ in range(args.steps)]
-    fwd_ev, rev_ev = ev(), ev()
+    fwd_ev, rev_ev, plain_ev = ev(), ev(), ev()
     sampler = ClockSampler(local)
     barrier()
     sampler.start()
     grads = sweep(args.steps, fwd_ev, rev_ev)
+    plain_forward(args.steps, plain_ev)
     barrier()
     clocks = sampler.stop()
-    t_fwd = max_over_ranks(sum(a.elapsed_time(b) for a, b in fwd_ev))
+    t_save = max_over_ranks(sum(a.elapsed_time(b) for a, b in fwd_ev))
     t_rev = max_over_ranks(sum(a.elapsed_time(b) for a, b in rev_ev))
-    t_adj = t_fwd + t_rev
+    t_fwd = max_over_ranks(sum(a.elapsed_time(b) for a, b in plain_ev))
+    t_adj = t_save + t_rev
     value = world * cells * args.steps / (t_adj * 1e-3)
-    # the same window through torch.utils.checkpoint gives the same words
+    # the same window eagerly through autograd and torch.utils.checkpoint
     _, ref = model.gradient(state0, weights, args.steps)
-    same = all(torch.equal(a, b) for a, b in zip(grads, ref))
+    rel = {n: float((a.double() - b.double()).norm() / max(float(b.double().norm()), 1e-300))
+           for n, a, b in zip(("th3d", "qv", "qc", "qr"), grads, ref)}
+    finite = {n: bool(torch.isfinite(a).all()) for n, a in zip(("th3d", "qv", "qc", "qr"), grads)}
+    finite_ref = {n: bool(torch.isfinite(b).all()) for n, b in zip(("th3d", "qv", "qc", "qr"), ref)}
+    norms = {n: float(a.double().norm()) for n, a in zip(("th3d", "qv", "qc", "qr"), grads)}
+    cloudy = int((state0[2] > 0).sum())
 
-    # per-kernel device time of one reverse step (launch profiler)
+    # per-kernel device time of one stage-saving step and its reverse
+    # (launch profiler, eager launches)
+    from gm1_b200.adjoint import StageCheckpointedAdjoint
+
+    sc = StageCheckpointedAdjoint(model)
     _native.profiler_enable(True)
-    with torch.no_grad():
-        nxt = model.step(*state0)
-    model.vjp_step(state0, weights)
+    _, stages = sc.forward(state0)
+    sc.reverse(stages, weights)
     torch.cuda.synchronize(device)
     _native.profiler_enable(False)
     stats = _native.profiler_collect()
-    del nxt
+    del stages
     launches = sum(x["launches"] for x in stats)
     peak, peak_kind = load_peaks()
     roofline = _kernel_roofline(stats, cells, peak, peak_kind)
@@ -886,7 +921,7 @@ def run_adjoint(args) -> None:
     flush.zero_()
     e0.record()
     dev_in = tuple(t.to(device, non_blocking=True) for t in pinned_in)
-    _, g = model.gradient(dev_in, weights, args.steps)
+    g = graphs.gradient(dev_in, weights, args.steps, store)
     for o, x in zip(pinned_out, g):
         o.copy_(x, non_blocking=True)
     e1.record()
@@ -894,6 +929,7 @@ def run_adjoint(args) -> None:
     e2e_ms = max_over_ranks(e0.elapsed_time(e1))
     e2e_value = world * cells * args.steps / (e2e_ms * 1e-3)
     h2d = sum(t.numel() * 4 for t in pinned_in)
+    del graphs
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -912,11 +948,19 @@ def run_adjoint(args) -> None:
         "data": f"synthetic (seeded Weisman-Klemp start, numpy default_rng({ADJOINT_INIT['seed']}), spun up "
                 f"{ADJOINT_SPINUP} steps by the moist model)",
         "config": {"workload": ADJOINT_NAME, "mode": "adjoint", "cells": cells,
-                   "checkpoints": "every large step (forward sweep stores each boundary; the reverse recomputes "
-                                  "one step from it)",
-                   "t_fwd_ms_per_step": t_fwd / args.steps, "t_rev_ms_per_step": t_rev / args.steps,
+                   "checkpoints": "every RK-stage boundary (the forward sweep keeps each scalar's stage states; "
+                                  "the reverse rebuilds only each stage's open-filled carrier)",
+                   "cuda_graphs": "plain step, stage-saving step and one-step reverse each replayed from one graph",
+                   "checkpoint_store_bytes": store.numel() * 4,
+                   "t_adj": "forward sweep with stage saves + reverse sweep; t_fwd: the plain forward step",
+                   "levels_per_chunk": {"fifth_order": model.chunk[1], "weno5": model.chunk[3]},
+                   "autotune_ms": tuner.table,
+                   "t_fwd_ms_per_step": t_fwd / args.steps, "t_forward_sweep_ms_per_step": t_save / args.steps,
+                   "t_reverse_sweep_ms_per_step": t_rev / args.steps,
                    "t_adj_over_t_fwd": t_adj / t_fwd, "target_t_adj_over_t_fwd": 3.0,
-                   "stepwise_equals_torch_checkpoint": same,
+                   "relative_l2_vs_autograd_checkpoint_path": rel, "gradient_finite": finite,
+                   "autograd_gradient_finite": finite_ref, "gradient_l2_norms": norms,
+                   "cloudy_cells_at_start": cloudy,
                    "l2": "flushed before every timed large step, forward and reverse (256 MiB write, outside the "
                          "event pair)",
                    "parallelism": f"replicas x{world}" if world > 1 else "single domain"},
@@ -944,7 +988,7 @@ def main() -> None:
     ap.add_argument("--members", type=int, default=64, help="ensemble members (--workload ensemble)")
     args = ap.parse_args()
     if args.steps is None:
-        args.steps = {"c3": 20, "moist-c2": 20, "ensemble": 10, "adjoint": 10}.get(args.workload, 2000)
+        args.steps = {"c3": 20, "moist-c2": 20, "ensemble": 10, "adjoint": 120}.get(args.workload, 2000)
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":

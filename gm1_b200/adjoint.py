@@ -5,11 +5,13 @@ model they serve.
 The reference has no adjoint.  What is differentiated here is this library's
 own forward operators, each with its adjoint kernel:
 
-  advection_tendency   pack + open fill (bcs, src/cm1core/cuda_sound3_open_boundary.py:
-                       249-335) + the whole-domain fifth-order / WENO5 tendency
+  advection_tendency   the open-filled carrier (pack + bcs, src/cm1core/
+                       cuda_sound3_open_boundary.py:249-335, one launch) + the
+                       whole-domain fifth-order / WENO5 tendency
                        (cpu_scalar_advection5_inplace, src/cm1core/cuda_advection5.py:
-                       440), mass fluxes frozen; adjoint gm1b_scalar_advection5_adjoint
-                       then gm1b_open_fill_scalar_adjoint
+                       440), mass fluxes frozen; adjoint
+                       gm1b_scalar_advection5_adjoint_open (face coefficients,
+                       then a gather that folds the fill's transpose)
   kessler_collection   autoconversion + accretion with the qc limiter
                        (cpu_gm1_kessler_local_inplace, src/cm1core/cuda_gm1_kessler_local.py:
                        251); adjoint gm1b_kessler_collection_adjoint
@@ -44,7 +46,7 @@ import torch.utils.checkpoint
 
 from . import _native
 from .advection import launch_cuda_scalar_advection5, padded_shapes
-from .moist_ops import open_fill, pack_scalar
+from .autotune import Autotuner
 from .periodic import rk_stage_dt_f32
 
 NG = 3
@@ -64,16 +66,25 @@ def _lib() -> ctypes.CDLL:
     if not getattr(lib, "_adjoint_bound", False):
         i32, f32, vp, sz = ctypes.c_int32, ctypes.c_float, ctypes.c_void_p, ctypes.c_size_t
         lib.gm1b_scalar_advection5_adjoint.argtypes = [i32, i32, i32, ctypes.POINTER(_AdjArrays), i32, i32, f32, f32,
-                                                       f32, ctypes.c_double, ctypes.c_uint32, vp]
+                                                       f32, ctypes.c_double, ctypes.c_uint32, vp, vp]
+        lib.gm1b_scalar_advection5_adjoint_open.argtypes = [i32, i32, i32, ctypes.POINTER(_AdjArrays), i32, i32, f32,
+                                                            f32, f32, ctypes.c_double, f32, vp, vp, vp, vp]
+        lib.gm1b_scalar_advection5_adjoint_workspace_bytes.argtypes = [i32, i32, i32]
+        lib.gm1b_scalar_advection5_adjoint_workspace_bytes.restype = sz
+        lib.gm1b_scalar_carrier_open.argtypes = [i32, i32, i32, vp, vp, vp]
+        ptr4 = ctypes.POINTER(vp)
+        lib.gm1b_warm_rain_cell.argtypes = [sz, vp, vp, vp, vp, ptr4, ptr4, f32, vp]
+        lib.gm1b_warm_rain_cell_adjoint.argtypes = [sz, vp, vp, vp, vp, ptr4, ptr4, ptr4, f32, vp]
         lib.gm1b_open_fill_scalar_adjoint.argtypes = [i32, i32, i32, vp, vp]
         lib.gm1b_tridiagonal_solve.argtypes = [i32, sz, vp, vp, vp, vp, vp, vp, i32, vp]
         lib.gm1b_kessler_collection.argtypes = [sz, vp, vp, f32, vp]
         lib.gm1b_kessler_collection_adjoint.argtypes = [sz, vp, vp, vp, vp, f32, vp]
         lib.gm1b_satadj1.argtypes = [sz] + [vp] * 7 + [vp]
         lib.gm1b_satadj1_adjoint.argtypes = [sz] + [vp] * 10 + [vp]
-        for n in ("gm1b_scalar_advection5_adjoint", "gm1b_open_fill_scalar_adjoint", "gm1b_tridiagonal_solve",
+        for n in ("gm1b_scalar_advection5_adjoint", "gm1b_scalar_advection5_adjoint_open", "gm1b_scalar_carrier_open",
+                  "gm1b_open_fill_scalar_adjoint", "gm1b_tridiagonal_solve",
                   "gm1b_kessler_collection", "gm1b_kessler_collection_adjoint", "gm1b_satadj1",
-                  "gm1b_satadj1_adjoint"):
+                  "gm1b_satadj1_adjoint", "gm1b_warm_rain_cell", "gm1b_warm_rain_cell_adjoint"):
             getattr(lib, n).restype = i32
         lib._adjoint_bound = True
     return lib
@@ -123,69 +134,99 @@ LATERAL_OPEN = (2, 2, 2, 2)
 OBC_OPEN = 0x2222
 
 
-def _tendency(flow: FrozenFlow, padded: torch.Tensor, nrk: int, weps: float) -> torch.Tensor:
+def _tendency(flow: FrozenFlow, padded: torch.Tensor, nrk: int, weps: float, chunk: int | None = None) -> torch.Tensor:
     f = flow.fields
     ten = torch.empty((flow.nk, flow.nj, flow.ni), dtype=torch.float32, device=padded.device)
     launch_cuda_scalar_advection5(
         padded, {n: f[n] for n in FLUX_NAMES}, {n: f[n] for n in ("c1", "c2", "rr0", "gz")}, f["divx"], ten, None,
         ni=flow.ni, nj=flow.nj, nk=flow.nk, nrk=nrk, dx=flow.dx, dy=flow.dy, dz=flow.dz, weps=weps,
-        lateral_sides=LATERAL_OPEN, write_fluxes=False)
+        lateral_sides=LATERAL_OPEN, write_fluxes=False, levels_per_chunk=chunk)
     return ten
 
 
 def _carrier(flow: FrozenFlow, scalar: torch.Tensor) -> torch.Tensor:
+    """The compact scalar in its open-filled padded carrier (one launch)."""
     ni, nj, nk = flow.ni, flow.nj, flow.nk
-    padded = torch.zeros(padded_shapes(ni, nj, nk)["scalar"], dtype=torch.float32, device=scalar.device)
-    pack_scalar(scalar, padded, ni=ni, nj=nj, nk=nk)
-    open_fill(padded, "scalar", ni=ni, nj=nj, nk=nk)
+    padded = torch.empty(padded_shapes(ni, nj, nk)["scalar"], dtype=torch.float32, device=scalar.device)
+    _native.check(_lib().gm1b_scalar_carrier_open(ni, nj, nk, _ptr(scalar, "scalar"), padded.data_ptr(),
+                                                  _stream(scalar.device)), "gm1b_scalar_carrier_open")
     return padded
 
 
-def advection_tendency_adjoint(flow: FrozenFlow, padded: torch.Tensor, tendency_adjoint: torch.Tensor,
-                               nrk: int, *, weps: float | None = None, fill_transpose: bool = True) -> torch.Tensor:
-    """dJ/d(compact scalar) for dJ/d(tendency): the advection adjoint on the
-    filled carrier, the open-fill transpose, then the interior.  With
-    ``fill_transpose=False``: dJ/d(carrier word), the whole padded array."""
-    ni, nj, nk = flow.ni, flow.nj, flow.nk
+def _adjoint_arrays(flow: FrozenFlow, scalar: torch.Tensor, lam: torch.Tensor, out: torch.Tensor) -> _AdjArrays:
     f = flow.fields
+    return _AdjArrays(scalar=_ptr(scalar, "scalar"), rru=f["rru"].data_ptr(), rrv=f["rrv"].data_ptr(),
+                      rrw=f["rrw"].data_ptr(), c1=f["c1"].data_ptr(), c2=f["c2"].data_ptr(), rr0=f["rr0"].data_ptr(),
+                      gz=f["gz"].data_ptr(), divx=f["divx"].data_ptr(), tendency_adjoint=_ptr(lam, "tendency_adjoint"),
+                      scalar_adjoint=out.data_ptr())
+
+
+def _workspace(flow: FrozenFlow, device) -> torch.Tensor:
+    n = _lib().gm1b_scalar_advection5_adjoint_workspace_bytes(flow.ni, flow.nj, flow.nk) // 4
+    return torch.empty(n, dtype=torch.float32, device=device)
+
+
+def advection_tendency_adjoint(flow: FrozenFlow, scalar: torch.Tensor, tendency_adjoint: torch.Tensor, nrk: int, *,
+                               weps: float | None = None, scale: float = 1.0,
+                               accumulate: torch.Tensor | None = None,
+                               running_sum: torch.Tensor | None = None) -> torch.Tensor:
+    """dJ/d(compact scalar) for dJ/d(tendency) = scale * tendency_adjoint, the
+    tendency taken on the compact scalar's open-filled carrier (the carrier
+    is read through the fill's index map; a face-coefficient pass, then one
+    gather per compact cell that folds the fill's transpose), plus
+    ``accumulate`` when given; with ``running_sum`` the result comes back
+    bare and running_sum receives accumulate + result."""
+    ni, nj, nk = flow.ni, flow.nj, flow.nk
+    lam = tendency_adjoint.contiguous()
+    out = torch.empty((nk, nj, ni), dtype=torch.float32, device=scalar.device)
+    a = _adjoint_arrays(flow, scalar.contiguous(), lam, out)
+    work = _workspace(flow, scalar.device)
+    _native.check(_lib().gm1b_scalar_advection5_adjoint_open(
+        ni, nj, nk, ctypes.byref(a), nrk, 1, flow.dx, flow.dy, flow.dz, flow.weps if weps is None else weps, scale,
+        None if accumulate is None else _ptr(accumulate, "accumulate"),
+        None if running_sum is None else _ptr(running_sum, "running_sum"), work.data_ptr(), _stream(scalar.device)),
+        "gm1b_scalar_advection5_adjoint_open")
+    return out
+
+
+def advection_carrier_adjoint(flow: FrozenFlow, padded: torch.Tensor, tendency_adjoint: torch.Tensor, nrk: int, *,
+                              weps: float | None = None) -> torch.Tensor:
+    """dJ/d(carrier word), the whole padded (nk+2, nj+6, ni+6) array, for
+    dJ/d(tendency) of the tendency on the padded scalar ``padded``."""
     lam = tendency_adjoint.contiguous()
     out = torch.empty_like(padded)
-    a = _AdjArrays(scalar=_ptr(padded, "padded"), rru=f["rru"].data_ptr(), rrv=f["rrv"].data_ptr(),
-                   rrw=f["rrw"].data_ptr(), c1=f["c1"].data_ptr(), c2=f["c2"].data_ptr(), rr0=f["rr0"].data_ptr(),
-                   gz=f["gz"].data_ptr(), divx=f["divx"].data_ptr(), tendency_adjoint=_ptr(lam, "tendency_adjoint"),
-                   scalar_adjoint=out.data_ptr())
-    st = _stream(padded.device)
-    lib = _lib()
-    _native.check(lib.gm1b_scalar_advection5_adjoint(ni, nj, nk, ctypes.byref(a), nrk, 1, flow.dx, flow.dy, flow.dz,
-                                                     flow.weps if weps is None else weps, OBC_OPEN, st),
-                  "gm1b_scalar_advection5_adjoint")
-    if not fill_transpose:
-        return out
-    _native.check(lib.gm1b_open_fill_scalar_adjoint(ni, nj, nk, out.data_ptr(), st), "gm1b_open_fill_scalar_adjoint")
-    return out[1:nk + 1, NG:NG + nj, NG:NG + ni].contiguous()
+    a = _adjoint_arrays(flow, padded, lam, out)
+    work = _workspace(flow, padded.device)
+    _native.check(_lib().gm1b_scalar_advection5_adjoint(
+        flow.ni, flow.nj, flow.nk, ctypes.byref(a), nrk, 1, flow.dx, flow.dy, flow.dz,
+        flow.weps if weps is None else weps, OBC_OPEN, work.data_ptr(), _stream(padded.device)),
+        "gm1b_scalar_advection5_adjoint")
+    return out
 
 
 class _AdvectionTendency(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, scalar, flow, nrk, weps):
-        padded = _carrier(flow, scalar.contiguous())
-        ctx.save_for_backward(padded)
+    def forward(ctx, scalar, flow, nrk, weps, chunk):
+        scalar = scalar.contiguous()
+        ctx.save_for_backward(scalar)
         ctx.flow, ctx.nrk, ctx.weps = flow, nrk, weps
-        return _tendency(flow, padded, nrk, weps)
+        return _tendency(flow, _carrier(flow, scalar), nrk, weps, chunk)
 
     @staticmethod
     def backward(ctx, grad):
-        (padded,) = ctx.saved_tensors
-        return advection_tendency_adjoint(ctx.flow, padded, grad, ctx.nrk, weps=ctx.weps), None, None, None
+        (scalar,) = ctx.saved_tensors
+        return advection_tendency_adjoint(ctx.flow, scalar, grad, ctx.nrk, weps=ctx.weps), None, None, None, None
 
 
-def advection_tendency(scalar: torch.Tensor, flow: FrozenFlow, nrk: int, weps: float | None = None) -> torch.Tensor:
+def advection_tendency(scalar: torch.Tensor, flow: FrozenFlow, nrk: int, weps: float | None = None,
+                       levels_per_chunk: int | None = None) -> torch.Tensor:
     """The open-sided fifth-order (nrk 1, 2) / WENO5 (nrk 3) tendency of a
     compact (nk, nj, ni) scalar, differentiable in the scalar; ``weps`` the
-    WENO epsilon (default: the flow's)."""
+    WENO epsilon (default: the flow's); ``levels_per_chunk`` the forward
+    kernel's z-chunk (None: the library default)."""
     if nrk not in (1, 2, 3):
         raise ValueError("nrk must be one of 1, 2, 3")
-    return _AdvectionTendency.apply(scalar, flow, nrk, float(flow.weps if weps is None else weps))
+    return _AdvectionTendency.apply(scalar, flow, nrk, float(flow.weps if weps is None else weps), levels_per_chunk)
 
 
 class _Collection(torch.autograd.Function):
@@ -292,7 +333,7 @@ class WarmRainTransport:
     checkpointing each large step when ``checkpoint`` is set."""
 
     def __init__(self, flow: FrozenFlow, dt: float, *, weps: Mapping[str, float] | None = None,
-                 checkpoint: bool = True):
+                 checkpoint: bool = True, tuner: Autotuner | None = None):
         if not dt > 0.0:
             raise ValueError("dt must be > 0")
         self.flow = flow
@@ -300,6 +341,16 @@ class WarmRainTransport:
         self.dt = float(dt)
         self.stage_dt = tuple(rk_stage_dt_f32(self.dt, nrk) for nrk in (1, 2, 3))
         self.checkpoint = checkpoint
+        # the forward tendency's z-chunk per stage kind (fifth order at
+        # nrk 1, 2; WENO5 at nrk 3), chosen for this grid by the tuner
+        self.chunk = {1: None, 2: None, 3: None}
+        if tuner is not None:
+            sample = _carrier(flow, flow.fields["th0"])
+            for nrk, kind in ((1, "scalar_advection5"), (3, "scalar_advection5_weno")):
+                best = tuner.choose(kind, flow.ni, flow.nj, flow.nk,
+                                    lambda c, nrk=nrk: _tendency(flow, sample, nrk, self.weps[0], c))
+                self.chunk[nrk] = best
+            self.chunk[2] = self.chunk[1]
 
     def step(self, th3d, qv, qc, qr):
         f = self.flow.fields
@@ -307,7 +358,8 @@ class WarmRainTransport:
         for s0, weps in zip((th3d, qv, qc, qr), self.weps):
             cur = s0
             for nrk in (1, 2, 3):
-                cur = s0 + self.stage_dt[nrk - 1] * advection_tendency(cur, self.flow, nrk, weps)
+                cur = torch.add(s0, advection_tendency(cur, self.flow, nrk, weps, self.chunk[nrk]),
+                                alpha=self.stage_dt[nrk - 1])
             new.append(cur)
         # the transport's undershoots clipped: the Kessler pieces take
         # non-negative water (the reference refuses qc, qr < 0)
@@ -351,3 +403,192 @@ class WarmRainTransport:
         j = sum((w * x).sum() for w, x in zip(weights, final))
         grads = torch.autograd.grad(j, leaves)
         return j.detach(), grads
+
+
+class StageCheckpointedAdjoint:
+    """The hand-written reverse of a WarmRainTransport step with checkpoints
+    at the RK-stage boundaries.
+
+    ``forward(x)`` runs the step and keeps each scalar's stage states
+    s_1, s_2, s_3 (s_0 is the step's input): with those, the reverse needs
+    no tendency recomputed: the advection adjoint reads each stage's
+    open-filled carrier through the fill's index map.  ``reverse(saved, lam)``
+    pulls dJ/d(step output) back to dJ/d(step input):
+
+      satadj1 adjoint at (s_3 theta', s_3 qv, qc after collection),
+      collection adjoint at the clipped s_3 qc, qr, the clip's mask
+      (torch.clamp's: the gradient passes at 0), then per scalar
+      lambda_0 = l_3 + l_2 + l_1 + T_1^T(s_0) dt_1 l_1 with
+      l_2 = T_3^T(s_2) dt_3 l_3 and l_1 = T_2^T(s_1) dt_2 l_2,
+      the dt scaling and the last sum fused into the gather kernel.
+
+    The same gradient as the autograd path (up to the order of the float
+    sums)."""
+
+    def __init__(self, model: WarmRainTransport):
+        self.model = model
+
+    def forward(self, x: tuple) -> tuple[tuple, tuple]:
+        m = self.model
+        f = m.flow.fields
+        stages = []
+        new = []
+        with torch.no_grad():
+            for s0, weps in zip(x, m.weps):
+                cur, kept = s0, [s0]
+                for nrk in (1, 2, 3):
+                    ten = _tendency(m.flow, _carrier(m.flow, cur), nrk, weps, m.chunk[nrk])
+                    cur = torch.add(s0, ten, alpha=m.stage_dt[nrk - 1])
+                    kept.append(cur)
+                stages.append(tuple(kept))
+                new.append(cur)
+            out = tuple(torch.empty_like(t) for t in new)
+            _warm_rain_cell(f, new, None, out, m.dt)
+        return out, tuple(stages)
+
+    def reverse(self, stages: tuple, lam: tuple) -> tuple:
+        m = self.model
+        f = m.flow.fields
+        with torch.no_grad():
+            l3s = tuple(torch.empty_like(st[3]) for st in stages)
+            _warm_rain_cell(f, tuple(st[3] for st in stages), tuple(t.contiguous() for t in lam), l3s, m.dt)
+            out = []
+            for st, l3, weps in zip(stages, l3s, m.weps):
+                acc = torch.empty_like(l3)
+                # l2 = T_3^T dt_3 l3 with acc = l3 + l2; l1 = T_2^T dt_2 l2
+                # with acc += l1; lambda_0 = acc + T_1^T dt_1 l1
+                l2 = advection_tendency_adjoint(m.flow, st[2], l3, 3, weps=weps, scale=m.stage_dt[2], accumulate=l3,
+                                                running_sum=acc)
+                l1 = advection_tendency_adjoint(m.flow, st[1], l2, 2, weps=weps, scale=m.stage_dt[1], accumulate=acc,
+                                                running_sum=acc)
+                out.append(advection_tendency_adjoint(m.flow, st[0], l1, 1, weps=weps, scale=m.stage_dt[0],
+                                                      accumulate=acc))
+        return tuple(out)
+
+
+def _warm_rain_cell(f, state, lam, out, dt):
+    """gm1b_warm_rain_cell (lam None) or its adjoint (lam = dJ/d(out), out
+    receiving dJ/d(state))."""
+    vp4 = ctypes.c_void_p * 4
+    st = vp4(*(_ptr(t, "state") for t in state))
+    o = vp4(*(_ptr(t, "out") for t in out))
+    thermo = [_ptr(f[n], n) for n in THERMO_NAMES]
+    stream = _stream(state[0].device)
+    if lam is None:
+        _native.check(_lib().gm1b_warm_rain_cell(state[0].numel(), *thermo, st, o, dt, stream), "gm1b_warm_rain_cell")
+    else:
+        lm = vp4(*(_ptr(t, "lam") for t in lam))
+        _native.check(_lib().gm1b_warm_rain_cell_adjoint(state[0].numel(), *thermo, st, lm, o, dt, stream),
+                      "gm1b_warm_rain_cell_adjoint")
+
+
+class StepGraphs:
+    """A model's plain forward step, its stage-saving forward step and the
+    one-step reverse of StageCheckpointedAdjoint, each captured once as a
+    CUDA graph over static flat buffers, so a sweep replays one graph per
+    step instead of launching its kernels one by one, and moves each step's
+    saved fields with one copy.
+
+    Flat layouts, (n, nk, nj, ni) float32: the state (th3d, qv, qc, qr) is 4
+    fields; a forward step's output is 16 (the next state, then s_1, s_2,
+    s_3 of each scalar in state order); the reverse reads 20 (the step's
+    input state, the 12 stage fields, dJ/d(step output)) and writes 4.
+    ``gradient`` gives the words of the eager StageCheckpointedAdjoint."""
+
+    def __init__(self, model: WarmRainTransport, like: tuple):
+        self.model = model
+        self.adjoint = StageCheckpointedAdjoint(model)
+        dev = like[0].device
+        shape = tuple(like[0].shape)
+        self.xin = torch.stack([t.detach() for t in like]).contiguous()
+        self.fout = torch.zeros((16,) + shape, dtype=torch.float32, device=dev)
+        self.rin = torch.zeros((20,) + shape, dtype=torch.float32, device=dev)
+        self.rin[:4].copy_(self.xin)
+        self.rout = torch.zeros((4,) + shape, dtype=torch.float32, device=dev)
+        self.sout = torch.zeros((4,) + shape, dtype=torch.float32, device=dev)
+        x = tuple(self.xin[q] for q in range(4))
+        stages_in = tuple((self.rin[q],) + tuple(self.rin[4 + 3 * q + r] for r in range(3)) for q in range(4))
+        lam_in = tuple(self.rin[16 + q] for q in range(4))
+
+        def fwd():
+            y, stages = self.adjoint.forward(x)
+            for q in range(4):
+                self.fout[q].copy_(y[q])
+                for r in range(3):
+                    self.fout[4 + 3 * q + r].copy_(stages[q][r + 1])
+
+        def rev():
+            g = self.adjoint.reverse(stages_in, lam_in)
+            for q in range(4):
+                self.rout[q].copy_(g[q])
+
+        def plain():
+            with torch.no_grad():
+                y = model.step(*x)
+            for q in range(4):
+                self.sout[q].copy_(y[q])
+
+        side = torch.cuda.Stream(dev)
+        side.wait_stream(torch.cuda.current_stream(dev))
+        with torch.cuda.stream(side):  # first launches outside the capture
+            for _ in range(2):
+                plain()
+                fwd()
+                rev()
+        torch.cuda.current_stream(dev).wait_stream(side)
+        self.g_step, self.g_fwd, self.g_rev = torch.cuda.CUDAGraph(), torch.cuda.CUDAGraph(), torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.g_step):
+            plain()
+        with torch.cuda.graph(self.g_fwd):
+            fwd()
+        with torch.cuda.graph(self.g_rev):
+            rev()
+
+    @staticmethod
+    def stack(state: tuple) -> torch.Tensor:
+        return torch.stack([t.detach() for t in state]).contiguous()
+
+    def step(self, x: torch.Tensor) -> torch.Tensor:
+        """The plain step of a stacked (4, nk, nj, ni) state."""
+        self.xin.copy_(x)
+        self.g_step.replay()
+        return self.sout.clone()
+
+    def forward(self, x: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:
+        """The stage-saving step of a stacked state: the (16, ...) block of
+        the next state and the stage fields (into ``out`` when given: a
+        sweep lays its whole checkpoint store out once)."""
+        self.xin.copy_(x)
+        self.g_fwd.replay()
+        if out is None:
+            return self.fout.clone()
+        out.copy_(self.fout)
+        return out
+
+    def store(self, steps: int) -> torch.Tensor:
+        """The checkpoint store of a ``steps``-step window: (steps, 16, nk,
+        nj, ni) float32, 64 words per cell per step."""
+        return torch.empty((steps,) + tuple(self.fout.shape), dtype=torch.float32, device=self.fout.device)
+
+    def reverse(self, x: torch.Tensor, saved: torch.Tensor, lam: torch.Tensor) -> torch.Tensor:
+        """dJ/d(stacked step input) from the step's input ``x``, its saved
+        (16, ...) block and dJ/d(step output)."""
+        self.rin[:4].copy_(x)
+        self.rin[4:16].copy_(saved[4:])
+        self.rin[16:].copy_(lam)
+        self.g_rev.replay()
+        return self.rout.clone()
+
+    def gradient(self, state: tuple, weights: tuple, steps: int, store: torch.Tensor | None = None) -> tuple:
+        """dJ/d state for J = sum <weights, final state>: a forward sweep
+        keeping every step's stage block in ``store`` (made here when not
+        given), then the reverse sweep."""
+        store = self.store(steps) if store is None else store
+        inputs, saved = [self.stack(state)], []
+        for q in range(steps):
+            saved.append(self.forward(inputs[-1], store[q]))
+            inputs.append(saved[-1][:4])
+        lam = self.stack(weights)
+        for q in reversed(range(steps)):
+            lam = self.reverse(inputs[q], saved[q], lam)
+        return tuple(lam[q] for q in range(4))

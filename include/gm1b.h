@@ -967,14 +967,41 @@ typedef struct gm1b_scalar_advection5_adjoint_arrays {
  * (face adjoint) * (mass flux) * d(reconstruction)/d(word), plus its
  * divergence and open-side terms.  The WENO-Z weights are differentiated at
  * their epsilon-regularised form (subgradient 0 for |b1 - b3| at b1 = b3
- * and beyond the 1e30 cap), upstrpd by its active limiter branch.  One
- * gather per word, no atomics.  Differentiates cpu_scalar_advection5_inplace
- * (src/cm1core/cuda_advection5.py:440) / cm1_adv5_scalar_tendency_v1 (:669).
+ * and beyond the 1e30 cap), upstrpd by its active limiter branch.
+ * Differentiates cpu_scalar_advection5_inplace (src/cm1core/cuda_advection5.py:
+ * 440) / cm1_adv5_scalar_tendency_v1 (:669).  Two passes, no atomics: each
+ * face writes its six coefficients (face adjoint x mass flux x the
+ * reconstruction's derivative at each stencil point) into the workspace
+ * (gm1b_scalar_advection5_adjoint_workspace_bytes), then each word gathers
+ * the coefficients of the faces that read it.  scalar_adjoint: the padded
+ * (nk+2, nj+6, ni+6) dJ/d(carrier word).
  */
+GM1B_API size_t gm1b_scalar_advection5_adjoint_workspace_bytes(int32_t ni, int32_t nj, int32_t nk);
 GM1B_API int32_t gm1b_scalar_advection5_adjoint(int32_t ni, int32_t nj, int32_t nk,
                                                 const gm1b_scalar_advection5_adjoint_arrays *arrays, int32_t nrk,
                                                 int32_t wflag, float dx, float dy, float dz, double weps,
-                                                uint32_t lateral_obc, void *stream);
+                                                uint32_t lateral_obc, void *workspace, void *stream);
+/* The same through the all-open carrier: scalar is the COMPACT (nk, nj, ni)
+ * scalar (its open-filled carrier, the words gm1b_scalar_carrier_open
+ * makes, is read through the fill's index map, never stored),
+ * scalar_adjoint the compact dJ/d scalar (the fill's transpose folded into
+ * the gather), for
+ * the tendency adjoint adjoint_scale * tendency_adjoint.  accumulate
+ * (compact, may be NULL, may equal scalar_adjoint) is added to the result;
+ * with running_sum (compact, needs accumulate) the result is written bare
+ * and running_sum = accumulate + result (the RK stage chain's two outputs). */
+GM1B_API int32_t gm1b_scalar_advection5_adjoint_open(int32_t ni, int32_t nj, int32_t nk,
+                                                     const gm1b_scalar_advection5_adjoint_arrays *arrays, int32_t nrk,
+                                                     int32_t wflag, float dx, float dy, float dz, double weps,
+                                                     float adjoint_scale, const float *accumulate, float *running_sum,
+                                                     void *workspace, void *stream);
+/* The compact (nk, nj, ni) scalar packed into its padded (nk+2, nj+6, ni+6)
+ * carrier with the all-open halo fill in one pass: the same words as
+ * zeroing, gm1b_pack_scalar and gm1b_open_fill(GM1B_FILL_SCALAR) in turn
+ * (cm1_rk_pack_scalar_v1 and bcs, src/cm1core/cuda_sound3_open_boundary.py:
+ * 249-335). */
+GM1B_API int32_t gm1b_scalar_carrier_open(int32_t ni, int32_t nj, int32_t nk, const float *scalar, float *padded,
+                                          void *stream);
 
 /* The transpose of gm1b_open_fill's scalar kind (bcs on open sides,
  * src/cm1core/cuda_sound3_open_boundary.py:249-335), in place on a padded
@@ -1024,6 +1051,22 @@ GM1B_API int32_t gm1b_satadj1(size_t cells, const float *th0, const float *pi0, 
 GM1B_API int32_t gm1b_satadj1_adjoint(size_t cells, const float *th0, const float *pi0, const float *pp3d,
                                       const float *prs, const float *th3d, const float *qv, const float *qc,
                                       float *g_th, float *g_qv, float *g_qc, void *stream);
+
+/*
+ * The cell step of the warm-rain transport model after its transport, in one
+ * pass: qc and qr clipped at 0, collection (gm1b_kessler_collection), then
+ * satadj1 - the same words as those pieces run in turn.  state and out: four
+ * host arrays of device pointers (th3d, qv, qc, qr), cells words each.  The
+ * adjoint takes the transported state and dJ/d(out) and writes dJ/d(state);
+ * the clip passes the adjoint where the state is >= 0.
+ */
+GM1B_API int32_t gm1b_warm_rain_cell(size_t cells, const float *th0, const float *pi0, const float *pp3d,
+                                     const float *prs, const float *const *state, float *const *out, float dt,
+                                     void *stream);
+GM1B_API int32_t gm1b_warm_rain_cell_adjoint(size_t cells, const float *th0, const float *pi0, const float *pp3d,
+                                             const float *prs, const float *const *state,
+                                             const float *const *out_adjoint, float *const *state_adjoint, float dt,
+                                             void *stream);
 
 /* ------------------------------------------------------------------------
  * The whole moist RK3 large step behind one entry point.
