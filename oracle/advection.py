@@ -13,9 +13,9 @@ import ctypes
 
 import numpy as np
 
-from oracle.periodic import load
+from oracle.periodic import C_REAL, REAL, load
 
-_F = ctypes.POINTER(ctypes.c_float)
+_F = ctypes.POINTER(C_REAL)
 
 
 class MassFluxArrays(ctypes.Structure):
@@ -31,7 +31,7 @@ class ScalarAdvArrays(ctypes.Structure):
 def _fill(struct, arrays):
     for name, _ in struct._fields_:
         a = arrays[name]
-        if a.dtype != np.float32 or not a.flags.c_contiguous:
+        if a.dtype != REAL or not a.flags.c_contiguous:
             raise ValueError(f"{name} must be C-contiguous float32")
         setattr(struct, name, a.ctypes.data_as(_F))
     return struct
@@ -41,19 +41,19 @@ def _lib():
     lib = load()
     if not getattr(lib, "_adv_ready", False):
         lib.oracle_terrain_mass_flux5.argtypes = [ctypes.POINTER(MassFluxArrays), ctypes.c_int, ctypes.c_int,
-                                                  ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_float]
+                                                  ctypes.c_int, C_REAL, C_REAL, C_REAL]
         lib.oracle_terrain_mass_flux5.restype = None
         lib.oracle_scalar_advection5.argtypes = [ctypes.POINTER(ScalarAdvArrays), ctypes.c_int, ctypes.c_int,
-                                                 ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_float,
-                                                 ctypes.c_float, ctypes.c_double, ctypes.c_uint]
+                                                 ctypes.c_int, ctypes.c_int, C_REAL, C_REAL,
+                                                 C_REAL, ctypes.c_double, ctypes.c_uint]
         lib.oracle_scalar_advection5.restype = None
         lib.oracle_scalar_advection5_column.argtypes = [ctypes.POINTER(ScalarAdvArrays), ctypes.c_int, ctypes.c_int,
-                                                        ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_float,
+                                                        ctypes.c_int, ctypes.c_int, C_REAL, C_REAL,
                                                         ctypes.c_double, ctypes.c_uint, ctypes.c_int, _F, _F,
-                                                        ctypes.c_float]
+                                                        C_REAL]
         lib.oracle_scalar_advection5_column.restype = None
-        lib.oracle_weno5.argtypes = [ctypes.c_float] * 5 + [ctypes.c_double]
-        lib.oracle_weno5.restype = ctypes.c_float
+        lib.oracle_weno5.argtypes = [C_REAL] * 5 + [ctypes.c_double]
+        lib.oracle_weno5.restype = C_REAL
         lib._adv_ready = True
     return lib
 
@@ -75,7 +75,7 @@ def scalar_advection5_column(arrays, *, ni, nj, nk, nrk, dx, dy, weps, flat, pro
     indexing), flat=True profile = mh (nk+2 words) with rdz."""
     use_weno = 1 if (wflag and nrk == 3) else 0
     s = _fill(ScalarAdvArrays(), arrays)
-    prof = np.ascontiguousarray(profile, dtype=np.float32)
+    prof = np.ascontiguousarray(profile, dtype=REAL)
     ptr = prof.ctypes.data_as(_F)
     _lib().oracle_scalar_advection5_column(ctypes.byref(s), ni, nj, nk, use_weno, dx, dy, weps, lateral_obc,
                                            2 if flat else 1, None if flat else ptr, ptr if flat else None, rdz)

@@ -19,6 +19,7 @@
 #include <math.h>
 #include <stdint.h>
 #include <string.h>
+#include "real.h"
 
 #define NG 3
 

@@ -8,15 +8,15 @@ import ctypes
 
 import numpy as np
 
-from oracle.periodic import load
+from oracle.periodic import C_REAL, REAL, load
 
-_F = ctypes.POINTER(ctypes.c_float)
+_F = ctypes.POINTER(C_REAL)
 
 
 def _lib():
     lib = load()
     if not getattr(lib, "_bridge_ready", False):
-        f = ctypes.c_float
+        f = C_REAL
         lib.oracle_eqtset2_cell.argtypes = [f, f, f, f, f, f, f, _F, _F]
         lib.oracle_eqtset2_cell.restype = None
         lib._bridge_ready = True
@@ -25,8 +25,8 @@ def _lib():
 
 def eqtset2_cell(th0, qv0, pi0, qc0, qi0, th3d, pp3d, q) -> np.ndarray:
     """(buoyancy, theta_rho, theta_term, pressure_term) of one cell."""
-    qq = np.ascontiguousarray(q, dtype=np.float32)
-    out = np.zeros(4, np.float32)
+    qq = np.ascontiguousarray(q, dtype=REAL)
+    out = np.zeros(4, REAL)
     _lib().oracle_eqtset2_cell(th0, qv0, pi0, qc0, qi0, th3d, pp3d, qq.ctypes.data_as(_F), out.ctypes.data_as(_F))
     return out
 
@@ -40,6 +40,6 @@ def eqtset2_stage_terms(*, ni, nj, nk, th0, qv0, pi0, th3d, q3d, pp3d, thv, ppte
         lib._terms_ready = True
     ptrs = []
     for a in (th0, qv0, pi0, th3d, q3d, pp3d, thv, ppterm, buoyancy, thterm, piadv):
-        assert a.dtype == np.float32 and a.flags.c_contiguous
+        assert a.dtype == REAL and a.flags.c_contiguous
         ptrs.append(a.ctypes.data_as(_F))
     lib.oracle_eqtset2_stage_terms(ni, nj, nk, *ptrs)

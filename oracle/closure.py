@@ -9,9 +9,9 @@ import ctypes
 
 import numpy as np
 
-from oracle.periodic import load
+from oracle.periodic import C_REAL, REAL, load
 
-_F = ctypes.POINTER(ctypes.c_float)
+_F = ctypes.POINTER(C_REAL)
 
 DEFORMATION_INPUTS = ("u3d", "v3d", "w3d", "rho", "rf", "c1", "c2", "gz", "rgz", "rgzu", "rgzv", "gx", "gy")
 NM_INPUTS = ("c1", "c2", "mf", "pi0", "th0", "prs", "pp3d", "th3d", "q3d")
@@ -21,7 +21,7 @@ NM_OUTPUTS = ("nm", "temperature", "qt", "thv", "qvci")
 def _lib():
     lib = load()
     if not getattr(lib, "_closure_ready", False):
-        i, f = ctypes.c_int, ctypes.c_float
+        i, f = ctypes.c_int, C_REAL
         lib.oracle_calcdef.argtypes = [i, i, i] + [_F] * 13 + [f, f, f, _F, _F]
         lib.oracle_calcdef.restype = i
         lib.oracle_moist_nm.argtypes = [i, i, i] + [_F] * 9 + [f] + [_F] * 5 + [ctypes.c_void_p,
@@ -34,7 +34,7 @@ def _lib():
 
 
 def _p(a: np.ndarray):
-    assert a.dtype == np.float32 and a.flags.c_contiguous
+    assert a.dtype == REAL and a.flags.c_contiguous
     return a.ctypes.data_as(_F)
 
 

@@ -17,6 +17,7 @@
 #include <math.h>
 #include <stdint.h>
 #include <stdlib.h>
+#include "real.h"
 
 #define I3(k, j, i, ny, nx) ((((int64_t)(k)) * (ny) + (j)) * (nx) + (i))
 

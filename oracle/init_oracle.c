@@ -19,6 +19,7 @@
  */
 #include <math.h>
 #include <stdint.h>
+#include "real.h"
 
 /* CM1 constants.F binary32 words */
 #define K_G 9.81f

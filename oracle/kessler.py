@@ -8,9 +8,9 @@ import ctypes
 
 import numpy as np
 
-from oracle.periodic import load
+from oracle.periodic import C_REAL, REAL, load
 
-_F = ctypes.POINTER(ctypes.c_float)
+_F = ctypes.POINTER(C_REAL)
 _D = ctypes.POINTER(ctypes.c_double)
 _U = ctypes.POINTER(ctypes.c_uint32)
 
@@ -25,7 +25,7 @@ class KesslerArrays(ctypes.Structure):
 def _lib():
     lib = load()
     if not getattr(lib, "_kessler_ready", False):
-        i, f = ctypes.c_int, ctypes.c_float
+        i, f = ctypes.c_int, C_REAL
         lib.oracle_kessler_driver.argtypes = [ctypes.POINTER(KesslerArrays), i, i, i, f, f, f, f, i,
                                               ctypes.POINTER(ctypes.c_int32)]
         lib.oracle_kessler_driver.restype = i
@@ -39,7 +39,7 @@ def kessler_driver(arrays, *, ni, nj, nk, dx, dy, dz, dt, eqtset, iterations=Non
     s = KesslerArrays()
     for n in FLOAT_NAMES:
         a = arrays[n]
-        assert a.dtype == np.float32 and a.flags.c_contiguous
+        assert a.dtype == REAL and a.flags.c_contiguous
         setattr(s, n, a.ctypes.data_as(_F))
     for n in ("asq", "qbudget"):
         assert arrays[n].dtype == np.float64
@@ -64,7 +64,7 @@ def kessler_large_step(arrays, held, *, ni, nj, nk, dx, dy, dz, dt, eqtset, nfal
     s = KesslerArrays()
     for n in FLOAT_NAMES:
         a = arrays[n]
-        assert a.dtype == np.float32 and a.flags.c_contiguous
+        assert a.dtype == REAL and a.flags.c_contiguous
         setattr(s, n, a.ctypes.data_as(_F))
     for n in ("asq", "qbudget"):
         setattr(s, n, arrays[n].ctypes.data_as(_D))
@@ -72,7 +72,7 @@ def kessler_large_step(arrays, held, *, ni, nj, nk, dx, dy, dz, dt, eqtset, nfal
     lib = _lib()
     if not getattr(lib, "_kls_ready", False):
         lib.oracle_kessler_large_step.argtypes = [ctypes.POINTER(KesslerArrays), ctypes.POINTER(_F)] + \
-            [ctypes.c_int] * 3 + [ctypes.c_float] * 4 + [ctypes.c_int, ctypes.POINTER(ctypes.c_int32)]
+            [ctypes.c_int] * 3 + [C_REAL] * 4 + [ctypes.c_int, ctypes.POINTER(ctypes.c_int32)]
         lib.oracle_kessler_large_step.restype = ctypes.c_int
         lib._kls_ready = True
     nf = nfall.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)) if nfall is not None else None

@@ -22,6 +22,7 @@
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
+#include "real.h"
 
 typedef struct {
     /* inputs */

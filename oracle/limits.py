@@ -8,9 +8,9 @@ import ctypes
 
 import numpy as np
 
-from oracle.periodic import load
+from oracle.periodic import C_REAL, REAL, load
 
-_F = ctypes.POINTER(ctypes.c_float)
+_F = ctypes.POINTER(C_REAL)
 _D = ctypes.c_double
 
 
@@ -23,7 +23,7 @@ def _lib():
         lib.oracle_diagnostic_substeps.restype = ctypes.c_int
         lib.oracle_advective_courant.argtypes = [_D] * 7
         lib.oracle_advective_courant.restype = _D
-        f = ctypes.c_float
+        f = C_REAL
         lib.oracle_courant_max.argtypes = [ctypes.c_int] * 3 + [_F] * 6 + [f, f, f, _F]
         lib.oracle_courant_max.restype = f
         lib._limits_ready = True
@@ -44,8 +44,8 @@ def advective_courant(dt, dx, dy, dz, u, v, w) -> float:
 
 def courant_max(u, v, w, uh, vh, mh, dtdx, dtdy, dtdz) -> tuple[float, np.ndarray]:
     nk, nj, ni1 = u.shape
-    arrs = [np.ascontiguousarray(a, dtype=np.float32) for a in (u, v, w, uh, vh, mh)]
-    level = np.zeros(nk, np.float32)
+    arrs = [np.ascontiguousarray(a, dtype=REAL) for a in (u, v, w, uh, vh, mh)]
+    level = np.zeros(nk, REAL)
     p = [a.ctypes.data_as(_F) for a in arrs]
     out = _lib().oracle_courant_max(ni1 - 1, nj, nk, *p, dtdx, dtdy, dtdz, level.ctypes.data_as(_F))
     return float(np.float32(out)), level

@@ -14,6 +14,7 @@
  */
 #include <math.h>
 #include <stdint.h>
+#include "real.h"
 
 double oracle_small_step_limit(double dx, double dy) { return 0.60 * (dx < dy ? dx : dy) / 360.0; }
 

@@ -21,6 +21,7 @@ from oracle import rk as ork
 from oracle import terrain_open as otos
 from oracle import tke as otke
 from oracle import tke_evolution as otev
+from oracle.periodic import REAL
 
 NUMQ = 3
 QMAG = 1.0e-2
@@ -45,7 +46,7 @@ class OracleMoistStep:
         # the oracle's acoustic stage always writes its column diagnostics
         for n in ("tri_aa", "tri_bb", "tri_cc", "tri_dd", "tri_pivot", "tri_residual"):
             if state[n].shape != state["pp3d"].shape:
-                state[n] = np.zeros(state["pp3d"].shape, np.float32)
+                state[n] = np.zeros(state["pp3d"].shape, REAL)
         self.k3 = dict(ni=cfg.ni, nj=cfg.nj, nk=cfg.nk)
         self.grid = dict(ni=cfg.ni, nj=cfg.nj, nk=cfg.nk, dx=cfg.dx, dy=cfg.dy, dz=cfg.dz)
         # a stretched column runs the flat (terrain_flag=.false.) family on

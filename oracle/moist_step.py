@@ -8,9 +8,9 @@ import ctypes
 
 import numpy as np
 
-from oracle.periodic import load
+from oracle.periodic import C_REAL, REAL, load
 
-_F = ctypes.POINTER(ctypes.c_float)
+_F = ctypes.POINTER(C_REAL)
 POST_NAMES = ("rru", "rrv", "rrw", "rgzu", "rgzv", "dzdx", "dzdy", "gz", "rho0_3d", "rf0", "thterm", "divergence",
               "theta_divergence_term", "divx")
 CHAIN_NAMES = ("scalar_a", "scalar_padded", "rho0_3d", "gz", "rgz", "rr0", "c1", "c2", "divx", "rru", "rrv", "rrw",
@@ -29,7 +29,7 @@ _Post, _Chain, _Held = _struct(POST_NAMES), _struct(CHAIN_NAMES), _struct(HELD_N
 
 
 def _p(a):
-    assert a.dtype == np.float32 and a.flags.c_contiguous
+    assert a.dtype == REAL and a.flags.c_contiguous
     return a.ctypes.data_as(_F)
 
 
@@ -39,20 +39,20 @@ def _lib():
         c = ctypes
         lib.oracle_open_fill.argtypes = [c.c_int] * 4 + [_F]
         lib.oracle_moist_buoyancy.argtypes = [c.c_int] * 3 + [_F] * 8
-        lib.oracle_post_acoustic_flux.argtypes = [c.c_int] * 3 + [c.POINTER(_Post)] + [c.c_float] * 3
-        lib.oracle_pdef_moisture_chain.argtypes = [c.c_int] * 3 + [c.POINTER(_Chain)] + [c.c_float] * 4 + \
+        lib.oracle_post_acoustic_flux.argtypes = [c.c_int] * 3 + [c.POINTER(_Post)] + [C_REAL] * 3
+        lib.oracle_pdef_moisture_chain.argtypes = [c.c_int] * 3 + [c.POINTER(_Chain)] + [C_REAL] * 4 + \
             [c.c_double, c.c_uint, c.c_int]
         lib.oracle_pdef_moisture_directional.argtypes = lib.oracle_pdef_moisture_chain.argtypes
         lib.oracle_pdef_moisture_directional.restype = None
-        lib.oracle_pdef_moisture_chain_column.argtypes = [c.c_int] * 3 + [c.POINTER(_Chain)] + [c.c_float] * 3 + \
-            [c.c_double, c.c_uint, c.c_int, c.c_int, _F, _F, c.c_float]
+        lib.oracle_pdef_moisture_chain_column.argtypes = [c.c_int] * 3 + [c.POINTER(_Chain)] + [C_REAL] * 3 + \
+            [c.c_double, c.c_uint, c.c_int, c.c_int, _F, _F, C_REAL]
         lib.oracle_pdef_moisture_chain_column.restype = None
-        lib.oracle_post_acoustic_flux_column.argtypes = [c.c_int] * 3 + [c.POINTER(_Post)] + [c.c_float] * 2 + \
-            [c.c_int] + [_F] * 5 + [c.c_float, _F, c.c_float]
+        lib.oracle_post_acoustic_flux_column.argtypes = [c.c_int] * 3 + [c.POINTER(_Post)] + [C_REAL] * 2 + \
+            [c.c_int] + [_F] * 5 + [C_REAL, _F, C_REAL]
         lib.oracle_post_acoustic_flux_column.restype = None
         lib.oracle_moist_buoyancy_flat.argtypes = [c.c_int] * 3 + [_F] * 4
         lib.oracle_moist_buoyancy_flat.restype = None
-        lib.oracle_held_compose.argtypes = [c.c_int] * 3 + [c.POINTER(_Held), c.c_float]
+        lib.oracle_held_compose.argtypes = [c.c_int] * 3 + [c.POINTER(_Held), C_REAL]
         lib.oracle_solve3_density.argtypes = [c.c_int] * 3 + [_F] * 5
         lib.oracle_pack_scalar.argtypes = [c.c_int] * 3 + [_F] * 2
         lib.oracle_bcwsfc.argtypes = [c.c_int] * 3 + [_F] * 6
@@ -81,7 +81,7 @@ def post_acoustic_flux_column(a, column, *, ni, nj, nk, dx, dy):
     """getdiv/getdivx on a stretched column: ``column`` holds flat, rho0p and
     sigma/sigmaf/rds/rdsf/ztop (terrain branch) or mh/rdz (flat column)."""
     s = _Post(**{n: _p(a[n]) for n in POST_NAMES})
-    keep = {n: np.ascontiguousarray(column[n], dtype=np.float32) for n in ("rho0p", "sigma", "sigmaf", "rds", "rdsf",
+    keep = {n: np.ascontiguousarray(column[n], dtype=REAL) for n in ("rho0p", "sigma", "sigmaf", "rds", "rdsf",
                                                                            "mh") if column.get(n) is not None}
     ptr = {n: (_p(keep[n]) if n in keep else None) for n in ("rho0p", "sigma", "sigmaf", "rds", "rdsf", "mh")}
     _lib().oracle_post_acoustic_flux_column(ni, nj, nk, ctypes.byref(s), dx, dy, 1 if column["flat"] else 0,
@@ -102,7 +102,7 @@ def pdef_moisture_chain_column(a, *, ni, nj, nk, dttmp, dx, dy, weps, lateral_ob
     """The chain on a stretched column: flat=False takes profile = rdsf
     (nk+3 words, CM1 indexing), flat=True profile = mh (nk+2 words) and rdz."""
     s = _Chain(**{n: _p(a[n]) for n in CHAIN_NAMES})
-    prof = np.ascontiguousarray(profile, dtype=np.float32)
+    prof = np.ascontiguousarray(profile, dtype=REAL)
     _lib().oracle_pdef_moisture_chain_column(ni, nj, nk, ctypes.byref(s), dttmp, dx, dy, weps, lateral_obc, pdefweno,
                                              2 if flat else 1, None if flat else _p(prof), _p(prof) if flat else None,
                                              rdz)

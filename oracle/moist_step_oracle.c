@@ -16,6 +16,7 @@
 #include <stddef.h>
 #include <stdint.h>
 #include <string.h>
+#include "real.h"
 
 typedef struct {
     int ni, nj, nk;

@@ -8,9 +8,9 @@ import ctypes
 
 import numpy as np
 
-from oracle.periodic import load
+from oracle.periodic import C_REAL, REAL, load
 
-_F = ctypes.POINTER(ctypes.c_float)
+_F = ctypes.POINTER(C_REAL)
 NAMES = ("u3d", "uten", "rru", "v3d", "vten", "rrv", "w3d", "wten", "rrw", "uh", "vh", "rho0_3d", "rf0", "rrf0", "c2",
          "gz", "gzu", "gzv", "rgzu", "rgzv", "dzdx", "dzdy", "divx")
 
@@ -24,7 +24,7 @@ def _lib():
     if not getattr(lib, "_mom_ready", False):
         lib.oracle_momentum_advection5.argtypes = [ctypes.c_int] * 3 + [ctypes.POINTER(MomArrays),
                                                                           ctypes.POINTER(ctypes.c_int)] + \
-            [ctypes.c_float] * 3
+            [C_REAL] * 3
         lib.oracle_momentum_advection5.restype = ctypes.c_int
         lib._mom_ready = True
     return lib
@@ -34,7 +34,7 @@ def momentum_advection5(a, *, ni, nj, nk, dx, dy, dz, lateral_sides=(2, 2, 2, 2)
     s = MomArrays()
     for n in NAMES:
         v = a[n]
-        assert v.dtype == np.float32 and v.flags.c_contiguous, n
+        assert v.dtype == REAL and v.flags.c_contiguous, n
         setattr(s, n, v.ctypes.data_as(_F))
     sides = (ctypes.c_int * 4)(*lateral_sides)
     rc = _lib().oracle_momentum_advection5(ni, nj, nk, ctypes.byref(s), sides, dx, dy, dz)
@@ -70,12 +70,12 @@ def momentum_advection5_column(a, column, *, ni, nj, nk, dx, dy, lateral_sides=(
     lib = _lib()
     if not getattr(lib, "_mom_column_ready", False):
         lib.oracle_momentum_advection5_column_phase.argtypes = (
-            [ctypes.c_int] * 3 + [ctypes.POINTER(MomArrays), ctypes.POINTER(ctypes.c_int), ctypes.c_float,
-                                  ctypes.c_float, ctypes.c_int, ctypes.c_int] + [_F] * 5 + [ctypes.c_float] +
-            [_F] * 3 + [ctypes.c_float])
+            [ctypes.c_int] * 3 + [ctypes.POINTER(MomArrays), ctypes.POINTER(ctypes.c_int), C_REAL,
+                                  C_REAL, ctypes.c_int, ctypes.c_int] + [_F] * 5 + [C_REAL] +
+            [_F] * 3 + [C_REAL])
         lib.oracle_momentum_advection5_column_phase.restype = ctypes.c_int
         lib._mom_column_ready = True
-    keep = {n: np.ascontiguousarray(column[n], dtype=np.float32) for n in COLUMN_PROFILES if column.get(n) is not None}
+    keep = {n: np.ascontiguousarray(column[n], dtype=REAL) for n in COLUMN_PROFILES if column.get(n) is not None}
     ptr = {n: (keep[n].ctypes.data_as(_F) if n in keep else None) for n in COLUMN_PROFILES}
     sides = (ctypes.c_int * 4)(*lateral_sides)
     rc = lib.oracle_momentum_advection5_column_phase(

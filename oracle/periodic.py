@@ -17,7 +17,14 @@ from pathlib import Path
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
-LIB_PATH = HERE / "liboracle_gm1.so"
+# Working precision of the oracle build this process loads: binary32, the
+# reference twins' arithmetic (liboracle_gm1.so), or, with
+# GM1B_ORACLE_REAL=f64, the same operators evaluated in binary64
+# (liboracle_gm1_f64.so, the FP64 run the float32 fields are measured against).
+F64 = os.environ.get("GM1B_ORACLE_REAL", "f32") == "f64"
+REAL = np.float64 if F64 else np.float32
+C_REAL = ctypes.c_double if F64 else ctypes.c_float
+LIB_PATH = HERE / ("liboracle_gm1_f64.so" if F64 else "liboracle_gm1.so")
 
 # Field order of gm1b_periodic_arrays (include/gm1b.h): the reference's
 # ALL_ARRAY_NAMES order.
@@ -40,7 +47,7 @@ SMEPS = 1.0e-30
 
 
 class PeriodicArrays(ctypes.Structure):
-    _fields_ = [(name, ctypes.POINTER(ctypes.c_float)) for name in NAMES]
+    _fields_ = [(name, ctypes.POINTER(C_REAL)) for name in NAMES]
 
 
 _lib = None
@@ -56,7 +63,7 @@ def load() -> ctypes.CDLL:
         if not LIB_PATH.exists():
             build()
         lib = ctypes.CDLL(str(LIB_PATH))
-        f = ctypes.c_float
+        f = C_REAL
         i = ctypes.c_int
         p = ctypes.POINTER(PeriodicArrays)
         lib.oracle_stage_schedule.argtypes = [f, i, i, ctypes.POINTER(i), ctypes.POINTER(f)]
@@ -93,15 +100,15 @@ def _struct(arrays: dict[str, np.ndarray], names=NAMES) -> PeriodicArrays:
         a = arrays.get(name)
         if a is None:
             continue
-        if a.dtype != np.float32 or not a.flags.c_contiguous or not a.flags.writeable:
+        if a.dtype != REAL or not a.flags.c_contiguous or not a.flags.writeable:
             raise ValueError(f"{name} must be a writable C-contiguous float32 array")
-        setattr(s, name, a.ctypes.data_as(ctypes.POINTER(ctypes.c_float)))
+        setattr(s, name, a.ctypes.data_as(ctypes.POINTER(C_REAL)))
     return s
 
 
 def stage_schedule(dt: float, nsound: int, nrk: int) -> tuple[int, float]:
     n = ctypes.c_int()
-    d = ctypes.c_float()
+    d = C_REAL()
     if load().oracle_stage_schedule(dt, nsound, nrk, ctypes.byref(n), ctypes.byref(d)) != 0:
         raise ValueError("invalid acoustic schedule arguments")
     return n.value, float(d.value)

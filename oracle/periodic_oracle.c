@@ -35,6 +35,7 @@
 #include <stdint.h>
 #include <string.h>
 
+#include "real.h"  /* before the header: its array structs take the working precision */
 #include "../include/gm1b.h"
 
 typedef gm1b_periodic_arrays A;

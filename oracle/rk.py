@@ -9,21 +9,21 @@ import ctypes
 
 import numpy as np
 
-from oracle.periodic import load
+from oracle.periodic import C_REAL, REAL, load
 
-_F = ctypes.POINTER(ctypes.c_float)
+_F = ctypes.POINTER(C_REAL)
 AXES = {"x": 0, "y": 1, "z": 2}
 
 
 def _p(a):
-    assert a.dtype == np.float32 and a.flags.c_contiguous
+    assert a.dtype == REAL and a.flags.c_contiguous
     return a.ctypes.data_as(_F)
 
 
 def _lib():
     lib = load()
     if not getattr(lib, "_rk_ready", False):
-        i, f = ctypes.c_int, ctypes.c_float
+        i, f = ctypes.c_int, C_REAL
         lib.oracle_theta_pack.argtypes = [_F, _F, _F, i, i, i]
         lib.oracle_theta_pack.restype = None
         lib.oracle_rk_compose.argtypes = [_F] * 9 + [ctypes.c_size_t, i, f]

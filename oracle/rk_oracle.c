@@ -18,6 +18,7 @@
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
+#include "real.h"
 
 #define NG 3
 #define SMEPS 0x1.4484cp-100f /* 1e-30 */

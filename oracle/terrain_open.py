@@ -10,9 +10,9 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from oracle.periodic import load
+from oracle.periodic import C_REAL, REAL, load
 
-_F = ctypes.POINTER(ctypes.c_float)
+_F = ctypes.POINTER(C_REAL)
 ARRAY_NAMES = ("ppi", "pp3d", "ppx", "ppd", "piadv", "ppterm", "ppten", "thv", "qk", "pk1", "pk2", "mm", "fpk",
                "divh", "hadvp", "dum3", "elim_c", "elim_d", "tri_aa", "tri_bb", "tri_cc", "tri_dd", "tri_pivot",
                "tri_residual", "ua", "u3d", "uten", "rru", "va", "v3d", "vten", "rrv", "wa", "w3d", "wten", "rrw",
@@ -46,17 +46,17 @@ def _lib():
     if not getattr(lib, "_tos_ready", False):
         c = ctypes
         lib.oracle_terrain_open_stage.argtypes = [c.POINTER(TosArrays), c.POINTER(TosMetrics)] + [c.c_int] * 4 + \
-            [c.c_float, c.c_int, c.c_float, c.c_float, c.c_double, c.c_float, c.c_float, c.c_uint, c.POINTER(c.c_float)]
+            [C_REAL, c.c_int, C_REAL, C_REAL, c.c_double, C_REAL, C_REAL, c.c_uint, c.POINTER(C_REAL)]
         lib.oracle_terrain_open_stage.restype = c.c_int
-        lib.oracle_terrain_edge_weights.argtypes = [c.c_int, c.c_float, c.POINTER(c.c_float), c.POINTER(c.c_float)]
+        lib.oracle_terrain_edge_weights.argtypes = [c.c_int, C_REAL, c.POINTER(C_REAL), c.POINTER(C_REAL)]
         lib.oracle_terrain_edge_weights.restype = None
         lib.oracle_terrain_open_stage_column.argtypes = [c.POINTER(TosArrays), c.POINTER(TosMetrics)] + \
-            [c.c_int] * 4 + [c.c_float, c.c_int, c.c_float, c.c_float] + [_F] * 4 + [c.c_float, _F] + \
-            [c.c_float, c.c_float, c.c_uint, c.POINTER(c.c_float)]
+            [c.c_int] * 4 + [C_REAL, c.c_int, C_REAL, C_REAL] + [_F] * 4 + [C_REAL, _F] + \
+            [C_REAL, C_REAL, c.c_uint, c.POINTER(C_REAL)]
         lib.oracle_terrain_open_stage_column.restype = c.c_int
         lib.oracle_terrain_open_stage_flat.argtypes = [c.POINTER(TosArrays), c.POINTER(TosMetrics)] + \
-            [c.c_int] * 4 + [c.c_float, c.c_int, c.c_float, c.c_float, _F, _F, c.c_float, c.c_uint] + \
-            [c.c_float, c.c_float, c.c_uint, c.POINTER(c.c_float)]
+            [c.c_int] * 4 + [C_REAL, c.c_int, C_REAL, C_REAL, _F, _F, C_REAL, c.c_uint] + \
+            [C_REAL, C_REAL, c.c_uint, c.POINTER(C_REAL)]
         lib.oracle_terrain_open_stage_flat.restype = c.c_int
         lib._tos_ready = True
     return lib
@@ -66,7 +66,7 @@ def _bind(struct_type, names, d):
     s = struct_type()
     for n in names:
         v = d[n]
-        assert v.dtype == np.float32 and v.flags.c_contiguous, n
+        assert v.dtype == REAL and v.flags.c_contiguous, n
         setattr(s, n, v.ctypes.data_as(_F))
     return s
 
@@ -74,7 +74,7 @@ def _bind(struct_type, names, d):
 def terrain_open_stage(a, m, *, ni, nj, nk, nrk, dt, nsound, dx, dy, dz, alph=0.6, kdiv=0.1,
                        ablations=ALL_ABLATIONS) -> StageDiagnostics:
     sa, sm = _bind(TosArrays, ARRAY_NAMES, a), _bind(TosMetrics, METRIC_NAMES, m)
-    diag = (ctypes.c_float * 3)()
+    diag = (C_REAL * 3)()
     rc = _lib().oracle_terrain_open_stage(ctypes.byref(sa), ctypes.byref(sm), ni, nj, nk, nrk, dt, nsound, dx, dy,
                                          float(dz), alph, kdiv, ablations, diag)
     if rc != 0:
@@ -88,9 +88,9 @@ def terrain_open_stage_column(a, m, column, *, ni, nj, nk, nrk, dt, nsound, dx, 
     sigmaf, rds, rdsf (CM1-indexed float32 profiles), ztop and rho0p (the
     padded base density, (nk+2, nj+6, ni+6))."""
     sa, sm = _bind(TosArrays, ARRAY_NAMES, a), _bind(TosMetrics, METRIC_NAMES, m)
-    prof = {n: np.ascontiguousarray(column[n], dtype=np.float32) for n in ("sigma", "sigmaf", "rds", "rdsf", "rho0p")}
+    prof = {n: np.ascontiguousarray(column[n], dtype=REAL) for n in ("sigma", "sigmaf", "rds", "rdsf", "rho0p")}
     assert prof["rho0p"].shape == (nk + 2, nj + 6, ni + 6)
-    diag = (ctypes.c_float * 3)()
+    diag = (C_REAL * 3)()
     ptr = {n: v.ctypes.data_as(_F) for n, v in prof.items()}
     rc = _lib().oracle_terrain_open_stage_column(ctypes.byref(sa), ctypes.byref(sm), ni, nj, nk, nrk, dt, nsound, dx,
                                                 dy, ptr["sigma"], ptr["sigmaf"], ptr["rds"], ptr["rdsf"],
@@ -106,9 +106,9 @@ def terrain_open_stage_flat(a, m, column, *, ni, nj, nk, nrk, dt, nsound, dx, dy
     """One stage on a flat stretched column: ``column`` maps mh (nk+2), mf
     (nk+3) and rdz; ``obc`` packs wbc | ebc << 4 | sbc << 8 | nbc << 12."""
     sa, sm = _bind(TosArrays, ARRAY_NAMES, a), _bind(TosMetrics, METRIC_NAMES, m)
-    mh = np.ascontiguousarray(column["mh"], dtype=np.float32)
-    mf = np.ascontiguousarray(column["mf"], dtype=np.float32)
-    diag = (ctypes.c_float * 3)()
+    mh = np.ascontiguousarray(column["mh"], dtype=REAL)
+    mf = np.ascontiguousarray(column["mf"], dtype=REAL)
+    diag = (C_REAL * 3)()
     rc = _lib().oracle_terrain_open_stage_flat(ctypes.byref(sa), ctypes.byref(sm), ni, nj, nk, nrk, dt, nsound, dx, dy,
                                               mh.ctypes.data_as(_F), mf.ctypes.data_as(_F),
                                               float(np.float32(column["rdz"])), obc, alph, kdiv, ablations, diag)
@@ -122,7 +122,7 @@ def terrain_open_three_stage(a, m, **kw) -> tuple[StageDiagnostics, ...]:
 
 
 def edge_weights(nk: int, dz: float) -> tuple[tuple[float, ...], tuple[float, ...]]:
-    cgs, cgt = (ctypes.c_float * 3)(), (ctypes.c_float * 3)()
+    cgs, cgt = (C_REAL * 3)(), (C_REAL * 3)()
     _lib().oracle_terrain_edge_weights(nk, dz, cgs, cgt)
     return tuple(cgs), tuple(cgt)
 

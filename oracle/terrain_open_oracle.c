@@ -28,6 +28,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include "real.h"  /* before the header: its array structs take the working precision */
 #include "../include/gm1b.h"
 
 int oracle_stage_schedule(float dt, int nsound, int nrk, int *nloop, float *dts);

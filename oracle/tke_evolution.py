@@ -10,9 +10,9 @@ import hashlib
 
 import numpy as np
 
-from oracle.periodic import load
+from oracle.periodic import C_REAL, REAL, load
 
-_F = ctypes.POINTER(ctypes.c_float)
+_F = ctypes.POINTER(C_REAL)
 DIFFUSION_NAMES = ("tke3d", "kmh", "kmv", "rho", "rf", "mh", "mf", "gz", "rgz", "rgzu", "rgzv", "tketen")
 STAGE_NAMES = ("tkea", "tketen", "c1", "c2", "rrf0", "gz", "rru", "rrv", "rrw", "divx")
 
@@ -20,7 +20,7 @@ STAGE_NAMES = ("tkea", "tketen", "c1", "c2", "rrf0", "gz", "rru", "rrv", "rrw", 
 def _lib():
     lib = load()
     if not getattr(lib, "_tkeevo_ready", False):
-        i, f = ctypes.c_int, ctypes.c_float
+        i, f = ctypes.c_int, C_REAL
         lib.oracle_tke_diffusion.argtypes = [i, i, i] + [_F] * 12 + [f, f, f, f]
         lib.oracle_tke_diffusion.restype = i
         lib.oracle_tke_rk_stage.argtypes = [i, i, i] + [_F] * 12 + [i, f, f, f, f]
@@ -34,7 +34,7 @@ def _lib():
 
 
 def _p(a):
-    assert a.dtype == np.float32 and a.flags.c_contiguous
+    assert a.dtype == REAL and a.flags.c_contiguous
     return a.ctypes.data_as(_F)
 
 

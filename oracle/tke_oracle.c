@@ -16,6 +16,7 @@
 #include <math.h>
 #include <stddef.h>
 #include <stdint.h>
+#include "real.h"
 
 typedef struct {
     const float *ruh, *rvh, *rmf, *nm, *defv, *defh;

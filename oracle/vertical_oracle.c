@@ -17,6 +17,7 @@
 #include <math.h>
 #include <stdint.h>
 #include <string.h>
+#include "real.h"
 
 typedef struct {
     int32_t nk1, nk2, nk3;
