@@ -675,10 +675,200 @@ __global__ void __launch_bounds__(256) kessler_recapture_kernel(gm1b_kessler_arr
 }  // namespace
 }  // namespace gm1b
 
-extern "C" int32_t gm1b_kessler_large_step(int32_t ni, int32_t nj, int32_t nk, const gm1b_kessler_arrays *arrays,
-                                           const gm1b_kessler_held *held, float dx, float dy, float dz, float dt,
-                                           int32_t equation_set, int32_t efall, void *workspace,
-                                           size_t workspace_size, void *stream) {
+// ---------------------------------------------------------------------------
+// final-RK dry-air mass correction, apmasscon = 1 (cpu_initial_dry_mass and
+// cpu_apmasscon_inplace, src/cm1core/cuda_apmasscon.py:190-325; CM1
+// init3d.F:2483-2527, solve2.F:1616-1656 and :1972-2030): per level the dry
+// mass ((rho*ruh)*rvh)*rmh and the Exner words pi0 + pp3d summed in binary64,
+// the levels summed in order, the uniform Exner correction
+// ((mass1/mass2)^rddcv - 1) * sum(pi) / cells in binary64 and rounded to
+// binary32, then pp3d += correction and prs, rho rebuilt from the equation
+// of state.  One CTA per level forms the level sums in a fixed order (each
+// thread a strided binary64 partial, then a shared-memory tree), as the
+// reference's CUDA reduction does; the twin sums each level serially, so
+// the two ledgers agree to binary64 rounding.
+// ---------------------------------------------------------------------------
+namespace gm1b {
+namespace {
+
+struct MassArgs {
+    const float *ruh, *rvh, *rmh, *pi0, *th0, *th3d, *qv;
+    float *pp3d, *prs, *rho, *rr;
+    int ni, nj, nk;
+};
+
+constexpr int kMassThreads = 256;
+
+__global__ void __launch_bounds__(kMassThreads) apmasscon_levels_kernel(MassArgs a, double *layers, int pressure) {
+    __shared__ double s_dry[kMassThreads], s_pi[kMassThreads];
+    const int k = blockIdx.x;
+    const size_t nxy = (size_t)a.ni * a.nj, base = (size_t)k * nxy;
+    double dry = 0.0, pis = 0.0;
+    for (size_t ij = threadIdx.x; ij < nxy; ij += kMassThreads) {
+        const int i = (int)(ij % a.ni), j = (int)(ij / a.ni);
+        const size_t q = base + ij;
+        float term = a.rho[q] * __ldg(a.ruh + i);
+        term = term * __ldg(a.rvh + j);
+        term = term * __ldg(a.rmh + q);
+        dry += (double)term;
+        if (pressure) pis += (double)(__ldg(a.pi0 + q) + a.pp3d[q]);
+    }
+    s_dry[threadIdx.x] = dry;
+    s_pi[threadIdx.x] = pis;
+    __syncthreads();
+    for (int stride = kMassThreads / 2; stride > 0; stride >>= 1) {
+        if (threadIdx.x < stride) {
+            s_dry[threadIdx.x] += s_dry[threadIdx.x + stride];
+            s_pi[threadIdx.x] += s_pi[threadIdx.x + stride];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        layers[k] = s_dry[0];
+        layers[a.nk + k] = s_pi[0];
+    }
+}
+
+// the dry-mass ledger (levels in order) into mass[0]; with only_if_unset a
+// non-zero mass[0] (a ledger already held, e.g. restored) is kept
+__global__ void dry_mass_finish_kernel(const double *layers, int nk, double *mass, int only_if_unset) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    if (only_if_unset && mass[0] != 0.0) return;
+    double total = 0.0;
+    for (int k = 0; k < nk; ++k) total += layers[k];
+    mass[0] = total;
+}
+
+// diag: mass2, the Exner sum, the binary64 correction, mass1
+__global__ void apmasscon_finish_kernel(const double *layers, int nk, const double *mass1, double cells, float rddcv,
+                                        float *correction, double *diag) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    double mass2 = 0.0, pis = 0.0;
+    for (int k = 0; k < nk; ++k) {
+        mass2 += layers[k];
+        pis += layers[nk + k];
+    }
+    double value = pow(mass1[0] / mass2, (double)rddcv) - 1.0;
+    value = value * pis;
+    value = value / cells;
+    correction[0] = (float)value;
+    if (diag != nullptr) {
+        diag[0] = mass2;
+        diag[1] = pis;
+        diag[2] = value;
+        diag[3] = mass1[0];
+    }
+}
+
+__global__ void __launch_bounds__(256) apmasscon_apply_kernel(MassArgs a, const float *correction, size_t n,
+                                                              KesslerEos c) {
+    const float corr = correction[0];
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+        const float pp = a.pp3d[q] + corr;
+        const float pi = __ldg(a.pi0 + q) + pp;
+        const float prs = c.p00 * powf(pi, c.cpdrd);
+        const float theta = __ldg(a.th0 + q) + __ldg(a.th3d + q);
+        const float vapor = fmaxf(0.0f, __ldg(a.qv + q));
+        const float gas = c.rd + vapor * c.rv;
+        float den = theta * pi;
+        den = den * gas;
+        const float rho = prs / den;
+        a.pp3d[q] = pp;
+        a.prs[q] = prs;
+        a.rho[q] = rho;
+        if (a.rr != nullptr) a.rr[q] = rho;
+    }
+}
+
+KesslerEos mass_eos() {
+    const float cp = 1005.7f, rd = 287.04f;
+    return KesslerEos{(float)((double)cp / (double)rd), 100000.0f, rd, 461.5f};
+}
+
+float mass_rddcv() {
+    const float cp = 1005.7f, rd = 287.04f;
+    const float cv = cp - rd;
+    return rd / cv;
+}
+
+size_t mass_workspace_bytes(int nk) { return sizeof(double) * (2 * (size_t)nk + 2); }
+
+int32_t mass_correction(const MassArgs &m, const double *mass1, double *diag, void *workspace, cudaStream_t st) {
+    double *layers = static_cast<double *>(workspace);
+    float *corr = reinterpret_cast<float *>(layers + 2 * (size_t)m.nk);
+    const size_t n = (size_t)m.ni * m.nj * m.nk;
+    {
+        ProfScope ps("apmasscon_levels_kernel", st);
+        apmasscon_levels_kernel<<<m.nk, kMassThreads, 0, st>>>(m, layers, 1);
+        ps.stop();
+    }
+    if (!launched("apmasscon_levels_kernel")) return GM1B_ERR_CUDA;
+    apmasscon_finish_kernel<<<1, 1, 0, st>>>(layers, m.nk, mass1, (double)n, mass_rddcv(), corr, diag);
+    if (!launched("apmasscon_finish_kernel")) return GM1B_ERR_CUDA;
+    const unsigned grid = (unsigned)std::min<size_t>((n + 255) / 256, (size_t)148 * 8);
+    {
+        ProfScope ps("apmasscon_apply_kernel", st);
+        apmasscon_apply_kernel<<<grid, 256, 0, st>>>(m, corr, n, mass_eos());
+        ps.stop();
+    }
+    return launched("apmasscon_apply_kernel") ? GM1B_OK : GM1B_ERR_CUDA;
+}
+
+bool mass_grid_ok(const char *who, int32_t ni, int32_t nj, int32_t nk) {
+    if (ni < 1 || nj < 1 || nk < 1 || nk > 65535) {
+        gm1b_set_error("%s: need ni, nj >= 1 and 1 <= nk <= 65535", who);
+        return false;
+    }
+    return true;
+}
+
+}  // namespace
+}  // namespace gm1b
+
+extern "C" size_t gm1b_apmasscon_workspace_bytes(int32_t nk) { return nk < 1 ? 0 : mass_workspace_bytes(nk); }
+
+extern "C" int32_t gm1b_dry_mass(int32_t ni, int32_t nj, int32_t nk, const float *rho, const float *ruh,
+                                 const float *rvh, const float *rmh, double *mass, int32_t only_if_unset,
+                                 void *workspace, void *stream) {
+    if (!mass_grid_ok("gm1b_dry_mass", ni, nj, nk)) return GM1B_ERR_ARGUMENT;
+    if (rho == nullptr || ruh == nullptr || rvh == nullptr || rmh == nullptr || mass == nullptr ||
+        workspace == nullptr) {
+        gm1b_set_error("gm1b_dry_mass: rho, ruh, rvh, rmh, mass and the workspace are required");
+        return GM1B_ERR_ARGUMENT;
+    }
+    MassArgs m{ruh, rvh, rmh, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, const_cast<float *>(rho), nullptr,
+               ni, nj, nk};
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    double *layers = static_cast<double *>(workspace);
+    apmasscon_levels_kernel<<<nk, kMassThreads, 0, st>>>(m, layers, 0);
+    if (!launched("apmasscon_levels_kernel")) return GM1B_ERR_CUDA;
+    dry_mass_finish_kernel<<<1, 1, 0, st>>>(layers, nk, mass, only_if_unset ? 1 : 0);
+    return launched("dry_mass_finish_kernel") ? GM1B_OK : GM1B_ERR_CUDA;
+}
+
+extern "C" int32_t gm1b_apmasscon(int32_t ni, int32_t nj, int32_t nk, const gm1b_apmasscon_arrays *arrays,
+                                  const double *mass1, double *diagnostics, void *workspace, void *stream) {
+    if (!mass_grid_ok("gm1b_apmasscon", ni, nj, nk)) return GM1B_ERR_ARGUMENT;
+    if (arrays == nullptr || mass1 == nullptr || workspace == nullptr) {
+        gm1b_set_error("gm1b_apmasscon: arrays, mass1 and the workspace are required");
+        return GM1B_ERR_ARGUMENT;
+    }
+    const gm1b_apmasscon_arrays &a = *arrays;
+    const void *need[] = {a.ruh, a.rvh, a.rmh, a.pi0, a.th0, a.th3d, a.qv, a.pp3d, a.prs, a.rho};
+    for (const void *q : need)
+        if (q == nullptr) {
+            gm1b_set_error("gm1b_apmasscon: a required array is NULL");
+            return GM1B_ERR_ARGUMENT;
+        }
+    const MassArgs m{a.ruh, a.rvh, a.rmh, a.pi0, a.th0, a.th3d, a.qv, a.pp3d, a.prs, a.rho, nullptr, ni, nj, nk};
+    return mass_correction(m, mass1, diagnostics, workspace, static_cast<cudaStream_t>(stream));
+}
+
+namespace {
+int32_t kessler_large_step(int32_t ni, int32_t nj, int32_t nk, const gm1b_kessler_arrays *arrays,
+                           const gm1b_kessler_held *held, float dx, float dy, float dz, float dt, int32_t equation_set,
+                           int32_t efall, void *workspace, size_t workspace_size, const double *mass1,
+                           double *mass_diagnostics, void *mass_workspace, void *stream) {
     if (arrays == nullptr || ni < 1 || nj < 1 || nk < 2) {
         gm1b_set_error("gm1b_kessler_large_step: need arrays, ni >= 1, nj >= 1, nk >= 2");
         return GM1B_ERR_ARGUMENT;
@@ -707,6 +897,13 @@ extern "C" int32_t gm1b_kessler_large_step(int32_t ni, int32_t nj, int32_t nk, c
         ps.stop();
     }
     if (!launched("kessler_pre_physics_kernel")) return GM1B_ERR_CUDA;
+    if (mass1 != nullptr) {  // apmasscon between the pre-physics EOS and the driver
+        const gm1b_kessler_arrays &k = *arrays;
+        const MassArgs m{k.ruh, k.rvh, k.rmh, k.pi0, k.th0, k.th3d, k.qv, k.pp3d, k.prs, k.rho,
+                         const_cast<float *>(k.rr), ni, nj, nk};
+        const int32_t mrc = mass_correction(m, mass1, mass_diagnostics, mass_workspace, st);
+        if (mrc != GM1B_OK) return mrc;
+    }
     const int32_t rc = gm1b_kessler_driver(ni, nj, nk, arrays, dx, dy, dz, dt, equation_set, efall, workspace,
                                            workspace_size, stream);
     if (rc != GM1B_OK || !eqt2) return rc;
@@ -716,4 +913,32 @@ extern "C" int32_t gm1b_kessler_large_step(int32_t ni, int32_t nj, int32_t nk, c
         ps.stop();
     }
     return launched("kessler_recapture_kernel") ? GM1B_OK : GM1B_ERR_CUDA;
+}
+}  // namespace
+
+extern "C" int32_t gm1b_kessler_large_step(int32_t ni, int32_t nj, int32_t nk, const gm1b_kessler_arrays *arrays,
+                                           const gm1b_kessler_held *held, float dx, float dy, float dz, float dt,
+                                           int32_t equation_set, int32_t efall, void *workspace,
+                                           size_t workspace_size, void *stream) {
+    return kessler_large_step(ni, nj, nk, arrays, held, dx, dy, dz, dt, equation_set, efall, workspace,
+                              workspace_size, nullptr, nullptr, nullptr, stream);
+}
+
+extern "C" int32_t gm1b_kessler_large_step_apmasscon(int32_t ni, int32_t nj, int32_t nk,
+                                                     const gm1b_kessler_arrays *arrays, const gm1b_kessler_held *held,
+                                                     float dx, float dy, float dz, float dt, int32_t equation_set,
+                                                     int32_t efall, void *workspace, size_t workspace_size,
+                                                     const double *mass1, double *mass_diagnostics,
+                                                     void *mass_workspace, void *stream) {
+    if (mass1 == nullptr || mass_workspace == nullptr || arrays == nullptr || arrays->ruh == nullptr ||
+        arrays->rvh == nullptr || arrays->rmh == nullptr) {
+        gm1b_set_error("gm1b_kessler_large_step_apmasscon: mass1, the mass workspace and ruh, rvh, rmh are required");
+        return GM1B_ERR_ARGUMENT;
+    }
+    if (nk > 65535) {
+        gm1b_set_error("gm1b_kessler_large_step_apmasscon: nk <= 65535");
+        return GM1B_ERR_ARGUMENT;
+    }
+    return kessler_large_step(ni, nj, nk, arrays, held, dx, dy, dz, dt, equation_set, efall, workspace,
+                              workspace_size, mass1, mass_diagnostics, mass_workspace, stream);
 }

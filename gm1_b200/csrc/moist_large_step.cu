@@ -62,6 +62,7 @@ struct gm1b_moist_step {
     cudaEvent_t ev[16] = {};
     void *kessler_ws = nullptr;
     size_t kessler_ws_bytes = 0;
+    void *mass_ws = nullptr;  // the dry-mass correction's level sums
     int32_t *status_acc = nullptr;  // 8 words
     float *courant = nullptr;       // 1 word
     uint32_t *courant_keys = nullptr;
@@ -496,8 +497,12 @@ int microphysics(Step &h, cudaStream_t st) {
     k.asq = s.asq;
     k.qbudget = s.qbudget;
     gm1b_kessler_held held{s.qpten, s.qtten, s.qvten, s.qcten};
-    TRY(gm1b_kessler_large_step(c.ni, c.nj, c.nk, &k, &held, c.dx, c.dy, c.dz, c.dt, 2, 0, h.kessler_ws,
-                                h.kessler_ws_bytes, st));
+    if (c.apmasscon)
+        TRY(gm1b_kessler_large_step_apmasscon(c.ni, c.nj, c.nk, &k, &held, c.dx, c.dy, c.dz, c.dt, 2, 0,
+                                              h.kessler_ws, h.kessler_ws_bytes, s.mass1, nullptr, h.mass_ws, st));
+    else
+        TRY(gm1b_kessler_large_step(c.ni, c.nj, c.nk, &k, &held, c.dx, c.dy, c.dz, c.dt, 2, 0, h.kessler_ws,
+                                    h.kessler_ws_bytes, st));
     TRY(fold(h, static_cast<const int32_t *>(h.kessler_ws), nullptr, st));
     return pp3d_compact(h, false, st);
 }
@@ -529,7 +534,8 @@ void release(Step *h) {
         if (q) cudaStreamDestroy(q);
     for (auto &e : h->ev)
         if (e) cudaEventDestroy(e);
-    void *bufs[] = {h->kessler_ws, h->status_acc, h->courant, h->courant_keys, h->ones_i, h->ones_j, h->mh_col};
+    void *bufs[] = {h->kessler_ws, h->status_acc, h->courant, h->courant_keys, h->ones_i, h->ones_j, h->mh_col,
+                    h->mass_ws};
     for (void *b : bufs)
         if (b) cudaFree(b);
     delete h;
@@ -594,6 +600,8 @@ extern "C" int32_t gm1b_moist_step_create(const gm1b_moist_step_config *config, 
     if (good) good = ok(cudaMalloc(&h->ones_i, (size_t)c.ni * sizeof(float)), "cudaMalloc");
     if (good) good = ok(cudaMalloc(&h->ones_j, (size_t)c.nj * sizeof(float)), "cudaMalloc");
     if (good) good = ok(cudaMalloc(&h->mh_col, (size_t)c.nk * sizeof(float)), "cudaMalloc");
+    if (good && c.apmasscon)
+        good = ok(cudaMalloc(&h->mass_ws, gm1b_apmasscon_workspace_bytes(c.nk)), "cudaMalloc (mass workspace)");
     if (good) {
         // uh = vh = 1 (uniform horizontal grid) and the mh column (the first
         // column of the 3-D mh), the Courant reduction's metric inputs
@@ -606,6 +614,13 @@ extern "C" int32_t gm1b_moist_step_create(const gm1b_moist_step_config *config, 
                ok(cudaMemset(h->status_acc, 0, 8 * sizeof(int32_t)), "status") &&
                ok(cudaMemset(h->kessler_ws, 0, h->kessler_ws_bytes), "Kessler workspace") &&
                ok(cudaDeviceSynchronize(), "set-up");
+    }
+    if (good && c.apmasscon) {
+        // init3d.F:2483-2527: the initial dry-air mass of the state, unless it
+        // carries one already
+        good = gm1b_dry_mass(c.ni, c.nj, c.nk, state->rho, state->ruh, state->rvh, metrics->rmh, state->mass1, 1,
+                             h->mass_ws, nullptr) == GM1B_OK &&
+               ok(cudaDeviceSynchronize(), "dry-mass ledger");
     }
     if (!good) {
         release(h);

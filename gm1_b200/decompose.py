@@ -17,7 +17,9 @@ next step reads them; the outer ghost cells of a halo are scratch of the fake
 edge.  Exchanges run in two phases, x then y over the x-widened rows, so the
 corner halos come from the diagonal neighbour through the x neighbour's
 fresh strip.  The FP64 Kessler budgets (asq, qbudget) accumulate over each
-rank's widened subdomain and are not reduced here.
+rank's widened subdomain and are not reduced here; the final-RK dry-air mass
+correction, a domain-wide reduction, is refused (local_steps) - a decomposed
+configuration runs with apmasscon=False.
 
 The exchange (one message per neighbour per phase, packed contiguous) runs
 over torch.distributed point-to-point sends (gloo on CPU tensors, NCCL on
@@ -303,6 +305,12 @@ def local_steps(cfg, host: Mapping[str, np.ndarray], metrics: Mapping[str, np.nd
     widened ni, nj)."""
     import dataclasses  # noqa: PLC0415
 
+    from .errors import refuse  # noqa: PLC0415
+
+    if getattr(cfg, "apmasscon", False) and len(subs) > 1:
+        refuse(code="GM1B-DECOMPOSE-APMASSCON", gate="decomposition", option="apmasscon", value=True,
+               reason="the dry-air mass correction is a domain-wide reduction; each widened subdomain would correct "
+                      "against its own ledger", remedy="decompose a configuration with apmasscon=False")
     out = {}
     for s in subs:
         if s.rank not in ranks:

@@ -7,6 +7,7 @@ CuPy arrays; the same array names, shapes, dtypes, keywords and refusals):
   gm1_kessler_driver_shapes                 src/cm1core/cuda_gm1_kessler_driver.py:183-206
   create_cuda_gm1_kessler_driver_workspace  src/cm1core/cuda_gm1_kessler_driver.py:806
   launch_cuda_gm1_kessler_driver            src/cm1core/cuda_gm1_kessler_driver.py:907
+  launch_cuda_apmasscon, cpu_initial_dry_mass  src/cm1core/cuda_apmasscon.py:596, :226
 
 Only efall = 0 is built (the benchmark configurations use it); efall = 1 is
 refused by name.  Device faults never stand in for errors: the saturation
@@ -246,12 +247,20 @@ class CudaGm1KesslerLargeStepTransition:
 
     def __init__(self, arrays: dict[str, torch.Tensor], carriers: Gm1KesslerHeldCarriers, *, ni: int, nj: int,
                  nk: int, dx: float, dy: float, dz: float, dt: float, selection: Gm1KesslerDriverSelection,
-                 stream: Any, workspace: Gm1KesslerDriverWorkspace, completed_transitions: int = 0) -> None:
+                 stream: Any, workspace: Gm1KesslerDriverWorkspace, completed_transitions: int = 0,
+                 mass1: torch.Tensor | None = None) -> None:
         self.arrays, self.carriers = arrays, carriers
         self.ni, self.nj, self.nk = ni, nj, nk
         self.dx, self.dy, self.dz, self.dt = dx, dy, dz, dt
         self.selection, self.stream, self.workspace = selection, stream, workspace
         self.completed_transitions = completed_transitions
+        # with a dry-mass ledger: the final-RK dry-air mass correction between
+        # the pre-physics equation of state and the driver (the reference's
+        # dry-mass hook at that point, CM1 apmasscon = 1)
+        self.mass1 = mass1
+        self.mass_workspace = None if mass1 is None else torch.empty(
+            (_apmasscon_lib().gm1b_apmasscon_workspace_bytes(nk) + 7) // 8, dtype=torch.float64, device=mass1.device)
+        self.mass_diagnostics = None if mass1 is None else torch.zeros(4, dtype=torch.float64, device=mass1.device)
 
     def apply(self, *, final_rk: bool = True, refl_10cm_due: bool = False,
               pre_component_hook: Any | None = None) -> Gm1KesslerLargeStepResult:
@@ -283,19 +292,28 @@ class CudaGm1KesslerLargeStepTransition:
             lib.gm1b_kessler_large_step.restype = c.c_int32
             lib._kls_bound = True
         with torch.cuda.device(device):
-            _native.check(lib.gm1b_kessler_large_step(self.ni, self.nj, self.nk, ctypes.byref(s), ctypes.byref(held),
-                                                      self.dx, self.dy, self.dz, self.dt, self.selection.equation_set,
-                                                      self.selection.efall,
-                                                      ctypes.c_void_p(self.workspace.buffer.data_ptr()),
-                                                      self.workspace.buffer.numel(), ctypes.c_void_p(st.cuda_stream)),
-                          "gm1b_kessler_large_step")
+            if self.mass1 is None:
+                _native.check(lib.gm1b_kessler_large_step(
+                    self.ni, self.nj, self.nk, ctypes.byref(s), ctypes.byref(held), self.dx, self.dy, self.dz,
+                    self.dt, self.selection.equation_set, self.selection.efall,
+                    ctypes.c_void_p(self.workspace.buffer.data_ptr()), self.workspace.buffer.numel(),
+                    ctypes.c_void_p(st.cuda_stream)), "gm1b_kessler_large_step")
+            else:
+                _native.check(_apmasscon_lib().gm1b_kessler_large_step_apmasscon(
+                    self.ni, self.nj, self.nk, ctypes.byref(s), ctypes.byref(held), self.dx, self.dy, self.dz,
+                    self.dt, self.selection.equation_set, self.selection.efall,
+                    ctypes.c_void_p(self.workspace.buffer.data_ptr()), self.workspace.buffer.numel(),
+                    ctypes.c_void_p(self.mass1.data_ptr()), ctypes.c_void_p(self.mass_diagnostics.data_ptr()),
+                    ctypes.c_void_p(self.mass_workspace.data_ptr()), ctypes.c_void_p(st.cuda_stream)),
+                    "gm1b_kessler_large_step_apmasscon")
             ev = torch.cuda.Event()
             ev.record(st)
         self.completed_transitions += 1
         return Gm1KesslerLargeStepResult(ev, self.completed_transitions, {
             "operator": "gm1-kessler-large-step", "equation_set": self.selection.equation_set,
-            "source_order": ("solve2-held-remove-snapshot", "solve2-pre-physics-eos", "cm1-mp_driver-ptype1",
-                             "solve3-held-recapture"),
+            "source_order": ("solve2-held-remove-snapshot", "solve2-pre-physics-eos") +
+                            (() if self.mass1 is None else ("solve2-apmasscon",)) +
+                            ("cm1-mp_driver-ptype1", "solve3-held-recapture"),
             "domain": {"ni": self.ni, "nj": self.nj, "nk": self.nk}})
 
 
@@ -303,7 +321,8 @@ def create_cuda_gm1_kessler_large_step_transition(
         arrays: Mapping[str, Any], *, ni: int, nj: int, nk: int, dx: float, dy: float, dz: float, dt: float,
         selection: Gm1KesslerDriverSelection, stream: Any | None = None,
         workspace: Gm1KesslerDriverWorkspace | None = None,
-        carriers: Gm1KesslerHeldCarriers | None = None) -> CudaGm1KesslerLargeStepTransition:
+        carriers: Gm1KesslerHeldCarriers | None = None,
+        mass1: torch.Tensor | None = None) -> CudaGm1KesslerLargeStepTransition:
     """Bind an already Kessler-initialised device state.  rr, fall_velocity,
     rain, prate, asq and qbudget are allocated (zero) when absent, as are the
     held carriers (the reference's fresh-start restart state)."""
@@ -340,5 +359,127 @@ def create_cuda_gm1_kessler_large_step_transition(
             raise ValueError(f"held {n} must be C-order CUDA float32 with shape {mass}")
     if workspace is None:
         workspace = create_cuda_gm1_kessler_driver_workspace(ni=ni, nj=nj, nk=nk, device=device)
+    if mass1 is not None and (not isinstance(mass1, torch.Tensor) or mass1.dtype != torch.float64
+                              or tuple(mass1.shape) != (1,) or mass1.device != device):
+        raise ValueError("mass1 must be a one-word float64 tensor on the state's device")
     return CudaGm1KesslerLargeStepTransition(bound, carriers, ni=ni, nj=nj, nk=nk, dx=dx, dy=dy, dz=dz, dt=dt,
-                                             selection=selection, stream=stream, workspace=workspace)
+                                             selection=selection, stream=stream, workspace=workspace, mass1=mass1)
+
+
+# ---------------------------------------------------------------------------
+# the final-RK dry-air mass correction (apmasscon = 1)
+# ---------------------------------------------------------------------------
+APMASSCON_INPUT_NAMES = ("ruh", "rvh", "rmh", "pi0", "th0", "th3d", "qv")
+APMASSCON_MUTABLE_NAMES = ("pp3d", "prs", "rho")
+APMASSCON_ARRAY_NAMES = APMASSCON_INPUT_NAMES + APMASSCON_MUTABLE_NAMES
+
+
+class _ApMassConArrays(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_void_p) for n in APMASSCON_ARRAY_NAMES]
+
+
+def _apmasscon_lib() -> ctypes.CDLL:
+    lib = _native.lib()
+    if not getattr(lib, "_apmasscon_bound", False):
+        c = ctypes
+        lib.gm1b_apmasscon_workspace_bytes.argtypes = [c.c_int32]
+        lib.gm1b_apmasscon_workspace_bytes.restype = c.c_size_t
+        lib.gm1b_apmasscon.argtypes = [c.c_int32] * 3 + [c.POINTER(_ApMassConArrays), c.c_void_p, c.c_void_p,
+                                                         c.c_void_p, c.c_void_p]
+        lib.gm1b_apmasscon.restype = c.c_int32
+        lib.gm1b_dry_mass.argtypes = [c.c_int32] * 3 + [c.c_void_p] * 5 + [c.c_int32, c.c_void_p, c.c_void_p]
+        lib.gm1b_dry_mass.restype = c.c_int32
+        lib.gm1b_kessler_large_step_apmasscon.argtypes = [c.c_int32] * 3 + [c.POINTER(_KesslerArrays),
+                                                                            c.POINTER(_HeldArrays)] + \
+            [c.c_float] * 4 + [c.c_int32, c.c_int32, c.c_void_p, c.c_size_t] + [c.c_void_p] * 4
+        lib.gm1b_kessler_large_step_apmasscon.restype = c.c_int32
+        lib._apmasscon_bound = True
+    return lib
+
+
+def apmasscon_array_shapes(ni: int, nj: int, nk: int) -> dict[str, tuple[int, ...]]:
+    scalar = (nk, nj, ni)
+    return {"ruh": (ni,), "rvh": (nj,), **{n: scalar for n in APMASSCON_ARRAY_NAMES if n not in ("ruh", "rvh")}}
+
+
+def _mass_arrays(arrays: Mapping[str, Any], ni: int, nj: int, nk: int) -> dict[str, torch.Tensor]:
+    shapes = apmasscon_array_shapes(ni, nj, nk)
+    missing = [n for n in APMASSCON_ARRAY_NAMES if n not in arrays]
+    if missing:
+        raise ValueError(f"missing apmasscon arrays: {', '.join(missing)}")
+    out = {}
+    for n in APMASSCON_ARRAY_NAMES:
+        t = arrays[n]
+        if not isinstance(t, torch.Tensor) or not t.is_cuda or t.dtype != torch.float32 \
+                or tuple(t.shape) != shapes[n] or not t.is_contiguous():
+            raise ValueError(f"{n} must be C-order CUDA float32 with shape {shapes[n]}")
+        out[n] = t
+    if len({t.data_ptr() for t in out.values()}) != len(out):
+        raise ValueError("apmasscon arrays must not alias")
+    return out
+
+
+def _mass_word(mass1: Any, device: torch.device) -> torch.Tensor:
+    if isinstance(mass1, torch.Tensor):
+        if mass1.dtype != torch.float64 or tuple(mass1.shape) != (1,) or mass1.device != device:
+            raise ValueError("mass1 must be a one-word float64 tensor on the arrays' device")
+        return mass1
+    if isinstance(mass1, bool) or not isinstance(mass1, (int, float)) or not math.isfinite(mass1) or mass1 <= 0.0:
+        raise ValueError("mass1 must be a finite positive dry-air mass")
+    return torch.tensor([float(mass1)], dtype=torch.float64, device=device)
+
+
+@dataclass(frozen=True, slots=True)
+class CudaApMassConLaunch:
+    ready_event: Any
+    diagnostics: torch.Tensor  # mass2, Exner sum, binary64 correction, mass1
+    receipt: Mapping[str, Any]
+
+
+def launch_cuda_apmasscon(arrays: Mapping[str, Any], *, ni: int, nj: int, nk: int, mass1: Any,
+                          stream: Any | None = None) -> CudaApMassConLaunch:
+    """The final-RK dry-air mass correction in place (pp3d, prs, rho),
+    without host synchronization; mass1 a float or a one-word float64 device
+    tensor (the initial ledger)."""
+    for name, value in (("ni", ni), ("nj", nj), ("nk", nk)):
+        if type(value) is not int or value < 1:
+            raise ValueError(f"{name} must be an integer >= 1")
+    a = _mass_arrays(arrays, ni, nj, nk)
+    device = a["rho"].device
+    m1 = _mass_word(mass1, device)
+    lib = _apmasscon_lib()
+    work = torch.empty((lib.gm1b_apmasscon_workspace_bytes(nk) + 7) // 8, dtype=torch.float64, device=device)
+    diag = torch.zeros(4, dtype=torch.float64, device=device)
+    st = torch.cuda.current_stream(device) if stream is None else stream
+    s = _ApMassConArrays(**{n: a[n].data_ptr() for n in APMASSCON_ARRAY_NAMES})
+    with torch.cuda.device(device):
+        _native.check(lib.gm1b_apmasscon(ni, nj, nk, ctypes.byref(s), m1.data_ptr(), diag.data_ptr(), work.data_ptr(),
+                                         ctypes.c_void_p(st.cuda_stream)), "gm1b_apmasscon")
+        for t in (work, m1, diag):  # temporaries in use on st until it reaches here
+            t.record_stream(st)
+        ev = torch.cuda.Event()
+        ev.record(st)
+    return CudaApMassConLaunch(ev, diag, {"operator": "gm1-apmasscon", "domain": {"ni": ni, "nj": nj, "nk": nk},
+                                          "source_order": ("layer-reductions", "correction", "eos-rebuild")})
+
+
+def dry_mass(rho: torch.Tensor, ruh: torch.Tensor, rvh: torch.Tensor, rmh: torch.Tensor, *, ni: int, nj: int, nk: int,
+             out: torch.Tensor | None = None, only_if_unset: bool = False, stream: Any | None = None) -> torch.Tensor:
+    """The dry-air mass ledger of a state (cpu_initial_dry_mass) into a
+    one-word float64 device tensor; with only_if_unset a non-zero out is kept."""
+    device = rho.device
+    for n, t, shape in (("rho", rho, (nk, nj, ni)), ("ruh", ruh, (ni,)), ("rvh", rvh, (nj,)), ("rmh", rmh, (nk, nj, ni))):
+        if not isinstance(t, torch.Tensor) or not t.is_cuda or t.dtype != torch.float32 or tuple(t.shape) != shape \
+                or not t.is_contiguous():
+            raise ValueError(f"{n} must be C-order CUDA float32 with shape {shape}")
+    if out is None:
+        out = torch.zeros(1, dtype=torch.float64, device=device)
+    lib = _apmasscon_lib()
+    work = torch.empty((lib.gm1b_apmasscon_workspace_bytes(nk) + 7) // 8, dtype=torch.float64, device=device)
+    st = torch.cuda.current_stream(device) if stream is None else stream
+    with torch.cuda.device(device):
+        _native.check(lib.gm1b_dry_mass(ni, nj, nk, rho.data_ptr(), ruh.data_ptr(), rvh.data_ptr(), rmh.data_ptr(),
+                                        out.data_ptr(), 1 if only_if_unset else 0, work.data_ptr(),
+                                        ctypes.c_void_p(st.cuda_stream)), "gm1b_dry_mass")
+        work.record_stream(st)
+    return out

@@ -46,7 +46,8 @@ from . import _native
 from . import moist_ops as mo
 from .advection import launch_cuda_gm1_child_stretched_scalar_advection5, launch_cuda_scalar_advection5
 from .closure import launch_cuda_flat_deformation, launch_cuda_moist_nm, launch_cuda_terrain_deformation
-from .kessler import (Gm1KesslerDriverSelection, Gm1KesslerHeldCarriers, create_cuda_gm1_kessler_large_step_transition)
+from .kessler import (Gm1KesslerDriverSelection, Gm1KesslerHeldCarriers, create_cuda_gm1_kessler_large_step_transition,
+                      dry_mass)
 from .limits import CM1_COURANT_STOP, advective_courant_number
 from .moist_bridge import launch_cuda_eqtset2_stage_terms
 from .scalar_rk import (compose_scalar_moist_rk_stage, moisture_weps_f64, scalar_moist_rk_stage_timestep_f32,
@@ -159,6 +160,10 @@ class MoistStepConfig:
     # None: the uniform column (the terrain operator family on flat metrics);
     # a spec: the flat (terrain_flag=.false.) family on that stretched column
     column: StretchedColumnSpec | None = None
+    # the final-RK dry-air mass correction (CM1 apmasscon = 1, the supercell
+    # namelist's): between the pre-physics equation of state and the Kessler
+    # driver, against the state's mass1 ledger
+    apmasscon: bool = True
 
     @property
     def obc(self) -> int:
@@ -223,11 +228,11 @@ def moist_state_shapes(ni: int, nj: int, nk: int) -> dict[str, tuple[int, ...]]:
               "cme", "ce1", "ce2", "csm", "kmh", "kmv", "khh", "khv", "tke_workspace"):
         s[n] = face
     s.update(uc=(nk, nj, ni + 1), vc=(nk, nj + 1, ni), wc=face, th0=(nk,), pi0=(nk,), qv0=(nk,), rain=(1, nj, ni),
-             prate=plane, asq=(3,), qbudget=(10,), ruh=(ni,), rvh=(nj,))
+             prate=plane, asq=(3,), qbudget=(10,), ruh=(ni,), rvh=(nj,), mass1=(1,))
     return s
 
 
-MOIST_STATE_DTYPES = {"saturation_mask": np.uint8, "asq": np.float64, "qbudget": np.float64}
+MOIST_STATE_DTYPES = {"saturation_mask": np.uint8, "asq": np.float64, "qbudget": np.float64, "mass1": np.float64}
 
 METRIC_NAMES = ("terrain_msl", "zh", "zf", "mh", "rmh", "mf", "rmf", "c1", "c2", "rho0_3d", "rr0", "rf0", "rrf0", "gz",
                 "rgz", "gzu", "rgzu", "gzv", "rgzv", "dzdx", "dzdy", "gx", "gxu", "gy", "gyv")
@@ -435,13 +440,20 @@ class MoistLargeStep:
         dev = s["u3d"].device
         self.concurrent = concurrent
         self._side = [torch.cuda.Stream(dev) for _ in range(SIDE_STREAMS)] if concurrent else []
+        if cfg.apmasscon:
+            # init3d.F:2483-2527: the initial dry-air mass of the state, unless
+            # it carries one (a restored ledger)
+            with torch.cuda.stream(torch.cuda.current_stream(s["rho"].device) if stream is None else stream):
+                dry_mass(s["rho"], s["ruh"], s["rvh"], m["rmh"], ni=ni, nj=nj, nk=nk, out=s["mass1"],
+                         only_if_unset=True)
         self.kessler = create_cuda_gm1_kessler_large_step_transition(
             {"ruh": s["ruh"], "rvh": s["rvh"], "rmh": m["rmh"], "mh": m["mh"], "pi0": s["pi0_3d"], "th0": s["th0_3d"],
              "rr": s["kessler_rr"], "rho": s["rho"], "pp3d": s["pp3d_c"], "th3d": s["th3d"], "prs": s["prs"],
              "qv": self.q_rows[0], "qc": self.q_rows[1], "qr": self.q_rows[2], "fall_velocity": s["fall_velocity"],
              "rain": s["rain"], "prate": s["prate"], "asq": s["asq"], "qbudget": s["qbudget"]},
             **self.grid, dt=cfg.dt, selection=Gm1KesslerDriverSelection(equation_set=2), stream=stream,
-            carriers=Gm1KesslerHeldCarriers(s["qpten"], s["qtten"], s["qvten"], s["qcten"]))
+            carriers=Gm1KesslerHeldCarriers(s["qpten"], s["qtten"], s["qvten"], s["qcten"]),
+            mass1=s["mass1"] if cfg.apmasscon else None)
         from .momentum import _Arrays as _MomArrays, _Column, _lib as _mom_lib, _STRUCT as _MOM
 
         self._mom_lib = _mom_lib()
@@ -861,7 +873,7 @@ NATIVE_STATE_NAMES = (
     "uc", "vc", "wc", "th0", "pi0", "qv0", "rain", "prate", "ruh", "rvh",
     "saturation_mask", "asq", "qbudget",
 ) + tuple(f"{n}_{r}" for r in (1, 2) for n in ("moisture_padded", "fx", "fy", "fz", "advx", "advy", "advz",
-                                                 "candidate"))
+                                                 "candidate")) + ("mass1",)
 NATIVE_METRIC_NAMES = METRIC_NAMES + ("mh_profile", "mf_profile", "rho0_padded")
 
 
@@ -877,7 +889,7 @@ class _NativeConfig(ctypes.Structure):
     _fields_ = [("ni", ctypes.c_int32), ("nj", ctypes.c_int32), ("nk", ctypes.c_int32), ("dx", ctypes.c_float),
                 ("dy", ctypes.c_float), ("dz", ctypes.c_float), ("dt", ctypes.c_float), ("nsound", ctypes.c_int32),
                 ("alph", ctypes.c_float), ("kdiv", ctypes.c_float), ("lateral_sides", ctypes.c_int32 * 4),
-                ("stretched", ctypes.c_int32), ("concurrent", ctypes.c_int32)]
+                ("stretched", ctypes.c_int32), ("concurrent", ctypes.c_int32), ("apmasscon", ctypes.c_int32)]
 
 
 def _native_lib():
@@ -923,7 +935,7 @@ class NativeMoistLargeStep:
         self._config = _NativeConfig(cfg.ni, cfg.nj, cfg.nk, cfg.dx, cfg.dy, cfg.dz, cfg.dt, cfg.nsound,
                                      float(np.float32(cfg.alph)), float(np.float32(cfg.kdiv)),
                                      (ctypes.c_int32 * 4)(*cfg.lateral_sides), 1 if cfg.stretched else 0,
-                                     1 if concurrent else 0)
+                                     1 if concurrent else 0, 1 if cfg.apmasscon else 0)
         lib = _native_lib()
         handle = ctypes.c_void_p()
         with torch.cuda.device(state["u3d"].device):

@@ -22,8 +22,9 @@ tkea and ppx with their RK-stage twins u3d, v3d, w3d, pp3d, th3d, q3d; rho,
 prs and the face density rf; the eqtset 2 rate carriers qpten, qtten, qvten,
 qcten; the TKE dissipation dissten the next closure reads; the rain
 accumulators rain and prate; the radiative lateral histories radbcw, radbce,
-radbcs, radbcn; the FP64 budgets asq and qbudget; and the scalars step count
-and model time.  Everything else of the state is either rebuilt from the
+radbcs, radbcn; the FP64 budgets asq and qbudget; the dry-air mass ledger
+mass1 of the final-RK mass correction (restart_write.F:412); and the scalars
+step count and model time.  Everything else of the state is either rebuilt from the
 configuration (the base state, whose SHA-256 the header records and a resume
 checks) or scratch the next step overwrites before reading.
 """
@@ -47,7 +48,7 @@ PROFILE = "gm1b.moist-restart/v1"
 
 CARRIED = ("ua", "va", "wa", "ppi", "tha", "qa", "tkea", "ppx", "u3d", "v3d", "w3d", "pp3d", "th3d", "q3d", "rho",
            "prs", "rf", "qpten", "qtten", "qvten", "qcten", "dissten", "rain", "prate", "radbcw", "radbce", "radbcs",
-           "radbcn", "asq", "qbudget")
+           "radbcn", "asq", "qbudget", "mass1")
 # the rebuilt base state a resume must find unchanged
 BASE_STATE = ("th0", "pi0", "qv0", "th0_3d", "pi0_3d", "uh", "vh", "ruh", "rvh")
 CONFIG_KEYS = ("ni", "nj", "nk", "dx", "dy", "dz", "dt", "nsound", "alph", "kdiv", "lateral_sides")

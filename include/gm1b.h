@@ -382,6 +382,46 @@ GM1B_API int32_t gm1b_kessler_large_step(int32_t ni, int32_t nj, int32_t nk, con
                                          void *stream);
 
 /*
+ * The final-RK dry-air mass correction, apmasscon = 1 (replaces
+ * launch_cuda_apmasscon, src/cm1core/cuda_apmasscon.py:596, and its CPU twin
+ * cpu_apmasscon_inplace :256; CM1 solve2.F:1616-1656, :1972-2030): the
+ * dry-mass ledger mass2 = sum over levels of the binary64 level sums of
+ * ((rho*ruh)*rvh)*rmh and the Exner sum of pi0 + pp3d, the binary64
+ * correction ((mass1/mass2)^rddcv - 1) * sum / cells rounded to binary32,
+ * then pp3d += correction and prs = p00 * pi^(cp/rd), rho = prs / ((theta *
+ * pi) * (rd + max(qv, 0) * rv)) rebuilt.  mass1 is a device word (the
+ * initial ledger, gm1b_dry_mass); diagnostics (device, 4 doubles, may be
+ * NULL) receive mass2, the Exner sum, the binary64 correction and mass1.
+ * Arrays mass-shaped (nk, nj, ni) except ruh (ni) and rvh (nj); workspace
+ * gm1b_apmasscon_workspace_bytes(nk).  Allocation-free; graph-capturable.
+ */
+typedef struct gm1b_apmasscon_arrays {
+    const float *ruh, *rvh, *rmh, *pi0, *th0, *th3d, *qv;
+    float *pp3d, *prs, *rho;
+} gm1b_apmasscon_arrays;
+
+GM1B_API size_t gm1b_apmasscon_workspace_bytes(int32_t nk);
+GM1B_API int32_t gm1b_apmasscon(int32_t ni, int32_t nj, int32_t nk, const gm1b_apmasscon_arrays *arrays,
+                                const double *mass1, double *diagnostics, void *workspace, void *stream);
+/* The dry-mass ledger of a state into mass[0] (cpu_initial_dry_mass,
+ * cuda_apmasscon.py:226; CM1 init3d.F:2483-2527); with only_if_unset a
+ * non-zero mass[0] is kept (a ledger already held, e.g. restored). */
+GM1B_API int32_t gm1b_dry_mass(int32_t ni, int32_t nj, int32_t nk, const float *rho, const float *ruh, const float *rvh,
+                               const float *rmh, double *mass, int32_t only_if_unset, void *workspace, void *stream);
+/* gm1b_kessler_large_step with the dry-mass correction between the
+ * pre-physics equation of state and the driver (where the reference's
+ * finish runs it, after remove-held-EOS and before pdefq: its
+ * large_step_schedule MASS_BEGIN / MASS_FINISH, gm1_runtime.py:1969-2007);
+ * rr takes the corrected rho.  The ruh, rvh and rmh of arrays weigh the
+ * ledger. */
+GM1B_API int32_t gm1b_kessler_large_step_apmasscon(int32_t ni, int32_t nj, int32_t nk,
+                                                   const gm1b_kessler_arrays *arrays, const gm1b_kessler_held *held,
+                                                   float dx, float dy, float dz, float dt, int32_t equation_set,
+                                                   int32_t efall, void *workspace, size_t workspace_size,
+                                                   const double *mass1, double *mass_diagnostics,
+                                                   void *mass_workspace, void *stream);
+
+/*
  * gm1b_kessler_driver without a workspace argument, for callers that cannot
  * allocate device memory of their own (for instance a Fortran or C host
  * model bound through this ABI whose device memory belongs to another
@@ -1104,6 +1144,10 @@ typedef struct gm1b_moist_state {
     double *asq, *qbudget;
     float *moisture_padded_1, *fx_1, *fy_1, *fz_1, *advx_1, *advy_1, *advz_1, *candidate_1;
     float *moisture_padded_2, *fx_2, *fy_2, *fz_2, *advx_2, *advy_2, *advz_2, *candidate_2;
+    /* the dry-air mass ledger mass1 (one double; with apmasscon, computed
+     * from the state at create when it holds 0, else kept - a restored
+     * ledger) */
+    double *mass1;
 } gm1b_moist_state;
 
 /* The metrics: the 25 terrain metrics of the padded lane (flat: gz = 1,
@@ -1129,6 +1173,10 @@ typedef struct gm1b_moist_step_config {
     int32_t lateral_sides[4];
     int32_t stretched;
     int32_t concurrent;
+    /* the final-RK dry-air mass correction (CM1 apmasscon = 1, the
+     * supercell namelist's): between the pre-physics equation of state and
+     * the Kessler driver, against the state's mass1 ledger */
+    int32_t apmasscon;
 } gm1b_moist_step_config;
 
 typedef struct gm1b_moist_step gm1b_moist_step;

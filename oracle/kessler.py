@@ -58,9 +58,44 @@ def kessler_driver(arrays, *, ni, nj, nk, dx, dy, dz, dt, eqtset, iterations=Non
 HELD_NAMES = ("qpten", "qtten", "qvten", "qcten")
 
 
-def kessler_large_step(arrays, held, *, ni, nj, nk, dx, dy, dz, dt, eqtset, nfall=None) -> int:
+def dry_mass(rho, ruh, rvh, rmh, *, ni, nj, nk) -> float:
+    """cpu_initial_dry_mass (src/cm1core/cuda_apmasscon.py:226) restated."""
+    lib = load()
+    if not getattr(lib, "_dry_mass_ready", False):
+        lib.oracle_dry_mass.argtypes = [_F] * 4 + [ctypes.c_int] * 3
+        lib.oracle_dry_mass.restype = ctypes.c_double
+        lib._dry_mass_ready = True
+    for a in (rho, ruh, rvh, rmh):
+        assert a.dtype == REAL and a.flags.c_contiguous
+    return float(lib.oracle_dry_mass(*(a.ctypes.data_as(_F) for a in (rho, ruh, rvh, rmh)), ni, nj, nk))
+
+
+APMASSCON_NAMES = ("ruh", "rvh", "rmh", "pi0", "th0", "th3d", "qv", "pp3d", "prs", "rho")
+
+
+def apmasscon(arrays, *, ni, nj, nk, mass1: float) -> np.ndarray:
+    """cpu_apmasscon_inplace (src/cm1core/cuda_apmasscon.py:256) restated,
+    in place; returns (mass2, Exner sum, binary64 correction, mass1)."""
+    lib = load()
+    if not getattr(lib, "_apmasscon_ready", False):
+        lib.oracle_apmasscon.argtypes = [_F] * 11 + [ctypes.c_int] * 3 + [ctypes.c_double, _D]
+        lib.oracle_apmasscon.restype = ctypes.c_int
+        lib._apmasscon_ready = True
+    for n in APMASSCON_NAMES:
+        assert arrays[n].dtype == REAL and arrays[n].flags.c_contiguous, n
+    diag = np.zeros(4, np.float64)
+    r = lib.oracle_apmasscon(*(arrays[n].ctypes.data_as(_F) for n in APMASSCON_NAMES), None, ni, nj, nk,
+                             float(mass1), diag.ctypes.data_as(_D))
+    if r != 0:
+        raise MemoryError("oracle_apmasscon")
+    return diag
+
+
+def kessler_large_step(arrays, held, *, ni, nj, nk, dx, dy, dz, dt, eqtset, nfall=None, mass1=None,
+                       mass_diag=None) -> int:
     """cpu_gm1_kessler_large_step_inplace restated: held remove/snapshot,
-    pre-physics EOS, the driver, held recapture (in place)."""
+    pre-physics EOS, (with mass1, a one-word float64 array: the dry-air mass
+    correction), the driver, held recapture (in place)."""
     s = KesslerArrays()
     for n in FLOAT_NAMES:
         a = arrays[n]
@@ -74,9 +109,17 @@ def kessler_large_step(arrays, held, *, ni, nj, nk, dx, dy, dz, dt, eqtset, nfal
         lib.oracle_kessler_large_step.argtypes = [ctypes.POINTER(KesslerArrays), ctypes.POINTER(_F)] + \
             [ctypes.c_int] * 3 + [C_REAL] * 4 + [ctypes.c_int, ctypes.POINTER(ctypes.c_int32)]
         lib.oracle_kessler_large_step.restype = ctypes.c_int
+        lib.oracle_kessler_large_step_apmasscon.argtypes = lib.oracle_kessler_large_step.argtypes + [_D, _D]
+        lib.oracle_kessler_large_step_apmasscon.restype = ctypes.c_int
         lib._kls_ready = True
     nf = nfall.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)) if nfall is not None else None
-    r = lib.oracle_kessler_large_step(ctypes.byref(s), hp, ni, nj, nk, dx, dy, dz, dt, eqtset, nf)
+    if mass1 is None:
+        r = lib.oracle_kessler_large_step(ctypes.byref(s), hp, ni, nj, nk, dx, dy, dz, dt, eqtset, nf)
+    else:
+        assert mass1.dtype == np.float64
+        md = mass_diag if mass_diag is not None else np.zeros(4, np.float64)
+        r = lib.oracle_kessler_large_step_apmasscon(ctypes.byref(s), hp, ni, nj, nk, dx, dy, dz, dt, eqtset, nf,
+                                                    mass1.ctypes.data_as(_D), md.ctypes.data_as(_D))
     if r == -1:
         raise ValueError("invalid Kessler arguments")
     if r < -100:

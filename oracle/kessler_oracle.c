@@ -349,8 +349,112 @@ int oracle_kessler_driver(const kessler_arrays *a, int ni, int nj, int nk, float
  * libm powf), rr = rho, the driver, held recapture.  held[0..3] = qpten,
  * qtten, qvten, qcten (ignored for equation set 1).  Returns the driver's
  * result. */
+/* ---------------------------------------------------------------------------
+ * The final-RK dry-air mass correction, apmasscon = 1: cpu_initial_dry_mass
+ * and cpu_apmasscon_inplace (src/cm1core/cuda_apmasscon.py:190-325): per
+ * level the twin's serial binary64 sums of ((rho*ruh)*rvh)*rmh and of
+ * pi0 + pp3d, the levels summed in order, the binary64 correction, then
+ * pp3d += correction and prs, rho from the equation of state.
+ * ------------------------------------------------------------------------- */
+static void mass_layers(const float *rho, const float *ruh, const float *rvh, const float *rmh, const float *pi0,
+                        const float *pp3d, int ni, int nj, int nk, double *dry, double *pis) {
+    for (int k = 0; k < nk; ++k) {
+        double d = 0.0, p = 0.0;
+        for (int j = 0; j < nj; ++j)
+            for (int i = 0; i < ni; ++i) {
+                const size_t q = ((size_t)k * nj + j) * ni + i;
+                float term = rho[q] * ruh[i];
+                term = term * rvh[j];
+                term = term * rmh[q];
+                d = d + (double)term;
+                if (pis != NULL) p = p + (double)(pi0[q] + pp3d[q]);
+            }
+        dry[k] = d;
+        if (pis != NULL) pis[k] = p;
+    }
+}
+
+double oracle_dry_mass(const float *rho, const float *ruh, const float *rvh, const float *rmh, int ni, int nj,
+                       int nk) {
+    double *dry = malloc(sizeof(double) * (size_t)nk);
+    if (dry == NULL) return -1.0;
+    mass_layers(rho, ruh, rvh, rmh, NULL, NULL, ni, nj, nk, dry, NULL);
+    double total = 0.0;
+    for (int k = 0; k < nk; ++k) total = total + dry[k];
+    free(dry);
+    return total;
+}
+
+/* diag: mass2, the Exner sum, the binary64 correction, mass1 */
+int oracle_apmasscon(const float *ruh, const float *rvh, const float *rmh, const float *pi0, const float *th0,
+                     const float *th3d, const float *qv, float *pp3d, float *prs, float *rho, float *rr, int ni,
+                     int nj, int nk, double mass1, double *diag) {
+    double *dry = malloc(sizeof(double) * (size_t)nk), *pis = malloc(sizeof(double) * (size_t)nk);
+    if (dry == NULL || pis == NULL) {
+        free(dry);
+        free(pis);
+        return -1;
+    }
+    mass_layers(rho, ruh, rvh, rmh, pi0, pp3d, ni, nj, nk, dry, pis);
+    double mass2 = 0.0, psum = 0.0;
+    for (int k = 0; k < nk; ++k) {
+        mass2 = mass2 + dry[k];
+        psum = psum + pis[k];
+    }
+    free(dry);
+    free(pis);
+    const float cp = 1005.7f, rd = 287.04f, rv = 461.5f;
+    const float cv = cp - rd;
+    const float rddcv = rd / cv;
+    const float cpdrd = cp / rd;
+    double value = pow(mass1 / mass2, (double)rddcv) - 1.0;
+    value = value * psum;
+    value = value / (double)((size_t)ni * nj * nk);
+    const float corr = (float)value;
+    if (diag != NULL) {
+        diag[0] = mass2;
+        diag[1] = psum;
+        diag[2] = value;
+        diag[3] = mass1;
+    }
+    const size_t n = (size_t)ni * nj * nk;
+    for (size_t q = 0; q < n; ++q) {
+        pp3d[q] = pp3d[q] + corr;
+        const float pi = pi0[q] + pp3d[q];
+        const float pressure = 100000.0f * powf(pi, cpdrd);
+        const float theta = th0[q] + th3d[q];
+        float vapor = qv[q] > 0.0f ? qv[q] : 0.0f;
+        if (qv[q] != qv[q]) vapor = qv[q];
+        const float gas = rd + vapor * rv;
+        float den = theta * pi;
+        den = den * gas;
+        prs[q] = pressure;
+        rho[q] = pressure / den;
+        if (rr != NULL) rr[q] = rho[q];
+    }
+    return 0;
+}
+
+int oracle_kessler_large_step_mass(const kessler_arrays *a, float *const held[4], int ni, int nj, int nk, float dx,
+                                   float dy, float dz, float dt, int eqtset, int *nfall, const double *mass1,
+                                   double *diag);
+
+/* the Kessler large step with the mass correction between the pre-physics
+ * equation of state and the driver */
+int oracle_kessler_large_step_apmasscon(const kessler_arrays *a, float *const held[4], int ni, int nj, int nk,
+                                        float dx, float dy, float dz, float dt, int eqtset, int *nfall,
+                                        const double *mass1, double *diag) {
+    return oracle_kessler_large_step_mass(a, held, ni, nj, nk, dx, dy, dz, dt, eqtset, nfall, mass1, diag);
+}
+
 int oracle_kessler_large_step(const kessler_arrays *a, float *const held[4], int ni, int nj, int nk, float dx,
                               float dy, float dz, float dt, int eqtset, int *nfall) {
+    return oracle_kessler_large_step_mass(a, held, ni, nj, nk, dx, dy, dz, dt, eqtset, nfall, NULL, NULL);
+}
+
+int oracle_kessler_large_step_mass(const kessler_arrays *a, float *const held[4], int ni, int nj, int nk, float dx,
+                                   float dy, float dz, float dt, int eqtset, int *nfall, const double *mass1,
+                                   double *diag) {
     const size_t n = (size_t)ni * nj * nk;
     float *state[4] = {a->pp3d, a->th3d, a->qv, a->qc};
     if (eqtset == 2)
@@ -377,6 +481,9 @@ int oracle_kessler_large_step(const kessler_arrays *a, float *const held[4], int
         a->rho[q] = rho;
         ((float *)a->rr)[q] = rho;
     }
+    if (mass1 != NULL && oracle_apmasscon(a->ruh, a->rvh, a->rmh, a->pi0, a->th0, a->th3d, a->qv, a->pp3d, a->prs,
+                                          a->rho, (float *)a->rr, ni, nj, nk, *mass1, diag) != 0)
+        return -1;
     const int r = oracle_kessler_driver(a, ni, nj, nk, dx, dy, dz, dt, eqtset, nfall);
     if (r < 0 || eqtset != 2) return r;
     for (int s = 0; s < 4; ++s)

@@ -43,6 +43,15 @@ def theta_weps() -> float:
 class OracleMoistStep:
     def __init__(self, cfg, state: dict[str, np.ndarray], metrics: dict[str, np.ndarray]) -> None:
         self.cfg, self.s, self.m = cfg, state, metrics
+        # CM1 apmasscon = 1 unless the configuration says otherwise; the
+        # initial dry-air mass of the state unless it carries one
+        self.apmasscon = bool(getattr(cfg, "apmasscon", True))
+        if self.apmasscon:
+            if "mass1" not in state:
+                state["mass1"] = np.zeros(1, np.float64)
+            if state["mass1"][0] == 0.0:
+                state["mass1"][0] = oks.dry_mass(state["rho"], state["ruh"], state["rvh"], metrics["rmh"],
+                                                 ni=cfg.ni, nj=cfg.nj, nk=cfg.nk)
         # the oracle's acoustic stage always writes its column diagnostics
         for n in ("tri_aa", "tri_bb", "tri_cc", "tri_dd", "tri_pivot", "tri_residual"):
             if state[n].shape != state["pp3d"].shape:
@@ -228,7 +237,10 @@ class OracleMoistStep:
              "fall_velocity": s["fall_velocity"], "rain": s["rain"], "prate": s["prate"], "asq": s["asq"],
              "qbudget": s["qbudget"]}
         held = {"qpten": s["qpten"], "qtten": s["qtten"], "qvten": s["qvten"], "qcten": s["qcten"]}
-        oks.kessler_large_step(a, held, **self.grid, dt=c.dt, eqtset=2)
+        # with apmasscon the dry-air mass correction between the pre-physics
+        # equation of state and the driver
+        oks.kessler_large_step(a, held, **self.grid, dt=c.dt, eqtset=2,
+                               mass1=s["mass1"] if self.apmasscon else None)
         s["pp3d"][1:c.nk + 1, 1:c.nj + 1, 1:c.ni + 1] = s["pp3d_c"]
 
     def solve3(self):

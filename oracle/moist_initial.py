@@ -24,7 +24,7 @@ NUMQ = 3
 QROWS = 6
 NG = 3
 DIAGNOSTIC_NAMES = ("tri_aa", "tri_bb", "tri_cc", "tri_dd", "tri_pivot", "tri_residual")
-DTYPES = {"saturation_mask": np.uint8, "asq": np.float64, "qbudget": np.float64}
+DTYPES = {"saturation_mask": np.uint8, "asq": np.float64, "qbudget": np.float64, "mass1": np.float64}
 
 
 def terrain_static_shapes(ni: int, nj: int, nk: int) -> dict[str, tuple[int, ...]]:
@@ -71,7 +71,7 @@ def moist_state_shapes(ni: int, nj: int, nk: int) -> dict[str, tuple[int, ...]]:
               "cme", "ce1", "ce2", "csm", "kmh", "kmv", "khh", "khv", "tke_workspace"):
         s[n] = face
     s.update(uc=(nk, nj, ni + 1), vc=(nk, nj + 1, ni), wc=face, th0=(nk,), pi0=(nk,), qv0=(nk,), rain=(1, nj, ni),
-             prate=plane, asq=(3,), qbudget=(10,), ruh=(ni,), rvh=(nj,))
+             prate=plane, asq=(3,), qbudget=(10,), ruh=(ni,), rvh=(nj,), mass1=(1,))
     return s
 
 

@@ -16,6 +16,8 @@ rebuilt the same inputs.
 Reference entry points used (their CPU twins, single-threaded NumPy):
   cpu_sound3_periodic_three_stage_inplace  src/cm1core/cuda_sound3_periodic.py:1071
   cpu_psolver3_trajectory_inplace          src/cm1core/cuda_psolver3_trajectory.py:761
+  cpu_initial_dry_mass, cpu_apmasscon_inplace  src/cm1core/cuda_apmasscon.py:226, :256
+  (and the others named by each make_* function)
 """
 
 from __future__ import annotations
@@ -330,6 +332,56 @@ def make_kessler(reference: Path) -> None:
         np.savez_compressed(HERE / f"{tag}.npz", meta=json.dumps(meta), **inputs, **outputs)
         print("wrote", tag, "max nfall", result["max_fall_substeps"],
               "iterations", int(result["satadj"]["iterations"].max()))
+
+
+APMASSCON_CASES = {
+    "apmasscon_9x7x12": (9, 7, 12, 51),
+    "apmasscon_13x6x10": (13, 6, 10, 52),
+}
+
+
+def apmasscon_fixture(ni: int, nj: int, nk: int, seed: int) -> dict[str, np.ndarray]:
+    """A moist, hydrostatic-looking column set (Exner from 1.0 down to 0.6,
+    theta 300-360 K, vapour up to 16 g/kg, moist density from the equation
+    of state with a few per-mille of seeded departure) and grid factors near
+    1 (ruh, rvh, rmh of a gently stretched grid)."""
+    rng = np.random.default_rng(seed)
+    f = np.float32
+    z = (np.arange(nk) + 0.5) / nk
+    pi0 = np.broadcast_to((1.0 - 0.4 * z)[:, None, None], (nk, nj, ni)).astype(f).copy()
+    th0 = np.broadcast_to((300.0 + 60.0 * z)[:, None, None], (nk, nj, ni)).astype(f).copy()
+    th3d = rng.uniform(-1.5, 2.5, (nk, nj, ni)).astype(f)
+    qv = (0.016 * np.exp(-3.0 * z)[:, None, None] * rng.uniform(0.7, 1.0, (nk, nj, ni))).astype(f)
+    qv[0, 0, :2] = f(-1.0e-6)  # a negative vapour word takes max(0, qv)
+    pp3d = rng.uniform(-2.0e-3, 2.0e-3, (nk, nj, ni)).astype(f)
+    pi = (pi0.astype(np.float64) + pp3d)
+    prs = (1.0e5 * pi ** (1005.7 / 287.04)).astype(f)
+    rho = (prs / ((th0.astype(np.float64) + th3d) * pi * (287.04 + np.maximum(qv, 0.0) * 461.5))
+           * rng.uniform(0.997, 1.003, (nk, nj, ni))).astype(f)
+    return {"ruh": rng.uniform(0.9, 1.1, ni).astype(f), "rvh": rng.uniform(0.9, 1.1, nj).astype(f),
+            "rmh": rng.uniform(0.95, 1.05, (nk, nj, ni)).astype(f), "pi0": pi0, "th0": th0, "th3d": th3d, "qv": qv,
+            "pp3d": pp3d, "prs": prs, "rho": rho}
+
+
+def make_apmasscon(reference: Path) -> None:
+    """The final-RK dry-air mass correction through the reference's CPU
+    twin: mass1 of a starting state (cpu_initial_dry_mass), then
+    cpu_apmasscon_inplace on a state whose dry mass has drifted."""
+    sys.path.insert(0, str(reference / "src"))
+    from cm1core.cuda_apmasscon import cpu_apmasscon_inplace, cpu_initial_dry_mass
+
+    for tag, (ni, nj, nk, seed) in APMASSCON_CASES.items():
+        start = apmasscon_fixture(ni, nj, nk, seed)
+        mass1 = cpu_initial_dry_mass(start, ni=ni, nj=nj, nk=nk)
+        a = apmasscon_fixture(ni, nj, nk, seed)
+        a["rho"] = (a["rho"] * np.float32(1.0021)).astype(np.float32)  # the drift the correction removes
+        inputs = {f"in_{k}": v.copy() for k, v in a.items()}
+        r = cpu_apmasscon_inplace(a, ni=ni, nj=nj, nk=nk, mass1=mass1)
+        outputs = {f"out_{k}": a[k] for k in ("pp3d", "prs", "rho")}
+        meta = dict(ni=ni, nj=nj, nk=nk, mass1=mass1, mass2=r.mass2_before_f64, pressure_sum=r.pressure_sum_before_f64,
+                    correction=r.correction_f32, mass_after=r.mass_after_f64)
+        np.savez_compressed(HERE / f"{tag}.npz", meta=json.dumps(meta), **inputs, **outputs)
+        print("wrote", tag, meta)
 
 
 KESSLER_LARGE_STEP_CASES = {
@@ -1176,7 +1228,7 @@ def make_warm_rain(reference: Path) -> None:
 def main() -> None:
     p = argparse.ArgumentParser()
     p.add_argument("--reference", type=Path, required=True, help="root of the reference source tree")
-    p.add_argument("what", choices=("small", "c1", "advection", "kessler", "tke", "rk", "bridge", "wk", "limits", "closure", "tkeevo", "momentum", "terrainopen", "kesslerstep", "fills", "vertical", "warmrain"))
+    p.add_argument("what", choices=("small", "c1", "advection", "kessler", "tke", "rk", "bridge", "wk", "limits", "closure", "tkeevo", "momentum", "terrainopen", "kesslerstep", "fills", "vertical", "warmrain", "apmasscon"))
     p.add_argument("--checkpoints", type=int, nargs="+", default=[1])
     args = p.parse_args()
     if args.what == "small":
@@ -1211,6 +1263,8 @@ def main() -> None:
         make_warm_rain(args.reference)
     elif args.what == "vertical":
         make_vertical(args.reference)
+    elif args.what == "apmasscon":
+        make_apmasscon(args.reference)
     else:
         make_c1(args.reference, sorted(set(args.checkpoints)))
 

@@ -2,7 +2,8 @@
 one domain run as 2x1 and 2x2 widened subdomains (32-cell halos) held by
 one process on one device, with the halo strips of the carried arrays
 exchanged by device copies after every large step, leaves interiors that are
-the single-domain GPU step's words after 3 steps (the Python composition on
+the single-domain GPU step's words after 3 steps (apmasscon off: the
+dry-mass correction is a domain-wide reduction) (the Python composition on
 the uniform column, the C entry point on the 80-level stretched column).  The
 FP64 budgets accumulate per widened subdomain; a lateral-boundary history is
 compared on the rank that holds that edge of the domain."""
@@ -26,10 +27,13 @@ EDGE = {"radbcw": lambda s, px, py: s.px == 0, "radbce": lambda s, px, py: s.px 
 COMPARED = tuple(n for n in CARRIED if n not in ("asq", "qbudget"))
 
 CASES = {
-    "python-uniform-2x1": (MoistLargeStep, MoistStepConfig(96, 40, 16, 1000.0, 1000.0, 250.0, 5.0, 10), 2, 1),
-    "python-uniform-2x2": (MoistLargeStep, MoistStepConfig(80, 72, 16, 1000.0, 1000.0, 250.0, 5.0, 10), 2, 2),
+    "python-uniform-2x1": (MoistLargeStep, MoistStepConfig(96, 40, 16, 1000.0, 1000.0, 250.0, 5.0, 10,
+                                                           apmasscon=False), 2, 1),
+    "python-uniform-2x2": (MoistLargeStep, MoistStepConfig(80, 72, 16, 1000.0, 1000.0, 250.0, 5.0, 10,
+                                                           apmasscon=False), 2, 2),
     "native-stretched-2x1": (NativeMoistLargeStep, MoistStepConfig(80, 32, 80, 100.0, 100.0, 100.0, 0.6, 8,
-                                                                   column=SUPERCELL_STRETCHED_COLUMN), 2, 1),
+                                                                   column=SUPERCELL_STRETCHED_COLUMN,
+                                                                   apmasscon=False), 2, 1),
 }
 
 

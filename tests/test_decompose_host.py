@@ -4,7 +4,8 @@ halo exchange (in-process and over two gloo ranks) leaves every halo cell of
 index-coded arrays equal to the single domain's; and the oracle's composed
 moist step, decomposed over 2x1 and 2x2 subdomains with a 32-cell halo and
 exchanged after every large step, leaves interiors word-identical to the
-single domain's after 3 steps (the FP64 budgets excepted: they accumulate
+single domain's after 3 steps (with apmasscon off: the dry-mass correction
+is a domain-wide reduction; the FP64 budgets excepted: they accumulate
 per widened subdomain; a lateral-boundary history is compared on the rank
 that holds that edge of the domain - elsewhere it belongs to a halo's outer
 edge)."""
@@ -41,8 +42,9 @@ def _cfg(ni, nj, stretched=False):
     column = SimpleNamespace(ztop_m=20800.0, str_bot_m=200.0, str_top_m=15800.0, dz_bot_m=20.0,
                              dz_top_m=500.0) if stretched else None
     nk, dx, dz, dt, ns = (80, 100.0, 100.0, 0.6, 8) if stretched else (12, 1000.0, 250.0, 5.0, 10)
+    # the dry-mass correction is a domain-wide reduction: off in a decomposed run
     return SimpleNamespace(ni=ni, nj=nj, nk=nk, dx=dx, dy=dx, dz=dz, dt=dt, nsound=ns, alph=0.60, kdiv=0.10,
-                           lateral_sides=(2, 2, 2, 2), obc=0x2222, column=column)
+                           lateral_sides=(2, 2, 2, 2), obc=0x2222, column=column, apmasscon=False)
 
 
 def _start(cfg):

@@ -60,3 +60,34 @@ def test_member_in_a_batch_equals_member_alone():
     # the members really differ (different sizes, bubbles and noise)
     assert batched.state(0)["th3d"].shape != batched.state(1)["th3d"].shape
     assert float(batched.state(1)["w3d"].abs().max()) > 0.0
+
+
+def test_member_in_the_batch_matches_the_oracle_composition():
+    """A member stepped inside the captured, multi-stream batch against the
+    oracle's composition of that member alone, each field on its own scale
+    (tests/moist_common.py SHORT_BARS), after 1 and 3 large steps."""
+    from oracle.moist_composition import OracleMoistStep  # noqa: PLC0415
+    from gm1_b200.ensemble import member_config  # noqa: PLC0415
+    from tests.moist_common import SHORT_BARS, check_errors, field_errors, format_errors  # noqa: PLC0415
+
+    members = _members()
+    hosts = [member_initial_state(m, SMALL) for m in members]
+    batched = MoistEnsemble(members, "cuda:0", streams=3, grid=SMALL, hosts=hosts)
+    host, metrics = hosts[1]
+    ref = OracleMoistStep(member_config(members[1], SMALL), {k: v.copy() for k, v in host.items()},
+                          {k: v.copy() for k, v in metrics.items()})
+    batched.step_eager()
+    ref.step()
+    torch.cuda.synchronize()
+    err = field_errors(batched.state(1), ref.s)
+    print("step 1", format_errors(err))
+    check_errors(err, SHORT_BARS, "ensemble member 1 step 1")
+    batched.capture()
+    for _ in range(2):
+        batched.replay()
+        ref.step()
+    torch.cuda.synchronize()
+    err = field_errors(batched.state(1), ref.s)
+    print("step 3", format_errors(err))
+    check_errors(err, SHORT_BARS, "ensemble member 1 step 3")
+    batched.release()

@@ -9,7 +9,7 @@ the acoustic, advection and pdef arithmetic then carries those ulps): each
 prognostic field measured on its own scale (the largest |value| of that
 field: u, v, w each, theta', pi', qv, qc, qr each, TKE) within
 tests/moist_common.py's SHORT_BARS after 1 and 3 steps (also at the full
-256x256x80 size after one step); over 60 steps, within three times the
+256x256x80 size after one step); over 60 steps, within four times the
 spread the oracle itself shows when its input theta' moves by one ulp; u, v
 and w are word-identical after one step.  A CUDA-graph replay of the step gives the
 eager words."""

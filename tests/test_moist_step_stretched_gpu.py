@@ -7,7 +7,7 @@ operators, after 1, 3 and 60 large steps, including the 80-level supercell
 column of the 640x768x80 configuration on a reduced plane.
 
 Bars (tests/moist_common.py measures each field on its own scale):
-SHORT_BARS after 1 and 3 steps; over 60 steps, three times the spread the
+SHORT_BARS after 1 and 3 steps; over 60 steps, four times the spread the
 oracle itself shows when its input theta' moves by one ulp.  The words differ
 only where Kessler and the TKE closure pass values through powf, expf and
 sqrtf (CUDA and the C library round their last bits differently) and the
