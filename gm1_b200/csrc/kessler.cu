@@ -683,10 +683,11 @@ __global__ void __launch_bounds__(256) kessler_recapture_kernel(gm1b_kessler_arr
 // the levels summed in order, the uniform Exner correction
 // ((mass1/mass2)^rddcv - 1) * sum(pi) / cells in binary64 and rounded to
 // binary32, then pp3d += correction and prs, rho rebuilt from the equation
-// of state.  One CTA per level forms the level sums in a fixed order (each
-// thread a strided binary64 partial, then a shared-memory tree), as the
-// reference's CUDA reduction does; the twin sums each level serially, so
-// the two ledgers agree to binary64 rounding.
+// of state.  The level sums are formed in a fixed order: 16 CTAs per level
+// (each thread a strided binary64 partial, then a shared-memory tree per
+// CTA, as the reference's one-CTA-per-level CUDA reduction does per block),
+// the level adding its 16 partials in order; the twin sums each level
+// serially, so the two ledgers agree to binary64 rounding.
 // ---------------------------------------------------------------------------
 namespace gm1b {
 namespace {
@@ -698,13 +699,17 @@ struct MassArgs {
 };
 
 constexpr int kMassThreads = 256;
+constexpr int kMassChunks = 16;  // CTAs per level: chunk c sums cells ij = c*256 + t + m*16*256
 
-__global__ void __launch_bounds__(kMassThreads) apmasscon_levels_kernel(MassArgs a, double *layers, int pressure) {
+// grid (nk, kMassChunks): each CTA a fixed share of one level, its binary64
+// partial sums at partials[(k * kMassChunks + c)] (dry) and at the same
+// index + nk * kMassChunks (Exner)
+__global__ void __launch_bounds__(kMassThreads) apmasscon_levels_kernel(MassArgs a, double *partials, int pressure) {
     __shared__ double s_dry[kMassThreads], s_pi[kMassThreads];
-    const int k = blockIdx.x;
+    const int k = blockIdx.x, c = blockIdx.y;
     const size_t nxy = (size_t)a.ni * a.nj, base = (size_t)k * nxy;
     double dry = 0.0, pis = 0.0;
-    for (size_t ij = threadIdx.x; ij < nxy; ij += kMassThreads) {
+    for (size_t ij = (size_t)c * kMassThreads + threadIdx.x; ij < nxy; ij += (size_t)kMassChunks * kMassThreads) {
         const int i = (int)(ij % a.ni), j = (int)(ij / a.ni);
         const size_t q = base + ij;
         float term = a.rho[q] * __ldg(a.ruh + i);
@@ -724,9 +729,16 @@ __global__ void __launch_bounds__(kMassThreads) apmasscon_levels_kernel(MassArgs
         __syncthreads();
     }
     if (threadIdx.x == 0) {
-        layers[k] = s_dry[0];
-        layers[a.nk + k] = s_pi[0];
+        partials[(size_t)k * kMassChunks + c] = s_dry[0];
+        partials[(size_t)(a.nk + k) * kMassChunks + c] = s_pi[0];
     }
+}
+
+// the level sums: each level's chunk partials added in chunk order
+__device__ __forceinline__ double level_sum(const double *partials, int row) {
+    double v = 0.0;
+    for (int c = 0; c < kMassChunks; ++c) v += partials[(size_t)row * kMassChunks + c];
+    return v;
 }
 
 // the dry-mass ledger (levels in order) into mass[0]; with only_if_unset a
@@ -735,7 +747,7 @@ __global__ void dry_mass_finish_kernel(const double *layers, int nk, double *mas
     if (blockIdx.x != 0 || threadIdx.x != 0) return;
     if (only_if_unset && mass[0] != 0.0) return;
     double total = 0.0;
-    for (int k = 0; k < nk; ++k) total += layers[k];
+    for (int k = 0; k < nk; ++k) total += level_sum(layers, k);
     mass[0] = total;
 }
 
@@ -745,8 +757,8 @@ __global__ void apmasscon_finish_kernel(const double *layers, int nk, const doub
     if (blockIdx.x != 0 || threadIdx.x != 0) return;
     double mass2 = 0.0, pis = 0.0;
     for (int k = 0; k < nk; ++k) {
-        mass2 += layers[k];
-        pis += layers[nk + k];
+        mass2 += level_sum(layers, k);
+        pis += level_sum(layers, nk + k);
     }
     double value = pow(mass1[0] / mass2, (double)rddcv) - 1.0;
     value = value * pis;
@@ -791,15 +803,15 @@ float mass_rddcv() {
     return rd / cv;
 }
 
-size_t mass_workspace_bytes(int nk) { return sizeof(double) * (2 * (size_t)nk + 2); }
+size_t mass_workspace_bytes(int nk) { return sizeof(double) * (2 * (size_t)nk * kMassChunks + 2); }
 
 int32_t mass_correction(const MassArgs &m, const double *mass1, double *diag, void *workspace, cudaStream_t st) {
     double *layers = static_cast<double *>(workspace);
-    float *corr = reinterpret_cast<float *>(layers + 2 * (size_t)m.nk);
+    float *corr = reinterpret_cast<float *>(layers + 2 * (size_t)m.nk * kMassChunks);
     const size_t n = (size_t)m.ni * m.nj * m.nk;
     {
         ProfScope ps("apmasscon_levels_kernel", st);
-        apmasscon_levels_kernel<<<m.nk, kMassThreads, 0, st>>>(m, layers, 1);
+        apmasscon_levels_kernel<<<dim3(m.nk, kMassChunks), kMassThreads, 0, st>>>(m, layers, 1);
         ps.stop();
     }
     if (!launched("apmasscon_levels_kernel")) return GM1B_ERR_CUDA;
@@ -840,7 +852,7 @@ extern "C" int32_t gm1b_dry_mass(int32_t ni, int32_t nj, int32_t nk, const float
                ni, nj, nk};
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     double *layers = static_cast<double *>(workspace);
-    apmasscon_levels_kernel<<<nk, kMassThreads, 0, st>>>(m, layers, 0);
+    apmasscon_levels_kernel<<<dim3(nk, kMassChunks), kMassThreads, 0, st>>>(m, layers, 0);
     if (!launched("apmasscon_levels_kernel")) return GM1B_ERR_CUDA;
     dry_mass_finish_kernel<<<1, 1, 0, st>>>(layers, nk, mass, only_if_unset ? 1 : 0);
     return launched("dry_mass_finish_kernel") ? GM1B_OK : GM1B_ERR_CUDA;
