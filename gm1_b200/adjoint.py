@@ -169,16 +169,21 @@ def _workspace(flow: FrozenFlow, device) -> torch.Tensor:
 def advection_tendency_adjoint(flow: FrozenFlow, scalar: torch.Tensor, tendency_adjoint: torch.Tensor, nrk: int, *,
                                weps: float | None = None, scale: float = 1.0,
                                accumulate: torch.Tensor | None = None,
-                               running_sum: torch.Tensor | None = None) -> torch.Tensor:
+                               running_sum: torch.Tensor | None = None,
+                               out: torch.Tensor | None = None) -> torch.Tensor:
     """dJ/d(compact scalar) for dJ/d(tendency) = scale * tendency_adjoint, the
     tendency taken on the compact scalar's open-filled carrier (the carrier
     is read through the fill's index map; a face-coefficient pass, then one
     gather per compact cell that folds the fill's transpose), plus
     ``accumulate`` when given; with ``running_sum`` the result comes back
-    bare and running_sum receives accumulate + result."""
+    bare and running_sum receives accumulate + result (into ``out`` when
+    given)."""
     ni, nj, nk = flow.ni, flow.nj, flow.nk
     lam = tendency_adjoint.contiguous()
-    out = torch.empty((nk, nj, ni), dtype=torch.float32, device=scalar.device)
+    if out is None:
+        out = torch.empty((nk, nj, ni), dtype=torch.float32, device=scalar.device)
+    elif not out.is_contiguous() or tuple(out.shape) != (nk, nj, ni) or out.dtype != torch.float32:
+        raise ValueError("out must be a contiguous float32 (nk, nj, ni) tensor")
     a = _adjoint_arrays(flow, scalar.contiguous(), lam, out)
     work = _workspace(flow, scalar.device)
     _native.check(_lib().gm1b_scalar_advection5_adjoint_open(
@@ -423,10 +428,16 @@ class StageCheckpointedAdjoint:
       the dt scaling and the last sum fused into the gather kernel.
 
     The same gradient as the autograd path (up to the order of the float
-    sums)."""
+    sums).  With ``streams`` > 1 the scalars' reverse chains (independent
+    after the cell adjoint) run on that many side streams forked from the
+    caller's stream and joined back (a CUDA graph capture keeps the fork);
+    two at a time keep their face scratch in L2.  The words do not depend on
+    it."""
 
-    def __init__(self, model: WarmRainTransport):
+    def __init__(self, model: WarmRainTransport, streams: int = 1):
         self.model = model
+        dev = model.flow.fields["th0"].device
+        self.streams = [torch.cuda.Stream(dev) for _ in range(streams)] if streams > 1 else []
 
     def forward(self, x: tuple) -> tuple[tuple, tuple]:
         m = self.model
@@ -452,17 +463,23 @@ class StageCheckpointedAdjoint:
         with torch.no_grad():
             l3s = tuple(torch.empty_like(st[3]) for st in stages)
             _warm_rain_cell(f, tuple(st[3] for st in stages), tuple(t.contiguous() for t in lam), l3s, m.dt)
-            out = []
-            for st, l3, weps in zip(stages, l3s, m.weps):
-                acc = torch.empty_like(l3)
-                # l2 = T_3^T dt_3 l3 with acc = l3 + l2; l1 = T_2^T dt_2 l2
-                # with acc += l1; lambda_0 = acc + T_1^T dt_1 l1
-                l2 = advection_tendency_adjoint(m.flow, st[2], l3, 3, weps=weps, scale=m.stage_dt[2], accumulate=l3,
-                                                running_sum=acc)
-                l1 = advection_tendency_adjoint(m.flow, st[1], l2, 2, weps=weps, scale=m.stage_dt[1], accumulate=acc,
-                                                running_sum=acc)
-                out.append(advection_tendency_adjoint(m.flow, st[0], l1, 1, weps=weps, scale=m.stage_dt[0],
-                                                      accumulate=acc))
+            out = [torch.empty_like(l3) for l3 in l3s]
+            main = torch.cuda.current_stream(l3s[0].device)
+            for side in self.streams:
+                side.wait_stream(main)
+            for q, (st, l3, weps) in enumerate(zip(stages, l3s, m.weps)):
+                with torch.cuda.stream(self.streams[q % len(self.streams)] if self.streams else main):
+                    acc = torch.empty_like(l3)
+                    # l2 = T_3^T dt_3 l3 with acc = l3 + l2; l1 = T_2^T dt_2 l2
+                    # with acc += l1; lambda_0 = acc + T_1^T dt_1 l1
+                    l2 = advection_tendency_adjoint(m.flow, st[2], l3, 3, weps=weps, scale=m.stage_dt[2],
+                                                    accumulate=l3, running_sum=acc)
+                    l1 = advection_tendency_adjoint(m.flow, st[1], l2, 2, weps=weps, scale=m.stage_dt[1],
+                                                    accumulate=acc, running_sum=acc)
+                    advection_tendency_adjoint(m.flow, st[0], l1, 1, weps=weps, scale=m.stage_dt[0], accumulate=acc,
+                                               out=out[q])
+            for side in self.streams:
+                main.wait_stream(side)
         return tuple(out)
 
 
@@ -495,9 +512,9 @@ class StepGraphs:
     input state, the 12 stage fields, dJ/d(step output)) and writes 4.
     ``gradient`` gives the words of the eager StageCheckpointedAdjoint."""
 
-    def __init__(self, model: WarmRainTransport, like: tuple):
+    def __init__(self, model: WarmRainTransport, like: tuple, streams: int = 2):
         self.model = model
-        self.adjoint = StageCheckpointedAdjoint(model)
+        self.adjoint = StageCheckpointedAdjoint(model, streams=streams)
         dev = like[0].device
         shape = tuple(like[0].shape)
         self.xin = torch.stack([t.detach() for t in like]).contiguous()
