@@ -584,7 +584,15 @@ def run_ensemble(args) -> None:
     my_cells = sum(m.cells for m in mine)
     total_cells = sum(cells_all)
     hosts = [member_initial_state(m) for m in mine]
-    batched = MoistEnsemble(mine, device, streams=8, hosts=hosts)
+    # the batched method picks each member grid shape's advection z-chunk
+    # with the project's autotuner (once per shape); the plain method keeps
+    # the kernels' defaults
+    from gm1_b200.autotune import Autotuner
+
+    tuner = Autotuner()
+    t_tune = time.perf_counter()
+    batched = MoistEnsemble(mine, device, streams=8, hosts=hosts, tuner=tuner)
+    t_tune = time.perf_counter() - t_tune
     plain = MoistEnsemble(mine, device, streams=1, hosts=hosts)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
     for _ in range(args.warmup):
@@ -683,6 +691,8 @@ def run_ensemble(args) -> None:
                                "bubble U[1,3] K jittered +-5 km, Kessler, WENO5, TKE, open-radiative laterals)",
                    "mode": "ensemble", "cells": total_cells, "members": args.members,
                    "batched": "one CUDA graph per ensemble step, members over 8 streams",
+                   "autotune": {"shapes": len(tuner.table) // 2, "set_up_s": round(t_tune, 2),
+                                "chunks": {k: v["best"] for k, v in list(tuner.table.items())[:8]}},
                    "plain_cell_updates_per_s": plain_value, "plain_ms_per_step": p_ms / args.steps,
                    "batched_over_plain": value / plain_value,
                    "l2": "flushed before every timed step (256 MiB write, outside the event pair)",

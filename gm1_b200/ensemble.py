@@ -94,7 +94,8 @@ class MoistEnsemble:
     and metrics, in member order) may be passed to skip building them."""
 
     def __init__(self, members: Sequence[EnsembleMember], device: torch.device | str, *, streams: int = 8,
-                 grid: dict | None = None, hosts: Sequence[tuple[dict, dict]] | None = None) -> None:
+                 grid: dict | None = None, hosts: Sequence[tuple[dict, dict]] | None = None,
+                 tuner: Any | None = None) -> None:
         if not members:
             raise ValueError("an ensemble needs at least one member")
         if streams < 1:
@@ -111,8 +112,12 @@ class MoistEnsemble:
             with torch.cuda.stream(st):
                 # members already overlap one another, so each steps its own
                 # operations in order on its stream
+                # with a tuner (gm1_b200.autotune.Autotuner) each member's
+                # advection z-chunk is picked for its grid shape, once per
+                # shape: members of one shape share the table's entry
                 self.steps.append(MoistLargeStep(member_config(mb, grid), upload(host, self.device),
-                                                 upload(metrics, self.device), stream=st, concurrent=False))
+                                                 upload(metrics, self.device), stream=st, concurrent=False,
+                                                 tuner=tuner))
         self.graph: torch.cuda.CUDAGraph | None = None
 
     @property

@@ -391,9 +391,13 @@ class MoistLargeStep:
     captured in a CUDA graph."""
 
     def __init__(self, cfg: MoistStepConfig, state: dict[str, torch.Tensor], metrics: dict[str, torch.Tensor], *,
-                 stream: Any | None = None, concurrent: bool = True) -> None:
+                 stream: Any | None = None, concurrent: bool = True, tuner: Any | None = None) -> None:
         self.cfg, self.s, self.m = cfg, state, metrics
         self.stream = stream
+        # the scalar advection's z-chunk per stage kind (fifth order, WENO5);
+        # None: the kernel's default, else picked for this grid by ``tuner``
+        # (gm1_b200.autotune.Autotuner) at the end of set-up
+        self.chunk = {False: None, True: None}
         ni, nj, nk = cfg.ni, cfg.nj, cfg.nk
         s, m = state, metrics
         self.k3 = dict(ni=ni, nj=nj, nk=nk)
@@ -494,6 +498,26 @@ class MoistLargeStep:
         self._ones_j = torch.ones(nj, dtype=torch.float32, device=dev)
         self._mh_col = m["mh"][:, 0, 0].contiguous()
         self.completed_steps = 0
+        if tuner is not None:
+            self._tune(tuner)
+
+    def _tune(self, tuner) -> None:
+        """The z-chunk of the fifth-order and the WENO5 scalar advection for
+        this grid shape: each candidate timed on the state's theta carrier
+        into a scratch tendency (the state is not written); the chunk changes
+        which CTA forms which level, not a word."""
+        s, m, cfg = self.s, self.m, self.cfg
+        st = self._st()
+        scratch = torch.empty_like(s["theta_adv"])
+        flux = {"rru": s["rru"], "rrv": s["rrv"], "rrw": s["rrw"]}
+        met = {"c1": m["c1"], "c2": m["c2"], "rr0": m["rr0"], "gz": m["gz"]}
+        kind = "moist_scalar_advection5" + ("_flat" if self.flat else "")
+        with torch.cuda.stream(st):
+            for weno in (False, True):
+                def run(c, weno=weno):
+                    self.chunk[weno] = c
+                    self._advect(s["theta_padded"], flux, met, scratch, theta_weps_f64(), 3 if weno else 1, st)
+                self.chunk[weno] = tuner.choose(kind + ("_weno" if weno else ""), cfg.ni, cfg.nj, cfg.nk, run)
 
     # -- helpers -----------------------------------------------------------
     def _st(self):
@@ -609,10 +633,12 @@ class MoistLargeStep:
             launch_cuda_gm1_child_stretched_scalar_advection5(padded, flux, met, s["divx"], tendency, None,
                                                               self.scalar_column, **self.k3, dx=cfg.dx, dy=cfg.dy,
                                                               nrk=nrk, weps=weps, stream=st,
-                                                              lateral_sides=cfg.lateral_sides, write_fluxes=False)
+                                                              lateral_sides=cfg.lateral_sides, write_fluxes=False,
+                                                              levels_per_chunk=self.chunk[nrk == 3])
         else:
             launch_cuda_scalar_advection5(padded, flux, met, s["divx"], tendency, None, weps=weps, **self.grid,
-                                          nrk=nrk, stream=st, lateral_sides=cfg.lateral_sides, write_fluxes=False)
+                                          nrk=nrk, stream=st, lateral_sides=cfg.lateral_sides, write_fluxes=False,
+                                          levels_per_chunk=self.chunk[nrk == 3])
 
     def _species_advection(self, r: int, nrk: int, st) -> None:
         s, m, cfg = self.s, self.m, self.cfg

@@ -220,3 +220,23 @@ def test_courant_stop_is_refused():
     with pytest.raises(CourantStop):
         dev.check()
     assert dev.status()["max_courant"] >= 1.5
+
+
+def test_tuned_step_gives_the_untuned_words():
+    """A step whose scalar-advection z-chunks the autotuner picked for its
+    grid leaves the words of the default chunks (the chunk decides which CTA
+    forms a level, not the level's words)."""
+    from gm1_b200.autotune import Autotuner  # noqa: PLC0415
+
+    cfg = MoistStepConfig(40, 24, 18, 1000.0, 1000.0, 250.0, 5.0, 10)
+    host, metrics = weisman_klemp_initial_state(cfg, seed=9, bubble_radius_m=(6000.0, 1400.0), bubble_cloud=1.0e-3)
+    tuner = Autotuner()
+    tuned = MoistLargeStep(cfg, upload(host), upload(metrics), tuner=tuner)
+    plain = MoistLargeStep(cfg, upload(host), upload(metrics))
+    assert len(tuner.table) == 2 and all(v["best"] in (1, 2, 4, 8, 16) for v in tuner.table.values())
+    for _ in range(2):
+        tuned.step()
+        plain.step()
+    torch.cuda.synchronize()
+    for n in FIELDS:
+        assert torch.equal(tuned.s[n], plain.s[n]), n
