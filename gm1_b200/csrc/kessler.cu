@@ -696,6 +696,9 @@ struct MassArgs {
     const float *ruh, *rvh, *rmh, *pi0, *th0, *th3d, *qv;
     float *pp3d, *prs, *rho, *rr;
     int ni, nj, nk;
+    // the ledger's cells: columns i0..i1-1 of rows j0..j1-1 (the whole plane
+    // unless a decomposed run sums its interior only)
+    int i0, i1, j0, j1;
 };
 
 constexpr int kMassThreads = 256;
@@ -707,11 +710,12 @@ constexpr int kMassChunks = 16;  // CTAs per level: chunk c sums cells ij = c*25
 __global__ void __launch_bounds__(kMassThreads) apmasscon_levels_kernel(MassArgs a, double *partials, int pressure) {
     __shared__ double s_dry[kMassThreads], s_pi[kMassThreads];
     const int k = blockIdx.x, c = blockIdx.y;
-    const size_t nxy = (size_t)a.ni * a.nj, base = (size_t)k * nxy;
+    const int wi = a.i1 - a.i0;
+    const size_t nw = (size_t)wi * (a.j1 - a.j0), base = (size_t)k * a.ni * a.nj;
     double dry = 0.0, pis = 0.0;
-    for (size_t ij = (size_t)c * kMassThreads + threadIdx.x; ij < nxy; ij += (size_t)kMassChunks * kMassThreads) {
-        const int i = (int)(ij % a.ni), j = (int)(ij / a.ni);
-        const size_t q = base + ij;
+    for (size_t ij = (size_t)c * kMassThreads + threadIdx.x; ij < nw; ij += (size_t)kMassChunks * kMassThreads) {
+        const int i = a.i0 + (int)(ij % wi), j = a.j0 + (int)(ij / wi);
+        const size_t q = base + (size_t)j * a.ni + i;
         float term = a.rho[q] * __ldg(a.ruh + i);
         term = term * __ldg(a.rvh + j);
         term = term * __ldg(a.rmh + q);
@@ -805,17 +809,21 @@ float mass_rddcv() {
 
 size_t mass_workspace_bytes(int nk) { return sizeof(double) * (2 * (size_t)nk * kMassChunks + 2); }
 
-int32_t mass_correction(const MassArgs &m, const double *mass1, double *diag, void *workspace, cudaStream_t st) {
+int32_t mass_partials(const MassArgs &m, double *partials, int pressure, cudaStream_t st) {
+    ProfScope ps("apmasscon_levels_kernel", st);
+    apmasscon_levels_kernel<<<dim3(m.nk, kMassChunks), kMassThreads, 0, st>>>(m, partials, pressure);
+    ps.stop();
+    return launched("apmasscon_levels_kernel") ? GM1B_OK : GM1B_ERR_CUDA;
+}
+
+// the correction from level partials already formed (and, in a decomposed
+// run, added over the subdomains), then the EOS rebuild of every cell
+int32_t mass_apply(const MassArgs &m, const double *partials, const double *mass1, double cells, double *diag,
+                   void *workspace, cudaStream_t st) {
     double *layers = static_cast<double *>(workspace);
     float *corr = reinterpret_cast<float *>(layers + 2 * (size_t)m.nk * kMassChunks);
     const size_t n = (size_t)m.ni * m.nj * m.nk;
-    {
-        ProfScope ps("apmasscon_levels_kernel", st);
-        apmasscon_levels_kernel<<<dim3(m.nk, kMassChunks), kMassThreads, 0, st>>>(m, layers, 1);
-        ps.stop();
-    }
-    if (!launched("apmasscon_levels_kernel")) return GM1B_ERR_CUDA;
-    apmasscon_finish_kernel<<<1, 1, 0, st>>>(layers, m.nk, mass1, (double)n, mass_rddcv(), corr, diag);
+    apmasscon_finish_kernel<<<1, 1, 0, st>>>(partials, m.nk, mass1, cells, mass_rddcv(), corr, diag);
     if (!launched("apmasscon_finish_kernel")) return GM1B_ERR_CUDA;
     const unsigned grid = (unsigned)std::min<size_t>((n + 255) / 256, (size_t)148 * 8);
     {
@@ -824,6 +832,13 @@ int32_t mass_correction(const MassArgs &m, const double *mass1, double *diag, vo
         ps.stop();
     }
     return launched("apmasscon_apply_kernel") ? GM1B_OK : GM1B_ERR_CUDA;
+}
+
+int32_t mass_correction(const MassArgs &m, const double *mass1, double *diag, void *workspace, cudaStream_t st) {
+    double *layers = static_cast<double *>(workspace);
+    const int32_t rc = mass_partials(m, layers, 1, st);
+    if (rc != GM1B_OK) return rc;
+    return mass_apply(m, layers, mass1, (double)((size_t)m.ni * m.nj * m.nk), diag, workspace, st);
 }
 
 bool mass_grid_ok(const char *who, int32_t ni, int32_t nj, int32_t nk) {
@@ -849,7 +864,7 @@ extern "C" int32_t gm1b_dry_mass(int32_t ni, int32_t nj, int32_t nk, const float
         return GM1B_ERR_ARGUMENT;
     }
     MassArgs m{ruh, rvh, rmh, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, const_cast<float *>(rho), nullptr,
-               ni, nj, nk};
+               ni, nj, nk, 0, ni, 0, nj};
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     double *layers = static_cast<double *>(workspace);
     apmasscon_levels_kernel<<<dim3(nk, kMassChunks), kMassThreads, 0, st>>>(m, layers, 0);
@@ -872,15 +887,22 @@ extern "C" int32_t gm1b_apmasscon(int32_t ni, int32_t nj, int32_t nk, const gm1b
             gm1b_set_error("gm1b_apmasscon: a required array is NULL");
             return GM1B_ERR_ARGUMENT;
         }
-    const MassArgs m{a.ruh, a.rvh, a.rmh, a.pi0, a.th0, a.th3d, a.qv, a.pp3d, a.prs, a.rho, nullptr, ni, nj, nk};
+    const MassArgs m{a.ruh, a.rvh, a.rmh, a.pi0, a.th0, a.th3d, a.qv, a.pp3d, a.prs, a.rho, nullptr, ni, nj, nk,
+                     0, ni, 0, nj};
     return mass_correction(m, mass1, diagnostics, workspace, static_cast<cudaStream_t>(stream));
 }
 
 namespace {
+// phase 0: the whole transition; with the dry-mass correction split for a
+// decomposed run, phase 1 (held removal, pre-physics EOS, the level partials
+// of the window into partials) and phase 2 (the correction from partials
+// already added over the subdomains, for `cells` cells, then the driver and
+// the recapture)
 int32_t kessler_large_step(int32_t ni, int32_t nj, int32_t nk, const gm1b_kessler_arrays *arrays,
                            const gm1b_kessler_held *held, float dx, float dy, float dz, float dt, int32_t equation_set,
                            int32_t efall, void *workspace, size_t workspace_size, const double *mass1,
-                           double *mass_diagnostics, void *mass_workspace, void *stream) {
+                           double *mass_diagnostics, void *mass_workspace, void *stream, int phase = 0,
+                           const int32_t *window = nullptr, double *partials = nullptr, double cells = 0.0) {
     if (arrays == nullptr || ni < 1 || nj < 1 || nk < 2) {
         gm1b_set_error("gm1b_kessler_large_step: need arrays, ni >= 1, nj >= 1, nk >= 2");
         return GM1B_ERR_ARGUMENT;
@@ -903,17 +925,26 @@ int32_t kessler_large_step(int32_t ni, int32_t nj, int32_t nk, const gm1b_kessle
     const KesslerEos c{(float)((double)cp / (double)rd), 100000.0f, rd, 461.5f};
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const unsigned grid = (unsigned)std::min<size_t>((n + 255) / 256, (size_t)148 * 8);
-    {
-        ProfScope ps("kessler_pre_physics_kernel", st);
-        kessler_pre_physics_kernel<<<grid, 256, 0, st>>>(*arrays, h, n, dt, eqt2 ? 1 : 0, c);
-        ps.stop();
-    }
-    if (!launched("kessler_pre_physics_kernel")) return GM1B_ERR_CUDA;
-    if (mass1 != nullptr) {  // apmasscon between the pre-physics EOS and the driver
-        const gm1b_kessler_arrays &k = *arrays;
-        const MassArgs m{k.ruh, k.rvh, k.rmh, k.pi0, k.th0, k.th3d, k.qv, k.pp3d, k.prs, k.rho,
-                         const_cast<float *>(k.rr), ni, nj, nk};
-        const int32_t mrc = mass_correction(m, mass1, mass_diagnostics, mass_workspace, st);
+    const gm1b_kessler_arrays &k = *arrays;
+    MassArgs m{k.ruh, k.rvh, k.rmh, k.pi0, k.th0, k.th3d, k.qv, k.pp3d, k.prs, k.rho,
+               const_cast<float *>(k.rr), ni, nj, nk, 0, ni, 0, nj};
+    if (phase != 2) {
+        {
+            ProfScope ps("kessler_pre_physics_kernel", st);
+            kessler_pre_physics_kernel<<<grid, 256, 0, st>>>(*arrays, h, n, dt, eqt2 ? 1 : 0, c);
+            ps.stop();
+        }
+        if (!launched("kessler_pre_physics_kernel")) return GM1B_ERR_CUDA;
+        if (phase == 1) {  // the window's level partials of the dry-mass ledger
+            m.i0 = window[0], m.i1 = window[1], m.j0 = window[2], m.j1 = window[3];
+            return mass_partials(m, partials, 1, st);
+        }
+        if (mass1 != nullptr) {  // apmasscon between the pre-physics EOS and the driver
+            const int32_t mrc = mass_correction(m, mass1, mass_diagnostics, mass_workspace, st);
+            if (mrc != GM1B_OK) return mrc;
+        }
+    } else {
+        const int32_t mrc = mass_apply(m, partials, mass1, cells, mass_diagnostics, mass_workspace, st);
         if (mrc != GM1B_OK) return mrc;
     }
     const int32_t rc = gm1b_kessler_driver(ni, nj, nk, arrays, dx, dy, dz, dt, equation_set, efall, workspace,
@@ -953,4 +984,75 @@ extern "C" int32_t gm1b_kessler_large_step_apmasscon(int32_t ni, int32_t nj, int
     }
     return kessler_large_step(ni, nj, nk, arrays, held, dx, dy, dz, dt, equation_set, efall, workspace,
                               workspace_size, mass1, mass_diagnostics, mass_workspace, stream);
+}
+
+extern "C" size_t gm1b_apmasscon_partials_words(int32_t nk) { return nk < 1 ? 0 : 2 * (size_t)nk * kMassChunks; }
+
+namespace {
+bool window_ok(const char *who, int32_t ni, int32_t nj, const int32_t *w) {
+    if (w == nullptr || w[0] < 0 || w[1] > ni || w[0] >= w[1] || w[2] < 0 || w[3] > nj || w[2] >= w[3]) {
+        gm1b_set_error("%s: the window (i0, i1, j0, j1) must be a non-empty part of the %dx%d plane", who, ni, nj);
+        return false;
+    }
+    return true;
+}
+}  // namespace
+
+extern "C" int32_t gm1b_apmasscon_partials(int32_t ni, int32_t nj, int32_t nk, const float *rho, const float *ruh,
+                                           const float *rvh, const float *rmh, const float *pi0, const float *pp3d,
+                                           const int32_t *window, int32_t pressure, double *partials, void *stream) {
+    if (!mass_grid_ok("gm1b_apmasscon_partials", ni, nj, nk) || !window_ok("gm1b_apmasscon_partials", ni, nj, window))
+        return GM1B_ERR_ARGUMENT;
+    if (rho == nullptr || ruh == nullptr || rvh == nullptr || rmh == nullptr || partials == nullptr ||
+        (pressure && (pi0 == nullptr || pp3d == nullptr))) {
+        gm1b_set_error("gm1b_apmasscon_partials: rho, ruh, rvh, rmh, partials (and pi0, pp3d for the Exner sum) "
+                       "are required");
+        return GM1B_ERR_ARGUMENT;
+    }
+    const MassArgs m{ruh, rvh, rmh, pi0, nullptr, nullptr, nullptr, const_cast<float *>(pp3d), nullptr,
+                     const_cast<float *>(rho), nullptr, ni, nj, nk, window[0], window[1], window[2], window[3]};
+    return mass_partials(m, partials, pressure ? 1 : 0, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int32_t gm1b_dry_mass_from_partials(int32_t nk, const double *partials, double *mass, int32_t only_if_unset,
+                                               void *stream) {
+    if (nk < 1 || partials == nullptr || mass == nullptr) {
+        gm1b_set_error("gm1b_dry_mass_from_partials: need nk >= 1, partials and mass");
+        return GM1B_ERR_ARGUMENT;
+    }
+    dry_mass_finish_kernel<<<1, 1, 0, static_cast<cudaStream_t>(stream)>>>(partials, nk, mass, only_if_unset ? 1 : 0);
+    return launched("dry_mass_finish_kernel") ? GM1B_OK : GM1B_ERR_CUDA;
+}
+
+extern "C" int32_t gm1b_kessler_large_step_apmasscon_begin(int32_t ni, int32_t nj, int32_t nk,
+                                                           const gm1b_kessler_arrays *arrays,
+                                                           const gm1b_kessler_held *held, float dt,
+                                                           int32_t equation_set, const int32_t *window,
+                                                           double *partials, void *stream) {
+    const char *who = "gm1b_kessler_large_step_apmasscon_begin";
+    if (arrays == nullptr || arrays->ruh == nullptr || arrays->rvh == nullptr || arrays->rmh == nullptr ||
+        partials == nullptr || !mass_grid_ok(who, ni, nj, nk) || !window_ok(who, ni, nj, window)) {
+        if (arrays == nullptr || partials == nullptr) gm1b_set_error("%s: arrays and partials are required", who);
+        return GM1B_ERR_ARGUMENT;
+    }
+    return kessler_large_step(ni, nj, nk, arrays, held, 1.0f, 1.0f, 1.0f, dt, equation_set, 0, nullptr, 0, nullptr,
+                              nullptr, nullptr, stream, 1, window, partials, 0.0);
+}
+
+extern "C" int32_t gm1b_kessler_large_step_apmasscon_end(int32_t ni, int32_t nj, int32_t nk,
+                                                         const gm1b_kessler_arrays *arrays,
+                                                         const gm1b_kessler_held *held, float dx, float dy, float dz,
+                                                         float dt, int32_t equation_set, int32_t efall,
+                                                         void *workspace, size_t workspace_size,
+                                                         const double *partials, double cells, const double *mass1,
+                                                         double *mass_diagnostics, void *mass_workspace,
+                                                         void *stream) {
+    if (partials == nullptr || mass1 == nullptr || mass_workspace == nullptr || !(cells > 0.0)) {
+        gm1b_set_error("gm1b_kessler_large_step_apmasscon_end: partials, mass1, the mass workspace and cells > 0 "
+                       "are required");
+        return GM1B_ERR_ARGUMENT;
+    }
+    return kessler_large_step(ni, nj, nk, arrays, held, dx, dy, dz, dt, equation_set, efall, workspace,
+                              workspace_size, mass1, mass_diagnostics, mass_workspace, stream, 2, nullptr,
+                              const_cast<double *>(partials), cells);
 }

@@ -17,9 +17,9 @@ next step reads them; the outer ghost cells of a halo are scratch of the fake
 edge.  Exchanges run in two phases, x then y over the x-widened rows, so the
 corner halos come from the diagonal neighbour through the x neighbour's
 fresh strip.  The FP64 Kessler budgets (asq, qbudget) accumulate over each
-rank's widened subdomain and are not reduced here; the final-RK dry-air mass
-correction, a domain-wide reduction, is refused (local_steps) - a decomposed
-configuration runs with apmasscon=False.
+rank's widened subdomain and are not reduced here.  The final-RK dry-air
+mass correction, a domain-wide reduction, is formed from the level sums of
+every subdomain's own cells added over the subdomains (DecomposedRun).
 
 The exchange (one message per neighbour per phase, packed contiguous) runs
 over torch.distributed point-to-point sends (gloo on CPU tensors, NCCL on
@@ -241,16 +241,80 @@ class HaloExchange:
 class DecomposedRun:
     """Large steps of a decomposed domain: each local subdomain's step
     (an object with .step(), e.g. MoistLargeStep on the widened
-    subdomain's state) followed by the halo exchange."""
+    subdomain's state) followed by the halo exchange.
 
-    def __init__(self, steps: Mapping[int, Any], exchange: HaloExchange, sync: Callable[[], None] | None = None):
+    With the final-RK dry-air mass correction on (the steps' cfg.apmasscon),
+    the correction is the domain's: each step runs up to the ledger
+    (step_begin), the level partials of every subdomain's own cells are added
+    - the local subdomains' in rank order, then over processes by an
+    all-reduce - and every subdomain finishes from the same sums
+    (step_end).  The ledger mass1 of the starting state is formed the same
+    way at set-up.  The added binary64 ledgers differ from the single
+    domain's only in the order of their sums, so the binary32 correction is
+    the single domain's word unless its binary64 value lies within the
+    sums' rounding of a binary32 rounding boundary."""
+
+    def __init__(self, steps: Mapping[int, Any], exchange: HaloExchange, sync: Callable[[], None] | None = None,
+                 group: Any = None):
         self.steps = dict(steps)
         self.x = exchange
         self.sync = sync
+        self.group = group
+        first = next(iter(self.steps.values()))
+        self.mass = bool(getattr(getattr(first, "cfg", None), "apmasscon", False)) and hasattr(first, "step_begin")
+        if getattr(getattr(first, "cfg", None), "apmasscon", False) and not self.mass:
+            from .errors import refuse  # noqa: PLC0415
+
+            refuse(code="GM1B-DECOMPOSE-APMASSCON", gate="decomposition", option="apmasscon", value=True,
+                   reason="the dry-air mass correction is a domain-wide reduction and this step runs as one call",
+                   remedy="decompose with MoistLargeStep (its step splits at the ledger) or apmasscon=False")
+        if self.mass:
+            self._mass_setup()
+
+    def _window(self, rank: int) -> tuple[int, int, int, int]:
+        s = self.x.subs[rank]
+        return (s.hw, s.hw + s.nx, s.hs, s.hs + s.ny)
+
+    def _sum(self, parts: Mapping[int, Any]):
+        import torch.distributed as dist  # noqa: PLC0415
+
+        ranks = sorted(parts)
+        total = parts[ranks[0]].clone()
+        for r in ranks[1:]:
+            total.add_(parts[r])
+        if dist.is_available() and dist.is_initialized() and dist.get_world_size(self.group) > 1:
+            dist.all_reduce(total, group=self.group)
+        return total
+
+    def _mass_setup(self) -> None:
+        import torch  # noqa: PLC0415
+
+        from .kessler import apmasscon_partials_words, dry_mass_from_partials, dry_mass_partials  # noqa: PLC0415
+
+        first = next(iter(self.steps.values()))
+        nk = first.cfg.nk
+        self.cells = sum(s.nx * s.ny for s in self.x.subs.values()) * nk
+        words = apmasscon_partials_words(nk)
+        self.partials = {r: torch.zeros(words, dtype=torch.float64, device=st.s["rho"].device)
+                         for r, st in self.steps.items()}
+        for r, st in self.steps.items():
+            s, m = st.s, st.m
+            dry_mass_partials(s["rho"], s["ruh"], s["rvh"], m["rmh"], ni=st.cfg.ni, nj=st.cfg.nj, nk=nk,
+                              window=self._window(r), partials=self.partials[r])
+        total = self._sum(self.partials)
+        for st in self.steps.values():
+            dry_mass_from_partials(total, nk, st.s["mass1"])
 
     def step(self) -> None:
-        for s in self.steps.values():
-            s.step()
+        if self.mass:
+            for r, s in self.steps.items():
+                s.step_begin(self._window(r), self.partials[r])
+            total = self._sum(self.partials)
+            for s in self.steps.values():
+                s.step_end(total, self.cells)
+        else:
+            for s in self.steps.values():
+                s.step()
         if self.sync is not None:
             self.sync()
         self.x.exchange()
@@ -305,12 +369,6 @@ def local_steps(cfg, host: Mapping[str, np.ndarray], metrics: Mapping[str, np.nd
     widened ni, nj)."""
     import dataclasses  # noqa: PLC0415
 
-    from .errors import refuse  # noqa: PLC0415
-
-    if getattr(cfg, "apmasscon", False) and len(subs) > 1:
-        refuse(code="GM1B-DECOMPOSE-APMASSCON", gate="decomposition", option="apmasscon", value=True,
-               reason="the dry-air mass correction is a domain-wide reduction; each widened subdomain would correct "
-                      "against its own ledger", remedy="decompose a configuration with apmasscon=False")
     out = {}
     for s in subs:
         if s.rank not in ranks:

@@ -309,6 +309,48 @@ class CudaGm1KesslerLargeStepTransition:
             ev = torch.cuda.Event()
             ev.record(st)
         self.completed_transitions += 1
+        return self._result(ev)
+
+    def _structs(self):
+        a, h = self.arrays, self.carriers
+        s = _KesslerArrays(**{n: t.data_ptr() for n, t in a.items() if n in ALL_ARRAY_NAMES})
+        held = _HeldArrays(**{n: getattr(h, n).data_ptr() for n in HELD_NAMES})
+        st = torch.cuda.current_stream(a["rho"].device) if self.stream is None else self.stream
+        return s, held, st
+
+    def begin(self, window: tuple[int, int, int, int], partials: torch.Tensor) -> None:
+        """The transition of a subdomain up to the dry-mass ledger: held
+        rates removed, the pre-physics EOS, and the level partials of its own
+        cells (window = (i0, i1, j0, j1) columns and rows) into partials
+        (float64, apmasscon_partials_words(nk) words)."""
+        if self.mass1 is None:
+            raise RuntimeError("begin/end split the dry-mass correction: build the transition with mass1")
+        s, held, st = self._structs()
+        w = (ctypes.c_int32 * 4)(*window)
+        with torch.cuda.device(self.arrays["rho"].device):
+            _native.check(_apmasscon_lib().gm1b_kessler_large_step_apmasscon_begin(
+                self.ni, self.nj, self.nk, ctypes.byref(s), ctypes.byref(held), self.dt, self.selection.equation_set,
+                w, ctypes.c_void_p(partials.data_ptr()), ctypes.c_void_p(st.cuda_stream)),
+                "gm1b_kessler_large_step_apmasscon_begin")
+
+    def end(self, partials: torch.Tensor, cells: int) -> Gm1KesslerLargeStepResult:
+        """The rest of the transition from the domain's added partials: the
+        correction for `cells` cells, the driver, the recapture."""
+        s, held, st = self._structs()
+        with torch.cuda.device(self.arrays["rho"].device):
+            _native.check(_apmasscon_lib().gm1b_kessler_large_step_apmasscon_end(
+                self.ni, self.nj, self.nk, ctypes.byref(s), ctypes.byref(held), self.dx, self.dy, self.dz, self.dt,
+                self.selection.equation_set, self.selection.efall, ctypes.c_void_p(self.workspace.buffer.data_ptr()),
+                self.workspace.buffer.numel(), ctypes.c_void_p(partials.data_ptr()), float(cells),
+                ctypes.c_void_p(self.mass1.data_ptr()), ctypes.c_void_p(self.mass_diagnostics.data_ptr()),
+                ctypes.c_void_p(self.mass_workspace.data_ptr()), ctypes.c_void_p(st.cuda_stream)),
+                "gm1b_kessler_large_step_apmasscon_end")
+            ev = torch.cuda.Event()
+            ev.record(st)
+        self.completed_transitions += 1
+        return self._result(ev)
+
+    def _result(self, ev) -> Gm1KesslerLargeStepResult:
         return Gm1KesslerLargeStepResult(ev, self.completed_transitions, {
             "operator": "gm1-kessler-large-step", "equation_set": self.selection.equation_set,
             "source_order": ("solve2-held-remove-snapshot", "solve2-pre-physics-eos") +
@@ -393,8 +435,50 @@ def _apmasscon_lib() -> ctypes.CDLL:
                                                                             c.POINTER(_HeldArrays)] + \
             [c.c_float] * 4 + [c.c_int32, c.c_int32, c.c_void_p, c.c_size_t] + [c.c_void_p] * 4
         lib.gm1b_kessler_large_step_apmasscon.restype = c.c_int32
+        lib.gm1b_apmasscon_partials_words.argtypes = [c.c_int32]
+        lib.gm1b_apmasscon_partials_words.restype = c.c_size_t
+        lib.gm1b_apmasscon_partials.argtypes = [c.c_int32] * 3 + [c.c_void_p] * 6 + [c.POINTER(c.c_int32), c.c_int32,
+                                                                                     c.c_void_p, c.c_void_p]
+        lib.gm1b_apmasscon_partials.restype = c.c_int32
+        lib.gm1b_dry_mass_from_partials.argtypes = [c.c_int32, c.c_void_p, c.c_void_p, c.c_int32, c.c_void_p]
+        lib.gm1b_dry_mass_from_partials.restype = c.c_int32
+        lib.gm1b_kessler_large_step_apmasscon_begin.argtypes = [c.c_int32] * 3 + [c.POINTER(_KesslerArrays),
+                                                                                  c.POINTER(_HeldArrays), c.c_float,
+                                                                                  c.c_int32, c.POINTER(c.c_int32),
+                                                                                  c.c_void_p, c.c_void_p]
+        lib.gm1b_kessler_large_step_apmasscon_begin.restype = c.c_int32
+        lib.gm1b_kessler_large_step_apmasscon_end.argtypes = [c.c_int32] * 3 + [c.POINTER(_KesslerArrays),
+                                                                                c.POINTER(_HeldArrays)] + \
+            [c.c_float] * 4 + [c.c_int32, c.c_int32, c.c_void_p, c.c_size_t, c.c_void_p, c.c_double] + [c.c_void_p] * 4
+        lib.gm1b_kessler_large_step_apmasscon_end.restype = c.c_int32
         lib._apmasscon_bound = True
     return lib
+
+
+def apmasscon_partials_words(nk: int) -> int:
+    return int(_apmasscon_lib().gm1b_apmasscon_partials_words(nk))
+
+
+def dry_mass_partials(rho, ruh, rvh, rmh, *, ni: int, nj: int, nk: int, window: tuple[int, int, int, int],
+                      partials: torch.Tensor, stream: Any | None = None) -> torch.Tensor:
+    """The dry-mass ledger's level partials over a window of cells (a
+    subdomain's own), to be added over the subdomains and finished by
+    dry_mass_from_partials."""
+    st = torch.cuda.current_stream(rho.device) if stream is None else stream
+    w = (ctypes.c_int32 * 4)(*window)
+    with torch.cuda.device(rho.device):
+        _native.check(_apmasscon_lib().gm1b_apmasscon_partials(
+            ni, nj, nk, rho.data_ptr(), ruh.data_ptr(), rvh.data_ptr(), rmh.data_ptr(), None, None, w, 0,
+            partials.data_ptr(), ctypes.c_void_p(st.cuda_stream)), "gm1b_apmasscon_partials")
+    return partials
+
+
+def dry_mass_from_partials(partials: torch.Tensor, nk: int, out: torch.Tensor, stream: Any | None = None) -> None:
+    st = torch.cuda.current_stream(out.device) if stream is None else stream
+    with torch.cuda.device(out.device):
+        _native.check(_apmasscon_lib().gm1b_dry_mass_from_partials(nk, partials.data_ptr(), out.data_ptr(), 0,
+                                                                   ctypes.c_void_p(st.cuda_stream)),
+                      "gm1b_dry_mass_from_partials")
 
 
 def apmasscon_array_shapes(ni: int, nj: int, nk: int) -> dict[str, tuple[int, ...]]:

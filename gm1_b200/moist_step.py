@@ -853,11 +853,9 @@ class MoistLargeStep:
                 self.stream = saved
         self._join(main, (bnd, tke))
 
-    def step(self) -> None:
-        """One large step: the operations of large_step_schedule() in order
-        (each stage's scalar / boundary / TKE tail concurrently when the step
-        is concurrent)."""
-        ops = large_step_schedule()
+    def _run_ops(self, ops) -> None:
+        """Operations of the schedule in order (each stage's scalar /
+        boundary / TKE tail concurrently when the step is concurrent)."""
         q = 0
         while q < len(ops):
             op = ops[q]
@@ -871,6 +869,43 @@ class MoistLargeStep:
                 continue
             self.execute(op)
             q += 1
+
+    def step(self) -> None:
+        """One large step: the operations of large_step_schedule() in order."""
+        self._run_ops(large_step_schedule())
+        self.completed_steps += 1
+
+    # -- a step split at the dry-mass ledger (a domain decomposed over
+    # subdomains forms the ledger over all of them between the halves) -----
+    def _microphysics_index(self) -> int:
+        ops = large_step_schedule()
+        return next(q for q, op in enumerate(ops) if op.phase is StepPhase.MICROPHYSICS)
+
+    def step_begin(self, window: tuple[int, int, int, int], partials: torch.Tensor) -> None:
+        """The step up to the dry-mass ledger: every operation before the
+        microphysics, then the Kessler transition's held removal and
+        pre-physics EOS and the level partials of the cells in window
+        (i0, i1, j0, j1) into partials."""
+        if not self.cfg.apmasscon:
+            raise RuntimeError("step_begin/step_end split the dry-mass correction: the configuration has none")
+        self._run_ops(large_step_schedule()[:self._microphysics_index()])
+        st = self._st()
+        with torch.cuda.stream(st):
+            self._interior_pp3d_to_compact()
+        self.kessler.stream = st
+        self.kessler.begin(window, partials)
+
+    def step_end(self, partials: torch.Tensor, cells: int) -> None:
+        """The rest of the step from the added partials of the domain's
+        `cells` cells: the correction, the Kessler driver and recapture, the
+        operations after the microphysics."""
+        st = self._st()
+        self.kessler.stream = st
+        self.kessler.end(partials, cells)
+        self.fold_kessler_status(st)
+        with torch.cuda.stream(st):
+            self._compact_pp3d_to_interior()
+        self._run_ops(large_step_schedule()[self._microphysics_index() + 1:])
         self.completed_steps += 1
 
 

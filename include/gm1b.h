@@ -421,6 +421,35 @@ GM1B_API int32_t gm1b_kessler_large_step_apmasscon(int32_t ni, int32_t nj, int32
                                                    const double *mass1, double *mass_diagnostics,
                                                    void *mass_workspace, void *stream);
 
+/* The correction of a domain split over subdomains (each a widened block of
+ * the domain, stepped on its own): the level partials of the dry-mass
+ * ledger and of the Exner sum over a window of cells (columns i0..i1-1 of
+ * rows j0..j1-1: the subdomain's own cells), gm1b_apmasscon_partials_words
+ * doubles; the subdomains' partials added word by word (in a fixed order, or
+ * by an all-reduce) give the domain's, from which every subdomain forms the
+ * same correction.  _begin runs the transition up to the ledger (held rates,
+ * pre-physics EOS, the window's partials), _end the rest from the added
+ * partials and the domain's cell count.  gm1b_dry_mass_from_partials turns
+ * added dry-mass partials (pressure = 0) into the ledger mass1. */
+GM1B_API size_t gm1b_apmasscon_partials_words(int32_t nk);
+GM1B_API int32_t gm1b_apmasscon_partials(int32_t ni, int32_t nj, int32_t nk, const float *rho, const float *ruh,
+                                         const float *rvh, const float *rmh, const float *pi0, const float *pp3d,
+                                         const int32_t *window, int32_t pressure, double *partials, void *stream);
+GM1B_API int32_t gm1b_dry_mass_from_partials(int32_t nk, const double *partials, double *mass, int32_t only_if_unset,
+                                             void *stream);
+GM1B_API int32_t gm1b_kessler_large_step_apmasscon_begin(int32_t ni, int32_t nj, int32_t nk,
+                                                         const gm1b_kessler_arrays *arrays,
+                                                         const gm1b_kessler_held *held, float dt,
+                                                         int32_t equation_set, const int32_t *window,
+                                                         double *partials, void *stream);
+GM1B_API int32_t gm1b_kessler_large_step_apmasscon_end(int32_t ni, int32_t nj, int32_t nk,
+                                                       const gm1b_kessler_arrays *arrays,
+                                                       const gm1b_kessler_held *held, float dx, float dy, float dz,
+                                                       float dt, int32_t equation_set, int32_t efall, void *workspace,
+                                                       size_t workspace_size, const double *partials, double cells,
+                                                       const double *mass1, double *mass_diagnostics,
+                                                       void *mass_workspace, void *stream);
+
 /*
  * gm1b_kessler_driver without a workspace argument, for callers that cannot
  * allocate device memory of their own (for instance a Fortran or C host

@@ -2,11 +2,14 @@
 one domain run as 2x1 and 2x2 widened subdomains (32-cell halos) held by
 one process on one device, with the halo strips of the carried arrays
 exchanged by device copies after every large step, leaves interiors that are
-the single-domain GPU step's words after 3 steps (apmasscon off: the
-dry-mass correction is a domain-wide reduction) (the Python composition on
-the uniform column, the C entry point on the 80-level stretched column).  The
-FP64 budgets accumulate per widened subdomain; a lateral-boundary history is
-compared on the rank that holds that edge of the domain."""
+the single-domain GPU step's words after 3 steps: the Python composition on
+the uniform and the stretched column with the dry-air mass correction (its
+ledger added over the subdomains; the binary64 mass1 within 1e-13 of the
+single domain's, summed in another order) and without it, and the C entry
+point (one call per step, so the correction off) on the 80-level stretched
+column.  The FP64 budgets accumulate per widened subdomain; a
+lateral-boundary history is compared on the rank that holds that edge of the
+domain."""
 
 from __future__ import annotations
 
@@ -24,7 +27,7 @@ pytestmark = pytest.mark.gpu
 HALO = 32
 EDGE = {"radbcw": lambda s, px, py: s.px == 0, "radbce": lambda s, px, py: s.px == px - 1,
         "radbcs": lambda s, px, py: s.py == 0, "radbcn": lambda s, px, py: s.py == py - 1}
-COMPARED = tuple(n for n in CARRIED if n not in ("asq", "qbudget"))
+COMPARED = tuple(n for n in CARRIED if n not in ("asq", "qbudget", "mass1"))
 
 CASES = {
     "python-uniform-2x1": (MoistLargeStep, MoistStepConfig(96, 40, 16, 1000.0, 1000.0, 250.0, 5.0, 10,
@@ -34,6 +37,11 @@ CASES = {
     "native-stretched-2x1": (NativeMoistLargeStep, MoistStepConfig(80, 32, 80, 100.0, 100.0, 100.0, 0.6, 8,
                                                                    column=SUPERCELL_STRETCHED_COLUMN,
                                                                    apmasscon=False), 2, 1),
+    # the dry-air mass correction on: its ledger added over the subdomains
+    "python-apmasscon-2x1": (MoistLargeStep, MoistStepConfig(96, 40, 16, 1000.0, 1000.0, 250.0, 5.0, 10), 2, 1),
+    "python-apmasscon-2x2": (MoistLargeStep, MoistStepConfig(80, 72, 16, 1000.0, 1000.0, 250.0, 5.0, 10), 2, 2),
+    "python-apmasscon-stretched-2x1": (MoistLargeStep, MoistStepConfig(80, 32, 80, 100.0, 100.0, 100.0, 0.6, 8,
+                                                                       column=SUPERCELL_STRETCHED_COLUMN), 2, 1),
 }
 
 
@@ -57,3 +65,6 @@ def test_decomposed_step_is_the_single_domain(case):
         want = global_interior(single.s, cfg.ni, cfg.nj, s, names)
         bad = [n for n in names if not np.array_equal(got[n].view(np.uint8), want[n].view(np.uint8))]
         assert not bad, (case, s.rank, bad)
+        if cfg.apmasscon:  # the domain's ledger, summed in another order
+            m1, m0 = float(steps[s.rank].s["mass1"].item()), float(single.s["mass1"].item())
+            assert abs(m1 - m0) <= 1e-13 * m0, (case, m1, m0)
