@@ -1,0 +1,141 @@
+"""The SGS stress of the flat (terrain_flag=.false.) stretched column on
+B200: CM1 gettau and the momentum stress divergence turbu/turbv/turbw.
+
+Drop-in mirror of the reference operator API (torch CUDA tensors in place of
+CuPy arrays; the same array names and shapes; the two-part binding is not
+built and is refused):
+
+  launch_cuda_flat_strain          the strain half of enqueue_flat_calcdef
+                                   src/cm1core/cuda_gm1_flat_stretched_closure.py:524
+  launch_cuda_flat_gettau          enqueue_flat_gettau           :551
+  launch_cuda_flat_momentum_stress enqueue_flat_momentum_stress  :574
+  launch_cuda_flat_sgs_stress      the three in order (the stress block of
+                                   cuda_cartesian_closure.py:1293-1317)
+
+Each enqueues on ``stream`` (default: the current stream) and returns at
+once; the tendencies are ADDED into uten, vten and wten.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from typing import Any, Mapping
+
+import torch
+
+from . import _native
+from .closure import _grid, _positive, _require
+from .errors import refuse
+from .periodic import CudaLaunch
+
+_FIELDS = ("u3d", "v3d", "w3d", "rho", "rf", "mh", "mf", "mh_profile", "kmh", "kmv", "s11", "s22", "s33", "s12",
+           "s13", "s23", "t11", "t22", "t33", "t12", "t13", "t23", "uten", "vten", "wten")
+STRAIN_NAMES = ("s11", "s22", "s33", "s12", "s13", "s23")
+TAU_NAMES = ("t11", "t22", "t33", "t12", "t13", "t23")
+STRAIN_ARRAY_NAMES = ("u3d", "v3d", "w3d", "rho", "rf", "mf", "mh_profile") + STRAIN_NAMES
+GETTAU_ARRAY_NAMES = STRAIN_NAMES + ("kmh", "kmv") + TAU_NAMES
+MOMENTUM_STRESS_ARRAY_NAMES = TAU_NAMES + ("kmh", "kmv", "rho", "rf", "mh", "mf", "u3d", "v3d", "w3d", "uten",
+                                           "vten", "wten")
+SGS_STRESS_ARRAY_NAMES = tuple(dict.fromkeys(STRAIN_ARRAY_NAMES + GETTAU_ARRAY_NAMES + MOMENTUM_STRESS_ARRAY_NAMES))
+MAX_NK = 200
+
+
+class _Arrays(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_void_p) for n in _FIELDS]
+
+
+def flat_stress_shapes(ni: int, nj: int, nk: int) -> dict[str, tuple[int, ...]]:
+    _grid(ni, nj, nk)
+    cell, face = (nk, nj, ni), (nk + 1, nj, ni)
+    return {"u3d": (nk, nj, ni + 1), "v3d": (nk, nj + 1, ni), "w3d": face, "rho": cell, "rf": face, "mh": cell,
+            "mf": face, "mh_profile": (nk + 2,), "kmh": face, "kmv": face,
+            **{n: cell for n in ("s11", "s22", "s33", "t11", "t22", "t33")},
+            "s12": (nk, nj + 1, ni + 1), "t12": (nk, nj + 1, ni + 1), "s13": (nk + 1, nj, ni + 1),
+            "t13": (nk + 1, nj, ni + 1), "s23": (nk + 1, nj + 1, ni), "t23": (nk + 1, nj + 1, ni),
+            "uten": (nk, nj, ni + 1), "vten": (nk, nj + 1, ni), "wten": face}
+
+
+def _bind(lib) -> None:
+    if getattr(lib, "_stress_bound", False):
+        return
+    i32, f32, vp = ctypes.c_int32, ctypes.c_float, ctypes.c_void_p
+    a = ctypes.POINTER(_Arrays)
+    lib.gm1b_flat_strain.argtypes = [i32, i32, i32, a, f32, f32, f32, vp]
+    lib.gm1b_flat_gettau.argtypes = [i32, i32, i32, a, vp]
+    lib.gm1b_flat_momentum_stress.argtypes = [i32, i32, i32, a, f32, f32, f32, f32, vp]
+    lib.gm1b_flat_sgs_stress.argtypes = [i32, i32, i32, a, f32, f32, f32, f32, vp]
+    for n in ("gm1b_flat_strain", "gm1b_flat_gettau", "gm1b_flat_momentum_stress", "gm1b_flat_sgs_stress"):
+        getattr(lib, n).restype = i32
+    lib._stress_bound = True
+
+
+def _prepare(arrays: Mapping[str, Any], names, ni, nj, nk, what):
+    _grid(ni, nj, nk)
+    if nk > MAX_NK:
+        raise ValueError(f"nk must be <= {MAX_NK} (the column solves' shared memory)")
+    a = _require(arrays, names, flat_stress_shapes(ni, nj, nk), what)
+    s = _Arrays(**{n: (a[n].data_ptr() if n in a else None) for n in _FIELDS})
+    lib = _native.lib()
+    _bind(lib)
+    return a, s, lib
+
+
+def _launch(a, fn, args, name, record) -> CudaLaunch:
+    device = next(iter(a.values())).device
+    st = torch.cuda.current_stream(device) if record["stream"] is None else record["stream"]
+    with torch.cuda.device(device):
+        _native.check(fn(*args, ctypes.c_void_p(st.cuda_stream)), name)
+        ev = torch.cuda.Event()
+        ev.record(st)
+    return CudaLaunch(ev, record["receipt"])
+
+
+def launch_cuda_flat_strain(arrays: Mapping[str, Any], *, ni: int, nj: int, nk: int, dx: float, dy: float,
+                            rdz: float, stream: Any | None = None) -> CudaLaunch:
+    """The strain carriers rho*Sij of the flat calcdef (gm1_flat_calcdef_mass_v1
+    and _face_v1): s11/s22/s33 at cells, s12 at every corner, s13/s23 on face
+    levels 1..nk-1.  ``mh_profile`` (nk+2 words, CM1-indexed) and the 3-D
+    face ``mf`` carry the stretching; ``rdz`` is the coordinate's 1/dz."""
+    dx, dy, rdz = _positive("dx", dx), _positive("dy", dy), _positive("rdz", rdz)
+    a, s, lib = _prepare(arrays, STRAIN_ARRAY_NAMES, ni, nj, nk, "flat-strain")
+    return _launch(a, lib.gm1b_flat_strain, (ni, nj, nk, ctypes.byref(s), dx, dy, rdz), "gm1b_flat_strain",
+                   {"stream": stream, "receipt": {"operator": "flat-strain", "cell_words": ni * nj * nk}})
+
+
+def launch_cuda_flat_gettau(arrays: Mapping[str, Any], *, ni: int, nj: int, nk: int,
+                            stream: Any | None = None) -> CudaLaunch:
+    """gettau with the free-slip lower and upper faces (enqueue_flat_gettau)."""
+    a, s, lib = _prepare(arrays, GETTAU_ARRAY_NAMES, ni, nj, nk, "flat-gettau")
+    return _launch(a, lib.gm1b_flat_gettau, (ni, nj, nk, ctypes.byref(s)), "gm1b_flat_gettau",
+                   {"stream": stream, "receipt": {"operator": "flat-gettau",
+                                                  "stress_words": nk * (3 * ni * nj + (ni + 1) * (nj + 1)) +
+                                                  (nk + 1) * ((ni + 1) * nj + ni * (nj + 1))}})
+
+
+def launch_cuda_flat_momentum_stress(arrays: Mapping[str, Any], *, ni: int, nj: int, nk: int, dx: float, dy: float,
+                                     rdz: float, dt: float, two_part: Any = None,
+                                     stream: Any | None = None) -> CudaLaunch:
+    """turbu, turbv and turbw with their implicit vertical solves added into
+    uten, vten and wten (enqueue_flat_momentum_stress).  The two-part
+    (sgsmodel 3/4) binding is not built."""
+    if two_part is not None:
+        refuse(code="CM1-SGS-STRESS-TWO-PART", gate="physics-seam", option="two_part", value="bound",
+               reason="the two-part dot2p block of turbuz/turbvz is not built on this path",
+               remedy="run sgsmodel 1 (two_part=None)")
+    dx, dy, rdz, dt = _positive("dx", dx), _positive("dy", dy), _positive("rdz", rdz), _positive("dt", dt)
+    a, s, lib = _prepare(arrays, MOMENTUM_STRESS_ARRAY_NAMES, ni, nj, nk, "flat-momentum-stress")
+    return _launch(a, lib.gm1b_flat_momentum_stress, (ni, nj, nk, ctypes.byref(s), dx, dy, rdz, dt),
+                   "gm1b_flat_momentum_stress",
+                   {"stream": stream, "receipt": {"operator": "flat-momentum-stress",
+                                                  "u_tendency_words": nk * nj * (ni + 1),
+                                                  "v_tendency_words": nk * (nj + 1) * ni,
+                                                  "w_tendency_words": (nk - 1) * nj * ni}})
+
+
+def launch_cuda_flat_sgs_stress(arrays: Mapping[str, Any], *, ni: int, nj: int, nk: int, dx: float, dy: float,
+                                rdz: float, dt: float, stream: Any | None = None) -> CudaLaunch:
+    """The strain carriers, gettau and the momentum stress in that order."""
+    dx, dy, rdz, dt = _positive("dx", dx), _positive("dy", dy), _positive("rdz", rdz), _positive("dt", dt)
+    a, s, lib = _prepare(arrays, SGS_STRESS_ARRAY_NAMES, ni, nj, nk, "flat-sgs-stress")
+    return _launch(a, lib.gm1b_flat_sgs_stress, (ni, nj, nk, ctypes.byref(s), dx, dy, rdz, dt),
+                   "gm1b_flat_sgs_stress", {"stream": stream, "receipt": {"operator": "flat-sgs-stress"}})

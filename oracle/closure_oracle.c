@@ -346,23 +346,16 @@ int oracle_moist_nm(int ni, int nj, int nk, const float* c1, const float* c2, co
  * (cuda_cartesian_closure.py:1130-1131).  mhp is the mh profile (nk+2,
  * CM1-indexed: mhp[k+1] belongs to mass level k); mf is the 3-D face array;
  * rdz the coordinate's reference 1/dz.  Open sides are index clamps. */
-int oracle_flat_calcdef(int ni, int nj, int nk, const float* u, const float* v, const float* w, const float* rho,
-                        const float* rf, const float* mf, const float* c1, const float* c2, const float* mhp,
-                        float dx, float dy, float rdz, float* defv, float* defh) {
+/* the six strain carriers rho*Sij of the flat calcdef (its mass and face
+ * passes): s11/s22/s33 (nk, nj, ni), s12 (nk, nj+1, ni+1) with every corner
+ * written (open sides take the nearest interior corner), s13 (nk+1, nj, ni+1)
+ * and s23 (nk+1, nj+1, ni) on face levels 1..nk-1 (levels 0 and nk left as
+ * they are) */
+int oracle_flat_strain(int ni, int nj, int nk, const float* u, const float* v, const float* w, const float* rho,
+                       const float* rf, const float* mf, const float* mhp, float dx, float dy, float rdz, float* s11,
+                       float* s22, float* s33, float* s12, float* s13, float* s23) {
   if (ni < 3 || nj < 3 || nk < 3) return -1;
   const float rdx = 1.0f / dx, rdy = 1.0f / dy;
-  const int64_t ncell = (int64_t)nk * nj * ni;
-  float* s11 = calloc(ncell, sizeof(float));
-  float* s22 = calloc(ncell, sizeof(float));
-  float* s33 = calloc(ncell, sizeof(float));
-  float* s12 = calloc((int64_t)nk * (nj + 1) * (ni + 1), sizeof(float));
-  float* s13 = calloc((int64_t)(nk + 1) * nj * (ni + 1), sizeof(float));
-  float* s23 = calloc((int64_t)(nk + 1) * (nj + 1) * ni, sizeof(float));
-  if (!s11 || !s22 || !s33 || !s12 || !s13 || !s23) return -2;
-  for (int64_t q = 0; q < (int64_t)(nk + 1) * nj * ni; ++q) {
-    defv[q] = 0.0f;
-    defh[q] = 0.0f;
-  }
   const int ux = ni + 1, vy = nj + 1;
   /* mass pass: s11, s22, s33 at cells, s12 at corners */
   for (int k = 0; k < nk; ++k)
@@ -407,6 +400,27 @@ int oracle_flat_calcdef(int ni, int nj, int nk, const float* u, const float* v, 
           s23[I3(kf, jc, ic, vy, ni)] = ((0.5f * (dw + dv)) * 0.5f) * dens;
         }
       }
+  return 0;
+}
+
+int oracle_flat_calcdef(int ni, int nj, int nk, const float* u, const float* v, const float* w, const float* rho,
+                        const float* rf, const float* mf, const float* c1, const float* c2, const float* mhp,
+                        float dx, float dy, float rdz, float* defv, float* defh) {
+  if (ni < 3 || nj < 3 || nk < 3) return -1;
+  const int64_t ncell = (int64_t)nk * nj * ni;
+  float* s11 = calloc(ncell, sizeof(float));
+  float* s22 = calloc(ncell, sizeof(float));
+  float* s33 = calloc(ncell, sizeof(float));
+  float* s12 = calloc((int64_t)nk * (nj + 1) * (ni + 1), sizeof(float));
+  float* s13 = calloc((int64_t)(nk + 1) * nj * (ni + 1), sizeof(float));
+  float* s23 = calloc((int64_t)(nk + 1) * (nj + 1) * ni, sizeof(float));
+  if (!s11 || !s22 || !s33 || !s12 || !s13 || !s23) return -2;
+  for (int64_t q = 0; q < (int64_t)(nk + 1) * nj * ni; ++q) {
+    defv[q] = 0.0f;
+    defh[q] = 0.0f;
+  }
+  const int ux = ni + 1, vy = nj + 1;
+  oracle_flat_strain(ni, nj, nk, u, v, w, rho, rf, mf, mhp, dx, dy, rdz, s11, s22, s33, s12, s13, s23);
   /* reduction (the pass both branches share) */
   for (int kf = 1; kf < nk; ++kf)
     for (int j = 0; j < nj; ++j)

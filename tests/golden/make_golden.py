@@ -17,6 +17,7 @@ Reference entry points used (their CPU twins, single-threaded NumPy):
   cpu_sound3_periodic_three_stage_inplace  src/cm1core/cuda_sound3_periodic.py:1071
   cpu_psolver3_trajectory_inplace          src/cm1core/cuda_psolver3_trajectory.py:761
   cpu_initial_dry_mass, cpu_apmasscon_inplace  src/cm1core/cuda_apmasscon.py:226, :256
+  cpu_sgs_stress_tendency_inplace          src/cm1core/cuda_sgs_stress_tendency.py:292
   (and the others named by each make_* function)
 """
 
@@ -1225,10 +1226,71 @@ def make_warm_rain(reference: Path) -> None:
         print("wrote", tag)
 
 
+# (ni, nj, nk, seed, level_uniform): level_uniform cases hold kmh/kmv
+# constant on each level and s12's edge corners equal to the nearest
+# interior corner (the flat calcdef's own edge rule), so the flat column's
+# gettau/turbu texts and this terrain twin form the same sums
+STRESS_CASES = {"stress_7x6x5": (7, 6, 5, 61, False), "stress_9x8x7": (9, 8, 7, 62, True)}
+
+
+def stress_fixture(ni: int, nj: int, nk: int, seed: int, level_uniform: bool = False) -> dict[str, np.ndarray]:
+    """Seeded inputs of the SGS stress: strains and eddy coefficients of
+    both signs and magnitudes, positive densities and column metrics, flat
+    terrain (gz = rgz = 1, zero slopes)."""
+    from oracle.stress import stress_shapes
+
+    rng = np.random.default_rng(seed)
+    sh = stress_shapes(ni, nj, nk)
+    f = np.float32
+    a = {}
+    for n in ("s11", "s22", "s33", "s12", "s13", "s23", "u3d", "v3d", "w3d"):
+        a[n] = rng.normal(0.0, 0.3, sh[n]).astype(f)
+    for n in ("kmh", "kmv"):
+        a[n] = rng.uniform(0.5, 40.0, sh[n]).astype(f)
+        if level_uniform:
+            a[n][:] = a[n][:, :1, :1]
+    if level_uniform:
+        jj = np.clip(np.arange(nj + 1), 1, nj - 1)
+        ii = np.clip(np.arange(ni + 1), 1, ni - 1)
+        a["s12"] = np.ascontiguousarray(a["s12"][:, jj][:, :, ii])
+    a["rho"] = rng.uniform(0.4, 1.2, sh["rho"]).astype(f)
+    a["rf"] = rng.uniform(0.4, 1.2, sh["rf"]).astype(f)
+    a["mh"] = rng.uniform(0.7, 1.4, sh["mh"]).astype(f)
+    a["mf"] = rng.uniform(0.7, 1.4, sh["mf"]).astype(f)
+    for n, s in (("gz", (nj, ni)), ("rgz", (nj, ni)), ("gzu", (nj, ni + 1)), ("rgzu", (nj, ni + 1)),
+                 ("gzv", (nj + 1, ni)), ("rgzv", (nj + 1, ni))):
+        a[n] = np.ones(s, f)
+    a["gxu"] = np.zeros((nk + 1, nj, ni + 1), f)
+    a["gyv"] = np.zeros((nk + 1, nj + 1, ni), f)
+    for n in ("t11", "t22", "t33", "t12", "t13", "t23"):
+        a[n] = np.zeros(sh[n], f)
+    for n in ("uten", "vten", "wten"):
+        a[n] = rng.normal(0.0, 1.0e-3, sh[n]).astype(f)
+    return a
+
+
+def make_stress(reference: Path) -> None:
+    """gettau and turbu/turbv/turbw through the reference's CPU twin
+    cpu_sgs_stress_tendency_inplace (src/cm1core/cuda_sgs_stress_tendency.py:292)
+    on seeded strains and coefficients, square 100 m grid, flat terrain."""
+    sys.path.insert(0, str(reference / "src"))
+    from cm1core.cuda_sgs_stress_tendency import cpu_sgs_stress_tendency_inplace
+
+    for tag, (ni, nj, nk, seed, level_uniform) in STRESS_CASES.items():
+        a = stress_fixture(ni, nj, nk, seed, level_uniform)
+        inputs = {f"in_{k}": v.copy() for k, v in a.items()}
+        cpu_sgs_stress_tendency_inplace(a, ni=ni, nj=nj, nk=nk, dx=100.0, dy=100.0, dz=50.0, dt=0.6)
+        outputs = {f"out_{k}": a[k].copy() for k in ("t11", "t22", "t33", "t12", "t13", "t23", "uten", "vten",
+                                                     "wten")}
+        meta = dict(ni=ni, nj=nj, nk=nk, dx=100.0, dy=100.0, dz=50.0, dt=0.6, level_uniform=level_uniform)
+        np.savez_compressed(HERE / f"{tag}.npz", meta=json.dumps(meta), **inputs, **outputs)
+        print("wrote", tag)
+
+
 def main() -> None:
     p = argparse.ArgumentParser()
     p.add_argument("--reference", type=Path, required=True, help="root of the reference source tree")
-    p.add_argument("what", choices=("small", "c1", "advection", "kessler", "tke", "rk", "bridge", "wk", "limits", "closure", "tkeevo", "momentum", "terrainopen", "kesslerstep", "fills", "vertical", "warmrain", "apmasscon"))
+    p.add_argument("what", choices=("small", "c1", "advection", "kessler", "tke", "rk", "bridge", "wk", "limits", "closure", "tkeevo", "momentum", "terrainopen", "kesslerstep", "fills", "vertical", "warmrain", "apmasscon", "stress"))
     p.add_argument("--checkpoints", type=int, nargs="+", default=[1])
     args = p.parse_args()
     if args.what == "small":
@@ -1265,6 +1327,8 @@ def main() -> None:
         make_vertical(args.reference)
     elif args.what == "apmasscon":
         make_apmasscon(args.reference)
+    elif args.what == "stress":
+        make_stress(args.reference)
     else:
         make_c1(args.reference, sorted(set(args.checkpoints)))
 
