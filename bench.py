@@ -449,6 +449,44 @@ def run_moist(args) -> None:
     ms_per_step = total_ms / args.steps
     value = world * cells * args.steps / (total_ms * 1e-3)
 
+    # ---- the same step with the closure's held tendencies on (SGS stress,
+    # scalar diffusion and upper Rayleigh damping once per step): a second
+    # handle on the same state, captured and timed the same way (stretched
+    # columns only) --------------------------------------------------------
+    stress_step = None
+    if cfg.stretched:
+        import dataclasses
+
+        scfg = dataclasses.replace(cfg, sgs_diffusion=True, rayleigh=True, dissipative_heating=True)
+        with torch.cuda.stream(stream):
+            smodel = NativeMoistLargeStep(scfg, dev_state, dev_metrics, stream=stream)
+            smodel.step()
+            stream.synchronize()
+            sgraph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(sgraph, stream=stream):
+                smodel.step()
+            for _ in range(2):
+                sgraph.replay()
+        s_start = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        s_end = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        barrier()
+        with torch.cuda.stream(stream):
+            for q in range(args.steps):
+                flush.zero_()
+                s_start[q].record(stream)
+                sgraph.replay()
+                s_end[q].record(stream)
+        barrier()
+        s_ms = max_over_ranks(sum(s.elapsed_time(e) for s, e in zip(s_start, s_end))) / args.steps
+        smodel.check()
+        del sgraph
+        smodel.close()
+        stress_step = {"ms_per_step": s_ms, "value": world * cells / (s_ms * 1e-3), "unit": UNIT,
+                       "note": "the same step with the closure's held tendencies on (MoistStepConfig.sgs_diffusion "
+                               ", .rayleigh and .dissipative_heating: strain, gettau, turbu/turbv/turbw and turbs of "
+                               "theta and qv/qc/qr once per step, the upper Rayleigh damping above 15 km, the "
+                               "dissipative heating; added in every RK stage)"}
+
     # ---- per-kernel device time (eager steps, launch profiler on) -------
     # run operation by operation on one stream: the profiler's event pairs
     # time each launch alone only when launches do not overlap
@@ -546,6 +584,8 @@ def run_moist(args) -> None:
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d},
         "clocks": clocks,
     }
+    if stress_step is not None:
+        line["with_held_closure"] = stress_step
     print(json.dumps(line), flush=True)
 
 

@@ -63,6 +63,8 @@ struct gm1b_moist_step {
     void *kessler_ws = nullptr;
     size_t kessler_ws_bytes = 0;
     void *mass_ws = nullptr;  // the dry-mass correction's level sums
+    float *stress_buf = nullptr;     // the SGS stress scratch (strains, stresses, held tendencies)
+    gm1b_flat_stress_arrays stress{};
     int32_t *status_acc = nullptr;  // 8 words
     float *courant = nullptr;       // 1 word
     uint32_t *courant_keys = nullptr;
@@ -223,8 +225,30 @@ int closure(Step &h, cudaStream_t st) {
     TRY(gm1b_sgs_tke(c.ni, c.nj, c.nk, &g, c.dx, c.dy, c.dz, st));
     TRY(copy(s.tke3d, s.tkea, Sizes(c).face * sizeof(float), st, "tke3d <- tkea"));
     gm1b_tke_evolution_arrays t = tke_arrays(h);
-    if (c.stretched) return gm1b_tke_diffusion_flat(c.ni, c.nj, c.nk, &t, c.dx, c.dy, h.rdz, c.dt, st);
-    return gm1b_tke_diffusion(c.ni, c.nj, c.nk, &t, c.dx, c.dy, c.dz, c.dt, st);
+    if (!c.stretched) return gm1b_tke_diffusion(c.ni, c.nj, c.nk, &t, c.dx, c.dy, c.dz, c.dt, st);
+    TRY(gm1b_tke_diffusion_flat(c.ni, c.nj, c.nk, &t, c.dx, c.dy, h.rdz, c.dt, st));
+    if (!c.sgs_diffusion && !c.rayleigh) return GM1B_OK;
+    // the held momentum tendencies: zeroed, then the SGS stress added (the
+    // Rayleigh damping joins them in the held phase)
+    const Sizes z(c);
+    TRY(zero(h.stress.uten, (size_t)c.nk * c.nj * (c.ni + 1) * sizeof(float), st, "zero held u"));
+    TRY(zero(h.stress.vten, (size_t)c.nk * (c.nj + 1) * c.ni * sizeof(float), st, "zero held v"));
+    TRY(zero(h.stress.wten, z.face * sizeof(float), st, "zero held w"));
+    if (!c.sgs_diffusion) return GM1B_OK;
+    return gm1b_flat_sgs_stress(c.ni, c.nj, c.nk, &h.stress, c.dx, c.dy, h.rdz, c.dt, st);
+}
+
+// the held momentum into the physical cells of the zeroed stage tendencies
+// (pack_cartesian_held_momentum, cuda_cartesian_dynamics.py:206)
+int seed_held_momentum(Step &h, cudaStream_t st) {
+    const gm1b_moist_state &s = h.s;
+    const int ni = h.c.ni, nj = h.c.nj, nk = h.c.nk;
+    const size_t uy = ni + 7, uz = (size_t)(nj + 6) * uy;
+    const size_t vy = ni + 6, vz = (size_t)(nj + 7) * vy;
+    const size_t wy = ni + 6, wz = (size_t)(nj + 6) * wy;
+    TRY(box_copy(s.uten + uz + 3 * uy + 3, uy, uz, h.stress.uten, ni + 1, (size_t)nj * (ni + 1), ni + 1, nj, nk, st));
+    TRY(box_copy(s.vten + vz + 3 * vy + 3, vy, vz, h.stress.vten, ni, (size_t)(nj + 1) * ni, ni, nj + 1, nk, st));
+    return box_copy(s.wten + wz + 3 * wy + 3, wy, wz, h.stress.wten, ni, (size_t)nj * ni, ni, nj, nk + 1, st);
 }
 
 int held_tendencies(Step &h, cudaStream_t st) {
@@ -233,6 +257,27 @@ int held_tendencies(Step &h, cudaStream_t st) {
     const Sizes z(c);
     TRY(zero(s.thheld, z.mass * sizeof(float), st, "zero thheld"));
     TRY(zero(s.qheld, kNumq * z.mass * sizeof(float), st, "zero qheld"));
+    if (c.rayleigh) {
+        // the damping added into the held momentum (uten1 + uten) and
+        // assigned to the held theta before the scalar diffusion adds to it
+        const gm1b_moist_metrics &m = h.m;
+        const gm1b_rayleigh_held_arrays ra{m.tauh, m.taus, m.tauf, m.u0, m.v0, s.uc, s.vc, s.wc, s.tha,
+                                           h.stress.uten, h.stress.vten, h.stress.wten, s.thheld};
+        TRY(gm1b_rayleigh_held(c.ni, c.nj, c.nk, &ra, 1, 1, c.rdalpha, st));
+    }
+    if (c.dissipative_heating) {
+        // idiss after the damping and before the subgrid turbulence
+        // (solve1.F:917-975)
+        const gm1b_dissipative_heating_arrays da{s.dissten, s.pi0, s.pp3d_c, s.qa, s.thheld};
+        TRY(gm1b_dissipative_heating(c.ni, c.nj, c.nk, &da, st));
+    }
+    if (c.sgs_diffusion) {
+        // turbs for theta and the moisture rows into the held thten1/qten the
+        // eqtset 2 composition then reads (solve1.F:1169-1233)
+        const gm1b_flat_scalar_turbulence_arrays ta{s.th0, s.tha, s.qa, s.rho, s.rr, s.rf, h.m.mh, h.m.mf,
+                                                    s.khh, s.khv, s.thheld, s.qheld};
+        TRY(gm1b_flat_scalar_turbulence(c.ni, c.nj, c.nk, kNumq, &ta, c.dx, c.dy, c.dz, c.dt, st));
+    }
     gm1b_held_arrays a{s.th0_3d, s.pi0_3d, s.rho, s.pp3d_c, s.tha, s.qa, s.qpten, s.qtten, s.qvten, s.qcten,
                        s.thheld, s.qheld, s.ppten};
     return gm1b_held_compose(c.ni, c.nj, c.nk, &a, c.dt, st);
@@ -281,6 +326,7 @@ int pre_acoustic(Step &h, int nrk, cudaStream_t st) {
     TRY(zero(s.uten, z.u * sizeof(float), st, "zero uten"));
     TRY(zero(s.vten, z.v * sizeof(float), st, "zero vten"));
     TRY(zero(s.wten, z.w * sizeof(float), st, "zero wten"));
+    if (c.sgs_diffusion || c.rayleigh) TRY(seed_held_momentum(h, st));
     gm1b_momentum5_arrays a = momentum_arrays(h);
     if (c.stretched) {
         // solve2.F:484-487 (bcwsfc, bc2d of w(1)) and :575 (bcw(rrw,0)) are
@@ -535,7 +581,7 @@ void release(Step *h) {
     for (auto &e : h->ev)
         if (e) cudaEventDestroy(e);
     void *bufs[] = {h->kessler_ws, h->status_acc, h->courant, h->courant_keys, h->ones_i, h->ones_j, h->mh_col,
-                    h->mass_ws};
+                    h->mass_ws, h->stress_buf};
     for (void *b : bufs)
         if (b) cudaFree(b);
     delete h;
@@ -573,13 +619,28 @@ extern "C" int32_t gm1b_moist_step_create(const gm1b_moist_step_config *config, 
             return GM1B_ERR_ARGUMENT;
         }
     const void *const *mp = reinterpret_cast<const void *const *>(metrics);
-    const size_t required = c.stretched ? sizeof(gm1b_moist_metrics) / sizeof(void *) : 25;
+    const size_t all = sizeof(gm1b_moist_metrics) / sizeof(void *);
+    const size_t required = c.stretched ? (c.rayleigh ? all : all - 5) : 25;
     for (size_t q = 0; q < required; ++q)
         if (mp[q] == nullptr) {
             gm1b_set_error("gm1b_moist_step_create: metric #%zu is NULL%s", q,
-                           q >= 25 ? " (a stretched column needs mh_profile, mf_profile and rho0_padded)" : "");
+                           q >= 28   ? " (the Rayleigh damping needs u0, v0, tauh, taus and tauf)"
+                           : q >= 25 ? " (a stretched column needs mh_profile, mf_profile and rho0_padded)"
+                                     : "");
             return GM1B_ERR_ARGUMENT;
         }
+    if (c.rayleigh && (!c.stretched || !(c.rdalpha >= 0.0f) || !isfinite(c.rdalpha))) {
+        gm1b_set_error("gm1b_moist_step_create: the Rayleigh damping needs a stretched column and a finite rdalpha >= 0");
+        return GM1B_ERR_ARGUMENT;
+    }
+    if (c.sgs_diffusion && !c.stretched) {
+        gm1b_set_error("gm1b_moist_step_create: the SGS diffusion is built for a stretched column's flat operator family");
+        return GM1B_ERR_ARGUMENT;
+    }
+    if (c.sgs_diffusion && c.nk > 200) {
+        gm1b_set_error("gm1b_moist_step_create: the SGS diffusion's column solves take nk <= 200");
+        return GM1B_ERR_ARGUMENT;
+    }
     Step *h = new Step;
     h->c = c;
     h->s = *state;
@@ -602,6 +663,42 @@ extern "C" int32_t gm1b_moist_step_create(const gm1b_moist_step_config *config, 
     if (good) good = ok(cudaMalloc(&h->mh_col, (size_t)c.nk * sizeof(float)), "cudaMalloc");
     if (good && c.apmasscon)
         good = ok(cudaMalloc(&h->mass_ws, gm1b_apmasscon_workspace_bytes(c.nk)), "cudaMalloc (mass workspace)");
+    if (good && (c.sgs_diffusion || c.rayleigh)) {
+        // strains and stresses, then the held u, v, w (the layouts of
+        // gm1b_flat_stress_arrays), carved from one allocation
+        const size_t ni = c.ni, nj = c.nj, nk = c.nk;
+        const size_t cell = nk * nj * ni, corner = nk * (nj + 1) * (ni + 1), s13 = (nk + 1) * nj * (ni + 1),
+                     s23 = (nk + 1) * (nj + 1) * ni, heldu = nk * nj * (ni + 1), heldv = nk * (nj + 1) * ni,
+                     heldw = (nk + 1) * nj * ni;
+        const size_t words[15] = {cell, cell, cell, corner, s13, s23, cell, cell, cell, corner, s13, s23,
+                                  heldu, heldv, heldw};
+        size_t total = 0;
+        for (size_t w : words) total += (w + 31) / 32 * 32;  // 128-byte aligned pieces
+        good = ok(cudaMalloc(&h->stress_buf, total * sizeof(float)), "cudaMalloc (SGS stress scratch)") &&
+               ok(cudaMemset(h->stress_buf, 0, total * sizeof(float)), "SGS stress scratch");
+        if (good) {
+            float *piece[15];
+            float *p = h->stress_buf;
+            for (int q = 0; q < 15; ++q) {
+                piece[q] = p;
+                p += (words[q] + 31) / 32 * 32;
+            }
+            gm1b_flat_stress_arrays &a = h->stress;
+            a.u3d = state->uc;
+            a.v3d = state->vc;
+            a.w3d = state->wc;
+            a.rho = state->rho;
+            a.rf = state->rf;
+            a.mh = metrics->mh;
+            a.mf = metrics->mf;
+            a.mh_profile = metrics->mh_profile;
+            a.kmh = state->kmh;
+            a.kmv = state->kmv;
+            float **dst[15] = {&a.s11, &a.s22, &a.s33, &a.s12, &a.s13, &a.s23, &a.t11, &a.t22,
+                               &a.t33, &a.t12, &a.t13, &a.t23, &a.uten, &a.vten, &a.wten};
+            for (int q = 0; q < 15; ++q) *dst[q] = piece[q];
+        }
+    }
     if (good) {
         // uh = vh = 1 (uniform horizontal grid) and the mh column (the first
         // column of the 3-D mh), the Courant reduction's metric inputs

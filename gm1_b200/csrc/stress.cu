@@ -19,6 +19,17 @@
 // (--fmad=false; the literal zero factors of vibeta = 0 are formed, so signed
 // zeros are what the reference's are).  Open sides are index clamps.
 //
+//   turbs for theta and the moisture rows (the flat fluxes and turbsz, the
+//   open-halo pad/pack copies as index clamps; no surface flux)
+//       src/cm1core/cuda_gm1_scalar_turbulence.py:453-466 (pad, pack)
+//       src/cm1core/cuda_gm1_flat_stretched_closure.py:335-381 (flux, apply)
+//       src/cm1core/cuda_cartesian_closure.py:1566-1633 (the per-scalar loop)
+//       (turbtend.F:60-434, :442-692; solve1.F:1169-1233)
+//   the dissipative heating, idiss = 1
+//       src/cm1core/eqtset2_energy_terms.py:176-215, :375-470 (solve1.F:744-848, :917-975)
+//   the upper Rayleigh damping held tendencies, irdamp = 1
+//       src/cm1core/cuda_rayleigh_held.py:213-254, :419-488 (solve1.F:412-454)
+//
 // Design: the strain and gettau passes are grid-stride elementwise kernels
 // over the union of their index spaces (one launch each).  The three column
 // solves run one thread per staggered column, 32 x 4 columns per CTA with
@@ -327,6 +338,191 @@ __global__ void __launch_bounds__(kCT) flat_turbw_kernel(StressArgs a) {
 #undef PF
 }
 
+
+// ---------------------------------------------------------- turbs (flat)
+// theta ((th0 - 300) + tha) and numq moisture rows; blockIdx.z picks the
+// scalar (0 theta, 1.. the rows).  The open-halo copies of the reference's
+// pad/pack texts are index clamps here, so no halo array is written; the x
+// and y face fluxes of each level are formed where the back substitution
+// needs them.
+struct TurbsArgs {
+    const float *th0, *tha, *qa, *rho, *rr, *rf, *mh, *mf, *khh, *khv;
+    float *thten, *qten;
+    int ni, nj, nk;
+    float dx, dy, dz, dt;
+};
+
+__device__ __forceinline__ float tcell(const TurbsArgs &a, const float *p, int k, int j, int i) {
+    return p[o3(k, clampi(j, a.nj), clampi(i, a.ni), a.nj, a.ni)];
+}
+// the open-halo scalar at a clamped cell; q == nullptr: theta
+__device__ __forceinline__ float sval(const TurbsArgs &a, const float *q, int k, int j, int i) {
+    const unsigned p = o3(k, clampi(j, a.nj), clampi(i, a.ni), a.nj, a.ni);
+    if (q != nullptr) return q[p];
+    return (a.th0[k] - 300.0f) + a.tha[p];
+}
+// x flux through the face between cells f-1 and f
+__device__ __forceinline__ float turbs_fx(const TurbsArgs &a, const float *q, int k, int j, int f, float rx) {
+    const float den = tcell(a, a.rho, k, j, f) + tcell(a, a.rho, k, j, f - 1);
+    const float kh = (tcell(a, a.khh, k, j, f) + tcell(a, a.khh, k, j, f - 1)) +
+                     (tcell(a, a.khh, k + 1, j, f) + tcell(a, a.khh, k + 1, j, f - 1));
+    return (((-0.125f * den) * kh) * (sval(a, q, k, j, f) - sval(a, q, k, j, f - 1))) * rx;
+}
+// y flux through the face between rows f-1 and f
+__device__ __forceinline__ float turbs_fy(const TurbsArgs &a, const float *q, int k, int f, int i, float ry) {
+    const float den = tcell(a, a.rho, k, f, i) + tcell(a, a.rho, k, f - 1, i);
+    const float kh = (tcell(a, a.khh, k, f, i) + tcell(a, a.khh, k, f - 1, i)) +
+                     (tcell(a, a.khh, k + 1, f, i) + tcell(a, a.khh, k + 1, f - 1, i));
+    return (((-0.125f * den) * kh) * (sval(a, q, k, f, i) - sval(a, q, k, f - 1, i))) * ry;
+}
+
+__global__ void __launch_bounds__(kCT) flat_turbs_kernel(TurbsArgs a) {
+    extern __shared__ float s_col[];
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kCX + tx;
+    const int ni = a.ni, nj = a.nj, nk = a.nk;
+    const int i = blockIdx.x * kCX + tx, j = blockIdx.y * kCY + ty;
+    if (i >= ni || j >= nj) return;
+    const size_t n = (size_t)ni * nj * nk;
+    const int sp = (int)blockIdx.z;
+    const float *q = sp == 0 ? nullptr : a.qa + (size_t)(sp - 1) * n;
+    float *target = sp == 0 ? a.thten : a.qten + (size_t)(sp - 1) * n;
+    const unsigned col = (unsigned)j * ni + i, lev = (unsigned)nj * ni;
+    float *cp = s_col, *dp = s_col + (size_t)nk * kCT;
+#define CP(k) cp[(unsigned)(k) * kCT + tid]
+#define DP(k) dp[(unsigned)(k) * kCT + tid]
+#define PF(p, k) p[(unsigned)(k) * lev + col]
+#define SC(k) sval(a, q, k, j, i)
+#define COEF(F, K) ((((PF(a.khv, F) * PF(a.mf, F)) * PF(a.rf, F)) * PF(a.mh, K)) * PF(a.rr, K))
+    const float rx = 1.0f / a.dx, ry = 1.0f / a.dy, rz = 1.0f / a.dz, dt = a.dt, rdt = 1.0f / dt;
+    const float tema = (((-1.0f * dt) * 1.0f) * rz) * rz;
+    const float temb = ((dt * 0.0f) * rz) * rz;
+    const float temc = dt * rz;
+    float sm = SC(0), sk = SC(1);  // scalar at k-1 and k of the next level
+    float r2 = COEF(1, 0);
+    float cfc = tema * r2, cfb = 1.0f - cfc;
+    float ex = (-r2) * sm + r2 * sk;
+    float bc = ((temc * 0.0f) * PF(a.mh, 0)) * PF(a.rr, 0);
+    float cfd = (sm + temb * ex) + bc;
+    float tem = 1.0f / cfb;
+    float cprev = (-cfc) * tem, dprev = cfd * tem;
+    CP(0) = cprev;
+    DP(0) = dprev;
+    for (int k = 1; k + 1 < nk; ++k) {
+        const float r1 = COEF(k, k);
+        r2 = COEF(k + 1, k);
+        const float cfa = tema * r1;
+        cfc = tema * r2;
+        cfb = (1.0f - cfa) - cfc;
+        const float sp1 = SC(k + 1);
+        ex = (r1 * sm - (r1 + r2) * sk) + r2 * sp1;
+        cfd = sk + temb * ex;
+        tem = 1.0f / (cfa * cprev + cfb);
+        cprev = (-cfc) * tem;
+        dprev = (cfd - cfa * dprev) * tem;
+        CP(k) = cprev;
+        DP(k) = dprev;
+        sm = sk;
+        sk = sp1;
+    }
+    float sol;
+    {
+        const int k = nk - 1;
+        const float r1 = COEF(k, k), cfa = tema * r1;
+        cfb = 1.0f - cfa;
+        ex = r1 * sm - r1 * sk;
+        bc = ((temc * 0.0f) * PF(a.mh, k)) * PF(a.rr, k);
+        cfd = (sk + temb * ex) - bc;
+        tem = 1.0f / (cfa * cprev + cfb);
+        sol = (cfd - cfa * dprev) * tem;
+    }
+    for (int k = nk - 1; k >= 0; --k) {
+        if (k != nk - 1) sol = CP(k) * sol + DP(k);
+        const float tz = (PF(a.rho, k) * (sol - SC(k))) * rdt;
+        float tx = -((turbs_fx(a, q, k, j, i + 1, rx) - turbs_fx(a, q, k, j, i, rx)) * rx);
+        if (i == 0 || i + 1 == ni) tx = 0.0f;
+        float ty = -((turbs_fy(a, q, k, j + 1, i, ry) - turbs_fy(a, q, k, j, i, ry)) * ry);
+        if (j == 0 || j + 1 == nj) ty = 0.0f;
+        const unsigned p = (unsigned)k * lev + col;
+        target[p] = target[p] + ((tx + ty) + tz) * PF(a.rr, k);
+    }
+#undef CP
+#undef DP
+#undef PF
+#undef SC
+#undef COEF
+}
+
+
+// ------------------------------------------------------ Rayleigh (upper)
+// irdamp = 1: uten1 = ((-rdalpha*0.5)*(tauh(i-1)+tauh(i)))*(ua - u0(k)), vten1
+// across j, wten1 = (-rdalpha*tauf)*wa, thten1 = (-rdalpha*taus)*tha.  tau
+// as one-halo 3-D arrays (the reference's layout) or as column profiles;
+// add_momentum adds the damping into the momentum outputs (the closure's
+// held sum uten1 + uten) and assigns thten1.
+struct RayArgs {
+    const float *tauh, *taus, *tauf, *u0, *v0, *ua, *va, *wa, *tha;
+    float *uten1, *vten1, *wten1, *thten1;
+    int ni, nj, nk;
+    float rdalpha;
+    int profiles, add_momentum;
+};
+
+__device__ __forceinline__ float tau_at(const RayArgs &a, const float *tau, int k, int jh, int ih) {
+    return a.profiles ? tau[k] : tau[((size_t)k * (a.nj + 2) + jh) * (size_t)(a.ni + 2) + ih];
+}
+
+__global__ void __launch_bounds__(kEW) rayleigh_held_kernel(RayArgs a) {
+    const int ni = a.ni, nj = a.nj, nk = a.nk;
+    const size_t first = (size_t)blockIdx.x * blockDim.x + threadIdx.x, step = (size_t)gridDim.x * blockDim.x;
+    const size_t nu = (size_t)nk * nj * (ni + 1), nv = (size_t)nk * (nj + 1) * ni, ns = (size_t)nk * nj * ni;
+    const float neg = -a.rdalpha, negh = neg * 0.5f;
+    for (size_t z = first; z < nu; z += step) {
+        const int f = (int)(z % (ni + 1)), j = (int)((z / (ni + 1)) % nj), k = (int)(z / ((size_t)(ni + 1) * nj));
+        const float pair = tau_at(a, a.tauh, k, j + 1, f) + tau_at(a, a.tauh, k, j + 1, f + 1);
+        const float d = (negh * pair) * (a.ua[z] - a.u0[k]);
+        a.uten1[z] = a.add_momentum ? d + a.uten1[z] : d;
+    }
+    for (size_t z = first; z < nv; z += step) {
+        const int i = (int)(z % ni), f = (int)((z / ni) % (nj + 1)), k = (int)(z / ((size_t)ni * (nj + 1)));
+        const float pair = tau_at(a, a.tauh, k, f, i + 1) + tau_at(a, a.tauh, k, f + 1, i + 1);
+        const float d = (negh * pair) * (a.va[z] - a.v0[k]);
+        a.vten1[z] = a.add_momentum ? d + a.vten1[z] : d;
+    }
+    for (size_t z = first; z < ns; z += step) {
+        const int i = (int)(z % ni), j = (int)((z / ni) % nj), k = (int)(z / ((size_t)ni * nj));
+        const float dw = (neg * tau_at(a, a.tauf, k, j + 1, i + 1)) * a.wa[z];
+        a.wten1[z] = a.add_momentum ? dw + a.wten1[z] : dw;
+        a.thten1[z] = (neg * tau_at(a, a.taus, k, j + 1, i + 1)) * a.tha[z];
+    }
+}
+
+
+// ---------------------------------------------------- dissipative heating
+// idiss = 1: thten1 += (0.5*(dissten(k)+dissten(k+1))) /
+// ((cpdcv*cvm)*(pi0+ppi)), cvm = ((cv + cvv*qv) + cpl*ql) + cpi*qice.
+struct DissArgs {
+    const float *dissten, *pi0, *ppi, *qa;
+    float *thten1;
+    int ni, nj, nk;
+};
+
+__global__ void __launch_bounds__(kEW) dissipative_heating_kernel(DissArgs a) {
+    const float rd = 287.04f, cp = 1005.7f, cpv = 1870.0f, rv = 461.5f, cpl = 4190.0f, cpi = 2106.0f;
+    const float cv = cp - rd, cvv = cpv - rv, cpdcv = cp / cv;
+    const size_t plane = (size_t)a.ni * a.nj, n = plane * a.nk;
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+        const int k = (int)(q / plane);
+        const float ql = a.qa[n + q] + a.qa[2 * n + q];
+        const float qice = (a.qa[3 * n + q] + a.qa[4 * n + q]) + a.qa[5 * n + q];
+        float cvm = cv + cvv * a.qa[q];
+        cvm = cvm + cpl * ql;
+        cvm = cvm + cpi * qice;
+        const float epsd = 0.5f * (a.dissten[q] + a.dissten[q + plane]);
+        const float den = (cpdcv * cvm) * (a.pi0[k] + a.ppi[q]);
+        a.thten1[q] = a.thten1[q] + epsd / den;
+    }
+}
+
 // ------------------------------------------------------------------ host
 int stress_args(int32_t ni, int32_t nj, int32_t nk, const gm1b_flat_stress_arrays *s, float dx, float dy, float rdz,
                 float dt, bool need_dt, StressArgs &a, const char *what) {
@@ -490,4 +686,89 @@ extern "C" int32_t gm1b_flat_sgs_stress(int32_t ni, int32_t nj, int32_t nk, cons
     TRY(gm1b_flat_strain(ni, nj, nk, arrays, dx, dy, rdz, stream));
     TRY(gm1b_flat_gettau(ni, nj, nk, arrays, stream));
     return gm1b_flat_momentum_stress(ni, nj, nk, arrays, dx, dy, rdz, dt, stream);
+}
+
+extern "C" int32_t gm1b_flat_scalar_turbulence(int32_t ni, int32_t nj, int32_t nk, int32_t numq,
+                                               const gm1b_flat_scalar_turbulence_arrays *arrays, float dx, float dy,
+                                               float dz, float dt, void *stream) {
+    const gm1b_flat_scalar_turbulence_arrays *s = arrays;
+    if (s == nullptr || ni < 3 || nj < 3 || nk < 3 || numq < 0 || numq > 6) {
+        gm1b_set_error("gm1b_flat_scalar_turbulence: need arrays, ni >= 3, nj >= 3, nk >= 3, numq in 0..6");
+        return GM1B_ERR_ARGUMENT;
+    }
+    if ((double)(nk + 1) * nj * ni * 7 >= 4294967296.0 || (double)(nk + 1) * nj * ni >= 2147483648.0) {
+        gm1b_set_error("gm1b_flat_scalar_turbulence: a %dx%dx%d grid is too large for 32-bit offsets", ni, nj, nk);
+        return GM1B_ERR_ARGUMENT;
+    }
+    if (!(dx > 0.0f && dy > 0.0f && dz > 0.0f && dt > 0.0f) || !isfinite(dx) || !isfinite(dy) || !isfinite(dz) ||
+        !isfinite(dt)) {
+        gm1b_set_error("gm1b_flat_scalar_turbulence: dx, dy, dz, dt must be finite and > 0");
+        return GM1B_ERR_ARGUMENT;
+    }
+    if (!all_set({s->th0, s->tha, s->rho, s->rr, s->rf, s->mh, s->mf, s->khh, s->khv, s->thten}) ||
+        (numq > 0 && !all_set({s->qa, s->qten}))) {
+        gm1b_set_error("gm1b_flat_scalar_turbulence: a required array is NULL");
+        return GM1B_ERR_ARGUMENT;
+    }
+    const size_t smem = (size_t)2 * nk * kCT * sizeof(float);
+    if (smem > 200 * 1024) {
+        gm1b_set_error("gm1b_flat_scalar_turbulence: nk=%d exceeds the column solve's shared memory (nk <= 200)", nk);
+        return GM1B_ERR_ARGUMENT;
+    }
+    TRY(configure(flat_turbs_kernel, smem, "flat_turbs_kernel"));
+    TurbsArgs a{s->th0, s->tha, s->qa, s->rho, s->rr, s->rf, s->mh, s->mf, s->khh, s->khv, s->thten, s->qten,
+                ni, nj, nk, dx, dy, dz, dt};
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    ProfScope ps("flat_turbs_kernel", st);
+    flat_turbs_kernel<<<dim3((ni + kCX - 1) / kCX, (nj + kCY - 1) / kCY, numq + 1), dim3(kCX, kCY), smem, st>>>(a);
+    ps.stop();
+    return launch_ok("flat_turbs_kernel") ? GM1B_OK : GM1B_ERR_CUDA;
+}
+
+extern "C" int32_t gm1b_rayleigh_held(int32_t ni, int32_t nj, int32_t nk, const gm1b_rayleigh_held_arrays *arrays,
+                                      int32_t profiles, int32_t add_momentum, float rdalpha, void *stream) {
+    const gm1b_rayleigh_held_arrays *s = arrays;
+    if (s == nullptr || ni < 1 || nj < 1 || nk < 1 || (profiles != 0 && profiles != 1) ||
+        (add_momentum != 0 && add_momentum != 1)) {
+        gm1b_set_error("gm1b_rayleigh_held: need arrays, ni, nj, nk >= 1, profiles and add_momentum 0 or 1");
+        return GM1B_ERR_ARGUMENT;
+    }
+    if (!(rdalpha >= 0.0f) || !isfinite(rdalpha)) {
+        gm1b_set_error("gm1b_rayleigh_held: rdalpha must be finite and >= 0");
+        return GM1B_ERR_ARGUMENT;
+    }
+    if (!all_set({s->tauh, s->taus, s->tauf, s->u0, s->v0, s->ua, s->va, s->wa, s->tha, s->uten1, s->vten1, s->wten1,
+                  s->thten1})) {
+        gm1b_set_error("gm1b_rayleigh_held: a required array is NULL");
+        return GM1B_ERR_ARGUMENT;
+    }
+    RayArgs a{s->tauh, s->taus, s->tauf, s->u0,    s->v0,    s->ua,    s->va,    s->wa, s->tha,
+              s->uten1, s->vten1, s->wten1, s->thten1, ni, nj, nk, rdalpha, profiles, add_momentum};
+    const size_t most = (size_t)nk * (nj + 1) * (ni + 1);
+    const size_t want = (most + kEW - 1) / kEW, cap = (size_t)148 * 16;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    ProfScope ps("rayleigh_held_kernel", st);
+    rayleigh_held_kernel<<<(unsigned)(want < cap ? want : cap), kEW, 0, st>>>(a);
+    ps.stop();
+    return launch_ok("rayleigh_held_kernel") ? GM1B_OK : GM1B_ERR_CUDA;
+}
+
+extern "C" int32_t gm1b_dissipative_heating(int32_t ni, int32_t nj, int32_t nk,
+                                            const gm1b_dissipative_heating_arrays *arrays, void *stream) {
+    const gm1b_dissipative_heating_arrays *s = arrays;
+    if (s == nullptr || ni < 1 || nj < 1 || nk < 1) {
+        gm1b_set_error("gm1b_dissipative_heating: need arrays and ni, nj, nk >= 1");
+        return GM1B_ERR_ARGUMENT;
+    }
+    if (!all_set({s->dissten, s->pi0, s->ppi, s->qa, s->thten1})) {
+        gm1b_set_error("gm1b_dissipative_heating: a required array is NULL");
+        return GM1B_ERR_ARGUMENT;
+    }
+    DissArgs a{s->dissten, s->pi0, s->ppi, s->qa, s->thten1, ni, nj, nk};
+    const size_t n = (size_t)ni * nj * nk, want = (n + kEW - 1) / kEW, cap = (size_t)148 * 16;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    ProfScope ps("dissipative_heating_kernel", st);
+    dissipative_heating_kernel<<<(unsigned)(want < cap ? want : cap), kEW, 0, st>>>(a);
+    ps.stop();
+    return launch_ok("dissipative_heating_kernel") ? GM1B_OK : GM1B_ERR_CUDA;
 }

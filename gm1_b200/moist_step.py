@@ -48,6 +48,7 @@ from .advection import launch_cuda_gm1_child_stretched_scalar_advection5, launch
 from .closure import launch_cuda_flat_deformation, launch_cuda_moist_nm, launch_cuda_terrain_deformation
 from .kessler import (Gm1KesslerDriverSelection, Gm1KesslerHeldCarriers, create_cuda_gm1_kessler_large_step_transition,
                       dry_mass)
+from .errors import refuse
 from .limits import CM1_COURANT_STOP, advective_courant_number
 from .moist_bridge import launch_cuda_eqtset2_stage_terms
 from .scalar_rk import (compose_scalar_moist_rk_stage, moisture_weps_f64, scalar_moist_rk_stage_timestep_f32,
@@ -164,6 +165,21 @@ class MoistStepConfig:
     # namelist's): between the pre-physics equation of state and the Kessler
     # driver, against the state's mass1 ledger
     apmasscon: bool = True
+    # the SGS stress and scalar diffusion held tendencies (CM1 gettau and
+    # turbu/turbv/turbw added into the momentum tendencies of every RK
+    # stage; turbs of theta and the moisture rows into the held theta and
+    # moisture tendencies); built for the flat family of a stretched column
+    sgs_diffusion: bool = False
+    # CM1's upper Rayleigh damping, irdamp = 1 (held u, v, w and theta
+    # tendencies toward the base state above rayleigh_zd_m at rate
+    # rayleigh_rdalpha; the supercell namelist's zd and rdalpha); built for
+    # the flat family of a stretched column
+    rayleigh: bool = False
+    # CM1's dissipative heating (idiss = 1, the supercell namelist's): the
+    # TKE closure's dissipation rate heats theta through the held tendency
+    dissipative_heating: bool = False
+    rayleigh_zd_m: float = 15000.0
+    rayleigh_rdalpha: float = 3.3333333333e-3
 
     @property
     def obc(self) -> int:
@@ -238,6 +254,50 @@ METRIC_NAMES = ("terrain_msl", "zh", "zf", "mh", "rmh", "mf", "rmf", "c1", "c2",
                 "rgz", "gzu", "rgzu", "gzv", "rgzv", "dzdx", "dzdy", "gx", "gxu", "gy", "gyv")
 
 
+def _libm_powf():
+    import ctypes
+    import ctypes.util
+
+    lib = ctypes.CDLL(ctypes.util.find_library("m") or "libm.so.6")
+    fn = lib.powf
+    fn.restype, fn.argtypes = ctypes.c_float, [ctypes.c_float, ctypes.c_float]
+    return fn
+
+
+def startup_thermodynamics(pi0_3d, pp3d, th0_3d, th3d, qv, c1, c2):
+    """prs, rho, rr and rf of a start from its pi, theta and qv, in the
+    reference's startup order (cpu_startup_thermodynamics,
+    src/cm1core/cuda_cartesian_startup.py:295-345; CM1 init3d): prs =
+    p00*powf(pi0 + pp3d, cp/rd) with the host C library's powf, rho =
+    prs/((theta*pi)*(rd + max(qv, 0)*rv)), rr = 1/rho, rf from c1/c2 inside
+    and the second-order extrapolation at the two boundary faces; binary32
+    one operation at a time."""
+    f = np.float32
+    rd, rv, p00 = f(287.04), f(461.5), f(100000.0)
+    cpdrd = f(f(1005.7) / rd)
+    pi = (np.asarray(pi0_3d, f) + np.asarray(pp3d, f)).astype(f)
+    powf = _libm_powf()
+    levels, inverse = np.unique(pi, return_inverse=True)
+    pw = np.array([powf(float(x), float(cpdrd)) for x in levels], f)[inverse].reshape(pi.shape)
+    prs = (p00 * pw).astype(f)
+    theta = (np.asarray(th0_3d, f) + np.asarray(th3d, f)).astype(f)
+    gas = (rd + (np.maximum(f(0.0), np.asarray(qv, f)) * rv).astype(f)).astype(f)
+    rho = (prs / ((theta * pi).astype(f) * gas).astype(f)).astype(f)
+    rr = (f(1.0) / rho).astype(f)
+    nk = rho.shape[0]
+    rf = np.zeros((nk + 1,) + rho.shape[1:], f)
+    rf[1:nk] = ((c1[1:nk] * rho[:-1]).astype(f) + (c2[1:nk] * rho[1:]).astype(f)).astype(f)
+    rf[0] = _extrap(rho[0], rho[1], rho[2])
+    rf[nk] = _extrap(rho[nk - 1], rho[nk - 2], rho[nk - 3])
+    return prs, rho, rr, rf
+
+
+def _extrap(a, b, c):
+    f = np.float32
+    s = ((f(1.875) * a).astype(f) + (f(-1.25) * b).astype(f)).astype(f)
+    return (s + (f(0.375) * c).astype(f)).astype(f)
+
+
 def weisman_klemp_initial_state(cfg: MoistStepConfig, *, seed: int = 0, bubble_k: float = 3.0,
                                 noise_k: float = 0.1, bubble_radius_m: tuple[float, float] = (10000.0, 1400.0),
                                 bubble_center_z_m: float = 1400.0, bubble_cloud: float = 0.0,
@@ -280,16 +340,24 @@ def weisman_klemp_initial_state(cfg: MoistStepConfig, *, seed: int = 0, bubble_k
     s["q3d"][0] = s["qv0"][:, None, None]
     s["q3d"][1] = np.where(r < 0.5, bubble_cloud, 0.0).astype(f)
     s["q3d"][2] = np.where(r < 0.5, bubble_rain, 0.0).astype(f)
-    tv = (s["th0_3d"].astype(np.float64) + s["th3d"]) * s["pi0_3d"] * (1.0 + 0.61 * s["q3d"][0])
-    s["rho"][:] = (col.pressure_pa[:, None, None] / (287.04 * tv)).astype(f)
     s["tke3d"][1:nk] = f(1.0e-4)
     for n in ("uh", "vh", "ruf", "rvf", "ruh", "rvh", "ones_mass"):
         s[n][:] = f(1.0)
-    m = flat_metrics(cfg, s["rho"]) if levels is None else stretched_metrics(cfg, levels, s["rho"])
-    rho = s["rho"]
-    s["rr"][:] = (f(1.0) / rho).astype(f)
-    s["rf"][1:nk] = (m["c1"][1:nk] * rho[:-1] + m["c2"][1:nk] * rho[1:]).astype(f)
-    s["rf"][0], s["rf"][nk] = rho[0], rho[nk - 1]
+    # the density of the start from its pi, theta and qv (the reference's
+    # startup thermodynamics); the metrics' c1/c2 then give rf
+    zero = np.zeros((nk + 1, nj, ni), f)
+    _, rho0, _, _ = startup_thermodynamics(s["pi0_3d"], s["pp3d_c"], s["th0_3d"], s["th3d"], s["q3d"][0], zero, zero)
+    m = flat_metrics(cfg, rho0) if levels is None else stretched_metrics(cfg, levels, rho0)
+    prs, rho, rr, rf = startup_thermodynamics(s["pi0_3d"], s["pp3d_c"], s["th0_3d"], s["th3d"], s["q3d"][0], m["c1"],
+                                              m["c2"])
+    s["prs"][:], s["rho"][:], s["rr"][:], s["rf"][:] = prs, rho, rr, rf
+    # the base-state winds and the upper damping profiles (CM1 irdamp = 1
+    # above the configuration's zd, param.F:8631-8673)
+    from .rayleigh import build_rayleigh_coefficients
+
+    m["u0"], m["v0"] = u0.copy(), v0.copy()
+    m["tauh"], m["taus"], m["tauf"] = build_rayleigh_coefficients(m["zh"][:, 0, 0], m["zf"][:, 0, 0],
+                                                                  damping_start_m=cfg.rayleigh_zd_m)
     for cur, base in (("ua", "u3d"), ("va", "v3d"), ("wa", "w3d"), ("tha", "th3d"), ("qa", "q3d"), ("tkea", "tke3d"),
                       ("ppi", "pp3d")):
         s[cur][:] = s[base]
@@ -490,6 +558,39 @@ class MoistLargeStep:
             self.flat_stage_arrays = {"tkea": s["tkea"], "tke3d": s["tke3d"], "tketen": s["tketen"], "c2": m["c2"],
                                       "rrf0": m["rrf0"], "rru": s["rru"], "rrv": s["rrv"], "rrw": s["rrw"],
                                       "divx": s["divx"]}
+        if cfg.rayleigh and not self.flat:
+            refuse(code="GM1B-RAYLEIGH-COLUMN", gate="physics-seam", option="rayleigh", value=True,
+                   reason="the Rayleigh damping is built for the flat operator family of a stretched column",
+                   remedy="give the configuration a stretched column, or rayleigh=False")
+        if cfg.sgs_diffusion:
+            if not self.flat:
+                refuse(code="GM1B-SGS-STRESS-COLUMN", gate="physics-seam", option="sgs_diffusion", value=True,
+                       reason="the SGS diffusion is built for the flat operator family of a stretched column",
+                       remedy="give the configuration a stretched column, or sgs_diffusion=False")
+            from .stress import STRAIN_NAMES, TAU_NAMES, flat_stress_shapes
+
+            shp = flat_stress_shapes(ni, nj, nk)
+            self.stress = {n: torch.zeros(shp[n], dtype=torch.float32, device=dev)
+                           for n in STRAIN_NAMES + TAU_NAMES + ("uten", "vten", "wten")}
+            self.stress_arrays = {"u3d": s["uc"], "v3d": s["vc"], "w3d": s["wc"], "rho": s["rho"], "rf": s["rf"],
+                                  "mh": m["mh"], "mf": m["mf"], "mh_profile": m["mh_profile"], "kmh": s["kmh"],
+                                  "kmv": s["kmv"], **self.stress}
+            self.turbs_arrays = {"th0": s["th0"], "tha": s["tha"], "qa": s["qa"], "rho": s["rho"], "rr": s["rr"],
+                                 "rf": s["rf"], "mh": m["mh"], "mf": m["mf"], "khh": s["khh"], "khv": s["khv"],
+                                 "thten1": s["thheld"], "qten": s["qheld"]}
+        if cfg.rayleigh and not cfg.sgs_diffusion:
+            from .stress import flat_stress_shapes as _shapes
+
+            shp = _shapes(ni, nj, nk)
+            self.stress = {n: torch.zeros(shp[n], dtype=torch.float32, device=dev) for n in ("uten", "vten", "wten")}
+        if cfg.rayleigh:
+            for n in ("u0", "v0", "tauh", "taus", "tauf"):
+                if n not in m:
+                    raise ValueError(f"a damped step needs metrics[{n!r}] (the builder's base-state winds and tau)")
+            self.rayleigh_arrays = {"tauh": m["tauh"], "taus": m["taus"], "tauf": m["tauf"], "u0": m["u0"],
+                                    "v0": m["v0"], "ua": s["uc"], "va": s["vc"], "wa": s["wc"][:nk], "tha": s["tha"],
+                                    "uten1": self.stress["uten"], "vten1": self.stress["vten"],
+                                    "wten1": self.stress["wten"][:nk], "thten1": s["thheld"]}
         # failure words folded on the device every step (gm1b_step_status_fold)
         self.status_acc = torch.zeros(8, dtype=torch.int32, device=dev)
         self._courant = torch.zeros(1, dtype=torch.float32, device=dev)
@@ -556,12 +657,54 @@ class MoistLargeStep:
                                            dt=cfg.dt, stream=st)
         else:
             launch_cuda_tke_diffusion(self.tke_arrays, **self.grid, dt=cfg.dt, stream=st)
+        if cfg.sgs_diffusion:
+            self._held_stress(st)
+        elif cfg.rayleigh:
+            with torch.cuda.stream(st):
+                for n in ("uten", "vten", "wten"):
+                    self.stress[n].zero_()
+
+    def _held_stress(self, st) -> None:
+        """The held momentum tendencies: zeroed, then the SGS stress added
+        (the closure's held phase, cuda_cartesian_closure.py:1202-1291, with
+        neither damper on so the Rayleigh terms are zero)."""
+        from .stress import launch_cuda_flat_sgs_stress
+
+        cfg = self.cfg
+        with torch.cuda.stream(st):
+            for n in ("uten", "vten", "wten"):
+                self.stress[n].zero_()
+        launch_cuda_flat_sgs_stress(self.stress_arrays, **self.k3, dx=cfg.dx, dy=cfg.dy, rdz=self.rdz, dt=cfg.dt,
+                                    stream=st)
 
     def held_tendencies(self) -> None:
         s, st = self.s, self._st()
         with torch.cuda.stream(st):
             s["thheld"].zero_()
             s["qheld"].zero_()
+        if self.cfg.rayleigh:
+            # the damping added into the held momentum (uten1 + uten of the
+            # closure's held sum) and assigned to the held theta before the
+            # scalar diffusion adds to it (solve1.F:412-454)
+            from .rayleigh import launch_cuda_rayleigh_held
+
+            launch_cuda_rayleigh_held(self.rayleigh_arrays, **self.k3, rdalpha=self.cfg.rayleigh_rdalpha,
+                                      profiles=True, add_momentum=True, stream=st)
+        if self.cfg.dissipative_heating:
+            # idiss: after the damping and before the subgrid turbulence
+            # (solve1.F:917-975)
+            from .stress import launch_cuda_dissipative_heating
+
+            launch_cuda_dissipative_heating({"dissten": s["dissten"], "pi0": s["pi0"], "ppi": s["pp3d_c"],
+                                             "qa": s["qa"], "thten1": s["thheld"]}, **self.k3, stream=st)
+        if self.cfg.sgs_diffusion:
+            # turbs for theta and the moisture rows into the held thten1/qten
+            # the eqtset 2 composition then reads (solve1.F:1169-1233)
+            from .stress import launch_cuda_flat_scalar_turbulence
+
+            cfg = self.cfg
+            launch_cuda_flat_scalar_turbulence(self.turbs_arrays, **self.k3, numq=NUMQ, dx=cfg.dx, dy=cfg.dy,
+                                               dz=cfg.dz, dt=cfg.dt, stream=st)
         mo.held_compose(self.held_arrays, **self.k3, dt=self.cfg.dt, stream=st)
 
     def pre_acoustic(self, nrk: int) -> None:
@@ -575,6 +718,13 @@ class MoistLargeStep:
             s["uten"].zero_()
             s["vten"].zero_()
             s["wten"].zero_()
+            if cfg.sgs_diffusion or cfg.rayleigh:
+                # the held momentum seeds the stage tendencies' physical cells
+                # (pack_cartesian_held_momentum, cuda_cartesian_dynamics.py:206)
+                nk, nj, ni = cfg.nk, cfg.nj, cfg.ni
+                s["uten"][1:nk + 1, 3:3 + nj, 3:4 + ni].copy_(self.stress["uten"])
+                s["vten"][1:nk + 1, 3:4 + nj, 3:3 + ni].copy_(self.stress["vten"])
+                s["wten"][1:nk + 2, 3:3 + nj, 3:3 + ni].copy_(self.stress["wten"])
         if self.flat:
             # solve2.F:484-487 (bcwsfc, bc2d of w(1)) and :575 (bcw(rrw,0)) are
             # terrain_flag statements: a flat column runs neither
@@ -935,7 +1085,8 @@ NATIVE_STATE_NAMES = (
     "saturation_mask", "asq", "qbudget",
 ) + tuple(f"{n}_{r}" for r in (1, 2) for n in ("moisture_padded", "fx", "fy", "fz", "advx", "advy", "advz",
                                                  "candidate")) + ("mass1",)
-NATIVE_METRIC_NAMES = METRIC_NAMES + ("mh_profile", "mf_profile", "rho0_padded")
+NATIVE_METRIC_NAMES = METRIC_NAMES + ("mh_profile", "mf_profile", "rho0_padded", "u0", "v0", "tauh", "taus",
+                                      "tauf")
 
 
 class _NativeState(ctypes.Structure):
@@ -950,7 +1101,9 @@ class _NativeConfig(ctypes.Structure):
     _fields_ = [("ni", ctypes.c_int32), ("nj", ctypes.c_int32), ("nk", ctypes.c_int32), ("dx", ctypes.c_float),
                 ("dy", ctypes.c_float), ("dz", ctypes.c_float), ("dt", ctypes.c_float), ("nsound", ctypes.c_int32),
                 ("alph", ctypes.c_float), ("kdiv", ctypes.c_float), ("lateral_sides", ctypes.c_int32 * 4),
-                ("stretched", ctypes.c_int32), ("concurrent", ctypes.c_int32), ("apmasscon", ctypes.c_int32)]
+                ("stretched", ctypes.c_int32), ("concurrent", ctypes.c_int32), ("apmasscon", ctypes.c_int32),
+                ("sgs_diffusion", ctypes.c_int32), ("rayleigh", ctypes.c_int32), ("rdalpha", ctypes.c_float),
+                ("dissipative_heating", ctypes.c_int32)]
 
 
 def _native_lib():
@@ -996,7 +1149,10 @@ class NativeMoistLargeStep:
         self._config = _NativeConfig(cfg.ni, cfg.nj, cfg.nk, cfg.dx, cfg.dy, cfg.dz, cfg.dt, cfg.nsound,
                                      float(np.float32(cfg.alph)), float(np.float32(cfg.kdiv)),
                                      (ctypes.c_int32 * 4)(*cfg.lateral_sides), 1 if cfg.stretched else 0,
-                                     1 if concurrent else 0, 1 if cfg.apmasscon else 0)
+                                     1 if concurrent else 0, 1 if cfg.apmasscon else 0,
+                                     1 if cfg.sgs_diffusion else 0, 1 if cfg.rayleigh else 0,
+                                     float(np.float32(cfg.rayleigh_rdalpha)),
+                                     1 if cfg.dissipative_heating else 0)
         lib = _native_lib()
         handle = ctypes.c_void_p()
         with torch.cuda.device(state["u3d"].device):

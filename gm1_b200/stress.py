@@ -139,3 +139,89 @@ def launch_cuda_flat_sgs_stress(arrays: Mapping[str, Any], *, ni: int, nj: int, 
     a, s, lib = _prepare(arrays, SGS_STRESS_ARRAY_NAMES, ni, nj, nk, "flat-sgs-stress")
     return _launch(a, lib.gm1b_flat_sgs_stress, (ni, nj, nk, ctypes.byref(s), dx, dy, rdz, dt),
                    "gm1b_flat_sgs_stress", {"stream": stream, "receipt": {"operator": "flat-sgs-stress"}})
+
+
+# ------------------------------------------------------------ turbs (flat)
+
+SCALAR_TURBULENCE_ARRAY_NAMES = ("th0", "tha", "qa", "rho", "rr", "rf", "mh", "mf", "khh", "khv", "thten1", "qten")
+
+
+class _TurbsArrays(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_void_p) for n in ("th0", "tha", "qa", "rho", "rr", "rf", "mh", "mf", "khh", "khv",
+                                               "thten", "qten")]
+
+
+def flat_scalar_turbulence_shapes(ni: int, nj: int, nk: int, numq: int) -> dict[str, tuple[int, ...]]:
+    _grid(ni, nj, nk)
+    cell, face = (nk, nj, ni), (nk + 1, nj, ni)
+    return {"th0": (nk,), "tha": cell, "qa": (numq, nk, nj, ni), "rho": cell, "rr": cell, "rf": face, "mh": cell,
+            "mf": face, "khh": face, "khv": face, "thten1": cell, "qten": (numq, nk, nj, ni)}
+
+
+def launch_cuda_flat_scalar_turbulence(arrays: Mapping[str, Any], *, ni: int, nj: int, nk: int, numq: int,
+                                       dx: float, dy: float, dz: float, dt: float,
+                                       stream: Any | None = None) -> CudaLaunch:
+    """turbs on the flat stretched column: theta ((th0 - 300) + tha) into
+    ``thten1``, then moisture rows 0..numq-1 of ``qa`` into those of
+    ``qten`` (added), with khh across the open-halo copies and the implicit
+    vertical diffusion with khv, zero surface flux (the scalar loop of the
+    closure's held phase on the flat lane, cuda_cartesian_closure.py:1566-1633).
+    ``qa`` and ``qten`` may hold more rows than numq (leading rows used);
+    ``dz`` is the coordinate's reference spacing."""
+    if isinstance(numq, bool) or not isinstance(numq, int) or not 0 <= numq <= 6:
+        raise ValueError("numq must be an integer in 0..6")
+    dx, dy, dz, dt = _positive("dx", dx), _positive("dy", dy), _positive("dz", dz), _positive("dt", dt)
+    _grid(ni, nj, nk)
+    if nk > MAX_NK:
+        raise ValueError(f"nk must be <= {MAX_NK} (the column solve's shared memory)")
+    shapes = flat_scalar_turbulence_shapes(ni, nj, nk, numq)
+    for n in ("qa", "qten"):
+        t = arrays.get(n)
+        if isinstance(t, torch.Tensor) and t.dim() == 4 and t.shape[0] >= numq:
+            shapes[n] = tuple(t.shape)
+    a = _require(arrays, SCALAR_TURBULENCE_ARRAY_NAMES, shapes, "flat-scalar-turbulence")
+    if tuple(a["qa"].shape[1:]) != (nk, nj, ni) or tuple(a["qten"].shape[1:]) != (nk, nj, ni):
+        raise ValueError("qa and qten must hold rows of shape (nk, nj, ni)")
+    s = _TurbsArrays(**{f: a["thten1" if f == "thten" else f].data_ptr() for f, _ in _TurbsArrays._fields_})
+    lib = _native.lib()
+    if not getattr(lib, "_turbs_bound", False):
+        i32, f32 = ctypes.c_int32, ctypes.c_float
+        lib.gm1b_flat_scalar_turbulence.argtypes = [i32, i32, i32, i32, ctypes.POINTER(_TurbsArrays), f32, f32, f32,
+                                                    f32, ctypes.c_void_p]
+        lib.gm1b_flat_scalar_turbulence.restype = i32
+        lib._turbs_bound = True
+    return _launch(a, lib.gm1b_flat_scalar_turbulence, (ni, nj, nk, numq, ctypes.byref(s), dx, dy, dz, dt),
+                   "gm1b_flat_scalar_turbulence",
+                   {"stream": stream, "receipt": {"operator": "flat-scalar-turbulence", "scalars": 1 + numq,
+                                                  "cell_words": ni * nj * nk}})
+
+
+# ------------------------------------------------------ dissipative heating
+
+DISSIPATIVE_HEATING_ARRAY_NAMES = ("dissten", "pi0", "ppi", "qa", "thten1")
+
+
+class _DissArrays(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_void_p) for n in DISSIPATIVE_HEATING_ARRAY_NAMES]
+
+
+def launch_cuda_dissipative_heating(arrays: Mapping[str, Any], *, ni: int, nj: int, nk: int,
+                                    stream: Any | None = None) -> CudaLaunch:
+    """CM1's dissipative heating (idiss = 1, Eqtset2IdissConsumer.apply,
+    src/cm1core/eqtset2_energy_terms.py:375) added into ``thten1``:
+    dissten (nk+1, nj, ni), pi0 (nk), ppi (nk, nj, ni), qa (6, nk, nj, ni)."""
+    for name, value in (("ni", ni), ("nj", nj), ("nk", nk)):
+        if isinstance(value, bool) or not isinstance(value, int) or value < 1:
+            raise ValueError(f"{name} must be a positive integer")
+    cell = (nk, nj, ni)
+    shapes = {"dissten": (nk + 1, nj, ni), "pi0": (nk,), "ppi": cell, "qa": (6, nk, nj, ni), "thten1": cell}
+    a = _require(arrays, DISSIPATIVE_HEATING_ARRAY_NAMES, shapes, "dissipative-heating")
+    s = _DissArrays(**{n: a[n].data_ptr() for n in DISSIPATIVE_HEATING_ARRAY_NAMES})
+    lib = _native.lib()
+    if not getattr(lib, "_diss_bound", False):
+        i32 = ctypes.c_int32
+        lib.gm1b_dissipative_heating.argtypes = [i32, i32, i32, ctypes.POINTER(_DissArrays), ctypes.c_void_p]
+        lib.gm1b_dissipative_heating.restype = i32
+        lib._diss_bound = True
+    return _launch(a, lib.gm1b_dissipative_heating, (ni, nj, nk, ctypes.byref(s)), "gm1b_dissipative_heating",
+                   {"stream": stream, "receipt": {"operator": "dissipative-heating", "cell_words": ni * nj * nk}})

@@ -841,6 +841,117 @@ typedef struct gm1b_flat_deformation_arrays {
 GM1B_API int32_t gm1b_flat_deformation(int32_t ni, int32_t nj, int32_t nk, const gm1b_flat_deformation_arrays *arrays,
                                        float dx, float dy, float rdz, void *stream);
 
+/* The SGS stress of the flat (terrain_flag=.false.) stretched column.
+ * Shapes (C order): u3d/uten (nk, nj, ni+1), v3d/vten (nk, nj+1, ni),
+ * w3d/wten/rf/mf/kmh/kmv (nk+1, nj, ni), rho/mh/s11/s22/s33/t11/t22/t33
+ * (nk, nj, ni), s12/t12 (nk, nj+1, ni+1), s13/t13 (nk+1, nj, ni+1), s23/t23
+ * (nk+1, nj+1, ni), mh_profile (nk+2, CM1-indexed: word k+1 is the mh of
+ * mass level k).  Each entry point reads and writes only the arrays it
+ * names below; the others may be NULL. */
+typedef struct gm1b_flat_stress_arrays {
+    const float *u3d, *v3d, *w3d, *rho, *rf, *mh, *mf, *mh_profile, *kmh, *kmv;
+    float *s11, *s22, *s33, *s12, *s13, *s23;
+    float *t11, *t22, *t33, *t12, *t13, *t23;
+    float *uten, *vten, *wten;
+} gm1b_flat_stress_arrays;
+
+/*
+ * The strain carriers rho*Sij of the flat calcdef's mass and face passes:
+ * s11/s22/s33 at cells, s12 at every corner (an open side takes the nearest
+ * interior corner), s13/s23 on face levels 1..nk-1 (levels 0 and nk not
+ * written).  Reads u3d, v3d, w3d, rho, rf, mf, mh_profile.  Replaces the
+ * strain half of enqueue_flat_calcdef (gm1_flat_calcdef_mass_v1 / _face_v1,
+ * src/cm1core/cuda_gm1_flat_stretched_closure.py:76-114, :524-548).
+ */
+GM1B_API int32_t gm1b_flat_strain(int32_t ni, int32_t nj, int32_t nk, const gm1b_flat_stress_arrays *arrays,
+                                  float dx, float dy, float rdz, void *stream);
+
+/*
+ * CM1 gettau with the free-slip lower and upper faces: t11/t22/t33 =
+ * s*(kmh(k)+kmh(k+1)), t12 from the clamped interior corner and the eight
+ * surrounding kmh, t13/t23 on every face level (levels 0 and nk copy levels
+ * 1 and nk-1).  Reads s11..s23, kmh, kmv.  Replaces enqueue_flat_gettau
+ * (src/cm1core/cuda_gm1_flat_stretched_closure.py:551).
+ */
+GM1B_API int32_t gm1b_flat_gettau(int32_t ni, int32_t nj, int32_t nk, const gm1b_flat_stress_arrays *arrays,
+                                  void *stream);
+
+/*
+ * CM1 turbu/turbuz, turbv/turbvz and turbw with their implicit vertical
+ * solves (doimpl = 1, the two-part block off), ADDED into uten, vten and
+ * wten (wten on faces 1..nk-1).  Reads t11..t23, kmh, kmv, rho, rf, mh, mf,
+ * u3d, v3d, w3d.  nk <= 200 (the column solves' shared memory).  Replaces
+ * enqueue_flat_momentum_stress with two_part=None
+ * (src/cm1core/cuda_gm1_flat_stretched_closure.py:574).
+ */
+GM1B_API int32_t gm1b_flat_momentum_stress(int32_t ni, int32_t nj, int32_t nk, const gm1b_flat_stress_arrays *arrays,
+                                           float dx, float dy, float rdz, float dt, void *stream);
+
+/* gm1b_flat_strain, gm1b_flat_gettau and gm1b_flat_momentum_stress in that
+ * order on one stream (the stress block of cuda_cartesian_closure.py:1293-1317
+ * with the strain carriers its calcdef left). */
+GM1B_API int32_t gm1b_flat_sgs_stress(int32_t ni, int32_t nj, int32_t nk, const gm1b_flat_stress_arrays *arrays,
+                                      float dx, float dy, float rdz, float dt, void *stream);
+
+/* th0 (nk); tha/rho/rr/mh/thten (nk, nj, ni); qa/qten rows of nk*nj*ni words
+ * (moisture row q at word q*nk*nj*ni); rf/mf/khh/khv (nk+1, nj, ni). */
+typedef struct gm1b_flat_scalar_turbulence_arrays {
+    const float *th0, *tha, *qa, *rho, *rr, *rf, *mh, *mf, *khh, *khv;
+    float *thten, *qten;
+} gm1b_flat_scalar_turbulence_arrays;
+
+/*
+ * CM1 turbs on the flat stretched column for theta ((th0 - 300) + tha) and
+ * then moisture rows 0..numq-1: the x/y diffusive fluxes with khh on the
+ * open-halo copies (index clamps) and the implicit vertical diffusion with
+ * khv, mh and mf, zero surface flux; ADDED into thten and the first numq
+ * rows of qten.  dz is the coordinate's reference spacing; nk <= 200.
+ * Replaces the scalar loop of the closure's held phase on the flat lane
+ * (cuda_cartesian_closure.py:1566-1633: gm1_turbs_pad_static_open_v1,
+ * gm1_turbs_pack_scalar_open_v1, gm1_flat_turbs_xy_flux_v1,
+ * gm1_flat_turbs_implicit_apply_v1).
+ */
+GM1B_API int32_t gm1b_flat_scalar_turbulence(int32_t ni, int32_t nj, int32_t nk, int32_t numq,
+                                             const gm1b_flat_scalar_turbulence_arrays *arrays, float dx, float dy,
+                                             float dz, float dt, void *stream);
+
+/* tauh/taus (nk, nj+2, ni+2) and tauf (nk+1, nj+2, ni+2) with one
+ * horizontal halo, or (profiles = 1) tauh/taus (nk) and tauf (nk+1)
+ * columns; u0/v0 (nk); ua/uten1 (nk, nj, ni+1); va/vten1 (nk, nj+1, ni);
+ * wa/tha/wten1/thten1 (nk, nj, ni) (wa the w faces 0..nk-1). */
+typedef struct gm1b_rayleigh_held_arrays {
+    const float *tauh, *taus, *tauf, *u0, *v0, *ua, *va, *wa, *tha;
+    float *uten1, *vten1, *wten1, *thten1;
+} gm1b_rayleigh_held_arrays;
+
+/*
+ * CM1's upper Rayleigh damping (irdamp = 1) held tendencies: uten1 =
+ * ((-rdalpha*0.5)*(tauh(i-1)+tauh(i)))*(ua - u0), vten1 the same across j,
+ * wten1 = (-rdalpha*tauf)*wa, thten1 = (-rdalpha*taus)*tha.  add_momentum
+ * = 0 assigns all four (cm1_rayleigh_held_physical_f32_v1); add_momentum = 1
+ * adds the damping into uten1/vten1/wten1 (the held sum uten1 + uten of
+ * cuda_cartesian_closure.py:1289-1291) and assigns thten1.  Replaces
+ * launch_cuda_rayleigh_held (src/cm1core/cuda_rayleigh_held.py:523).
+ */
+GM1B_API int32_t gm1b_rayleigh_held(int32_t ni, int32_t nj, int32_t nk, const gm1b_rayleigh_held_arrays *arrays,
+                                    int32_t profiles, int32_t add_momentum, float rdalpha, void *stream);
+
+/* dissten (nk+1, nj, ni), pi0 (nk), ppi/thten1 (nk, nj, ni), qa six rows of
+ * nk*nj*ni words (qv qc qr qi qs qg). */
+typedef struct gm1b_dissipative_heating_arrays {
+    const float *dissten, *pi0, *ppi, *qa;
+    float *thten1;
+} gm1b_dissipative_heating_arrays;
+
+/*
+ * CM1's dissipative heating (idiss = 1), ADDED into thten1: per cell
+ * (0.5*(dissten(k)+dissten(k+1))) / ((cpdcv*cvm)*(pi0+ppi)) with the moist
+ * heat capacity cvm = ((cv + cvv*qv) + cpl*(qc+qr)) + cpi*((qi+qs)+qg).
+ * Replaces Eqtset2IdissConsumer.apply (src/cm1core/eqtset2_energy_terms.py:375).
+ */
+GM1B_API int32_t gm1b_dissipative_heating(int32_t ni, int32_t nj, int32_t nk,
+                                          const gm1b_dissipative_heating_arrays *arrays, void *stream);
+
 /* c1/c2/mf/nm (nk+1, nj, ni), pi0/th0 (nk), prs/pp3d/th3d and the cell
  * outputs (nk, nj, ni), q3d (6, nk, nj, ni) in the order qv qc qr qi qs qg,
  * saturation_mask uint8 (nk, nj, ni).  counts (optional, NULL = not
@@ -1187,6 +1298,10 @@ typedef struct gm1b_moist_metrics {
     const float *terrain_msl, *zh, *zf, *mh, *rmh, *mf, *rmf, *c1, *c2, *rho0_3d, *rr0, *rf0, *rrf0, *gz, *rgz, *gzu,
         *rgzu, *gzv, *rgzv, *dzdx, *dzdy, *gx, *gxu, *gy, *gyv;
     const float *mh_profile, *mf_profile, *rho0_padded;
+    /* the upper Rayleigh damping (read when the configuration turns it on):
+     * the base-state winds u0/v0 (nk) and the damping profiles tauh/taus
+     * (nk) and tauf (nk+1) */
+    const float *u0, *v0, *tauh, *taus, *tauf;
 } gm1b_moist_metrics;
 
 /* dz: the uniform layer depth, or a stretched column's reference dz
@@ -1206,6 +1321,20 @@ typedef struct gm1b_moist_step_config {
      * supercell namelist's): between the pre-physics equation of state and
      * the Kessler driver, against the state's mass1 ledger */
     int32_t apmasscon;
+    /* the SGS stress and scalar diffusion held tendencies (gettau and
+     * turbu/turbv/turbw once per large step, added into the momentum
+     * tendencies of every RK stage; turbs of theta and the moisture rows
+     * into thheld/qheld before the eqtset 2 composition); stretched columns
+     * only.  The handle allocates the stress scratch. */
+    int32_t sgs_diffusion;
+    /* CM1's upper Rayleigh damping, irdamp = 1 (the held u, v, w and theta
+     * tendencies of solve1.F:412-454 at rate rdalpha on the metrics' tau
+     * profiles); stretched columns only */
+    int32_t rayleigh;
+    float rdalpha;
+    /* CM1's dissipative heating, idiss = 1 (the TKE closure's dissipation
+     * rate into the held theta, solve1.F:917-975) */
+    int32_t dissipative_heating;
 } gm1b_moist_step_config;
 
 typedef struct gm1b_moist_step gm1b_moist_step;

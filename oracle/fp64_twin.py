@@ -37,6 +37,12 @@ def _cfg_dict(cfg) -> dict:
     d = {k: getattr(cfg, k) for k in CFG_KEYS}
     d["lateral_sides"] = list(d["lateral_sides"])
     d["stretched"] = getattr(cfg, "column", None) is not None
+    d["apmasscon"] = bool(getattr(cfg, "apmasscon", True))
+    d["sgs_diffusion"] = bool(getattr(cfg, "sgs_diffusion", False))
+    d["rayleigh"] = bool(getattr(cfg, "rayleigh", False))
+    d["dissipative_heating"] = bool(getattr(cfg, "dissipative_heating", False))
+    d["rayleigh_zd_m"] = float(getattr(cfg, "rayleigh_zd_m", 15000.0))
+    d["rayleigh_rdalpha"] = float(getattr(cfg, "rayleigh_rdalpha", 3.3333333333e-3))
     return d
 
 

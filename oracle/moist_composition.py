@@ -14,6 +14,7 @@ import numpy as np
 from oracle import advection as oadv
 from oracle import bridge as obr
 from oracle import closure as ocl
+from oracle import stress as ost
 from oracle import kessler as oks
 from oracle import moist_step as oms
 from oracle import momentum as omom
@@ -64,6 +65,19 @@ class OracleMoistStep:
         # :1220-1231, :1254-1269, :1293; cuda_cartesian_closure.py:1133-1141,
         # :1191-1197, :1658-1663)
         self.flat = getattr(cfg, "column", None) is not None
+        # the SGS stress and scalar diffusion held tendencies (gettau +
+        # turbu/turbv/turbw and turbs of the closure's held phase,
+        # cuda_cartesian_closure.py:1268-1291): built for the flat family
+        # the stretched column runs
+        self.sgs_diffusion = bool(getattr(cfg, "sgs_diffusion", False))
+        # CM1's upper Rayleigh damping (irdamp = 1, solve1.F:412-454), its
+        # coefficients and base-state winds from the metrics
+        self.rayleigh = bool(getattr(cfg, "rayleigh", False))
+        if self.sgs_diffusion or self.rayleigh:
+            if not self.flat:
+                raise ValueError("the SGS diffusion and the Rayleigh damping are built for the stretched column's "
+                                 "flat operator family only")
+            self.stress = ost.zeros(cfg.ni, cfg.nj, cfg.nk, ost.STRAIN_NAMES + ost.TAU_NAMES + ost.TENDENCY_NAMES)
         if self.flat:
             self.rdz = float(np.float32(np.float32(1.0) / np.float32(cfg.dz)))
             self.hx = dict(ni=cfg.ni, nj=cfg.nj, nk=cfg.nk, dx=cfg.dx, dy=cfg.dy)
@@ -101,6 +115,22 @@ class OracleMoistStep:
             otev.tke_diffusion_flat(self._tke(), **self.hx, rdz=self.rdz, dt=c.dt)
         else:
             otev.tke_diffusion(self._tke(), **self.grid, dt=c.dt)
+        if self.sgs_diffusion:
+            self._held_stress()
+        elif self.rayleigh:
+            for n in ost.TENDENCY_NAMES:
+                self.stress[n][:] = 0
+
+    def _held_stress(self):
+        """The held momentum tendencies: zero, then the SGS stress added
+        (turbu/turbv/turbw into the zeroed tile tendencies; no Rayleigh
+        damping, so uten1 = 0 and the held sum is the stress)."""
+        s, m, c, st = self.s, self.m, self.cfg, self.stress
+        for n in ost.TENDENCY_NAMES:
+            st[n][:] = 0
+        a = {"u3d": s["uc"], "v3d": s["vc"], "w3d": s["wc"], "rho": s["rho"], "rf": s["rf"], "mh": m["mh"],
+             "mf": m["mf"], "mh_profile": m["mh_profile"], "kmh": s["kmh"], "kmv": s["kmv"], **st}
+        ost.flat_sgs_stress(a, **self.hx, rdz=self.rdz, dt=c.dt)
 
     def _tke(self):
         s, m = self.s, self.m
@@ -110,9 +140,28 @@ class OracleMoistStep:
                 "rru": s["rru"], "rrv": s["rrv"], "rrw": s["rrw"], "divx": s["divx"]}
 
     def held_tendencies(self):
-        s = self.s
+        s, m, c = self.s, self.m, self.cfg
         s["thheld"][:] = 0
         s["qheld"][:] = 0
+        if self.rayleigh:
+            # added into the held momentum (uten1 + uten), assigned to thheld
+            nk = c.nk
+            a = {"tauh": m["tauh"], "taus": m["taus"], "tauf": m["tauf"], "u0": m["u0"], "v0": m["v0"],
+                 "ua": s["uc"], "va": s["vc"], "wa": s["wc"][:nk], "tha": s["tha"], "uten1": self.stress["uten"],
+                 "vten1": self.stress["vten"], "wten1": self.stress["wten"][:nk], "thten1": s["thheld"]}
+            ost.rayleigh_held(a, ni=c.ni, nj=c.nj, nk=nk, rdalpha=getattr(c, "rayleigh_rdalpha", 3.3333333333e-3),
+                              profiles=True, add_momentum=True)
+        if getattr(c, "dissipative_heating", False):
+            # idiss after the damping, before the subgrid turbulence
+            ost.dissipative_heating({"dissten": s["dissten"], "pi0": s["pi0"], "ppi": s["pp3d_c"], "qa": s["qa"],
+                                     "thten1": s["thheld"]}, **self.k3)
+        if self.sgs_diffusion:
+            # turbs for theta and the moisture rows into the held thten1/qten
+            # the eqtset 2 composition then reads (solve1.F:1169-1233)
+            a = {"th0": s["th0"], "tha": s["tha"], "qa": s["qa"], "rho": s["rho"], "rr": s["rr"], "rf": s["rf"],
+                 "mh": m["mh"], "mf": m["mf"], "khh": s["khh"], "khv": s["khv"], "thten1": s["thheld"],
+                 "qten": s["qheld"]}
+            ost.flat_scalar_turbulence(a, **self.hx, numq=s["qheld"].shape[0], dz=c.dz, dt=c.dt)
         oms.held_compose({"th0": s["th0_3d"], "pi0": s["pi0_3d"], "rho": s["rho"], "ppi": s["pp3d_c"],
                           "tha": s["tha"], "qa": s["qa"], "qpten": s["qpten"], "qtten": s["qtten"],
                           "qvten": s["qvten"], "qcten": s["qcten"], "thheld": s["thheld"], "qheld": s["qheld"],
@@ -132,6 +181,13 @@ class OracleMoistStep:
         s["uten"][:] = 0
         s["vten"][:] = 0
         s["wten"][:] = 0
+        if self.sgs_diffusion or self.rayleigh:
+            # the held momentum seeds the stage tendencies' physical cells
+            # (pack_cartesian_held_momentum, cuda_cartesian_dynamics.py:206)
+            nk, nj, ni = c.nk, c.nj, c.ni
+            s["uten"][1:nk + 1, 3:3 + nj, 3:4 + ni] = self.stress["uten"]
+            s["vten"][1:nk + 1, 3:4 + nj, 3:3 + ni] = self.stress["vten"]
+            s["wten"][1:nk + 2, 3:3 + nj, 3:3 + ni] = self.stress["wten"]
         if self.flat:
             omom.momentum_advection5_column(self._mom(), self.column, **self.hx, lateral_sides=c.lateral_sides)
             oms.moist_buoyancy_flat(s["dum8"], m["c1"], m["c2"], s["wten"], **self.k3)

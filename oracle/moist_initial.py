@@ -183,17 +183,68 @@ def weisman_klemp_initial_state(cfg, *, seed: int = 0, bubble_k: float = 3.0, no
     s["q3d"][0] = s["qv0"][:, None, None]
     s["q3d"][1] = np.where(r < 0.5, bubble_cloud, 0.0).astype(f)
     s["q3d"][2] = np.where(r < 0.5, bubble_rain, 0.0).astype(f)
-    tv = (s["th0_3d"].astype(np.float64) + s["th3d"]) * s["pi0_3d"] * (1.0 + 0.61 * s["q3d"][0])
-    s["rho"][:] = (col["prs0"][:, None, None] / (287.04 * tv)).astype(f)
+    # the density of the start from its pi, theta and qv (the reference's
+    # startup thermodynamics); the metrics' c1/c2 then give rf
     s["tke3d"][1:nk] = f(1.0e-4)
     for n in ("uh", "vh", "ruf", "rvf", "ruh", "rvh", "ones_mass"):
         s[n][:] = f(1.0)
-    m = flat_metrics(ni, nj, nk, cfg.dz, s["rho"]) if lv is None else stretched_metrics(ni, nj, nk, lv, s["rho"])
-    rho = s["rho"]
-    s["rr"][:] = (f(1.0) / rho).astype(f)
-    s["rf"][1:nk] = (m["c1"][1:nk] * rho[:-1] + m["c2"][1:nk] * rho[1:]).astype(f)
-    s["rf"][0], s["rf"][nk] = rho[0], rho[nk - 1]
+    zero = np.zeros((nk + 1, nj, ni), f)
+    _, rho0, _, _ = startup_thermodynamics(s["pi0_3d"], s["pp3d_c"], s["th0_3d"], s["th3d"], s["q3d"][0], zero, zero)
+    m = flat_metrics(ni, nj, nk, cfg.dz, rho0) if lv is None else stretched_metrics(ni, nj, nk, lv, rho0)
+    prs, rho, rr, rf = startup_thermodynamics(s["pi0_3d"], s["pp3d_c"], s["th0_3d"], s["th3d"], s["q3d"][0], m["c1"],
+                                              m["c2"])
+    s["prs"][:], s["rho"][:], s["rr"][:], s["rf"][:] = prs, rho, rr, rf
+    # the base-state winds and the upper damping profiles above zd
+    from oracle.stress import rayleigh_coefficients
+
+    m["u0"], m["v0"] = u0.astype(f), v0.astype(f)
+    m["tauh"], m["taus"], m["tauf"] = rayleigh_coefficients(m["zh"][:, 0, 0], m["zf"][:, 0, 0],
+                                                            damping_start_m=getattr(cfg, "rayleigh_zd_m", 15000.0))
     for cur, base in (("ua", "u3d"), ("va", "v3d"), ("wa", "w3d"), ("tha", "th3d"), ("qa", "q3d"), ("tkea", "tke3d"),
                       ("ppi", "pp3d")):
         s[cur][:] = s[base]
     return s, m
+
+
+def _libm_powf():
+    import ctypes
+    import ctypes.util
+
+    lib = ctypes.CDLL(ctypes.util.find_library("m") or "libm.so.6")
+    fn = lib.powf
+    fn.restype, fn.argtypes = ctypes.c_float, [ctypes.c_float, ctypes.c_float]
+    return fn
+
+
+def startup_thermodynamics(pi0_3d, pp3d, th0_3d, th3d, qv, c1, c2):
+    """prs, rho, rr and rf of a start from its pi, theta and qv, in the
+    reference's startup order (cpu_startup_thermodynamics,
+    src/cm1core/cuda_cartesian_startup.py:295-345; CM1 init3d): prs =
+    p00*powf(pi0 + pp3d, cp/rd) with the host C library's powf, rho =
+    prs/((theta*pi)*(rd + max(qv, 0)*rv)), rr = 1/rho, rf from c1/c2 inside
+    and the second-order extrapolation at the two boundary faces; binary32
+    one operation at a time."""
+    f = np.float32
+    rd, rv, p00 = f(287.04), f(461.5), f(100000.0)
+    cpdrd = f(f(1005.7) / rd)
+    pi = (np.asarray(pi0_3d, f) + np.asarray(pp3d, f)).astype(f)
+    powf = _libm_powf()
+    levels, inverse = np.unique(pi, return_inverse=True)
+    pw = np.array([powf(float(x), float(cpdrd)) for x in levels], f)[inverse].reshape(pi.shape)
+    prs = (p00 * pw).astype(f)
+    theta = (np.asarray(th0_3d, f) + np.asarray(th3d, f)).astype(f)
+    gas = (rd + (np.maximum(f(0.0), np.asarray(qv, f)) * rv).astype(f)).astype(f)
+    rho = (prs / ((theta * pi).astype(f) * gas).astype(f)).astype(f)
+    rr = (f(1.0) / rho).astype(f)
+    nk = rho.shape[0]
+    rf = np.zeros((nk + 1,) + rho.shape[1:], f)
+    rf[1:nk] = ((c1[1:nk] * rho[:-1]).astype(f) + (c2[1:nk] * rho[1:]).astype(f)).astype(f)
+    rf[0] = _extrap(rho[0], rho[1], rho[2])
+    rf[nk] = _extrap(rho[nk - 1], rho[nk - 2], rho[nk - 3])
+    return prs, rho, rr, rf
+
+
+def _extrap(a, b, c):
+    f = np.float32
+    s = ((f(1.875) * a).astype(f) + (f(-1.25) * b).astype(f)).astype(f)
+    return (s + (f(0.375) * c).astype(f)).astype(f)

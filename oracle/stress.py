@@ -85,3 +85,72 @@ def flat_sgs_stress(a, *, ni, nj, nk, dx, dy, rdz, dt) -> None:
 def zeros(ni, nj, nk, names) -> dict[str, np.ndarray]:
     sh = stress_shapes(ni, nj, nk)
     return {n: np.zeros(sh[n], REAL) for n in names}
+
+
+SCALAR_TURBULENCE_INPUTS = ("th0", "tha", "qa", "rho", "rr", "rf", "mh", "mf", "khh", "khv")
+
+
+def flat_scalar_turbulence(a, *, ni, nj, nk, numq, dx, dy, dz, dt) -> None:
+    """turbs for theta and moisture rows 0..numq-1, added into thten1 and qten."""
+    lib = load()
+    if not getattr(lib, "_turbs_ready", False):
+        i, f = ctypes.c_int, C_REAL
+        lib.oracle_flat_scalar_turbulence.argtypes = [i, i, i, i] + [_F] * 10 + [f, f, f, f, _F, _F]
+        lib.oracle_flat_scalar_turbulence.restype = i
+        lib._turbs_ready = True
+    for n in ("qa", "qten"):
+        assert a[n].shape[0] >= numq and a[n].shape[1:] == (nk, nj, ni)
+    rc = lib.oracle_flat_scalar_turbulence(ni, nj, nk, numq, *(_p(a[n]) for n in SCALAR_TURBULENCE_INPUTS), dx, dy,
+                                           dz, dt, _p(a["thten1"]), _p(a["qten"]))
+    if rc != 0:
+        raise ValueError(f"oracle_flat_scalar_turbulence failed ({rc})")
+
+
+# ------------------------------------------------------------------ Rayleigh
+RAYLEIGH_INPUTS = ("tauh", "taus", "tauf", "u0", "v0", "ua", "va", "wa", "tha")
+
+
+def rayleigh_coefficients(zh, zf, *, damping_start_m):
+    """(tauh, taus, tauf): cpu_build_rayleigh_coefficients's formula
+    (src/cm1core/cuda_rayleigh_held.py:264-383; CM1 param.F:8652-8671) in
+    binary32 with numpy's float32 cosine; zf's last level is the top."""
+    f = np.float32
+    zh, zf = np.asarray(zh, f), np.asarray(zf, f)
+    start, top = f(damping_start_m), zf[-1]
+
+    def tau(z):
+        ratio = np.divide(np.subtract(z, start, dtype=f), np.subtract(top[None], start, dtype=f), dtype=f)
+        cosine = np.cos(np.multiply(f(np.pi), ratio, dtype=f), dtype=f)
+        value = np.multiply(f(0.5), np.subtract(f(1.0), cosine, dtype=f), dtype=f)
+        return np.where(z > start, value, f(0.0)).astype(f)
+
+    th = tau(zh)
+    return th, th.copy(), tau(zf)
+
+
+def rayleigh_held(a, *, ni, nj, nk, rdalpha, profiles=False, add_momentum=False) -> None:
+    """The irdamp = 1 held tendencies into uten1, vten1, wten1 and thten1."""
+    lib = load()
+    if not getattr(lib, "_rayleigh_ready", False):
+        i, f = ctypes.c_int, C_REAL
+        lib.oracle_rayleigh_held.argtypes = [i, i, i] + [_F] * 9 + [i, i, f] + [_F] * 4
+        lib.oracle_rayleigh_held.restype = i
+        lib._rayleigh_ready = True
+    rc = lib.oracle_rayleigh_held(ni, nj, nk, *(_p(a[n]) for n in RAYLEIGH_INPUTS), 1 if profiles else 0,
+                                  1 if add_momentum else 0, float(np.float32(rdalpha)),
+                                  *(_p(a[n]) for n in ("uten1", "vten1", "wten1", "thten1")))
+    if rc != 0:
+        raise ValueError(f"oracle_rayleigh_held failed ({rc})")
+
+
+def dissipative_heating(a, *, ni, nj, nk) -> None:
+    """idiss = 1: the dissipative heating added into thten1."""
+    lib = load()
+    if not getattr(lib, "_diss_ready", False):
+        i = ctypes.c_int
+        lib.oracle_dissipative_heating.argtypes = [i, i, i] + [_F] * 5
+        lib.oracle_dissipative_heating.restype = i
+        lib._diss_ready = True
+    rc = lib.oracle_dissipative_heating(ni, nj, nk, *(_p(a[n]) for n in ("dissten", "pi0", "ppi", "qa", "thten1")))
+    if rc != 0:
+        raise ValueError(f"oracle_dissipative_heating failed ({rc})")

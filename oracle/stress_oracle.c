@@ -243,3 +243,201 @@ int oracle_flat_momentum_stress(int ni, int nj, int nk, const float* t11, const 
   free(buf);
   return 0;
 }
+
+/* ------------------------------------------------------------------------
+ * turbs on the flat column (numq moisture rows after theta), the four open
+ * sides, no surface flux (iflux = 0):
+ *   the open-halo copies        gm1_turbs_pad_static_open_v1 / _pack_scalar_open_v1
+ *                               src/cm1core/cuda_gm1_scalar_turbulence.py:453-466
+ *                               (theta is (th0 - 300) + tha, bc.F:180-364)
+ *   the flat fluxes and turbsz  gm1_flat_turbs_xy_flux_v1 / _implicit_apply_v1
+ *                               src/cm1core/cuda_gm1_flat_stretched_closure.py:335-381
+ *                               (turbtend.F:60-434, :442-692; solve1.F:1169-1233)
+ * th0 (nk), tha/rho/rr/mh (nk, nj, ni), qa and qten (rows of nk*nj*ni),
+ * rf/mf/khh/khv (nk+1, nj, ni).  The tendencies are ADDED into thten and
+ * the first numq rows of qten.  dz is the coordinate's reference spacing.
+ */
+typedef struct {
+  int ni, nj, nk;
+  const float *th0, *tha, *q; /* q != NULL: a moisture row, else theta */
+} scalar_src;
+
+/* the open-halo scalar at a clamped cell */
+static float sval(const scalar_src* s, int k, int j, int i) {
+  const int64_t p = I3(k, clampi(j, 0, s->nj - 1), clampi(i, 0, s->ni - 1), s->nj, s->ni);
+  if (s->q) return s->q[p];
+  return (s->th0[k] - 300.0f) + s->tha[p];
+}
+
+/* x flux through the face between cells f-1 and f (f in [0, ni]) */
+static float flux_x(const scalar_src* s, const float* rho, const float* khh, int k, int j, int f, float rx) {
+  const int nj = s->nj, ni = s->ni;
+  const float den = cell(rho, k, j, f, nj, ni) + cell(rho, k, j, f - 1, nj, ni);
+  const float kh = (cell(khh, k, j, f, nj, ni) + cell(khh, k, j, f - 1, nj, ni)) +
+                   (cell(khh, k + 1, j, f, nj, ni) + cell(khh, k + 1, j, f - 1, nj, ni));
+  return (((-0.125f * den) * kh) * (sval(s, k, j, f) - sval(s, k, j, f - 1))) * rx;
+}
+
+/* y flux through the face between rows f-1 and f (f in [0, nj]) */
+static float flux_y(const scalar_src* s, const float* rho, const float* khh, int k, int f, int i, float ry) {
+  const int nj = s->nj, ni = s->ni;
+  const float den = cell(rho, k, f, i, nj, ni) + cell(rho, k, f - 1, i, nj, ni);
+  const float kh = (cell(khh, k, f, i, nj, ni) + cell(khh, k, f - 1, i, nj, ni)) +
+                   (cell(khh, k + 1, f, i, nj, ni) + cell(khh, k + 1, f - 1, i, nj, ni));
+  return (((-0.125f * den) * kh) * (sval(s, k, f, i) - sval(s, k, f - 1, i))) * ry;
+}
+
+static void turbs_one(const scalar_src* s, const float* rho, const float* rr, const float* rf, const float* mh,
+                      const float* mf, const float* khh, const float* khv, float dx, float dy, float dz, float dt,
+                      float* target, float* cp, float* dp) {
+  const int ni = s->ni, nj = s->nj, nk = s->nk;
+  const float rx = 1.0f / dx, ry = 1.0f / dy, rz = 1.0f / dz, rdt = 1.0f / dt;
+  const float tema = (((-1.0f * dt) * 1.0f) * rz) * rz;
+  const float temb = ((dt * 0.0f) * rz) * rz;
+  const float temc = dt * rz;
+  for (int j = 0; j < nj; ++j)
+    for (int i = 0; i < ni; ++i) {
+#define SC(k) sval(s, k, j, i)
+#define COEF(F, K) \
+  ((((khv[I3(F, j, i, nj, ni)] * mf[I3(F, j, i, nj, ni)]) * rf[I3(F, j, i, nj, ni)]) * mh[I3(K, j, i, nj, ni)]) * \
+   rr[I3(K, j, i, nj, ni)])
+      const int64_t col = I3(0, j, i, nj, ni);
+      float r2 = COEF(1, 0);
+      float cfc = tema * r2, cfb = 1.0f - cfc;
+      float ex = (-r2) * SC(0) + r2 * SC(1);
+      float bc = ((temc * 0.0f) * mh[col]) * rr[col];
+      float cfd = (SC(0) + temb * ex) + bc;
+      float tem = 1.0f / cfb;
+      cp[0] = (-cfc) * tem;
+      dp[0] = cfd * tem;
+      for (int k = 1; k + 1 < nk; ++k) {
+        const float r1 = COEF(k, k);
+        r2 = COEF(k + 1, k);
+        const float cfa = tema * r1;
+        cfc = tema * r2;
+        cfb = (1.0f - cfa) - cfc;
+        ex = (r1 * SC(k - 1) - (r1 + r2) * SC(k)) + r2 * SC(k + 1);
+        cfd = SC(k) + temb * ex;
+        tem = 1.0f / (cfa * cp[k - 1] + cfb);
+        cp[k] = (-cfc) * tem;
+        dp[k] = (cfd - cfa * dp[k - 1]) * tem;
+      }
+      const int k = nk - 1;
+      const int64_t top = I3(k, j, i, nj, ni);
+      const float r1 = COEF(k, k), cfa = tema * r1;
+      cfb = 1.0f - cfa;
+      ex = r1 * SC(k - 1) - r1 * SC(k);
+      bc = ((temc * 0.0f) * mh[top]) * rr[top];
+      cfd = (SC(k) + temb * ex) - bc;
+      tem = 1.0f / (cfa * cp[k - 1] + cfb);
+      float sol = (cfd - cfa * dp[k - 1]) * tem;
+      for (int kk = nk - 1; kk >= 0; --kk) {
+        const int64_t mass = I3(kk, j, i, nj, ni);
+        if (kk != nk - 1) sol = cp[kk] * sol + dp[kk];
+        const float tz = (rho[mass] * (sol - SC(kk))) * rdt;
+        float tx = -((flux_x(s, rho, khh, kk, j, i + 1, rx) - flux_x(s, rho, khh, kk, j, i, rx)) * rx);
+        if (i == 0 || i + 1 == ni) tx = 0.0f;
+        float ty = -((flux_y(s, rho, khh, kk, j + 1, i, ry) - flux_y(s, rho, khh, kk, j, i, ry)) * ry);
+        if (j == 0 || j + 1 == nj) ty = 0.0f;
+        target[mass] = target[mass] + ((tx + ty) + tz) * rr[mass];
+      }
+#undef SC
+#undef COEF
+    }
+}
+
+int oracle_flat_scalar_turbulence(int ni, int nj, int nk, int numq, const float* th0, const float* tha,
+                                  const float* qa, const float* rho, const float* rr, const float* rf,
+                                  const float* mh, const float* mf, const float* khh, const float* khv, float dx,
+                                  float dy, float dz, float dt, float* thten, float* qten) {
+  if (ni < 3 || nj < 3 || nk < 3 || numq < 0) return -1;
+  float* buf = malloc(sizeof(float) * 2 * (size_t)nk);
+  if (!buf) return -2;
+  const int64_t n = (int64_t)ni * nj * nk;
+  scalar_src s = {ni, nj, nk, th0, tha, NULL};
+  turbs_one(&s, rho, rr, rf, mh, mf, khh, khv, dx, dy, dz, dt, thten, buf, buf + nk);
+  for (int q = 0; q < numq; ++q) {
+    s.q = qa + q * n;
+    turbs_one(&s, rho, rr, rf, mh, mf, khh, khv, dx, dy, dz, dt, qten + q * n, buf, buf + nk);
+  }
+  free(buf);
+  return 0;
+}
+
+/* ------------------------------------------------------------------------
+ * Upper Rayleigh damping, irdamp = 1 (cpu_rayleigh_held_inplace and its
+ * kernel cm1_rayleigh_held_physical_f32_v1,
+ * src/cm1core/cuda_rayleigh_held.py:213-254, :419-488; CM1 solve1.F:412-454):
+ *   uten1 = ((-rdalpha*0.5)*(tauh(i-1)+tauh(i)))*(ua - u0(k)), vten1 the
+ *   same across j, wten1 = (-rdalpha*tauf)*wa, thten1 = (-rdalpha*taus)*tha.
+ * profiles = 0: tauh/taus (nk, nj+2, ni+2) and tauf (nk+1, nj+2, ni+2) with
+ * one horizontal halo (the reference's layout); profiles = 1: tauh/taus
+ * (nk) and tauf (nk+1) column profiles.  add_momentum = 1 adds the damping
+ * into the momentum outputs (uten1 = damping + uten1, the closure's held
+ * sum cuda_cartesian_closure.py:1289-1291) and assigns thten1.
+ */
+static float tau_at(const float* tau, int profiles, int k, int jh, int ih, int nj, int ni) {
+  return profiles ? tau[k] : tau[I3(k, jh, ih, nj + 2, ni + 2)];
+}
+
+int oracle_rayleigh_held(int ni, int nj, int nk, const float* tauh, const float* taus, const float* tauf,
+                         const float* u0, const float* v0, const float* ua, const float* va, const float* wa,
+                         const float* tha, int profiles, int add_momentum, float rdalpha, float* uten1,
+                         float* vten1, float* wten1, float* thten1) {
+  if (ni < 1 || nj < 1 || nk < 1) return -1;
+  const float neg = -rdalpha, negh = neg * 0.5f;
+  for (int k = 0; k < nk; ++k)
+    for (int j = 0; j < nj; ++j)
+      for (int f = 0; f <= ni; ++f) {
+        const float pair = tau_at(tauh, profiles, k, j + 1, f, nj, ni) + tau_at(tauh, profiles, k, j + 1, f + 1, nj, ni);
+        const int64_t z = I3(k, j, f, nj, ni + 1);
+        const float d = (negh * pair) * (ua[z] - u0[k]);
+        uten1[z] = add_momentum ? d + uten1[z] : d;
+      }
+  for (int k = 0; k < nk; ++k)
+    for (int f = 0; f <= nj; ++f)
+      for (int i = 0; i < ni; ++i) {
+        const float pair = tau_at(tauh, profiles, k, f, i + 1, nj, ni) + tau_at(tauh, profiles, k, f + 1, i + 1, nj, ni);
+        const int64_t z = I3(k, f, i, nj + 1, ni);
+        const float d = (negh * pair) * (va[z] - v0[k]);
+        vten1[z] = add_momentum ? d + vten1[z] : d;
+      }
+  for (int k = 0; k < nk; ++k)
+    for (int j = 0; j < nj; ++j)
+      for (int i = 0; i < ni; ++i) {
+        const int64_t z = I3(k, j, i, nj, ni);
+        const float dw = (neg * tau_at(tauf, profiles, k, j + 1, i + 1, nj, ni)) * wa[z];
+        wten1[z] = add_momentum ? dw + wten1[z] : dw;
+        thten1[z] = (neg * tau_at(taus, profiles, k, j + 1, i + 1, nj, ni)) * tha[z];
+      }
+  return 0;
+}
+
+/* ------------------------------------------------------------------------
+ * Dissipative heating, idiss = 1 (cpu_idiss_cell_f32 and the consumer
+ * Eqtset2IdissConsumer.apply, src/cm1core/eqtset2_energy_terms.py:176-215,
+ * :375-470; CM1 solve1.F:744-848, :917-975): per cell
+ *   cvm = ((cv + cvv*qv) + cpl*(qc+qr)) + cpi*((qi+qs)+qg)
+ *   thten1 += (0.5*(dissten(k)+dissten(k+1))) / ((cpdcv*cvm)*(pi0+ppi))
+ * dissten (nk+1, nj, ni), pi0 (nk), ppi/thten1 (nk, nj, ni), qa six rows of
+ * nk*nj*ni words (qv qc qr qi qs qg).
+ */
+int oracle_dissipative_heating(int ni, int nj, int nk, const float* dissten, const float* pi0, const float* ppi,
+                               const float* qa, float* thten1) {
+  if (ni < 1 || nj < 1 || nk < 1) return -1;
+  const float rd = 287.04f, cp = 1005.7f, cpv = 1870.0f, rv = 461.5f, cpl = 4190.0f, cpi = 2106.0f;
+  const float cv = cp - rd, cvv = cpv - rv, cpdcv = cp / cv;
+  const int64_t n = (int64_t)ni * nj * nk, plane = (int64_t)ni * nj;
+  for (int64_t q = 0; q < n; ++q) {
+    const int k = (int)(q / plane);
+    const float ql = qa[n + q] + qa[2 * n + q];
+    const float qice = (qa[3 * n + q] + qa[4 * n + q]) + qa[5 * n + q];
+    float cvm = cv + cvv * qa[q];
+    cvm = cvm + cpl * ql;
+    cvm = cvm + cpi * qice;
+    const float epsd = 0.5f * (dissten[q] + dissten[q + plane]);
+    const float den = (cpdcv * cvm) * (pi0[k] + ppi[q]);
+    thten1[q] = thten1[q] + epsd / den;
+  }
+  return 0;
+}

@@ -18,6 +18,9 @@ Reference entry points used (their CPU twins, single-threaded NumPy):
   cpu_psolver3_trajectory_inplace          src/cm1core/cuda_psolver3_trajectory.py:761
   cpu_initial_dry_mass, cpu_apmasscon_inplace  src/cm1core/cuda_apmasscon.py:226, :256
   cpu_sgs_stress_tendency_inplace          src/cm1core/cuda_sgs_stress_tendency.py:292
+  cpu_gm1_scalar_turbulence_inplace        src/cm1core/cuda_gm1_scalar_turbulence.py:414
+  cpu_build_rayleigh_coefficients, cpu_rayleigh_held_inplace  src/cm1core/cuda_rayleigh_held.py:264, :213
+  cpu_idiss_cell_f32                       src/cm1core/eqtset2_energy_terms.py:176
   (and the others named by each make_* function)
 """
 
@@ -1287,10 +1290,125 @@ def make_stress(reference: Path) -> None:
         print("wrote", tag)
 
 
+# (ni, nj, nk, seed): dx = dy = 128 m, so every product with 1/dx is exact
+# and the terrain twin's fluxes on flat metrics form the flat text's words
+TURBS_CASES = {"turbs_8x7x6": (8, 7, 6, 71), "turbs_11x9x10": (11, 9, 10, 72)}
+
+
+def turbs_fixture(ni: int, nj: int, nk: int, seed: int) -> dict[str, np.ndarray]:
+    """Seeded inputs of turbs: theta and six moisture rows with horizontal
+    and vertical structure, positive diffusivities, densities and column
+    metrics, flat terrain."""
+    rng = np.random.default_rng(seed)
+    f = np.float32
+    mass, face = (nk, nj, ni), (nk + 1, nj, ni)
+    a = {"th0": np.linspace(300.0, 340.0, nk).astype(f), "tha": rng.normal(0.0, 1.5, mass).astype(f),
+         "qa": np.abs(rng.normal(0.0, 4.0e-3, (6, nk, nj, ni))).astype(f),
+         "rho": rng.uniform(0.4, 1.2, mass).astype(f)}
+    a["rr"] = (f(1.0) / a["rho"]).astype(f)
+    a["rf"] = rng.uniform(0.4, 1.2, face).astype(f)
+    a["mh"] = rng.uniform(0.7, 1.4, mass).astype(f)
+    a["mf"] = rng.uniform(0.7, 1.4, face).astype(f)
+    a["khh"] = rng.uniform(0.5, 80.0, face).astype(f)
+    a["khv"] = rng.uniform(0.5, 80.0, face).astype(f)
+    for n, s in (("gz", (nj, ni)), ("rgz", (nj, ni)), ("rgzu", (nj, ni + 1)), ("rgzv", (nj + 1, ni))):
+        a[n] = np.ones(s, f)
+    for n, s in (("gx", face), ("gxu", (nk + 1, nj, ni + 1)), ("gy", face), ("gyv", (nk + 1, nj + 1, ni))):
+        a[n] = np.zeros(s, f)
+    a["thten1"] = rng.normal(0.0, 1.0e-3, mass).astype(f)
+    a["qten"] = rng.normal(0.0, 1.0e-6, (6, nk, nj, ni)).astype(f)
+    return a
+
+
+def make_turbs(reference: Path) -> None:
+    """turbs for theta and the six moisture rows through the reference's
+    CPU twin cpu_gm1_scalar_turbulence_inplace
+    (src/cm1core/cuda_gm1_scalar_turbulence.py:414) on flat metrics."""
+    sys.path.insert(0, str(reference / "src"))
+    from cm1core.cuda_gm1_scalar_turbulence import cpu_gm1_scalar_turbulence_inplace
+
+    for tag, (ni, nj, nk, seed) in TURBS_CASES.items():
+        a = turbs_fixture(ni, nj, nk, seed)
+        inputs = {f"in_{k}": v.copy() for k, v in a.items()}
+        cpu_gm1_scalar_turbulence_inplace(a, ni=ni, nj=nj, nk=nk, dx=128.0, dy=128.0, dz=40.0, dt=0.6)
+        outputs = {f"out_{k}": a[k].copy() for k in ("thten1", "qten")}
+        meta = dict(ni=ni, nj=nj, nk=nk, dx=128.0, dy=128.0, dz=40.0, dt=0.6)
+        np.savez_compressed(HERE / f"{tag}.npz", meta=json.dumps(meta), **inputs, **outputs)
+        print("wrote", tag)
+
+
+# (ni, nj, nk, seed): the reference's sealed damping selection (irdamp 1,
+# 15 km top, damping from 12 km, rdalpha 1/300) on a uniform 200 m column
+RAYLEIGH_CASES = {"rayleigh_9x7x75": (9, 7, 75, 81), "rayleigh_6x8x75": (6, 8, 75, 82)}
+
+
+def make_rayleigh(reference: Path) -> None:
+    """The damping coefficients and the held tendencies through the
+    reference's own CPU code: cpu_build_rayleigh_coefficients on the one-halo
+    heights of a uniform 200 m, 75-level column, and cpu_rayleigh_held_inplace
+    (src/cm1core/cuda_rayleigh_held.py:213, :264) on seeded winds and theta."""
+    sys.path.insert(0, str(reference / "src"))
+    from cm1core.cuda_rayleigh_held import cpu_build_rayleigh_coefficients, cpu_rayleigh_held_inplace
+
+    f = np.float32
+    for tag, (ni, nj, nk, seed) in RAYLEIGH_CASES.items():
+        rng = np.random.default_rng(seed)
+        zf1 = (np.arange(nk + 1) * 200.0).astype(f)
+        zh1 = ((np.arange(nk) + 0.5) * 200.0).astype(f)
+        zh = np.ascontiguousarray(np.broadcast_to(zh1[:, None, None], (nk, nj + 2, ni + 2)))
+        zf = np.ascontiguousarray(np.broadcast_to(zf1[:, None, None], (nk + 1, nj + 2, ni + 2)))
+        co = cpu_build_rayleigh_coefficients(zh, zf)
+        a = {"tauh": co.tauh, "taus": co.taus, "tauf": co.tauf,
+             "u0": rng.normal(5.0, 8.0, nk).astype(f), "v0": rng.normal(0.0, 4.0, nk).astype(f),
+             "ua": rng.normal(6.0, 9.0, (nk, nj, ni + 1)).astype(f),
+             "va": rng.normal(0.0, 5.0, (nk, nj + 1, ni)).astype(f),
+             "wa": rng.normal(0.0, 2.0, (nk, nj, ni)).astype(f), "tha": rng.normal(0.0, 2.0, (nk, nj, ni)).astype(f),
+             "uten1": np.zeros((nk, nj, ni + 1), f), "vten1": np.zeros((nk, nj + 1, ni), f),
+             "wten1": np.zeros((nk, nj, ni), f), "thten1": np.zeros((nk, nj, ni), f)}
+        inputs = {f"in_{k}": v.copy() for k, v in a.items()}
+        cpu_rayleigh_held_inplace(a, ni=ni, nj=nj, nk=nk)
+        outputs = {f"out_{k}": a[k].copy() for k in ("uten1", "vten1", "wten1", "thten1")}
+        meta = dict(ni=ni, nj=nj, nk=nk, dz=200.0, damping_start_m=12000.0, rdalpha=0.0033333333333)
+        np.savez_compressed(HERE / f"{tag}.npz", meta=json.dumps(meta), zh=zh1, zf=zf1, **inputs, **outputs)
+        print("wrote", tag)
+
+
+IDISS_CASES = {"idiss_7x6x9": (7, 6, 9, 91)}
+
+
+def make_idiss(reference: Path) -> None:
+    """The dissipative heating cell by cell through the reference's own
+    scalar mirror cpu_idiss_cell_f32 (src/cm1core/eqtset2_energy_terms.py:176)
+    on seeded dissipation rates, pressures and six moisture rows."""
+    sys.path.insert(0, str(reference / "src"))
+    from cm1core.eqtset2_energy_terms import cpu_idiss_cell_f32
+
+    f = np.float32
+    for tag, (ni, nj, nk, seed) in IDISS_CASES.items():
+        rng = np.random.default_rng(seed)
+        a = {"dissten": rng.uniform(0.0, 0.05, (nk + 1, nj, ni)).astype(f),
+             "pi0": np.linspace(1.0, 0.55, nk).astype(f), "ppi": rng.normal(0.0, 2e-3, (nk, nj, ni)).astype(f),
+             "qa": np.abs(rng.normal(0.0, 3e-3, (6, nk, nj, ni))).astype(f),
+             "thten1": rng.normal(0.0, 1e-3, (nk, nj, ni)).astype(f)}
+        out = a["thten1"].copy()
+        for k in range(nk):
+            for j in range(nj):
+                for i in range(ni):
+                    q = a["qa"][:, k, j, i]
+                    r = cpu_idiss_cell_f32(thten1=float(out[k, j, i]), dissten_lower=float(a["dissten"][k, j, i]),
+                                           dissten_upper=float(a["dissten"][k + 1, j, i]), pi0=float(a["pi0"][k]),
+                                           ppi=float(a["ppi"][k, j, i]), qv=float(q[0]), qc=float(q[1]),
+                                           qr=float(q[2]), qi=float(q[3]), qs=float(q[4]), qg=float(q[5]))
+                    out[k, j, i] = r["thten1"]
+        np.savez_compressed(HERE / f"{tag}.npz", meta=json.dumps(dict(ni=ni, nj=nj, nk=nk)),
+                            **{f"in_{k}": v for k, v in a.items()}, out_thten1=out)
+        print("wrote", tag)
+
+
 def main() -> None:
     p = argparse.ArgumentParser()
     p.add_argument("--reference", type=Path, required=True, help="root of the reference source tree")
-    p.add_argument("what", choices=("small", "c1", "advection", "kessler", "tke", "rk", "bridge", "wk", "limits", "closure", "tkeevo", "momentum", "terrainopen", "kesslerstep", "fills", "vertical", "warmrain", "apmasscon", "stress"))
+    p.add_argument("what", choices=("small", "c1", "advection", "kessler", "tke", "rk", "bridge", "wk", "limits", "closure", "tkeevo", "momentum", "terrainopen", "kesslerstep", "fills", "vertical", "warmrain", "apmasscon", "stress", "turbs", "rayleigh", "idiss"))
     p.add_argument("--checkpoints", type=int, nargs="+", default=[1])
     args = p.parse_args()
     if args.what == "small":
@@ -1329,6 +1447,12 @@ def main() -> None:
         make_apmasscon(args.reference)
     elif args.what == "stress":
         make_stress(args.reference)
+    elif args.what == "turbs":
+        make_turbs(args.reference)
+    elif args.what == "rayleigh":
+        make_rayleigh(args.reference)
+    elif args.what == "idiss":
+        make_idiss(args.reference)
     else:
         make_c1(args.reference, sorted(set(args.checkpoints)))
 

@@ -60,7 +60,7 @@ def test_whole_step_struct_order_matches_header():
 
     assert _header_fields("gm1b_moist_state") == list(NATIVE_STATE_NAMES)
     assert _header_fields("gm1b_moist_metrics") == list(NATIVE_METRIC_NAMES)
-    assert ctypes.sizeof(_NativeConfig) == 4 * (3 + 4 + 1 + 2 + 4 + 3)
+    assert ctypes.sizeof(_NativeConfig) == 4 * (3 + 4 + 1 + 2 + 4 + 7)
 
 
 def test_whole_step_entry_rejects_bad_arguments_without_a_device():

@@ -4,7 +4,10 @@ halo exchange (in-process and over two gloo ranks) leaves every halo cell of
 index-coded arrays equal to the single domain's; and the oracle's composed
 moist step, decomposed over 2x1 and 2x2 subdomains with a 32-cell halo and
 exchanged after every large step, leaves interiors word-identical to the
-single domain's after 3 steps (with apmasscon off: the dry-mass correction
+single domain's after 3 steps, the stretched column also with the SGS
+stress, scalar diffusion, Rayleigh damping and dissipative heating held
+tendencies on (with
+apmasscon off: the dry-mass correction
 is a domain-wide reduction; the FP64 budgets excepted: they accumulate
 per widened subdomain; a lateral-boundary history is compared on the rank
 that holds that edge of the domain - elsewhere it belongs to a halo's outer
@@ -38,13 +41,15 @@ def compared(s, px, py):
     return tuple(n for n in COMPARED if n not in EDGE or EDGE[n](s, px, py))
 
 
-def _cfg(ni, nj, stretched=False):
+def _cfg(ni, nj, stretched=False, sgs_diffusion=False):
     column = SimpleNamespace(ztop_m=20800.0, str_bot_m=200.0, str_top_m=15800.0, dz_bot_m=20.0,
                              dz_top_m=500.0) if stretched else None
     nk, dx, dz, dt, ns = (80, 100.0, 100.0, 0.6, 8) if stretched else (12, 1000.0, 250.0, 5.0, 10)
     # the dry-mass correction is a domain-wide reduction: off in a decomposed run
     return SimpleNamespace(ni=ni, nj=nj, nk=nk, dx=dx, dy=dx, dz=dz, dt=dt, nsound=ns, alph=0.60, kdiv=0.10,
-                           lateral_sides=(2, 2, 2, 2), obc=0x2222, column=column, apmasscon=False)
+                           lateral_sides=(2, 2, 2, 2), obc=0x2222, column=column, apmasscon=False,
+                           sgs_diffusion=sgs_diffusion, rayleigh=sgs_diffusion,
+                           dissipative_heating=sgs_diffusion)
 
 
 def _start(cfg):
@@ -126,9 +131,10 @@ def _decomposed_oracle(cfg, host, metrics, subs, steps):
     return runs
 
 
-@pytest.mark.parametrize("px,py,stretched", [(2, 1, False), (2, 2, False), (2, 1, True)])
-def test_decomposed_oracle_composition_is_the_single_domain(px, py, stretched):
-    cfg = _cfg(80 if px > 1 else 40, 72 if py > 1 else 24, stretched)
+@pytest.mark.parametrize("px,py,stretched,stress", [(2, 1, False, False), (2, 2, False, False), (2, 1, True, False),
+                                                    (1, 2, True, True)])
+def test_decomposed_oracle_composition_is_the_single_domain(px, py, stretched, stress):
+    cfg = _cfg(80 if px > 1 else 40, 72 if py > 1 else 24, stretched, stress)
     host, metrics = _start(cfg)
     single = OracleMoistStep(cfg, {k: v.copy() for k, v in host.items()}, {k: v.copy() for k, v in metrics.items()})
     subs = partition(cfg.ni, cfg.nj, px, py, HALO)

@@ -3,7 +3,9 @@ run of the same operators (the oracle's composition with every binary32
 operation evaluated in binary64, oracle/fp64_twin.py), after 1 and 10 large
 steps, on the uniform column (configuration 2's physics on a 24x20x16 grid)
 and on the 80-level stretched supercell column of configuration 3 (48x40
-plane), starts with cloud and rain in the bubble.
+plane; also with the SGS stress, scalar diffusion and Rayleigh damping held
+tendencies on),
+starts with cloud and rain in the bubble.
 
 Stated tolerance (tests/fp64_common.py): the GPU's error against the FP64
 run, each field on its own scale, at most four times the binary32 oracle's
@@ -32,6 +34,13 @@ CASES = {
     "stretched-48x40x80": (MoistStepConfig(48, 40, 80, 100.0, 100.0, 100.0, 0.6, 8, column=SUPERCELL_STRETCHED_COLUMN),
                            dict(seed=7, bubble_radius_m=(1500.0, 800.0), bubble_center_z_m=800.0,
                                 bubble_cloud=1.0e-3, bubble_rain=5.0e-4)),
+    # the same column with the closure's held tendencies (SGS stress, scalar
+    # diffusion, upper Rayleigh damping, dissipative heating)
+    "stretched-48x40x80-held": (MoistStepConfig(48, 40, 80, 100.0, 100.0, 100.0, 0.6, 8,
+                                                column=SUPERCELL_STRETCHED_COLUMN, sgs_diffusion=True,
+                                                rayleigh=True, dissipative_heating=True),
+                               dict(seed=7, bubble_radius_m=(1500.0, 800.0), bubble_center_z_m=800.0,
+                                    bubble_cloud=1.0e-3, bubble_rain=5.0e-4)),
 }
 
 

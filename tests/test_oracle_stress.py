@@ -142,3 +142,97 @@ def test_a_sheared_u_alone_drives_only_u():
     assert np.any(a["uten"])
     assert not np.any(a["vten"])
     assert not np.any(a["wten"])
+
+
+# ------------------------------------------------------------------ turbs
+# The reference's CPU twin of turbs, cpu_gm1_scalar_turbulence_inplace
+# (src/cm1core/cuda_gm1_scalar_turbulence.py:414), runs the terrain texts;
+# on flat metrics (gz = rgz = 1, zero slopes) with dx = dy = 128 m every
+# product with 1/dx is exact and its terrain terms add exact zeros, so the
+# flat text's words are the twin's: pinned bit for bit.
+TURBS_CASES = ("turbs_8x7x6", "turbs_11x9x10")
+
+
+@pytest.mark.parametrize("tag", TURBS_CASES)
+def test_flat_turbs_is_the_twin_word_for_word(tag):
+    meta, inp, out = _load(tag)
+    a = {k: np.ascontiguousarray(v).copy() for k, v in inp.items()}
+    ost.flat_scalar_turbulence(a, ni=meta["ni"], nj=meta["nj"], nk=meta["nk"], numq=6, dx=meta["dx"], dy=meta["dy"],
+                               dz=meta["dz"], dt=meta["dt"])
+    for n in ("thten1", "qten"):
+        assert np.array_equal(a[n].view(np.uint32), out[n].view(np.uint32)), n
+        assert np.any(a[n] != inp[n]), n
+
+
+def test_turbs_of_uniform_scalars_only_rounds():
+    """Horizontally and vertically uniform theta and moisture: no flux, and
+    the implicit solve returns the field to within its rounding."""
+    ni, nj, nk = 7, 6, 9
+    rng = np.random.default_rng(9)
+    f = np.float32
+    a = {"th0": np.full(nk, 300.0, f), "tha": np.full((nk, nj, ni), 2.5, f),
+         "qa": np.full((3, nk, nj, ni), 4.0e-3, f), "rho": rng.uniform(0.5, 1.1, (nk, nj, ni)).astype(f),
+         "rf": rng.uniform(0.5, 1.1, (nk + 1, nj, ni)).astype(f), "mh": np.ones((nk, nj, ni), f),
+         "mf": np.ones((nk + 1, nj, ni), f), "khh": rng.uniform(1, 50, (nk + 1, nj, ni)).astype(f),
+         "khv": rng.uniform(1, 50, (nk + 1, nj, ni)).astype(f), "thten1": np.zeros((nk, nj, ni), f),
+         "qten": np.zeros((3, nk, nj, ni), f)}
+    a["rr"] = (f(1.0) / a["rho"]).astype(f)
+    ost.flat_scalar_turbulence(a, ni=ni, nj=nj, nk=nk, numq=3, dx=100.0, dy=100.0, dz=50.0, dt=0.6)
+    assert np.max(np.abs(a["thten1"])) <= 8 * np.spacing(f(2.5)) / 0.6 * 3.0
+    assert np.max(np.abs(a["qten"])) <= 8 * np.spacing(f(4.0e-3)) / 0.6 * 3.0
+
+
+# --------------------------------------------------------------- Rayleigh
+# cpu_build_rayleigh_coefficients and cpu_rayleigh_held_inplace
+# (src/cm1core/cuda_rayleigh_held.py:264, :213) on the reference's sealed
+# damping selection: the coefficient builders (the oracle's and the
+# package's host set-up) and the held tendencies pinned bit for bit.
+RAYLEIGH_CASES = ("rayleigh_9x7x75", "rayleigh_6x8x75")
+
+
+@pytest.mark.parametrize("tag", RAYLEIGH_CASES)
+def test_rayleigh_coefficients_and_held_tendencies_are_the_twins(tag):
+    from gm1_b200.rayleigh import build_rayleigh_coefficients
+
+    z = np.load(GOLDEN / f"{tag}.npz")
+    meta, inp, out = _load(tag)
+    for tau in (ost.rayleigh_coefficients(z["zh"], z["zf"], damping_start_m=meta["damping_start_m"]),
+                build_rayleigh_coefficients(z["zh"], z["zf"], damping_start_m=meta["damping_start_m"])):
+        for got, name in zip(tau, ("tauh", "taus", "tauf")):
+            assert np.array_equal(got.view(np.uint32), inp[name][:, 0, 0].view(np.uint32)), name
+    assert np.count_nonzero(inp["tauh"][:, 0, 0]) > 0
+    a = {k: np.ascontiguousarray(v).copy() for k, v in inp.items()}
+    ost.rayleigh_held(a, ni=meta["ni"], nj=meta["nj"], nk=meta["nk"], rdalpha=meta["rdalpha"])
+    for n in ("uten1", "vten1", "wten1", "thten1"):
+        assert np.array_equal(a[n].view(np.uint32), out[n].view(np.uint32)), n
+    # the column-profile layout gives the same words on laterally uniform tau
+    b = {k: np.ascontiguousarray(v).copy() for k, v in inp.items()}
+    for name in ("tauh", "taus", "tauf"):
+        b[name] = np.ascontiguousarray(inp[name][:, 0, 0])
+    ost.rayleigh_held(b, ni=meta["ni"], nj=meta["nj"], nk=meta["nk"], rdalpha=meta["rdalpha"], profiles=True)
+    for n in ("uten1", "vten1", "wten1", "thten1"):
+        assert np.array_equal(b[n].view(np.uint32), out[n].view(np.uint32)), n
+
+
+def test_rayleigh_add_momentum_is_the_held_sum():
+    meta, inp, out = _load("rayleigh_9x7x75")
+    a = {k: np.ascontiguousarray(v).copy() for k, v in inp.items()}
+    rng = np.random.default_rng(3)
+    held = {n: rng.normal(0.0, 1e-3, a[n].shape).astype(np.float32) for n in ("uten1", "vten1", "wten1")}
+    for n, v in held.items():
+        a[n][:] = v
+    ost.rayleigh_held(a, ni=meta["ni"], nj=meta["nj"], nk=meta["nk"], rdalpha=meta["rdalpha"], add_momentum=True)
+    for n, v in held.items():
+        assert np.array_equal(a[n], (out[n] + v).astype(np.float32)), n
+    assert np.array_equal(a["thten1"], out["thten1"])
+
+
+# ------------------------------------------------------ dissipative heating
+def test_dissipative_heating_is_the_twins_cell_formula():
+    """cpu_idiss_cell_f32 (src/cm1core/eqtset2_energy_terms.py:176), the
+    reference's scalar mirror, cell by cell (golden idiss_7x6x9.npz)."""
+    meta, inp, out = _load("idiss_7x6x9")
+    a = {k: np.ascontiguousarray(v).copy() for k, v in inp.items()}
+    ost.dissipative_heating(a, ni=meta["ni"], nj=meta["nj"], nk=meta["nk"])
+    assert np.array_equal(a["thten1"].view(np.uint32), out["thten1"].view(np.uint32))
+    assert np.any(a["thten1"] != inp["thten1"])

@@ -113,3 +113,80 @@ def test_refusals():
         launch_cuda_flat_gettau(bad, ni=ni, nj=nj, nk=nk)
     with pytest.raises(ValueError):
         launch_cuda_flat_momentum_stress({**d, "vten": d["uten"]}, ni=ni, nj=nj, nk=nk, dx=DX, dy=DX, rdz=rdz, dt=DT)
+
+
+# ------------------------------------------------------------------ turbs
+def _turbs_inputs(ni, nj, nk, numq, seed):
+    rng = np.random.default_rng(seed)
+    f = np.float32
+    mh, mf, rdz = _column(nk)
+    mass, face = (nk, nj, ni), (nk + 1, nj, ni)
+    a = {"th0": np.linspace(300.0, 345.0, nk).astype(f), "tha": rng.normal(0.0, 2.0, mass).astype(f),
+         "qa": np.abs(rng.normal(0.0, 5e-3, (6, nk, nj, ni))).astype(f),
+         "rho": (np.linspace(1.15, 0.2, nk, dtype=f)[:, None, None] * rng.uniform(0.98, 1.02, mass)).astype(f),
+         "rf": (np.linspace(1.16, 0.19, nk + 1, dtype=f)[:, None, None] * rng.uniform(0.98, 1.02, face)).astype(f),
+         "mh": np.broadcast_to(mh[:, None, None], mass).astype(f), "mf": np.broadcast_to(mf[:, None, None], face).astype(f),
+         "khh": rng.uniform(0.0, 90.0, face).astype(f), "khv": rng.uniform(0.0, 90.0, face).astype(f),
+         "thten1": rng.normal(0.0, 1e-3, mass).astype(f), "qten": rng.normal(0.0, 1e-7, (numq, nk, nj, ni)).astype(f)}
+    a["rr"] = (f(1.0) / a["rho"]).astype(f)
+    return a, float(np.float32(1.0) / np.float32(rdz))
+
+
+@pytest.mark.parametrize("ni,nj,nk,numq,seed", [(64, 48, 80, 3, 11), (13, 9, 7, 6, 12), (3, 4, 3, 1, 13),
+                                                (17, 3, 5, 0, 14)])
+def test_flat_turbs_is_the_oracle_word_for_word(ni, nj, nk, numq, seed):
+    from gm1_b200.stress import launch_cuda_flat_scalar_turbulence
+
+    a, dz = _turbs_inputs(ni, nj, nk, numq, seed)
+    d = _dev(a)
+    ost.flat_scalar_turbulence(a, ni=ni, nj=nj, nk=nk, numq=numq, dx=DX, dy=DX, dz=dz, dt=DT)
+    launch_cuda_flat_scalar_turbulence(d, ni=ni, nj=nj, nk=nk, numq=numq, dx=DX, dy=DX, dz=dz, dt=DT)
+    torch.cuda.synchronize()
+    _same(d, a, ("thten1", "qten"))
+    assert np.array_equal(d["qa"].cpu().numpy(), a["qa"])
+
+
+# --------------------------------------------------------------- Rayleigh
+@pytest.mark.parametrize("profiles,add_momentum", [(False, False), (True, False), (True, True)])
+def test_rayleigh_held_is_the_oracle_word_for_word(profiles, add_momentum):
+    from gm1_b200.rayleigh import build_rayleigh_coefficients, launch_cuda_rayleigh_held
+
+    ni, nj, nk = 70, 33, 80
+    rng = np.random.default_rng(21)
+    f = np.float32
+    zf = np.concatenate([[0.0], np.cumsum(np.linspace(20.0, 500.0, nk))]).astype(f)
+    zh = (0.5 * (zf[:-1] + zf[1:])).astype(f)
+    tauh, taus, tauf = build_rayleigh_coefficients(zh, zf, damping_start_m=15000.0)
+    if not profiles:
+        tauh, taus, tauf = (np.ascontiguousarray(np.broadcast_to(t[:, None, None], (t.shape[0], nj + 2, ni + 2)))
+                            for t in (tauh, taus, tauf))
+    a = {"tauh": tauh, "taus": taus, "tauf": tauf, "u0": rng.normal(5, 8, nk).astype(f),
+         "v0": rng.normal(0, 4, nk).astype(f), "ua": rng.normal(6, 9, (nk, nj, ni + 1)).astype(f),
+         "va": rng.normal(0, 5, (nk, nj + 1, ni)).astype(f), "wa": rng.normal(0, 2, (nk, nj, ni)).astype(f),
+         "tha": rng.normal(0, 2, (nk, nj, ni)).astype(f), "uten1": rng.normal(0, 1e-3, (nk, nj, ni + 1)).astype(f),
+         "vten1": rng.normal(0, 1e-3, (nk, nj + 1, ni)).astype(f), "wten1": rng.normal(0, 1e-3, (nk, nj, ni)).astype(f),
+         "thten1": rng.normal(0, 1e-3, (nk, nj, ni)).astype(f)}
+    d = _dev(a)
+    ost.rayleigh_held(a, ni=ni, nj=nj, nk=nk, rdalpha=1.0 / 300.0, profiles=profiles, add_momentum=add_momentum)
+    launch_cuda_rayleigh_held(d, ni=ni, nj=nj, nk=nk, rdalpha=1.0 / 300.0, profiles=profiles,
+                              add_momentum=add_momentum)
+    torch.cuda.synchronize()
+    _same(d, a, ("uten1", "vten1", "wten1", "thten1"))
+    assert np.count_nonzero(a["thten1"]) > 0
+
+
+# ---------------------------------------------------- dissipative heating
+def test_dissipative_heating_is_the_oracle_word_for_word():
+    from gm1_b200.stress import launch_cuda_dissipative_heating
+
+    ni, nj, nk = 70, 33, 80
+    rng = np.random.default_rng(31)
+    f = np.float32
+    a = {"dissten": rng.uniform(0.0, 0.05, (nk + 1, nj, ni)).astype(f), "pi0": np.linspace(1.0, 0.4, nk).astype(f),
+         "ppi": rng.normal(0.0, 2e-3, (nk, nj, ni)).astype(f), "qa": np.abs(rng.normal(0, 3e-3, (6, nk, nj, ni))).astype(f),
+         "thten1": rng.normal(0.0, 1e-3, (nk, nj, ni)).astype(f)}
+    d = _dev(a)
+    ost.dissipative_heating(a, ni=ni, nj=nj, nk=nk)
+    launch_cuda_dissipative_heating(d, ni=ni, nj=nj, nk=nk)
+    torch.cuda.synchronize()
+    _same(d, a, ("thten1",))
