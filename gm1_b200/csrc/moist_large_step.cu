@@ -64,6 +64,7 @@ struct gm1b_moist_step {
     size_t kessler_ws_bytes = 0;
     void *mass_ws = nullptr;  // the dry-mass correction's level sums
     float *stress_buf = nullptr;     // the SGS stress scratch (strains, stresses, held tendencies)
+    float *turbs_work = nullptr;     // the scalar turbulence's workspace
     gm1b_flat_stress_arrays stress{};
     int32_t *status_acc = nullptr;  // 8 words
     float *courant = nullptr;       // 1 word
@@ -275,7 +276,7 @@ int held_tendencies(Step &h, cudaStream_t st) {
         // turbs for theta and the moisture rows into the held thten1/qten the
         // eqtset 2 composition then reads (solve1.F:1169-1233)
         const gm1b_flat_scalar_turbulence_arrays ta{s.th0, s.tha, s.qa, s.rho, s.rr, s.rf, h.m.mh, h.m.mf,
-                                                    s.khh, s.khv, s.thheld, s.qheld};
+                                                    s.khh, s.khv, s.thheld, s.qheld, h.turbs_work};
         TRY(gm1b_flat_scalar_turbulence(c.ni, c.nj, c.nk, kNumq, &ta, c.dx, c.dy, c.dz, c.dt, st));
     }
     gm1b_held_arrays a{s.th0_3d, s.pi0_3d, s.rho, s.pp3d_c, s.tha, s.qa, s.qpten, s.qtten, s.qvten, s.qcten,
@@ -581,7 +582,7 @@ void release(Step *h) {
     for (auto &e : h->ev)
         if (e) cudaEventDestroy(e);
     void *bufs[] = {h->kessler_ws, h->status_acc, h->courant, h->courant_keys, h->ones_i, h->ones_j, h->mh_col,
-                    h->mass_ws, h->stress_buf};
+                    h->mass_ws, h->stress_buf, h->turbs_work};
     for (void *b : bufs)
         if (b) cudaFree(b);
     delete h;
@@ -663,6 +664,11 @@ extern "C" int32_t gm1b_moist_step_create(const gm1b_moist_step_config *config, 
     if (good) good = ok(cudaMalloc(&h->mh_col, (size_t)c.nk * sizeof(float)), "cudaMalloc");
     if (good && c.apmasscon)
         good = ok(cudaMalloc(&h->mass_ws, gm1b_apmasscon_workspace_bytes(c.nk)), "cudaMalloc (mass workspace)");
+    if (good && c.sgs_diffusion)
+        good = ok(cudaMalloc(&h->turbs_work,
+                             (size_t)gm1b_flat_scalar_turbulence_workspace_words(c.ni, c.nj, c.nk, kNumq) *
+                                 sizeof(float)),
+                  "cudaMalloc (scalar turbulence workspace)");
     if (good && (c.sgs_diffusion || c.rayleigh)) {
         // strains and stresses, then the held u, v, w (the layouts of
         // gm1b_flat_stress_arrays), carved from one allocation

@@ -340,118 +340,149 @@ __global__ void __launch_bounds__(kCT) flat_turbw_kernel(StressArgs a) {
 
 
 // ---------------------------------------------------------- turbs (flat)
-// theta ((th0 - 300) + tha) and numq moisture rows; blockIdx.z picks the
-// scalar (0 theta, 1.. the rows).  The open-halo copies of the reference's
-// pad/pack texts are index clamps here, so no halo array is written; the x
-// and y face fluxes of each level are formed where the back substitution
-// needs them.
+// theta ((th0 - 300) + tha) and numq moisture rows.  The open-halo copies of
+// the reference's pad/pack texts are index clamps here, so no halo array is
+// written.  Two passes: the horizontal pass forms, per cell, the x and y
+// flux divergence tx + ty of every scalar into the workspace (each face's
+// factor (-0.125*(rho_l + rho_r))*(the four khh) formed once and shared by
+// all scalars); the column pass solves turbsz's tridiagonal for each scalar
+// and adds ((tx + ty) + tz)*rr, the reference's sum in its order.
 struct TurbsArgs {
     const float *th0, *tha, *qa, *rho, *rr, *rf, *mh, *mf, *khh, *khv;
-    float *thten, *qten;
-    int ni, nj, nk;
+    float *thten, *qten, *work;
+    int ni, nj, nk, nsc;
     float dx, dy, dz, dt;
 };
 
 __device__ __forceinline__ float tcell(const TurbsArgs &a, const float *p, int k, int j, int i) {
     return p[o3(k, clampi(j, a.nj), clampi(i, a.ni), a.nj, a.ni)];
 }
-// the open-halo scalar at a clamped cell; q == nullptr: theta
-__device__ __forceinline__ float sval(const TurbsArgs &a, const float *q, int k, int j, int i) {
+// the open-halo scalar sc (0 theta, 1.. the moisture rows) at a clamped cell
+__device__ __forceinline__ float sval(const TurbsArgs &a, int sc, int k, int j, int i) {
     const unsigned p = o3(k, clampi(j, a.nj), clampi(i, a.ni), a.nj, a.ni);
-    if (q != nullptr) return q[p];
+    if (sc > 0) return a.qa[(size_t)(sc - 1) * ((size_t)a.ni * a.nj * a.nk) + p];
     return (a.th0[k] - 300.0f) + a.tha[p];
 }
-// x flux through the face between cells f-1 and f
-__device__ __forceinline__ float turbs_fx(const TurbsArgs &a, const float *q, int k, int j, int f, float rx) {
+// the face factor (-0.125*(rho(a)+rho(a-1)))*((khh(k)+khh(k)) + (khh(k+1)+khh(k+1)))
+// across x face f (cells f-1, f) or y face f (rows f-1, f)
+__device__ __forceinline__ float fac_x(const TurbsArgs &a, int k, int j, int f) {
     const float den = tcell(a, a.rho, k, j, f) + tcell(a, a.rho, k, j, f - 1);
     const float kh = (tcell(a, a.khh, k, j, f) + tcell(a, a.khh, k, j, f - 1)) +
                      (tcell(a, a.khh, k + 1, j, f) + tcell(a, a.khh, k + 1, j, f - 1));
-    return (((-0.125f * den) * kh) * (sval(a, q, k, j, f) - sval(a, q, k, j, f - 1))) * rx;
+    return (-0.125f * den) * kh;
 }
-// y flux through the face between rows f-1 and f
-__device__ __forceinline__ float turbs_fy(const TurbsArgs &a, const float *q, int k, int f, int i, float ry) {
+__device__ __forceinline__ float fac_y(const TurbsArgs &a, int k, int f, int i) {
     const float den = tcell(a, a.rho, k, f, i) + tcell(a, a.rho, k, f - 1, i);
     const float kh = (tcell(a, a.khh, k, f, i) + tcell(a, a.khh, k, f - 1, i)) +
                      (tcell(a, a.khh, k + 1, f, i) + tcell(a, a.khh, k + 1, f - 1, i));
-    return (((-0.125f * den) * kh) * (sval(a, q, k, f, i) - sval(a, q, k, f - 1, i))) * ry;
+    return (-0.125f * den) * kh;
 }
 
-__global__ void __launch_bounds__(kCT) flat_turbs_kernel(TurbsArgs a) {
+__global__ void __launch_bounds__(kCT) flat_turbs_horizontal_kernel(TurbsArgs a) {
+    const int i = blockIdx.x * kCX + threadIdx.x, j = blockIdx.y * kCY + threadIdx.y, k = blockIdx.z;
+    const int ni = a.ni, nj = a.nj;
+    if (i >= ni || j >= nj) return;
+    const size_t n = (size_t)ni * nj * a.nk, p = o3(k, j, i, nj, ni);
+    const float rx = 1.0f / a.dx, ry = 1.0f / a.dy;
+    const bool xin = !(i == 0 || i + 1 == ni), yin = !(j == 0 || j + 1 == nj);
+    float fw = 0.0f, fe = 0.0f, fs = 0.0f, fn = 0.0f;
+    if (xin) {
+        fw = fac_x(a, k, j, i);
+        fe = fac_x(a, k, j, i + 1);
+    }
+    if (yin) {
+        fs = fac_y(a, k, j, i);
+        fn = fac_y(a, k, j + 1, i);
+    }
+    for (int sc = 0; sc < a.nsc; ++sc) {
+        float tx = 0.0f, ty = 0.0f;
+        const float s0 = sval(a, sc, k, j, i);
+        if (xin) {
+            const float xw = (fw * (s0 - sval(a, sc, k, j, i - 1))) * rx;
+            const float xe = (fe * (sval(a, sc, k, j, i + 1) - s0)) * rx;
+            tx = -((xe - xw) * rx);
+        }
+        if (yin) {
+            const float ys = (fs * (s0 - sval(a, sc, k, j - 1, i))) * ry;
+            const float yn = (fn * (sval(a, sc, k, j + 1, i) - s0)) * ry;
+            ty = -((yn - ys) * ry);
+        }
+        a.work[(size_t)sc * n + p] = tx + ty;
+    }
+}
+
+__global__ void __launch_bounds__(kCT) flat_turbs_column_kernel(TurbsArgs a) {
     extern __shared__ float s_col[];
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kCX + tx;
     const int ni = a.ni, nj = a.nj, nk = a.nk;
     const int i = blockIdx.x * kCX + tx, j = blockIdx.y * kCY + ty;
     if (i >= ni || j >= nj) return;
     const size_t n = (size_t)ni * nj * nk;
-    const int sp = (int)blockIdx.z;
-    const float *q = sp == 0 ? nullptr : a.qa + (size_t)(sp - 1) * n;
-    float *target = sp == 0 ? a.thten : a.qten + (size_t)(sp - 1) * n;
     const unsigned col = (unsigned)j * ni + i, lev = (unsigned)nj * ni;
     float *cp = s_col, *dp = s_col + (size_t)nk * kCT;
 #define CP(k) cp[(unsigned)(k) * kCT + tid]
 #define DP(k) dp[(unsigned)(k) * kCT + tid]
 #define PF(p, k) p[(unsigned)(k) * lev + col]
-#define SC(k) sval(a, q, k, j, i)
 #define COEF(F, K) ((((PF(a.khv, F) * PF(a.mf, F)) * PF(a.rf, F)) * PF(a.mh, K)) * PF(a.rr, K))
-    const float rx = 1.0f / a.dx, ry = 1.0f / a.dy, rz = 1.0f / a.dz, dt = a.dt, rdt = 1.0f / dt;
+    const float rz = 1.0f / a.dz, dt = a.dt, rdt = 1.0f / dt;
     const float tema = (((-1.0f * dt) * 1.0f) * rz) * rz;
     const float temb = ((dt * 0.0f) * rz) * rz;
     const float temc = dt * rz;
-    float sm = SC(0), sk = SC(1);  // scalar at k-1 and k of the next level
-    float r2 = COEF(1, 0);
-    float cfc = tema * r2, cfb = 1.0f - cfc;
-    float ex = (-r2) * sm + r2 * sk;
-    float bc = ((temc * 0.0f) * PF(a.mh, 0)) * PF(a.rr, 0);
-    float cfd = (sm + temb * ex) + bc;
-    float tem = 1.0f / cfb;
-    float cprev = (-cfc) * tem, dprev = cfd * tem;
-    CP(0) = cprev;
-    DP(0) = dprev;
-    for (int k = 1; k + 1 < nk; ++k) {
-        const float r1 = COEF(k, k);
-        r2 = COEF(k + 1, k);
-        const float cfa = tema * r1;
-        cfc = tema * r2;
-        cfb = (1.0f - cfa) - cfc;
-        const float sp1 = SC(k + 1);
-        ex = (r1 * sm - (r1 + r2) * sk) + r2 * sp1;
-        cfd = sk + temb * ex;
-        tem = 1.0f / (cfa * cprev + cfb);
-        cprev = (-cfc) * tem;
-        dprev = (cfd - cfa * dprev) * tem;
-        CP(k) = cprev;
-        DP(k) = dprev;
-        sm = sk;
-        sk = sp1;
-    }
-    float sol;
-    {
-        const int k = nk - 1;
-        const float r1 = COEF(k, k), cfa = tema * r1;
-        cfb = 1.0f - cfa;
-        ex = r1 * sm - r1 * sk;
-        bc = ((temc * 0.0f) * PF(a.mh, k)) * PF(a.rr, k);
-        cfd = (sk + temb * ex) - bc;
-        tem = 1.0f / (cfa * cprev + cfb);
-        sol = (cfd - cfa * dprev) * tem;
-    }
-    for (int k = nk - 1; k >= 0; --k) {
-        if (k != nk - 1) sol = CP(k) * sol + DP(k);
-        const float tz = (PF(a.rho, k) * (sol - SC(k))) * rdt;
-        float tx = -((turbs_fx(a, q, k, j, i + 1, rx) - turbs_fx(a, q, k, j, i, rx)) * rx);
-        if (i == 0 || i + 1 == ni) tx = 0.0f;
-        float ty = -((turbs_fy(a, q, k, j + 1, i, ry) - turbs_fy(a, q, k, j, i, ry)) * ry);
-        if (j == 0 || j + 1 == nj) ty = 0.0f;
-        const unsigned p = (unsigned)k * lev + col;
-        target[p] = target[p] + ((tx + ty) + tz) * PF(a.rr, k);
+    for (int sc = 0; sc < a.nsc; ++sc) {
+        float *target = sc == 0 ? a.thten : a.qten + (size_t)(sc - 1) * n;
+        const float *h = a.work + (size_t)sc * n;
+#define SC(k) sval(a, sc, k, j, i)
+        float sm = SC(0), sk = SC(1);  // scalar at k-1 and k of the next level
+        float r2 = COEF(1, 0);
+        float cfc = tema * r2, cfb = 1.0f - cfc;
+        float ex = (-r2) * sm + r2 * sk;
+        float bc = ((temc * 0.0f) * PF(a.mh, 0)) * PF(a.rr, 0);
+        float cfd = (sm + temb * ex) + bc;
+        float tem = 1.0f / cfb;
+        float cprev = (-cfc) * tem, dprev = cfd * tem;
+        CP(0) = cprev;
+        DP(0) = dprev;
+        for (int k = 1; k + 1 < nk; ++k) {
+            const float r1 = COEF(k, k);
+            r2 = COEF(k + 1, k);
+            const float cfa = tema * r1;
+            cfc = tema * r2;
+            cfb = (1.0f - cfa) - cfc;
+            const float sp1 = SC(k + 1);
+            ex = (r1 * sm - (r1 + r2) * sk) + r2 * sp1;
+            cfd = sk + temb * ex;
+            tem = 1.0f / (cfa * cprev + cfb);
+            cprev = (-cfc) * tem;
+            dprev = (cfd - cfa * dprev) * tem;
+            CP(k) = cprev;
+            DP(k) = dprev;
+            sm = sk;
+            sk = sp1;
+        }
+        float sol;
+        {
+            const int k = nk - 1;
+            const float r1 = COEF(k, k), cfa = tema * r1;
+            cfb = 1.0f - cfa;
+            ex = r1 * sm - r1 * sk;
+            bc = ((temc * 0.0f) * PF(a.mh, k)) * PF(a.rr, k);
+            cfd = (sk + temb * ex) - bc;
+            tem = 1.0f / (cfa * cprev + cfb);
+            sol = (cfd - cfa * dprev) * tem;
+        }
+        for (int k = nk - 1; k >= 0; --k) {
+            if (k != nk - 1) sol = CP(k) * sol + DP(k);
+            const float tz = (PF(a.rho, k) * (sol - SC(k))) * rdt;
+            const unsigned p = (unsigned)k * lev + col;
+            target[p] = target[p] + (h[p] + tz) * PF(a.rr, k);
+        }
+#undef SC
     }
 #undef CP
 #undef DP
 #undef PF
-#undef SC
 #undef COEF
 }
-
 
 // ------------------------------------------------------ Rayleigh (upper)
 // irdamp = 1: uten1 = ((-rdalpha*0.5)*(tauh(i-1)+tauh(i)))*(ua - u0(k)), vten1
@@ -688,6 +719,11 @@ extern "C" int32_t gm1b_flat_sgs_stress(int32_t ni, int32_t nj, int32_t nk, cons
     return gm1b_flat_momentum_stress(ni, nj, nk, arrays, dx, dy, rdz, dt, stream);
 }
 
+extern "C" int64_t gm1b_flat_scalar_turbulence_workspace_words(int32_t ni, int32_t nj, int32_t nk, int32_t numq) {
+    if (ni < 1 || nj < 1 || nk < 1 || numq < 0) return 0;
+    return (int64_t)(numq + 1) * ni * nj * nk;
+}
+
 extern "C" int32_t gm1b_flat_scalar_turbulence(int32_t ni, int32_t nj, int32_t nk, int32_t numq,
                                                const gm1b_flat_scalar_turbulence_arrays *arrays, float dx, float dy,
                                                float dz, float dt, void *stream) {
@@ -696,7 +732,7 @@ extern "C" int32_t gm1b_flat_scalar_turbulence(int32_t ni, int32_t nj, int32_t n
         gm1b_set_error("gm1b_flat_scalar_turbulence: need arrays, ni >= 3, nj >= 3, nk >= 3, numq in 0..6");
         return GM1B_ERR_ARGUMENT;
     }
-    if ((double)(nk + 1) * nj * ni * 7 >= 4294967296.0 || (double)(nk + 1) * nj * ni >= 2147483648.0) {
+    if ((double)(nk + 1) * nj * ni >= 2147483648.0) {
         gm1b_set_error("gm1b_flat_scalar_turbulence: a %dx%dx%d grid is too large for 32-bit offsets", ni, nj, nk);
         return GM1B_ERR_ARGUMENT;
     }
@@ -705,9 +741,9 @@ extern "C" int32_t gm1b_flat_scalar_turbulence(int32_t ni, int32_t nj, int32_t n
         gm1b_set_error("gm1b_flat_scalar_turbulence: dx, dy, dz, dt must be finite and > 0");
         return GM1B_ERR_ARGUMENT;
     }
-    if (!all_set({s->th0, s->tha, s->rho, s->rr, s->rf, s->mh, s->mf, s->khh, s->khv, s->thten}) ||
+    if (!all_set({s->th0, s->tha, s->rho, s->rr, s->rf, s->mh, s->mf, s->khh, s->khv, s->thten, s->workspace}) ||
         (numq > 0 && !all_set({s->qa, s->qten}))) {
-        gm1b_set_error("gm1b_flat_scalar_turbulence: a required array is NULL");
+        gm1b_set_error("gm1b_flat_scalar_turbulence: a required array (or the workspace) is NULL");
         return GM1B_ERR_ARGUMENT;
     }
     const size_t smem = (size_t)2 * nk * kCT * sizeof(float);
@@ -715,14 +751,21 @@ extern "C" int32_t gm1b_flat_scalar_turbulence(int32_t ni, int32_t nj, int32_t n
         gm1b_set_error("gm1b_flat_scalar_turbulence: nk=%d exceeds the column solve's shared memory (nk <= 200)", nk);
         return GM1B_ERR_ARGUMENT;
     }
-    TRY(configure(flat_turbs_kernel, smem, "flat_turbs_kernel"));
+    TRY(configure(flat_turbs_column_kernel, smem, "flat_turbs_column_kernel"));
     TurbsArgs a{s->th0, s->tha, s->qa, s->rho, s->rr, s->rf, s->mh, s->mf, s->khh, s->khv, s->thten, s->qten,
-                ni, nj, nk, dx, dy, dz, dt};
+                s->workspace, ni, nj, nk, numq + 1, dx, dy, dz, dt};
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    ProfScope ps("flat_turbs_kernel", st);
-    flat_turbs_kernel<<<dim3((ni + kCX - 1) / kCX, (nj + kCY - 1) / kCY, numq + 1), dim3(kCX, kCY), smem, st>>>(a);
+    const dim3 tile(kCX, kCY), cols((ni + kCX - 1) / kCX, (nj + kCY - 1) / kCY);
+    {
+        ProfScope ps("flat_turbs_horizontal_kernel", st);
+        flat_turbs_horizontal_kernel<<<dim3(cols.x, cols.y, nk), tile, 0, st>>>(a);
+        ps.stop();
+        if (!launch_ok("flat_turbs_horizontal_kernel")) return GM1B_ERR_CUDA;
+    }
+    ProfScope ps("flat_turbs_column_kernel", st);
+    flat_turbs_column_kernel<<<cols, tile, smem, st>>>(a);
     ps.stop();
-    return launch_ok("flat_turbs_kernel") ? GM1B_OK : GM1B_ERR_CUDA;
+    return launch_ok("flat_turbs_column_kernel") ? GM1B_OK : GM1B_ERR_CUDA;
 }
 
 extern "C" int32_t gm1b_rayleigh_held(int32_t ni, int32_t nj, int32_t nk, const gm1b_rayleigh_held_arrays *arrays,

@@ -575,9 +575,12 @@ class MoistLargeStep:
             self.stress_arrays = {"u3d": s["uc"], "v3d": s["vc"], "w3d": s["wc"], "rho": s["rho"], "rf": s["rf"],
                                   "mh": m["mh"], "mf": m["mf"], "mh_profile": m["mh_profile"], "kmh": s["kmh"],
                                   "kmv": s["kmv"], **self.stress}
+            from .stress import scalar_turbulence_workspace
+
             self.turbs_arrays = {"th0": s["th0"], "tha": s["tha"], "qa": s["qa"], "rho": s["rho"], "rr": s["rr"],
                                  "rf": s["rf"], "mh": m["mh"], "mf": m["mf"], "khh": s["khh"], "khv": s["khv"],
-                                 "thten1": s["thheld"], "qten": s["qheld"]}
+                                 "thten1": s["thheld"], "qten": s["qheld"],
+                                 "workspace": scalar_turbulence_workspace(ni, nj, nk, NUMQ, dev)}
         if cfg.rayleigh and not cfg.sgs_diffusion:
             from .stress import flat_stress_shapes as _shapes
 

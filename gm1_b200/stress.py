@@ -143,19 +143,28 @@ def launch_cuda_flat_sgs_stress(arrays: Mapping[str, Any], *, ni: int, nj: int, 
 
 # ------------------------------------------------------------ turbs (flat)
 
-SCALAR_TURBULENCE_ARRAY_NAMES = ("th0", "tha", "qa", "rho", "rr", "rf", "mh", "mf", "khh", "khv", "thten1", "qten")
+SCALAR_TURBULENCE_ARRAY_NAMES = ("th0", "tha", "qa", "rho", "rr", "rf", "mh", "mf", "khh", "khv", "thten1", "qten",
+                                 "workspace")
 
 
 class _TurbsArrays(ctypes.Structure):
     _fields_ = [(n, ctypes.c_void_p) for n in ("th0", "tha", "qa", "rho", "rr", "rf", "mh", "mf", "khh", "khv",
-                                               "thten", "qten")]
+                                               "thten", "qten", "workspace")]
+
+
+def scalar_turbulence_workspace(ni: int, nj: int, nk: int, numq: int, device) -> torch.Tensor:
+    """The device scratch launch_cuda_flat_scalar_turbulence takes as
+    ``workspace``: the horizontal flux divergence of each of the 1 + numq
+    scalars."""
+    return torch.empty((numq + 1, nk, nj, ni), dtype=torch.float32, device=device)
 
 
 def flat_scalar_turbulence_shapes(ni: int, nj: int, nk: int, numq: int) -> dict[str, tuple[int, ...]]:
     _grid(ni, nj, nk)
     cell, face = (nk, nj, ni), (nk + 1, nj, ni)
     return {"th0": (nk,), "tha": cell, "qa": (numq, nk, nj, ni), "rho": cell, "rr": cell, "rf": face, "mh": cell,
-            "mf": face, "khh": face, "khv": face, "thten1": cell, "qten": (numq, nk, nj, ni)}
+            "mf": face, "khh": face, "khv": face, "thten1": cell, "qten": (numq, nk, nj, ni),
+            "workspace": (numq + 1, nk, nj, ni)}
 
 
 def launch_cuda_flat_scalar_turbulence(arrays: Mapping[str, Any], *, ni: int, nj: int, nk: int, numq: int,
@@ -167,7 +176,8 @@ def launch_cuda_flat_scalar_turbulence(arrays: Mapping[str, Any], *, ni: int, nj
     vertical diffusion with khv, zero surface flux (the scalar loop of the
     closure's held phase on the flat lane, cuda_cartesian_closure.py:1566-1633).
     ``qa`` and ``qten`` may hold more rows than numq (leading rows used);
-    ``dz`` is the coordinate's reference spacing."""
+    ``workspace`` is scalar_turbulence_workspace()'s scratch; ``dz`` is the
+    coordinate's reference spacing."""
     if isinstance(numq, bool) or not isinstance(numq, int) or not 0 <= numq <= 6:
         raise ValueError("numq must be an integer in 0..6")
     dx, dy, dz, dt = _positive("dx", dx), _positive("dy", dy), _positive("dz", dz), _positive("dt", dt)

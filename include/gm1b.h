@@ -894,11 +894,16 @@ GM1B_API int32_t gm1b_flat_sgs_stress(int32_t ni, int32_t nj, int32_t nk, const 
                                       float dx, float dy, float rdz, float dt, void *stream);
 
 /* th0 (nk); tha/rho/rr/mh/thten (nk, nj, ni); qa/qten rows of nk*nj*ni words
- * (moisture row q at word q*nk*nj*ni); rf/mf/khh/khv (nk+1, nj, ni). */
+ * (moisture row q at word q*nk*nj*ni); rf/mf/khh/khv (nk+1, nj, ni);
+ * workspace gm1b_flat_scalar_turbulence_workspace_words() words of device
+ * scratch (the horizontal flux divergence of every scalar). */
 typedef struct gm1b_flat_scalar_turbulence_arrays {
     const float *th0, *tha, *qa, *rho, *rr, *rf, *mh, *mf, *khh, *khv;
-    float *thten, *qten;
+    float *thten, *qten, *workspace;
 } gm1b_flat_scalar_turbulence_arrays;
+
+/* Words of the scalar turbulence's workspace: (numq + 1)*nk*nj*ni. */
+GM1B_API int64_t gm1b_flat_scalar_turbulence_workspace_words(int32_t ni, int32_t nj, int32_t nk, int32_t numq);
 
 /*
  * CM1 turbs on the flat stretched column for theta ((th0 - 300) + tha) and

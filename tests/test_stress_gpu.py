@@ -137,8 +137,11 @@ def _turbs_inputs(ni, nj, nk, numq, seed):
 def test_flat_turbs_is_the_oracle_word_for_word(ni, nj, nk, numq, seed):
     from gm1_b200.stress import launch_cuda_flat_scalar_turbulence
 
+    from gm1_b200.stress import scalar_turbulence_workspace
+
     a, dz = _turbs_inputs(ni, nj, nk, numq, seed)
     d = _dev(a)
+    d["workspace"] = scalar_turbulence_workspace(ni, nj, nk, numq, d["tha"].device)
     ost.flat_scalar_turbulence(a, ni=ni, nj=nj, nk=nk, numq=numq, dx=DX, dy=DX, dz=dz, dt=DT)
     launch_cuda_flat_scalar_turbulence(d, ni=ni, nj=nj, nk=nk, numq=numq, dx=DX, dy=DX, dz=dz, dt=DT)
     torch.cuda.synchronize()
