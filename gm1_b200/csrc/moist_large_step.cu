@@ -26,14 +26,18 @@ namespace gm1b {
 namespace {
 
 // copy of a (nz, ny, nx) box between two arrays of different row and level
-// strides (compact <-> padded sub-box)
-__global__ void box_copy_kernel(float *__restrict__ dst, size_t dst_sy, size_t dst_sz, const float *__restrict__ src,
-                                size_t src_sy, size_t src_sz, int nx, int ny, int nz) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y;
-    const int k = blockIdx.z;
-    if (i >= nx || j >= ny || k >= nz) return;
-    dst[(size_t)k * dst_sz + (size_t)j * dst_sy + i] = src[(size_t)k * src_sz + (size_t)j * src_sy + i];
+// strides (compact <-> padded sub-box): one warp per row, rows grid-strided
+constexpr int kCopyRows = 8;  // rows (warps) per CTA
+__global__ void __launch_bounds__(32 * kCopyRows)
+    box_copy_kernel(float *__restrict__ dst, size_t dst_sy, size_t dst_sz, const float *__restrict__ src,
+                    size_t src_sy, size_t src_sz, int nx, int ny, int nz) {
+    const size_t rows = (size_t)ny * nz;
+    for (size_t r = (size_t)blockIdx.x * kCopyRows + threadIdx.y; r < rows; r += (size_t)gridDim.x * kCopyRows) {
+        const size_t j = r % ny, k = r / ny;
+        float *d = dst + k * dst_sz + j * dst_sy;
+        const float *s = src + k * src_sz + j * src_sy;
+        for (int i = threadIdx.x; i < nx; i += 32) d[i] = s[i];
+    }
 }
 
 __global__ void add_inplace_kernel(float *__restrict__ acc, const float *__restrict__ x, size_t n) {
@@ -81,9 +85,10 @@ constexpr int kNumq = 3;
 
 int box_copy(float *dst, size_t dst_sy, size_t dst_sz, const float *src, size_t src_sy, size_t src_sz, int nx, int ny,
              int nz, cudaStream_t st) {
-    const dim3 grid((nx + 127) / 128, ny, nz);
+    const size_t rows = (size_t)ny * nz, want = (rows + kCopyRows - 1) / kCopyRows, cap = (size_t)148 * 32;
     ProfScope ps("box_copy_kernel", st);
-    box_copy_kernel<<<grid, 128, 0, st>>>(dst, dst_sy, dst_sz, src, src_sy, src_sz, nx, ny, nz);
+    box_copy_kernel<<<(unsigned)(want < cap ? want : cap), dim3(32, kCopyRows), 0, st>>>(dst, dst_sy, dst_sz, src,
+                                                                                         src_sy, src_sz, nx, ny, nz);
     ps.stop();
     return ok(cudaPeekAtLastError(), "box_copy_kernel") ? GM1B_OK : GM1B_ERR_CUDA;
 }

@@ -13,7 +13,8 @@
  * The reference has no NumPy twin of these texts: this restates the CUDA
  * source statement by statement (binary32, one operation at a time, built
  * with -ffp-contract=off; the literal zero factors of vibeta = 0 are formed
- * so signed zeros stay what they are).  Open sides are index clamps (CM1's
+ * so signed zeros stay what they are), pinned word for word to those texts
+ * compiled and run on the host (tests/golden/make_kernel_text_golden.py).  Open sides are index clamps (CM1's
  * zero-gradient halo).  Shapes (C order): s11/s22/s33/t11/t22/t33/rho/mh
  * (nk, nj, ni); s12/t12 (nk, nj+1, ni+1); s13/t13 (nk+1, nj, ni+1);
  * s23/t23 (nk+1, nj+1, ni); kmh/kmv/rf/mf/w/wten (nk+1, nj, ni);

@@ -68,3 +68,21 @@ def table_header() -> list[str]:
 
 def describe(errs) -> str:
     return "; ".join(f"step {s}: gpu {format_errors(g)} | oracle {format_errors(o)}" for s, (g, o) in errs.items())
+
+
+def check_long_run(cfg, host: dict, metrics: dict, make_gpu_step, steps: int = 60, every: int = 10,
+                   what: str = "") -> dict:
+    """A long run's worst error against the FP64 run, GPU beside the binary32
+    oracle: over the checkpoints every ``every`` steps, each field's largest
+    GPU error (max and RMS on the field's scale) at most FP64_FACTOR times the
+    oracle's largest plus FP64_FLOOR.  Returns {step: (gpu, oracle)}."""
+    from tests.moist_common import check_errors, worst
+
+    errs = fp64_errors(cfg, host, metrics, tuple(range(every, steps + 1, every)), make_gpu_step)
+    zero = {n: (0.0, 0.0) for n in FIELDS}
+    gpu_w, ora_w = zero, zero
+    for step, (g, o) in sorted(errs.items()):
+        print(what, "after", step, "gpu vs fp64:", format_errors(g), "| oracle vs fp64:", format_errors(o))
+        gpu_w, ora_w = worst(gpu_w, g), worst(ora_w, o)
+    check_errors(gpu_w, fp64_bars(ora_w), f"{what} worst over {steps} steps against the FP64 run")
+    return errs

@@ -8,7 +8,8 @@ Cases: configuration 2 at its full 256x256x80 size after one large step (the
 benchmark's seeded Weisman-Klemp start: +3 K bubble of 10 km x 1.5 km at
 1.5 km, U(+-0.1 K) noise, seed 2), and the 80-level stretched supercell
 column of configuration 3 on a 128x128 plane after 1 and 20 large steps
-(bubble 3 km x 1.5 km).  Each cell of the table is "GPU / oracle", the
+(bubble 3 km x 1.5 km), also with the closure's held tendencies (SGS stress,
+scalar diffusion, Rayleigh damping, dissipative heating).  Each cell of the table is "GPU / oracle", the
 largest |error| divided by the field's largest |value| in the FP64 run.
 """
 
@@ -38,6 +39,11 @@ def main() -> None:
          dict(seed=2, bubble_k=3.0, noise_k=0.1, bubble_radius_m=(10000.0, 1500.0), bubble_center_z_m=1500.0), (1,)),
         (f"C3 column {c3[0]}x{c3[1]}x{c3[2]}",
          MoistStepConfig(*c3, 100.0, 100.0, 100.0, 0.6, 8, column=SUPERCELL_STRETCHED_COLUMN),
+         dict(seed=2, bubble_k=3.0, noise_k=0.1, bubble_radius_m=(3000.0, 1500.0), bubble_center_z_m=1500.0),
+         (1, 20)),
+        (f"C3 column {c3[0]}x{c3[1]}x{c3[2]}, held closure",
+         MoistStepConfig(*c3, 100.0, 100.0, 100.0, 0.6, 8, column=SUPERCELL_STRETCHED_COLUMN, sgs_diffusion=True,
+                         rayleigh=True, dissipative_heating=True),
          dict(seed=2, bubble_k=3.0, noise_k=0.1, bubble_radius_m=(3000.0, 1500.0), bubble_center_z_m=1500.0),
          (1, 20)),
     ]

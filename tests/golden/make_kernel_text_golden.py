@@ -14,6 +14,7 @@ directory, runs its kernels one thread index at a time in their launch
 order, and stores whole input/output array sets as .npz fixtures here.
 
     python tests/golden/make_kernel_text_golden.py --reference /path/to/gm1 flat-closure
+    python tests/golden/make_kernel_text_golden.py --reference /path/to/gm1 flat-stress
 
 The fixtures pin the oracle restatements (tests/test_oracle_flat_closure.py)
 and through them the CUDA kernels.
@@ -202,13 +203,112 @@ def make_flat_closure(reference: Path) -> None:
             print("wrote", path.name)
 
 
+# ---------------------------------------------------------------------------
+# flat stretched-column held closure: gettau, turbu/turbv/turbw, turbs
+# ---------------------------------------------------------------------------
+def make_flat_stress(reference: Path) -> None:
+    """The strain passes, gettau (enqueue_flat_gettau), the momentum stress
+    (enqueue_flat_momentum_stress, two_part=None) and the flat turbs of theta
+    and three moisture rows (the pad/pack texts of
+    cuda_gm1_scalar_turbulence.py, then gm1_flat_turbs_xy_flux_v1 and
+    gm1_flat_turbs_implicit_apply_v1 with iflux = 0) on the flat closure's
+    fixtures, in the closure's launch order."""
+    sys.path.insert(0, str(reference / "src"))
+    import cm1core.cuda_gm1_flat_stretched_closure as fc
+    import cm1core.cuda_gm1_scalar_turbulence as st
+
+    grids = ((12, 10, 10, 21), (9, 13, 14, 22))
+    with tempfile.TemporaryDirectory() as tmp:
+        work = Path(tmp)
+        closure = HostKernels(fc.flat_stretched_closure_source(max_nk=64), work, "flat_closure")
+        scalar = HostKernels(st.CUDA_GM1_SCALAR_TURBULENCE_SOURCE, work, "scalar_turbulence")
+        for ni, nj, nk, seed in grids:
+            a = flat_closure_fixture(ni, nj, nk, seed)
+            rng = np.random.default_rng(seed + 100)
+            mass, face = (nk, nj, ni), (nk + 1, nj, ni)
+            a["rr"] = f32(np.float32(1.0) / a["rho"])
+            a["khh"] = f32(rng.uniform(0.0, 60.0, face))
+            a["khv"] = f32(rng.uniform(0.0, 60.0, face))
+            a["th0"] = f32(np.linspace(300.0, 330.0, nk))
+            a["tha"] = f32(rng.normal(0.0, 1.5, mass))
+            a["qa"] = f32(np.abs(rng.normal(0.0, 4e-3, (6, nk, nj, ni))))
+            for n, sh in (("uten", (nk, nj, ni + 1)), ("vten", (nk, nj + 1, ni)), ("wten", face)):
+                a[n] = f32(rng.normal(0.0, 1e-3, sh))
+            a["thten1"] = f32(rng.normal(0.0, 1e-4, mass))
+            a["qten"] = f32(rng.normal(0.0, 1e-7, (6, nk, nj, ni)))
+            dx, dy, dt = 450.0, 520.0, 2.0
+            rdx, rdy = np.float32(np.float32(1.0) / np.float32(dx)), np.float32(np.float32(1.0) / np.float32(dy))
+            rdz = float(a["rdz"])
+            u = np.uint32
+            dims = (u(ni), u(nj), u(nk))
+            out: dict[str, np.ndarray] = {}
+            s11, s22, s33 = (np.zeros(mass, np.float32) for _ in range(3))
+            s12 = np.zeros((nk, nj + 1, ni + 1), np.float32)
+            s13 = np.zeros((nk + 1, nj, ni + 1), np.float32)
+            s23 = np.zeros((nk + 1, nj + 1, ni), np.float32)
+            closure.grid_stride("gm1_flat_calcdef_mass_v1", a["u3d"], a["v3d"], a["w3d"], a["rho"], a["mh_profile"],
+                                s11, s22, s33, s12, *dims, float(rdx), float(rdy), rdz)
+            closure.grid_stride("gm1_flat_calcdef_face_v1", a["u3d"], a["v3d"], a["w3d"], a["rf"], a["mf"], s13, s23,
+                                *dims, float(rdx), float(rdy), rdz)
+            out.update(s11=s11, s22=s22, s33=s33, s12=s12, s13=s13, s23=s23)
+            t11, t22, t33 = (np.zeros(mass, np.float32) for _ in range(3))
+            t12 = np.zeros((nk, nj + 1, ni + 1), np.float32)
+            t13 = np.zeros((nk + 1, nj, ni + 1), np.float32)
+            t23 = np.zeros((nk + 1, nj + 1, ni), np.float32)
+            closure.grid_stride("gm1_flat_gettau_normal_v1", s11, s22, s33, a["kmh"], t11, t22, t33, *dims)
+            closure.grid_stride("gm1_flat_gettau_t12_v1", s12, a["kmh"], t12, *dims)
+            closure.grid_stride("gm1_flat_gettau_t13_v1", s13, a["kmv"], t13, *dims)
+            closure.grid_stride("gm1_flat_gettau_t23_v1", s23, a["kmv"], t23, *dims)
+            out.update(t11=t11, t22=t22, t33=t33, t12=t12, t13=t13, t23=t23)
+            uten, vten, wten = a["uten"].copy(), a["vten"].copy(), a["wten"].copy()
+            common = (a["kmv"], a["rho"], a["rf"], a["mh"], a["mf"], a["mh_profile"])
+            closure.per_thread("gm1_flat_turbu_v1", nj * (ni + 1), t11, t12, t13, *common, a["u3d"], a["w3d"], uten,
+                               a["mh_profile"], uten, *dims, float(rdx), float(rdy), rdz, dt, u(0))
+            closure.per_thread("gm1_flat_turbv_v1", (nj + 1) * ni, t12, t22, t23, *common, a["v3d"], a["w3d"], vten,
+                               a["mh_profile"], vten, *dims, float(rdx), float(rdy), rdz, dt, u(0))
+            closure.per_thread("gm1_flat_turbw_v1", nj * ni, t13, t23, t33, a["kmh"], a["rho"], a["rf"], a["mh"],
+                               a["mf"], a["w3d"], wten, *dims, float(rdx), float(rdy), rdz, dt)
+            out.update(uten=uten, vten=vten, wten=wten)
+            # turbs: theta then qv, qc, qr (solve1.F:1169-1233), dz the
+            # coordinate's reference spacing, no surface flux
+            hx, hy = ni + 2, nj + 2
+            rhoh = np.zeros((nk, hy, hx), np.float32)
+            khhh = np.zeros((nk + 1, hy, hx), np.float32)
+            gzh, rgzh = np.zeros((hy, hx), np.float32), np.zeros((hy, hx), np.float32)
+            ones = np.ones((nj, ni), np.float32)
+            scalar.grid_stride("gm1_turbs_pad_static_open_v1", a["rho"], a["khh"], ones, ones, rhoh, khhh, gzh, rgzh,
+                               *dims)
+            thten1, qten = a["thten1"].copy(), a["qten"].copy()
+            fx = np.zeros((nk, nj, ni + 1), np.float32)
+            fy = np.zeros((nk, nj + 1, ni), np.float32)
+            cp, dp = np.zeros(mass, np.float32), np.zeros(mass, np.float32)
+            sflux = np.zeros((nj, ni), np.float32)
+            dz = float(np.float32(1.0) / np.float32(rdz))
+            for species, target in ((0xFFFFFFFF, thten1), (0, qten[0]), (1, qten[1]), (2, qten[2])):
+                sh = np.zeros((nk, hy, hx), np.float32)
+                scalar.grid_stride("gm1_turbs_pack_scalar_open_v1", a["th0"], a["tha"], a["qa"], sh, *dims,
+                                   u(species))
+                closure.grid_stride("gm1_flat_turbs_xy_flux_v1", sh, rhoh, khhh, fx, fy, *dims, dx, dy)
+                closure.per_thread("gm1_flat_turbs_implicit_apply_v1", ni * nj, sh, a["rho"], a["rr"], a["rf"],
+                                   a["mh"], a["mf"], a["khv"], fx, fy, sflux, cp, dp, target, *dims, dx, dy, dz, dt,
+                                   u(0))
+            out.update(thten1=thten1, qten=qten)
+            path = HERE / f"flat_stress_{ni}x{nj}x{nk}.npz"
+            np.savez_compressed(path, meta=np.array([ni, nj, nk], np.int32), dx=np.float32(dx), dy=np.float32(dy),
+                                dt=np.float32(dt), dz=np.float32(dz), **{f"in_{k}": v for k, v in a.items()},
+                                **{f"out_{k}": v for k, v in out.items()})
+            print("wrote", path.name)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", type=Path, required=True)
-    ap.add_argument("what", choices=["flat-closure"])
+    ap.add_argument("what", choices=["flat-closure", "flat-stress"])
     args = ap.parse_args()
     if args.what == "flat-closure":
         make_flat_closure(args.reference)
+    elif args.what == "flat-stress":
+        make_flat_stress(args.reference)
 
 
 if __name__ == "__main__":

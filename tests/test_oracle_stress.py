@@ -236,3 +236,32 @@ def test_dissipative_heating_is_the_twins_cell_formula():
     ost.dissipative_heating(a, ni=meta["ni"], nj=meta["nj"], nk=meta["nk"])
     assert np.array_equal(a["thten1"].view(np.uint32), out["thten1"].view(np.uint32))
     assert np.any(a["thten1"] != inp["thten1"])
+
+
+# ------------------------------------------- the reference's own flat texts
+# tests/golden/make_kernel_text_golden.py flat-stress runs the reference's
+# CUDA texts of the flat stretched-column closure on the host (the strain
+# passes, gettau, turbu/turbv/turbw and turbs with its pad/pack copies, the
+# binary32 intrinsics as IEEE operations): the restatement is word-identical.
+FLAT_TEXT_CASES = ("flat_stress_12x10x10", "flat_stress_9x13x14")
+
+
+@pytest.mark.parametrize("tag", FLAT_TEXT_CASES)
+def test_flat_stress_and_turbs_are_the_reference_texts_word_for_word(tag):
+    z = np.load(GOLDEN / f"{tag}.npz")
+    ni, nj, nk = (int(x) for x in z["meta"])
+    dx, dy, dt, dz = (float(z[k]) for k in ("dx", "dy", "dt", "dz"))
+    a = {k[3:]: np.ascontiguousarray(z[k]).copy() for k in z.files if k.startswith("in_")}
+    rdz = float(a["rdz"].item())
+    a.update(ost.zeros(ni, nj, nk, ost.STRAIN_NAMES + ost.TAU_NAMES))
+    ost.flat_sgs_stress(a, ni=ni, nj=nj, nk=nk, dx=dx, dy=dy, rdz=rdz, dt=dt)
+    for n in ost.STRAIN_NAMES + ost.TAU_NAMES + ost.TENDENCY_NAMES:
+        got, want = a[n], z["out_" + n]
+        if n in ("s13", "s23"):  # the texts write face levels 1..nk-1 only
+            got, want = got[1:nk], want[1:nk]
+        assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), n
+    b = {k: a[k] for k in ost.SCALAR_TURBULENCE_INPUTS}
+    b["thten1"], b["qten"] = a["thten1"].copy(), a["qten"].copy()
+    ost.flat_scalar_turbulence(b, ni=ni, nj=nj, nk=nk, numq=3, dx=dx, dy=dy, dz=dz, dt=dt)
+    for n in ("thten1", "qten"):
+        assert np.array_equal(b[n].view(np.uint32), z["out_" + n].view(np.uint32)), n
