@@ -10,8 +10,8 @@ prognostic field measured on its own scale (the largest |value| of that
 field: u, v, w each, theta', pi', qv, qc, qr each, TKE) within
 tests/moist_common.py's SHORT_BARS after 1 and 3 steps (also at the full
 256x256x80 size after one step); over 60 steps, the GPU's worst error
-against the FP64 run of the same operators at most four times the binary32
-oracle's own (tests/fp64_common.py); u, v and w are word-identical after
+against the FP64 run of the same operators at most sixteen times the binary32
+oracle's own (tests/fp64_common.py: LONG_RUN_FACTOR); u, v and w are word-identical after
 one step.  A CUDA-graph replay of the step gives the
 eager words."""
 

@@ -8,8 +8,8 @@ column of the 640x768x80 configuration on a reduced plane.
 
 Bars (tests/moist_common.py measures each field on its own scale):
 SHORT_BARS after 1 and 3 steps; over 60 steps, the GPU's worst error against
-the FP64 run of the same operators at most four times the binary32 oracle's
-own (tests/fp64_common.py).  The words differ
+the FP64 run of the same operators at most sixteen times the binary32
+oracle's own (tests/fp64_common.py: LONG_RUN_FACTOR).  The words differ
 only where Kessler and the TKE closure pass values through powf, expf and
 sqrtf (CUDA and the C library round their last bits differently) and the
 rest of the step carries those ulps."""
