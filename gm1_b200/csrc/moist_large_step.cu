@@ -231,8 +231,10 @@ int closure(Step &h, cudaStream_t st) {
     TRY(gm1b_sgs_tke(c.ni, c.nj, c.nk, &g, c.dx, c.dy, c.dz, st));
     TRY(copy(s.tke3d, s.tkea, Sizes(c).face * sizeof(float), st, "tke3d <- tkea"));
     gm1b_tke_evolution_arrays t = tke_arrays(h);
-    if (!c.stretched) return gm1b_tke_diffusion(c.ni, c.nj, c.nk, &t, c.dx, c.dy, c.dz, c.dt, st);
-    TRY(gm1b_tke_diffusion_flat(c.ni, c.nj, c.nk, &t, c.dx, c.dy, h.rdz, c.dt, st));
+    if (c.stretched)
+        TRY(gm1b_tke_diffusion_flat(c.ni, c.nj, c.nk, &t, c.dx, c.dy, h.rdz, c.dt, st));
+    else
+        TRY(gm1b_tke_diffusion(c.ni, c.nj, c.nk, &t, c.dx, c.dy, c.dz, c.dt, st));
     if (!c.sgs_diffusion && !c.rayleigh) return GM1B_OK;
     // the held momentum tendencies: zeroed, then the SGS stress added (the
     // Rayleigh damping joins them in the held phase)
@@ -626,17 +628,16 @@ extern "C" int32_t gm1b_moist_step_create(const gm1b_moist_step_config *config, 
         }
     const void *const *mp = reinterpret_cast<const void *const *>(metrics);
     const size_t all = sizeof(gm1b_moist_metrics) / sizeof(void *);
-    const size_t required = c.stretched ? (c.rayleigh ? all : all - 5) : 25;
-    for (size_t q = 0; q < required; ++q)
-        if (mp[q] == nullptr) {
+    for (size_t q = 0; q < all; ++q)
+        if (mp[q] == nullptr && (q < 25 || (q < 28 && c.stretched) || (q >= 28 && c.rayleigh))) {
             gm1b_set_error("gm1b_moist_step_create: metric #%zu is NULL%s", q,
                            q >= 28   ? " (the Rayleigh damping needs u0, v0, tauh, taus and tauf)"
                            : q >= 25 ? " (a stretched column needs mh_profile, mf_profile and rho0_padded)"
                                      : "");
             return GM1B_ERR_ARGUMENT;
         }
-    if (c.rayleigh && (!c.stretched || !(c.rdalpha >= 0.0f) || !isfinite(c.rdalpha))) {
-        gm1b_set_error("gm1b_moist_step_create: the Rayleigh damping needs a stretched column and a finite rdalpha >= 0");
+    if (c.rayleigh && (!(c.rdalpha >= 0.0f) || !isfinite(c.rdalpha))) {
+        gm1b_set_error("gm1b_moist_step_create: the Rayleigh damping needs a finite rdalpha >= 0");
         return GM1B_ERR_ARGUMENT;
     }
     if (c.sgs_diffusion && !c.stretched) {

@@ -558,10 +558,6 @@ class MoistLargeStep:
             self.flat_stage_arrays = {"tkea": s["tkea"], "tke3d": s["tke3d"], "tketen": s["tketen"], "c2": m["c2"],
                                       "rrf0": m["rrf0"], "rru": s["rru"], "rrv": s["rrv"], "rrw": s["rrw"],
                                       "divx": s["divx"]}
-        if cfg.rayleigh and not self.flat:
-            refuse(code="GM1B-RAYLEIGH-COLUMN", gate="physics-seam", option="rayleigh", value=True,
-                   reason="the Rayleigh damping is built for the flat operator family of a stretched column",
-                   remedy="give the configuration a stretched column, or rayleigh=False")
         if cfg.sgs_diffusion:
             if not self.flat:
                 refuse(code="GM1B-SGS-STRESS-COLUMN", gate="physics-seam", option="sgs_diffusion", value=True,

@@ -73,10 +73,9 @@ class OracleMoistStep:
         # CM1's upper Rayleigh damping (irdamp = 1, solve1.F:412-454), its
         # coefficients and base-state winds from the metrics
         self.rayleigh = bool(getattr(cfg, "rayleigh", False))
+        if self.sgs_diffusion and not self.flat:
+            raise ValueError("the SGS diffusion is built for the stretched column's flat operator family only")
         if self.sgs_diffusion or self.rayleigh:
-            if not self.flat:
-                raise ValueError("the SGS diffusion and the Rayleigh damping are built for the stretched column's "
-                                 "flat operator family only")
             self.stress = ost.zeros(cfg.ni, cfg.nj, cfg.nk, ost.STRAIN_NAMES + ost.TAU_NAMES + ost.TENDENCY_NAMES)
         if self.flat:
             self.rdz = float(np.float32(np.float32(1.0) / np.float32(cfg.dz)))

@@ -15,7 +15,8 @@ error against the FP64 run in tests/test_moist_fp64_gpu.py (the implicit
 vertical diffusion forms (solution - w)/dt, a difference of nearly equal
 words, so w carries the libm ulps of the closure further than the other
 fields do); the C entry point gives the Python composition's words; the
-diffusion and the damping move the state; a uniform column refuses them."""
+diffusion and the damping move the state; on the uniform column the damping
+and the heating match too, and the SGS diffusion is refused."""
 
 from __future__ import annotations
 
@@ -115,9 +116,46 @@ def test_the_held_closure_moves_the_state():
     assert du_ray < du_off
 
 
-def test_a_uniform_column_refuses_the_held_closure():
-    for kw in (dict(sgs_diffusion=True), dict(rayleigh=True)):
-        cfg = MoistStepConfig(24, 20, 16, 1000.0, 1000.0, 250.0, 5.0, 10, **kw)
-        host, metrics = weisman_klemp_initial_state(cfg, seed=3, bubble_radius_m=(6000.0, 1400.0))
-        with pytest.raises(CM1Refusal):
-            MoistLargeStep(cfg, upload(host), upload(metrics))
+def _uniform(**kw):
+    cfg = MoistStepConfig(40, 33, 80, 1000.0, 1000.0, 250.0, 5.0, 10, **kw)
+    host, metrics = weisman_klemp_initial_state(cfg, seed=3, bubble_radius_m=(6000.0, 1400.0), bubble_cloud=1.0e-3,
+                                                bubble_rain=5.0e-4)
+    # a wind departure from the base state in the damping layer (above 15 km)
+    host["u3d"][64:80] += np.float32(2.5)
+    host["v3d"][64:80] -= np.float32(1.5)
+    host["w3d"][64:80] += np.float32(0.25)
+    for cur, base in (("ua", "u3d"), ("va", "v3d"), ("wa", "w3d")):
+        host[cur][:] = host[base]
+    return cfg, host, metrics
+
+
+def test_uniform_column_damping_and_heating_match_the_oracle():
+    """The damping and the dissipative heating do not depend on the column
+    family: on the uniform column (configuration 2's terrain family) the
+    first step's held tendencies match the oracle's and the C entry point
+    gives the Python composition's words."""
+    cfg, host, metrics = _uniform(rayleigh=True, dissipative_heating=True)
+    dev = MoistLargeStep(cfg, upload(host), upload(metrics))
+    ref = OracleMoistStep(cfg, {k: v.copy() for k, v in host.items()}, {k: v.copy() for k, v in metrics.items()})
+    nat = NativeMoistLargeStep(cfg, upload(host), upload(metrics), concurrent=True)
+    dev.step()
+    ref.step()
+    nat.step()
+    torch.cuda.synchronize()
+    for n in ("uten", "vten", "wten"):
+        g, r = dev.stress[n].cpu().numpy().astype(np.float64), ref.stress[n].astype(np.float64)
+        assert np.max(np.abs(r)) > 0.0, n
+        assert np.max(np.abs(g - r)) <= 1e-5 * np.max(np.abs(r)), n
+    g, r = dev.s["thheld"].cpu().numpy().astype(np.float64), ref.s["thheld"].astype(np.float64)
+    assert np.max(np.abs(g - r)) <= 1e-5 * np.max(np.abs(r))
+    bad = [n for n in COMPARED
+           if not np.array_equal(dev.s[n].cpu().numpy().view(np.uint8), nat.s[n].cpu().numpy().view(np.uint8))]
+    assert bad == []
+    nat.close()
+
+
+def test_a_uniform_column_refuses_the_sgs_diffusion():
+    cfg = MoistStepConfig(24, 20, 16, 1000.0, 1000.0, 250.0, 5.0, 10, sgs_diffusion=True)
+    host, metrics = weisman_klemp_initial_state(cfg, seed=3, bubble_radius_m=(6000.0, 1400.0))
+    with pytest.raises(CM1Refusal):
+        MoistLargeStep(cfg, upload(host), upload(metrics))
