@@ -23,7 +23,7 @@ ROOT = PKG.parent
 LIB_DIR = PKG / "lib"
 LIB = LIB_DIR / "libgm1b.so"
 SOURCES = ("capi.cu", "periodic_lane.cu", "advection5.cu", "kessler.cu", "tke.cu", "scalar_rk.cu",
-           "moist_bridge.cu", "initial_state.cu", "limits.cu", "closure.cu", "stress.cu", "tke_evolution.cu", "momentum5.cu", "terrain_open.cu", "moist_step.cu", "vertical.cu", "moist_large_step.cu", "adjoint.cu", "selftest.cu")
+           "moist_bridge.cu", "initial_state.cu", "limits.cu", "closure.cu", "stress.cu", "stress_terrain.cu", "tke_evolution.cu", "momentum5.cu", "terrain_open.cu", "moist_step.cu", "vertical.cu", "moist_large_step.cu", "adjoint.cu", "selftest.cu")
 ARCH = ("-gencode", "arch=compute_100a,code=sm_100a")
 FLAGS = (
     "-O3", "-std=c++17", "-lineinfo",

@@ -243,7 +243,14 @@ int closure(Step &h, cudaStream_t st) {
     TRY(zero(h.stress.vten, (size_t)c.nk * (c.nj + 1) * c.ni * sizeof(float), st, "zero held v"));
     TRY(zero(h.stress.wten, z.face * sizeof(float), st, "zero held w"));
     if (!c.sgs_diffusion) return GM1B_OK;
-    return gm1b_flat_sgs_stress(c.ni, c.nj, c.nk, &h.stress, c.dx, c.dy, h.rdz, c.dt, st);
+    if (c.stretched) return gm1b_flat_sgs_stress(c.ni, c.nj, c.nk, &h.stress, c.dx, c.dy, h.rdz, c.dt, st);
+    // the uniform column: the terrain texts on its flat metrics
+    const gm1b_flat_stress_arrays &f = h.stress;
+    const gm1b_terrain_stress_arrays ta{f.u3d, f.v3d, f.w3d, f.rho, f.rf,  f.mh,  f.mf,  f.kmh, f.kmv, m.gz,
+                                        m.rgz, m.gzu, m.rgzu, m.gzv, m.rgzv, m.gx, m.gy, m.gxu, m.gyv, f.s11,
+                                        f.s22, f.s33, f.s12, f.s13, f.s23, f.t11, f.t22, f.t33, f.t12, f.t13,
+                                        f.t23, f.uten, f.vten, f.wten};
+    return gm1b_terrain_sgs_stress(c.ni, c.nj, c.nk, &ta, c.dx, c.dy, c.dz, c.dt, st);
 }
 
 // the held momentum into the physical cells of the zeroed stage tendencies
@@ -282,9 +289,17 @@ int held_tendencies(Step &h, cudaStream_t st) {
     if (c.sgs_diffusion) {
         // turbs for theta and the moisture rows into the held thten1/qten the
         // eqtset 2 composition then reads (solve1.F:1169-1233)
-        const gm1b_flat_scalar_turbulence_arrays ta{s.th0, s.tha, s.qa, s.rho, s.rr, s.rf, h.m.mh, h.m.mf,
-                                                    s.khh, s.khv, s.thheld, s.qheld, h.turbs_work};
-        TRY(gm1b_flat_scalar_turbulence(c.ni, c.nj, c.nk, kNumq, &ta, c.dx, c.dy, c.dz, c.dt, st));
+        const gm1b_moist_metrics &m = h.m;
+        if (c.stretched) {
+            const gm1b_flat_scalar_turbulence_arrays ta{s.th0, s.tha, s.qa, s.rho, s.rr, s.rf, m.mh, m.mf,
+                                                        s.khh, s.khv, s.thheld, s.qheld, h.turbs_work};
+            TRY(gm1b_flat_scalar_turbulence(c.ni, c.nj, c.nk, kNumq, &ta, c.dx, c.dy, c.dz, c.dt, st));
+        } else {
+            const gm1b_terrain_scalar_turbulence_arrays ta{
+                s.th0, s.tha, s.qa,   s.rho,  s.rr, s.rf,  m.mh, m.mf,     s.khh, s.khv, m.gz,
+                m.rgz, m.rgzu, m.rgzv, m.gx, m.gxu, m.gy, m.gyv, s.thheld, s.qheld, h.turbs_work};
+            TRY(gm1b_terrain_scalar_turbulence(c.ni, c.nj, c.nk, kNumq, &ta, c.dx, c.dy, c.dz, c.dt, st));
+        }
     }
     gm1b_held_arrays a{s.th0_3d, s.pi0_3d, s.rho, s.pp3d_c, s.tha, s.qa, s.qpten, s.qtten, s.qvten, s.qcten,
                        s.thheld, s.qheld, s.ppten};
@@ -640,10 +655,6 @@ extern "C" int32_t gm1b_moist_step_create(const gm1b_moist_step_config *config, 
         gm1b_set_error("gm1b_moist_step_create: the Rayleigh damping needs a finite rdalpha >= 0");
         return GM1B_ERR_ARGUMENT;
     }
-    if (c.sgs_diffusion && !c.stretched) {
-        gm1b_set_error("gm1b_moist_step_create: the SGS diffusion is built for a stretched column's flat operator family");
-        return GM1B_ERR_ARGUMENT;
-    }
     if (c.sgs_diffusion && c.nk > 200) {
         gm1b_set_error("gm1b_moist_step_create: the SGS diffusion's column solves take nk <= 200");
         return GM1B_ERR_ARGUMENT;
@@ -672,7 +683,8 @@ extern "C" int32_t gm1b_moist_step_create(const gm1b_moist_step_config *config, 
         good = ok(cudaMalloc(&h->mass_ws, gm1b_apmasscon_workspace_bytes(c.nk)), "cudaMalloc (mass workspace)");
     if (good && c.sgs_diffusion)
         good = ok(cudaMalloc(&h->turbs_work,
-                             (size_t)gm1b_flat_scalar_turbulence_workspace_words(c.ni, c.nj, c.nk, kNumq) *
+                             (size_t)(c.stretched ? gm1b_flat_scalar_turbulence_workspace_words(c.ni, c.nj, c.nk, kNumq)
+                                                  : gm1b_terrain_scalar_turbulence_workspace_words(c.ni, c.nj, c.nk, kNumq)) *
                                  sizeof(float)),
                   "cudaMalloc (scalar turbulence workspace)");
     if (good && (c.sgs_diffusion || c.rayleigh)) {

@@ -168,12 +168,12 @@ class MoistStepConfig:
     # the SGS stress and scalar diffusion held tendencies (CM1 gettau and
     # turbu/turbv/turbw added into the momentum tendencies of every RK
     # stage; turbs of theta and the moisture rows into the held theta and
-    # moisture tendencies); built for the flat family of a stretched column
+    # moisture tendencies): the flat texts on a stretched column, the
+    # terrain texts on the uniform one
     sgs_diffusion: bool = False
     # CM1's upper Rayleigh damping, irdamp = 1 (held u, v, w and theta
     # tendencies toward the base state above rayleigh_zd_m at rate
-    # rayleigh_rdalpha; the supercell namelist's zd and rdalpha); built for
-    # the flat family of a stretched column
+    # rayleigh_rdalpha; the supercell namelist's zd and rdalpha)
     rayleigh: bool = False
     # CM1's dissipative heating (idiss = 1, the supercell namelist's): the
     # TKE closure's dissipation rate heats theta through the held tendency
@@ -559,24 +559,27 @@ class MoistLargeStep:
                                       "rrf0": m["rrf0"], "rru": s["rru"], "rrv": s["rrv"], "rrw": s["rrw"],
                                       "divx": s["divx"]}
         if cfg.sgs_diffusion:
-            if not self.flat:
-                refuse(code="GM1B-SGS-STRESS-COLUMN", gate="physics-seam", option="sgs_diffusion", value=True,
-                       reason="the SGS diffusion is built for the flat operator family of a stretched column",
-                       remedy="give the configuration a stretched column, or sgs_diffusion=False")
-            from .stress import STRAIN_NAMES, TAU_NAMES, flat_stress_shapes
+            # the flat texts on a stretched column, the terrain texts on the
+            # uniform one (its flat metrics: gz = 1, zero slopes)
+            from .stress import (STRAIN_NAMES, TAU_NAMES, TERRAIN_METRIC_NAMES, flat_stress_shapes,
+                                 scalar_turbulence_workspace, terrain_scalar_turbulence_workspace)
 
             shp = flat_stress_shapes(ni, nj, nk)
             self.stress = {n: torch.zeros(shp[n], dtype=torch.float32, device=dev)
                            for n in STRAIN_NAMES + TAU_NAMES + ("uten", "vten", "wten")}
             self.stress_arrays = {"u3d": s["uc"], "v3d": s["vc"], "w3d": s["wc"], "rho": s["rho"], "rf": s["rf"],
-                                  "mh": m["mh"], "mf": m["mf"], "mh_profile": m["mh_profile"], "kmh": s["kmh"],
-                                  "kmv": s["kmv"], **self.stress}
-            from .stress import scalar_turbulence_workspace
-
+                                  "mh": m["mh"], "mf": m["mf"], "kmh": s["kmh"], "kmv": s["kmv"], **self.stress}
             self.turbs_arrays = {"th0": s["th0"], "tha": s["tha"], "qa": s["qa"], "rho": s["rho"], "rr": s["rr"],
                                  "rf": s["rf"], "mh": m["mh"], "mf": m["mf"], "khh": s["khh"], "khv": s["khv"],
-                                 "thten1": s["thheld"], "qten": s["qheld"],
-                                 "workspace": scalar_turbulence_workspace(ni, nj, nk, NUMQ, dev)}
+                                 "thten1": s["thheld"], "qten": s["qheld"]}
+            if self.flat:
+                self.stress_arrays["mh_profile"] = m["mh_profile"]
+                self.turbs_arrays["workspace"] = scalar_turbulence_workspace(ni, nj, nk, NUMQ, dev)
+            else:
+                metrics = {n: m[n] for n in TERRAIN_METRIC_NAMES}
+                self.stress_arrays.update(metrics)
+                self.turbs_arrays.update(metrics)
+                self.turbs_arrays["workspace"] = terrain_scalar_turbulence_workspace(ni, nj, nk, NUMQ, dev)
         if cfg.rayleigh and not cfg.sgs_diffusion:
             from .stress import flat_stress_shapes as _shapes
 
@@ -667,14 +670,18 @@ class MoistLargeStep:
         """The held momentum tendencies: zeroed, then the SGS stress added
         (the closure's held phase, cuda_cartesian_closure.py:1202-1291, with
         neither damper on so the Rayleigh terms are zero)."""
-        from .stress import launch_cuda_flat_sgs_stress
+        from .stress import launch_cuda_flat_sgs_stress, launch_cuda_terrain_sgs_stress
 
         cfg = self.cfg
         with torch.cuda.stream(st):
             for n in ("uten", "vten", "wten"):
                 self.stress[n].zero_()
-        launch_cuda_flat_sgs_stress(self.stress_arrays, **self.k3, dx=cfg.dx, dy=cfg.dy, rdz=self.rdz, dt=cfg.dt,
-                                    stream=st)
+        if self.flat:
+            launch_cuda_flat_sgs_stress(self.stress_arrays, **self.k3, dx=cfg.dx, dy=cfg.dy, rdz=self.rdz, dt=cfg.dt,
+                                        stream=st)
+        else:
+            launch_cuda_terrain_sgs_stress(self.stress_arrays, **self.k3, dx=cfg.dx, dy=cfg.dy, dz=cfg.dz,
+                                           dt=cfg.dt, stream=st)
 
     def held_tendencies(self) -> None:
         s, st = self.s, self._st()
@@ -699,11 +706,11 @@ class MoistLargeStep:
         if self.cfg.sgs_diffusion:
             # turbs for theta and the moisture rows into the held thten1/qten
             # the eqtset 2 composition then reads (solve1.F:1169-1233)
-            from .stress import launch_cuda_flat_scalar_turbulence
+            from .stress import launch_cuda_flat_scalar_turbulence, launch_cuda_terrain_scalar_turbulence
 
             cfg = self.cfg
-            launch_cuda_flat_scalar_turbulence(self.turbs_arrays, **self.k3, numq=NUMQ, dx=cfg.dx, dy=cfg.dy,
-                                               dz=cfg.dz, dt=cfg.dt, stream=st)
+            turbs = launch_cuda_flat_scalar_turbulence if self.flat else launch_cuda_terrain_scalar_turbulence
+            turbs(self.turbs_arrays, **self.k3, numq=NUMQ, dx=cfg.dx, dy=cfg.dy, dz=cfg.dz, dt=cfg.dt, stream=st)
         mo.held_compose(self.held_arrays, **self.k3, dt=self.cfg.dt, stream=st)
 
     def pre_acoustic(self, nrk: int) -> None:

@@ -235,3 +235,150 @@ def launch_cuda_dissipative_heating(arrays: Mapping[str, Any], *, ni: int, nj: i
         lib._diss_bound = True
     return _launch(a, lib.gm1b_dissipative_heating, (ni, nj, nk, ctypes.byref(s)), "gm1b_dissipative_heating",
                    {"stream": stream, "receipt": {"operator": "dissipative-heating", "cell_words": ni * nj * nk}})
+
+
+# ------------------------------------------------------- the terrain texts
+# The uniform column's family: the strain of cpu_terrain_deformation_inplace
+# (src/cm1core/cuda_terrain_deformation.py:234-736), gettau and turbu/turbv/
+# turbw of cpu_sgs_stress_tendency_inplace
+# (src/cm1core/cuda_sgs_stress_tendency.py:292-449), turbs of
+# cpu_gm1_scalar_turbulence_inplace
+# (src/cm1core/cuda_gm1_scalar_turbulence.py:230-430) - kernels in
+# csrc/stress_terrain.cu.
+
+TERRAIN_METRIC_NAMES = ("gz", "rgz", "gzu", "rgzu", "gzv", "rgzv", "gx", "gy", "gxu", "gyv")
+_TERRAIN_FIELDS = ("u3d", "v3d", "w3d", "rho", "rf", "mh", "mf", "kmh", "kmv") + TERRAIN_METRIC_NAMES + \
+    STRAIN_NAMES + TAU_NAMES + ("uten", "vten", "wten")
+TERRAIN_STRAIN_ARRAY_NAMES = ("u3d", "v3d", "w3d", "rho", "rf", "gz", "rgz", "rgzu", "rgzv", "gx", "gy") + \
+    STRAIN_NAMES
+TERRAIN_STRESS_ARRAY_NAMES = STRAIN_NAMES + TAU_NAMES + ("kmh", "kmv", "rho", "rf", "mh", "mf", "gz", "rgz", "gzu",
+                                                         "rgzu", "gzv", "rgzv", "gxu", "gyv", "u3d", "v3d", "w3d",
+                                                         "uten", "vten", "wten")
+TERRAIN_SGS_STRESS_ARRAY_NAMES = tuple(dict.fromkeys(TERRAIN_STRAIN_ARRAY_NAMES + TERRAIN_STRESS_ARRAY_NAMES))
+TERRAIN_SCALAR_TURBULENCE_ARRAY_NAMES = ("th0", "tha", "qa", "rho", "rr", "rf", "mh", "mf", "khh", "khv", "gz",
+                                         "rgz", "rgzu", "rgzv", "gx", "gxu", "gy", "gyv", "thten1", "qten",
+                                         "workspace")
+
+
+class _TerrainArrays(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_void_p) for n in _TERRAIN_FIELDS]
+
+
+class _TerrainTurbsArrays(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_void_p) for n in ("th0", "tha", "qa", "rho", "rr", "rf", "mh", "mf", "khh", "khv",
+                                               "gz", "rgz", "rgzu", "rgzv", "gx", "gxu", "gy", "gyv", "thten",
+                                               "qten", "workspace")]
+
+
+def terrain_metric_shapes(ni: int, nj: int, nk: int) -> dict[str, tuple[int, ...]]:
+    face = (nk + 1, nj, ni)
+    return {"gz": (nj, ni), "rgz": (nj, ni), "gzu": (nj, ni + 1), "rgzu": (nj, ni + 1), "gzv": (nj + 1, ni),
+            "rgzv": (nj + 1, ni), "gx": face, "gy": face, "gxu": (nk + 1, nj, ni + 1), "gyv": (nk + 1, nj + 1, ni)}
+
+
+def terrain_stress_shapes(ni: int, nj: int, nk: int) -> dict[str, tuple[int, ...]]:
+    shapes = {n: s for n, s in flat_stress_shapes(ni, nj, nk).items() if n != "mh_profile"}
+    shapes.update(terrain_metric_shapes(ni, nj, nk))
+    return shapes
+
+
+def _bind_terrain(lib) -> None:
+    if getattr(lib, "_terrain_stress_bound", False):
+        return
+    i32, f32, vp = ctypes.c_int32, ctypes.c_float, ctypes.c_void_p
+    a = ctypes.POINTER(_TerrainArrays)
+    lib.gm1b_terrain_strain.argtypes = [i32, i32, i32, a, f32, f32, f32, vp]
+    lib.gm1b_terrain_stress.argtypes = [i32, i32, i32, a, f32, f32, f32, f32, vp]
+    lib.gm1b_terrain_sgs_stress.argtypes = [i32, i32, i32, a, f32, f32, f32, f32, vp]
+    lib.gm1b_terrain_scalar_turbulence.argtypes = [i32, i32, i32, i32, ctypes.POINTER(_TerrainTurbsArrays), f32, f32,
+                                                   f32, f32, vp]
+    lib.gm1b_terrain_scalar_turbulence_workspace_words.argtypes = [i32, i32, i32, i32]
+    lib.gm1b_terrain_scalar_turbulence_workspace_words.restype = ctypes.c_int64
+    for n in ("gm1b_terrain_strain", "gm1b_terrain_stress", "gm1b_terrain_sgs_stress",
+              "gm1b_terrain_scalar_turbulence"):
+        getattr(lib, n).restype = i32
+    lib._terrain_stress_bound = True
+
+
+def _prepare_terrain(arrays: Mapping[str, Any], names, ni, nj, nk, what):
+    _grid(ni, nj, nk)
+    if nk > MAX_NK:
+        raise ValueError(f"nk must be <= {MAX_NK} (the column solves' shared memory)")
+    a = _require(arrays, names, terrain_stress_shapes(ni, nj, nk), what)
+    s = _TerrainArrays(**{n: (a[n].data_ptr() if n in a else None) for n in _TERRAIN_FIELDS})
+    lib = _native.lib()
+    _bind_terrain(lib)
+    return a, s, lib
+
+
+def launch_cuda_terrain_strain(arrays: Mapping[str, Any], *, ni: int, nj: int, nk: int, dx: float, dy: float,
+                               dz: float, stream: Any | None = None) -> CudaLaunch:
+    """The strain carriers rho*Sij of the terrain calcdef: s11/s22/s33 at
+    cells, s12 at every corner, s13/s23 on face levels 1..nk-1."""
+    dx, dy, dz = _positive("dx", dx), _positive("dy", dy), _positive("dz", dz)
+    a, s, lib = _prepare_terrain(arrays, TERRAIN_STRAIN_ARRAY_NAMES, ni, nj, nk, "terrain-strain")
+    return _launch(a, lib.gm1b_terrain_strain, (ni, nj, nk, ctypes.byref(s), dx, dy, dz), "gm1b_terrain_strain",
+                   {"stream": stream, "receipt": {"operator": "terrain-strain"}})
+
+
+def launch_cuda_terrain_stress(arrays: Mapping[str, Any], *, ni: int, nj: int, nk: int, dx: float, dy: float,
+                               dz: float, dt: float, stream: Any | None = None) -> CudaLaunch:
+    """gettau and turbu/turbv/turbw of the terrain texts (four open sides,
+    implicit vertical solves, free-slip bottom and top), the stress ADDED
+    into uten/vten/wten (wten on faces 1..nk-1)."""
+    dx, dy, dz, dt = _positive("dx", dx), _positive("dy", dy), _positive("dz", dz), _positive("dt", dt)
+    a, s, lib = _prepare_terrain(arrays, TERRAIN_STRESS_ARRAY_NAMES, ni, nj, nk, "terrain-stress")
+    return _launch(a, lib.gm1b_terrain_stress, (ni, nj, nk, ctypes.byref(s), dx, dy, dz, dt), "gm1b_terrain_stress",
+                   {"stream": stream, "receipt": {"operator": "terrain-stress"}})
+
+
+def launch_cuda_terrain_sgs_stress(arrays: Mapping[str, Any], *, ni: int, nj: int, nk: int, dx: float, dy: float,
+                                   dz: float, dt: float, stream: Any | None = None) -> CudaLaunch:
+    """The terrain strain carriers, gettau and the momentum stress in that
+    order (cpu_sgs_stress_tendency_inplace with the strain its calcdef
+    left)."""
+    dx, dy, dz, dt = _positive("dx", dx), _positive("dy", dy), _positive("dz", dz), _positive("dt", dt)
+    a, s, lib = _prepare_terrain(arrays, TERRAIN_SGS_STRESS_ARRAY_NAMES, ni, nj, nk, "terrain-sgs-stress")
+    return _launch(a, lib.gm1b_terrain_sgs_stress, (ni, nj, nk, ctypes.byref(s), dx, dy, dz, dt),
+                   "gm1b_terrain_sgs_stress", {"stream": stream, "receipt": {"operator": "terrain-sgs-stress"}})
+
+
+def terrain_scalar_turbulence_workspace(ni: int, nj: int, nk: int, numq: int, device) -> torch.Tensor:
+    """The device scratch launch_cuda_terrain_scalar_turbulence takes as
+    ``workspace``: the x and y fluxes of each of the 1 + numq scalars."""
+    return torch.empty((numq + 1) * (nk * nj * (ni + 1) + nk * (nj + 1) * ni), dtype=torch.float32, device=device)
+
+
+def launch_cuda_terrain_scalar_turbulence(arrays: Mapping[str, Any], *, ni: int, nj: int, nk: int, numq: int,
+                                          dx: float, dy: float, dz: float, dt: float,
+                                          stream: Any | None = None) -> CudaLaunch:
+    """turbs on the terrain texts: theta ((th0 - 300) + tha) into
+    ``thten1``, then moisture rows 0..numq-1 of ``qa`` into those of
+    ``qten`` (added); the x/y fluxes with their terrain terms, the implicit
+    vertical diffusion with khv, zero surface flux.  ``qa``/``qten`` may
+    hold more rows than numq; ``workspace`` is
+    terrain_scalar_turbulence_workspace()'s scratch."""
+    if isinstance(numq, bool) or not isinstance(numq, int) or not 0 <= numq <= 6:
+        raise ValueError("numq must be an integer in 0..6")
+    dx, dy, dz, dt = _positive("dx", dx), _positive("dy", dy), _positive("dz", dz), _positive("dt", dt)
+    _grid(ni, nj, nk)
+    if nk > MAX_NK:
+        raise ValueError(f"nk must be <= {MAX_NK} (the column solve's shared memory)")
+    shapes = {n: s for n, s in flat_scalar_turbulence_shapes(ni, nj, nk, numq).items()}
+    shapes.update(terrain_metric_shapes(ni, nj, nk))
+    shapes["workspace"] = ((numq + 1) * (nk * nj * (ni + 1) + nk * (nj + 1) * ni),)
+    for n in ("qa", "qten"):
+        t = arrays.get(n)
+        if isinstance(t, torch.Tensor) and t.dim() == 4 and t.shape[0] >= numq:
+            shapes[n] = tuple(t.shape)
+    a = _require(arrays, TERRAIN_SCALAR_TURBULENCE_ARRAY_NAMES, shapes, "terrain-scalar-turbulence")
+    if tuple(a["qa"].shape[1:]) != (nk, nj, ni) or tuple(a["qten"].shape[1:]) != (nk, nj, ni):
+        raise ValueError("qa and qten must hold rows of shape (nk, nj, ni)")
+    s = _TerrainTurbsArrays(**{f: a["thten1" if f == "thten" else f].data_ptr()
+                               for f, _ in _TerrainTurbsArrays._fields_})
+    lib = _native.lib()
+    _bind_terrain(lib)
+    return _launch(a, lib.gm1b_terrain_scalar_turbulence, (ni, nj, nk, numq, ctypes.byref(s), dx, dy, dz, dt),
+                   "gm1b_terrain_scalar_turbulence",
+                   {"stream": stream, "receipt": {"operator": "terrain-scalar-turbulence", "scalars": 1 + numq,
+                                                  "cell_words": ni * nj * nk}})

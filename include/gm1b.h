@@ -920,6 +920,72 @@ GM1B_API int32_t gm1b_flat_scalar_turbulence(int32_t ni, int32_t nj, int32_t nk,
                                              const gm1b_flat_scalar_turbulence_arrays *arrays, float dx, float dy,
                                              float dz, float dt, void *stream);
 
+/* The terrain texts' stress (the uniform column's family): compact arrays,
+ * shapes as gm1b_flat_stress_arrays, plus the column metrics gz/rgz (nj,
+ * ni), gzu/rgzu (nj, ni+1), gzv/rgzv (nj+1, ni) and the slopes gx/gy (nk+1,
+ * nj, ni), gxu (nk+1, nj, ni+1), gyv (nk+1, nj+1, ni). */
+typedef struct gm1b_terrain_stress_arrays {
+    const float *u3d, *v3d, *w3d, *rho, *rf, *mh, *mf, *kmh, *kmv;
+    const float *gz, *rgz, *gzu, *rgzu, *gzv, *rgzv, *gx, *gy, *gxu, *gyv;
+    float *s11, *s22, *s33, *s12, *s13, *s23;
+    float *t11, *t22, *t33, *t12, *t13, *t23;
+    float *uten, *vten, *wten;
+} gm1b_terrain_stress_arrays;
+
+/*
+ * The strain carriers rho*Sij of the terrain calcdef: s11/s22/s33 at cells,
+ * s12 at every corner (an open side takes the nearest interior corner),
+ * s13/s23 on face levels 1..nk-1.  Reads u3d, v3d, w3d, rho, rf, gz, rgz,
+ * rgzu, rgzv, gx, gy.  Replaces the strain half of
+ * cpu_terrain_deformation_inplace
+ * (src/cm1core/cuda_terrain_deformation.py:234-736).
+ */
+GM1B_API int32_t gm1b_terrain_strain(int32_t ni, int32_t nj, int32_t nk, const gm1b_terrain_stress_arrays *arrays,
+                                     float dx, float dy, float dz, void *stream);
+
+/*
+ * CM1 gettau (t13/t23 levels 0 and nk copy levels 1 and nk-1, the eight-kmh
+ * t12 at the clamped corner columns) and turbu/turbuz, turbv/turbvz and
+ * turbw on the terrain texts with their implicit vertical solves (doimpl =
+ * 1, four open sides, free-slip bottom and top), ADDED into uten, vten and
+ * wten (wten on faces 1..nk-1).  nk <= 200.  Replaces
+ * cpu_sgs_stress_tendency_inplace and its kernels
+ * (src/cm1core/cuda_sgs_stress_tendency.py:292-449).
+ */
+GM1B_API int32_t gm1b_terrain_stress(int32_t ni, int32_t nj, int32_t nk, const gm1b_terrain_stress_arrays *arrays,
+                                     float dx, float dy, float dz, float dt, void *stream);
+
+/* gm1b_terrain_strain then gm1b_terrain_stress on one stream. */
+GM1B_API int32_t gm1b_terrain_sgs_stress(int32_t ni, int32_t nj, int32_t nk,
+                                         const gm1b_terrain_stress_arrays *arrays, float dx, float dy, float dz,
+                                         float dt, void *stream);
+
+/* As gm1b_flat_scalar_turbulence_arrays with the terrain column metrics of
+ * gm1b_terrain_stress_arrays (gz, rgz, rgzu, rgzv, gx, gxu, gy, gyv) and
+ * gm1b_terrain_scalar_turbulence_workspace_words() words of workspace (the
+ * x and y fluxes of every scalar). */
+typedef struct gm1b_terrain_scalar_turbulence_arrays {
+    const float *th0, *tha, *qa, *rho, *rr, *rf, *mh, *mf, *khh, *khv;
+    const float *gz, *rgz, *rgzu, *rgzv, *gx, *gxu, *gy, *gyv;
+    float *thten, *qten, *workspace;
+} gm1b_terrain_scalar_turbulence_arrays;
+
+/* Words of the terrain scalar turbulence's workspace:
+ * (numq + 1)*(nk*nj*(ni+1) + nk*(nj+1)*ni). */
+GM1B_API int64_t gm1b_terrain_scalar_turbulence_workspace_words(int32_t ni, int32_t nj, int32_t nk, int32_t numq);
+
+/*
+ * CM1 turbs on the terrain texts for theta ((th0 - 300) + tha) and moisture
+ * rows 0..numq-1 (numq <= 6): the x/y fluxes with their terrain terms, the
+ * implicit vertical diffusion with khv, zero surface flux; ADDED into thten
+ * and the first numq rows of qten.  nk <= 200.  Replaces
+ * cpu_gm1_scalar_turbulence_inplace and its kernels
+ * (src/cm1core/cuda_gm1_scalar_turbulence.py:230-430, :453-510).
+ */
+GM1B_API int32_t gm1b_terrain_scalar_turbulence(int32_t ni, int32_t nj, int32_t nk, int32_t numq,
+                                                const gm1b_terrain_scalar_turbulence_arrays *arrays, float dx,
+                                                float dy, float dz, float dt, void *stream);
+
 /* tauh/taus (nk, nj+2, ni+2) and tauf (nk+1, nj+2, ni+2) with one
  * horizontal halo, or (profiles = 1) tauh/taus (nk) and tauf (nk+1)
  * columns; u0/v0 (nk); ua/uten1 (nk, nj, ni+1); va/vten1 (nk, nj+1, ni);

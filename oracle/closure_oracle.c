@@ -39,22 +39,19 @@ static float atw(const float* q, int kf, int j, int i, int nk, int ny, int nx) {
   return 0.5f * (q[I3(kf - 1, j, i, ny, nx)] + q[I3(kf, j, i, ny, nx)]);
 }
 
-int oracle_calcdef(int ni, int nj, int nk, const float* u, const float* v, const float* w, const float* rho,
-                   const float* rf, const float* c1, const float* c2, const float* gz, const float* rgz,
-                   const float* rgzu, const float* rgzv, const float* gx, const float* gy, float dx, float dy,
-                   float dz, float* defv, float* defh) {
+/* the six strain carriers rho*Sij of the terrain calcdef (its mass and face
+ * passes, cpu_terrain_deformation_inplace): s11/s22/s33 (nk, nj, ni), s12
+ * (nk, nj+1, ni+1) at every corner from the nearest interior corner, s13
+ * (nk+1, nj, ni+1) and s23 (nk+1, nj+1, ni) on face levels 1..nk-1 (levels
+ * 0 and nk left as they are) */
+int oracle_terrain_strain(int ni, int nj, int nk, const float* u, const float* v, const float* w, const float* rho,
+                          const float* rf, const float* gz, const float* rgz, const float* rgzu, const float* rgzv,
+                          const float* gx, const float* gy, float dx, float dy, float dz, float* s11, float* s22,
+                          float* s33, float* s12, float* s13, float* s23) {
   if (ni < 3 || nj < 3 || nk < 3) return -1;
   const float rdx = 1.0f / dx, rdy = 1.0f / dy, rds = 1.0f / dz;
   const float half = 0.5f, quarter = 0.25f;
   const float zt = (float)nk * dz;
-  const int64_t ncell = (int64_t)nk * nj * ni;
-  float* s11 = calloc(ncell, sizeof(float));
-  float* s22 = calloc(ncell, sizeof(float));
-  float* s33 = calloc(ncell, sizeof(float));
-  float* s12 = calloc((int64_t)nk * (nj + 1) * (ni + 1), sizeof(float));
-  float* s13 = calloc((int64_t)(nk + 1) * nj * (ni + 1), sizeof(float));
-  float* s23 = calloc((int64_t)(nk + 1) * (nj + 1) * ni, sizeof(float));
-  if (!s11 || !s22 || !s33 || !s12 || !s13 || !s23) return -2;
   const int ux = ni + 1, vy = nj + 1;
   for (int k = 0; k < nk; ++k) {
     const float sig_lo = (float)k * dz, sig_hi = (float)(k + 1) * dz;
@@ -137,6 +134,25 @@ int oracle_calcdef(int ni, int nj, int nk, const float* u, const float* v, const
       }
     }
   }
+  return 0;
+}
+
+int oracle_calcdef(int ni, int nj, int nk, const float* u, const float* v, const float* w, const float* rho,
+                   const float* rf, const float* c1, const float* c2, const float* gz, const float* rgz,
+                   const float* rgzu, const float* rgzv, const float* gx, const float* gy, float dx, float dy,
+                   float dz, float* defv, float* defh) {
+  if (ni < 3 || nj < 3 || nk < 3) return -1;
+  const float half = 0.5f, quarter = 0.25f;
+  const int64_t ncell = (int64_t)nk * nj * ni;
+  float* s11 = calloc(ncell, sizeof(float));
+  float* s22 = calloc(ncell, sizeof(float));
+  float* s33 = calloc(ncell, sizeof(float));
+  float* s12 = calloc((int64_t)nk * (nj + 1) * (ni + 1), sizeof(float));
+  float* s13 = calloc((int64_t)(nk + 1) * nj * (ni + 1), sizeof(float));
+  float* s23 = calloc((int64_t)(nk + 1) * (nj + 1) * ni, sizeof(float));
+  if (!s11 || !s22 || !s33 || !s12 || !s13 || !s23) return -2;
+  oracle_terrain_strain(ni, nj, nk, u, v, w, rho, rf, gz, rgz, rgzu, rgzv, gx, gy, dx, dy, dz, s11, s22, s33, s12, s13,
+                        s23);
   for (int j = 0; j < nj; ++j)
     for (int i = 0; i < ni; ++i) {
       defv[I3(0, j, i, nj, ni)] = 0.0f;

@@ -41,6 +41,9 @@ def theta_weps() -> float:
     return float(np.float32(np.float32(10.0) * np.float32(EPS)))
 
 
+# the column metrics the terrain texts of the SGS stress and turbs read
+TERRAIN_METRICS = ("gz", "rgz", "gzu", "rgzu", "gzv", "rgzv", "gx", "gy", "gxu", "gyv")
+
 class OracleMoistStep:
     def __init__(self, cfg, state: dict[str, np.ndarray], metrics: dict[str, np.ndarray]) -> None:
         self.cfg, self.s, self.m = cfg, state, metrics
@@ -67,14 +70,13 @@ class OracleMoistStep:
         self.flat = getattr(cfg, "column", None) is not None
         # the SGS stress and scalar diffusion held tendencies (gettau +
         # turbu/turbv/turbw and turbs of the closure's held phase,
-        # cuda_cartesian_closure.py:1268-1291): built for the flat family
-        # the stretched column runs
+        # cuda_cartesian_closure.py:1268-1291): the flat texts on a
+        # stretched column, the terrain texts (cpu_sgs_stress_tendency_inplace,
+        # cpu_gm1_scalar_turbulence_inplace) on the uniform one
         self.sgs_diffusion = bool(getattr(cfg, "sgs_diffusion", False))
         # CM1's upper Rayleigh damping (irdamp = 1, solve1.F:412-454), its
         # coefficients and base-state winds from the metrics
         self.rayleigh = bool(getattr(cfg, "rayleigh", False))
-        if self.sgs_diffusion and not self.flat:
-            raise ValueError("the SGS diffusion is built for the stretched column's flat operator family only")
         if self.sgs_diffusion or self.rayleigh:
             self.stress = ost.zeros(cfg.ni, cfg.nj, cfg.nk, ost.STRAIN_NAMES + ost.TAU_NAMES + ost.TENDENCY_NAMES)
         if self.flat:
@@ -128,8 +130,11 @@ class OracleMoistStep:
         for n in ost.TENDENCY_NAMES:
             st[n][:] = 0
         a = {"u3d": s["uc"], "v3d": s["vc"], "w3d": s["wc"], "rho": s["rho"], "rf": s["rf"], "mh": m["mh"],
-             "mf": m["mf"], "mh_profile": m["mh_profile"], "kmh": s["kmh"], "kmv": s["kmv"], **st}
-        ost.flat_sgs_stress(a, **self.hx, rdz=self.rdz, dt=c.dt)
+             "mf": m["mf"], "kmh": s["kmh"], "kmv": s["kmv"], **st}
+        if self.flat:
+            ost.flat_sgs_stress({**a, "mh_profile": m["mh_profile"]}, **self.hx, rdz=self.rdz, dt=c.dt)
+        else:
+            ost.terrain_sgs_stress({**a, **{n: m[n] for n in TERRAIN_METRICS}}, **self.grid, dt=c.dt)
 
     def _tke(self):
         s, m = self.s, self.m
@@ -160,7 +165,11 @@ class OracleMoistStep:
             a = {"th0": s["th0"], "tha": s["tha"], "qa": s["qa"], "rho": s["rho"], "rr": s["rr"], "rf": s["rf"],
                  "mh": m["mh"], "mf": m["mf"], "khh": s["khh"], "khv": s["khv"], "thten1": s["thheld"],
                  "qten": s["qheld"]}
-            ost.flat_scalar_turbulence(a, **self.hx, numq=s["qheld"].shape[0], dz=c.dz, dt=c.dt)
+            if self.flat:
+                ost.flat_scalar_turbulence(a, **self.hx, numq=s["qheld"].shape[0], dz=c.dz, dt=c.dt)
+            else:
+                ost.terrain_scalar_turbulence({**a, **{n: m[n] for n in TERRAIN_METRICS}}, **self.grid,
+                                              numq=s["qheld"].shape[0], dt=c.dt)
         oms.held_compose({"th0": s["th0_3d"], "pi0": s["pi0_3d"], "rho": s["rho"], "ppi": s["pp3d_c"],
                           "tha": s["tha"], "qa": s["qa"], "qpten": s["qpten"], "qtten": s["qtten"],
                           "qvten": s["qvten"], "qcten": s["qcten"], "thheld": s["thheld"], "qheld": s["qheld"],

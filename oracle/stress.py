@@ -1,8 +1,12 @@
-"""ctypes driver of the flat-column SGS stress oracle (stress_oracle.c and
-the strain passes of closure_oracle.c) - TEST INFRASTRUCTURE ONLY.
-Restates enqueue_flat_calcdef's strain passes, enqueue_flat_gettau and
-enqueue_flat_momentum_stress (src/cm1core/cuda_gm1_flat_stretched_closure.py:
-76-114, :134-292, :524-618)."""
+"""ctypes driver of the SGS stress oracles (stress_oracle.c,
+stress_terrain_oracle.c and the strain passes of closure_oracle.c) - TEST
+INFRASTRUCTURE ONLY.  Restates enqueue_flat_calcdef's strain passes,
+enqueue_flat_gettau and enqueue_flat_momentum_stress
+(src/cm1core/cuda_gm1_flat_stretched_closure.py:76-114, :134-292, :524-618)
+and, for the uniform column's terrain texts, the twins
+cpu_sgs_stress_tendency_inplace (src/cm1core/cuda_sgs_stress_tendency.py:292)
+and cpu_gm1_scalar_turbulence_inplace
+(src/cm1core/cuda_gm1_scalar_turbulence.py:230)."""
 
 from __future__ import annotations
 
@@ -154,3 +158,61 @@ def dissipative_heating(a, *, ni, nj, nk) -> None:
     rc = lib.oracle_dissipative_heating(ni, nj, nk, *(_p(a[n]) for n in ("dissten", "pi0", "ppi", "qa", "thten1")))
     if rc != 0:
         raise ValueError(f"oracle_dissipative_heating failed ({rc})")
+
+
+# --------------------------------------------------- the terrain texts
+TERRAIN_STRAIN_INPUTS = ("u3d", "v3d", "w3d", "rho", "rf", "gz", "rgz", "rgzu", "rgzv", "gx", "gy")
+TERRAIN_MOMENTUM_INPUTS = TAU_NAMES + ("kmh", "kmv", "rho", "rf", "mh", "mf", "gz", "rgz", "gzu", "rgzu", "gzv",
+                                       "rgzv", "gxu", "gyv", "u3d", "v3d", "w3d")
+TERRAIN_TURBS_INPUTS = ("th0", "tha", "qa", "rho", "rr", "rf", "mh", "mf", "khh", "khv", "gz", "rgz", "rgzu",
+                        "rgzv", "gx", "gxu", "gy", "gyv")
+
+
+def _terrain_lib():
+    lib = load()
+    if not getattr(lib, "_terrain_stress_ready", False):
+        i, f = ctypes.c_int, C_REAL
+        lib.oracle_terrain_strain.argtypes = [i, i, i] + [_F] * 11 + [f, f, f] + [_F] * 6
+        lib.oracle_terrain_strain.restype = i
+        lib.oracle_terrain_gettau.argtypes = [i, i, i] + [_F] * 14
+        lib.oracle_terrain_gettau.restype = i
+        lib.oracle_terrain_momentum_stress.argtypes = [i, i, i] + [_F] * 23 + [f, f, f, f] + [_F] * 3
+        lib.oracle_terrain_momentum_stress.restype = i
+        lib.oracle_terrain_scalar_turbulence.argtypes = [i, i, i, i] + [_F] * 18 + [f, f, f, f, _F, _F]
+        lib.oracle_terrain_scalar_turbulence.restype = i
+        lib._terrain_stress_ready = True
+    return lib
+
+
+def terrain_strain(a, *, ni, nj, nk, dx, dy, dz) -> None:
+    rc = _terrain_lib().oracle_terrain_strain(ni, nj, nk, *(_p(a[n]) for n in TERRAIN_STRAIN_INPUTS), dx, dy, dz,
+                                              *(_p(a[n]) for n in STRAIN_NAMES))
+    if rc != 0:
+        raise ValueError(f"oracle_terrain_strain failed ({rc})")
+
+
+def terrain_gettau(a, *, ni, nj, nk) -> None:
+    rc = _terrain_lib().oracle_terrain_gettau(ni, nj, nk, *(_p(a[n]) for n in STRAIN_NAMES), _p(a["kmh"]),
+                                              _p(a["kmv"]), *(_p(a[n]) for n in TAU_NAMES))
+    if rc != 0:
+        raise ValueError(f"oracle_terrain_gettau failed ({rc})")
+
+
+def terrain_momentum_stress(a, *, ni, nj, nk, dx, dy, dz, dt) -> None:
+    rc = _terrain_lib().oracle_terrain_momentum_stress(ni, nj, nk, *(_p(a[n]) for n in TERRAIN_MOMENTUM_INPUTS), dx, dy,
+                                                       dz, dt, *(_p(a[n]) for n in TENDENCY_NAMES))
+    if rc != 0:
+        raise ValueError(f"oracle_terrain_momentum_stress failed ({rc})")
+
+
+def terrain_sgs_stress(a, *, ni, nj, nk, dx, dy, dz, dt) -> None:
+    terrain_strain(a, ni=ni, nj=nj, nk=nk, dx=dx, dy=dy, dz=dz)
+    terrain_gettau(a, ni=ni, nj=nj, nk=nk)
+    terrain_momentum_stress(a, ni=ni, nj=nj, nk=nk, dx=dx, dy=dy, dz=dz, dt=dt)
+
+
+def terrain_scalar_turbulence(a, *, ni, nj, nk, numq, dx, dy, dz, dt) -> None:
+    rc = _terrain_lib().oracle_terrain_scalar_turbulence(ni, nj, nk, numq, *(_p(a[n]) for n in TERRAIN_TURBS_INPUTS),
+                                                         dx, dy, dz, dt, _p(a["thten1"]), _p(a["qten"]))
+    if rc != 0:
+        raise ValueError(f"oracle_terrain_scalar_turbulence failed ({rc})")

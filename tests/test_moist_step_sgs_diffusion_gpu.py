@@ -16,7 +16,8 @@ vertical diffusion forms (solution - w)/dt, a difference of nearly equal
 words, so w carries the libm ulps of the closure further than the other
 fields do); the C entry point gives the Python composition's words; the
 diffusion and the damping move the state; on the uniform column the damping
-and the heating match too, and the SGS diffusion is refused."""
+and the heating match too, and so does the SGS diffusion on the terrain
+texts."""
 
 from __future__ import annotations
 
@@ -26,7 +27,6 @@ import numpy as np
 import pytest
 import torch
 
-from gm1_b200.errors import CM1Refusal
 from gm1_b200.moist_step import (SUPERCELL_STRETCHED_COLUMN, MoistLargeStep, MoistStepConfig, NativeMoistLargeStep,
                                  StretchedColumnSpec, upload, weisman_klemp_initial_state)
 from oracle.moist_composition import OracleMoistStep
@@ -129,12 +129,14 @@ def _uniform(**kw):
     return cfg, host, metrics
 
 
-def test_uniform_column_damping_and_heating_match_the_oracle():
+@pytest.mark.parametrize("sgs", [False, True])
+def test_uniform_column_held_closure_matches_the_oracle(sgs):
     """The damping and the dissipative heating do not depend on the column
-    family: on the uniform column (configuration 2's terrain family) the
-    first step's held tendencies match the oracle's and the C entry point
-    gives the Python composition's words."""
-    cfg, host, metrics = _uniform(rayleigh=True, dissipative_heating=True)
+    family, and the SGS stress and turbs run the terrain texts there: on
+    the uniform column (configuration 2's terrain family) the first step's
+    held tendencies match the oracle's and the C entry point gives the
+    Python composition's words."""
+    cfg, host, metrics = _uniform(sgs_diffusion=sgs, rayleigh=True, dissipative_heating=True)
     dev = MoistLargeStep(cfg, upload(host), upload(metrics))
     ref = OracleMoistStep(cfg, {k: v.copy() for k, v in host.items()}, {k: v.copy() for k, v in metrics.items()})
     nat = NativeMoistLargeStep(cfg, upload(host), upload(metrics), concurrent=True)
@@ -146,16 +148,11 @@ def test_uniform_column_damping_and_heating_match_the_oracle():
         g, r = dev.stress[n].cpu().numpy().astype(np.float64), ref.stress[n].astype(np.float64)
         assert np.max(np.abs(r)) > 0.0, n
         assert np.max(np.abs(g - r)) <= 1e-5 * np.max(np.abs(r)), n
-    g, r = dev.s["thheld"].cpu().numpy().astype(np.float64), ref.s["thheld"].astype(np.float64)
-    assert np.max(np.abs(g - r)) <= 1e-5 * np.max(np.abs(r))
+    for n in ("thheld",) + (("qheld",) if sgs else ()):
+        g, r = dev.s[n].cpu().numpy().astype(np.float64), ref.s[n].astype(np.float64)
+        assert np.max(np.abs(r)) > 0.0, n
+        assert np.max(np.abs(g - r)) <= 1e-5 * np.max(np.abs(r)), n
     bad = [n for n in COMPARED
            if not np.array_equal(dev.s[n].cpu().numpy().view(np.uint8), nat.s[n].cpu().numpy().view(np.uint8))]
     assert bad == []
     nat.close()
-
-
-def test_a_uniform_column_refuses_the_sgs_diffusion():
-    cfg = MoistStepConfig(24, 20, 16, 1000.0, 1000.0, 250.0, 5.0, 10, sgs_diffusion=True)
-    host, metrics = weisman_klemp_initial_state(cfg, seed=3, bubble_radius_m=(6000.0, 1400.0))
-    with pytest.raises(CM1Refusal):
-        MoistLargeStep(cfg, upload(host), upload(metrics))

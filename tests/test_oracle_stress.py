@@ -265,3 +265,29 @@ def test_flat_stress_and_turbs_are_the_reference_texts_word_for_word(tag):
     ost.flat_scalar_turbulence(b, ni=ni, nj=nj, nk=nk, numq=3, dx=dx, dy=dy, dz=dz, dt=dt)
     for n in ("thten1", "qten"):
         assert np.array_equal(b[n].view(np.uint32), z["out_" + n].view(np.uint32)), n
+
+
+# ------------------------------------------------------ the terrain texts
+# The uniform column runs the terrain texts (gettau, turbu/turbv/turbw,
+# turbs) the twins state: the restatements give their words bit for bit.
+@pytest.mark.parametrize("tag", CASES)
+def test_terrain_stress_is_the_twin_word_for_word(tag):
+    meta, inp, out = _load(tag)
+    ni, nj, nk = meta["ni"], meta["nj"], meta["nk"]
+    a = {k: np.ascontiguousarray(v).copy() for k, v in inp.items()}
+    ost.terrain_gettau(a, ni=ni, nj=nj, nk=nk)
+    ost.terrain_momentum_stress(a, ni=ni, nj=nj, nk=nk, dx=meta["dx"], dy=meta["dy"], dz=meta["dz"], dt=meta["dt"])
+    for n in ost.TAU_NAMES + ost.TENDENCY_NAMES:
+        assert np.array_equal(a[n].view(np.uint32), out[n].view(np.uint32)), n
+    for n in ost.TENDENCY_NAMES:
+        assert np.any(a[n] != inp[n]), n
+
+
+@pytest.mark.parametrize("tag", TURBS_CASES)
+def test_terrain_turbs_is_the_twin_word_for_word(tag):
+    meta, inp, out = _load(tag)
+    a = {k: np.ascontiguousarray(v).copy() for k, v in inp.items()}
+    ost.terrain_scalar_turbulence(a, ni=meta["ni"], nj=meta["nj"], nk=meta["nk"], numq=6, dx=meta["dx"],
+                                  dy=meta["dy"], dz=meta["dz"], dt=meta["dt"])
+    for n in ("thten1", "qten"):
+        assert np.array_equal(a[n].view(np.uint32), out[n].view(np.uint32)), n
