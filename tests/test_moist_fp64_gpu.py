@@ -41,6 +41,12 @@ CASES = {
                                                 rayleigh=True, dissipative_heating=True),
                                dict(seed=7, bubble_radius_m=(1500.0, 800.0), bubble_center_z_m=800.0,
                                     bubble_cloud=1.0e-3, bubble_rain=5.0e-4)),
+    # the uniform column's terrain texts of the stress and turbs, with the
+    # damping layer brought down into its 4 km
+    "uniform-24x20x16-held": (MoistStepConfig(24, 20, 16, 1000.0, 1000.0, 250.0, 5.0, 10, sgs_diffusion=True,
+                                              rayleigh=True, dissipative_heating=True, rayleigh_zd_m=3000.0),
+                              dict(seed=7, bubble_radius_m=(6000.0, 1400.0), bubble_cloud=1.0e-3,
+                                   bubble_rain=5.0e-4)),
 }
 
 
