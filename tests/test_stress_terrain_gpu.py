@@ -71,14 +71,16 @@ def test_terrain_stress_is_the_oracle_word_for_word(ni, nj, nk, seed):
     a = _stress_inputs(ni, nj, nk, seed)
     d = _dev(a)
     ost.terrain_strain(a, ni=ni, nj=nj, nk=nk, dx=DX, dy=DY, dz=DZ)
-    launch_cuda_terrain_strain(d, ni=ni, nj=nj, nk=nk, dx=DX, dy=DY, dz=DZ).synchronize()
+    launch_cuda_terrain_strain(d, ni=ni, nj=nj, nk=nk, dx=DX, dy=DY, dz=DZ)
+    torch.cuda.synchronize()
     # s13/s23 levels 0 and nk are not written by either
     _same(d, a, ("s11", "s22", "s33", "s12"))
     for n in ("s13", "s23"):
         assert np.array_equal(d[n].cpu().numpy()[1:nk].view(np.uint32), a[n][1:nk].view(np.uint32)), n
     ost.terrain_gettau(a, ni=ni, nj=nj, nk=nk)
     ost.terrain_momentum_stress(a, ni=ni, nj=nj, nk=nk, dx=DX, dy=DY, dz=DZ, dt=DT)
-    launch_cuda_terrain_stress(d, ni=ni, nj=nj, nk=nk, dx=DX, dy=DY, dz=DZ, dt=DT).synchronize()
+    launch_cuda_terrain_stress(d, ni=ni, nj=nj, nk=nk, dx=DX, dy=DY, dz=DZ, dt=DT)
+    torch.cuda.synchronize()
     _same(d, a, ost.TAU_NAMES + ("uten", "vten", "wten"))
     assert float(torch.abs(d["uten"] - torch.from_numpy(_stress_inputs(ni, nj, nk, seed)["uten"]).cuda()).max()) > 0
 
@@ -89,7 +91,8 @@ def test_the_chained_terrain_entry_point_is_the_two_passes():
     d1, d2 = _dev(a), _dev(a)
     launch_cuda_terrain_strain(d1, ni=ni, nj=nj, nk=nk, dx=DX, dy=DY, dz=DZ)
     launch_cuda_terrain_stress(d1, ni=ni, nj=nj, nk=nk, dx=DX, dy=DY, dz=DZ, dt=DT)
-    launch_cuda_terrain_sgs_stress(d2, ni=ni, nj=nj, nk=nk, dx=DX, dy=DY, dz=DZ, dt=DT).synchronize()
+    launch_cuda_terrain_sgs_stress(d2, ni=ni, nj=nj, nk=nk, dx=DX, dy=DY, dz=DZ, dt=DT)
+    torch.cuda.synchronize()
     for n in ost.TAU_NAMES + ("uten", "vten", "wten", "s11", "s12"):
         assert torch.equal(d1[n].view(torch.int32), d2[n].view(torch.int32)), n
 
@@ -117,7 +120,8 @@ def test_terrain_turbs_is_the_oracle_word_for_word(ni, nj, nk, numq, seed):
     d["workspace"] = terrain_scalar_turbulence_workspace(ni, nj, nk, numq, d["tha"].device)
     ost.terrain_scalar_turbulence(a, ni=ni, nj=nj, nk=nk, numq=numq, dx=DX, dy=DY, dz=DZ, dt=DT)
     launch_cuda_terrain_scalar_turbulence(d, ni=ni, nj=nj, nk=nk, numq=numq, dx=DX, dy=DY, dz=DZ,
-                                          dt=DT).synchronize()
+                                          dt=DT)
+    torch.cuda.synchronize()
     _same(d, a, ("thten1", "qten"))
     if numq < 6:  # rows past numq untouched
         assert np.array_equal(d["qten"].cpu().numpy()[numq:], _turbs_inputs(ni, nj, nk, seed)["qten"][numq:])
