@@ -198,6 +198,7 @@ __global__ void __launch_bounds__(kCT) flat_turb_uv_kernel(StressArgs a) {
     float cprev = -(cfc * inv), dprev = cfd * inv;
     CP(0) = cprev;
     DP(0) = dprev;
+    #pragma unroll 4
     for (int k = 1; k < K - 1; ++k) {
         rr0 = 1.0f / (0.5f * PAIR(a.rho, k));
         tem = PAIR(a.mh, k) * rr0;
@@ -234,6 +235,7 @@ __global__ void __launch_bounds__(kCT) flat_turb_uv_kernel(StressArgs a) {
     }
     // back substitution, the vertical term and the tendency per level
     float d7_up = 0.0f;
+    #pragma unroll 4
     for (int k = K - 1; k >= 0; --k) {
         if (k < K - 1) sol = CP(k) * sol + DP(k);
         const float rho_p = PAIR(a.rho, k);
@@ -292,6 +294,7 @@ __global__ void __launch_bounds__(kCT) flat_turbw_kernel(StressArgs a) {
     float cprev = -(cfc * inv), dprev = cfd * inv;
     CP(0) = cprev;
     DP(0) = dprev;
+    #pragma unroll 4
     for (int f = 2; f < K - 1; ++f) {
         rrf = PF(a.mf, f) / PF(a.rf, f);
         const float r1 = (((kmh_m + kmh_u) * PF(a.mh, f - 1)) * PF(a.rho, f - 1)) * rrf;
@@ -322,6 +325,7 @@ __global__ void __launch_bounds__(kCT) flat_turbw_kernel(StressArgs a) {
         inv = 1.0f / (cfa * cprev + cfb);
         sol = (cfd - cfa * dprev) * inv;
     }
+    #pragma unroll 4
     for (int f = K - 1; f >= 1; --f) {
         if (f < K - 1) sol = CP(f - 1) * sol + DP(f - 1);
         const float rff = PF(a.rf, f);

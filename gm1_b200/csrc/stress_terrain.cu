@@ -240,6 +240,7 @@ __global__ void __launch_bounds__(kCT) terrain_turb_uv_kernel(TArgs a) {
         DP(0) = cfd * inv;
     }
     float cprev = CP(0), dprev = DP(0);
+    #pragma unroll 4
     for (int k = 1; k < nk - 1; ++k) {
         const float rr0 = 1.0f / (0.5f * PAIR(a.rho, k)), common = PAIR(a.mh, k) * rr0;
         const float r1v = kmv_u * (mf_u * (rf_u * common));
@@ -274,6 +275,7 @@ __global__ void __launch_bounds__(kCT) terrain_turb_uv_kernel(TArgs a) {
     }
     const float g = DIR == 0 ? a.gzu[(unsigned)cy * ux + cx] : a.gzv[(unsigned)cy * ni + cx];
     float cross_up = 0.0f;  // cross(k+1); zero above the top level
+    #pragma unroll 4
     for (int k = nk - 1; k >= 0; --k) {
         if (k < nk - 1) sol = CP(k) * sol + DP(k);
         float cross = 0.0f;
@@ -350,6 +352,7 @@ __global__ void __launch_bounds__(kCT) terrain_turbw_kernel(TArgs a) {
         DP(0) = cfd * inv;
     }
     float cprev = CP(0), dprev = DP(0);
+    #pragma unroll 4
     for (int f = 2; f < nk - 1; ++f) {
         const float rrf = PF(a.mf, f) / PF(a.rf, f);
         const float r1v = (PF(a.kmh, f - 1) + PF(a.kmh, f)) * (PF(a.mh, f - 1) * (PF(a.rho, f - 1) * rrf));
@@ -370,6 +373,7 @@ __global__ void __launch_bounds__(kCT) terrain_turbw_kernel(TArgs a) {
         sol = (cfd - cfa * dprev) * (1.0f / (cfa * cprev + cfb));
     }
     const float g = a.gz[col];
+    #pragma unroll 4
     for (int f = nk - 1; f >= 1; --f) {
         if (f < nk - 1) sol = CP(f - 1) * sol + DP(f - 1);
         const float d1 = 0.25f * ((T13(f + 1, i) + T13(f + 1, i + 1)) + (T13(f, i) + T13(f, i + 1)));
@@ -508,6 +512,7 @@ __global__ void __launch_bounds__(kCT) terrain_turbs_column_kernel(SArgs a) {
         float cprev = (-cfc) * tem, dprev = cfd * tem;
         CP(0) = cprev;
         DP(0) = dprev;
+        #pragma unroll 4
         for (int k = 1; k + 1 < nk; ++k) {
             const float r1 = COEF(k, k);
             r2 = COEF(k + 1, k);
@@ -536,6 +541,7 @@ __global__ void __launch_bounds__(kCT) terrain_turbs_column_kernel(SArgs a) {
             tem = 1.0f / (cfa * cprev + cfb);
             sol = (cfd - cfa * dprev) * tem;
         }
+        #pragma unroll 4
         for (int k = nk - 1; k >= 0; --k) {
             if (k != nk - 1) sol = CP(k) * sol + DP(k);
             const float turbz = (PF(a.rho, k) * (sol - SC(k))) * rdt;
